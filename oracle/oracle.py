@@ -1,0 +1,298 @@
+"""CPU oracle for the finite-difference hot path -- TEST INFRASTRUCTURE ONLY.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` may import this module, and only as the checker or the timed CPU
+baseline; the product (``sweep_b200``) never imports, links or calls it.
+
+It restates, in numpy plus the C kernels of ``fd_oracle.c`` (built by this
+directory's Makefile into ``liboracle_f32.so`` / ``liboracle_f64.so``), the
+reference's compiled ``impl='c'`` path:
+
+* host-side set-up, restated from the reference's Python:
+  ``fd_coefficients`` / ``second_derivative_coefficients_fp32``
+  (``src/sweep/scalars.py:51-93``), ``_build_fd_coefficients``
+  (``src/sweep/propagator/_c.py:1134-1156``), ``setup_pml`` /
+  ``set_cpml_profiles_r`` (``src/sweep/equations/pml.py:157-269``; defaults
+  ``max_vel=4500``, ``pml_freq=25``: ``src/sweep/propagator/base.py:1039-1040``),
+  runtime geometry (``src/sweep/core/geometry.py:23-58``,
+  ``src/sweep/propagator/_c.py:2184-2207``), replicate model padding and its
+  crop adjoint (``src/sweep/utils/torch.py:8-41``);
+* the per-step kernels (see ``fd_oracle.c``).
+
+Pinned against the reference's own outputs: ``tests/golden/*.npz`` were made by
+the reference itself (``tests/golden/make_golden.py``), and
+``tests/test_oracle_golden.py`` checks this oracle against them.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import subprocess
+from fractions import Fraction
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+_LIBS: dict = {}
+
+
+def build() -> None:
+    """Compile the oracle's C kernels (both precisions) with the Makefile."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+def _lib(prec: str):
+    if prec not in _LIBS:
+        path = HERE / f"liboracle_{prec}.so"
+        if not path.exists():
+            build()
+        lib = ctypes.CDLL(str(path))
+        real = ctypes.c_float if prec == "f32" else ctypes.c_double
+        P = ctypes.c_void_p
+        i, l = ctypes.c_int, ctypes.c_longlong
+        geo = [i, i, i, i, i, P, real, real, real, P, P, P, P, P, P, P, P, P, l, i, P, P, i, P]
+        lib.oracle_a2d_tape_len.restype = l
+        lib.oracle_a2d_tape_len.argtypes = [i, i, i, i, i, P]
+        lib.oracle_a2d_forward.restype = i
+        lib.oracle_a2d_forward.argtypes = geo + [P, P]
+        lib.oracle_a2d_backward.restype = i
+        lib.oracle_a2d_backward.argtypes = geo + [P, P, P, P]
+        geo3 = [i, i, i, i, i, i, P, real, real, real, real, P, P,
+                P, P, P, P, P, P, P, P, P, P, l, i, P, P, i, P]
+        if not hasattr(lib, "oracle_a3d_tape_len"):
+            _LIBS[prec] = lib
+            return lib
+        lib.oracle_a3d_tape_len.restype = l
+        lib.oracle_a3d_tape_len.argtypes = [i, i, i, i, i, i, P]
+        lib.oracle_a3d_forward.restype = i
+        lib.oracle_a3d_forward.argtypes = geo3 + [P, P]
+        lib.oracle_a3d_backward.restype = i
+        lib.oracle_a3d_backward.argtypes = geo3 + [P, P, P, P]
+        _LIBS[prec] = lib
+    return _LIBS[prec]
+
+
+# ----------------------------------------------------------------- scalars
+def fd_coefficients(derivative_order: int, accuracy_order: int) -> np.ndarray:
+    """Centred Taylor coefficients of the positive taps (``scalars.py:51-67``)."""
+    n = accuracy_order // 2
+    pts = np.arange(-n, n + 1, dtype=np.float64)
+    mat = np.array([pts ** i for i in range(2 * n + 1)])
+    rhs = np.zeros(2 * n + 1)
+    rhs[derivative_order] = math.factorial(derivative_order)
+    return np.linalg.solve(mat, rhs)[-n:]
+
+
+def second_derivative_coefficients_fp32(order: int):
+    """float32 ``(c0, c)`` with ``c0 + 2 sum(c) == 0`` exactly (``scalars.py:69-93``)."""
+    c = fd_coefficients(2, order)
+    c0 = np.float32(-2 * c.sum())
+    c = c.astype(np.float32)
+    residual = Fraction(float(c0)) + 2 * sum(Fraction(float(x)) for x in c)
+    if residual:
+        c[-1] = np.float32(float(Fraction(float(c[-1])) - residual / 2))
+    return c0, c
+
+
+def fd_tables(M: int):
+    """``(lap, grad)`` float32 tables of length M+1 (``_c.py:1134-1156``)."""
+    c0, c = second_derivative_coefficients_fp32(2 * M)
+    lap = np.zeros(M + 1, np.float32)
+    lap[0] = -c0
+    lap[1:] = c
+    grad = np.zeros(M + 1, np.float32)
+    grad[1:] = fd_coefficients(1, 2 * M).astype(np.float32)
+    return lap, grad
+
+
+# -------------------------------------------------------------------- CPML
+def setup_pml(width, start, max_pml, dt, n, max_vel, pml_freq, r_val=0.001, n_power=2, eps=1e-9):
+    """a, b profiles of one axis in float32 (``pml.py:216-269``)."""
+    dtype = np.float32
+    alpha0 = math.pi * pml_freq
+    if max_pml == 0:
+        return np.zeros(n, dtype), np.zeros(n, dtype)
+    sigma0 = -(1 + n_power) * max_vel * math.log(r_val) / (2 * max_pml)
+    x = np.arange(n, dtype=dtype) + dtype(0.0)
+    f0 = (dtype(start[0]) - x) / dtype(width[0]) if width[0] else np.zeros_like(x)
+    f1 = (x - dtype(start[1])) / dtype(width[1]) if width[1] else np.zeros_like(x)
+    frac = np.clip(np.maximum(f0, f1), 0.0, 1.0)
+    sigma = dtype(sigma0) * (frac ** n_power)
+    alpha = dtype(alpha0) * (dtype(1.0) - frac)
+    sa = sigma + alpha
+    sa = np.where(np.abs(sa) < eps, dtype(eps), sa)
+    a = np.exp(-sa * abs(dt)).astype(dtype, copy=False)
+    b = (sigma / sa) * (a - dtype(1.0))
+    a = a.copy()
+    a[frac == 0] = dtype(0.0)
+    return a, b.astype(dtype, copy=False)
+
+
+def cpml_profiles(pads, M, dt, spacing, shape, max_vel=4500.0, pml_freq=25.0):
+    """Per axis (shape order) ``(a, b, db)`` on the runtime grid (``pml.py:157-214``).
+
+    ``pads``: flat per-face PML widths ``[lo0, hi0, lo1, hi1, ...]``;
+    ``shape``: the runtime shape (physical + 2 pad + 2 M per axis)."""
+    out = []
+    for d, n in enumerate(shape):
+        w = pads[2 * d: 2 * d + 2]
+        start = [float(M + w[0]), float(n - 1 - M - w[1])]
+        max_pml = max(w[0] * spacing[d], w[1] * spacing[d])
+        a, b = setup_pml(w, start, max_pml, dt, n, max_vel, pml_freq)
+        db = np.gradient(b, spacing[d])
+        out.append((a, b, db.astype(np.float32)))
+    return out
+
+
+# ---------------------------------------------------------------- geometry
+def _batch_io(wavelet, src, rec, ndim):
+    """``(B, 1, nt)`` wavelet, ``(B, 1, ndim)`` sources, ``(B, nrec, ndim)`` receivers."""
+    src = np.asarray(src, np.int64).reshape(-1, ndim)
+    B = src.shape[0]
+    w = np.asarray(wavelet, np.float32)
+    if w.ndim == 1:
+        w = np.broadcast_to(w, (B, w.shape[0]))
+    rec = np.asarray(rec, np.int64).reshape(B, -1, ndim)
+    return np.ascontiguousarray(w[:, None, :]), src[:, None, :], rec
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class _Acoustic:
+    """Shared set-up of the 2-D / 3-D acoustic oracle runs."""
+
+    def __init__(self, vp, wavelet, src, rec, dh, dt, abcn, order=8, prec="f32",
+                 max_vel=4500.0, pml_freq=25.0):
+        self.prec = prec
+        self.real = np.float32 if prec == "f32" else np.float64
+        vp = np.asarray(vp, np.float32)
+        self.ndim = 2 if src is not None and np.asarray(src).shape[-1] == 2 else 3
+        nd = self.ndim
+        self.per_shot = vp.ndim == nd + 1
+        self.M = M = order // 2
+        w, s, r = _batch_io(wavelet, src, rec, nd)
+        self.B, self.nt = w.shape[0], w.shape[-1]
+        phys = vp.shape[-nd:]
+        self.phys = phys
+        self.pad = abcn
+        self.shape = tuple(n + 2 * abcn + 2 * M for n in phys)
+        padw = [(abcn + M, abcn + M)] * nd
+        lead = [(0, 0)] if self.per_shot else []
+        self.vp = np.ascontiguousarray(np.pad(vp, lead + padw, mode="edge").astype(self.real))
+        self.vp_stride = int(np.prod(self.shape)) if self.per_shot else 0
+        sp = dh if np.ndim(dh) else [dh] * nd
+        self.spacing = [float(x) for x in sp]
+        self.dt = float(dt)
+        prof = cpml_profiles([abcn] * (2 * nd), M, dt, self.spacing, self.shape, max_vel, pml_freq)
+        self.prof = [tuple(np.ascontiguousarray(x.astype(self.real)) for x in p) for p in prof]
+        lap, grad = fd_tables(M)
+        self.lap, self.grad = lap.astype(self.real), grad.astype(self.real)
+        off = abcn + M
+        self.src = np.ascontiguousarray((s + off).astype(np.int32))
+        self.rec = np.ascontiguousarray((r + off).astype(np.int32))
+        self.wavelet = np.ascontiguousarray(w.astype(self.real))
+        self.nrec = self.rec.shape[1]
+        self.nsrc = 1
+
+    def crop(self, g):
+        M, a = self.M, self.pad
+        sl = tuple(slice(a + M, a + M + n) for n in self.phys)
+        return g[(Ellipsis,) + sl]
+
+
+class Acoustic2D(_Acoustic):
+    def _geo(self):
+        nz, nx = self.shape
+        (az, bz, dbz), (ax, bx, dbx) = self.prof
+        pad = np.array([self.pad] * 4, np.int32)
+        self._keep = (pad, az, bz, dbz, ax, bx, dbx)
+        return [self.B, nz, nx, self.nt, self.M, _ptr(pad), self.dt, self.spacing[0],
+                self.spacing[1], _ptr(self.lap), _ptr(self.grad), _ptr(az), _ptr(bz),
+                _ptr(dbz), _ptr(ax), _ptr(bx), _ptr(dbx), _ptr(self.vp), self.vp_stride,
+                self.nsrc, _ptr(self.src), _ptr(self.wavelet), self.nrec, _ptr(self.rec)]
+
+    def forward(self, keep_tape=True):
+        lib = _lib(self.prec)
+        nz, nx = self.shape
+        pad = np.array([self.pad] * 4, np.int32)
+        rec = np.zeros((self.B, self.nrec, self.nt), self.real)
+        self.tape = None
+        if keep_tape:
+            n = lib.oracle_a2d_tape_len(self.B, nz, nx, self.nt, self.M, _ptr(pad))
+            self.tape = np.zeros(n, self.real)
+        rc = lib.oracle_a2d_forward(*self._geo(), _ptr(rec),
+                                    _ptr(self.tape) if keep_tape else None)
+        assert rc == 0
+        return rec.transpose(0, 2, 1)[..., None]                 # (B, nt, nrec, 1)
+
+    def backward(self, adj):
+        """``adj``: record cotangent in the canonical ``(B, nt, nrec, 1)`` layout."""
+        lib = _lib(self.prec)
+        a = np.ascontiguousarray(np.asarray(adj)[..., 0].transpose(0, 2, 1).astype(self.real))
+        g = np.zeros(((self.B,) if self.per_shot else ()) + self.shape, self.real)
+        gw = np.zeros((self.B, 1, self.nt), self.real)
+        rc = lib.oracle_a2d_backward(*self._geo(), _ptr(a), _ptr(self.tape), _ptr(g), _ptr(gw))
+        assert rc == 0
+        return self.crop(g), gw[:, 0, :]
+
+
+class Acoustic3D(_Acoustic):
+    def _geo(self):
+        nz, ny, nx = self.shape
+        (az, bz, dbz), (ay, by, dby), (ax, bx, dbx) = self.prof
+        pad = np.array([self.pad] * 6, np.int32)
+        self._keep = (pad,)
+        return [self.B, nz, ny, nx, self.nt, self.M, _ptr(pad), self.dt, self.spacing[0],
+                self.spacing[1], self.spacing[2], _ptr(self.lap), _ptr(self.grad),
+                _ptr(az), _ptr(bz), _ptr(dbz), _ptr(ay), _ptr(by), _ptr(dby),
+                _ptr(ax), _ptr(bx), _ptr(dbx), _ptr(self.vp), self.vp_stride,
+                self.nsrc, _ptr(self.src), _ptr(self.wavelet), self.nrec, _ptr(self.rec)]
+
+    def forward(self, keep_tape=True):
+        lib = _lib(self.prec)
+        nz, ny, nx = self.shape
+        pad = np.array([self.pad] * 6, np.int32)
+        rec = np.zeros((self.B, self.nrec, self.nt), self.real)
+        self.tape = None
+        if keep_tape:
+            n = lib.oracle_a3d_tape_len(self.B, nz, ny, nx, self.nt, self.M, _ptr(pad))
+            self.tape = np.zeros(n, self.real)
+        rc = lib.oracle_a3d_forward(*self._geo(), _ptr(rec),
+                                    _ptr(self.tape) if keep_tape else None)
+        assert rc == 0
+        return rec.transpose(0, 2, 1)[..., None]
+
+    def backward(self, adj):
+        lib = _lib(self.prec)
+        a = np.ascontiguousarray(np.asarray(adj)[..., 0].transpose(0, 2, 1).astype(self.real))
+        g = np.zeros(self.shape, self.real)
+        gw = np.zeros((self.B, 1, self.nt), self.real)
+        rc = lib.oracle_a3d_backward(*self._geo(), _ptr(a), _ptr(self.tape), _ptr(g), _ptr(gw))
+        assert rc == 0
+        return self.crop(g), gw[:, 0, :]
+
+
+def acoustic_gradient(vp, wavelet, src, rec, obs, dh, dt, abcn, order=8, prec="f32", **kw):
+    """Record, loss ``0.5 ||pred - obs||^2``, model gradient (cropped, summed over
+    shots for a shared model) and wavelet gradient (summed over shots for a
+    shared wavelet), like ``PropTorch(impl='c')`` + ``loss.backward()``."""
+    ndim = np.asarray(src).shape[-1]
+    cls = Acoustic2D if ndim == 2 else Acoustic3D
+    run = cls(vp, wavelet, src, rec, dh, dt, abcn, order, prec, **kw)
+    pred = run.forward(keep_tape=True)
+    res = pred - np.asarray(obs, run.real)
+    loss = 0.5 * float(np.sum(res.astype(np.float64) ** 2))
+    g, gw = run.backward(res)
+    if np.asarray(wavelet).ndim == 1:
+        gw = gw.sum(0)
+    return pred, loss, g, gw
+
+
+def acoustic_forward(vp, wavelet, src, rec, dh, dt, abcn, order=8, prec="f32", **kw):
+    ndim = np.asarray(src).shape[-1]
+    cls = Acoustic2D if ndim == 2 else Acoustic3D
+    return cls(vp, wavelet, src, rec, dh, dt, abcn, order, prec, **kw).forward(keep_tape=False)

@@ -1,0 +1,253 @@
+"""Generate the golden fixtures under ``tests/golden/`` from the reference itself.
+
+This script imports the reference package (DeepWave-KAUST/sweep) from its
+source tree and runs its own compiled path, ``PropTorch(..., impl='c')`` on
+the CPU device.  On a CPU device the reference builds its "host core": the
+same C++/CUDA kernel sources as its CUDA core compiled by g++ with
+``-ffp-contract=off`` (reference ``src/sweep/backend/c/hostcore.py:1-80``),
+which the reference's own tests hold to rel < 1e-5 of its CUDA core
+(reference ``test/test_host_core.py:250-255``).  The outputs (records and
+gradients, float32) are saved as small ``.npz`` files together with every input,
+so the parity tests never need the reference at run time.
+
+Usage (in a container that has the reference checked out)::
+
+    TORCH_EXTENSIONS_DIR=/tmp/sweep_ref_build \
+    PYTHONPATH=/root/reference/src python tests/golden/make_golden.py
+
+The reference's own build step (a one-time g++ build of its host core into
+``TORCH_EXTENSIONS_DIR``) runs on first use.  Nothing here is imported by the
+library or the tests.
+"""
+from __future__ import annotations
+
+import os
+import sys
+from pathlib import Path
+
+import numpy as np
+import torch
+
+REF_SRC = os.environ.get("SWEEP_REFERENCE_SRC", "/root/reference/src")
+if REF_SRC not in sys.path:
+    sys.path.insert(0, REF_SRC)
+
+from sweep.equations import Acoustic, Acoustic3D, Elastic  # noqa: E402
+from sweep.propagator.options import BoundarySaving, Ckpt, Full  # noqa: E402
+from sweep.propagator.torch import PropTorch  # noqa: E402
+from sweep.signal import ricker  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+torch.set_num_threads(max(1, os.cpu_count() or 1))
+
+
+def _wavelet(nt, dt, f, delay):
+    t = np.arange(nt, dtype=np.float64) * dt
+    return ricker(t - delay, f).astype(np.float32)
+
+
+def _layered(nz, nx, rng, vmin, vmax, nlayers):
+    """Small layered model: sorted random interface depths, monotone velocities."""
+    depths = np.sort(rng.uniform(0, nz, size=nlayers - 1))
+    vels = np.linspace(vmin, vmax, nlayers) * (1 + 0.03 * rng.standard_normal(nlayers))
+    z = np.arange(nz)[:, None] + 2.0 * np.sin(np.arange(nx)[None, :] * 2 * np.pi / nx * rng.uniform(1, 3))
+    idx = np.searchsorted(depths, z)
+    return vels[idx].astype(np.float32)
+
+
+def _run(solver, wavelet, src, rec, models, obs, need_wavelet_grad):
+    """Forward plus backward of 0.5 * ||pred - obs||^2, all in float32."""
+    models = [torch.tensor(m, requires_grad=True) for m in models]
+    w = torch.tensor(wavelet, requires_grad=need_wavelet_grad)
+    pred = solver(w, src, rec, models=models)
+    loss = 0.5 * ((pred - torch.tensor(obs)) ** 2).sum()
+    loss.backward()
+    out = {"pred": pred.detach().numpy(), "loss": np.float64(loss.detach())}
+    for i, m in enumerate(models):
+        out[f"grad{i}"] = m.grad.numpy().copy()
+    if need_wavelet_grad:
+        out["grad_wavelet"] = w.grad.numpy().copy()
+    return out
+
+
+def _forward(solver, wavelet, src, rec, models):
+    with torch.no_grad():
+        return solver(torch.tensor(wavelet), src, rec,
+                      models=[torch.tensor(m) for m in models]).numpy()
+
+
+def acoustic2d_c1():
+    """The 2-D two-layer case: 96x128, dh 10, dt 2 ms, nt 800, order 8, CPML 20."""
+    nz, nx, nt, dt, dh, abcn = 96, 128, 800, 0.002, 10.0, 20
+    vp_true = np.full((nz, nx), 1500.0, np.float32)
+    vp_true[nz // 2:] = 2500.0
+    vp_init = np.full((nz, nx), 1500.0, np.float32)
+    w = _wavelet(nt, dt, 10.0, 0.14)
+    src = np.array([[32, 48]], np.int64)
+    rec = np.array([[[96, 48]]], np.int64)
+    res = {}
+    for mode, mem in (("bs", BoundarySaving()), ("full", Full())):
+        eq = Acoustic(spatial_order=8, device="cpu")
+        solver = PropTorch(eq, shape=(nz, nx), dh=dh, dt=dt, abcn=abcn, impl="c",
+                           device="cpu", memory=mem)
+        obs = _forward(solver, w, src, rec, [vp_true])
+        r = _run(solver, w, src, rec, [vp_init], obs, True)
+        res[mode] = (obs, r)
+    obs, r = res["bs"]
+    np.savez_compressed(
+        OUT / "acoustic2d_c1.npz",
+        nz=nz, nx=nx, nt=nt, dt=dt, dh=dh, abcn=abcn, order=8,
+        vp_true=vp_true, vp_init=vp_init, wavelet=w, src=src, rec=rec,
+        obs=obs, pred=r["pred"], loss=r["loss"], grad_vp=r["grad0"],
+        grad_wavelet=r["grad_wavelet"],
+        grad_vp_full=res["full"][1]["grad0"],
+        grad_wavelet_full=res["full"][1]["grad_wavelet"],
+    )
+
+
+def acoustic2d_multi():
+    """3 shots of uneven geometry on a layered model, per-shot wavelets,
+    receiver lists padded with off-grid coordinates, one source inside the
+    boundary-saving restore strip and one receiver in the CPML pad."""
+    rng = np.random.default_rng(7)
+    nz, nx, nt, dt, dh, abcn = 40, 60, 300, 0.001, 10.0, 10
+    vp_true = _layered(nz, nx, rng, 1500.0, 3000.0, 5)
+    vp_init = np.full((nz, nx), 1800.0, np.float32) + 20.0 * rng.standard_normal((nz, nx)).astype(np.float32)
+    w = np.stack([_wavelet(nt, dt, 15.0, 0.06), _wavelet(nt, dt, 12.0, 0.08),
+                  _wavelet(nt, dt, 18.0, 0.05)]).astype(np.float32)
+    # (x, z) per shot; shot 1 sits inside the restore strip (z = 2)
+    src = np.array([[10, 8], [33, 2], [50, 20]], np.int64)
+    nrec = [12, 7, 9]
+    nrec_max = max(nrec)
+    rec = np.full((3, nrec_max, 2), -1000, np.int64)       # off-grid padding
+    for b, n in enumerate(nrec):
+        xs = np.sort(rng.choice(np.arange(1, nx - 1), size=n, replace=False))
+        rec[b, :n, 0] = xs
+        rec[b, :n, 1] = rng.integers(1, nz - 1, size=n)
+    rec[2, 0] = (nx + 3, 5)                                 # inside the CPML pad, still on the grid
+    res = {}
+    for mode, mem in (("bs", BoundarySaving()), ("full", Full()), ("ckpt", Ckpt(chunks=37))):
+        eq = Acoustic(spatial_order=8, device="cpu")
+        solver = PropTorch(eq, shape=(nz, nx), dh=dh, dt=dt, abcn=abcn, impl="c",
+                           device="cpu", memory=mem)
+        obs = _forward(solver, w, src, rec, [vp_true])
+        r = _run(solver, w, src, rec, [vp_init], obs, True)
+        res[mode] = (obs, r)
+    obs, r = res["bs"]
+    np.savez_compressed(
+        OUT / "acoustic2d_multi.npz",
+        nz=nz, nx=nx, nt=nt, dt=dt, dh=dh, abcn=abcn, order=8,
+        vp_true=vp_true, vp_init=vp_init, wavelet=w, src=src, rec=rec,
+        obs=obs, pred=r["pred"], loss=r["loss"], grad_vp=r["grad0"],
+        grad_wavelet=r["grad_wavelet"],
+        grad_vp_full=res["full"][1]["grad0"], grad_vp_ckpt=res["ckpt"][1]["grad0"],
+    )
+
+
+def acoustic2d_pershot():
+    """Per-shot models (B, nz, nx): each shot propagates in its own model and
+    keeps its own gradient."""
+    rng = np.random.default_rng(11)
+    nz, nx, nt, dt, dh, abcn = 32, 44, 220, 0.001, 10.0, 8
+    B = 2
+    vp_true = np.stack([_layered(nz, nx, rng, 1500.0, 2800.0, 4) for _ in range(B)])
+    vp_init = np.stack([np.full((nz, nx), 1700.0 + 100 * b, np.float32) for b in range(B)])
+    w = _wavelet(nt, dt, 15.0, 0.06)
+    src = np.array([[12, 6], [30, 10]], np.int64)
+    rec = np.array([[[5, 3], [20, 3], [35, 3]], [[8, 25], [22, 25], [40, 25]]], np.int64)
+    eq = Acoustic(spatial_order=8, device="cpu")
+    solver = PropTorch(eq, shape=(nz, nx), dh=dh, dt=dt, abcn=abcn, impl="c", device="cpu",
+                       memory=BoundarySaving())
+    obs = _forward(solver, w, src, rec, [vp_true])
+    r = _run(solver, w, src, rec, [vp_init], obs, False)
+    np.savez_compressed(
+        OUT / "acoustic2d_pershot.npz",
+        nz=nz, nx=nx, nt=nt, dt=dt, dh=dh, abcn=abcn, order=8,
+        vp_true=vp_true, vp_init=vp_init, wavelet=w, src=src, rec=rec,
+        obs=obs, pred=r["pred"], loss=r["loss"], grad_vp=r["grad0"],
+    )
+
+
+def acoustic3d():
+    """A small 3-D case: 2 shots, 6 receivers each, order 8, CPML 8."""
+    rng = np.random.default_rng(3)
+    nz, ny, nx, nt, dt, dh, abcn = 20, 18, 24, 160, 0.001, 10.0, 8
+    vp_true = np.full((nz, ny, nx), 1800.0, np.float32)
+    vp_true[nz // 2:] = 2600.0
+    vp_true += (30.0 * rng.standard_normal((nz, ny, nx))).astype(np.float32)
+    vp_init = np.full((nz, ny, nx), 2000.0, np.float32)
+    w = _wavelet(nt, dt, 15.0, 0.06)
+    src = np.array([[6, 5, 4], [17, 12, 3]], np.int64)          # (x, y, z)
+    rec = np.zeros((2, 6, 3), np.int64)
+    for b in range(2):
+        rec[b, :, 0] = rng.integers(1, nx - 1, 6)
+        rec[b, :, 1] = rng.integers(1, ny - 1, 6)
+        rec[b, :, 2] = rng.integers(1, nz - 1, 6)
+    res = {}
+    for mode, mem in (("bs", BoundarySaving()), ("full", Full())):
+        eq = Acoustic3D(spatial_order=8, device="cpu")
+        solver = PropTorch(eq, shape=(nz, ny, nx), dh=dh, dt=dt, abcn=abcn, impl="c",
+                           device="cpu", memory=mem)
+        obs = _forward(solver, w, src, rec, [vp_true])
+        r = _run(solver, w, src, rec, [vp_init], obs, True)
+        res[mode] = (obs, r)
+    obs, r = res["bs"]
+    np.savez_compressed(
+        OUT / "acoustic3d.npz",
+        nz=nz, ny=ny, nx=nx, nt=nt, dt=dt, dh=dh, abcn=abcn, order=8,
+        vp_true=vp_true, vp_init=vp_init, wavelet=w, src=src, rec=rec,
+        obs=obs, pred=r["pred"], loss=r["loss"], grad_vp=r["grad0"],
+        grad_wavelet=r["grad_wavelet"], grad_vp_full=res["full"][1]["grad0"],
+    )
+
+
+def elastic2d():
+    """Isotropic elastic: 2 explosive shots, (vx, vz) receivers, vp/vs/rho gradients."""
+    rng = np.random.default_rng(5)
+    nz, nx, nt, dt, dh, abcn = 40, 56, 300, 0.0005, 5.0, 10
+    vp_true = _layered(nz, nx, rng, 1800.0, 3200.0, 4)
+    vs_true = (vp_true / 1.73).astype(np.float32)
+    rho_true = (310.0 * vp_true ** 0.25).astype(np.float32)
+    vp_init = np.full((nz, nx), 2200.0, np.float32)
+    vs_init = (vp_init / 1.73).astype(np.float32)
+    rho_init = (310.0 * vp_init ** 0.25).astype(np.float32)
+    w = _wavelet(nt, dt, 25.0, 0.04)
+    src = np.array([[14, 6], [40, 9]], np.int64)
+    rec = np.zeros((2, 8, 2), np.int64)
+    for b in range(2):
+        rec[b, :, 0] = np.linspace(3, nx - 4, 8).astype(np.int64)
+        rec[b, :, 1] = 3 + b
+    res = {}
+    for mode, mem in (("bs", BoundarySaving()), ("full", Full())):
+        eq = Elastic(spatial_order=8, device="cpu")
+        solver = PropTorch(eq, shape=(nz, nx), dh=dh, dt=dt, abcn=abcn, impl="c",
+                           device="cpu", memory=mem)
+        obs = _forward(solver, w, src, rec, [vp_true, vs_true, rho_true])
+        r = _run(solver, w, src, rec, [vp_init, vs_init, rho_init], obs, False)
+        res[mode] = (obs, r)
+    obs, r = res["bs"]
+    np.savez_compressed(
+        OUT / "elastic2d.npz",
+        nz=nz, nx=nx, nt=nt, dt=dt, dh=dh, abcn=abcn, order=8,
+        vp_true=vp_true, vs_true=vs_true, rho_true=rho_true,
+        vp_init=vp_init, vs_init=vs_init, rho_init=rho_init,
+        wavelet=w, src=src, rec=rec, obs=obs, pred=r["pred"], loss=r["loss"],
+        grad_vp=r["grad0"], grad_vs=r["grad1"], grad_rho=r["grad2"],
+        grad_vp_full=res["full"][1]["grad0"], grad_vs_full=res["full"][1]["grad1"],
+        grad_rho_full=res["full"][1]["grad2"],
+    )
+
+
+CASES = {
+    "acoustic2d_c1": acoustic2d_c1,
+    "acoustic2d_multi": acoustic2d_multi,
+    "acoustic2d_pershot": acoustic2d_pershot,
+    "acoustic3d": acoustic3d,
+    "elastic2d": elastic2d,
+}
+
+if __name__ == "__main__":
+    names = sys.argv[1:] or list(CASES)
+    for name in names:
+        CASES[name]()
+        print("wrote", name)
