@@ -1,0 +1,117 @@
+/*
+ * sweep_b200.h -- C ABI of libsweep_b200.so, the B200 (sm_100a) finite-difference
+ * core behind sweep_b200.PropTorch.
+ *
+ * This boundary replaces the reference's compiled-core entry
+ *     int sweep_call(int entry, const void* in, void* out, char* err, int err_cap)
+ * (reference src/sweep/csrc/core/capi.h:225) for the entries of the hot path:
+ *     acoustic2d 0 forward, 2 backward_bs, 3 backward_ckpt  (capi.h:39-45)
+ *     acoustic3d 5 forward, 7 backward_bs, 8 backward_ckpt  (capi.h:46-52)
+ *     elastic2d 60 forward, 62 backward_bs                  (capi.h:96-100)
+ * with one plain function per (equation family, pass) instead of an entry
+ * number, and one POD descriptor instead of the reference's ForwardInputCore /
+ * BackwardInputCore Buf structs (reference src/sweep/csrc/core/input_core.h).
+ *
+ * Conventions shared by every entry point (same as the reference's ABI:
+ * capi.h:2-7, buf.h:13-17, capi.cu:578-580):
+ *   - the caller allocates EVERY buffer, outputs included; pointers are device
+ *     pointers unless stated otherwise; nothing here owns memory;
+ *   - fields are float32, shot-major, x fastest: (B, nz, nx) / (B, nz, ny, nx)
+ *     on the runtime grid (physical + PML pad + stencil halo M per face);
+ *   - coordinates are runtime-grid int32 (x, z) / (x, y, z) per shot; a
+ *     coordinate outside the grid is skipped (reference common.cu:24-28);
+ *   - records are (B, nt, nrec) -- the canonical (B, nt, nrec, nfield) layout
+ *     of the reference's Python API with nfield folded -- and record cotangents
+ *     are read in the same layout;
+ *   - work is enqueued on `stream` (a cudaStream_t, NULL = legacy default) and
+ *     is asynchronous; results are valid in stream order;
+ *   - return 0 on success, else non-zero with a NUL-terminated message copied
+ *     into err[0..err_cap); nothing is thrown across the boundary.
+ */
+#ifndef SWEEP_B200_H
+#define SWEEP_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SWEEP_B200_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define SWEEP_B200_API __attribute__((visibility("default")))
+#else
+#define SWEEP_B200_API
+#endif
+
+/* Scalar-wave (acoustic, constant density) problem: 2-D when ndim == 2
+ * (ny == 1, the y entries unused), 3-D when ndim == 3.  Replaces the geometry,
+ * model and source/receiver fields of the reference's ForwardInputCore
+ * (reference src/sweep/backend/c/abi.py:108-166). */
+typedef struct sweep_acoustic_desc {
+    int32_t ndim;            /* 2 or 3 */
+    int32_t B;               /* shots advanced together */
+    int32_t nz, ny, nx;      /* runtime grid */
+    int32_t nt;              /* time steps */
+    int32_t M;               /* stencil half-width (spatial order / 2); 4 */
+    int32_t pad[6];          /* PML pad per face: z_lo, z_hi, y_lo, y_hi, x_lo, x_hi */
+    float dt, dz, dy, dx;
+    float lap[8];            /* lap[1..M]: second-derivative taps (lap[0] unused) */
+    float grad[8];           /* grad[1..M]: centred first-derivative taps */
+    const float *az, *bz, *dbz;   /* CPML profiles per axis: a, b, d b / d axis */
+    const float *ay, *by, *dby;   /* (length nz / ny / nx); y unused in 2-D */
+    const float *ax, *bx, *dbx;
+    const float* vp;         /* (B|1, cells) velocity on the runtime grid */
+    int64_t vp_stride;       /* 0: one model shared by every shot; else cells per shot */
+    int32_t nsrc;            /* sources per shot */
+    const int32_t* src_loc;  /* (B, nsrc, ndim) */
+    const float* wavelet;    /* (B, nsrc, nt) raw amplitudes added to the field */
+    int32_t nrec;            /* receivers per shot (padded to a rectangle) */
+    const int32_t* rec_loc;  /* (B, nrec, ndim) */
+} sweep_acoustic_desc;
+
+/* Memory modes of the backward (reference src/sweep/propagator/options.py:186-246). */
+#define SWEEP_MEM_BOUNDARY   0   /* save boundary strips each step; replay them in reverse */
+#define SWEEP_MEM_CHECKPOINT 1   /* save state every `ckpt_every` steps; re-run each chunk */
+
+/* Bytes the caller must allocate: `workspace` (scratch, reusable between calls
+ * once the previous call has finished on its stream) and `tape` (written by
+ * the forward, read by the backward; keep it between the two).  `mem_mode` is
+ * SWEEP_MEM_BOUNDARY or SWEEP_MEM_CHECKPOINT; `ckpt_every` the checkpoint
+ * interval (ignored for boundary saving).  Host-side only, no device work. */
+SWEEP_B200_API int sweep_b200_acoustic_sizes(const sweep_acoustic_desc* d, int32_t mem_mode, int32_t ckpt_every,
+                              int64_t* workspace_bytes, int64_t* tape_bytes,
+                              char* err, int32_t err_cap);
+
+/* Forward propagation (reference entry 0 / 5: eq_driver.cuh:357-453).
+ * record: (B, nt, nrec) out.  tape: NULL for a forward without a later
+ * backward, else `tape_bytes` of device memory the backward will read. */
+SWEEP_B200_API int sweep_b200_acoustic_forward(const sweep_acoustic_desc* d, int32_t mem_mode, int32_t ckpt_every,
+                                float* record, void* tape,
+                                void* workspace, int64_t workspace_bytes,
+                                void* stream, char* err, int32_t err_cap);
+
+/* Adjoint propagation and gradient accumulation (reference entries 2/3 and
+ * 7/8: eq_driver.cuh:721-1135).  adj: (B, nt, nrec) record cotangent.
+ * grad_vp: (B|1, cells) on the runtime grid, same stride rule as vp,
+ * OVERWRITTEN with d loss / d vp (zero outside the physical box).
+ * grad_wavelet: (B, nsrc, nt) overwritten, or NULL.  illum_src / illum_rec:
+ * (B|1, cells) overwritten with sum_t u_tt^2 and sum_t lambda^2 over the
+ * physical box (reference acoustic2d/kernels.cu:133), or NULL. */
+SWEEP_B200_API int sweep_b200_acoustic_backward(const sweep_acoustic_desc* d, int32_t mem_mode, int32_t ckpt_every,
+                                 const float* adj, const void* tape,
+                                 float* grad_vp, float* grad_wavelet,
+                                 float* illum_src, float* illum_rec,
+                                 void* workspace, int64_t workspace_bytes,
+                                 void* stream, char* err, int32_t err_cap);
+
+/* ABI version (SWEEP_B200_ABI_VERSION) -- checked by the Python loader, like
+ * the reference's sweep_core_abi_version() (reference loader.py:92-138). */
+SWEEP_B200_API int sweep_b200_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SWEEP_B200_H */

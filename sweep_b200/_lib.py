@@ -1,0 +1,95 @@
+"""ctypes binding of ``libsweep_b200.so`` (declared in ``include/sweep_b200.h``).
+
+The Python side of the C ABI, in the role of the reference's ctypes layer
+(reference ``src/sweep/backend/c/entries.py:119-146``, ``loader.py:29-138``):
+load the core once, check its ABI version and that every declared symbol is
+exported, pack plain descriptors, run each call on torch's current stream and
+turn a non-zero return into ``RuntimeError`` with the core's message.
+
+There is no fallback: if the library is missing or fails to load, every call
+raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = Path(os.environ.get("SWEEP_B200_LIB", HERE / "libsweep_b200.so"))
+ABI_VERSION = 1
+ERR_CAP = 4096
+
+c_i32, c_i64, c_f32, c_p = ctypes.c_int32, ctypes.c_int64, ctypes.c_float, ctypes.c_void_p
+
+# Every symbol include/sweep_b200.h declares.
+SYMBOLS = (
+    "sweep_b200_abi_version",
+    "sweep_b200_acoustic_sizes",
+    "sweep_b200_acoustic_forward",
+    "sweep_b200_acoustic_backward",
+)
+
+MEM_BOUNDARY = 0
+MEM_CHECKPOINT = 1
+
+
+class AcousticDesc(ctypes.Structure):
+    """Mirror of ``sweep_acoustic_desc``."""
+    _fields_ = [
+        ("ndim", c_i32), ("B", c_i32), ("nz", c_i32), ("ny", c_i32), ("nx", c_i32),
+        ("nt", c_i32), ("M", c_i32), ("pad", c_i32 * 6),
+        ("dt", c_f32), ("dz", c_f32), ("dy", c_f32), ("dx", c_f32),
+        ("lap", c_f32 * 8), ("grad", c_f32 * 8),
+        ("az", c_p), ("bz", c_p), ("dbz", c_p),
+        ("ay", c_p), ("by", c_p), ("dby", c_p),
+        ("ax", c_p), ("bx", c_p), ("dbx", c_p),
+        ("vp", c_p), ("vp_stride", c_i64),
+        ("nsrc", c_i32), ("src_loc", c_p), ("wavelet", c_p),
+        ("nrec", c_i32), ("rec_loc", c_p),
+    ]
+
+
+_lib = None
+
+
+def load():
+    """The loaded core; raises if it is missing, stale or incomplete."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(
+            f"sweep_b200: the CUDA core {LIB_PATH} is not built; run "
+            "`python -c 'import __graft_entry__ as g; g.build()'` (or make -C sweep_b200/csrc)")
+    lib = ctypes.CDLL(str(LIB_PATH))
+    missing = [s for s in SYMBOLS if not hasattr(lib, s)]
+    if missing:
+        raise RuntimeError(f"sweep_b200: {LIB_PATH} lacks symbols {missing}")
+    lib.sweep_b200_abi_version.restype = ctypes.c_int
+    ver = lib.sweep_b200_abi_version()
+    if ver != ABI_VERSION:
+        raise RuntimeError(f"sweep_b200: core ABI {ver} != expected {ABI_VERSION}; rebuild it")
+    P = ctypes.POINTER(AcousticDesc)
+    lib.sweep_b200_acoustic_sizes.argtypes = [P, c_i32, c_i32, ctypes.POINTER(c_i64),
+                                              ctypes.POINTER(c_i64), ctypes.c_char_p, c_i32]
+    lib.sweep_b200_acoustic_forward.argtypes = [P, c_i32, c_i32, c_p, c_p, c_p, c_i64, c_p,
+                                                ctypes.c_char_p, c_i32]
+    lib.sweep_b200_acoustic_backward.argtypes = [P, c_i32, c_i32, c_p, c_p, c_p, c_p, c_p, c_p,
+                                                 c_p, c_i64, c_p, ctypes.c_char_p, c_i32]
+    for s in SYMBOLS[1:]:
+        getattr(lib, s).restype = ctypes.c_int
+    _lib = lib
+    return lib
+
+
+def check(rc: int, err) -> None:
+    if rc != 0:
+        raise RuntimeError("sweep_b200 core: " + err.value.decode(errors="replace"))
+
+
+def call(name: str, *args) -> None:
+    """Call entry ``name`` with the error buffer appended; raise on failure."""
+    lib = load()
+    err = ctypes.create_string_buffer(ERR_CAP)
+    check(getattr(lib, name)(*args, err, ERR_CAP), err)

@@ -1,0 +1,54 @@
+// capi.cu -- the extern "C" entry points declared in include/sweep_b200.h.
+// Each one validates, dispatches on the equation family, and turns any error
+// into (non-zero return, message) -- nothing is thrown across the boundary.
+#include "common.cuh"
+
+namespace sweep {
+namespace a2d {
+void sizes(const sweep_acoustic_desc*, int, int, int64_t*, int64_t*);
+void forward(const sweep_acoustic_desc*, int, int, float*, void*, void*, int64_t, cudaStream_t);
+void backward(const sweep_acoustic_desc*, int, int, const float*, const void*, float*, float*,
+              float*, float*, void*, int64_t, cudaStream_t);
+}  // namespace a2d
+}  // namespace sweep
+
+using namespace sweep;
+
+extern "C" int sweep_b200_abi_version(void) { return SWEEP_B200_ABI_VERSION; }
+
+extern "C" int sweep_b200_acoustic_sizes(const sweep_acoustic_desc* d, int32_t mem_mode, int32_t ckpt_every,
+                                         int64_t* workspace_bytes, int64_t* tape_bytes,
+                                         char* err, int32_t err_cap)
+{
+    return guarded(err, err_cap, [&] {
+        SWEEP_REQUIRE(d && workspace_bytes && tape_bytes, "null argument");
+        SWEEP_REQUIRE(d->ndim == 2, "acoustic: ndim %d is not built", d->ndim);
+        a2d::sizes(d, mem_mode, ckpt_every, workspace_bytes, tape_bytes);
+    });
+}
+
+extern "C" int sweep_b200_acoustic_forward(const sweep_acoustic_desc* d, int32_t mem_mode, int32_t ckpt_every,
+                                           float* record, void* tape, void* workspace, int64_t workspace_bytes,
+                                           void* stream, char* err, int32_t err_cap)
+{
+    return guarded(err, err_cap, [&] {
+        SWEEP_REQUIRE(d != nullptr, "null descriptor");
+        SWEEP_REQUIRE(d->ndim == 2, "acoustic: ndim %d is not built", d->ndim);
+        a2d::forward(d, mem_mode, ckpt_every, record, tape, workspace, workspace_bytes,
+                     static_cast<cudaStream_t>(stream));
+    });
+}
+
+extern "C" int sweep_b200_acoustic_backward(const sweep_acoustic_desc* d, int32_t mem_mode, int32_t ckpt_every,
+                                            const float* adj, const void* tape, float* grad_vp,
+                                            float* grad_wavelet, float* illum_src, float* illum_rec,
+                                            void* workspace, int64_t workspace_bytes, void* stream,
+                                            char* err, int32_t err_cap)
+{
+    return guarded(err, err_cap, [&] {
+        SWEEP_REQUIRE(d != nullptr, "null descriptor");
+        SWEEP_REQUIRE(d->ndim == 2, "acoustic: ndim %d is not built", d->ndim);
+        a2d::backward(d, mem_mode, ckpt_every, adj, tape, grad_vp, grad_wavelet, illum_src, illum_rec,
+                      workspace, workspace_bytes, static_cast<cudaStream_t>(stream));
+    });
+}

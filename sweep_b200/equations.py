@@ -1,0 +1,71 @@
+"""Equation descriptors of the hot path, mirroring the reference's
+``src/sweep/equations/acoustic.py:48-133`` (``Acoustic``),
+``acoustic3d.py:50-185`` (``Acoustic3D``) and ``elastic.py:19-310``
+(``Elastic``): the constructor keywords, model names and default
+source / receiver fields the propagator reads."""
+from __future__ import annotations
+
+
+class _Equation:
+    C_NAME = ""
+    MODEL_NAMES: tuple = ()
+    NDIM = 2
+    SOURCE_FIELDS: tuple = ()
+    RECEIVER_FIELDS: tuple = ()
+    default_pml_type = "cpmlr"
+
+    def __init__(self, spatial_order=4, device="cpu", backend="torch", dim=None):
+        if spatial_order % 2 or spatial_order < 2:
+            raise ValueError(f"spatial_order must be an even integer >= 2, got {spatial_order}")
+        if backend != "torch":
+            raise ValueError("sweep_b200 equations run on the torch backend only")
+        self.so = int(spatial_order)
+        self.spatial_order = self.so
+        self.M = self.so // 2
+        self.device = device
+        self.backend = backend
+        self.ndim = self.NDIM
+
+    @property
+    def model_names(self):
+        return list(self.MODEL_NAMES)
+
+    @property
+    def default_source_fields(self):
+        return list(self.SOURCE_FIELDS)
+
+    @property
+    def default_receiver_fields(self):
+        return list(self.RECEIVER_FIELDS)
+
+
+class Acoustic(_Equation):
+    """Second-order 2-D constant-density acoustic wave equation with CPML
+    (``u_tt = vp^2 Lap u``; one pressure-like field ``h1``)."""
+    C_NAME = "acoustic2d"
+    MODEL_NAMES = ("vp",)
+    NDIM = 2
+    SOURCE_FIELDS = ("h1",)
+    RECEIVER_FIELDS = ("h1",)
+
+
+class Acoustic3D(_Equation):
+    """Second-order 3-D constant-density acoustic wave equation with CPML."""
+    C_NAME = "acoustic3d"
+    MODEL_NAMES = ("vp",)
+    NDIM = 3
+    SOURCE_FIELDS = ("h1",)
+    RECEIVER_FIELDS = ("h1",)
+
+
+class Elastic(_Equation):
+    """First-order 2-D isotropic elastic velocity-stress equation on a
+    staggered grid (Virieux 1986): fields vx, vz, sxx, szz, sxz; models
+    vp, vs, rho; explosive source (sxx, szz) and (vx, vz) receivers by default."""
+    C_NAME = "elastic2d"
+    MODEL_NAMES = ("vp", "vs", "rho")
+    NDIM = 2
+    SOURCE_FIELDS = ("sxx", "szz")
+    RECEIVER_FIELDS = ("vx", "vz")
+    FIELDS = ("vx", "vz", "sxx", "szz", "sxz")
+    default_pml_type = "cpmls"

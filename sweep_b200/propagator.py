@@ -1,0 +1,313 @@
+"""``PropTorch``: the drop-in propagator over the B200 core.
+
+Mirrors the reference's ``PropTorch(equation, shape, dh, dt, abcn, impl='c',
+memory=...)`` and its call ``solver(wavelet, sources, receivers, models=[...])``
+(reference ``src/sweep/propagator/torch.py:576-825``,
+``src/sweep/propagator/_c.py:2209-2599``): the same constructor keywords,
+input modes, coordinate and padding conventions and record layout
+``(B, nt, nrec, nfield)``, and ``.backward()`` fills the models' (and, for the
+acoustic equations, the wavelet's) gradients through a
+``torch.autograd.Function`` whose forward and backward each make one call into
+``libsweep_b200.so``.
+
+Host-side conventions restated from the reference:
+* runtime grid = physical + ``abcn`` PML cells + ``M = so/2`` halo per face
+  (``core/geometry.py:23-58``); coordinates shift by ``abcn + M``
+  (``_c.py:2196-2207``);
+* models are replicate-padded to the runtime grid and the gradient cropped back
+  (``utils/torch.py:8-41``); a shared model is used by every shot and its
+  gradient summed over shots (``_c.py:2110-2155``);
+* the wavelet is the raw amplitude added to the field at the source cell each
+  step (``common/common.cu:11-36``);
+* a second backward through the same forward is refused (``_c.py:612-625``).
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+import torch.nn.functional as F
+
+from . import _lib
+from .equations import Acoustic, Acoustic3D, Elastic
+from .options import BoundarySaving, Ckpt, Full
+from .pml import cpml_profiles_r, cpml_profiles_s
+from .scalars import centred_tables, staggered_grid_coes
+
+__all__ = ["PropTorch"]
+
+
+def _as_tensor(x, dtype, device):
+    if isinstance(x, torch.Tensor):
+        return x.to(device=device, dtype=dtype)
+    return torch.as_tensor(np.asarray(x), dtype=dtype, device=device)
+
+
+def normalize_io(wavelet, sources, receivers, ndim):
+    """Input modes of the reference (``core/validation.py:35-127``).
+
+    Returns ``(mode, B, nsrc)``: 'A1' shared wavelet ``(nt,)`` + sources
+    ``(B, ndim)``; 'A2' per-shot wavelets ``(B, nt)`` + sources ``(B, ndim)``;
+    'B' one super-shot of ``nsrc`` sources ``(1, nsrc, ndim)`` with a wavelet
+    ``(nt,)`` or ``(nsrc, nt)``."""
+    ws = tuple(wavelet.shape)
+    ss = tuple(np.shape(sources))
+    rs = tuple(np.shape(receivers))
+    if len(rs) != 3 or rs[-1] != ndim:
+        raise ValueError(f"receivers must be (B, nrec, {ndim}); got {rs}")
+    if len(ss) == 2 and ss[-1] == ndim:
+        B = ss[0]
+        if len(ws) == 1:
+            mode = "A1"
+        elif len(ws) == 2 and ws[0] == B:
+            mode = "A2"
+        else:
+            raise ValueError(f"wavelet must be (nt,) or (nshots={B}, nt); got {ws}")
+        nsrc = 1
+    elif len(ss) == 3 and ss[0] == 1 and ss[-1] == ndim:
+        B, nsrc = 1, ss[1]
+        if not (len(ws) == 1 or (len(ws) == 2 and ws[0] == nsrc)):
+            raise ValueError(f"wavelet must be (nt,) or (nsrc={nsrc}, nt) in source-encoding mode; got {ws}")
+        mode = "B"
+    else:
+        raise ValueError(f"sources must be (nshots, {ndim}) or (1, nsrc, {ndim}); got {ss}")
+    if rs[0] != B:
+        raise ValueError(f"receivers batch ({rs[0]}) must equal the shot count ({B})")
+    return mode, B, nsrc
+
+
+class _Geometry:
+    """Everything a core call needs besides the model and wavelet tensors."""
+
+    def __init__(self, prop, B, nsrc, nrec, nt, src_rt, rec_rt, device, max_vel, pml_freq):
+        eq = prop.equation
+        self.ndim = eq.NDIM
+        self.M = eq.M
+        self.B, self.nsrc, self.nrec, self.nt = B, nsrc, nrec, nt
+        self.shape = prop.runtime_shape
+        self.device = device
+        self.dt = prop.dt
+        self.spacing = prop.spacing
+        pads = [prop.abcn] * (2 * self.ndim)
+        if isinstance(eq, Elastic):
+            prof = cpml_profiles_s(pads, self.M, prop.dt, self.spacing, self.shape, max_vel, pml_freq)
+        else:
+            prof = cpml_profiles_r(pads, self.M, prop.dt, self.spacing, self.shape, max_vel, pml_freq)
+        self.prof = [[torch.from_numpy(np.ascontiguousarray(a)).to(device) for a in p] for p in prof]
+        self.src = torch.from_numpy(np.ascontiguousarray(src_rt, dtype=np.int32)).to(device)
+        self.rec = torch.from_numpy(np.ascontiguousarray(rec_rt, dtype=np.int32)).to(device)
+        self.pad = prop.abcn
+
+    def acoustic_desc(self, vp, wavelet):
+        d = _lib.AcousticDesc()
+        d.ndim = self.ndim
+        d.B = self.B
+        if self.ndim == 2:
+            d.nz, d.ny, d.nx = self.shape[0], 1, self.shape[1]
+        else:
+            d.nz, d.ny, d.nx = self.shape
+        d.nt = self.nt
+        d.M = self.M
+        for i in range(6):
+            d.pad[i] = self.pad if (self.ndim == 3 or i not in (2, 3)) else 0
+        d.dt = self.dt
+        if self.ndim == 2:
+            d.dz, d.dy, d.dx = self.spacing[0], 1.0, self.spacing[1]
+        else:
+            d.dz, d.dy, d.dx = self.spacing
+        lap, grad = centred_tables(self.M)
+        for k in range(self.M + 1):
+            d.lap[k] = float(lap[k])
+            d.grad[k] = float(grad[k])
+        if self.ndim == 2:
+            (az, bz, dbz), (ax, bx, dbx) = self.prof
+            ay = by = dby = None
+        else:
+            (az, bz, dbz), (ay, by, dby), (ax, bx, dbx) = self.prof
+        for name, t in (("az", az), ("bz", bz), ("dbz", dbz), ("ay", ay), ("by", by),
+                        ("dby", dby), ("ax", ax), ("bx", bx), ("dbx", dbx)):
+            setattr(d, name, t.data_ptr() if t is not None else None)
+        cells = int(np.prod(self.shape))
+        d.vp = vp.data_ptr()
+        d.vp_stride = cells if vp.dim() == self.ndim + 1 else 0
+        d.nsrc = self.nsrc
+        d.src_loc = self.src.data_ptr()
+        d.wavelet = wavelet.data_ptr()
+        d.nrec = self.nrec
+        d.rec_loc = self.rec.data_ptr()
+        return d
+
+
+def _stream_ptr(device):
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+class _AcousticFn(torch.autograd.Function):
+    """vp (runtime grid, shared ``(*shape)`` or per-shot ``(B, *shape)``) and
+    wavelet ``(B, nsrc, nt)`` -> record ``(B, nt, nrec, 1)``."""
+
+    @staticmethod
+    def forward(ctx, vp, wavelet, prop, geo, mem_mode, ckpt_every):
+        vp = vp.contiguous()
+        wavelet = wavelet.contiguous()
+        desc = geo.acoustic_desc(vp, wavelet)
+        ws_b, tape_b = _lib.c_i64(), _lib.c_i64()
+        _lib.call("sweep_b200_acoustic_sizes", desc, mem_mode, ckpt_every, ws_b, tape_b)
+        need_bwd = any(ctx.needs_input_grad[:2])
+        ws = prop._workspace(ws_b.value, vp.device)
+        tape = torch.empty(tape_b.value, dtype=torch.uint8, device=vp.device) if need_bwd else None
+        record = torch.empty((geo.B, geo.nt, geo.nrec), dtype=torch.float32, device=vp.device)
+        _lib.call("sweep_b200_acoustic_forward", desc, mem_mode, ckpt_every, record.data_ptr(),
+                  tape.data_ptr() if tape is not None else None, ws.data_ptr(), ws.numel(),
+                  _stream_ptr(vp.device))
+        ctx.save_for_backward(vp, wavelet)
+        ctx.tape = tape
+        ctx.geo, ctx.prop, ctx.mem_mode, ctx.ckpt_every = geo, prop, mem_mode, ckpt_every
+        return record[..., None]
+
+    @staticmethod
+    def backward(ctx, grad_record):
+        if ctx.tape is None:
+            raise RuntimeError("sweep_b200: this forward has already been back-propagated (or ran "
+                               "without gradients); a second backward is refused")
+        vp, wavelet = ctx.saved_tensors
+        geo, prop = ctx.geo, ctx.prop
+        adj = grad_record[..., 0].to(torch.float32).contiguous()
+        desc = geo.acoustic_desc(vp, wavelet)
+        ws_b, tape_b = _lib.c_i64(), _lib.c_i64()
+        _lib.call("sweep_b200_acoustic_sizes", desc, ctx.mem_mode, ctx.ckpt_every, ws_b, tape_b)
+        ws = prop._workspace(ws_b.value, vp.device)
+        grad_vp = torch.empty_like(vp)
+        grad_w = torch.empty_like(wavelet) if ctx.needs_input_grad[1] else None
+        illum = prop.compute_illumination
+        i_s = torch.empty_like(vp) if illum else None
+        i_r = torch.empty_like(vp) if illum else None
+        _lib.call("sweep_b200_acoustic_backward", desc, ctx.mem_mode, ctx.ckpt_every, adj.data_ptr(),
+                  ctx.tape.data_ptr(), grad_vp.data_ptr(),
+                  grad_w.data_ptr() if grad_w is not None else None,
+                  i_s.data_ptr() if illum else None, i_r.data_ptr() if illum else None,
+                  ws.data_ptr(), ws.numel(), _stream_ptr(vp.device))
+        ctx.tape = None
+        if illum:
+            prop._set_illumination(i_s, i_r)
+        return grad_vp, grad_w, None, None, None, None
+
+
+class PropTorch(torch.nn.Module):
+    """Propagator over the B200 core (``impl='c'``; the only implementation).
+
+    Args mirror the reference's ``PropBase`` (``propagator/base.py:31-120``):
+    ``equation``, ``shape`` (physical ``(nz, nx)`` / ``(nz, ny, nx)``), ``dh``
+    (scalar or per axis in shape order), ``dt``, ``abcn`` (PML cells per face,
+    default 50), ``memory`` (``BoundarySaving()`` default, ``Full()``,
+    ``Ckpt(chunks)``), ``device``/``dev``, ``source_type`` /
+    ``receiver_type`` (field names; elastic only)."""
+
+    def __init__(self, equation, shape, dh=10.0, dt=0.002, abcn=50, impl="c", memory=None,
+                 device=None, dev=None, source_type=None, receiver_type=None,
+                 use_ckpt=None, ckpt_chunks=100, free_surface=False, **kwargs):
+        super().__init__()
+        if impl not in (None, "c", "auto"):
+            raise NotImplementedError(f"sweep_b200 implements impl='c' only (got impl={impl!r})")
+        if free_surface:
+            raise NotImplementedError("sweep_b200: free surfaces are not built (absorbing faces only)")
+        unknown = set(kwargs) - {"nt", "B", "pml_type", "backend"}
+        if unknown:
+            raise TypeError(f"PropTorch got unexpected keyword arguments {sorted(unknown)}")
+        self.equation = equation
+        self.impl = "c"
+        nd = equation.NDIM
+        if len(shape) != nd:
+            raise ValueError(f"{type(equation).__name__} needs a {nd}-D shape, got {shape}")
+        self.shape = tuple(int(s) for s in shape)
+        self.spacing = [float(x) for x in (dh if np.ndim(dh) else [dh] * nd)]
+        self.dt = float(dt)
+        self.abcn = int(abcn)
+        if self.abcn < 1:
+            raise NotImplementedError("sweep_b200: every face needs an absorbing layer (abcn >= 1)")
+        M = equation.M
+        self.runtime_shape = tuple(n + 2 * self.abcn + 2 * M for n in self.shape)
+        if memory is None:
+            memory = Ckpt(chunks=ckpt_chunks) if use_ckpt else BoundarySaving()
+        if not isinstance(memory, (BoundarySaving, Full, Ckpt)):
+            raise TypeError("memory must be BoundarySaving(), Full() or Ckpt(chunks)")
+        self.memory = memory
+        self.device = torch.device(device or dev or equation.device or "cuda")
+        self.source_type = list(source_type or equation.default_source_fields)
+        self.receiver_type = list(receiver_type or equation.default_receiver_fields)
+        self.compute_illumination = False
+        self.source_illumination = None
+        self.receiver_illumination = None
+        self._ws = None
+
+    # ---------------------------------------------------------------- helpers
+    def _workspace(self, nbytes, device):
+        if self._ws is None or self._ws.numel() < nbytes or self._ws.device != device:
+            self._ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=device)
+        return self._ws
+
+    def _set_illumination(self, i_s, i_r):
+        crop = self._crop
+        if i_s.dim() == self.equation.NDIM + 1 and i_s.shape[0] == 1:
+            i_s, i_r = i_s[0], i_r[0]
+        self.source_illumination = crop(i_s)
+        self.receiver_illumination = crop(i_r)
+
+    def _crop(self, g):
+        p = self.abcn + self.equation.M
+        sl = tuple(slice(p, p + n) for n in self.shape)
+        return g[(Ellipsis,) + sl]
+
+    def _pad_model(self, m):
+        """Replicate-pad a physical model to the runtime grid (autograd crops back)."""
+        p = self.abcn + self.equation.M
+        nd = self.equation.NDIM
+        per_shot = m.dim() == nd + 1
+        x = m if per_shot else m[None]
+        x = F.pad(x[:, None] if nd == 2 else x[:, None], [p, p] * nd, mode="replicate")[:, 0]
+        return x if per_shot else x[0]
+
+    def _mem_mode(self):
+        if isinstance(self.memory, Ckpt):
+            return _lib.MEM_CHECKPOINT, int(self.memory.chunks)
+        return _lib.MEM_BOUNDARY, 0
+
+    # ---------------------------------------------------------------- forward
+    def forward(self, wavelet, sources, receivers, models=None, max_vel=4500.0, pml_freq=25.0):
+        eq = self.equation
+        nd = eq.NDIM
+        dev = self.device
+        if dev.type != "cuda":
+            raise RuntimeError("sweep_b200 runs on a CUDA device only (no CPU path)")
+        if models is None or len(models) != len(eq.MODEL_NAMES):
+            raise ValueError(f"{type(eq).__name__} needs models={list(eq.MODEL_NAMES)}")
+        for name, m in zip(eq.MODEL_NAMES, models):
+            if not isinstance(m, torch.Tensor) or m.dtype != torch.float32:
+                raise TypeError(f"model {name!r} must be a float32 torch.Tensor")
+            if tuple(m.shape[-nd:]) != self.shape:
+                raise ValueError(f"model {name!r} has shape {tuple(m.shape)}, expected {self.shape}")
+        wavelet = _as_tensor(wavelet, torch.float32, dev) if not (
+            isinstance(wavelet, torch.Tensor) and wavelet.device == dev and wavelet.dtype == torch.float32) else wavelet
+        mode, B, nsrc = normalize_io(wavelet, sources, receivers, nd)
+        nt = wavelet.shape[-1]
+        src = np.asarray(sources.detach().cpu() if isinstance(sources, torch.Tensor) else sources, np.int64)
+        rec = np.asarray(receivers.detach().cpu() if isinstance(receivers, torch.Tensor) else receivers, np.int64)
+        src = src.reshape(B, nsrc, nd) + (self.abcn + eq.M)
+        rec = rec.reshape(B, -1, nd) + (self.abcn + eq.M)
+        nrec = rec.shape[1]
+        if mode == "A1":
+            wb = wavelet[None, None, :].expand(B, 1, nt)
+        elif mode == "A2":
+            wb = wavelet[:, None, :]
+        else:
+            wb = wavelet[None, None, :].expand(1, nsrc, nt) if wavelet.dim() == 1 else wavelet[None]
+        for m in models:
+            if m.dim() == nd + 1 and m.shape[0] != B:
+                raise ValueError(f"per-shot model batch ({m.shape[0]}) must equal the shot count ({B})")
+            if m.dim() == nd + 1 and isinstance(eq, Acoustic3D):
+                raise NotImplementedError("Acoustic3D takes one shared model (no per-shot models)")
+        geo = _Geometry(self, B, nsrc, nrec, nt, src, rec, dev, max_vel, pml_freq)
+        mem_mode, ckpt_every = self._mem_mode()
+        padded = [self._pad_model(m.to(dev)) for m in models]
+        if isinstance(eq, (Acoustic, Acoustic3D)):
+            return _AcousticFn.apply(padded[0], wb, self, geo, mem_mode, ckpt_every)
+        raise NotImplementedError(f"{type(eq).__name__} is not built yet")

@@ -1,0 +1,79 @@
+"""The C ABI without a GPU: the library loads, exports every symbol its header
+declares, reports the right ABI version, and the host-side size query and
+argument checks work (no device work is issued)."""
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+HEADER = ROOT / "include" / "sweep_b200.h"
+
+
+def _declared():
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"SWEEP_B200_API\s+\w+\s+(sweep_b200_\w+)\s*\(", text)))
+
+
+def test_header_and_loader_agree():
+    from sweep_b200 import _lib
+    assert sorted(_lib.SYMBOLS) == _declared()
+
+
+def test_library_exports_every_declared_symbol():
+    from sweep_b200 import _lib
+    lib = _lib.load()
+    for name in _declared():
+        assert hasattr(lib, name), name
+    assert lib.sweep_b200_abi_version() == _lib.ABI_VERSION
+
+
+def _desc(B=2, nz=40, nx=60, nt=10, nsrc=1, nrec=3, M=4):
+    from sweep_b200 import _lib
+    d = _lib.AcousticDesc()
+    d.ndim, d.B, d.nz, d.ny, d.nx, d.nt, d.M = 2, B, nz, 1, nx, nt, M
+    for i, p in enumerate([5, 5, 0, 0, 5, 5]):
+        d.pad[i] = p
+    d.dt, d.dz, d.dy, d.dx = 1e-3, 10.0, 1.0, 10.0
+    d.nsrc, d.nrec = nsrc, nrec
+    return d
+
+
+def test_sizes_query_is_host_only():
+    from sweep_b200 import _lib
+    d = _desc()
+    ws, tape = _lib.c_i64(), _lib.c_i64()
+    _lib.call("sweep_b200_acoustic_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
+    n = 2 * 40 * 60
+    assert ws.value >= 14 * n * 4     # 3 adjoint + 8 adjoint-CPML + 3 reconstruction fields
+    # strips (M + 1 = 5 wide) of a 22 x 42 physical box, per step and shot, plus the last two states
+    pz, px = 40 - 2 * 9, 60 - 2 * 9
+    nstrip = 2 * 5 * px + 2 * 5 * (pz - 10)
+    assert tape.value >= (10 * 2 * nstrip + 2 * n) * 4
+
+
+def test_errors_come_back_as_messages():
+    from sweep_b200 import _lib
+    d = _desc(M=3)
+    ws, tape = _lib.c_i64(), _lib.c_i64()
+    with pytest.raises(RuntimeError, match="order 8"):
+        _lib.call("sweep_b200_acoustic_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
+    d = _desc()
+    d.pad[0] = 0
+    with pytest.raises(RuntimeError, match="PML pad"):
+        _lib.call("sweep_b200_acoustic_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
+    with pytest.raises(RuntimeError, match="null"):
+        _lib.call("sweep_b200_acoustic_sizes", None, _lib.MEM_BOUNDARY, 0, ws, tape)
+
+
+def test_propagator_refuses_cpu_and_other_impls():
+    import torch
+    from sweep_b200 import Acoustic, PropTorch
+    with pytest.raises(NotImplementedError):
+        PropTorch(Acoustic(8), shape=(20, 20), impl="eager")
+    p = PropTorch(Acoustic(8), shape=(20, 20), abcn=5, device="cpu")
+    vp = torch.full((20, 20), 2000.0)
+    with pytest.raises(RuntimeError, match="CUDA"):
+        p(np.zeros(10, np.float32), np.array([[5, 5]]), np.array([[[6, 6]]]), models=[vp])

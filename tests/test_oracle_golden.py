@@ -1,0 +1,72 @@
+"""The CPU oracle against the reference's own outputs (tests/golden/, made by
+tests/golden/make_golden.py from the reference's impl='c' host core).
+
+These pin the oracle: every GPU parity test trusts it only because these pass."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+GOLD = Path(__file__).resolve().parent / "golden"
+
+
+def rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def _args(d):
+    return float(d["dh"]), float(d["dt"]), int(d["abcn"])
+
+
+@pytest.mark.parametrize("case", ["acoustic2d_c1", "acoustic2d_multi", "acoustic2d_pershot"])
+def test_acoustic2d_oracle_matches_reference(case):
+    d = np.load(GOLD / f"{case}.npz")
+    obs = O.acoustic_forward(d["vp_true"], d["wavelet"], d["src"], d["rec"], *_args(d))
+    assert rel(obs, d["obs"]) < 2e-5
+    pred, loss, g, gw = O.acoustic_gradient(d["vp_init"], d["wavelet"], d["src"], d["rec"], d["obs"], *_args(d))
+    assert rel(pred, d["pred"]) < 2e-5
+    assert abs(loss - float(d["loss"])) <= 1e-4 * abs(float(d["loss"]))
+    assert rel(g, d["grad_vp"]) < 1e-5
+    if "grad_wavelet" in d:
+        assert rel(gw, d["grad_wavelet"]) < 1e-5
+
+
+def test_acoustic2d_memory_modes_agree_in_reference():
+    """The reference's own memory modes agree; so one backward (boundary
+    saving) stands for all of them."""
+    d = np.load(GOLD / "acoustic2d_multi.npz")
+    assert rel(d["grad_vp_full"], d["grad_vp"]) < 1e-5
+    assert rel(d["grad_vp_ckpt"], d["grad_vp"]) < 1e-5
+
+
+def test_acoustic2d_fp64_oracle_close_to_fp32():
+    d = np.load(GOLD / "acoustic2d_multi.npz")
+    p32, _, g32, _ = O.acoustic_gradient(d["vp_init"], d["wavelet"], d["src"], d["rec"], d["obs"], *_args(d), prec="f32")
+    p64, _, g64, _ = O.acoustic_gradient(d["vp_init"], d["wavelet"], d["src"], d["rec"], d["obs"], *_args(d), prec="f64")
+    assert rel(p32, p64) < 1e-5
+    assert rel(g32, g64) < 1e-4
+
+
+def test_off_grid_receivers_record_zero():
+    d = np.load(GOLD / "acoustic2d_multi.npz")
+    obs = O.acoustic_forward(d["vp_true"], d["wavelet"], d["src"], d["rec"], *_args(d))
+    # shot 1 has 7 receivers; the padding (x = -1000) lands off the grid
+    assert np.all(obs[1, :, 7:, 0] == 0)
+    assert np.all(d["obs"][1, :, 7:, 0] == 0)
+
+
+def test_coefficient_tables_zero_sum():
+    """The float32 Laplacian taps sum to exactly zero and equal the reference
+    kernels' compile-time constants (operators/laplace.cuh:331-335)."""
+    from fractions import Fraction
+    lap, grad = O.fd_tables(4)
+    assert Fraction(float(lap[0])) == 2 * sum(Fraction(float(x)) for x in lap[1:])
+    f = np.float32
+    c0, c1, c2, c3 = f(205 / 72), f(8 / 5), f(-1 / 5), f(8 / 315)
+    c4 = ((f(0.5) * c0 - c1) - c2) - c3
+    assert list(lap[1:]) == [c1, c2, c3, c4]
+    assert list(grad[1:]) == [f(4 / 5), f(-1 / 5), f(4 / 105), f(-1 / 280)]
