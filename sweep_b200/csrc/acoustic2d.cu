@@ -1,8 +1,8 @@
 // acoustic2d.cu -- 2-D constant-density acoustic propagation on B200 (sm_100a):
 // 8th-order-in-space / 2nd-order-in-time leapfrog with CPML, a fused forward
 // step and a fused reverse step (exact adjoint + boundary-saving
-// reconstruction + vp imaging), both tiled over shared memory and batched over
-// shots.
+// reconstruction + vp imaging), both tiled over shared memory, fed by TMA and
+// batched over shots.
 //
 // Numerics follow the reference's compiled path (impl='c'):
 //   forward step       reference src/sweep/csrc/cuda/equations/acoustic2d/forward_split.cu:40-168
@@ -12,20 +12,26 @@
 //   step order         reference src/sweep/csrc/cuda/common/eq_driver.cuh:377-434, 814-880,
 //                      .../acoustic2d/driver_traits.cuh:529-635
 // with the same expression trees (difference-form Laplacian with __fsub_rn
-// taps, fused d(a psi) tap form, the adjoint's transposed CPML terms).
+// taps, fused d(a psi) tap form, the adjoint's transposed CPML terms) in the
+// reference CUDA core's arithmetic mode (flush-to-zero, fast division).
 //
 // Layout and schedule (the B200 part):
-//   * one CTA = one 64x32 (x, z) tile for a group of G shots; the tile of the
-//     stencil input plus its 4-cell halo is staged once per shot in shared
-//     memory and every tap is read from there;
-//   * with a shared model the velocity tile is staged once per CTA for all G
-//     shots, and the gradient of the G shots is summed in registers and
-//     flushed once per step into a Kahan-compensated per-group accumulator;
-//   * point sources, receivers and boundary strips are handled by the CTA
-//     that owns the cell, in the same launch as the stencil (no separate
-//     injection / gather / strip kernels);
+//   * every internal field is pitched: rows of P floats (P = nx rounded up to
+//     32), so each row starts on a 128-byte line and TMA can address it;
+//   * one CTA = one 64 x 32 (x, z) tile for a group of G shots; per shot, one
+//     thread issues TMA tile loads (the stencil input with its 4-cell halo,
+//     and the centre tiles) into shared memory, double-buffered across the
+//     shot loop so the next shot's tiles are in flight while this one computes;
+//   * the model enters as precomputed coefficient fields (vp^2 dt^2 in the two
+//     roundings the reference uses, and vp itself), read once per CTA for a
+//     shared model;
+//   * the gradient of the G shots is summed in registers and flushed once per
+//     step into a Kahan-compensated per-group accumulator;
+//   * point sources, receivers and boundary strips are handled by the CTA that
+//     owns the cell, in the same launch as the stencil;
 //   * one launch per forward step and one per reverse step.
 #include "common.cuh"
+#include "tma.cuh"
 
 namespace sweep {
 namespace a2d {
@@ -35,13 +41,18 @@ constexpr int TX = 64, TZ = 32;      // tile
 constexpr int NTH = 256;             // threads per CTA (8 warps)
 constexpr int SW = TX + 2 * M;       // staged tile width (with halo)
 constexpr int SH = TZ + 2 * M;       // staged tile height
-constexpr int SN = SW * SH;
-constexpr int RPW = TZ / 8;          // rows per warp
-constexpr int CPT = 2 * RPW;         // cells per thread
+constexpr int SN = SW * SH;          // staged halo tile, floats
+constexpr int TN = TX * TZ;          // centre tile, floats
+constexpr int CPT = TN / NTH;        // cells per thread (8)
+
+enum ErrCode { ERR_TMA_WAIT_FWD = 1, ERR_TMA_WAIT_REV = 2 };
 
 struct Params {
     int B, nz, nx, nt, nsrc, nrec;
+    int P;                           // row pitch (floats)
     int ntx, ntz, G, per_shot;
+    long long S;                     // shot stride (nz * P)
+    long long ms;                    // model stride: 0 (shared) or S
     float dt, dz, dx;
     float lc[M + 1], gc[M + 1];
     int z0, z1, x0, x1;              // physical box (runtime grid)
@@ -51,46 +62,48 @@ struct Params {
     int wzl, wzh, wxl, wxh;          // strip widths
     int n_top, n_bot, n_left, nstrip;
     const float *az, *bz, *dbz, *ax, *bx, *dbx;
-    const float* vp;
-    long long vp_stride;
+    const float* cf;                 // ((v*v)*dt)*dt, pitched (forward / reconstruction)
+    const float* vv;                 // v, pitched (imaging)
     const float* wavelet;
     EventTable src, rec;
+    int* err;
+};
+
+struct FwdMaps {
+    CUtensorMap halo[3];             // the three wavefield buffers, (SW x SH) boxes
+    CUtensorMap tile[3];             // the same buffers, (TX x TZ) boxes
+};
+
+struct RevMaps {
+    CUtensorMap lh[3], lt[3];        // adjoint field buffers: halo / centre boxes
+    CUtensorMap rh[3], rt[3];        // reconstruction buffers: halo / centre boxes
+    CUtensorMap ch;                  // (v*v)*(dt*dt), halo box
 };
 
 struct FwdPtrs {
-    const float* u_prev; const float* u_now; float* u_next;
+    float* u_next;
     const float* psix; const float* psiz; float* psixn; float* psizn;
     float* zetax; float* zetaz;
     float* record;                   // (B, nt, nrec)
     float* strips;                   // this step's strip slot (B, nstrip) or null
+    int now, prev;                   // buffer indices of u_now / u_prev
 };
 
 struct RevPtrs {
-    const float* l_prev; const float* l_now; float* l_next;
+    float* l_next;
     const float *apx, *apz, *azx, *azz;   // adjoint CPML memories (read)
     float *apx_o, *apz_o, *azx_o, *azz_o; // adjoint CPML memories (written)
-    const float* r_prev; const float* r_now; float* r_next;
+    float* r_next;
     const float* strips;             // saved U[it-1] strips (B, nstrip) or null
     const float* adj;                // (B, nt, nrec)
     float* grad_w;                   // (B, nsrc, nt) or null
-    float* gacc; float* gcomp;       // Kahan accumulator slots (nslot, cells)
-    float* illum_s; float* illum_r;  // (nslot, cells) or null
+    float* gacc; float* gcomp;       // Kahan accumulator slots (nslot, S)
+    float* illum_s; float* illum_r;  // (nslot, S) or null
+    int lnow, lprev, rnow, rprev;    // buffer indices
 };
 
 // ------------------------------------------------------------------ device
 __device__ __forceinline__ float tap(float uk, float u0) { return __fsub_rn(uk, u0); }
-
-// Stage a (SH x SW) window of field g (one shot, nz x nx) whose (0,0) is the
-// runtime cell (tz0 - M, tx0 - M); cells off the grid read 0.
-__device__ __forceinline__ void stage(float* s, const float* __restrict__ g, int nz, int nx,
-                                      int tz0, int tx0)
-{
-    for (int i = threadIdx.x; i < SN; i += NTH) {
-        const int r = i / SW, c = i - r * SW;
-        const int iz = tz0 - M + r, ix = tx0 - M + c;
-        s[i] = (iz >= 0 && iz < nz && ix >= 0 && ix < nx) ? __ldg(g + (long long)iz * nx + ix) : 0.f;
-    }
-}
 
 // Difference-form Laplacian along the axis of stride `st` (1: x, SW: z) at the
 // staged centre p (reference operators/laplace.cuh:327-380; minus tap first).
@@ -115,9 +128,9 @@ __device__ __forceinline__ float grad_s(const float* p, int st, const Params& P,
 }
 
 // Fused d(a psi)/d axis in tap form (reference acoustic2d/kernels.cuh:30-77):
-// profile a at axis index ia, psi read from global memory at linear index i.
+// profile a at axis index ia, psi read from global memory at offset i.
 __device__ __forceinline__ float grad_apsi(const float* __restrict__ a, int ia,
-                                           const float* __restrict__ psi, long long i, long long st,
+                                           const float* __restrict__ psi, int i, int st,
                                            const Params& P, float h)
 {
     float acc = P.gc[1] * (__ldg(a + ia + 1) * __ldg(psi + i + st) - __ldg(a + ia - 1) * __ldg(psi + i - st));
@@ -146,65 +159,99 @@ __device__ __forceinline__ bool computed(const Params& P, int iz, int ix)
     return iz >= M && iz < P.nz - M && ix >= M && ix < P.nx - M;
 }
 
+__device__ __forceinline__ int cell_r(int k) { return (threadIdx.x >> 5) + 8 * (k >> 1); }
+__device__ __forceinline__ int cell_c(int k) { return (threadIdx.x & 31) + 32 * (k & 1); }
+
 // ----------------------------------------------------------- forward step
+struct FwdSmem {
+    float now[2][SN];
+    float prev[2][TN];
+    float out[TN];
+    uint64_t bar[2];
+};
+
 // u_next = 2 u - u_prev + vp^2 dt^2 (Lap u + CPML terms) on [M, n-M)^2, then
 // (same launch) strip save of u_now, source injection into u_next and receiver
 // gather from u_next -- the per-step order of the reference's forward loop.
-__global__ void __launch_bounds__(NTH) fwd_kernel(const Params P, const FwdPtrs F, const int it)
+__global__ void __launch_bounds__(NTH) fwd_kernel(const __grid_constant__ FwdMaps MP, const Params P,
+                                                  const FwdPtrs F, const int it)
 {
-    extern __shared__ float smem[];
-    float* s_u = smem;               // SN
-    float* s_o = smem + SN;          // TZ * TX staging of u_next (event tiles)
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    FwdSmem& sm = *reinterpret_cast<FwdSmem*>(smem_raw);
     const int tx0 = blockIdx.x * TX, tz0 = blockIdx.y * TZ;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const long long N = (long long)P.nz * P.nx;
+    const int b0 = blockIdx.z * P.G;
+    const int nloc = min(P.G, P.B - b0);
     const int tile = blockIdx.y * P.ntx + blockIdx.x;
     const int ntiles = P.ntx * P.ntz;
     const bool band = tx0 < P.bx_lo || tx0 + TX > P.bx_hi || tz0 < P.bz_lo || tz0 + TZ > P.bz_hi;
+    const bool full = tx0 >= M && tx0 + TX <= P.nx - M && tz0 >= M && tz0 + TZ <= P.nz - M;
     const bool strip_tile = F.strips != nullptr &&
         tx0 < P.x1 && tx0 + TX > P.x0 && tz0 < P.z1 && tz0 + TZ > P.z0 &&
         !(tx0 >= P.x0 + P.wxl && tx0 + TX <= P.x1 - P.wxh &&
           tz0 >= P.z0 + P.wzl && tz0 + TZ <= P.z1 - P.wzh);
+    constexpr uint32_t kBytes = (SN + TN) * 4;
 
-    for (int g = 0; g < P.G; ++g) {
-        const int b = blockIdx.z * P.G + g;
-        if (b >= P.B) break;
-        const float* un = F.u_now + b * N;
-        const float* vp = P.vp + b * P.vp_stride;
-        __syncthreads();
-        stage(s_u, un, P.nz, P.nx, tz0, tx0);
-        __syncthreads();
+    if (threadIdx.x == 0) {
+        tma::mbar_init(&sm.bar[0], 1);
+        tma::mbar_init(&sm.bar[1], 1);
+        tma::fence_barrier_init();
+    }
+    __syncthreads();
+    auto issue = [&](int s, int b) {
+        tma::mbar_expect_tx(&sm.bar[s], kBytes);
+        tma::load_3d(sm.now[s], &MP.halo[F.now], &sm.bar[s], tx0 - M, tz0 - M, b);
+        tma::load_3d(sm.prev[s], &MP.tile[F.prev], &sm.bar[s], tx0, tz0, b);
+    };
+    if (threadIdx.x == 0) {
+        issue(0, b0);
+        if (nloc > 1) issue(1, b0 + 1);
+    }
+
+    // model coefficients of this thread's cells (shared model: once per CTA)
+    float cf[CPT];
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) {
+        const int iz = tz0 + cell_r(k), ix = tx0 + cell_c(k);
+        cf[k] = computed(P, iz, ix) ? __ldg(P.cf + b0 * P.ms + iz * P.P + ix) : 0.f;
+    }
+
+    for (int g = 0; g < nloc; ++g) {
+        const int b = b0 + g;
+        const int s = g & 1;
+        const bool ok = tma::mbar_wait(&sm.bar[s], (g >> 1) & 1, P.err, ERR_TMA_WAIT_FWD);
+        if (__syncthreads_or(!ok)) return;
+        const float* now = sm.now[s];
+        const float* prev = sm.prev[s];
+        const long long bo = (long long)b * P.S;
 
         float out[CPT];
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
-            const int r = warp + 8 * (k >> 1), c = lane + 32 * (k & 1);
+            const int r = cell_r(k), c = cell_c(k);
             const int iz = tz0 + r, ix = tx0 + c;
             out[k] = 0.f;
-            if (!computed(P, iz, ix)) continue;
-            const long long i = (long long)iz * P.nx + ix;
-            const float* p = s_u + (r + M) * SW + (c + M);
+            if (!full && !computed(P, iz, ix)) continue;
+            const float* p = now + (r + M) * SW + (c + M);
             const float lx = lap_s(p, 1, P, P.dx);
             const float lz = lap_s(p, SW, P, P.dz);
-            const float v = __ldg(vp + i);
-            const float v2dt2 = ((v * v) * P.dt) * P.dt;
             float w;
             const bool cx = ix < P.bx_lo || ix >= P.bx_hi;
             const bool cz = iz < P.bz_lo || iz >= P.bz_hi;
             if (!band || (!cx && !cz)) {
                 w = lx + lz;
             } else {
+                const int i = iz * P.P + ix;
                 w = 0.f;
                 if (cx) {
                     const float a = __ldg(P.ax + ix), bb = __ldg(P.bx + ix), db = __ldg(P.dbx + ix);
                     const float du = grad_s(p, 1, P, P.dx);
-                    const float* psx = F.psix + b * N;
+                    const float* psx = F.psix + bo;
                     const float dap = grad_apsi(P.ax, ix, psx, i, 1, P, P.dx);
                     const float tmp = ((1.0f + bb) * lx + db * du) + dap;
-                    float* zx = F.zetax + b * N;
+                    float* zx = F.zetax + bo;
                     const float z = zx[i];
                     w += (1.0f + bb) * tmp + a * z;
-                    F.psixn[b * N + i] = bb * du + a * __ldg(psx + i);
+                    F.psixn[bo + i] = bb * du + a * __ldg(psx + i);
                     zx[i] = bb * tmp + a * z;
                 } else {
                     w += lx;
@@ -212,19 +259,19 @@ __global__ void __launch_bounds__(NTH) fwd_kernel(const Params P, const FwdPtrs 
                 if (cz) {
                     const float a = __ldg(P.az + iz), bb = __ldg(P.bz + iz), db = __ldg(P.dbz + iz);
                     const float du = grad_s(p, SW, P, P.dz);
-                    const float* psz = F.psiz + b * N;
-                    const float dap = grad_apsi(P.az, iz, psz, i, P.nx, P, P.dz);
+                    const float* psz = F.psiz + bo;
+                    const float dap = grad_apsi(P.az, iz, psz, i, P.P, P, P.dz);
                     const float tmp = ((1.0f + bb) * lz + db * du) + dap;
-                    float* zz = F.zetaz + b * N;
+                    float* zz = F.zetaz + bo;
                     const float z = zz[i];
                     w += (1.0f + bb) * tmp + a * z;
-                    F.psizn[b * N + i] = bb * du + a * __ldg(psz + i);
+                    F.psizn[bo + i] = bb * du + a * __ldg(psz + i);
                     zz[i] = bb * tmp + a * z;
                 } else {
                     w += lz;
                 }
             }
-            out[k] = 2.0f * p[0] - __ldg(F.u_prev + b * N + i) + v2dt2 * w;
+            out[k] = 2.0f * p[0] - prev[r * TX + c] + cf[k] * w;
             if (strip_tile) {
                 const int si = strip_index(P, iz, ix);
                 if (si >= 0) F.strips[(long long)b * P.nstrip + si] = p[0];
@@ -237,33 +284,44 @@ __global__ void __launch_bounds__(NTH) fwd_kernel(const Params P, const FwdPtrs 
         const int r_beg = P.rec.off[key], r_end = P.rec.off[key + 1];
         if (s_beg != s_end || r_beg != r_end) {
 #pragma unroll
-            for (int k = 0; k < CPT; ++k)
-                s_o[(warp + 8 * (k >> 1)) * TX + lane + 32 * (k & 1)] = out[k];
+            for (int k = 0; k < CPT; ++k) sm.out[cell_r(k) * TX + cell_c(k)] = out[k];
             __syncthreads();
             for (int e = s_beg + threadIdx.x; e < s_end; e += NTH) {
                 const int2 ev = P.src.ev[e];
-                atomicAdd(s_o + ev.x, __ldg(P.wavelet + (long long)ev.y * P.nt + it));
+                atomicAdd(sm.out + ev.x, __ldg(P.wavelet + (long long)ev.y * P.nt + it));
             }
             __syncthreads();
             for (int e = r_beg + threadIdx.x; e < r_end; e += NTH) {
                 const int2 ev = P.rec.ev[e];
                 const int rb = ev.y / P.nrec, rr = ev.y - rb * P.nrec;
-                F.record[((long long)rb * P.nt + it) * P.nrec + rr] = s_o[ev.x];
+                F.record[((long long)rb * P.nt + it) * P.nrec + rr] = sm.out[ev.x];
             }
 #pragma unroll
-            for (int k = 0; k < CPT; ++k)
-                out[k] = s_o[(warp + 8 * (k >> 1)) * TX + lane + 32 * (k & 1)];
+            for (int k = 0; k < CPT; ++k) out[k] = sm.out[cell_r(k) * TX + cell_c(k)];
         }
+        float* un = F.u_next + bo;
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
-            const int r = warp + 8 * (k >> 1), c = lane + 32 * (k & 1);
-            const int iz = tz0 + r, ix = tx0 + c;
-            if (computed(P, iz, ix)) F.u_next[b * N + (long long)iz * P.nx + ix] = out[k];
+            const int iz = tz0 + cell_r(k), ix = tx0 + cell_c(k);
+            if (full || computed(P, iz, ix)) un[iz * P.P + ix] = out[k];
         }
+        __syncthreads();                 // every thread is done with stage s
+        if (threadIdx.x == 0 && g + 2 < nloc) issue(s, b + 2);
     }
 }
 
 // ------------------------------------------------------------ reverse step
+struct RevSmem {
+    float l[2][SN];                  // lambda(it+1) tile + halo
+    float lp[2][TN];                 // lambda(it+2) centre
+    float r[2][SN];                  // u(it) tile + halo
+    float rp[2][TN];                 // u(it+1) centre
+    float c[SN];                     // (v*v)*(dt*dt) tile + halo
+    float lo[TN];                    // staging (event tiles)
+    float ro[TN];
+    uint64_t bar[3];
+};
+
 // One launch per reverse step `it` of the boundary-saving backward:
 //   lambda_next = exact adjoint step of lambda (CPML transposed in the ring),
 //   + record cotangent at the receivers               (-> lambda(it))
@@ -272,65 +330,85 @@ __global__ void __launch_bounds__(NTH) fwd_kernel(const Params P, const FwdPtrs 
 //   saved strips elsewhere in the physical box, and the vp image
 //   2 dt^2 u_tt lambda(it) / vp accumulated, u_tt = (u(it-1) - s(it) - 2 u(it) + u(it+1)) / dt^2;
 //   then the source added back.
-__global__ void __launch_bounds__(NTH) rev_kernel(const Params P, const RevPtrs R, const int it,
-                                                   const int do_recon)
+__global__ void __launch_bounds__(NTH) rev_kernel(const __grid_constant__ RevMaps MP, const Params P,
+                                                  const RevPtrs R, const int it, const int do_recon)
 {
-    extern __shared__ float smem[];
-    float* s_l = smem;               // lambda(it+1) tile + halo
-    float* s_c = smem + SN;          // vp^2 dt^2 tile + halo
-    float* s_r = smem + 2 * SN;      // u(it) tile + halo (reconstruction)
-    float* s_lo = smem + 3 * SN;     // staging (event tiles)
-    float* s_ro = s_lo + TZ * TX;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    RevSmem& sm = *reinterpret_cast<RevSmem*>(smem_raw);
     const int tx0 = blockIdx.x * TX, tz0 = blockIdx.y * TZ;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const long long N = (long long)P.nz * P.nx;
+    const int b0 = blockIdx.z * P.G;
+    const int nloc = min(P.G, P.B - b0);
     const int tile = blockIdx.y * P.ntx + blockIdx.x;
     const int ntiles = P.ntx * P.ntz;
     const float dt2 = P.dt * P.dt;
     const float invdx2 = 1.0f / (P.dx * P.dx), invdz2 = 1.0f / (P.dz * P.dz);
     const float invdx = 1.0f / P.dx, invdz = 1.0f / P.dz;
     const bool ring = tx0 < P.px0 || tx0 + TX > P.px1 || tz0 < P.pz0 || tz0 + TZ > P.pz1;
+    const bool full = tx0 >= M && tx0 + TX <= P.nx - M && tz0 >= M && tz0 + TZ <= P.nz - M;
     const bool phys_any = tx0 < P.x1 && tx0 + TX > P.x0 && tz0 < P.z1 && tz0 + TZ > P.z0;
     const bool phys_tile = do_recon && phys_any;
-    const bool recon_tile = phys_tile && tx0 < P.rx1 && tx0 + TX > P.rx0 && tz0 < P.rz1 && tz0 + TZ > P.rz0;
+    const uint32_t kBytes = (SN + TN + (phys_tile ? SN + TN : 0)) * 4;
+
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < 3; ++i) tma::mbar_init(&sm.bar[i], 1);
+        tma::fence_barrier_init();
+    }
+    __syncthreads();
+    auto issue = [&](int s, int b) {
+        tma::mbar_expect_tx(&sm.bar[s], kBytes);
+        tma::load_3d(sm.l[s], &MP.lh[R.lnow], &sm.bar[s], tx0 - M, tz0 - M, b);
+        tma::load_3d(sm.lp[s], &MP.lt[R.lprev], &sm.bar[s], tx0, tz0, b);
+        if (phys_tile) {
+            tma::load_3d(sm.r[s], &MP.rh[R.rnow], &sm.bar[s], tx0 - M, tz0 - M, b);
+            tma::load_3d(sm.rp[s], &MP.rt[R.rprev], &sm.bar[s], tx0, tz0, b);
+        }
+    };
+    if (threadIdx.x == 0) {
+        tma::mbar_expect_tx(&sm.bar[2], SN * 4);
+        tma::load_3d(sm.c, &MP.ch, &sm.bar[2], tx0 - M, tz0 - M, P.ms ? b0 : 0);
+        issue(0, b0);
+        if (nloc > 1) issue(1, b0 + 1);
+    }
+    // per-cell model values (shared model or one shot per CTA: loaded once)
+    float cfr[CPT], vr[CPT];
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) {
+        const int iz = tz0 + cell_r(k), ix = tx0 + cell_c(k);
+        const bool in = computed(P, iz, ix);
+        cfr[k] = in ? __ldg(P.cf + b0 * P.ms + iz * P.P + ix) : 0.f;
+        vr[k] = in ? __ldg(P.vv + b0 * P.ms + iz * P.P + ix) : 1.f;
+    }
+    {
+        const bool ok = tma::mbar_wait(&sm.bar[2], 0, P.err, ERR_TMA_WAIT_REV);
+        if (__syncthreads_or(!ok)) return;
+    }
 
     float gsum[CPT], isum_s[CPT], isum_r[CPT];
 #pragma unroll
     for (int k = 0; k < CPT; ++k) { gsum[k] = 0.f; isum_s[k] = 0.f; isum_r[k] = 0.f; }
-    bool staged_c = false;
 
-    for (int g = 0; g < P.G; ++g) {
-        const int b = blockIdx.z * P.G + g;
-        if (b >= P.B) break;
-        const long long bo = b * N;
-        const float* vp = P.vp + b * P.vp_stride;
-        __syncthreads();
-        if (!staged_c) {
-            // vp^2 dt^2 with halo (GW_AT of reference acoustic2d/kernels.cuh:370)
-            for (int i = threadIdx.x; i < SN; i += NTH) {
-                const int r = i / SW, c = i - r * SW;
-                const int iz = tz0 - M + r, ix = tx0 - M + c;
-                float v = 0.f;
-                if (iz >= 0 && iz < P.nz && ix >= 0 && ix < P.nx) v = __ldg(vp + (long long)iz * P.nx + ix);
-                s_c[i] = (v * v) * dt2;
-            }
-            staged_c = !P.per_shot;
-        }
-        stage(s_l, R.l_now + bo, P.nz, P.nx, tz0, tx0);
-        if (recon_tile) stage(s_r, R.r_now + bo, P.nz, P.nx, tz0, tx0);
-        __syncthreads();
+    for (int g = 0; g < nloc; ++g) {
+        const int b = b0 + g;
+        const int s = g & 1;
+        const bool ok = tma::mbar_wait(&sm.bar[s], (g >> 1) & 1, P.err, ERR_TMA_WAIT_REV);
+        if (__syncthreads_or(!ok)) return;
+        const long long bo = (long long)b * P.S;
+        const float* sl = sm.l[s];
+        const float* slp = sm.lp[s];
+        const float* sr = sm.r[s];
+        const float* srp = sm.rp[s];
 
         float lo[CPT], ro[CPT];
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
-            const int r = warp + 8 * (k >> 1), c = lane + 32 * (k & 1);
+            const int r = cell_r(k), c = cell_c(k);
             const int iz = tz0 + r, ix = tx0 + c;
             lo[k] = 0.f; ro[k] = 0.f;
-            if (!computed(P, iz, ix)) continue;
-            const long long i = (long long)iz * P.nx + ix;
+            if (!full && !computed(P, iz, ix)) continue;
+            const int i = iz * P.P + ix;
             const int sc = (r + M) * SW + (c + M);
-            const float* pl = s_l + sc;
-            const float* pc = s_c + sc;
+            const float* pl = sl + sc;
+            const float* pc = sm.c + sc;
             const float gun = pl[0];
             const float gw = pc[0] * gun;
             const bool pure = !ring || (ix >= P.px0 && ix < P.px1 && iz >= P.pz0 && iz < P.pz1);
@@ -341,7 +419,7 @@ __global__ void __launch_bounds__(NTH) rev_kernel(const Params P, const RevPtrs 
                     lapx += P.lc[kk] * (tap(pc[kk] * pl[kk], gw) + tap(pc[-kk] * pl[-kk], gw));
                     lapz += P.lc[kk] * (tap(pc[kk * SW] * pl[kk * SW], gw) + tap(pc[-kk * SW] * pl[-kk * SW], gw));
                 }
-                lo[k] = 2.0f * gun - __ldg(R.l_prev + bo + i) + lapx * invdx2 + lapz * invdz2;
+                lo[k] = 2.0f * gun - slp[r * TX + c] + lapx * invdx2 + lapz * invdz2;
             } else {
                 const float ax_ = __ldg(P.ax + ix), az_ = __ldg(P.az + iz);
                 const float bx_ = __ldg(P.bx + ix), bz_ = __ldg(P.bz + iz);
@@ -371,7 +449,7 @@ __global__ void __launch_bounds__(NTH) rev_kernel(const Params P, const RevPtrs 
 #pragma unroll
                 for (int kk = 1; kk <= M; ++kk) {
                     const int cp = iz + kk, cm = iz - kk;
-                    const long long o = (long long)kk * P.nx;
+                    const int o = kk * P.P;
                     const float bp = __ldg(P.bz + cp), bm = __ldg(P.bz + cm);
                     const float tp = bp * __ldg(zz + i + o) + ((1.0f + bp) * pc[kk * SW]) * pl[kk * SW];
                     const float tm = bm * __ldg(zz + i - o) + ((1.0f + bm) * pc[-kk * SW]) * pl[-kk * SW];
@@ -381,7 +459,7 @@ __global__ void __launch_bounds__(NTH) rev_kernel(const Params P, const RevPtrs 
                     Dqz += P.gc[kk] * (tp - tm);
                 }
                 Lz *= invdz2; Dgz *= invdz; Dqz *= invdz;
-                lo[k] = 2.0f * gun - __ldg(R.l_prev + bo + i) + (Lx + Lz - Dgx - Dgz);
+                lo[k] = 2.0f * gun - slp[r * TX + c] + (Lx + Lz - Dgx - Dgz);
                 R.apx_o[bo + i] = ax_ * (__ldg(px + i) - Dqx);
                 R.apz_o[bo + i] = az_ * (__ldg(pz + i) - Dqz);
                 R.azx_o[bo + i] = ax_ * (zx0 + gw);
@@ -389,10 +467,9 @@ __global__ void __launch_bounds__(NTH) rev_kernel(const Params P, const RevPtrs 
             }
             if (phys_tile && iz >= P.z0 && iz < P.z1 && ix >= P.x0 && ix < P.x1) {
                 if (iz >= P.rz0 && iz < P.rz1 && ix >= P.rx0 && ix < P.rx1) {
-                    const float* pr = s_r + sc;
-                    const float v = __ldg(vp + i);
+                    const float* pr = sr + sc;
                     const float wsum = lap_s(pr, 1, P, P.dx) + lap_s(pr, SW, P, P.dz);
-                    ro[k] = 2.0f * pr[0] - __ldg(R.r_prev + bo + i) + (v * v) * P.dt * P.dt * wsum;
+                    ro[k] = 2.0f * pr[0] - srp[r * TX + c] + cfr[k] * wsum;
                 } else {
                     ro[k] = __ldg(R.strips + (long long)b * P.nstrip + strip_index(P, iz, ix));
                 }
@@ -406,54 +483,53 @@ __global__ void __launch_bounds__(NTH) rev_kernel(const Params P, const RevPtrs 
         if (events) {
 #pragma unroll
             for (int k = 0; k < CPT; ++k) {
-                const int o = (warp + 8 * (k >> 1)) * TX + lane + 32 * (k & 1);
-                s_lo[o] = lo[k]; s_ro[o] = ro[k];
+                const int o = cell_r(k) * TX + cell_c(k);
+                sm.lo[o] = lo[k]; sm.ro[o] = ro[k];
             }
             __syncthreads();
             for (int e = r_beg + threadIdx.x; e < r_end; e += NTH) {
                 const int2 ev = P.rec.ev[e];
                 const int rb = ev.y / P.nrec, rr = ev.y - rb * P.nrec;
-                atomicAdd(s_lo + ev.x, __ldg(R.adj + ((long long)rb * P.nt + it) * P.nrec + rr));
+                atomicAdd(sm.lo + ev.x, __ldg(R.adj + ((long long)rb * P.nt + it) * P.nrec + rr));
             }
             if (do_recon) {
                 for (int e = s_beg + threadIdx.x; e < s_end; e += NTH) {
                     const int2 ev = P.src.ev[e];
                     const int iz = tz0 + ev.x / TX, ix = tx0 + ev.x % TX;
                     if (strip_index(P, iz, ix) >= 0)
-                        atomicAdd(s_ro + ev.x, -__ldg(P.wavelet + (long long)ev.y * P.nt + it));
+                        atomicAdd(sm.ro + ev.x, -__ldg(P.wavelet + (long long)ev.y * P.nt + it));
                 }
             }
             __syncthreads();
             if (R.grad_w) {
                 for (int e = s_beg + threadIdx.x; e < s_end; e += NTH) {
                     const int2 ev = P.src.ev[e];
-                    R.grad_w[(long long)ev.y * P.nt + it] = s_lo[ev.x];
+                    R.grad_w[(long long)ev.y * P.nt + it] = sm.lo[ev.x];
                 }
             }
 #pragma unroll
             for (int k = 0; k < CPT; ++k) {
-                const int o = (warp + 8 * (k >> 1)) * TX + lane + 32 * (k & 1);
-                lo[k] = s_lo[o]; ro[k] = s_ro[o];
+                const int o = cell_r(k) * TX + cell_c(k);
+                lo[k] = sm.lo[o]; ro[k] = sm.ro[o];
             }
         }
 
         // imaging (physical box), illumination, stores
+        float* ln = R.l_next + bo;
         float gl[CPT];
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
-            const int r = warp + 8 * (k >> 1), c = lane + 32 * (k & 1);
+            const int r = cell_r(k), c = cell_c(k);
             const int iz = tz0 + r, ix = tx0 + c;
             gl[k] = 0.f;
-            if (!computed(P, iz, ix)) continue;
-            const long long i = (long long)iz * P.nx + ix;
-            R.l_next[bo + i] = lo[k];
+            if (!full && !computed(P, iz, ix)) continue;
+            ln[iz * P.P + ix] = lo[k];
             if (!(phys_any && iz >= P.z0 && iz < P.z1 && ix >= P.x0 && ix < P.x1)) continue;
             if (do_recon) {
-                const float u0 = recon_tile ? s_r[(r + M) * SW + (c + M)] : __ldg(R.r_now + bo + i);
-                const float up = __ldg(R.r_prev + bo + i);
-                const float v = __ldg(vp + i);
+                const float u0 = sr[(r + M) * SW + (c + M)];
+                const float up = srp[r * TX + c];
                 const float utt = (ro[k] - 2 * u0 + up) / dt2;
-                gl[k] = 2.f * P.dt * P.dt * utt * lo[k] / v;
+                gl[k] = 2.f * P.dt * P.dt * utt * lo[k] / vr[k];
                 if (R.illum_s) isum_s[k] += utt * utt;
             }
             if (R.illum_s) isum_r[k] += lo[k] * lo[k];
@@ -462,49 +538,35 @@ __global__ void __launch_bounds__(NTH) rev_kernel(const Params P, const RevPtrs 
             __syncthreads();
             for (int e = s_beg + threadIdx.x; e < s_end; e += NTH) {
                 const int2 ev = P.src.ev[e];
-                atomicAdd(s_ro + ev.x, __ldg(P.wavelet + (long long)ev.y * P.nt + it));
+                atomicAdd(sm.ro + ev.x, __ldg(P.wavelet + (long long)ev.y * P.nt + it));
             }
             __syncthreads();
 #pragma unroll
-            for (int k = 0; k < CPT; ++k)
-                ro[k] = s_ro[(warp + 8 * (k >> 1)) * TX + lane + 32 * (k & 1)];
+            for (int k = 0; k < CPT; ++k) ro[k] = sm.ro[cell_r(k) * TX + cell_c(k)];
         }
-#pragma unroll
-        for (int k = 0; k < CPT; ++k) {
-            const int r = warp + 8 * (k >> 1), c = lane + 32 * (k & 1);
-            const int iz = tz0 + r, ix = tx0 + c;
-            if (phys_tile && iz >= P.z0 && iz < P.z1 && ix >= P.x0 && ix < P.x1)
-                R.r_next[bo + (long long)iz * P.nx + ix] = ro[k];
-            gsum[k] += gl[k];
-        }
-        if (P.per_shot && (do_recon || R.illum_s)) {
-            // flush this shot into its own slot
+        if (phys_tile) {
+            float* rn = R.r_next + bo;
 #pragma unroll
             for (int k = 0; k < CPT; ++k) {
-                const int r = warp + 8 * (k >> 1), c = lane + 32 * (k & 1);
-                const int iz = tz0 + r, ix = tx0 + c;
-                if (!(phys_any && iz >= P.z0 && iz < P.z1 && ix >= P.x0 && ix < P.x1)) continue;
-                const long long o = bo + (long long)iz * P.nx + ix;
-                const float y = gsum[k] - R.gcomp[o];
-                const float t = R.gacc[o] + y;
-                R.gcomp[o] = (t - R.gacc[o]) - y;
-                R.gacc[o] = t;
-                gsum[k] = 0.f;
-                if (R.illum_s) {
-                    R.illum_s[o] += isum_s[k]; R.illum_r[o] += isum_r[k];
-                    isum_s[k] = 0.f; isum_r[k] = 0.f;
-                }
+                const int iz = tz0 + cell_r(k), ix = tx0 + cell_c(k);
+                if (iz >= P.z0 && iz < P.z1 && ix >= P.x0 && ix < P.x1) rn[iz * P.P + ix] = ro[k];
             }
         }
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) gsum[k] += gl[k];
+        __syncthreads();                 // every thread is done with stage s
+        if (threadIdx.x == 0 && g + 2 < nloc) issue(s, b + 2);
     }
-    if (!P.per_shot && phys_any && (do_recon || R.illum_s)) {
-        const long long so = (long long)blockIdx.z * N;
+
+    // Kahan-compensated flush into this CTA's accumulator slot (per shot for
+    // per-shot models, which run one shot per CTA; per shot group otherwise)
+    if (phys_any && (do_recon || R.illum_s)) {
+        const long long so = (long long)(P.per_shot ? b0 : blockIdx.z) * P.S;
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
-            const int r = warp + 8 * (k >> 1), c = lane + 32 * (k & 1);
-            const int iz = tz0 + r, ix = tx0 + c;
+            const int iz = tz0 + cell_r(k), ix = tx0 + cell_c(k);
             if (!(iz >= P.z0 && iz < P.z1 && ix >= P.x0 && ix < P.x1)) continue;
-            const long long o = so + (long long)iz * P.nx + ix;
+            const long long o = so + iz * P.P + ix;
             const float y = gsum[k] - R.gcomp[o];
             const float t = R.gacc[o] + y;
             R.gcomp[o] = (t - R.gacc[o]) - y;
@@ -514,19 +576,43 @@ __global__ void __launch_bounds__(NTH) rev_kernel(const Params P, const RevPtrs 
     }
 }
 
-// Sum the Kahan slots (value minus compensation) into the output gradient.
+// Model-derived fields, pitched: cf = ((v*v)*dt)*dt (forward, reconstruction),
+// ca = (v*v)*(dt*dt) (adjoint taps), vv = v (imaging); 0 (vv: 1) in the pitch pad.
+__global__ void prep_kernel(const float* __restrict__ vp, int nm, int nz, int nx, int P, float dt,
+                            float* __restrict__ cf, float* __restrict__ ca, float* __restrict__ vv)
+{
+    const long long n = (long long)nm * nz * P;
+    const float dt2 = dt * dt;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long row = i / P;
+        const int ix = (int)(i - row * P);
+        if (ix < nx) {
+            const float v = vp[row * nx + ix];
+            cf[i] = ((v * v) * dt) * dt;
+            ca[i] = (v * v) * dt2;
+            vv[i] = v;
+        } else {
+            cf[i] = 0.f; ca[i] = 0.f; vv[i] = 1.f;
+        }
+    }
+}
+
+// Sum the Kahan slots (value minus compensation) into the caller's unpitched
+// gradient (and illuminations).
 __global__ void finalize_kernel(const float* __restrict__ acc, const float* __restrict__ comp,
                                 const float* __restrict__ is, const float* __restrict__ ir,
-                                int nslot_in, int nout, long long N,
+                                int nslot_in, int nout, int nz, int nx, int P,
                                 float* __restrict__ grad, float* __restrict__ ois, float* __restrict__ oir)
 {
+    const long long N = (long long)nz * nx, S = (long long)nz * P;
     const long long n = (long long)nout * N;
     const int per = nslot_in / nout;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const long long o = i / N, c = i - o * N;
+        const long long iz = c / nx, ix = c - iz * nx;
         float s = 0.f, a = 0.f, bsum = 0.f;
         for (int k = 0; k < per; ++k) {
-            const long long j = (o * per + k) * N + c;
+            const long long j = (o * per + k) * S + iz * P + ix;
             s += acc[j] - comp[j];
             if (is) { a += is[j]; bsum += ir[j]; }
         }
@@ -535,17 +621,28 @@ __global__ void finalize_kernel(const float* __restrict__ acc, const float* __re
     }
 }
 
+// Unpitched (B, nz, nx) <-> pitched (B, nz, P) copies of whole wavefields.
+__global__ void pitch_copy_kernel(const float* __restrict__ src, float* __restrict__ dst, int B, int nz, int nx,
+                                  int P, int to_pitched)
+{
+    const long long n = (long long)B * nz * nx;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long row = i / nx, ix = i - row * nx;
+        if (to_pitched) dst[row * P + ix] = src[i];
+        else dst[i] = src[row * P + ix];
+    }
+}
+
 // ------------------------------------------------------------------- host
 struct Plan {
     Params P;
-    int nslot;            // gradient accumulator slots
-    long long N;
+    int nslot;                       // gradient accumulator slots
+    int nm;                          // model copies (1 shared, B per-shot)
     dim3 grid;
 };
 
-static void build_events(const Plan& pl, const std::vector<int32_t>& loc, int n, HostEvents& out)
+static void build_events(const Params& P, const std::vector<int32_t>& loc, int n, HostEvents& out)
 {
-    const Params& P = pl.P;
     const int ntiles = P.ntx * P.ntz;
     std::vector<int32_t> cnt((size_t)P.B * ntiles + 1, 0);
     std::vector<int> key(loc.size() / 2, -1);
@@ -569,6 +666,31 @@ static void build_events(const Plan& pl, const std::vector<int32_t>& loc, int n,
     }
 }
 
+// Shots per CTA: the fewest waves x shots-per-CTA over 148 SMs at `occ` CTAs
+// per SM (the time one step takes scales with both), ties to more shots per CTA.
+static int choose_group(int ntiles, int B, int occ)
+{
+    if (const char* e = getenv("SWEEP_B200_SHOTS_PER_CTA")) {
+        const int g = atoi(e);
+        if (g >= 1) return std::min(g, B);
+    }
+    int best = 1;
+    double best_cost = 1e30;
+    for (int G = 1; G <= std::min(B, 16); ++G) {
+        const int groups = (B + G - 1) / G;
+        const long long ctas = (long long)ntiles * groups;
+        const long long slots = 148LL * occ;
+        const long long waves = (ctas + slots - 1) / slots;
+        // + one pipeline fill per CTA, worth about one shot
+        const double cost = (double)waves * (G + 1);
+        if (cost < best_cost - 1e-9 || (cost <= best_cost + 1e-9 && G > best)) {
+            best = G;
+            best_cost = cost;
+        }
+    }
+    return best;
+}
+
 static Plan make_plan(const sweep_acoustic_desc* d)
 {
     SWEEP_REQUIRE(d != nullptr, "null descriptor");
@@ -576,6 +698,7 @@ static Plan make_plan(const sweep_acoustic_desc* d)
     SWEEP_REQUIRE(d->M == M, "acoustic2d: only spatial order 8 (M = 4) is built (got M = %d)", d->M);
     SWEEP_REQUIRE(d->B >= 1 && d->nt >= 1, "acoustic2d: B and nt must be >= 1");
     SWEEP_REQUIRE(d->nsrc >= 0 && d->nrec >= 0, "acoustic2d: negative source/receiver count");
+    SWEEP_REQUIRE(d->nz >= 2 * M + 1 && d->nx >= 2 * M + 1, "acoustic2d: grid too small");
     for (int f = 0; f < 4; ++f) {
         const int p = d->pad[f < 2 ? f : f + 2];
         SWEEP_REQUIRE(p >= 1, "acoustic2d: every face needs a PML pad >= 1 (face %d has %d)", f, p);
@@ -584,6 +707,9 @@ static Plan make_plan(const sweep_acoustic_desc* d)
     Params& P = pl.P;
     P.B = d->B; P.nz = d->nz; P.nx = d->nx; P.nt = d->nt;
     P.nsrc = d->nsrc; P.nrec = d->nrec;
+    P.P = (d->nx + 31) / 32 * 32;
+    P.S = (long long)d->nz * P.P;
+    SWEEP_REQUIRE(P.S < (1LL << 31), "acoustic2d: one shot's grid must hold < 2^31 cells");
     const int pzl = d->pad[0], pzh = d->pad[1], pxl = d->pad[4], pxh = d->pad[5];
     P.z0 = pzl + M; P.z1 = d->nz - pzh - M;
     P.x0 = pxl + M; P.x1 = d->nx - pxh - M;
@@ -607,106 +733,144 @@ static Plan make_plan(const sweep_acoustic_desc* d)
     P.rz0 = P.z0 + P.wzl; P.rz1 = P.z1 - P.wzh;
     P.rx0 = P.x0 + P.wxl; P.rx1 = P.x1 - P.wxh;
     P.az = d->az; P.bz = d->bz; P.dbz = d->dbz; P.ax = d->ax; P.bx = d->bx; P.dbx = d->dbx;
-    P.vp = d->vp; P.vp_stride = d->vp_stride;
     P.per_shot = d->vp_stride != 0;
+    P.ms = P.per_shot ? P.S : 0;
+    pl.nm = P.per_shot ? d->B : 1;
     P.wavelet = d->wavelet;
     P.ntx = (d->nx + TX - 1) / TX;
     P.ntz = (d->nz + TZ - 1) / TZ;
     const int ntiles = P.ntx * P.ntz;
-    // shots per CTA: enough CTAs for ~4 waves over 148 SMs
-    int G = (int)((long long)ntiles * P.B / (148LL * 4));
-    G = std::max(1, std::min(G, 8));
-    G = std::min(G, P.B);
-    P.G = G;
-    pl.N = (long long)d->nz * d->nx;
-    const int ngroups = (P.B + G - 1) / G;
+    P.G = P.per_shot ? 1 : choose_group(ntiles, P.B, 2);
+    const int ngroups = (P.B + P.G - 1) / P.G;
     pl.nslot = P.per_shot ? P.B : ngroups;
     pl.grid = dim3(P.ntx, P.ntz, ngroups);
     return pl;
 }
 
-struct FwdWork {
-    float* u[3];
-    float *psix, *psiz, *psixn, *psizn, *zetax, *zetaz;
+struct Common {
+    float *cf, *ca, *vv;
     int32_t *src_off, *rec_off;
     int2 *src_ev, *rec_ev;
+    int* err;
+};
+
+struct FwdWork {
+    Common c;
+    float* u[3];
+    float *psix, *psiz, *psixn, *psizn, *zetax, *zetaz;
 };
 
 struct RevWork {
+    Common c;
     float* l[3];
     float* aux[8];
     float* r[3];
     float *gacc, *gcomp, *is, *ir;
-    int32_t *src_off, *rec_off;
-    int2 *src_ev, *rec_ev;
 };
 
-static void carve_events(Carve& c, const Plan& pl, int32_t*& so, int32_t*& ro, int2*& se, int2*& re)
+static Common carve_common(Carve& c, const Plan& pl)
 {
+    Common w{};
+    const long long nmS = (long long)pl.nm * pl.P.S;
+    w.cf = c.take<float>(nmS);
+    w.ca = c.take<float>(nmS);
+    w.vv = c.take<float>(nmS);
     const long long nkey = (long long)pl.P.B * pl.P.ntx * pl.P.ntz + 1;
-    so = c.take<int32_t>(nkey);
-    ro = c.take<int32_t>(nkey);
-    se = c.take<int2>((long long)pl.P.B * std::max(pl.P.nsrc, 1));
-    re = c.take<int2>((long long)pl.P.B * std::max(pl.P.nrec, 1));
+    w.src_off = c.take<int32_t>(nkey);
+    w.rec_off = c.take<int32_t>(nkey);
+    w.src_ev = c.take<int2>((long long)pl.P.B * std::max(pl.P.nsrc, 1));
+    w.rec_ev = c.take<int2>((long long)pl.P.B * std::max(pl.P.nrec, 1));
+    w.err = c.take<int>(1);
+    return w;
 }
 
 static FwdWork carve_fwd(Carve& c, const Plan& pl)
 {
     FwdWork w{};
-    const long long n = (long long)pl.P.B * pl.N;
+    w.c = carve_common(c, pl);
+    const long long n = (long long)pl.P.B * pl.P.S;
     for (auto& p : w.u) p = c.take<float>(n);
     w.psix = c.take<float>(n); w.psiz = c.take<float>(n);
     w.psixn = c.take<float>(n); w.psizn = c.take<float>(n);
     w.zetax = c.take<float>(n); w.zetaz = c.take<float>(n);
-    carve_events(c, pl, w.src_off, w.rec_off, w.src_ev, w.rec_ev);
     return w;
 }
 
 static RevWork carve_rev(Carve& c, const Plan& pl, bool illum)
 {
     RevWork w{};
-    const long long n = (long long)pl.P.B * pl.N;
+    w.c = carve_common(c, pl);
+    const long long n = (long long)pl.P.B * pl.P.S;
     for (auto& p : w.l) p = c.take<float>(n);
     for (auto& p : w.aux) p = c.take<float>(n);
     for (auto& p : w.r) p = c.take<float>(n);
-    w.gacc = c.take<float>((long long)pl.nslot * pl.N);
-    w.gcomp = c.take<float>((long long)pl.nslot * pl.N);
+    w.gacc = c.take<float>((long long)pl.nslot * pl.P.S);
+    w.gcomp = c.take<float>((long long)pl.nslot * pl.P.S);
     if (illum) {
-        w.is = c.take<float>((long long)pl.nslot * pl.N);
-        w.ir = c.take<float>((long long)pl.nslot * pl.N);
+        w.is = c.take<float>((long long)pl.nslot * pl.P.S);
+        w.ir = c.take<float>((long long)pl.nslot * pl.P.S);
     }
-    carve_events(c, pl, w.src_off, w.rec_off, w.src_ev, w.rec_ev);
     return w;
 }
 
+// tape: strips of every step (nt, B, nstrip), then (U[nt-1], U[nt]) pitched
 static int64_t tape_bytes(const Plan& pl)
 {
     Carve c(nullptr);
     c.take<float>((long long)pl.P.nt * pl.P.B * pl.P.nstrip);
-    c.take<float>(2LL * pl.P.B * pl.N);
+    c.take<float>(2LL * pl.P.B * pl.P.S);
     return c.off;
 }
 
-static void upload_events(const sweep_acoustic_desc* d, Plan& pl, cudaStream_t st,
-                          int32_t* so, int32_t* ro, int2* se, int2* re, HostEvents& hs, HostEvents& hr)
+static float* tape_last(void* tape, const Plan& pl)
 {
-    const int B = d->B;
-    std::vector<int32_t> sl((size_t)B * d->nsrc * 2), rl((size_t)B * d->nrec * 2);
+    Carve c(tape);
+    c.take<float>((long long)pl.P.nt * pl.P.B * pl.P.nstrip);
+    return c.take<float>(2LL * pl.P.B * pl.P.S);
+}
+
+// Per-call set-up shared by both passes: model fields, event tables, error flag.
+static void setup_common(const sweep_acoustic_desc* d, Plan& pl, const Common& w, cudaStream_t st,
+                         HostEvents& hs, HostEvents& hr)
+{
+    Params& P = pl.P;
+    prep_kernel<<<592, 256, 0, st>>>(d->vp, pl.nm, d->nz, d->nx, P.P, d->dt, w.cf, w.ca, w.vv);
+    SWEEP_LAUNCH_CHECK();
+    P.cf = w.cf; P.vv = w.vv;
+    std::vector<int32_t> sl((size_t)d->B * d->nsrc * 2), rl((size_t)d->B * d->nrec * 2);
     if (!sl.empty()) SWEEP_CUDA(cudaMemcpyAsync(sl.data(), d->src_loc, sl.size() * 4, cudaMemcpyDeviceToHost, st));
     if (!rl.empty()) SWEEP_CUDA(cudaMemcpyAsync(rl.data(), d->rec_loc, rl.size() * 4, cudaMemcpyDeviceToHost, st));
     SWEEP_CUDA(cudaStreamSynchronize(st));
-    build_events(pl, sl, d->nsrc, hs);
-    build_events(pl, rl, d->nrec, hr);
-    SWEEP_CUDA(cudaMemcpyAsync(so, hs.off.data(), hs.off.size() * 4, cudaMemcpyHostToDevice, st));
-    SWEEP_CUDA(cudaMemcpyAsync(ro, hr.off.data(), hr.off.size() * 4, cudaMemcpyHostToDevice, st));
-    if (!hs.ev.empty()) SWEEP_CUDA(cudaMemcpyAsync(se, hs.ev.data(), hs.ev.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
-    if (!hr.ev.empty()) SWEEP_CUDA(cudaMemcpyAsync(re, hr.ev.data(), hr.ev.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
-    pl.P.src.off = so; pl.P.src.ev = se;
-    pl.P.rec.off = ro; pl.P.rec.ev = re;
+    build_events(P, sl, d->nsrc, hs);
+    build_events(P, rl, d->nrec, hr);
+    SWEEP_CUDA(cudaMemcpyAsync(w.src_off, hs.off.data(), hs.off.size() * 4, cudaMemcpyHostToDevice, st));
+    SWEEP_CUDA(cudaMemcpyAsync(w.rec_off, hr.off.data(), hr.off.size() * 4, cudaMemcpyHostToDevice, st));
+    if (!hs.ev.empty()) SWEEP_CUDA(cudaMemcpyAsync(w.src_ev, hs.ev.data(), hs.ev.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
+    if (!hr.ev.empty()) SWEEP_CUDA(cudaMemcpyAsync(w.rec_ev, hr.ev.data(), hr.ev.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
+    P.src.off = w.src_off; P.src.ev = w.src_ev;
+    P.rec.off = w.rec_off; P.rec.ev = w.rec_ev;
+    SWEEP_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
+    P.err = w.err;
 }
 
-static size_t fwd_smem() { return (SN + TZ * TX) * sizeof(float); }
-static size_t rev_smem() { return (3 * SN + 2 * TZ * TX) * sizeof(float); }
+static void check_err(const Common& w, cudaStream_t st, const char* what)
+{
+    int h = 0;
+    SWEEP_CUDA(cudaMemcpyAsync(&h, w.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SWEEP_CUDA(cudaStreamSynchronize(st));
+    SWEEP_REQUIRE(h == 0, "acoustic2d %s: a tile load did not complete in time (code %d); results are invalid", what, h);
+}
+
+static CUtensorMap field_map(const float* base, const Params& P, int nb, bool halo)
+{
+    const uint64_t dims[3] = {(uint64_t)P.nx, (uint64_t)P.nz, (uint64_t)nb};
+    const uint64_t strides[2] = {(uint64_t)P.P, (uint64_t)P.S};
+    const uint32_t box[3] = {(uint32_t)(halo ? SW : TX), (uint32_t)(halo ? SH : TZ), 1u};
+    return tma::make_map(base, 3, dims, strides, box);
+}
+
+static size_t fwd_smem() { return sizeof(FwdSmem); }
+static size_t rev_smem() { return sizeof(RevSmem); }
 
 static void set_attrs()
 {
@@ -738,39 +902,47 @@ void forward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* 
     SWEEP_REQUIRE(ws != nullptr && ws_bytes >= need_ws, "acoustic2d forward: workspace too small (%lld < %lld)",
                   (long long)ws_bytes, (long long)need_ws);
     SWEEP_REQUIRE(record != nullptr || d->nrec == 0, "acoustic2d forward: null record");
+    SWEEP_REQUIRE(d->vp != nullptr, "acoustic2d forward: null vp");
     set_attrs();
     Plan pl = make_plan(d);
     Carve c(ws);
     FwdWork w = carve_fwd(c, pl);
     HostEvents hs, hr;
-    upload_events(d, pl, st, w.src_off, w.rec_off, w.src_ev, w.rec_ev, hs, hr);
-    const long long n = (long long)pl.P.B * pl.N;
+    setup_common(d, pl, w.c, st, hs, hr);
+    const Params& P = pl.P;
+    const long long n = (long long)P.B * P.S;
     for (auto* p : w.u) SWEEP_CUDA(cudaMemsetAsync(p, 0, n * 4, st));
     for (auto* p : {w.psix, w.psiz, w.psixn, w.psizn, w.zetax, w.zetaz})
         SWEEP_CUDA(cudaMemsetAsync(p, 0, n * 4, st));
     if (d->nrec > 0)
         SWEEP_CUDA(cudaMemsetAsync(record, 0, (size_t)d->B * d->nt * d->nrec * 4, st));
+    FwdMaps maps;
+    for (int i = 0; i < 3; ++i) {
+        maps.halo[i] = field_map(w.u[i], P, P.B, true);
+        maps.tile[i] = field_map(w.u[i], P, P.B, false);
+    }
     float* strips = static_cast<float*>(tape);
     FwdPtrs F{};
     F.record = record;
-    float *up = w.u[0], *un = w.u[1], *ux = w.u[2];
+    F.zetax = w.zetax; F.zetaz = w.zetaz;
+    int ip = 0, in = 1, ix = 2;
     float *px = w.psix, *pz = w.psiz, *pxn = w.psixn, *pzn = w.psizn;
     for (int it = 0; it < d->nt; ++it) {
-        F.u_prev = up; F.u_now = un; F.u_next = ux;
+        F.now = in; F.prev = ip; F.u_next = w.u[ix];
         F.psix = px; F.psiz = pz; F.psixn = pxn; F.psizn = pzn;
-        F.zetax = w.zetax; F.zetaz = w.zetaz;
-        F.strips = strips ? strips + (long long)it * pl.P.B * pl.P.nstrip : nullptr;
-        fwd_kernel<<<pl.grid, NTH, fwd_smem(), st>>>(pl.P, F, it);
+        F.strips = strips ? strips + (long long)it * P.B * P.nstrip : nullptr;
+        fwd_kernel<<<pl.grid, NTH, fwd_smem(), st>>>(maps, P, F, it);
         SWEEP_LAUNCH_CHECK();
-        float* t = up; up = un; un = ux; ux = t;
+        const int t = ip; ip = in; in = ix; ix = t;
         std::swap(px, pxn); std::swap(pz, pzn);
     }
     if (strips) {
-        float* last = strips + (long long)d->nt * pl.P.B * pl.P.nstrip;
-        // (U[nt-1], U[nt]) per shot
-        SWEEP_CUDA(cudaMemcpyAsync(last, up, n * 4, cudaMemcpyDeviceToDevice, st));
-        SWEEP_CUDA(cudaMemcpyAsync(last + n, un, n * 4, cudaMemcpyDeviceToDevice, st));
+        float* last = tape_last(tape, pl);
+        // (U[nt-1], U[nt]) per shot, pitched
+        SWEEP_CUDA(cudaMemcpyAsync(last, w.u[ip], n * 4, cudaMemcpyDeviceToDevice, st));
+        SWEEP_CUDA(cudaMemcpyAsync(last + n, w.u[in], n * 4, cudaMemcpyDeviceToDevice, st));
     }
+    check_err(w.c, st, "forward");
 }
 
 void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const float* adj, const void* tape,
@@ -782,6 +954,7 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     SWEEP_REQUIRE(ws != nullptr && ws_bytes >= need_ws, "acoustic2d backward: workspace too small");
     SWEEP_REQUIRE(tape != nullptr, "acoustic2d backward: null tape");
     SWEEP_REQUIRE(grad_vp != nullptr, "acoustic2d backward: null grad_vp");
+    SWEEP_REQUIRE(adj != nullptr || d->nrec == 0, "acoustic2d backward: null record cotangent");
     SWEEP_REQUIRE((illum_s == nullptr) == (illum_r == nullptr), "acoustic2d backward: pass both illuminations or neither");
     set_attrs();
     Plan pl = make_plan(d);
@@ -789,49 +962,59 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     const bool illum = illum_s != nullptr;
     RevWork w = carve_rev(c, pl, illum);
     HostEvents hs, hr;
-    upload_events(d, pl, st, w.src_off, w.rec_off, w.src_ev, w.rec_ev, hs, hr);
-    const long long n = (long long)pl.P.B * pl.N;
+    setup_common(d, pl, w.c, st, hs, hr);
+    const Params& P = pl.P;
+    const long long n = (long long)P.B * P.S;
     for (auto* p : w.l) SWEEP_CUDA(cudaMemsetAsync(p, 0, n * 4, st));
     for (auto* p : w.aux) SWEEP_CUDA(cudaMemsetAsync(p, 0, n * 4, st));
     SWEEP_CUDA(cudaMemsetAsync(w.r[2], 0, n * 4, st));
-    SWEEP_CUDA(cudaMemsetAsync(w.gacc, 0, (size_t)pl.nslot * pl.N * 4, st));
-    SWEEP_CUDA(cudaMemsetAsync(w.gcomp, 0, (size_t)pl.nslot * pl.N * 4, st));
+    SWEEP_CUDA(cudaMemsetAsync(w.gacc, 0, (size_t)pl.nslot * P.S * 4, st));
+    SWEEP_CUDA(cudaMemsetAsync(w.gcomp, 0, (size_t)pl.nslot * P.S * 4, st));
     if (illum) {
-        SWEEP_CUDA(cudaMemsetAsync(w.is, 0, (size_t)pl.nslot * pl.N * 4, st));
-        SWEEP_CUDA(cudaMemsetAsync(w.ir, 0, (size_t)pl.nslot * pl.N * 4, st));
+        SWEEP_CUDA(cudaMemsetAsync(w.is, 0, (size_t)pl.nslot * P.S * 4, st));
+        SWEEP_CUDA(cudaMemsetAsync(w.ir, 0, (size_t)pl.nslot * P.S * 4, st));
     }
     if (grad_w && d->nsrc > 0)
         SWEEP_CUDA(cudaMemsetAsync(grad_w, 0, (size_t)d->B * d->nsrc * d->nt * 4, st));
     const float* strips = static_cast<const float*>(tape);
-    const float* last = strips + (long long)d->nt * pl.P.B * pl.P.nstrip;
+    const float* last = tape_last(const_cast<void*>(tape), pl);
     // seed: prev = U[nt], now = U[nt-1]  (reference driver_traits.cuh:493-505; the
     // rim outside the physical box is never read by the reconstruction)
     SWEEP_CUDA(cudaMemcpyAsync(w.r[0], last + n, n * 4, cudaMemcpyDeviceToDevice, st));
     SWEEP_CUDA(cudaMemcpyAsync(w.r[1], last, n * 4, cudaMemcpyDeviceToDevice, st));
+    RevMaps maps;
+    for (int i = 0; i < 3; ++i) {
+        maps.lh[i] = field_map(w.l[i], P, P.B, true);
+        maps.lt[i] = field_map(w.l[i], P, P.B, false);
+        maps.rh[i] = field_map(w.r[i], P, P.B, true);
+        maps.rt[i] = field_map(w.r[i], P, P.B, false);
+    }
+    maps.ch = field_map(w.c.ca, P, pl.nm, true);
     RevPtrs R{};
     R.adj = adj; R.grad_w = grad_w;
     R.gacc = w.gacc; R.gcomp = w.gcomp;
     R.illum_s = w.is; R.illum_r = w.ir;
-    float *lp = w.l[0], *ln = w.l[1], *lx = w.l[2];
-    float *rp = w.r[0], *rn = w.r[1], *rx = w.r[2];
+    int lp = 0, ln = 1, lx = 2;
+    int rp = 0, rn = 1, rx = 2;
     int cur = 0;
     for (int it = d->nt - 1; it >= 0; --it) {
         const int do_recon = it > 0 ? 1 : 0;
-        R.l_prev = lp; R.l_now = ln; R.l_next = lx;
+        R.lprev = lp; R.lnow = ln; R.l_next = w.l[lx];
         R.apx = w.aux[0 + cur]; R.apz = w.aux[2 + cur]; R.azx = w.aux[4 + cur]; R.azz = w.aux[6 + cur];
         R.apx_o = w.aux[1 - cur]; R.apz_o = w.aux[3 - cur]; R.azx_o = w.aux[5 - cur]; R.azz_o = w.aux[7 - cur];
-        R.r_prev = rp; R.r_now = rn; R.r_next = rx;
-        R.strips = do_recon ? strips + (long long)(it - 1) * pl.P.B * pl.P.nstrip : nullptr;
-        rev_kernel<<<pl.grid, NTH, rev_smem(), st>>>(pl.P, R, it, do_recon);
+        R.rprev = rp; R.rnow = rn; R.r_next = w.r[rx];
+        R.strips = do_recon ? strips + (long long)(it - 1) * P.B * P.nstrip : nullptr;
+        rev_kernel<<<pl.grid, NTH, rev_smem(), st>>>(maps, P, R, it, do_recon);
         SWEEP_LAUNCH_CHECK();
-        float* t = lp; lp = ln; ln = lx; lx = t;
+        int t = lp; lp = ln; ln = lx; lx = t;
         cur = 1 - cur;
         if (do_recon) { t = rp; rp = rn; rn = rx; rx = t; }
     }
-    const int nout = pl.P.per_shot ? d->B : 1;
-    finalize_kernel<<<1184, 256, 0, st>>>(w.gacc, w.gcomp, w.is, w.ir, pl.nslot, nout, pl.N,
+    const int nout = P.per_shot ? d->B : 1;
+    finalize_kernel<<<1184, 256, 0, st>>>(w.gacc, w.gcomp, w.is, w.ir, pl.nslot, nout, d->nz, d->nx, P.P,
                                           grad_vp, illum_s, illum_r);
     SWEEP_LAUNCH_CHECK();
+    check_err(w.c, st, "backward");
 }
 
 }  // namespace a2d
