@@ -30,7 +30,7 @@
 //   * point sources, receivers and boundary strips are handled by the CTA that
 //     owns the cell, in the same launch as the stencil;
 //   * one launch per forward step and one per reverse step.
-#include "common.cuh"
+#include "acoustic2d.cuh"
 #include "tma.cuh"
 
 namespace sweep {
@@ -641,29 +641,33 @@ struct Plan {
     dim3 grid;
 };
 
-static void build_events(const Params& P, const std::vector<int32_t>& loc, int n, HostEvents& out)
+// CSR of the events of (shot, tile): off[key .. key+1) indexes ev, each
+// (tile-local cell, global event id), in event order.  `loc` is the host copy
+// of the (B, n, 2) coordinates; `fill` is (B * ntiles) scratch.
+static int build_events(const Params& P, const int32_t* loc, int n, int32_t* off, int2* ev, int32_t* fill)
 {
     const int ntiles = P.ntx * P.ntz;
-    std::vector<int32_t> cnt((size_t)P.B * ntiles + 1, 0);
-    std::vector<int> key(loc.size() / 2, -1);
-    for (int b = 0; b < P.B; ++b)
-        for (int s = 0; s < n; ++s) {
-            const int e = b * n + s;
-            const int ix = loc[2 * e], iz = loc[2 * e + 1];
-            // cells of the outer stencil halo are never updated: treated as off-grid
-            if (ix < M || ix >= P.nx - M || iz < M || iz >= P.nz - M) continue;
-            key[e] = b * ntiles + (iz / TZ) * P.ntx + ix / TX;
-            cnt[key[e] + 1]++;
-        }
-    for (size_t i = 1; i < cnt.size(); ++i) cnt[i] += cnt[i - 1];
-    out.off = cnt;
-    out.ev.assign(cnt.back(), make_int2(0, 0));
-    std::vector<int32_t> fill(cnt.begin(), cnt.end() - 1);
-    for (int e = 0; e < (int)key.size(); ++e) {
-        if (key[e] < 0) continue;
+    const int nkey = P.B * ntiles;
+    for (int i = 0; i <= nkey; ++i) off[i] = 0;
+    auto key_of = [&](int e) -> int {
         const int ix = loc[2 * e], iz = loc[2 * e + 1];
-        out.ev[fill[key[e]]++] = make_int2((iz % TZ) * TX + ix % TX, e);
+        // cells of the outer stencil halo are never updated: treated as off-grid
+        if (ix < M || ix >= P.nx - M || iz < M || iz >= P.nz - M) return -1;
+        return (e / n) * ntiles + (iz / TZ) * P.ntx + ix / TX;
+    };
+    for (int e = 0; e < P.B * n; ++e) {
+        const int k = key_of(e);
+        if (k >= 0) off[k + 1]++;
     }
+    for (int i = 1; i <= nkey; ++i) off[i] += off[i - 1];
+    for (int i = 0; i < nkey; ++i) fill[i] = off[i];
+    for (int e = 0; e < P.B * n; ++e) {
+        const int k = key_of(e);
+        if (k < 0) continue;
+        const int ix = loc[2 * e], iz = loc[2 * e + 1];
+        ev[fill[k]++] = make_int2((iz % TZ) * TX + ix % TX, e);
+    }
+    return off[nkey];
 }
 
 // Shots per CTA: the fewest waves x shots-per-CTA over 148 SMs at `occ` CTAs
@@ -829,24 +833,40 @@ static float* tape_last(void* tape, const Plan& pl)
     return c.take<float>(2LL * pl.P.B * pl.P.S);
 }
 
+struct VecStage {
+    std::vector<int32_t> ls, lr, os, orr, fill;
+    std::vector<int2> es, er;
+    HostStage h{};
+    VecStage(const Params& P)
+        : ls((size_t)P.B * P.nsrc * 2 + 1), lr((size_t)P.B * P.nrec * 2 + 1),
+          os((size_t)P.B * P.ntx * P.ntz + 1), orr((size_t)P.B * P.ntx * P.ntz + 1),
+          fill((size_t)P.B * P.ntx * P.ntz + 1), es((size_t)P.B * P.nsrc + 1), er((size_t)P.B * P.nrec + 1)
+    {
+        h = HostStage{ls.data(), lr.data(), os.data(), orr.data(), es.data(), er.data(), fill.data()};
+    }
+};
+
 // Per-call set-up shared by both passes: model fields, event tables, error flag.
 static void setup_common(const sweep_acoustic_desc* d, Plan& pl, const Common& w, cudaStream_t st,
-                         HostEvents& hs, HostEvents& hr)
+                         const HostStage& h)
 {
     Params& P = pl.P;
     prep_kernel<<<592, 256, 0, st>>>(d->vp, pl.nm, d->nz, d->nx, P.P, d->dt, w.cf, w.ca, w.vv);
     SWEEP_LAUNCH_CHECK();
     P.cf = w.cf; P.vv = w.vv;
-    std::vector<int32_t> sl((size_t)d->B * d->nsrc * 2), rl((size_t)d->B * d->nrec * 2);
-    if (!sl.empty()) SWEEP_CUDA(cudaMemcpyAsync(sl.data(), d->src_loc, sl.size() * 4, cudaMemcpyDeviceToHost, st));
-    if (!rl.empty()) SWEEP_CUDA(cudaMemcpyAsync(rl.data(), d->rec_loc, rl.size() * 4, cudaMemcpyDeviceToHost, st));
+    const size_t ns = (size_t)d->B * d->nsrc * 2, nr = (size_t)d->B * d->nrec * 2;
+    if (ns) SWEEP_CUDA(cudaMemcpyAsync(h.loc_src, d->src_loc, ns * 4, cudaMemcpyDeviceToHost, st));
+    if (nr) SWEEP_CUDA(cudaMemcpyAsync(h.loc_rec, d->rec_loc, nr * 4, cudaMemcpyDeviceToHost, st));
     SWEEP_CUDA(cudaStreamSynchronize(st));
-    build_events(P, sl, d->nsrc, hs);
-    build_events(P, rl, d->nrec, hr);
-    SWEEP_CUDA(cudaMemcpyAsync(w.src_off, hs.off.data(), hs.off.size() * 4, cudaMemcpyHostToDevice, st));
-    SWEEP_CUDA(cudaMemcpyAsync(w.rec_off, hr.off.data(), hr.off.size() * 4, cudaMemcpyHostToDevice, st));
-    if (!hs.ev.empty()) SWEEP_CUDA(cudaMemcpyAsync(w.src_ev, hs.ev.data(), hs.ev.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
-    if (!hr.ev.empty()) SWEEP_CUDA(cudaMemcpyAsync(w.rec_ev, hr.ev.data(), hr.ev.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
+    const int nsev = build_events(P, h.loc_src, d->nsrc, h.off_src, h.ev_src, h.fill);
+    const int nrev = build_events(P, h.loc_rec, d->nrec, h.off_rec, h.ev_rec, h.fill);
+    const size_t nkey = (size_t)P.B * P.ntx * P.ntz + 1;
+    SWEEP_CUDA(cudaMemcpyAsync(w.src_off, h.off_src, nkey * 4, cudaMemcpyHostToDevice, st));
+    SWEEP_CUDA(cudaMemcpyAsync(w.rec_off, h.off_rec, nkey * 4, cudaMemcpyHostToDevice, st));
+    if (nsev) SWEEP_CUDA(cudaMemcpyAsync(w.src_ev, h.ev_src, nsev * sizeof(int2), cudaMemcpyHostToDevice, st));
+    if (nrev) SWEEP_CUDA(cudaMemcpyAsync(w.rec_ev, h.ev_rec, nrev * sizeof(int2), cudaMemcpyHostToDevice, st));
+    // the host staging may be reused or released once the copies have read it
+    SWEEP_CUDA(cudaStreamSynchronize(st));
     P.src.off = w.src_off; P.src.ev = w.src_ev;
     P.rec.off = w.rec_off; P.rec.ev = w.rec_ev;
     SWEEP_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
@@ -894,21 +914,39 @@ void sizes(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, int64_t* 
     *tape = tape_bytes(pl);
 }
 
-void forward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* record, void* tape,
-             void* ws, int64_t ws_bytes, cudaStream_t st)
+int64_t forward_only_bytes(const sweep_acoustic_desc* d)
 {
-    int64_t need_ws, need_tape;
-    sizes(d, mem_mode, ckpt_every, &need_ws, &need_tape);
-    SWEEP_REQUIRE(ws != nullptr && ws_bytes >= need_ws, "acoustic2d forward: workspace too small (%lld < %lld)",
-                  (long long)ws_bytes, (long long)need_ws);
+    Plan pl = make_plan(d);
+    Carve c(nullptr);
+    carve_fwd(c, pl);
+    return c.off;
+}
+
+void stage_sizes(const sweep_acoustic_desc* d, int64_t* nkey, int64_t* nev_src, int64_t* nev_rec)
+{
+    Plan pl = make_plan(d);
+    *nkey = (int64_t)pl.P.B * pl.P.ntx * pl.P.ntz + 1;
+    *nev_src = (int64_t)d->B * d->nsrc;
+    *nev_rec = (int64_t)d->B * d->nrec;
+}
+
+void forward_with(const sweep_acoustic_desc* d, float* record, void* tape, void* ws, int64_t ws_bytes,
+                  cudaStream_t st, const HostStage* stage)
+{
     SWEEP_REQUIRE(record != nullptr || d->nrec == 0, "acoustic2d forward: null record");
     SWEEP_REQUIRE(d->vp != nullptr, "acoustic2d forward: null vp");
     set_attrs();
     Plan pl = make_plan(d);
     Carve c(ws);
     FwdWork w = carve_fwd(c, pl);
-    HostEvents hs, hr;
-    setup_common(d, pl, w.c, st, hs, hr);
+    SWEEP_REQUIRE(ws != nullptr && ws_bytes >= c.off, "acoustic2d forward: workspace too small (%lld < %lld)",
+                  (long long)ws_bytes, (long long)c.off);
+    if (stage) {
+        setup_common(d, pl, w.c, st, *stage);
+    } else {
+        VecStage vs(pl.P);
+        setup_common(d, pl, w.c, st, vs.h);
+    }
     const Params& P = pl.P;
     const long long n = (long long)P.B * P.S;
     for (auto* p : w.u) SWEEP_CUDA(cudaMemsetAsync(p, 0, n * 4, st));
@@ -945,6 +983,16 @@ void forward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* 
     check_err(w.c, st, "forward");
 }
 
+void forward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* record, void* tape,
+             void* ws, int64_t ws_bytes, cudaStream_t st)
+{
+    int64_t need_ws, need_tape;
+    sizes(d, mem_mode, ckpt_every, &need_ws, &need_tape);
+    SWEEP_REQUIRE(ws != nullptr && ws_bytes >= need_ws, "acoustic2d forward: workspace too small (%lld < %lld)",
+                  (long long)ws_bytes, (long long)need_ws);
+    forward_with(d, record, tape, ws, ws_bytes, st, nullptr);
+}
+
 void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const float* adj, const void* tape,
               float* grad_vp, float* grad_w, float* illum_s, float* illum_r,
               void* ws, int64_t ws_bytes, cudaStream_t st)
@@ -961,8 +1009,10 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     Carve c(ws);
     const bool illum = illum_s != nullptr;
     RevWork w = carve_rev(c, pl, illum);
-    HostEvents hs, hr;
-    setup_common(d, pl, w.c, st, hs, hr);
+    {
+        VecStage vs(pl.P);
+        setup_common(d, pl, w.c, st, vs.h);
+    }
     const Params& P = pl.P;
     const long long n = (long long)P.B * P.S;
     for (auto* p : w.l) SWEEP_CUDA(cudaMemsetAsync(p, 0, n * 4, st));

@@ -1,16 +1,7 @@
 // capi.cu -- the extern "C" entry points declared in include/sweep_b200.h.
 // Each one validates, dispatches on the equation family, and turns any error
 // into (non-zero return, message) -- nothing is thrown across the boundary.
-#include "common.cuh"
-
-namespace sweep {
-namespace a2d {
-void sizes(const sweep_acoustic_desc*, int, int, int64_t*, int64_t*);
-void forward(const sweep_acoustic_desc*, int, int, float*, void*, void*, int64_t, cudaStream_t);
-void backward(const sweep_acoustic_desc*, int, int, const float*, const void*, float*, float*,
-              float*, float*, void*, int64_t, cudaStream_t);
-}  // namespace a2d
-}  // namespace sweep
+#include "acoustic2d.cuh"
 
 using namespace sweep;
 

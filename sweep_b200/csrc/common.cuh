@@ -94,9 +94,5 @@ struct EventTable {
     const int2* ev = nullptr;       // (count)
 };
 
-struct HostEvents {
-    std::vector<int32_t> off;
-    std::vector<int2> ev;
-};
 
 }  // namespace sweep
