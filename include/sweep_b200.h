@@ -106,6 +106,23 @@ SWEEP_B200_API int sweep_b200_acoustic_backward(const sweep_acoustic_desc* d, in
                                  void* workspace, int64_t workspace_bytes,
                                  void* stream, char* err, int32_t err_cap);
 
+/* Allocation-free forward (records only) for callers that cannot allocate
+ * device memory -- code running where cudaMalloc is not allowed or not wanted
+ * (inside another library's memory manager, a loop that must not allocate, a
+ * process whose device memory is already handed out).  No counterpart in the
+ * reference: it is the 2-D acoustic forward of sweep_b200_acoustic_forward
+ * (no tape, no backward) with its scratch in a static 64 MiB array that every
+ * GPU loading this library holds until exit.  The caller passes the inputs
+ * (d) and the output (record, (B, nt, nrec)).  A problem needing more scratch
+ * than the array, or more than 65536 shot-tiles or 32768 sources / receivers,
+ * is rejected with an error.  The first call on a device looks up the
+ * array's address (cudaGetSymbolAddress) with that device current: make it
+ * before any stream capture.  Every call shares the array: calls that overlap
+ * on the GPU race; each call clears what must start at zero.  Calls no
+ * cudaMalloc, cudaFree or other allocating routine. */
+SWEEP_B200_API int sweep_b200_acoustic_forward_noalloc(const sweep_acoustic_desc* d, float* record,
+                                                       void* stream, char* err, int32_t err_cap);
+
 /* ABI version (SWEEP_B200_ABI_VERSION) -- checked by the Python loader, like
  * the reference's sweep_core_abi_version() (reference loader.py:92-138). */
 SWEEP_B200_API int sweep_b200_abi_version(void);

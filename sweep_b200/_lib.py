@@ -28,6 +28,7 @@ SYMBOLS = (
     "sweep_b200_acoustic_sizes",
     "sweep_b200_acoustic_forward",
     "sweep_b200_acoustic_backward",
+    "sweep_b200_acoustic_forward_noalloc",
 )
 
 MEM_BOUNDARY = 0
@@ -77,6 +78,7 @@ def load():
                                                 ctypes.c_char_p, c_i32]
     lib.sweep_b200_acoustic_backward.argtypes = [P, c_i32, c_i32, c_p, c_p, c_p, c_p, c_p, c_p,
                                                  c_p, c_i64, c_p, ctypes.c_char_p, c_i32]
+    lib.sweep_b200_acoustic_forward_noalloc.argtypes = [P, c_p, c_p, ctypes.c_char_p, c_i32]
     for s in SYMBOLS[1:]:
         getattr(lib, s).restype = ctypes.c_int
     _lib = lib
