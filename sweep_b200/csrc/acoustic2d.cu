@@ -66,6 +66,7 @@ struct Params {
     const float* vv;                 // v, pitched (imaging)
     const float* wavelet;
     EventTable src, rec;
+    const int* order;                // tile slots, heaviest (CPML ring) tiles first
     int* err;
 };
 
@@ -178,10 +179,10 @@ __global__ void __launch_bounds__(NTH) fwd_kernel(const __grid_constant__ FwdMap
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     FwdSmem& sm = *reinterpret_cast<FwdSmem*>(smem_raw);
-    const int tx0 = blockIdx.x * TX, tz0 = blockIdx.y * TZ;
-    const int b0 = blockIdx.z * P.G;
+    const int tile = P.order[blockIdx.y];
+    const int tx0 = (tile % P.ntx) * TX, tz0 = (tile / P.ntx) * TZ;
+    const int b0 = blockIdx.x * P.G;
     const int nloc = min(P.G, P.B - b0);
-    const int tile = blockIdx.y * P.ntx + blockIdx.x;
     const int ntiles = P.ntx * P.ntz;
     const bool band = tx0 < P.bx_lo || tx0 + TX > P.bx_hi || tz0 < P.bz_lo || tz0 + TZ > P.bz_hi;
     const bool full = tx0 >= M && tx0 + TX <= P.nx - M && tz0 >= M && tz0 + TZ <= P.nz - M;
@@ -245,13 +246,14 @@ __global__ void __launch_bounds__(NTH) fwd_kernel(const __grid_constant__ FwdMap
                 if (cx) {
                     const float a = __ldg(P.ax + ix), bb = __ldg(P.bx + ix), db = __ldg(P.dbx + ix);
                     const float du = grad_s(p, 1, P, P.dx);
-                    const float* psx = F.psix + bo;
+                    const float* __restrict__ psx = F.psix + bo;
                     const float dap = grad_apsi(P.ax, ix, psx, i, 1, P, P.dx);
                     const float tmp = ((1.0f + bb) * lx + db * du) + dap;
-                    float* zx = F.zetax + bo;
+                    float* __restrict__ zx = F.zetax + bo;
+                    float* __restrict__ pxn = F.psixn + bo;
                     const float z = zx[i];
                     w += (1.0f + bb) * tmp + a * z;
-                    F.psixn[bo + i] = bb * du + a * __ldg(psx + i);
+                    pxn[i] = bb * du + a * __ldg(psx + i);
                     zx[i] = bb * tmp + a * z;
                 } else {
                     w += lx;
@@ -259,13 +261,14 @@ __global__ void __launch_bounds__(NTH) fwd_kernel(const __grid_constant__ FwdMap
                 if (cz) {
                     const float a = __ldg(P.az + iz), bb = __ldg(P.bz + iz), db = __ldg(P.dbz + iz);
                     const float du = grad_s(p, SW, P, P.dz);
-                    const float* psz = F.psiz + bo;
+                    const float* __restrict__ psz = F.psiz + bo;
                     const float dap = grad_apsi(P.az, iz, psz, i, P.P, P, P.dz);
                     const float tmp = ((1.0f + bb) * lz + db * du) + dap;
-                    float* zz = F.zetaz + bo;
+                    float* __restrict__ zz = F.zetaz + bo;
+                    float* __restrict__ pzn = F.psizn + bo;
                     const float z = zz[i];
                     w += (1.0f + bb) * tmp + a * z;
-                    F.psizn[bo + i] = bb * du + a * __ldg(psz + i);
+                    pzn[i] = bb * du + a * __ldg(psz + i);
                     zz[i] = bb * tmp + a * z;
                 } else {
                     w += lz;
@@ -335,10 +338,10 @@ __global__ void __launch_bounds__(NTH) rev_kernel(const __grid_constant__ RevMap
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     RevSmem& sm = *reinterpret_cast<RevSmem*>(smem_raw);
-    const int tx0 = blockIdx.x * TX, tz0 = blockIdx.y * TZ;
-    const int b0 = blockIdx.z * P.G;
+    const int tile = P.order[blockIdx.y];
+    const int tx0 = (tile % P.ntx) * TX, tz0 = (tile / P.ntx) * TZ;
+    const int b0 = blockIdx.x * P.G;
     const int nloc = min(P.G, P.B - b0);
-    const int tile = blockIdx.y * P.ntx + blockIdx.x;
     const int ntiles = P.ntx * P.ntz;
     const float dt2 = P.dt * P.dt;
     const float invdx2 = 1.0f / (P.dx * P.dx), invdz2 = 1.0f / (P.dz * P.dz);
@@ -423,10 +426,14 @@ __global__ void __launch_bounds__(NTH) rev_kernel(const __grid_constant__ RevMap
             } else {
                 const float ax_ = __ldg(P.ax + ix), az_ = __ldg(P.az + iz);
                 const float bx_ = __ldg(P.bx + ix), bz_ = __ldg(P.bz + iz);
-                const float* zx = R.azx + bo;
-                const float* zz = R.azz + bo;
-                const float* px = R.apx + bo;
-                const float* pz = R.apz + bo;
+                const float* __restrict__ zx = R.azx + bo;
+                const float* __restrict__ zz = R.azz + bo;
+                const float* __restrict__ px = R.apx + bo;
+                const float* __restrict__ pz = R.apz + bo;
+                float* __restrict__ pxo = R.apx_o + bo;
+                float* __restrict__ pzo = R.apz_o + bo;
+                float* __restrict__ zxo = R.azx_o + bo;
+                float* __restrict__ zzo = R.azz_o + bo;
                 const float zx0 = __ldg(zx + i), zz0 = __ldg(zz + i);
                 const float gtx0 = bx_ * zx0 + (1.0f + bx_) * gw;
                 const float gtz0 = bz_ * zz0 + (1.0f + bz_) * gw;
@@ -460,10 +467,10 @@ __global__ void __launch_bounds__(NTH) rev_kernel(const __grid_constant__ RevMap
                 }
                 Lz *= invdz2; Dgz *= invdz; Dqz *= invdz;
                 lo[k] = 2.0f * gun - slp[r * TX + c] + (Lx + Lz - Dgx - Dgz);
-                R.apx_o[bo + i] = ax_ * (__ldg(px + i) - Dqx);
-                R.apz_o[bo + i] = az_ * (__ldg(pz + i) - Dqz);
-                R.azx_o[bo + i] = ax_ * (zx0 + gw);
-                R.azz_o[bo + i] = az_ * (zz0 + gw);
+                pxo[i] = ax_ * (__ldg(px + i) - Dqx);
+                pzo[i] = az_ * (__ldg(pz + i) - Dqz);
+                zxo[i] = ax_ * (zx0 + gw);
+                zzo[i] = az_ * (zz0 + gw);
             }
             if (phys_tile && iz >= P.z0 && iz < P.z1 && ix >= P.x0 && ix < P.x1) {
                 if (iz >= P.rz0 && iz < P.rz1 && ix >= P.rx0 && ix < P.rx1) {
@@ -561,7 +568,7 @@ __global__ void __launch_bounds__(NTH) rev_kernel(const __grid_constant__ RevMap
     // Kahan-compensated flush into this CTA's accumulator slot (per shot for
     // per-shot models, which run one shot per CTA; per shot group otherwise)
     if (phys_any && (do_recon || R.illum_s)) {
-        const long long so = (long long)(P.per_shot ? b0 : blockIdx.z) * P.S;
+        const long long so = (long long)(P.per_shot ? b0 : blockIdx.x) * P.S;
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
             const int iz = tz0 + cell_r(k), ix = tx0 + cell_c(k);
@@ -636,9 +643,10 @@ __global__ void pitch_copy_kernel(const float* __restrict__ src, float* __restri
 // ------------------------------------------------------------------- host
 struct Plan {
     Params P;
-    int nslot;                       // gradient accumulator slots
+    int nslot;                       // gradient accumulator slots (backward)
     int nm;                          // model copies (1 shared, B per-shot)
-    dim3 grid;
+    int Gf, Gr;                      // shots per CTA: forward, backward
+    dim3 gridf, gridr;
 };
 
 // CSR of the events of (shot, tile): off[key .. key+1) indexes ev, each
@@ -670,29 +678,18 @@ static int build_events(const Params& P, const int32_t* loc, int n, int32_t* off
     return off[nkey];
 }
 
-// Shots per CTA: the fewest waves x shots-per-CTA over 148 SMs at `occ` CTAs
-// per SM (the time one step takes scales with both), ties to more shots per CTA.
-static int choose_group(int ntiles, int B, int occ)
+// Shots per CTA: `preferred` (measured best on B200 for this kernel), capped so
+// the grid still fills the GPU; overridable through the environment variable
+// `env` for tuning.
+static int choose_group(int ntiles, int B, const char* env, int preferred)
 {
-    if (const char* e = getenv("SWEEP_B200_SHOTS_PER_CTA")) {
+    if (const char* e = getenv(env)) {
         const int g = atoi(e);
         if (g >= 1) return std::min(g, B);
     }
-    int best = 1;
-    double best_cost = 1e30;
-    for (int G = 1; G <= std::min(B, 16); ++G) {
-        const int groups = (B + G - 1) / G;
-        const long long ctas = (long long)ntiles * groups;
-        const long long slots = 148LL * occ;
-        const long long waves = (ctas + slots - 1) / slots;
-        // + one pipeline fill per CTA, worth about one shot
-        const double cost = (double)waves * (G + 1);
-        if (cost < best_cost - 1e-9 || (cost <= best_cost + 1e-9 && G > best)) {
-            best = G;
-            best_cost = cost;
-        }
-    }
-    return best;
+    int G = std::min(preferred, B);
+    while (G > 1 && (long long)ntiles * ((B + G - 1) / G) < 2LL * 148) --G;
+    return std::max(G, 1);
 }
 
 static Plan make_plan(const sweep_acoustic_desc* d)
@@ -744,10 +741,13 @@ static Plan make_plan(const sweep_acoustic_desc* d)
     P.ntx = (d->nx + TX - 1) / TX;
     P.ntz = (d->nz + TZ - 1) / TZ;
     const int ntiles = P.ntx * P.ntz;
-    P.G = P.per_shot ? 1 : choose_group(ntiles, P.B, 2);
-    const int ngroups = (P.B + P.G - 1) / P.G;
-    pl.nslot = P.per_shot ? P.B : ngroups;
-    pl.grid = dim3(P.ntx, P.ntz, ngroups);
+    pl.Gf = P.per_shot ? 1 : choose_group(ntiles, P.B, "SWEEP_B200_SHOTS_PER_CTA_FWD", 2);
+    pl.Gr = P.per_shot ? 1 : choose_group(ntiles, P.B, "SWEEP_B200_SHOTS_PER_CTA_REV", 4);
+    // blockIdx.x = shot group (fastest), blockIdx.y = tile slot
+    pl.gridf = dim3((P.B + pl.Gf - 1) / pl.Gf, ntiles);
+    pl.gridr = dim3((P.B + pl.Gr - 1) / pl.Gr, ntiles);
+    pl.nslot = P.per_shot ? P.B : (int)pl.gridr.x;
+    P.G = pl.Gr;
     return pl;
 }
 
@@ -755,6 +755,7 @@ struct Common {
     float *cf, *ca, *vv;
     int32_t *src_off, *rec_off;
     int2 *src_ev, *rec_ev;
+    int* order;
     int* err;
 };
 
@@ -784,6 +785,7 @@ static Common carve_common(Carve& c, const Plan& pl)
     w.rec_off = c.take<int32_t>(nkey);
     w.src_ev = c.take<int2>((long long)pl.P.B * std::max(pl.P.nsrc, 1));
     w.rec_ev = c.take<int2>((long long)pl.P.B * std::max(pl.P.nrec, 1));
+    w.order = c.take<int>((long long)pl.P.ntx * pl.P.ntz);
     w.err = c.take<int>(1);
     return w;
 }
@@ -834,17 +836,32 @@ static float* tape_last(void* tape, const Plan& pl)
 }
 
 struct VecStage {
-    std::vector<int32_t> ls, lr, os, orr, fill;
+    std::vector<int32_t> ls, lr, os, orr, fill, ord;
     std::vector<int2> es, er;
     HostStage h{};
     VecStage(const Params& P)
         : ls((size_t)P.B * P.nsrc * 2 + 1), lr((size_t)P.B * P.nrec * 2 + 1),
           os((size_t)P.B * P.ntx * P.ntz + 1), orr((size_t)P.B * P.ntx * P.ntz + 1),
-          fill((size_t)P.B * P.ntx * P.ntz + 1), es((size_t)P.B * P.nsrc + 1), er((size_t)P.B * P.nrec + 1)
+          fill((size_t)P.B * P.ntx * P.ntz + 1), ord((size_t)P.ntx * P.ntz),
+          es((size_t)P.B * P.nsrc + 1), er((size_t)P.B * P.nrec + 1)
     {
-        h = HostStage{ls.data(), lr.data(), os.data(), orr.data(), es.data(), er.data(), fill.data()};
+        h = HostStage{ls.data(), lr.data(), os.data(), orr.data(), es.data(), er.data(), fill.data(), ord.data()};
     }
 };
+
+// Tile slots, heaviest first (the block scheduler hands out blocks in order):
+// tiles crossing both CPML rings, then one, then the interior.  No allocation.
+static void tile_order(const Params& P, int32_t* order)
+{
+    const int ntiles = P.ntx * P.ntz;
+    int n = 0;
+    for (int want = 2; want >= 0; --want)
+        for (int t = 0; t < ntiles; ++t) {
+            const int tx0 = (t % P.ntx) * TX, tz0 = (t / P.ntx) * TZ;
+            const bool rx = tx0 < P.px0 || tx0 + TX > P.px1, rz = tz0 < P.pz0 || tz0 + TZ > P.pz1;
+            if ((rx ? 1 : 0) + (rz ? 1 : 0) == want) order[n++] = t;
+        }
+}
 
 // Per-call set-up shared by both passes: model fields, event tables, error flag.
 static void setup_common(const sweep_acoustic_desc* d, Plan& pl, const Common& w, cudaStream_t st,
@@ -869,6 +886,10 @@ static void setup_common(const sweep_acoustic_desc* d, Plan& pl, const Common& w
     SWEEP_CUDA(cudaStreamSynchronize(st));
     P.src.off = w.src_off; P.src.ev = w.src_ev;
     P.rec.off = w.rec_off; P.rec.ev = w.rec_ev;
+    tile_order(P, h.order);
+    SWEEP_CUDA(cudaMemcpyAsync(w.order, h.order, (size_t)P.ntx * P.ntz * sizeof(int), cudaMemcpyHostToDevice, st));
+    SWEEP_CUDA(cudaStreamSynchronize(st));
+    P.order = w.order;
     SWEEP_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
     P.err = w.err;
 }
@@ -954,6 +975,8 @@ void forward_with(const sweep_acoustic_desc* d, float* record, void* tape, void*
         SWEEP_CUDA(cudaMemsetAsync(p, 0, n * 4, st));
     if (d->nrec > 0)
         SWEEP_CUDA(cudaMemsetAsync(record, 0, (size_t)d->B * d->nt * d->nrec * 4, st));
+    Params PF = P;
+    PF.G = pl.Gf;
     FwdMaps maps;
     for (int i = 0; i < 3; ++i) {
         maps.halo[i] = field_map(w.u[i], P, P.B, true);
@@ -969,7 +992,7 @@ void forward_with(const sweep_acoustic_desc* d, float* record, void* tape, void*
         F.now = in; F.prev = ip; F.u_next = w.u[ix];
         F.psix = px; F.psiz = pz; F.psixn = pxn; F.psizn = pzn;
         F.strips = strips ? strips + (long long)it * P.B * P.nstrip : nullptr;
-        fwd_kernel<<<pl.grid, NTH, fwd_smem(), st>>>(maps, P, F, it);
+        fwd_kernel<<<pl.gridf, NTH, fwd_smem(), st>>>(maps, PF, F, it);
         SWEEP_LAUNCH_CHECK();
         const int t = ip; ip = in; in = ix; ix = t;
         std::swap(px, pxn); std::swap(pz, pzn);
@@ -1054,7 +1077,7 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
         R.apx_o = w.aux[1 - cur]; R.apz_o = w.aux[3 - cur]; R.azx_o = w.aux[5 - cur]; R.azz_o = w.aux[7 - cur];
         R.rprev = rp; R.rnow = rn; R.r_next = w.r[rx];
         R.strips = do_recon ? strips + (long long)(it - 1) * P.B * P.nstrip : nullptr;
-        rev_kernel<<<pl.grid, NTH, rev_smem(), st>>>(maps, P, R, it, do_recon);
+        rev_kernel<<<pl.gridr, NTH, rev_smem(), st>>>(maps, P, R, it, do_recon);
         SWEEP_LAUNCH_CHECK();
         int t = lp; lp = ln; ln = lx; lx = t;
         cur = 1 - cur;

@@ -14,6 +14,7 @@ struct HostStage {
     int32_t *off_src, *off_rec;      // (B * ntiles + 1)
     int2 *ev_src, *ev_rec;           // (B * nsrc), (B * nrec)
     int32_t* fill;                   // (B * ntiles)
+    int32_t* order;                  // (ntiles)
 };
 
 void sizes(const sweep_acoustic_desc*, int, int, int64_t*, int64_t*);

@@ -36,7 +36,7 @@ std::mutex g_mutex;
 void* g_scratch_ptr[kMaxDevices] = {};
 
 int32_t h_loc_src[2 * kMaxEvents], h_loc_rec[2 * kMaxEvents];
-int32_t h_off_src[kMaxKeys + 1], h_off_rec[kMaxKeys + 1], h_fill[kMaxKeys + 1];
+int32_t h_off_src[kMaxKeys + 1], h_off_rec[kMaxKeys + 1], h_fill[kMaxKeys + 1], h_order[kMaxKeys + 1];
 int2 h_ev_src[kMaxEvents], h_ev_rec[kMaxEvents];
 
 // Device address of this device's scratch array, looked up once per device.
@@ -77,7 +77,7 @@ extern "C" SWEEP_B200_API int sweep_b200_acoustic_forward_noalloc(const sweep_ac
                       (long long)nes, (long long)ner);
         std::lock_guard<std::mutex> lock(g_mutex);
         void* ws = scratch_of_current_device();
-        const a2d::HostStage stage{h_loc_src, h_loc_rec, h_off_src, h_off_rec, h_ev_src, h_ev_rec, h_fill};
+        const a2d::HostStage stage{h_loc_src, h_loc_rec, h_off_src, h_off_rec, h_ev_src, h_ev_rec, h_fill, h_order};
         a2d::forward_with(d, record, nullptr, ws, kNoAllocScratchBytes, static_cast<cudaStream_t>(stream),
                           &stage);
     });
