@@ -1,0 +1,839 @@
+// acoustic3d.cu -- 3-D constant-density acoustic propagation on B200 (sm_100a):
+// 8th-order-in-space / 2nd-order-in-time leapfrog with CPML, exact adjoint,
+// boundary-saving reconstruction and vp imaging.
+//
+// Numerics follow the reference's compiled path (impl='c'):
+//   forward step       reference src/sweep/csrc/cuda/equations/acoustic3d/forward_split.cu:79-290
+//                      (interior; CPML shell with the product-rule split
+//                      a * d(psi) + d(a) * psi on the band plus one cell)
+//   adjoint step       reference .../acoustic3d/adjoint_split.cu:14-320
+//   reconstruction     reference .../acoustic3d/forward_split.cu:292-372
+//   reverse step order reference .../acoustic3d/driver_traits.cuh:481-590
+//
+// Schedule (the B200 part): the stencil kernels stream along z.  A CTA owns a
+// 32 x 8 block of (x, y) columns for one shot; each thread keeps the nine
+// z-taps of its column in a register queue and reads the x / y taps from a
+// shared-memory plane (with its 4-cell halo) that is loaded one plane ahead
+// while the current plane computes.  Every field is pitched (x rows of
+// P = round_up(nx, 32) floats).  Point sources, receivers and boundary strips
+// are small gather / scatter kernels between the stencil launches.
+#include "common.cuh"
+
+namespace sweep {
+namespace a3d {
+
+constexpr int M = 4;
+constexpr int BXC = 32, BYC = 8;               // columns per CTA
+constexpr int PW = BXC + 2 * M, PH = BYC + 2 * M;
+constexpr int PN = PW * PH;                    // staged plane, floats
+constexpr int NTH = BXC * BYC;
+
+struct Params {
+    int B, nz, ny, nx, nt, nsrc, nrec;
+    int P;                                     // x pitch (floats)
+    long long SP, S;                           // plane stride, shot stride
+    int zc, nzc;                               // z chunk length, chunks
+    float dt, dz, dy, dx;
+    float lc[M + 1], gc[M + 1];
+    int z0, z1, y0, y1, x0, x1;                // physical box
+    int ex0, ex1, ey0, ey1, ez0, ez1;          // forward CPML branch: ix < ex0 || ix >= ex1 ...
+    int qx0, qx1, qy0, qy1, qz0, qz1;          // adjoint clear box / reconstruction box
+    int wzl, wzh, wyl, wyh, wxl, wxh;          // strip widths
+    long long n_top, n_bot, nring, nstrip;
+    const float *az, *bz, *dbz, *ay, *by, *dby, *ax, *bx, *dbx;
+    const float *cf, *ca, *vv;                 // model fields, pitched (one copy: shared model)
+};
+
+// ------------------------------------------------------------------ device
+__device__ __forceinline__ float tap(float uk, float u0) { return __fsub_rn(uk, u0); }
+
+// difference-form Laplacian at p along stride st (reference laplace.cuh:327-380)
+__device__ __forceinline__ float lap_p(const float* p, long long st, const Params& P, float h)
+{
+    const float u0 = p[0];
+    float acc = P.lc[1] * (tap(p[-st], u0) + tap(p[st], u0));
+    acc = acc + P.lc[2] * (tap(p[-2 * st], u0) + tap(p[2 * st], u0));
+    acc = acc + P.lc[3] * (tap(p[-3 * st], u0) + tap(p[3 * st], u0));
+    acc = acc + P.lc[4] * (tap(p[-4 * st], u0) + tap(p[4 * st], u0));
+    return acc / (h * h);
+}
+
+// the same on a register queue q[0..8] (q[4] the centre)
+__device__ __forceinline__ float lap_q(const float* q, const Params& P, float h)
+{
+    const float u0 = q[M];
+    float acc = P.lc[1] * (tap(q[M - 1], u0) + tap(q[M + 1], u0));
+    acc = acc + P.lc[2] * (tap(q[M - 2], u0) + tap(q[M + 2], u0));
+    acc = acc + P.lc[3] * (tap(q[M - 3], u0) + tap(q[M + 3], u0));
+    acc = acc + P.lc[4] * (tap(q[M - 4], u0) + tap(q[M + 4], u0));
+    return acc / (h * h);
+}
+
+// centred first derivative at p along stride st (reference gradient.cuh:49-88)
+__device__ __forceinline__ float grad_p(const float* p, long long st, const Params& P, float h)
+{
+    float acc = P.gc[1] * (p[st] - p[-st]);
+    acc = acc + P.gc[2] * (p[2 * st] - p[-2 * st]);
+    acc = acc + P.gc[3] * (p[3 * st] - p[-3 * st]);
+    acc = acc + P.gc[4] * (p[4 * st] - p[-4 * st]);
+    return acc / h;
+}
+
+__device__ __forceinline__ float grad_q(const float* q, const Params& P, float h)
+{
+    float acc = P.gc[1] * (q[M + 1] - q[M - 1]);
+    acc = acc + P.gc[2] * (q[M + 2] - q[M - 2]);
+    acc = acc + P.gc[3] * (q[M + 3] - q[M - 3]);
+    acc = acc + P.gc[4] * (q[M + 4] - q[M - 4]);
+    return acc / h;
+}
+
+// strip cell s -> (iz, iy, ix): z faces (full x-y), y faces over the inner z
+// planes, x faces over the inner z planes and inner y rows
+__device__ __forceinline__ void strip_coord(const Params& P, long long s, int& iz, int& iy, int& ix)
+{
+    const int bx = P.x1 - P.x0, by = P.y1 - P.y0;
+    const long long pl = (long long)bx * by;
+    if (s < P.n_top) {
+        iz = P.z0 + (int)(s / pl); const long long r = s % pl; iy = P.y0 + (int)(r / bx); ix = P.x0 + (int)(r % bx);
+        return;
+    }
+    s -= P.n_top;
+    if (s < P.n_bot) {
+        iz = P.z1 - P.wzh + (int)(s / pl); const long long r = s % pl; iy = P.y0 + (int)(r / bx); ix = P.x0 + (int)(r % bx);
+        return;
+    }
+    s -= P.n_bot;
+    iz = P.z0 + P.wzl + (int)(s / P.nring);
+    long long r = s % P.nring;
+    if (r < (long long)P.wyl * bx) { iy = P.y0 + (int)(r / bx); ix = P.x0 + (int)(r % bx); return; }
+    r -= (long long)P.wyl * bx;
+    if (r < (long long)P.wyh * bx) { iy = P.y1 - P.wyh + (int)(r / bx); ix = P.x0 + (int)(r % bx); return; }
+    r -= (long long)P.wyh * bx;
+    const int ww = P.wxl + P.wxh;
+    iy = P.y0 + P.wyl + (int)(r / ww);
+    const int c = (int)(r % ww);
+    ix = c < P.wxl ? P.x0 + c : P.x1 - P.wxh + (c - P.wxl);
+}
+
+__device__ __forceinline__ bool in_phys(const Params& P, int iz, int iy, int ix)
+{
+    return iz >= P.z0 && iz < P.z1 && iy >= P.y0 && iy < P.y1 && ix >= P.x0 && ix < P.x1;
+}
+
+__device__ __forceinline__ bool in_recon(const Params& P, int iz, int iy, int ix)
+{
+    return iz >= P.qz0 && iz < P.qz1 && iy >= P.qy0 && iy < P.qy1 && ix >= P.qx0 && ix < P.qx1;
+}
+
+// Load plane iz of field f (one shot) with its x / y halo into registers
+// (staging for the plane that the next iteration will use).
+struct PlaneLoader {
+    static constexpr int PER = (PN + NTH - 1) / NTH;
+    float v[PER];
+    __device__ __forceinline__ void load(const float* __restrict__ f, const Params& P, int iz, int gy0, int gx0, int tid)
+    {
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            const int e = tid + j * NTH;
+            float x = 0.f;
+            if (e < PN) {
+                const int r = e / PW, c = e - r * PW;
+                const int gy = gy0 + r, gx = gx0 + c;
+                if (gy >= 0 && gy < P.ny && gx >= 0 && gx < P.nx)
+                    x = __ldg(f + iz * P.SP + (long long)gy * P.P + gx);
+            }
+            v[j] = x;
+        }
+    }
+    __device__ __forceinline__ void store(float* dst, int tid)
+    {
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            const int e = tid + j * NTH;
+            if (e < PN) dst[e] = v[j];
+        }
+    }
+};
+
+// ----------------------------------------------------------- forward step
+struct F3 {
+    const float* u_now; const float* u_prev; float* u_next;
+    const float *psx, *psy, *psz;              // CPML psi (read)
+    float *psxn, *psyn, *pszn;                 // CPML psi (written)
+    float *zx, *zy, *zz;                       // CPML zeta (in place)
+};
+
+// u_next = 2 u - u_prev + vp^2 dt^2 (Lap u + CPML terms) on [M, n-M)^3.
+// The CPML branch of an axis runs on its band plus one cell (reference
+// forward_split.cu:150-156) and uses the product-rule split
+// tmp = (((1 + b) Lap + db du) + a dpsi) + da psi (forward_split.cu:171-172).
+__global__ void __launch_bounds__(NTH) f3_step(const Params P, const F3 F)
+{
+    __shared__ float pl[2][PN];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BXC + tx;
+    const int gx0 = blockIdx.x * BXC - M, gy0 = blockIdx.y * BYC - M;
+    const int ix = blockIdx.x * BXC + tx, iy = blockIdx.y * BYC + ty;
+    const int b = blockIdx.z / P.nzc, zci = blockIdx.z - b * P.nzc;
+    const int zb = max(M, zci * P.zc), ze = min(P.nz - M, (zci + 1) * P.zc);
+    if (zb >= ze) return;
+    const bool col = ix >= M && ix < P.nx - M && iy >= M && iy < P.ny - M;
+    const bool cin = ix < P.nx && iy < P.ny;
+    const long long bo = (long long)b * P.S;
+    const float* __restrict__ un = F.u_now + bo;
+    const long long colo = (long long)iy * P.P + ix;
+    float q[2 * M + 1];
+#pragma unroll
+    for (int k = 0; k < 2 * M; ++k) q[k] = cin ? __ldg(un + (zb - M + k) * P.SP + colo) : 0.f;
+    PlaneLoader L;
+    L.load(un, P, zb, gy0, gx0, tid);
+    L.store(pl[0], tid);
+    for (int z = zb; z < ze; ++z) {
+        const int s = (z - zb) & 1;
+        q[2 * M] = cin ? __ldg(un + (z + M) * P.SP + colo) : 0.f;
+        __syncthreads();
+        const bool more = z + 1 < ze;
+        if (more) L.load(un, P, z + 1, gy0, gx0, tid);
+        if (col) {
+            const float* p = pl[s] + (ty + M) * PW + (tx + M);
+            const float lx = lap_p(p, 1, P, P.dx);
+            const float ly = lap_p(p, PW, P, P.dy);
+            const float lz = lap_q(q, P, P.dz);
+            const bool inx = ix < P.ex0 || ix >= P.ex1;
+            const bool iny = iy < P.ey0 || iy >= P.ey1;
+            const bool inz = z < P.ez0 || z >= P.ez1;
+            const long long i = bo + z * P.SP + colo;
+            float w;
+            if (!inx && !iny && !inz) {
+                w = (lx + ly) + lz;
+            } else {
+                w = 0.f;
+                if (inx) {
+                    const float du = grad_p(p, 1, P, P.dx);
+                    const float dps = grad_p(F.psx + i, 1, P, P.dx);
+                    const float a = __ldg(P.ax + ix), bb = __ldg(P.bx + ix), db = __ldg(P.dbx + ix);
+                    const float da = grad_p(P.ax + ix, 1, P, P.dx);
+                    const float ps = F.psx[i], zt = F.zx[i];
+                    const float tmp = (((1.f + bb) * lx + db * du) + a * dps) + da * ps;
+                    w += (1.f + bb) * tmp + a * zt;
+                    F.psxn[i] = bb * du + a * ps;
+                    F.zx[i] = bb * tmp + a * zt;
+                } else {
+                    w += lx;
+                }
+                if (iny) {
+                    const float du = grad_p(p, PW, P, P.dy);
+                    const float dps = grad_p(F.psy + i, P.P, P, P.dy);
+                    const float a = __ldg(P.ay + iy), bb = __ldg(P.by + iy), db = __ldg(P.dby + iy);
+                    const float da = grad_p(P.ay + iy, 1, P, P.dy);
+                    const float ps = F.psy[i], zt = F.zy[i];
+                    const float tmp = (((1.f + bb) * ly + db * du) + a * dps) + da * ps;
+                    w += (1.f + bb) * tmp + a * zt;
+                    F.psyn[i] = bb * du + a * ps;
+                    F.zy[i] = bb * tmp + a * zt;
+                } else {
+                    w += ly;
+                }
+                if (inz) {
+                    const float du = grad_q(q, P, P.dz);
+                    const float dps = grad_p(F.psz + i, P.SP, P, P.dz);
+                    const float a = __ldg(P.az + z), bb = __ldg(P.bz + z), db = __ldg(P.dbz + z);
+                    const float da = grad_p(P.az + z, 1, P, P.dz);
+                    const float ps = F.psz[i], zt = F.zz[i];
+                    const float tmp = (((1.f + bb) * lz + db * du) + a * dps) + da * ps;
+                    w += (1.f + bb) * tmp + a * zt;
+                    F.pszn[i] = bb * du + a * ps;
+                    F.zz[i] = bb * tmp + a * zt;
+                } else {
+                    w += lz;
+                }
+            }
+            F.u_next[i] = 2.f * q[M] - __ldg(F.u_prev + i) + __ldg(P.cf + z * P.SP + colo) * w;
+        }
+        if (more) L.store(pl[1 - s], tid);
+#pragma unroll
+        for (int k = 0; k < 2 * M; ++k) q[k] = q[k + 1];
+    }
+}
+
+// ------------------------------------------------- point events and strips
+// A coordinate in the outer stencil halo (never updated) counts as off the grid.
+__device__ __forceinline__ bool event_cell(const Params& P, const int* loc, long long e, long long& off)
+{
+    const int x = loc[3 * e], y = loc[3 * e + 1], z = loc[3 * e + 2];
+    if (x < M || x >= P.nx - M || y < M || y >= P.ny - M || z < M || z >= P.nz - M) return false;
+    off = (long long)z * P.SP + (long long)y * P.P + x;
+    return true;
+}
+
+// u[b, cell] += sign * amplitude of event (b, s) at step it.  rec_layout: the
+// amplitudes are a record cotangent (B, nt, n); else a wavelet (B, n, nt).
+// strip_only: only events whose cell lies in the restored boundary strips.
+__global__ void inject3(const Params P, float* __restrict__ u, const float* __restrict__ amp,
+                        const int* __restrict__ loc, int n, int it, int rec_layout, float sign, int strip_only)
+{
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (e >= (long long)P.B * n) return;
+    const int b = (int)(e / n), s = (int)(e - (long long)b * n);
+    long long off;
+    if (!event_cell(P, loc, e, off)) return;
+    if (strip_only) {
+        const int x = loc[3 * e], y = loc[3 * e + 1], z = loc[3 * e + 2];
+        if (!in_phys(P, z, y, x) || in_recon(P, z, y, x)) return;
+    }
+    const float a = rec_layout ? amp[((long long)b * P.nt + it) * n + s] : amp[((long long)b * n + s) * P.nt + it];
+    atomicAdd(u + (long long)b * P.S + off, sign * a);
+}
+
+// out[b, it, r] = u[b, cell]  (record layout)  or  out[b, s, it] = u[b, cell]
+// (wavelet-gradient layout)
+__global__ void gather3(const Params P, const float* __restrict__ u, float* __restrict__ out,
+                        const int* __restrict__ loc, int n, int it, int rec_layout)
+{
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (e >= (long long)P.B * n) return;
+    const int b = (int)(e / n), s = (int)(e - (long long)b * n);
+    long long off;
+    if (!event_cell(P, loc, e, off)) return;
+    const float v = u[(long long)b * P.S + off];
+    if (rec_layout) out[((long long)b * P.nt + it) * n + s] = v;
+    else out[((long long)b * n + s) * P.nt + it] = v;
+}
+
+// boundary strips: save (tape <- u) or restore (u <- tape), every shot
+__global__ void strips3(const Params P, float* __restrict__ u, float* __restrict__ tape, int restore)
+{
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (e >= (long long)P.B * P.nstrip) return;
+    const int b = (int)(e / P.nstrip);
+    int iz, iy, ix;
+    strip_coord(P, e - (long long)b * P.nstrip, iz, iy, ix);
+    float* c = u + (long long)b * P.S + (long long)iz * P.SP + (long long)iy * P.P + ix;
+    if (restore) *c = tape[e];
+    else tape[e] = *c;
+}
+
+__device__ __forceinline__ void kahan_add(float* acc, float* comp, long long o, float g)
+{
+    const float y = g - comp[o];
+    const float t = acc[o] + y;
+    comp[o] = (t - acc[o]) - y;
+    acc[o] = t;
+}
+
+struct Img {
+    const float *r_prev, *r_now, *r_next, *lam;   // u(it+1), u(it), u(it-1) - s(it), lambda(it)
+    float *gacc, *gcomp, *is, *ir;              // per-shot slots (B, S)
+};
+
+// vp imaging of the strip cells (reference acoustic2d/kernels.cu:83-131; the
+// 3-D twin acoustic3d/kernels.cu), after the restore and the strip-source removal
+__global__ void strip_image3(const Params P, const Img I)
+{
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (e >= (long long)P.B * P.nstrip) return;
+    const int b = (int)(e / P.nstrip);
+    int iz, iy, ix;
+    strip_coord(P, e - (long long)b * P.nstrip, iz, iy, ix);
+    const long long c = (long long)iz * P.SP + (long long)iy * P.P + ix;
+    const long long o = (long long)b * P.S + c;
+    const float dt2 = P.dt * P.dt;
+    const float utt = (I.r_next[o] - 2 * I.r_now[o] + I.r_prev[o]) / dt2;
+    const float lam = I.lam[o];
+    kahan_add(I.gacc, I.gcomp, o, 2.f * P.dt * P.dt * utt * lam / __ldg(P.vv + c));
+    if (I.is) { I.is[o] += utt * utt; I.ir[o] += lam * lam; }
+}
+
+// ------------------------------------------------------------ adjoint step
+// gw = ((v*v)*dt^2) * lambda, the tap value of the adjoint Laplacian
+// (reference adjoint_split.cu GW_AT); planes and queues hold gw.
+struct GwLoader {
+    static constexpr int PER = (PN + NTH - 1) / NTH;
+    float v[PER];
+    __device__ __forceinline__ void load(const float* __restrict__ l, const float* __restrict__ c, const Params& P,
+                                         int iz, int gy0, int gx0, int tid)
+    {
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            const int e = tid + j * NTH;
+            float x = 0.f;
+            if (e < PN) {
+                const int r = e / PW, cc = e - r * PW;
+                const int gy = gy0 + r, gx = gx0 + cc;
+                if (gy >= 0 && gy < P.ny && gx >= 0 && gx < P.nx) {
+                    const long long o = iz * P.SP + (long long)gy * P.P + gx;
+                    x = __ldg(c + o) * __ldg(l + o);
+                }
+            }
+            v[j] = x;
+        }
+    }
+    __device__ __forceinline__ void store(float* dst, int tid)
+    {
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            const int e = tid + j * NTH;
+            if (e < PN) dst[e] = v[j];
+        }
+    }
+};
+
+struct A3 {
+    const float* l_now; const float* l_prev; float* l_next;
+    const float *px, *py, *pz, *zx, *zy, *zz;          // adjoint CPML memories (read)
+    float *pxo, *pyo, *pzo, *zxo, *zyo, *zzo;          // (written)
+};
+
+// The transposed CPML terms of one axis at linear offset i (shot base bo),
+// stride st, profiles (a, b, db) at axis index c (reference adjoint_split.cu:205-255).
+__device__ __forceinline__ void adj_axis(const Params& P, const float* __restrict__ a, const float* __restrict__ bv,
+                                         const float* __restrict__ dbv, const float* __restrict__ lam,
+                                         const float* __restrict__ ca, const float* __restrict__ psi,
+                                         const float* __restrict__ zeta, long long i, long long ic, long long st,
+                                         int c, float gw, float h, float& L, float& Dg, float* pso, float* zto)
+{
+    const float a_ = __ldg(a + c), b_ = __ldg(bv + c);
+    const float da = grad_p(a + c, 1, P, h);
+    const float gt0 = b_ * zeta[i] + (1.0f + b_) * gw;
+    const float l0 = (1.0f + b_) * gt0;
+    float Lq = 0.0f, Dgg = 0.0f, Dq = 0.0f;
+#pragma unroll
+    for (int k = 1; k <= M; ++k) {
+        const long long np = i + k * st, nm = i - k * st;
+        const long long cp_ = ic + k * st, cm_ = ic - k * st;
+        const float bp = __ldg(bv + c + k), bm = __ldg(bv + c - k);
+        const float tp = bp * zeta[np] + ((1.0f + bp) * __ldg(ca + cp_)) * lam[np];
+        const float tm = bm * zeta[nm] + ((1.0f + bm) * __ldg(ca + cm_)) * lam[nm];
+        Lq += P.lc[k] * (tap((1.0f + bp) * tp, l0) + tap((1.0f + bm) * tm, l0));
+        Dgg += P.gc[k] * ((bp * psi[np] + __ldg(dbv + c + k) * tp) - (bm * psi[nm] + __ldg(dbv + c - k) * tm));
+        Dq += P.gc[k] * (__ldg(a + c + k) * tp - __ldg(a + c - k) * tm);
+    }
+    L = Lq * (1.0f / (h * h));
+    Dg = Dgg * (1.0f / h);
+    Dq = Dq * (1.0f / h);
+    pso[i] = (a_ * psi[i] + da * gt0) - Dq;
+    zto[i] = a_ * (zeta[i] + gw);
+}
+
+// lambda_next = exact transpose of the forward step (reference adjoint_split.cu:14-320):
+// pure interior  2 l - l_prev + Lap(gw) (difference form around gw);
+// shell          per axis outside the clear box the transposed CPML terms,
+//                inside it the bare Laplacian of gw.
+__global__ void __launch_bounds__(NTH) a3_step(const Params P, const A3 A)
+{
+    __shared__ float pl[2][PN];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BXC + tx;
+    const int gx0 = blockIdx.x * BXC - M, gy0 = blockIdx.y * BYC - M;
+    const int ix = blockIdx.x * BXC + tx, iy = blockIdx.y * BYC + ty;
+    const int b = blockIdx.z / P.nzc, zci = blockIdx.z - b * P.nzc;
+    const int zb = max(M, zci * P.zc), ze = min(P.nz - M, (zci + 1) * P.zc);
+    if (zb >= ze) return;
+    const bool col = ix >= M && ix < P.nx - M && iy >= M && iy < P.ny - M;
+    const bool cin = ix < P.nx && iy < P.ny;
+    const long long bo = (long long)b * P.S;
+    const float* __restrict__ ln = A.l_now + bo;
+    const long long colo = (long long)iy * P.P + ix;
+    const float invdx2 = 1.0f / (P.dx * P.dx), invdy2 = 1.0f / (P.dy * P.dy), invdz2 = 1.0f / (P.dz * P.dz);
+    float q[2 * M + 1];
+#pragma unroll
+    for (int k = 0; k < 2 * M; ++k) {
+        const long long o = (zb - M + k) * P.SP + colo;
+        q[k] = cin ? __ldg(P.ca + o) * __ldg(ln + o) : 0.f;
+    }
+    GwLoader L;
+    L.load(ln, P.ca, P, zb, gy0, gx0, tid);
+    L.store(pl[0], tid);
+    for (int z = zb; z < ze; ++z) {
+        const int s = (z - zb) & 1;
+        {
+            const long long o = (z + M) * P.SP + colo;
+            q[2 * M] = cin ? __ldg(P.ca + o) * __ldg(ln + o) : 0.f;
+        }
+        __syncthreads();
+        const bool more = z + 1 < ze;
+        if (more) L.load(ln, P.ca, P, z + 1, gy0, gx0, tid);
+        if (col) {
+            const float* p = pl[s] + (ty + M) * PW + (tx + M);
+            const long long ic = z * P.SP + colo;
+            const long long i = bo + ic;
+            const float gun = ln[ic];
+            const float gw = q[M];
+            const bool inx = ix < P.qx0 || ix >= P.qx1;
+            const bool iny = iy < P.qy0 || iy >= P.qy1;
+            const bool inz = z < P.qz0 || z >= P.qz1;
+            const float lprev = __ldg(A.l_prev + i);
+            if (!inx && !iny && !inz) {
+                float lapx = 0.0f, lapy = 0.0f, lapz = 0.0f;
+#pragma unroll
+                for (int k = 1; k <= M; ++k) {
+                    lapx += P.lc[k] * (tap(p[k], gw) + tap(p[-k], gw));
+                    lapy += P.lc[k] * (tap(p[k * PW], gw) + tap(p[-k * PW], gw));
+                    lapz += P.lc[k] * (tap(q[M + k], gw) + tap(q[M - k], gw));
+                }
+                A.l_next[i] = 2.0f * gun - lprev + lapx * invdx2 + lapy * invdy2 + lapz * invdz2;
+            } else {
+                float Lx, Ly, Lz, Dgx = 0.f, Dgy = 0.f, Dgz = 0.f;
+                if (inx) {
+                    adj_axis(P, P.ax, P.bx, P.dbx, A.l_now + bo, P.ca, A.px + bo, A.zx + bo, ic, ic, 1, ix, gw,
+                             P.dx, Lx, Dgx, A.pxo + bo, A.zxo + bo);
+                } else {
+                    Lx = 0.0f;
+#pragma unroll
+                    for (int k = 1; k <= M; ++k) Lx += P.lc[k] * (tap(p[k], gw) + tap(p[-k], gw));
+                    Lx *= invdx2;
+                }
+                if (iny) {
+                    adj_axis(P, P.ay, P.by, P.dby, A.l_now + bo, P.ca, A.py + bo, A.zy + bo, ic, ic, P.P, iy, gw,
+                             P.dy, Ly, Dgy, A.pyo + bo, A.zyo + bo);
+                } else {
+                    Ly = 0.0f;
+#pragma unroll
+                    for (int k = 1; k <= M; ++k) Ly += P.lc[k] * (tap(p[k * PW], gw) + tap(p[-k * PW], gw));
+                    Ly *= invdy2;
+                }
+                if (inz) {
+                    adj_axis(P, P.az, P.bz, P.dbz, A.l_now + bo, P.ca, A.pz + bo, A.zz + bo, ic, ic, P.SP, z, gw,
+                             P.dz, Lz, Dgz, A.pzo + bo, A.zzo + bo);
+                } else {
+                    Lz = 0.0f;
+#pragma unroll
+                    for (int k = 1; k <= M; ++k) Lz += P.lc[k] * (tap(q[M + k], gw) + tap(q[M - k], gw));
+                    Lz *= invdz2;
+                }
+                A.l_next[i] = 2.0f * gun - lprev + (Lx + Ly + Lz - Dgx - Dgy - Dgz);
+            }
+        }
+        if (more) L.store(pl[1 - s], tid);
+#pragma unroll
+        for (int k = 0; k < 2 * M; ++k) q[k] = q[k + 1];
+    }
+}
+
+// ---------------------------------------------- reconstruction and imaging
+struct R3 {
+    const float* r_now; const float* r_prev; float* r_next;  // u(it), u(it+1), u(it-1) - s(it)
+    const float* lam;                                       // lambda(it)
+    float *gacc, *gcomp, *is, *ir;                          // per-shot slots (B, S)
+};
+
+// u(it-1) = 2 u(it) - u(it+1) + vp^2 dt^2 Lap u(it) on the reconstruction box
+// (the physical box minus the restored strips) with the fused vp image
+// 2 dt^2 u_tt lambda(it) / vp (reference forward_split.cu:292-372).
+__global__ void __launch_bounds__(NTH) r3_recon(const Params P, const R3 R)
+{
+    __shared__ float pl[2][PN];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BXC + tx;
+    const int gx0 = blockIdx.x * BXC - M, gy0 = blockIdx.y * BYC - M;
+    const int ix = blockIdx.x * BXC + tx, iy = blockIdx.y * BYC + ty;
+    const int b = blockIdx.z / P.nzc, zci = blockIdx.z - b * P.nzc;
+    const int zb = max(P.qz0, zci * P.zc), ze = min(P.qz1, (zci + 1) * P.zc);
+    if (zb >= ze) return;
+    const bool col = ix >= P.qx0 && ix < P.qx1 && iy >= P.qy0 && iy < P.qy1;
+    const bool cin = ix < P.nx && iy < P.ny;
+    const long long bo = (long long)b * P.S;
+    const float* __restrict__ rn = R.r_now + bo;
+    const long long colo = (long long)iy * P.P + ix;
+    const float dt2 = P.dt * P.dt;
+    float q[2 * M + 1];
+#pragma unroll
+    for (int k = 0; k < 2 * M; ++k) q[k] = cin ? __ldg(rn + (zb - M + k) * P.SP + colo) : 0.f;
+    PlaneLoader L;
+    L.load(rn, P, zb, gy0, gx0, tid);
+    L.store(pl[0], tid);
+    for (int z = zb; z < ze; ++z) {
+        const int s = (z - zb) & 1;
+        q[2 * M] = cin ? __ldg(rn + (z + M) * P.SP + colo) : 0.f;
+        __syncthreads();
+        const bool more = z + 1 < ze;
+        if (more) L.load(rn, P, z + 1, gy0, gx0, tid);
+        if (col) {
+            const float* p = pl[s] + (ty + M) * PW + (tx + M);
+            const float w = (lap_p(p, 1, P, P.dx) + lap_p(p, PW, P, P.dy)) + lap_q(q, P, P.dz);
+            const long long ic = z * P.SP + colo;
+            const long long i = bo + ic;
+            const float u0 = q[M], up = __ldg(R.r_prev + i);
+            const float un = 2.0f * u0 - up + __ldg(P.cf + ic) * w;
+            R.r_next[i] = un;
+            const float utt = (un - 2 * u0 + up) / dt2;
+            const float lam = __ldg(R.lam + i);
+            kahan_add(R.gacc, R.gcomp, i, 2.f * P.dt * P.dt * utt * lam / __ldg(P.vv + ic));
+            if (R.is) { R.is[i] += utt * utt; R.ir[i] += lam * lam; }
+        }
+        if (more) L.store(pl[1 - s], tid);
+#pragma unroll
+        for (int k = 0; k < 2 * M; ++k) q[k] = q[k + 1];
+    }
+}
+
+// receiver illumination of the last adjoint step (it == 0), physical box
+__global__ void illum_tail3(const Params P, const float* __restrict__ lam, float* __restrict__ ir)
+{
+    const long long bx = P.x1 - P.x0, by = P.y1 - P.y0, bz = P.z1 - P.z0;
+    const long long n = (long long)P.B * bz * by * bx;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        long long r = e;
+        const int ix = P.x0 + (int)(r % bx); r /= bx;
+        const int iy = P.y0 + (int)(r % by); r /= by;
+        const int iz = P.z0 + (int)(r % bz); const int b = (int)(r / bz);
+        const long long o = (long long)b * P.S + (long long)iz * P.SP + (long long)iy * P.P + ix;
+        ir[o] += lam[o] * lam[o];
+    }
+}
+
+// model fields, pitched: cf = ((v*v)*dt)*dt, ca = (v*v)*(dt*dt), vv = v
+__global__ void prep3(const float* __restrict__ vp, int rows, int nx, int P, float dt,
+                      float* __restrict__ cf, float* __restrict__ ca, float* __restrict__ vv)
+{
+    const long long n = (long long)rows * P;
+    const float dt2 = dt * dt;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long row = i / P;
+        const int ix = (int)(i - row * P);
+        if (ix < nx) {
+            const float v = vp[row * nx + ix];
+            cf[i] = ((v * v) * dt) * dt; ca[i] = (v * v) * dt2; vv[i] = v;
+        } else {
+            cf[i] = 0.f; ca[i] = 0.f; vv[i] = 1.f;
+        }
+    }
+}
+
+// sum of the per-shot Kahan slots into the caller's unpitched (1, nz, ny, nx) gradient
+__global__ void finalize3(const float* __restrict__ acc, const float* __restrict__ comp,
+                          const float* __restrict__ is, const float* __restrict__ ir, int B, int rows, int nx,
+                          int P, long long S, float* __restrict__ g, float* __restrict__ ois, float* __restrict__ oir)
+{
+    const long long n = (long long)rows * nx;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long row = i / nx, ix = i - row * nx;
+        const long long c = row * P + ix;
+        float s = 0.f, a = 0.f, r = 0.f;
+        for (int b = 0; b < B; ++b) {
+            s += acc[b * S + c] - comp[b * S + c];
+            if (is) { a += is[b * S + c]; r += ir[b * S + c]; }
+        }
+        g[i] = s;
+        if (ois) { ois[i] = a; oir[i] = r; }
+    }
+}
+
+// ------------------------------------------------------------------- host
+static Params make_params(const sweep_acoustic_desc* d)
+{
+    SWEEP_REQUIRE(d != nullptr, "null descriptor");
+    SWEEP_REQUIRE(d->ndim == 3, "acoustic3d: ndim must be 3 (got %d)", d->ndim);
+    SWEEP_REQUIRE(d->M == M, "acoustic3d: only spatial order 8 (M = 4) is built (got M = %d)", d->M);
+    SWEEP_REQUIRE(d->B >= 1 && d->nt >= 1, "acoustic3d: B and nt must be >= 1");
+    SWEEP_REQUIRE(d->vp_stride == 0, "acoustic3d takes one model shared by every shot");
+    SWEEP_REQUIRE(d->nsrc >= 0 && d->nrec >= 0, "acoustic3d: negative source/receiver count");
+    for (int f = 0; f < 6; ++f)
+        SWEEP_REQUIRE(d->pad[f] >= 1, "acoustic3d: every face needs a PML pad >= 1 (face %d has %d)", f, d->pad[f]);
+    Params P{};
+    P.B = d->B; P.nz = d->nz; P.ny = d->ny; P.nx = d->nx; P.nt = d->nt;
+    P.nsrc = d->nsrc; P.nrec = d->nrec;
+    P.P = (d->nx + 31) / 32 * 32;
+    P.SP = (long long)d->ny * P.P;
+    P.S = (long long)d->nz * P.SP;
+    P.dt = d->dt; P.dz = d->dz; P.dy = d->dy; P.dx = d->dx;
+    for (int k = 0; k <= M; ++k) { P.lc[k] = d->lap[k]; P.gc[k] = d->grad[k]; }
+    P.z0 = d->pad[0] + M; P.z1 = d->nz - d->pad[1] - M;
+    P.y0 = d->pad[2] + M; P.y1 = d->ny - d->pad[3] - M;
+    P.x0 = d->pad[4] + M; P.x1 = d->nx - d->pad[5] - M;
+    SWEEP_REQUIRE(P.z1 > P.z0 && P.y1 > P.y0 && P.x1 > P.x0, "acoustic3d: empty physical box");
+    P.ex0 = P.x0 + 1; P.ex1 = P.x1 - 1; P.ey0 = P.y0 + 1; P.ey1 = P.y1 - 1; P.ez0 = P.z0 + 1; P.ez1 = P.z1 - 1;
+    P.qz0 = d->pad[0] + 2 * M + 1; P.qz1 = d->nz - (d->pad[1] + 2 * M + 1);
+    P.qy0 = d->pad[2] + 2 * M + 1; P.qy1 = d->ny - (d->pad[3] + 2 * M + 1);
+    P.qx0 = d->pad[4] + 2 * M + 1; P.qx1 = d->nx - (d->pad[5] + 2 * M + 1);
+    auto widths = [](int extent, int w, int& lo, int& hi) {
+        lo = std::min(w, std::max(extent, 0));
+        hi = std::min(w, std::max(extent - lo, 0));
+    };
+    const int w = M + 1;
+    widths(P.z1 - P.z0, w, P.wzl, P.wzh);
+    widths(P.y1 - P.y0, w, P.wyl, P.wyh);
+    widths(P.x1 - P.x0, w, P.wxl, P.wxh);
+    const long long bx = P.x1 - P.x0, by = P.y1 - P.y0;
+    const long long bzi = std::max(0, (P.z1 - P.wzh) - (P.z0 + P.wzl));
+    const long long byi = std::max(0LL, by - P.wyl - P.wyh);
+    P.n_top = P.wzl * bx * by; P.n_bot = P.wzh * bx * by;
+    P.nring = (P.wyl + P.wyh) * bx + byi * (P.wxl + P.wxh);
+    P.nstrip = P.n_top + P.n_bot + bzi * P.nring;
+    P.az = d->az; P.bz = d->bz; P.dbz = d->dbz; P.ay = d->ay; P.by = d->by; P.dby = d->dby;
+    P.ax = d->ax; P.bx = d->bx; P.dbx = d->dbx;
+    // z chunks: enough CTAs to fill the GPU twice, chunks of at least 16 planes
+    const long long cols = (long long)((d->nx + BXC - 1) / BXC) * ((d->ny + BYC - 1) / BYC) * d->B;
+    int nzc = (int)std::max(1LL, (2LL * 148 + cols - 1) / cols);
+    nzc = std::max(1, std::min(nzc, d->nz / 16));
+    P.zc = (d->nz + nzc - 1) / nzc;
+    P.nzc = (d->nz + P.zc - 1) / P.zc;
+    return P;
+}
+
+static dim3 stencil_grid(const Params& P)
+{
+    return dim3((P.nx + BXC - 1) / BXC, (P.ny + BYC - 1) / BYC, P.B * P.nzc);
+}
+
+struct Work {
+    float *cf, *ca, *vv;
+    float* f[22];                    // forward: u x3, psi x6, zeta x3; reverse: see backward()
+};
+
+static Work carve(Carve& c, const Params& P, int nfields)
+{
+    Work w{};
+    w.cf = c.take<float>(P.S); w.ca = c.take<float>(P.S); w.vv = c.take<float>(P.S);
+    for (int i = 0; i < nfields; ++i) w.f[i] = c.take<float>((long long)P.B * P.S);
+    return w;
+}
+
+static int64_t tape_bytes(const Params& P)
+{
+    Carve c(nullptr);
+    c.take<float>((long long)P.nt * P.B * P.nstrip);
+    c.take<float>(2LL * P.B * P.S);
+    return c.off;
+}
+
+static float* tape_last(void* tape, const Params& P)
+{
+    Carve c(tape);
+    c.take<float>((long long)P.nt * P.B * P.nstrip);
+    return c.take<float>(2LL * P.B * P.S);
+}
+
+static constexpr int kFwdFields = 12, kRevFields = 22;
+
+void sizes(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, int64_t* ws, int64_t* tape)
+{
+    SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY, "acoustic3d: unknown memory mode %d", mem_mode);
+    (void)ckpt_every;
+    const Params P = make_params(d);
+    Carve c(nullptr);
+    carve(c, P, std::max(kFwdFields, kRevFields));
+    *ws = c.off;
+    *tape = tape_bytes(P);
+}
+
+static inline unsigned blocks_for(long long n, int threads) { return (unsigned)std::max(1LL, (n + threads - 1) / threads); }
+
+void forward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* record, void* tape,
+             void* ws, int64_t ws_bytes, cudaStream_t st)
+{
+    int64_t need_ws, need_tape;
+    sizes(d, mem_mode, ckpt_every, &need_ws, &need_tape);
+    SWEEP_REQUIRE(ws != nullptr && ws_bytes >= need_ws, "acoustic3d forward: workspace too small (%lld < %lld)",
+                  (long long)ws_bytes, (long long)need_ws);
+    SWEEP_REQUIRE(record != nullptr || d->nrec == 0, "acoustic3d forward: null record");
+    Params P = make_params(d);
+    Carve c(ws);
+    Work w = carve(c, P, kFwdFields);
+    const long long rows = (long long)d->nz * d->ny;
+    prep3<<<592, 256, 0, st>>>(d->vp, (int)rows, d->nx, P.P, d->dt, w.cf, w.ca, w.vv);
+    SWEEP_LAUNCH_CHECK();
+    P.cf = w.cf; P.ca = w.ca; P.vv = w.vv;
+    const long long n = (long long)P.B * P.S;
+    for (int i = 0; i < kFwdFields; ++i) SWEEP_CUDA(cudaMemsetAsync(w.f[i], 0, n * 4, st));
+    if (d->nrec > 0) SWEEP_CUDA(cudaMemsetAsync(record, 0, (size_t)d->B * d->nt * d->nrec * 4, st));
+    float* strips = static_cast<float*>(tape);
+    const dim3 grid = stencil_grid(P), block(BXC, BYC);
+    const unsigned gs = blocks_for((long long)P.B * P.nsrc, 128), gr = blocks_for((long long)P.B * P.nrec, 128);
+    const unsigned gst = blocks_for((long long)P.B * P.nstrip, 256);
+    int ip = 0, in = 1, ix = 2;
+    float* ps[3] = {w.f[3], w.f[4], w.f[5]};
+    float* psn[3] = {w.f[6], w.f[7], w.f[8]};
+    for (int it = 0; it < d->nt; ++it) {
+        F3 F{w.f[in], w.f[ip], w.f[ix], ps[0], ps[1], ps[2], psn[0], psn[1], psn[2], w.f[9], w.f[10], w.f[11]};
+        f3_step<<<grid, block, 0, st>>>(P, F);
+        SWEEP_LAUNCH_CHECK();
+        if (strips && P.nstrip > 0)
+            strips3<<<gst, 256, 0, st>>>(P, w.f[in], strips + (long long)it * P.B * P.nstrip, 0);
+        if (d->nsrc > 0)
+            inject3<<<gs, 128, 0, st>>>(P, w.f[ix], d->wavelet, d->src_loc, d->nsrc, it, 0, 1.f, 0);
+        if (d->nrec > 0)
+            gather3<<<gr, 128, 0, st>>>(P, w.f[ix], record, d->rec_loc, d->nrec, it, 1);
+        SWEEP_LAUNCH_CHECK();
+        const int t = ip; ip = in; in = ix; ix = t;
+        for (int a = 0; a < 3; ++a) std::swap(ps[a], psn[a]);
+    }
+    if (strips) {
+        float* last = tape_last(tape, P);
+        SWEEP_CUDA(cudaMemcpyAsync(last, w.f[ip], n * 4, cudaMemcpyDeviceToDevice, st));       // U[nt-1]
+        SWEEP_CUDA(cudaMemcpyAsync(last + n, w.f[in], n * 4, cudaMemcpyDeviceToDevice, st));   // U[nt]
+    }
+}
+
+void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const float* adj, const void* tape,
+              float* grad_vp, float* grad_w, float* illum_s, float* illum_r,
+              void* ws, int64_t ws_bytes, cudaStream_t st)
+{
+    int64_t need_ws, need_tape;
+    sizes(d, mem_mode, ckpt_every, &need_ws, &need_tape);
+    SWEEP_REQUIRE(ws != nullptr && ws_bytes >= need_ws, "acoustic3d backward: workspace too small");
+    SWEEP_REQUIRE(tape != nullptr && grad_vp != nullptr, "acoustic3d backward: null tape or gradient");
+    SWEEP_REQUIRE(adj != nullptr || d->nrec == 0, "acoustic3d backward: null record cotangent");
+    SWEEP_REQUIRE((illum_s == nullptr) == (illum_r == nullptr), "acoustic3d backward: pass both illuminations or neither");
+    Params P = make_params(d);
+    Carve c(ws);
+    Work w = carve(c, P, kRevFields);
+    const long long rows = (long long)d->nz * d->ny;
+    prep3<<<592, 256, 0, st>>>(d->vp, (int)rows, d->nx, P.P, d->dt, w.cf, w.ca, w.vv);
+    SWEEP_LAUNCH_CHECK();
+    P.cf = w.cf; P.ca = w.ca; P.vv = w.vv;
+    const long long n = (long long)P.B * P.S;
+    const bool illum = illum_s != nullptr;
+    // fields: 0-2 lambda, 3-14 adjoint CPML (psi x,y,z and zeta x,y,z, two
+    // buffers each), 15-17 reconstruction, 18-19 Kahan slots, 20-21 illumination
+    for (int i = 0; i < kRevFields; ++i) SWEEP_CUDA(cudaMemsetAsync(w.f[i], 0, n * 4, st));
+    if (grad_w && d->nsrc > 0) SWEEP_CUDA(cudaMemsetAsync(grad_w, 0, (size_t)d->B * d->nsrc * d->nt * 4, st));
+    const float* strips = static_cast<const float*>(tape);
+    const float* last = tape_last(const_cast<void*>(tape), P);
+    SWEEP_CUDA(cudaMemcpyAsync(w.f[15], last + n, n * 4, cudaMemcpyDeviceToDevice, st));   // prev = U[nt]
+    SWEEP_CUDA(cudaMemcpyAsync(w.f[16], last, n * 4, cudaMemcpyDeviceToDevice, st));       // now  = U[nt-1]
+    const dim3 grid = stencil_grid(P), block(BXC, BYC);
+    const unsigned gs = blocks_for((long long)P.B * P.nsrc, 128), gr = blocks_for((long long)P.B * P.nrec, 128);
+    const unsigned gst = blocks_for((long long)P.B * P.nstrip, 256);
+    int lp = 0, ln = 1, lx = 2, rp = 15, rn = 16, rx = 17, cur = 0;
+    float* gacc = w.f[18];
+    float* gcomp = w.f[19];
+    float* is = illum ? w.f[20] : nullptr;
+    float* ir = illum ? w.f[21] : nullptr;
+    for (int it = d->nt - 1; it >= 0; --it) {
+        float* a_in[6];
+        float* a_out[6];
+        for (int k = 0; k < 6; ++k) { a_in[k] = w.f[3 + 2 * k + cur]; a_out[k] = w.f[3 + 2 * k + 1 - cur]; }
+        A3 A{w.f[ln], w.f[lp], w.f[lx], a_in[0], a_in[1], a_in[2], a_in[3], a_in[4], a_in[5],
+             a_out[0], a_out[1], a_out[2], a_out[3], a_out[4], a_out[5]};
+        a3_step<<<grid, block, 0, st>>>(P, A);
+        SWEEP_LAUNCH_CHECK();
+        if (d->nrec > 0)
+            inject3<<<gr, 128, 0, st>>>(P, w.f[lx], adj, d->rec_loc, d->nrec, it, 1, 1.f, 0);
+        int t = lp; lp = ln; ln = lx; lx = t;
+        cur = 1 - cur;
+        if (grad_w && d->nsrc > 0)
+            gather3<<<gs, 128, 0, st>>>(P, w.f[ln], grad_w, d->src_loc, d->nsrc, it, 0);
+        if (it > 0) {
+            R3 R{w.f[rn], w.f[rp], w.f[rx], w.f[ln], gacc, gcomp, is, ir};
+            r3_recon<<<grid, block, 0, st>>>(P, R);
+            if (P.nstrip > 0) {
+                strips3<<<gst, 256, 0, st>>>(P, w.f[rx], const_cast<float*>(strips) + (long long)(it - 1) * P.B * P.nstrip, 1);
+                if (d->nsrc > 0)
+                    inject3<<<gs, 128, 0, st>>>(P, w.f[rx], d->wavelet, d->src_loc, d->nsrc, it, 0, -1.f, 1);
+                Img I{w.f[rp], w.f[rn], w.f[rx], w.f[ln], gacc, gcomp, is, ir};
+                strip_image3<<<gst, 256, 0, st>>>(P, I);
+            }
+            if (d->nsrc > 0)
+                inject3<<<gs, 128, 0, st>>>(P, w.f[rx], d->wavelet, d->src_loc, d->nsrc, it, 0, 1.f, 0);
+            SWEEP_LAUNCH_CHECK();
+            t = rp; rp = rn; rn = rx; rx = t;
+        } else if (illum) {
+            illum_tail3<<<592, 256, 0, st>>>(P, w.f[ln], ir);
+            SWEEP_LAUNCH_CHECK();
+        }
+    }
+    finalize3<<<592, 256, 0, st>>>(gacc, gcomp, is, ir, P.B, (int)rows, d->nx, P.P, P.S, grad_vp, illum_s, illum_r);
+    SWEEP_LAUNCH_CHECK();
+}
+
+}  // namespace a3d
+}  // namespace sweep

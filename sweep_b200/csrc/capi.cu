@@ -3,6 +3,15 @@
 // into (non-zero return, message) -- nothing is thrown across the boundary.
 #include "acoustic2d.cuh"
 
+namespace sweep {
+namespace a3d {
+void sizes(const sweep_acoustic_desc*, int, int, int64_t*, int64_t*);
+void forward(const sweep_acoustic_desc*, int, int, float*, void*, void*, int64_t, cudaStream_t);
+void backward(const sweep_acoustic_desc*, int, int, const float*, const void*, float*, float*,
+              float*, float*, void*, int64_t, cudaStream_t);
+}  // namespace a3d
+}  // namespace sweep
+
 using namespace sweep;
 
 extern "C" int sweep_b200_abi_version(void) { return SWEEP_B200_ABI_VERSION; }
@@ -13,8 +22,9 @@ extern "C" int sweep_b200_acoustic_sizes(const sweep_acoustic_desc* d, int32_t m
 {
     return guarded(err, err_cap, [&] {
         SWEEP_REQUIRE(d && workspace_bytes && tape_bytes, "null argument");
-        SWEEP_REQUIRE(d->ndim == 2, "acoustic: ndim %d is not built", d->ndim);
-        a2d::sizes(d, mem_mode, ckpt_every, workspace_bytes, tape_bytes);
+        SWEEP_REQUIRE(d->ndim == 2 || d->ndim == 3, "acoustic: ndim %d is not built", d->ndim);
+        if (d->ndim == 2) a2d::sizes(d, mem_mode, ckpt_every, workspace_bytes, tape_bytes);
+        else a3d::sizes(d, mem_mode, ckpt_every, workspace_bytes, tape_bytes);
     });
 }
 
@@ -24,9 +34,13 @@ extern "C" int sweep_b200_acoustic_forward(const sweep_acoustic_desc* d, int32_t
 {
     return guarded(err, err_cap, [&] {
         SWEEP_REQUIRE(d != nullptr, "null descriptor");
-        SWEEP_REQUIRE(d->ndim == 2, "acoustic: ndim %d is not built", d->ndim);
-        a2d::forward(d, mem_mode, ckpt_every, record, tape, workspace, workspace_bytes,
-                     static_cast<cudaStream_t>(stream));
+        SWEEP_REQUIRE(d->ndim == 2 || d->ndim == 3, "acoustic: ndim %d is not built", d->ndim);
+        if (d->ndim == 2)
+            a2d::forward(d, mem_mode, ckpt_every, record, tape, workspace, workspace_bytes,
+                         static_cast<cudaStream_t>(stream));
+        else
+            a3d::forward(d, mem_mode, ckpt_every, record, tape, workspace, workspace_bytes,
+                         static_cast<cudaStream_t>(stream));
     });
 }
 
@@ -38,8 +52,12 @@ extern "C" int sweep_b200_acoustic_backward(const sweep_acoustic_desc* d, int32_
 {
     return guarded(err, err_cap, [&] {
         SWEEP_REQUIRE(d != nullptr, "null descriptor");
-        SWEEP_REQUIRE(d->ndim == 2, "acoustic: ndim %d is not built", d->ndim);
-        a2d::backward(d, mem_mode, ckpt_every, adj, tape, grad_vp, grad_wavelet, illum_src, illum_rec,
-                      workspace, workspace_bytes, static_cast<cudaStream_t>(stream));
+        SWEEP_REQUIRE(d->ndim == 2 || d->ndim == 3, "acoustic: ndim %d is not built", d->ndim);
+        if (d->ndim == 2)
+            a2d::backward(d, mem_mode, ckpt_every, adj, tape, grad_vp, grad_wavelet, illum_src, illum_rec,
+                          workspace, workspace_bytes, static_cast<cudaStream_t>(stream));
+        else
+            a3d::backward(d, mem_mode, ckpt_every, adj, tape, grad_vp, grad_wavelet, illum_src, illum_rec,
+                          workspace, workspace_bytes, static_cast<cudaStream_t>(stream));
     });
 }
