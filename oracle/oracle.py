@@ -70,6 +70,14 @@ def _lib(prec: str):
         lib.oracle_a3d_forward.argtypes = geo3 + [P, P]
         lib.oracle_a3d_backward.restype = i
         lib.oracle_a3d_backward.argtypes = geo3 + [P, P, P, P]
+        geo_el = [i, i, i, i, i, P, real, real, real, P, P, P, P, P, l,
+                  i, P, P, i, P, i, P, i, P]
+        lib.oracle_el2d_tape_len.restype = l
+        lib.oracle_el2d_tape_len.argtypes = [i, i, i, i, i, P]
+        lib.oracle_el2d_forward.restype = i
+        lib.oracle_el2d_forward.argtypes = geo_el + [P, P]
+        lib.oracle_el2d_backward.restype = i
+        lib.oracle_el2d_backward.argtypes = geo_el + [P, P, P, P, P]
         _LIBS[prec] = lib
     return _LIBS[prec]
 
@@ -108,14 +116,16 @@ def fd_tables(M: int):
 
 
 # -------------------------------------------------------------------- CPML
-def setup_pml(width, start, max_pml, dt, n, max_vel, pml_freq, r_val=0.001, n_power=2, eps=1e-9):
-    """a, b profiles of one axis in float32 (``pml.py:216-269``)."""
+def setup_pml(width, start, max_pml, dt, n, max_vel, pml_freq, r_val=0.001, n_power=2, eps=1e-9,
+              offset=0.0):
+    """a, b profiles of one axis in float32 (``pml.py:216-269``); ``offset`` 0.5
+    gives the half-grid profiles of the staggered CPML."""
     dtype = np.float32
     alpha0 = math.pi * pml_freq
     if max_pml == 0:
         return np.zeros(n, dtype), np.zeros(n, dtype)
     sigma0 = -(1 + n_power) * max_vel * math.log(r_val) / (2 * max_pml)
-    x = np.arange(n, dtype=dtype) + dtype(0.0)
+    x = np.arange(n, dtype=dtype) + dtype(offset)
     f0 = (dtype(start[0]) - x) / dtype(width[0]) if width[0] else np.zeros_like(x)
     f1 = (x - dtype(start[1])) / dtype(width[1]) if width[1] else np.zeros_like(x)
     frac = np.clip(np.maximum(f0, f1), 0.0, 1.0)
@@ -143,6 +153,35 @@ def cpml_profiles(pads, M, dt, spacing, shape, max_vel=4500.0, pml_freq=25.0):
         a, b = setup_pml(w, start, max_pml, dt, n, max_vel, pml_freq)
         db = np.gradient(b, spacing[d])
         out.append((a, b, db.astype(np.float32)))
+    return out
+
+
+def cpml_profiles_s(pads, M, dt, spacing, shape, max_vel=4500.0, pml_freq=25.0):
+    """Staggered-grid profiles per axis (shape order): ``(a, b, a_half, b_half)``
+    (``pml.py:81-154``; half = positions offset by half a cell)."""
+    out = []
+    for d, n in enumerate(shape):
+        w = pads[2 * d: 2 * d + 2]
+        start = [M + w[0], n - 1 - M - w[1]]
+        max_pml = max(w[0] * spacing[d], w[1] * spacing[d])
+        a, b = setup_pml(w, start, max_pml, dt, n, max_vel, pml_freq, offset=0.0)
+        ah, bh = setup_pml(w, start, max_pml, dt, n, max_vel, pml_freq, offset=0.5)
+        out.append((a, b, ah, bh))
+    return out
+
+
+def staggered_coefficients(M: int):
+    """Exact staggered first-derivative weights ``a_1..a_M`` as Fractions
+    (``scalars.py:25-49``; order 8 gives 1225/1024, -245/3072, 49/5120,
+    -5/7168, the constants of ``operators/staggered.cuh:351-354``)."""
+    out = []
+    for m in range(1, M + 1):
+        a = Fraction((-1) ** (m + 1), 2 * m - 1)
+        for n in range(1, M + 1):
+            if n != m:
+                num = (2 * n - 1) ** 2
+                a *= abs(Fraction(num, num - (2 * m - 1) ** 2))
+        out.append(a)
     return out
 
 
@@ -296,3 +335,107 @@ def acoustic_forward(vp, wavelet, src, rec, dh, dt, abcn, order=8, prec="f32", *
     ndim = np.asarray(src).shape[-1]
     cls = Acoustic2D if ndim == 2 else Acoustic3D
     return cls(vp, wavelet, src, rec, dh, dt, abcn, order, prec, **kw).forward(keep_tape=False)
+
+
+# ------------------------------------------------------------------ elastic
+ELASTIC_FIELDS = ("vx", "vz", "sxx", "szz", "sxz")
+
+
+class Elastic2D:
+    """2-D isotropic elastic oracle run (``fd_oracle_el.c``): models
+    ``vp, vs, rho`` of shape ``(nz, nx)`` or per shot ``(B, nz, nx)``; source
+    fields default to the explosive ``(sxx, szz)``, receiver fields to
+    ``(vx, vz)`` (``src/sweep/equations/elastic.py:123-128``)."""
+
+    def __init__(self, vp, vs, rho, wavelet, src, rec, dh, dt, abcn, order=8, prec="f32",
+                 source_fields=("sxx", "szz"), receiver_fields=("vx", "vz"),
+                 max_vel=4500.0, pml_freq=25.0):
+        self.prec = prec
+        self.real = np.float32 if prec == "f32" else np.float64
+        models = [np.asarray(m, np.float32) for m in (vp, vs, rho)]
+        self.per_shot = models[0].ndim == 3
+        self.M = M = order // 2
+        w, s, r = _batch_io(wavelet, src, rec, 2)
+        self.B, self.nt = w.shape[0], w.shape[-1]
+        self.phys = models[0].shape[-2:]
+        self.pad = abcn
+        self.shape = tuple(n + 2 * abcn + 2 * M for n in self.phys)
+        padw = [(abcn + M, abcn + M)] * 2
+        lead = [(0, 0)] if self.per_shot else []
+        self.models = [np.ascontiguousarray(np.pad(m, lead + padw, mode="edge").astype(self.real))
+                       for m in models]
+        self.m_stride = int(np.prod(self.shape)) if self.per_shot else 0
+        sp = dh if np.ndim(dh) else [dh] * 2
+        self.spacing = [float(x) for x in sp]
+        self.dt = float(dt)
+        prof = cpml_profiles_s([abcn] * 4, M, dt, self.spacing, self.shape, max_vel, pml_freq)
+        (az, bz, azh, bzh), (ax, bx, axh, bxh) = prof
+        self.prof = np.ascontiguousarray(
+            np.concatenate([az, bz, azh, bzh, ax, bx, axh, bxh]).astype(self.real))
+        c = staggered_coefficients(M)
+        self.coef = np.array([0.0] + [float(x) for x in c], np.float64).astype(self.real)
+        if self.real is np.float32:
+            self.coef = np.array([0.0] + [np.float32(float(x)) for x in c], np.float32)
+        off = abcn + M
+        self.src = np.ascontiguousarray((s + off).astype(np.int32))
+        self.rec = np.ascontiguousarray((r + off).astype(np.int32))
+        self.wavelet = np.ascontiguousarray(w.astype(self.real))
+        self.nrec = self.rec.shape[1]
+        self.sf = np.array([ELASTIC_FIELDS.index(f) for f in source_fields], np.int32)
+        self.rf = np.array([ELASTIC_FIELDS.index(f) for f in receiver_fields], np.int32)
+
+    def _geo(self):
+        nz, nx = self.shape
+        self._pad = np.array([self.pad] * 4, np.int32)
+        return [self.B, nz, nx, self.nt, self.M, _ptr(self._pad), self.dt, self.spacing[0],
+                self.spacing[1], _ptr(self.coef), _ptr(self.prof), _ptr(self.models[0]),
+                _ptr(self.models[1]), _ptr(self.models[2]), self.m_stride,
+                1, _ptr(self.src), _ptr(self.wavelet), len(self.sf), _ptr(self.sf),
+                self.nrec, _ptr(self.rec), len(self.rf), _ptr(self.rf)]
+
+    def crop(self, g):
+        M, a = self.M, self.pad
+        sl = tuple(slice(a + M, a + M + n) for n in self.phys)
+        return g[(Ellipsis,) + sl]
+
+    def forward(self, keep_tape=True):
+        """Records ``(B, nt, nrec, nfield)``."""
+        lib = _lib(self.prec)
+        nz, nx = self.shape
+        rec = np.zeros((self.B, self.nt, self.nrec, len(self.rf)), self.real)
+        self.tape = None
+        if keep_tape:
+            pad = np.array([self.pad] * 4, np.int32)
+            n = lib.oracle_el2d_tape_len(self.B, nz, nx, self.nt, self.M, _ptr(pad))
+            self.tape = np.zeros(n, self.real)
+        rc = lib.oracle_el2d_forward(*self._geo(), _ptr(rec),
+                                     _ptr(self.tape) if keep_tape else None)
+        assert rc == 0
+        return rec
+
+    def backward(self, adj):
+        """``adj``: record cotangent ``(B, nt, nrec, nfield)``; returns the
+        cropped ``(grad_vp, grad_vs, grad_rho)``."""
+        lib = _lib(self.prec)
+        a = np.ascontiguousarray(np.asarray(adj).astype(self.real))
+        shp = ((self.B,) if self.per_shot else ()) + self.shape
+        g = [np.zeros(shp, self.real) for _ in range(3)]
+        rc = lib.oracle_el2d_backward(*self._geo(), _ptr(a), _ptr(self.tape),
+                                      _ptr(g[0]), _ptr(g[1]), _ptr(g[2]))
+        assert rc == 0
+        return tuple(self.crop(x) for x in g)
+
+
+def elastic_gradient(vp, vs, rho, wavelet, src, rec, obs, dh, dt, abcn, order=8, prec="f32", **kw):
+    """Record, loss ``0.5 ||pred - obs||^2`` and cropped ``(vp, vs, rho)``
+    gradients (summed over shots for shared models)."""
+    run = Elastic2D(vp, vs, rho, wavelet, src, rec, dh, dt, abcn, order, prec, **kw)
+    pred = run.forward(keep_tape=True)
+    res = pred - np.asarray(obs, run.real)
+    loss = 0.5 * float(np.sum(res.astype(np.float64) ** 2))
+    return pred, loss, run.backward(res)
+
+
+def elastic_forward(vp, vs, rho, wavelet, src, rec, dh, dt, abcn, order=8, prec="f32", **kw):
+    return Elastic2D(vp, vs, rho, wavelet, src, rec, dh, dt, abcn, order, prec, **kw).forward(
+        keep_tape=False)

@@ -88,3 +88,43 @@ def test_acoustic3d_oracle_matches_reference():
     # 0 is exact; the oracle keeps every shot.
     assert rel(gw[0], d["grad_wavelet"]) < 1e-5
     assert np.abs(gw[1]).max() > 0
+
+
+def _el_args(d):
+    return float(d["dh"]), float(d["dt"]), int(d["abcn"]), int(d["order"])
+
+
+@pytest.mark.parametrize("prec,tol", [("f32", 2e-6), ("f64", 5e-6)])
+def test_elastic2d_oracle_matches_reference(prec, tol):
+    """Records and vp / vs / rho gradients of the reference's boundary-saving
+    elastic path (explosive sources, (vx, vz) receivers)."""
+    d = np.load(GOLD / "elastic2d.npz")
+    obs = O.elastic_forward(d["vp_true"], d["vs_true"], d["rho_true"], d["wavelet"], d["src"],
+                            d["rec"], *_el_args(d), prec=prec)
+    assert obs.shape == d["obs"].shape
+    assert rel(obs, d["obs"]) < tol
+    pred, loss, (gvp, gvs, grho) = O.elastic_gradient(
+        d["vp_init"], d["vs_init"], d["rho_init"], d["wavelet"], d["src"], d["rec"], d["obs"],
+        *_el_args(d), prec=prec)
+    assert rel(pred, d["pred"]) < tol
+    assert abs(loss - float(d["loss"])) < 1e-5 * float(d["loss"])
+    assert rel(gvp, d["grad_vp"]) < 5 * tol
+    assert rel(gvs, d["grad_vs"]) < 5 * tol
+    assert rel(grho, d["grad_rho"]) < 5 * tol
+
+
+def test_elastic2d_reference_full_and_boundary_modes_agree():
+    """The reference's full-storage gradient adds the it = 0 image the
+    boundary-saving reverse skips; the two differ at the 1e-6 level."""
+    d = np.load(GOLD / "elastic2d.npz")
+    for k in ("vp", "vs", "rho"):
+        assert rel(d[f"grad_{k}_full"], d[f"grad_{k}"]) < 1e-5
+
+
+def test_staggered_coefficients_match_compiled_constants():
+    """Order 8 gives the compile-time constants of operators/staggered.cuh:351-354."""
+    from fractions import Fraction
+    c = O.staggered_coefficients(4)
+    assert c == [Fraction(1225, 1024), Fraction(-245, 3072), Fraction(49, 5120), Fraction(-5, 7168)]
+    assert O.staggered_coefficients(1) == [Fraction(1)]
+    assert O.staggered_coefficients(2) == [Fraction(9, 8), Fraction(-1, 24)]
