@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define SWEEP_B200_ABI_VERSION 1
+#define SWEEP_B200_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define SWEEP_B200_API __attribute__((visibility("default")))
@@ -122,6 +122,58 @@ SWEEP_B200_API int sweep_b200_acoustic_backward(const sweep_acoustic_desc* d, in
  * cudaMalloc, cudaFree or other allocating routine. */
 SWEEP_B200_API int sweep_b200_acoustic_forward_noalloc(const sweep_acoustic_desc* d, float* record,
                                                        void* stream, char* err, int32_t err_cap);
+
+/* 2-D isotropic elastic problem (velocity-stress, staggered grid).  Replaces
+ * the geometry, model and source/receiver fields of the reference's
+ * ForwardInputCore for the elastic2d entries (reference
+ * src/sweep/backend/c/abi.py:108-166, elastic2d/driver_traits.cuh:110-150).
+ * Wavefield indices: 0 vx, 1 vz, 2 sxx, 3 szz, 4 sxz (reference
+ * src/sweep/csrc/cuda/common/elastic.h:715-725). */
+typedef struct sweep_elastic_desc {
+    int32_t B;               /* shots advanced together */
+    int32_t nz, nx;          /* runtime grid */
+    int32_t nt;              /* time steps */
+    int32_t M;               /* stencil half-width (spatial order / 2); 4 */
+    int32_t pad[4];          /* PML pad per face: z_lo, z_hi, x_lo, x_hi */
+    float dt, dz, dx;
+    const float *az, *bz, *azh, *bzh;   /* staggered CPML profiles (length nz): */
+    const float *ax, *bx, *axh, *bxh;   /* integer and half-cell positions (nx) */
+    const float *vp, *vs, *rho;  /* (B|1, nz, nx) models on the runtime grid */
+    int64_t model_stride;    /* 0: models shared by every shot; else nz * nx */
+    int32_t nsrc;            /* sources per shot */
+    const int32_t* src_loc;  /* (B, nsrc, 2) runtime (x, z) */
+    const float* wavelet;    /* (B, nsrc, nt) amplitude added to every source field */
+    int32_t nsrc_fields;     /* 1..3 */
+    int32_t src_fields[5];   /* wavefield indices the wavelet is added to */
+    int32_t nrec;            /* receivers per shot (padded to a rectangle) */
+    const int32_t* rec_loc;  /* (B, nrec, 2) */
+    int32_t nrec_fields;     /* 1..5 */
+    int32_t rec_fields[5];   /* wavefield indices recorded, in record order */
+} sweep_elastic_desc;
+
+/* Sizes of the elastic workspace and tape (as sweep_b200_acoustic_sizes). */
+SWEEP_B200_API int sweep_b200_elastic_sizes(const sweep_elastic_desc* d, int32_t mem_mode, int32_t ckpt_every,
+                                            int64_t* workspace_bytes, int64_t* tape_bytes,
+                                            char* err, int32_t err_cap);
+
+/* Elastic forward (reference entry 60: sg_driver.cuh:291-340).  record:
+ * (B, nt, nrec, nrec_fields) out.  tape: NULL (no backward to follow) or
+ * `tape_bytes` of device memory for the backward. */
+SWEEP_B200_API int sweep_b200_elastic_forward(const sweep_elastic_desc* d, int32_t mem_mode, int32_t ckpt_every,
+                                              float* record, void* tape,
+                                              void* workspace, int64_t workspace_bytes,
+                                              void* stream, char* err, int32_t err_cap);
+
+/* Elastic adjoint and vp / vs / rho gradients (reference entry 62:
+ * sg_driver.cuh:760-806).  adj: (B, nt, nrec, nrec_fields) record cotangent.
+ * grad_vp / grad_vs / grad_rho: (B|1, nz, nx), same stride rule as the
+ * models, OVERWRITTEN (zero outside the physical box).  The wavelet gradient
+ * is not produced, as in the reference (src/sweep/propagator/_c.py:2368-2374). */
+SWEEP_B200_API int sweep_b200_elastic_backward(const sweep_elastic_desc* d, int32_t mem_mode, int32_t ckpt_every,
+                                               const float* adj, const void* tape,
+                                               float* grad_vp, float* grad_vs, float* grad_rho,
+                                               void* workspace, int64_t workspace_bytes,
+                                               void* stream, char* err, int32_t err_cap);
 
 /* ABI version (SWEEP_B200_ABI_VERSION) -- checked by the Python loader, like
  * the reference's sweep_core_abi_version() (reference loader.py:92-138). */

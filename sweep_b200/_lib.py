@@ -17,7 +17,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIB_PATH = Path(os.environ.get("SWEEP_B200_LIB", HERE / "libsweep_b200.so"))
-ABI_VERSION = 1
+ABI_VERSION = 2
 ERR_CAP = 4096
 
 c_i32, c_i64, c_f32, c_p = ctypes.c_int32, ctypes.c_int64, ctypes.c_float, ctypes.c_void_p
@@ -29,6 +29,9 @@ SYMBOLS = (
     "sweep_b200_acoustic_forward",
     "sweep_b200_acoustic_backward",
     "sweep_b200_acoustic_forward_noalloc",
+    "sweep_b200_elastic_sizes",
+    "sweep_b200_elastic_forward",
+    "sweep_b200_elastic_backward",
 )
 
 MEM_BOUNDARY = 0
@@ -48,6 +51,22 @@ class AcousticDesc(ctypes.Structure):
         ("vp", c_p), ("vp_stride", c_i64),
         ("nsrc", c_i32), ("src_loc", c_p), ("wavelet", c_p),
         ("nrec", c_i32), ("rec_loc", c_p),
+    ]
+
+
+class ElasticDesc(ctypes.Structure):
+    """Mirror of ``sweep_elastic_desc``."""
+    _fields_ = [
+        ("B", c_i32), ("nz", c_i32), ("nx", c_i32), ("nt", c_i32), ("M", c_i32),
+        ("pad", c_i32 * 4),
+        ("dt", c_f32), ("dz", c_f32), ("dx", c_f32),
+        ("az", c_p), ("bz", c_p), ("azh", c_p), ("bzh", c_p),
+        ("ax", c_p), ("bx", c_p), ("axh", c_p), ("bxh", c_p),
+        ("vp", c_p), ("vs", c_p), ("rho", c_p), ("model_stride", c_i64),
+        ("nsrc", c_i32), ("src_loc", c_p), ("wavelet", c_p),
+        ("nsrc_fields", c_i32), ("src_fields", c_i32 * 5),
+        ("nrec", c_i32), ("rec_loc", c_p),
+        ("nrec_fields", c_i32), ("rec_fields", c_i32 * 5),
     ]
 
 
@@ -79,6 +98,13 @@ def load():
     lib.sweep_b200_acoustic_backward.argtypes = [P, c_i32, c_i32, c_p, c_p, c_p, c_p, c_p, c_p,
                                                  c_p, c_i64, c_p, ctypes.c_char_p, c_i32]
     lib.sweep_b200_acoustic_forward_noalloc.argtypes = [P, c_p, c_p, ctypes.c_char_p, c_i32]
+    E = ctypes.POINTER(ElasticDesc)
+    lib.sweep_b200_elastic_sizes.argtypes = [E, c_i32, c_i32, ctypes.POINTER(c_i64),
+                                             ctypes.POINTER(c_i64), ctypes.c_char_p, c_i32]
+    lib.sweep_b200_elastic_forward.argtypes = [E, c_i32, c_i32, c_p, c_p, c_p, c_i64, c_p,
+                                               ctypes.c_char_p, c_i32]
+    lib.sweep_b200_elastic_backward.argtypes = [E, c_i32, c_i32, c_p, c_p, c_p, c_p, c_p, c_p,
+                                                c_i64, c_p, ctypes.c_char_p, c_i32]
     for s in SYMBOLS[1:]:
         getattr(lib, s).restype = ctypes.c_int
     _lib = lib

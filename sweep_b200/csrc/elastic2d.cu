@@ -1,0 +1,1054 @@
+// elastic2d.cu -- 2-D isotropic elastic (velocity-stress, staggered grid)
+// forward and boundary-saving adjoint for sm_100a.
+//
+// Restates the reference's elastic2d path (src/sweep/csrc/cuda/equations/
+// elastic2d/, common/sg_driver.cuh) with a different kernel structure:
+//
+//   forward, per step (reference: velocity kernel, stress kernel, add_source
+//   per field, 5 boundary saves, record per field = 2 + 2 + 5 + 2 launches):
+//     fwd_vel   velocity update with its 4 CPML memories   kernels.cuh:48-138
+//     fwd_str   stress update with its 4 CPML memories     kernels.cuh:182-311
+//               + source injection, the 5-field boundary-strip save and the
+//               receiver gather of the same step, done by the CTA that owns
+//               the cell                                   sg_driver.cuh:291-340
+//   reverse, per step (reference: 8-13 launches, sg_driver.cuh:786-806):
+//     rev_str   stress reconstruction (NOPML) + strip restore, the residual
+//               injection, the vp/vs/rho imaging and the receiver rho fix,
+//               sharing the velocity derivatives between reconstruction and
+//               imaging                                    kernels.cuh:455-535,
+//                                                          601-663; common.cu:77-117
+//     rev_sadj  stress-adjoint apply; the four q fields (stress-adjoint
+//               prepare, kernels.cuh:548-750) are built in shared memory for
+//               the tile and its halo instead of a global round trip
+//     rev_vadj  velocity-adjoint apply with p built the same way
+//               (kernels.cuh:873-1019) + carrier capture, velocity
+//               reconstruction (NOPML) and strip restore  kernels.cuh:365-450,
+//                                                          driver_traits.cuh:758-826
+//
+// Building q / p in shared memory lets every CTA recompute them for its halo,
+// so the adjoint CPML memories are double-buffered (read the old set, write
+// the new one) and neighbouring CTAs never race on them.
+//
+// Layout: fields are pitched (B, nz, P), P = nx rounded up to 32 floats.
+// CPML memories live in per-axis slabs (x: (B, nz, WX), z: (B, WZ, P)) that
+// cover the PML band plus one cell (the half-cell profile reaches one cell
+// further inward on the high side; reference context.h:359-400 keeps wider
+// slabs for the same reason).  Tiles are 32 x 32 cells, 256 threads, 4 rows
+// per thread.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "common.cuh"
+#include "elastic2d.cuh"
+
+namespace sweep {
+namespace el2d {
+
+constexpr int M = 4;
+constexpr int TX = 32, TZ = 32, NTH = 256, RPT = TZ / 8;
+constexpr int HX = TX + 2 * M, HZ = TZ + 2 * M, HN = HX * HZ;
+
+// Staggered first-derivative weights of order 8 (reference
+// operators/staggered.cuh:351-354; scalars.py:25-49).
+#define C1 (1225.f / 1024.f)
+#define C2 (-245.f / 3072.f)
+#define C3 (49.f / 5120.f)
+#define C4 (-5.f / 7168.f)
+
+enum { VX = 0, VZ = 1, SXX = 2, SZZ = 3, SXZ = 4 };
+
+struct Geo {
+    int B, nz, nx, nt, P;
+    long long S;                    // pitched cells per shot
+    int z0, z1, x0, x1;             // physical box
+    int XL, XH, ZL, ZH;             // CPML band (pad + M) per face
+    int SXL, SXH, SZL, SZH;         // slab side widths (band + 1)
+    int WX, WZ;                     // slab widths
+    int ntx, ntz;
+    int bw, bh, nstrip;             // strip geometry
+    float dt, idx, idz;
+    const float *az, *bz, *azh, *bzh, *ax, *bx, *axh, *bxh;
+    int nsrc, nrec, nsf, nrf;
+    int sf[5], rf[5];
+    long long ms;                   // model stride between shots (0 or S)
+    EventTable src, rec;
+    const float* wavelet;           // (B, nsrc, nt)
+};
+
+// Models on the pitched grid, one copy (shared) or B copies (per shot).
+struct Models {
+    const float *rho, *lam, *mu, *bv, *vp, *vs;   // bv = dt * (1 / rho)
+};
+
+// Memory-variable slabs of one wavefield set: x slab m_x[k] (B, nz, WX) and
+// z slab m_z[k] (B, WZ, P).
+struct Slabs {
+    float* x[4];
+    float* z[4];
+};
+
+__device__ __forceinline__ int xslab(const Geo& G, int ix)
+{
+    return ix < G.SXL ? ix : (ix >= G.nx - G.SXH ? G.SXL + ix - (G.nx - G.SXH) : -1);
+}
+__device__ __forceinline__ int zslab(const Geo& G, int iz)
+{
+    return iz < G.SZL ? iz : (iz >= G.nz - G.SZH ? G.SZL + iz - (G.nz - G.SZH) : -1);
+}
+__device__ __forceinline__ bool in_pml(const Geo& G, int ix, int iz)
+{
+    return ix < G.XL || ix >= G.nx - G.XH || iz < G.ZL || iz >= G.nz - G.ZH;
+}
+__device__ __forceinline__ bool in_core(const Geo& G, int ix, int iz)
+{
+    return ix >= M && ix < G.nx - M && iz >= M && iz < G.nz - M;
+}
+// Reverse (NOPML) reconstruction region: the box minus one cell per face
+// (reference kernels.cuh:430-440, band abcn + M + 1).
+__device__ __forceinline__ bool in_recon(const Geo& G, int ix, int iz)
+{
+    return ix > G.x0 && ix < G.x1 - 1 && iz > G.z0 && iz < G.z1 - 1;
+}
+__device__ __forceinline__ bool in_box(const Geo& G, int ix, int iz)
+{
+    return ix >= G.x0 && ix < G.x1 && iz >= G.z0 && iz < G.z1;
+}
+
+// Index of (iz, ix) in the boundary-strip set, or -1.  The set is the union
+// of the reference's four bands, width M + 1 at offset -M around the physical
+// box (reference boundary/strip.cuh:81-114): M rows above and below the box
+// over its width, the box's first and last rows over the box width plus M
+// cells each side, and the M + 1 cells each side of the inner box rows.  Every
+// cell is stored once.
+__device__ __forceinline__ int strip_index(const Geo& G, int iz, int ix)
+{
+    constexpr int W = M + 1;
+    if (iz >= G.z0 - M && iz < G.z0) {
+        return (ix >= G.x0 && ix < G.x1) ? (iz - (G.z0 - M)) * G.bw + ix - G.x0 : -1;
+    }
+    if (iz >= G.z1 && iz < G.z1 + M) {
+        return (ix >= G.x0 && ix < G.x1) ? (M + iz - G.z1) * G.bw + ix - G.x0 : -1;
+    }
+    if (iz < G.z0 || iz >= G.z1 || ix < G.x0 - M || ix >= G.x1 + M) return -1;
+    const int row = G.bw + 2 * M, base = 2 * M * G.bw;
+    if (iz == G.z0) return base + ix - (G.x0 - M);
+    if (iz == G.z1 - 1) return base + row + ix - (G.x0 - M);
+    const int r = base + 2 * row + (iz - G.z0 - 1) * 2 * W;
+    if (ix <= G.x0) return r + ix - (G.x0 - M);
+    if (ix >= G.x1 - 1) return r + W + ix - (G.x1 - 1);
+    return -1;
+}
+
+// ---------------------------------------------------------------- stencils
+// D+ / D- on a shared tile (pitch HX) at flat index c (reference
+// operators/staggered.cuh:356-430, same term order).
+__device__ __forceinline__ float dpx(const float* t, int c, float inv)
+{
+    return (C1 * (t[c + 1] - t[c]) + C2 * (t[c + 2] - t[c - 1]) + C3 * (t[c + 3] - t[c - 2]) +
+            C4 * (t[c + 4] - t[c - 3])) * inv;
+}
+__device__ __forceinline__ float dmx(const float* t, int c, float inv)
+{
+    return (C1 * (t[c] - t[c - 1]) + C2 * (t[c + 1] - t[c - 2]) + C3 * (t[c + 2] - t[c - 3]) +
+            C4 * (t[c + 3] - t[c - 4])) * inv;
+}
+__device__ __forceinline__ float dpz(const float* t, int c, float inv)
+{
+    return (C1 * (t[c + HX] - t[c]) + C2 * (t[c + 2 * HX] - t[c - HX]) +
+            C3 * (t[c + 3 * HX] - t[c - 2 * HX]) + C4 * (t[c + 4 * HX] - t[c - 3 * HX])) * inv;
+}
+__device__ __forceinline__ float dmz(const float* t, int c, float inv)
+{
+    return (C1 * (t[c] - t[c - HX]) + C2 * (t[c + HX] - t[c - 2 * HX]) +
+            C3 * (t[c + 2 * HX] - t[c - 3 * HX]) + C4 * (t[c + 3 * HX] - t[c - 4 * HX])) * inv;
+}
+
+// Cooperative load of one field's tile plus an M-cell halo (zero outside the
+// grid) into shared memory.
+__device__ __forceinline__ void load_tile(float* t, const float* __restrict__ g, const Geo& G, int tz0, int tx0)
+{
+    for (int k = threadIdx.x + threadIdx.y * TX; k < HN; k += NTH) {
+        const int lz = k / HX, lx = k - lz * HX;
+        const int iz = tz0 - M + lz, ix = tx0 - M + lx;
+        float v = 0.f;
+        if ((unsigned)iz < (unsigned)G.nz && (unsigned)ix < (unsigned)G.nx) v = __ldg(g + (long long)iz * G.P + ix);
+        t[k] = v;
+    }
+}
+
+// Add w to the stress field `fld` (one of SXX, SZZ, SXZ) held in registers.
+__device__ __forceinline__ void add_to(int fld, float w, float& sxx, float& szz, float& sxz)
+{
+    if (fld == SXX) sxx += w;
+    else if (fld == SZZ) szz += w;
+    else sxz += w;
+}
+
+__device__ __forceinline__ void tile_origin(const Geo& G, int tile, int& tz0, int& tx0)
+{
+    tz0 = (tile / G.ntx) * TZ;
+    tx0 = (tile % G.ntx) * TX;
+}
+
+// ------------------------------------------------------------------ forward
+struct FwdArgs {
+    Geo G;
+    Models m;
+    float* f[5];          // vx, vz, sxx, szz, sxz
+    Slabs mem;            // forward memories: x {vxx, vzx, sxxx, sxzx}, z {vzz, vxz, szzz, sxzz}
+    float* strips;        // this step's strip slot (B, 5, nstrip) or null
+    float* record;        // (B, nt, nrec, nrf)
+    int it;
+};
+// memory slot names
+enum { XM_VXX = 0, XM_VZX = 1, XM_SXXX = 2, XM_SXZX = 3 };
+enum { ZM_VZZ = 0, ZM_VXZ = 1, ZM_SZZZ = 2, ZM_SXZZ = 3 };
+
+// Velocity step (reference kernels.cuh:48-138).
+__global__ void __launch_bounds__(NTH) fwd_vel(FwdArgs A)
+{
+    extern __shared__ float sm[];
+    float *tsxx = sm, *tszz = sm + HN, *tsxz = sm + 2 * HN;
+    const Geo& G = A.G;
+    const int b = blockIdx.y;
+    int tz0, tx0;
+    tile_origin(G, blockIdx.x, tz0, tx0);
+    const long long so = (long long)b * G.S;
+    load_tile(tsxx, A.f[SXX] + so, G, tz0, tx0);
+    load_tile(tszz, A.f[SZZ] + so, G, tz0, tx0);
+    load_tile(tsxz, A.f[SXZ] + so, G, tz0, tx0);
+    __syncthreads();
+    const int lx = threadIdx.x, ix = tx0 + lx;
+    const float* __restrict__ bv = A.m.bv + (long long)b * G.ms;
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+        const int lz = threadIdx.y + 8 * r, iz = tz0 + lz;
+        if (!in_core(G, ix, iz)) continue;
+        const int c = (lz + M) * HX + lx + M;
+        float dsxx_dx = dpx(tsxx, c, G.idx);
+        float dsxz_dz = dmz(tsxz, c, G.idz);
+        float dsxz_dx = dmx(tsxz, c, G.idx);
+        float dszz_dz = dpz(tszz, c, G.idz);
+        const long long i = (long long)iz * G.P + ix;
+        if (in_pml(G, ix, iz)) {
+            const int xs = xslab(G, ix), zs = zslab(G, iz);
+            if (zs >= 0) {
+                const long long zi = ((long long)b * G.WZ + zs) * G.P + ix;
+                float m = G.azh[iz] * A.mem.z[ZM_SZZZ][zi] + G.bzh[iz] * dszz_dz;
+                A.mem.z[ZM_SZZZ][zi] = m; dszz_dz += m;
+            }
+            if (xs >= 0) {
+                const long long xi = ((long long)b * G.nz + iz) * G.WX + xs;
+                float m = G.ax[ix] * A.mem.x[XM_SXZX][xi] + G.bx[ix] * dsxz_dx;
+                A.mem.x[XM_SXZX][xi] = m; dsxz_dx += m;
+            }
+            if (zs >= 0) {
+                const long long zi = ((long long)b * G.WZ + zs) * G.P + ix;
+                float m = G.az[iz] * A.mem.z[ZM_SXZZ][zi] + G.bz[iz] * dsxz_dz;
+                A.mem.z[ZM_SXZZ][zi] = m; dsxz_dz += m;
+            }
+            if (xs >= 0) {
+                const long long xi = ((long long)b * G.nz + iz) * G.WX + xs;
+                float m = G.axh[ix] * A.mem.x[XM_SXXX][xi] + G.bxh[ix] * dsxx_dx;
+                A.mem.x[XM_SXXX][xi] = m; dsxx_dx += m;
+            }
+        }
+        const float k = bv[i];
+        A.f[VX][so + i] += k * (dsxx_dx + dsxz_dz);
+        A.f[VZ][so + i] += k * (dsxz_dx + dszz_dz);
+    }
+}
+
+// Stress step (reference kernels.cuh:182-311, no free surface), then the
+// step's point work for the cells this CTA owns: source injection into the
+// stress source fields, the 5-field strip save and the receiver gather
+// (reference sg_driver.cuh:300-340 order: inject, save, record).
+__global__ void __launch_bounds__(NTH) fwd_str(FwdArgs A)
+{
+    extern __shared__ float sm[];
+    float *tvx = sm, *tvz = sm + HN;
+    const Geo& G = A.G;
+    const int b = blockIdx.y, tile = blockIdx.x;
+    int tz0, tx0;
+    tile_origin(G, tile, tz0, tx0);
+    const long long so = (long long)b * G.S;
+    load_tile(tvx, A.f[VX] + so, G, tz0, tx0);
+    load_tile(tvz, A.f[VZ] + so, G, tz0, tx0);
+    const int key = b * G.ntx * G.ntz + tile;
+    const int s0 = G.src.off[key], s1 = G.src.off[key + 1];
+    __syncthreads();
+    const int lx = threadIdx.x, ix = tx0 + lx;
+    const float* __restrict__ lam_ = A.m.lam + (long long)b * G.ms;
+    const float* __restrict__ mu_ = A.m.mu + (long long)b * G.ms;
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+        const int lz = threadIdx.y + 8 * r, iz = tz0 + lz;
+        if (iz >= G.nz || ix >= G.nx) continue;
+        const int c = (lz + M) * HX + lx + M;
+        const long long i = (long long)iz * G.P + ix;
+        float sxx = A.f[SXX][so + i], szz = A.f[SZZ][so + i], sxz = A.f[SXZ][so + i];
+        if (in_core(G, ix, iz)) {
+            float dvx_dx = dmx(tvx, c, G.idx);
+            float dvz_dz = dmz(tvz, c, G.idz);
+            float dvx_dz = dpz(tvx, c, G.idz);
+            float dvz_dx = dpx(tvz, c, G.idx);
+            const float lam = lam_[i], mu = mu_[i];
+            const bool pml = in_pml(G, ix, iz);
+            const int xs = pml ? xslab(G, ix) : -1, zs = pml ? zslab(G, iz) : -1;
+            const long long zi = ((long long)b * G.WZ + zs) * G.P + ix;
+            const long long xi = ((long long)b * G.nz + iz) * G.WX + xs;
+            if (zs >= 0) {
+                float m = G.az[iz] * A.mem.z[ZM_VZZ][zi] + G.bz[iz] * dvz_dz;
+                A.mem.z[ZM_VZZ][zi] = m; dvz_dz += m;
+            }
+            if (xs >= 0) {
+                float m = G.ax[ix] * A.mem.x[XM_VXX][xi] + G.bx[ix] * dvx_dx;
+                A.mem.x[XM_VXX][xi] = m; dvx_dx += m;
+            }
+            sxx += G.dt * ((lam + 2.f * mu) * dvx_dx + lam * dvz_dz);
+            szz += G.dt * ((lam + 2.f * mu) * dvz_dz + lam * dvx_dx);
+            if (zs >= 0) {
+                float m = G.azh[iz] * A.mem.z[ZM_VXZ][zi] + G.bzh[iz] * dvx_dz;
+                A.mem.z[ZM_VXZ][zi] = m; dvx_dz += m;
+            }
+            if (xs >= 0) {
+                float m = G.axh[ix] * A.mem.x[XM_VZX][xi] + G.bxh[ix] * dvz_dx;
+                A.mem.x[XM_VZX][xi] = m; dvz_dx += m;
+            }
+            sxz += G.dt * mu * (dvx_dz + dvz_dx);
+        }
+        // point sources of this cell (usually none in the tile)
+        const int cell = lz * TX + lx;
+        for (int e = s0; e < s1; ++e) {
+            const int2 ev = G.src.ev[e];
+            if (ev.x != cell) continue;
+            const float w = G.wavelet[(long long)ev.y * G.nt + A.it];
+            for (int k = 0; k < G.nsf; ++k) add_to(G.sf[k], w, sxx, szz, sxz);
+        }
+        A.f[SXX][so + i] = sxx;
+        A.f[SZZ][so + i] = szz;
+        A.f[SXZ][so + i] = sxz;
+        if (A.strips) {
+            const int si = strip_index(G, iz, ix);
+            if (si >= 0) {
+                float* st = A.strips + (long long)b * 5 * G.nstrip + si;
+                st[0] = tvx[c];
+                st[G.nstrip] = tvz[c];
+                st[2 * G.nstrip] = sxx;
+                st[3 * G.nstrip] = szz;
+                st[4 * G.nstrip] = sxz;
+            }
+        }
+    }
+    // receivers of this tile: read back the final values of the step
+    const int r0 = G.rec.off[key], r1 = G.rec.off[key + 1];
+    if (r1 > r0) {
+        __syncthreads();
+        for (int e = r0 + threadIdx.x + threadIdx.y * TX; e < r1; e += NTH) {
+            const int2 ev = G.rec.ev[e];
+            const int iz = tz0 + ev.x / TX, ix = tx0 + ev.x % TX;
+            const long long i = so + (long long)iz * G.P + ix;
+            float* out = A.record + ((long long)(b * G.nt + A.it) * G.nrec + (ev.y - b * G.nrec)) * G.nrf;
+            for (int k = 0; k < G.nrf; ++k) out[k] = A.f[G.rf[k]][i];
+        }
+    }
+}
+
+// ------------------------------------------------------------------ reverse
+struct RevArgs {
+    Geo G;
+    Models m;
+    float* f[5];          // reconstructed forward fields
+    float* cvx;           // carriers: v of the next step (box cells)
+    float* cvz;
+    float* a[5];          // adjoint fields (stress ones hold the negated adjoint)
+    Slabs mo, mn;         // adjoint memories: read set (old), write set (new)
+    const float* strips;  // saved strips of step it - 1, (B, 5, nstrip)
+    const float* adj;     // (B, nt, nrec, nrf) residuals
+    float* gvp;           // gradient slots (nslot, S)
+    float* gvs;
+    float* grho;
+    int G_shots;          // shots per CTA of rev_str (shared models)
+    int it;
+};
+// adjoint memory slots: x {vxx, vzx, sxxx, sxzx}, z {vzz, vxz, szzz, sxzz}
+
+// Reverse stress half for shots [g*G_shots, ...): residual injection
+// (reference inject_residuals, signs: stress -1, velocity +1), stress
+// reconstruction on the NOPML region with the forward source removed
+// (kernels.cuh:455-493 after uninject_forward_source) or strip restore, the
+// fused vp / vs / rho imaging on the physical box (kernels.cuh:601-663) and
+// the receiver rho correction (common.cu:77-117).  The gradient contributions
+// of the CTA's shots are summed in registers and added to slot blockIdx.y.
+__global__ void __launch_bounds__(NTH) rev_str(RevArgs A)
+{
+    extern __shared__ float sm[];
+    float *tvx = sm, *tvz = sm + HN;
+    const Geo& G = A.G;
+    const int tile = blockIdx.x, grp = blockIdx.y;
+    int tz0, tx0;
+    tile_origin(G, tile, tz0, tx0);
+    const int lx = threadIdx.x, ix = tx0 + lx;
+    const int b_lo = grp * A.G_shots, b_hi = min(G.B, b_lo + A.G_shots);
+    float gvp[RPT], gvs[RPT], grho[RPT];
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) gvp[r] = gvs[r] = grho[r] = 0.f;
+    const int tid = threadIdx.x + threadIdx.y * TX;
+
+    for (int b = b_lo; b < b_hi; ++b) {
+        const long long so = (long long)b * G.S;
+        const int key = b * G.ntx * G.ntz + tile;
+        const int r0 = G.rec.off[key], r1 = G.rec.off[key + 1];
+        const int s0 = G.src.off[key], s1 = G.src.off[key + 1];
+        __syncthreads();                       // previous shot's tiles consumed
+        load_tile(tvx, A.f[VX] + so, G, tz0, tx0);
+        load_tile(tvz, A.f[VZ] + so, G, tz0, tx0);
+        // residuals of step it into the adjoint fields of this tile's receivers
+        for (int e = r0 + tid; e < r1; e += NTH) {
+            const int2 ev = G.rec.ev[e];
+            const long long i = so + (long long)(tz0 + ev.x / TX) * G.P + tx0 + ev.x % TX;
+            const float* res = A.adj + ((long long)(b * G.nt + A.it) * G.nrec + (ev.y - b * G.nrec)) * G.nrf;
+            for (int k = 0; k < G.nrf; ++k) {
+                const int fld = G.rf[k];
+                atomicAdd(A.a[fld] + i, fld >= SXX ? -res[k] : res[k]);
+            }
+        }
+        __syncthreads();
+        const float* __restrict__ lam_ = A.m.lam + (long long)b * G.ms;
+        const float* __restrict__ mu_ = A.m.mu + (long long)b * G.ms;
+        const float* __restrict__ rho_ = A.m.rho + (long long)b * G.ms;
+        const float* __restrict__ vp_ = A.m.vp + (long long)b * G.ms;
+        const float* __restrict__ vs_ = A.m.vs + (long long)b * G.ms;
+        const float* st = A.strips + (long long)b * 5 * G.nstrip;
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            const int lz = threadIdx.y + 8 * r, iz = tz0 + lz;
+            if (iz >= G.nz || ix >= G.nx) continue;
+            const long long i = (long long)iz * G.P + ix;
+            if (!in_core(G, ix, iz)) {
+                const int si = strip_index(G, iz, ix);
+                if (si >= 0) {
+                    A.f[SXX][so + i] = st[2 * G.nstrip + si];
+                    A.f[SZZ][so + i] = st[3 * G.nstrip + si];
+                    A.f[SXZ][so + i] = st[4 * G.nstrip + si];
+                }
+                continue;
+            }
+            const int c = (lz + M) * HX + lx + M;
+            const float dvx_dx = dmx(tvx, c, G.idx);
+            const float dvz_dz = dmz(tvz, c, G.idz);
+            const float dvx_dz = dpz(tvx, c, G.idz);
+            const float dvz_dx = dpx(tvz, c, G.idx);
+            if (in_recon(G, ix, iz)) {
+                float sxx = A.f[SXX][so + i], szz = A.f[SZZ][so + i], sxz = A.f[SXZ][so + i];
+                const int cell = lz * TX + lx;
+                for (int e = s0; e < s1; ++e) {
+                    const int2 ev = G.src.ev[e];
+                    if (ev.x != cell) continue;
+                    const float w = G.wavelet[(long long)ev.y * G.nt + A.it];
+                    for (int k = 0; k < G.nsf; ++k) add_to(G.sf[k], -w, sxx, szz, sxz);
+                }
+                const float lam = lam_[i], mu = mu_[i];
+                A.f[SXX][so + i] = sxx - G.dt * ((lam + 2.f * mu) * dvx_dx + lam * dvz_dz);
+                A.f[SZZ][so + i] = szz - G.dt * ((lam + 2.f * mu) * dvz_dz + lam * dvx_dx);
+                A.f[SXZ][so + i] = sxz - G.dt * mu * (dvx_dz + dvz_dx);
+            } else {
+                const int si = strip_index(G, iz, ix);
+                if (si >= 0) {
+                    A.f[SXX][so + i] = st[2 * G.nstrip + si];
+                    A.f[SZZ][so + i] = st[3 * G.nstrip + si];
+                    A.f[SXZ][so + i] = st[4 * G.nstrip + si];
+                }
+            }
+            if (in_box(G, ix, iz)) {
+                const float bsxx = A.a[SXX][so + i], bszz = A.a[SZZ][so + i], bsxz = A.a[SXZ][so + i];
+                float gl = (bsxx + bszz) * (dvx_dx + dvz_dz);
+                float gm = 2.f * (bsxx * dvx_dx + bszz * dvz_dz);
+                gm += bsxz * (dvx_dz + dvz_dx);
+                const float rho = rho_[i], vp = vp_[i], vs = vs_[i];
+                gvp[r] += -2.f * rho * vp * gl * G.dt;
+                gvs[r] += -(-4.f * rho * vs * gl + 2.f * rho * vs * gm) * G.dt;
+                float gr = (A.a[VX][so + i] * (tvx[c] - A.cvx[so + i]) + A.a[VZ][so + i] * (tvz[c] - A.cvz[so + i])) / rho;
+                gr -= gl * (vp * vp - 2.f * vs * vs) * G.dt + gm * (vs * vs) * G.dt;
+                grho[r] += gr;
+            }
+        }
+    }
+    // add the group's image to its slot
+    const long long slot = (long long)grp * G.S;
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+        const int iz = tz0 + threadIdx.y + 8 * r;
+        if (!in_box(G, ix, iz)) continue;
+        const long long i = slot + (long long)iz * G.P + ix;
+        A.gvp[i] += gvp[r];
+        A.gvs[i] += gvs[r];
+        A.grho[i] += grho[r];
+    }
+    // receiver rho correction after the image (velocity receivers in the box)
+    bool any = false;
+    for (int b = b_lo; b < b_hi; ++b) {
+        const int key = b * G.ntx * G.ntz + tile;
+        any |= G.rec.off[key + 1] > G.rec.off[key];
+    }
+    if (!any) return;
+    __syncthreads();
+    for (int b = b_lo; b < b_hi; ++b) {
+        const long long so = (long long)b * G.S;
+        const int key = b * G.ntx * G.ntz + tile;
+        const float* __restrict__ rho_ = A.m.rho + (long long)b * G.ms;
+        for (int e = G.rec.off[key] + tid; e < G.rec.off[key + 1]; e += NTH) {
+            const int2 ev = G.rec.ev[e];
+            const int iz = tz0 + ev.x / TX, jx = tx0 + ev.x % TX;
+            if (!in_box(G, jx, iz)) continue;
+            const long long i = (long long)iz * G.P + jx;
+            const float* res = A.adj + ((long long)(b * G.nt + A.it) * G.nrec + (ev.y - b * G.nrec)) * G.nrf;
+            for (int k = 0; k < G.nrf; ++k) {
+                const int fld = G.rf[k];
+                if (fld > VZ) continue;
+                const float now = A.f[fld][so + i];
+                const float nxt = (fld == VX ? A.cvx : A.cvz)[so + i];
+                atomicAdd(A.grho + slot + i, -res[k] * (now - nxt) / rho_[i]);
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ bool owns(int lz, int lx)
+{
+    return lz >= M && lz < M + TZ && lx >= M && lx < M + TX;
+}
+
+// Stress-adjoint apply (reference kernels.cuh:807-837) with q = (qxx, qzz,
+// qxz, qzx) of the stress-adjoint prepare (kernels.cuh:676-750) built in
+// shared memory for the tile and its halo.  The owner of a cell writes its new
+// adjoint CPML memories.
+__global__ void __launch_bounds__(NTH) rev_sadj(RevArgs A)
+{
+    extern __shared__ float sm[];
+    float* tq[4] = {sm, sm + HN, sm + 2 * HN, sm + 3 * HN};
+    const Geo& G = A.G;
+    const int b = blockIdx.y;
+    int tz0, tx0;
+    tile_origin(G, blockIdx.x, tz0, tx0);
+    const long long so = (long long)b * G.S;
+    const float* __restrict__ lam_ = A.m.lam + (long long)b * G.ms;
+    const float* __restrict__ mu_ = A.m.mu + (long long)b * G.ms;
+    for (int k = threadIdx.x + threadIdx.y * TX; k < HN; k += NTH) {
+        const int lz = k / HX, lx = k - lz * HX;
+        const int iz = tz0 - M + lz, ix = tx0 - M + lx;
+        float q0 = 0.f, q1 = 0.f, q2 = 0.f, q3 = 0.f;
+        if ((unsigned)iz < (unsigned)G.nz && (unsigned)ix < (unsigned)G.nx) {
+            const long long i = (long long)iz * G.P + ix;
+            const float bsxx = A.a[SXX][so + i], bszz = A.a[SZZ][so + i], bsxz = A.a[SXZ][so + i];
+            const float lam = lam_[i], mu = mu_[i];
+            q0 = G.dt * ((lam + 2.f * mu) * bsxx + lam * bszz);
+            q1 = G.dt * ((lam + 2.f * mu) * bszz + lam * bsxx);
+            q2 = G.dt * mu * bsxz;
+            q3 = G.dt * mu * bsxz;
+            if (in_pml(G, ix, iz)) {
+                const bool own = owns(lz, lx);
+                const int xs = xslab(G, ix), zs = zslab(G, iz);
+                if (xs >= 0) {
+                    const long long xi = ((long long)b * G.nz + iz) * G.WX + xs;
+                    const float t0 = A.mo.x[XM_VXX][xi] + q0, t3 = A.mo.x[XM_VZX][xi] + q3;
+                    if (own) {
+                        A.mn.x[XM_VXX][xi] = G.ax[ix] * t0;
+                        A.mn.x[XM_VZX][xi] = G.axh[ix] * t3;
+                    }
+                    q0 = q0 + G.bx[ix] * t0;
+                    q3 = q3 + G.bxh[ix] * t3;
+                }
+                if (zs >= 0) {
+                    const long long zi = ((long long)b * G.WZ + zs) * G.P + ix;
+                    const float t1 = A.mo.z[ZM_VZZ][zi] + q1, t2 = A.mo.z[ZM_VXZ][zi] + q2;
+                    if (own) {
+                        A.mn.z[ZM_VZZ][zi] = G.az[iz] * t1;
+                        A.mn.z[ZM_VXZ][zi] = G.azh[iz] * t2;
+                    }
+                    q1 = q1 + G.bz[iz] * t1;
+                    q2 = q2 + G.bzh[iz] * t2;
+                }
+            }
+        }
+        tq[0][k] = q0; tq[1][k] = q1; tq[2][k] = q2; tq[3][k] = q3;
+    }
+    __syncthreads();
+    const int lx = threadIdx.x, ix = tx0 + lx;
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+        const int lz = threadIdx.y + 8 * r, iz = tz0 + lz;
+        if (!in_core(G, ix, iz)) continue;
+        const int c = (lz + M) * HX + lx + M;
+        const long long i = so + (long long)iz * G.P + ix;
+        A.a[VX][i] += dpx(tq[0], c, G.idx) + dmz(tq[2], c, G.idz);
+        A.a[VZ][i] += dmx(tq[3], c, G.idx) + dpz(tq[1], c, G.idz);
+    }
+}
+
+// Velocity-adjoint apply (reference kernels.cuh:989-1019) with p = (pxx,
+// pzz, pxz, pzx) of the velocity-adjoint prepare (kernels.cuh:873-958) built
+// in shared memory, then the reverse velocity half of the forward
+// reconstruction: carrier capture of v(it) on the box, the NOPML velocity
+// step (kernels.cuh:365-401) and the velocity strip restore of step it - 1.
+__global__ void __launch_bounds__(NTH) rev_vadj(RevArgs A)
+{
+    extern __shared__ float sm[];
+    float* tp[4] = {sm, sm + HN, sm + 2 * HN, sm + 3 * HN};
+    float *tsxx = sm + 4 * HN, *tszz = sm + 5 * HN, *tsxz = sm + 6 * HN;
+    const Geo& G = A.G;
+    const int b = blockIdx.y;
+    int tz0, tx0;
+    tile_origin(G, blockIdx.x, tz0, tx0);
+    const long long so = (long long)b * G.S;
+    const float* __restrict__ bv_ = A.m.bv + (long long)b * G.ms;
+    for (int k = threadIdx.x + threadIdx.y * TX; k < HN; k += NTH) {
+        const int lz = k / HX, lx = k - lz * HX;
+        const int iz = tz0 - M + lz, ix = tx0 - M + lx;
+        float p0 = 0.f, p1 = 0.f, p2 = 0.f, p3 = 0.f;
+        if ((unsigned)iz < (unsigned)G.nz && (unsigned)ix < (unsigned)G.nx) {
+            const long long i = (long long)iz * G.P + ix;
+            const float k_ = bv_[i];
+            const float avx = A.a[VX][so + i], avz = A.a[VZ][so + i];
+            p0 = k_ * avx;      // pxx
+            p2 = k_ * avx;      // pxz
+            p3 = k_ * avz;      // pzx
+            p1 = k_ * avz;      // pzz
+            if (in_pml(G, ix, iz)) {
+                const bool own = owns(lz, lx);
+                const int xs = xslab(G, ix), zs = zslab(G, iz);
+                if (xs >= 0) {
+                    const long long xi = ((long long)b * G.nz + iz) * G.WX + xs;
+                    const float t0 = A.mo.x[XM_SXXX][xi] + p0, t3 = A.mo.x[XM_SXZX][xi] + p3;
+                    if (own) {
+                        A.mn.x[XM_SXXX][xi] = G.axh[ix] * t0;
+                        A.mn.x[XM_SXZX][xi] = G.ax[ix] * t3;
+                    }
+                    p0 = p0 + G.bxh[ix] * t0;
+                    p3 = p3 + G.bx[ix] * t3;
+                }
+                if (zs >= 0) {
+                    const long long zi = ((long long)b * G.WZ + zs) * G.P + ix;
+                    const float t2 = A.mo.z[ZM_SXZZ][zi] + p2, t1 = A.mo.z[ZM_SZZZ][zi] + p1;
+                    if (own) {
+                        A.mn.z[ZM_SXZZ][zi] = G.az[iz] * t2;
+                        A.mn.z[ZM_SZZZ][zi] = G.azh[iz] * t1;
+                    }
+                    p2 = p2 + G.bz[iz] * t2;
+                    p1 = p1 + G.bzh[iz] * t1;
+                }
+            }
+        }
+        tp[0][k] = p0; tp[1][k] = p1; tp[2][k] = p2; tp[3][k] = p3;
+    }
+    load_tile(tsxx, A.f[SXX] + so, G, tz0, tx0);
+    load_tile(tszz, A.f[SZZ] + so, G, tz0, tx0);
+    load_tile(tsxz, A.f[SXZ] + so, G, tz0, tx0);
+    __syncthreads();
+    const int lx = threadIdx.x, ix = tx0 + lx;
+    const float* st = A.strips + (long long)b * 5 * G.nstrip;
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+        const int lz = threadIdx.y + 8 * r, iz = tz0 + lz;
+        if (!in_core(G, ix, iz)) continue;
+        const int c = (lz + M) * HX + lx + M;
+        const long long i = (long long)iz * G.P + ix;
+        A.a[SXX][so + i] += dmx(tp[0], c, G.idx);
+        A.a[SZZ][so + i] += dmz(tp[1], c, G.idz);
+        A.a[SXZ][so + i] += dpz(tp[2], c, G.idz) + dpx(tp[3], c, G.idx);
+        if (!in_box(G, ix, iz)) continue;
+        const float vx = A.f[VX][so + i], vz = A.f[VZ][so + i];
+        A.cvx[so + i] = vx;
+        A.cvz[so + i] = vz;
+        if (in_recon(G, ix, iz)) {
+            const float k_ = bv_[i];
+            A.f[VX][so + i] = vx - k_ * (dpx(tsxx, c, G.idx) + dmz(tsxz, c, G.idz));
+            A.f[VZ][so + i] = vz - k_ * (dmx(tsxz, c, G.idx) + dpz(tszz, c, G.idz));
+        }
+    }
+    // strips (box ring and the M cells outside it) of step it - 1
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+        const int lz = threadIdx.y + 8 * r, iz = tz0 + lz;
+        if (iz >= G.nz || ix >= G.nx || in_recon(G, ix, iz)) continue;
+        const int si = strip_index(G, iz, ix);
+        if (si < 0) continue;
+        const long long i = so + (long long)iz * G.P + ix;
+        A.f[VX][i] = st[si];
+        A.f[VZ][i] = st[G.nstrip + si];
+    }
+}
+
+// Models onto the pitched grid: rho, Lame parameters (reference
+// derived_models.cu:27-37, same rounding), bv = dt * (1 / rho) (the velocity
+// kernels' dt * inv_rho, kernels.cuh:73, 389, 901), vp and vs for the imaging.
+__global__ void prep_kernel(const float* __restrict__ vp, const float* __restrict__ vs,
+                            const float* __restrict__ rho, int nm, int nz, int nx, int P, float dt,
+                            float* orho, float* olam, float* omu, float* obv, float* ovp, float* ovs)
+{
+    const long long n = (long long)nm * nz * nx;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        const long long b = k / ((long long)nz * nx), rem = k - b * nz * nx;
+        const int iz = (int)(rem / nx), ix = (int)(rem - (long long)iz * nx);
+        const long long o = (b * nz + iz) * P + ix;
+        const float v = vp[k], s = vs[k], r = rho[k];
+        orho[o] = r;
+        omu[o] = __fmul_rn(__fmul_rn(r, s), s);
+        olam[o] = __fmul_rn(r, __fsub_rn(__fmul_rn(v, v), __fmul_rn(__fmul_rn(2.0f, s), s)));
+        obv[o] = dt * (1.f / r);
+        ovp[o] = v;
+        ovs[o] = s;
+    }
+}
+
+// Gradient output: sum of the slots in slot order on the physical box, zero
+// elsewhere, unpitched (nout, nz, nx); slot s of a per-shot model is shot s.
+__global__ void finalize_kernel(const float* __restrict__ slots, int nslot, int per_shot, Geo G, float* out)
+{
+    const int nout = per_shot ? nslot : 1;
+    const long long n = (long long)nout * G.nz * G.nx;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        const long long b = k / ((long long)G.nz * G.nx), rem = k - b * G.nz * G.nx;
+        const int iz = (int)(rem / G.nx), ix = (int)(rem - (long long)iz * G.nx);
+        float v = 0.f;
+        if (in_box(G, ix, iz)) {
+            const long long o = (long long)iz * G.P + ix;
+            if (per_shot) {
+                v = slots[b * G.S + o];
+            } else {
+                for (int s = 0; s < nslot; ++s) v += slots[s * G.S + o];
+            }
+        }
+        out[k] = v;
+    }
+}
+
+// ------------------------------------------------------------------- host
+struct Plan {
+    Geo G;
+    int nm;          // model copies
+    int gshots;      // shots per rev_str CTA
+    int nslot;       // gradient slots
+};
+
+static int env_int(const char* name, int dflt)
+{
+    if (const char* e = getenv(name)) {
+        const int v = atoi(e);
+        if (v >= 1) return v;
+    }
+    return dflt;
+}
+
+static Plan make_plan(const sweep_elastic_desc* d)
+{
+    SWEEP_REQUIRE(d != nullptr, "null descriptor");
+    SWEEP_REQUIRE(d->M == M, "elastic2d: only spatial order 8 (M = 4) is built (got M = %d)", d->M);
+    SWEEP_REQUIRE(d->B >= 1 && d->nt >= 1, "elastic2d: B and nt must be >= 1");
+    SWEEP_REQUIRE(d->nsrc >= 0 && d->nrec >= 0, "elastic2d: negative source/receiver count");
+    SWEEP_REQUIRE(d->nsrc_fields >= 1 && d->nsrc_fields <= 3, "elastic2d: 1 to 3 source fields (got %d)", d->nsrc_fields);
+    for (int k = 0; k < d->nsrc_fields; ++k)
+        SWEEP_REQUIRE(d->src_fields[k] >= SXX && d->src_fields[k] <= SXZ,
+                      "elastic2d: source field %d is not built (stress fields sxx, szz, sxz only)", d->src_fields[k]);
+    SWEEP_REQUIRE(d->nrec_fields >= 1 && d->nrec_fields <= 5, "elastic2d: 1 to 5 receiver fields (got %d)", d->nrec_fields);
+    for (int k = 0; k < d->nrec_fields; ++k)
+        SWEEP_REQUIRE(d->rec_fields[k] >= 0 && d->rec_fields[k] <= SXZ, "elastic2d: bad receiver field %d", d->rec_fields[k]);
+    for (int f = 0; f < 4; ++f)
+        SWEEP_REQUIRE(d->pad[f] >= 1, "elastic2d: every face needs a PML pad >= 1 (face %d has %d)", f, d->pad[f]);
+    Plan pl{};
+    Geo& G = pl.G;
+    G.B = d->B; G.nz = d->nz; G.nx = d->nx; G.nt = d->nt;
+    G.P = (d->nx + 31) / 32 * 32;
+    G.S = (long long)d->nz * G.P;
+    SWEEP_REQUIRE(G.S < (1LL << 31), "elastic2d: one shot's grid must hold < 2^31 cells");
+    G.z0 = d->pad[0] + M; G.z1 = d->nz - d->pad[1] - M;
+    G.x0 = d->pad[2] + M; G.x1 = d->nx - d->pad[3] - M;
+    G.bw = G.x1 - G.x0; G.bh = G.z1 - G.z0;
+    SWEEP_REQUIRE(G.bw >= 2 && G.bh >= 2, "elastic2d: the physical box must be at least 2 x 2 cells");
+    G.ZL = d->pad[0] + M; G.ZH = d->pad[1] + M; G.XL = d->pad[2] + M; G.XH = d->pad[3] + M;
+    G.SZL = std::min(G.ZL + 1, d->nz); G.SZH = std::min(G.ZH + 1, d->nz - G.SZL);
+    G.SXL = std::min(G.XL + 1, d->nx); G.SXH = std::min(G.XH + 1, d->nx - G.SXL);
+    G.WX = G.SXL + G.SXH; G.WZ = G.SZL + G.SZH;
+    G.ntx = (d->nx + TX - 1) / TX; G.ntz = (d->nz + TZ - 1) / TZ;
+    G.nstrip = 2 * M * G.bw + 2 * (G.bw + 2 * M) + (G.bh - 2) * 2 * (M + 1);
+    G.dt = d->dt; G.idx = 1.f / d->dx; G.idz = 1.f / d->dz;
+    G.az = d->az; G.bz = d->bz; G.azh = d->azh; G.bzh = d->bzh;
+    G.ax = d->ax; G.bx = d->bx; G.axh = d->axh; G.bxh = d->bxh;
+    G.nsrc = d->nsrc; G.nrec = d->nrec; G.nsf = d->nsrc_fields; G.nrf = d->nrec_fields;
+    for (int k = 0; k < 5; ++k) { G.sf[k] = d->src_fields[k]; G.rf[k] = d->rec_fields[k]; }
+    const bool per_shot = d->model_stride != 0;
+    SWEEP_REQUIRE(!per_shot || d->model_stride == (int64_t)d->nz * d->nx,
+                  "elastic2d: model_stride must be 0 or nz * nx");
+    G.ms = per_shot ? G.S : 0;
+    G.wavelet = d->wavelet;
+    pl.nm = per_shot ? d->B : 1;
+    pl.gshots = per_shot ? 1 : std::min(env_int("SWEEP_B200_EL_SHOTS_PER_CTA", 4), d->B);
+    pl.nslot = (d->B + pl.gshots - 1) / pl.gshots;
+    return pl;
+}
+
+struct Common {
+    float *rho, *lam, *mu, *bv, *vp, *vs;
+    int32_t *src_off, *rec_off;
+    int2 *src_ev, *rec_ev;
+};
+
+static void carve_common(Carve& c, const Plan& pl, Common& w)
+{
+    const Geo& G = pl.G;
+    const long long mc = (long long)pl.nm * G.S;
+    w.rho = c.take<float>(mc); w.lam = c.take<float>(mc); w.mu = c.take<float>(mc);
+    w.bv = c.take<float>(mc); w.vp = c.take<float>(mc); w.vs = c.take<float>(mc);
+    const long long nkey = (long long)G.B * G.ntx * G.ntz + 1;
+    w.src_off = c.take<int32_t>(nkey);
+    w.rec_off = c.take<int32_t>(nkey);
+    w.src_ev = c.take<int2>((long long)G.B * G.nsrc + 1);
+    w.rec_ev = c.take<int2>((long long)G.B * G.nrec + 1);
+}
+
+static void carve_slabs(Carve& c, const Geo& G, Slabs& s)
+{
+    for (int k = 0; k < 4; ++k) s.x[k] = c.take<float>((long long)G.B * G.nz * G.WX);
+    for (int k = 0; k < 4; ++k) s.z[k] = c.take<float>((long long)G.B * G.WZ * G.P);
+}
+
+struct FwdWs {
+    Common cm;
+    float* f[5];
+    Slabs mem;
+    char* zero0;          // [zero0, zero1) cleared before the time loop
+    char* zero1;
+};
+
+static void carve_fwd(Carve& c, const Plan& pl, FwdWs& w)
+{
+    carve_common(c, pl, w.cm);
+    c.take<char>(0);
+    w.zero0 = c.base ? c.base + c.off : nullptr;
+    for (int k = 0; k < 5; ++k) w.f[k] = c.take<float>((long long)pl.G.B * pl.G.S);
+    carve_slabs(c, pl.G, w.mem);
+    c.take<char>(0);
+    w.zero1 = c.base ? c.base + c.off : nullptr;
+}
+
+struct RevWs {
+    Common cm;
+    float* f[5];
+    float *cvx, *cvz;
+    float* a[5];
+    Slabs m[2];
+    float *gvp, *gvs, *grho;
+    char* zero0;
+    char* zero1;
+};
+
+static void carve_rev(Carve& c, const Plan& pl, RevWs& w)
+{
+    carve_common(c, pl, w.cm);
+    const Geo& G = pl.G;
+    for (int k = 0; k < 5; ++k) w.f[k] = c.take<float>((long long)G.B * G.S);
+    c.take<char>(0);
+    w.zero0 = c.base ? c.base + c.off : nullptr;
+    w.cvx = c.take<float>((long long)G.B * G.S);
+    w.cvz = c.take<float>((long long)G.B * G.S);
+    for (int k = 0; k < 5; ++k) w.a[k] = c.take<float>((long long)G.B * G.S);
+    carve_slabs(c, G, w.m[0]);
+    carve_slabs(c, G, w.m[1]);
+    w.gvp = c.take<float>((long long)pl.nslot * G.S);
+    w.gvs = c.take<float>((long long)pl.nslot * G.S);
+    w.grho = c.take<float>((long long)pl.nslot * G.S);
+    c.take<char>(0);
+    w.zero1 = c.base ? c.base + c.off : nullptr;
+}
+
+// tape: strips of every step (nt, B, 5, nstrip), then the final 5-field state
+// (5, B, nz, P)
+static int64_t tape_bytes(const Plan& pl)
+{
+    Carve c(nullptr);
+    c.take<float>((long long)pl.G.nt * pl.G.B * 5 * pl.G.nstrip);
+    c.take<float>(5LL * pl.G.B * pl.G.S);
+    return c.off;
+}
+
+static float* tape_last(void* tape, const Plan& pl)
+{
+    Carve c(tape);
+    c.take<float>((long long)pl.G.nt * pl.G.B * 5 * pl.G.nstrip);
+    return c.take<float>(5LL * pl.G.B * pl.G.S);
+}
+
+// CSR of the point events of (shot, tile), like the 2-D acoustic path: the
+// tile-local cell and the global event id b * n + s.  Every in-grid cell
+// counts (the reference skips only off-grid coordinates, common.cu:24-28).
+static int build_events(const Geo& G, const int32_t* loc, int n, int32_t* off, int2* ev, std::vector<int32_t>& fill)
+{
+    const int ntiles = G.ntx * G.ntz, nkey = G.B * ntiles;
+    for (int i = 0; i <= nkey; ++i) off[i] = 0;
+    auto key_of = [&](int e) -> int {
+        const int ix = loc[2 * e], iz = loc[2 * e + 1];
+        if (ix < 0 || ix >= G.nx || iz < 0 || iz >= G.nz) return -1;
+        return (e / n) * ntiles + (iz / TZ) * G.ntx + ix / TX;
+    };
+    for (int e = 0; e < G.B * n; ++e) {
+        const int k = key_of(e);
+        if (k >= 0) off[k + 1]++;
+    }
+    for (int i = 1; i <= nkey; ++i) off[i] += off[i - 1];
+    fill.assign(off, off + nkey);
+    for (int e = 0; e < G.B * n; ++e) {
+        const int k = key_of(e);
+        if (k < 0) continue;
+        const int ix = loc[2 * e], iz = loc[2 * e + 1];
+        ev[fill[k]++] = make_int2((iz % TZ) * TX + ix % TX, e);
+    }
+    return off[nkey];
+}
+
+static void setup_common(const sweep_elastic_desc* d, Plan& pl, const Common& w, cudaStream_t st)
+{
+    Geo& G = pl.G;
+    SWEEP_REQUIRE(d->vp && d->vs && d->rho, "elastic2d: null model pointer");
+    prep_kernel<<<592, 256, 0, st>>>(d->vp, d->vs, d->rho, pl.nm, d->nz, d->nx, G.P, d->dt,
+                                     w.rho, w.lam, w.mu, w.bv, w.vp, w.vs);
+    SWEEP_LAUNCH_CHECK();
+    std::vector<int32_t> ls((size_t)d->B * d->nsrc * 2 + 1), lr((size_t)d->B * d->nrec * 2 + 1);
+    const size_t ns = (size_t)d->B * d->nsrc * 2, nr = (size_t)d->B * d->nrec * 2;
+    if (ns) SWEEP_CUDA(cudaMemcpyAsync(ls.data(), d->src_loc, ns * 4, cudaMemcpyDeviceToHost, st));
+    if (nr) SWEEP_CUDA(cudaMemcpyAsync(lr.data(), d->rec_loc, nr * 4, cudaMemcpyDeviceToHost, st));
+    SWEEP_CUDA(cudaStreamSynchronize(st));
+    const size_t nkey = (size_t)G.B * G.ntx * G.ntz + 1;
+    std::vector<int32_t> os(nkey), orr(nkey), fill;
+    std::vector<int2> es((size_t)d->B * d->nsrc + 1), er((size_t)d->B * d->nrec + 1);
+    const int nsev = build_events(G, ls.data(), d->nsrc, os.data(), es.data(), fill);
+    const int nrev = build_events(G, lr.data(), d->nrec, orr.data(), er.data(), fill);
+    SWEEP_CUDA(cudaMemcpyAsync(w.src_off, os.data(), nkey * 4, cudaMemcpyHostToDevice, st));
+    SWEEP_CUDA(cudaMemcpyAsync(w.rec_off, orr.data(), nkey * 4, cudaMemcpyHostToDevice, st));
+    if (nsev) SWEEP_CUDA(cudaMemcpyAsync(w.src_ev, es.data(), nsev * sizeof(int2), cudaMemcpyHostToDevice, st));
+    if (nrev) SWEEP_CUDA(cudaMemcpyAsync(w.rec_ev, er.data(), nrev * sizeof(int2), cudaMemcpyHostToDevice, st));
+    SWEEP_CUDA(cudaStreamSynchronize(st));   // host staging released on return
+    G.src.off = w.src_off; G.src.ev = w.src_ev;
+    G.rec.off = w.rec_off; G.rec.ev = w.rec_ev;
+}
+
+static Models models_of(const Common& w)
+{
+    return Models{w.rho, w.lam, w.mu, w.bv, w.vp, w.vs};
+}
+
+constexpr size_t SM_FWD_VEL = 3 * HN * sizeof(float);
+constexpr size_t SM_FWD_STR = 2 * HN * sizeof(float);
+constexpr size_t SM_REV_STR = 2 * HN * sizeof(float);
+constexpr size_t SM_REV_SADJ = 4 * HN * sizeof(float);
+constexpr size_t SM_REV_VADJ = 7 * HN * sizeof(float);
+
+void sizes(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, int64_t* ws, int64_t* tape)
+{
+    SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY, "elastic2d: only boundary saving is built");
+    (void)ckpt_every;
+    Plan pl = make_plan(d);
+    Carve cf(nullptr);
+    FwdWs fw{};
+    carve_fwd(cf, pl, fw);
+    Carve cr(nullptr);
+    RevWs rw{};
+    carve_rev(cr, pl, rw);
+    *ws = std::max(cf.off, cr.off);
+    *tape = tape_bytes(pl);
+}
+
+void forward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, float* record, void* tape,
+             void* ws, int64_t ws_bytes, cudaStream_t st)
+{
+    SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY, "elastic2d: only boundary saving is built");
+    (void)ckpt_every;
+    SWEEP_REQUIRE(record != nullptr || d->nrec == 0, "elastic2d forward: null record");
+    Plan pl = make_plan(d);
+    Carve c(ws);
+    FwdWs w{};
+    carve_fwd(c, pl, w);
+    SWEEP_REQUIRE(ws != nullptr && c.off <= ws_bytes, "elastic2d forward: workspace too small (%lld < %lld bytes)",
+                  (long long)ws_bytes, (long long)c.off);
+    SWEEP_CUDA(cudaMemsetAsync(w.zero0, 0, w.zero1 - w.zero0, st));
+    if (record && d->nrec)
+        SWEEP_CUDA(cudaMemsetAsync(record, 0, sizeof(float) * (size_t)d->B * d->nt * d->nrec * d->nrec_fields, st));
+    setup_common(d, pl, w.cm, st);
+    FwdArgs A{};
+    A.G = pl.G;
+    A.m = models_of(w.cm);
+    for (int k = 0; k < 5; ++k) A.f[k] = w.f[k];
+    A.mem = w.mem;
+    A.record = record;
+    const Geo& G = pl.G;
+    const dim3 grid(G.ntx * G.ntz, G.B), block(TX, 8);
+    float* strips = static_cast<float*>(tape);
+    for (int it = 0; it < G.nt; ++it) {
+        A.it = it;
+        A.strips = strips ? strips + (long long)it * G.B * 5 * G.nstrip : nullptr;
+        fwd_vel<<<grid, block, SM_FWD_VEL, st>>>(A);
+        fwd_str<<<grid, block, SM_FWD_STR, st>>>(A);
+    }
+    SWEEP_LAUNCH_CHECK();
+    if (tape) {
+        float* last = tape_last(tape, pl);
+        for (int k = 0; k < 5; ++k)
+            SWEEP_CUDA(cudaMemcpyAsync(last + (long long)k * G.B * G.S, w.f[k], sizeof(float) * G.B * G.S,
+                                       cudaMemcpyDeviceToDevice, st));
+    }
+}
+
+void backward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, const float* adj, const void* tape,
+              float* grad_vp, float* grad_vs, float* grad_rho, void* ws, int64_t ws_bytes, cudaStream_t st)
+{
+    SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY, "elastic2d: only boundary saving is built");
+    (void)ckpt_every;
+    SWEEP_REQUIRE(tape != nullptr, "elastic2d backward: null tape");
+    SWEEP_REQUIRE(grad_vp && grad_vs && grad_rho, "elastic2d backward: null gradient output");
+    SWEEP_REQUIRE(adj != nullptr || d->nrec == 0, "elastic2d backward: null adjoint source");
+    Plan pl = make_plan(d);
+    Carve c(ws);
+    RevWs w{};
+    carve_rev(c, pl, w);
+    SWEEP_REQUIRE(ws != nullptr && c.off <= ws_bytes, "elastic2d backward: workspace too small (%lld < %lld bytes)",
+                  (long long)ws_bytes, (long long)c.off);
+    SWEEP_CUDA(cudaMemsetAsync(w.zero0, 0, w.zero1 - w.zero0, st));
+    setup_common(d, pl, w.cm, st);
+    const Geo& G = pl.G;
+    const float* last = tape_last(const_cast<void*>(tape), pl);
+    for (int k = 0; k < 5; ++k)
+        SWEEP_CUDA(cudaMemcpyAsync(w.f[k], last + (long long)k * G.B * G.S, sizeof(float) * G.B * G.S,
+                                   cudaMemcpyDeviceToDevice, st));
+    RevArgs A{};
+    A.G = G;
+    A.m = models_of(w.cm);
+    for (int k = 0; k < 5; ++k) { A.f[k] = w.f[k]; A.a[k] = w.a[k]; }
+    A.cvx = w.cvx; A.cvz = w.cvz;
+    A.adj = adj;
+    A.gvp = w.gvp; A.gvs = w.gvs; A.grho = w.grho;
+    A.G_shots = pl.gshots;
+    const dim3 block(TX, 8);
+    const dim3 grid_s(G.ntx * G.ntz, pl.nslot), grid_b(G.ntx * G.ntz, G.B);
+    const float* strips = static_cast<const float*>(tape);
+    int cur = 0;
+    for (int it = G.nt - 1; it >= 1; --it) {
+        A.it = it;
+        A.strips = strips + (long long)(it - 1) * G.B * 5 * G.nstrip;
+        A.mo = w.m[cur];
+        A.mn = w.m[cur ^ 1];
+        rev_str<<<grid_s, block, SM_REV_STR, st>>>(A);
+        rev_sadj<<<grid_b, block, SM_REV_SADJ, st>>>(A);
+        rev_vadj<<<grid_b, block, SM_REV_VADJ, st>>>(A);
+        cur ^= 1;
+    }
+    SWEEP_LAUNCH_CHECK();
+    const int per_shot = G.ms != 0;
+    finalize_kernel<<<592, 256, 0, st>>>(w.gvp, pl.nslot, per_shot, G, grad_vp);
+    finalize_kernel<<<592, 256, 0, st>>>(w.gvs, pl.nslot, per_shot, G, grad_vs);
+    finalize_kernel<<<592, 256, 0, st>>>(w.grho, pl.nslot, per_shot, G, grad_rho);
+    SWEEP_LAUNCH_CHECK();
+}
+
+}  // namespace el2d
+}  // namespace sweep

@@ -137,6 +137,37 @@ class _Geometry:
         return d
 
 
+    def elastic_desc(self, models, wavelet, src_fields, rec_fields):
+        vp, vs, rho = models
+        d = _lib.ElasticDesc()
+        d.B = self.B
+        d.nz, d.nx = self.shape
+        d.nt = self.nt
+        d.M = self.M
+        for i in range(4):
+            d.pad[i] = self.pad
+        d.dt = self.dt
+        d.dz, d.dx = self.spacing
+        (az, bz, azh, bzh), (ax, bx, axh, bxh) = self.prof
+        for name, t in (("az", az), ("bz", bz), ("azh", azh), ("bzh", bzh),
+                        ("ax", ax), ("bx", bx), ("axh", axh), ("bxh", bxh)):
+            setattr(d, name, t.data_ptr())
+        d.vp, d.vs, d.rho = vp.data_ptr(), vs.data_ptr(), rho.data_ptr()
+        d.model_stride = int(np.prod(self.shape)) if vp.dim() == 3 else 0
+        d.nsrc = self.nsrc
+        d.src_loc = self.src.data_ptr()
+        d.wavelet = wavelet.data_ptr()
+        d.nsrc_fields = len(src_fields)
+        for k, f in enumerate(src_fields):
+            d.src_fields[k] = f
+        d.nrec = self.nrec
+        d.rec_loc = self.rec.data_ptr()
+        d.nrec_fields = len(rec_fields)
+        for k, f in enumerate(rec_fields):
+            d.rec_fields[k] = f
+        return d
+
+
 def _stream_ptr(device):
     return torch.cuda.current_stream(device).cuda_stream
 
@@ -190,6 +221,54 @@ class _AcousticFn(torch.autograd.Function):
         if illum:
             prop._set_illumination(i_s, i_r)
         return grad_vp, grad_w, None, None, None, None
+
+
+class _ElasticFn(torch.autograd.Function):
+    """vp, vs, rho (runtime grid, shared or per shot, all alike) and the
+    wavelet ``(B, nsrc, nt)`` -> record ``(B, nt, nrec, nfield)``.  The
+    backward returns the three model gradients; the wavelet gradient is not
+    produced (refused up front, as the reference's impl='c' does)."""
+
+    @staticmethod
+    def forward(ctx, vp, vs, rho, wavelet, prop, geo, fields, mem_mode, ckpt_every):
+        models = [m.contiguous() for m in (vp, vs, rho)]
+        wavelet = wavelet.contiguous()
+        sf, rf = fields
+        desc = geo.elastic_desc(models, wavelet, sf, rf)
+        ws_b, tape_b = _lib.c_i64(), _lib.c_i64()
+        _lib.call("sweep_b200_elastic_sizes", desc, mem_mode, ckpt_every, ws_b, tape_b)
+        need_bwd = any(ctx.needs_input_grad[:3])
+        dev = vp.device
+        ws = prop._workspace(ws_b.value, dev)
+        tape = torch.empty(tape_b.value, dtype=torch.uint8, device=dev) if need_bwd else None
+        record = torch.empty((geo.B, geo.nt, geo.nrec, len(rf)), dtype=torch.float32, device=dev)
+        _lib.call("sweep_b200_elastic_forward", desc, mem_mode, ckpt_every, record.data_ptr(),
+                  tape.data_ptr() if tape is not None else None, ws.data_ptr(), ws.numel(),
+                  _stream_ptr(dev))
+        ctx.save_for_backward(*models, wavelet)
+        ctx.tape = tape
+        ctx.geo, ctx.prop, ctx.fields = geo, prop, fields
+        ctx.mem_mode, ctx.ckpt_every = mem_mode, ckpt_every
+        return record
+
+    @staticmethod
+    def backward(ctx, grad_record):
+        if ctx.tape is None:
+            raise RuntimeError("sweep_b200: this forward has already been back-propagated (or ran "
+                               "without gradients); a second backward is refused")
+        vp, vs, rho, wavelet = ctx.saved_tensors
+        geo, prop = ctx.geo, ctx.prop
+        adj = grad_record.to(torch.float32).contiguous()
+        desc = geo.elastic_desc([vp, vs, rho], wavelet, *ctx.fields)
+        ws_b, tape_b = _lib.c_i64(), _lib.c_i64()
+        _lib.call("sweep_b200_elastic_sizes", desc, ctx.mem_mode, ctx.ckpt_every, ws_b, tape_b)
+        ws = prop._workspace(ws_b.value, vp.device)
+        g = [torch.empty_like(vp) for _ in range(3)]
+        _lib.call("sweep_b200_elastic_backward", desc, ctx.mem_mode, ctx.ckpt_every, adj.data_ptr(),
+                  ctx.tape.data_ptr(), g[0].data_ptr(), g[1].data_ptr(), g[2].data_ptr(),
+                  ws.data_ptr(), ws.numel(), _stream_ptr(vp.device))
+        ctx.tape = None
+        return g[0], g[1], g[2], None, None, None, None, None, None
 
 
 class PropTorch(torch.nn.Module):
@@ -266,6 +345,21 @@ class PropTorch(torch.nn.Module):
         x = F.pad(x[:, None] if nd == 2 else x[:, None], [p, p] * nd, mode="replicate")[:, 0]
         return x if per_shot else x[0]
 
+    def _elastic_fields(self):
+        """Source / receiver field indices (reference ``_c.py:1163-1176``)."""
+        names = list(self.equation.FIELDS)
+        for role, kinds in (("source_type", self.source_type), ("receiver_type", self.receiver_type)):
+            missing = [k for k in kinds if k not in names]
+            if not kinds or missing:
+                raise ValueError(f"Invalid {role} entries {missing or kinds}; available wavefields are {names}")
+        sf = [names.index(k) for k in self.source_type]
+        if any(f < 2 for f in sf):
+            raise NotImplementedError("sweep_b200: velocity (body-force) sources are not built; "
+                                      "use stress source fields (sxx, szz, sxz)")
+        if len(set(sf)) != len(sf) or len(self.receiver_type) > 5:
+            raise ValueError("source_type / receiver_type must not repeat a field")
+        return sf, [names.index(k) for k in self.receiver_type]
+
     def _mem_mode(self):
         if isinstance(self.memory, Ckpt):
             return _lib.MEM_CHECKPOINT, int(self.memory.chunks)
@@ -310,4 +404,13 @@ class PropTorch(torch.nn.Module):
         padded = [self._pad_model(m.to(dev)) for m in models]
         if isinstance(eq, (Acoustic, Acoustic3D)):
             return _AcousticFn.apply(padded[0], wb, self, geo, mem_mode, ckpt_every)
-        raise NotImplementedError(f"{type(eq).__name__} is not built yet")
+        if isinstance(eq, Elastic):
+            if len({m.dim() for m in models}) != 1:
+                raise ValueError("vp, vs and rho must all be shared (nz, nx) or all per shot (B, nz, nx)")
+            if wavelet.requires_grad and torch.is_grad_enabled():
+                raise NotImplementedError(
+                    "impl='c' Elastic does not return the wavelet gradient (its compiled backward "
+                    "returns the model gradients only). Detach the wavelet.")
+            fields = self._elastic_fields()
+            return _ElasticFn.apply(*padded, wb, self, geo, fields, mem_mode, ckpt_every)
+        raise NotImplementedError(f"{type(eq).__name__} is not built")

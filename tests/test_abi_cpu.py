@@ -77,3 +77,35 @@ def test_propagator_refuses_cpu_and_other_impls():
     vp = torch.full((20, 20), 2000.0)
     with pytest.raises(RuntimeError, match="CUDA"):
         p(np.zeros(10, np.float32), np.array([[5, 5]]), np.array([[[6, 6]]]), models=[vp])
+
+
+def _edesc(B=2, nz=40, nx=60, nt=10, nsrc=1, nrec=3, M=4):
+    from sweep_b200 import _lib
+    d = _lib.ElasticDesc()
+    d.B, d.nz, d.nx, d.nt, d.M = B, nz, nx, nt, M
+    for i in range(4):
+        d.pad[i] = 5
+    d.dt, d.dz, d.dx = 1e-3, 10.0, 10.0
+    d.nsrc, d.nrec = nsrc, nrec
+    d.nsrc_fields, d.nrec_fields = 2, 2
+    d.src_fields[0], d.src_fields[1] = 2, 3
+    d.rec_fields[0], d.rec_fields[1] = 0, 1
+    return d
+
+
+def test_elastic_sizes_and_errors():
+    from sweep_b200 import _lib
+    d = _edesc()
+    ws, tape = _lib.c_i64(), _lib.c_i64()
+    _lib.call("sweep_b200_elastic_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
+    n = 2 * 40 * 64                                  # pitched to 64 columns
+    assert ws.value >= 17 * n * 4                    # 5 forward + 2 carriers + 5 adjoint + 3 x 2 gradient slots
+    pz, px = 40 - 18, 60 - 18
+    nstrip = 2 * 4 * px + 2 * (px + 8) + (pz - 2) * 10
+    assert tape.value >= (10 * 2 * 5 * nstrip + 5 * n) * 4
+    d.src_fields[0] = 1
+    with pytest.raises(RuntimeError, match="not built"):
+        _lib.call("sweep_b200_elastic_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
+    d = _edesc(M=2)
+    with pytest.raises(RuntimeError, match="order 8"):
+        _lib.call("sweep_b200_elastic_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
