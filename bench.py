@@ -1,5 +1,6 @@
 """Benchmark of the FD hot path: one step = one full-waveform gradient
-(forward + adjoint) of a 32-shot 2-D acoustic survey.
+(forward + adjoint) of a 32-shot 2-D acoustic survey (default), or with
+``--workload elastic2d`` of a 16-shot 2-D elastic survey (vp / vs / rho).
 
 Workload (synthetic, seeded): 256 x 768 grid (nz x nx), dh 12.5 m, dt 1 ms,
 nt 3000, order 8, CPML 40 cells; a 12-layer model with sinusoidally perturbed
@@ -88,6 +89,38 @@ def cell_steps(nshot=NSHOT, nt=None):
     return RT[0] * RT[1] * nshot * (NT if nt is None else nt)
 
 
+# Elastic workload (--workload elastic2d): 400 x 1200, dh 5 m, dt 0.5 ms,
+# nt 4000, order 8, CPML 40; vp layered 1800-4500 m/s, vs = vp / 1.73,
+# rho = 310 vp^0.25; 16 explosive shots (10 Hz Ricker), 600 two-component
+# receivers per shot at z = 3.
+E_NZ, E_NX, E_NT, E_DT, E_DH, E_ABCN = 400, 1200, 4000, 0.0005, 5.0, 40
+E_NSHOT, E_NREC, E_F0, E_DELAY = 16, 600, 10.0, 0.12
+E_RT = (E_NZ + 2 * E_ABCN + 2 * M, E_NX + 2 * E_ABCN + 2 * M)
+# algorithmic bytes per runtime cell-step: forward velocity 7 floats + stress
+# 8; reverse stress half 15, stress-adjoint 7, velocity-adjoint + velocity
+# reconstruction 17 (one read and one write of every field a kernel touches;
+# CPML memories and the shared, L2-resident models not counted)
+E_BYTES_FWD, E_BYTES_REV = 60, 156
+
+
+def elastic_survey(seed=SEED):
+    from scipy.ndimage import gaussian_filter
+    from sweep_b200 import ricker
+    rng = np.random.default_rng(seed + 3)
+    vp_true = layered_model(E_NZ, E_NX, E_DH, rng, nlayers=12, vmin=1800.0, vmax=4500.0)
+    vp_init = gaussian_filter(vp_true.astype(np.float64), 8.0).astype(np.float32)
+    models = []
+    for vp in (vp_true, vp_init):
+        models.append([vp, (vp / 1.73).astype(np.float32), (310.0 * vp ** 0.25).astype(np.float32)])
+    sx = np.sort(rng.choice(np.arange(10, E_NX - 10), E_NSHOT, replace=False))
+    src = np.stack([sx, np.full(E_NSHOT, 3)], -1)
+    rec = np.zeros((E_NSHOT, E_NREC, 2), np.int64)
+    rec[:, :, 0] = np.linspace(0, E_NX - 1, E_NREC).astype(np.int64)[None]
+    rec[:, :, 1] = 3
+    w = ricker(np.arange(E_NT) * E_DT - E_DELAY, E_F0).astype(np.float32)
+    return models[0], models[1], w, src, rec
+
+
 # ------------------------------------------------------------------- clocks
 class ClockSampler:
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -144,19 +177,164 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-# -------------------------------------------------------------- CPU baseline
-def cpu_oracle_run(nt_sample, shots=1):
-    """Gradient of `shots` shots of the workload with the CPU oracle (float32,
-    OpenMP over all host threads); returns (cell-steps, seconds)."""
-    from oracle import oracle as O
-    vp_true, vp_init, w, src, rec = survey()
-    w = w[:nt_sample]
-    src, rec = src[:shots], rec[:shots]
-    obs = O.acoustic_forward(vp_true, w, src, rec, DH, DT, ABCN)
-    t0 = time.perf_counter()
-    O.acoustic_gradient(vp_init, w, src, rec, obs, DH, DT, ABCN)
-    dt = time.perf_counter() - t0
-    return cell_steps(shots, nt_sample), dt
+# --------------------------------------------------------------- workloads
+class AcousticWorkload:
+    name = "acoustic2d"
+    nt, nshot, rt = NT, NSHOT, RT
+    bytes_fwd, bytes_rev = BYTES_FWD, BYTES_REV
+    kernel = "sweep::a2d::rev_kernel (fused adjoint + reconstruction + imaging step)"
+    cpu_nt = 1000
+
+    def config(self, args):
+        return {"workload": f"acoustic2d {NZ}x{NX} (runtime {RT[0]}x{RT[1]}), {NSHOT} shots, nt {NT}, "
+                            f"order 8, CPML {ABCN}, fwd+adj gradient, boundary saving",
+                "grid": [NZ, NX], "runtime_grid": list(RT), "shots_per_gpu": NSHOT, "nt": NT,
+                "dh": DH, "dt": DT, "abcn": ABCN, "order": ORDER, "seed": SEED,
+                "cells_counted": "runtime grid (physical + PML + halo) x shots x nt",
+                "physical_fraction": NZ * NX / (RT[0] * RT[1]),
+                "l2": "working set per step > L2 (inputs larger than L2; no flush)",
+                "parallelism": f"shots: {NSHOT} per GPU x {args.gpus} GPU(s)"}
+
+    def build(self, dev):
+        from sweep_b200 import Acoustic, PropTorch
+        vp_true, vp_init, w, src, rec = survey()
+        solver = PropTorch(Acoustic(spatial_order=ORDER, device=dev), shape=(NZ, NX), dh=DH, dt=DT,
+                           abcn=ABCN, device=dev)
+        return solver, [vp_true], [vp_init], w, src, rec
+
+    def launches(self):
+        return 2 * self.nt + 1
+
+    def cpu_run(self, nt_sample, shots=1):
+        """Gradient of `shots` shots with the CPU oracle (float32, OpenMP over
+        all host threads); returns (cell-steps, seconds)."""
+        from oracle import oracle as O
+        vp_true, vp_init, w, src, rec = survey()
+        w, src, rec = w[:nt_sample], src[:shots], rec[:shots]
+        obs = O.acoustic_forward(vp_true, w, src, rec, DH, DT, ABCN)
+        t0 = time.perf_counter()
+        O.acoustic_gradient(vp_init, w, src, rec, obs, DH, DT, ABCN)
+        return RT[0] * RT[1] * shots * nt_sample, time.perf_counter() - t0
+
+
+class ElasticWorkload:
+    name = "elastic2d"
+    nt, nshot, rt = E_NT, E_NSHOT, E_RT
+    bytes_fwd, bytes_rev = E_BYTES_FWD, E_BYTES_REV
+    kernel = ("sweep::el2d reverse step (rev_str + rev_sadj + rev_vadj: reconstruction, imaging, "
+              "stress- and velocity-adjoint)")
+    cpu_nt = 300
+
+    def config(self, args):
+        return {"workload": f"elastic2d {E_NZ}x{E_NX} (runtime {E_RT[0]}x{E_RT[1]}), {E_NSHOT} shots, "
+                            f"nt {E_NT}, order 8, CPML {E_ABCN}, vp/vs/rho fwd+adj gradient, boundary saving",
+                "grid": [E_NZ, E_NX], "runtime_grid": list(E_RT), "shots_per_gpu": E_NSHOT, "nt": E_NT,
+                "dh": E_DH, "dt": E_DT, "abcn": E_ABCN, "order": ORDER, "receivers": E_NREC,
+                "seed": SEED, "cells_counted": "runtime grid (physical + PML + halo) x shots x nt",
+                "physical_fraction": E_NZ * E_NX / (E_RT[0] * E_RT[1]),
+                "l2": "working set per step > L2 (inputs larger than L2; no flush)",
+                "parallelism": f"shots: {E_NSHOT} per GPU x {args.gpus} GPU(s)"}
+
+    def build(self, dev):
+        from sweep_b200 import Elastic, PropTorch
+        m_true, m_init, w, src, rec = elastic_survey()
+        solver = PropTorch(Elastic(spatial_order=ORDER, device=dev), shape=(E_NZ, E_NX), dh=E_DH,
+                           dt=E_DT, abcn=E_ABCN, device=dev)
+        return solver, m_true, m_init, w, src, rec
+
+    def launches(self):
+        return 5 * self.nt + 2
+
+    def cpu_run(self, nt_sample, shots=1):
+        from oracle import oracle as O
+        m_true, m_init, w, src, rec = elastic_survey()
+        w, src, rec = w[:nt_sample], src[:shots], rec[:shots]
+        obs = O.elastic_forward(*m_true, w, src, rec, E_DH, E_DT, E_ABCN)
+        t0 = time.perf_counter()
+        O.elastic_gradient(*m_init, w, src, rec, obs, E_DH, E_DT, E_ABCN)
+        return E_RT[0] * E_RT[1] * shots * nt_sample, time.perf_counter() - t0
+
+
+# 3-D workload (--workload acoustic3d): 256^3, dh 10 m, dt 1 ms, nt 2000,
+# order 8, CPML 24; 8-layer dipping model (1500-4000 m/s) with a +600 m/s
+# Gaussian anomaly; 16 shots on a 4 x 4 surface grid, a 128 x 128 receiver
+# array at 2-cell spacing, 10 Hz Ricker.  The 16 shots run as 4 calls of 4
+# shots: the boundary-saving tape of one call (4 shots x 2000 steps of
+# strips) is ~63 GB.
+A3_N, A3_NT, A3_DT, A3_DH, A3_ABCN = 256, 2000, 0.001, 10.0, 24
+A3_NSHOT, A3_BATCH, A3_F0, A3_DELAY = 16, 4, 10.0, 0.12
+A3_RT = (A3_N + 2 * A3_ABCN + 2 * M,) * 3
+
+
+def acoustic3d_survey(seed=SEED):
+    from scipy.ndimage import gaussian_filter
+    from sweep_b200 import ricker
+    rng = np.random.default_rng(seed + 7)
+    n = A3_N
+    z, y, x = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    depth = np.sort(rng.uniform(0.08 * n, 0.92 * n, 7))
+    vel = np.linspace(1500.0, 4000.0, 8)
+    idx = np.zeros((n, n, n), np.int32)
+    for d0 in depth:
+        strike = rng.uniform(0, 2 * np.pi)
+        dip = np.deg2rad(rng.uniform(0, 15))
+        surf = d0 + np.tan(dip) * ((x - n / 2) * np.cos(strike) + (y - n / 2) * np.sin(strike))
+        idx += (z > surf).astype(np.int32)
+    vp = vel[idx]
+    cz, cy, cx = rng.uniform(0.3 * n, 0.7 * n), rng.uniform(0.3 * n, 0.7 * n), rng.uniform(0.3 * n, 0.7 * n)
+    vp += 600.0 * np.exp(-((z - cz) ** 2 + (y - cy) ** 2 + (x - cx) ** 2) / (2 * 30.0 ** 2))
+    vp_true = vp.astype(np.float32)
+    vp_init = gaussian_filter(vp_true.astype(np.float64), 8.0).astype(np.float32)
+    g = np.linspace(n / 8, n - n / 8, 4).astype(np.int64)
+    src = np.array([[xs, ys, 2] for ys in g for xs in g], np.int64)
+    r = np.arange(0, 2 * 128, 2)
+    rx, ry = np.meshgrid(r, r, indexing="xy")
+    one = np.stack([rx.ravel(), ry.ravel(), np.full(rx.size, 2)], -1)
+    rec = np.broadcast_to(one, (A3_NSHOT,) + one.shape).copy()
+    w = ricker(np.arange(A3_NT) * A3_DT - A3_DELAY, A3_F0).astype(np.float32)
+    return [vp_true], [vp_init], w, src, rec
+
+
+class Acoustic3DWorkload:
+    name = "acoustic3d"
+    nt, nshot, rt = A3_NT, A3_NSHOT, A3_RT
+    bytes_fwd, bytes_rev = BYTES_FWD, BYTES_REV
+    kernel = "sweep::a3d reverse step (a3_step + r3_recon + strip kernels)"
+    cpu_nt = 20
+    batch = A3_BATCH
+
+    def config(self, args):
+        return {"workload": f"acoustic3d {A3_N}^3 (runtime {A3_RT[0]}^3), {A3_NSHOT} shots in calls of "
+                            f"{A3_BATCH}, nt {self.nt}, order 8, CPML {A3_ABCN}, fwd+adj gradient, boundary saving",
+                "grid": [A3_N] * 3, "runtime_grid": list(A3_RT), "shots_per_gpu": A3_NSHOT,
+                "shots_per_call": A3_BATCH, "nt": self.nt, "dh": A3_DH, "dt": A3_DT, "abcn": A3_ABCN,
+                "order": ORDER, "receivers": 128 * 128, "seed": SEED,
+                "cells_counted": "runtime grid (physical + PML + halo) x shots x nt",
+                "physical_fraction": (A3_N / A3_RT[0]) ** 3,
+                "l2": "working set per step > L2 (inputs larger than L2; no flush)",
+                "parallelism": f"shots: {A3_NSHOT} per GPU x {args.gpus} GPU(s)"}
+
+    def build(self, dev):
+        from sweep_b200 import Acoustic3D, PropTorch
+        m_true, m_init, w, src, rec = acoustic3d_survey()
+        solver = PropTorch(Acoustic3D(spatial_order=ORDER, device=dev), shape=(A3_N,) * 3, dh=A3_DH,
+                           dt=A3_DT, abcn=A3_ABCN, device=dev)
+        return solver, m_true, m_init, w, src, rec
+
+    def launches(self):
+        return (A3_NSHOT // A3_BATCH) * 7 * self.nt
+
+    def cpu_run(self, nt_sample, shots=1):
+        from oracle import oracle as O
+        m_true, m_init, w, src, rec = acoustic3d_survey()
+        w, src, rec = w[:nt_sample], src[:shots], rec[:shots]
+        obs = O.acoustic_forward(m_true[0], w, src, rec, A3_DH, A3_DT, A3_ABCN)
+        t0 = time.perf_counter()
+        O.acoustic_gradient(m_init[0], w, src, rec, obs, A3_DH, A3_DT, A3_ABCN)
+        return A3_RT[0] ** 3 * shots * nt_sample, time.perf_counter() - t0
+
+
+WORKLOADS = {"acoustic2d": AcousticWorkload, "elastic2d": ElasticWorkload, "acoustic3d": Acoustic3DWorkload}
 
 
 def cpu_threads():
@@ -167,28 +345,28 @@ def cpu_threads():
 
 
 # ---------------------------------------------------------------- reference
-def run_reference(args):
+def run_reference(args, wl):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from oracle import oracle as O
     O.build()
-    nt_sample = 1000
+    nt_sample = wl.cpu_nt
     for _ in range(args.warmup):
-        cpu_oracle_run(nt_sample)
+        wl.cpu_run(nt_sample)
     tot_cells, tot_s = 0, 0.0
     for _ in range(args.steps):
-        c, s = cpu_oracle_run(nt_sample)
+        c, s = wl.cpu_run(nt_sample)
         tot_cells += c
         tot_s += s
     value = tot_cells / tot_s / 1e9
-    sample = f"1 of {NSHOT} shots, first {nt_sample} of {NT} steps, forward + adjoint gradient"
+    sample = f"1 of {wl.nshot} shots, first {nt_sample} of {wl.nt} steps, forward + adjoint gradient"
     line = {
         "impl": "reference", "metric": "Gcell-updates/s fwd+adj", "value": value,
         "unit": "Gcell/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": tot_s / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": config_block(args),
+        "config": wl.config(args),
         "cpu_baseline": {"value": value, "unit": "Gcell/s", "cores": cpu_threads(), "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": "Gcell/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -196,19 +374,8 @@ def run_reference(args):
     print(json.dumps(line))
 
 
-def config_block(args):
-    return {"workload": "acoustic2d 256x768 (runtime 344x856), 32 shots, nt 3000, order 8, CPML 40, "
-                        "fwd+adj gradient, boundary saving",
-            "grid": [NZ, NX], "runtime_grid": list(RT), "shots_per_gpu": NSHOT, "nt": NT,
-            "dh": DH, "dt": DT, "abcn": ABCN, "order": ORDER, "seed": SEED,
-            "cells_counted": "runtime grid (physical + PML + halo) x shots x nt",
-            "physical_fraction": NZ * NX / (RT[0] * RT[1]),
-            "l2": "working set per step > L2 (inputs larger than L2; no flush)",
-            "parallelism": f"shots: {NSHOT} per GPU x {args.gpus} GPU(s)"}
-
-
 # ---------------------------------------------------------------------- GPU
-def run_gpu(args):
+def run_gpu(args, wl):
     import torch
     import torch.distributed as dist
 
@@ -221,28 +388,38 @@ def run_gpu(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
 
-    from sweep_b200 import Acoustic, PropTorch
-    vp_true, vp_init, w, src, rec = survey()
-    solver = PropTorch(Acoustic(spatial_order=ORDER, device=dev), shape=(NZ, NX), dh=DH, dt=DT,
-                       abcn=ABCN, device=dev)
+    solver, m_true, m_init, w, src, rec = wl.build(dev)
     w_d = torch.tensor(w, device=dev)
+    bsz = getattr(wl, "batch", wl.nshot)
+    batches = [slice(b, min(b + bsz, wl.nshot)) for b in range(0, wl.nshot, bsz)]
     with torch.no_grad():
-        obs = solver(w_d, src, rec, models=[torch.tensor(vp_true, device=dev)])
-    vp_d = torch.tensor(vp_init, device=dev)
+        mt = [torch.tensor(m, device=dev) for m in m_true]
+        obs = torch.cat([solver(w_d, src[sl], rec[sl], models=mt) for sl in batches])
+        del mt
+    ms_d = [torch.tensor(m, device=dev) for m in m_init]
     torch.cuda.synchronize()
 
-    def step(vp_in, w_in, obs_in, ev=None):
-        vp = vp_in.detach().requires_grad_(True)
-        if ev: ev[0].record()
-        pred = solver(w_in, src, rec, models=[vp])
-        loss = 0.5 * ((pred - obs_in) ** 2).sum()
-        if ev: ev[1].record()
-        loss.backward()
-        if ev: ev[2].record()
-        g = vp.grad
+    def step(ms_in, w_in, obs_in, ev=None):
+        # one gradient of the whole survey: the shot batches run one after the
+        # other and their gradients accumulate into the models' .grad
+        ms = [m.detach().requires_grad_(True) for m in ms_in]
+        loss = 0.0
+        for sl in batches:
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(3)] if ev is not None else None
+            if e: e[0].record()
+            pred = solver(w_in, src[sl], rec[sl], models=ms)
+            lb = 0.5 * ((pred - obs_in[sl]) ** 2).sum()
+            if e: e[1].record()
+            lb.backward()
+            if e:
+                e[2].record()
+                ev.append(e)
+            loss = loss + lb.detach()
+        gs = [m.grad for m in ms]
         if world > 1:
-            dist.all_reduce(g)
-        return loss, g
+            for g in gs:
+                dist.all_reduce(g)
+        return loss, gs
 
     def barrier():
         if world > 1:
@@ -250,22 +427,22 @@ def run_gpu(args):
         torch.cuda.synchronize()
 
     for _ in range(args.warmup):
-        step(vp_d, w_d, obs)
+        step(ms_d, w_d, obs)
     barrier()
 
     # ---- device-resident timing
-    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    evs = [[] for _ in range(args.steps)]     # per step: (start, forward done, backward done) per batch
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         barrier()
         t0.record()
         for k in range(args.steps):
-            step(vp_d, w_d, obs, evs[k])
+            step(ms_d, w_d, obs, evs[k])
         t1.record()
         barrier()
     ms = t0.elapsed_time(t1) / args.steps
-    fwd_ms = float(np.mean([e[0].elapsed_time(e[1]) for e in evs]))
-    rev_ms = float(np.mean([e[1].elapsed_time(e[2]) for e in evs]))
+    fwd_ms = float(np.mean([sum(e[0].elapsed_time(e[1]) for e in st) for st in evs]))
+    rev_ms = float(np.mean([sum(e[1].elapsed_time(e[2]) for e in st) for st in evs]))
     clocks = clk.summary()
     if world > 1:
         t = torch.tensor([ms], device=dev)
@@ -273,31 +450,38 @@ def run_gpu(args):
         ms = float(t)
 
     # ---- end-to-end through the public API with host buffers
-    vp_h = torch.tensor(vp_init).pin_memory()
+    ms_h = [torch.tensor(m).pin_memory() for m in m_init]
     w_h = torch.tensor(w).pin_memory()
     obs_h = obs.cpu().pin_memory()
-    g_h = torch.empty(vp_init.shape, dtype=torch.float32).pin_memory()
-    h2d = vp_h.numel() * 4 + w_h.numel() * 4 + obs_h.numel() * 4
-    d2h = g_h.numel() * 4 + 4
-    for _ in range(2):
-        step(vp_h.to(dev, non_blocking=True), w_h.to(dev, non_blocking=True), obs_h.to(dev, non_blocking=True))
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(args.steps):
-        loss, g = step(vp_h.to(dev, non_blocking=True), w_h.to(dev, non_blocking=True),
-                       obs_h.to(dev, non_blocking=True))
-        g_h.copy_(g, non_blocking=True)
+    g_h = [torch.empty(m.shape, dtype=torch.float32).pin_memory() for m in m_init]
+    h2d = sum(m.numel() * 4 for m in ms_h) + w_h.numel() * 4 + obs_h.numel() * 4
+    d2h = sum(g.numel() * 4 for g in g_h) + 4
+
+    def e2e_step():
+        loss, gs = step([m.to(dev, non_blocking=True) for m in ms_h], w_h.to(dev, non_blocking=True),
+                        obs_h.to(dev, non_blocking=True))
+        for gh, g in zip(g_h, gs):
+            gh.copy_(g, non_blocking=True)
         float(loss)
-    e1.record()
-    barrier()
-    e2e_ms = e0.elapsed_time(e1) / args.steps
+
+    e2e_ms = float("nan")
+    if not args.no_e2e:
+        for _ in range(2):
+            e2e_step()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            e2e_step()
+        e1.record()
+        barrier()
+        e2e_ms = e0.elapsed_time(e1) / args.steps
     if world > 1:
         t = torch.tensor([e2e_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t)
 
-    cells = cell_steps()
+    cells = int(np.prod(wl.rt)) * wl.nshot * wl.nt
     value = cells * world / (ms * 1e-3) / 1e9
     e2e_value = cells * world / (e2e_ms * 1e-3) / 1e9
     peaks = {}
@@ -305,27 +489,27 @@ def run_gpu(args):
     if pk.exists():
         peaks = json.loads(pk.read_text())
     hbm = float(peaks.get("hbm_gbs", 6650.0))
-    per_launch_cells = RT[0] * RT[1] * NSHOT
-    rev_launch_ms = rev_ms / NT
-    achieved = per_launch_cells * BYTES_REV / (rev_launch_ms * 1e-3) / 1e9
+    per_launch_cells = int(np.prod(wl.rt)) * wl.nshot
+    rev_launch_ms = rev_ms / wl.nt
+    achieved = per_launch_cells * wl.bytes_rev / (rev_launch_ms * 1e-3) / 1e9
     line = {
         "metric": "Gcell-updates/s fwd+adj", "value": value, "unit": "Gcell/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded layered model, see config)",
-        "config": config_block(args),
+        "config": wl.config(args),
         "forward_ms": fwd_ms, "backward_ms": rev_ms,
-        "roofline": {"kernel": "sweep::a2d::rev_kernel (fused adjoint + reconstruction + imaging step)",
+        "roofline": {"kernel": wl.kernel,
                      "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if pk.exists() else "fallback 6650",
-                     "algorithmic_bytes_per_launch": per_launch_cells * BYTES_REV,
+                     "algorithmic_bytes_per_launch": per_launch_cells * wl.bytes_rev,
                      "launch_ms": rev_launch_ms,
                      "launch_ms_how": "CUDA events around the backward call on the launch stream / nt",
                      "traffic": None},
-        "forward_roofline": {"achieved": per_launch_cells * BYTES_FWD / (fwd_ms / NT * 1e-3) / 1e9,
-                             "unit": "GB/s", "bytes_per_cell_step": BYTES_FWD},
-        "gpu_launches": args.steps * (2 * NT + 1),
+        "forward_roofline": {"achieved": per_launch_cells * wl.bytes_fwd / (fwd_ms / wl.nt * 1e-3) / 1e9,
+                             "unit": "GB/s", "bytes_per_cell_step": wl.bytes_fwd},
+        "gpu_launches": args.steps * wl.launches(),
         "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": "Gcell/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
@@ -333,10 +517,11 @@ def run_gpu(args):
     if rank == 0 and not args.no_cpu_baseline:
         from oracle import oracle as O
         O.build()
-        c, s = cpu_oracle_run(1000)
+        c, s = wl.cpu_run(wl.cpu_nt)
         line["cpu_baseline"] = {"value": c / s / 1e9, "unit": "Gcell/s", "cores": cpu_threads(),
                                 "kind": "port",
-                                "sample": f"1 of {NSHOT} shots, first 1000 of {NT} steps, fwd+adj gradient"}
+                                "sample": f"1 of {wl.nshot} shots, first {wl.cpu_nt} of {wl.nt} steps, "
+                                          "fwd+adj gradient"}
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
@@ -350,16 +535,23 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true",
+                    help="skip the end-to-end leg (long workloads; the bench line then has no e2e value)")
+    ap.add_argument("--workload", default="acoustic2d", choices=sorted(WORKLOADS),
+                    help="acoustic2d: the 32-shot 256x768 survey (default); elastic2d: the 16-shot "
+                         "400x1200 elastic survey")
     ap.add_argument("--nt", type=int, default=None,
                     help="shorter time axis (profiling captures only; the bench line is for the full nt)")
     args = ap.parse_args()
+    wl = WORKLOADS[args.workload]()
     if args.nt:
-        global NT
-        NT = int(args.nt)
+        wl.nt = int(args.nt)
+        global NT, E_NT, A3_NT
+        NT, E_NT, A3_NT = wl.nt, wl.nt, wl.nt
     if args.impl == "reference":
-        run_reference(args)
+        run_reference(args, wl)
     else:
-        run_gpu(args)
+        run_gpu(args, wl)
 
 
 if __name__ == "__main__":

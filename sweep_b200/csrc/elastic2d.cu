@@ -165,17 +165,38 @@ __device__ __forceinline__ float dmz(const float* t, int c, float inv)
             C3 * (t[c + 2 * HX] - t[c - 3 * HX]) + C4 * (t[c + 3 * HX] - t[c - 4 * HX])) * inv;
 }
 
-// Cooperative load of one field's tile plus an M-cell halo (zero outside the
-// grid) into shared memory.
-__device__ __forceinline__ void load_tile(float* t, const float* __restrict__ g, const Geo& G, int tz0, int tx0)
+// Cooperative load of NF fields' tiles plus an M-cell halo (zero outside the
+// grid) into shared memory: every thread issues all its global loads before
+// its first shared store, so the loads of a CTA are in flight together.
+constexpr int NLD = (HN + NTH - 1) / NTH;   // loads per thread per field
+
+template <int NF>
+__device__ __forceinline__ void load_tiles(float* const (&t)[NF], const float* const (&g)[NF], const Geo& G,
+                                           int tz0, int tx0)
 {
-    for (int k = threadIdx.x + threadIdx.y * TX; k < HN; k += NTH) {
+    const int tid = threadIdx.x + threadIdx.y * TX;
+    float v[NF][NLD];
+    long long off[NLD];
+    bool ok[NLD];
+#pragma unroll
+    for (int j = 0; j < NLD; ++j) {
+        const int k = tid + j * NTH;
         const int lz = k / HX, lx = k - lz * HX;
         const int iz = tz0 - M + lz, ix = tx0 - M + lx;
-        float v = 0.f;
-        if ((unsigned)iz < (unsigned)G.nz && (unsigned)ix < (unsigned)G.nx) v = __ldg(g + (long long)iz * G.P + ix);
-        t[k] = v;
+        ok[j] = k < HN && (unsigned)iz < (unsigned)G.nz && (unsigned)ix < (unsigned)G.nx;
+        off[j] = (long long)iz * G.P + ix;
     }
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+#pragma unroll
+        for (int j = 0; j < NLD; ++j) v[f][j] = ok[j] ? __ldg(g[f] + off[j]) : 0.f;
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+#pragma unroll
+        for (int j = 0; j < NLD; ++j) {
+            const int k = tid + j * NTH;
+            if (k < HN) t[f][k] = v[f][j];
+        }
 }
 
 // Add w to the stress field `fld` (one of SXX, SZZ, SXZ) held in registers.
@@ -216,9 +237,11 @@ __global__ void __launch_bounds__(NTH) fwd_vel(FwdArgs A)
     int tz0, tx0;
     tile_origin(G, blockIdx.x, tz0, tx0);
     const long long so = (long long)b * G.S;
-    load_tile(tsxx, A.f[SXX] + so, G, tz0, tx0);
-    load_tile(tszz, A.f[SZZ] + so, G, tz0, tx0);
-    load_tile(tsxz, A.f[SXZ] + so, G, tz0, tx0);
+    {
+        float* const t[3] = {tsxx, tszz, tsxz};
+        const float* const g[3] = {A.f[SXX] + so, A.f[SZZ] + so, A.f[SXZ] + so};
+        load_tiles<3>(t, g, G, tz0, tx0);
+    }
     __syncthreads();
     const int lx = threadIdx.x, ix = tx0 + lx;
     const float* __restrict__ bv = A.m.bv + (long long)b * G.ms;
@@ -274,8 +297,11 @@ __global__ void __launch_bounds__(NTH) fwd_str(FwdArgs A)
     int tz0, tx0;
     tile_origin(G, tile, tz0, tx0);
     const long long so = (long long)b * G.S;
-    load_tile(tvx, A.f[VX] + so, G, tz0, tx0);
-    load_tile(tvz, A.f[VZ] + so, G, tz0, tx0);
+    {
+        float* const t[2] = {tvx, tvz};
+        const float* const g[2] = {A.f[VX] + so, A.f[VZ] + so};
+        load_tiles<2>(t, g, G, tz0, tx0);
+    }
     const int key = b * G.ntx * G.ntz + tile;
     const int s0 = G.src.off[key], s1 = G.src.off[key + 1];
     __syncthreads();
@@ -403,8 +429,11 @@ __global__ void __launch_bounds__(NTH) rev_str(RevArgs A)
         const int r0 = G.rec.off[key], r1 = G.rec.off[key + 1];
         const int s0 = G.src.off[key], s1 = G.src.off[key + 1];
         __syncthreads();                       // previous shot's tiles consumed
-        load_tile(tvx, A.f[VX] + so, G, tz0, tx0);
-        load_tile(tvz, A.f[VZ] + so, G, tz0, tx0);
+        {
+            float* const t[2] = {tvx, tvz};
+            const float* const g[2] = {A.f[VX] + so, A.f[VZ] + so};
+            load_tiles<2>(t, g, G, tz0, tx0);
+        }
         // residuals of step it into the adjoint fields of this tile's receivers
         for (int e = r0 + tid; e < r1; e += NTH) {
             const int2 ev = G.rec.ev[e];
@@ -536,41 +565,54 @@ __global__ void __launch_bounds__(NTH) rev_sadj(RevArgs A)
     const long long so = (long long)b * G.S;
     const float* __restrict__ lam_ = A.m.lam + (long long)b * G.ms;
     const float* __restrict__ mu_ = A.m.mu + (long long)b * G.ms;
-    for (int k = threadIdx.x + threadIdx.y * TX; k < HN; k += NTH) {
+    const int tid = threadIdx.x + threadIdx.y * TX;
+    float rs[NLD][5];
+#pragma unroll
+    for (int j = 0; j < NLD; ++j) {
+        const int k = tid + j * NTH;
         const int lz = k / HX, lx = k - lz * HX;
         const int iz = tz0 - M + lz, ix = tx0 - M + lx;
-        float q0 = 0.f, q1 = 0.f, q2 = 0.f, q3 = 0.f;
-        if ((unsigned)iz < (unsigned)G.nz && (unsigned)ix < (unsigned)G.nx) {
-            const long long i = (long long)iz * G.P + ix;
-            const float bsxx = A.a[SXX][so + i], bszz = A.a[SZZ][so + i], bsxz = A.a[SXZ][so + i];
-            const float lam = lam_[i], mu = mu_[i];
-            q0 = G.dt * ((lam + 2.f * mu) * bsxx + lam * bszz);
-            q1 = G.dt * ((lam + 2.f * mu) * bszz + lam * bsxx);
-            q2 = G.dt * mu * bsxz;
-            q3 = G.dt * mu * bsxz;
-            if (in_pml(G, ix, iz)) {
-                const bool own = owns(lz, lx);
-                const int xs = xslab(G, ix), zs = zslab(G, iz);
-                if (xs >= 0) {
-                    const long long xi = ((long long)b * G.nz + iz) * G.WX + xs;
-                    const float t0 = A.mo.x[XM_VXX][xi] + q0, t3 = A.mo.x[XM_VZX][xi] + q3;
-                    if (own) {
-                        A.mn.x[XM_VXX][xi] = G.ax[ix] * t0;
-                        A.mn.x[XM_VZX][xi] = G.axh[ix] * t3;
-                    }
-                    q0 = q0 + G.bx[ix] * t0;
-                    q3 = q3 + G.bxh[ix] * t3;
+        const bool ok = k < HN && (unsigned)iz < (unsigned)G.nz && (unsigned)ix < (unsigned)G.nx;
+        const long long i = (long long)iz * G.P + ix;
+        rs[j][0] = ok ? A.a[SXX][so + i] : 0.f;
+        rs[j][1] = ok ? A.a[SZZ][so + i] : 0.f;
+        rs[j][2] = ok ? A.a[SXZ][so + i] : 0.f;
+        rs[j][3] = ok ? lam_[i] : 0.f;
+        rs[j][4] = ok ? mu_[i] : 0.f;
+    }
+#pragma unroll
+    for (int j = 0; j < NLD; ++j) {
+        const int k = tid + j * NTH;
+        if (k >= HN) continue;
+        const int lz = k / HX, lx = k - lz * HX;
+        const int iz = tz0 - M + lz, ix = tx0 - M + lx;
+        const float bsxx = rs[j][0], bszz = rs[j][1], bsxz = rs[j][2], lam = rs[j][3], mu = rs[j][4];
+        float q0 = G.dt * ((lam + 2.f * mu) * bsxx + lam * bszz);
+        float q1 = G.dt * ((lam + 2.f * mu) * bszz + lam * bsxx);
+        float q2 = G.dt * mu * bsxz;
+        float q3 = G.dt * mu * bsxz;
+        if ((unsigned)iz < (unsigned)G.nz && (unsigned)ix < (unsigned)G.nx && in_pml(G, ix, iz)) {
+            const bool own = owns(lz, lx);
+            const int xs = xslab(G, ix), zs = zslab(G, iz);
+            if (xs >= 0) {
+                const long long xi = ((long long)b * G.nz + iz) * G.WX + xs;
+                const float t0 = A.mo.x[XM_VXX][xi] + q0, t3 = A.mo.x[XM_VZX][xi] + q3;
+                if (own) {
+                    A.mn.x[XM_VXX][xi] = G.ax[ix] * t0;
+                    A.mn.x[XM_VZX][xi] = G.axh[ix] * t3;
                 }
-                if (zs >= 0) {
-                    const long long zi = ((long long)b * G.WZ + zs) * G.P + ix;
-                    const float t1 = A.mo.z[ZM_VZZ][zi] + q1, t2 = A.mo.z[ZM_VXZ][zi] + q2;
-                    if (own) {
-                        A.mn.z[ZM_VZZ][zi] = G.az[iz] * t1;
-                        A.mn.z[ZM_VXZ][zi] = G.azh[iz] * t2;
-                    }
-                    q1 = q1 + G.bz[iz] * t1;
-                    q2 = q2 + G.bzh[iz] * t2;
+                q0 = q0 + G.bx[ix] * t0;
+                q3 = q3 + G.bxh[ix] * t3;
+            }
+            if (zs >= 0) {
+                const long long zi = ((long long)b * G.WZ + zs) * G.P + ix;
+                const float t1 = A.mo.z[ZM_VZZ][zi] + q1, t2 = A.mo.z[ZM_VXZ][zi] + q2;
+                if (own) {
+                    A.mn.z[ZM_VZZ][zi] = G.az[iz] * t1;
+                    A.mn.z[ZM_VXZ][zi] = G.azh[iz] * t2;
                 }
+                q1 = q1 + G.bz[iz] * t1;
+                q2 = q2 + G.bzh[iz] * t2;
             }
         }
         tq[0][k] = q0; tq[1][k] = q1; tq[2][k] = q2; tq[3][k] = q3;
@@ -604,48 +646,61 @@ __global__ void __launch_bounds__(NTH) rev_vadj(RevArgs A)
     tile_origin(G, blockIdx.x, tz0, tx0);
     const long long so = (long long)b * G.S;
     const float* __restrict__ bv_ = A.m.bv + (long long)b * G.ms;
-    for (int k = threadIdx.x + threadIdx.y * TX; k < HN; k += NTH) {
+    const int tid = threadIdx.x + threadIdx.y * TX;
+    float rv[NLD][3];
+#pragma unroll
+    for (int j = 0; j < NLD; ++j) {
+        const int k = tid + j * NTH;
         const int lz = k / HX, lx = k - lz * HX;
         const int iz = tz0 - M + lz, ix = tx0 - M + lx;
-        float p0 = 0.f, p1 = 0.f, p2 = 0.f, p3 = 0.f;
-        if ((unsigned)iz < (unsigned)G.nz && (unsigned)ix < (unsigned)G.nx) {
-            const long long i = (long long)iz * G.P + ix;
-            const float k_ = bv_[i];
-            const float avx = A.a[VX][so + i], avz = A.a[VZ][so + i];
-            p0 = k_ * avx;      // pxx
-            p2 = k_ * avx;      // pxz
-            p3 = k_ * avz;      // pzx
-            p1 = k_ * avz;      // pzz
-            if (in_pml(G, ix, iz)) {
-                const bool own = owns(lz, lx);
-                const int xs = xslab(G, ix), zs = zslab(G, iz);
-                if (xs >= 0) {
-                    const long long xi = ((long long)b * G.nz + iz) * G.WX + xs;
-                    const float t0 = A.mo.x[XM_SXXX][xi] + p0, t3 = A.mo.x[XM_SXZX][xi] + p3;
-                    if (own) {
-                        A.mn.x[XM_SXXX][xi] = G.axh[ix] * t0;
-                        A.mn.x[XM_SXZX][xi] = G.ax[ix] * t3;
-                    }
-                    p0 = p0 + G.bxh[ix] * t0;
-                    p3 = p3 + G.bx[ix] * t3;
+        const bool ok = k < HN && (unsigned)iz < (unsigned)G.nz && (unsigned)ix < (unsigned)G.nx;
+        const long long i = (long long)iz * G.P + ix;
+        rv[j][0] = ok ? A.a[VX][so + i] : 0.f;
+        rv[j][1] = ok ? A.a[VZ][so + i] : 0.f;
+        rv[j][2] = ok ? bv_[i] : 0.f;
+    }
+#pragma unroll
+    for (int j = 0; j < NLD; ++j) {
+        const int k = tid + j * NTH;
+        if (k >= HN) continue;
+        const int lz = k / HX, lx = k - lz * HX;
+        const int iz = tz0 - M + lz, ix = tx0 - M + lx;
+        const float avx = rv[j][0], avz = rv[j][1], k_ = rv[j][2];
+        float p0 = k_ * avx;      // pxx
+        float p2 = k_ * avx;      // pxz
+        float p3 = k_ * avz;      // pzx
+        float p1 = k_ * avz;      // pzz
+        if ((unsigned)iz < (unsigned)G.nz && (unsigned)ix < (unsigned)G.nx && in_pml(G, ix, iz)) {
+            const bool own = owns(lz, lx);
+            const int xs = xslab(G, ix), zs = zslab(G, iz);
+            if (xs >= 0) {
+                const long long xi = ((long long)b * G.nz + iz) * G.WX + xs;
+                const float t0 = A.mo.x[XM_SXXX][xi] + p0, t3 = A.mo.x[XM_SXZX][xi] + p3;
+                if (own) {
+                    A.mn.x[XM_SXXX][xi] = G.axh[ix] * t0;
+                    A.mn.x[XM_SXZX][xi] = G.ax[ix] * t3;
                 }
-                if (zs >= 0) {
-                    const long long zi = ((long long)b * G.WZ + zs) * G.P + ix;
-                    const float t2 = A.mo.z[ZM_SXZZ][zi] + p2, t1 = A.mo.z[ZM_SZZZ][zi] + p1;
-                    if (own) {
-                        A.mn.z[ZM_SXZZ][zi] = G.az[iz] * t2;
-                        A.mn.z[ZM_SZZZ][zi] = G.azh[iz] * t1;
-                    }
-                    p2 = p2 + G.bz[iz] * t2;
-                    p1 = p1 + G.bzh[iz] * t1;
+                p0 = p0 + G.bxh[ix] * t0;
+                p3 = p3 + G.bx[ix] * t3;
+            }
+            if (zs >= 0) {
+                const long long zi = ((long long)b * G.WZ + zs) * G.P + ix;
+                const float t2 = A.mo.z[ZM_SXZZ][zi] + p2, t1 = A.mo.z[ZM_SZZZ][zi] + p1;
+                if (own) {
+                    A.mn.z[ZM_SXZZ][zi] = G.az[iz] * t2;
+                    A.mn.z[ZM_SZZZ][zi] = G.azh[iz] * t1;
                 }
+                p2 = p2 + G.bz[iz] * t2;
+                p1 = p1 + G.bzh[iz] * t1;
             }
         }
         tp[0][k] = p0; tp[1][k] = p1; tp[2][k] = p2; tp[3][k] = p3;
     }
-    load_tile(tsxx, A.f[SXX] + so, G, tz0, tx0);
-    load_tile(tszz, A.f[SZZ] + so, G, tz0, tx0);
-    load_tile(tsxz, A.f[SXZ] + so, G, tz0, tx0);
+    {
+        float* const t[3] = {tsxx, tszz, tsxz};
+        const float* const g[3] = {A.f[SXX] + so, A.f[SZZ] + so, A.f[SXZ] + so};
+        load_tiles<3>(t, g, G, tz0, tx0);
+    }
     __syncthreads();
     const int lx = threadIdx.x, ix = tx0 + lx;
     const float* st = A.strips + (long long)b * 5 * G.nstrip;

@@ -132,3 +132,78 @@ def test_velocity_sources_are_refused():
     ms = [torch.tensor(d[k], device=DEV) for k in ("vp_init", "vs_init", "rho_init")]
     with pytest.raises(NotImplementedError, match="velocity"):
         s(torch.tensor(d["wavelet"], device=DEV), d["src"], d["rec"], models=ms)
+
+
+def _fd_case():
+    rng = np.random.default_rng(21)
+    nz, nx, nt, dt, dh, abcn = 40, 48, 260, 0.0005, 5.0, 10
+    z = np.arange(nz)[:, None] + np.zeros((1, nx))
+    vp = (2000 + 20.0 * z + 30 * rng.standard_normal((nz, nx))).astype(np.float32)
+    vs = (vp / 1.73).astype(np.float32)
+    rho = (310 * vp ** 0.25).astype(np.float32)
+    t = np.arange(nt) * dt
+    w = ((1 - 2 * (np.pi * 25 * (t - 0.04)) ** 2) * np.exp(-(np.pi * 25 * (t - 0.04)) ** 2)).astype(np.float32)
+    src = np.array([[24, 5]])
+    rec = np.zeros((1, 12, 2), np.int64)
+    rec[0, :, 0] = np.linspace(2, nx - 3, 12)
+    rec[0, :, 1] = 3
+    vt = vp.copy()
+    vt[20:] *= 1.1
+    obs = O.elastic_forward(vt, (vt / 1.73).astype(np.float32), (310 * vt ** 0.25).astype(np.float32),
+                            w, src, rec, dh, dt, abcn, prec="f64").astype(np.float32)
+    return dict(vp=vp, vs=vs, rho=rho, w=w, src=src, rec=rec, obs=obs, dh=dh, dt=dt, abcn=abcn, rng=rng)
+
+
+def test_gradient_matches_central_differences_at_32_cells():
+    """vp / vs / rho gradients at 32 random interior cells against central
+    differences of the loss, taken with the float64 oracle forward (its own
+    adjoint agrees with them to ~1e-6)."""
+    c = _fd_case()
+    s = _solver(c["vp"].shape, c["dh"], c["dt"], c["abcn"])
+    _, g = _grad_run(s, c["w"], c["src"], c["rec"], [c["vp"], c["vs"], c["rho"]], c["obs"])
+    nz, nx = c["vp"].shape
+    cells = [(int(c["rng"].integers(2, nz - 2)), int(c["rng"].integers(2, nx - 2))) for _ in range(32)]
+    base = [c[k].astype(np.float64) for k in ("vp", "vs", "rho")]
+
+    def loss(k, iz, ix, h):
+        ms = [m.copy() for m in base]
+        ms[k][iz, ix] += h
+        p = O.Elastic2D(*ms, c["w"], c["src"], c["rec"], c["dh"], c["dt"], c["abcn"], prec="f64").forward(False)
+        return 0.5 * np.sum((p - c["obs"]) ** 2)
+
+    for k, name in enumerate(("vp", "vs", "rho")):
+        fd = np.array([(loss(k, iz, ix, 1.0) - loss(k, iz, ix, -1.0)) / 2.0 for iz, ix in cells])
+        an = np.array([g[k][iz, ix] for iz, ix in cells], np.float64)
+        print(f"{name}: 32-cell gradient vs central differences rel {rel(an, fd):.2e}")
+        assert rel(an, fd) < 1e-3
+
+
+def test_directional_derivative_through_own_forward():
+    """<g, dm> against (L(m + e dm) - L(m - e dm)) / 2e with the float32 CUDA
+    forward and a float64 loss, along dm = g / max|g| per model (outer 2-cell
+    ring zeroed: those cells are replicated across the PML pad and the
+    gradient is the crop of a runtime-grid gradient).  Along the gradient the
+    first-order change has no cancellation, so it stands well above the float32
+    rounding of the records."""
+    c = _fd_case()
+    s = _solver(c["vp"].shape, c["dh"], c["dt"], c["abcn"])
+    ms0 = [c["vp"], c["vs"], c["rho"]]
+    _, g = _grad_run(s, c["w"], c["src"], c["rec"], ms0, c["obs"])
+    dms = []
+    for gk in g:
+        dm = (gk / np.abs(gk).max()).astype(np.float32)
+        dm[:2], dm[-2:], dm[:, :2], dm[:, -2:] = 0, 0, 0, 0
+        dms.append(dm)
+    obs = torch.tensor(c["obs"], device=DEV, dtype=torch.float64)
+
+    def loss(e):
+        with torch.no_grad():
+            p = s(torch.tensor(c["w"], device=DEV), c["src"], c["rec"],
+                  models=[torch.tensor(m + e * dm, device=DEV) for m, dm in zip(ms0, dms)])
+        return 0.5 * float(((p.double() - obs) ** 2).sum())
+
+    eps = 0.5
+    fd = (loss(eps) - loss(-eps)) / (2 * eps)
+    an = float(sum(np.sum(gk.astype(np.float64) * dm) for gk, dm in zip(g, dms)))
+    print(f"directional derivative: fd {fd:.6e} adjoint {an:.6e}")
+    assert abs(fd - an) <= 2e-3 * abs(an), (fd, an)
