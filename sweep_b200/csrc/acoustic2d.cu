@@ -294,7 +294,7 @@ __global__ void __launch_bounds__(NTH) fwd_kernel(const __grid_constant__ FwdMap
                 atomicAdd(sm.out + ev.x, __ldg(P.wavelet + (long long)ev.y * P.nt + it));
             }
             __syncthreads();
-            for (int e = r_beg + threadIdx.x; e < r_end; e += NTH) {
+            for (int e = r_beg + threadIdx.x; F.record && e < r_end; e += NTH) {
                 const int2 ev = P.rec.ev[e];
                 const int rb = ev.y / P.nrec, rr = ev.y - rb * P.nrec;
                 F.record[((long long)rb * P.nt + it) * P.nrec + rr] = sm.out[ev.x];
@@ -835,6 +835,42 @@ static float* tape_last(void* tape, const Plan& pl)
     return c.take<float>(2LL * pl.P.B * pl.P.S);
 }
 
+// Checkpointed boundary saving (SWEEP_MEM_CHECKPOINT, chunk length k): for
+// every chunk c >= 1 the tape holds the forward state before step c k -- the
+// wavefield pair (U[ck-1], U[ck]), the CPML psi (x, z) and zeta (x, z) -- and
+// the strips of U[ck-1].  The backward replays each chunk from its checkpoint,
+// keeping that chunk's strips only, and runs the boundary-saving reverse step
+// over it (the reference re-runs each chunk from a checkpoint as well,
+// checkpoint_runtime.cuh:15-362, eq_driver.cuh:928-1135).
+constexpr int kStateFields = 6;
+
+static int nchunks(const Plan& pl, int k) { return (pl.P.nt + k - 1) / k; }
+
+static long long ckpt_stride(const Plan& pl)
+{
+    Carve c(nullptr);
+    c.take<float>(kStateFields * (long long)pl.P.B * pl.P.S);
+    c.take<float>((long long)pl.P.B * pl.P.nstrip);
+    return (c.off + 255) & ~255LL;
+}
+
+static int64_t tape_bytes_ckpt(const Plan& pl, int k)
+{
+    return (int64_t)std::max(nchunks(pl, k) - 1, 1) * ckpt_stride(pl);
+}
+
+// state field f of checkpoint c (c >= 1), then its strips
+static float* ckpt_field(void* tape, const Plan& pl, int c, int f)
+{
+    char* base = static_cast<char*>(tape) + (long long)(c - 1) * ckpt_stride(pl);
+    return reinterpret_cast<float*>(base) + (long long)f * pl.P.B * pl.P.S;
+}
+
+static float* ckpt_strips(void* tape, const Plan& pl, int c)
+{
+    return ckpt_field(tape, pl, c, kStateFields);
+}
+
 struct VecStage {
     std::vector<int32_t> ls, lr, os, orr, fill, ord;
     std::vector<int2> es, er;
@@ -922,17 +958,44 @@ static void set_attrs()
     done = true;
 }
 
+// Backward workspace of the checkpoint mode: the reverse set, the forward set
+// the replay runs in, and the strips of one chunk (k + 1 steps).
+static void carve_rev_ckpt(Carve& c, const Plan& pl, bool illum, int k, RevWork& rw, FwdWork& fw, float*& chunk)
+{
+    rw = carve_rev(c, pl, illum);
+    const long long n = (long long)pl.P.B * pl.P.S;
+    for (auto& p : fw.u) p = c.take<float>(n);
+    fw.psix = c.take<float>(n); fw.psiz = c.take<float>(n);
+    fw.psixn = c.take<float>(n); fw.psizn = c.take<float>(n);
+    fw.zetax = c.take<float>(n); fw.zetaz = c.take<float>(n);
+    fw.c = rw.c;
+    chunk = c.take<float>((long long)(k + 1) * pl.P.B * pl.P.nstrip);
+}
+
+static void check_mode(int mem_mode, int ckpt_every)
+{
+    SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY || mem_mode == SWEEP_MEM_CHECKPOINT,
+                  "acoustic2d: unknown memory mode %d", mem_mode);
+    SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY || ckpt_every >= 1,
+                  "acoustic2d: checkpoint interval must be >= 1 (got %d)", ckpt_every);
+}
+
 void sizes(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, int64_t* ws, int64_t* tape)
 {
-    SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY, "acoustic2d: only boundary saving is built for 2-D");
-    (void)ckpt_every;
+    check_mode(mem_mode, ckpt_every);
     Plan pl = make_plan(d);
     Carve cf(nullptr);
     carve_fwd(cf, pl);
     Carve cr(nullptr);
-    carve_rev(cr, pl, true);
+    if (mem_mode == SWEEP_MEM_CHECKPOINT) {
+        RevWork rw; FwdWork fw; float* chunk;
+        carve_rev_ckpt(cr, pl, true, ckpt_every, rw, fw, chunk);
+        *tape = tape_bytes_ckpt(pl, ckpt_every);
+    } else {
+        carve_rev(cr, pl, true);
+        *tape = tape_bytes(pl);
+    }
     *ws = std::max(cf.off, cr.off);
-    *tape = tape_bytes(pl);
 }
 
 int64_t forward_only_bytes(const sweep_acoustic_desc* d)
@@ -951,8 +1014,51 @@ void stage_sizes(const sweep_acoustic_desc* d, int64_t* nkey, int64_t* nev_src, 
     *nev_rec = (int64_t)d->B * d->nrec;
 }
 
-void forward_with(const sweep_acoustic_desc* d, float* record, void* tape, void* ws, int64_t ws_bytes,
-                  cudaStream_t st, const HostStage* stage)
+// Rotating forward state: wavefield buffer indices and the CPML psi pair.
+struct FwdState {
+    int ip = 0, in = 1, ix = 2;
+    float *px, *pz, *pxn, *pzn;
+};
+
+static FwdMaps fwd_maps(const FwdWork& w, const Params& P)
+{
+    FwdMaps maps;
+    for (int i = 0; i < 3; ++i) {
+        maps.halo[i] = field_map(w.u[i], P, P.B, true);
+        maps.tile[i] = field_map(w.u[i], P, P.B, false);
+    }
+    return maps;
+}
+
+// Forward steps [it0, it1): one fwd_kernel launch per step; `strips_of(it)`
+// is the strip slot step `it` writes (null: none), `record` may be null.
+template <class StripsOf>
+static void forward_steps(const Plan& pl, const FwdMaps& maps, const FwdWork& w, float* record, FwdState& S,
+                          int it0, int it1, StripsOf strips_of, cudaStream_t st)
+{
+    Params PF = pl.P;
+    PF.G = pl.Gf;
+    FwdPtrs F{};
+    F.record = record;
+    F.zetax = w.zetax; F.zetaz = w.zetaz;
+    for (int it = it0; it < it1; ++it) {
+        F.now = S.in; F.prev = S.ip; F.u_next = w.u[S.ix];
+        F.psix = S.px; F.psiz = S.pz; F.psixn = S.pxn; F.psizn = S.pzn;
+        F.strips = strips_of(it);
+        fwd_kernel<<<pl.gridf, NTH, fwd_smem(), st>>>(maps, PF, F, it);
+        SWEEP_LAUNCH_CHECK();
+        const int t = S.ip; S.ip = S.in; S.in = S.ix; S.ix = t;
+        std::swap(S.px, S.pxn); std::swap(S.pz, S.pzn);
+    }
+}
+
+static void copy_dd(float* dst, const float* src, long long n, cudaStream_t st)
+{
+    SWEEP_CUDA(cudaMemcpyAsync(dst, src, n * 4, cudaMemcpyDeviceToDevice, st));
+}
+
+void forward_with(const sweep_acoustic_desc* d, int ckpt_every, float* record, void* tape, void* ws,
+                  int64_t ws_bytes, cudaStream_t st, const HostStage* stage)
 {
     SWEEP_REQUIRE(record != nullptr || d->nrec == 0, "acoustic2d forward: null record");
     SWEEP_REQUIRE(d->vp != nullptr, "acoustic2d forward: null vp");
@@ -975,33 +1081,34 @@ void forward_with(const sweep_acoustic_desc* d, float* record, void* tape, void*
         SWEEP_CUDA(cudaMemsetAsync(p, 0, n * 4, st));
     if (d->nrec > 0)
         SWEEP_CUDA(cudaMemsetAsync(record, 0, (size_t)d->B * d->nt * d->nrec * 4, st));
-    Params PF = P;
-    PF.G = pl.Gf;
-    FwdMaps maps;
-    for (int i = 0; i < 3; ++i) {
-        maps.halo[i] = field_map(w.u[i], P, P.B, true);
-        maps.tile[i] = field_map(w.u[i], P, P.B, false);
-    }
-    float* strips = static_cast<float*>(tape);
-    FwdPtrs F{};
-    F.record = record;
-    F.zetax = w.zetax; F.zetaz = w.zetaz;
-    int ip = 0, in = 1, ix = 2;
-    float *px = w.psix, *pz = w.psiz, *pxn = w.psixn, *pzn = w.psizn;
-    for (int it = 0; it < d->nt; ++it) {
-        F.now = in; F.prev = ip; F.u_next = w.u[ix];
-        F.psix = px; F.psiz = pz; F.psixn = pxn; F.psizn = pzn;
-        F.strips = strips ? strips + (long long)it * P.B * P.nstrip : nullptr;
-        fwd_kernel<<<pl.gridf, NTH, fwd_smem(), st>>>(maps, PF, F, it);
-        SWEEP_LAUNCH_CHECK();
-        const int t = ip; ip = in; in = ix; ix = t;
-        std::swap(px, pxn); std::swap(pz, pzn);
-    }
-    if (strips) {
-        float* last = tape_last(tape, pl);
-        // (U[nt-1], U[nt]) per shot, pitched
-        SWEEP_CUDA(cudaMemcpyAsync(last, w.u[ip], n * 4, cudaMemcpyDeviceToDevice, st));
-        SWEEP_CUDA(cudaMemcpyAsync(last + n, w.u[in], n * 4, cudaMemcpyDeviceToDevice, st));
+    const FwdMaps maps = fwd_maps(w, P);
+    FwdState S;
+    S.px = w.psix; S.pz = w.psiz; S.pxn = w.psixn; S.pzn = w.psizn;
+    if (ckpt_every <= 0) {
+        float* strips = static_cast<float*>(tape);
+        forward_steps(pl, maps, w, record, S, 0, d->nt,
+                      [&](int it) { return strips ? strips + (long long)it * P.B * P.nstrip : nullptr; }, st);
+        if (strips) {
+            float* last = tape_last(tape, pl);
+            // (U[nt-1], U[nt]) per shot, pitched
+            copy_dd(last, w.u[S.ip], n, st);
+            copy_dd(last + n, w.u[S.in], n, st);
+        }
+    } else {
+        const int k = ckpt_every, C = nchunks(pl, k);
+        for (int ch = 0; ch < C; ++ch) {
+            const int it0 = ch * k, it1 = std::min(d->nt, it0 + k);
+            if (tape && ch >= 1) {
+                const float* state[kStateFields] = {w.u[S.ip], w.u[S.in], S.px, S.pz, w.zetax, w.zetaz};
+                for (int f = 0; f < kStateFields; ++f) copy_dd(ckpt_field(tape, pl, ch, f), state[f], n, st);
+            }
+            // the last step of a chunk keeps its strips with the next checkpoint
+            forward_steps(pl, maps, w, record, S, it0, it1,
+                          [&](int it) {
+                              return (tape && it == it1 - 1 && ch + 1 < C) ? ckpt_strips(tape, pl, ch + 1) : nullptr;
+                          },
+                          st);
+        }
     }
     check_err(w.c, st, "forward");
 }
@@ -1013,7 +1120,7 @@ void forward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* 
     sizes(d, mem_mode, ckpt_every, &need_ws, &need_tape);
     SWEEP_REQUIRE(ws != nullptr && ws_bytes >= need_ws, "acoustic2d forward: workspace too small (%lld < %lld)",
                   (long long)ws_bytes, (long long)need_ws);
-    forward_with(d, record, tape, ws, ws_bytes, st, nullptr);
+    forward_with(d, mem_mode == SWEEP_MEM_CHECKPOINT ? ckpt_every : 0, record, tape, ws, ws_bytes, st, nullptr);
 }
 
 void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const float* adj, const void* tape,
@@ -1031,7 +1138,12 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     Plan pl = make_plan(d);
     Carve c(ws);
     const bool illum = illum_s != nullptr;
-    RevWork w = carve_rev(c, pl, illum);
+    const bool ckpt = mem_mode == SWEEP_MEM_CHECKPOINT;
+    RevWork w;
+    FwdWork fw{};
+    float* chunk = nullptr;
+    if (ckpt) carve_rev_ckpt(c, pl, illum, ckpt_every, w, fw, chunk);
+    else w = carve_rev(c, pl, illum);
     {
         VecStage vs(pl.P);
         setup_common(d, pl, w.c, st, vs.h);
@@ -1049,12 +1161,6 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     }
     if (grad_w && d->nsrc > 0)
         SWEEP_CUDA(cudaMemsetAsync(grad_w, 0, (size_t)d->B * d->nsrc * d->nt * 4, st));
-    const float* strips = static_cast<const float*>(tape);
-    const float* last = tape_last(const_cast<void*>(tape), pl);
-    // seed: prev = U[nt], now = U[nt-1]  (reference driver_traits.cuh:493-505; the
-    // rim outside the physical box is never read by the reconstruction)
-    SWEEP_CUDA(cudaMemcpyAsync(w.r[0], last + n, n * 4, cudaMemcpyDeviceToDevice, st));
-    SWEEP_CUDA(cudaMemcpyAsync(w.r[1], last, n * 4, cudaMemcpyDeviceToDevice, st));
     RevMaps maps;
     for (int i = 0; i < 3; ++i) {
         maps.lh[i] = field_map(w.l[i], P, P.B, true);
@@ -1068,20 +1174,57 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     R.gacc = w.gacc; R.gcomp = w.gcomp;
     R.illum_s = w.is; R.illum_r = w.ir;
     int lp = 0, ln = 1, lx = 2;
-    int rp = 0, rn = 1, rx = 2;
     int cur = 0;
-    for (int it = d->nt - 1; it >= 0; --it) {
-        const int do_recon = it > 0 ? 1 : 0;
-        R.lprev = lp; R.lnow = ln; R.l_next = w.l[lx];
-        R.apx = w.aux[0 + cur]; R.apz = w.aux[2 + cur]; R.azx = w.aux[4 + cur]; R.azz = w.aux[6 + cur];
-        R.apx_o = w.aux[1 - cur]; R.apz_o = w.aux[3 - cur]; R.azx_o = w.aux[5 - cur]; R.azz_o = w.aux[7 - cur];
-        R.rprev = rp; R.rnow = rn; R.r_next = w.r[rx];
-        R.strips = do_recon ? strips + (long long)(it - 1) * P.B * P.nstrip : nullptr;
-        rev_kernel<<<pl.gridr, NTH, rev_smem(), st>>>(maps, P, R, it, do_recon);
-        SWEEP_LAUNCH_CHECK();
-        int t = lp; lp = ln; ln = lx; lx = t;
-        cur = 1 - cur;
-        if (do_recon) { t = rp; rp = rn; rn = rx; rx = t; }
+    // Reverse steps [it0, it1) top down; the reconstruction starts from
+    // r[0] = U[it1], r[1] = U[it1 - 1]; strips_of(it) holds the strips of U[it].
+    auto reverse = [&](int it0, int it1, auto strips_of) {
+        int rp = 0, rn = 1, rx = 2;
+        for (int it = it1 - 1; it >= it0; --it) {
+            const int do_recon = it > 0 ? 1 : 0;
+            R.lprev = lp; R.lnow = ln; R.l_next = w.l[lx];
+            R.apx = w.aux[0 + cur]; R.apz = w.aux[2 + cur]; R.azx = w.aux[4 + cur]; R.azz = w.aux[6 + cur];
+            R.apx_o = w.aux[1 - cur]; R.apz_o = w.aux[3 - cur]; R.azx_o = w.aux[5 - cur]; R.azz_o = w.aux[7 - cur];
+            R.rprev = rp; R.rnow = rn; R.r_next = w.r[rx];
+            R.strips = do_recon ? strips_of(it - 1) : nullptr;
+            rev_kernel<<<pl.gridr, NTH, rev_smem(), st>>>(maps, P, R, it, do_recon);
+            SWEEP_LAUNCH_CHECK();
+            int t = lp; lp = ln; ln = lx; lx = t;
+            cur = 1 - cur;
+            if (do_recon) { t = rp; rp = rn; rn = rx; rx = t; }
+        }
+    };
+    if (!ckpt) {
+        const float* strips = static_cast<const float*>(tape);
+        const float* last = tape_last(const_cast<void*>(tape), pl);
+        // seed: prev = U[nt], now = U[nt-1]  (reference driver_traits.cuh:493-505; the
+        // rim outside the physical box is never read by the reconstruction)
+        copy_dd(w.r[0], last + n, n, st);
+        copy_dd(w.r[1], last, n, st);
+        reverse(0, d->nt, [&](int t) { return strips + (long long)t * P.B * P.nstrip; });
+    } else {
+        const int k = ckpt_every, C = nchunks(pl, k);
+        const FwdMaps fmaps = fwd_maps(fw, P);
+        void* tp = const_cast<void*>(tape);
+        const long long cs = (long long)P.B * P.nstrip;
+        for (int ch = C - 1; ch >= 0; --ch) {
+            const int it0 = ch * k, it1 = std::min(d->nt, it0 + k);
+            FwdState S;
+            S.px = fw.psix; S.pz = fw.psiz; S.pxn = fw.psixn; S.pzn = fw.psizn;
+            if (ch == 0) {
+                for (auto* p : {fw.u[0], fw.u[1], fw.psix, fw.psiz, fw.zetax, fw.zetaz})
+                    SWEEP_CUDA(cudaMemsetAsync(p, 0, n * 4, st));
+            } else {
+                float* state[kStateFields] = {fw.u[0], fw.u[1], fw.psix, fw.psiz, fw.zetax, fw.zetaz};
+                for (int f = 0; f < kStateFields; ++f) copy_dd(state[f], ckpt_field(tp, pl, ch, f), n, st);
+                copy_dd(chunk, ckpt_strips(tp, pl, ch), cs, st);          // strips of U[it0 - 1]
+            }
+            // replay: chunk slot j holds the strips of U[it0 - 1 + j]
+            forward_steps(pl, fmaps, fw, nullptr, S, it0, it1,
+                          [&](int it) { return chunk + (long long)(it - it0 + 1) * cs; }, st);
+            copy_dd(w.r[0], fw.u[S.in], n, st);       // U[it1]
+            copy_dd(w.r[1], fw.u[S.ip], n, st);       // U[it1 - 1]
+            reverse(it0, it1, [&](int t) { return chunk + (long long)(t - (it0 - 1)) * cs; });
+        }
     }
     const int nout = P.per_shot ? d->B : 1;
     finalize_kernel<<<1184, 256, 0, st>>>(w.gacc, w.gcomp, w.is, w.ir, pl.nslot, nout, d->nz, d->nx, P.P,

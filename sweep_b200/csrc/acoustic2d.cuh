@@ -25,9 +25,10 @@ void backward(const sweep_acoustic_desc*, int, int, const float*, const void*, f
 int64_t forward_only_bytes(const sweep_acoustic_desc* d);
 // Event-table staging sizes: shot-tile keys (+1) and events of each kind.
 void stage_sizes(const sweep_acoustic_desc* d, int64_t* nkey, int64_t* nev_src, int64_t* nev_rec);
-// Forward with an explicit workspace and host staging (stage == nullptr: growable).
-void forward_with(const sweep_acoustic_desc* d, float* record, void* tape, void* ws, int64_t ws_bytes,
-                  cudaStream_t st, const HostStage* stage);
+// Forward with an explicit workspace and host staging (stage == nullptr: growable);
+// ckpt_every > 0 writes the checkpoint-mode tape.
+void forward_with(const sweep_acoustic_desc* d, int ckpt_every, float* record, void* tape, void* ws,
+                  int64_t ws_bytes, cudaStream_t st, const HostStage* stage);
 
 }  // namespace a2d
 }  // namespace sweep

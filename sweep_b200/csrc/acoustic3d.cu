@@ -676,7 +676,7 @@ static dim3 stencil_grid(const Params& P)
 
 struct Work {
     float *cf, *ca, *vv;
-    float* f[22];                    // forward: u x3, psi x6, zeta x3; reverse: see backward()
+    float* f[34];                    // forward: u x3, psi x6, zeta x3; reverse: see backward()
 };
 
 static Work carve(Carve& c, const Params& P, int nfields)
@@ -704,18 +704,104 @@ static float* tape_last(void* tape, const Params& P)
 
 static constexpr int kFwdFields = 12, kRevFields = 22;
 
+// Checkpointed boundary saving (SWEEP_MEM_CHECKPOINT, chunk length k): for
+// every chunk c >= 1 the tape holds the forward state before step c k -- the
+// wavefield pair (U[ck-1], U[ck]), CPML psi (x, y, z) and zeta (x, y, z) --
+// and the strips of U[ck-1]; the backward replays each chunk from its
+// checkpoint into the strips of that chunk and runs the boundary-saving
+// reverse steps over it (reference checkpoint_runtime.cuh:15-362,
+// eq_driver.cuh:928-1135: chunked replay).
+static constexpr int kStateFields = 8;
+
+static int nchunks(const Params& P, int k) { return (P.nt + k - 1) / k; }
+
+static long long ckpt_stride(const Params& P)
+{
+    Carve c(nullptr);
+    c.take<float>(kStateFields * (long long)P.B * P.S);
+    c.take<float>((long long)P.B * std::max(P.nstrip, 1LL));
+    return (c.off + 255) & ~255LL;
+}
+
+static float* ckpt_field(void* tape, const Params& P, int c, int f)
+{
+    char* base = static_cast<char*>(tape) + (long long)(c - 1) * ckpt_stride(P);
+    return reinterpret_cast<float*>(base) + (long long)f * P.B * P.S;
+}
+
+static float* ckpt_strips(void* tape, const Params& P, int c) { return ckpt_field(tape, P, c, kStateFields); }
+
 void sizes(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, int64_t* ws, int64_t* tape)
 {
-    SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY, "acoustic3d: unknown memory mode %d", mem_mode);
-    (void)ckpt_every;
+    SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY || mem_mode == SWEEP_MEM_CHECKPOINT,
+                  "acoustic3d: unknown memory mode %d", mem_mode);
+    SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY || ckpt_every >= 1,
+                  "acoustic3d: checkpoint interval must be >= 1 (got %d)", ckpt_every);
     const Params P = make_params(d);
     Carve c(nullptr);
-    carve(c, P, std::max(kFwdFields, kRevFields));
+    if (mem_mode == SWEEP_MEM_CHECKPOINT) {
+        carve(c, P, kRevFields + kFwdFields);
+        c.take<float>((long long)(ckpt_every + 1) * P.B * P.nstrip);
+        *tape = (int64_t)std::max(nchunks(P, ckpt_every) - 1, 1) * ckpt_stride(P);
+    } else {
+        carve(c, P, std::max(kFwdFields, kRevFields));
+        *tape = tape_bytes(P);
+    }
     *ws = c.off;
-    *tape = tape_bytes(P);
 }
 
 static inline unsigned blocks_for(long long n, int threads) { return (unsigned)std::max(1LL, (n + threads - 1) / threads); }
+
+static void copy_dd(float* dst, const float* src, long long n, cudaStream_t st)
+{
+    SWEEP_CUDA(cudaMemcpyAsync(dst, src, n * 4, cudaMemcpyDeviceToDevice, st));
+}
+
+// Rotating forward state over the 12 forward fields f[0..11] of a set:
+// wavefield buffer indices and the current / next CPML psi triples.
+struct FwdState {
+    float* const* f;
+    int ip = 0, in = 1, ix = 2;
+    float* ps[3];
+    float* psn[3];
+    explicit FwdState(float* const* fields) : f(fields)
+    {
+        for (int a = 0; a < 3; ++a) { ps[a] = f[3 + a]; psn[a] = f[6 + a]; }
+    }
+    float* zeta(int a) const { return f[9 + a]; }
+};
+
+// Forward steps [it0, it1): stencil, strips of U[it] (strips_of(it), null:
+// none), source injection, receiver gather (record may be null).
+template <class StripsOf>
+static void forward_steps(const sweep_acoustic_desc* d, const Params& P, FwdState& S, float* record, int it0,
+                          int it1, StripsOf strips_of, cudaStream_t st)
+{
+    const dim3 grid = stencil_grid(P), block(BXC, BYC);
+    const unsigned gs = blocks_for((long long)P.B * P.nsrc, 128), gr = blocks_for((long long)P.B * P.nrec, 128);
+    const unsigned gst = blocks_for((long long)P.B * P.nstrip, 256);
+    for (int it = it0; it < it1; ++it) {
+        F3 F{S.f[S.in], S.f[S.ip], S.f[S.ix], S.ps[0], S.ps[1], S.ps[2], S.psn[0], S.psn[1], S.psn[2],
+             S.zeta(0), S.zeta(1), S.zeta(2)};
+        f3_step<<<grid, block, 0, st>>>(P, F);
+        SWEEP_LAUNCH_CHECK();
+        float* strips = strips_of(it);
+        if (strips && P.nstrip > 0) strips3<<<gst, 256, 0, st>>>(P, S.f[S.in], strips, 0);
+        if (d->nsrc > 0)
+            inject3<<<gs, 128, 0, st>>>(P, S.f[S.ix], d->wavelet, d->src_loc, d->nsrc, it, 0, 1.f, 0);
+        if (d->nrec > 0 && record)
+            gather3<<<gr, 128, 0, st>>>(P, S.f[S.ix], record, d->rec_loc, d->nrec, it, 1);
+        SWEEP_LAUNCH_CHECK();
+        const int t = S.ip; S.ip = S.in; S.in = S.ix; S.ix = t;
+        for (int a = 0; a < 3; ++a) std::swap(S.ps[a], S.psn[a]);
+    }
+}
+
+static void state_fields(const FwdState& S, float* out[kStateFields])
+{
+    out[0] = S.f[S.ip]; out[1] = S.f[S.in];
+    for (int a = 0; a < 3; ++a) { out[2 + a] = S.ps[a]; out[5 + a] = S.zeta(a); }
+}
 
 void forward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* record, void* tape,
              void* ws, int64_t ws_bytes, cudaStream_t st)
@@ -735,31 +821,30 @@ void forward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* 
     const long long n = (long long)P.B * P.S;
     for (int i = 0; i < kFwdFields; ++i) SWEEP_CUDA(cudaMemsetAsync(w.f[i], 0, n * 4, st));
     if (d->nrec > 0) SWEEP_CUDA(cudaMemsetAsync(record, 0, (size_t)d->B * d->nt * d->nrec * 4, st));
-    float* strips = static_cast<float*>(tape);
-    const dim3 grid = stencil_grid(P), block(BXC, BYC);
-    const unsigned gs = blocks_for((long long)P.B * P.nsrc, 128), gr = blocks_for((long long)P.B * P.nrec, 128);
-    const unsigned gst = blocks_for((long long)P.B * P.nstrip, 256);
-    int ip = 0, in = 1, ix = 2;
-    float* ps[3] = {w.f[3], w.f[4], w.f[5]};
-    float* psn[3] = {w.f[6], w.f[7], w.f[8]};
-    for (int it = 0; it < d->nt; ++it) {
-        F3 F{w.f[in], w.f[ip], w.f[ix], ps[0], ps[1], ps[2], psn[0], psn[1], psn[2], w.f[9], w.f[10], w.f[11]};
-        f3_step<<<grid, block, 0, st>>>(P, F);
-        SWEEP_LAUNCH_CHECK();
-        if (strips && P.nstrip > 0)
-            strips3<<<gst, 256, 0, st>>>(P, w.f[in], strips + (long long)it * P.B * P.nstrip, 0);
-        if (d->nsrc > 0)
-            inject3<<<gs, 128, 0, st>>>(P, w.f[ix], d->wavelet, d->src_loc, d->nsrc, it, 0, 1.f, 0);
-        if (d->nrec > 0)
-            gather3<<<gr, 128, 0, st>>>(P, w.f[ix], record, d->rec_loc, d->nrec, it, 1);
-        SWEEP_LAUNCH_CHECK();
-        const int t = ip; ip = in; in = ix; ix = t;
-        for (int a = 0; a < 3; ++a) std::swap(ps[a], psn[a]);
+    FwdState S(w.f);
+    if (mem_mode != SWEEP_MEM_CHECKPOINT) {
+        float* strips = static_cast<float*>(tape);
+        forward_steps(d, P, S, record, 0, d->nt,
+                      [&](int it) { return strips ? strips + (long long)it * P.B * P.nstrip : nullptr; }, st);
+        if (strips) {
+            float* last = tape_last(tape, P);
+            copy_dd(last, S.f[S.ip], n, st);        // U[nt-1]
+            copy_dd(last + n, S.f[S.in], n, st);    // U[nt]
+        }
+        return;
     }
-    if (strips) {
-        float* last = tape_last(tape, P);
-        SWEEP_CUDA(cudaMemcpyAsync(last, w.f[ip], n * 4, cudaMemcpyDeviceToDevice, st));       // U[nt-1]
-        SWEEP_CUDA(cudaMemcpyAsync(last + n, w.f[in], n * 4, cudaMemcpyDeviceToDevice, st));   // U[nt]
+    const int k = ckpt_every, C = nchunks(P, k);
+    for (int ch = 0; ch < C; ++ch) {
+        const int it0 = ch * k, it1 = std::min(d->nt, it0 + k);
+        if (tape && ch >= 1) {
+            float* state[kStateFields];
+            state_fields(S, state);
+            for (int f = 0; f < kStateFields; ++f) copy_dd(ckpt_field(tape, P, ch, f), state[f], n, st);
+        }
+        // the last step of a chunk keeps its strips with the next checkpoint
+        forward_steps(d, P, S, record, it0, it1,
+                      [&](int it) { return (tape && it == it1 - 1 && ch + 1 < C) ? ckpt_strips(tape, P, ch + 1) : nullptr; },
+                      st);
     }
 }
 
@@ -773,62 +858,96 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     SWEEP_REQUIRE(tape != nullptr && grad_vp != nullptr, "acoustic3d backward: null tape or gradient");
     SWEEP_REQUIRE(adj != nullptr || d->nrec == 0, "acoustic3d backward: null record cotangent");
     SWEEP_REQUIRE((illum_s == nullptr) == (illum_r == nullptr), "acoustic3d backward: pass both illuminations or neither");
+    const bool ckpt = mem_mode == SWEEP_MEM_CHECKPOINT;
     Params P = make_params(d);
     Carve c(ws);
-    Work w = carve(c, P, kRevFields);
+    // fields: 0-2 lambda, 3-14 adjoint CPML (psi x,y,z and zeta x,y,z, two
+    // buffers each), 15-17 reconstruction, 18-19 Kahan slots, 20-21
+    // illumination; checkpoint mode: 22-33 the forward set of the replay,
+    // then the strips of one chunk
+    Work w = carve(c, P, ckpt ? kRevFields + kFwdFields : kRevFields);
+    float* chunk = ckpt ? c.take<float>((long long)(ckpt_every + 1) * P.B * P.nstrip) : nullptr;
     const long long rows = (long long)d->nz * d->ny;
     prep3<<<592, 256, 0, st>>>(d->vp, (int)rows, d->nx, P.P, d->dt, w.cf, w.ca, w.vv);
     SWEEP_LAUNCH_CHECK();
     P.cf = w.cf; P.ca = w.ca; P.vv = w.vv;
     const long long n = (long long)P.B * P.S;
     const bool illum = illum_s != nullptr;
-    // fields: 0-2 lambda, 3-14 adjoint CPML (psi x,y,z and zeta x,y,z, two
-    // buffers each), 15-17 reconstruction, 18-19 Kahan slots, 20-21 illumination
     for (int i = 0; i < kRevFields; ++i) SWEEP_CUDA(cudaMemsetAsync(w.f[i], 0, n * 4, st));
     if (grad_w && d->nsrc > 0) SWEEP_CUDA(cudaMemsetAsync(grad_w, 0, (size_t)d->B * d->nsrc * d->nt * 4, st));
-    const float* strips = static_cast<const float*>(tape);
-    const float* last = tape_last(const_cast<void*>(tape), P);
-    SWEEP_CUDA(cudaMemcpyAsync(w.f[15], last + n, n * 4, cudaMemcpyDeviceToDevice, st));   // prev = U[nt]
-    SWEEP_CUDA(cudaMemcpyAsync(w.f[16], last, n * 4, cudaMemcpyDeviceToDevice, st));       // now  = U[nt-1]
     const dim3 grid = stencil_grid(P), block(BXC, BYC);
     const unsigned gs = blocks_for((long long)P.B * P.nsrc, 128), gr = blocks_for((long long)P.B * P.nrec, 128);
     const unsigned gst = blocks_for((long long)P.B * P.nstrip, 256);
-    int lp = 0, ln = 1, lx = 2, rp = 15, rn = 16, rx = 17, cur = 0;
+    int lp = 0, ln = 1, lx = 2, cur = 0;
     float* gacc = w.f[18];
     float* gcomp = w.f[19];
     float* is = illum ? w.f[20] : nullptr;
     float* ir = illum ? w.f[21] : nullptr;
-    for (int it = d->nt - 1; it >= 0; --it) {
-        float* a_in[6];
-        float* a_out[6];
-        for (int k = 0; k < 6; ++k) { a_in[k] = w.f[3 + 2 * k + cur]; a_out[k] = w.f[3 + 2 * k + 1 - cur]; }
-        A3 A{w.f[ln], w.f[lp], w.f[lx], a_in[0], a_in[1], a_in[2], a_in[3], a_in[4], a_in[5],
-             a_out[0], a_out[1], a_out[2], a_out[3], a_out[4], a_out[5]};
-        a3_step<<<grid, block, 0, st>>>(P, A);
-        SWEEP_LAUNCH_CHECK();
-        if (d->nrec > 0)
-            inject3<<<gr, 128, 0, st>>>(P, w.f[lx], adj, d->rec_loc, d->nrec, it, 1, 1.f, 0);
-        int t = lp; lp = ln; ln = lx; lx = t;
-        cur = 1 - cur;
-        if (grad_w && d->nsrc > 0)
-            gather3<<<gs, 128, 0, st>>>(P, w.f[ln], grad_w, d->src_loc, d->nsrc, it, 0);
-        if (it > 0) {
-            R3 R{w.f[rn], w.f[rp], w.f[rx], w.f[ln], gacc, gcomp, is, ir};
-            r3_recon<<<grid, block, 0, st>>>(P, R);
-            if (P.nstrip > 0) {
-                strips3<<<gst, 256, 0, st>>>(P, w.f[rx], const_cast<float*>(strips) + (long long)(it - 1) * P.B * P.nstrip, 1);
+    // Reverse steps [it0, it1) top down from prev = U[it1] (f[15]), now =
+    // U[it1 - 1] (f[16]); strips_of(t) holds the strips of U[t].
+    auto reverse = [&](int it0, int it1, auto strips_of) {
+        int rp = 15, rn = 16, rx = 17;
+        for (int it = it1 - 1; it >= it0; --it) {
+            float* a_in[6];
+            float* a_out[6];
+            for (int k = 0; k < 6; ++k) { a_in[k] = w.f[3 + 2 * k + cur]; a_out[k] = w.f[3 + 2 * k + 1 - cur]; }
+            A3 A{w.f[ln], w.f[lp], w.f[lx], a_in[0], a_in[1], a_in[2], a_in[3], a_in[4], a_in[5],
+                 a_out[0], a_out[1], a_out[2], a_out[3], a_out[4], a_out[5]};
+            a3_step<<<grid, block, 0, st>>>(P, A);
+            SWEEP_LAUNCH_CHECK();
+            if (d->nrec > 0)
+                inject3<<<gr, 128, 0, st>>>(P, w.f[lx], adj, d->rec_loc, d->nrec, it, 1, 1.f, 0);
+            int t = lp; lp = ln; ln = lx; lx = t;
+            cur = 1 - cur;
+            if (grad_w && d->nsrc > 0)
+                gather3<<<gs, 128, 0, st>>>(P, w.f[ln], grad_w, d->src_loc, d->nsrc, it, 0);
+            if (it > 0) {
+                R3 R{w.f[rn], w.f[rp], w.f[rx], w.f[ln], gacc, gcomp, is, ir};
+                r3_recon<<<grid, block, 0, st>>>(P, R);
+                if (P.nstrip > 0) {
+                    strips3<<<gst, 256, 0, st>>>(P, w.f[rx], strips_of(it - 1), 1);
+                    if (d->nsrc > 0)
+                        inject3<<<gs, 128, 0, st>>>(P, w.f[rx], d->wavelet, d->src_loc, d->nsrc, it, 0, -1.f, 1);
+                    Img I{w.f[rp], w.f[rn], w.f[rx], w.f[ln], gacc, gcomp, is, ir};
+                    strip_image3<<<gst, 256, 0, st>>>(P, I);
+                }
                 if (d->nsrc > 0)
-                    inject3<<<gs, 128, 0, st>>>(P, w.f[rx], d->wavelet, d->src_loc, d->nsrc, it, 0, -1.f, 1);
-                Img I{w.f[rp], w.f[rn], w.f[rx], w.f[ln], gacc, gcomp, is, ir};
-                strip_image3<<<gst, 256, 0, st>>>(P, I);
+                    inject3<<<gs, 128, 0, st>>>(P, w.f[rx], d->wavelet, d->src_loc, d->nsrc, it, 0, 1.f, 0);
+                SWEEP_LAUNCH_CHECK();
+                t = rp; rp = rn; rn = rx; rx = t;
+            } else if (illum) {
+                illum_tail3<<<592, 256, 0, st>>>(P, w.f[ln], ir);
+                SWEEP_LAUNCH_CHECK();
             }
-            if (d->nsrc > 0)
-                inject3<<<gs, 128, 0, st>>>(P, w.f[rx], d->wavelet, d->src_loc, d->nsrc, it, 0, 1.f, 0);
-            SWEEP_LAUNCH_CHECK();
-            t = rp; rp = rn; rn = rx; rx = t;
-        } else if (illum) {
-            illum_tail3<<<592, 256, 0, st>>>(P, w.f[ln], ir);
-            SWEEP_LAUNCH_CHECK();
+        }
+    };
+    if (!ckpt) {
+        float* strips = const_cast<float*>(static_cast<const float*>(tape));
+        const float* last = tape_last(const_cast<void*>(tape), P);
+        copy_dd(w.f[15], last + n, n, st);   // prev = U[nt]
+        copy_dd(w.f[16], last, n, st);       // now  = U[nt-1]
+        reverse(0, d->nt, [&](int t) { return strips + (long long)t * P.B * P.nstrip; });
+    } else {
+        const int k = ckpt_every, C = nchunks(P, k);
+        void* tp = const_cast<void*>(tape);
+        const long long cs = (long long)P.B * P.nstrip;
+        float* const* fw = w.f + kRevFields;
+        for (int ch = C - 1; ch >= 0; --ch) {
+            const int it0 = ch * k, it1 = std::min(d->nt, it0 + k);
+            FwdState S(fw);
+            float* state[kStateFields];
+            state_fields(S, state);
+            if (ch == 0) {
+                for (int f = 0; f < kStateFields; ++f) SWEEP_CUDA(cudaMemsetAsync(state[f], 0, n * 4, st));
+            } else {
+                for (int f = 0; f < kStateFields; ++f) copy_dd(state[f], ckpt_field(tp, P, ch, f), n, st);
+                copy_dd(chunk, ckpt_strips(tp, P, ch), cs, st);       // strips of U[it0 - 1]
+            }
+            // replay: chunk slot j holds the strips of U[it0 - 1 + j]
+            forward_steps(d, P, S, nullptr, it0, it1, [&](int it) { return chunk + (long long)(it - it0 + 1) * cs; }, st);
+            copy_dd(w.f[15], S.f[S.in], n, st);      // U[it1]
+            copy_dd(w.f[16], S.f[S.ip], n, st);      // U[it1 - 1]
+            reverse(it0, it1, [&](int t) { return chunk + (long long)(t - (it0 - 1)) * cs; });
         }
     }
     finalize3<<<592, 256, 0, st>>>(gacc, gcomp, is, ir, P.B, (int)rows, d->nx, P.P, P.S, grad_vp, illum_s, illum_r);

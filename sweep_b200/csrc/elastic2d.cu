@@ -370,7 +370,7 @@ __global__ void __launch_bounds__(NTH) fwd_str(FwdArgs A)
     }
     // receivers of this tile: read back the final values of the step
     const int r0 = G.rec.off[key], r1 = G.rec.off[key + 1];
-    if (r1 > r0) {
+    if (A.record && r1 > r0) {
         __syncthreads();
         for (int e = r0 + threadIdx.x + threadIdx.y * TX; e < r1; e += NTH) {
             const int2 ev = G.rec.ev[e];
@@ -897,6 +897,8 @@ struct RevWs {
     float *gvp, *gvs, *grho;
     char* zero0;
     char* zero1;
+    Slabs fmem;           // checkpoint mode: forward CPML memories of the replay
+    float* chunk;         // checkpoint mode: strips of one chunk, (k + 1, B, 5, nstrip)
 };
 
 static void carve_rev(Carve& c, const Plan& pl, RevWs& w)
@@ -916,6 +918,64 @@ static void carve_rev(Carve& c, const Plan& pl, RevWs& w)
     w.grho = c.take<float>((long long)pl.nslot * G.S);
     c.take<char>(0);
     w.zero1 = c.base ? c.base + c.off : nullptr;
+}
+
+static void carve_rev_ckpt(Carve& c, const Plan& pl, int k, RevWs& w)
+{
+    carve_rev(c, pl, w);
+    carve_slabs(c, pl.G, w.fmem);
+    w.chunk = c.take<float>((long long)(k + 1) * pl.G.B * 5 * pl.G.nstrip);
+}
+
+// Checkpointed boundary saving (SWEEP_MEM_CHECKPOINT, chunk length k): for
+// every chunk c >= 1 the tape holds the state after step c k - 1 -- the five
+// fields and the eight forward CPML memories -- and the strips of that step;
+// the backward replays each chunk from its checkpoint into the strips of that
+// chunk and runs the boundary-saving reverse steps over it (the reference's
+// staggered driver replays chunks as well, sg_driver.cuh:911-925).
+static long long slab_floats(const Geo& G)
+{
+    return 4LL * G.B * G.nz * G.WX + 4LL * G.B * G.WZ * G.P;
+}
+
+static long long ckpt_stride(const Plan& pl)
+{
+    Carve c(nullptr);
+    c.take<float>(5LL * pl.G.B * pl.G.S);
+    c.take<float>(slab_floats(pl.G));
+    c.take<float>((long long)pl.G.B * 5 * pl.G.nstrip);
+    return (c.off + 255) & ~255LL;
+}
+
+static int nchunks(const Plan& pl, int k) { return (pl.G.nt + k - 1) / k; }
+
+struct Ckpt {
+    float* f[5];
+    float* mem;           // the 8 slabs, x then z, in carve_slabs order
+    float* strips;
+};
+
+static Ckpt ckpt_at(void* tape, const Plan& pl, int ch)
+{
+    Carve c(static_cast<char*>(tape) + (long long)(ch - 1) * ckpt_stride(pl));
+    Ckpt k{};
+    for (int f = 0; f < 5; ++f) k.f[f] = c.take<float>((long long)pl.G.B * pl.G.S);
+    k.mem = c.take<float>(slab_floats(pl.G));
+    k.strips = c.take<float>((long long)pl.G.B * 5 * pl.G.nstrip);
+    return k;
+}
+
+// Copy the 8 slabs between a Slabs set and a packed checkpoint range.
+static void slabs_copy(const Slabs& s, float* packed, const Geo& G, bool to_packed, cudaStream_t st)
+{
+    long long o = 0;
+    for (int k = 0; k < 8; ++k) {
+        float* p = k < 4 ? s.x[k] : s.z[k - 4];
+        const long long cnt = k < 4 ? (long long)G.B * G.nz * G.WX : (long long)G.B * G.WZ * G.P;
+        if (to_packed) SWEEP_CUDA(cudaMemcpyAsync(packed + o, p, cnt * 4, cudaMemcpyDeviceToDevice, st));
+        else SWEEP_CUDA(cudaMemcpyAsync(p, packed + o, cnt * 4, cudaMemcpyDeviceToDevice, st));
+        o += cnt;
+    }
 }
 
 // tape: strips of every step (nt, B, 5, nstrip), then the final 5-field state
@@ -999,26 +1059,53 @@ constexpr size_t SM_REV_STR = 2 * HN * sizeof(float);
 constexpr size_t SM_REV_SADJ = 4 * HN * sizeof(float);
 constexpr size_t SM_REV_VADJ = 7 * HN * sizeof(float);
 
+static void check_mode(int mem_mode, int ckpt_every)
+{
+    SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY || mem_mode == SWEEP_MEM_CHECKPOINT,
+                  "elastic2d: unknown memory mode %d", mem_mode);
+    SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY || ckpt_every >= 1,
+                  "elastic2d: checkpoint interval must be >= 1 (got %d)", ckpt_every);
+}
+
 void sizes(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, int64_t* ws, int64_t* tape)
 {
-    SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY, "elastic2d: only boundary saving is built");
-    (void)ckpt_every;
+    check_mode(mem_mode, ckpt_every);
     Plan pl = make_plan(d);
     Carve cf(nullptr);
     FwdWs fw{};
     carve_fwd(cf, pl, fw);
     Carve cr(nullptr);
     RevWs rw{};
-    carve_rev(cr, pl, rw);
+    if (mem_mode == SWEEP_MEM_CHECKPOINT) {
+        carve_rev_ckpt(cr, pl, ckpt_every, rw);
+        *tape = (int64_t)std::max(nchunks(pl, ckpt_every) - 1, 1) * ckpt_stride(pl);
+    } else {
+        carve_rev(cr, pl, rw);
+        *tape = tape_bytes(pl);
+    }
     *ws = std::max(cf.off, cr.off);
-    *tape = tape_bytes(pl);
+}
+
+// Forward steps [it0, it1) on the fields / memories of A; strips_of(it) is
+// the strip slot of step it (null: none).
+template <class StripsOf>
+static void forward_steps(FwdArgs& A, int it0, int it1, StripsOf strips_of, cudaStream_t st)
+{
+    const Geo& G = A.G;
+    const dim3 grid(G.ntx * G.ntz, G.B), block(TX, 8);
+    for (int it = it0; it < it1; ++it) {
+        A.it = it;
+        A.strips = strips_of(it);
+        fwd_vel<<<grid, block, SM_FWD_VEL, st>>>(A);
+        fwd_str<<<grid, block, SM_FWD_STR, st>>>(A);
+    }
+    SWEEP_LAUNCH_CHECK();
 }
 
 void forward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, float* record, void* tape,
              void* ws, int64_t ws_bytes, cudaStream_t st)
 {
-    SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY, "elastic2d: only boundary saving is built");
-    (void)ckpt_every;
+    check_mode(mem_mode, ckpt_every);
     SWEEP_REQUIRE(record != nullptr || d->nrec == 0, "elastic2d forward: null record");
     Plan pl = make_plan(d);
     Carve c(ws);
@@ -1037,44 +1124,53 @@ void forward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, float* r
     A.mem = w.mem;
     A.record = record;
     const Geo& G = pl.G;
-    const dim3 grid(G.ntx * G.ntz, G.B), block(TX, 8);
-    float* strips = static_cast<float*>(tape);
-    for (int it = 0; it < G.nt; ++it) {
-        A.it = it;
-        A.strips = strips ? strips + (long long)it * G.B * 5 * G.nstrip : nullptr;
-        fwd_vel<<<grid, block, SM_FWD_VEL, st>>>(A);
-        fwd_str<<<grid, block, SM_FWD_STR, st>>>(A);
+    const long long n = (long long)G.B * G.S;
+    if (mem_mode == SWEEP_MEM_BOUNDARY) {
+        float* strips = static_cast<float*>(tape);
+        forward_steps(A, 0, G.nt, [&](int it) { return strips ? strips + (long long)it * G.B * 5 * G.nstrip : nullptr; },
+                      st);
+        if (tape) {
+            float* last = tape_last(tape, pl);
+            for (int k = 0; k < 5; ++k)
+                SWEEP_CUDA(cudaMemcpyAsync(last + k * n, w.f[k], sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+        }
+        return;
     }
-    SWEEP_LAUNCH_CHECK();
-    if (tape) {
-        float* last = tape_last(tape, pl);
-        for (int k = 0; k < 5; ++k)
-            SWEEP_CUDA(cudaMemcpyAsync(last + (long long)k * G.B * G.S, w.f[k], sizeof(float) * G.B * G.S,
-                                       cudaMemcpyDeviceToDevice, st));
+    const int k = ckpt_every, C = nchunks(pl, k);
+    for (int ch = 0; ch < C; ++ch) {
+        const int it0 = ch * k, it1 = std::min(G.nt, it0 + k);
+        if (tape && ch >= 1) {
+            const Ckpt cp = ckpt_at(tape, pl, ch);
+            for (int f = 0; f < 5; ++f)
+                SWEEP_CUDA(cudaMemcpyAsync(cp.f[f], w.f[f], sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+            slabs_copy(w.mem, cp.mem, G, true, st);
+        }
+        // the last step of a chunk keeps its strips with the next checkpoint
+        forward_steps(A, it0, it1,
+                      [&](int it) { return (tape && it == it1 - 1 && ch + 1 < C) ? ckpt_at(tape, pl, ch + 1).strips : nullptr; },
+                      st);
     }
 }
 
 void backward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, const float* adj, const void* tape,
               float* grad_vp, float* grad_vs, float* grad_rho, void* ws, int64_t ws_bytes, cudaStream_t st)
 {
-    SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY, "elastic2d: only boundary saving is built");
-    (void)ckpt_every;
+    check_mode(mem_mode, ckpt_every);
     SWEEP_REQUIRE(tape != nullptr, "elastic2d backward: null tape");
     SWEEP_REQUIRE(grad_vp && grad_vs && grad_rho, "elastic2d backward: null gradient output");
     SWEEP_REQUIRE(adj != nullptr || d->nrec == 0, "elastic2d backward: null adjoint source");
+    const bool ckpt = mem_mode == SWEEP_MEM_CHECKPOINT;
     Plan pl = make_plan(d);
     Carve c(ws);
     RevWs w{};
-    carve_rev(c, pl, w);
+    if (ckpt) carve_rev_ckpt(c, pl, ckpt_every, w);
+    else carve_rev(c, pl, w);
     SWEEP_REQUIRE(ws != nullptr && c.off <= ws_bytes, "elastic2d backward: workspace too small (%lld < %lld bytes)",
                   (long long)ws_bytes, (long long)c.off);
     SWEEP_CUDA(cudaMemsetAsync(w.zero0, 0, w.zero1 - w.zero0, st));
     setup_common(d, pl, w.cm, st);
     const Geo& G = pl.G;
-    const float* last = tape_last(const_cast<void*>(tape), pl);
-    for (int k = 0; k < 5; ++k)
-        SWEEP_CUDA(cudaMemcpyAsync(w.f[k], last + (long long)k * G.B * G.S, sizeof(float) * G.B * G.S,
-                                   cudaMemcpyDeviceToDevice, st));
+    const long long n = (long long)G.B * G.S;
     RevArgs A{};
     A.G = G;
     A.m = models_of(w.cm);
@@ -1085,19 +1181,59 @@ void backward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, const f
     A.G_shots = pl.gshots;
     const dim3 block(TX, 8);
     const dim3 grid_s(G.ntx * G.ntz, pl.nslot), grid_b(G.ntx * G.ntz, G.B);
-    const float* strips = static_cast<const float*>(tape);
     int cur = 0;
-    for (int it = G.nt - 1; it >= 1; --it) {
-        A.it = it;
-        A.strips = strips + (long long)(it - 1) * G.B * 5 * G.nstrip;
-        A.mo = w.m[cur];
-        A.mn = w.m[cur ^ 1];
-        rev_str<<<grid_s, block, SM_REV_STR, st>>>(A);
-        rev_sadj<<<grid_b, block, SM_REV_SADJ, st>>>(A);
-        rev_vadj<<<grid_b, block, SM_REV_VADJ, st>>>(A);
-        cur ^= 1;
+    // Reverse steps it1 - 1 .. max(it0, 1) (the staggered reverse has no
+    // it = 0 step) on the reconstruction state after step it1 - 1;
+    // strips_of(t) holds the strips of the state after step t.
+    auto reverse = [&](int it0, int it1, auto strips_of) {
+        for (int it = it1 - 1; it >= std::max(it0, 1); --it) {
+            A.it = it;
+            A.strips = strips_of(it - 1);
+            A.mo = w.m[cur];
+            A.mn = w.m[cur ^ 1];
+            rev_str<<<grid_s, block, SM_REV_STR, st>>>(A);
+            rev_sadj<<<grid_b, block, SM_REV_SADJ, st>>>(A);
+            rev_vadj<<<grid_b, block, SM_REV_VADJ, st>>>(A);
+            cur ^= 1;
+        }
+        SWEEP_LAUNCH_CHECK();
+    };
+    if (!ckpt) {
+        const float* strips = static_cast<const float*>(tape);
+        const float* last = tape_last(const_cast<void*>(tape), pl);
+        for (int k = 0; k < 5; ++k)
+            SWEEP_CUDA(cudaMemcpyAsync(w.f[k], last + k * n, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+        reverse(0, G.nt, [&](int t) { return strips + (long long)t * G.B * 5 * G.nstrip; });
+    } else {
+        const int k = ckpt_every, C = nchunks(pl, k);
+        void* tp = const_cast<void*>(tape);
+        const long long cs = (long long)G.B * 5 * G.nstrip;
+        FwdArgs F{};
+        F.G = G;
+        F.m = A.m;
+        for (int f = 0; f < 5; ++f) F.f[f] = w.f[f];     // replay straight into the reconstruction fields
+        F.mem = w.fmem;
+        F.record = nullptr;
+        for (int ch = C - 1; ch >= 0; --ch) {
+            const int it0 = ch * k, it1 = std::min(G.nt, it0 + k);
+            if (ch == 0) {
+                for (int f = 0; f < 5; ++f) SWEEP_CUDA(cudaMemsetAsync(w.f[f], 0, sizeof(float) * n, st));
+                for (int s2 = 0; s2 < 4; ++s2) {
+                    SWEEP_CUDA(cudaMemsetAsync(w.fmem.x[s2], 0, sizeof(float) * G.B * G.nz * G.WX, st));
+                    SWEEP_CUDA(cudaMemsetAsync(w.fmem.z[s2], 0, sizeof(float) * G.B * G.WZ * G.P, st));
+                }
+            } else {
+                const Ckpt cp = ckpt_at(tp, pl, ch);
+                for (int f = 0; f < 5; ++f)
+                    SWEEP_CUDA(cudaMemcpyAsync(w.f[f], cp.f[f], sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+                slabs_copy(w.fmem, cp.mem, G, false, st);
+                SWEEP_CUDA(cudaMemcpyAsync(w.chunk, cp.strips, sizeof(float) * cs, cudaMemcpyDeviceToDevice, st));
+            }
+            // replay: chunk slot j holds the strips after step it0 - 1 + j
+            forward_steps(F, it0, it1, [&](int it) { return w.chunk + (long long)(it - it0 + 1) * cs; }, st);
+            reverse(it0, it1, [&](int t) { return (const float*)w.chunk + (long long)(t - (it0 - 1)) * cs; });
+        }
     }
-    SWEEP_LAUNCH_CHECK();
     const int per_shot = G.ms != 0;
     finalize_kernel<<<592, 256, 0, st>>>(w.gvp, pl.nslot, per_shot, G, grad_vp);
     finalize_kernel<<<592, 256, 0, st>>>(w.gvs, pl.nslot, per_shot, G, grad_vs);

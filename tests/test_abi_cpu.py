@@ -109,3 +109,29 @@ def test_elastic_sizes_and_errors():
     d = _edesc(M=2)
     with pytest.raises(RuntimeError, match="order 8"):
         _lib.call("sweep_b200_elastic_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
+
+
+@pytest.mark.parametrize("kind", ["acoustic2d", "acoustic3d", "elastic2d"])
+def test_checkpoint_tape_is_smaller_for_long_runs(kind):
+    """A long run's checkpoint tape (state every k steps) is a fraction of the
+    boundary-saving tape (strips every step); the workspace grows by the
+    replay set and one chunk of strips."""
+    from sweep_b200 import _lib
+    nt = 4000
+    if kind == "elastic2d":
+        d = _edesc(nz=120, nx=160, nt=nt)
+        fn = "sweep_b200_elastic_sizes"
+    else:
+        d = _desc(nz=120, nx=160, nt=nt)
+        if kind == "acoustic3d":
+            d.ndim, d.ny = 3, 48
+            for i in range(6):
+                d.pad[i] = 5
+        fn = "sweep_b200_acoustic_sizes"
+    ws_b, tape_b, ws_c, tape_c = _lib.c_i64(), _lib.c_i64(), _lib.c_i64(), _lib.c_i64()
+    _lib.call(fn, d, _lib.MEM_BOUNDARY, 0, ws_b, tape_b)
+    _lib.call(fn, d, _lib.MEM_CHECKPOINT, 500, ws_c, tape_c)
+    assert tape_c.value < tape_b.value
+    assert ws_c.value > ws_b.value
+    with pytest.raises(RuntimeError, match="interval"):
+        _lib.call(fn, d, _lib.MEM_CHECKPOINT, 0, ws_c, tape_c)
