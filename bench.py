@@ -322,7 +322,11 @@ class Acoustic3DWorkload:
         return solver, m_true, m_init, w, src, rec
 
     def launches(self):
-        return (A3_NSHOT // A3_BATCH) * 7 * self.nt
+        # per call: forward 4 per step (stencil, strips, injection, gather) and
+        # reverse 7 (adjoint, cotangent injection, reconstruction, strip
+        # restore, strip un-injection, strip image, source re-injection), prep
+        # and finalize
+        return -(-self.nshot // self.batch) * (11 * self.nt + 3)
 
     def cpu_run(self, nt_sample, shots=1):
         from oracle import oracle as O
@@ -389,6 +393,7 @@ def run_gpu(args, wl):
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
 
     solver, m_true, m_init, w, src, rec = wl.build(dev)
+    src, rec = src[:wl.nshot], rec[:wl.nshot]
     w_d = torch.tensor(w, device=dev)
     bsz = getattr(wl, "batch", wl.nshot)
     batches = [slice(b, min(b + bsz, wl.nshot)) for b in range(0, wl.nshot, bsz)]
@@ -542,12 +547,18 @@ def main():
                          "400x1200 elastic survey")
     ap.add_argument("--nt", type=int, default=None,
                     help="shorter time axis (profiling captures only; the bench line is for the full nt)")
+    ap.add_argument("--shots", type=int, default=None,
+                    help="fewer shots (profiling captures of a few GB only; the bench line is for the full survey)")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]()
     if args.nt:
         wl.nt = int(args.nt)
         global NT, E_NT, A3_NT
         NT, E_NT, A3_NT = wl.nt, wl.nt, wl.nt
+    if args.shots:
+        wl.nshot = min(int(args.shots), wl.nshot)
+        if hasattr(wl, "batch"):
+            wl.batch = min(wl.batch, wl.nshot)
     if args.impl == "reference":
         run_reference(args, wl)
     else:

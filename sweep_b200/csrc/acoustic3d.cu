@@ -168,7 +168,7 @@ struct F3 {
 // The CPML branch of an axis runs on its band plus one cell (reference
 // forward_split.cu:150-156) and uses the product-rule split
 // tmp = (((1 + b) Lap + db du) + a dpsi) + da psi (forward_split.cu:171-172).
-__global__ void __launch_bounds__(NTH) f3_step(const Params P, const F3 F)
+__global__ void __launch_bounds__(NTH, 4) f3_step(const Params P, const F3 F)
 {
     __shared__ float pl[2][PN];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BXC + tx;
@@ -419,7 +419,7 @@ __device__ __forceinline__ void adj_axis(const Params& P, const float* __restric
 // pure interior  2 l - l_prev + Lap(gw) (difference form around gw);
 // shell          per axis outside the clear box the transposed CPML terms,
 //                inside it the bare Laplacian of gw.
-__global__ void __launch_bounds__(NTH) a3_step(const Params P, const A3 A)
+__global__ void __launch_bounds__(NTH, 4) a3_step(const Params P, const A3 A)
 {
     __shared__ float pl[2][PN];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BXC + tx;
@@ -519,7 +519,7 @@ struct R3 {
 // u(it-1) = 2 u(it) - u(it+1) + vp^2 dt^2 Lap u(it) on the reconstruction box
 // (the physical box minus the restored strips) with the fused vp image
 // 2 dt^2 u_tt lambda(it) / vp (reference forward_split.cu:292-372).
-__global__ void __launch_bounds__(NTH) r3_recon(const Params P, const R3 R)
+__global__ void __launch_bounds__(NTH, 4) r3_recon(const Params P, const R3 R)
 {
     __shared__ float pl[2][PN];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BXC + tx;
@@ -660,9 +660,11 @@ static Params make_params(const sweep_acoustic_desc* d)
     P.nstrip = P.n_top + P.n_bot + bzi * P.nring;
     P.az = d->az; P.bz = d->bz; P.dbz = d->dbz; P.ay = d->ay; P.by = d->by; P.dby = d->dby;
     P.ax = d->ax; P.bx = d->bx; P.dbx = d->dbx;
-    // z chunks: enough CTAs to fill the GPU twice, chunks of at least 16 planes
+    // z chunks: enough CTAs for two waves at 4 CTAs per SM (the stencil
+    // kernels are capped at 64 registers for that occupancy), chunks of at
+    // least 16 planes
     const long long cols = (long long)((d->nx + BXC - 1) / BXC) * ((d->ny + BYC - 1) / BYC) * d->B;
-    int nzc = (int)std::max(1LL, (2LL * 148 + cols - 1) / cols);
+    int nzc = (int)std::max(1LL, (2LL * 4 * 148 + cols - 1) / cols);
     nzc = std::max(1, std::min(nzc, d->nz / 16));
     P.zc = (d->nz + nzc - 1) / nzc;
     P.nzc = (d->nz + P.zc - 1) / P.zc;
