@@ -228,7 +228,7 @@ enum { XM_VXX = 0, XM_VZX = 1, XM_SXXX = 2, XM_SXZX = 3 };
 enum { ZM_VZZ = 0, ZM_VXZ = 1, ZM_SZZZ = 2, ZM_SXZZ = 3 };
 
 // Velocity step (reference kernels.cuh:48-138).
-__global__ void __launch_bounds__(NTH) fwd_vel(FwdArgs A)
+__global__ void __launch_bounds__(NTH, 6) fwd_vel(FwdArgs A)
 {
     extern __shared__ float sm[];
     float *tsxx = sm, *tszz = sm + HN, *tsxz = sm + 2 * HN;
@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(NTH) fwd_vel(FwdArgs A)
 // step's point work for the cells this CTA owns: source injection into the
 // stress source fields, the 5-field strip save and the receiver gather
 // (reference sg_driver.cuh:300-340 order: inject, save, record).
-__global__ void __launch_bounds__(NTH) fwd_str(FwdArgs A)
+__global__ void __launch_bounds__(NTH, 6) fwd_str(FwdArgs A)
 {
     extern __shared__ float sm[];
     float *tvx = sm, *tvz = sm + HN;
@@ -408,7 +408,7 @@ struct RevArgs {
 // fused vp / vs / rho imaging on the physical box (kernels.cuh:601-663) and
 // the receiver rho correction (common.cu:77-117).  The gradient contributions
 // of the CTA's shots are summed in registers and added to slot blockIdx.y.
-__global__ void __launch_bounds__(NTH) rev_str(RevArgs A)
+__global__ void __launch_bounds__(NTH, 4) rev_str(RevArgs A)
 {
     extern __shared__ float sm[];
     float *tvx = sm, *tvz = sm + HN;
@@ -554,7 +554,7 @@ __device__ __forceinline__ bool owns(int lz, int lx)
 // qxz, qzx) of the stress-adjoint prepare (kernels.cuh:676-750) built in
 // shared memory for the tile and its halo.  The owner of a cell writes its new
 // adjoint CPML memories.
-__global__ void __launch_bounds__(NTH) rev_sadj(RevArgs A)
+__global__ void __launch_bounds__(NTH, 4) rev_sadj(RevArgs A)
 {
     extern __shared__ float sm[];
     float* tq[4] = {sm, sm + HN, sm + 2 * HN, sm + 3 * HN};
@@ -635,7 +635,7 @@ __global__ void __launch_bounds__(NTH) rev_sadj(RevArgs A)
 // in shared memory, then the reverse velocity half of the forward
 // reconstruction: carrier capture of v(it) on the box, the NOPML velocity
 // step (kernels.cuh:365-401) and the velocity strip restore of step it - 1.
-__global__ void __launch_bounds__(NTH) rev_vadj(RevArgs A)
+__global__ void __launch_bounds__(NTH, 4) rev_vadj(RevArgs A)
 {
     extern __shared__ float sm[];
     float* tp[4] = {sm, sm + HN, sm + 2 * HN, sm + 3 * HN};
