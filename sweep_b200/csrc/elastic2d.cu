@@ -42,6 +42,7 @@
 
 #include "common.cuh"
 #include "elastic2d.cuh"
+#include "tma.cuh"
 
 namespace sweep {
 namespace el2d {
@@ -75,7 +76,12 @@ struct Geo {
     long long ms;                   // model stride between shots (0 or S)
     EventTable src, rec;
     const float* wavelet;           // (B, nsrc, nt)
+    int gf;                         // shots per CTA of the forward kernels
+    int* err;                       // bounded-wait failure flag (0 = none)
 };
+
+enum { ERR_WAIT_FWD = 1, ERR_WAIT_REV = 2 };
+constexpr int CN = TX * TZ;         // floats of a centre tile
 
 // Models on the pitched grid, one copy (shared) or B copies (per shot).
 struct Models {
@@ -227,60 +233,168 @@ struct FwdArgs {
 enum { XM_VXX = 0, XM_VZX = 1, XM_SXXX = 2, XM_SXZX = 3 };
 enum { ZM_VZZ = 0, ZM_VXZ = 1, ZM_SZZZ = 2, ZM_SXZZ = 3 };
 
-// Velocity step (reference kernels.cuh:48-138).
-__global__ void __launch_bounds__(NTH, 6) fwd_vel(FwdArgs A)
+// Does tile (tz0, tx0) reach the CPML band (pad + M per face)?
+__device__ __forceinline__ bool tile_in_pml(const Geo& G, int tz0, int tx0)
 {
-    extern __shared__ float sm[];
-    float *tsxx = sm, *tszz = sm + HN, *tsxz = sm + 2 * HN;
-    const Geo& G = A.G;
-    const int b = blockIdx.y;
-    int tz0, tx0;
-    tile_origin(G, blockIdx.x, tz0, tx0);
-    const long long so = (long long)b * G.S;
-    {
-        float* const t[3] = {tsxx, tszz, tsxz};
-        const float* const g[3] = {A.f[SXX] + so, A.f[SZZ] + so, A.f[SXZ] + so};
-        load_tiles<3>(t, g, G, tz0, tx0);
+    return tx0 < G.XL || tx0 + TX > G.nx - G.XH || tz0 < G.ZL || tz0 + TZ > G.nz - G.ZH;
+}
+
+// Two CPML memories of one axis at one cell: their slab offset (-1: the cell
+// has no memory on that axis) and old values.
+struct MemPair {
+    long long at;
+    float a, b;
+};
+
+__device__ __forceinline__ MemPair load_mem_z(const Geo& G, const Slabs& m, int k0, int k1, int b, int iz, int ix)
+{
+    MemPair p{-1, 0.f, 0.f};
+    if (iz >= G.nz || ix >= G.nx || !in_pml(G, ix, iz)) return p;
+    const int zs = zslab(G, iz);
+    if (zs < 0) return p;
+    p.at = ((long long)b * G.WZ + zs) * G.P + ix;
+    p.a = m.z[k0][p.at];
+    p.b = m.z[k1][p.at];
+    return p;
+}
+
+__device__ __forceinline__ MemPair load_mem_x(const Geo& G, const Slabs& m, int k0, int k1, int b, int iz, int ix)
+{
+    MemPair p{-1, 0.f, 0.f};
+    if (iz >= G.nz || ix >= G.nx || !in_pml(G, ix, iz)) return p;
+    const int xs = xslab(G, ix);
+    if (xs < 0) return p;
+    p.at = ((long long)b * G.nz + iz) * G.WX + xs;
+    p.a = m.x[k0][p.at];
+    p.b = m.x[k1][p.at];
+    return p;
+}
+
+// TMA tensor maps of the five wavefields: (HX x HZ) boxes for the stencil
+// inputs with their halo, (TX x TZ) boxes for the centre tiles.
+struct FwdMaps {
+    CUtensorMap halo[5];
+    CUtensorMap tile[5];
+};
+
+// Shared memory of the forward kernels: two pipeline stages, each holding
+// one shot's halo'd stencil inputs and centre tiles.
+template <int NH, int NC>
+struct StageSmem {
+    float h[2][NH][HN];
+    float c[2][NC][CN];
+    uint64_t bar[2];
+};
+using VelSmem = StageSmem<3, 2>;   // sxx, szz, sxz halos; vx, vz centres
+using StrSmem = StageSmem<2, 3>;   // vx, vz halos; sxx, szz, sxz centres
+
+// One CTA = one tile for G shots.  Thread 0 issues each shot's TMA loads into
+// a 2-stage mbarrier pipeline, so shot g+1's tiles are in flight while shot g
+// computes; every wait is bounded and sets the call's error flag.
+template <int NH, int NC, class Issue>
+__device__ __forceinline__ void pipeline_start(StageSmem<NH, NC>& sm, int nloc, int b0, Issue issue)
+{
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        tma::mbar_init(&sm.bar[0], 1);
+        tma::mbar_init(&sm.bar[1], 1);
+        tma::fence_barrier_init();
     }
     __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        issue(0, b0);
+        if (nloc > 1) issue(1, b0 + 1);
+    }
+}
+
+// After a failed wait on shot g's stage: wait (bounded) for the copies this
+// CTA still has in flight -- shot g's and, if issued, shot g+1's -- then exit.
+template <int NH, int NC>
+__device__ __forceinline__ void drain(StageSmem<NH, NC>& sm, int g, int nloc, int* err, int code)
+{
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        tma::mbar_wait(&sm.bar[g & 1], (g >> 1) & 1, err, code);
+        if (g + 1 < nloc) tma::mbar_wait(&sm.bar[(g + 1) & 1], ((g + 1) >> 1) & 1, err, code);
+    }
+}
+
+// Velocity step (reference kernels.cuh:48-138).
+__global__ void __launch_bounds__(NTH, 4) fwd_vel(const __grid_constant__ FwdMaps MP, FwdArgs A)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    VelSmem& sm = *reinterpret_cast<VelSmem*>(smem_raw);
+    const Geo& G = A.G;
+    int tz0, tx0;
+    tile_origin(G, blockIdx.x, tz0, tx0);
+    const int b0 = blockIdx.y * G.gf, nloc = min(G.gf, G.B - b0);
+    constexpr uint32_t kBytes = (3 * HN + 2 * CN) * 4;
+    auto issue = [&](int s, int b) {
+        tma::mbar_expect_tx(&sm.bar[s], kBytes);
+        for (int f = 0; f < 3; ++f) tma::load_3d(sm.h[s][f], &MP.halo[SXX + f], &sm.bar[s], tx0 - M, tz0 - M, b);
+        for (int f = 0; f < 2; ++f) tma::load_3d(sm.c[s][f], &MP.tile[VX + f], &sm.bar[s], tx0, tz0, b);
+    };
+    pipeline_start(sm, nloc, b0, issue);
     const int lx = threadIdx.x, ix = tx0 + lx;
-    const float* __restrict__ bv = A.m.bv + (long long)b * G.ms;
+    // dt / rho of this thread's cells (a shared model: once for every shot)
+    float bvr[RPT];
 #pragma unroll
     for (int r = 0; r < RPT; ++r) {
-        const int lz = threadIdx.y + 8 * r, iz = tz0 + lz;
-        if (!in_core(G, ix, iz)) continue;
-        const int c = (lz + M) * HX + lx + M;
-        float dsxx_dx = dpx(tsxx, c, G.idx);
-        float dsxz_dz = dmz(tsxz, c, G.idz);
-        float dsxz_dx = dmx(tsxz, c, G.idx);
-        float dszz_dz = dpz(tszz, c, G.idz);
-        const long long i = (long long)iz * G.P + ix;
-        if (in_pml(G, ix, iz)) {
-            const int xs = xslab(G, ix), zs = zslab(G, iz);
-            if (zs >= 0) {
-                const long long zi = ((long long)b * G.WZ + zs) * G.P + ix;
-                float m = G.azh[iz] * A.mem.z[ZM_SZZZ][zi] + G.bzh[iz] * dszz_dz;
-                A.mem.z[ZM_SZZZ][zi] = m; dszz_dz += m;
-            }
-            if (xs >= 0) {
-                const long long xi = ((long long)b * G.nz + iz) * G.WX + xs;
-                float m = G.ax[ix] * A.mem.x[XM_SXZX][xi] + G.bx[ix] * dsxz_dx;
-                A.mem.x[XM_SXZX][xi] = m; dsxz_dx += m;
-            }
-            if (zs >= 0) {
-                const long long zi = ((long long)b * G.WZ + zs) * G.P + ix;
-                float m = G.az[iz] * A.mem.z[ZM_SXZZ][zi] + G.bz[iz] * dsxz_dz;
-                A.mem.z[ZM_SXZZ][zi] = m; dsxz_dz += m;
-            }
-            if (xs >= 0) {
-                const long long xi = ((long long)b * G.nz + iz) * G.WX + xs;
-                float m = G.axh[ix] * A.mem.x[XM_SXXX][xi] + G.bxh[ix] * dsxx_dx;
-                A.mem.x[XM_SXXX][xi] = m; dsxx_dx += m;
+        const int iz = tz0 + threadIdx.y + 8 * r;
+        bvr[r] = in_core(G, ix, iz) ? A.m.bv[(long long)b0 * G.ms + (long long)iz * G.P + ix] : 0.f;
+    }
+    const bool ring = tile_in_pml(G, tz0, tx0);
+    for (int g = 0; g < nloc; ++g) {
+        const int b = b0 + g, s = g & 1;
+        // the CPML memories of this thread's cells, loaded while the tiles arrive
+        MemPair mz[RPT], mx[RPT];
+        if (ring) {
+#pragma unroll
+            for (int r = 0; r < RPT; ++r) {
+                const int iz = tz0 + threadIdx.y + 8 * r;
+                mz[r] = load_mem_z(G, A.mem, ZM_SZZZ, ZM_SXZZ, b, iz, ix);
+                mx[r] = load_mem_x(G, A.mem, XM_SXZX, XM_SXXX, b, iz, ix);
             }
         }
-        const float k = bv[i];
-        A.f[VX][so + i] += k * (dsxx_dx + dsxz_dz);
-        A.f[VZ][so + i] += k * (dsxz_dx + dszz_dz);
+        const bool ok = tma::mbar_wait(&sm.bar[s], (g >> 1) & 1, G.err, ERR_WAIT_FWD);
+        if (__syncthreads_or(!ok)) {
+            drain(sm, g, nloc, G.err, ERR_WAIT_FWD);
+            return;
+        }
+        const float *tsxx = sm.h[s][0], *tszz = sm.h[s][1], *tsxz = sm.h[s][2];
+        const long long so = (long long)b * G.S;
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            const int lz = threadIdx.y + 8 * r, iz = tz0 + lz;
+            if (!in_core(G, ix, iz)) continue;
+            const int c = (lz + M) * HX + lx + M;
+            float dsxx_dx = dpx(tsxx, c, G.idx);
+            float dsxz_dz = dmz(tsxz, c, G.idz);
+            float dsxz_dx = dmx(tsxz, c, G.idx);
+            float dszz_dz = dpz(tszz, c, G.idz);
+            const long long i = (long long)iz * G.P + ix;
+            if (ring && in_pml(G, ix, iz)) {
+                if (mz[r].at >= 0) {
+                    float m0 = G.azh[iz] * mz[r].a + G.bzh[iz] * dszz_dz;
+                    dszz_dz += m0;
+                    float m1 = G.az[iz] * mz[r].b + G.bz[iz] * dsxz_dz;
+                    dsxz_dz += m1;
+                    A.mem.z[ZM_SZZZ][mz[r].at] = m0;
+                    A.mem.z[ZM_SXZZ][mz[r].at] = m1;
+                }
+                if (mx[r].at >= 0) {
+                    float m0 = G.ax[ix] * mx[r].a + G.bx[ix] * dsxz_dx;
+                    dsxz_dx += m0;
+                    float m1 = G.axh[ix] * mx[r].b + G.bxh[ix] * dsxx_dx;
+                    dsxx_dx += m1;
+                    A.mem.x[XM_SXZX][mx[r].at] = m0;
+                    A.mem.x[XM_SXXX][mx[r].at] = m1;
+                }
+            }
+            const int cc = lz * TX + lx;
+            A.f[VX][so + i] = sm.c[s][0][cc] + bvr[r] * (dsxx_dx + dsxz_dz);
+            A.f[VZ][so + i] = sm.c[s][1][cc] + bvr[r] * (dsxz_dx + dszz_dz);
+        }
+        __syncthreads();                       // every thread is done with stage s
+        if (threadIdx.x == 0 && threadIdx.y == 0 && g + 2 < nloc) issue(s, b + 2);
     }
 }
 
@@ -288,97 +402,124 @@ __global__ void __launch_bounds__(NTH, 6) fwd_vel(FwdArgs A)
 // step's point work for the cells this CTA owns: source injection into the
 // stress source fields, the 5-field strip save and the receiver gather
 // (reference sg_driver.cuh:300-340 order: inject, save, record).
-__global__ void __launch_bounds__(NTH, 6) fwd_str(FwdArgs A)
+__global__ void __launch_bounds__(NTH, 4) fwd_str(const __grid_constant__ FwdMaps MP, FwdArgs A)
 {
-    extern __shared__ float sm[];
-    float *tvx = sm, *tvz = sm + HN;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    StrSmem& sm = *reinterpret_cast<StrSmem*>(smem_raw);
     const Geo& G = A.G;
-    const int b = blockIdx.y, tile = blockIdx.x;
+    const int tile = blockIdx.x;
     int tz0, tx0;
     tile_origin(G, tile, tz0, tx0);
-    const long long so = (long long)b * G.S;
-    {
-        float* const t[2] = {tvx, tvz};
-        const float* const g[2] = {A.f[VX] + so, A.f[VZ] + so};
-        load_tiles<2>(t, g, G, tz0, tx0);
-    }
-    const int key = b * G.ntx * G.ntz + tile;
-    const int s0 = G.src.off[key], s1 = G.src.off[key + 1];
-    __syncthreads();
+    const int b0 = blockIdx.y * G.gf, nloc = min(G.gf, G.B - b0);
+    constexpr uint32_t kBytes = (2 * HN + 3 * CN) * 4;
+    auto issue = [&](int s, int b) {
+        tma::mbar_expect_tx(&sm.bar[s], kBytes);
+        for (int f = 0; f < 2; ++f) tma::load_3d(sm.h[s][f], &MP.halo[VX + f], &sm.bar[s], tx0 - M, tz0 - M, b);
+        for (int f = 0; f < 3; ++f) tma::load_3d(sm.c[s][f], &MP.tile[SXX + f], &sm.bar[s], tx0, tz0, b);
+    };
+    pipeline_start(sm, nloc, b0, issue);
     const int lx = threadIdx.x, ix = tx0 + lx;
-    const float* __restrict__ lam_ = A.m.lam + (long long)b * G.ms;
-    const float* __restrict__ mu_ = A.m.mu + (long long)b * G.ms;
+    float lamr[RPT], mur[RPT];
 #pragma unroll
     for (int r = 0; r < RPT; ++r) {
-        const int lz = threadIdx.y + 8 * r, iz = tz0 + lz;
-        if (iz >= G.nz || ix >= G.nx) continue;
-        const int c = (lz + M) * HX + lx + M;
-        const long long i = (long long)iz * G.P + ix;
-        float sxx = A.f[SXX][so + i], szz = A.f[SZZ][so + i], sxz = A.f[SXZ][so + i];
-        if (in_core(G, ix, iz)) {
-            float dvx_dx = dmx(tvx, c, G.idx);
-            float dvz_dz = dmz(tvz, c, G.idz);
-            float dvx_dz = dpz(tvx, c, G.idz);
-            float dvz_dx = dpx(tvz, c, G.idx);
-            const float lam = lam_[i], mu = mu_[i];
-            const bool pml = in_pml(G, ix, iz);
-            const int xs = pml ? xslab(G, ix) : -1, zs = pml ? zslab(G, iz) : -1;
-            const long long zi = ((long long)b * G.WZ + zs) * G.P + ix;
-            const long long xi = ((long long)b * G.nz + iz) * G.WX + xs;
-            if (zs >= 0) {
-                float m = G.az[iz] * A.mem.z[ZM_VZZ][zi] + G.bz[iz] * dvz_dz;
-                A.mem.z[ZM_VZZ][zi] = m; dvz_dz += m;
-            }
-            if (xs >= 0) {
-                float m = G.ax[ix] * A.mem.x[XM_VXX][xi] + G.bx[ix] * dvx_dx;
-                A.mem.x[XM_VXX][xi] = m; dvx_dx += m;
-            }
-            sxx += G.dt * ((lam + 2.f * mu) * dvx_dx + lam * dvz_dz);
-            szz += G.dt * ((lam + 2.f * mu) * dvz_dz + lam * dvx_dx);
-            if (zs >= 0) {
-                float m = G.azh[iz] * A.mem.z[ZM_VXZ][zi] + G.bzh[iz] * dvx_dz;
-                A.mem.z[ZM_VXZ][zi] = m; dvx_dz += m;
-            }
-            if (xs >= 0) {
-                float m = G.axh[ix] * A.mem.x[XM_VZX][xi] + G.bxh[ix] * dvz_dx;
-                A.mem.x[XM_VZX][xi] = m; dvz_dx += m;
-            }
-            sxz += G.dt * mu * (dvx_dz + dvz_dx);
-        }
-        // point sources of this cell (usually none in the tile)
-        const int cell = lz * TX + lx;
-        for (int e = s0; e < s1; ++e) {
-            const int2 ev = G.src.ev[e];
-            if (ev.x != cell) continue;
-            const float w = G.wavelet[(long long)ev.y * G.nt + A.it];
-            for (int k = 0; k < G.nsf; ++k) add_to(G.sf[k], w, sxx, szz, sxz);
-        }
-        A.f[SXX][so + i] = sxx;
-        A.f[SZZ][so + i] = szz;
-        A.f[SXZ][so + i] = sxz;
-        if (A.strips) {
-            const int si = strip_index(G, iz, ix);
-            if (si >= 0) {
-                float* st = A.strips + (long long)b * 5 * G.nstrip + si;
-                st[0] = tvx[c];
-                st[G.nstrip] = tvz[c];
-                st[2 * G.nstrip] = sxx;
-                st[3 * G.nstrip] = szz;
-                st[4 * G.nstrip] = sxz;
-            }
-        }
+        const int iz = tz0 + threadIdx.y + 8 * r;
+        const bool in = in_core(G, ix, iz);
+        const long long i = (long long)b0 * G.ms + (long long)iz * G.P + ix;
+        lamr[r] = in ? A.m.lam[i] : 0.f;
+        mur[r] = in ? A.m.mu[i] : 0.f;
     }
-    // receivers of this tile: read back the final values of the step
-    const int r0 = G.rec.off[key], r1 = G.rec.off[key + 1];
-    if (A.record && r1 > r0) {
-        __syncthreads();
-        for (int e = r0 + threadIdx.x + threadIdx.y * TX; e < r1; e += NTH) {
-            const int2 ev = G.rec.ev[e];
-            const int iz = tz0 + ev.x / TX, ix = tx0 + ev.x % TX;
-            const long long i = so + (long long)iz * G.P + ix;
-            float* out = A.record + ((long long)(b * G.nt + A.it) * G.nrec + (ev.y - b * G.nrec)) * G.nrf;
-            for (int k = 0; k < G.nrf; ++k) out[k] = A.f[G.rf[k]][i];
+    const int ntl = G.ntx * G.ntz;
+    const bool ring = tile_in_pml(G, tz0, tx0);
+    for (int g = 0; g < nloc; ++g) {
+        const int b = b0 + g, s = g & 1;
+        const bool ok = tma::mbar_wait(&sm.bar[s], (g >> 1) & 1, G.err, ERR_WAIT_FWD);
+        if (__syncthreads_or(!ok)) {
+            drain(sm, g, nloc, G.err, ERR_WAIT_FWD);
+            return;
         }
+        const float *tvx = sm.h[s][0], *tvz = sm.h[s][1];
+        const long long so = (long long)b * G.S;
+        const int key = b * ntl + tile;
+        MemPair mz[RPT], mx[RPT];
+        if (ring) {
+#pragma unroll
+            for (int r = 0; r < RPT; ++r) {
+                const int iz = tz0 + threadIdx.y + 8 * r;
+                mz[r] = load_mem_z(G, A.mem, ZM_VZZ, ZM_VXZ, b, iz, ix);
+                mx[r] = load_mem_x(G, A.mem, XM_VXX, XM_VZX, b, iz, ix);
+            }
+        }
+        const int s0 = G.src.off[key], s1 = G.src.off[key + 1];
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            const int lz = threadIdx.y + 8 * r, iz = tz0 + lz;
+            if (iz >= G.nz || ix >= G.nx) continue;
+            const int c = (lz + M) * HX + lx + M;
+            const int cell = lz * TX + lx;
+            const long long i = (long long)iz * G.P + ix;
+            float sxx = sm.c[s][0][cell], szz = sm.c[s][1][cell], sxz = sm.c[s][2][cell];
+            if (in_core(G, ix, iz)) {
+                float dvx_dx = dmx(tvx, c, G.idx);
+                float dvz_dz = dmz(tvz, c, G.idz);
+                float dvx_dz = dpz(tvx, c, G.idz);
+                float dvz_dx = dpx(tvz, c, G.idx);
+                const float lam = lamr[r], mu = mur[r];
+                const bool pml = ring && in_pml(G, ix, iz);
+                if (pml && mz[r].at >= 0) {
+                    float m = G.az[iz] * mz[r].a + G.bz[iz] * dvz_dz;
+                    A.mem.z[ZM_VZZ][mz[r].at] = m; dvz_dz += m;
+                }
+                if (pml && mx[r].at >= 0) {
+                    float m = G.ax[ix] * mx[r].a + G.bx[ix] * dvx_dx;
+                    A.mem.x[XM_VXX][mx[r].at] = m; dvx_dx += m;
+                }
+                sxx += G.dt * ((lam + 2.f * mu) * dvx_dx + lam * dvz_dz);
+                szz += G.dt * ((lam + 2.f * mu) * dvz_dz + lam * dvx_dx);
+                if (pml && mz[r].at >= 0) {
+                    float m = G.azh[iz] * mz[r].b + G.bzh[iz] * dvx_dz;
+                    A.mem.z[ZM_VXZ][mz[r].at] = m; dvx_dz += m;
+                }
+                if (pml && mx[r].at >= 0) {
+                    float m = G.axh[ix] * mx[r].b + G.bxh[ix] * dvz_dx;
+                    A.mem.x[XM_VZX][mx[r].at] = m; dvz_dx += m;
+                }
+                sxz += G.dt * mu * (dvx_dz + dvz_dx);
+            }
+            // point sources of this cell (usually none in the tile)
+            for (int e = s0; e < s1; ++e) {
+                const int2 ev = G.src.ev[e];
+                if (ev.x != cell) continue;
+                const float w = G.wavelet[(long long)ev.y * G.nt + A.it];
+                for (int k = 0; k < G.nsf; ++k) add_to(G.sf[k], w, sxx, szz, sxz);
+            }
+            A.f[SXX][so + i] = sxx;
+            A.f[SZZ][so + i] = szz;
+            A.f[SXZ][so + i] = sxz;
+            if (A.strips) {
+                const int si = strip_index(G, iz, ix);
+                if (si >= 0) {
+                    float* st = A.strips + (long long)b * 5 * G.nstrip + si;
+                    st[0] = tvx[c];
+                    st[G.nstrip] = tvz[c];
+                    st[2 * G.nstrip] = sxx;
+                    st[3 * G.nstrip] = szz;
+                    st[4 * G.nstrip] = sxz;
+                }
+            }
+        }
+        // receivers of this (shot, tile): read back the final values of the step
+        const int r0 = G.rec.off[key], r1 = G.rec.off[key + 1];
+        __syncthreads();                       // stage s consumed; this shot's stores visible
+        if (A.record && r1 > r0) {
+            for (int e = r0 + threadIdx.x + threadIdx.y * TX; e < r1; e += NTH) {
+                const int2 ev = G.rec.ev[e];
+                const int iz = tz0 + ev.x / TX, jx = tx0 + ev.x % TX;
+                const long long i = so + (long long)iz * G.P + jx;
+                float* out = A.record + ((long long)(b * G.nt + A.it) * G.nrec + (ev.y - b * G.nrec)) * G.nrf;
+                for (int k = 0; k < G.nrf; ++k) out[k] = A.f[G.rf[k]][i];
+            }
+        }
+        if (threadIdx.x == 0 && threadIdx.y == 0 && g + 2 < nloc) issue(s, b + 2);
     }
 }
 
@@ -840,6 +981,11 @@ static Plan make_plan(const sweep_elastic_desc* d)
     G.wavelet = d->wavelet;
     pl.nm = per_shot ? d->B : 1;
     pl.gshots = per_shot ? 1 : std::min(env_int("SWEEP_B200_EL_SHOTS_PER_CTA", 4), d->B);
+    // forward: shots per CTA, keeping at least two waves of CTAs
+    const long long ntl = (long long)G.ntx * G.ntz;
+    int gf = per_shot ? 1 : std::min(env_int("SWEEP_B200_EL_SHOTS_PER_CTA_FWD", 4), d->B);
+    while (gf > 1 && ntl * ((d->B + gf - 1) / gf) < 2LL * 148 * 4) --gf;
+    G.gf = gf;
     pl.nslot = (d->B + pl.gshots - 1) / pl.gshots;
     return pl;
 }
@@ -848,6 +994,7 @@ struct Common {
     float *rho, *lam, *mu, *bv, *vp, *vs;
     int32_t *src_off, *rec_off;
     int2 *src_ev, *rec_ev;
+    int* err;
 };
 
 static void carve_common(Carve& c, const Plan& pl, Common& w)
@@ -861,6 +1008,7 @@ static void carve_common(Carve& c, const Plan& pl, Common& w)
     w.rec_off = c.take<int32_t>(nkey);
     w.src_ev = c.take<int2>((long long)G.B * G.nsrc + 1);
     w.rec_ev = c.take<int2>((long long)G.B * G.nrec + 1);
+    w.err = c.take<int>(1);
 }
 
 static void carve_slabs(Carve& c, const Geo& G, Slabs& s)
@@ -1046,6 +1194,34 @@ static void setup_common(const sweep_elastic_desc* d, Plan& pl, const Common& w,
     SWEEP_CUDA(cudaStreamSynchronize(st));   // host staging released on return
     G.src.off = w.src_off; G.src.ev = w.src_ev;
     G.rec.off = w.rec_off; G.rec.ev = w.rec_ev;
+    SWEEP_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
+    G.err = w.err;
+}
+
+static void check_err(const Common& w, cudaStream_t st, const char* what)
+{
+    int h = 0;
+    SWEEP_CUDA(cudaMemcpyAsync(&h, w.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SWEEP_CUDA(cudaStreamSynchronize(st));
+    SWEEP_REQUIRE(h == 0, "elastic2d %s: a tile load did not complete in time (code %d); results are invalid", what, h);
+}
+
+static CUtensorMap field_map(const float* base, const Geo& G, bool halo)
+{
+    const uint64_t dims[3] = {(uint64_t)G.nx, (uint64_t)G.nz, (uint64_t)G.B};
+    const uint64_t strides[2] = {(uint64_t)G.P, (uint64_t)G.S};
+    const uint32_t box[3] = {(uint32_t)(halo ? HX : TX), (uint32_t)(halo ? HZ : TZ), 1u};
+    return tma::make_map(base, 3, dims, strides, box);
+}
+
+static FwdMaps fwd_maps(float* const* f, const Geo& G)
+{
+    FwdMaps m;
+    for (int k = 0; k < 5; ++k) {
+        m.halo[k] = field_map(f[k], G, true);
+        m.tile[k] = field_map(f[k], G, false);
+    }
+    return m;
 }
 
 static Models models_of(const Common& w)
@@ -1053,8 +1229,17 @@ static Models models_of(const Common& w)
     return Models{w.rho, w.lam, w.mu, w.bv, w.vp, w.vs};
 }
 
-constexpr size_t SM_FWD_VEL = 3 * HN * sizeof(float);
-constexpr size_t SM_FWD_STR = 2 * HN * sizeof(float);
+constexpr size_t SM_FWD_VEL = sizeof(VelSmem);
+constexpr size_t SM_FWD_STR = sizeof(StrSmem);
+
+static void set_attrs()
+{
+    static bool done = false;
+    if (done) return;
+    SWEEP_CUDA(cudaFuncSetAttribute(fwd_vel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_FWD_VEL));
+    SWEEP_CUDA(cudaFuncSetAttribute(fwd_str, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_FWD_STR));
+    done = true;
+}
 constexpr size_t SM_REV_STR = 2 * HN * sizeof(float);
 constexpr size_t SM_REV_SADJ = 4 * HN * sizeof(float);
 constexpr size_t SM_REV_VADJ = 7 * HN * sizeof(float);
@@ -1092,12 +1277,14 @@ template <class StripsOf>
 static void forward_steps(FwdArgs& A, int it0, int it1, StripsOf strips_of, cudaStream_t st)
 {
     const Geo& G = A.G;
-    const dim3 grid(G.ntx * G.ntz, G.B), block(TX, 8);
+    set_attrs();
+    const FwdMaps maps = fwd_maps(A.f, G);
+    const dim3 grid(G.ntx * G.ntz, (G.B + G.gf - 1) / G.gf), block(TX, 8);
     for (int it = it0; it < it1; ++it) {
         A.it = it;
         A.strips = strips_of(it);
-        fwd_vel<<<grid, block, SM_FWD_VEL, st>>>(A);
-        fwd_str<<<grid, block, SM_FWD_STR, st>>>(A);
+        fwd_vel<<<grid, block, SM_FWD_VEL, st>>>(maps, A);
+        fwd_str<<<grid, block, SM_FWD_STR, st>>>(maps, A);
     }
     SWEEP_LAUNCH_CHECK();
 }
@@ -1134,6 +1321,7 @@ void forward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, float* r
             for (int k = 0; k < 5; ++k)
                 SWEEP_CUDA(cudaMemcpyAsync(last + k * n, w.f[k], sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
         }
+        check_err(w.cm, st, "forward");
         return;
     }
     const int k = ckpt_every, C = nchunks(pl, k);
@@ -1150,6 +1338,7 @@ void forward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, float* r
                       [&](int it) { return (tape && it == it1 - 1 && ch + 1 < C) ? ckpt_at(tape, pl, ch + 1).strips : nullptr; },
                       st);
     }
+    check_err(w.cm, st, "forward");
 }
 
 void backward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, const float* adj, const void* tape,
@@ -1239,6 +1428,7 @@ void backward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, const f
     finalize_kernel<<<592, 256, 0, st>>>(w.gvs, pl.nslot, per_shot, G, grad_vs);
     finalize_kernel<<<592, 256, 0, st>>>(w.grho, pl.nslot, per_shot, G, grad_rho);
     SWEEP_LAUNCH_CHECK();
+    check_err(w.cm, st, "backward");
 }
 
 }  // namespace el2d
