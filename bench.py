@@ -392,6 +392,7 @@ def run_gpu(args, wl):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
 
+    from sweep_b200.distributed import all_reduce_
     solver, m_true, m_init, w, src, rec = wl.build(dev)
     src, rec = src[:wl.nshot], rec[:wl.nshot]
     w_d = torch.tensor(w, device=dev)
@@ -422,8 +423,7 @@ def run_gpu(args, wl):
             loss = loss + lb.detach()
         gs = [m.grad for m in ms]
         if world > 1:
-            for g in gs:
-                dist.all_reduce(g)
+            all_reduce_(gs)                  # shot-parallel FWI: one SUM per model gradient
         return loss, gs
 
     def barrier():

@@ -707,6 +707,14 @@ __global__ void __launch_bounds__(NTH, 4) rev_sadj(RevArgs A)
     const float* __restrict__ lam_ = A.m.lam + (long long)b * G.ms;
     const float* __restrict__ mu_ = A.m.mu + (long long)b * G.ms;
     const int tid = threadIdx.x + threadIdx.y * TX;
+    const float* __restrict__ mo_vxx = A.mo.x[XM_VXX];
+    const float* __restrict__ mo_vzx = A.mo.x[XM_VZX];
+    const float* __restrict__ mo_vzz = A.mo.z[ZM_VZZ];
+    const float* __restrict__ mo_vxz = A.mo.z[ZM_VXZ];
+    float* __restrict__ mn_vxx = A.mn.x[XM_VXX];
+    float* __restrict__ mn_vzx = A.mn.x[XM_VZX];
+    float* __restrict__ mn_vzz = A.mn.z[ZM_VZZ];
+    float* __restrict__ mn_vxz = A.mn.z[ZM_VXZ];
     float rs[NLD][5];
 #pragma unroll
     for (int j = 0; j < NLD; ++j) {
@@ -737,20 +745,20 @@ __global__ void __launch_bounds__(NTH, 4) rev_sadj(RevArgs A)
             const int xs = xslab(G, ix), zs = zslab(G, iz);
             if (xs >= 0) {
                 const long long xi = ((long long)b * G.nz + iz) * G.WX + xs;
-                const float t0 = A.mo.x[XM_VXX][xi] + q0, t3 = A.mo.x[XM_VZX][xi] + q3;
+                const float t0 = mo_vxx[xi] + q0, t3 = mo_vzx[xi] + q3;
                 if (own) {
-                    A.mn.x[XM_VXX][xi] = G.ax[ix] * t0;
-                    A.mn.x[XM_VZX][xi] = G.axh[ix] * t3;
+                    mn_vxx[xi] = G.ax[ix] * t0;
+                    mn_vzx[xi] = G.axh[ix] * t3;
                 }
                 q0 = q0 + G.bx[ix] * t0;
                 q3 = q3 + G.bxh[ix] * t3;
             }
             if (zs >= 0) {
                 const long long zi = ((long long)b * G.WZ + zs) * G.P + ix;
-                const float t1 = A.mo.z[ZM_VZZ][zi] + q1, t2 = A.mo.z[ZM_VXZ][zi] + q2;
+                const float t1 = mo_vzz[zi] + q1, t2 = mo_vxz[zi] + q2;
                 if (own) {
-                    A.mn.z[ZM_VZZ][zi] = G.az[iz] * t1;
-                    A.mn.z[ZM_VXZ][zi] = G.azh[iz] * t2;
+                    mn_vzz[zi] = G.az[iz] * t1;
+                    mn_vxz[zi] = G.azh[iz] * t2;
                 }
                 q1 = q1 + G.bz[iz] * t1;
                 q2 = q2 + G.bzh[iz] * t2;
@@ -788,6 +796,14 @@ __global__ void __launch_bounds__(NTH, 4) rev_vadj(RevArgs A)
     const long long so = (long long)b * G.S;
     const float* __restrict__ bv_ = A.m.bv + (long long)b * G.ms;
     const int tid = threadIdx.x + threadIdx.y * TX;
+    const float* __restrict__ mo_sxxx = A.mo.x[XM_SXXX];
+    const float* __restrict__ mo_sxzx = A.mo.x[XM_SXZX];
+    const float* __restrict__ mo_sxzz = A.mo.z[ZM_SXZZ];
+    const float* __restrict__ mo_szzz = A.mo.z[ZM_SZZZ];
+    float* __restrict__ mn_sxxx = A.mn.x[XM_SXXX];
+    float* __restrict__ mn_sxzx = A.mn.x[XM_SXZX];
+    float* __restrict__ mn_sxzz = A.mn.z[ZM_SXZZ];
+    float* __restrict__ mn_szzz = A.mn.z[ZM_SZZZ];
     float rv[NLD][3];
 #pragma unroll
     for (int j = 0; j < NLD; ++j) {
@@ -816,20 +832,20 @@ __global__ void __launch_bounds__(NTH, 4) rev_vadj(RevArgs A)
             const int xs = xslab(G, ix), zs = zslab(G, iz);
             if (xs >= 0) {
                 const long long xi = ((long long)b * G.nz + iz) * G.WX + xs;
-                const float t0 = A.mo.x[XM_SXXX][xi] + p0, t3 = A.mo.x[XM_SXZX][xi] + p3;
+                const float t0 = mo_sxxx[xi] + p0, t3 = mo_sxzx[xi] + p3;
                 if (own) {
-                    A.mn.x[XM_SXXX][xi] = G.axh[ix] * t0;
-                    A.mn.x[XM_SXZX][xi] = G.ax[ix] * t3;
+                    mn_sxxx[xi] = G.axh[ix] * t0;
+                    mn_sxzx[xi] = G.ax[ix] * t3;
                 }
                 p0 = p0 + G.bxh[ix] * t0;
                 p3 = p3 + G.bx[ix] * t3;
             }
             if (zs >= 0) {
                 const long long zi = ((long long)b * G.WZ + zs) * G.P + ix;
-                const float t2 = A.mo.z[ZM_SXZZ][zi] + p2, t1 = A.mo.z[ZM_SZZZ][zi] + p1;
+                const float t2 = mo_sxzz[zi] + p2, t1 = mo_szzz[zi] + p1;
                 if (own) {
-                    A.mn.z[ZM_SXZZ][zi] = G.az[iz] * t2;
-                    A.mn.z[ZM_SZZZ][zi] = G.azh[iz] * t1;
+                    mn_sxzz[zi] = G.az[iz] * t2;
+                    mn_szzz[zi] = G.azh[iz] * t1;
                 }
                 p2 = p2 + G.bz[iz] * t2;
                 p1 = p1 + G.bzh[iz] * t1;
