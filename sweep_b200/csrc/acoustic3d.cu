@@ -18,6 +18,7 @@
 // P = round_up(nx, 32) floats).  Point sources, receivers and boundary strips
 // are small gather / scatter kernels between the stencil launches.
 #include "common.cuh"
+#include "tma.cuh"
 
 namespace sweep {
 namespace a3d {
@@ -164,13 +165,37 @@ struct F3 {
     float *zx, *zy, *zz;                       // CPML zeta (in place)
 };
 
+// Forward plane ring: stage q holds the wavefield plane u(q) with its x / y
+// halo, and the centre tiles of u_prev(q - M) and of the model for plane
+// q - M.  Computing plane z needs stages z - M .. z + M; with NS3 stages the
+// loads run NS3 - 2M - 1 = 3 planes ahead of the compute, TMA-issued by one
+// thread on one mbarrier per stage.
+constexpr int NS3 = 12;
+constexpr int CN3 = BXC * BYC;
+struct F3Smem {
+    float u[NS3][PN];
+    float up[NS3][CN3];
+    float cf[NS3][CN3];
+    uint64_t bar[NS3];
+};
+
+struct F3Maps {
+    CUtensorMap uh[3];              // the three wavefield buffers, (PW x PH) boxes
+    CUtensorMap uc[3];              // the same buffers, (BXC x BYC) boxes
+    CUtensorMap cf;                 // ((v*v)*dt)*dt, (BXC x BYC) boxes
+};
+
+enum { ERR_WAIT_F3 = 1 };
+
 // u_next = 2 u - u_prev + vp^2 dt^2 (Lap u + CPML terms) on [M, n-M)^3.
 // The CPML branch of an axis runs on its band plus one cell (reference
 // forward_split.cu:150-156) and uses the product-rule split
 // tmp = (((1 + b) Lap + db du) + a dpsi) + da psi (forward_split.cu:171-172).
-__global__ void __launch_bounds__(NTH, 4) f3_step(const Params P, const F3 F)
+__global__ void __launch_bounds__(NTH, 4) f3_step(const __grid_constant__ F3Maps MP, const Params P, const F3 F,
+                                                  const int uin, const int uprev, int* err)
 {
-    __shared__ float pl[2][PN];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    F3Smem& sm = *reinterpret_cast<F3Smem*>(smem_raw);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BXC + tx;
     const int gx0 = blockIdx.x * BXC - M, gy0 = blockIdx.y * BYC - M;
     const int ix = blockIdx.x * BXC + tx, iy = blockIdx.y * BYC + ty;
@@ -178,24 +203,49 @@ __global__ void __launch_bounds__(NTH, 4) f3_step(const Params P, const F3 F)
     const int zb = max(M, zci * P.zc), ze = min(P.nz - M, (zci + 1) * P.zc);
     if (zb >= ze) return;
     const bool col = ix >= M && ix < P.nx - M && iy >= M && iy < P.ny - M;
-    const bool cin = ix < P.nx && iy < P.ny;
     const long long bo = (long long)b * P.S;
-    const float* __restrict__ un = F.u_now + bo;
     const long long colo = (long long)iy * P.P + ix;
-    float q[2 * M + 1];
-#pragma unroll
-    for (int k = 0; k < 2 * M; ++k) q[k] = cin ? __ldg(un + (zb - M + k) * P.SP + colo) : 0.f;
-    PlaneLoader L;
-    L.load(un, P, zb, gy0, gx0, tid);
-    L.store(pl[0], tid);
+    const int q0 = zb - M, q1 = ze + M;                // stages [q0, q1)
+    auto slot = [&](int q) { return (q - q0) % NS3; };
+    auto parity = [&](int q) { return (uint32_t)(((q - q0) / NS3) & 1); };
+    auto issue = [&](int q) {
+        const int sl = slot(q);
+        const bool cen = q - M >= zb && q - M < ze;     // u_prev / model of plane q - M
+        tma::mbar_expect_tx(&sm.bar[sl], (uint32_t)(PN + (cen ? 2 * CN3 : 0)) * 4u);
+        tma::load_4d(sm.u[sl], &MP.uh[uin], &sm.bar[sl], gx0, gy0, q, b);
+        if (cen) {
+            tma::load_4d(sm.up[sl], &MP.uc[uprev], &sm.bar[sl], gx0 + M, gy0 + M, q - M, b);
+            tma::load_3d(sm.cf[sl], &MP.cf, &sm.bar[sl], gx0 + M, gy0 + M, q - M);
+        }
+    };
+    if (tid == 0) {
+        for (int i = 0; i < NS3; ++i) tma::mbar_init(&sm.bar[i], 1);
+        tma::fence_barrier_init();
+    }
+    __syncthreads();
+    int next = q0;                                     // first stage not yet issued (thread 0)
+    if (tid == 0)
+        for (; next < min(q1, q0 + NS3); ++next) issue(next);
+    // a failed wait: drain (bounded) every stage still in flight, then exit
+    auto fail = [&](int q) {
+        if (tid == 0)
+            for (int r = q; r < next; ++r) tma::mbar_wait(&sm.bar[slot(r)], parity(r), err, ERR_WAIT_F3);
+    };
+    for (int q = q0; q < zb + M; ++q) {
+        const bool ok = tma::mbar_wait(&sm.bar[slot(q)], parity(q), err, ERR_WAIT_F3);
+        if (__syncthreads_or(!ok)) { fail(q); return; }
+    }
+    const int cidx = (ty + M) * PW + (tx + M);
     for (int z = zb; z < ze; ++z) {
-        const int s = (z - zb) & 1;
-        q[2 * M] = cin ? __ldg(un + (z + M) * P.SP + colo) : 0.f;
-        __syncthreads();
-        const bool more = z + 1 < ze;
-        if (more) L.load(un, P, z + 1, gy0, gx0, tid);
+        {
+            const bool ok = tma::mbar_wait(&sm.bar[slot(z + M)], parity(z + M), err, ERR_WAIT_F3);
+            if (__syncthreads_or(!ok)) { fail(z + M); return; }
+        }
         if (col) {
-            const float* p = pl[s] + (ty + M) * PW + (tx + M);
+            float q[2 * M + 1];
+#pragma unroll
+            for (int k = 0; k <= 2 * M; ++k) q[k] = sm.u[slot(z - M + k)][cidx];
+            const float* p = sm.u[slot(z)] + cidx;
             const float lx = lap_p(p, 1, P, P.dx);
             const float ly = lap_p(p, PW, P, P.dy);
             const float lz = lap_q(q, P, P.dz);
@@ -248,11 +298,11 @@ __global__ void __launch_bounds__(NTH, 4) f3_step(const Params P, const F3 F)
                     w += lz;
                 }
             }
-            F.u_next[i] = 2.f * q[M] - __ldg(F.u_prev + i) + __ldg(P.cf + z * P.SP + colo) * w;
+            const int cc = ty * BXC + tx;
+            F.u_next[i] = 2.f * q[M] - sm.up[slot(z + M)][cc] + sm.cf[slot(z + M)][cc] * w;
         }
-        if (more) L.store(pl[1 - s], tid);
-#pragma unroll
-        for (int k = 0; k < 2 * M; ++k) q[k] = q[k + 1];
+        __syncthreads();                               // every thread is done with stage z - M
+        if (tid == 0 && next < q1) issue(next++);      // reuses the slot of stage z - M
     }
 }
 
@@ -679,6 +729,7 @@ static dim3 stencil_grid(const Params& P)
 struct Work {
     float *cf, *ca, *vv;
     float* f[34];                    // forward: u x3, psi x6, zeta x3; reverse: see backward()
+    int* err;                        // bounded-wait failure flag
 };
 
 static Work carve(Carve& c, const Params& P, int nfields)
@@ -686,7 +737,32 @@ static Work carve(Carve& c, const Params& P, int nfields)
     Work w{};
     w.cf = c.take<float>(P.S); w.ca = c.take<float>(P.S); w.vv = c.take<float>(P.S);
     for (int i = 0; i < nfields; ++i) w.f[i] = c.take<float>((long long)P.B * P.S);
+    w.err = c.take<int>(1);
     return w;
+}
+
+static void check_err(const Work& w, cudaStream_t st, const char* what)
+{
+    int h = 0;
+    SWEEP_CUDA(cudaMemcpyAsync(&h, w.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SWEEP_CUDA(cudaStreamSynchronize(st));
+    SWEEP_REQUIRE(h == 0, "acoustic3d %s: a plane load did not complete in time (code %d); results are invalid", what, h);
+}
+
+// 4-D (x, y, z, shot) map of a wavefield buffer, or 3-D (x, y, z) of the model.
+static CUtensorMap plane_map(const float* base, const Params& P, int nb, bool halo)
+{
+    const uint32_t bx = halo ? PW : BXC, by = halo ? PH : BYC;
+    if (nb == 0) {
+        const uint64_t dims[3] = {(uint64_t)P.nx, (uint64_t)P.ny, (uint64_t)P.nz};
+        const uint64_t strides[2] = {(uint64_t)P.P, (uint64_t)P.SP};
+        const uint32_t box[3] = {bx, by, 1u};
+        return tma::make_map(base, 3, dims, strides, box);
+    }
+    const uint64_t dims[4] = {(uint64_t)P.nx, (uint64_t)P.ny, (uint64_t)P.nz, (uint64_t)nb};
+    const uint64_t strides[3] = {(uint64_t)P.P, (uint64_t)P.SP, (uint64_t)P.S};
+    const uint32_t box[4] = {bx, by, 1u, 1u};
+    return tma::make_map(base, 4, dims, strides, box);
 }
 
 static int64_t tape_bytes(const Params& P)
@@ -777,15 +853,26 @@ struct FwdState {
 // none), source injection, receiver gather (record may be null).
 template <class StripsOf>
 static void forward_steps(const sweep_acoustic_desc* d, const Params& P, FwdState& S, float* record, int it0,
-                          int it1, StripsOf strips_of, cudaStream_t st)
+                          int it1, StripsOf strips_of, int* err, cudaStream_t st)
 {
     const dim3 grid = stencil_grid(P), block(BXC, BYC);
     const unsigned gs = blocks_for((long long)P.B * P.nsrc, 128), gr = blocks_for((long long)P.B * P.nrec, 128);
     const unsigned gst = blocks_for((long long)P.B * P.nstrip, 256);
+    static bool attr = false;
+    if (!attr) {
+        SWEEP_CUDA(cudaFuncSetAttribute(f3_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(F3Smem)));
+        attr = true;
+    }
+    F3Maps maps;
+    for (int k = 0; k < 3; ++k) {
+        maps.uh[k] = plane_map(S.f[k], P, P.B, true);
+        maps.uc[k] = plane_map(S.f[k], P, P.B, false);
+    }
+    maps.cf = plane_map(P.cf, P, 0, false);
     for (int it = it0; it < it1; ++it) {
         F3 F{S.f[S.in], S.f[S.ip], S.f[S.ix], S.ps[0], S.ps[1], S.ps[2], S.psn[0], S.psn[1], S.psn[2],
              S.zeta(0), S.zeta(1), S.zeta(2)};
-        f3_step<<<grid, block, 0, st>>>(P, F);
+        f3_step<<<grid, block, sizeof(F3Smem), st>>>(maps, P, F, S.in, S.ip, err);
         SWEEP_LAUNCH_CHECK();
         float* strips = strips_of(it);
         if (strips && P.nstrip > 0) strips3<<<gst, 256, 0, st>>>(P, S.f[S.in], strips, 0);
@@ -822,17 +909,19 @@ void forward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* 
     P.cf = w.cf; P.ca = w.ca; P.vv = w.vv;
     const long long n = (long long)P.B * P.S;
     for (int i = 0; i < kFwdFields; ++i) SWEEP_CUDA(cudaMemsetAsync(w.f[i], 0, n * 4, st));
+    SWEEP_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
     if (d->nrec > 0) SWEEP_CUDA(cudaMemsetAsync(record, 0, (size_t)d->B * d->nt * d->nrec * 4, st));
     FwdState S(w.f);
     if (mem_mode != SWEEP_MEM_CHECKPOINT) {
         float* strips = static_cast<float*>(tape);
         forward_steps(d, P, S, record, 0, d->nt,
-                      [&](int it) { return strips ? strips + (long long)it * P.B * P.nstrip : nullptr; }, st);
+                      [&](int it) { return strips ? strips + (long long)it * P.B * P.nstrip : nullptr; }, w.err, st);
         if (strips) {
             float* last = tape_last(tape, P);
             copy_dd(last, S.f[S.ip], n, st);        // U[nt-1]
             copy_dd(last + n, S.f[S.in], n, st);    // U[nt]
         }
+        check_err(w, st, "forward");
         return;
     }
     const int k = ckpt_every, C = nchunks(P, k);
@@ -846,8 +935,9 @@ void forward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* 
         // the last step of a chunk keeps its strips with the next checkpoint
         forward_steps(d, P, S, record, it0, it1,
                       [&](int it) { return (tape && it == it1 - 1 && ch + 1 < C) ? ckpt_strips(tape, P, ch + 1) : nullptr; },
-                      st);
+                      w.err, st);
     }
+    check_err(w, st, "forward");
 }
 
 void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const float* adj, const void* tape,
@@ -876,6 +966,7 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     const long long n = (long long)P.B * P.S;
     const bool illum = illum_s != nullptr;
     for (int i = 0; i < kRevFields; ++i) SWEEP_CUDA(cudaMemsetAsync(w.f[i], 0, n * 4, st));
+    SWEEP_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
     if (grad_w && d->nsrc > 0) SWEEP_CUDA(cudaMemsetAsync(grad_w, 0, (size_t)d->B * d->nsrc * d->nt * 4, st));
     const dim3 grid = stencil_grid(P), block(BXC, BYC);
     const unsigned gs = blocks_for((long long)P.B * P.nsrc, 128), gr = blocks_for((long long)P.B * P.nrec, 128);
@@ -946,7 +1037,8 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
                 copy_dd(chunk, ckpt_strips(tp, P, ch), cs, st);       // strips of U[it0 - 1]
             }
             // replay: chunk slot j holds the strips of U[it0 - 1 + j]
-            forward_steps(d, P, S, nullptr, it0, it1, [&](int it) { return chunk + (long long)(it - it0 + 1) * cs; }, st);
+            forward_steps(d, P, S, nullptr, it0, it1, [&](int it) { return chunk + (long long)(it - it0 + 1) * cs; },
+                          w.err, st);
             copy_dd(w.f[15], S.f[S.in], n, st);      // U[it1]
             copy_dd(w.f[16], S.f[S.ip], n, st);      // U[it1 - 1]
             reverse(it0, it1, [&](int t) { return chunk + (long long)(t - (it0 - 1)) * cs; });
@@ -954,6 +1046,7 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     }
     finalize3<<<592, 256, 0, st>>>(gacc, gcomp, is, ir, P.B, (int)rows, d->nx, P.P, P.S, grad_vp, illum_s, illum_r);
     SWEEP_LAUNCH_CHECK();
+    check_err(w, st, "backward");
 }
 
 }  // namespace a3d
