@@ -566,12 +566,34 @@ struct R3 {
     float *gacc, *gcomp, *is, *ir;                          // per-shot slots (B, S)
 };
 
+// Reconstruction plane ring: the halo planes of u(it) ring as in the
+// forward (NS3 stages); the per-plane centre tiles -- u(it+1), lambda(it),
+// the two model fields and the two Kahan slots -- sit in a ring of
+// NSC3 = NS3 - 2M stages, filled with the halo plane M planes ahead and
+// counted on its barrier.
+constexpr int NSC3 = NS3 - 2 * M;
+struct R3Smem {
+    float u[NS3][PN];
+    float c[NSC3][6][CN3];
+    uint64_t bar[NS3];
+};
+
+struct R3Maps {
+    CUtensorMap uh[3];              // reconstruction buffers, (PW x PH) boxes
+    CUtensorMap uc[3];              // the same, centre boxes
+    CUtensorMap lc[3];              // lambda buffers, centre boxes
+    CUtensorMap cf, vv;             // model fields, centre boxes
+    CUtensorMap ga, gc;             // Kahan accumulator and compensation slots, centre boxes
+};
+
 // u(it-1) = 2 u(it) - u(it+1) + vp^2 dt^2 Lap u(it) on the reconstruction box
 // (the physical box minus the restored strips) with the fused vp image
 // 2 dt^2 u_tt lambda(it) / vp (reference forward_split.cu:292-372).
-__global__ void __launch_bounds__(NTH, 4) r3_recon(const Params P, const R3 R)
+__global__ void __launch_bounds__(NTH, 4) r3_recon(const __grid_constant__ R3Maps MP, const Params P, const R3 R,
+                                                   const int rnow, const int rprev, const int lnow, int* err)
 {
-    __shared__ float pl[2][PN];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    R3Smem& sm = *reinterpret_cast<R3Smem*>(smem_raw);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BXC + tx;
     const int gx0 = blockIdx.x * BXC - M, gy0 = blockIdx.y * BYC - M;
     const int ix = blockIdx.x * BXC + tx, iy = blockIdx.y * BYC + ty;
@@ -579,39 +601,73 @@ __global__ void __launch_bounds__(NTH, 4) r3_recon(const Params P, const R3 R)
     const int zb = max(P.qz0, zci * P.zc), ze = min(P.qz1, (zci + 1) * P.zc);
     if (zb >= ze) return;
     const bool col = ix >= P.qx0 && ix < P.qx1 && iy >= P.qy0 && iy < P.qy1;
-    const bool cin = ix < P.nx && iy < P.ny;
     const long long bo = (long long)b * P.S;
-    const float* __restrict__ rn = R.r_now + bo;
     const long long colo = (long long)iy * P.P + ix;
     const float dt2 = P.dt * P.dt;
-    float q[2 * M + 1];
-#pragma unroll
-    for (int k = 0; k < 2 * M; ++k) q[k] = cin ? __ldg(rn + (zb - M + k) * P.SP + colo) : 0.f;
-    PlaneLoader L;
-    L.load(rn, P, zb, gy0, gx0, tid);
-    L.store(pl[0], tid);
+    const int q0 = zb - M, q1 = ze + M;
+    auto slot = [&](int q) { return (q - q0) % NS3; };
+    auto cslot = [&](int z) { return (z - zb) % NSC3; };
+    auto parity = [&](int q) { return (uint32_t)(((q - q0) / NS3) & 1); };
+    auto issue = [&](int q) {
+        const int sl = slot(q), z = q - M;
+        const bool cen = z >= zb && z < ze;
+        tma::mbar_expect_tx(&sm.bar[sl], (uint32_t)(PN + (cen ? 6 * CN3 : 0)) * 4u);
+        tma::load_4d(sm.u[sl], &MP.uh[rnow], &sm.bar[sl], gx0, gy0, q, b);
+        if (cen) {
+            float(*c)[CN3] = sm.c[cslot(z)];
+            const int x = gx0 + M, y = gy0 + M;
+            tma::load_4d(c[0], &MP.uc[rprev], &sm.bar[sl], x, y, z, b);
+            tma::load_4d(c[1], &MP.lc[lnow], &sm.bar[sl], x, y, z, b);
+            tma::load_3d(c[2], &MP.cf, &sm.bar[sl], x, y, z);
+            tma::load_3d(c[3], &MP.vv, &sm.bar[sl], x, y, z);
+            tma::load_4d(c[4], &MP.ga, &sm.bar[sl], x, y, z, b);
+            tma::load_4d(c[5], &MP.gc, &sm.bar[sl], x, y, z, b);
+        }
+    };
+    if (tid == 0) {
+        for (int i = 0; i < NS3; ++i) tma::mbar_init(&sm.bar[i], 1);
+        tma::fence_barrier_init();
+    }
+    __syncthreads();
+    int next = q0;
+    if (tid == 0)
+        for (; next < min(q1, q0 + NS3); ++next) issue(next);
+    auto fail = [&](int q) {
+        if (tid == 0)
+            for (int r = q; r < next; ++r) tma::mbar_wait(&sm.bar[slot(r)], parity(r), err, ERR_WAIT_F3);
+    };
+    for (int q = q0; q < zb + M; ++q) {
+        const bool ok = tma::mbar_wait(&sm.bar[slot(q)], parity(q), err, ERR_WAIT_F3);
+        if (__syncthreads_or(!ok)) { fail(q); return; }
+    }
+    const int cidx = (ty + M) * PW + (tx + M), cc = ty * BXC + tx;
     for (int z = zb; z < ze; ++z) {
-        const int s = (z - zb) & 1;
-        q[2 * M] = cin ? __ldg(rn + (z + M) * P.SP + colo) : 0.f;
-        __syncthreads();
-        const bool more = z + 1 < ze;
-        if (more) L.load(rn, P, z + 1, gy0, gx0, tid);
+        {
+            const bool ok = tma::mbar_wait(&sm.bar[slot(z + M)], parity(z + M), err, ERR_WAIT_F3);
+            if (__syncthreads_or(!ok)) { fail(z + M); return; }
+        }
         if (col) {
-            const float* p = pl[s] + (ty + M) * PW + (tx + M);
+            float q[2 * M + 1];
+#pragma unroll
+            for (int k = 0; k <= 2 * M; ++k) q[k] = sm.u[slot(z - M + k)][cidx];
+            const float* p = sm.u[slot(z)] + cidx;
             const float w = (lap_p(p, 1, P, P.dx) + lap_p(p, PW, P, P.dy)) + lap_q(q, P, P.dz);
-            const long long ic = z * P.SP + colo;
-            const long long i = bo + ic;
-            const float u0 = q[M], up = __ldg(R.r_prev + i);
-            const float un = 2.0f * u0 - up + __ldg(P.cf + ic) * w;
+            const float(*c)[CN3] = sm.c[cslot(z)];
+            const long long i = bo + z * P.SP + colo;
+            const float u0 = q[M], up = c[0][cc];
+            const float un = 2.0f * u0 - up + c[2][cc] * w;
             R.r_next[i] = un;
             const float utt = (un - 2 * u0 + up) / dt2;
-            const float lam = __ldg(R.lam + i);
-            kahan_add(R.gacc, R.gcomp, i, 2.f * P.dt * P.dt * utt * lam / __ldg(P.vv + ic));
+            const float lam = c[1][cc];
+            const float g = 2.f * P.dt * P.dt * utt * lam / c[3][cc];
+            const float y = g - c[5][cc];
+            const float t = c[4][cc] + y;
+            R.gcomp[i] = (t - c[4][cc]) - y;
+            R.gacc[i] = t;
             if (R.is) { R.is[i] += utt * utt; R.ir[i] += lam * lam; }
         }
-        if (more) L.store(pl[1 - s], tid);
-#pragma unroll
-        for (int k = 0; k < 2 * M; ++k) q[k] = q[k + 1];
+        __syncthreads();
+        if (tid == 0 && next < q1) issue(next++);
     }
 }
 
@@ -976,6 +1032,21 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     float* gcomp = w.f[19];
     float* is = illum ? w.f[20] : nullptr;
     float* ir = illum ? w.f[21] : nullptr;
+    static bool attr = false;
+    if (!attr) {
+        SWEEP_CUDA(cudaFuncSetAttribute(r3_recon, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(R3Smem)));
+        attr = true;
+    }
+    R3Maps rmaps;
+    for (int k = 0; k < 3; ++k) {
+        rmaps.uh[k] = plane_map(w.f[15 + k], P, P.B, true);
+        rmaps.uc[k] = plane_map(w.f[15 + k], P, P.B, false);
+        rmaps.lc[k] = plane_map(w.f[k], P, P.B, false);
+    }
+    rmaps.cf = plane_map(P.cf, P, 0, false);
+    rmaps.vv = plane_map(P.vv, P, 0, false);
+    rmaps.ga = plane_map(gacc, P, P.B, false);
+    rmaps.gc = plane_map(gcomp, P, P.B, false);
     // Reverse steps [it0, it1) top down from prev = U[it1] (f[15]), now =
     // U[it1 - 1] (f[16]); strips_of(t) holds the strips of U[t].
     auto reverse = [&](int it0, int it1, auto strips_of) {
@@ -996,7 +1067,7 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
                 gather3<<<gs, 128, 0, st>>>(P, w.f[ln], grad_w, d->src_loc, d->nsrc, it, 0);
             if (it > 0) {
                 R3 R{w.f[rn], w.f[rp], w.f[rx], w.f[ln], gacc, gcomp, is, ir};
-                r3_recon<<<grid, block, 0, st>>>(P, R);
+                r3_recon<<<grid, block, sizeof(R3Smem), st>>>(rmaps, P, R, rn - 15, rp - 15, ln, w.err);
                 if (P.nstrip > 0) {
                     strips3<<<gst, 256, 0, st>>>(P, w.f[rx], strips_of(it - 1), 1);
                     if (d->nsrc > 0)
