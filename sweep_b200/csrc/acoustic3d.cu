@@ -171,6 +171,7 @@ struct F3 {
 // loads run NS3 - 2M - 1 = 3 planes ahead of the compute, TMA-issued by one
 // thread on one mbarrier per stage.
 constexpr int NS3 = 12;
+constexpr int NSC3 = NS3 - 2 * M;   // centre ring of the reverse kernels
 constexpr int CN3 = BXC * BYC;
 struct F3Smem {
     float u[NS3][PN];
@@ -395,38 +396,8 @@ __global__ void strip_image3(const Params P, const Img I)
 }
 
 // ------------------------------------------------------------ adjoint step
-// gw = ((v*v)*dt^2) * lambda, the tap value of the adjoint Laplacian
-// (reference adjoint_split.cu GW_AT); planes and queues hold gw.
-struct GwLoader {
-    static constexpr int PER = (PN + NTH - 1) / NTH;
-    float v[PER];
-    __device__ __forceinline__ void load(const float* __restrict__ l, const float* __restrict__ c, const Params& P,
-                                         int iz, int gy0, int gx0, int tid)
-    {
-#pragma unroll
-        for (int j = 0; j < PER; ++j) {
-            const int e = tid + j * NTH;
-            float x = 0.f;
-            if (e < PN) {
-                const int r = e / PW, cc = e - r * PW;
-                const int gy = gy0 + r, gx = gx0 + cc;
-                if (gy >= 0 && gy < P.ny && gx >= 0 && gx < P.nx) {
-                    const long long o = iz * P.SP + (long long)gy * P.P + gx;
-                    x = __ldg(c + o) * __ldg(l + o);
-                }
-            }
-            v[j] = x;
-        }
-    }
-    __device__ __forceinline__ void store(float* dst, int tid)
-    {
-#pragma unroll
-        for (int j = 0; j < PER; ++j) {
-            const int e = tid + j * NTH;
-            if (e < PN) dst[e] = v[j];
-        }
-    }
-};
+// gw = ((v*v)*dt^2) * lambda is the tap value of the adjoint Laplacian
+// (reference adjoint_split.cu GW_AT).
 
 struct A3 {
     const float* l_now; const float* l_prev; float* l_next;
@@ -434,13 +405,15 @@ struct A3 {
     float *pxo, *pyo, *pzo, *zxo, *zyo, *zzo;          // (written)
 };
 
-// The transposed CPML terms of one axis at linear offset i (shot base bo),
-// stride st, profiles (a, b, db) at axis index c (reference adjoint_split.cu:205-255).
+// The transposed CPML terms of one axis at linear offset i, stride st,
+// profiles (a, b, db) at axis index c (reference adjoint_split.cu:205-255).
+// cav / lav: (v*v)*dt^2 and lambda at the 2M+1 cells along the axis around i
+// (from shared memory), gw = their product at i.
 __device__ __forceinline__ void adj_axis(const Params& P, const float* __restrict__ a, const float* __restrict__ bv,
-                                         const float* __restrict__ dbv, const float* __restrict__ lam,
-                                         const float* __restrict__ ca, const float* __restrict__ psi,
-                                         const float* __restrict__ zeta, long long i, long long ic, long long st,
-                                         int c, float gw, float h, float& L, float& Dg, float* pso, float* zto)
+                                         const float* __restrict__ dbv, const float (&cav)[2 * M + 1],
+                                         const float (&lav)[2 * M + 1], const float* __restrict__ psi,
+                                         const float* __restrict__ zeta, long long i, long long st, int c, float gw,
+                                         float h, float& L, float& Dg, float* pso, float* zto)
 {
     const float a_ = __ldg(a + c), b_ = __ldg(bv + c);
     const float da = grad_p(a + c, 1, P, h);
@@ -450,10 +423,9 @@ __device__ __forceinline__ void adj_axis(const Params& P, const float* __restric
 #pragma unroll
     for (int k = 1; k <= M; ++k) {
         const long long np = i + k * st, nm = i - k * st;
-        const long long cp_ = ic + k * st, cm_ = ic - k * st;
         const float bp = __ldg(bv + c + k), bm = __ldg(bv + c - k);
-        const float tp = bp * zeta[np] + ((1.0f + bp) * __ldg(ca + cp_)) * lam[np];
-        const float tm = bm * zeta[nm] + ((1.0f + bm) * __ldg(ca + cm_)) * lam[nm];
+        const float tp = bp * zeta[np] + ((1.0f + bp) * cav[M + k]) * lav[M + k];
+        const float tm = bm * zeta[nm] + ((1.0f + bm) * cav[M - k]) * lav[M - k];
         Lq += P.lc[k] * (tap((1.0f + bp) * tp, l0) + tap((1.0f + bm) * tm, l0));
         Dgg += P.gc[k] * ((bp * psi[np] + __ldg(dbv + c + k) * tp) - (bm * psi[nm] + __ldg(dbv + c - k) * tm));
         Dq += P.gc[k] * (__ldg(a + c + k) * tp - __ldg(a + c - k) * tm);
@@ -465,13 +437,33 @@ __device__ __forceinline__ void adj_axis(const Params& P, const float* __restric
     zto[i] = a_ * (zeta[i] + gw);
 }
 
+// Adjoint plane ring: stage q holds lambda(q) and (v*v)*dt^2 of plane q with
+// their x / y halo; lambda(it+1) of plane q - M sits in a centre ring of
+// NSC3 stages.  A CTA whose columns and planes all lie in the clear box turns
+// the model plane into gw = ((v*v)*dt^2) * lambda in place once per stage;
+// the others form the tap products from the two planes.
+struct A3Smem {
+    float l[NS3][PN];
+    float c[NS3][PN];
+    float lp[NSC3][CN3];
+    uint64_t bar[NS3];
+};
+
+struct A3Maps {
+    CUtensorMap lh[3];              // lambda buffers, (PW x PH) boxes
+    CUtensorMap lc[3];              // the same, centre boxes
+    CUtensorMap ch;                 // (v*v)*(dt*dt), (PW x PH) boxes
+};
+
 // lambda_next = exact transpose of the forward step (reference adjoint_split.cu:14-320):
 // pure interior  2 l - l_prev + Lap(gw) (difference form around gw);
 // shell          per axis outside the clear box the transposed CPML terms,
 //                inside it the bare Laplacian of gw.
-__global__ void __launch_bounds__(NTH, 4) a3_step(const Params P, const A3 A)
+__global__ void __launch_bounds__(NTH, 3) a3_step(const __grid_constant__ A3Maps MP, const Params P, const A3 A,
+                                                  const int lnow, const int lprev, int* err)
 {
-    __shared__ float pl[2][PN];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    A3Smem& sm = *reinterpret_cast<A3Smem*>(smem_raw);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BXC + tx;
     const int gx0 = blockIdx.x * BXC - M, gy0 = blockIdx.y * BYC - M;
     const int ix = blockIdx.x * BXC + tx, iy = blockIdx.y * BYC + ty;
@@ -479,83 +471,123 @@ __global__ void __launch_bounds__(NTH, 4) a3_step(const Params P, const A3 A)
     const int zb = max(M, zci * P.zc), ze = min(P.nz - M, (zci + 1) * P.zc);
     if (zb >= ze) return;
     const bool col = ix >= M && ix < P.nx - M && iy >= M && iy < P.ny - M;
-    const bool cin = ix < P.nx && iy < P.ny;
     const long long bo = (long long)b * P.S;
-    const float* __restrict__ ln = A.l_now + bo;
     const long long colo = (long long)iy * P.P + ix;
     const float invdx2 = 1.0f / (P.dx * P.dx), invdy2 = 1.0f / (P.dy * P.dy), invdz2 = 1.0f / (P.dz * P.dz);
-    float q[2 * M + 1];
-#pragma unroll
-    for (int k = 0; k < 2 * M; ++k) {
-        const long long o = (zb - M + k) * P.SP + colo;
-        q[k] = cin ? __ldg(P.ca + o) * __ldg(ln + o) : 0.f;
+    // clean: every column of the CTA inside the x / y clear box, every plane inside the z one
+    const int cx0 = blockIdx.x * BXC, cy0 = blockIdx.y * BYC;
+    const bool clean = cx0 >= P.qx0 && cx0 + BXC <= P.qx1 && cy0 >= P.qy0 && cy0 + BYC <= P.qy1 &&
+                       zb >= P.qz0 && ze <= P.qz1;
+    const int q0 = zb - M, q1 = ze + M;
+    auto slot = [&](int q) { return (q - q0) % NS3; };
+    auto cslot = [&](int z) { return (z - zb) % NSC3; };
+    auto parity = [&](int q) { return (uint32_t)(((q - q0) / NS3) & 1); };
+    auto issue = [&](int q) {
+        const int sl = slot(q), z = q - M;
+        const bool cen = z >= zb && z < ze;
+        tma::mbar_expect_tx(&sm.bar[sl], (uint32_t)(2 * PN + (cen ? CN3 : 0)) * 4u);
+        tma::load_4d(sm.l[sl], &MP.lh[lnow], &sm.bar[sl], gx0, gy0, q, b);
+        tma::load_3d(sm.c[sl], &MP.ch, &sm.bar[sl], gx0, gy0, q);
+        if (cen) tma::load_4d(sm.lp[cslot(z)], &MP.lc[lprev], &sm.bar[sl], gx0 + M, gy0 + M, z, b);
+    };
+    if (tid == 0) {
+        for (int i = 0; i < NS3; ++i) tma::mbar_init(&sm.bar[i], 1);
+        tma::fence_barrier_init();
     }
-    GwLoader L;
-    L.load(ln, P.ca, P, zb, gy0, gx0, tid);
-    L.store(pl[0], tid);
-    for (int z = zb; z < ze; ++z) {
-        const int s = (z - zb) & 1;
-        {
-            const long long o = (z + M) * P.SP + colo;
-            q[2 * M] = cin ? __ldg(P.ca + o) * __ldg(ln + o) : 0.f;
+    __syncthreads();
+    int next = q0;
+    if (tid == 0)
+        for (; next < min(q1, q0 + NS3); ++next) issue(next);
+    auto fail = [&](int q) {
+        if (tid == 0)
+            for (int r = q; r < next; ++r) tma::mbar_wait(&sm.bar[slot(r)], parity(r), err, ERR_WAIT_F3);
+    };
+    // wait for stage q and, in a clean CTA, turn its model plane into gw
+    auto arrive = [&](int q) -> bool {
+        const bool ok = tma::mbar_wait(&sm.bar[slot(q)], parity(q), err, ERR_WAIT_F3);
+        if (__syncthreads_or(!ok)) return false;
+        if (clean) {
+            float* c = sm.c[slot(q)];
+            const float* l = sm.l[slot(q)];
+            for (int e = tid; e < PN; e += NTH) c[e] = c[e] * l[e];
+            __syncthreads();
         }
-        __syncthreads();
-        const bool more = z + 1 < ze;
-        if (more) L.load(ln, P.ca, P, z + 1, gy0, gx0, tid);
+        return true;
+    };
+    for (int q = q0; q < zb + M; ++q)
+        if (!arrive(q)) { fail(q); return; }
+    const int cidx = (ty + M) * PW + (tx + M), cc = ty * BXC + tx;
+    for (int z = zb; z < ze; ++z) {
+        if (!arrive(z + M)) { fail(z + M); return; }
         if (col) {
-            const float* p = pl[s] + (ty + M) * PW + (tx + M);
+            const float* pl = sm.l[slot(z)] + cidx;
+            const float* pc = sm.c[slot(z)] + cidx;
+            // gw at offset o of plane slot s
+            auto gwat = [&](int s, int o) { return clean ? sm.c[s][cidx + o] : sm.c[s][cidx + o] * sm.l[s][cidx + o]; };
             const long long ic = z * P.SP + colo;
             const long long i = bo + ic;
-            const float gun = ln[ic];
-            const float gw = q[M];
+            const float gun = pl[0];
+            const float gw = clean ? pc[0] : pc[0] * gun;
             const bool inx = ix < P.qx0 || ix >= P.qx1;
             const bool iny = iy < P.qy0 || iy >= P.qy1;
             const bool inz = z < P.qz0 || z >= P.qz1;
-            const float lprev = __ldg(A.l_prev + i);
+            const float lprevv = sm.lp[cslot(z)][cc];
+            const int sz = slot(z);
             if (!inx && !iny && !inz) {
                 float lapx = 0.0f, lapy = 0.0f, lapz = 0.0f;
 #pragma unroll
                 for (int k = 1; k <= M; ++k) {
-                    lapx += P.lc[k] * (tap(p[k], gw) + tap(p[-k], gw));
-                    lapy += P.lc[k] * (tap(p[k * PW], gw) + tap(p[-k * PW], gw));
-                    lapz += P.lc[k] * (tap(q[M + k], gw) + tap(q[M - k], gw));
+                    lapx += P.lc[k] * (tap(gwat(sz, k), gw) + tap(gwat(sz, -k), gw));
+                    lapy += P.lc[k] * (tap(gwat(sz, k * PW), gw) + tap(gwat(sz, -k * PW), gw));
+                    lapz += P.lc[k] * (tap(gwat(slot(z + k), 0), gw) + tap(gwat(slot(z - k), 0), gw));
                 }
-                A.l_next[i] = 2.0f * gun - lprev + lapx * invdx2 + lapy * invdy2 + lapz * invdz2;
+                A.l_next[i] = 2.0f * gun - lprevv + lapx * invdx2 + lapy * invdy2 + lapz * invdz2;
             } else {
                 float Lx, Ly, Lz, Dgx = 0.f, Dgy = 0.f, Dgz = 0.f;
+                float cav[2 * M + 1], lav[2 * M + 1];
                 if (inx) {
-                    adj_axis(P, P.ax, P.bx, P.dbx, A.l_now + bo, P.ca, A.px + bo, A.zx + bo, ic, ic, 1, ix, gw,
-                             P.dx, Lx, Dgx, A.pxo + bo, A.zxo + bo);
+#pragma unroll
+                    for (int k = -M; k <= M; ++k) { cav[M + k] = pc[k]; lav[M + k] = pl[k]; }
+                    adj_axis(P, P.ax, P.bx, P.dbx, cav, lav, A.px + bo, A.zx + bo, ic, 1, ix, gw, P.dx, Lx, Dgx,
+                             A.pxo + bo, A.zxo + bo);
                 } else {
                     Lx = 0.0f;
 #pragma unroll
-                    for (int k = 1; k <= M; ++k) Lx += P.lc[k] * (tap(p[k], gw) + tap(p[-k], gw));
+                    for (int k = 1; k <= M; ++k) Lx += P.lc[k] * (tap(gwat(sz, k), gw) + tap(gwat(sz, -k), gw));
                     Lx *= invdx2;
                 }
                 if (iny) {
-                    adj_axis(P, P.ay, P.by, P.dby, A.l_now + bo, P.ca, A.py + bo, A.zy + bo, ic, ic, P.P, iy, gw,
-                             P.dy, Ly, Dgy, A.pyo + bo, A.zyo + bo);
+#pragma unroll
+                    for (int k = -M; k <= M; ++k) { cav[M + k] = pc[k * PW]; lav[M + k] = pl[k * PW]; }
+                    adj_axis(P, P.ay, P.by, P.dby, cav, lav, A.py + bo, A.zy + bo, ic, P.P, iy, gw, P.dy, Ly, Dgy,
+                             A.pyo + bo, A.zyo + bo);
                 } else {
                     Ly = 0.0f;
 #pragma unroll
-                    for (int k = 1; k <= M; ++k) Ly += P.lc[k] * (tap(p[k * PW], gw) + tap(p[-k * PW], gw));
+                    for (int k = 1; k <= M; ++k)
+                        Ly += P.lc[k] * (tap(gwat(sz, k * PW), gw) + tap(gwat(sz, -k * PW), gw));
                     Ly *= invdy2;
                 }
                 if (inz) {
-                    adj_axis(P, P.az, P.bz, P.dbz, A.l_now + bo, P.ca, A.pz + bo, A.zz + bo, ic, ic, P.SP, z, gw,
-                             P.dz, Lz, Dgz, A.pzo + bo, A.zzo + bo);
+#pragma unroll
+                    for (int k = -M; k <= M; ++k) {
+                        cav[M + k] = sm.c[slot(z + k)][cidx];
+                        lav[M + k] = sm.l[slot(z + k)][cidx];
+                    }
+                    adj_axis(P, P.az, P.bz, P.dbz, cav, lav, A.pz + bo, A.zz + bo, ic, P.SP, z, gw, P.dz, Lz, Dgz,
+                             A.pzo + bo, A.zzo + bo);
                 } else {
                     Lz = 0.0f;
 #pragma unroll
-                    for (int k = 1; k <= M; ++k) Lz += P.lc[k] * (tap(q[M + k], gw) + tap(q[M - k], gw));
+                    for (int k = 1; k <= M; ++k)
+                        Lz += P.lc[k] * (tap(gwat(slot(z + k), 0), gw) + tap(gwat(slot(z - k), 0), gw));
                     Lz *= invdz2;
                 }
-                A.l_next[i] = 2.0f * gun - lprev + (Lx + Ly + Lz - Dgx - Dgy - Dgz);
+                A.l_next[i] = 2.0f * gun - lprevv + (Lx + Ly + Lz - Dgx - Dgy - Dgz);
             }
         }
-        if (more) L.store(pl[1 - s], tid);
-#pragma unroll
-        for (int k = 0; k < 2 * M; ++k) q[k] = q[k + 1];
+        __syncthreads();
+        if (tid == 0 && next < q1) issue(next++);
     }
 }
 
@@ -571,7 +603,6 @@ struct R3 {
 // the two model fields and the two Kahan slots -- sit in a ring of
 // NSC3 = NS3 - 2M stages, filled with the halo plane M planes ahead and
 // counted on its barrier.
-constexpr int NSC3 = NS3 - 2 * M;
 struct R3Smem {
     float u[NS3][PN];
     float c[NSC3][6][CN3];
@@ -1035,8 +1066,15 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     static bool attr = false;
     if (!attr) {
         SWEEP_CUDA(cudaFuncSetAttribute(r3_recon, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(R3Smem)));
+        SWEEP_CUDA(cudaFuncSetAttribute(a3_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(A3Smem)));
         attr = true;
     }
+    A3Maps amaps;
+    for (int k = 0; k < 3; ++k) {
+        amaps.lh[k] = plane_map(w.f[k], P, P.B, true);
+        amaps.lc[k] = plane_map(w.f[k], P, P.B, false);
+    }
+    amaps.ch = plane_map(P.ca, P, 0, true);
     R3Maps rmaps;
     for (int k = 0; k < 3; ++k) {
         rmaps.uh[k] = plane_map(w.f[15 + k], P, P.B, true);
@@ -1057,7 +1095,7 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
             for (int k = 0; k < 6; ++k) { a_in[k] = w.f[3 + 2 * k + cur]; a_out[k] = w.f[3 + 2 * k + 1 - cur]; }
             A3 A{w.f[ln], w.f[lp], w.f[lx], a_in[0], a_in[1], a_in[2], a_in[3], a_in[4], a_in[5],
                  a_out[0], a_out[1], a_out[2], a_out[3], a_out[4], a_out[5]};
-            a3_step<<<grid, block, 0, st>>>(P, A);
+            a3_step<<<grid, block, sizeof(A3Smem), st>>>(amaps, P, A, ln, lp, w.err);
             SWEEP_LAUNCH_CHECK();
             if (d->nrec > 0)
                 inject3<<<gr, 128, 0, st>>>(P, w.f[lx], adj, d->rec_loc, d->nrec, it, 1, 1.f, 0);
