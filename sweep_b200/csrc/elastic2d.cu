@@ -147,6 +147,16 @@ __device__ __forceinline__ int strip_index(const Geo& G, int iz, int ix)
     return -1;
 }
 
+// Does tile (tz0, tx0) hold any strip cell?  The strips lie within M cells
+// of the physical box's edges; a tile strictly inside the reconstruction
+// region or strictly outside the box plus M has none.
+__device__ __forceinline__ bool tile_has_strips(const Geo& G, int tz0, int tx0)
+{
+    const bool outside = tx0 + TX <= G.x0 - M || tx0 >= G.x1 + M || tz0 + TZ <= G.z0 - M || tz0 >= G.z1 + M;
+    const bool inside = tx0 > G.x0 && tx0 + TX < G.x1 - 1 && tz0 > G.z0 && tz0 + TZ < G.z1 - 1;
+    return !outside && !inside;
+}
+
 // ---------------------------------------------------------------- stencils
 // D+ / D- on a shared tile (pitch HX) at flat index c (reference
 // operators/staggered.cuh:356-430, same term order).
@@ -430,6 +440,7 @@ __global__ void __launch_bounds__(NTH, 4) fwd_str(const __grid_constant__ FwdMap
     }
     const int ntl = G.ntx * G.ntz;
     const bool ring = tile_in_pml(G, tz0, tx0);
+    const bool stile = A.strips != nullptr && tile_has_strips(G, tz0, tx0);
     for (int g = 0; g < nloc; ++g) {
         const int b = b0 + g, s = g & 1;
         const bool ok = tma::mbar_wait(&sm.bar[s], (g >> 1) & 1, G.err, ERR_WAIT_FWD);
@@ -495,7 +506,7 @@ __global__ void __launch_bounds__(NTH, 4) fwd_str(const __grid_constant__ FwdMap
             A.f[SXX][so + i] = sxx;
             A.f[SZZ][so + i] = szz;
             A.f[SXZ][so + i] = sxz;
-            if (A.strips) {
+            if (stile) {
                 const int si = strip_index(G, iz, ix);
                 if (si >= 0) {
                     float* st = A.strips + (long long)b * 5 * G.nstrip + si;
