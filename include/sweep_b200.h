@@ -175,6 +175,25 @@ SWEEP_B200_API int sweep_b200_elastic_backward(const sweep_elastic_desc* d, int3
                                                void* workspace, int64_t workspace_bytes,
                                                void* stream, char* err, int32_t err_cap);
 
+/* BF16 3x3 convolution (stride 1, zero padding 1) as an implicit GEMM on the
+ * tensor cores with FP32 accumulation, for the learned FWI preconditioner.
+ * No counterpart in the reference (it has no learned component).
+ * Activations are NHWC bf16 with c a multiple of 8; 16-byte aligned.
+ *   out[p, j] = sum_{t, ch} act[p + sign * off(t), ch] * bt[j, t * c + ch] (+ bias[j])
+ * out: (n, h, w, nout) float32.  sign +1 is the forward pass with
+ * bt = weights (nout, 3, 3, c); sign -1 is the data gradient with act = the
+ * output gradient and bt = the weights transposed per tap to (c_in, 3, 3, c). */
+SWEEP_B200_API int sweep_b200_conv3x3_gemm(const void* act, const void* bt, const float* bias, float* out,
+                                           int32_t n, int32_t h, int32_t w, int32_t c, int32_t nout,
+                                           int32_t sign, void* stream, char* err, int32_t err_cap);
+
+/* Weight gradient of the same convolution: dw (co, 3, 3, c) float32,
+ * OVERWRITTEN with sum_p dy[p, o] x[p + off(t), ch]; x (n, h, w, c) and
+ * dy (n, h, w, co) bf16, c and co multiples of 8. */
+SWEEP_B200_API int sweep_b200_conv3x3_wgrad(const void* x, const void* dy, float* dw, int32_t n, int32_t h,
+                                            int32_t w, int32_t c, int32_t co, void* stream, char* err,
+                                            int32_t err_cap);
+
 /* ABI version (SWEEP_B200_ABI_VERSION) -- checked by the Python loader, like
  * the reference's sweep_core_abi_version() (reference loader.py:92-138). */
 SWEEP_B200_API int sweep_b200_abi_version(void);

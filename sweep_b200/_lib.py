@@ -32,6 +32,8 @@ SYMBOLS = (
     "sweep_b200_elastic_sizes",
     "sweep_b200_elastic_forward",
     "sweep_b200_elastic_backward",
+    "sweep_b200_conv3x3_gemm",
+    "sweep_b200_conv3x3_wgrad",
 )
 
 MEM_BOUNDARY = 0
@@ -105,6 +107,10 @@ def load():
                                                ctypes.c_char_p, c_i32]
     lib.sweep_b200_elastic_backward.argtypes = [E, c_i32, c_i32, c_p, c_p, c_p, c_p, c_p, c_p,
                                                 c_i64, c_p, ctypes.c_char_p, c_i32]
+    lib.sweep_b200_conv3x3_gemm.argtypes = [c_p, c_p, c_p, c_p, c_i32, c_i32, c_i32, c_i32, c_i32, c_i32, c_p,
+                                            ctypes.c_char_p, c_i32]
+    lib.sweep_b200_conv3x3_wgrad.argtypes = [c_p, c_p, c_p, c_i32, c_i32, c_i32, c_i32, c_i32, c_p,
+                                             ctypes.c_char_p, c_i32]
     for s in SYMBOLS[1:]:
         getattr(lib, s).restype = ctypes.c_int
     _lib = lib
