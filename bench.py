@@ -533,6 +533,58 @@ def run_gpu(args, wl):
         dist.destroy_process_group()
 
 
+# ----------------------------------------------------------------- FWI (C5)
+def run_fwi(args):
+    """Learned-preconditioned FWI against the plain illumination-preconditioned
+    gradient: the U-Net (4 levels, 32 base channels, BF16 tensor-core
+    convolutions) is trained on pairs this solver makes from seeded random
+    layered models; both FWIs then run from the same smoothed start on a
+    held-out model.  value = plain 20-iteration wall time / the learned run's
+    wall time to reach the plain run's final data misfit."""
+    import torch
+    from sweep_b200.precondition import Survey, fwi, layered_model, make_pairs, smooth, train
+    from sweep_b200.unet import UNet
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    sv = Survey(device="cuda:0")
+    t0 = time.perf_counter()
+    xs, ys = make_pairs(sv, args.pairs, seed=SEED)
+    torch.cuda.synchronize()
+    t_pairs = time.perf_counter() - t0
+    net = UNet(base=32, levels=4, seed=0).to(dev)
+    t0 = time.perf_counter()
+    hist = train(net, xs, ys, steps=args.train_steps, batch=16, lr=1e-3, seed=SEED)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    rng = np.random.default_rng(SEED + 99)
+    vt = torch.tensor(layered_model(sv.nz, sv.nx, rng), device=dev)
+    v0 = torch.tensor(smooth(vt.cpu().numpy()), device=dev)
+    with torch.no_grad():
+        obs = sv.model(vt)
+    sv.misfit(v0, obs)                                   # warm-up of the solver path
+    vp_p, hp, tp, _ = fwi(sv, v0, obs, 20)
+    vp_l, hl, tl, nl = fwi(sv, v0, obs, 20, net=net)
+    target = hp[-1]
+    reach = next((t for f, t in zip(hl[1:], tl) if f <= target), None)
+    rms = lambda v: float(((v - vt) ** 2).mean().sqrt())
+    line = {
+        "metric": "FWI time-to-misfit learned vs plain", "unit": "x (plain time / learned time)",
+        "value": (tp[-1] / reach) if reach else None, "higher_is_better": True, "n_gpus": 1,
+        "data": "synthetic (seeded random layered models)",
+        "config": {"workload": "learned-preconditioned 2-D acoustic FWI, 128x384, dh 10, dt 1 ms, nt 1200, "
+                               "8 shots, 20 iterations, 3-point line search",
+                   "pairs": args.pairs, "train_steps": args.train_steps, "batch": 16, "lr": 1e-3,
+                   "unet": "4 levels, 32 base channels, 3x3 conv, GELU, BF16 / FP32 accumulation"},
+        "plain": {"misfit": hp, "seconds": tp, "model_rms": rms(vp_p)},
+        "learned": {"misfit": hl, "seconds": tl, "model_rms": rms(vp_l), "learned_steps": nl,
+                    "seconds_to_plain_misfit": reach},
+        "start_model_rms": rms(v0),
+        "train": {"pair_seconds": t_pairs, "train_seconds": t_train, "loss_first": float(np.mean(hist[:50])),
+                  "loss_last": float(np.mean(hist[-50:]))},
+    }
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -542,7 +594,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the end-to-end leg (long workloads; the bench line then has no e2e value)")
-    ap.add_argument("--workload", default="acoustic2d", choices=sorted(WORKLOADS),
+    ap.add_argument("--pairs", type=int, default=1024, help="fwi workload: training pairs")
+    ap.add_argument("--train-steps", type=int, default=6000, help="fwi workload: U-Net training steps")
+    ap.add_argument("--workload", default="acoustic2d", choices=sorted(WORKLOADS) + ["fwi"],
                     help="acoustic2d: the 32-shot 256x768 survey (default); elastic2d: the 16-shot "
                          "400x1200 elastic survey")
     ap.add_argument("--nt", type=int, default=None,
@@ -550,6 +604,9 @@ def main():
     ap.add_argument("--shots", type=int, default=None,
                     help="fewer shots (profiling captures of a few GB only; the bench line is for the full survey)")
     args = ap.parse_args()
+    if args.workload == "fwi":
+        run_fwi(args)
+        return
     wl = WORKLOADS[args.workload]()
     if args.nt:
         wl.nt = int(args.nt)

@@ -71,7 +71,7 @@ class Survey:
             loss.backward()
         finally:
             self.solver.compute_illumination = False
-        return float(loss), m.grad.detach(), self.solver.source_illumination.detach()
+        return float(loss.detach()), m.grad.detach(), self.solver.source_illumination.detach()
 
 
 def layered_model(nz, nx, rng, vmin=1500.0, vmax=4000.0, nlayers=8):
@@ -143,32 +143,42 @@ def train(net, xs, ys, steps, batch=16, lr=1e-3, seed=0, log_every=0):
     return hist
 
 
-def _line_search(survey, vp, d, obs, f0, alpha0):
+def _line_search(survey, vp, d, obs, f0, alpha0, shrink=4):
     """3-point line search along d: misfit at 0, a and 2a; the parabola's
-    minimiser (clipped to [0, 4a]) if it improves, else the best tried point."""
-    f1 = survey.misfit(vp + alpha0 * d, obs)
-    f2 = survey.misfit(vp + 2 * alpha0 * d, obs)
-    den = f0 - 2 * f1 + f2
-    best_a, best_f = (alpha0, f1) if f1 <= f2 else (2 * alpha0, f2)
-    if den > 0:
-        a = alpha0 * (3 * f0 - 4 * f1 + f2) / (2 * den)
-        a = min(max(a, 0.0), 4 * alpha0)
-        if a > 0:
-            fa = survey.misfit(vp + a * d, obs)
-            if fa < best_f:
-                best_a, best_f = a, fa
+    minimiser (clipped to [0, 4a]) if it improves, else the best tried point.
+    Without a decrease the trial step shrinks 4-fold, ``shrink`` times at most."""
+    a0 = alpha0
+    for _ in range(shrink + 1):
+        f1 = survey.misfit(vp + a0 * d, obs)
+        f2 = survey.misfit(vp + 2 * a0 * d, obs)
+        den = f0 - 2 * f1 + f2
+        best_a, best_f = (a0, f1) if f1 <= f2 else (2 * a0, f2)
+        if den > 0:
+            a = a0 * (3 * f0 - 4 * f1 + f2) / (2 * den)
+            a = min(max(a, 0.0), 4 * a0)
+            if a > 0:
+                fa = survey.misfit(vp + a * d, obs)
+                if fa < best_f:
+                    best_a, best_f = a, fa
+        if best_f < f0:
+            return best_a, best_f
+        a0 *= 0.25
     return best_a, best_f
 
 
-def fwi(survey: Survey, v0, obs, iters, net=None, step_ms=20.0, vmin=1400.0, vmax=4600.0):
-    """Gradient-descent FWI.  Each iteration scales the direction to a
-    ``step_ms`` (m/s) maximum trial update and line-searches it.  With a
-    network, its direction is tried first and kept when the data misfit drops;
-    otherwise the plain illumination-preconditioned step is taken.  Returns
-    (vp, misfit before each iteration and after the last, wall-clock seconds
-    after each iteration, number of learned steps taken)."""
+def fwi(survey: Survey, v0, obs, iters, net=None, step_ms=20.0, vmin=1400.0, vmax=4600.0, accept=0.01):
+    """Gradient-descent FWI.  Each iteration scales the direction to unit
+    maximum and line-searches it (3 points); the first trial step is 1.5 times
+    the last step taken along that kind of direction (``step_ms`` m/s to start
+    the plain direction, 4 ``step_ms`` the learned one, which predicts the
+    whole remaining update).  With a network its direction is tried first and
+    kept when it lowers the data misfit by at least the fraction ``accept``;
+    otherwise the plain illumination-preconditioned step is taken.  Returns (vp, misfit before
+    each iteration and after the last, wall-clock seconds after each
+    iteration, number of learned steps taken)."""
     vp = v0.detach().clone()
     hist, times, learned = [], [], 0
+    a_plain, a_learned = step_ms, 4 * step_ms
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(iters):
@@ -180,17 +190,19 @@ def fwi(survey: Survey, v0, obs, iters, net=None, step_ms=20.0, vmin=1400.0, vma
             with torch.no_grad():
                 dl = net(features(g, il, vp)[None])[0, 0].float()
             dl = dl / (dl.abs().max() + 1e-30)
-            al, fl = _line_search(survey, vp, dl, obs, f0, step_ms)
-            if fl < f0:
+            al, fl = _line_search(survey, vp, dl, obs, f0, a_learned)
+            if fl < (1.0 - accept) * f0:
                 step = (fl, vp + al * dl)
+                a_learned = max(1.5 * al, step_ms)
                 learned += 1
         if step is None:
             dp = plain_direction(g, il)
             dp = dp / (dp.abs().max() + 1e-30)
-            ap, fp = _line_search(survey, vp, dp, obs, f0, step_ms)
+            ap, fp = _line_search(survey, vp, dp, obs, f0, a_plain)
             if fp >= f0:
                 break
             step = (fp, vp + ap * dp)
+            a_plain = max(1.5 * ap, 0.25 * step_ms)
         vp = step[1].clamp(vmin, vmax)
         torch.cuda.synchronize()
         hist.append(step[0])
