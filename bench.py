@@ -184,6 +184,11 @@ class AcousticWorkload:
     bytes_fwd, bytes_rev = BYTES_FWD, BYTES_REV
     kernel = "sweep::a2d::rev_kernel (fused adjoint + reconstruction + imaging step)"
     cpu_nt = 1000
+    # ncu dram__bytes_read.sum + dram__bytes_write.sum of one rev_kernel launch of
+    # this grid at 32 shots (236.6 + 96.7 MB; the capture's time axis is 20
+    # steps, which does not change a launch), per shot:
+    # profiles/acoustic2d_c2_launches.md
+    traffic = {"bytes_per_shot": 333.3e6 / 32, "source": "ncu, one rev_kernel launch, 256x768 x 32 shots (nt 20)"}
 
     def config(self, args):
         return {"workload": f"acoustic2d {NZ}x{NX} (runtime {RT[0]}x{RT[1]}), {NSHOT} shots, nt {NT}, "
@@ -224,6 +229,7 @@ class ElasticWorkload:
     kernel = ("sweep::el2d reverse step (rev_str + rev_sadj + rev_vadj: reconstruction, imaging, "
               "stress- and velocity-adjoint)")
     cpu_nt = 300
+    traffic = None
 
     def config(self, args):
         return {"workload": f"elastic2d {E_NZ}x{E_NX} (runtime {E_RT[0]}x{E_RT[1]}), {E_NSHOT} shots, "
@@ -301,6 +307,11 @@ class Acoustic3DWorkload:
     bytes_fwd, bytes_rev = BYTES_FWD, BYTES_REV
     kernel = "sweep::a3d reverse step (a3_step + r3_recon + strip kernels)"
     cpu_nt = 20
+    # ncu DRAM bytes of a3_step + r3_recon for one shot (881 + 873 MB,
+    # profiles/acoustic3d_c4_kernels.md), scaled by the shots of a reverse step:
+    # both kernels stream every shot's fields once, so traffic grows with shots
+    traffic = {"bytes_per_shot": 881e6 + 873e6,
+               "source": "ncu, a3_step + r3_recon of one 256^3 shot, x shots per step"}
     batch = A3_BATCH
 
     def config(self, args):
@@ -511,7 +522,8 @@ def run_gpu(args, wl):
                      "algorithmic_bytes_per_launch": per_launch_cells * wl.bytes_rev,
                      "launch_ms": rev_launch_ms,
                      "launch_ms_how": "CUDA events around the backward call on the launch stream / nt",
-                     "traffic": None},
+                     "traffic": wl.traffic["bytes_per_shot"] * wl.nshot if wl.traffic else None,
+                     "traffic_source": wl.traffic["source"] if wl.traffic else None},
         "forward_roofline": {"achieved": per_launch_cells * wl.bytes_fwd / (fwd_ms / wl.nt * 1e-3) / 1e9,
                              "unit": "GB/s", "bytes_per_cell_step": wl.bytes_fwd},
         "gpu_launches": args.steps * wl.launches(),

@@ -322,8 +322,21 @@ struct RevSmem {
     float c[SN];                     // (v*v)*(dt*dt) tile + halo
     float lo[TN];                    // staging (event tiles)
     float ro[TN];
+    float bx[SW], dbx[SW];           // CPML b and db/dx at the staged columns (0 off the grid)
+    float bz[SH], dbz[SH];           // the same at the staged rows
     uint64_t bar[3];
 };
+
+// Reverse-step cell ownership: thread t holds rows 4 (t / 32) .. + 3 and
+// columns 2 (t % 32), + 1 of the tile -- cell k = 2 j + i is (row j, column i)
+// of that block -- so the x and z stencil windows of its 8 cells are read
+// once as float2 rows and shared between them.
+__device__ __forceinline__ int rcell_r(int k) { return 4 * (threadIdx.x >> 5) + (k >> 1); }
+__device__ __forceinline__ int rcell_c(int k) { return 2 * (threadIdx.x & 31) + (k & 1); }
+
+__device__ __forceinline__ float2 ld2(const float* p) { return *reinterpret_cast<const float2*>(p); }
+__device__ __forceinline__ float2 ldg2(const float* p) { return __ldg(reinterpret_cast<const float2*>(p)); }
+__device__ __forceinline__ float comp(const float2 v, int e) { return e ? v.y : v.x; }
 
 // One launch per reverse step `it` of the boundary-saving backward:
 //   lambda_next = exact adjoint step of lambda (CPML transposed in the ring),
@@ -333,8 +346,12 @@ struct RevSmem {
 //   saved strips elsewhere in the physical box, and the vp image
 //   2 dt^2 u_tt lambda(it) / vp accumulated, u_tt = (u(it-1) - s(it) - 2 u(it) + u(it+1)) / dt^2;
 //   then the source added back.
-__global__ void __launch_bounds__(NTH) rev_kernel(const __grid_constant__ RevMaps MP, const Params P,
-                                                  const RevPtrs R, const int it, const int do_recon)
+// The CPML form of the adjoint is applied per axis: a cell whose x (z)
+// neighbourhood has b = db = 0 takes the plain x (z) Laplacian, which is what
+// the CPML form reduces to there, and leaves that axis's memories untouched
+// (they enter every update multiplied by b of their own cell).
+__global__ void __launch_bounds__(NTH, 2) rev_kernel(const __grid_constant__ RevMaps MP, const Params P,
+                                                     const RevPtrs R, const int it, const int do_recon)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     RevSmem& sm = *reinterpret_cast<RevSmem*>(smem_raw);
@@ -347,10 +364,25 @@ __global__ void __launch_bounds__(NTH) rev_kernel(const __grid_constant__ RevMap
     const float invdx2 = 1.0f / (P.dx * P.dx), invdz2 = 1.0f / (P.dz * P.dz);
     const float invdx = 1.0f / P.dx, invdz = 1.0f / P.dz;
     const bool ring = tx0 < P.px0 || tx0 + TX > P.px1 || tz0 < P.pz0 || tz0 + TZ > P.pz1;
-    const bool full = tx0 >= M && tx0 + TX <= P.nx - M && tz0 >= M && tz0 + TZ <= P.nz - M;
     const bool phys_any = tx0 < P.x1 && tx0 + TX > P.x0 && tz0 < P.z1 && tz0 + TZ > P.z0;
     const bool phys_tile = do_recon && phys_any;
     const uint32_t kBytes = (SN + TN + (phys_tile ? SN + TN : 0)) * 4;
+
+    // this thread's block: rows r0 .. r0+3, columns c0, c0+1 (global gz0.., gx0..)
+    const int r0 = 4 * (threadIdx.x >> 5), c0 = 2 * (threadIdx.x & 31);
+    const int gz0 = tz0 + r0, gx0 = tx0 + c0;
+    unsigned cm = 0, pm = 0, rm = 0;  // bit k: computed / physical box / reconstruction box
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) {
+        const int iz = gz0 + (k >> 1), ix = gx0 + (k & 1);
+        if (computed(P, iz, ix)) cm |= 1u << k;
+        if (iz >= P.z0 && iz < P.z1 && ix >= P.x0 && ix < P.x1) pm |= 1u << k;
+        if (iz >= P.rz0 && iz < P.rz1 && ix >= P.rx0 && ix < P.rx1) rm |= 1u << k;
+    }
+    auto xband = [&](int ix) { return ix < P.px0 || ix >= P.px1; };
+    auto zband = [&](int iz) { return iz < P.pz0 || iz >= P.pz1; };
+    const bool xc = ring && cm && (xband(gx0) || xband(gx0 + 1));
+    const bool zc = ring && cm && (zband(gz0) || zband(gz0 + 1) || zband(gz0 + 2) || zband(gz0 + 3));
 
     if (threadIdx.x == 0) {
         for (int i = 0; i < 3; ++i) tma::mbar_init(&sm.bar[i], 1);
@@ -372,23 +404,41 @@ __global__ void __launch_bounds__(NTH) rev_kernel(const __grid_constant__ RevMap
         issue(0, b0);
         if (nloc > 1) issue(1, b0 + 1);
     }
-    // per-cell model values (shared model or one shot per CTA: loaded once)
-    float cfr[CPT], vr[CPT];
+    if (ring) {
+        for (int t = threadIdx.x; t < SW + SH; t += NTH) {
+            if (t < SW) {
+                const int ix = tx0 - M + t;
+                const bool in = ix >= 0 && ix < P.nx;
+                sm.bx[t] = in ? __ldg(P.bx + ix) : 0.f;
+                sm.dbx[t] = in ? __ldg(P.dbx + ix) : 0.f;
+            } else {
+                const int q = t - SW, iz = tz0 - M + q;
+                const bool in = iz >= 0 && iz < P.nz;
+                sm.bz[q] = in ? __ldg(P.bz + iz) : 0.f;
+                sm.dbz[q] = in ? __ldg(P.dbz + iz) : 0.f;
+            }
+        }
+    }
+    // per-cell vp (shared model or one shot per CTA: loaded once; the
+    // reconstruction coefficient ((v*v)*dt)*dt is formed from it as the
+    // forward's is); a column pair is computed together or its second cell is not
+    float vr[CPT];
 #pragma unroll
-    for (int k = 0; k < CPT; ++k) {
-        const int iz = tz0 + cell_r(k), ix = tx0 + cell_c(k);
-        const bool in = computed(P, iz, ix);
-        cfr[k] = in ? __ldg(P.cf + b0 * P.ms + iz * P.P + ix) : 0.f;
-        vr[k] = in ? __ldg(P.vv + b0 * P.ms + iz * P.P + ix) : 1.f;
+    for (int j = 0; j < 4; ++j) {
+        float2 v2 = make_float2(1.f, 1.f);
+        if (cm >> (2 * j) & 1) v2 = ldg2(P.vv + b0 * P.ms + (long long)(gz0 + j) * P.P + gx0);
+        vr[2 * j] = v2.x; vr[2 * j + 1] = (cm >> (2 * j + 1) & 1) ? v2.y : 1.f;
     }
     {
         const bool ok = tma::mbar_wait(&sm.bar[2], 0, P.err, ERR_TMA_WAIT_REV);
         if (__syncthreads_or(!ok)) return;
     }
 
-    float gsum[CPT], isum_s[CPT], isum_r[CPT];
+    // illumination (when asked for) goes straight to this CTA's slot, shot by shot
+    const long long slot = (long long)(P.per_shot ? b0 : blockIdx.x) * P.S;
+    float gsum[CPT];
 #pragma unroll
-    for (int k = 0; k < CPT; ++k) { gsum[k] = 0.f; isum_s[k] = 0.f; isum_r[k] = 0.f; }
+    for (int k = 0; k < CPT; ++k) gsum[k] = 0.f;
 
     for (int g = 0; g < nloc; ++g) {
         const int b = b0 + g;
@@ -400,85 +450,209 @@ __global__ void __launch_bounds__(NTH) rev_kernel(const __grid_constant__ RevMap
         const float* slp = sm.lp[s];
         const float* sr = sm.r[s];
         const float* srp = sm.rp[s];
+        const float* sc = sm.c;
 
         float lo[CPT], ro[CPT];
 #pragma unroll
-        for (int k = 0; k < CPT; ++k) {
-            const int r = cell_r(k), c = cell_c(k);
-            const int iz = tz0 + r, ix = tx0 + c;
-            lo[k] = 0.f; ro[k] = 0.f;
-            if (!full && !computed(P, iz, ix)) continue;
-            const int i = iz * P.P + ix;
-            const int sc = (r + M) * SW + (c + M);
-            const float* pl = sl + sc;
-            const float* pc = sm.c + sc;
-            const float gun = pl[0];
-            const float gw = pc[0] * gun;
-            const bool pure = !ring || (ix >= P.px0 && ix < P.px1 && iz >= P.pz0 && iz < P.pz1);
-            if (pure) {
-                float lapx = 0.0f, lapz = 0.0f;
+        for (int k = 0; k < CPT; ++k) { lo[k] = 0.f; ro[k] = 0.f; }
+        if (cm) {
+            // c * lambda down the block's two columns, staged rows r0 .. r0+11
+            float2 G[12];
 #pragma unroll
-                for (int kk = 1; kk <= M; ++kk) {
-                    lapx += P.lc[kk] * (tap(pc[kk] * pl[kk], gw) + tap(pc[-kk] * pl[-kk], gw));
-                    lapz += P.lc[kk] * (tap(pc[kk * SW] * pl[kk * SW], gw) + tap(pc[-kk * SW] * pl[-kk * SW], gw));
-                }
-                lo[k] = 2.0f * gun - slp[r * TX + c] + lapx * invdx2 + lapz * invdz2;
-            } else {
-                const float ax_ = __ldg(P.ax + ix), az_ = __ldg(P.az + iz);
-                const float bx_ = __ldg(P.bx + ix), bz_ = __ldg(P.bz + iz);
-                const float* __restrict__ zx = R.azx + bo;
-                const float* __restrict__ zz = R.azz + bo;
-                const float* __restrict__ px = R.apx + bo;
-                const float* __restrict__ pz = R.apz + bo;
-                float* __restrict__ pxo = R.apx_o + bo;
-                float* __restrict__ pzo = R.apz_o + bo;
-                float* __restrict__ zxo = R.azx_o + bo;
-                float* __restrict__ zzo = R.azz_o + bo;
-                const float zx0 = __ldg(zx + i), zz0 = __ldg(zz + i);
-                const float gtx0 = bx_ * zx0 + (1.0f + bx_) * gw;
-                const float gtz0 = bz_ * zz0 + (1.0f + bz_) * gw;
-                const float lx0 = (1.0f + bx_) * gtx0;
-                float Lx = 0.0f, Dgx = 0.0f, Dqx = 0.0f;
-#pragma unroll
-                for (int kk = 1; kk <= M; ++kk) {
-                    const int cp = ix + kk, cm = ix - kk;
-                    const float bp = __ldg(P.bx + cp), bm = __ldg(P.bx + cm);
-                    const float tp = bp * __ldg(zx + i + kk) + ((1.0f + bp) * pc[kk]) * pl[kk];
-                    const float tm = bm * __ldg(zx + i - kk) + ((1.0f + bm) * pc[-kk]) * pl[-kk];
-                    Lx += P.lc[kk] * (tap((1.0f + bp) * tp, lx0) + tap((1.0f + bm) * tm, lx0));
-                    Dgx += P.gc[kk] * ((bp * __ldg(px + i + kk) + __ldg(P.dbx + cp) * tp)
-                                     - (bm * __ldg(px + i - kk) + __ldg(P.dbx + cm) * tm));
-                    Dqx += P.gc[kk] * (tp - tm);
-                }
-                Lx *= invdx2; Dgx *= invdx; Dqx *= invdx;
-                const float lz0 = (1.0f + bz_) * gtz0;
-                float Lz = 0.0f, Dgz = 0.0f, Dqz = 0.0f;
-#pragma unroll
-                for (int kk = 1; kk <= M; ++kk) {
-                    const int cp = iz + kk, cm = iz - kk;
-                    const int o = kk * P.P;
-                    const float bp = __ldg(P.bz + cp), bm = __ldg(P.bz + cm);
-                    const float tp = bp * __ldg(zz + i + o) + ((1.0f + bp) * pc[kk * SW]) * pl[kk * SW];
-                    const float tm = bm * __ldg(zz + i - o) + ((1.0f + bm) * pc[-kk * SW]) * pl[-kk * SW];
-                    Lz += P.lc[kk] * (tap((1.0f + bp) * tp, lz0) + tap((1.0f + bm) * tm, lz0));
-                    Dgz += P.gc[kk] * ((bp * __ldg(pz + i + o) + __ldg(P.dbz + cp) * tp)
-                                     - (bm * __ldg(pz + i - o) + __ldg(P.dbz + cm) * tm));
-                    Dqz += P.gc[kk] * (tp - tm);
-                }
-                Lz *= invdz2; Dgz *= invdz; Dqz *= invdz;
-                lo[k] = 2.0f * gun - slp[r * TX + c] + (Lx + Lz - Dgx - Dgz);
-                pxo[i] = ax_ * (__ldg(px + i) - Dqx);
-                pzo[i] = az_ * (__ldg(pz + i) - Dqz);
-                zxo[i] = ax_ * (zx0 + gw);
-                zzo[i] = az_ * (zz0 + gw);
+            for (int q = 0; q < 12; ++q) {
+                const int o = (r0 + q) * SW + c0 + M;
+                const float2 l2 = ld2(sl + o), c2 = ld2(sc + o);
+                G[q] = make_float2(c2.x * l2.x, c2.y * l2.y);
             }
-            if (phys_tile && iz >= P.z0 && iz < P.z1 && ix >= P.x0 && ix < P.x1) {
-                if (iz >= P.rz0 && iz < P.rz1 && ix >= P.rx0 && ix < P.rx1) {
-                    const float* pr = sr + sc;
-                    const float wsum = lap_s(pr, 1, P, P.dx) + lap_s(pr, SW, P, P.dz);
-                    ro[k] = 2.0f * pr[0] - srp[r * TX + c] + cfr[k] * wsum;
+            float ux[CPT];               // x part of the adjoint update
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int so = (r0 + M + j) * SW + c0;      // window start (staged column c0)
+                if (!xc) {
+                    float gw[10];
+#pragma unroll
+                    for (int p = 0; p < 5; ++p) {
+                        if (p == 2) continue;
+                        const float2 l2 = ld2(sl + so + 2 * p), c2 = ld2(sc + so + 2 * p);
+                        gw[2 * p] = c2.x * l2.x; gw[2 * p + 1] = c2.y * l2.y;
+                    }
+                    gw[4] = G[4 + j].x; gw[5] = G[4 + j].y;
+#pragma unroll
+                    for (int i = 0; i < 2; ++i) {
+                        const float g0 = gw[4 + i];
+                        float a = 0.0f;
+#pragma unroll
+                        for (int kk = 1; kk <= M; ++kk)
+                            a += P.lc[kk] * (tap(gw[4 + i + kk], g0) + tap(gw[4 + i - kk], g0));
+                        ux[2 * j + i] = a * invdx2;
+                    }
                 } else {
-                    ro[k] = __ldg(R.strips + (long long)b * P.nstrip + strip_index(P, iz, ix));
+                    const int iz = gz0 + j;
+                    const bool rowin = iz < P.nz;
+                    const long long ro_ = bo + (long long)iz * P.P;
+                    float tq[10], sq[10], hq[10], zc0[2], pc0[2];
+#pragma unroll
+                    for (int p = 0; p < 5; ++p) {
+                        const float2 l2 = ld2(sl + so + 2 * p), c2 = ld2(sc + so + 2 * p);
+                        const int ix = gx0 - M + 2 * p;
+                        float2 z2 = make_float2(0.f, 0.f), p2 = make_float2(0.f, 0.f);
+                        if (rowin && ix >= 0 && ix < P.nx) {
+                            z2 = ldg2(R.azx + ro_ + ix);
+                            p2 = ldg2(R.apx + ro_ + ix);
+                        }
+#pragma unroll
+                        for (int e = 0; e < 2; ++e) {
+                            const int q = 2 * p + e;
+                            const float bq = sm.bx[c0 + q], dbq = sm.dbx[c0 + q];
+                            const float zq = comp(z2, e), pq = comp(p2, e);
+                            tq[q] = bq * zq + ((1.0f + bq) * comp(c2, e)) * comp(l2, e);
+                            sq[q] = (1.0f + bq) * tq[q];
+                            hq[q] = bq * pq + dbq * tq[q];
+                            if (q == 4 || q == 5) { zc0[q - 4] = zq; pc0[q - 4] = pq; }
+                        }
+                    }
+#pragma unroll
+                    for (int i = 0; i < 2; ++i) {
+                        const float b_ = sm.bx[c0 + M + i];
+                        const float gwc = comp(G[4 + j], i);
+                        const float l0 = (1.0f + b_) * (b_ * zc0[i] + (1.0f + b_) * gwc);
+                        float L = 0.0f, Dg = 0.0f, Dq = 0.0f;
+#pragma unroll
+                        for (int kk = 1; kk <= M; ++kk) {
+                            L += P.lc[kk] * (tap(sq[4 + i + kk], l0) + tap(sq[4 + i - kk], l0));
+                            Dg += P.gc[kk] * (hq[4 + i + kk] - hq[4 + i - kk]);
+                            Dq += P.gc[kk] * (tq[4 + i + kk] - tq[4 + i - kk]);
+                        }
+                        ux[2 * j + i] = L * invdx2 - Dg * invdx;
+                        if (cm >> (2 * j + i) & 1) {
+                            const float a = __ldg(P.ax + gx0 + i);
+                            R.apx_o[ro_ + gx0 + i] = a * (pc0[i] - Dq * invdx);
+                            R.azx_o[ro_ + gx0 + i] = a * (zc0[i] + gwc);
+                        }
+                    }
+                }
+            }
+            // z part, then lambda_next = 2 lambda - lambda_prev + x part + z part
+            if (!zc) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+#pragma unroll
+                    for (int i = 0; i < 2; ++i) {
+                        const float g0 = comp(G[4 + j], i);
+                        float a = 0.0f;
+#pragma unroll
+                        for (int kk = 1; kk <= M; ++kk)
+                            a += P.lc[kk] * (tap(comp(G[4 + j + kk], i), g0) + tap(comp(G[4 + j - kk], i), g0));
+                        ux[2 * j + i] += a * invdz2;
+                    }
+            } else {
+                // centre terms (and the zeta update, which needs nothing else)
+                float l0[CPT];
+                const bool colin = gx0 < P.nx;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int iz = gz0 + j;
+                    const float b_ = sm.bz[r0 + M + j];
+                    float2 z2 = make_float2(0.f, 0.f);
+                    const long long o = bo + (long long)iz * P.P + gx0;
+                    if (colin && iz < P.nz) z2 = ldg2(R.azz + o);
+                    const float a = (cm >> (2 * j) & 1) ? __ldg(P.az + iz) : 0.f;
+#pragma unroll
+                    for (int i = 0; i < 2; ++i) {
+                        const float gwc = comp(G[4 + j], i);
+                        l0[2 * j + i] = (1.0f + b_) * (b_ * comp(z2, i) + (1.0f + b_) * gwc);
+                        if (cm >> (2 * j + i) & 1) R.azz_o[o + i] = a * (comp(z2, i) + gwc);
+                    }
+                }
+                // one column at a time (keeps the accumulators of 4 cells live)
+#pragma unroll 1
+                for (int i = 0; i < 2; ++i) {
+                    float L[4], Dg[4], Dq[4];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) { L[j] = 0.f; Dg[j] = 0.f; Dq[j] = 0.f; }
+                    const bool cin = colin && (i == 0 || gx0 + 1 < P.nx);
+#pragma unroll
+                    for (int q = 0; q < 12; ++q) {
+                        const int iz = gz0 - M + q;
+                        const int o = (r0 + q) * SW + c0 + M + i;
+                        float zq = 0.f, pq = 0.f;
+                        if (cin && iz >= 0 && iz < P.nz) {
+                            const long long go = bo + (long long)iz * P.P + gx0 + i;
+                            zq = __ldg(R.azz + go); pq = __ldg(R.apz + go);
+                        }
+                        const float bq = sm.bz[r0 + q], dbq = sm.dbz[r0 + q];
+                        const float t = bq * zq + ((1.0f + bq) * sc[o]) * sl[o];
+                        const float sv = (1.0f + bq) * t;
+                        const float h = bq * pq + dbq * t;
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            const int kk = q - M - j;
+                            if (kk == 0 || kk < -M || kk > M) continue;
+                            const int ka = kk < 0 ? -kk : kk;
+                            L[j] += P.lc[ka] * tap(sv, i ? l0[2 * j + 1] : l0[2 * j]);
+                            Dg[j] += kk > 0 ? P.gc[ka] * h : -(P.gc[ka] * h);
+                            Dq[j] += kk > 0 ? P.gc[ka] * t : -(P.gc[ka] * t);
+                        }
+                    }
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int k = 2 * j + i;
+                        const float d = L[j] * invdz2 - Dg[j] * invdz;
+                        if (i) ux[2 * j + 1] += d; else ux[2 * j] += d;
+                        if (cm >> k & 1) {
+                            const long long o = bo + (long long)(gz0 + j) * P.P + gx0 + i;
+                            R.apz_o[o] = __ldg(P.az + gz0 + j) * (__ldg(R.apz + o) - Dq[j] * invdz);
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const float2 lp2 = ld2(slp + (r0 + j) * TX + c0);
+                const float2 l2 = ld2(sl + (r0 + M + j) * SW + c0 + M);
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                    const int k = 2 * j + i;
+                    if (cm >> k & 1) lo[k] = 2.0f * comp(l2, i) - comp(lp2, i) + ux[k];
+                }
+            }
+
+            // reconstruction of u(it-1): stencil in the reconstruction box,
+            // saved strips in the rest of the physical box
+            if (phys_tile && pm) {
+                float2 U[12];
+#pragma unroll
+                for (int q = 0; q < 12; ++q) U[q] = ld2(sr + (r0 + q) * SW + c0 + M);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int so = (r0 + M + j) * SW + c0;
+                    float u[10];
+#pragma unroll
+                    for (int p = 0; p < 5; ++p) {
+                        if (p == 2) continue;
+                        const float2 v = ld2(sr + so + 2 * p);
+                        u[2 * p] = v.x; u[2 * p + 1] = v.y;
+                    }
+                    u[4] = U[4 + j].x; u[5] = U[4 + j].y;
+                    const float2 up2 = ld2(srp + (r0 + j) * TX + c0);
+#pragma unroll
+                    for (int i = 0; i < 2; ++i) {
+                        const int k = 2 * j + i;
+                        if (rm >> k & 1) {
+                            const float u0 = u[4 + i];
+                            float ax = 0.0f, az = 0.0f;
+#pragma unroll
+                            for (int kk = 1; kk <= M; ++kk) {
+                                ax += P.lc[kk] * (tap(u[4 + i + kk], u0) + tap(u[4 + i - kk], u0));
+                                az += P.lc[kk] * (tap(comp(U[4 + j + kk], i), u0) + tap(comp(U[4 + j - kk], i), u0));
+                            }
+                            const float wsum = ax / (P.dx * P.dx) + az / (P.dz * P.dz);
+                            const float cf = ((vr[k] * vr[k]) * P.dt) * P.dt;
+                            ro[k] = 2.0f * u0 - comp(up2, i) + cf * wsum;
+                        } else if (pm >> k & 1) {
+                            ro[k] = __ldg(R.strips + (long long)b * P.nstrip + strip_index(P, gz0 + j, gx0 + i));
+                        }
+                    }
                 }
             }
         }
@@ -490,7 +664,7 @@ __global__ void __launch_bounds__(NTH) rev_kernel(const __grid_constant__ RevMap
         if (events) {
 #pragma unroll
             for (int k = 0; k < CPT; ++k) {
-                const int o = cell_r(k) * TX + cell_c(k);
+                const int o = rcell_r(k) * TX + rcell_c(k);
                 sm.lo[o] = lo[k]; sm.ro[o] = ro[k];
             }
             __syncthreads();
@@ -516,7 +690,7 @@ __global__ void __launch_bounds__(NTH) rev_kernel(const __grid_constant__ RevMap
             }
 #pragma unroll
             for (int k = 0; k < CPT; ++k) {
-                const int o = cell_r(k) * TX + cell_c(k);
+                const int o = rcell_r(k) * TX + rcell_c(k);
                 lo[k] = sm.lo[o]; ro[k] = sm.ro[o];
             }
         }
@@ -525,21 +699,31 @@ __global__ void __launch_bounds__(NTH) rev_kernel(const __grid_constant__ RevMap
         float* ln = R.l_next + bo;
         float gl[CPT];
 #pragma unroll
-        for (int k = 0; k < CPT; ++k) {
-            const int r = cell_r(k), c = cell_c(k);
-            const int iz = tz0 + r, ix = tx0 + c;
-            gl[k] = 0.f;
-            if (!full && !computed(P, iz, ix)) continue;
-            ln[iz * P.P + ix] = lo[k];
-            if (!(phys_any && iz >= P.z0 && iz < P.z1 && ix >= P.x0 && ix < P.x1)) continue;
-            if (do_recon) {
-                const float u0 = sr[(r + M) * SW + (c + M)];
-                const float up = srp[r * TX + c];
-                const float utt = (ro[k] - 2 * u0 + up) / dt2;
-                gl[k] = 2.f * P.dt * P.dt * utt * lo[k] / vr[k];
-                if (R.illum_s) isum_s[k] += utt * utt;
+        for (int j = 0; j < 4; ++j) {
+            const long long o = (long long)(gz0 + j) * P.P + gx0;
+            const int k0 = 2 * j;
+            if ((cm >> k0 & 3) == 3) {
+                *reinterpret_cast<float2*>(ln + o) = make_float2(lo[k0], lo[k0 + 1]);
+            } else if (cm >> k0 & 1) {
+                ln[o] = lo[k0];
             }
-            if (R.illum_s) isum_r[k] += lo[k] * lo[k];
+            const float2 u02 = ld2(sr + (r0 + M + j) * SW + c0 + M);
+            const float2 up2 = ld2(srp + (r0 + j) * TX + c0);
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const int k = k0 + i;
+                gl[k] = 0.f;
+                if (!(pm >> k & 1)) continue;
+                float utt = 0.f;
+                if (do_recon) {
+                    utt = (ro[k] - 2 * comp(u02, i) + comp(up2, i)) / dt2;
+                    gl[k] = 2.f * P.dt * P.dt * utt * lo[k] / vr[k];
+                }
+                if (R.illum_s) {
+                    R.illum_s[slot + o + i] += utt * utt;
+                    R.illum_r[slot + o + i] += lo[k] * lo[k];
+                }
+            }
         }
         if (events && do_recon) {
             __syncthreads();
@@ -549,14 +733,20 @@ __global__ void __launch_bounds__(NTH) rev_kernel(const __grid_constant__ RevMap
             }
             __syncthreads();
 #pragma unroll
-            for (int k = 0; k < CPT; ++k) ro[k] = sm.ro[cell_r(k) * TX + cell_c(k)];
+            for (int k = 0; k < CPT; ++k) ro[k] = sm.ro[rcell_r(k) * TX + rcell_c(k)];
         }
         if (phys_tile) {
             float* rn = R.r_next + bo;
 #pragma unroll
-            for (int k = 0; k < CPT; ++k) {
-                const int iz = tz0 + cell_r(k), ix = tx0 + cell_c(k);
-                if (iz >= P.z0 && iz < P.z1 && ix >= P.x0 && ix < P.x1) rn[iz * P.P + ix] = ro[k];
+            for (int j = 0; j < 4; ++j) {
+                const long long o = (long long)(gz0 + j) * P.P + gx0;
+                const int k0 = 2 * j;
+                if ((pm >> k0 & 3) == 3) {
+                    *reinterpret_cast<float2*>(rn + o) = make_float2(ro[k0], ro[k0 + 1]);
+                } else {
+                    if (pm >> k0 & 1) rn[o] = ro[k0];
+                    if (pm >> (k0 + 1) & 1) rn[o + 1] = ro[k0 + 1];
+                }
             }
         }
 #pragma unroll
@@ -567,18 +757,15 @@ __global__ void __launch_bounds__(NTH) rev_kernel(const __grid_constant__ RevMap
 
     // Kahan-compensated flush into this CTA's accumulator slot (per shot for
     // per-shot models, which run one shot per CTA; per shot group otherwise)
-    if (phys_any && (do_recon || R.illum_s)) {
-        const long long so = (long long)(P.per_shot ? b0 : blockIdx.x) * P.S;
+    if (pm && do_recon) {
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
-            const int iz = tz0 + cell_r(k), ix = tx0 + cell_c(k);
-            if (!(iz >= P.z0 && iz < P.z1 && ix >= P.x0 && ix < P.x1)) continue;
-            const long long o = so + iz * P.P + ix;
+            if (!(pm >> k & 1)) continue;
+            const long long o = slot + (long long)(gz0 + (k >> 1)) * P.P + gx0 + (k & 1);
             const float y = gsum[k] - R.gcomp[o];
             const float t = R.gacc[o] + y;
             R.gcomp[o] = (t - R.gacc[o]) - y;
             R.gacc[o] = t;
-            if (R.illum_s) { R.illum_s[o] += isum_s[k]; R.illum_r[o] += isum_r[k]; }
         }
     }
 }
