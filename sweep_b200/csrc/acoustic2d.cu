@@ -44,6 +44,7 @@ constexpr int SH = TZ + 2 * M;       // staged tile height
 constexpr int SN = SW * SH;          // staged halo tile, floats
 constexpr int TN = TX * TZ;          // centre tile, floats
 constexpr int CPT = TN / NTH;        // cells per thread (8)
+constexpr int kMaxG = 16;            // shots per CTA, at most
 
 enum ErrCode { ERR_TMA_WAIT_FWD = 1, ERR_TMA_WAIT_REV = 2 };
 
@@ -160,14 +161,55 @@ __device__ __forceinline__ bool computed(const Params& P, int iz, int ix)
     return iz >= M && iz < P.nz - M && ix >= M && ix < P.nx - M;
 }
 
+
 __device__ __forceinline__ int cell_r(int k) { return (threadIdx.x >> 5) + 8 * (k >> 1); }
 __device__ __forceinline__ int cell_c(int k) { return (threadIdx.x & 31) + 32 * (k & 1); }
+
+// Reverse-step cell ownership: thread t holds rows 4 (t / 32) .. + 3 and
+// columns 2 (t % 32), + 1 of the tile -- cell k = 2 j + i is (row j, column i)
+// of that block -- so the x and z stencil windows of its 8 cells are read
+// once as float2 rows and shared between them.
+__device__ __forceinline__ int rcell_r(int k) { return 4 * (threadIdx.x >> 5) + (k >> 1); }
+__device__ __forceinline__ int rcell_c(int k) { return 2 * (threadIdx.x & 31) + (k & 1); }
+
+__device__ __forceinline__ float2 ld2(const float* p) { return *reinterpret_cast<const float2*>(p); }
+__device__ __forceinline__ float2 ldg2(const float* p) { return __ldg(reinterpret_cast<const float2*>(p)); }
+__device__ __forceinline__ float comp(const float2 v, int e) { return e ? v.y : v.x; }
+
+// Save u_now of this tile's boundary strips from its staged copy `now`
+// (rows of SW floats, origin at (tz0 - M, tx0 - M)) into the strip set of one
+// shot, `dst`: the four strip rectangles of strip_index, cut to the tile and
+// walked by the whole CTA (rows of 8 or 64 slots, one cell per thread).
+__device__ __forceinline__ void save_strips(const Params& P, const float* now, float* __restrict__ dst,
+                                            int tx0, int tz0)
+{
+    const int bw = P.x1 - P.x0, zi0 = P.z0 + P.wzl, zi1 = P.z1 - P.wzh;
+    auto rect = [&](int za, int zb, int xa, int xb, int base, int rw, int rz, int rx) {
+        za = max(za, tz0); zb = min(zb, tz0 + TZ);
+        xa = max(xa, tx0); xb = min(xb, tx0 + TX);
+        if (za >= zb || xa >= xb) return;
+        const int w = xb - xa;
+        const int sh = w <= 8 ? 3 : 6;
+        const int n = (zb - za) << sh;
+        for (int e = threadIdx.x; e < n; e += NTH) {
+            const int c = e & ((1 << sh) - 1);
+            if (c >= w) continue;
+            const int iz = za + (e >> sh), ix = xa + c;
+            dst[base + (iz - rz) * rw + (ix - rx)] = now[(iz - tz0 + M) * SW + (ix - tx0 + M)];
+        }
+    };
+    rect(P.z0, zi0, P.x0, P.x1, 0, bw, P.z0, P.x0);
+    rect(zi1, P.z1, P.x0, P.x1, P.n_top, bw, zi1, P.x0);
+    rect(zi0, zi1, P.x0, P.x0 + P.wxl, P.n_top + P.n_bot, P.wxl, zi0, P.x0);
+    rect(zi0, zi1, P.x1 - P.wxh, P.x1, P.n_top + P.n_bot + P.n_left, P.wxh, zi0, P.x1 - P.wxh);
+}
 
 // ----------------------------------------------------------- forward step
 struct FwdSmem {
     float now[2][SN];
     float prev[2][TN];
     float out[TN];
+    int4 evr[kMaxG];                 // per shot of the CTA: source and receiver event ranges
     uint64_t bar[2];
 };
 
@@ -206,6 +248,10 @@ __global__ void __launch_bounds__(NTH) fwd_kernel(const __grid_constant__ FwdMap
     if (threadIdx.x == 0) {
         issue(0, b0);
         if (nloc > 1) issue(1, b0 + 1);
+    }
+    if (threadIdx.x < nloc) {
+        const int key = (b0 + threadIdx.x) * ntiles + tile;
+        sm.evr[threadIdx.x] = make_int4(P.src.off[key], P.src.off[key + 1], P.rec.off[key], P.rec.off[key + 1]);
     }
 
     // model coefficients of this thread's cells (shared model: once per CTA)
@@ -275,16 +321,12 @@ __global__ void __launch_bounds__(NTH) fwd_kernel(const __grid_constant__ FwdMap
                 }
             }
             out[k] = 2.0f * p[0] - prev[r * TX + c] + cf[k] * w;
-            if (strip_tile) {
-                const int si = strip_index(P, iz, ix);
-                if (si >= 0) F.strips[(long long)b * P.nstrip + si] = p[0];
-            }
         }
+        if (strip_tile) save_strips(P, now, F.strips + (long long)b * P.nstrip, tx0, tz0);
 
         // point sources and receivers of this (shot, tile)
-        const int key = b * ntiles + tile;
-        const int s_beg = P.src.off[key], s_end = P.src.off[key + 1];
-        const int r_beg = P.rec.off[key], r_end = P.rec.off[key + 1];
+        const int4 er = sm.evr[g];
+        const int s_beg = er.x, s_end = er.y, r_beg = er.z, r_end = er.w;
         if (s_beg != s_end || r_beg != r_end) {
 #pragma unroll
             for (int k = 0; k < CPT; ++k) sm.out[cell_r(k) * TX + cell_c(k)] = out[k];
@@ -324,19 +366,9 @@ struct RevSmem {
     float ro[TN];
     float bx[SW], dbx[SW];           // CPML b and db/dx at the staged columns (0 off the grid)
     float bz[SH], dbz[SH];           // the same at the staged rows
+    int4 evr[kMaxG];                 // per shot of the CTA: source and receiver event ranges
     uint64_t bar[3];
 };
-
-// Reverse-step cell ownership: thread t holds rows 4 (t / 32) .. + 3 and
-// columns 2 (t % 32), + 1 of the tile -- cell k = 2 j + i is (row j, column i)
-// of that block -- so the x and z stencil windows of its 8 cells are read
-// once as float2 rows and shared between them.
-__device__ __forceinline__ int rcell_r(int k) { return 4 * (threadIdx.x >> 5) + (k >> 1); }
-__device__ __forceinline__ int rcell_c(int k) { return 2 * (threadIdx.x & 31) + (k & 1); }
-
-__device__ __forceinline__ float2 ld2(const float* p) { return *reinterpret_cast<const float2*>(p); }
-__device__ __forceinline__ float2 ldg2(const float* p) { return __ldg(reinterpret_cast<const float2*>(p)); }
-__device__ __forceinline__ float comp(const float2 v, int e) { return e ? v.y : v.x; }
 
 // One launch per reverse step `it` of the boundary-saving backward:
 //   lambda_next = exact adjoint step of lambda (CPML transposed in the ring),
@@ -403,6 +435,10 @@ __global__ void __launch_bounds__(NTH, 2) rev_kernel(const __grid_constant__ Rev
         tma::load_3d(sm.c, &MP.ch, &sm.bar[2], tx0 - M, tz0 - M, P.ms ? b0 : 0);
         issue(0, b0);
         if (nloc > 1) issue(1, b0 + 1);
+    }
+    if (threadIdx.x < nloc) {
+        const int key = (b0 + threadIdx.x) * ntiles + tile;
+        sm.evr[threadIdx.x] = make_int4(P.src.off[key], P.src.off[key + 1], P.rec.off[key], P.rec.off[key + 1]);
     }
     if (ring) {
         for (int t = threadIdx.x; t < SW + SH; t += NTH) {
@@ -657,9 +693,8 @@ __global__ void __launch_bounds__(NTH, 2) rev_kernel(const __grid_constant__ Rev
             }
         }
 
-        const int key = b * ntiles + tile;
-        const int s_beg = P.src.off[key], s_end = P.src.off[key + 1];
-        const int r_beg = P.rec.off[key], r_end = P.rec.off[key + 1];
+        const int4 er = sm.evr[g];
+        const int s_beg = er.x, s_end = er.y, r_beg = er.z, r_end = er.w;
         const bool events = s_beg != s_end || r_beg != r_end;
         if (events) {
 #pragma unroll
@@ -872,9 +907,9 @@ static int choose_group(int ntiles, int B, const char* env, int preferred)
 {
     if (const char* e = getenv(env)) {
         const int g = atoi(e);
-        if (g >= 1) return std::min(g, B);
+        if (g >= 1) return std::min({g, B, kMaxG});
     }
-    int G = std::min(preferred, B);
+    int G = std::min({preferred, B, kMaxG});
     while (G > 1 && (long long)ntiles * ((B + G - 1) / G) < 2LL * 148) --G;
     return std::max(G, 1);
 }
@@ -929,7 +964,7 @@ static Plan make_plan(const sweep_acoustic_desc* d)
     P.ntz = (d->nz + TZ - 1) / TZ;
     const int ntiles = P.ntx * P.ntz;
     pl.Gf = P.per_shot ? 1 : choose_group(ntiles, P.B, "SWEEP_B200_SHOTS_PER_CTA_FWD", 2);
-    pl.Gr = P.per_shot ? 1 : choose_group(ntiles, P.B, "SWEEP_B200_SHOTS_PER_CTA_REV", 4);
+    pl.Gr = P.per_shot ? 1 : choose_group(ntiles, P.B, "SWEEP_B200_SHOTS_PER_CTA_REV", 8);
     // blockIdx.x = shot group (fastest), blockIdx.y = tile slot
     pl.gridf = dim3((P.B + pl.Gf - 1) / pl.Gf, ntiles);
     pl.gridr = dim3((P.B + pl.Gr - 1) / pl.Gr, ntiles);
