@@ -80,6 +80,7 @@ struct RevMaps {
     CUtensorMap lh[3], lt[3];        // adjoint field buffers: halo / centre boxes
     CUtensorMap rh[3], rt[3];        // reconstruction buffers: halo / centre boxes
     CUtensorMap ch;                  // (v*v)*(dt*dt), halo box
+    CUtensorMap am[8];               // adjoint CPML memories: x ones with an x halo, z ones with a z halo
 };
 
 struct FwdPtrs {
@@ -102,6 +103,7 @@ struct RevPtrs {
     float* gacc; float* gcomp;       // Kahan accumulator slots (nslot, S)
     float* illum_s; float* illum_r;  // (nslot, S) or null
     int lnow, lprev, rnow, rprev;    // buffer indices
+    int cur;                         // CPML memories read this step: am[0 + cur], am[2 + cur], am[4 + cur], am[6 + cur]
 };
 
 // ------------------------------------------------------------------ device
@@ -428,6 +430,13 @@ __global__ void __launch_bounds__(NTH, 2) rev_kernel(const __grid_constant__ Rev
         if (phys_tile) {
             tma::load_3d(sm.r[s], &MP.rh[R.rnow], &sm.bar[s], tx0 - M, tz0 - M, b);
             tma::load_3d(sm.rp[s], &MP.rt[R.rprev], &sm.bar[s], tx0, tz0, b);
+        }
+        if (ring) {
+            // the CPML memories this shot's ring cells read, into L2 ahead of use
+            tma::prefetch_3d(&MP.am[0 + R.cur], tx0 - M, tz0, b);
+            tma::prefetch_3d(&MP.am[4 + R.cur], tx0 - M, tz0, b);
+            tma::prefetch_3d(&MP.am[2 + R.cur], tx0, tz0 - M, b);
+            tma::prefetch_3d(&MP.am[6 + R.cur], tx0, tz0 - M, b);
         }
     };
     if (threadIdx.x == 0) {
@@ -1168,6 +1177,16 @@ static CUtensorMap field_map(const float* base, const Params& P, int nb, bool ha
     return tma::make_map(base, 3, dims, strides, box);
 }
 
+// A CPML memory (full grid, pitched) with the box its ring cells read: x
+// memories (TX + 2M) x TZ, z memories TX x (TZ + 2M).
+static CUtensorMap mem_map(const float* base, const Params& P, bool xmem)
+{
+    const uint64_t dims[3] = {(uint64_t)P.nx, (uint64_t)P.nz, (uint64_t)P.B};
+    const uint64_t strides[2] = {(uint64_t)P.P, (uint64_t)P.S};
+    const uint32_t box[3] = {(uint32_t)(xmem ? SW : TX), (uint32_t)(xmem ? TZ : SH), 1u};
+    return tma::make_map(base, 3, dims, strides, box);
+}
+
 static size_t fwd_smem() { return sizeof(FwdSmem); }
 static size_t rev_smem() { return sizeof(RevSmem); }
 
@@ -1391,6 +1410,7 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
         maps.rt[i] = field_map(w.r[i], P, P.B, false);
     }
     maps.ch = field_map(w.c.ca, P, pl.nm, true);
+    for (int i = 0; i < 8; ++i) maps.am[i] = mem_map(w.aux[i], P, (i >> 1) == 0 || (i >> 1) == 2);
     RevPtrs R{};
     R.adj = adj; R.grad_w = grad_w;
     R.gacc = w.gacc; R.gcomp = w.gcomp;
@@ -1406,6 +1426,7 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
             R.lprev = lp; R.lnow = ln; R.l_next = w.l[lx];
             R.apx = w.aux[0 + cur]; R.apz = w.aux[2 + cur]; R.azx = w.aux[4 + cur]; R.azz = w.aux[6 + cur];
             R.apx_o = w.aux[1 - cur]; R.apz_o = w.aux[3 - cur]; R.azx_o = w.aux[5 - cur]; R.azz_o = w.aux[7 - cur];
+            R.cur = cur;
             R.rprev = rp; R.rnow = rn; R.r_next = w.r[rx];
             R.strips = do_recon ? strips_of(it - 1) : nullptr;
             rev_kernel<<<pl.gridr, NTH, rev_smem(), st>>>(maps, P, R, it, do_recon);

@@ -121,6 +121,16 @@ __device__ __forceinline__ void load_3d(void* dst, const CUtensorMap* map, uint6
         : "memory");
 }
 
+// Prefetch the box at (x, y, z) of `map` into L2 (no shared memory, no
+// completion to wait for).
+__device__ __forceinline__ void prefetch_3d(const CUtensorMap* map, int x, int y, int z)
+{
+    asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(x), "r"(y), "r"(z)
+                 : "memory");
+}
+
 __device__ __forceinline__ void load_4d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y, int z, int w)
 {
     asm volatile(
