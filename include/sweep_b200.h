@@ -194,6 +194,11 @@ SWEEP_B200_API int sweep_b200_conv3x3_wgrad(const void* x, const void* dy, float
                                             int32_t w, int32_t c, int32_t co, void* stream, char* err,
                                             int32_t err_cap);
 
+/* Waits for `stream` and reports (then clears) a timed-out tensor-core wait
+ * in any convolution launched since the last call: the convolution entries
+ * return at launch, so their device-side failures surface here. */
+SWEEP_B200_API int sweep_b200_conv3x3_status(void* stream, char* err, int32_t err_cap);
+
 /* ABI version (SWEEP_B200_ABI_VERSION) -- checked by the Python loader, like
  * the reference's sweep_core_abi_version() (reference loader.py:92-138). */
 SWEEP_B200_API int sweep_b200_abi_version(void);

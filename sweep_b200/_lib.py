@@ -34,6 +34,7 @@ SYMBOLS = (
     "sweep_b200_elastic_backward",
     "sweep_b200_conv3x3_gemm",
     "sweep_b200_conv3x3_wgrad",
+    "sweep_b200_conv3x3_status",
 )
 
 MEM_BOUNDARY = 0
@@ -111,6 +112,7 @@ def load():
                                             ctypes.c_char_p, c_i32]
     lib.sweep_b200_conv3x3_wgrad.argtypes = [c_p, c_p, c_p, c_i32, c_i32, c_i32, c_i32, c_i32, c_p,
                                              ctypes.c_char_p, c_i32]
+    lib.sweep_b200_conv3x3_status.argtypes = [c_p, ctypes.c_char_p, c_i32]
     for s in SYMBOLS[1:]:
         getattr(lib, s).restype = ctypes.c_int
     _lib = lib

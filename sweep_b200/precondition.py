@@ -24,6 +24,7 @@ import torch
 from .equations import Acoustic
 from .propagator import PropTorch
 from .signal import ricker
+from .unet import check as unet_check
 
 __all__ = ["Survey", "layered_model", "plain_direction", "make_pairs", "train", "fwi"]
 
@@ -140,6 +141,7 @@ def train(net, xs, ys, steps, batch=16, lr=1e-3, seed=0, log_every=0):
         hist.append(float(loss))
         if log_every and s % log_every == 0:
             print(f"step {s}: loss {hist[-1]:.4f}")
+    unet_check(xs.device)
     return hist
 
 

@@ -21,7 +21,7 @@ import torch.nn.functional as F
 
 from . import _lib
 
-__all__ = ["conv3x3", "UNet"]
+__all__ = ["conv3x3", "check", "UNet"]
 
 
 def _stream(t):
@@ -71,6 +71,13 @@ class _Conv3x3(torch.autograd.Function):
 def conv3x3(x, w, b):
     """BF16 3x3 convolution (stride 1, zero padding 1), FP32 accumulation."""
     return _Conv3x3.apply(x, w, b)
+
+
+def check(device=None):
+    """Wait for the current stream and raise if a convolution launched since
+    the last check timed out on the device (its outputs are then invalid)."""
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+    _lib.call("sweep_b200_conv3x3_status", torch.cuda.current_stream(dev).cuda_stream)
 
 
 class _Conv(torch.nn.Module):
@@ -123,6 +130,7 @@ class UNet(torch.nn.Module):
             self.out.w.mul_(0.1)
 
     def forward(self, x):
+        check(x.device)                  # the previous step's convolutions (forward and backward)
         b, c, h, w = x.shape
         if h % 2 ** (self.levels - 1) or w % 2 ** (self.levels - 1):
             raise ValueError(f"input size {h}x{w} must be a multiple of {2 ** (self.levels - 1)}")

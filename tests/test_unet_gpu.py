@@ -37,6 +37,7 @@ def test_conv_kernels_match_float64(n, h, w, c, co):
     out = torch.empty((n, h, w, co), device=DEV)
     _lib.call("sweep_b200_conv3x3_gemm", xd.data_ptr(), wd.data_ptr(), bd.data_ptr(), out.data_ptr(),
               n, h, w, c, co, 1, st)
+    _lib.call("sweep_b200_conv3x3_status", st)
     ref = _ref_conv(x, wt) + bias.double()
     assert rel(out.cpu(), ref) < 1e-5
     # data gradient: the adjoint of the forward
@@ -44,6 +45,7 @@ def test_conv_kernels_match_float64(n, h, w, c, co):
     gx = torch.empty((n, h, w, c), device=DEV)
     _lib.call("sweep_b200_conv3x3_gemm", dyd.data_ptr(), wtt.data_ptr(), None, gx.data_ptr(),
               n, h, w, co, c, -1, st)
+    _lib.call("sweep_b200_conv3x3_status", st)
     xr = x.double().requires_grad_(True)
     yr = _ref_conv(xr, wt)
     yr.backward(dy.double())
