@@ -185,10 +185,10 @@ class AcousticWorkload:
     kernel = "sweep::a2d::rev_kernel (fused adjoint + reconstruction + imaging step)"
     cpu_nt = 1000
     # ncu dram__bytes_read.sum + dram__bytes_write.sum of one rev_kernel launch of
-    # this grid at 32 shots (236.6 + 96.7 MB; the capture's time axis is 20
+    # this grid at 32 shots (241.9 + 69.3 MB; the capture's time axis is 20
     # steps, which does not change a launch), per shot:
     # profiles/acoustic2d_c2_launches.md
-    traffic = {"bytes_per_shot": 333.3e6 / 32, "source": "ncu, one rev_kernel launch, 256x768 x 32 shots (nt 20)"}
+    traffic = {"bytes_per_shot": 311.2e6 / 32, "source": "ncu, one rev_kernel launch, 256x768 x 32 shots (nt 20)"}
 
     def config(self, args):
         return {"workload": f"acoustic2d {NZ}x{NX} (runtime {RT[0]}x{RT[1]}), {NSHOT} shots, nt {NT}, "
