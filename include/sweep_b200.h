@@ -74,6 +74,14 @@ typedef struct sweep_acoustic_desc {
 /* Memory modes of the backward (reference src/sweep/propagator/options.py:186-246). */
 #define SWEEP_MEM_BOUNDARY   0   /* save boundary strips each step; replay them in reverse */
 #define SWEEP_MEM_CHECKPOINT 1   /* save state every `ckpt_every` steps; re-run each chunk */
+/* Boundary saving with the strips held in fewer bytes (reference
+ * BoundarySaving(storage_dtype=...), options.py:194-212; boundarysaver.cu:
+ * 906-1100).  Compute stays FP32.  fp16 and int8 quantise each face of the
+ * strip set per shot in blocks of 256 cells against the block's max |value|
+ * (one FP32 scale per block); bf16 rounds each value.  2-D acoustic only. */
+#define SWEEP_MEM_BOUNDARY_FP16 2
+#define SWEEP_MEM_BOUNDARY_BF16 3
+#define SWEEP_MEM_BOUNDARY_INT8 4
 
 /* Bytes the caller must allocate: `workspace` (scratch, reusable between calls
  * once the previous call has finished on its stream) and `tape` (written by

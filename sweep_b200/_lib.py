@@ -39,6 +39,9 @@ SYMBOLS = (
 
 MEM_BOUNDARY = 0
 MEM_CHECKPOINT = 1
+MEM_BOUNDARY_FP16 = 2            # boundary saving, strips stored as scaled fp16 / bf16 / scaled int8
+MEM_BOUNDARY_BF16 = 3
+MEM_BOUNDARY_INT8 = 4
 
 
 class AcousticDesc(ctypes.Structure):

@@ -30,6 +30,9 @@
 //   * point sources, receivers and boundary strips are handled by the CTA that
 //     owns the cell, in the same launch as the stencil;
 //   * one launch per forward step and one per reverse step.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include "acoustic2d.cuh"
 #include "tma.cuh"
 
@@ -47,6 +50,23 @@ constexpr int CPT = TN / NTH;        // cells per thread (8)
 constexpr int kMaxG = 16;            // shots per CTA, at most
 
 enum ErrCode { ERR_TMA_WAIT_FWD = 1, ERR_TMA_WAIT_REV = 2 };
+
+// Boundary-strip storage of the boundary-saving tape.  fp32 and bf16 keep the
+// strip set (each cell once, strip_index order); fp16 and int8 keep the
+// reference's four faces (top and bottom rows across the box, left and right
+// columns down the whole box, corners in two faces), each quantised per shot
+// in blocks of kQB cells against the block's max |value|
+// (reference boundarysaver.cu:906-1100).
+enum StripFmt { SF_F32 = 0, SF_F16 = 1, SF_BF16 = 2, SF_I8 = 3 };
+constexpr int kQB = 256;
+
+struct StripStore {
+    int fmt;                         // StripFmt
+    int w;                           // face band width (M + 1)
+    int cells[4], blocks[4];         // per shot and face (top, bottom, left, right): scaled formats
+    long long pay[4], scl[4];        // byte offsets of each face's codes and scales in a step slot
+    long long step;                  // bytes of one step slot
+};
 
 struct Params {
     int B, nz, nx, nt, nsrc, nrec;
@@ -69,6 +89,7 @@ struct Params {
     EventTable src, rec;
     const int* order;                // tile slots, heaviest (CPML ring) tiles first
     int* err;
+    StripStore st;
 };
 
 struct FwdMaps {
@@ -88,7 +109,8 @@ struct FwdPtrs {
     const float* psix; const float* psiz; float* psixn; float* psizn;
     float* zetax; float* zetaz;
     float* record;                   // (B, nt, nrec)
-    float* strips;                   // this step's strip slot (B, nstrip) or null
+    void* strips;                    // this step's strips (B, nstrip): float, or bf16 when sbf16; or null
+    int sbf16;
     int now, prev;                   // buffer indices of u_now / u_prev
 };
 
@@ -97,7 +119,7 @@ struct RevPtrs {
     const float *apx, *apz, *azx, *azz;   // adjoint CPML memories (read)
     float *apx_o, *apz_o, *azx_o, *azz_o; // adjoint CPML memories (written)
     float* r_next;
-    const float* strips;             // saved U[it-1] strips (B, nstrip) or null
+    const void* strips;              // step slot holding the strips of U[it-1] (format P.st), or null
     const float* adj;                // (B, nt, nrec)
     float* grad_w;                   // (B, nsrc, nt) or null
     float* gacc; float* gcomp;       // Kahan accumulator slots (nslot, S)
@@ -158,6 +180,54 @@ __device__ __forceinline__ int strip_index(const Params& P, int iz, int ix)
     return -1;
 }
 
+// Face f (0 top, 1 bottom, 2 left, 3 right) cell `idx` of the scaled
+// formats -> grid cell (reference boundarysaver.cu:72-112 face indexing:
+// top / bottom (width, box width), left / right (box height, width)).
+__device__ __forceinline__ void face_cell(const Params& P, int f, int idx, int& iz, int& ix)
+{
+    const int w = P.st.w, bw = P.x1 - P.x0;
+    if (f < 2) {
+        const int r = idx / bw;
+        iz = (f == 0 ? P.z0 : P.z1 - w) + r;
+        ix = P.x0 + (idx - r * bw);
+    } else {
+        const int r = idx / w;
+        iz = P.z0 + r;
+        ix = (f == 2 ? P.x0 : P.x1 - w) + (idx - r * w);
+    }
+}
+
+// The face a scaled-format restore reads strip cell (iz, ix) from: the last of
+// the faces holding it in the reference's restore order top, bottom, left,
+// right (a corner cell takes its left or right face's value).
+__device__ __forceinline__ int face_index(const Params& P, int iz, int ix, int& f)
+{
+    const int w = P.st.w, bw = P.x1 - P.x0;
+    if (ix >= P.x1 - w) { f = 3; return (iz - P.z0) * w + (ix - (P.x1 - w)); }
+    if (ix < P.x0 + w) { f = 2; return (iz - P.z0) * w + (ix - P.x0); }
+    if (iz >= P.z1 - w) { f = 1; return (iz - (P.z1 - w)) * bw + (ix - P.x0); }
+    f = 0;
+    return (iz - P.z0) * bw + (ix - P.x0);
+}
+
+// Saved value of strip cell (iz, ix) of shot b from a step slot (dequantised
+// as the reference does: fp16 code x scale; int8 (code - 128) x scale / 127).
+__device__ __forceinline__ float strip_value(const Params& P, const void* slot, int b, int iz, int ix)
+{
+    const StripStore& S = P.st;
+    if (S.fmt == SF_F32) return __ldg(static_cast<const float*>(slot) + (long long)b * P.nstrip + strip_index(P, iz, ix));
+    if (S.fmt == SF_BF16)
+        return __bfloat162float(static_cast<const __nv_bfloat16*>(slot)[(long long)b * P.nstrip + strip_index(P, iz, ix)]);
+    int f;
+    const int i = face_index(P, iz, ix, f);
+    const char* base = static_cast<const char*>(slot);
+    const float scale = reinterpret_cast<const float*>(base + S.scl[f])[(long long)b * S.blocks[f] + i / kQB];
+    const long long e = (long long)b * S.cells[f] + i;
+    if (S.fmt == SF_F16) return __half2float(reinterpret_cast<const __half*>(base + S.pay[f])[e]) * scale;
+    const float s = scale * (1.0f / 127.0f);
+    return ((float)reinterpret_cast<const uint8_t*>(base + S.pay[f])[e] - 128.0f) * s;
+}
+
 __device__ __forceinline__ bool computed(const Params& P, int iz, int ix)
 {
     return iz >= M && iz < P.nz - M && ix >= M && ix < P.nx - M;
@@ -182,7 +252,8 @@ __device__ __forceinline__ float comp(const float2 v, int e) { return e ? v.y : 
 // (rows of SW floats, origin at (tz0 - M, tx0 - M)) into the strip set of one
 // shot, `dst`: the four strip rectangles of strip_index, cut to the tile and
 // walked by the whole CTA (rows of 8 or 64 slots, one cell per thread).
-__device__ __forceinline__ void save_strips(const Params& P, const float* now, float* __restrict__ dst,
+template <class T>
+__device__ __forceinline__ void save_strips(const Params& P, const float* now, T* __restrict__ dst,
                                             int tx0, int tz0)
 {
     const int bw = P.x1 - P.x0, zi0 = P.z0 + P.wzl, zi1 = P.z1 - P.wzh;
@@ -197,7 +268,7 @@ __device__ __forceinline__ void save_strips(const Params& P, const float* now, f
             const int c = e & ((1 << sh) - 1);
             if (c >= w) continue;
             const int iz = za + (e >> sh), ix = xa + c;
-            dst[base + (iz - rz) * rw + (ix - rx)] = now[(iz - tz0 + M) * SW + (ix - tx0 + M)];
+            dst[base + (iz - rz) * rw + (ix - rx)] = static_cast<T>(now[(iz - tz0 + M) * SW + (ix - tx0 + M)]);
         }
     };
     rect(P.z0, zi0, P.x0, P.x1, 0, bw, P.z0, P.x0);
@@ -324,7 +395,12 @@ __global__ void __launch_bounds__(NTH) fwd_kernel(const __grid_constant__ FwdMap
             }
             out[k] = 2.0f * p[0] - prev[r * TX + c] + cf[k] * w;
         }
-        if (strip_tile) save_strips(P, now, F.strips + (long long)b * P.nstrip, tx0, tz0);
+        if (strip_tile) {
+            if (F.sbf16)
+                save_strips(P, now, static_cast<__nv_bfloat16*>(F.strips) + (long long)b * P.nstrip, tx0, tz0);
+            else
+                save_strips(P, now, static_cast<float*>(F.strips) + (long long)b * P.nstrip, tx0, tz0);
+        }
 
         // point sources and receivers of this (shot, tile)
         const int4 er = sm.evr[g];
@@ -695,7 +771,7 @@ __global__ void __launch_bounds__(NTH, 2) rev_kernel(const __grid_constant__ Rev
                             const float cf = ((vr[k] * vr[k]) * P.dt) * P.dt;
                             ro[k] = 2.0f * u0 - comp(up2, i) + cf * wsum;
                         } else if (pm >> k & 1) {
-                            ro[k] = __ldg(R.strips + (long long)b * P.nstrip + strip_index(P, gz0 + j, gx0 + i));
+                            ro[k] = strip_value(P, R.strips, b, gz0 + j, gx0 + i);
                         }
                     }
                 }
@@ -811,6 +887,49 @@ __global__ void __launch_bounds__(NTH, 2) rev_kernel(const __grid_constant__ Rev
             R.gcomp[o] = (t - R.gacc[o]) - y;
             R.gacc[o] = t;
         }
+    }
+}
+
+// One step's strips (fp32 strip set, `strips`) into the scaled faces of a step
+// slot: one CTA per (shot, face, block of kQB cells) -- max |value| of the
+// block, its scale, the codes (reference boundarysaver.cu:957-990, 1050-1080:
+// int8 round(v 127 / max) + 128 clamped to [0, 255]; fp16 v / max rounded).
+__global__ void __launch_bounds__(kQB) quantize_strips(const Params P, const float* __restrict__ strips, void* slot)
+{
+    const StripStore& S = P.st;
+    const int per = S.blocks[0] + S.blocks[1] + S.blocks[2] + S.blocks[3];
+    const int b = blockIdx.x / per;
+    int j = blockIdx.x - b * per, f = 0;
+    while (f < 3 && j >= S.blocks[f]) { j -= S.blocks[f]; ++f; }
+    const int idx = j * kQB + threadIdx.x;
+    const bool in = idx < S.cells[f];
+    float v = 0.f;
+    if (in) {
+        int iz, ix;
+        face_cell(P, f, idx, iz, ix);
+        v = strips[(long long)b * P.nstrip + strip_index(P, iz, ix)];
+    }
+    float m = fabsf(v);
+#pragma unroll
+    for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __shared__ float wmax[kQB / 32];
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = m;
+    __syncthreads();
+    m = wmax[0];
+#pragma unroll
+    for (int i = 1; i < kQB / 32; ++i) m = fmaxf(m, wmax[i]);
+    char* base = static_cast<char*>(slot);
+    if (threadIdx.x == 0) reinterpret_cast<float*>(base + S.scl[f])[(long long)b * S.blocks[f] + j] = m;
+    if (!in) return;
+    const long long e = (long long)b * S.cells[f] + idx;
+    if (S.fmt == SF_F16) {
+        const float inv = m > 0.0f ? 1.0f / m : 0.0f;
+        reinterpret_cast<__half*>(base + S.pay[f])[e] = __float2half(v * inv);
+    } else {
+        const float qs = m > 0.0f ? 127.0f / m : 0.0f;
+        int q = __float2int_rn(v * qs) + 128;
+        q = q < 0 ? 0 : (q > 255 ? 255 : q);
+        reinterpret_cast<uint8_t*>(base + S.pay[f])[e] = (uint8_t)q;
     }
 }
 
@@ -994,6 +1113,7 @@ struct FwdWork {
     Common c;
     float* u[3];
     float *psix, *psiz, *psixn, *psizn, *zetax, *zetaz;
+    float* scratch;                  // one step's fp32 strips ahead of their quantisation (scaled formats)
 };
 
 struct RevWork {
@@ -1030,6 +1150,7 @@ static FwdWork carve_fwd(Carve& c, const Plan& pl)
     w.psix = c.take<float>(n); w.psiz = c.take<float>(n);
     w.psixn = c.take<float>(n); w.psizn = c.take<float>(n);
     w.zetax = c.take<float>(n); w.zetaz = c.take<float>(n);
+    if (pl.P.st.fmt == SF_F16 || pl.P.st.fmt == SF_I8) w.scratch = c.take<float>((long long)pl.P.B * pl.P.nstrip);
     return w;
 }
 
@@ -1050,20 +1171,56 @@ static RevWork carve_rev(Carve& c, const Plan& pl, bool illum)
     return w;
 }
 
-// tape: strips of every step (nt, B, nstrip), then (U[nt-1], U[nt]) pitched
+// Strip storage of a memory mode: the step-slot layout of the boundary-saving
+// tape (the checkpoint mode keeps its chunk strips as fp32).
+static void set_store(Plan& pl, int mem_mode)
+{
+    Params& P = pl.P;
+    StripStore& S = P.st;
+    S = StripStore{};
+    S.w = M + 1;
+    S.fmt = mem_mode == SWEEP_MEM_BOUNDARY_FP16 ? SF_F16
+          : mem_mode == SWEEP_MEM_BOUNDARY_BF16 ? SF_BF16
+          : mem_mode == SWEEP_MEM_BOUNDARY_INT8 ? SF_I8 : SF_F32;
+    auto up = [](long long v, long long a) { return (v + a - 1) / a * a; };
+    if (S.fmt == SF_F32 || S.fmt == SF_BF16) {
+        S.step = up((long long)P.B * P.nstrip * (S.fmt == SF_F32 ? 4 : 2), 256);
+        return;
+    }
+    const int bw = P.x1 - P.x0, bh = P.z1 - P.z0;
+    SWEEP_REQUIRE(bw >= 2 * S.w && bh >= 2 * S.w,
+                  "acoustic2d: fp16 / int8 strip storage needs a physical box of at least %d cells per axis "
+                  "(got %d x %d)", 2 * S.w, bh, bw);
+    const int cells[4] = {S.w * bw, S.w * bw, bh * S.w, bh * S.w};
+    const int esz = S.fmt == SF_F16 ? 2 : 1;
+    long long off = 0;
+    for (int f = 0; f < 4; ++f) {
+        S.cells[f] = cells[f];
+        S.blocks[f] = (cells[f] + kQB - 1) / kQB;
+        S.pay[f] = off;
+        off = up(off + (long long)P.B * cells[f] * esz, 16);
+    }
+    for (int f = 0; f < 4; ++f) {
+        S.scl[f] = off;
+        off = up(off + (long long)P.B * S.blocks[f] * 4, 16);
+    }
+    S.step = up(off, 256);
+}
+
+// tape: one strip slot per step (P.st.step bytes), then (U[nt-1], U[nt]) pitched
 static int64_t tape_bytes(const Plan& pl)
 {
-    Carve c(nullptr);
-    c.take<float>((long long)pl.P.nt * pl.P.B * pl.P.nstrip);
-    c.take<float>(2LL * pl.P.B * pl.P.S);
-    return c.off;
+    return (int64_t)pl.P.nt * pl.P.st.step + 2LL * pl.P.B * pl.P.S * 4;
+}
+
+static void* tape_slot(const void* tape, const Plan& pl, int it)
+{
+    return const_cast<char*>(static_cast<const char*>(tape)) + (long long)it * pl.P.st.step;
 }
 
 static float* tape_last(void* tape, const Plan& pl)
 {
-    Carve c(tape);
-    c.take<float>((long long)pl.P.nt * pl.P.B * pl.P.nstrip);
-    return c.take<float>(2LL * pl.P.B * pl.P.S);
+    return static_cast<float*>(tape_slot(tape, pl, pl.P.nt));
 }
 
 // Checkpointed boundary saving (SWEEP_MEM_CHECKPOINT, chunk length k): for
@@ -1215,9 +1372,11 @@ static void carve_rev_ckpt(Carve& c, const Plan& pl, bool illum, int k, RevWork&
 
 static void check_mode(int mem_mode, int ckpt_every)
 {
-    SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY || mem_mode == SWEEP_MEM_CHECKPOINT,
+    SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY || mem_mode == SWEEP_MEM_CHECKPOINT ||
+                      mem_mode == SWEEP_MEM_BOUNDARY_FP16 || mem_mode == SWEEP_MEM_BOUNDARY_BF16 ||
+                      mem_mode == SWEEP_MEM_BOUNDARY_INT8,
                   "acoustic2d: unknown memory mode %d", mem_mode);
-    SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY || ckpt_every >= 1,
+    SWEEP_REQUIRE(mem_mode != SWEEP_MEM_CHECKPOINT || ckpt_every >= 1,
                   "acoustic2d: checkpoint interval must be >= 1 (got %d)", ckpt_every);
 }
 
@@ -1225,6 +1384,7 @@ void sizes(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, int64_t* 
 {
     check_mode(mem_mode, ckpt_every);
     Plan pl = make_plan(d);
+    set_store(pl, mem_mode);
     Carve cf(nullptr);
     carve_fwd(cf, pl);
     Carve cr(nullptr);
@@ -1282,12 +1442,20 @@ static void forward_steps(const Plan& pl, const FwdMaps& maps, const FwdWork& w,
     FwdPtrs F{};
     F.record = record;
     F.zetax = w.zetax; F.zetaz = w.zetaz;
+    const bool scaled = PF.st.fmt == SF_F16 || PF.st.fmt == SF_I8;
+    const int qblocks = PF.B * (PF.st.blocks[0] + PF.st.blocks[1] + PF.st.blocks[2] + PF.st.blocks[3]);
     for (int it = it0; it < it1; ++it) {
         F.now = S.in; F.prev = S.ip; F.u_next = w.u[S.ix];
         F.psix = S.px; F.psiz = S.pz; F.psixn = S.pxn; F.psizn = S.pzn;
-        F.strips = strips_of(it);
+        void* slot = strips_of(it);
+        F.strips = (slot && scaled) ? static_cast<void*>(w.scratch) : slot;
+        F.sbf16 = PF.st.fmt == SF_BF16;
         fwd_kernel<<<pl.gridf, NTH, fwd_smem(), st>>>(maps, PF, F, it);
         SWEEP_LAUNCH_CHECK();
+        if (slot && scaled) {
+            quantize_strips<<<qblocks, kQB, 0, st>>>(PF, w.scratch, slot);
+            SWEEP_LAUNCH_CHECK();
+        }
         const int t = S.ip; S.ip = S.in; S.in = S.ix; S.ix = t;
         std::swap(S.px, S.pxn); std::swap(S.pz, S.pzn);
     }
@@ -1298,13 +1466,14 @@ static void copy_dd(float* dst, const float* src, long long n, cudaStream_t st)
     SWEEP_CUDA(cudaMemcpyAsync(dst, src, n * 4, cudaMemcpyDeviceToDevice, st));
 }
 
-void forward_with(const sweep_acoustic_desc* d, int ckpt_every, float* record, void* tape, void* ws,
+void forward_with(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* record, void* tape, void* ws,
                   int64_t ws_bytes, cudaStream_t st, const HostStage* stage)
 {
     SWEEP_REQUIRE(record != nullptr || d->nrec == 0, "acoustic2d forward: null record");
     SWEEP_REQUIRE(d->vp != nullptr, "acoustic2d forward: null vp");
     set_attrs();
     Plan pl = make_plan(d);
+    set_store(pl, ckpt_every > 0 ? SWEEP_MEM_CHECKPOINT : mem_mode);
     Carve c(ws);
     FwdWork w = carve_fwd(c, pl);
     SWEEP_REQUIRE(ws != nullptr && ws_bytes >= c.off, "acoustic2d forward: workspace too small (%lld < %lld)",
@@ -1326,10 +1495,9 @@ void forward_with(const sweep_acoustic_desc* d, int ckpt_every, float* record, v
     FwdState S;
     S.px = w.psix; S.pz = w.psiz; S.pxn = w.psixn; S.pzn = w.psizn;
     if (ckpt_every <= 0) {
-        float* strips = static_cast<float*>(tape);
         forward_steps(pl, maps, w, record, S, 0, d->nt,
-                      [&](int it) { return strips ? strips + (long long)it * P.B * P.nstrip : nullptr; }, st);
-        if (strips) {
+                      [&](int it) { return tape ? tape_slot(tape, pl, it) : nullptr; }, st);
+        if (tape) {
             float* last = tape_last(tape, pl);
             // (U[nt-1], U[nt]) per shot, pitched
             copy_dd(last, w.u[S.ip], n, st);
@@ -1361,7 +1529,8 @@ void forward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* 
     sizes(d, mem_mode, ckpt_every, &need_ws, &need_tape);
     SWEEP_REQUIRE(ws != nullptr && ws_bytes >= need_ws, "acoustic2d forward: workspace too small (%lld < %lld)",
                   (long long)ws_bytes, (long long)need_ws);
-    forward_with(d, mem_mode == SWEEP_MEM_CHECKPOINT ? ckpt_every : 0, record, tape, ws, ws_bytes, st, nullptr);
+    forward_with(d, mem_mode, mem_mode == SWEEP_MEM_CHECKPOINT ? ckpt_every : 0, record, tape, ws, ws_bytes, st,
+                 nullptr);
 }
 
 void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const float* adj, const void* tape,
@@ -1377,6 +1546,7 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     SWEEP_REQUIRE((illum_s == nullptr) == (illum_r == nullptr), "acoustic2d backward: pass both illuminations or neither");
     set_attrs();
     Plan pl = make_plan(d);
+    set_store(pl, mem_mode);
     Carve c(ws);
     const bool illum = illum_s != nullptr;
     const bool ckpt = mem_mode == SWEEP_MEM_CHECKPOINT;
@@ -1437,13 +1607,12 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
         }
     };
     if (!ckpt) {
-        const float* strips = static_cast<const float*>(tape);
         const float* last = tape_last(const_cast<void*>(tape), pl);
         // seed: prev = U[nt], now = U[nt-1]  (reference driver_traits.cuh:493-505; the
         // rim outside the physical box is never read by the reconstruction)
         copy_dd(w.r[0], last + n, n, st);
         copy_dd(w.r[1], last, n, st);
-        reverse(0, d->nt, [&](int t) { return strips + (long long)t * P.B * P.nstrip; });
+        reverse(0, d->nt, [&](int t) { return tape_slot(tape, pl, t); });
     } else {
         const int k = ckpt_every, C = nchunks(pl, k);
         const FwdMaps fmaps = fwd_maps(fw, P);

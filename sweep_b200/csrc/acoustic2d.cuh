@@ -26,8 +26,8 @@ int64_t forward_only_bytes(const sweep_acoustic_desc* d);
 // Event-table staging sizes: shot-tile keys (+1) and events of each kind.
 void stage_sizes(const sweep_acoustic_desc* d, int64_t* nkey, int64_t* nev_src, int64_t* nev_rec);
 // Forward with an explicit workspace and host staging (stage == nullptr: growable);
-// ckpt_every > 0 writes the checkpoint-mode tape.
-void forward_with(const sweep_acoustic_desc* d, int ckpt_every, float* record, void* tape, void* ws,
+// `mem_mode` as in the C ABI; ckpt_every > 0 writes the checkpoint-mode tape.
+void forward_with(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* record, void* tape, void* ws,
                   int64_t ws_bytes, cudaStream_t st, const HostStage* stage);
 
 }  // namespace a2d

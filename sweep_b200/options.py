@@ -10,13 +10,29 @@ from dataclasses import dataclass
 class BoundarySaving:
     """Save the (M+1)-wide boundary strips of the physical box every step on
     the GPU and rebuild the forward field backwards from them (the impl='c'
-    default)."""
+    default).
+
+    ``storage_dtype`` (reference ``options.py:194-212``) sets how the saved
+    strips are held; compute stays FP32:
+
+    * ``'fp32'``: 4 bytes per cell, exact;
+    * ``'bf16'``: 2 bytes per cell, each value rounded to bfloat16;
+    * ``'fp16'``: 2 bytes per cell plus one FP32 scale per 256 cells: each
+      face of the strip set is normalised per shot, block by block, by the
+      block's max |value| before rounding to fp16 (safe at any amplitude);
+    * ``'int8'``: 1 byte per cell plus the same scales: symmetric 8-bit codes
+      of the normalised values.
+
+    The reduced formats are built for 2-D acoustic propagation."""
     storage: str = "gpu"
+    storage_dtype: str = "fp32"
 
     def __post_init__(self):
         if self.storage != "gpu":
             raise NotImplementedError("sweep_b200 keeps the boundary ring in GPU memory only "
                                       "(storage='gpu')")
+        if self.storage_dtype not in ("fp32", "fp16", "bf16", "int8"):
+            raise ValueError("BoundarySaving.storage_dtype must be 'fp32', 'fp16', 'bf16', or 'int8'.")
 
 
 @dataclass(frozen=True)

@@ -363,7 +363,12 @@ class PropTorch(torch.nn.Module):
     def _mem_mode(self):
         if isinstance(self.memory, Ckpt):
             return _lib.MEM_CHECKPOINT, int(self.memory.chunks)
-        return _lib.MEM_BOUNDARY, 0
+        sd = getattr(self.memory, "storage_dtype", "fp32")
+        if sd != "fp32" and (self.equation.NDIM != 2 or isinstance(self.equation, Elastic)):
+            raise NotImplementedError(f"BoundarySaving(storage_dtype={sd!r}) is built for 2-D acoustic "
+                                      "propagation only; use 'fp32' here")
+        return {"fp32": _lib.MEM_BOUNDARY, "fp16": _lib.MEM_BOUNDARY_FP16, "bf16": _lib.MEM_BOUNDARY_BF16,
+                "int8": _lib.MEM_BOUNDARY_INT8}[sd], 0
 
     # ---------------------------------------------------------------- forward
     def forward(self, wavelet, sources, receivers, models=None, max_vel=4500.0, pml_freq=25.0):

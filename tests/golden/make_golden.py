@@ -168,6 +168,35 @@ def acoustic2d_pershot():
     )
 
 
+def acoustic2d_storage():
+    """Boundary saving with the strips held as fp16 / bf16 / int8 (reference
+    BoundarySaving(storage_dtype=...)): 3 shots on a 48 x 300 layered model, so
+    each strip face spans several 256-cell quantisation blocks."""
+    rng = np.random.default_rng(23)
+    nz, nx, nt, dt, dh, abcn = 48, 300, 300, 0.001, 10.0, 10
+    vp_true = _layered(nz, nx, rng, 1500.0, 3200.0, 5)
+    vp_init = np.full((nz, nx), 1900.0, np.float32) + 25.0 * rng.standard_normal((nz, nx)).astype(np.float32)
+    w = _wavelet(nt, dt, 15.0, 0.06)
+    src = np.array([[40, 6], [150, 3], [260, 20]], np.int64)
+    rx = np.arange(4, nx - 4, 6)
+    rec = np.broadcast_to(np.stack([rx, np.full(rx.size, 2)], -1), (3, rx.size, 2)).copy()
+    out = {}
+    for sd in ("fp32", "fp16", "bf16", "int8"):
+        eq = Acoustic(spatial_order=8, device="cpu")
+        solver = PropTorch(eq, shape=(nz, nx), dh=dh, dt=dt, abcn=abcn, impl="c", device="cpu",
+                           memory=BoundarySaving(storage_dtype=sd))
+        if sd == "fp32":
+            obs = _forward(solver, w, src, rec, [vp_true])
+        r = _run(solver, w, src, rec, [vp_init], obs, False)
+        out[f"grad_vp_{sd}"] = r["grad0"]
+        out[f"loss_{sd}"] = r["loss"]
+    np.savez_compressed(
+        OUT / "acoustic2d_storage.npz",
+        nz=nz, nx=nx, nt=nt, dt=dt, dh=dh, abcn=abcn, order=8,
+        vp_true=vp_true, vp_init=vp_init, wavelet=w, src=src, rec=rec, obs=obs, **out,
+    )
+
+
 def acoustic3d():
     """A small 3-D case: 2 shots, 6 receivers each, order 8, CPML 8."""
     rng = np.random.default_rng(3)
@@ -242,6 +271,7 @@ CASES = {
     "acoustic2d_c1": acoustic2d_c1,
     "acoustic2d_multi": acoustic2d_multi,
     "acoustic2d_pershot": acoustic2d_pershot,
+    "acoustic2d_storage": acoustic2d_storage,
     "acoustic3d": acoustic3d,
     "elastic2d": elastic2d,
 }

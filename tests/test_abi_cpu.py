@@ -135,3 +135,35 @@ def test_checkpoint_tape_is_smaller_for_long_runs(kind):
     assert ws_c.value > ws_b.value
     with pytest.raises(RuntimeError, match="interval"):
         _lib.call(fn, d, _lib.MEM_CHECKPOINT, 0, ws_c, tape_c)
+
+
+def test_reduced_strip_storage_tape_sizes():
+    """Boundary-saving tapes by strip format (host-side sizes query): bf16
+    about half of fp32, fp16 half plus one FP32 scale per 256 cells of each
+    face, int8 a quarter plus the scales; fp16 / int8 refuse a physical box
+    narrower than two bands, and 3-D refuses the reduced formats."""
+    from sweep_b200 import _lib
+    nt = 400
+    d = _desc(nz=120, nx=160, nt=nt)
+    got = {}
+    for name, mode in (("fp32", _lib.MEM_BOUNDARY), ("fp16", _lib.MEM_BOUNDARY_FP16),
+                       ("bf16", _lib.MEM_BOUNDARY_BF16), ("int8", _lib.MEM_BOUNDARY_INT8)):
+        ws, tape = _lib.c_i64(), _lib.c_i64()
+        _lib.call("sweep_b200_acoustic_sizes", d, mode, 0, ws, tape)
+        got[name] = tape.value
+    n = 2 * 120 * 160 * 4 * 2                 # the last two states, pitched rows of 160 floats
+    strips = {k: v - n for k, v in got.items()}
+    assert 0.49 < strips["bf16"] / strips["fp32"] < 0.52
+    assert 0.5 < strips["fp16"] / strips["fp32"] < 0.56
+    assert 0.25 < strips["int8"] / strips["fp32"] < 0.31
+    small = _desc(nz=26, nx=160, nt=nt)        # an 8-row physical box
+    ws, tape = _lib.c_i64(), _lib.c_i64()
+    _lib.call("sweep_b200_acoustic_sizes", small, _lib.MEM_BOUNDARY_BF16, 0, ws, tape)
+    with pytest.raises(RuntimeError, match="at least 10 cells"):
+        _lib.call("sweep_b200_acoustic_sizes", small, _lib.MEM_BOUNDARY_INT8, 0, ws, tape)
+    d3 = _desc(nz=40, nx=40, nt=10)
+    d3.ndim, d3.ny = 3, 40
+    for i in range(6):
+        d3.pad[i] = 5
+    with pytest.raises(RuntimeError, match="memory mode"):
+        _lib.call("sweep_b200_acoustic_sizes", d3, _lib.MEM_BOUNDARY_INT8, 0, ws, tape)

@@ -1,0 +1,57 @@
+"""Boundary saving with the strips held as fp16 / bf16 / int8, on the GPU,
+against the reference's own runs of the same storage formats (golden fixture
+``acoustic2d_storage``: reference BoundarySaving(storage_dtype=...)).
+
+Two bars per format (written here):
+  * the gradient within 1e-3 relative L2 of the reference's gradient for that
+    format (the path's gradient bar);
+  * the change the format makes to the gradient (format minus fp32) within
+    ``PERT_TOL`` relative L2 of the reference's change.  A quantiser with other
+    blocks, scales or rounding gives a change of the same size but a different
+    pattern (relative error near 1), so this pins the codes themselves; the
+    bound leaves room for the float32 noise between the two codes (about 7e-7
+    of the gradient) against changes of 1.3e-5 (fp16) to 3.1e-4 (int8), and for
+    bf16 / int8 roundings that tip the other way on values that differ in the
+    last float32 bit (measured on a B200: 6.5e-2 fp16, 4.5e-2 bf16, 1.7e-2 int8)."""
+import numpy as np
+import pytest
+import torch
+
+from tests._util import load, rel
+
+pytestmark = pytest.mark.gpu
+DEV = torch.device("cuda:0")
+GRAD_TOL = 1e-3
+PERT_TOL = {"fp16": 0.25, "bf16": 0.1, "int8": 0.05}
+
+
+def _grad(d, storage_dtype):
+    from sweep_b200 import Acoustic, BoundarySaving, PropTorch
+    s = PropTorch(Acoustic(spatial_order=8, device=DEV), shape=tuple(d["vp_true"].shape),
+                  dh=float(d["dh"]), dt=float(d["dt"]), abcn=int(d["abcn"]), device=DEV,
+                  memory=BoundarySaving(storage_dtype=storage_dtype))
+    vp = torch.tensor(d["vp_init"], device=DEV, requires_grad=True)
+    pred = s(torch.tensor(d["wavelet"], device=DEV), d["src"], d["rec"], models=[vp])
+    loss = 0.5 * ((pred - torch.tensor(d["obs"], device=DEV)) ** 2).sum()
+    loss.backward()
+    torch.cuda.synchronize()
+    return vp.grad.double().cpu().numpy()
+
+
+def test_fp32_baseline_matches_reference():
+    d = load("acoustic2d_storage")
+    assert rel(_grad(d, "fp32"), d["grad_vp_fp32"]) < GRAD_TOL
+
+
+@pytest.mark.parametrize("sd", ["fp16", "bf16", "int8"])
+def test_reduced_storage_matches_reference(sd):
+    d = load("acoustic2d_storage")
+    g32 = _grad(d, "fp32")
+    g = _grad(d, sd)
+    ref32, ref = d["grad_vp_fp32"].astype(np.float64), d[f"grad_vp_{sd}"].astype(np.float64)
+    err = rel(g, ref)
+    pert = rel(g - g32, ref - ref32)
+    print(f"{sd}: gradient vs reference {err:.2e}; change vs reference change {pert:.2e} "
+          f"(change {rel(ref, ref32):.2e} of the gradient)")
+    assert err < GRAD_TOL
+    assert pert < PERT_TOL[sd]
