@@ -17,6 +17,9 @@
 // while the current plane computes.  Every field is pitched (x rows of
 // P = round_up(nx, 32) floats).  Point sources, receivers and boundary strips
 // are small gather / scatter kernels between the stencil launches.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include "common.cuh"
 #include "tma.cuh"
 
@@ -28,6 +31,23 @@ constexpr int BXC = 32, BYC = 8;               // columns per CTA
 constexpr int PW = BXC + 2 * M, PH = BYC + 2 * M;
 constexpr int PN = PW * PH;                    // staged plane, floats
 constexpr int NTH = BXC * BYC;
+
+// Boundary-strip storage of the boundary-saving tape.  fp32 and bf16 keep the
+// strip set (each cell once, strip_coord order); fp16 and int8 keep the
+// reference's six faces (z faces across the box, y faces down the whole box,
+// x faces through it; edges in two or three faces), each quantised per shot
+// in blocks of kQB cells against the block's max |value| (reference
+// boundarysaver.cu:207-330 face layout, 906-1100 quantisation).
+enum StripFmt { SF_F32 = 0, SF_F16 = 1, SF_BF16 = 2, SF_I8 = 3 };
+constexpr int kQB = 256;
+
+struct StripStore {
+    int fmt;                         // StripFmt
+    int w;                           // face band width (M + 1)
+    int cells[6], blocks[6];         // per shot and face (top, bottom, front, back, left, right)
+    long long pay[6], scl[6];        // byte offsets of each face's codes and scales in a step slot
+    long long step;                  // bytes of one step slot
+};
 
 struct Params {
     int B, nz, ny, nx, nt, nsrc, nrec;
@@ -43,6 +63,7 @@ struct Params {
     long long n_top, n_bot, nring, nstrip;
     const float *az, *bz, *dbz, *ay, *by, *dby, *ax, *bx, *dbx;
     const float *cf, *ca, *vv;                 // model fields, pitched (one copy: shared model)
+    StripStore st;
 };
 
 // ------------------------------------------------------------------ device
@@ -115,6 +136,57 @@ __device__ __forceinline__ void strip_coord(const Params& P, long long s, int& i
     iy = P.y0 + P.wyl + (int)(r / ww);
     const int c = (int)(r % ww);
     ix = c < P.wxl ? P.x0 + c : P.x1 - P.wxh + (c - P.wxl);
+}
+
+// Inverse of strip_coord: the strip-set index of a strip cell.
+__device__ __forceinline__ long long strip_index3(const Params& P, int iz, int iy, int ix)
+{
+    const long long bx = P.x1 - P.x0, by = P.y1 - P.y0;
+    if (iz < P.z0 + P.wzl) return ((long long)(iz - P.z0) * by + (iy - P.y0)) * bx + (ix - P.x0);
+    if (iz >= P.z1 - P.wzh) return P.n_top + ((long long)(iz - (P.z1 - P.wzh)) * by + (iy - P.y0)) * bx + (ix - P.x0);
+    long long s = P.n_top + P.n_bot + (long long)(iz - (P.z0 + P.wzl)) * P.nring;
+    if (iy < P.y0 + P.wyl) return s + (long long)(iy - P.y0) * bx + (ix - P.x0);
+    s += (long long)P.wyl * bx;
+    if (iy >= P.y1 - P.wyh) return s + (long long)(iy - (P.y1 - P.wyh)) * bx + (ix - P.x0);
+    s += (long long)P.wyh * bx;
+    const int ww = P.wxl + P.wxh;
+    return s + (long long)(iy - (P.y0 + P.wyl)) * ww + (ix < P.x0 + P.wxl ? ix - P.x0 : P.wxl + ix - (P.x1 - P.wxh));
+}
+
+// Face f (0 top, 1 bottom, 2 front, 3 back, 4 left, 5 right) cell `idx` of
+// the scaled formats -> grid cell (z faces (width, box y, box x); y faces
+// (box z, width, box x); x faces (box z, box y, width)).
+__device__ __forceinline__ void face_cell3(const Params& P, int f, long long idx, int& iz, int& iy, int& ix)
+{
+    const int w = P.st.w, bx = P.x1 - P.x0, by = P.y1 - P.y0;
+    if (f < 2) {
+        ix = P.x0 + (int)(idx % bx); idx /= bx;
+        iy = P.y0 + (int)(idx % by);
+        iz = (f == 0 ? P.z0 : P.z1 - w) + (int)(idx / by);
+    } else if (f < 4) {
+        ix = P.x0 + (int)(idx % bx); idx /= bx;
+        iy = (f == 2 ? P.y0 : P.y1 - w) + (int)(idx % w);
+        iz = P.z0 + (int)(idx / w);
+    } else {
+        ix = (f == 4 ? P.x0 : P.x1 - w) + (int)(idx % w); idx /= w;
+        iy = P.y0 + (int)(idx % by);
+        iz = P.z0 + (int)(idx / by);
+    }
+}
+
+// The face a scaled-format restore reads strip cell (iz, iy, ix) from: the
+// last of the faces holding it in the reference's restore order (top, bottom,
+// front, back, left, right).
+__device__ __forceinline__ long long face_index3(const Params& P, int iz, int iy, int ix, int& f)
+{
+    const int w = P.st.w, bx = P.x1 - P.x0, by = P.y1 - P.y0;
+    if (ix >= P.x1 - w) { f = 5; return ((long long)(iz - P.z0) * by + (iy - P.y0)) * w + (ix - (P.x1 - w)); }
+    if (ix < P.x0 + w) { f = 4; return ((long long)(iz - P.z0) * by + (iy - P.y0)) * w + (ix - P.x0); }
+    if (iy >= P.y1 - w) { f = 3; return ((long long)(iz - P.z0) * w + (iy - (P.y1 - w))) * bx + (ix - P.x0); }
+    if (iy < P.y0 + w) { f = 2; return ((long long)(iz - P.z0) * w + (iy - P.y0)) * bx + (ix - P.x0); }
+    if (iz >= P.z1 - w) { f = 1; return ((long long)(iz - (P.z1 - w)) * by + (iy - P.y0)) * bx + (ix - P.x0); }
+    f = 0;
+    return ((long long)(iz - P.z0) * by + (iy - P.y0)) * bx + (ix - P.x0);
 }
 
 __device__ __forceinline__ bool in_phys(const Params& P, int iz, int iy, int ix)
@@ -351,8 +423,10 @@ __global__ void gather3(const Params P, const float* __restrict__ u, float* __re
     else out[((long long)b * n + s) * P.nt + it] = v;
 }
 
-// boundary strips: save (tape <- u) or restore (u <- tape), every shot
-__global__ void strips3(const Params P, float* __restrict__ u, float* __restrict__ tape, int restore)
+// boundary strips: save (slot <- u; the scaled formats into `scratch`, for
+// quantise_strips3) or restore (u <- slot, dequantised as the reference does:
+// fp16 code x scale; int8 (code - 128) x scale / 127), every shot
+__global__ void strips3(const Params P, float* __restrict__ u, void* slot, float* __restrict__ scratch, int restore)
 {
     const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (e >= (long long)P.B * P.nstrip) return;
@@ -360,8 +434,71 @@ __global__ void strips3(const Params P, float* __restrict__ u, float* __restrict
     int iz, iy, ix;
     strip_coord(P, e - (long long)b * P.nstrip, iz, iy, ix);
     float* c = u + (long long)b * P.S + (long long)iz * P.SP + (long long)iy * P.P + ix;
-    if (restore) *c = tape[e];
-    else tape[e] = *c;
+    const StripStore& S = P.st;
+    if (!restore) {
+        if (S.fmt == SF_F32) static_cast<float*>(slot)[e] = *c;
+        else if (S.fmt == SF_BF16) static_cast<__nv_bfloat16*>(slot)[e] = __float2bfloat16(*c);
+        else scratch[e] = *c;
+        return;
+    }
+    if (S.fmt == SF_F32) { *c = static_cast<const float*>(slot)[e]; return; }
+    if (S.fmt == SF_BF16) { *c = __bfloat162float(static_cast<const __nv_bfloat16*>(slot)[e]); return; }
+    int f;
+    const long long i = face_index3(P, iz, iy, ix, f);
+    const char* base = static_cast<const char*>(slot);
+    const float scale = reinterpret_cast<const float*>(base + S.scl[f])[(long long)b * S.blocks[f] + i / kQB];
+    const long long q = (long long)b * S.cells[f] + i;
+    if (S.fmt == SF_F16) {
+        *c = __half2float(reinterpret_cast<const __half*>(base + S.pay[f])[q]) * scale;
+    } else {
+        const float sc = scale * (1.0f / 127.0f);
+        *c = ((float)reinterpret_cast<const uint8_t*>(base + S.pay[f])[q] - 128.0f) * sc;
+    }
+}
+
+// One step's strips (fp32 strip set in `scratch`) into the scaled faces of a
+// step slot: one CTA per (shot, face, block of kQB cells) -- max |value| of
+// the block, its scale, the codes (reference boundarysaver.cu:957-990,
+// 1050-1080: int8 round(v 127 / max) + 128 clamped to [0, 255]; fp16 v / max).
+__global__ void __launch_bounds__(kQB) quantize_strips3(const Params P, const float* __restrict__ scratch, void* slot)
+{
+    const StripStore& S = P.st;
+    int per = 0;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) per += S.blocks[f];
+    const int b = blockIdx.x / per;
+    int j = blockIdx.x - b * per, f = 0;
+    while (f < 5 && j >= S.blocks[f]) { j -= S.blocks[f]; ++f; }
+    const long long idx = (long long)j * kQB + threadIdx.x;
+    const bool in = idx < S.cells[f];
+    float v = 0.f;
+    if (in) {
+        int iz, iy, ix;
+        face_cell3(P, f, idx, iz, iy, ix);
+        v = scratch[(long long)b * P.nstrip + strip_index3(P, iz, iy, ix)];
+    }
+    float m = fabsf(v);
+#pragma unroll
+    for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __shared__ float wmax[kQB / 32];
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = m;
+    __syncthreads();
+    m = wmax[0];
+#pragma unroll
+    for (int i = 1; i < kQB / 32; ++i) m = fmaxf(m, wmax[i]);
+    char* base = static_cast<char*>(slot);
+    if (threadIdx.x == 0) reinterpret_cast<float*>(base + S.scl[f])[(long long)b * S.blocks[f] + j] = m;
+    if (!in) return;
+    const long long q = (long long)b * S.cells[f] + idx;
+    if (S.fmt == SF_F16) {
+        const float inv = m > 0.0f ? 1.0f / m : 0.0f;
+        reinterpret_cast<__half*>(base + S.pay[f])[q] = __float2half(v * inv);
+    } else {
+        const float qs = m > 0.0f ? 127.0f / m : 0.0f;
+        int c = __float2int_rn(v * qs) + 128;
+        c = c < 0 ? 0 : (c > 255 ? 255 : c);
+        reinterpret_cast<uint8_t*>(base + S.pay[f])[q] = (uint8_t)c;
+    }
 }
 
 __device__ __forceinline__ void kahan_add(float* acc, float* comp, long long o, float g)
@@ -817,6 +954,7 @@ struct Work {
     float *cf, *ca, *vv;
     float* f[34];                    // forward: u x3, psi x6, zeta x3; reverse: see backward()
     int* err;                        // bounded-wait failure flag
+    float* scratch;                  // one step's fp32 strips ahead of their quantisation (scaled formats)
 };
 
 static Work carve(Carve& c, const Params& P, int nfields)
@@ -825,6 +963,7 @@ static Work carve(Carve& c, const Params& P, int nfields)
     w.cf = c.take<float>(P.S); w.ca = c.take<float>(P.S); w.vv = c.take<float>(P.S);
     for (int i = 0; i < nfields; ++i) w.f[i] = c.take<float>((long long)P.B * P.S);
     w.err = c.take<int>(1);
+    if (P.st.fmt == SF_F16 || P.st.fmt == SF_I8) w.scratch = c.take<float>((long long)P.B * P.nstrip);
     return w;
 }
 
@@ -852,19 +991,55 @@ static CUtensorMap plane_map(const float* base, const Params& P, int nb, bool ha
     return tma::make_map(base, 4, dims, strides, box);
 }
 
+// Strip storage of a memory mode: the step-slot layout of the boundary-saving
+// tape (the checkpoint mode keeps its chunk strips as fp32).
+static void set_store(Params& P, int mem_mode)
+{
+    StripStore& S = P.st;
+    S = StripStore{};
+    S.w = M + 1;
+    S.fmt = mem_mode == SWEEP_MEM_BOUNDARY_FP16 ? SF_F16
+          : mem_mode == SWEEP_MEM_BOUNDARY_BF16 ? SF_BF16
+          : mem_mode == SWEEP_MEM_BOUNDARY_INT8 ? SF_I8 : SF_F32;
+    auto up = [](long long v, long long a) { return (v + a - 1) / a * a; };
+    if (S.fmt == SF_F32 || S.fmt == SF_BF16) {
+        S.step = up((long long)P.B * P.nstrip * (S.fmt == SF_F32 ? 4 : 2), 256);
+        return;
+    }
+    const long long bx = P.x1 - P.x0, by = P.y1 - P.y0, bz = P.z1 - P.z0;
+    SWEEP_REQUIRE(bx >= 2 * S.w && by >= 2 * S.w && bz >= 2 * S.w,
+                  "acoustic3d: fp16 / int8 strip storage needs a physical box of at least %d cells per axis", 2 * S.w);
+    const long long cells[6] = {S.w * by * bx, S.w * by * bx, bz * S.w * bx, bz * S.w * bx, bz * by * S.w, bz * by * S.w};
+    const int esz = S.fmt == SF_F16 ? 2 : 1;
+    long long off = 0;
+    for (int f = 0; f < 6; ++f) {
+        SWEEP_REQUIRE(cells[f] < (1LL << 31), "acoustic3d: a strip face holds too many cells");
+        S.cells[f] = (int)cells[f];
+        S.blocks[f] = (int)((cells[f] + kQB - 1) / kQB);
+        S.pay[f] = off;
+        off = up(off + (long long)P.B * cells[f] * esz, 16);
+    }
+    for (int f = 0; f < 6; ++f) {
+        S.scl[f] = off;
+        off = up(off + (long long)P.B * S.blocks[f] * 4, 16);
+    }
+    S.step = up(off, 256);
+}
+
+// tape: one strip slot per step (P.st.step bytes), then (U[nt-1], U[nt]) pitched
 static int64_t tape_bytes(const Params& P)
 {
-    Carve c(nullptr);
-    c.take<float>((long long)P.nt * P.B * P.nstrip);
-    c.take<float>(2LL * P.B * P.S);
-    return c.off;
+    return (int64_t)P.nt * P.st.step + 2LL * P.B * P.S * 4;
+}
+
+static void* tape_slot(const void* tape, const Params& P, int it)
+{
+    return const_cast<char*>(static_cast<const char*>(tape)) + (long long)it * P.st.step;
 }
 
 static float* tape_last(void* tape, const Params& P)
 {
-    Carve c(tape);
-    c.take<float>((long long)P.nt * P.B * P.nstrip);
-    return c.take<float>(2LL * P.B * P.S);
+    return static_cast<float*>(tape_slot(tape, P, P.nt));
 }
 
 static constexpr int kFwdFields = 12, kRevFields = 22;
@@ -898,11 +1073,14 @@ static float* ckpt_strips(void* tape, const Params& P, int c) { return ckpt_fiel
 
 void sizes(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, int64_t* ws, int64_t* tape)
 {
-    SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY || mem_mode == SWEEP_MEM_CHECKPOINT,
+    SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY || mem_mode == SWEEP_MEM_CHECKPOINT ||
+                      mem_mode == SWEEP_MEM_BOUNDARY_FP16 || mem_mode == SWEEP_MEM_BOUNDARY_BF16 ||
+                      mem_mode == SWEEP_MEM_BOUNDARY_INT8,
                   "acoustic3d: unknown memory mode %d", mem_mode);
-    SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY || ckpt_every >= 1,
+    SWEEP_REQUIRE(mem_mode != SWEEP_MEM_CHECKPOINT || ckpt_every >= 1,
                   "acoustic3d: checkpoint interval must be >= 1 (got %d)", ckpt_every);
-    const Params P = make_params(d);
+    Params P = make_params(d);
+    set_store(P, mem_mode);
     Carve c(nullptr);
     if (mem_mode == SWEEP_MEM_CHECKPOINT) {
         carve(c, P, kRevFields + kFwdFields);
@@ -940,8 +1118,11 @@ struct FwdState {
 // none), source injection, receiver gather (record may be null).
 template <class StripsOf>
 static void forward_steps(const sweep_acoustic_desc* d, const Params& P, FwdState& S, float* record, int it0,
-                          int it1, StripsOf strips_of, int* err, cudaStream_t st)
+                          int it1, StripsOf strips_of, int* err, float* scratch, cudaStream_t st)
 {
+    const bool scaled = P.st.fmt == SF_F16 || P.st.fmt == SF_I8;
+    int qper = 0;
+    for (int f = 0; f < 6; ++f) qper += P.st.blocks[f];
     const dim3 grid = stencil_grid(P), block(BXC, BYC);
     const unsigned gs = blocks_for((long long)P.B * P.nsrc, 128), gr = blocks_for((long long)P.B * P.nrec, 128);
     const unsigned gst = blocks_for((long long)P.B * P.nstrip, 256);
@@ -961,8 +1142,11 @@ static void forward_steps(const sweep_acoustic_desc* d, const Params& P, FwdStat
              S.zeta(0), S.zeta(1), S.zeta(2)};
         f3_step<<<grid, block, sizeof(F3Smem), st>>>(maps, P, F, S.in, S.ip, err);
         SWEEP_LAUNCH_CHECK();
-        float* strips = strips_of(it);
-        if (strips && P.nstrip > 0) strips3<<<gst, 256, 0, st>>>(P, S.f[S.in], strips, 0);
+        void* slot = strips_of(it);
+        if (slot && P.nstrip > 0) {
+            strips3<<<gst, 256, 0, st>>>(P, S.f[S.in], slot, scratch, 0);
+            if (scaled) quantize_strips3<<<(unsigned)(P.B * qper), kQB, 0, st>>>(P, scratch, slot);
+        }
         if (d->nsrc > 0)
             inject3<<<gs, 128, 0, st>>>(P, S.f[S.ix], d->wavelet, d->src_loc, d->nsrc, it, 0, 1.f, 0);
         if (d->nrec > 0 && record)
@@ -988,6 +1172,7 @@ void forward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* 
                   (long long)ws_bytes, (long long)need_ws);
     SWEEP_REQUIRE(record != nullptr || d->nrec == 0, "acoustic3d forward: null record");
     Params P = make_params(d);
+    set_store(P, mem_mode);
     Carve c(ws);
     Work w = carve(c, P, kFwdFields);
     const long long rows = (long long)d->nz * d->ny;
@@ -1000,10 +1185,9 @@ void forward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* 
     if (d->nrec > 0) SWEEP_CUDA(cudaMemsetAsync(record, 0, (size_t)d->B * d->nt * d->nrec * 4, st));
     FwdState S(w.f);
     if (mem_mode != SWEEP_MEM_CHECKPOINT) {
-        float* strips = static_cast<float*>(tape);
-        forward_steps(d, P, S, record, 0, d->nt,
-                      [&](int it) { return strips ? strips + (long long)it * P.B * P.nstrip : nullptr; }, w.err, st);
-        if (strips) {
+        forward_steps(d, P, S, record, 0, d->nt, [&](int it) { return tape ? tape_slot(tape, P, it) : nullptr; },
+                      w.err, w.scratch, st);
+        if (tape) {
             float* last = tape_last(tape, P);
             copy_dd(last, S.f[S.ip], n, st);        // U[nt-1]
             copy_dd(last + n, S.f[S.in], n, st);    // U[nt]
@@ -1022,7 +1206,7 @@ void forward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* 
         // the last step of a chunk keeps its strips with the next checkpoint
         forward_steps(d, P, S, record, it0, it1,
                       [&](int it) { return (tape && it == it1 - 1 && ch + 1 < C) ? ckpt_strips(tape, P, ch + 1) : nullptr; },
-                      w.err, st);
+                      w.err, w.scratch, st);
     }
     check_err(w, st, "forward");
 }
@@ -1039,6 +1223,7 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     SWEEP_REQUIRE((illum_s == nullptr) == (illum_r == nullptr), "acoustic3d backward: pass both illuminations or neither");
     const bool ckpt = mem_mode == SWEEP_MEM_CHECKPOINT;
     Params P = make_params(d);
+    set_store(P, mem_mode);
     Carve c(ws);
     // fields: 0-2 lambda, 3-14 adjoint CPML (psi x,y,z and zeta x,y,z, two
     // buffers each), 15-17 reconstruction, 18-19 Kahan slots, 20-21
@@ -1107,7 +1292,7 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
                 R3 R{w.f[rn], w.f[rp], w.f[rx], w.f[ln], gacc, gcomp, is, ir};
                 r3_recon<<<grid, block, sizeof(R3Smem), st>>>(rmaps, P, R, rn - 15, rp - 15, ln, w.err);
                 if (P.nstrip > 0) {
-                    strips3<<<gst, 256, 0, st>>>(P, w.f[rx], strips_of(it - 1), 1);
+                    strips3<<<gst, 256, 0, st>>>(P, w.f[rx], strips_of(it - 1), nullptr, 1);
                     if (d->nsrc > 0)
                         inject3<<<gs, 128, 0, st>>>(P, w.f[rx], d->wavelet, d->src_loc, d->nsrc, it, 0, -1.f, 1);
                     Img I{w.f[rp], w.f[rn], w.f[rx], w.f[ln], gacc, gcomp, is, ir};
@@ -1124,11 +1309,10 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
         }
     };
     if (!ckpt) {
-        float* strips = const_cast<float*>(static_cast<const float*>(tape));
         const float* last = tape_last(const_cast<void*>(tape), P);
         copy_dd(w.f[15], last + n, n, st);   // prev = U[nt]
         copy_dd(w.f[16], last, n, st);       // now  = U[nt-1]
-        reverse(0, d->nt, [&](int t) { return strips + (long long)t * P.B * P.nstrip; });
+        reverse(0, d->nt, [&](int t) { return tape_slot(tape, P, t); });
     } else {
         const int k = ckpt_every, C = nchunks(P, k);
         void* tp = const_cast<void*>(tape);
@@ -1147,7 +1331,7 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
             }
             // replay: chunk slot j holds the strips of U[it0 - 1 + j]
             forward_steps(d, P, S, nullptr, it0, it1, [&](int it) { return chunk + (long long)(it - it0 + 1) * cs; },
-                          w.err, st);
+                          w.err, w.scratch, st);
             copy_dd(w.f[15], S.f[S.in], n, st);      // U[it1]
             copy_dd(w.f[16], S.f[S.ip], n, st);      // U[it1 - 1]
             reverse(it0, it1, [&](int t) { return chunk + (long long)(t - (it0 - 1)) * cs; });

@@ -23,7 +23,7 @@ class BoundarySaving:
     * ``'int8'``: 1 byte per cell plus the same scales: symmetric 8-bit codes
       of the normalised values.
 
-    The reduced formats are built for 2-D acoustic propagation."""
+    The reduced formats are built for acoustic propagation (2-D and 3-D)."""
     storage: str = "gpu"
     storage_dtype: str = "fp32"
 

@@ -364,9 +364,9 @@ class PropTorch(torch.nn.Module):
         if isinstance(self.memory, Ckpt):
             return _lib.MEM_CHECKPOINT, int(self.memory.chunks)
         sd = getattr(self.memory, "storage_dtype", "fp32")
-        if sd != "fp32" and (self.equation.NDIM != 2 or isinstance(self.equation, Elastic)):
-            raise NotImplementedError(f"BoundarySaving(storage_dtype={sd!r}) is built for 2-D acoustic "
-                                      "propagation only; use 'fp32' here")
+        if sd != "fp32" and isinstance(self.equation, Elastic):
+            raise NotImplementedError(f"BoundarySaving(storage_dtype={sd!r}) is built for acoustic "
+                                      "propagation (2-D and 3-D); use 'fp32' for Elastic")
         return {"fp32": _lib.MEM_BOUNDARY, "fp16": _lib.MEM_BOUNDARY_FP16, "bf16": _lib.MEM_BOUNDARY_BF16,
                 "int8": _lib.MEM_BOUNDARY_INT8}[sd], 0
 

@@ -197,6 +197,39 @@ def acoustic2d_storage():
     )
 
 
+def acoustic3d_storage():
+    """3-D boundary saving with fp16 / bf16 / int8 strips (reference
+    BoundarySaving(storage_dtype=...)): 2 shots on a 22 x 20 x 26 model, so the
+    six faces span several 256-cell quantisation blocks."""
+    rng = np.random.default_rng(29)
+    nz, ny, nx, nt, dt, dh, abcn = 22, 20, 26, 160, 0.001, 10.0, 8
+    vp_true = np.full((nz, ny, nx), 1800.0, np.float32)
+    vp_true[nz // 2:] = 2500.0
+    vp_true += (30.0 * rng.standard_normal((nz, ny, nx))).astype(np.float32)
+    vp_init = np.full((nz, ny, nx), 2000.0, np.float32)
+    w = _wavelet(nt, dt, 15.0, 0.06)
+    src = np.array([[7, 6, 5], [18, 13, 4]], np.int64)           # (x, y, z)
+    rec = np.zeros((2, 8, 3), np.int64)
+    for b in range(2):
+        rec[b, :, 0] = rng.integers(1, nx - 1, 8)
+        rec[b, :, 1] = rng.integers(1, ny - 1, 8)
+        rec[b, :, 2] = rng.integers(1, nz - 1, 8)
+    out = {}
+    for sd in ("fp32", "fp16", "bf16", "int8"):
+        eq = Acoustic3D(spatial_order=8, device="cpu")
+        solver = PropTorch(eq, shape=(nz, ny, nx), dh=dh, dt=dt, abcn=abcn, impl="c", device="cpu",
+                           memory=BoundarySaving(storage_dtype=sd))
+        if sd == "fp32":
+            obs = _forward(solver, w, src, rec, [vp_true])
+        r = _run(solver, w, src, rec, [vp_init], obs, False)
+        out[f"grad_vp_{sd}"] = r["grad0"]
+    np.savez_compressed(
+        OUT / "acoustic3d_storage.npz",
+        nz=nz, ny=ny, nx=nx, nt=nt, dt=dt, dh=dh, abcn=abcn, order=8,
+        vp_true=vp_true, vp_init=vp_init, wavelet=w, src=src, rec=rec, obs=obs, **out,
+    )
+
+
 def acoustic3d():
     """A small 3-D case: 2 shots, 6 receivers each, order 8, CPML 8."""
     rng = np.random.default_rng(3)
@@ -273,6 +306,7 @@ CASES = {
     "acoustic2d_pershot": acoustic2d_pershot,
     "acoustic2d_storage": acoustic2d_storage,
     "acoustic3d": acoustic3d,
+    "acoustic3d_storage": acoustic3d_storage,
     "elastic2d": elastic2d,
 }
 

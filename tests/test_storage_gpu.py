@@ -1,6 +1,7 @@
 """Boundary saving with the strips held as fp16 / bf16 / int8, on the GPU,
-against the reference's own runs of the same storage formats (golden fixture
-``acoustic2d_storage``: reference BoundarySaving(storage_dtype=...)).
+against the reference's own runs of the same storage formats (golden fixtures
+``acoustic2d_storage`` and ``acoustic3d_storage``: reference
+BoundarySaving(storage_dtype=...)).
 
 Two bars per format (written here):
   * the gradient within 1e-3 relative L2 of the reference's gradient for that
@@ -26,8 +27,9 @@ PERT_TOL = {"fp16": 0.25, "bf16": 0.1, "int8": 0.05}
 
 
 def _grad(d, storage_dtype):
-    from sweep_b200 import Acoustic, BoundarySaving, PropTorch
-    s = PropTorch(Acoustic(spatial_order=8, device=DEV), shape=tuple(d["vp_true"].shape),
+    from sweep_b200 import Acoustic, Acoustic3D, BoundarySaving, PropTorch
+    eq = (Acoustic3D if d["vp_true"].ndim == 3 else Acoustic)(spatial_order=8, device=DEV)
+    s = PropTorch(eq, shape=tuple(d["vp_true"].shape),
                   dh=float(d["dh"]), dt=float(d["dt"]), abcn=int(d["abcn"]), device=DEV,
                   memory=BoundarySaving(storage_dtype=storage_dtype))
     vp = torch.tensor(d["vp_init"], device=DEV, requires_grad=True)
@@ -38,20 +40,25 @@ def _grad(d, storage_dtype):
     return vp.grad.double().cpu().numpy()
 
 
-def test_fp32_baseline_matches_reference():
-    d = load("acoustic2d_storage")
+CASES = ["acoustic2d_storage", "acoustic3d_storage"]
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_fp32_baseline_matches_reference(case):
+    d = load(case)
     assert rel(_grad(d, "fp32"), d["grad_vp_fp32"]) < GRAD_TOL
 
 
+@pytest.mark.parametrize("case", CASES)
 @pytest.mark.parametrize("sd", ["fp16", "bf16", "int8"])
-def test_reduced_storage_matches_reference(sd):
-    d = load("acoustic2d_storage")
+def test_reduced_storage_matches_reference(case, sd):
+    d = load(case)
     g32 = _grad(d, "fp32")
     g = _grad(d, sd)
     ref32, ref = d["grad_vp_fp32"].astype(np.float64), d[f"grad_vp_{sd}"].astype(np.float64)
     err = rel(g, ref)
     pert = rel(g - g32, ref - ref32)
-    print(f"{sd}: gradient vs reference {err:.2e}; change vs reference change {pert:.2e} "
+    print(f"{case} {sd}: gradient vs reference {err:.2e}; change vs reference change {pert:.2e} "
           f"(change {rel(ref, ref32):.2e} of the gradient)")
     assert err < GRAD_TOL
     assert pert < PERT_TOL[sd]
