@@ -78,8 +78,7 @@ typedef struct sweep_acoustic_desc {
  * BoundarySaving(storage_dtype=...), options.py:194-212; boundarysaver.cu:
  * 906-1100).  Compute stays FP32.  fp16 and int8 quantise each face of the
  * strip set per shot in blocks of 256 cells against the block's max |value|
- * (one FP32 scale per block); bf16 rounds each value.  Acoustic (2-D and
- * 3-D) only. */
+ * (one FP32 scale per block; elastic: per field); bf16 rounds each value. */
 #define SWEEP_MEM_BOUNDARY_FP16 2
 #define SWEEP_MEM_BOUNDARY_BF16 3
 #define SWEEP_MEM_BOUNDARY_INT8 4

@@ -1618,6 +1618,11 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
         const FwdMaps fmaps = fwd_maps(fw, P);
         void* tp = const_cast<void*>(tape);
         const long long cs = (long long)P.B * P.nstrip;
+        // the replay set starts clear: the fields a checkpoint does not hold
+        // (the third wavefield buffer, the next psi pair) are read in their
+        // stencil halo and outside the CPML band, which no step writes
+        for (auto* p : {fw.u[0], fw.u[1], fw.u[2], fw.psix, fw.psiz, fw.psixn, fw.psizn, fw.zetax, fw.zetaz})
+            SWEEP_CUDA(cudaMemsetAsync(p, 0, n * 4, st));
         for (int ch = C - 1; ch >= 0; --ch) {
             const int it0 = ch * k, it1 = std::min(d->nt, it0 + k);
             FwdState S;

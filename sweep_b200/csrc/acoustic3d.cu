@@ -1318,6 +1318,10 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
         void* tp = const_cast<void*>(tape);
         const long long cs = (long long)P.B * P.nstrip;
         float* const* fw = w.f + kRevFields;
+        // the replay set starts clear: the fields a checkpoint does not hold
+        // (the third wavefield buffer, the next-psi triple) are read in their
+        // stencil halo and outside the CPML band, which no step writes
+        for (int i = 0; i < kFwdFields; ++i) SWEEP_CUDA(cudaMemsetAsync(fw[i], 0, n * 4, st));
         for (int ch = C - 1; ch >= 0; --ch) {
             const int it0 = ch * k, it1 = std::min(d->nt, it0 + k);
             FwdState S(fw);

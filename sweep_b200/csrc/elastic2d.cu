@@ -35,6 +35,9 @@
 // further inward on the high side; reference context.h:359-400 keeps wider
 // slabs for the same reason).  Tiles are 32 x 32 cells, 256 threads, 4 rows
 // per thread.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -60,6 +63,22 @@ constexpr int HX = TX + 2 * M, HZ = TZ + 2 * M, HN = HX * HZ;
 
 enum { VX = 0, VZ = 1, SXX = 2, SZZ = 3, SXZ = 4 };
 
+// Boundary-strip storage of the boundary-saving tape.  fp32 and bf16 keep the
+// strip set (B, 5, nstrip); fp16 and int8 keep the reference's four bands per
+// field (top and bottom: M + 1 rows from M outside the box over its width;
+// left and right: M + 1 columns down the box), each quantised per field and
+// shot in blocks of kQB cells against the block's max |value| (reference
+// boundarysaver.cu:906-1100, elastic2d/driver_traits.cuh:270-291).
+enum StripFmt { SF_F32 = 0, SF_F16 = 1, SF_BF16 = 2, SF_I8 = 3 };
+constexpr int kQB = 256;
+
+struct StripStore {
+    int fmt;                        // StripFmt
+    int cells[4], blocks[4];        // per field and shot, per band (top, bottom, left, right)
+    long long pay[4], scl[4];       // byte offsets of each band's codes (5, B, cells) and scales (5, B, blocks)
+    long long step;                 // bytes of one step slot
+};
+
 struct Geo {
     int B, nz, nx, nt, P;
     long long S;                    // pitched cells per shot
@@ -78,6 +97,7 @@ struct Geo {
     const float* wavelet;           // (B, nsrc, nt)
     int gf;                         // shots per CTA of the forward kernels
     int* err;                       // bounded-wait failure flag (0 = none)
+    StripStore st;
 };
 
 enum { ERR_WAIT_FWD = 1, ERR_WAIT_REV = 2 };
@@ -145,6 +165,55 @@ __device__ __forceinline__ int strip_index(const Geo& G, int iz, int ix)
     if (ix <= G.x0) return r + ix - (G.x0 - M);
     if (ix >= G.x1 - 1) return r + W + ix - (G.x1 - 1);
     return -1;
+}
+
+// Band f (0 top, 1 bottom, 2 left, 3 right; width M + 1 at offset -M) cell
+// `idx` of the scaled formats -> grid cell.
+__device__ __forceinline__ void band_cell(const Geo& G, int f, int idx, int& iz, int& ix)
+{
+    constexpr int W = M + 1;
+    if (f < 2) {
+        const int r = idx / G.bw;
+        iz = (f == 0 ? G.z0 - M : G.z1 - 1) + r;
+        ix = G.x0 + (idx - r * G.bw);
+    } else {
+        const int r = idx / W;
+        iz = G.z0 + r;
+        ix = (f == 2 ? G.x0 - M : G.x1 - 1) + (idx - r * W);
+    }
+}
+
+// The band a scaled-format restore reads strip cell (iz, ix) from: the last
+// of the bands holding it in the reference's restore order top, bottom,
+// left, right.
+__device__ __forceinline__ int band_index(const Geo& G, int iz, int ix, int& f)
+{
+    constexpr int W = M + 1;
+    const bool rows = iz >= G.z0 && iz < G.z1;
+    if (rows && ix >= G.x1 - 1) { f = 3; return (iz - G.z0) * W + (ix - (G.x1 - 1)); }
+    if (rows && ix <= G.x0) { f = 2; return (iz - G.z0) * W + (ix - (G.x0 - M)); }
+    if (iz >= G.z1 - 1) { f = 1; return (iz - (G.z1 - 1)) * G.bw + (ix - G.x0); }
+    f = 0;
+    return (iz - (G.z0 - M)) * G.bw + (ix - G.x0);
+}
+
+// Saved value of field k at strip cell (iz, ix) (strip index si) of shot b
+// (dequantised as the reference does: fp16 code x scale; int8
+// (code - 128) x scale / 127).
+__device__ __forceinline__ float strip_val(const Geo& G, const void* slot, int b, int k, int iz, int ix, int si)
+{
+    const StripStore& S = G.st;
+    const long long e = ((long long)b * 5 + k) * G.nstrip + si;
+    if (S.fmt == SF_F32) return static_cast<const float*>(slot)[e];
+    if (S.fmt == SF_BF16) return __bfloat162float(static_cast<const __nv_bfloat16*>(slot)[e]);
+    int f;
+    const int i = band_index(G, iz, ix, f);
+    const char* base = static_cast<const char*>(slot);
+    const long long row = (long long)k * G.B + b;
+    const float scale = reinterpret_cast<const float*>(base + S.scl[f])[row * S.blocks[f] + i / kQB];
+    const long long q = row * S.cells[f] + i;
+    if (S.fmt == SF_F16) return __half2float(reinterpret_cast<const __half*>(base + S.pay[f])[q]) * scale;
+    return ((float)reinterpret_cast<const uint8_t*>(base + S.pay[f])[q] - 128.0f) * (scale * (1.0f / 127.0f));
 }
 
 // Does tile (tz0, tx0) hold any strip cell?  The strips lie within M cells
@@ -235,7 +304,7 @@ struct FwdArgs {
     Models m;
     float* f[5];          // vx, vz, sxx, szz, sxz
     Slabs mem;            // forward memories: x {vxx, vzx, sxxx, sxzx}, z {vzz, vxz, szzz, sxzz}
-    float* strips;        // this step's strip slot (B, 5, nstrip) or null
+    void* strips;         // this step's strips (B, 5, nstrip): float, or bf16 when G.st.fmt is bf16; or null
     float* record;        // (B, nt, nrec, nrf)
     int it;
 };
@@ -509,12 +578,22 @@ __global__ void __launch_bounds__(NTH, 4) fwd_str(const __grid_constant__ FwdMap
             if (stile) {
                 const int si = strip_index(G, iz, ix);
                 if (si >= 0) {
-                    float* st = A.strips + (long long)b * 5 * G.nstrip + si;
-                    st[0] = tvx[c];
-                    st[G.nstrip] = tvz[c];
-                    st[2 * G.nstrip] = sxx;
-                    st[3 * G.nstrip] = szz;
-                    st[4 * G.nstrip] = sxz;
+                    const long long e = (long long)b * 5 * G.nstrip + si;
+                    if (G.st.fmt == SF_BF16) {
+                        __nv_bfloat16* st = static_cast<__nv_bfloat16*>(A.strips) + e;
+                        st[0] = __float2bfloat16(tvx[c]);
+                        st[G.nstrip] = __float2bfloat16(tvz[c]);
+                        st[2 * G.nstrip] = __float2bfloat16(sxx);
+                        st[3 * G.nstrip] = __float2bfloat16(szz);
+                        st[4 * G.nstrip] = __float2bfloat16(sxz);
+                    } else {
+                        float* st = static_cast<float*>(A.strips) + e;
+                        st[0] = tvx[c];
+                        st[G.nstrip] = tvz[c];
+                        st[2 * G.nstrip] = sxx;
+                        st[3 * G.nstrip] = szz;
+                        st[4 * G.nstrip] = sxz;
+                    }
                 }
             }
         }
@@ -543,7 +622,7 @@ struct RevArgs {
     float* cvz;
     float* a[5];          // adjoint fields (stress ones hold the negated adjoint)
     Slabs mo, mn;         // adjoint memories: read set (old), write set (new)
-    const float* strips;  // saved strips of step it - 1, (B, 5, nstrip)
+    const void* strips;   // step slot holding the strips of step it - 1 (format G.st)
     const float* adj;     // (B, nt, nrec, nrf) residuals
     float* gvp;           // gradient slots (nslot, S)
     float* gvs;
@@ -602,7 +681,6 @@ __global__ void __launch_bounds__(NTH, 4) rev_str(RevArgs A)
         const float* __restrict__ rho_ = A.m.rho + (long long)b * G.ms;
         const float* __restrict__ vp_ = A.m.vp + (long long)b * G.ms;
         const float* __restrict__ vs_ = A.m.vs + (long long)b * G.ms;
-        const float* st = A.strips + (long long)b * 5 * G.nstrip;
 #pragma unroll
         for (int r = 0; r < RPT; ++r) {
             const int lz = threadIdx.y + 8 * r, iz = tz0 + lz;
@@ -611,9 +689,9 @@ __global__ void __launch_bounds__(NTH, 4) rev_str(RevArgs A)
             if (!in_core(G, ix, iz)) {
                 const int si = strip_index(G, iz, ix);
                 if (si >= 0) {
-                    A.f[SXX][so + i] = st[2 * G.nstrip + si];
-                    A.f[SZZ][so + i] = st[3 * G.nstrip + si];
-                    A.f[SXZ][so + i] = st[4 * G.nstrip + si];
+                    A.f[SXX][so + i] = strip_val(G, A.strips, b, SXX, iz, ix, si);
+                    A.f[SZZ][so + i] = strip_val(G, A.strips, b, SZZ, iz, ix, si);
+                    A.f[SXZ][so + i] = strip_val(G, A.strips, b, SXZ, iz, ix, si);
                 }
                 continue;
             }
@@ -638,9 +716,9 @@ __global__ void __launch_bounds__(NTH, 4) rev_str(RevArgs A)
             } else {
                 const int si = strip_index(G, iz, ix);
                 if (si >= 0) {
-                    A.f[SXX][so + i] = st[2 * G.nstrip + si];
-                    A.f[SZZ][so + i] = st[3 * G.nstrip + si];
-                    A.f[SXZ][so + i] = st[4 * G.nstrip + si];
+                    A.f[SXX][so + i] = strip_val(G, A.strips, b, SXX, iz, ix, si);
+                    A.f[SZZ][so + i] = strip_val(G, A.strips, b, SZZ, iz, ix, si);
+                    A.f[SXZ][so + i] = strip_val(G, A.strips, b, SXZ, iz, ix, si);
                 }
             }
             if (in_box(G, ix, iz)) {
@@ -871,7 +949,6 @@ __global__ void __launch_bounds__(NTH, 4) rev_vadj(RevArgs A)
     }
     __syncthreads();
     const int lx = threadIdx.x, ix = tx0 + lx;
-    const float* st = A.strips + (long long)b * 5 * G.nstrip;
 #pragma unroll
     for (int r = 0; r < RPT; ++r) {
         const int lz = threadIdx.y + 8 * r, iz = tz0 + lz;
@@ -899,8 +976,52 @@ __global__ void __launch_bounds__(NTH, 4) rev_vadj(RevArgs A)
         const int si = strip_index(G, iz, ix);
         if (si < 0) continue;
         const long long i = so + (long long)iz * G.P + ix;
-        A.f[VX][i] = st[si];
-        A.f[VZ][i] = st[G.nstrip + si];
+        A.f[VX][i] = strip_val(G, A.strips, b, VX, iz, ix, si);
+        A.f[VZ][i] = strip_val(G, A.strips, b, VZ, iz, ix, si);
+    }
+}
+
+// One step's strips (fp32 strip set (B, 5, nstrip) in `scratch`) into the
+// scaled bands of a step slot: one CTA per (field, shot, band, block of kQB
+// cells) -- max |value| of the block, its scale, the codes (reference
+// boundarysaver.cu:957-990, 1050-1080).
+__global__ void __launch_bounds__(kQB) quantize_strips(const Geo G, const float* __restrict__ scratch, void* slot)
+{
+    const StripStore& S = G.st;
+    const int per = S.blocks[0] + S.blocks[1] + S.blocks[2] + S.blocks[3];
+    const int row = blockIdx.x / per;                 // field k * B + shot b
+    const int k = row / G.B, b = row - k * G.B;
+    int j = blockIdx.x - row * per, f = 0;
+    while (f < 3 && j >= S.blocks[f]) { j -= S.blocks[f]; ++f; }
+    const int idx = j * kQB + threadIdx.x;
+    const bool in = idx < S.cells[f];
+    float v = 0.f;
+    if (in) {
+        int iz, ix;
+        band_cell(G, f, idx, iz, ix);
+        v = scratch[((long long)b * 5 + k) * G.nstrip + strip_index(G, iz, ix)];
+    }
+    float m = fabsf(v);
+#pragma unroll
+    for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __shared__ float wmax[kQB / 32];
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = m;
+    __syncthreads();
+    m = wmax[0];
+#pragma unroll
+    for (int i = 1; i < kQB / 32; ++i) m = fmaxf(m, wmax[i]);
+    char* base = static_cast<char*>(slot);
+    if (threadIdx.x == 0) reinterpret_cast<float*>(base + S.scl[f])[(long long)row * S.blocks[f] + j] = m;
+    if (!in) return;
+    const long long q = (long long)row * S.cells[f] + idx;
+    if (S.fmt == SF_F16) {
+        const float inv = m > 0.0f ? 1.0f / m : 0.0f;
+        reinterpret_cast<__half*>(base + S.pay[f])[q] = __float2half(v * inv);
+    } else {
+        const float qs = m > 0.0f ? 127.0f / m : 0.0f;
+        int c = __float2int_rn(v * qs) + 128;
+        c = c < 0 ? 0 : (c > 255 ? 255 : c);
+        reinterpret_cast<uint8_t*>(base + S.pay[f])[q] = (uint8_t)c;
     }
 }
 
@@ -1050,6 +1171,7 @@ struct FwdWs {
     Slabs mem;
     char* zero0;          // [zero0, zero1) cleared before the time loop
     char* zero1;
+    float* scratch;       // one step's fp32 strips ahead of their quantisation (scaled formats)
 };
 
 static void carve_fwd(Carve& c, const Plan& pl, FwdWs& w)
@@ -1061,6 +1183,7 @@ static void carve_fwd(Carve& c, const Plan& pl, FwdWs& w)
     carve_slabs(c, pl.G, w.mem);
     c.take<char>(0);
     w.zero1 = c.base ? c.base + c.off : nullptr;
+    if (pl.G.st.fmt == SF_F16 || pl.G.st.fmt == SF_I8) w.scratch = c.take<float>(5LL * pl.G.B * pl.G.nstrip);
 }
 
 struct RevWs {
@@ -1153,21 +1276,53 @@ static void slabs_copy(const Slabs& s, float* packed, const Geo& G, bool to_pack
     }
 }
 
-// tape: strips of every step (nt, B, 5, nstrip), then the final 5-field state
-// (5, B, nz, P)
+// Strip storage of a memory mode: the step-slot layout of the boundary-saving
+// tape (the checkpoint mode keeps its chunk strips as fp32).
+static void set_store(Plan& pl, int mem_mode)
+{
+    Geo& G = pl.G;
+    StripStore& S = G.st;
+    S = StripStore{};
+    S.fmt = mem_mode == SWEEP_MEM_BOUNDARY_FP16 ? SF_F16
+          : mem_mode == SWEEP_MEM_BOUNDARY_BF16 ? SF_BF16
+          : mem_mode == SWEEP_MEM_BOUNDARY_INT8 ? SF_I8 : SF_F32;
+    auto up = [](long long v, long long a) { return (v + a - 1) / a * a; };
+    const long long per = (long long)G.B * 5 * G.nstrip;
+    if (S.fmt == SF_F32 || S.fmt == SF_BF16) {
+        S.step = up(per * (S.fmt == SF_F32 ? 4 : 2), 256);
+        return;
+    }
+    const int cells[4] = {(M + 1) * G.bw, (M + 1) * G.bw, G.bh * (M + 1), G.bh * (M + 1)};
+    const int esz = S.fmt == SF_F16 ? 2 : 1;
+    long long off = 0;
+    for (int f = 0; f < 4; ++f) {
+        S.cells[f] = cells[f];
+        S.blocks[f] = (cells[f] + kQB - 1) / kQB;
+        S.pay[f] = off;
+        off = up(off + 5LL * G.B * cells[f] * esz, 16);
+    }
+    for (int f = 0; f < 4; ++f) {
+        S.scl[f] = off;
+        off = up(off + 5LL * G.B * S.blocks[f] * 4, 16);
+    }
+    S.step = up(off, 256);
+}
+
+// tape: one strip slot per step (G.st.step bytes), then the final 5-field
+// state (5, B, nz, P)
 static int64_t tape_bytes(const Plan& pl)
 {
-    Carve c(nullptr);
-    c.take<float>((long long)pl.G.nt * pl.G.B * 5 * pl.G.nstrip);
-    c.take<float>(5LL * pl.G.B * pl.G.S);
-    return c.off;
+    return (int64_t)pl.G.nt * pl.G.st.step + 5LL * pl.G.B * pl.G.S * 4;
+}
+
+static void* tape_slot(const void* tape, const Plan& pl, int it)
+{
+    return const_cast<char*>(static_cast<const char*>(tape)) + (long long)it * pl.G.st.step;
 }
 
 static float* tape_last(void* tape, const Plan& pl)
 {
-    Carve c(tape);
-    c.take<float>((long long)pl.G.nt * pl.G.B * 5 * pl.G.nstrip);
-    return c.take<float>(5LL * pl.G.B * pl.G.S);
+    return static_cast<float*>(tape_slot(tape, pl, pl.G.nt));
 }
 
 // CSR of the point events of (shot, tile), like the 2-D acoustic path: the
@@ -1273,9 +1428,11 @@ constexpr size_t SM_REV_VADJ = 7 * HN * sizeof(float);
 
 static void check_mode(int mem_mode, int ckpt_every)
 {
-    SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY || mem_mode == SWEEP_MEM_CHECKPOINT,
+    SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY || mem_mode == SWEEP_MEM_CHECKPOINT ||
+                      mem_mode == SWEEP_MEM_BOUNDARY_FP16 || mem_mode == SWEEP_MEM_BOUNDARY_BF16 ||
+                      mem_mode == SWEEP_MEM_BOUNDARY_INT8,
                   "elastic2d: unknown memory mode %d", mem_mode);
-    SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY || ckpt_every >= 1,
+    SWEEP_REQUIRE(mem_mode != SWEEP_MEM_CHECKPOINT || ckpt_every >= 1,
                   "elastic2d: checkpoint interval must be >= 1 (got %d)", ckpt_every);
 }
 
@@ -1283,6 +1440,7 @@ void sizes(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, int64_t* w
 {
     check_mode(mem_mode, ckpt_every);
     Plan pl = make_plan(d);
+    set_store(pl, mem_mode);
     Carve cf(nullptr);
     FwdWs fw{};
     carve_fwd(cf, pl, fw);
@@ -1301,17 +1459,21 @@ void sizes(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, int64_t* w
 // Forward steps [it0, it1) on the fields / memories of A; strips_of(it) is
 // the strip slot of step it (null: none).
 template <class StripsOf>
-static void forward_steps(FwdArgs& A, int it0, int it1, StripsOf strips_of, cudaStream_t st)
+static void forward_steps(FwdArgs& A, int it0, int it1, StripsOf strips_of, float* scratch, cudaStream_t st)
 {
     const Geo& G = A.G;
     set_attrs();
     const FwdMaps maps = fwd_maps(A.f, G);
     const dim3 grid(G.ntx * G.ntz, (G.B + G.gf - 1) / G.gf), block(TX, 8);
+    const bool scaled = G.st.fmt == SF_F16 || G.st.fmt == SF_I8;
+    const unsigned qblocks = (unsigned)(5 * G.B * (G.st.blocks[0] + G.st.blocks[1] + G.st.blocks[2] + G.st.blocks[3]));
     for (int it = it0; it < it1; ++it) {
         A.it = it;
-        A.strips = strips_of(it);
+        void* slot = strips_of(it);
+        A.strips = (slot && scaled) ? static_cast<void*>(scratch) : slot;
         fwd_vel<<<grid, block, SM_FWD_VEL, st>>>(maps, A);
         fwd_str<<<grid, block, SM_FWD_STR, st>>>(maps, A);
+        if (slot && scaled) quantize_strips<<<qblocks, kQB, 0, st>>>(G, scratch, slot);
     }
     SWEEP_LAUNCH_CHECK();
 }
@@ -1322,6 +1484,7 @@ void forward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, float* r
     check_mode(mem_mode, ckpt_every);
     SWEEP_REQUIRE(record != nullptr || d->nrec == 0, "elastic2d forward: null record");
     Plan pl = make_plan(d);
+    set_store(pl, mem_mode);
     Carve c(ws);
     FwdWs w{};
     carve_fwd(c, pl, w);
@@ -1339,10 +1502,8 @@ void forward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, float* r
     A.record = record;
     const Geo& G = pl.G;
     const long long n = (long long)G.B * G.S;
-    if (mem_mode == SWEEP_MEM_BOUNDARY) {
-        float* strips = static_cast<float*>(tape);
-        forward_steps(A, 0, G.nt, [&](int it) { return strips ? strips + (long long)it * G.B * 5 * G.nstrip : nullptr; },
-                      st);
+    if (mem_mode != SWEEP_MEM_CHECKPOINT) {
+        forward_steps(A, 0, G.nt, [&](int it) { return tape ? tape_slot(tape, pl, it) : nullptr; }, w.scratch, st);
         if (tape) {
             float* last = tape_last(tape, pl);
             for (int k = 0; k < 5; ++k)
@@ -1363,7 +1524,7 @@ void forward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, float* r
         // the last step of a chunk keeps its strips with the next checkpoint
         forward_steps(A, it0, it1,
                       [&](int it) { return (tape && it == it1 - 1 && ch + 1 < C) ? ckpt_at(tape, pl, ch + 1).strips : nullptr; },
-                      st);
+                      nullptr, st);
     }
     check_err(w.cm, st, "forward");
 }
@@ -1377,6 +1538,7 @@ void backward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, const f
     SWEEP_REQUIRE(adj != nullptr || d->nrec == 0, "elastic2d backward: null adjoint source");
     const bool ckpt = mem_mode == SWEEP_MEM_CHECKPOINT;
     Plan pl = make_plan(d);
+    set_store(pl, mem_mode);
     Carve c(ws);
     RevWs w{};
     if (ckpt) carve_rev_ckpt(c, pl, ckpt_every, w);
@@ -1415,11 +1577,10 @@ void backward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, const f
         SWEEP_LAUNCH_CHECK();
     };
     if (!ckpt) {
-        const float* strips = static_cast<const float*>(tape);
         const float* last = tape_last(const_cast<void*>(tape), pl);
         for (int k = 0; k < 5; ++k)
             SWEEP_CUDA(cudaMemcpyAsync(w.f[k], last + k * n, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
-        reverse(0, G.nt, [&](int t) { return strips + (long long)t * G.B * 5 * G.nstrip; });
+        reverse(0, G.nt, [&](int t) { return tape_slot(tape, pl, t); });
     } else {
         const int k = ckpt_every, C = nchunks(pl, k);
         void* tp = const_cast<void*>(tape);
@@ -1446,7 +1607,7 @@ void backward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, const f
                 SWEEP_CUDA(cudaMemcpyAsync(w.chunk, cp.strips, sizeof(float) * cs, cudaMemcpyDeviceToDevice, st));
             }
             // replay: chunk slot j holds the strips after step it0 - 1 + j
-            forward_steps(F, it0, it1, [&](int it) { return w.chunk + (long long)(it - it0 + 1) * cs; }, st);
+            forward_steps(F, it0, it1, [&](int it) { return w.chunk + (long long)(it - it0 + 1) * cs; }, nullptr, st);
             reverse(it0, it1, [&](int t) { return (const float*)w.chunk + (long long)(t - (it0 - 1)) * cs; });
         }
     }

@@ -23,7 +23,8 @@ class BoundarySaving:
     * ``'int8'``: 1 byte per cell plus the same scales: symmetric 8-bit codes
       of the normalised values.
 
-    The reduced formats are built for acoustic propagation (2-D and 3-D)."""
+    Every equation takes every format (Elastic quantises each of its five
+    fields on its own)."""
     storage: str = "gpu"
     storage_dtype: str = "fp32"
 

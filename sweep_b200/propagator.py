@@ -23,6 +23,8 @@ Host-side conventions restated from the reference:
 """
 from __future__ import annotations
 
+import os
+
 import numpy as np
 import torch
 import torch.nn.functional as F
@@ -320,8 +322,14 @@ class PropTorch(torch.nn.Module):
 
     # ---------------------------------------------------------------- helpers
     def _workspace(self, nbytes, device):
+        """The core's scratch (reused between calls).  With the environment
+        variable SWEEP_B200_POISON_WORKSPACE=1 it is filled with 0xFF bytes
+        (float NaN) before every call, so a read of scratch that the call
+        never wrote shows up in its results."""
         if self._ws is None or self._ws.numel() < nbytes or self._ws.device != device:
             self._ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=device)
+        if os.environ.get("SWEEP_B200_POISON_WORKSPACE") == "1":
+            self._ws.fill_(255)
         return self._ws
 
     def _set_illumination(self, i_s, i_r):
@@ -364,9 +372,6 @@ class PropTorch(torch.nn.Module):
         if isinstance(self.memory, Ckpt):
             return _lib.MEM_CHECKPOINT, int(self.memory.chunks)
         sd = getattr(self.memory, "storage_dtype", "fp32")
-        if sd != "fp32" and isinstance(self.equation, Elastic):
-            raise NotImplementedError(f"BoundarySaving(storage_dtype={sd!r}) is built for acoustic "
-                                      "propagation (2-D and 3-D); use 'fp32' for Elastic")
         return {"fp32": _lib.MEM_BOUNDARY, "fp16": _lib.MEM_BOUNDARY_FP16, "bf16": _lib.MEM_BOUNDARY_BF16,
                 "int8": _lib.MEM_BOUNDARY_INT8}[sd], 0
 

@@ -21,3 +21,11 @@ def pytest_collection_modifyitems(config, items):
     for item in items:
         if "gpu" in item.keywords:
             item.add_marker(skip)
+
+
+@pytest.fixture(autouse=True)
+def _poison_workspace(monkeypatch):
+    """Every propagation in the tests runs on a workspace filled with NaN
+    bytes, so a read of scratch that a call never wrote fails its test instead
+    of passing on whatever an earlier allocation left behind."""
+    monkeypatch.setenv("SWEEP_B200_POISON_WORKSPACE", "1")

@@ -300,6 +300,43 @@ def elastic2d():
     )
 
 
+def elastic2d_storage():
+    """Elastic boundary saving with fp16 / bf16 / int8 strips (reference
+    BoundarySaving(storage_dtype=...): each of the five fields quantised per
+    band on its own): 2 explosive shots on a 40 x 120 layered model."""
+    rng = np.random.default_rng(31)
+    nz, nx, nt, dt, dh, abcn = 40, 120, 300, 0.0005, 5.0, 10
+    vp_true = _layered(nz, nx, rng, 1800.0, 3200.0, 4)
+    vs_true = (vp_true / 1.73).astype(np.float32)
+    rho_true = (310.0 * vp_true ** 0.25).astype(np.float32)
+    vp_init = np.full((nz, nx), 2200.0, np.float32)
+    vs_init = (vp_init / 1.73).astype(np.float32)
+    rho_init = (310.0 * vp_init ** 0.25).astype(np.float32)
+    w = _wavelet(nt, dt, 25.0, 0.04)
+    src = np.array([[30, 6], [90, 9]], np.int64)
+    rec = np.zeros((2, 12, 2), np.int64)
+    for b in range(2):
+        rec[b, :, 0] = np.linspace(3, nx - 4, 12).astype(np.int64)
+        rec[b, :, 1] = 3 + b
+    out = {}
+    for sd in ("fp32", "fp16", "bf16", "int8"):
+        eq = Elastic(spatial_order=8, device="cpu")
+        solver = PropTorch(eq, shape=(nz, nx), dh=dh, dt=dt, abcn=abcn, impl="c", device="cpu",
+                           memory=BoundarySaving(storage_dtype=sd))
+        if sd == "fp32":
+            obs = _forward(solver, w, src, rec, [vp_true, vs_true, rho_true])
+        r = _run(solver, w, src, rec, [vp_init, vs_init, rho_init], obs, False)
+        for i, name in enumerate(("vp", "vs", "rho")):
+            out[f"grad_{name}_{sd}"] = r[f"grad{i}"]
+    np.savez_compressed(
+        OUT / "elastic2d_storage.npz",
+        nz=nz, nx=nx, nt=nt, dt=dt, dh=dh, abcn=abcn, order=8,
+        vp_true=vp_true, vs_true=vs_true, rho_true=rho_true,
+        vp_init=vp_init, vs_init=vs_init, rho_init=rho_init,
+        wavelet=w, src=src, rec=rec, obs=obs, **out,
+    )
+
+
 CASES = {
     "acoustic2d_c1": acoustic2d_c1,
     "acoustic2d_multi": acoustic2d_multi,
@@ -308,6 +345,7 @@ CASES = {
     "acoustic3d": acoustic3d,
     "acoustic3d_storage": acoustic3d_storage,
     "elastic2d": elastic2d,
+    "elastic2d_storage": elastic2d_storage,
 }
 
 if __name__ == "__main__":

@@ -170,5 +170,10 @@ def test_reduced_strip_storage_tape_sizes():
         _lib.call("sweep_b200_acoustic_sizes", d3, mode, 0, ws, tape)
         t3[name] = tape.value
     assert t3["int8"] < t3["fp32"]
+    te = {}
+    for name, mode in (("fp32", _lib.MEM_BOUNDARY), ("bf16", _lib.MEM_BOUNDARY_BF16), ("int8", _lib.MEM_BOUNDARY_INT8)):
+        _lib.call("sweep_b200_elastic_sizes", _edesc(nz=60, nx=60, nt=10), mode, 0, ws, tape)
+        te[name] = tape.value
+    assert te["int8"] < te["bf16"] < te["fp32"]
     with pytest.raises(RuntimeError, match="memory mode"):
-        _lib.call("sweep_b200_elastic_sizes", _edesc(nz=60, nx=60, nt=10), _lib.MEM_BOUNDARY_INT8, 0, ws, tape)
+        _lib.call("sweep_b200_elastic_sizes", _edesc(nz=60, nx=60, nt=10), 7, 0, ws, tape)

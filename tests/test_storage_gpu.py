@@ -62,3 +62,37 @@ def test_reduced_storage_matches_reference(case, sd):
           f"(change {rel(ref, ref32):.2e} of the gradient)")
     assert err < GRAD_TOL
     assert pert < PERT_TOL[sd]
+
+
+def _egrads(d, storage_dtype):
+    from sweep_b200 import BoundarySaving, Elastic, PropTorch
+    s = PropTorch(Elastic(spatial_order=8, device=DEV), shape=tuple(d["vp_true"].shape),
+                  dh=float(d["dh"]), dt=float(d["dt"]), abcn=int(d["abcn"]), device=DEV,
+                  memory=BoundarySaving(storage_dtype=storage_dtype))
+    ms = [torch.tensor(d[f"{n}_init"], device=DEV, requires_grad=True) for n in ("vp", "vs", "rho")]
+    pred = s(torch.tensor(d["wavelet"], device=DEV), d["src"], d["rec"], models=ms)
+    loss = 0.5 * ((pred.double() - torch.tensor(d["obs"], device=DEV).double()) ** 2).sum()
+    loss.backward()
+    torch.cuda.synchronize()
+    return [m.grad.double().cpu().numpy() for m in ms]
+
+
+# elastic changes are smaller (fp16 5e-6 .. 1.2e-5 of the gradients) against
+# the same float32 noise, hence the wider bounds
+E_PERT_TOL = {"fp16": 0.5, "bf16": 0.15, "int8": 0.1}
+
+
+@pytest.mark.parametrize("sd", ["fp16", "bf16", "int8"])
+def test_elastic_reduced_storage_matches_reference(sd):
+    d = load("elastic2d_storage")
+    g32 = _egrads(d, "fp32")
+    g = _egrads(d, sd)
+    for i, n in enumerate(("vp", "vs", "rho")):
+        ref32, ref = d[f"grad_{n}_fp32"].astype(np.float64), d[f"grad_{n}_{sd}"].astype(np.float64)
+        err = rel(g[i], ref)
+        pert = rel(g[i] - g32[i], ref - ref32)
+        print(f"elastic {sd} {n}: gradient vs reference {err:.2e}; change vs reference change {pert:.2e} "
+              f"(change {rel(ref, ref32):.2e})")
+        assert rel(g32[i], ref32) < GRAD_TOL
+        assert err < GRAD_TOL
+        assert pert < E_PERT_TOL[sd]
