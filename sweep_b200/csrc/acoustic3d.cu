@@ -900,8 +900,12 @@ static Params make_params(const sweep_acoustic_desc* d)
     SWEEP_REQUIRE(d->B >= 1 && d->nt >= 1, "acoustic3d: B and nt must be >= 1");
     SWEEP_REQUIRE(d->vp_stride == 0, "acoustic3d takes one model shared by every shot");
     SWEEP_REQUIRE(d->nsrc >= 0 && d->nrec >= 0, "acoustic3d: negative source/receiver count");
+    // a free surface is the top face without PML cells (pad 0): its M halo
+    // planes above the surface are never updated and stay zero
     for (int f = 0; f < 6; ++f)
-        SWEEP_REQUIRE(d->pad[f] >= 1, "acoustic3d: every face needs a PML pad >= 1 (face %d has %d)", f, d->pad[f]);
+        SWEEP_REQUIRE(d->pad[f] >= (f == 0 ? 0 : 1),
+                      "acoustic3d: every face but the top (free surface) needs a PML pad >= 1 (face %d has %d)", f,
+                      d->pad[f]);
     Params P{};
     P.B = d->B; P.nz = d->nz; P.ny = d->ny; P.nx = d->nx; P.nt = d->nt;
     P.nsrc = d->nsrc; P.nrec = d->nrec;

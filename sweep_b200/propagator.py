@@ -13,7 +13,9 @@ acoustic equations, the wavelet's) gradients through a
 Host-side conventions restated from the reference:
 * runtime grid = physical + ``abcn`` PML cells + ``M = so/2`` halo per face
   (``core/geometry.py:23-58``); coordinates shift by ``abcn + M``
-  (``_c.py:2196-2207``);
+  (``_c.py:2196-2207``); ``free_surface=True`` (acoustic) drops the top
+  face's PML cells, so the surface row sits M cells from the grid's top and
+  the halo rows above it stay at zero pressure;
 * models are replicate-padded to the runtime grid and the gradient cropped back
   (``utils/torch.py:8-41``); a shared model is used by every shot and its
   gradient summed over shots (``_c.py:2110-2155``);
@@ -89,7 +91,7 @@ class _Geometry:
         self.device = device
         self.dt = prop.dt
         self.spacing = prop.spacing
-        pads = [prop.abcn] * (2 * self.ndim)
+        pads = list(prop.pads)
         if isinstance(eq, Elastic):
             prof = cpml_profiles_s(pads, self.M, prop.dt, self.spacing, self.shape, max_vel, pml_freq)
         else:
@@ -97,7 +99,7 @@ class _Geometry:
         self.prof = [[torch.from_numpy(np.ascontiguousarray(a)).to(device) for a in p] for p in prof]
         self.src = torch.from_numpy(np.ascontiguousarray(src_rt, dtype=np.int32)).to(device)
         self.rec = torch.from_numpy(np.ascontiguousarray(rec_rt, dtype=np.int32)).to(device)
-        self.pad = prop.abcn
+        self.pads = list(prop.pads)          # per face in shape order: lo, hi per axis
 
     def acoustic_desc(self, vp, wavelet):
         d = _lib.AcousticDesc()
@@ -109,8 +111,10 @@ class _Geometry:
             d.nz, d.ny, d.nx = self.shape
         d.nt = self.nt
         d.M = self.M
-        for i in range(6):
-            d.pad[i] = self.pad if (self.ndim == 3 or i not in (2, 3)) else 0
+        pz, px = self.pads[0:2], self.pads[-2:]
+        py = self.pads[2:4] if self.ndim == 3 else [0, 0]
+        for i, p in enumerate(pz + py + px):
+            d.pad[i] = p
         d.dt = self.dt
         if self.ndim == 2:
             d.dz, d.dy, d.dx = self.spacing[0], 1.0, self.spacing[1]
@@ -147,7 +151,7 @@ class _Geometry:
         d.nt = self.nt
         d.M = self.M
         for i in range(4):
-            d.pad[i] = self.pad
+            d.pad[i] = self.pads[i]
         d.dt = self.dt
         d.dz, d.dx = self.spacing
         (az, bz, azh, bzh), (ax, bx, axh, bxh) = self.prof
@@ -289,8 +293,6 @@ class PropTorch(torch.nn.Module):
         super().__init__()
         if impl not in (None, "c", "auto"):
             raise NotImplementedError(f"sweep_b200 implements impl='c' only (got impl={impl!r})")
-        if free_surface:
-            raise NotImplementedError("sweep_b200: free surfaces are not built (absorbing faces only)")
         unknown = set(kwargs) - {"nt", "B", "pml_type", "backend"}
         if unknown:
             raise TypeError(f"PropTorch got unexpected keyword arguments {sorted(unknown)}")
@@ -304,9 +306,23 @@ class PropTorch(torch.nn.Module):
         self.dt = float(dt)
         self.abcn = int(abcn)
         if self.abcn < 1:
-            raise NotImplementedError("sweep_b200: every face needs an absorbing layer (abcn >= 1)")
+            raise NotImplementedError("sweep_b200: the absorbing faces need a layer (abcn >= 1)")
+        if not isinstance(free_surface, (bool, np.bool_)):
+            raise NotImplementedError("sweep_b200: free_surface=True (the top face) is built; per-face "
+                                      "free surfaces are not")
+        if free_surface and isinstance(equation, Elastic):
+            raise NotImplementedError("sweep_b200: an Elastic free surface (image method) is not built")
+        self.free_surface = bool(free_surface)
+        # PML cells per face in shape order (lo, hi per axis); a free surface
+        # takes the top face's pad away and leaves the M halo rows above the
+        # surface at zero pressure (reference ``PropTorch(free_surface=True)``:
+        # pad (0, abcn, ...), ``propagator/base.py:181-240``)
+        self.pads = [self.abcn] * (2 * nd)
+        if self.free_surface:
+            self.pads[0] = 0
         M = equation.M
-        self.runtime_shape = tuple(n + 2 * self.abcn + 2 * M for n in self.shape)
+        self.runtime_shape = tuple(n + self.pads[2 * a] + self.pads[2 * a + 1] + 2 * M
+                                   for a, n in enumerate(self.shape))
         if memory is None:
             memory = Ckpt(chunks=ckpt_chunks) if use_ckpt else BoundarySaving()
         if not isinstance(memory, (BoundarySaving, Full, Ckpt)):
@@ -340,18 +356,26 @@ class PropTorch(torch.nn.Module):
         self.receiver_illumination = crop(i_r)
 
     def _crop(self, g):
-        p = self.abcn + self.equation.M
-        sl = tuple(slice(p, p + n) for n in self.shape)
+        M = self.equation.M
+        sl = tuple(slice(self.pads[2 * a] + M, self.pads[2 * a] + M + n) for a, n in enumerate(self.shape))
         return g[(Ellipsis,) + sl]
 
     def _pad_model(self, m):
         """Replicate-pad a physical model to the runtime grid (autograd crops back)."""
-        p = self.abcn + self.equation.M
+        M = self.equation.M
         nd = self.equation.NDIM
         per_shot = m.dim() == nd + 1
         x = m if per_shot else m[None]
-        x = F.pad(x[:, None] if nd == 2 else x[:, None], [p, p] * nd, mode="replicate")[:, 0]
+        widths = []
+        for a in reversed(range(nd)):            # F.pad runs from the last axis
+            widths += [self.pads[2 * a] + M, self.pads[2 * a + 1] + M]
+        x = F.pad(x[:, None], widths, mode="replicate")[:, 0]
         return x if per_shot else x[0]
+
+    def _shift(self):
+        """Runtime-grid offset of a coordinate, in the coordinate order (x[, y], z)."""
+        nd, M = self.equation.NDIM, self.equation.M
+        return np.array([self.pads[2 * (nd - 1 - c)] + M for c in range(nd)], np.int64)
 
     def _elastic_fields(self):
         """Source / receiver field indices (reference ``_c.py:1163-1176``)."""
@@ -395,8 +419,8 @@ class PropTorch(torch.nn.Module):
         nt = wavelet.shape[-1]
         src = np.asarray(sources.detach().cpu() if isinstance(sources, torch.Tensor) else sources, np.int64)
         rec = np.asarray(receivers.detach().cpu() if isinstance(receivers, torch.Tensor) else receivers, np.int64)
-        src = src.reshape(B, nsrc, nd) + (self.abcn + eq.M)
-        rec = rec.reshape(B, -1, nd) + (self.abcn + eq.M)
+        src = src.reshape(B, nsrc, nd) + self._shift()
+        rec = rec.reshape(B, -1, nd) + self._shift()
         nrec = rec.shape[1]
         if mode == "A1":
             wb = wavelet[None, None, :].expand(B, 1, nt)

@@ -337,12 +337,72 @@ def elastic2d_storage():
     )
 
 
+def acoustic2d_free_surface():
+    """2-D free surface (reference PropTorch(free_surface=True): no PML on the
+    top face): 2 shots near the surface, receivers on the surface rows, a
+    layered model; boundary saving and full modes, wavelet gradient."""
+    rng = np.random.default_rng(37)
+    nz, nx, nt, dt, dh, abcn = 48, 90, 500, 0.001, 10.0, 12
+    vp_true = _layered(nz, nx, rng, 1500.0, 3000.0, 5)
+    vp_init = np.full((nz, nx), 1800.0, np.float32) + 20.0 * rng.standard_normal((nz, nx)).astype(np.float32)
+    w = np.stack([_wavelet(nt, dt, 15.0, 0.06), _wavelet(nt, dt, 12.0, 0.08)]).astype(np.float32)
+    src = np.array([[20, 2], [70, 0]], np.int64)
+    rx = np.arange(2, nx - 2, 5)
+    rec = np.broadcast_to(np.stack([rx, np.full(rx.size, 1)], -1), (2, rx.size, 2)).copy()
+    res = {}
+    for mode, mem in (("bs", BoundarySaving()), ("full", Full())):
+        eq = Acoustic(spatial_order=8, device="cpu")
+        solver = PropTorch(eq, shape=(nz, nx), dh=dh, dt=dt, abcn=abcn, impl="c", device="cpu",
+                           memory=mem, free_surface=True)
+        obs = _forward(solver, w, src, rec, [vp_true])
+        r = _run(solver, w, src, rec, [vp_init], obs, True)
+        res[mode] = (obs, r)
+    obs, r = res["bs"]
+    np.savez_compressed(
+        OUT / "acoustic2d_free_surface.npz",
+        nz=nz, nx=nx, nt=nt, dt=dt, dh=dh, abcn=abcn, order=8,
+        vp_true=vp_true, vp_init=vp_init, wavelet=w, src=src, rec=rec,
+        obs=obs, pred=r["pred"], loss=r["loss"], grad_vp=r["grad0"], grad_wavelet=r["grad_wavelet"],
+        grad_vp_full=res["full"][1]["grad0"],
+    )
+
+
+def acoustic3d_free_surface():
+    """3-D free surface: 2 shots just under the surface, receivers on it."""
+    rng = np.random.default_rng(41)
+    nz, ny, nx, nt, dt, dh, abcn = 20, 18, 24, 180, 0.001, 10.0, 8
+    vp_true = np.full((nz, ny, nx), 1800.0, np.float32)
+    vp_true[nz // 2:] = 2600.0
+    vp_true += (30.0 * rng.standard_normal((nz, ny, nx))).astype(np.float32)
+    vp_init = np.full((nz, ny, nx), 2000.0, np.float32)
+    w = _wavelet(nt, dt, 15.0, 0.06)
+    src = np.array([[6, 5, 1], [17, 12, 2]], np.int64)          # (x, y, z)
+    rec = np.zeros((2, 8, 3), np.int64)
+    for b in range(2):
+        rec[b, :, 0] = rng.integers(1, nx - 1, 8)
+        rec[b, :, 1] = rng.integers(1, ny - 1, 8)
+        rec[b, :, 2] = 0
+    eq = Acoustic3D(spatial_order=8, device="cpu")
+    solver = PropTorch(eq, shape=(nz, ny, nx), dh=dh, dt=dt, abcn=abcn, impl="c", device="cpu",
+                       memory=BoundarySaving(), free_surface=True)
+    obs = _forward(solver, w, src, rec, [vp_true])
+    r = _run(solver, w, src, rec, [vp_init], obs, True)
+    np.savez_compressed(
+        OUT / "acoustic3d_free_surface.npz",
+        nz=nz, ny=ny, nx=nx, nt=nt, dt=dt, dh=dh, abcn=abcn, order=8,
+        vp_true=vp_true, vp_init=vp_init, wavelet=w, src=src, rec=rec,
+        obs=obs, pred=r["pred"], loss=r["loss"], grad_vp=r["grad0"], grad_wavelet=r["grad_wavelet"],
+    )
+
+
 CASES = {
     "acoustic2d_c1": acoustic2d_c1,
     "acoustic2d_multi": acoustic2d_multi,
     "acoustic2d_pershot": acoustic2d_pershot,
     "acoustic2d_storage": acoustic2d_storage,
     "acoustic3d": acoustic3d,
+    "acoustic2d_free_surface": acoustic2d_free_surface,
+    "acoustic3d_free_surface": acoustic3d_free_surface,
     "acoustic3d_storage": acoustic3d_storage,
     "elastic2d": elastic2d,
     "elastic2d_storage": elastic2d_storage,
