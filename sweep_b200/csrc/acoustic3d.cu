@@ -546,14 +546,15 @@ struct A3 {
 // profiles (a, b, db) at axis index c (reference adjoint_split.cu:205-255).
 // cav / lav: (v*v)*dt^2 and lambda at the 2M+1 cells along the axis around i
 // (from shared memory), gw = their product at i.
+// da: the centred derivative of a at c (grad_p(a + c, 1, P, h); the x and y
+// ones are fixed per thread, so the caller hoists them out of the plane loop).
 __device__ __forceinline__ void adj_axis(const Params& P, const float* __restrict__ a, const float* __restrict__ bv,
                                          const float* __restrict__ dbv, const float (&cav)[2 * M + 1],
                                          const float (&lav)[2 * M + 1], const float* __restrict__ psi,
                                          const float* __restrict__ zeta, long long i, long long st, int c, float gw,
-                                         float h, float& L, float& Dg, float* pso, float* zto)
+                                         float h, float da, float& L, float& Dg, float* pso, float* zto)
 {
     const float a_ = __ldg(a + c), b_ = __ldg(bv + c);
-    const float da = grad_p(a + c, 1, P, h);
     const float gt0 = b_ * zeta[i] + (1.0f + b_) * gw;
     const float l0 = (1.0f + b_) * gt0;
     float Lq = 0.0f, Dgg = 0.0f, Dq = 0.0f;
@@ -654,6 +655,8 @@ __global__ void __launch_bounds__(NTH, 3) a3_step(const __grid_constant__ A3Maps
     for (int q = q0; q < zb + M; ++q)
         if (!arrive(q)) { fail(q); return; }
     const int cidx = (ty + M) * PW + (tx + M), cc = ty * BXC + tx;
+    const float dax = (col && (ix < P.qx0 || ix >= P.qx1)) ? grad_p(P.ax + ix, 1, P, P.dx) : 0.f;
+    const float day = (col && (iy < P.qy0 || iy >= P.qy1)) ? grad_p(P.ay + iy, 1, P, P.dy) : 0.f;
     for (int z = zb; z < ze; ++z) {
         if (!arrive(z + M)) { fail(z + M); return; }
         if (col) {
@@ -685,8 +688,8 @@ __global__ void __launch_bounds__(NTH, 3) a3_step(const __grid_constant__ A3Maps
                 if (inx) {
 #pragma unroll
                     for (int k = -M; k <= M; ++k) { cav[M + k] = pc[k]; lav[M + k] = pl[k]; }
-                    adj_axis(P, P.ax, P.bx, P.dbx, cav, lav, A.px + bo, A.zx + bo, ic, 1, ix, gw, P.dx, Lx, Dgx,
-                             A.pxo + bo, A.zxo + bo);
+                    adj_axis(P, P.ax, P.bx, P.dbx, cav, lav, A.px + bo, A.zx + bo, ic, 1, ix, gw, P.dx, dax, Lx,
+                             Dgx, A.pxo + bo, A.zxo + bo);
                 } else {
                     Lx = 0.0f;
 #pragma unroll
@@ -696,8 +699,8 @@ __global__ void __launch_bounds__(NTH, 3) a3_step(const __grid_constant__ A3Maps
                 if (iny) {
 #pragma unroll
                     for (int k = -M; k <= M; ++k) { cav[M + k] = pc[k * PW]; lav[M + k] = pl[k * PW]; }
-                    adj_axis(P, P.ay, P.by, P.dby, cav, lav, A.py + bo, A.zy + bo, ic, P.P, iy, gw, P.dy, Ly, Dgy,
-                             A.pyo + bo, A.zyo + bo);
+                    adj_axis(P, P.ay, P.by, P.dby, cav, lav, A.py + bo, A.zy + bo, ic, P.P, iy, gw, P.dy, day, Ly,
+                             Dgy, A.pyo + bo, A.zyo + bo);
                 } else {
                     Ly = 0.0f;
 #pragma unroll
@@ -711,8 +714,8 @@ __global__ void __launch_bounds__(NTH, 3) a3_step(const __grid_constant__ A3Maps
                         cav[M + k] = sm.c[slot(z + k)][cidx];
                         lav[M + k] = sm.l[slot(z + k)][cidx];
                     }
-                    adj_axis(P, P.az, P.bz, P.dbz, cav, lav, A.pz + bo, A.zz + bo, ic, P.SP, z, gw, P.dz, Lz, Dgz,
-                             A.pzo + bo, A.zzo + bo);
+                    adj_axis(P, P.az, P.bz, P.dbz, cav, lav, A.pz + bo, A.zz + bo, ic, P.SP, z, gw, P.dz,
+                             grad_p(P.az + z, 1, P, P.dz), Lz, Dgz, A.pzo + bo, A.zzo + bo);
                 } else {
                     Lz = 0.0f;
 #pragma unroll
