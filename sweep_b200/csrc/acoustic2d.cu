@@ -1050,12 +1050,11 @@ static Plan make_plan(const sweep_acoustic_desc* d)
     SWEEP_REQUIRE(d->B >= 1 && d->nt >= 1, "acoustic2d: B and nt must be >= 1");
     SWEEP_REQUIRE(d->nsrc >= 0 && d->nrec >= 0, "acoustic2d: negative source/receiver count");
     SWEEP_REQUIRE(d->nz >= 2 * M + 1 && d->nx >= 2 * M + 1, "acoustic2d: grid too small");
-    // a free surface is the top face without PML cells (pad 0): its M halo
-    // rows above the surface are never updated and stay zero
+    // a free surface is a face without PML cells (pad 0): the M halo cells
+    // beyond it are never updated and stay zero
     for (int f = 0; f < 4; ++f) {
         const int p = d->pad[f < 2 ? f : f + 2];
-        SWEEP_REQUIRE(p >= (f == 0 ? 0 : 1),
-                      "acoustic2d: every face but the top (free surface) needs a PML pad >= 1 (face %d has %d)", f, p);
+        SWEEP_REQUIRE(p >= 0, "acoustic2d: negative PML pad on face %d (%d)", f, p);
     }
     Plan pl{};
     Params& P = pl.P;

@@ -79,6 +79,39 @@ def normalize_io(wavelet, sources, receivers, ndim):
     return mode, B, nsrc
 
 
+FACE_NAMES = {2: ("top", "bottom", "left", "right"), 3: ("top", "bottom", "front", "back", "left", "right")}
+
+
+def free_faces(spec, nd):
+    """Free-surface faces as a tuple of 2*nd bools in shape order (z_lo, z_hi,
+    [y_lo, y_hi,] x_lo, x_hi), from the reference's spellings
+    (``equations/_edges.py:66-140``): ``True`` (the top face) / ``False`` /
+    ``None``, a face name or names (``'top'``, ``['top', 'left']``), a
+    2*nd sequence of bools, or a dict of name -> bool."""
+    names = FACE_NAMES[nd]
+    n = 2 * nd
+    if spec is None or isinstance(spec, (bool, np.bool_)):
+        return tuple([bool(spec)] + [False] * (n - 1))
+    if isinstance(spec, str):
+        spec = [spec]
+    if isinstance(spec, dict):
+        items = [(k, bool(v)) for k, v in spec.items()]
+    else:
+        spec = list(spec)
+        if spec and all(isinstance(v, str) for v in spec):
+            items = [(k, True) for k in spec]
+        elif len(spec) == n:
+            return tuple(bool(v) for v in spec)
+        else:
+            raise ValueError(f"free_surface: give face names {names} or {n} bools, got {spec!r}")
+    faces = [False] * n
+    for k, v in items:
+        if k not in names:
+            raise ValueError(f"unknown free-surface face {k!r}; the {nd}-D faces are {names}")
+        faces[names.index(k)] = v
+    return tuple(faces)
+
+
 class _Geometry:
     """Everything a core call needs besides the model and wavelet tensors."""
 
@@ -307,19 +340,18 @@ class PropTorch(torch.nn.Module):
         self.abcn = int(abcn)
         if self.abcn < 1:
             raise NotImplementedError("sweep_b200: the absorbing faces need a layer (abcn >= 1)")
-        if not isinstance(free_surface, (bool, np.bool_)):
-            raise NotImplementedError("sweep_b200: free_surface=True (the top face) is built; per-face "
-                                      "free surfaces are not")
-        if free_surface and isinstance(equation, Elastic):
+        self.fs_faces = free_faces(free_surface, nd)
+        if any(self.fs_faces) and isinstance(equation, Elastic):
             raise NotImplementedError("sweep_b200: an Elastic free surface (image method) is not built")
-        self.free_surface = bool(free_surface)
+        if nd == 3 and any(self.fs_faces[1:]):
+            raise NotImplementedError("per-face free surfaces are 2-D only (as in the reference); "
+                                      "3-D takes free_surface=True (the top face)")
+        self.free_surface = any(self.fs_faces)
         # PML cells per face in shape order (lo, hi per axis); a free surface
-        # takes the top face's pad away and leaves the M halo rows above the
-        # surface at zero pressure (reference ``PropTorch(free_surface=True)``:
-        # pad (0, abcn, ...), ``propagator/base.py:181-240``)
-        self.pads = [self.abcn] * (2 * nd)
-        if self.free_surface:
-            self.pads[0] = 0
+        # takes its face's pad away and leaves the M halo cells beyond it at
+        # zero pressure (reference ``PropTorch(free_surface=...)``: pad 0 on
+        # the free faces, ``propagator/base.py:181-240``)
+        self.pads = [0 if f else self.abcn for f in self.fs_faces]
         M = equation.M
         self.runtime_shape = tuple(n + self.pads[2 * a] + self.pads[2 * a + 1] + 2 * M
                                    for a, n in enumerate(self.shape))

@@ -367,6 +367,35 @@ def acoustic2d_free_surface():
     )
 
 
+def acoustic2d_free_faces():
+    """2-D per-face free surfaces (reference PropTorch(free_surface=[...])):
+    ['bottom', 'right'] and ['top', 'left'], one shot each near the free
+    faces, receivers along them."""
+    rng = np.random.default_rng(43)
+    nz, nx, nt, dt, dh, abcn = 40, 64, 400, 0.001, 10.0, 10
+    vp_true = _layered(nz, nx, rng, 1500.0, 2800.0, 4)
+    vp_init = np.full((nz, nx), 1800.0, np.float32) + 20.0 * rng.standard_normal((nz, nx)).astype(np.float32)
+    w = _wavelet(nt, dt, 15.0, 0.06)
+    out = {}
+    for tag, faces, src, rec in (
+            ("br", ["bottom", "right"], [[50, 30]], [[[60, z] for z in range(4, 38, 3)]]),
+            ("tl", ["top", "left"], [[8, 3]], [[[x, 1] for x in range(2, 60, 4)]])):
+        src = np.array(src, np.int64)
+        rec = np.array(rec, np.int64)
+        eq = Acoustic(spatial_order=8, device="cpu")
+        solver = PropTorch(eq, shape=(nz, nx), dh=dh, dt=dt, abcn=abcn, impl="c", device="cpu",
+                           memory=BoundarySaving(), free_surface=faces)
+        obs = _forward(solver, w, src, rec, [vp_true])
+        r = _run(solver, w, src, rec, [vp_init], obs, True)
+        out.update({f"src_{tag}": src, f"rec_{tag}": rec, f"obs_{tag}": obs, f"pred_{tag}": r["pred"],
+                    f"grad_vp_{tag}": r["grad0"], f"grad_wavelet_{tag}": r["grad_wavelet"]})
+    np.savez_compressed(
+        OUT / "acoustic2d_free_faces.npz",
+        nz=nz, nx=nx, nt=nt, dt=dt, dh=dh, abcn=abcn, order=8,
+        vp_true=vp_true, vp_init=vp_init, wavelet=w, **out,
+    )
+
+
 def acoustic3d_free_surface():
     """3-D free surface: 2 shots just under the surface, receivers on it."""
     rng = np.random.default_rng(41)
@@ -403,6 +432,7 @@ CASES = {
     "acoustic3d": acoustic3d,
     "acoustic2d_free_surface": acoustic2d_free_surface,
     "acoustic3d_free_surface": acoustic3d_free_surface,
+    "acoustic2d_free_faces": acoustic2d_free_faces,
     "acoustic3d_storage": acoustic3d_storage,
     "elastic2d": elastic2d,
     "elastic2d_storage": elastic2d_storage,

@@ -61,11 +61,18 @@ def test_errors_come_back_as_messages():
     with pytest.raises(RuntimeError, match="order 8"):
         _lib.call("sweep_b200_acoustic_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
     d = _desc()
-    d.pad[0] = 0                               # the top face may be a free surface
+    d.pad[0] = d.pad[5] = 0                    # free-surface faces (2-D: any)
     _lib.call("sweep_b200_acoustic_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
-    d.pad[5] = 0                               # no other face may lose its PML
+    d.pad[4] = -1
     with pytest.raises(RuntimeError, match="PML pad"):
         _lib.call("sweep_b200_acoustic_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
+    d3 = _desc(nz=30, nx=30)
+    d3.ndim, d3.ny = 3, 30
+    for i in range(6):
+        d3.pad[i] = 5
+    d3.pad[4] = 0                              # 3-D: the top face only
+    with pytest.raises(RuntimeError, match="PML pad"):
+        _lib.call("sweep_b200_acoustic_sizes", d3, _lib.MEM_BOUNDARY, 0, ws, tape)
     with pytest.raises(RuntimeError, match="null"):
         _lib.call("sweep_b200_acoustic_sizes", None, _lib.MEM_BOUNDARY, 0, ws, tape)
 
@@ -179,3 +186,17 @@ def test_reduced_strip_storage_tape_sizes():
     assert te["int8"] < te["bf16"] < te["fp32"]
     with pytest.raises(RuntimeError, match="memory mode"):
         _lib.call("sweep_b200_elastic_sizes", _edesc(nz=60, nx=60, nt=10), 7, 0, ws, tape)
+
+
+def test_free_surface_spellings():
+    """The reference's free_surface spellings (equations/_edges.py:66-140)."""
+    from sweep_b200.propagator import free_faces
+    assert free_faces(True, 2) == (True, False, False, False)
+    assert free_faces(False, 3) == (False,) * 6
+    assert free_faces(None, 2) == (False,) * 4
+    assert free_faces("left", 2) == (False, False, True, False)
+    assert free_faces(["top", "right"], 2) == (True, False, False, True)
+    assert free_faces({"bottom": 1, "top": 0}, 2) == (False, True, False, False)
+    assert free_faces([1, 0, 0, 1], 2) == (True, False, False, True)
+    with pytest.raises(ValueError, match="unknown"):
+        free_faces(["front"], 2)

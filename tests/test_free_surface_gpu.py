@@ -72,3 +72,27 @@ def test_free_surface_changes_the_data():
     d = load("acoustic2d_free_surface")
     obs_abs, _, _, _ = _run(d, free_surface=False)
     assert rel(obs_abs, d["obs"]) > 0.1
+
+
+@pytest.mark.parametrize("tag,faces", [("br", ["bottom", "right"]), ("tl", ["top", "left"])])
+def test_per_face_free_surfaces_match_reference(tag, faces):
+    """2-D free surfaces on any faces (reference free_surface=[...])."""
+    from sweep_b200 import Acoustic, PropTorch
+    d = load("acoustic2d_free_faces")
+    s = PropTorch(Acoustic(spatial_order=8, device=DEV), shape=tuple(d["vp_true"].shape), dh=float(d["dh"]),
+                  dt=float(d["dt"]), abcn=int(d["abcn"]), device=DEV, free_surface=faces)
+    src, rec = d[f"src_{tag}"], d[f"rec_{tag}"]
+    with torch.no_grad():
+        obs = s(torch.tensor(d["wavelet"], device=DEV), src, rec,
+                models=[torch.tensor(d["vp_true"], device=DEV)]).cpu().numpy()
+    vp = torch.tensor(d["vp_init"], device=DEV, requires_grad=True)
+    w = torch.tensor(d["wavelet"], device=DEV, requires_grad=True)
+    pred = s(w, src, rec, models=[vp])
+    loss = 0.5 * ((pred - torch.tensor(d[f"obs_{tag}"], device=DEV)) ** 2).sum()
+    loss.backward()
+    torch.cuda.synchronize()
+    print(f"{faces}: records {rel(obs, d[f'obs_{tag}']):.2e} grad {rel(vp.grad.cpu().numpy(), d[f'grad_vp_{tag}']):.2e}")
+    assert rel(obs, d[f"obs_{tag}"]) < REC_TOL
+    assert rel(pred.detach().cpu().numpy(), d[f"pred_{tag}"]) < REC_TOL
+    assert rel(vp.grad.cpu().numpy(), d[f"grad_vp_{tag}"]) < GRAD_TOL
+    assert rel(w.grad.cpu().numpy(), d[f"grad_wavelet_{tag}"]) < GRAD_TOL
