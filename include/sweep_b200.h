@@ -82,6 +82,11 @@ typedef struct sweep_acoustic_desc {
 #define SWEEP_MEM_BOUNDARY_FP16 2
 #define SWEEP_MEM_BOUNDARY_BF16 3
 #define SWEEP_MEM_BOUNDARY_INT8 4
+/* OR'ed into a boundary-saving mode (0, 2, 3, 4): `tape` is pinned HOST
+ * memory (reference BoundarySaving(storage='cpu'), boundary/runtime.cuh:
+ * 91-620); the strips pass through a small device ring in the workspace and a
+ * copy stream.  Acoustic 2-D and 3-D. */
+#define SWEEP_MEM_HOST_TAPE 0x100
 
 /* Bytes the caller must allocate: `workspace` (scratch, reusable between calls
  * once the previous call has finished on its stream) and `tape` (written by

@@ -42,6 +42,7 @@ MEM_CHECKPOINT = 1
 MEM_BOUNDARY_FP16 = 2            # boundary saving, strips stored as scaled fp16 / bf16 / scaled int8
 MEM_BOUNDARY_BF16 = 3
 MEM_BOUNDARY_INT8 = 4
+MEM_HOST_TAPE = 0x100           # OR'ed into a boundary-saving mode: the tape is pinned host memory
 
 
 class AcousticDesc(ctypes.Structure):

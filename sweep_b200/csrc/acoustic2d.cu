@@ -993,6 +993,7 @@ __global__ void pitch_copy_kernel(const float* __restrict__ src, float* __restri
 // ------------------------------------------------------------------- host
 struct Plan {
     Params P;
+    bool host_tape = false;          // boundary-saving tape in pinned host memory (SWEEP_MEM_HOST_TAPE)
     int nslot;                       // gradient accumulator slots (backward)
     int nm;                          // model copies (1 shared, B per-shot)
     int Gf, Gr;                      // shots per CTA: forward, backward
@@ -1116,6 +1117,7 @@ struct FwdWork {
     float* u[3];
     float *psix, *psiz, *psixn, *psizn, *zetax, *zetaz;
     float* scratch;                  // one step's fp32 strips ahead of their quantisation (scaled formats)
+    char* ring;                      // host tape: HostRing::R device strip slots
 };
 
 struct RevWork {
@@ -1124,6 +1126,7 @@ struct RevWork {
     float* aux[8];
     float* r[3];
     float *gacc, *gcomp, *is, *ir;
+    char* ring;                      // host tape: HostRing::R device strip slots
 };
 
 static Common carve_common(Carve& c, const Plan& pl)
@@ -1153,6 +1156,7 @@ static FwdWork carve_fwd(Carve& c, const Plan& pl)
     w.psixn = c.take<float>(n); w.psizn = c.take<float>(n);
     w.zetax = c.take<float>(n); w.zetaz = c.take<float>(n);
     if (pl.P.st.fmt == SF_F16 || pl.P.st.fmt == SF_I8) w.scratch = c.take<float>((long long)pl.P.B * pl.P.nstrip);
+    if (pl.host_tape) w.ring = c.take<char>((long long)HostRing::R * pl.P.st.step);
     return w;
 }
 
@@ -1170,6 +1174,7 @@ static RevWork carve_rev(Carve& c, const Plan& pl, bool illum)
         w.is = c.take<float>((long long)pl.nslot * pl.P.S);
         w.ir = c.take<float>((long long)pl.nslot * pl.P.S);
     }
+    if (pl.host_tape) w.ring = c.take<char>((long long)HostRing::R * pl.P.st.step);
     return w;
 }
 
@@ -1177,6 +1182,8 @@ static RevWork carve_rev(Carve& c, const Plan& pl, bool illum)
 // tape (the checkpoint mode keeps its chunk strips as fp32).
 static void set_store(Plan& pl, int mem_mode)
 {
+    pl.host_tape = (mem_mode & SWEEP_MEM_HOST_TAPE) != 0;
+    mem_mode &= ~SWEEP_MEM_HOST_TAPE;
     Params& P = pl.P;
     StripStore& S = P.st;
     S = StripStore{};
@@ -1234,7 +1241,11 @@ static float* tape_last(void* tape, const Plan& pl)
 // checkpoint_runtime.cuh:15-362, eq_driver.cuh:928-1135).
 constexpr int kStateFields = 6;
 
-static int nchunks(const Plan& pl, int k) { return (pl.P.nt + k - 1) / k; }
+static int nchunks(const Plan& pl, int k)
+{
+    SWEEP_REQUIRE(k >= 1, "acoustic2d: checkpoint interval must be >= 1 (got %d)", k);
+    return (pl.P.nt + k - 1) / k;
+}
 
 static long long ckpt_stride(const Plan& pl)
 {
@@ -1374,12 +1385,21 @@ static void carve_rev_ckpt(Carve& c, const Plan& pl, bool illum, int k, RevWork&
 
 static void check_mode(int mem_mode, int ckpt_every)
 {
+    if (mem_mode & SWEEP_MEM_HOST_TAPE) {
+        mem_mode &= ~SWEEP_MEM_HOST_TAPE;
+        SWEEP_REQUIRE(mem_mode != SWEEP_MEM_CHECKPOINT, "acoustic2d: a host tape goes with boundary saving only");
+    }
     SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY || mem_mode == SWEEP_MEM_CHECKPOINT ||
                       mem_mode == SWEEP_MEM_BOUNDARY_FP16 || mem_mode == SWEEP_MEM_BOUNDARY_BF16 ||
                       mem_mode == SWEEP_MEM_BOUNDARY_INT8,
                   "acoustic2d: unknown memory mode %d", mem_mode);
     SWEEP_REQUIRE(mem_mode != SWEEP_MEM_CHECKPOINT || ckpt_every >= 1,
                   "acoustic2d: checkpoint interval must be >= 1 (got %d)", ckpt_every);
+}
+
+static void copy_any(void* dst, const void* src, long long bytes, cudaStream_t st)
+{
+    SWEEP_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, st));
 }
 
 void sizes(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, int64_t* ws, int64_t* tape)
@@ -1437,7 +1457,7 @@ static FwdMaps fwd_maps(const FwdWork& w, const Params& P)
 // is the strip slot step `it` writes (null: none), `record` may be null.
 template <class StripsOf>
 static void forward_steps(const Plan& pl, const FwdMaps& maps, const FwdWork& w, float* record, FwdState& S,
-                          int it0, int it1, StripsOf strips_of, cudaStream_t st)
+                          int it0, int it1, StripsOf strips_of, cudaStream_t st, HostRing* hr = nullptr)
 {
     Params PF = pl.P;
     PF.G = pl.Gf;
@@ -1450,6 +1470,7 @@ static void forward_steps(const Plan& pl, const FwdMaps& maps, const FwdWork& w,
         F.now = S.in; F.prev = S.ip; F.u_next = w.u[S.ix];
         F.psix = S.px; F.psiz = S.pz; F.psixn = S.pxn; F.psizn = S.pzn;
         void* slot = strips_of(it);
+        if (slot && hr) hr->before_write(it);
         F.strips = (slot && scaled) ? static_cast<void*>(w.scratch) : slot;
         F.sbf16 = PF.st.fmt == SF_BF16;
         fwd_kernel<<<pl.gridf, NTH, fwd_smem(), st>>>(maps, PF, F, it);
@@ -1458,6 +1479,7 @@ static void forward_steps(const Plan& pl, const FwdMaps& maps, const FwdWork& w,
             quantize_strips<<<qblocks, kQB, 0, st>>>(PF, w.scratch, slot);
             SWEEP_LAUNCH_CHECK();
         }
+        if (slot && hr) hr->after_write(it);
         const int t = S.ip; S.ip = S.in; S.in = S.ix; S.ix = t;
         std::swap(S.px, S.pxn); std::swap(S.pz, S.pzn);
     }
@@ -1496,7 +1518,15 @@ void forward_with(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, fl
     const FwdMaps maps = fwd_maps(w, P);
     FwdState S;
     S.px = w.psix; S.pz = w.psiz; S.pxn = w.psixn; S.pzn = w.psizn;
-    if (ckpt_every <= 0) {
+    if (ckpt_every <= 0 && tape && pl.host_tape) {
+        HostRing hr;
+        hr.open(w.ring, tape, P.st.step, st);
+        forward_steps(pl, maps, w, record, S, 0, d->nt, [&](int it) { return hr.slot(it); }, st, &hr);
+        hr.close();
+        float* last = tape_last(tape, pl);
+        copy_any(last, w.u[S.ip], n * 4, st);
+        copy_any(last + n, w.u[S.in], n * 4, st);
+    } else if (ckpt_every <= 0) {
         forward_steps(pl, maps, w, record, S, 0, d->nt,
                       [&](int it) { return tape ? tape_slot(tape, pl, it) : nullptr; }, st);
         if (tape) {
@@ -1591,6 +1621,8 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     int cur = 0;
     // Reverse steps [it0, it1) top down; the reconstruction starts from
     // r[0] = U[it1], r[1] = U[it1 - 1]; strips_of(it) holds the strips of U[it].
+    HostRing hr;
+    const bool host = pl.host_tape && !ckpt;
     auto reverse = [&](int it0, int it1, auto strips_of) {
         int rp = 0, rn = 1, rx = 2;
         for (int it = it1 - 1; it >= it0; --it) {
@@ -1601,8 +1633,13 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
             R.cur = cur;
             R.rprev = rp; R.rnow = rn; R.r_next = w.r[rx];
             R.strips = do_recon ? strips_of(it - 1) : nullptr;
+            if (host && do_recon) hr.before_read(it - 1);
             rev_kernel<<<pl.gridr, NTH, rev_smem(), st>>>(maps, P, R, it, do_recon);
             SWEEP_LAUNCH_CHECK();
+            if (host && do_recon) {
+                hr.after_read(it - 1);
+                if (it - 1 - HostRing::R >= 0) hr.fetch(it - 1 - HostRing::R, true);
+            }
             int t = lp; lp = ln; ln = lx; lx = t;
             cur = 1 - cur;
             if (do_recon) { t = rp; rp = rn; rn = rx; rx = t; }
@@ -1612,9 +1649,16 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
         const float* last = tape_last(const_cast<void*>(tape), pl);
         // seed: prev = U[nt], now = U[nt-1]  (reference driver_traits.cuh:493-505; the
         // rim outside the physical box is never read by the reconstruction)
-        copy_dd(w.r[0], last + n, n, st);
-        copy_dd(w.r[1], last, n, st);
-        reverse(0, d->nt, [&](int t) { return tape_slot(tape, pl, t); });
+        copy_any(w.r[0], last + n, n * 4, st);
+        copy_any(w.r[1], last, n * 4, st);
+        if (host) {
+            hr.open(w.ring, const_cast<void*>(tape), P.st.step, st);
+            for (int t = d->nt - 2; t >= 0 && t > d->nt - 2 - HostRing::R; --t) hr.fetch(t, false);
+            reverse(0, d->nt, [&](int t) { return hr.slot(t); });
+            hr.close();
+        } else {
+            reverse(0, d->nt, [&](int t) { return tape_slot(tape, pl, t); });
+        }
     } else {
         const int k = ckpt_every, C = nchunks(pl, k);
         const FwdMaps fmaps = fwd_maps(fw, P);

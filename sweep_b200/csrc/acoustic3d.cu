@@ -47,6 +47,7 @@ struct StripStore {
     int cells[6], blocks[6];         // per shot and face (top, bottom, front, back, left, right)
     long long pay[6], scl[6];        // byte offsets of each face's codes and scales in a step slot
     long long step;                  // bytes of one step slot
+    int host;                        // the tape is pinned host memory (SWEEP_MEM_HOST_TAPE)
 };
 
 struct Params {
@@ -962,6 +963,7 @@ struct Work {
     float* f[34];                    // forward: u x3, psi x6, zeta x3; reverse: see backward()
     int* err;                        // bounded-wait failure flag
     float* scratch;                  // one step's fp32 strips ahead of their quantisation (scaled formats)
+    char* ring;                      // host tape: HostRing::R device strip slots
 };
 
 static Work carve(Carve& c, const Params& P, int nfields)
@@ -971,6 +973,7 @@ static Work carve(Carve& c, const Params& P, int nfields)
     for (int i = 0; i < nfields; ++i) w.f[i] = c.take<float>((long long)P.B * P.S);
     w.err = c.take<int>(1);
     if (P.st.fmt == SF_F16 || P.st.fmt == SF_I8) w.scratch = c.take<float>((long long)P.B * P.nstrip);
+    if (P.st.host) w.ring = c.take<char>((long long)HostRing::R * P.st.step);
     return w;
 }
 
@@ -1004,6 +1007,8 @@ static void set_store(Params& P, int mem_mode)
 {
     StripStore& S = P.st;
     S = StripStore{};
+    S.host = (mem_mode & SWEEP_MEM_HOST_TAPE) != 0;
+    mem_mode &= ~SWEEP_MEM_HOST_TAPE;
     S.w = M + 1;
     S.fmt = mem_mode == SWEEP_MEM_BOUNDARY_FP16 ? SF_F16
           : mem_mode == SWEEP_MEM_BOUNDARY_BF16 ? SF_BF16
@@ -1060,7 +1065,11 @@ static constexpr int kFwdFields = 12, kRevFields = 22;
 // eq_driver.cuh:928-1135: chunked replay).
 static constexpr int kStateFields = 8;
 
-static int nchunks(const Params& P, int k) { return (P.nt + k - 1) / k; }
+static int nchunks(const Params& P, int k)
+{
+    SWEEP_REQUIRE(k >= 1, "acoustic3d: checkpoint interval must be >= 1 (got %d)", k);
+    return (P.nt + k - 1) / k;
+}
 
 static long long ckpt_stride(const Params& P)
 {
@@ -1080,10 +1089,13 @@ static float* ckpt_strips(void* tape, const Params& P, int c) { return ckpt_fiel
 
 void sizes(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, int64_t* ws, int64_t* tape)
 {
-    SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY || mem_mode == SWEEP_MEM_CHECKPOINT ||
-                      mem_mode == SWEEP_MEM_BOUNDARY_FP16 || mem_mode == SWEEP_MEM_BOUNDARY_BF16 ||
-                      mem_mode == SWEEP_MEM_BOUNDARY_INT8,
+    const int base_mode = mem_mode & ~SWEEP_MEM_HOST_TAPE;
+    SWEEP_REQUIRE(base_mode == SWEEP_MEM_BOUNDARY || base_mode == SWEEP_MEM_CHECKPOINT ||
+                      base_mode == SWEEP_MEM_BOUNDARY_FP16 || base_mode == SWEEP_MEM_BOUNDARY_BF16 ||
+                      base_mode == SWEEP_MEM_BOUNDARY_INT8,
                   "acoustic3d: unknown memory mode %d", mem_mode);
+    SWEEP_REQUIRE(!(mem_mode & SWEEP_MEM_HOST_TAPE) || base_mode != SWEEP_MEM_CHECKPOINT,
+                  "acoustic3d: a host tape goes with boundary saving only");
     SWEEP_REQUIRE(mem_mode != SWEEP_MEM_CHECKPOINT || ckpt_every >= 1,
                   "acoustic3d: checkpoint interval must be >= 1 (got %d)", ckpt_every);
     Params P = make_params(d);
@@ -1125,7 +1137,8 @@ struct FwdState {
 // none), source injection, receiver gather (record may be null).
 template <class StripsOf>
 static void forward_steps(const sweep_acoustic_desc* d, const Params& P, FwdState& S, float* record, int it0,
-                          int it1, StripsOf strips_of, int* err, float* scratch, cudaStream_t st)
+                          int it1, StripsOf strips_of, int* err, float* scratch, cudaStream_t st,
+                          HostRing* hr = nullptr)
 {
     const bool scaled = P.st.fmt == SF_F16 || P.st.fmt == SF_I8;
     int qper = 0;
@@ -1151,8 +1164,10 @@ static void forward_steps(const sweep_acoustic_desc* d, const Params& P, FwdStat
         SWEEP_LAUNCH_CHECK();
         void* slot = strips_of(it);
         if (slot && P.nstrip > 0) {
+            if (hr) hr->before_write(it);
             strips3<<<gst, 256, 0, st>>>(P, S.f[S.in], slot, scratch, 0);
             if (scaled) quantize_strips3<<<(unsigned)(P.B * qper), kQB, 0, st>>>(P, scratch, slot);
+            if (hr) hr->after_write(it);
         }
         if (d->nsrc > 0)
             inject3<<<gs, 128, 0, st>>>(P, S.f[S.ix], d->wavelet, d->src_loc, d->nsrc, it, 0, 1.f, 0);
@@ -1191,7 +1206,17 @@ void forward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* 
     SWEEP_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
     if (d->nrec > 0) SWEEP_CUDA(cudaMemsetAsync(record, 0, (size_t)d->B * d->nt * d->nrec * 4, st));
     FwdState S(w.f);
-    if (mem_mode != SWEEP_MEM_CHECKPOINT) {
+    if (mem_mode != SWEEP_MEM_CHECKPOINT && tape && P.st.host) {
+        HostRing hr;
+        hr.open(w.ring, tape, P.st.step, st);
+        forward_steps(d, P, S, record, 0, d->nt, [&](int it) { return hr.slot(it); }, w.err, w.scratch, st, &hr);
+        hr.close();
+        float* last = tape_last(tape, P);
+        SWEEP_CUDA(cudaMemcpyAsync(last, S.f[S.ip], n * 4, cudaMemcpyDefault, st));       // U[nt-1]
+        SWEEP_CUDA(cudaMemcpyAsync(last + n, S.f[S.in], n * 4, cudaMemcpyDefault, st));   // U[nt]
+        check_err(w, st, "forward");
+        return;
+    } else if (mem_mode != SWEEP_MEM_CHECKPOINT) {
         forward_steps(d, P, S, record, 0, d->nt, [&](int it) { return tape ? tape_slot(tape, P, it) : nullptr; },
                       w.err, w.scratch, st);
         if (tape) {
@@ -1279,6 +1304,8 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     rmaps.gc = plane_map(gcomp, P, P.B, false);
     // Reverse steps [it0, it1) top down from prev = U[it1] (f[15]), now =
     // U[it1 - 1] (f[16]); strips_of(t) holds the strips of U[t].
+    HostRing hr;
+    const bool host = P.st.host && !ckpt;
     auto reverse = [&](int it0, int it1, auto strips_of) {
         int rp = 15, rn = 16, rx = 17;
         for (int it = it1 - 1; it >= it0; --it) {
@@ -1299,7 +1326,12 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
                 R3 R{w.f[rn], w.f[rp], w.f[rx], w.f[ln], gacc, gcomp, is, ir};
                 r3_recon<<<grid, block, sizeof(R3Smem), st>>>(rmaps, P, R, rn - 15, rp - 15, ln, w.err);
                 if (P.nstrip > 0) {
+                    if (host) hr.before_read(it - 1);
                     strips3<<<gst, 256, 0, st>>>(P, w.f[rx], strips_of(it - 1), nullptr, 1);
+                    if (host) {
+                        hr.after_read(it - 1);
+                        if (it - 1 - HostRing::R >= 0) hr.fetch(it - 1 - HostRing::R, true);
+                    }
                     if (d->nsrc > 0)
                         inject3<<<gs, 128, 0, st>>>(P, w.f[rx], d->wavelet, d->src_loc, d->nsrc, it, 0, -1.f, 1);
                     Img I{w.f[rp], w.f[rn], w.f[rx], w.f[ln], gacc, gcomp, is, ir};
@@ -1317,9 +1349,16 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     };
     if (!ckpt) {
         const float* last = tape_last(const_cast<void*>(tape), P);
-        copy_dd(w.f[15], last + n, n, st);   // prev = U[nt]
-        copy_dd(w.f[16], last, n, st);       // now  = U[nt-1]
-        reverse(0, d->nt, [&](int t) { return tape_slot(tape, P, t); });
+        SWEEP_CUDA(cudaMemcpyAsync(w.f[15], last + n, n * 4, cudaMemcpyDefault, st));   // prev = U[nt]
+        SWEEP_CUDA(cudaMemcpyAsync(w.f[16], last, n * 4, cudaMemcpyDefault, st));       // now  = U[nt-1]
+        if (host && P.nstrip > 0) {
+            hr.open(w.ring, const_cast<void*>(tape), P.st.step, st);
+            for (int t = d->nt - 2; t >= 0 && t > d->nt - 2 - HostRing::R; --t) hr.fetch(t, false);
+            reverse(0, d->nt, [&](int t) { return hr.slot(t); });
+            hr.close();
+        } else {
+            reverse(0, d->nt, [&](int t) { return tape_slot(tape, P, t); });
+        }
     } else {
         const int k = ckpt_every, C = nchunks(P, k);
         void* tp = const_cast<void*>(tape);

@@ -85,6 +85,78 @@ struct Carve {
     }
 };
 
+// Boundary-saving tape in pinned host memory (reference
+// BoundarySaving(storage='cpu'), boundary/runtime.cuh:91-620): the step
+// kernels write a ring of R device slots; a copy stream moves forward slot it
+// to host slot it and, in the reverse, brings host slots back into the ring
+// ahead of their use.  Events order every reuse of a ring slot; close() makes
+// the caller's stream wait for every copy.
+struct HostRing {
+    static constexpr int R = 4;
+    char* ring = nullptr;            // R device slots of `step` bytes
+    char* host = nullptr;            // the host tape (pinned)
+    long long step = 0;
+    cudaStream_t main = nullptr, copy = nullptr;
+    cudaEvent_t ready[R], freed[R];
+
+    void open(void* ring_, void* host_, long long step_, cudaStream_t st)
+    {
+        ring = static_cast<char*>(ring_);
+        host = static_cast<char*>(host_);
+        step = step_;
+        main = st;
+        SWEEP_CUDA(cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking));
+        for (int i = 0; i < R; ++i) {
+            SWEEP_CUDA(cudaEventCreateWithFlags(&ready[i], cudaEventDisableTiming));
+            SWEEP_CUDA(cudaEventCreateWithFlags(&freed[i], cudaEventDisableTiming));
+        }
+        after(main, copy);           // the copies start after the work queued so far
+    }
+    void* slot(int t) const { return ring + (long long)(t % R) * step; }
+    // forward: the copy that last emptied slot(t) must be done before step t writes it
+    void before_write(int t)
+    {
+        if (t >= R) SWEEP_CUDA(cudaStreamWaitEvent(main, freed[t % R], 0));
+    }
+    // forward: once step t's kernels are done, move slot(t) to host slot t
+    void after_write(int t)
+    {
+        SWEEP_CUDA(cudaEventRecord(ready[t % R], main));
+        SWEEP_CUDA(cudaStreamWaitEvent(copy, ready[t % R], 0));
+        SWEEP_CUDA(cudaMemcpyAsync(host + (long long)t * step, slot(t), step, cudaMemcpyDeviceToHost, copy));
+        SWEEP_CUDA(cudaEventRecord(freed[t % R], copy));
+    }
+    // reverse: host slot t into the ring, after the slot's last reader when `reused`
+    void fetch(int t, bool reused)
+    {
+        if (reused) SWEEP_CUDA(cudaStreamWaitEvent(copy, freed[t % R], 0));
+        SWEEP_CUDA(cudaMemcpyAsync(slot(t), host + (long long)t * step, step, cudaMemcpyHostToDevice, copy));
+        SWEEP_CUDA(cudaEventRecord(ready[t % R], copy));
+    }
+    void before_read(int t) { SWEEP_CUDA(cudaStreamWaitEvent(main, ready[t % R], 0)); }
+    void after_read(int t) { SWEEP_CUDA(cudaEventRecord(freed[t % R], main)); }
+    void close()
+    {
+        if (!copy) return;
+        after(copy, main);
+        for (int i = 0; i < R; ++i) {
+            cudaEventDestroy(ready[i]);
+            cudaEventDestroy(freed[i]);
+        }
+        cudaStreamDestroy(copy);     // released once its queued work is done
+        copy = nullptr;
+    }
+    // `later` waits for the work queued on `earlier` so far
+    static void after(cudaStream_t earlier, cudaStream_t later)
+    {
+        cudaEvent_t e;
+        SWEEP_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        SWEEP_CUDA(cudaEventRecord(e, earlier));
+        SWEEP_CUDA(cudaStreamWaitEvent(later, e, 0));
+        SWEEP_CUDA(cudaEventDestroy(e));
+    }
+};
+
 // Source / receiver events grouped by (shot, tile): a CSR table so that the
 // CTA owning a tile finds its point sources and receivers without scanning the
 // whole list.  `cell` is the tile-local linear cell index, `id` the global

@@ -1245,7 +1245,11 @@ static long long ckpt_stride(const Plan& pl)
     return (c.off + 255) & ~255LL;
 }
 
-static int nchunks(const Plan& pl, int k) { return (pl.G.nt + k - 1) / k; }
+static int nchunks(const Plan& pl, int k)
+{
+    SWEEP_REQUIRE(k >= 1, "elastic2d: checkpoint interval must be >= 1 (got %d)", k);
+    return (pl.G.nt + k - 1) / k;
+}
 
 struct Ckpt {
     float* f[5];

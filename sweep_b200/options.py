@@ -24,14 +24,20 @@ class BoundarySaving:
       of the normalised values.
 
     Every equation takes every format (Elastic quantises each of its five
-    fields on its own)."""
+    fields on its own).
+
+    ``storage='cpu'`` (reference ``options.py:186-192``) keeps the tape in
+    pinned host memory: the step kernels write a small device ring and a copy
+    stream moves each step's strips to the host (forward) and back ahead of
+    their use (backward), so the tape no longer takes GPU memory (acoustic 2-D
+    and 3-D)."""
     storage: str = "gpu"
     storage_dtype: str = "fp32"
 
     def __post_init__(self):
-        if self.storage != "gpu":
-            raise NotImplementedError("sweep_b200 keeps the boundary ring in GPU memory only "
-                                      "(storage='gpu')")
+        if self.storage not in ("gpu", "cpu"):
+            raise NotImplementedError("sweep_b200 keeps the boundary strips in GPU memory (storage='gpu') or "
+                                      "in pinned host memory (storage='cpu'); disk storage is not built")
         if self.storage_dtype not in ("fp32", "fp16", "bf16", "int8"):
             raise ValueError("BoundarySaving.storage_dtype must be 'fp32', 'fp16', 'bf16', or 'int8'.")
 

@@ -224,7 +224,12 @@ class _AcousticFn(torch.autograd.Function):
         _lib.call("sweep_b200_acoustic_sizes", desc, mem_mode, ckpt_every, ws_b, tape_b)
         need_bwd = any(ctx.needs_input_grad[:2])
         ws = prop._workspace(ws_b.value, vp.device)
-        tape = torch.empty(tape_b.value, dtype=torch.uint8, device=vp.device) if need_bwd else None
+        if not need_bwd:
+            tape = None
+        elif mem_mode & _lib.MEM_HOST_TAPE:
+            tape = torch.empty(tape_b.value, dtype=torch.uint8, pin_memory=True)
+        else:
+            tape = torch.empty(tape_b.value, dtype=torch.uint8, device=vp.device)
         record = torch.empty((geo.B, geo.nt, geo.nrec), dtype=torch.float32, device=vp.device)
         _lib.call("sweep_b200_acoustic_forward", desc, mem_mode, ckpt_every, record.data_ptr(),
                   tape.data_ptr() if tape is not None else None, ws.data_ptr(), ws.numel(),
@@ -428,8 +433,13 @@ class PropTorch(torch.nn.Module):
         if isinstance(self.memory, Ckpt):
             return _lib.MEM_CHECKPOINT, int(self.memory.chunks)
         sd = getattr(self.memory, "storage_dtype", "fp32")
-        return {"fp32": _lib.MEM_BOUNDARY, "fp16": _lib.MEM_BOUNDARY_FP16, "bf16": _lib.MEM_BOUNDARY_BF16,
-                "int8": _lib.MEM_BOUNDARY_INT8}[sd], 0
+        mode = {"fp32": _lib.MEM_BOUNDARY, "fp16": _lib.MEM_BOUNDARY_FP16, "bf16": _lib.MEM_BOUNDARY_BF16,
+                "int8": _lib.MEM_BOUNDARY_INT8}[sd]
+        if getattr(self.memory, "storage", "gpu") == "cpu":
+            if isinstance(self.equation, Elastic):
+                raise NotImplementedError("BoundarySaving(storage='cpu') is built for the acoustic equations")
+            mode |= _lib.MEM_HOST_TAPE
+        return mode, 0
 
     # ---------------------------------------------------------------- forward
     def forward(self, wavelet, sources, receivers, models=None, max_vel=4500.0, pml_freq=25.0):

@@ -96,3 +96,24 @@ def test_elastic_reduced_storage_matches_reference(sd):
         assert rel(g32[i], ref32) < GRAD_TOL
         assert err < GRAD_TOL
         assert pert < E_PERT_TOL[sd]
+
+
+@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("sd", ["fp32", "int8"])
+def test_host_tape_is_bit_identical(case, sd):
+    """BoundarySaving(storage='cpu'): the same tape bytes go through pinned host
+    memory, so the gradient is bit-identical to the device tape's."""
+    from sweep_b200 import Acoustic, Acoustic3D, BoundarySaving, PropTorch
+    d = load(case)
+    grads = []
+    for storage in ("gpu", "cpu"):
+        eq = (Acoustic3D if d["vp_true"].ndim == 3 else Acoustic)(spatial_order=8, device=DEV)
+        s = PropTorch(eq, shape=tuple(d["vp_true"].shape), dh=float(d["dh"]), dt=float(d["dt"]),
+                      abcn=int(d["abcn"]), device=DEV, memory=BoundarySaving(storage=storage, storage_dtype=sd))
+        vp = torch.tensor(d["vp_init"], device=DEV, requires_grad=True)
+        pred = s(torch.tensor(d["wavelet"], device=DEV), d["src"], d["rec"], models=[vp])
+        loss = 0.5 * ((pred - torch.tensor(d["obs"], device=DEV)) ** 2).sum()
+        loss.backward()
+        torch.cuda.synchronize()
+        grads.append(vp.grad.cpu().numpy())
+    assert np.array_equal(grads[0], grads[1])
