@@ -177,6 +177,16 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+# Boundary-saving tape of the acoustic workloads: (storage, strip dtype); the
+# default line is the reference's default, fp32 strips in GPU memory
+STRIPS = ["gpu", "fp32"]
+
+
+def boundary_memory():
+    from sweep_b200 import BoundarySaving
+    return BoundarySaving(storage=STRIPS[0], storage_dtype=STRIPS[1])
+
+
 # --------------------------------------------------------------- workloads
 class AcousticWorkload:
     name = "acoustic2d"
@@ -198,13 +208,14 @@ class AcousticWorkload:
                 "cells_counted": "runtime grid (physical + PML + halo) x shots x nt",
                 "physical_fraction": NZ * NX / (RT[0] * RT[1]),
                 "l2": "working set per step > L2 (inputs larger than L2; no flush)",
+                "boundary_tape": f"{STRIPS[1]} strips in {STRIPS[0]} memory",
                 "parallelism": f"shots: {NSHOT} per GPU x {args.gpus} GPU(s)"}
 
     def build(self, dev):
         from sweep_b200 import Acoustic, PropTorch
         vp_true, vp_init, w, src, rec = survey()
         solver = PropTorch(Acoustic(spatial_order=ORDER, device=dev), shape=(NZ, NX), dh=DH, dt=DT,
-                           abcn=ABCN, device=dev)
+                           abcn=ABCN, device=dev, memory=boundary_memory())
         return solver, [vp_true], [vp_init], w, src, rec
 
     def launches(self):
@@ -323,13 +334,14 @@ class Acoustic3DWorkload:
                 "cells_counted": "runtime grid (physical + PML + halo) x shots x nt",
                 "physical_fraction": (A3_N / A3_RT[0]) ** 3,
                 "l2": "working set per step > L2 (inputs larger than L2; no flush)",
+                "boundary_tape": f"{STRIPS[1]} strips in {STRIPS[0]} memory",
                 "parallelism": f"shots: {A3_NSHOT} per GPU x {args.gpus} GPU(s)"}
 
     def build(self, dev):
         from sweep_b200 import Acoustic3D, PropTorch
         m_true, m_init, w, src, rec = acoustic3d_survey()
         solver = PropTorch(Acoustic3D(spatial_order=ORDER, device=dev), shape=(A3_N,) * 3, dh=A3_DH,
-                           dt=A3_DT, abcn=A3_ABCN, device=dev)
+                           dt=A3_DT, abcn=A3_ABCN, device=dev, memory=boundary_memory())
         return solver, m_true, m_init, w, src, rec
 
     def launches(self):
@@ -604,6 +616,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--storage", default="gpu", choices=["gpu", "cpu"],
+                    help="acoustic workloads: boundary tape in GPU memory or pinned host memory")
+    ap.add_argument("--strip-dtype", default="fp32", choices=["fp32", "fp16", "bf16", "int8"],
+                    help="acoustic workloads: boundary strip storage format (fp32 is exact)")
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the end-to-end leg (long workloads; the bench line then has no e2e value)")
     ap.add_argument("--pairs", type=int, default=1024, help="fwi workload: training pairs")
@@ -616,6 +632,7 @@ def main():
     ap.add_argument("--shots", type=int, default=None,
                     help="fewer shots (profiling captures of a few GB only; the bench line is for the full survey)")
     args = ap.parse_args()
+    STRIPS[:] = [args.storage, args.strip_dtype]
     if args.workload == "fwi":
         run_fwi(args)
         return
