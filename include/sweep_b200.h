@@ -85,7 +85,7 @@ typedef struct sweep_acoustic_desc {
 /* OR'ed into a boundary-saving mode (0, 2, 3, 4): `tape` is pinned HOST
  * memory (reference BoundarySaving(storage='cpu'), boundary/runtime.cuh:
  * 91-620); the strips pass through a small device ring in the workspace and a
- * copy stream.  Acoustic 2-D and 3-D. */
+ * copy stream.  Every equation. */
 #define SWEEP_MEM_HOST_TAPE 0x100
 
 /* Bytes the caller must allocate: `workspace` (scratch, reusable between calls

@@ -1075,6 +1075,7 @@ struct Plan {
     int nm;          // model copies
     int gshots;      // shots per rev_str CTA
     int nslot;       // gradient slots
+    bool host_tape;  // boundary-saving tape in pinned host memory (SWEEP_MEM_HOST_TAPE)
 };
 
 static int env_int(const char* name, int dflt)
@@ -1172,6 +1173,7 @@ struct FwdWs {
     char* zero0;          // [zero0, zero1) cleared before the time loop
     char* zero1;
     float* scratch;       // one step's fp32 strips ahead of their quantisation (scaled formats)
+    char* ring;           // host tape: HostRing::R device strip slots
 };
 
 static void carve_fwd(Carve& c, const Plan& pl, FwdWs& w)
@@ -1184,6 +1186,7 @@ static void carve_fwd(Carve& c, const Plan& pl, FwdWs& w)
     c.take<char>(0);
     w.zero1 = c.base ? c.base + c.off : nullptr;
     if (pl.G.st.fmt == SF_F16 || pl.G.st.fmt == SF_I8) w.scratch = c.take<float>(5LL * pl.G.B * pl.G.nstrip);
+    if (pl.host_tape) w.ring = c.take<char>((long long)HostRing::R * pl.G.st.step);
 }
 
 struct RevWs {
@@ -1197,6 +1200,7 @@ struct RevWs {
     char* zero1;
     Slabs fmem;           // checkpoint mode: forward CPML memories of the replay
     float* chunk;         // checkpoint mode: strips of one chunk, (k + 1, B, 5, nstrip)
+    char* ring;           // host tape: HostRing::R device strip slots
 };
 
 static void carve_rev(Carve& c, const Plan& pl, RevWs& w)
@@ -1216,6 +1220,7 @@ static void carve_rev(Carve& c, const Plan& pl, RevWs& w)
     w.grho = c.take<float>((long long)pl.nslot * G.S);
     c.take<char>(0);
     w.zero1 = c.base ? c.base + c.off : nullptr;
+    if (pl.host_tape) w.ring = c.take<char>((long long)HostRing::R * G.st.step);
 }
 
 static void carve_rev_ckpt(Carve& c, const Plan& pl, int k, RevWs& w)
@@ -1284,6 +1289,8 @@ static void slabs_copy(const Slabs& s, float* packed, const Geo& G, bool to_pack
 // tape (the checkpoint mode keeps its chunk strips as fp32).
 static void set_store(Plan& pl, int mem_mode)
 {
+    pl.host_tape = (mem_mode & SWEEP_MEM_HOST_TAPE) != 0;
+    mem_mode &= ~SWEEP_MEM_HOST_TAPE;
     Geo& G = pl.G;
     StripStore& S = G.st;
     S = StripStore{};
@@ -1432,6 +1439,10 @@ constexpr size_t SM_REV_VADJ = 7 * HN * sizeof(float);
 
 static void check_mode(int mem_mode, int ckpt_every)
 {
+    if (mem_mode & SWEEP_MEM_HOST_TAPE) {
+        mem_mode &= ~SWEEP_MEM_HOST_TAPE;
+        SWEEP_REQUIRE(mem_mode != SWEEP_MEM_CHECKPOINT, "elastic2d: a host tape goes with boundary saving only");
+    }
     SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY || mem_mode == SWEEP_MEM_CHECKPOINT ||
                       mem_mode == SWEEP_MEM_BOUNDARY_FP16 || mem_mode == SWEEP_MEM_BOUNDARY_BF16 ||
                       mem_mode == SWEEP_MEM_BOUNDARY_INT8,
@@ -1463,7 +1474,8 @@ void sizes(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, int64_t* w
 // Forward steps [it0, it1) on the fields / memories of A; strips_of(it) is
 // the strip slot of step it (null: none).
 template <class StripsOf>
-static void forward_steps(FwdArgs& A, int it0, int it1, StripsOf strips_of, float* scratch, cudaStream_t st)
+static void forward_steps(FwdArgs& A, int it0, int it1, StripsOf strips_of, float* scratch, cudaStream_t st,
+                          HostRing* hr = nullptr)
 {
     const Geo& G = A.G;
     set_attrs();
@@ -1476,8 +1488,10 @@ static void forward_steps(FwdArgs& A, int it0, int it1, StripsOf strips_of, floa
         void* slot = strips_of(it);
         A.strips = (slot && scaled) ? static_cast<void*>(scratch) : slot;
         fwd_vel<<<grid, block, SM_FWD_VEL, st>>>(maps, A);
+        if (slot && hr) hr->before_write(it);
         fwd_str<<<grid, block, SM_FWD_STR, st>>>(maps, A);
         if (slot && scaled) quantize_strips<<<qblocks, kQB, 0, st>>>(G, scratch, slot);
+        if (slot && hr) hr->after_write(it);
     }
     SWEEP_LAUNCH_CHECK();
 }
@@ -1507,11 +1521,17 @@ void forward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, float* r
     const Geo& G = pl.G;
     const long long n = (long long)G.B * G.S;
     if (mem_mode != SWEEP_MEM_CHECKPOINT) {
-        forward_steps(A, 0, G.nt, [&](int it) { return tape ? tape_slot(tape, pl, it) : nullptr; }, w.scratch, st);
+        HostRing hr;
+        const bool host = tape && pl.host_tape;
+        if (host) hr.open(w.ring, tape, G.st.step, st);
+        forward_steps(A, 0, G.nt,
+                      [&](int it) { return !tape ? nullptr : host ? hr.slot(it) : tape_slot(tape, pl, it); },
+                      w.scratch, st, host ? &hr : nullptr);
+        if (host) hr.close();
         if (tape) {
             float* last = tape_last(tape, pl);
             for (int k = 0; k < 5; ++k)
-                SWEEP_CUDA(cudaMemcpyAsync(last + k * n, w.f[k], sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+                SWEEP_CUDA(cudaMemcpyAsync(last + k * n, w.f[k], sizeof(float) * n, cudaMemcpyDefault, st));
         }
         check_err(w.cm, st, "forward");
         return;
@@ -1567,15 +1587,22 @@ void backward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, const f
     // Reverse steps it1 - 1 .. max(it0, 1) (the staggered reverse has no
     // it = 0 step) on the reconstruction state after step it1 - 1;
     // strips_of(t) holds the strips of the state after step t.
+    HostRing hr;
+    const bool host = pl.host_tape && !ckpt;
     auto reverse = [&](int it0, int it1, auto strips_of) {
         for (int it = it1 - 1; it >= std::max(it0, 1); --it) {
             A.it = it;
             A.strips = strips_of(it - 1);
             A.mo = w.m[cur];
             A.mn = w.m[cur ^ 1];
+            if (host) hr.before_read(it - 1);
             rev_str<<<grid_s, block, SM_REV_STR, st>>>(A);
             rev_sadj<<<grid_b, block, SM_REV_SADJ, st>>>(A);
             rev_vadj<<<grid_b, block, SM_REV_VADJ, st>>>(A);
+            if (host) {
+                hr.after_read(it - 1);
+                if (it - 1 - HostRing::R >= 0) hr.fetch(it - 1 - HostRing::R, true);
+            }
             cur ^= 1;
         }
         SWEEP_LAUNCH_CHECK();
@@ -1583,8 +1610,15 @@ void backward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, const f
     if (!ckpt) {
         const float* last = tape_last(const_cast<void*>(tape), pl);
         for (int k = 0; k < 5; ++k)
-            SWEEP_CUDA(cudaMemcpyAsync(w.f[k], last + k * n, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
-        reverse(0, G.nt, [&](int t) { return tape_slot(tape, pl, t); });
+            SWEEP_CUDA(cudaMemcpyAsync(w.f[k], last + k * n, sizeof(float) * n, cudaMemcpyDefault, st));
+        if (host) {
+            hr.open(w.ring, const_cast<void*>(tape), G.st.step, st);
+            for (int t = G.nt - 2; t >= 0 && t > G.nt - 2 - HostRing::R; --t) hr.fetch(t, false);
+            reverse(0, G.nt, [&](int t) { return hr.slot(t); });
+            hr.close();
+        } else {
+            reverse(0, G.nt, [&](int t) { return tape_slot(tape, pl, t); });
+        }
     } else {
         const int k = ckpt_every, C = nchunks(pl, k);
         void* tp = const_cast<void*>(tape);

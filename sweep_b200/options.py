@@ -29,8 +29,8 @@ class BoundarySaving:
     ``storage='cpu'`` (reference ``options.py:186-192``) keeps the tape in
     pinned host memory: the step kernels write a small device ring and a copy
     stream moves each step's strips to the host (forward) and back ahead of
-    their use (backward), so the tape no longer takes GPU memory (acoustic 2-D
-    and 3-D)."""
+    their use (backward), so the tape no longer takes GPU memory (every
+    equation)."""
     storage: str = "gpu"
     storage_dtype: str = "fp32"
 

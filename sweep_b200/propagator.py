@@ -284,7 +284,12 @@ class _ElasticFn(torch.autograd.Function):
         need_bwd = any(ctx.needs_input_grad[:3])
         dev = vp.device
         ws = prop._workspace(ws_b.value, dev)
-        tape = torch.empty(tape_b.value, dtype=torch.uint8, device=dev) if need_bwd else None
+        if not need_bwd:
+            tape = None
+        elif mem_mode & _lib.MEM_HOST_TAPE:
+            tape = torch.empty(tape_b.value, dtype=torch.uint8, pin_memory=True)
+        else:
+            tape = torch.empty(tape_b.value, dtype=torch.uint8, device=dev)
         record = torch.empty((geo.B, geo.nt, geo.nrec, len(rf)), dtype=torch.float32, device=dev)
         _lib.call("sweep_b200_elastic_forward", desc, mem_mode, ckpt_every, record.data_ptr(),
                   tape.data_ptr() if tape is not None else None, ws.data_ptr(), ws.numel(),
@@ -436,8 +441,6 @@ class PropTorch(torch.nn.Module):
         mode = {"fp32": _lib.MEM_BOUNDARY, "fp16": _lib.MEM_BOUNDARY_FP16, "bf16": _lib.MEM_BOUNDARY_BF16,
                 "int8": _lib.MEM_BOUNDARY_INT8}[sd]
         if getattr(self.memory, "storage", "gpu") == "cpu":
-            if isinstance(self.equation, Elastic):
-                raise NotImplementedError("BoundarySaving(storage='cpu') is built for the acoustic equations")
             mode |= _lib.MEM_HOST_TAPE
         return mode, 0
 

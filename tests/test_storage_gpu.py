@@ -117,3 +117,20 @@ def test_host_tape_is_bit_identical(case, sd):
         torch.cuda.synchronize()
         grads.append(vp.grad.cpu().numpy())
     assert np.array_equal(grads[0], grads[1])
+
+
+def test_elastic_host_tape_is_bit_identical():
+    from sweep_b200 import BoundarySaving, Elastic, PropTorch
+    d = load("elastic2d_storage")
+    out = []
+    for storage in ("gpu", "cpu"):
+        s = PropTorch(Elastic(spatial_order=8, device=DEV), shape=tuple(d["vp_true"].shape), dh=float(d["dh"]),
+                      dt=float(d["dt"]), abcn=int(d["abcn"]), device=DEV,
+                      memory=BoundarySaving(storage=storage, storage_dtype="bf16"))
+        ms = [torch.tensor(d[f"{n}_init"], device=DEV, requires_grad=True) for n in ("vp", "vs", "rho")]
+        pred = s(torch.tensor(d["wavelet"], device=DEV), d["src"], d["rec"], models=ms)
+        (0.5 * ((pred - torch.tensor(d["obs"], device=DEV)) ** 2).sum()).backward()
+        torch.cuda.synchronize()
+        out.append([m.grad.cpu().numpy() for m in ms])
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
