@@ -327,9 +327,9 @@ class Acoustic3DWorkload:
 
     def config(self, args):
         return {"workload": f"acoustic3d {A3_N}^3 (runtime {A3_RT[0]}^3), {A3_NSHOT} shots in calls of "
-                            f"{A3_BATCH}, nt {self.nt}, order 8, CPML {A3_ABCN}, fwd+adj gradient, boundary saving",
+                            f"{self.batch}, nt {self.nt}, order 8, CPML {A3_ABCN}, fwd+adj gradient, boundary saving",
                 "grid": [A3_N] * 3, "runtime_grid": list(A3_RT), "shots_per_gpu": A3_NSHOT,
-                "shots_per_call": A3_BATCH, "nt": self.nt, "dh": A3_DH, "dt": A3_DT, "abcn": A3_ABCN,
+                "shots_per_call": self.batch, "nt": self.nt, "dh": A3_DH, "dt": A3_DT, "abcn": A3_ABCN,
                 "order": ORDER, "receivers": 128 * 128, "seed": SEED,
                 "cells_counted": "runtime grid (physical + PML + halo) x shots x nt",
                 "physical_fraction": (A3_N / A3_RT[0]) ** 3,
@@ -616,6 +616,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shots-per-call", type=int, default=None,
+                    help="acoustic3d: shots per solver call (default 4, what a device tape fits)")
     ap.add_argument("--storage", default="gpu", choices=["gpu", "cpu"],
                     help="acoustic workloads: boundary tape in GPU memory or pinned host memory")
     ap.add_argument("--strip-dtype", default="fp32", choices=["fp32", "fp16", "bf16", "int8"],
@@ -643,8 +645,10 @@ def main():
         NT, E_NT, A3_NT = wl.nt, wl.nt, wl.nt
     if args.shots:
         wl.nshot = min(int(args.shots), wl.nshot)
-        if hasattr(wl, "batch"):
-            wl.batch = min(wl.batch, wl.nshot)
+    if args.shots_per_call and hasattr(wl, "batch"):
+        wl.batch = int(args.shots_per_call)
+    if hasattr(wl, "batch"):
+        wl.batch = min(wl.batch, wl.nshot)
     if args.impl == "reference":
         run_reference(args, wl)
     else:
