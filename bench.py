@@ -233,6 +233,63 @@ class AcousticWorkload:
         return RT[0] * RT[1] * shots * nt_sample, time.perf_counter() - t0
 
 
+# Small 2-D workload (--workload acoustic2d_c1): the reference's own
+# CPU-runnable case.  96 x 128, dh 10 m, dt 2 ms, nt 800, order 8, CPML 20;
+# two layers (1500 m/s upper half, 2500 m/s lower half), start model 1500
+# m/s; one 10 Hz Ricker delayed 0.14 s at (x 32, z 48), one receiver at
+# (x 96, z 48).  The runtime grid (144 x 176) fits in L2: the step loop is
+# launch- and latency-bound, which is where the captured CUDA graphs count.
+C1_NZ, C1_NX, C1_NT, C1_DT, C1_DH, C1_ABCN = 96, 128, 800, 0.002, 10.0, 20
+C1_RT = (C1_NZ + 2 * C1_ABCN + 2 * M, C1_NX + 2 * C1_ABCN + 2 * M)
+
+
+def c1_survey():
+    from sweep_b200 import ricker
+    vp_true = np.full((C1_NZ, C1_NX), 1500.0, np.float32)
+    vp_true[C1_NZ // 2:] = 2500.0
+    vp_init = np.full((C1_NZ, C1_NX), 1500.0, np.float32)
+    w = ricker(np.arange(C1_NT) * C1_DT - 0.14, 10.0).astype(np.float32)
+    return vp_true, vp_init, w, np.array([[32, 48]]), np.array([[[96, 48]]])
+
+
+class AcousticC1Workload:
+    name = "acoustic2d_c1"
+    nt, nshot, rt = C1_NT, 1, C1_RT
+    bytes_fwd, bytes_rev = BYTES_FWD, BYTES_REV
+    kernel = "sweep::a2d::rev_kernel (fused adjoint + reconstruction + imaging step)"
+    cpu_nt = C1_NT
+    traffic = None
+
+    def config(self, args):
+        return {"workload": f"acoustic2d {C1_NZ}x{C1_NX} (runtime {C1_RT[0]}x{C1_RT[1]}), 1 shot, nt {C1_NT}, "
+                            f"order 8, CPML {C1_ABCN}, fwd+adj gradient, boundary saving",
+                "grid": [C1_NZ, C1_NX], "runtime_grid": list(C1_RT), "shots_per_gpu": 1, "nt": C1_NT,
+                "dh": C1_DH, "dt": C1_DT, "abcn": C1_ABCN, "order": ORDER,
+                "cells_counted": "runtime grid (physical + PML + halo) x shots x nt",
+                "l2": "working set fits in L2 (0.5 MB per field): latency- and launch-bound, no flush",
+                "boundary_tape": f"{STRIPS[1]} strips in {STRIPS[0]} memory",
+                "parallelism": f"replicas: 1 shot per GPU x {args.gpus} GPU(s)"}
+
+    def build(self, dev):
+        from sweep_b200 import Acoustic, PropTorch
+        vp_true, vp_init, w, src, rec = c1_survey()
+        solver = PropTorch(Acoustic(spatial_order=ORDER, device=dev), shape=(C1_NZ, C1_NX), dh=C1_DH,
+                           dt=C1_DT, abcn=C1_ABCN, device=dev, memory=boundary_memory())
+        return solver, [vp_true], [vp_init], w, src, rec
+
+    def launches(self):
+        return 2 * self.nt + 1
+
+    def cpu_run(self, nt_sample, shots=1):
+        from oracle import oracle as O
+        vp_true, vp_init, w, src, rec = c1_survey()
+        w = w[:nt_sample]
+        obs = O.acoustic_forward(vp_true, w, src, rec, C1_DH, C1_DT, C1_ABCN)
+        t0 = time.perf_counter()
+        O.acoustic_gradient(vp_init, w, src, rec, obs, C1_DH, C1_DT, C1_ABCN)
+        return C1_RT[0] * C1_RT[1] * nt_sample, time.perf_counter() - t0
+
+
 class ElasticWorkload:
     name = "elastic2d"
     nt, nshot, rt = E_NT, E_NSHOT, E_RT
@@ -361,7 +418,8 @@ class Acoustic3DWorkload:
         return A3_RT[0] ** 3 * shots * nt_sample, time.perf_counter() - t0
 
 
-WORKLOADS = {"acoustic2d": AcousticWorkload, "elastic2d": ElasticWorkload, "acoustic3d": Acoustic3DWorkload}
+WORKLOADS = {"acoustic2d": AcousticWorkload, "acoustic2d_c1": AcousticC1Workload, "elastic2d": ElasticWorkload,
+             "acoustic3d": Acoustic3DWorkload}
 
 
 def cpu_threads():
@@ -417,15 +475,18 @@ def run_gpu(args, wl):
 
     from sweep_b200.distributed import all_reduce_
     solver, m_true, m_init, w, src, rec = wl.build(dev)
+    solver.autotune = bool(args.autotune)
     src, rec = src[:wl.nshot], rec[:wl.nshot]
     w_d = torch.tensor(w, device=dev)
     bsz = getattr(wl, "batch", wl.nshot)
     batches = [slice(b, min(b + bsz, wl.nshot)) for b in range(0, wl.nshot, bsz)]
     with torch.no_grad():
         mt = [torch.tensor(m, device=dev) for m in m_true]
+        # with --autotune the first call of the shape tunes its schedule (untimed)
         obs = torch.cat([solver(w_d, src[sl], rec[sl], models=mt) for sl in batches])
         del mt
     ms_d = [torch.tensor(m, device=dev) for m in m_init]
+    schedule = solver.launch_schedule(len(w), src[batches[0]], rec[batches[0]], ms_d)
     torch.cuda.synchronize()
 
     def step(ms_in, w_in, obs_in, ev=None):
@@ -525,7 +586,11 @@ def run_gpu(args, wl):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded layered model, see config)",
-        "config": wl.config(args),
+        "config": dict(wl.config(args), schedule=schedule,
+                       autotune=None if solver.tune_report is None else
+                       {"seconds": solver.tune_report["seconds"], "nt": solver.tune_report["nt"],
+                        "trials_ms": {k: {str(v): 1e3 * t for v, t in r.items()}
+                                      for k, r in solver.tune_report["trials"].items()}}),
         "forward_ms": fwd_ms, "backward_ms": rev_ms,
         "roofline": {"kernel": wl.kernel,
                      "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
@@ -629,12 +694,19 @@ def main():
     ap.add_argument("--workload", default="acoustic2d", choices=sorted(WORKLOADS) + ["fwi"],
                     help="acoustic2d: the 32-shot 256x768 survey (default); elastic2d: the 16-shot "
                          "400x1200 elastic survey")
+    ap.add_argument("--graph-steps", type=int, default=None,
+                    help="time steps per captured CUDA graph in the step loops (0: plain stream launches; "
+                         "default: the library's built-in choice)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="tune the launch schedule of the workload's shape before timing (untimed)")
     ap.add_argument("--nt", type=int, default=None,
                     help="shorter time axis (profiling captures only; the bench line is for the full nt)")
     ap.add_argument("--shots", type=int, default=None,
                     help="fewer shots (profiling captures of a few GB only; the bench line is for the full survey)")
     args = ap.parse_args()
     STRIPS[:] = [args.storage, args.strip_dtype]
+    if args.graph_steps is not None:
+        os.environ["SWEEP_B200_GRAPH_STEPS"] = str(int(args.graph_steps))
     if args.workload == "fwi":
         run_fwi(args)
         return

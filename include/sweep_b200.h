@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define SWEEP_B200_ABI_VERSION 2
+#define SWEEP_B200_ABI_VERSION 3
 
 #if defined(__GNUC__)
 #define SWEEP_B200_API __attribute__((visibility("default")))
@@ -211,6 +211,44 @@ SWEEP_B200_API int sweep_b200_conv3x3_wgrad(const void* x, const void* dy, float
  * in any convolution launched since the last call: the convolution entries
  * return at launch, so their device-side failures surface here. */
 SWEEP_B200_API int sweep_b200_conv3x3_status(void* stream, char* err, int32_t err_cap);
+
+/* Launch schedule of one problem shape.  No counterpart in the reference: its
+ * launch shapes are fixed per kernel (reference
+ * src/sweep/csrc/cuda/launch/config.h:65-70) and its time loop issues every
+ * launch from the host (eq_driver.cuh:357-453).  A schedule is recorded per
+ * shape -- equation family, ndim, shots B, runtime grid, PML pads and whether
+ * models are per shot; nt, sources and receivers are not part of it -- in a
+ * process-wide table behind a mutex, read by every later call of that shape.
+ * The autotuner (sweep_b200.autotune) times candidates and records the
+ * fastest.  A field left at its "built-in" value keeps the library's default;
+ * a per-shot-model problem always runs one shot per CTA. */
+typedef struct sweep_b200_schedule {
+    int32_t shots_fwd;    /* shots per CTA of the forward step kernels (2-D acoustic
+                           * fwd_kernel, elastic fwd_vel / fwd_str); 0 = built-in */
+    int32_t shots_rev;    /* shots per CTA of the reverse kernels that sum the image
+                           * (2-D acoustic rev_kernel, elastic rev_str); 0 = built-in */
+    int32_t z_chunks;     /* 3-D acoustic: z chunks each column block is cut into
+                           * (grid depth per shot); 0 = built-in */
+    int32_t graph_steps;  /* time steps per captured CUDA graph in the step loops
+                           * (0: plain stream launches; < 0: built-in); host-tape
+                           * loops always use plain launches */
+} sweep_b200_schedule;
+
+#define SWEEP_FAMILY_ACOUSTIC 0   /* desc is a sweep_acoustic_desc (2-D or 3-D) */
+#define SWEEP_FAMILY_ELASTIC  1   /* desc is a sweep_elastic_desc */
+
+/* Record `s` as the schedule of the shape of `desc` (replacing any earlier
+ * one).  Host-side only, no device work. */
+SWEEP_B200_API int sweep_b200_schedule_set(int32_t family, const void* desc, const sweep_b200_schedule* s,
+                                           char* err, int32_t err_cap);
+
+/* The schedule a call with `desc` would run, every field resolved (recorded
+ * value, else environment override, else built-in default).  Host-side only. */
+SWEEP_B200_API int sweep_b200_schedule_get(int32_t family, const void* desc, sweep_b200_schedule* out,
+                                           char* err, int32_t err_cap);
+
+/* Forget every recorded schedule.  Host-side only. */
+SWEEP_B200_API int sweep_b200_schedule_clear(void);
 
 /* ABI version (SWEEP_B200_ABI_VERSION) -- checked by the Python loader, like
  * the reference's sweep_core_abi_version() (reference loader.py:92-138). */

@@ -2,9 +2,10 @@
 ``PropTorch(..., impl='c')`` -- 2-D/3-D acoustic and 2-D elastic propagation
 with adjoint gradients, on hand-written sm_100a CUDA kernels behind a C ABI
 (``include/sweep_b200.h``)."""
+from . import autotune
 from .equations import Acoustic, Acoustic3D, Elastic
 from .options import BoundarySaving, Ckpt, Full
 from .propagator import PropTorch
 from .signal import ricker
 
-__all__ = ["Acoustic", "Acoustic3D", "Elastic", "BoundarySaving", "Ckpt", "Full", "PropTorch", "ricker"]
+__all__ = ["autotune", "Acoustic", "Acoustic3D", "Elastic", "BoundarySaving", "Ckpt", "Full", "PropTorch", "ricker"]

@@ -17,7 +17,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIB_PATH = Path(os.environ.get("SWEEP_B200_LIB", HERE / "libsweep_b200.so"))
-ABI_VERSION = 2
+ABI_VERSION = 3
 ERR_CAP = 4096
 
 c_i32, c_i64, c_f32, c_p = ctypes.c_int32, ctypes.c_int64, ctypes.c_float, ctypes.c_void_p
@@ -35,6 +35,9 @@ SYMBOLS = (
     "sweep_b200_conv3x3_gemm",
     "sweep_b200_conv3x3_wgrad",
     "sweep_b200_conv3x3_status",
+    "sweep_b200_schedule_set",
+    "sweep_b200_schedule_get",
+    "sweep_b200_schedule_clear",
 )
 
 MEM_BOUNDARY = 0
@@ -43,6 +46,9 @@ MEM_BOUNDARY_FP16 = 2            # boundary saving, strips stored as scaled fp16
 MEM_BOUNDARY_BF16 = 3
 MEM_BOUNDARY_INT8 = 4
 MEM_HOST_TAPE = 0x100           # OR'ed into a boundary-saving mode: the tape is pinned host memory
+
+FAMILY_ACOUSTIC = 0
+FAMILY_ELASTIC = 1
 
 
 class AcousticDesc(ctypes.Structure):
@@ -75,6 +81,11 @@ class ElasticDesc(ctypes.Structure):
         ("nrec", c_i32), ("rec_loc", c_p),
         ("nrec_fields", c_i32), ("rec_fields", c_i32 * 5),
     ]
+
+
+class Schedule(ctypes.Structure):
+    """Mirror of ``sweep_b200_schedule``."""
+    _fields_ = [("shots_fwd", c_i32), ("shots_rev", c_i32), ("z_chunks", c_i32), ("graph_steps", c_i32)]
 
 
 _lib = None
@@ -117,6 +128,10 @@ def load():
     lib.sweep_b200_conv3x3_wgrad.argtypes = [c_p, c_p, c_p, c_i32, c_i32, c_i32, c_i32, c_i32, c_p,
                                              ctypes.c_char_p, c_i32]
     lib.sweep_b200_conv3x3_status.argtypes = [c_p, ctypes.c_char_p, c_i32]
+    S = ctypes.POINTER(Schedule)
+    lib.sweep_b200_schedule_set.argtypes = [c_i32, c_p, S, ctypes.c_char_p, c_i32]
+    lib.sweep_b200_schedule_get.argtypes = [c_i32, c_p, S, ctypes.c_char_p, c_i32]
+    lib.sweep_b200_schedule_clear.argtypes = []
     for s in SYMBOLS[1:]:
         getattr(lib, s).restype = ctypes.c_int
     _lib = lib

@@ -998,6 +998,7 @@ struct Plan {
     int nm;                          // model copies (1 shared, B per-shot)
     int Gf, Gr;                      // shots per CTA: forward, backward
     dim3 gridf, gridr;
+    int graph_steps;                 // time steps per captured CUDA graph (0: stream launches)
 };
 
 // CSR of the events of (shot, tile): off[key .. key+1) indexes ev, each
@@ -1029,11 +1030,12 @@ static int build_events(const Params& P, const int32_t* loc, int n, int32_t* off
     return off[nkey];
 }
 
-// Shots per CTA: `preferred` (measured best on B200 for this kernel), capped so
-// the grid still fills the GPU; overridable through the environment variable
-// `env` for tuning.
-static int choose_group(int ntiles, int B, const char* env, int preferred)
+// Shots per CTA: the shape's recorded schedule value if any, else the
+// environment variable `env`, else `preferred` (measured best on B200 for this
+// kernel) capped so the grid still fills the GPU.
+static int choose_group(int ntiles, int B, const char* env, int preferred, int recorded)
 {
+    if (recorded >= 1) return std::min({recorded, B, kMaxG});
     if (const char* e = getenv(env)) {
         const int g = atoi(e);
         if (g >= 1) return std::min({g, B, kMaxG});
@@ -1094,8 +1096,10 @@ static Plan make_plan(const sweep_acoustic_desc* d)
     P.ntx = (d->nx + TX - 1) / TX;
     P.ntz = (d->nz + TZ - 1) / TZ;
     const int ntiles = P.ntx * P.ntz;
-    pl.Gf = P.per_shot ? 1 : choose_group(ntiles, P.B, "SWEEP_B200_SHOTS_PER_CTA_FWD", 2);
-    pl.Gr = P.per_shot ? 1 : choose_group(ntiles, P.B, "SWEEP_B200_SHOTS_PER_CTA_REV", 8);
+    const sweep_b200_schedule sc = recorded_schedule(d);
+    pl.Gf = P.per_shot ? 1 : choose_group(ntiles, P.B, "SWEEP_B200_SHOTS_PER_CTA_FWD", 2, sc.shots_fwd);
+    pl.Gr = P.per_shot ? 1 : choose_group(ntiles, P.B, "SWEEP_B200_SHOTS_PER_CTA_REV", 8, sc.shots_rev);
+    pl.graph_steps = resolve_graph_steps(sc.graph_steps);
     // blockIdx.x = shot group (fastest), blockIdx.y = tile slot
     pl.gridf = dim3((P.B + pl.Gf - 1) / pl.Gf, ntiles);
     pl.gridr = dim3((P.B + pl.Gr - 1) / pl.Gr, ntiles);
@@ -1421,6 +1425,15 @@ void sizes(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, int64_t* 
     *ws = std::max(cf.off, cr.off);
 }
 
+void schedule_of(const sweep_acoustic_desc* d, sweep_b200_schedule* out)
+{
+    const Plan pl = make_plan(d);
+    out->shots_fwd = pl.Gf;
+    out->shots_rev = pl.Gr;
+    out->z_chunks = 0;
+    out->graph_steps = pl.graph_steps;
+}
+
 int64_t forward_only_bytes(const sweep_acoustic_desc* d)
 {
     Plan pl = make_plan(d);
@@ -1457,8 +1470,10 @@ static FwdMaps fwd_maps(const FwdWork& w, const Params& P)
 // is the strip slot step `it` writes (null: none), `record` may be null.
 template <class StripsOf>
 static void forward_steps(const Plan& pl, const FwdMaps& maps, const FwdWork& w, float* record, FwdState& S,
-                          int it0, int it1, StripsOf strips_of, cudaStream_t st, HostRing* hr = nullptr)
+                          int it0, int it1, StripsOf strips_of, cudaStream_t st, HostRing* hr = nullptr,
+                          bool graphs = true)
 {
+    StepGraphs gs(st, (hr || !graphs) ? 0 : pl.graph_steps);
     Params PF = pl.P;
     PF.G = pl.Gf;
     FwdPtrs F{};
@@ -1473,16 +1488,19 @@ static void forward_steps(const Plan& pl, const FwdMaps& maps, const FwdWork& w,
         if (slot && hr) hr->before_write(it);
         F.strips = (slot && scaled) ? static_cast<void*>(w.scratch) : slot;
         F.sbf16 = PF.st.fmt == SF_BF16;
-        fwd_kernel<<<pl.gridf, NTH, fwd_smem(), st>>>(maps, PF, F, it);
+        const cudaStream_t ls = gs.stream();
+        fwd_kernel<<<pl.gridf, NTH, fwd_smem(), ls>>>(maps, PF, F, it);
         SWEEP_LAUNCH_CHECK();
         if (slot && scaled) {
-            quantize_strips<<<qblocks, kQB, 0, st>>>(PF, w.scratch, slot);
+            quantize_strips<<<qblocks, kQB, 0, ls>>>(PF, w.scratch, slot);
             SWEEP_LAUNCH_CHECK();
         }
         if (slot && hr) hr->after_write(it);
+        gs.step_done();
         const int t = S.ip; S.ip = S.in; S.in = S.ix; S.ix = t;
         std::swap(S.px, S.pxn); std::swap(S.pz, S.pzn);
     }
+    gs.flush();
 }
 
 static void copy_dd(float* dst, const float* src, long long n, cudaStream_t st)
@@ -1518,6 +1536,9 @@ void forward_with(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, fl
     const FwdMaps maps = fwd_maps(w, P);
     FwdState S;
     S.px = w.psix; S.pz = w.psiz; S.pxn = w.psixn; S.pzn = w.psizn;
+    // a caller-staged call (the allocation-free entry) issues plain launches:
+    // instantiating a graph allocates
+    const bool graphs = stage == nullptr;
     if (ckpt_every <= 0 && tape && pl.host_tape) {
         HostRing hr;
         hr.open(w.ring, tape, P.st.step, st);
@@ -1528,7 +1549,7 @@ void forward_with(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, fl
         copy_any(last + n, w.u[S.in], n * 4, st);
     } else if (ckpt_every <= 0) {
         forward_steps(pl, maps, w, record, S, 0, d->nt,
-                      [&](int it) { return tape ? tape_slot(tape, pl, it) : nullptr; }, st);
+                      [&](int it) { return tape ? tape_slot(tape, pl, it) : nullptr; }, st, nullptr, graphs);
         if (tape) {
             float* last = tape_last(tape, pl);
             // (U[nt-1], U[nt]) per shot, pitched
@@ -1548,7 +1569,7 @@ void forward_with(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, fl
                           [&](int it) {
                               return (tape && it == it1 - 1 && ch + 1 < C) ? ckpt_strips(tape, pl, ch + 1) : nullptr;
                           },
-                          st);
+                          st, nullptr, graphs);
         }
     }
     check_err(w.c, st, "forward");
@@ -1624,6 +1645,7 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     HostRing hr;
     const bool host = pl.host_tape && !ckpt;
     auto reverse = [&](int it0, int it1, auto strips_of) {
+        StepGraphs gs(st, host ? 0 : pl.graph_steps);
         int rp = 0, rn = 1, rx = 2;
         for (int it = it1 - 1; it >= it0; --it) {
             const int do_recon = it > 0 ? 1 : 0;
@@ -1634,16 +1656,18 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
             R.rprev = rp; R.rnow = rn; R.r_next = w.r[rx];
             R.strips = do_recon ? strips_of(it - 1) : nullptr;
             if (host && do_recon) hr.before_read(it - 1);
-            rev_kernel<<<pl.gridr, NTH, rev_smem(), st>>>(maps, P, R, it, do_recon);
+            rev_kernel<<<pl.gridr, NTH, rev_smem(), gs.stream()>>>(maps, P, R, it, do_recon);
             SWEEP_LAUNCH_CHECK();
             if (host && do_recon) {
                 hr.after_read(it - 1);
                 if (it - 1 - HostRing::R >= 0) hr.fetch(it - 1 - HostRing::R, true);
             }
+            gs.step_done();
             int t = lp; lp = ln; ln = lx; lx = t;
             cur = 1 - cur;
             if (do_recon) { t = rp; rp = rn; rn = rx; rx = t; }
         }
+        gs.flush();
     };
     if (!ckpt) {
         const float* last = tape_last(const_cast<void*>(tape), pl);

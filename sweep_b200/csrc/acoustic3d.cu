@@ -55,6 +55,7 @@ struct Params {
     int P;                                     // x pitch (floats)
     long long SP, S;                           // plane stride, shot stride
     int zc, nzc;                               // z chunk length, chunks
+    int graph_steps;                           // host only: time steps per captured CUDA graph
     float dt, dz, dy, dx;
     float lc[M + 1], gc[M + 1];
     int z0, z1, y0, y1, x0, x1;                // physical box
@@ -945,9 +946,12 @@ static Params make_params(const sweep_acoustic_desc* d)
     // z chunks: enough CTAs for two waves at 4 CTAs per SM (the stencil
     // kernels are capped at 64 registers for that occupancy), chunks of at
     // least 16 planes
+    // (or the shape's recorded schedule value)
     const long long cols = (long long)((d->nx + BXC - 1) / BXC) * ((d->ny + BYC - 1) / BYC) * d->B;
-    int nzc = (int)std::max(1LL, (2LL * 4 * 148 + cols - 1) / cols);
+    const sweep_b200_schedule sc = recorded_schedule(d);
+    int nzc = sc.z_chunks >= 1 ? sc.z_chunks : (int)std::max(1LL, (2LL * 4 * 148 + cols - 1) / cols);
     nzc = std::max(1, std::min(nzc, d->nz / 16));
+    P.graph_steps = resolve_graph_steps(sc.graph_steps);
     P.zc = (d->nz + nzc - 1) / nzc;
     P.nzc = (d->nz + P.zc - 1) / P.zc;
     return P;
@@ -1087,6 +1091,15 @@ static float* ckpt_field(void* tape, const Params& P, int c, int f)
 
 static float* ckpt_strips(void* tape, const Params& P, int c) { return ckpt_field(tape, P, c, kStateFields); }
 
+void schedule_of(const sweep_acoustic_desc* d, sweep_b200_schedule* out)
+{
+    const Params P = make_params(d);
+    out->shots_fwd = 0;
+    out->shots_rev = 0;
+    out->z_chunks = P.nzc;
+    out->graph_steps = P.graph_steps;
+}
+
 void sizes(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, int64_t* ws, int64_t* tape)
 {
     const int base_mode = mem_mode & ~SWEEP_MEM_HOST_TAPE;
@@ -1157,26 +1170,30 @@ static void forward_steps(const sweep_acoustic_desc* d, const Params& P, FwdStat
         maps.uc[k] = plane_map(S.f[k], P, P.B, false);
     }
     maps.cf = plane_map(P.cf, P, 0, false);
+    StepGraphs sg(st, hr ? 0 : P.graph_steps);
     for (int it = it0; it < it1; ++it) {
         F3 F{S.f[S.in], S.f[S.ip], S.f[S.ix], S.ps[0], S.ps[1], S.ps[2], S.psn[0], S.psn[1], S.psn[2],
              S.zeta(0), S.zeta(1), S.zeta(2)};
-        f3_step<<<grid, block, sizeof(F3Smem), st>>>(maps, P, F, S.in, S.ip, err);
+        const cudaStream_t ls = sg.stream();
+        f3_step<<<grid, block, sizeof(F3Smem), ls>>>(maps, P, F, S.in, S.ip, err);
         SWEEP_LAUNCH_CHECK();
         void* slot = strips_of(it);
         if (slot && P.nstrip > 0) {
             if (hr) hr->before_write(it);
-            strips3<<<gst, 256, 0, st>>>(P, S.f[S.in], slot, scratch, 0);
-            if (scaled) quantize_strips3<<<(unsigned)(P.B * qper), kQB, 0, st>>>(P, scratch, slot);
+            strips3<<<gst, 256, 0, ls>>>(P, S.f[S.in], slot, scratch, 0);
+            if (scaled) quantize_strips3<<<(unsigned)(P.B * qper), kQB, 0, ls>>>(P, scratch, slot);
             if (hr) hr->after_write(it);
         }
         if (d->nsrc > 0)
-            inject3<<<gs, 128, 0, st>>>(P, S.f[S.ix], d->wavelet, d->src_loc, d->nsrc, it, 0, 1.f, 0);
+            inject3<<<gs, 128, 0, ls>>>(P, S.f[S.ix], d->wavelet, d->src_loc, d->nsrc, it, 0, 1.f, 0);
         if (d->nrec > 0 && record)
-            gather3<<<gr, 128, 0, st>>>(P, S.f[S.ix], record, d->rec_loc, d->nrec, it, 1);
+            gather3<<<gr, 128, 0, ls>>>(P, S.f[S.ix], record, d->rec_loc, d->nrec, it, 1);
         SWEEP_LAUNCH_CHECK();
+        sg.step_done();
         const int t = S.ip; S.ip = S.in; S.in = S.ix; S.ix = t;
         for (int a = 0; a < 3; ++a) std::swap(S.ps[a], S.psn[a]);
     }
+    sg.flush();
 }
 
 static void state_fields(const FwdState& S, float* out[kStateFields])
@@ -1307,45 +1324,49 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     HostRing hr;
     const bool host = P.st.host && !ckpt;
     auto reverse = [&](int it0, int it1, auto strips_of) {
+        StepGraphs sg(st, host ? 0 : P.graph_steps);
         int rp = 15, rn = 16, rx = 17;
         for (int it = it1 - 1; it >= it0; --it) {
+            const cudaStream_t ls = sg.stream();
             float* a_in[6];
             float* a_out[6];
             for (int k = 0; k < 6; ++k) { a_in[k] = w.f[3 + 2 * k + cur]; a_out[k] = w.f[3 + 2 * k + 1 - cur]; }
             A3 A{w.f[ln], w.f[lp], w.f[lx], a_in[0], a_in[1], a_in[2], a_in[3], a_in[4], a_in[5],
                  a_out[0], a_out[1], a_out[2], a_out[3], a_out[4], a_out[5]};
-            a3_step<<<grid, block, sizeof(A3Smem), st>>>(amaps, P, A, ln, lp, w.err);
+            a3_step<<<grid, block, sizeof(A3Smem), ls>>>(amaps, P, A, ln, lp, w.err);
             SWEEP_LAUNCH_CHECK();
             if (d->nrec > 0)
-                inject3<<<gr, 128, 0, st>>>(P, w.f[lx], adj, d->rec_loc, d->nrec, it, 1, 1.f, 0);
+                inject3<<<gr, 128, 0, ls>>>(P, w.f[lx], adj, d->rec_loc, d->nrec, it, 1, 1.f, 0);
             int t = lp; lp = ln; ln = lx; lx = t;
             cur = 1 - cur;
             if (grad_w && d->nsrc > 0)
-                gather3<<<gs, 128, 0, st>>>(P, w.f[ln], grad_w, d->src_loc, d->nsrc, it, 0);
+                gather3<<<gs, 128, 0, ls>>>(P, w.f[ln], grad_w, d->src_loc, d->nsrc, it, 0);
             if (it > 0) {
                 R3 R{w.f[rn], w.f[rp], w.f[rx], w.f[ln], gacc, gcomp, is, ir};
-                r3_recon<<<grid, block, sizeof(R3Smem), st>>>(rmaps, P, R, rn - 15, rp - 15, ln, w.err);
+                r3_recon<<<grid, block, sizeof(R3Smem), ls>>>(rmaps, P, R, rn - 15, rp - 15, ln, w.err);
                 if (P.nstrip > 0) {
                     if (host) hr.before_read(it - 1);
-                    strips3<<<gst, 256, 0, st>>>(P, w.f[rx], strips_of(it - 1), nullptr, 1);
+                    strips3<<<gst, 256, 0, ls>>>(P, w.f[rx], strips_of(it - 1), nullptr, 1);
                     if (host) {
                         hr.after_read(it - 1);
                         if (it - 1 - HostRing::R >= 0) hr.fetch(it - 1 - HostRing::R, true);
                     }
                     if (d->nsrc > 0)
-                        inject3<<<gs, 128, 0, st>>>(P, w.f[rx], d->wavelet, d->src_loc, d->nsrc, it, 0, -1.f, 1);
+                        inject3<<<gs, 128, 0, ls>>>(P, w.f[rx], d->wavelet, d->src_loc, d->nsrc, it, 0, -1.f, 1);
                     Img I{w.f[rp], w.f[rn], w.f[rx], w.f[ln], gacc, gcomp, is, ir};
-                    strip_image3<<<gst, 256, 0, st>>>(P, I);
+                    strip_image3<<<gst, 256, 0, ls>>>(P, I);
                 }
                 if (d->nsrc > 0)
-                    inject3<<<gs, 128, 0, st>>>(P, w.f[rx], d->wavelet, d->src_loc, d->nsrc, it, 0, 1.f, 0);
+                    inject3<<<gs, 128, 0, ls>>>(P, w.f[rx], d->wavelet, d->src_loc, d->nsrc, it, 0, 1.f, 0);
                 SWEEP_LAUNCH_CHECK();
                 t = rp; rp = rn; rn = rx; rx = t;
             } else if (illum) {
-                illum_tail3<<<592, 256, 0, st>>>(P, w.f[ln], ir);
+                illum_tail3<<<592, 256, 0, ls>>>(P, w.f[ln], ir);
                 SWEEP_LAUNCH_CHECK();
             }
+            sg.step_done();
         }
+        sg.flush();
     };
     if (!ckpt) {
         const float* last = tape_last(const_cast<void*>(tape), P);

@@ -157,6 +157,84 @@ struct HostRing {
     }
 };
 
+// Per-shape launch schedule (sweep_b200_schedule): the recorded one, or all
+// built-in (zeros, graph_steps -1).  Thread-safe; defined in schedule.cu.
+sweep_b200_schedule recorded_schedule(const sweep_acoustic_desc* d);
+sweep_b200_schedule recorded_schedule(const sweep_elastic_desc* d);
+
+// Time steps per captured graph when neither the schedule nor the
+// environment (SWEEP_B200_GRAPH_STEPS) sets it.
+constexpr int kGraphStepsDefault = 64;
+int resolve_graph_steps(int recorded);
+
+// A run of time steps issued as CUDA graphs of up to `steps` steps each.  The
+// launches of a chunk are captured on a private non-blocking stream (capture
+// runs nothing), the graph is instantiated and launched on the caller's
+// stream, and the next chunk is captured while the previous one runs on the
+// GPU.  The captured launches are the stream path's launches in the same
+// order, so results are identical.  steps <= 0: every launch goes straight to
+// the caller's stream.  Use: take stream() for each step's launches, call
+// step_done() after them, and flush() once after the loop, before anything
+// else is queued on the caller's stream.
+class StepGraphs {
+public:
+    StepGraphs(cudaStream_t st, int steps) : st_(st), steps_(steps)
+    {
+        if (steps_ > 0) SWEEP_CUDA(cudaStreamCreateWithFlags(&cs_, cudaStreamNonBlocking));
+    }
+    StepGraphs(const StepGraphs&) = delete;
+    StepGraphs& operator=(const StepGraphs&) = delete;
+    ~StepGraphs()
+    {
+        abort_capture();
+        if (cs_) cudaStreamDestroy(cs_);
+    }
+    cudaStream_t stream()
+    {
+        if (steps_ <= 0) return st_;
+        if (!capturing_) {
+            SWEEP_CUDA(cudaStreamBeginCapture(cs_, cudaStreamCaptureModeThreadLocal));
+            capturing_ = true;
+        }
+        return cs_;
+    }
+    void step_done()
+    {
+        if (capturing_ && ++n_ >= steps_) flush();
+    }
+    void flush()
+    {
+        if (!capturing_) return;
+        capturing_ = false;
+        n_ = 0;
+        cudaGraph_t g = nullptr;
+        SWEEP_CUDA(cudaStreamEndCapture(cs_, &g));
+        cudaGraphExec_t ge = nullptr;
+        const cudaError_t ei = cudaGraphInstantiate(&ge, g, 0);
+        cudaGraphDestroy(g);
+        SWEEP_CUDA(ei);
+        const cudaError_t el = cudaGraphLaunch(ge, st_);
+        cudaGraphExecDestroy(ge);    // an executable graph in flight is freed when it completes
+        SWEEP_CUDA(el);
+        ++launched_;
+    }
+    int graphs_launched() const { return launched_; }
+
+private:
+    void abort_capture()
+    {
+        if (!capturing_) return;
+        capturing_ = false;
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(cs_, &g);
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+    }
+    cudaStream_t st_, cs_ = nullptr;
+    int steps_, n_ = 0, launched_ = 0;
+    bool capturing_ = false;
+};
+
 // Source / receiver events grouped by (shot, tile): a CSR table so that the
 // CTA owning a tile finds its point sources and receivers without scanning the
 // whole list.  `cell` is the tile-local linear cell index, `id` the global

@@ -1074,6 +1074,7 @@ struct Plan {
     Geo G;
     int nm;          // model copies
     int gshots;      // shots per rev_str CTA
+    int graph_steps; // time steps per captured CUDA graph (0: stream launches)
     int nslot;       // gradient slots
     bool host_tape;  // boundary-saving tape in pinned host memory (SWEEP_MEM_HOST_TAPE)
 };
@@ -1129,12 +1130,18 @@ static Plan make_plan(const sweep_elastic_desc* d)
     G.ms = per_shot ? G.S : 0;
     G.wavelet = d->wavelet;
     pl.nm = per_shot ? d->B : 1;
-    pl.gshots = per_shot ? 1 : std::min(env_int("SWEEP_B200_EL_SHOTS_PER_CTA", 4), d->B);
-    // forward: shots per CTA, keeping at least two waves of CTAs
+    // shots per CTA: the shape's recorded schedule value if any, else the
+    // environment, else the measured default (the forward's capped to keep at
+    // least two waves of CTAs)
+    const sweep_b200_schedule sc = recorded_schedule(d);
+    pl.gshots = per_shot ? 1
+                         : std::min(sc.shots_rev >= 1 ? sc.shots_rev : env_int("SWEEP_B200_EL_SHOTS_PER_CTA", 4), d->B);
     const long long ntl = (long long)G.ntx * G.ntz;
     int gf = per_shot ? 1 : std::min(env_int("SWEEP_B200_EL_SHOTS_PER_CTA_FWD", 4), d->B);
     while (gf > 1 && ntl * ((d->B + gf - 1) / gf) < 2LL * 148 * 4) --gf;
+    if (!per_shot && sc.shots_fwd >= 1) gf = std::min(sc.shots_fwd, d->B);
     G.gf = gf;
+    pl.graph_steps = resolve_graph_steps(sc.graph_steps);
     pl.nslot = (d->B + pl.gshots - 1) / pl.gshots;
     return pl;
 }
@@ -1451,6 +1458,15 @@ static void check_mode(int mem_mode, int ckpt_every)
                   "elastic2d: checkpoint interval must be >= 1 (got %d)", ckpt_every);
 }
 
+void schedule_of(const sweep_elastic_desc* d, sweep_b200_schedule* out)
+{
+    const Plan pl = make_plan(d);
+    out->shots_fwd = pl.G.gf;
+    out->shots_rev = pl.gshots;
+    out->z_chunks = 0;
+    out->graph_steps = pl.graph_steps;
+}
+
 void sizes(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, int64_t* ws, int64_t* tape)
 {
     check_mode(mem_mode, ckpt_every);
@@ -1475,8 +1491,9 @@ void sizes(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, int64_t* w
 // the strip slot of step it (null: none).
 template <class StripsOf>
 static void forward_steps(FwdArgs& A, int it0, int it1, StripsOf strips_of, float* scratch, cudaStream_t st,
-                          HostRing* hr = nullptr)
+                          int graph_steps, HostRing* hr = nullptr)
 {
+    StepGraphs gs(st, hr ? 0 : graph_steps);
     const Geo& G = A.G;
     set_attrs();
     const FwdMaps maps = fwd_maps(A.f, G);
@@ -1487,13 +1504,16 @@ static void forward_steps(FwdArgs& A, int it0, int it1, StripsOf strips_of, floa
         A.it = it;
         void* slot = strips_of(it);
         A.strips = (slot && scaled) ? static_cast<void*>(scratch) : slot;
-        fwd_vel<<<grid, block, SM_FWD_VEL, st>>>(maps, A);
+        const cudaStream_t ls = gs.stream();
+        fwd_vel<<<grid, block, SM_FWD_VEL, ls>>>(maps, A);
         if (slot && hr) hr->before_write(it);
-        fwd_str<<<grid, block, SM_FWD_STR, st>>>(maps, A);
-        if (slot && scaled) quantize_strips<<<qblocks, kQB, 0, st>>>(G, scratch, slot);
+        fwd_str<<<grid, block, SM_FWD_STR, ls>>>(maps, A);
+        if (slot && scaled) quantize_strips<<<qblocks, kQB, 0, ls>>>(G, scratch, slot);
         if (slot && hr) hr->after_write(it);
+        SWEEP_LAUNCH_CHECK();
+        gs.step_done();
     }
-    SWEEP_LAUNCH_CHECK();
+    gs.flush();
 }
 
 void forward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, float* record, void* tape,
@@ -1526,7 +1546,7 @@ void forward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, float* r
         if (host) hr.open(w.ring, tape, G.st.step, st);
         forward_steps(A, 0, G.nt,
                       [&](int it) { return !tape ? nullptr : host ? hr.slot(it) : tape_slot(tape, pl, it); },
-                      w.scratch, st, host ? &hr : nullptr);
+                      w.scratch, st, pl.graph_steps, host ? &hr : nullptr);
         if (host) hr.close();
         if (tape) {
             float* last = tape_last(tape, pl);
@@ -1548,7 +1568,7 @@ void forward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, float* r
         // the last step of a chunk keeps its strips with the next checkpoint
         forward_steps(A, it0, it1,
                       [&](int it) { return (tape && it == it1 - 1 && ch + 1 < C) ? ckpt_at(tape, pl, ch + 1).strips : nullptr; },
-                      nullptr, st);
+                      nullptr, st, pl.graph_steps);
     }
     check_err(w.cm, st, "forward");
 }
@@ -1590,22 +1610,26 @@ void backward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, const f
     HostRing hr;
     const bool host = pl.host_tape && !ckpt;
     auto reverse = [&](int it0, int it1, auto strips_of) {
+        StepGraphs gs(st, host ? 0 : pl.graph_steps);
         for (int it = it1 - 1; it >= std::max(it0, 1); --it) {
             A.it = it;
             A.strips = strips_of(it - 1);
             A.mo = w.m[cur];
             A.mn = w.m[cur ^ 1];
             if (host) hr.before_read(it - 1);
-            rev_str<<<grid_s, block, SM_REV_STR, st>>>(A);
-            rev_sadj<<<grid_b, block, SM_REV_SADJ, st>>>(A);
-            rev_vadj<<<grid_b, block, SM_REV_VADJ, st>>>(A);
+            const cudaStream_t ls = gs.stream();
+            rev_str<<<grid_s, block, SM_REV_STR, ls>>>(A);
+            rev_sadj<<<grid_b, block, SM_REV_SADJ, ls>>>(A);
+            rev_vadj<<<grid_b, block, SM_REV_VADJ, ls>>>(A);
             if (host) {
                 hr.after_read(it - 1);
                 if (it - 1 - HostRing::R >= 0) hr.fetch(it - 1 - HostRing::R, true);
             }
+            SWEEP_LAUNCH_CHECK();
+            gs.step_done();
             cur ^= 1;
         }
-        SWEEP_LAUNCH_CHECK();
+        gs.flush();
     };
     if (!ckpt) {
         const float* last = tape_last(const_cast<void*>(tape), pl);
@@ -1645,7 +1669,8 @@ void backward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, const f
                 SWEEP_CUDA(cudaMemcpyAsync(w.chunk, cp.strips, sizeof(float) * cs, cudaMemcpyDeviceToDevice, st));
             }
             // replay: chunk slot j holds the strips after step it0 - 1 + j
-            forward_steps(F, it0, it1, [&](int it) { return w.chunk + (long long)(it - it0 + 1) * cs; }, nullptr, st);
+            forward_steps(F, it0, it1, [&](int it) { return w.chunk + (long long)(it - it0 + 1) * cs; }, nullptr, st,
+                          pl.graph_steps);
             reverse(it0, it1, [&](int t) { return (const float*)w.chunk + (long long)(t - (it0 - 1)) * cs; });
         }
     }

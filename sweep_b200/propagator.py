@@ -328,11 +328,19 @@ class PropTorch(torch.nn.Module):
     (scalar or per axis in shape order), ``dt``, ``abcn`` (PML cells per face,
     default 50), ``memory`` (``BoundarySaving()`` default, ``Full()``,
     ``Ckpt(chunks)``), ``device``/``dev``, ``source_type`` /
-    ``receiver_type`` (field names; elastic only)."""
+    ``receiver_type`` (field names; elastic only).
+
+    Launch schedule (no counterpart in the reference, whose launch shapes are
+    fixed): ``autotune=True`` times candidate schedules on the first call of
+    each problem shape (``sweep_b200.autotune.tune``) and records the fastest
+    for every later call of that shape; ``schedule={...}`` records the given
+    fields instead (``shots_fwd``, ``shots_rev``, ``z_chunks``,
+    ``graph_steps``).  ``tune_report`` holds the tuner's last report."""
 
     def __init__(self, equation, shape, dh=10.0, dt=0.002, abcn=50, impl="c", memory=None,
                  device=None, dev=None, source_type=None, receiver_type=None,
-                 use_ckpt=None, ckpt_chunks=100, free_surface=False, **kwargs):
+                 use_ckpt=None, ckpt_chunks=100, free_surface=False, autotune=False, schedule=None,
+                 **kwargs):
         super().__init__()
         if impl not in (None, "c", "auto"):
             raise NotImplementedError(f"sweep_b200 implements impl='c' only (got impl={impl!r})")
@@ -377,6 +385,9 @@ class PropTorch(torch.nn.Module):
         self.source_illumination = None
         self.receiver_illumination = None
         self._ws = None
+        self.autotune = bool(autotune)
+        self.schedule = dict(schedule) if schedule is not None else None
+        self.tune_report = None
 
     # ---------------------------------------------------------------- helpers
     def _workspace(self, nbytes, device):
@@ -444,6 +455,35 @@ class PropTorch(torch.nn.Module):
             mode |= _lib.MEM_HOST_TAPE
         return mode, 0
 
+    def _desc(self, geo, padded, wb, fields):
+        wb = wb.contiguous()
+        if fields is not None:
+            return geo.elastic_desc([m.contiguous() for m in padded], wb, *fields)
+        return geo.acoustic_desc(padded[0].contiguous(), wb)
+
+    def _apply_schedule(self, geo, padded, wb, fields, mem_mode, ckpt_every):
+        from . import autotune
+        desc = self._desc(geo, padded, wb, fields)
+        if self.schedule is not None:
+            autotune.set_schedule(desc, self.schedule)
+        elif not autotune.tuned(desc):
+            self.tune_report = autotune.tune(self, geo, padded, wb, fields, mem_mode, ckpt_every)
+
+    def launch_schedule(self, wavelet_len, sources, receivers, models):
+        """The schedule (resolved fields) a call with these inputs would run."""
+        from . import autotune
+        nd = self.equation.NDIM
+        src = np.asarray(sources.detach().cpu() if isinstance(sources, torch.Tensor) else sources, np.int64)
+        rec = np.asarray(receivers.detach().cpu() if isinstance(receivers, torch.Tensor) else receivers, np.int64)
+        B = src.shape[0]
+        src = src.reshape(B, -1, nd) + self._shift()
+        rec = rec.reshape(B, -1, nd) + self._shift()
+        geo = _Geometry(self, B, src.shape[1], rec.shape[1], int(wavelet_len), src, rec, self.device, 4500.0, 25.0)
+        padded = [self._pad_model(m.to(self.device)) for m in models]
+        wb = torch.zeros((B, src.shape[1], int(wavelet_len)), dtype=torch.float32, device=self.device)
+        fields = self._elastic_fields() if isinstance(self.equation, Elastic) else None
+        return autotune.get_schedule(self._desc(geo, padded, wb, fields))
+
     # ---------------------------------------------------------------- forward
     def forward(self, wavelet, sources, receivers, models=None, max_vel=4500.0, pml_freq=25.0):
         eq = self.equation
@@ -481,6 +521,9 @@ class PropTorch(torch.nn.Module):
         geo = _Geometry(self, B, nsrc, nrec, nt, src, rec, dev, max_vel, pml_freq)
         mem_mode, ckpt_every = self._mem_mode()
         padded = [self._pad_model(m.to(dev)) for m in models]
+        fields = self._elastic_fields() if isinstance(eq, Elastic) else None
+        if self.autotune or self.schedule is not None:
+            self._apply_schedule(geo, padded, wb, fields, mem_mode, ckpt_every)
         if isinstance(eq, (Acoustic, Acoustic3D)):
             return _AcousticFn.apply(padded[0], wb, self, geo, mem_mode, ckpt_every)
         if isinstance(eq, Elastic):
@@ -490,6 +533,5 @@ class PropTorch(torch.nn.Module):
                 raise NotImplementedError(
                     "impl='c' Elastic does not return the wavelet gradient (its compiled backward "
                     "returns the model gradients only). Detach the wavelet.")
-            fields = self._elastic_fields()
             return _ElasticFn.apply(*padded, wb, self, geo, fields, mem_mode, ckpt_every)
         raise NotImplementedError(f"{type(eq).__name__} is not built")

@@ -200,3 +200,45 @@ def test_free_surface_spellings():
     assert free_faces([1, 0, 0, 1], 2) == (True, False, False, True)
     with pytest.raises(ValueError, match="unknown"):
         free_faces(["front"], 2)
+
+
+def test_schedule_table_is_host_only_and_keyed_by_shape():
+    """The per-shape schedule table: recorded fields win, the rest resolve to
+    the built-in choice; nt, sources and receivers are not part of the key;
+    out-of-range values are refused with a message."""
+    from sweep_b200 import _lib, autotune
+    autotune.clear_schedules()
+    try:
+        d = _desc(B=8, nz=120, nx=200)
+        base = autotune.get_schedule(d)
+        assert base["shots_fwd"] >= 1 and base["shots_rev"] >= 1 and base["graph_steps"] >= 0
+        autotune.set_schedule(d, {"shots_rev": 4, "graph_steps": 0})
+        got = autotune.get_schedule(d)
+        assert got["shots_rev"] == 4 and got["graph_steps"] == 0 and got["shots_fwd"] == base["shots_fwd"]
+        d.nt, d.nrec = 999, 7                   # same shape: same schedule
+        assert autotune.get_schedule(d) == got
+        other = _desc(B=4, nz=120, nx=200)      # another shot count: another shape
+        assert autotune.get_schedule(other)["graph_steps"] == base["graph_steps"]
+        d.vp_stride = 120 * 200                 # per-shot models always run one shot per CTA
+        assert autotune.get_schedule(d)["shots_rev"] == 1
+        with pytest.raises(RuntimeError, match="shots_fwd"):
+            autotune.set_schedule(d, {"shots_fwd": 17})
+        with pytest.raises(ValueError, match="unknown schedule"):
+            autotune.set_schedule(d, {"tile": 3})
+        d3 = _desc(B=2, nz=64, nx=64)
+        d3.ndim, d3.ny = 3, 64
+        for i in range(6):
+            d3.pad[i] = 5
+        autotune.set_schedule(d3, {"z_chunks": 2})
+        assert autotune.get_schedule(d3)["z_chunks"] == 2
+        e = _lib.ElasticDesc()
+        e.B, e.nz, e.nx, e.nt, e.M = 6, 80, 90, 10, 4
+        for i in range(4):
+            e.pad[i] = 10
+        e.nsrc_fields, e.src_fields[0], e.nrec_fields = 1, 2, 1
+        autotune.set_schedule(e, {"shots_fwd": 3, "shots_rev": 2})
+        s = autotune.get_schedule(e)
+        assert (s["shots_fwd"], s["shots_rev"]) == (3, 2)
+    finally:
+        autotune.clear_schedules()
+    assert autotune.get_schedule(_desc(B=8, nz=120, nx=200)) == base
