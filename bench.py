@@ -337,6 +337,9 @@ class ElasticWorkload:
 # strips) is ~63 GB.
 A3_N, A3_NT, A3_DT, A3_DH, A3_ABCN = 256, 2000, 0.001, 10.0, 24
 A3_NSHOT, A3_BATCH, A3_F0, A3_DELAY = 16, 4, 10.0, 0.12
+# boundary storage budget of one call: a shot group whose boundary-saving tape
+# exceeds it checkpoints every 100 steps instead
+A3_BUDGET_GB, A3_CKPT = 60.0, 100
 A3_RT = (A3_N + 2 * A3_ABCN + 2 * M,) * 3
 
 
@@ -381,6 +384,7 @@ class Acoustic3DWorkload:
     traffic = {"bytes_per_shot": 881e6 + 873e6,
                "source": "ncu, a3_step + r3_recon of one 256^3 shot, x shots per step"}
     batch = A3_BATCH
+    budget_gb = A3_BUDGET_GB
 
     def config(self, args):
         return {"workload": f"acoustic3d {A3_N}^3 (runtime {A3_RT[0]}^3), {A3_NSHOT} shots in calls of "
@@ -392,13 +396,19 @@ class Acoustic3DWorkload:
                 "physical_fraction": (A3_N / A3_RT[0]) ** 3,
                 "l2": "working set per step > L2 (inputs larger than L2; no flush)",
                 "boundary_tape": f"{STRIPS[1]} strips in {STRIPS[0]} memory",
+                "memory_rule": f"boundary saving when a call's tape fits {A3_BUDGET_GB:g} GB, else checkpoints "
+                               f"every {A3_CKPT} steps; shots per call: the most whose boundary tape fits "
+                               f"(at most {A3_BATCH}) unless --shots-per-call is given",
                 "parallelism": f"shots: {A3_NSHOT} per GPU x {args.gpus} GPU(s)"}
 
     def build(self, dev):
         from sweep_b200 import Acoustic3D, PropTorch
         m_true, m_init, w, src, rec = acoustic3d_survey()
+        from sweep_b200 import BoundarySaving
         solver = PropTorch(Acoustic3D(spatial_order=ORDER, device=dev), shape=(A3_N,) * 3, dh=A3_DH,
-                           dt=A3_DT, abcn=A3_ABCN, device=dev, memory=boundary_memory())
+                           dt=A3_DT, abcn=A3_ABCN, device=dev,
+                           memory=BoundarySaving(storage=STRIPS[0], storage_dtype=STRIPS[1],
+                                                 budget_gb=A3_BUDGET_GB, ckpt_chunks=A3_CKPT))
         return solver, m_true, m_init, w, src, rec
 
     def launches(self):
@@ -477,12 +487,16 @@ def run_gpu(args, wl):
     solver, m_true, m_init, w, src, rec = wl.build(dev)
     solver.autotune = bool(args.autotune)
     src, rec = src[:wl.nshot], rec[:wl.nshot]
+    if getattr(wl, "budget_gb", None) and not args.shots_per_call:
+        # shot groups: the most shots whose boundary-saving tape fits the budget
+        per_shot = solver.tape_bytes(len(w), src[:1], rec[:1], [torch.tensor(m, device=dev) for m in m_init])
+        wl.batch = max(1, min(wl.batch, wl.nshot, int(wl.budget_gb * 1e9 // per_shot)))
     w_d = torch.tensor(w, device=dev)
     bsz = getattr(wl, "batch", wl.nshot)
     batches = [slice(b, min(b + bsz, wl.nshot)) for b in range(0, wl.nshot, bsz)]
     with torch.no_grad():
         mt = [torch.tensor(m, device=dev) for m in m_true]
-        # with --autotune the first call of the shape tunes its schedule (untimed)
+        # the first call of the shape tunes its schedule (untimed; --no-autotune skips it)
         obs = torch.cat([solver(w_d, src[sl], rec[sl], models=mt) for sl in batches])
         del mt
     ms_d = [torch.tensor(m, device=dev) for m in m_init]
@@ -586,7 +600,7 @@ def run_gpu(args, wl):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded layered model, see config)",
-        "config": dict(wl.config(args), schedule=schedule,
+        "config": dict(wl.config(args), schedule=schedule, memory=solver.last_memory,
                        autotune=None if solver.tune_report is None else
                        {"seconds": solver.tune_report["seconds"], "nt": solver.tune_report["nt"],
                         "trials_ms": {k: {str(v): 1e3 * t for v, t in r.items()}
@@ -697,8 +711,9 @@ def main():
     ap.add_argument("--graph-steps", type=int, default=None,
                     help="time steps per captured CUDA graph in the step loops (0: plain stream launches; "
                          "default: the library's built-in choice)")
-    ap.add_argument("--autotune", action="store_true",
-                    help="tune the launch schedule of the workload's shape before timing (untimed)")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="skip the launch-schedule autotuner (by default the first call of the workload's "
+                         "shape tunes its schedule, before and outside the timed region)")
     ap.add_argument("--nt", type=int, default=None,
                     help="shorter time axis (profiling captures only; the bench line is for the full nt)")
     ap.add_argument("--shots", type=int, default=None,

@@ -83,7 +83,7 @@ def clear_schedules() -> None:
     _tuned.clear()
 
 
-def _candidates(desc, builtin: dict, mem_mode: int) -> list:
+def _candidates(desc, builtin: dict, mem_mode: int, nt_tune: int) -> list:
     """(knob, values, forward_only) in tuning order."""
     knobs = []
     if isinstance(desc, _lib.ElasticDesc):
@@ -100,11 +100,18 @@ def _candidates(desc, builtin: dict, mem_mode: int) -> list:
             knobs.append(("shots_rev", sorted({g for g in (2, 4, 8, 16) if g <= B} | {builtin["shots_rev"]}), False))
     else:
         z = builtin["z_chunks"]
-        zmax = max(1, desc.nz // 16)
-        knobs.append(("z_chunks", sorted({max(1, z // 2), z, min(zmax, 2 * z)}), False))
+        knobs.append(("z_chunks", sorted({max(1, z // 2), z, min(_zmax(desc), 2 * z)}), False))
     if not mem_mode & _lib.MEM_HOST_TAPE:
-        knobs.append(("graph_steps", sorted({0, 64, builtin["graph_steps"]}), False))
+        # a graph's capture and instantiation overlap the previous graph's run:
+        # the trial holds four graphs, so that it sees the steady state of a
+        # long time axis rather than the first graph's set-up alone
+        knobs.append(("graph_steps", [0, max(1, min(64, nt_tune // 4))], False))
     return knobs
+
+
+def _zmax(desc) -> int:
+    """Most z chunks the core takes for this grid (chunks of >= 16 planes)."""
+    return max(1, desc.nz // 16)
 
 
 def _time(run, repeats: int) -> float:
@@ -135,7 +142,7 @@ def tune(prop, geo, padded, wavelet, fields, mem_mode: int, ckpt_every: int,
     t_start = time.perf_counter()
     elastic = fields is not None
     if nt_tune is None:
-        nt_tune = 32 if elastic else (64 if geo.ndim == 2 else 8)
+        nt_tune = 128 if elastic else (256 if geo.ndim == 2 else 16)
     nt_tune = max(2, min(int(nt_tune), geo.nt))
     g = copy.copy(geo)
     g.nt = nt_tune
@@ -167,11 +174,17 @@ def tune(prop, geo, padded, wavelet, fields, mem_mode: int, ckpt_every: int,
     current = dict(builtin)
     trials = {}
     try:
-        for knob, values, forward_only in _candidates(desc, builtin, mem_mode):
+        for knob, values, forward_only in _candidates(desc, builtin, mem_mode, nt_tune):
             res = {}
+            run = fwd if forward_only else fwd_bwd
             for v in values:
                 set_schedule(desc, dict(current, **{knob: v}))
-                res[v] = _time(fwd if forward_only else fwd_bwd, repeats)
+                res[v] = _time(run, repeats)
+            # z chunks: keep doubling while the largest count tried is the fastest
+            while knob == "z_chunks" and min(res, key=res.get) == max(res) and 2 * max(res) <= _zmax(desc):
+                v = 2 * max(res)
+                set_schedule(desc, dict(current, **{knob: v}))
+                res[v] = _time(run, repeats)
             current[knob] = min(res, key=res.get)
             trials[knob] = res
     finally:

@@ -311,6 +311,9 @@ __global__ void __launch_bounds__(NTH, 4) f3_step(const __grid_constant__ F3Maps
         if (__syncthreads_or(!ok)) { fail(q); return; }
     }
     const int cidx = (ty + M) * PW + (tx + M);
+    // the x / y profile derivatives d a / d axis of this thread's column (constant along z)
+    const float dax = (col && (ix < P.ex0 || ix >= P.ex1)) ? grad_p(P.ax + ix, 1, P, P.dx) : 0.f;
+    const float day = (col && (iy < P.ey0 || iy >= P.ey1)) ? grad_p(P.ay + iy, 1, P, P.dy) : 0.f;
     for (int z = zb; z < ze; ++z) {
         {
             const bool ok = tma::mbar_wait(&sm.bar[slot(z + M)], parity(z + M), err, ERR_WAIT_F3);
@@ -337,7 +340,7 @@ __global__ void __launch_bounds__(NTH, 4) f3_step(const __grid_constant__ F3Maps
                     const float du = grad_p(p, 1, P, P.dx);
                     const float dps = grad_p(F.psx + i, 1, P, P.dx);
                     const float a = __ldg(P.ax + ix), bb = __ldg(P.bx + ix), db = __ldg(P.dbx + ix);
-                    const float da = grad_p(P.ax + ix, 1, P, P.dx);
+                    const float da = dax;
                     const float ps = F.psx[i], zt = F.zx[i];
                     const float tmp = (((1.f + bb) * lx + db * du) + a * dps) + da * ps;
                     w += (1.f + bb) * tmp + a * zt;
@@ -350,7 +353,7 @@ __global__ void __launch_bounds__(NTH, 4) f3_step(const __grid_constant__ F3Maps
                     const float du = grad_p(p, PW, P, P.dy);
                     const float dps = grad_p(F.psy + i, P.P, P, P.dy);
                     const float a = __ldg(P.ay + iy), bb = __ldg(P.by + iy), db = __ldg(P.dby + iy);
-                    const float da = grad_p(P.ay + iy, 1, P, P.dy);
+                    const float da = day;
                     const float ps = F.psy[i], zt = F.zy[i];
                     const float tmp = (((1.f + bb) * ly + db * du) + a * dps) + da * ps;
                     w += (1.f + bb) * tmp + a * zt;
@@ -943,13 +946,15 @@ static Params make_params(const sweep_acoustic_desc* d)
     P.nstrip = P.n_top + P.n_bot + bzi * P.nring;
     P.az = d->az; P.bz = d->bz; P.dbz = d->dbz; P.ay = d->ay; P.by = d->by; P.dby = d->dby;
     P.ax = d->ax; P.bx = d->bx; P.dbx = d->dbx;
-    // z chunks: enough CTAs for two waves at 4 CTAs per SM (the stencil
-    // kernels are capped at 64 registers for that occupancy), chunks of at
-    // least 16 planes
-    // (or the shape's recorded schedule value)
+    // z chunks: enough CTAs for eight waves at 4 CTAs per SM (the stencil
+    // kernels are capped at 64 registers for that occupancy; CTAs in the CPML
+    // shell take ~3x an interior CTA's time, and many short CTAs balance them
+    // across the SMs: measured on the 256^3 survey, 4-shot calls, 1 / 2 / 4
+    // chunks per column took 96.7 / 86.7 / 83.2 ms for 16 steps), chunks of
+    // at least 16 planes -- or the shape's recorded schedule value
     const long long cols = (long long)((d->nx + BXC - 1) / BXC) * ((d->ny + BYC - 1) / BYC) * d->B;
     const sweep_b200_schedule sc = recorded_schedule(d);
-    int nzc = sc.z_chunks >= 1 ? sc.z_chunks : (int)std::max(1LL, (2LL * 4 * 148 + cols - 1) / cols);
+    int nzc = sc.z_chunks >= 1 ? sc.z_chunks : (int)std::max(1LL, (8LL * 4 * 148 + cols - 1) / cols);
     nzc = std::max(1, std::min(nzc, d->nz / 16));
     P.graph_steps = resolve_graph_steps(sc.graph_steps);
     P.zc = (d->nz + nzc - 1) / nzc;

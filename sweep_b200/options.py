@@ -30,11 +30,22 @@ class BoundarySaving:
     pinned host memory: the step kernels write a small device ring and a copy
     stream moves each step's strips to the host (forward) and back ahead of
     their use (backward), so the tape no longer takes GPU memory (every
-    equation)."""
+    equation).
+
+    ``budget_gb`` (no counterpart in the reference) bounds the tape of one
+    call: a call whose boundary-saving tape would exceed it checkpoints the
+    state every ``ckpt_chunks`` steps instead (``Ckpt(chunks=ckpt_chunks)``);
+    ``PropTorch.last_memory`` reports which one the last call ran."""
     storage: str = "gpu"
     storage_dtype: str = "fp32"
+    budget_gb: float | None = None
+    ckpt_chunks: int = 100
 
     def __post_init__(self):
+        if self.budget_gb is not None and not float(self.budget_gb) > 0:
+            raise ValueError("BoundarySaving.budget_gb must be a positive number of GB (or None)")
+        if int(self.ckpt_chunks) < 1:
+            raise ValueError("BoundarySaving.ckpt_chunks must be >= 1")
         if self.storage not in ("gpu", "cpu"):
             raise NotImplementedError("sweep_b200 keeps the boundary strips in GPU memory (storage='gpu') or "
                                       "in pinned host memory (storage='cpu'); disk storage is not built")

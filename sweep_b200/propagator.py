@@ -385,6 +385,7 @@ class PropTorch(torch.nn.Module):
         self.source_illumination = None
         self.receiver_illumination = None
         self._ws = None
+        self.last_memory = None
         self.autotune = bool(autotune)
         self.schedule = dict(schedule) if schedule is not None else None
         self.tune_report = None
@@ -461,6 +462,33 @@ class PropTorch(torch.nn.Module):
             return geo.elastic_desc([m.contiguous() for m in padded], wb, *fields)
         return geo.acoustic_desc(padded[0].contiguous(), wb)
 
+    def _tape_bytes(self, desc, fields, mem_mode, ckpt_every):
+        ws_b, tape_b = _lib.c_i64(), _lib.c_i64()
+        name = "sweep_b200_elastic_sizes" if fields is not None else "sweep_b200_acoustic_sizes"
+        _lib.call(name, desc, mem_mode, ckpt_every, ws_b, tape_b)
+        return int(tape_b.value)
+
+    def _apply_budget(self, geo, padded, wb, fields, mem_mode, ckpt_every):
+        """Memory mode of this call: boundary saving while its tape fits
+        ``BoundarySaving.budget_gb``, else checkpoints every ``ckpt_chunks``
+        steps; recorded in ``last_memory``."""
+        mem = self.memory
+        budget = getattr(mem, "budget_gb", None)
+        if budget is None:
+            self.last_memory = {"mode": "checkpoint" if mem_mode == _lib.MEM_CHECKPOINT else "boundary",
+                                "chunks": ckpt_every or None}
+            return mem_mode, ckpt_every
+        desc = self._desc(geo, padded, wb, fields)
+        tape = self._tape_bytes(desc, fields, mem_mode, ckpt_every)
+        if tape <= float(budget) * 1e9:
+            self.last_memory = {"mode": "boundary", "tape_bytes": tape, "budget_bytes": float(budget) * 1e9}
+            return mem_mode, ckpt_every
+        k = int(mem.ckpt_chunks)
+        ck_tape = self._tape_bytes(desc, fields, _lib.MEM_CHECKPOINT, k)
+        self.last_memory = {"mode": "checkpoint", "chunks": k, "tape_bytes": ck_tape,
+                            "boundary_tape_bytes": tape, "budget_bytes": float(budget) * 1e9}
+        return _lib.MEM_CHECKPOINT, k
+
     def _apply_schedule(self, geo, padded, wb, fields, mem_mode, ckpt_every):
         from . import autotune
         desc = self._desc(geo, padded, wb, fields)
@@ -472,6 +500,18 @@ class PropTorch(torch.nn.Module):
     def launch_schedule(self, wavelet_len, sources, receivers, models):
         """The schedule (resolved fields) a call with these inputs would run."""
         from . import autotune
+        geo, padded, wb, fields = self._probe(wavelet_len, sources, receivers, models)
+        return autotune.get_schedule(self._desc(geo, padded, wb, fields))
+
+    def tape_bytes(self, wavelet_len, sources, receivers, models):
+        """Bytes of the tape a gradient call with these inputs keeps between
+        its forward and backward, under this solver's memory option as given
+        (before any ``budget_gb`` switch)."""
+        geo, padded, wb, fields = self._probe(wavelet_len, sources, receivers, models)
+        mem_mode, ckpt_every = self._mem_mode()
+        return self._tape_bytes(self._desc(geo, padded, wb, fields), fields, mem_mode, ckpt_every)
+
+    def _probe(self, wavelet_len, sources, receivers, models):
         nd = self.equation.NDIM
         src = np.asarray(sources.detach().cpu() if isinstance(sources, torch.Tensor) else sources, np.int64)
         rec = np.asarray(receivers.detach().cpu() if isinstance(receivers, torch.Tensor) else receivers, np.int64)
@@ -482,7 +522,7 @@ class PropTorch(torch.nn.Module):
         padded = [self._pad_model(m.to(self.device)) for m in models]
         wb = torch.zeros((B, src.shape[1], int(wavelet_len)), dtype=torch.float32, device=self.device)
         fields = self._elastic_fields() if isinstance(self.equation, Elastic) else None
-        return autotune.get_schedule(self._desc(geo, padded, wb, fields))
+        return geo, padded, wb, fields
 
     # ---------------------------------------------------------------- forward
     def forward(self, wavelet, sources, receivers, models=None, max_vel=4500.0, pml_freq=25.0):
@@ -524,6 +564,7 @@ class PropTorch(torch.nn.Module):
         fields = self._elastic_fields() if isinstance(eq, Elastic) else None
         if self.autotune or self.schedule is not None:
             self._apply_schedule(geo, padded, wb, fields, mem_mode, ckpt_every)
+        mem_mode, ckpt_every = self._apply_budget(geo, padded, wb, fields, mem_mode, ckpt_every)
         if isinstance(eq, (Acoustic, Acoustic3D)):
             return _AcousticFn.apply(padded[0], wb, self, geo, mem_mode, ckpt_every)
         if isinstance(eq, Elastic):

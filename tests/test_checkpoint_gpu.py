@@ -76,3 +76,21 @@ def test_elastic_checkpoint(chunks):
         print(f"elastic chunks={chunks} {name}: ckpt vs boundary {rel(a, b):.2e}, vs reference {rel(a, d[ref]):.2e}")
         assert rel(a, d[ref]) < GRAD_TOL
         assert rel(a, b) < 1e-4
+
+
+@pytest.mark.parametrize("case,eq_name", [("acoustic2d_multi", "Acoustic"), ("acoustic3d", "Acoustic3D")])
+def test_tape_budget_switches_to_checkpoints(case, eq_name):
+    """BoundarySaving(budget_gb=...): a call whose boundary-saving tape fits
+    runs boundary saving, one whose tape does not checkpoints every
+    ckpt_chunks steps -- the same results, bit for bit, as asking for that
+    mode directly."""
+    import sweep_b200
+    from sweep_b200 import BoundarySaving, Ckpt
+    eq = getattr(sweep_b200, eq_name)
+    d = load(case)
+    p_bs, g_bs = _acoustic(d, BoundarySaving(), eq)
+    p_ck, g_ck = _acoustic(d, Ckpt(chunks=29), eq)
+    p_big, g_big = _acoustic(d, BoundarySaving(budget_gb=100.0, ckpt_chunks=29), eq)
+    p_small, g_small = _acoustic(d, BoundarySaving(budget_gb=1e-6, ckpt_chunks=29), eq)
+    assert np.array_equal(p_big, p_bs) and np.array_equal(g_big, g_bs)
+    assert np.array_equal(p_small, p_ck) and np.array_equal(g_small, g_ck)

@@ -113,7 +113,8 @@ def test_autotune_records_a_schedule_and_keeps_parity(case):
     from sweep_b200 import autotune
     pred, grads, gw, s = _run(case, autotune=True)
     rep = s.tune_report
-    assert rep is not None and rep["schedule"]["graph_steps"] in rep["trials"]["graph_steps"]
+    assert rep is not None and set(rep["trials"]) >= {"graph_steps"}
+    assert rep["schedule"]["graph_steps"] in rep["trials"]["graph_steps"]
     for knob, res in rep["trials"].items():
         assert rep["schedule"][knob] == min(res, key=res.get), knob
     d = load(case)
