@@ -64,6 +64,10 @@ struct Params {
     int wzl, wzh, wyl, wyh, wxl, wxh;          // strip widths
     long long n_top, n_bot, nring, nstrip;
     const float *az, *bz, *dbz, *ay, *by, *dby, *ax, *bx, *dbx;
+    // the same profiles packed per index as {a, b, d b / d axis, d a / d axis}
+    // (one 16-byte load per neighbour in the CPML terms); d a / d axis is the
+    // centred derivative grad_p(a + i) on [M, n - M), 0 outside
+    const float4 *pz, *py, *px;
     const float *cf, *ca, *vv;                 // model fields, pitched (one copy: shared model)
     StripStore st;
 };
@@ -311,9 +315,6 @@ __global__ void __launch_bounds__(NTH, 4) f3_step(const __grid_constant__ F3Maps
         if (__syncthreads_or(!ok)) { fail(q); return; }
     }
     const int cidx = (ty + M) * PW + (tx + M);
-    // the x / y profile derivatives d a / d axis of this thread's column (constant along z)
-    const float dax = (col && (ix < P.ex0 || ix >= P.ex1)) ? grad_p(P.ax + ix, 1, P, P.dx) : 0.f;
-    const float day = (col && (iy < P.ey0 || iy >= P.ey1)) ? grad_p(P.ay + iy, 1, P, P.dy) : 0.f;
     for (int z = zb; z < ze; ++z) {
         {
             const bool ok = tma::mbar_wait(&sm.bar[slot(z + M)], parity(z + M), err, ERR_WAIT_F3);
@@ -339,8 +340,8 @@ __global__ void __launch_bounds__(NTH, 4) f3_step(const __grid_constant__ F3Maps
                 if (inx) {
                     const float du = grad_p(p, 1, P, P.dx);
                     const float dps = grad_p(F.psx + i, 1, P, P.dx);
-                    const float a = __ldg(P.ax + ix), bb = __ldg(P.bx + ix), db = __ldg(P.dbx + ix);
-                    const float da = dax;
+                    const float4 pr = __ldg(P.px + ix);
+                    const float a = pr.x, bb = pr.y, db = pr.z, da = pr.w;
                     const float ps = F.psx[i], zt = F.zx[i];
                     const float tmp = (((1.f + bb) * lx + db * du) + a * dps) + da * ps;
                     w += (1.f + bb) * tmp + a * zt;
@@ -352,8 +353,8 @@ __global__ void __launch_bounds__(NTH, 4) f3_step(const __grid_constant__ F3Maps
                 if (iny) {
                     const float du = grad_p(p, PW, P, P.dy);
                     const float dps = grad_p(F.psy + i, P.P, P, P.dy);
-                    const float a = __ldg(P.ay + iy), bb = __ldg(P.by + iy), db = __ldg(P.dby + iy);
-                    const float da = day;
+                    const float4 pr = __ldg(P.py + iy);
+                    const float a = pr.x, bb = pr.y, db = pr.z, da = pr.w;
                     const float ps = F.psy[i], zt = F.zy[i];
                     const float tmp = (((1.f + bb) * ly + db * du) + a * dps) + da * ps;
                     w += (1.f + bb) * tmp + a * zt;
@@ -365,8 +366,8 @@ __global__ void __launch_bounds__(NTH, 4) f3_step(const __grid_constant__ F3Maps
                 if (inz) {
                     const float du = grad_q(q, P, P.dz);
                     const float dps = grad_p(F.psz + i, P.SP, P, P.dz);
-                    const float a = __ldg(P.az + z), bb = __ldg(P.bz + z), db = __ldg(P.dbz + z);
-                    const float da = grad_p(P.az + z, 1, P, P.dz);
+                    const float4 pr = __ldg(P.pz + z);
+                    const float a = pr.x, bb = pr.y, db = pr.z, da = pr.w;
                     const float ps = F.psz[i], zt = F.zz[i];
                     const float tmp = (((1.f + bb) * lz + db * du) + a * dps) + da * ps;
                     w += (1.f + bb) * tmp + a * zt;
@@ -548,30 +549,30 @@ struct A3 {
 };
 
 // The transposed CPML terms of one axis at linear offset i, stride st,
-// profiles (a, b, db) at axis index c (reference adjoint_split.cu:205-255).
-// cav / lav: (v*v)*dt^2 and lambda at the 2M+1 cells along the axis around i
-// (from shared memory), gw = their product at i.
-// da: the centred derivative of a at c (grad_p(a + c, 1, P, h); the x and y
-// ones are fixed per thread, so the caller hoists them out of the plane loop).
-__device__ __forceinline__ void adj_axis(const Params& P, const float* __restrict__ a, const float* __restrict__ bv,
-                                         const float* __restrict__ dbv, const float (&cav)[2 * M + 1],
+// packed profiles pr = {a, b, db, da} at axis index c (reference
+// adjoint_split.cu:205-255).  cav / lav: (v*v)*dt^2 and lambda at the 2M+1
+// cells along the axis around i (from shared memory), gw = their product at i.
+__device__ __forceinline__ void adj_axis(const Params& P, const float4* __restrict__ pr,
+                                         const float (&cav)[2 * M + 1],
                                          const float (&lav)[2 * M + 1], const float* __restrict__ psi,
                                          const float* __restrict__ zeta, long long i, long long st, int c, float gw,
-                                         float h, float da, float& L, float& Dg, float* pso, float* zto)
+                                         float h, float& L, float& Dg, float* pso, float* zto)
 {
-    const float a_ = __ldg(a + c), b_ = __ldg(bv + c);
+    const float4 p0 = __ldg(pr + c);
+    const float a_ = p0.x, b_ = p0.y, da = p0.w;
     const float gt0 = b_ * zeta[i] + (1.0f + b_) * gw;
     const float l0 = (1.0f + b_) * gt0;
     float Lq = 0.0f, Dgg = 0.0f, Dq = 0.0f;
 #pragma unroll
     for (int k = 1; k <= M; ++k) {
         const long long np = i + k * st, nm = i - k * st;
-        const float bp = __ldg(bv + c + k), bm = __ldg(bv + c - k);
+        const float4 pp = __ldg(pr + c + k), pm = __ldg(pr + c - k);
+        const float bp = pp.y, bm = pm.y;
         const float tp = bp * zeta[np] + ((1.0f + bp) * cav[M + k]) * lav[M + k];
         const float tm = bm * zeta[nm] + ((1.0f + bm) * cav[M - k]) * lav[M - k];
         Lq += P.lc[k] * (tap((1.0f + bp) * tp, l0) + tap((1.0f + bm) * tm, l0));
-        Dgg += P.gc[k] * ((bp * psi[np] + __ldg(dbv + c + k) * tp) - (bm * psi[nm] + __ldg(dbv + c - k) * tm));
-        Dq += P.gc[k] * (__ldg(a + c + k) * tp - __ldg(a + c - k) * tm);
+        Dgg += P.gc[k] * ((bp * psi[np] + pp.z * tp) - (bm * psi[nm] + pm.z * tm));
+        Dq += P.gc[k] * (pp.x * tp - pm.x * tm);
     }
     L = Lq * (1.0f / (h * h));
     Dg = Dgg * (1.0f / h);
@@ -660,8 +661,6 @@ __global__ void __launch_bounds__(NTH, 3) a3_step(const __grid_constant__ A3Maps
     for (int q = q0; q < zb + M; ++q)
         if (!arrive(q)) { fail(q); return; }
     const int cidx = (ty + M) * PW + (tx + M), cc = ty * BXC + tx;
-    const float dax = (col && (ix < P.qx0 || ix >= P.qx1)) ? grad_p(P.ax + ix, 1, P, P.dx) : 0.f;
-    const float day = (col && (iy < P.qy0 || iy >= P.qy1)) ? grad_p(P.ay + iy, 1, P, P.dy) : 0.f;
     for (int z = zb; z < ze; ++z) {
         if (!arrive(z + M)) { fail(z + M); return; }
         if (col) {
@@ -693,8 +692,8 @@ __global__ void __launch_bounds__(NTH, 3) a3_step(const __grid_constant__ A3Maps
                 if (inx) {
 #pragma unroll
                     for (int k = -M; k <= M; ++k) { cav[M + k] = pc[k]; lav[M + k] = pl[k]; }
-                    adj_axis(P, P.ax, P.bx, P.dbx, cav, lav, A.px + bo, A.zx + bo, ic, 1, ix, gw, P.dx, dax, Lx,
-                             Dgx, A.pxo + bo, A.zxo + bo);
+                    adj_axis(P, P.px, cav, lav, A.px + bo, A.zx + bo, ic, 1, ix, gw, P.dx, Lx, Dgx, A.pxo + bo,
+                             A.zxo + bo);
                 } else {
                     Lx = 0.0f;
 #pragma unroll
@@ -704,8 +703,8 @@ __global__ void __launch_bounds__(NTH, 3) a3_step(const __grid_constant__ A3Maps
                 if (iny) {
 #pragma unroll
                     for (int k = -M; k <= M; ++k) { cav[M + k] = pc[k * PW]; lav[M + k] = pl[k * PW]; }
-                    adj_axis(P, P.ay, P.by, P.dby, cav, lav, A.py + bo, A.zy + bo, ic, P.P, iy, gw, P.dy, day, Ly,
-                             Dgy, A.pyo + bo, A.zyo + bo);
+                    adj_axis(P, P.py, cav, lav, A.py + bo, A.zy + bo, ic, P.P, iy, gw, P.dy, Ly, Dgy, A.pyo + bo,
+                             A.zyo + bo);
                 } else {
                     Ly = 0.0f;
 #pragma unroll
@@ -719,8 +718,8 @@ __global__ void __launch_bounds__(NTH, 3) a3_step(const __grid_constant__ A3Maps
                         cav[M + k] = sm.c[slot(z + k)][cidx];
                         lav[M + k] = sm.l[slot(z + k)][cidx];
                     }
-                    adj_axis(P, P.az, P.bz, P.dbz, cav, lav, A.pz + bo, A.zz + bo, ic, P.SP, z, gw, P.dz,
-                             grad_p(P.az + z, 1, P, P.dz), Lz, Dgz, A.pzo + bo, A.zzo + bo);
+                    adj_axis(P, P.pz, cav, lav, A.pz + bo, A.zz + bo, ic, P.SP, z, gw, P.dz, Lz, Dgz, A.pzo + bo,
+                             A.zzo + bo);
                 } else {
                     Lz = 0.0f;
 #pragma unroll
@@ -863,6 +862,17 @@ __global__ void illum_tail3(const Params P, const float* __restrict__ lam, float
 }
 
 // model fields, pitched: cf = ((v*v)*dt)*dt, ca = (v*v)*(dt*dt), vv = v
+// {a, b, d b, d a} per index of one axis (d a: grad_p of the a profile on
+// [M, n - M), as the stencil kernels computed it in place before).
+__global__ void pack_prof3(const float* __restrict__ a, const float* __restrict__ b, const float* __restrict__ db,
+                           int n, float h, const Params P, float4* __restrict__ out)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float da = (i >= M && i < n - M) ? grad_p(a + i, 1, P, h) : 0.f;
+        out[i] = make_float4(a[i], b[i], db[i], da);
+    }
+}
+
 __global__ void prep3(const float* __restrict__ vp, int rows, int nx, int P, float dt,
                       float* __restrict__ cf, float* __restrict__ ca, float* __restrict__ vv)
 {
@@ -973,17 +983,33 @@ struct Work {
     int* err;                        // bounded-wait failure flag
     float* scratch;                  // one step's fp32 strips ahead of their quantisation (scaled formats)
     char* ring;                      // host tape: HostRing::R device strip slots
+    float4 *pz, *py, *px;            // packed CPML profiles per axis
 };
 
 static Work carve(Carve& c, const Params& P, int nfields)
 {
     Work w{};
     w.cf = c.take<float>(P.S); w.ca = c.take<float>(P.S); w.vv = c.take<float>(P.S);
+    w.pz = c.take<float4>(P.nz); w.py = c.take<float4>(P.ny); w.px = c.take<float4>(P.nx);
     for (int i = 0; i < nfields; ++i) w.f[i] = c.take<float>((long long)P.B * P.S);
     w.err = c.take<int>(1);
     if (P.st.fmt == SF_F16 || P.st.fmt == SF_I8) w.scratch = c.take<float>((long long)P.B * P.nstrip);
     if (P.st.host) w.ring = c.take<char>((long long)HostRing::R * P.st.step);
     return w;
+}
+
+// Model fields and packed profiles of a call (shared by both passes).
+static void prep_call(const sweep_acoustic_desc* d, Params& P, const Work& w, cudaStream_t st)
+{
+    const long long rows = (long long)d->nz * d->ny;
+    prep3<<<592, 256, 0, st>>>(d->vp, (int)rows, d->nx, P.P, d->dt, w.cf, w.ca, w.vv);
+    SWEEP_LAUNCH_CHECK();
+    P.cf = w.cf; P.ca = w.ca; P.vv = w.vv;
+    pack_prof3<<<1, 256, 0, st>>>(d->az, d->bz, d->dbz, d->nz, d->dz, P, w.pz);
+    pack_prof3<<<1, 256, 0, st>>>(d->ay, d->by, d->dby, d->ny, d->dy, P, w.py);
+    pack_prof3<<<1, 256, 0, st>>>(d->ax, d->bx, d->dbx, d->nx, d->dx, P, w.px);
+    SWEEP_LAUNCH_CHECK();
+    P.pz = w.pz; P.py = w.py; P.px = w.px;
 }
 
 static void check_err(const Work& w, cudaStream_t st, const char* what)
@@ -1219,10 +1245,7 @@ void forward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* 
     set_store(P, mem_mode);
     Carve c(ws);
     Work w = carve(c, P, kFwdFields);
-    const long long rows = (long long)d->nz * d->ny;
-    prep3<<<592, 256, 0, st>>>(d->vp, (int)rows, d->nx, P.P, d->dt, w.cf, w.ca, w.vv);
-    SWEEP_LAUNCH_CHECK();
-    P.cf = w.cf; P.ca = w.ca; P.vv = w.vv;
+    prep_call(d, P, w, st);
     const long long n = (long long)P.B * P.S;
     for (int i = 0; i < kFwdFields; ++i) SWEEP_CUDA(cudaMemsetAsync(w.f[i], 0, n * 4, st));
     SWEEP_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
@@ -1286,9 +1309,7 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     Work w = carve(c, P, ckpt ? kRevFields + kFwdFields : kRevFields);
     float* chunk = ckpt ? c.take<float>((long long)(ckpt_every + 1) * P.B * P.nstrip) : nullptr;
     const long long rows = (long long)d->nz * d->ny;
-    prep3<<<592, 256, 0, st>>>(d->vp, (int)rows, d->nx, P.P, d->dt, w.cf, w.ca, w.vv);
-    SWEEP_LAUNCH_CHECK();
-    P.cf = w.cf; P.ca = w.ca; P.vv = w.vv;
+    prep_call(d, P, w, st);
     const long long n = (long long)P.B * P.S;
     const bool illum = illum_s != nullptr;
     for (int i = 0; i < kRevFields; ++i) SWEEP_CUDA(cudaMemsetAsync(w.f[i], 0, n * 4, st));
