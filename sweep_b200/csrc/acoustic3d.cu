@@ -310,16 +310,20 @@ __global__ void __launch_bounds__(NTH, 4) f3_step(const __grid_constant__ F3Maps
         if (tid == 0)
             for (int r = q; r < next; ++r) tma::mbar_wait(&sm.bar[slot(r)], parity(r), err, ERR_WAIT_F3);
     };
-    for (int q = q0; q < zb + M; ++q) {
-        const bool ok = tma::mbar_wait(&sm.bar[slot(q)], parity(q), err, ERR_WAIT_F3);
-        if (__syncthreads_or(!ok)) { fail(q); return; }
-    }
+    // Each thread waits for the stages it reads itself; a failed wait is
+    // noted and the whole CTA leaves at the end of that plane, at the one
+    // block barrier a plane has (results are then invalid and the host
+    // reports the error).  Leaving, thread 0 waits (bounded) for every stage
+    // still in flight: from q0 at the first plane (no slot reused yet), else
+    // from z + M (every earlier stage was waited for at an earlier barrier).
+    bool bad = false;
+    auto await = [&](int q) {
+        if (!tma::mbar_wait(&sm.bar[slot(q)], parity(q), err, ERR_WAIT_F3)) bad = true;
+    };
+    for (int q = q0; q < zb + M; ++q) await(q);
     const int cidx = (ty + M) * PW + (tx + M);
     for (int z = zb; z < ze; ++z) {
-        {
-            const bool ok = tma::mbar_wait(&sm.bar[slot(z + M)], parity(z + M), err, ERR_WAIT_F3);
-            if (__syncthreads_or(!ok)) { fail(z + M); return; }
-        }
+        await(z + M);
         if (col) {
             float q[2 * M + 1];
 #pragma unroll
@@ -380,7 +384,8 @@ __global__ void __launch_bounds__(NTH, 4) f3_step(const __grid_constant__ F3Maps
             const int cc = ty * BXC + tx;
             F.u_next[i] = 2.f * q[M] - sm.up[slot(z + M)][cc] + sm.cf[slot(z + M)][cc] * w;
         }
-        __syncthreads();                               // every thread is done with stage z - M
+        // every thread is done with stage z - M (and has waited for z + M)
+        if (__syncthreads_or(bad)) { fail(z == zb ? q0 : z + M); return; }
         if (tid == 0 && next < q1) issue(next++);      // reuses the slot of stage z - M
     }
 }
@@ -646,23 +651,26 @@ __global__ void __launch_bounds__(NTH, 3) a3_step(const __grid_constant__ A3Maps
         if (tid == 0)
             for (int r = q; r < next; ++r) tma::mbar_wait(&sm.bar[slot(r)], parity(r), err, ERR_WAIT_F3);
     };
-    // wait for stage q and, in a clean CTA, turn its model plane into gw
+    // Wait for stage q and, in a clean CTA, turn its model plane into gw.
+    // Each thread waits itself; a failed wait is noted and the CTA leaves
+    // together at the next block barrier: the conversion barrier of a clean
+    // CTA, else the one that ends the plane.
+    bool bad = false;
     auto arrive = [&](int q) -> bool {
-        const bool ok = tma::mbar_wait(&sm.bar[slot(q)], parity(q), err, ERR_WAIT_F3);
-        if (__syncthreads_or(!ok)) return false;
+        if (!tma::mbar_wait(&sm.bar[slot(q)], parity(q), err, ERR_WAIT_F3)) bad = true;
         if (clean) {
             float* c = sm.c[slot(q)];
             const float* l = sm.l[slot(q)];
             for (int e = tid; e < PN; e += NTH) c[e] = c[e] * l[e];
-            __syncthreads();
+            if (__syncthreads_or(bad)) return false;
         }
         return true;
     };
     for (int q = q0; q < zb + M; ++q)
-        if (!arrive(q)) { fail(q); return; }
+        if (!arrive(q)) { fail(q0); return; }
     const int cidx = (ty + M) * PW + (tx + M), cc = ty * BXC + tx;
     for (int z = zb; z < ze; ++z) {
-        if (!arrive(z + M)) { fail(z + M); return; }
+        if (!arrive(z + M)) { fail(z == zb ? q0 : z + M); return; }
         if (col) {
             const float* pl = sm.l[slot(z)] + cidx;
             const float* pc = sm.c[slot(z)] + cidx;
@@ -730,7 +738,7 @@ __global__ void __launch_bounds__(NTH, 3) a3_step(const __grid_constant__ A3Maps
                 A.l_next[i] = 2.0f * gun - lprevv + (Lx + Ly + Lz - Dgx - Dgy - Dgz);
             }
         }
-        __syncthreads();
+        if (__syncthreads_or(bad)) { fail(z == zb ? q0 : z + M); return; }
         if (tid == 0 && next < q1) issue(next++);
     }
 }
@@ -811,16 +819,15 @@ __global__ void __launch_bounds__(NTH, 4) r3_recon(const __grid_constant__ R3Map
         if (tid == 0)
             for (int r = q; r < next; ++r) tma::mbar_wait(&sm.bar[slot(r)], parity(r), err, ERR_WAIT_F3);
     };
-    for (int q = q0; q < zb + M; ++q) {
-        const bool ok = tma::mbar_wait(&sm.bar[slot(q)], parity(q), err, ERR_WAIT_F3);
-        if (__syncthreads_or(!ok)) { fail(q); return; }
-    }
+    // one block barrier per plane; a failed wait leaves at it (as f3_step)
+    bool bad = false;
+    auto await = [&](int q) {
+        if (!tma::mbar_wait(&sm.bar[slot(q)], parity(q), err, ERR_WAIT_F3)) bad = true;
+    };
+    for (int q = q0; q < zb + M; ++q) await(q);
     const int cidx = (ty + M) * PW + (tx + M), cc = ty * BXC + tx;
     for (int z = zb; z < ze; ++z) {
-        {
-            const bool ok = tma::mbar_wait(&sm.bar[slot(z + M)], parity(z + M), err, ERR_WAIT_F3);
-            if (__syncthreads_or(!ok)) { fail(z + M); return; }
-        }
+        await(z + M);
         if (col) {
             float q[2 * M + 1];
 #pragma unroll
@@ -841,7 +848,7 @@ __global__ void __launch_bounds__(NTH, 4) r3_recon(const __grid_constant__ R3Map
             R.gacc[i] = t;
             if (R.is) { R.is[i] += utt * utt; R.ir[i] += lam * lam; }
         }
-        __syncthreads();
+        if (__syncthreads_or(bad)) { fail(z == zb ? q0 : z + M); return; }
         if (tid == 0 && next < q1) issue(next++);
     }
 }
