@@ -335,11 +335,20 @@ __global__ void __launch_bounds__(NTH) fwd_kernel(const __grid_constant__ FwdMap
         cf[k] = computed(P, iz, ix) ? __ldg(P.cf + b0 * P.ms + iz * P.P + ix) : 0.f;
     }
 
+    __syncthreads();                     // the event ranges (sm.evr) are written
+    // Each thread waits for shot g's tiles itself; a failed wait is noted and
+    // the CTA leaves together at the barrier that ends the shot, after
+    // thread 0 has waited (bounded) for the loads still in flight.
+    bool bad = false;
+    auto leave = [&](int g) {
+        if (threadIdx.x == 0)
+            for (int h = g; h < min(g + 2, nloc); ++h)
+                tma::mbar_wait(&sm.bar[h & 1], (h >> 1) & 1, P.err, ERR_TMA_WAIT_FWD);
+    };
     for (int g = 0; g < nloc; ++g) {
         const int b = b0 + g;
         const int s = g & 1;
-        const bool ok = tma::mbar_wait(&sm.bar[s], (g >> 1) & 1, P.err, ERR_TMA_WAIT_FWD);
-        if (__syncthreads_or(!ok)) return;
+        if (!tma::mbar_wait(&sm.bar[s], (g >> 1) & 1, P.err, ERR_TMA_WAIT_FWD)) bad = true;
         const float* now = sm.now[s];
         const float* prev = sm.prev[s];
         const long long bo = (long long)b * P.S;
@@ -428,7 +437,8 @@ __global__ void __launch_bounds__(NTH) fwd_kernel(const __grid_constant__ FwdMap
             const int iz = tz0 + cell_r(k), ix = tx0 + cell_c(k);
             if (full || computed(P, iz, ix)) un[iz * P.P + ix] = out[k];
         }
-        __syncthreads();                 // every thread is done with stage s
+        // every thread is done with stage s (and has waited for it)
+        if (__syncthreads_or(bad)) { leave(g); return; }
         if (threadIdx.x == 0 && g + 2 < nloc) issue(s, b + 2);
     }
 }
@@ -446,6 +456,9 @@ struct RevSmem {
     float bz[SH], dbz[SH];           // the same at the staged rows
     int4 evr[kMaxG];                 // per shot of the CTA: source and receiver event ranges
     uint64_t bar[3];
+    int bad[2];                      // a thread's wait for shot g failed: bad[g & 1] (read after the
+                                     // shot's barrier; by parity, so shot g + 1's write cannot meet
+                                     // a slower thread's read for shot g)
 };
 
 // One launch per reverse step `it` of the boundary-saving backward:
@@ -497,6 +510,7 @@ __global__ void __launch_bounds__(NTH, 2) rev_kernel(const __grid_constant__ Rev
     if (threadIdx.x == 0) {
         for (int i = 0; i < 3; ++i) tma::mbar_init(&sm.bar[i], 1);
         tma::fence_barrier_init();
+        sm.bad[0] = sm.bad[1] = 0;
     }
     __syncthreads();
     auto issue = [&](int s, int b) {
@@ -561,11 +575,17 @@ __global__ void __launch_bounds__(NTH, 2) rev_kernel(const __grid_constant__ Rev
 #pragma unroll
     for (int k = 0; k < CPT; ++k) gsum[k] = 0.f;
 
+    // one block barrier per shot, as in fwd_kernel (the failure flag in
+    // shared memory: a register kept across the shot loop would spill)
+    auto leave = [&](int g) {
+        if (threadIdx.x == 0)
+            for (int h = g; h < min(g + 2, nloc); ++h)
+                tma::mbar_wait(&sm.bar[h & 1], (h >> 1) & 1, P.err, ERR_TMA_WAIT_REV);
+    };
     for (int g = 0; g < nloc; ++g) {
         const int b = b0 + g;
         const int s = g & 1;
-        const bool ok = tma::mbar_wait(&sm.bar[s], (g >> 1) & 1, P.err, ERR_TMA_WAIT_REV);
-        if (__syncthreads_or(!ok)) return;
+        if (!tma::mbar_wait(&sm.bar[s], (g >> 1) & 1, P.err, ERR_TMA_WAIT_REV)) sm.bad[s] = 1;
         const long long bo = (long long)b * P.S;
         const float* sl = sm.l[s];
         const float* slp = sm.lp[s];
@@ -871,7 +891,9 @@ __global__ void __launch_bounds__(NTH, 2) rev_kernel(const __grid_constant__ Rev
         }
 #pragma unroll
         for (int k = 0; k < CPT; ++k) gsum[k] += gl[k];
-        __syncthreads();                 // every thread is done with stage s
+        // every thread is done with stage s (and has waited for it)
+        __syncthreads();
+        if (sm.bad[s]) { leave(g); return; }
         if (threadIdx.x == 0 && g + 2 < nloc) issue(s, b + 2);
     }
 
