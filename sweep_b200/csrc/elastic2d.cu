@@ -363,6 +363,7 @@ struct StageSmem {
     float h[2][NH][HN];
     float c[2][NC][CN];
     uint64_t bar[2];
+    int bad[2];      // a thread's wait for shot g failed: bad[g & 1] (read after the shot's barrier)
 };
 using VelSmem = StageSmem<3, 2>;   // sxx, szz, sxz halos; vx, vz centres
 using StrSmem = StageSmem<2, 3>;   // vx, vz halos; sxx, szz, sxz centres
@@ -377,6 +378,7 @@ __device__ __forceinline__ void pipeline_start(StageSmem<NH, NC>& sm, int nloc, 
         tma::mbar_init(&sm.bar[0], 1);
         tma::mbar_init(&sm.bar[1], 1);
         tma::fence_barrier_init();
+        sm.bad[0] = sm.bad[1] = 0;
     }
     __syncthreads();
     if (threadIdx.x == 0 && threadIdx.y == 0) {
@@ -421,6 +423,7 @@ __global__ void __launch_bounds__(NTH, 4) fwd_vel(const __grid_constant__ FwdMap
         bvr[r] = in_core(G, ix, iz) ? A.m.bv[(long long)b0 * G.ms + (long long)iz * G.P + ix] : 0.f;
     }
     const bool ring = tile_in_pml(G, tz0, tx0);
+    bool bad = false;
     for (int g = 0; g < nloc; ++g) {
         const int b = b0 + g, s = g & 1;
         // the CPML memories of this thread's cells, loaded while the tiles arrive
@@ -433,11 +436,9 @@ __global__ void __launch_bounds__(NTH, 4) fwd_vel(const __grid_constant__ FwdMap
                 mx[r] = load_mem_x(G, A.mem, XM_SXZX, XM_SXXX, b, iz, ix);
             }
         }
-        const bool ok = tma::mbar_wait(&sm.bar[s], (g >> 1) & 1, G.err, ERR_WAIT_FWD);
-        if (__syncthreads_or(!ok)) {
-            drain(sm, g, nloc, G.err, ERR_WAIT_FWD);
-            return;
-        }
+        // each thread waits for the stage itself; a failed wait leaves at the
+        // barrier that ends the shot (after drain)
+        if (!tma::mbar_wait(&sm.bar[s], (g >> 1) & 1, G.err, ERR_WAIT_FWD)) bad = true;
         const float *tsxx = sm.h[s][0], *tszz = sm.h[s][1], *tsxz = sm.h[s][2];
         const long long so = (long long)b * G.S;
 #pragma unroll
@@ -472,7 +473,10 @@ __global__ void __launch_bounds__(NTH, 4) fwd_vel(const __grid_constant__ FwdMap
             A.f[VX][so + i] = sm.c[s][0][cc] + bvr[r] * (dsxx_dx + dsxz_dz);
             A.f[VZ][so + i] = sm.c[s][1][cc] + bvr[r] * (dsxz_dx + dszz_dz);
         }
-        __syncthreads();                       // every thread is done with stage s
+        if (__syncthreads_or(bad)) {           // every thread is done with stage s
+            drain(sm, g, nloc, G.err, ERR_WAIT_FWD);
+            return;
+        }
         if (threadIdx.x == 0 && threadIdx.y == 0 && g + 2 < nloc) issue(s, b + 2);
     }
 }
@@ -512,11 +516,11 @@ __global__ void __launch_bounds__(NTH, 4) fwd_str(const __grid_constant__ FwdMap
     const bool stile = A.strips != nullptr && tile_has_strips(G, tz0, tx0);
     for (int g = 0; g < nloc; ++g) {
         const int b = b0 + g, s = g & 1;
-        const bool ok = tma::mbar_wait(&sm.bar[s], (g >> 1) & 1, G.err, ERR_WAIT_FWD);
-        if (__syncthreads_or(!ok)) {
-            drain(sm, g, nloc, G.err, ERR_WAIT_FWD);
-            return;
-        }
+        // each thread waits for the stage itself; a failed wait leaves at the
+        // barrier that ends the shot (after drain).  The flag is in shared
+        // memory, by parity, so shot g + 1's write cannot meet a slower
+        // thread's read for shot g (a register kept across the loop spills).
+        if (!tma::mbar_wait(&sm.bar[s], (g >> 1) & 1, G.err, ERR_WAIT_FWD)) sm.bad[s] = 1;
         const float *tvx = sm.h[s][0], *tvz = sm.h[s][1];
         const long long so = (long long)b * G.S;
         const int key = b * ntl + tile;
@@ -600,6 +604,10 @@ __global__ void __launch_bounds__(NTH, 4) fwd_str(const __grid_constant__ FwdMap
         // receivers of this (shot, tile): read back the final values of the step
         const int r0 = G.rec.off[key], r1 = G.rec.off[key + 1];
         __syncthreads();                       // stage s consumed; this shot's stores visible
+        if (sm.bad[s]) {
+            drain(sm, g, nloc, G.err, ERR_WAIT_FWD);
+            return;
+        }
         if (A.record && r1 > r0) {
             for (int e = r0 + threadIdx.x + threadIdx.y * TX; e < r1; e += NTH) {
                 const int2 ev = G.rec.ev[e];
