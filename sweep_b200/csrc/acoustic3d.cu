@@ -651,26 +651,30 @@ __global__ void __launch_bounds__(NTH, 3) a3_step(const __grid_constant__ A3Maps
         if (tid == 0)
             for (int r = q; r < next; ++r) tma::mbar_wait(&sm.bar[slot(r)], parity(r), err, ERR_WAIT_F3);
     };
-    // Wait for stage q and, in a clean CTA, turn its model plane into gw.
-    // Each thread waits itself; a failed wait is noted and the CTA leaves
-    // together at the next block barrier: the conversion barrier of a clean
-    // CTA, else the one that ends the plane.
+    // Each thread waits for the stages it reads itself; a failed wait is
+    // noted and the CTA leaves together at the next block barrier.  A clean
+    // CTA turns each stage's model plane into gw = ((v*v)*dt^2) * lambda, each
+    // thread its share: the first plane's stages before one barrier, then
+    // stage z + M + 1 at the end of plane z, before the barrier that ends the
+    // plane -- one barrier per plane in every CTA.
     bool bad = false;
-    auto arrive = [&](int q) -> bool {
+    auto await = [&](int q) {
         if (!tma::mbar_wait(&sm.bar[slot(q)], parity(q), err, ERR_WAIT_F3)) bad = true;
-        if (clean) {
-            float* c = sm.c[slot(q)];
-            const float* l = sm.l[slot(q)];
-            for (int e = tid; e < PN; e += NTH) c[e] = c[e] * l[e];
-            if (__syncthreads_or(bad)) return false;
-        }
-        return true;
     };
-    for (int q = q0; q < zb + M; ++q)
-        if (!arrive(q)) { fail(q0); return; }
+    auto convert = [&](int q) {
+        float* c = sm.c[slot(q)];
+        const float* l = sm.l[slot(q)];
+        for (int e = tid; e < PN; e += NTH) c[e] = c[e] * l[e];
+    };
+    if (clean) {
+        for (int q = q0; q <= zb + M; ++q) { await(q); convert(q); }
+        if (__syncthreads_or(bad)) { fail(q0); return; }
+    } else {
+        for (int q = q0; q < zb + M; ++q) await(q);
+    }
     const int cidx = (ty + M) * PW + (tx + M), cc = ty * BXC + tx;
     for (int z = zb; z < ze; ++z) {
-        if (!arrive(z + M)) { fail(z == zb ? q0 : z + M); return; }
+        if (!clean) await(z + M);
         if (col) {
             const float* pl = sm.l[slot(z)] + cidx;
             const float* pc = sm.c[slot(z)] + cidx;
@@ -738,7 +742,11 @@ __global__ void __launch_bounds__(NTH, 3) a3_step(const __grid_constant__ A3Maps
                 A.l_next[i] = 2.0f * gun - lprevv + (Lx + Ly + Lz - Dgx - Dgy - Dgz);
             }
         }
-        if (__syncthreads_or(bad)) { fail(z == zb ? q0 : z + M); return; }
+        // the last stage every thread has waited for (its slot is not one
+        // plane z reads: the ring holds NS3 > 2M + 2 stages)
+        int last = z + M;
+        if (clean && z + 1 < ze) { await(z + M + 1); convert(z + M + 1); last = z + M + 1; }
+        if (__syncthreads_or(bad)) { fail(z == zb && !clean ? q0 : last); return; }
         if (tid == 0 && next < q1) issue(next++);
     }
 }
