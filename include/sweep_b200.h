@@ -87,6 +87,15 @@ typedef struct sweep_acoustic_desc {
  * 91-620); the strips pass through a small device ring in the workspace and a
  * copy stream.  Every equation. */
 #define SWEEP_MEM_HOST_TAPE 0x100
+/* Recursive checkpointing with a fixed snapshot budget (reference
+ * Ckpt(mode='recursive', count=N), options.py:348-370; entries 4 / 9 / 64,
+ * capi.h:39-103): the forward keeps no tape; the backward bisects the time
+ * axis, holding at most `ckpt_every` = N forward states at once, replays each
+ * leaf of SWEEP_RECURSIVE_LEAF steps into its boundary strips and runs the
+ * boundary-saving reverse over it.  Leaves fall on multiples of the leaf
+ * length, so the gradient equals SWEEP_MEM_CHECKPOINT's with that interval. */
+#define SWEEP_MEM_RECURSIVE 5
+#define SWEEP_RECURSIVE_LEAF 64
 
 /* Bytes the caller must allocate: `workspace` (scratch, reusable between calls
  * once the previous call has finished on its stream) and `tape` (written by

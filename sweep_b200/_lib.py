@@ -46,6 +46,8 @@ MEM_BOUNDARY_FP16 = 2            # boundary saving, strips stored as scaled fp16
 MEM_BOUNDARY_BF16 = 3
 MEM_BOUNDARY_INT8 = 4
 MEM_HOST_TAPE = 0x100           # OR'ed into a boundary-saving mode: the tape is pinned host memory
+MEM_RECURSIVE = 5               # recursive checkpointing, ckpt_every = snapshot budget
+RECURSIVE_LEAF = 64
 
 FAMILY_ACOUSTIC = 0
 FAMILY_ELASTIC = 1

@@ -33,6 +33,8 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <functional>
+
 #include "acoustic2d.cuh"
 #include "tma.cuh"
 
@@ -1413,14 +1415,17 @@ static void check_mode(int mem_mode, int ckpt_every)
 {
     if (mem_mode & SWEEP_MEM_HOST_TAPE) {
         mem_mode &= ~SWEEP_MEM_HOST_TAPE;
-        SWEEP_REQUIRE(mem_mode != SWEEP_MEM_CHECKPOINT, "acoustic2d: a host tape goes with boundary saving only");
+        SWEEP_REQUIRE(mem_mode != SWEEP_MEM_CHECKPOINT && mem_mode != SWEEP_MEM_RECURSIVE,
+                      "acoustic2d: a host tape goes with boundary saving only");
     }
     SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY || mem_mode == SWEEP_MEM_CHECKPOINT ||
                       mem_mode == SWEEP_MEM_BOUNDARY_FP16 || mem_mode == SWEEP_MEM_BOUNDARY_BF16 ||
-                      mem_mode == SWEEP_MEM_BOUNDARY_INT8,
+                      mem_mode == SWEEP_MEM_BOUNDARY_INT8 || mem_mode == SWEEP_MEM_RECURSIVE,
                   "acoustic2d: unknown memory mode %d", mem_mode);
     SWEEP_REQUIRE(mem_mode != SWEEP_MEM_CHECKPOINT || ckpt_every >= 1,
                   "acoustic2d: checkpoint interval must be >= 1 (got %d)", ckpt_every);
+    SWEEP_REQUIRE(mem_mode != SWEEP_MEM_RECURSIVE || ckpt_every >= 1,
+                  "acoustic2d: the recursive checkpoint budget must be >= 1 (got %d)", ckpt_every);
 }
 
 static void copy_any(void* dst, const void* src, long long bytes, cudaStream_t st)
@@ -1440,6 +1445,11 @@ void sizes(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, int64_t* 
         RevWork rw; FwdWork fw; float* chunk;
         carve_rev_ckpt(cr, pl, true, ckpt_every, rw, fw, chunk);
         *tape = tape_bytes_ckpt(pl, ckpt_every);
+    } else if (mem_mode == SWEEP_MEM_RECURSIVE) {
+        RevWork rw; FwdWork fw; float* chunk;
+        carve_rev_ckpt(cr, pl, true, SWEEP_RECURSIVE_LEAF, rw, fw, chunk);
+        cr.take<char>((long long)ckpt_every * ckpt_stride(pl));      // the snapshot slots
+        *tape = 256;                                                   // nothing is kept
     } else {
         carve_rev(cr, pl, true);
         *tape = tape_bytes(pl);
@@ -1604,8 +1614,89 @@ void forward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* 
     sizes(d, mem_mode, ckpt_every, &need_ws, &need_tape);
     SWEEP_REQUIRE(ws != nullptr && ws_bytes >= need_ws, "acoustic2d forward: workspace too small (%lld < %lld)",
                   (long long)ws_bytes, (long long)need_ws);
-    forward_with(d, mem_mode, mem_mode == SWEEP_MEM_CHECKPOINT ? ckpt_every : 0, record, tape, ws, ws_bytes, st,
-                 nullptr);
+    // recursive checkpointing keeps nothing from the forward: the backward
+    // replays from the initial state
+    forward_with(d, mem_mode == SWEEP_MEM_RECURSIVE ? SWEEP_MEM_BOUNDARY : mem_mode,
+                 mem_mode == SWEEP_MEM_CHECKPOINT ? ckpt_every : 0, record,
+                 mem_mode == SWEEP_MEM_RECURSIVE ? nullptr : tape, ws, ws_bytes, st, nullptr);
+}
+
+// Recursive checkpointing (SWEEP_MEM_RECURSIVE; reference
+// Ckpt(mode='recursive', count), sg_driver.cuh / eq_driver.cuh recursive
+// runners): reverse [0, nt) leaf by leaf, last leaf first.  An interval
+// [a, b) longer than one leaf is bisected at a leaf boundary m: the forward is
+// replayed from the state at a to m, the state at m (and the strips of
+// U[m - 1]) goes into the next free snapshot slot, [m, b) is processed, the
+// slot is freed and [a, m) follows.  With no slot left, each leaf of [a, b)
+// replays from the state at a.  A leaf [a, e) is replayed from the state at a
+// into its strips and reversed by the boundary-saving step, exactly as a
+// checkpoint chunk; the leaves are the chunks of SWEEP_MEM_CHECKPOINT with
+// interval SWEEP_RECURSIVE_LEAF, so the gradient is that mode's.
+template <class Reverse>
+static void backward_recursive(const Plan& pl, FwdWork& fw, RevWork& w, float* chunk, char* snaps, int count,
+                               cudaStream_t st, Reverse& reverse)
+{
+    const Params& P = pl.P;
+    const int L = SWEEP_RECURSIVE_LEAF;
+    const long long n = (long long)P.B * P.S, cs = (long long)P.B * P.nstrip;
+    const FwdMaps fmaps = fwd_maps(fw, P);
+    float* state[kStateFields] = {fw.u[0], fw.u[1], fw.psix, fw.psiz, fw.zetax, fw.zetaz};
+    // the replay set starts clear (see the checkpoint mode)
+    for (auto* p : {fw.u[0], fw.u[1], fw.u[2], fw.psix, fw.psiz, fw.psixn, fw.psizn, fw.zetax, fw.zetaz})
+        SWEEP_CUDA(cudaMemsetAsync(p, 0, n * 4, st));
+    FwdState S;
+    // the state before step a: snapshot slot k, or the initial (zero) state for k < 0
+    auto restore = [&](int k) {
+        S = FwdState{};
+        S.px = fw.psix; S.pz = fw.psiz; S.pxn = fw.psixn; S.pzn = fw.psizn;
+        for (int f = 0; f < kStateFields; ++f) {
+            if (k < 0) SWEEP_CUDA(cudaMemsetAsync(state[f], 0, n * 4, st));
+            else copy_dd(state[f], ckpt_field(snaps, pl, k + 1, f), n, st);
+        }
+    };
+    auto save = [&](int k) {
+        const float* cur[kStateFields] = {fw.u[S.ip], fw.u[S.in], S.px, S.pz, fw.zetax, fw.zetaz};
+        for (int f = 0; f < kStateFields; ++f) copy_dd(ckpt_field(snaps, pl, k + 1, f), cur[f], n, st);
+    };
+    // replay [a, e) from the current state into the chunk's strips, then reverse it
+    auto leaf = [&](int a, int e) {
+        forward_steps(pl, fmaps, fw, nullptr, S, a, e, [&](int it) { return chunk + (long long)(it - a + 1) * cs; },
+                      st);
+        copy_dd(w.r[0], fw.u[S.in], n, st);       // U[e]
+        copy_dd(w.r[1], fw.u[S.ip], n, st);       // U[e - 1]
+        reverse(a, e, [&](int t) { return chunk + (long long)(t - (a - 1)) * cs; });
+    };
+    std::function<void(int, int, int, int)> process = [&](int a, int b, int ka, int free) {
+        const int nleaf = (b - a + L - 1) / L;
+        if (nleaf <= 1) {
+            restore(ka);
+            if (a > 0) copy_dd(chunk, ckpt_strips(snaps, pl, ka + 1), cs, st);   // strips of U[a - 1]
+            leaf(a, b);
+            return;
+        }
+        if (free > 0) {
+            const int k = count - free, m = a + L * ((nleaf + 1) / 2);
+            restore(ka);
+            forward_steps(pl, fmaps, fw, nullptr, S, a, m,
+                          [&](int it) { return it == m - 1 ? ckpt_strips(snaps, pl, k + 1) : nullptr; }, st);
+            save(k);
+            process(m, b, k, free - 1);
+            process(a, m, ka, free);
+            return;
+        }
+        for (int c0 = a + (nleaf - 1) * L; c0 >= a; c0 -= L) {
+            restore(ka);
+            if (c0 > a)
+                forward_steps(pl, fmaps, fw, nullptr, S, a, c0, [&](int it) { return it == c0 - 1 ? chunk : nullptr; },
+                              st);
+            else if (a > 0)
+                copy_dd(chunk, ckpt_strips(snaps, pl, ka + 1), cs, st);
+            leaf(c0, std::min(b, c0 + L));
+        }
+    };
+    // a snapshot slot k holds the state before its step and the strips of the step before
+    SWEEP_REQUIRE(count >= 1, "acoustic2d: the recursive checkpoint budget must be >= 1");
+    process(0, P.nt, -1, count);
 }
 
 void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const float* adj, const void* tape,
@@ -1625,11 +1716,16 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     Carve c(ws);
     const bool illum = illum_s != nullptr;
     const bool ckpt = mem_mode == SWEEP_MEM_CHECKPOINT;
+    const bool recursive = mem_mode == SWEEP_MEM_RECURSIVE;
     RevWork w;
     FwdWork fw{};
     float* chunk = nullptr;
+    char* snaps = nullptr;
     if (ckpt) carve_rev_ckpt(c, pl, illum, ckpt_every, w, fw, chunk);
-    else w = carve_rev(c, pl, illum);
+    else if (recursive) {
+        carve_rev_ckpt(c, pl, illum, SWEEP_RECURSIVE_LEAF, w, fw, chunk);
+        snaps = c.take<char>((long long)ckpt_every * ckpt_stride(pl));
+    } else w = carve_rev(c, pl, illum);
     {
         VecStage vs(pl.P);
         setup_common(d, pl, w.c, st, vs.h);
@@ -1665,7 +1761,7 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     // Reverse steps [it0, it1) top down; the reconstruction starts from
     // r[0] = U[it1], r[1] = U[it1 - 1]; strips_of(it) holds the strips of U[it].
     HostRing hr;
-    const bool host = pl.host_tape && !ckpt;
+    const bool host = pl.host_tape && !ckpt && !recursive;
     auto reverse = [&](int it0, int it1, auto strips_of) {
         StepGraphs gs(st, host ? 0 : pl.graph_steps);
         int rp = 0, rn = 1, rx = 2;
@@ -1691,7 +1787,9 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
         }
         gs.flush();
     };
-    if (!ckpt) {
+    if (recursive) {
+        backward_recursive(pl, fw, w, chunk, snaps, ckpt_every, st, reverse);
+    } else if (!ckpt) {
         const float* last = tape_last(const_cast<void*>(tape), pl);
         // seed: prev = U[nt], now = U[nt-1]  (reference driver_traits.cuh:493-505; the
         // rim outside the physical box is never read by the reconstruction)

@@ -20,6 +20,8 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <functional>
+
 #include "common.cuh"
 #include "tma.cuh"
 
@@ -1151,12 +1153,15 @@ void sizes(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, int64_t* 
     const int base_mode = mem_mode & ~SWEEP_MEM_HOST_TAPE;
     SWEEP_REQUIRE(base_mode == SWEEP_MEM_BOUNDARY || base_mode == SWEEP_MEM_CHECKPOINT ||
                       base_mode == SWEEP_MEM_BOUNDARY_FP16 || base_mode == SWEEP_MEM_BOUNDARY_BF16 ||
-                      base_mode == SWEEP_MEM_BOUNDARY_INT8,
+                      base_mode == SWEEP_MEM_BOUNDARY_INT8 || base_mode == SWEEP_MEM_RECURSIVE,
                   "acoustic3d: unknown memory mode %d", mem_mode);
-    SWEEP_REQUIRE(!(mem_mode & SWEEP_MEM_HOST_TAPE) || base_mode != SWEEP_MEM_CHECKPOINT,
+    SWEEP_REQUIRE(!(mem_mode & SWEEP_MEM_HOST_TAPE) ||
+                      (base_mode != SWEEP_MEM_CHECKPOINT && base_mode != SWEEP_MEM_RECURSIVE),
                   "acoustic3d: a host tape goes with boundary saving only");
     SWEEP_REQUIRE(mem_mode != SWEEP_MEM_CHECKPOINT || ckpt_every >= 1,
                   "acoustic3d: checkpoint interval must be >= 1 (got %d)", ckpt_every);
+    SWEEP_REQUIRE(mem_mode != SWEEP_MEM_RECURSIVE || ckpt_every >= 1,
+                  "acoustic3d: the recursive checkpoint budget must be >= 1 (got %d)", ckpt_every);
     Params P = make_params(d);
     set_store(P, mem_mode);
     Carve c(nullptr);
@@ -1164,6 +1169,11 @@ void sizes(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, int64_t* 
         carve(c, P, kRevFields + kFwdFields);
         c.take<float>((long long)(ckpt_every + 1) * P.B * P.nstrip);
         *tape = (int64_t)std::max(nchunks(P, ckpt_every) - 1, 1) * ckpt_stride(P);
+    } else if (mem_mode == SWEEP_MEM_RECURSIVE) {
+        carve(c, P, kRevFields + kFwdFields);
+        c.take<float>((long long)(SWEEP_RECURSIVE_LEAF + 1) * P.B * P.nstrip);
+        c.take<char>((long long)ckpt_every * ckpt_stride(P));           // the snapshot slots
+        *tape = 256;                                                     // nothing is kept
     } else {
         carve(c, P, std::max(kFwdFields, kRevFields));
         *tape = tape_bytes(P);
@@ -1266,6 +1276,12 @@ void forward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* 
     SWEEP_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
     if (d->nrec > 0) SWEEP_CUDA(cudaMemsetAsync(record, 0, (size_t)d->B * d->nt * d->nrec * 4, st));
     FwdState S(w.f);
+    if (mem_mode == SWEEP_MEM_RECURSIVE) {
+        // recursive checkpointing keeps nothing: the backward replays from the initial state
+        forward_steps(d, P, S, record, 0, d->nt, [&](int) { return (void*)nullptr; }, w.err, w.scratch, st);
+        check_err(w, st, "forward");
+        return;
+    }
     if (mem_mode != SWEEP_MEM_CHECKPOINT && tape && P.st.host) {
         HostRing hr;
         hr.open(w.ring, tape, P.st.step, st);
@@ -1303,6 +1319,74 @@ void forward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* 
     check_err(w, st, "forward");
 }
 
+// Recursive checkpointing (SWEEP_MEM_RECURSIVE): the 2-D driver's bisection
+// (acoustic2d.cu backward_recursive) over the 3-D replay set w.f[kRevFields..]:
+// at most `count` snapshot slots, each the checkpoint layout (state fields,
+// then the strips of the step before); leaves of SWEEP_RECURSIVE_LEAF steps,
+// the chunks of SWEEP_MEM_CHECKPOINT with that interval.
+template <class Reverse>
+static void backward_recursive(const sweep_acoustic_desc* d, const Params& P, Work& w, float* chunk, char* snaps,
+                               int count, cudaStream_t st, Reverse& reverse)
+{
+    const int L = SWEEP_RECURSIVE_LEAF;
+    const long long n = (long long)P.B * P.S, cs = (long long)P.B * P.nstrip;
+    float* const* fw = w.f + kRevFields;
+    // the replay set starts clear (see the checkpoint mode)
+    for (int i = 0; i < kFwdFields; ++i) SWEEP_CUDA(cudaMemsetAsync(fw[i], 0, n * 4, st));
+    FwdState S(fw);
+    auto restore = [&](int k) {
+        S = FwdState(fw);
+        float* state[kStateFields];
+        state_fields(S, state);
+        for (int f = 0; f < kStateFields; ++f) {
+            if (k < 0) SWEEP_CUDA(cudaMemsetAsync(state[f], 0, n * 4, st));
+            else copy_dd(state[f], ckpt_field(snaps, P, k + 1, f), n, st);
+        }
+    };
+    auto save = [&](int k) {
+        float* state[kStateFields];
+        state_fields(S, state);
+        for (int f = 0; f < kStateFields; ++f) copy_dd(ckpt_field(snaps, P, k + 1, f), state[f], n, st);
+    };
+    auto replay = [&](int a, int e, auto strips_of) {
+        forward_steps(d, P, S, nullptr, a, e, strips_of, w.err, w.scratch, st);
+    };
+    auto leaf = [&](int a, int e) {
+        replay(a, e, [&](int it) { return (void*)(chunk + (long long)(it - a + 1) * cs); });
+        copy_dd(w.f[15], S.f[S.in], n, st);      // U[e]
+        copy_dd(w.f[16], S.f[S.ip], n, st);      // U[e - 1]
+        reverse(a, e, [&](int t) { return chunk + (long long)(t - (a - 1)) * cs; });
+    };
+    std::function<void(int, int, int, int)> process = [&](int a, int b, int ka, int free) {
+        const int nleaf = (b - a + L - 1) / L;
+        if (nleaf <= 1) {
+            restore(ka);
+            if (a > 0) copy_dd(chunk, ckpt_strips(snaps, P, ka + 1), cs, st);   // strips of U[a - 1]
+            leaf(a, b);
+            return;
+        }
+        if (free > 0) {
+            const int k = count - free, m = a + L * ((nleaf + 1) / 2);
+            restore(ka);
+            replay(a, m, [&](int it) { return (void*)(it == m - 1 ? ckpt_strips(snaps, P, k + 1) : nullptr); });
+            save(k);
+            process(m, b, k, free - 1);
+            process(a, m, ka, free);
+            return;
+        }
+        for (int c0 = a + (nleaf - 1) * L; c0 >= a; c0 -= L) {
+            restore(ka);
+            if (c0 > a)
+                replay(a, c0, [&](int it) { return (void*)(it == c0 - 1 ? chunk : nullptr); });
+            else if (a > 0)
+                copy_dd(chunk, ckpt_strips(snaps, P, ka + 1), cs, st);
+            leaf(c0, std::min(b, c0 + L));
+        }
+    };
+    SWEEP_REQUIRE(count >= 1, "acoustic3d: the recursive checkpoint budget must be >= 1");
+    process(0, P.nt, -1, count);
+}
+
 void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const float* adj, const void* tape,
               float* grad_vp, float* grad_w, float* illum_s, float* illum_r,
               void* ws, int64_t ws_bytes, cudaStream_t st)
@@ -1314,6 +1398,7 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     SWEEP_REQUIRE(adj != nullptr || d->nrec == 0, "acoustic3d backward: null record cotangent");
     SWEEP_REQUIRE((illum_s == nullptr) == (illum_r == nullptr), "acoustic3d backward: pass both illuminations or neither");
     const bool ckpt = mem_mode == SWEEP_MEM_CHECKPOINT;
+    const bool recursive = mem_mode == SWEEP_MEM_RECURSIVE;
     Params P = make_params(d);
     set_store(P, mem_mode);
     Carve c(ws);
@@ -1321,8 +1406,10 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     // buffers each), 15-17 reconstruction, 18-19 Kahan slots, 20-21
     // illumination; checkpoint mode: 22-33 the forward set of the replay,
     // then the strips of one chunk
-    Work w = carve(c, P, ckpt ? kRevFields + kFwdFields : kRevFields);
-    float* chunk = ckpt ? c.take<float>((long long)(ckpt_every + 1) * P.B * P.nstrip) : nullptr;
+    Work w = carve(c, P, (ckpt || recursive) ? kRevFields + kFwdFields : kRevFields);
+    float* chunk = ckpt ? c.take<float>((long long)(ckpt_every + 1) * P.B * P.nstrip)
+                 : recursive ? c.take<float>((long long)(SWEEP_RECURSIVE_LEAF + 1) * P.B * P.nstrip) : nullptr;
+    char* snaps = recursive ? c.take<char>((long long)ckpt_every * ckpt_stride(P)) : nullptr;
     const long long rows = (long long)d->nz * d->ny;
     prep_call(d, P, w, st);
     const long long n = (long long)P.B * P.S;
@@ -1363,7 +1450,7 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     // Reverse steps [it0, it1) top down from prev = U[it1] (f[15]), now =
     // U[it1 - 1] (f[16]); strips_of(t) holds the strips of U[t].
     HostRing hr;
-    const bool host = P.st.host && !ckpt;
+    const bool host = P.st.host && !ckpt && !recursive;
     auto reverse = [&](int it0, int it1, auto strips_of) {
         StepGraphs sg(st, host ? 0 : P.graph_steps);
         int rp = 15, rn = 16, rx = 17;
@@ -1409,7 +1496,9 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
         }
         sg.flush();
     };
-    if (!ckpt) {
+    if (recursive) {
+        backward_recursive(d, P, w, chunk, snaps, ckpt_every, st, reverse);
+    } else if (!ckpt) {
         const float* last = tape_last(const_cast<void*>(tape), P);
         SWEEP_CUDA(cudaMemcpyAsync(w.f[15], last + n, n * 4, cudaMemcpyDefault, st));   // prev = U[nt]
         SWEEP_CUDA(cudaMemcpyAsync(w.f[16], last, n * 4, cudaMemcpyDefault, st));       // now  = U[nt-1]

@@ -41,6 +41,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 #include <vector>
 
 #include "common.cuh"
@@ -1456,14 +1457,17 @@ static void check_mode(int mem_mode, int ckpt_every)
 {
     if (mem_mode & SWEEP_MEM_HOST_TAPE) {
         mem_mode &= ~SWEEP_MEM_HOST_TAPE;
-        SWEEP_REQUIRE(mem_mode != SWEEP_MEM_CHECKPOINT, "elastic2d: a host tape goes with boundary saving only");
+        SWEEP_REQUIRE(mem_mode != SWEEP_MEM_CHECKPOINT && mem_mode != SWEEP_MEM_RECURSIVE,
+                      "elastic2d: a host tape goes with boundary saving only");
     }
     SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY || mem_mode == SWEEP_MEM_CHECKPOINT ||
                       mem_mode == SWEEP_MEM_BOUNDARY_FP16 || mem_mode == SWEEP_MEM_BOUNDARY_BF16 ||
-                      mem_mode == SWEEP_MEM_BOUNDARY_INT8,
+                      mem_mode == SWEEP_MEM_BOUNDARY_INT8 || mem_mode == SWEEP_MEM_RECURSIVE,
                   "elastic2d: unknown memory mode %d", mem_mode);
     SWEEP_REQUIRE(mem_mode != SWEEP_MEM_CHECKPOINT || ckpt_every >= 1,
                   "elastic2d: checkpoint interval must be >= 1 (got %d)", ckpt_every);
+    SWEEP_REQUIRE(mem_mode != SWEEP_MEM_RECURSIVE || ckpt_every >= 1,
+                  "elastic2d: the recursive checkpoint budget must be >= 1 (got %d)", ckpt_every);
 }
 
 void schedule_of(const sweep_elastic_desc* d, sweep_b200_schedule* out)
@@ -1488,6 +1492,10 @@ void sizes(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, int64_t* w
     if (mem_mode == SWEEP_MEM_CHECKPOINT) {
         carve_rev_ckpt(cr, pl, ckpt_every, rw);
         *tape = (int64_t)std::max(nchunks(pl, ckpt_every) - 1, 1) * ckpt_stride(pl);
+    } else if (mem_mode == SWEEP_MEM_RECURSIVE) {
+        carve_rev_ckpt(cr, pl, SWEEP_RECURSIVE_LEAF, rw);
+        cr.take<char>((long long)ckpt_every * ckpt_stride(pl));         // the snapshot slots
+        *tape = 256;                                                     // nothing is kept
     } else {
         carve_rev(cr, pl, rw);
         *tape = tape_bytes(pl);
@@ -1548,6 +1556,7 @@ void forward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, float* r
     A.record = record;
     const Geo& G = pl.G;
     const long long n = (long long)G.B * G.S;
+    if (mem_mode == SWEEP_MEM_RECURSIVE) tape = nullptr;     // the backward replays from the initial state
     if (mem_mode != SWEEP_MEM_CHECKPOINT) {
         HostRing hr;
         const bool host = tape && pl.host_tape;
@@ -1589,12 +1598,17 @@ void backward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, const f
     SWEEP_REQUIRE(grad_vp && grad_vs && grad_rho, "elastic2d backward: null gradient output");
     SWEEP_REQUIRE(adj != nullptr || d->nrec == 0, "elastic2d backward: null adjoint source");
     const bool ckpt = mem_mode == SWEEP_MEM_CHECKPOINT;
+    const bool recursive = mem_mode == SWEEP_MEM_RECURSIVE;
     Plan pl = make_plan(d);
     set_store(pl, mem_mode);
     Carve c(ws);
     RevWs w{};
+    char* snaps = nullptr;
     if (ckpt) carve_rev_ckpt(c, pl, ckpt_every, w);
-    else carve_rev(c, pl, w);
+    else if (recursive) {
+        carve_rev_ckpt(c, pl, SWEEP_RECURSIVE_LEAF, w);
+        snaps = c.take<char>((long long)ckpt_every * ckpt_stride(pl));
+    } else carve_rev(c, pl, w);
     SWEEP_REQUIRE(ws != nullptr && c.off <= ws_bytes, "elastic2d backward: workspace too small (%lld < %lld bytes)",
                   (long long)ws_bytes, (long long)c.off);
     SWEEP_CUDA(cudaMemsetAsync(w.zero0, 0, w.zero1 - w.zero0, st));
@@ -1616,7 +1630,7 @@ void backward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, const f
     // it = 0 step) on the reconstruction state after step it1 - 1;
     // strips_of(t) holds the strips of the state after step t.
     HostRing hr;
-    const bool host = pl.host_tape && !ckpt;
+    const bool host = pl.host_tape && !ckpt && !recursive;
     auto reverse = [&](int it0, int it1, auto strips_of) {
         StepGraphs gs(st, host ? 0 : pl.graph_steps);
         for (int it = it1 - 1; it >= std::max(it0, 1); --it) {
@@ -1639,7 +1653,80 @@ void backward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, const f
         }
         gs.flush();
     };
-    if (!ckpt) {
+    if (recursive) {
+        // Recursive checkpointing (SWEEP_MEM_RECURSIVE): the bisection of the
+        // acoustic drivers (acoustic2d.cu backward_recursive); a snapshot slot
+        // is the checkpoint layout (five fields, eight CPML slabs, strips of the
+        // step before), the replay runs straight into the reconstruction fields
+        // as in the checkpoint mode, leaves are SWEEP_RECURSIVE_LEAF steps.
+        const int L = SWEEP_RECURSIVE_LEAF, count = ckpt_every;
+        const long long cs = (long long)G.B * 5 * G.nstrip;
+        FwdArgs F{};
+        F.G = G;
+        F.m = A.m;
+        for (int f = 0; f < 5; ++f) F.f[f] = w.f[f];
+        F.mem = w.fmem;
+        F.record = nullptr;
+        auto restore = [&](int k) {
+            if (k < 0) {
+                for (int f = 0; f < 5; ++f) SWEEP_CUDA(cudaMemsetAsync(w.f[f], 0, sizeof(float) * n, st));
+                for (int s2 = 0; s2 < 4; ++s2) {
+                    SWEEP_CUDA(cudaMemsetAsync(w.fmem.x[s2], 0, sizeof(float) * G.B * G.nz * G.WX, st));
+                    SWEEP_CUDA(cudaMemsetAsync(w.fmem.z[s2], 0, sizeof(float) * G.B * G.WZ * G.P, st));
+                }
+            } else {
+                const Ckpt cp = ckpt_at(snaps, pl, k + 1);
+                for (int f = 0; f < 5; ++f)
+                    SWEEP_CUDA(cudaMemcpyAsync(w.f[f], cp.f[f], sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+                slabs_copy(w.fmem, cp.mem, G, false, st);
+            }
+        };
+        auto save = [&](int k) {
+            const Ckpt cp = ckpt_at(snaps, pl, k + 1);
+            for (int f = 0; f < 5; ++f)
+                SWEEP_CUDA(cudaMemcpyAsync(cp.f[f], w.f[f], sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+            slabs_copy(w.fmem, cp.mem, G, true, st);
+        };
+        auto strips_from = [&](int k) {        // strips of the step before snapshot k into chunk slot 0
+            SWEEP_CUDA(cudaMemcpyAsync(w.chunk, ckpt_at(snaps, pl, k + 1).strips, sizeof(float) * cs,
+                                       cudaMemcpyDeviceToDevice, st));
+        };
+        auto leaf = [&](int a, int e) {
+            forward_steps(F, a, e, [&](int it) { return w.chunk + (long long)(it - a + 1) * cs; }, nullptr, st,
+                          pl.graph_steps);
+            reverse(a, e, [&](int t) { return (const float*)w.chunk + (long long)(t - (a - 1)) * cs; });
+        };
+        std::function<void(int, int, int, int)> process = [&](int a, int b, int ka, int free) {
+            const int nleaf = (b - a + L - 1) / L;
+            if (nleaf <= 1) {
+                restore(ka);
+                if (a > 0) strips_from(ka);
+                leaf(a, b);
+                return;
+            }
+            if (free > 0) {
+                const int k = count - free, m = a + L * ((nleaf + 1) / 2);
+                restore(ka);
+                float* ks = ckpt_at(snaps, pl, k + 1).strips;
+                forward_steps(F, a, m, [&](int it) { return it == m - 1 ? ks : nullptr; }, nullptr, st,
+                              pl.graph_steps);
+                save(k);
+                process(m, b, k, free - 1);
+                process(a, m, ka, free);
+                return;
+            }
+            for (int c0 = a + (nleaf - 1) * L; c0 >= a; c0 -= L) {
+                restore(ka);
+                if (c0 > a)
+                    forward_steps(F, a, c0, [&](int it) { return it == c0 - 1 ? w.chunk : nullptr; }, nullptr, st,
+                                  pl.graph_steps);
+                else if (a > 0)
+                    strips_from(ka);
+                leaf(c0, std::min(b, c0 + L));
+            }
+        };
+        process(0, G.nt, -1, count);
+    } else if (!ckpt) {
         const float* last = tape_last(const_cast<void*>(tape), pl);
         for (int k = 0; k < 5; ++k)
             SWEEP_CUDA(cudaMemcpyAsync(w.f[k], last + k * n, sizeof(float) * n, cudaMemcpyDefault, st));

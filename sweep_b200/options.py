@@ -63,13 +63,29 @@ class Full:
 
 @dataclass(frozen=True)
 class Ckpt:
-    """Checkpoint the forward state every ``chunks`` steps and re-run each
-    chunk during the backward."""
+    """Checkpointing, the reference's two modes (``options.py:346-370``):
+
+    * ``mode='chunk'`` (default): checkpoint the forward state every
+      ``chunks`` steps and re-run each chunk during the backward;
+    * ``mode='recursive'``: keep nothing from the forward; the backward
+      bisects the time axis holding at most ``count`` forward states at once,
+      replays each 64-step leaf from the nearest one and reverses it (the
+      gradient equals ``Ckpt(chunks=64)``'s; memory is ``count`` states
+      instead of ``nt / chunks``, at the price of more replayed steps)."""
     chunks: int = 100
     mode: str = "chunk"
+    count: int = 0
 
     def __post_init__(self):
-        if int(self.chunks) < 1:
-            raise ValueError("Ckpt(chunks) must be >= 1")
-        if self.mode != "chunk":
-            raise NotImplementedError("sweep_b200 implements chunked checkpointing (mode='chunk')")
+        if self.mode == "chunk":
+            if int(self.chunks) < 1:
+                raise ValueError("Ckpt(chunks) must be >= 1")
+            if int(self.count) != 0:
+                raise ValueError("Ckpt.count is only valid when mode='recursive'.")
+        elif self.mode == "recursive":
+            if int(self.count) < 1:
+                raise ValueError("Ckpt.count must be >= 1 when mode='recursive'.")
+            if int(self.chunks) != 100:
+                raise ValueError("Ckpt.chunks is only valid when mode='chunk'.")
+        else:
+            raise ValueError("Ckpt.mode must be 'chunk' or 'recursive'.")

@@ -448,6 +448,8 @@ class PropTorch(torch.nn.Module):
 
     def _mem_mode(self):
         if isinstance(self.memory, Ckpt):
+            if self.memory.mode == "recursive":
+                return _lib.MEM_RECURSIVE, int(self.memory.count)
             return _lib.MEM_CHECKPOINT, int(self.memory.chunks)
         sd = getattr(self.memory, "storage_dtype", "fp32")
         mode = {"fp32": _lib.MEM_BOUNDARY, "fp16": _lib.MEM_BOUNDARY_FP16, "bf16": _lib.MEM_BOUNDARY_BF16,
@@ -475,7 +477,8 @@ class PropTorch(torch.nn.Module):
         mem = self.memory
         budget = getattr(mem, "budget_gb", None)
         if budget is None:
-            self.last_memory = {"mode": "checkpoint" if mem_mode == _lib.MEM_CHECKPOINT else "boundary",
+            self.last_memory = {"mode": {_lib.MEM_CHECKPOINT: "checkpoint",
+                                         _lib.MEM_RECURSIVE: "recursive"}.get(mem_mode, "boundary"),
                                 "chunks": ckpt_every or None}
             return mem_mode, ckpt_every
         desc = self._desc(geo, padded, wb, fields)

@@ -242,3 +242,25 @@ def test_schedule_table_is_host_only_and_keyed_by_shape():
     finally:
         autotune.clear_schedules()
     assert autotune.get_schedule(_desc(B=8, nz=120, nx=200)) == base
+
+
+def test_recursive_checkpoint_options_and_sizes():
+    """Ckpt(mode='recursive', count=N) follows the reference's option rules;
+    its tape is a token (nothing is kept from the forward) and its workspace
+    grows by one snapshot per unit of budget."""
+    from sweep_b200 import Ckpt, _lib
+    assert Ckpt(mode="recursive", count=3).count == 3
+    with pytest.raises(ValueError):
+        Ckpt(mode="recursive")
+    with pytest.raises(ValueError):
+        Ckpt(chunks=10, count=2)
+    with pytest.raises(ValueError):
+        Ckpt(mode="revolve", count=2)
+    d = _desc(B=2, nz=40, nx=60, nt=300)
+    ws1, ws2, tape = _lib.c_i64(), _lib.c_i64(), _lib.c_i64()
+    _lib.call("sweep_b200_acoustic_sizes", d, _lib.MEM_RECURSIVE, 1, ws1, tape)
+    assert tape.value <= 256
+    _lib.call("sweep_b200_acoustic_sizes", d, _lib.MEM_RECURSIVE, 5, ws2, tape)
+    assert ws2.value > ws1.value
+    with pytest.raises(RuntimeError, match="budget"):
+        _lib.call("sweep_b200_acoustic_sizes", d, _lib.MEM_RECURSIVE, 0, ws1, tape)

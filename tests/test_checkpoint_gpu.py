@@ -94,3 +94,47 @@ def test_tape_budget_switches_to_checkpoints(case, eq_name):
     p_small, g_small = _acoustic(d, BoundarySaving(budget_gb=1e-6, ckpt_chunks=29), eq)
     assert np.array_equal(p_big, p_bs) and np.array_equal(g_big, g_bs)
     assert np.array_equal(p_small, p_ck) and np.array_equal(g_small, g_ck)
+
+
+@pytest.mark.parametrize("case,eq_name,count", [
+    ("acoustic2d_multi", "Acoustic", 1), ("acoustic2d_multi", "Acoustic", 8),
+    ("acoustic2d_c1", "Acoustic", 2), ("acoustic2d_c1", "Acoustic", 3),
+    ("acoustic3d", "Acoustic3D", 1), ("acoustic3d", "Acoustic3D", 4),
+])
+def test_acoustic_recursive_checkpointing(case, eq_name, count):
+    """Ckpt(mode='recursive', count=N): the backward bisects the time axis
+    with at most N snapshots and reverses 64-step leaves, the chunks of
+    Ckpt(chunks=64) -- records and gradients bit-identical to that mode (a
+    budget too small for the bisection depth replays leaves from the nearest
+    snapshot), and within the bars of the reference."""
+    import sweep_b200
+    from sweep_b200 import Ckpt
+    eq = getattr(sweep_b200, eq_name)
+    d = load(case)
+    p_ck, g_ck = _acoustic(d, Ckpt(chunks=64), eq)
+    p_rc, g_rc = _acoustic(d, Ckpt(mode="recursive", count=count), eq)
+    assert np.array_equal(p_rc, p_ck)
+    assert np.array_equal(g_rc, g_ck)
+    assert rel(g_rc, d["grad_vp"]) < GRAD_TOL
+
+
+@pytest.mark.parametrize("count", [1, 3])
+def test_elastic_recursive_checkpointing(count):
+    from sweep_b200 import Ckpt, Elastic, PropTorch
+    d = load("elastic2d")
+
+    def run(memory):
+        s = PropTorch(Elastic(spatial_order=8, device=DEV), shape=tuple(d["vp_true"].shape), dh=float(d["dh"]),
+                      dt=float(d["dt"]), abcn=int(d["abcn"]), device=DEV, memory=memory)
+        ms = [torch.tensor(d[k], device=DEV, requires_grad=True) for k in ("vp_init", "vs_init", "rho_init")]
+        pred = s(torch.tensor(d["wavelet"], device=DEV), d["src"], d["rec"], models=ms)
+        (0.5 * ((pred - torch.tensor(d["obs"], device=DEV)) ** 2).sum()).backward()
+        torch.cuda.synchronize()
+        return pred.detach().cpu().numpy(), [m.grad.cpu().numpy() for m in ms]
+
+    p_ck, g_ck = run(Ckpt(chunks=64))
+    p_rc, g_rc = run(Ckpt(mode="recursive", count=count))
+    assert np.array_equal(p_rc, p_ck)
+    for a, b, ref in zip(g_rc, g_ck, ("grad_vp", "grad_vs", "grad_rho")):
+        assert np.array_equal(a, b)
+        assert rel(a, d[ref]) < GRAD_TOL
