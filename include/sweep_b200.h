@@ -100,8 +100,9 @@ typedef struct sweep_acoustic_desc {
 /* Bytes the caller must allocate: `workspace` (scratch, reusable between calls
  * once the previous call has finished on its stream) and `tape` (written by
  * the forward, read by the backward; keep it between the two).  `mem_mode` is
- * SWEEP_MEM_BOUNDARY or SWEEP_MEM_CHECKPOINT; `ckpt_every` the checkpoint
- * interval (ignored for boundary saving).  Host-side only, no device work. */
+ * one of the SWEEP_MEM_* modes above; `ckpt_every` the checkpoint interval
+ * (SWEEP_MEM_CHECKPOINT), the snapshot budget (SWEEP_MEM_RECURSIVE), else
+ * ignored.  Host-side only, no device work. */
 SWEEP_B200_API int sweep_b200_acoustic_sizes(const sweep_acoustic_desc* d, int32_t mem_mode, int32_t ckpt_every,
                               int64_t* workspace_bytes, int64_t* tape_bytes,
                               char* err, int32_t err_cap);
