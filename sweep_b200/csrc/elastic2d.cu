@@ -92,7 +92,9 @@ struct Geo {
     float dt, idx, idz;
     const float *az, *bz, *azh, *bzh, *ax, *bx, *axh, *bxh;
     int nsrc, nrec, nsf, nrf;
-    int sf[5], rf[5];
+    int sf[5], rf[5];               // stress source fields (nsf), receiver fields (nrf)
+    int nvf, vf[2];                 // velocity (body-force) source fields
+    const int *src_loc, *rec_loc;   // (B, nsrc, 2), (B, nrec, 2) runtime (x, z)
     long long ms;                   // model stride between shots (0 or S)
     EventTable src, rec;
     const float* wavelet;           // (B, nsrc, nt)
@@ -622,6 +624,78 @@ __global__ void __launch_bounds__(NTH, 4) fwd_str(const __grid_constant__ FwdMap
     }
 }
 
+// Body-force (velocity) sources, forward (reference sg_driver inject_source on
+// a velocity field, common.cu:11-36): after the stress step, add the wavelet to
+// vx / vz at each source cell of shot blockIdx.x, then -- that cell's step
+// outputs having been written before the injection by fwd_str -- store the
+// injected value again into the step's boundary strips (fp32 or bf16 here;
+// the scaled formats are quantised from this fp32 slot afterwards) and into
+// the record of any receiver on the cell.  A separate launch: every fwd_str
+// CTA reads the velocities of its halo, which the injection must not race.
+__global__ void vsrc_forward(const Geo G, float* vx, float* vz, void* strips, float* record, int it)
+{
+    const int b = blockIdx.x;
+    const long long so = (long long)b * G.S;
+    float* const vf[2] = {vx, vz};
+    for (int s = threadIdx.x; s < G.nsrc; s += blockDim.x) {
+        const int ix = G.src_loc[2 * ((long long)b * G.nsrc + s)], iz = G.src_loc[2 * ((long long)b * G.nsrc + s) + 1];
+        if (ix < 0 || ix >= G.nx || iz < 0 || iz >= G.nz) continue;
+        const float w = G.wavelet[((long long)b * G.nsrc + s) * G.nt + it];
+        for (int k = 0; k < G.nvf; ++k) atomicAdd(vf[G.vf[k]] + so + (long long)iz * G.P + ix, w);
+    }
+    __syncthreads();                          // the injected values are visible to the block
+    for (int s = threadIdx.x; strips && s < G.nsrc; s += blockDim.x) {
+        const int ix = G.src_loc[2 * ((long long)b * G.nsrc + s)], iz = G.src_loc[2 * ((long long)b * G.nsrc + s) + 1];
+        if (ix < 0 || ix >= G.nx || iz < 0 || iz >= G.nz) continue;
+        const int si = strip_index(G, iz, ix);
+        if (si < 0) continue;
+        for (int k = 0; k < G.nvf; ++k) {
+            const int fld = G.vf[k];
+            const float v = vf[fld][so + (long long)iz * G.P + ix];
+            const long long e = ((long long)b * 5 + fld) * G.nstrip + si;
+            if (G.st.fmt == SF_BF16) static_cast<__nv_bfloat16*>(strips)[e] = __float2bfloat16(v);
+            else static_cast<float*>(strips)[e] = v;
+        }
+    }
+    for (int r = threadIdx.x; record && r < G.nrec; r += blockDim.x) {
+        const int ix = G.rec_loc[2 * ((long long)b * G.nrec + r)], iz = G.rec_loc[2 * ((long long)b * G.nrec + r) + 1];
+        if (ix < 0 || ix >= G.nx || iz < 0 || iz >= G.nz) continue;
+        bool on_source = false;
+        for (int s = 0; s < G.nsrc && !on_source; ++s)
+            on_source = G.src_loc[2 * ((long long)b * G.nsrc + s)] == ix && G.src_loc[2 * ((long long)b * G.nsrc + s) + 1] == iz;
+        if (!on_source) continue;
+        float* out = record + ((long long)(b * G.nt + it) * G.nrec + r) * G.nrf;
+        for (int k = 0; k < G.nrf; ++k)
+            if (G.rf[k] <= VZ) out[k] = vf[G.rf[k]][so + (long long)iz * G.P + ix];
+    }
+}
+
+// Body-force sources, reverse step it (reference fix_rho_grad_at_sources,
+// common.cu:40-75, then uninject_forward_source; elastic2d/driver_traits.cuh
+// 380-410): before this step's residuals enter the adjoint, add
+// (adjoint v * w) / rho to the rho-gradient slot of the shot at each source
+// cell, and take the wavelet back out of the reconstructed vx / vz there.
+__global__ void vsrc_reverse(const Geo G, const float* avx, const float* avz, float* vx, float* vz,
+                             float* grho, const float* rho, int g_shots, int it)
+{
+    const int b = blockIdx.x;
+    const long long so = (long long)b * G.S;
+    const float* const av[2] = {avx, avz};
+    float* const vf[2] = {vx, vz};
+    float* const gslot = grho + (long long)(b / g_shots) * G.S;
+    for (int s = threadIdx.x; s < G.nsrc; s += blockDim.x) {
+        const int ix = G.src_loc[2 * ((long long)b * G.nsrc + s)], iz = G.src_loc[2 * ((long long)b * G.nsrc + s) + 1];
+        if (ix < 0 || ix >= G.nx || iz < 0 || iz >= G.nz) continue;
+        const long long c = (long long)iz * G.P + ix;
+        const float w = G.wavelet[((long long)b * G.nsrc + s) * G.nt + it];
+        for (int k = 0; k < G.nvf; ++k) {
+            const int fld = G.vf[k];
+            atomicAdd(gslot + c, (av[fld][so + c] * w) / rho[(long long)b * G.ms + c]);
+            atomicAdd(vf[fld] + so + c, -w);
+        }
+    }
+}
+
 // ------------------------------------------------------------------ reverse
 struct RevArgs {
     Geo G;
@@ -1103,10 +1177,13 @@ static Plan make_plan(const sweep_elastic_desc* d)
     SWEEP_REQUIRE(d->M == M, "elastic2d: only spatial order 8 (M = 4) is built (got M = %d)", d->M);
     SWEEP_REQUIRE(d->B >= 1 && d->nt >= 1, "elastic2d: B and nt must be >= 1");
     SWEEP_REQUIRE(d->nsrc >= 0 && d->nrec >= 0, "elastic2d: negative source/receiver count");
-    SWEEP_REQUIRE(d->nsrc_fields >= 1 && d->nsrc_fields <= 3, "elastic2d: 1 to 3 source fields (got %d)", d->nsrc_fields);
-    for (int k = 0; k < d->nsrc_fields; ++k)
-        SWEEP_REQUIRE(d->src_fields[k] >= SXX && d->src_fields[k] <= SXZ,
-                      "elastic2d: source field %d is not built (stress fields sxx, szz, sxz only)", d->src_fields[k]);
+    SWEEP_REQUIRE(d->nsrc_fields >= 1 && d->nsrc_fields <= 5, "elastic2d: 1 to 5 source fields (got %d)", d->nsrc_fields);
+    for (int k = 0; k < d->nsrc_fields; ++k) {
+        SWEEP_REQUIRE(d->src_fields[k] >= VX && d->src_fields[k] <= SXZ, "elastic2d: bad source field %d",
+                      d->src_fields[k]);
+        for (int j = 0; j < k; ++j)
+            SWEEP_REQUIRE(d->src_fields[j] != d->src_fields[k], "elastic2d: source field %d repeated", d->src_fields[k]);
+    }
     SWEEP_REQUIRE(d->nrec_fields >= 1 && d->nrec_fields <= 5, "elastic2d: 1 to 5 receiver fields (got %d)", d->nrec_fields);
     for (int k = 0; k < d->nrec_fields; ++k)
         SWEEP_REQUIRE(d->rec_fields[k] >= 0 && d->rec_fields[k] <= SXZ, "elastic2d: bad receiver field %d", d->rec_fields[k]);
@@ -1131,8 +1208,16 @@ static Plan make_plan(const sweep_elastic_desc* d)
     G.dt = d->dt; G.idx = 1.f / d->dx; G.idz = 1.f / d->dz;
     G.az = d->az; G.bz = d->bz; G.azh = d->azh; G.bzh = d->bzh;
     G.ax = d->ax; G.bx = d->bx; G.axh = d->axh; G.bxh = d->bxh;
-    G.nsrc = d->nsrc; G.nrec = d->nrec; G.nsf = d->nsrc_fields; G.nrf = d->nrec_fields;
-    for (int k = 0; k < 5; ++k) { G.sf[k] = d->src_fields[k]; G.rf[k] = d->rec_fields[k]; }
+    G.nsrc = d->nsrc; G.nrec = d->nrec; G.nrf = d->nrec_fields;
+    for (int k = 0; k < 5; ++k) G.rf[k] = d->rec_fields[k];
+    // stress sources are added inside the stress kernels; velocity (body-force)
+    // sources by vsrc_forward / vsrc_reverse around them
+    G.nsf = G.nvf = 0;
+    for (int k = 0; k < d->nsrc_fields; ++k) {
+        if (d->src_fields[k] >= SXX) G.sf[G.nsf++] = d->src_fields[k];
+        else G.vf[G.nvf++] = d->src_fields[k];
+    }
+    G.src_loc = d->src_loc; G.rec_loc = d->rec_loc;
     const bool per_shot = d->model_stride != 0;
     SWEEP_REQUIRE(!per_shot || d->model_stride == (int64_t)d->nz * d->nx,
                   "elastic2d: model_stride must be 0 or nz * nx");
@@ -1524,6 +1609,7 @@ static void forward_steps(FwdArgs& A, int it0, int it1, StripsOf strips_of, floa
         fwd_vel<<<grid, block, SM_FWD_VEL, ls>>>(maps, A);
         if (slot && hr) hr->before_write(it);
         fwd_str<<<grid, block, SM_FWD_STR, ls>>>(maps, A);
+        if (G.nvf) vsrc_forward<<<G.B, 128, 0, ls>>>(G, A.f[VX], A.f[VZ], A.strips, A.record, it);
         if (slot && scaled) quantize_strips<<<qblocks, kQB, 0, ls>>>(G, scratch, slot);
         if (slot && hr) hr->after_write(it);
         SWEEP_LAUNCH_CHECK();
@@ -1640,6 +1726,8 @@ void backward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, const f
             A.mn = w.m[cur ^ 1];
             if (host) hr.before_read(it - 1);
             const cudaStream_t ls = gs.stream();
+            if (G.nvf)
+                vsrc_reverse<<<G.B, 128, 0, ls>>>(G, A.a[VX], A.a[VZ], A.f[VX], A.f[VZ], A.grho, A.m.rho, A.G_shots, it);
             rev_str<<<grid_s, block, SM_REV_STR, ls>>>(A);
             rev_sadj<<<grid_b, block, SM_REV_SADJ, ls>>>(A);
             rev_vadj<<<grid_b, block, SM_REV_VADJ, ls>>>(A);

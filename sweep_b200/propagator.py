@@ -439,9 +439,6 @@ class PropTorch(torch.nn.Module):
             if not kinds or missing:
                 raise ValueError(f"Invalid {role} entries {missing or kinds}; available wavefields are {names}")
         sf = [names.index(k) for k in self.source_type]
-        if any(f < 2 for f in sf):
-            raise NotImplementedError("sweep_b200: velocity (body-force) sources are not built; "
-                                      "use stress source fields (sxx, szz, sxz)")
         if len(set(sf)) != len(sf) or len(self.receiver_type) > 5:
             raise ValueError("source_type / receiver_type must not repeat a field")
         return sf, [names.index(k) for k in self.receiver_type]

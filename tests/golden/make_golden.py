@@ -300,6 +300,40 @@ def elastic2d():
     )
 
 
+def elastic2d_vsrc():
+    """Isotropic elastic with body-force (velocity) sources on vx and vz: shot
+    0 has its source inside the boundary-strip band and a receiver on the
+    source cell; (vx, vz, sxx) receivers; vp/vs/rho gradients."""
+    rng = np.random.default_rng(11)
+    nz, nx, nt, dt, dh, abcn = 40, 56, 300, 0.0005, 5.0, 10
+    vp_true = _layered(nz, nx, rng, 1800.0, 3200.0, 4)
+    vs_true = (vp_true / 1.73).astype(np.float32)
+    rho_true = (310.0 * vp_true ** 0.25).astype(np.float32)
+    vp_init = np.full((nz, nx), 2200.0, np.float32)
+    vs_init = (vp_init / 1.73).astype(np.float32)
+    rho_init = (310.0 * vp_init ** 0.25).astype(np.float32)
+    w = _wavelet(nt, dt, 25.0, 0.04)
+    src = np.array([[14, 2], [40, 9]], np.int64)
+    rec = np.zeros((2, 8, 2), np.int64)
+    for b in range(2):
+        rec[b, :, 0] = np.linspace(3, nx - 4, 8).astype(np.int64)
+        rec[b, :, 1] = 3 + b
+    rec[0, 0] = (14, 2)                       # a receiver on shot 0's source cell
+    eq = Elastic(spatial_order=8, device="cpu")
+    solver = PropTorch(eq, shape=(nz, nx), dh=dh, dt=dt, abcn=abcn, impl="c", device="cpu",
+                       memory=BoundarySaving(), source_type=["vx", "vz"], receiver_type=["vx", "vz", "sxx"])
+    obs = _forward(solver, w, src, rec, [vp_true, vs_true, rho_true])
+    r = _run(solver, w, src, rec, [vp_init, vs_init, rho_init], obs, False)
+    np.savez_compressed(
+        OUT / "elastic2d_vsrc.npz",
+        nz=nz, nx=nx, nt=nt, dt=dt, dh=dh, abcn=abcn, order=8,
+        vp_true=vp_true, vs_true=vs_true, rho_true=rho_true,
+        vp_init=vp_init, vs_init=vs_init, rho_init=rho_init,
+        wavelet=w, src=src, rec=rec, obs=obs, pred=r["pred"], loss=r["loss"],
+        grad_vp=r["grad0"], grad_vs=r["grad1"], grad_rho=r["grad2"],
+    )
+
+
 def elastic2d_storage():
     """Elastic boundary saving with fp16 / bf16 / int8 strips (reference
     BoundarySaving(storage_dtype=...): each of the five fields quantised per
@@ -436,6 +470,7 @@ CASES = {
     "acoustic3d_storage": acoustic3d_storage,
     "elastic2d": elastic2d,
     "elastic2d_storage": elastic2d_storage,
+    "elastic2d_vsrc": elastic2d_vsrc,
 }
 
 if __name__ == "__main__":

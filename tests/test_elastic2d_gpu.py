@@ -126,12 +126,32 @@ def test_wavelet_gradient_and_second_backward_are_refused():
         loss.backward()
 
 
-def test_velocity_sources_are_refused():
-    d = load("elastic2d")
-    s = _solver(tuple(d["vp_true"].shape), float(d["dh"]), float(d["dt"]), int(d["abcn"]), source_type=["vz"])
-    ms = [torch.tensor(d[k], device=DEV) for k in ("vp_init", "vs_init", "rho_init")]
-    with pytest.raises(NotImplementedError, match="velocity"):
-        s(torch.tensor(d["wavelet"], device=DEV), d["src"], d["rec"], models=ms)
+@pytest.mark.parametrize("memory", ["boundary", "ckpt", "recursive"])
+def test_velocity_sources_match_reference_golden(memory):
+    """Body-force sources on vx and vz (shot 0's inside the boundary strips,
+    with a receiver on its cell), (vx, vz, sxx) receivers: records within
+    1e-4 and vp / vs / rho gradients within 1e-3 of the reference, in every
+    memory mode, and against the float64 oracle."""
+    from sweep_b200 import BoundarySaving, Ckpt
+    d = load("elastic2d_vsrc")
+    mem = {"boundary": BoundarySaving(), "ckpt": Ckpt(chunks=41),
+           "recursive": Ckpt(mode="recursive", count=2)}[memory]
+    s = _solver(tuple(d["vp_true"].shape), float(d["dh"]), float(d["dt"]), int(d["abcn"]),
+                source_type=["vx", "vz"], receiver_type=["vx", "vz", "sxx"], memory=mem)
+    with torch.no_grad():
+        obs = s(torch.tensor(d["wavelet"], device=DEV), d["src"], d["rec"],
+                models=[torch.tensor(d[k], device=DEV) for k in ("vp_true", "vs_true", "rho_true")])
+    assert rel(obs.cpu().numpy(), d["obs"]) < REC_TOL
+    pred, grads = _grad_run(s, d["wavelet"], d["src"], d["rec"], [d["vp_init"], d["vs_init"], d["rho_init"]],
+                            d["obs"])
+    assert rel(pred, d["pred"]) < REC_TOL
+    _, _, g64 = O.elastic_gradient(d["vp_init"], d["vs_init"], d["rho_init"], d["wavelet"], d["src"], d["rec"],
+                                   d["obs"], float(d["dh"]), float(d["dt"]), int(d["abcn"]), prec="f64",
+                                   source_fields=("vx", "vz"), receiver_fields=("vx", "vz", "sxx"))
+    for g, ref, o in zip(grads, ("grad_vp", "grad_vs", "grad_rho"), g64):
+        print(f"velocity sources ({memory}) {ref}: vs reference {rel(g, d[ref]):.2e}, vs fp64 oracle {rel(g, o):.2e}")
+        assert rel(g, d[ref]) < GRAD_TOL
+        assert rel(g, o) < GRAD_TOL
 
 
 def _fd_case():

@@ -113,6 +113,26 @@ def test_elastic2d_oracle_matches_reference(prec, tol):
     assert rel(grho, d["grad_rho"]) < 5 * tol
 
 
+@pytest.mark.parametrize("prec,tol", [("f32", 2e-6), ("f64", 5e-6)])
+def test_elastic2d_velocity_sources_oracle_matches_reference(prec, tol):
+    """Body-force sources on vx and vz (one inside the boundary strips, a
+    receiver on its cell), (vx, vz, sxx) receivers: records and vp / vs / rho
+    gradients, the rho one with the source correction of common.cu:40-75."""
+    d = np.load(GOLD / "elastic2d_vsrc.npz")
+    kw = dict(source_fields=("vx", "vz"), receiver_fields=("vx", "vz", "sxx"))
+    obs = O.elastic_forward(d["vp_true"], d["vs_true"], d["rho_true"], d["wavelet"], d["src"],
+                            d["rec"], *_el_args(d), prec=prec, **kw)
+    assert obs.shape == d["obs"].shape
+    assert rel(obs, d["obs"]) < tol
+    pred, loss, (gvp, gvs, grho) = O.elastic_gradient(
+        d["vp_init"], d["vs_init"], d["rho_init"], d["wavelet"], d["src"], d["rec"], d["obs"],
+        *_el_args(d), prec=prec, **kw)
+    assert rel(pred, d["pred"]) < tol
+    assert rel(gvp, d["grad_vp"]) < 5 * tol
+    assert rel(gvs, d["grad_vs"]) < 5 * tol
+    assert rel(grho, d["grad_rho"]) < 5 * tol
+
+
 def test_elastic2d_reference_full_and_boundary_modes_agree():
     """The reference's full-storage gradient adds the it = 0 image the
     boundary-saving reverse skips; the two differ at the 1e-6 level."""
