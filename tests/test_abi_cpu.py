@@ -112,8 +112,13 @@ def test_elastic_sizes_and_errors():
     pz, px = 40 - 18, 60 - 18
     nstrip = 2 * 4 * px + 2 * (px + 8) + (pz - 2) * 10
     assert tape.value >= (10 * 2 * 5 * nstrip + 5 * n) * 4
-    d.src_fields[0] = 1
-    with pytest.raises(RuntimeError, match="not built"):
+    d.src_fields[0] = 1                               # a body-force (vz) source is built
+    _lib.call("sweep_b200_elastic_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
+    d.src_fields[0] = 7
+    with pytest.raises(RuntimeError, match="bad source field"):
+        _lib.call("sweep_b200_elastic_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
+    d.nsrc_fields, d.src_fields[0], d.src_fields[1] = 2, 3, 3
+    with pytest.raises(RuntimeError, match="repeated"):
         _lib.call("sweep_b200_elastic_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
     d = _edesc(M=2)
     with pytest.raises(RuntimeError, match="order 8"):
