@@ -219,7 +219,9 @@ class AcousticWorkload:
         return solver, [vp_true], [vp_init], w, src, rec
 
     def launches(self):
-        return 2 * self.nt + 1
+        # per gradient: the forward's prep_kernel and one fwd_kernel per step,
+        # the backward's prep_kernel, one rev_kernel per step and finalize_kernel
+        return 2 * self.nt + 3
 
     def cpu_run(self, nt_sample, shots=1):
         """Gradient of `shots` shots with the CPU oracle (float32, OpenMP over
@@ -278,7 +280,9 @@ class AcousticC1Workload:
         return solver, [vp_true], [vp_init], w, src, rec
 
     def launches(self):
-        return 2 * self.nt + 1
+        # per gradient: the forward's prep_kernel and one fwd_kernel per step,
+        # the backward's prep_kernel, one rev_kernel per step and finalize_kernel
+        return 2 * self.nt + 3
 
     def cpu_run(self, nt_sample, shots=1):
         from oracle import oracle as O
@@ -414,9 +418,9 @@ class Acoustic3DWorkload:
     def launches(self):
         # per call: forward 4 per step (stencil, strips, injection, gather) and
         # reverse 7 (adjoint, cotangent injection, reconstruction, strip
-        # restore, strip un-injection, strip image, source re-injection), prep
-        # and finalize
-        return -(-self.nshot // self.batch) * (11 * self.nt + 3)
+        # restore, strip un-injection, strip image, source re-injection); per
+        # pass prep3 and three pack_prof3, and finalize3
+        return -(-self.nshot // self.batch) * (11 * self.nt + 9)
 
     def cpu_run(self, nt_sample, shots=1):
         from oracle import oracle as O
