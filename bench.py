@@ -707,8 +707,8 @@ def main():
                     help="acoustic workloads: boundary strip storage format (fp32 is exact)")
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the end-to-end leg (long workloads; the bench line then has no e2e value)")
-    ap.add_argument("--pairs", type=int, default=1024, help="fwi workload: training pairs")
-    ap.add_argument("--train-steps", type=int, default=6000, help="fwi workload: U-Net training steps")
+    ap.add_argument("--pairs", type=int, default=2000, help="fwi workload: training pairs")
+    ap.add_argument("--train-steps", type=int, default=20000, help="fwi workload: U-Net training steps")
     ap.add_argument("--workload", default="acoustic2d", choices=sorted(WORKLOADS) + ["fwi"],
                     help="acoustic2d: the 32-shot 256x768 survey (default); elastic2d: the 16-shot "
                          "400x1200 elastic survey")
