@@ -593,11 +593,16 @@ __device__ __forceinline__ void adj_axis(const Params& P, const float4* __restri
 // NSC3 stages.  A CTA whose columns and planes all lie in the clear box turns
 // the model plane into gw = ((v*v)*dt^2) * lambda in place once per stage;
 // the others form the tap products from the two planes.
+// The adjoint's ring is two stages shorter than the forward's (planes one
+// ahead instead of three), so that four CTAs fit an SM.
+constexpr int NSA = 2 * M + 2;
+constexpr int NSCA = NSA - 2 * M;
+
 struct A3Smem {
-    float l[NS3][PN];
-    float c[NS3][PN];
-    float lp[NSC3][CN3];
-    uint64_t bar[NS3];
+    float l[NSA][PN];
+    float c[NSA][PN];
+    float lp[NSCA][CN3];
+    uint64_t bar[NSA];
 };
 
 struct A3Maps {
@@ -610,7 +615,7 @@ struct A3Maps {
 // pure interior  2 l - l_prev + Lap(gw) (difference form around gw);
 // shell          per axis outside the clear box the transposed CPML terms,
 //                inside it the bare Laplacian of gw.
-__global__ void __launch_bounds__(NTH, 3) a3_step(const __grid_constant__ A3Maps MP, const Params P, const A3 A,
+__global__ void __launch_bounds__(NTH, 4) a3_step(const __grid_constant__ A3Maps MP, const Params P, const A3 A,
                                                   const int lnow, const int lprev, int* err)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -630,9 +635,9 @@ __global__ void __launch_bounds__(NTH, 3) a3_step(const __grid_constant__ A3Maps
     const bool clean = cx0 >= P.qx0 && cx0 + BXC <= P.qx1 && cy0 >= P.qy0 && cy0 + BYC <= P.qy1 &&
                        zb >= P.qz0 && ze <= P.qz1;
     const int q0 = zb - M, q1 = ze + M;
-    auto slot = [&](int q) { return (q - q0) % NS3; };
-    auto cslot = [&](int z) { return (z - zb) % NSC3; };
-    auto parity = [&](int q) { return (uint32_t)(((q - q0) / NS3) & 1); };
+    auto slot = [&](int q) { return (q - q0) % NSA; };
+    auto cslot = [&](int z) { return (z - zb) % NSCA; };
+    auto parity = [&](int q) { return (uint32_t)(((q - q0) / NSA) & 1); };
     auto issue = [&](int q) {
         const int sl = slot(q), z = q - M;
         const bool cen = z >= zb && z < ze;
@@ -642,13 +647,13 @@ __global__ void __launch_bounds__(NTH, 3) a3_step(const __grid_constant__ A3Maps
         if (cen) tma::load_4d(sm.lp[cslot(z)], &MP.lc[lprev], &sm.bar[sl], gx0 + M, gy0 + M, z, b);
     };
     if (tid == 0) {
-        for (int i = 0; i < NS3; ++i) tma::mbar_init(&sm.bar[i], 1);
+        for (int i = 0; i < NSA; ++i) tma::mbar_init(&sm.bar[i], 1);
         tma::fence_barrier_init();
     }
     __syncthreads();
     int next = q0;
     if (tid == 0)
-        for (; next < min(q1, q0 + NS3); ++next) issue(next);
+        for (; next < min(q1, q0 + NSA); ++next) issue(next);
     auto fail = [&](int q) {
         if (tid == 0)
             for (int r = q; r < next; ++r) tma::mbar_wait(&sm.bar[slot(r)], parity(r), err, ERR_WAIT_F3);
@@ -745,7 +750,7 @@ __global__ void __launch_bounds__(NTH, 3) a3_step(const __grid_constant__ A3Maps
             }
         }
         // the last stage every thread has waited for (its slot is not one
-        // plane z reads: the ring holds NS3 > 2M + 2 stages)
+        // plane z reads: the ring holds NSA > 2M + 2 stages)
         int last = z + M;
         if (clean && z + 1 < ze) { await(z + M + 1); convert(z + M + 1); last = z + M + 1; }
         if (__syncthreads_or(bad)) { fail(z == zb && !clean ? q0 : last); return; }
