@@ -269,3 +269,47 @@ def test_recursive_checkpoint_options_and_sizes():
     assert ws2.value > ws1.value
     with pytest.raises(RuntimeError, match="budget"):
         _lib.call("sweep_b200_acoustic_sizes", d, _lib.MEM_RECURSIVE, 0, ws1, tape)
+
+
+def test_autotune_candidates_follow_the_shape():
+    """The tuner's knobs: shot grouping only with several shots sharing a
+    model, z chunks only in 3-D (doubling bounded by 16-plane chunks), graph
+    length only without a host tape; each knob's values include the
+    built-in choice."""
+    from sweep_b200 import _lib, autotune
+    d = _desc(B=8, nz=120, nx=200)
+    base = {"shots_fwd": 2, "shots_rev": 8, "z_chunks": 0, "graph_steps": 64}
+    knobs = {k: v for k, v, _ in autotune._candidates(d, base, _lib.MEM_BOUNDARY, 256)}
+    assert set(knobs) == {"shots_fwd", "shots_rev", "graph_steps"}
+    assert 2 in knobs["shots_fwd"] and 8 in knobs["shots_rev"] and max(knobs["shots_rev"]) <= 8
+    assert knobs["graph_steps"] == [0, 64]
+    host = {k for k, _, _ in autotune._candidates(d, base, _lib.MEM_BOUNDARY | _lib.MEM_HOST_TAPE, 256)}
+    assert "graph_steps" not in host
+    d.vp_stride = 120 * 200                          # per-shot models: one shot per CTA, nothing to group
+    assert {k for k, _, _ in autotune._candidates(d, base, _lib.MEM_BOUNDARY, 256)} == {"graph_steps"}
+    d3 = _desc(B=4, nz=64, nx=64)
+    d3.ndim, d3.ny = 3, 64
+    knobs3 = {k: v for k, v, _ in autotune._candidates(d3, dict(base, z_chunks=2), _lib.MEM_BOUNDARY, 16)}
+    assert knobs3["z_chunks"] == [1, 2, 4] and autotune._zmax(d3) == 4
+    assert knobs3["graph_steps"] == [0, 4]
+
+
+def test_tape_budget_rule_is_host_side():
+    """BoundarySaving(budget_gb=...) picks the memory mode from the host-only
+    size query: boundary saving while the tape fits, else checkpoints."""
+    import numpy as np
+    import torch
+    from sweep_b200 import Acoustic, BoundarySaving, PropTorch, _lib
+    vp = torch.full((30, 40), 2000.0)
+    src, rec = np.array([[5, 2], [20, 2]]), np.array([[[10, 2]], [[30, 2]]])
+    for budget, mode in ((100.0, "boundary"), (1e-6, "checkpoint")):
+        s = PropTorch(Acoustic(spatial_order=8, device="cpu"), shape=(30, 40), dh=10.0, dt=1e-3, abcn=10,
+                      device="cpu", memory=BoundarySaving(budget_gb=budget, ckpt_chunks=25))
+        tape = s.tape_bytes(200, src, rec, [vp])
+        geo, padded, wb, fields = s._probe(200, src, rec, [vp])
+        got = s._apply_budget(geo, padded, wb, fields, _lib.MEM_BOUNDARY, 0)
+        assert s.last_memory["mode"] == mode
+        if mode == "boundary":
+            assert got == (_lib.MEM_BOUNDARY, 0) and s.last_memory["tape_bytes"] == tape
+        else:
+            assert got == (_lib.MEM_CHECKPOINT, 25) and s.last_memory["boundary_tape_bytes"] == tape
