@@ -5,9 +5,9 @@
  * This boundary replaces the reference's compiled-core entry
  *     int sweep_call(int entry, const void* in, void* out, char* err, int err_cap)
  * (reference src/sweep/csrc/core/capi.h:225) for the entries of the hot path:
- *     acoustic2d 0 forward, 2 backward_bs, 3 backward_ckpt  (capi.h:39-45)
- *     acoustic3d 5 forward, 7 backward_bs, 8 backward_ckpt  (capi.h:46-52)
- *     elastic2d 60 forward, 62 backward_bs                  (capi.h:96-100)
+ *     acoustic2d 0 forward, 2 backward_bs, 3 backward_ckpt, 4 backward_recursive_ckpt  (capi.h:39-45)
+ *     acoustic3d 5 forward, 7 backward_bs, 8 backward_ckpt, 9 backward_recursive_ckpt  (capi.h:46-52)
+ *     elastic2d 60 forward, 62 backward_bs, 63 backward_ckpt, 64 backward_recursive_ckpt (capi.h:96-103)
  * with one plain function per (equation family, pass) instead of an entry
  * number, and one POD descriptor instead of the reference's ForwardInputCore /
  * BackwardInputCore Buf structs (reference src/sweep/csrc/core/input_core.h).
@@ -115,8 +115,8 @@ SWEEP_B200_API int sweep_b200_acoustic_forward(const sweep_acoustic_desc* d, int
                                 void* workspace, int64_t workspace_bytes,
                                 void* stream, char* err, int32_t err_cap);
 
-/* Adjoint propagation and gradient accumulation (reference entries 2/3 and
- * 7/8: eq_driver.cuh:721-1135).  adj: (B, nt, nrec) record cotangent.
+/* Adjoint propagation and gradient accumulation (reference entries 2/3/4 and
+ * 7/8/9: eq_driver.cuh:721-1135).  adj: (B, nt, nrec) record cotangent.
  * grad_vp: (B|1, cells) on the runtime grid, same stride rule as vp,
  * OVERWRITTEN with d loss / d vp (zero outside the physical box).
  * grad_wavelet: (B, nsrc, nt) overwritten, or NULL.  illum_src / illum_rec:
