@@ -313,3 +313,24 @@ def test_tape_budget_rule_is_host_side():
             assert got == (_lib.MEM_BOUNDARY, 0) and s.last_memory["tape_bytes"] == tape
         else:
             assert got == (_lib.MEM_CHECKPOINT, 25) and s.last_memory["boundary_tape_bytes"] == tape
+
+
+def test_recursive_sizes_every_equation():
+    """The recursive mode's sizes for 3-D acoustic and elastic: a token tape,
+    a workspace that grows with the snapshot budget and exceeds the
+    boundary-saving one by at least one snapshot; a host tape is refused."""
+    from sweep_b200 import _lib
+    d3 = _desc(B=1, nz=40, nx=40, nt=200)
+    d3.ndim, d3.ny = 3, 40
+    for i in range(6):
+        d3.pad[i] = 5
+    e = _edesc(nt=200)
+    for name, d in (("sweep_b200_acoustic_sizes", d3), ("sweep_b200_elastic_sizes", e)):
+        ws_bs, ws1, ws4, tape = _lib.c_i64(), _lib.c_i64(), _lib.c_i64(), _lib.c_i64()
+        _lib.call(name, d, _lib.MEM_BOUNDARY, 0, ws_bs, tape)
+        _lib.call(name, d, _lib.MEM_RECURSIVE, 1, ws1, tape)
+        assert tape.value <= 256
+        _lib.call(name, d, _lib.MEM_RECURSIVE, 4, ws4, tape)
+        assert ws4.value > ws1.value > ws_bs.value
+        with pytest.raises(RuntimeError, match="host tape"):
+            _lib.call(name, d, _lib.MEM_RECURSIVE | _lib.MEM_HOST_TAPE, 2, ws1, tape)
