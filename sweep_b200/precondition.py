@@ -1,6 +1,7 @@
 """Learned preconditioning of acoustic FWI: training pairs made by this
 solver, U-Net training, and the FWI loop with the plain illumination-
-preconditioned gradient as fallback and judge.
+preconditioned gradient as the fallback: a learned step is kept only when
+the data misfit drops.
 
 * ``plain_direction``: -grad / (illumination + eps max(illumination)), the
   reference's plain preconditioning (``_c.py:1050-1058``, used in
