@@ -33,6 +33,9 @@
  */
 #include <stdlib.h>
 #include <string.h>
+#if defined(__x86_64__) || defined(__i386__)
+#include <xmmintrin.h>
+#endif
 
 #ifndef REAL
 #define REAL float
@@ -40,6 +43,37 @@
 #define R(x) ((REAL)(x))
 
 typedef long long i64;
+
+/* ------------------------------------------------------ subnormals as zero */
+/* oracle_ftz(1) sets flush-to-zero and denormals-are-zero in every thread of
+ * the OpenMP team (the caller's included), oracle_ftz(0) restores each
+ * thread's previous mode.  The device flushes float subnormals (the CUDA
+ * path's -ftz=true) and so does the reference's host core
+ * (src/sweep/csrc/host/launch.h:45-83): on x86 every subnormal operand or
+ * result otherwise takes a microcode assist, which slows a decaying
+ * wavefield several times over.  The Python wrapper brackets every oracle
+ * call with the pair. */
+static unsigned ftz_saved;
+static int ftz_held;
+#pragma omp threadprivate(ftz_saved, ftz_held)
+
+void oracle_ftz(int on)
+{
+#if defined(__x86_64__) || defined(__i386__)
+    #pragma omp parallel
+    {
+        if (on) {
+            if (!ftz_held) { ftz_saved = _mm_getcsr(); ftz_held = 1; }
+            _mm_setcsr(ftz_saved | 0x8040u);
+        } else if (ftz_held) {
+            _mm_setcsr(ftz_saved);
+            ftz_held = 0;
+        }
+    }
+#else
+    (void)on;
+#endif
+}
 
 /* ------------------------------------------------------------------ helpers */
 
@@ -341,7 +375,8 @@ int oracle_a2d_backward(
     const REAL* az, const REAL* bz, const REAL* dbz, const REAL* ax, const REAL* bx, const REAL* dbx,
     const REAL* vp, i64 vp_stride,
     int nsrc, const int* src, const REAL* wavelet, int nrec, const int* rec,
-    const REAL* adj, const REAL* tape, REAL* grad_vp, REAL* grad_wavelet)
+    const REAL* adj, const REAL* tape, REAL* grad_vp, REAL* grad_wavelet,
+    REAL* illum_s, REAL* illum_r)
 {
     A2D p = {B, nz, nx, nt, M, {pad[0], pad[1], pad[2], pad[3]}, dt, dz, dx, lap, gco,
              az, bz, dbz, ax, bx, dbx, vp, vp_stride, nsrc, src, wavelet, nrec, rec};
@@ -395,7 +430,17 @@ int oracle_a2d_backward(
                     grad_wavelet[((i64)b * nsrc + s) * nt + it] += ln[(i64)iz * nx + ix];
                 }
             }
-            if (it == 0) break;   /* the it == 0 tail: no reconstruction, no imaging */
+            if (it == 0) {
+                /* the it == 0 tail: no reconstruction, no imaging; the receiver
+                   illumination still takes lambda(0)^2 (driver_traits.cuh:515-527) */
+                if (illum_r)
+                    for (int iz = z0; iz < z1; ++iz)
+                        for (int ix = x0; ix < x1; ++ix) {
+                            const i64 i = (i64)iz * nx + ix;
+                            illum_r[i] += ln[i] * ln[i];
+                        }
+                break;
+            }
             /* NOPML reconstruction + fused imaging (kernels.cuh:474-528) */
             #pragma omp parallel for schedule(static)
             for (int iz = rz0; iz < rz1; ++iz) {
@@ -426,6 +471,18 @@ int oracle_a2d_backward(
                 REAL utt = ((rnx[i] - R(2) * rn[i]) + rp[i]) / dt2;
                 g[i] = g[i] + ((((R(2) * dt) * dt) * utt) * ln[i]) / vpb[i];
             }
+            /* illumination on the physical box, the three time levels the
+               imaging used, before the source injection (kernels.cu:133-182,
+               driver_traits.cuh:610-626): sum_t u_tt^2 and sum_t lambda^2,
+               summed over shots */
+            if (illum_s)
+                for (int iz = z0; iz < z1; ++iz)
+                    for (int ix = x0; ix < x1; ++ix) {
+                        const i64 i = (i64)iz * nx + ix;
+                        illum_r[i] += ln[i] * ln[i];
+                        const REAL utt = ((rnx[i] - R(2) * rn[i]) + rp[i]) / dt2;
+                        illum_s[i] += utt * utt;
+                    }
             inject2(&p, b, rnx, wavelet, nsrc, src, it, R(1));
             { REAL* t = rp; rp = rn; rn = rnx; rnx = t; }
         }

@@ -231,7 +231,8 @@ int oracle_a3d_forward(A3D_ARGS, REAL* record, REAL* tape)
 
 /* exact adjoint step of shot b (adjoint_split.cu:14-320) */
 static void a3d_adjoint(const A3D* p, int b, const REAL* ln, const REAL* lp, REAL* lx_,
-                        REAL* const ps[3], REAL* const zt[3], REAL* const pso[3], REAL* const zto[3])
+                        REAL* const ps[3], REAL* const zt[3], REAL* const pso[3], REAL* const zto[3],
+                        REAL* gwb)
 {
     const int nz = p->nz, ny = p->ny, nx = p->nx, M = p->M;
     const i64 sy = nx, sz = (i64)nx * ny;
@@ -246,7 +247,10 @@ static void a3d_adjoint(const A3D* p, int b, const REAL* ln, const REAL* lp, REA
     const REAL* dbv[3] = {p->dbx, p->dby, p->dbz};
     const int lo[3] = {p->pad[4] + 2 * M + 1, p->pad[2] + 2 * M + 1, p->pad[0] + 2 * M + 1};
     const int hi[3] = {nx - (p->pad[5] + 2 * M + 1), ny - (p->pad[3] + 2 * M + 1), nz - (p->pad[1] + 2 * M + 1)};
-#define GW(n) ((((vp[n] * vp[n]) * dt2)) * ln[n])
+    /* gw = ((vp * vp) * dt^2) * lambda once per cell (the taps below read it) */
+    #pragma omp parallel for schedule(static)
+    for (i64 i = 0; i < (i64)nz * sz; ++i) gwb[i] = ((vp[i] * vp[i]) * dt2) * ln[i];
+#define GW(n) (gwb[n])
     #pragma omp parallel for schedule(static)
     for (int iz = M; iz < nz - M; ++iz)
         for (int iy = M; iy < ny - M; ++iy)
@@ -306,7 +310,8 @@ static void a3d_adjoint(const A3D* p, int b, const REAL* ln, const REAL* lp, REA
 #undef GW
 }
 
-int oracle_a3d_backward(A3D_ARGS, const REAL* adj, const REAL* tape, REAL* grad_vp, REAL* grad_wavelet)
+int oracle_a3d_backward(A3D_ARGS, const REAL* adj, const REAL* tape, REAL* grad_vp, REAL* grad_wavelet,
+                        REAL* illum_s, REAL* illum_r)
 {
     A3D_INIT(p);
     const i64 n = (i64)nz * ny * nx;
@@ -316,7 +321,7 @@ int oracle_a3d_backward(A3D_ARGS, const REAL* adj, const REAL* tape, REAL* grad_
     char* in_strip = (char*)calloc((size_t)n, 1);
     strip_cells_3d(&p, M + 1, cells);
     for (int c = 0; c < ns; ++c) in_strip[cells[c]] = 1;
-    REAL* buf = (REAL*)malloc(sizeof(REAL) * n * 19);
+    REAL* buf = (REAL*)malloc(sizeof(REAL) * n * 20);
     if (!buf || !cells || !in_strip) { free(buf); free(cells); free(in_strip); return 1; }
     int z0 = pad[0] + M, z1 = nz - pad[1] - M, y0 = pad[2] + M, y1 = ny - pad[3] - M;
     int x0 = pad[4] + M, x1 = nx - pad[5] - M;
@@ -325,19 +330,20 @@ int oracle_a3d_backward(A3D_ARGS, const REAL* adj, const REAL* tape, REAL* grad_
     const int rx0 = pad[4] + 2 * M + 1, rx1 = nx - (pad[5] + 2 * M + 1);
     const REAL dt2 = dt * dt;
     for (int b = 0; b < B; ++b) {
-        memset(buf, 0, sizeof(REAL) * n * 19);
+        memset(buf, 0, sizeof(REAL) * n * 20);
         REAL *lp = buf, *ln = buf + n, *lx = buf + 2 * n;
         REAL* aps[2][3] = {{buf + 3 * n, buf + 4 * n, buf + 5 * n}, {buf + 6 * n, buf + 7 * n, buf + 8 * n}};
         REAL* azt[2][3] = {{buf + 9 * n, buf + 10 * n, buf + 11 * n}, {buf + 12 * n, buf + 13 * n, buf + 14 * n}};
         REAL *rp = buf + 15 * n, *rn = buf + 16 * n, *rx = buf + 17 * n;
         REAL* g = buf + 18 * n;
+        REAL* gwb = buf + 19 * n;
         const REAL* vpb = vp + b * vp_stride;
         int cur = 0;
         const REAL* last = tape + (i64)nt * B * ns + (i64)b * 2 * n;
         memcpy(rp, last + n, sizeof(REAL) * n);
         memcpy(rn, last, sizeof(REAL) * n);
         for (int it = nt - 1; it >= 0; --it) {
-            a3d_adjoint(&p, b, ln, lp, lx, aps[cur], azt[cur], aps[1 - cur], azt[1 - cur]);
+            a3d_adjoint(&p, b, ln, lp, lx, aps[cur], azt[cur], aps[1 - cur], azt[1 - cur], gwb);
             inject3(&p, b, lx, adj, nrec, rec, it, R(1));
             { REAL* t = lp; lp = ln; ln = lx; lx = t; }
             cur = 1 - cur;
@@ -348,7 +354,18 @@ int oracle_a3d_backward(A3D_ARGS, const REAL* adj, const REAL* tape, REAL* grad_
                     grad_wavelet[((i64)b * nsrc + s) * nt + it] += ln[((i64)c[2] * ny + c[1]) * nx + c[0]];
                 }
             }
-            if (it == 0) break;
+            if (it == 0) {
+                /* receiver illumination of the it == 0 tail
+                   (acoustic3d/driver_traits.cuh:467-478) */
+                if (illum_r)
+                    for (int iz = z0; iz < z1; ++iz)
+                        for (int iy = y0; iy < y1; ++iy)
+                            for (int ix = x0; ix < x1; ++ix) {
+                                const i64 i = iz * sz + iy * sy + ix;
+                                illum_r[i] += ln[i] * ln[i];
+                            }
+                break;
+            }
             #pragma omp parallel for schedule(static)
             for (int iz = rz0; iz < rz1; ++iz)
                 for (int iy = ry0; iy < ry1; ++iy)
@@ -374,10 +391,21 @@ int oracle_a3d_backward(A3D_ARGS, const REAL* adj, const REAL* tape, REAL* grad_
                 REAL utt = ((rx[i] - R(2) * rn[i]) + rp[i]) / dt2;
                 g[i] = g[i] + ((((R(2) * dt) * dt) * utt) * ln[i]) / vpb[i];
             }
+            /* illumination on the physical box after the strip imaging, before
+               the source injection (acoustic3d/driver_traits.cuh:556-575,
+               kernels.cu:150-200), summed over shots */
+            if (illum_s)
+                for (int iz = z0; iz < z1; ++iz)
+                    for (int iy = y0; iy < y1; ++iy)
+                        for (int ix = x0; ix < x1; ++ix) {
+                            const i64 i = iz * sz + iy * sy + ix;
+                            illum_r[i] += ln[i] * ln[i];
+                            const REAL utt = ((rx[i] - R(2) * rn[i]) + rp[i]) / dt2;
+                            illum_s[i] += utt * utt;
+                        }
             inject3(&p, b, rx, wavelet, nsrc, src, it, R(1));
             { REAL* t = rp; rp = rn; rn = rx; rx = t; }
         }
-        (void)z0; (void)z1; (void)y0; (void)y1; (void)x0; (void)x1;
         REAL* gout = grad_vp + b * vp_stride;
         for (i64 i = 0; i < n; ++i) gout[i] += g[i];
     }

@@ -43,6 +43,31 @@ def build() -> None:
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
 
 
+class _FlushToZero:
+    """The loaded oracle library with every ``oracle_*`` compute entry run
+    between ``oracle_ftz(1)`` and ``oracle_ftz(0)``: subnormals flushed to
+    zero in the OpenMP threads for the call, as the device does."""
+
+    def __init__(self, lib):
+        self._lib = lib
+        lib.oracle_ftz.argtypes = [ctypes.c_int]
+        lib.oracle_ftz.restype = None
+
+    def __getattr__(self, name):
+        fn = getattr(self._lib, name)
+        if not name.startswith("oracle_") or name.endswith("_tape_len") or name == "oracle_ftz":
+            return fn
+        lib = self._lib
+
+        def call(*args):
+            lib.oracle_ftz(1)
+            try:
+                return fn(*args)
+            finally:
+                lib.oracle_ftz(0)
+        return call
+
+
 def _lib(prec: str):
     if prec not in _LIBS:
         path = HERE / f"liboracle_{prec}.so"
@@ -58,18 +83,18 @@ def _lib(prec: str):
         lib.oracle_a2d_forward.restype = i
         lib.oracle_a2d_forward.argtypes = geo + [P, P]
         lib.oracle_a2d_backward.restype = i
-        lib.oracle_a2d_backward.argtypes = geo + [P, P, P, P]
+        lib.oracle_a2d_backward.argtypes = geo + [P, P, P, P, P, P]
         geo3 = [i, i, i, i, i, i, P, real, real, real, real, P, P,
                 P, P, P, P, P, P, P, P, P, P, l, i, P, P, i, P]
         if not hasattr(lib, "oracle_a3d_tape_len"):
-            _LIBS[prec] = lib
-            return lib
+            _LIBS[prec] = _FlushToZero(lib)
+            return _LIBS[prec]
         lib.oracle_a3d_tape_len.restype = l
         lib.oracle_a3d_tape_len.argtypes = [i, i, i, i, i, i, P]
         lib.oracle_a3d_forward.restype = i
         lib.oracle_a3d_forward.argtypes = geo3 + [P, P]
         lib.oracle_a3d_backward.restype = i
-        lib.oracle_a3d_backward.argtypes = geo3 + [P, P, P, P]
+        lib.oracle_a3d_backward.argtypes = geo3 + [P, P, P, P, P, P]
         geo_el = [i, i, i, i, i, P, real, real, real, P, P, P, P, P, l,
                   i, P, P, i, P, i, P, i, P]
         lib.oracle_el2d_tape_len.restype = l
@@ -78,7 +103,7 @@ def _lib(prec: str):
         lib.oracle_el2d_forward.argtypes = geo_el + [P, P]
         lib.oracle_el2d_backward.restype = i
         lib.oracle_el2d_backward.argtypes = geo_el + [P, P, P, P, P]
-        _LIBS[prec] = lib
+        _LIBS[prec] = _FlushToZero(lib)
     return _LIBS[prec]
 
 
@@ -268,14 +293,21 @@ class Acoustic2D(_Acoustic):
         assert rc == 0
         return rec.transpose(0, 2, 1)[..., None]                 # (B, nt, nrec, 1)
 
-    def backward(self, adj):
-        """``adj``: record cotangent in the canonical ``(B, nt, nrec, 1)`` layout."""
+    def backward(self, adj, illum=False):
+        """``adj``: record cotangent in the canonical ``(B, nt, nrec, 1)`` layout.
+        With ``illum``, also the source and receiver illuminations
+        (``sum_t u_tt^2``, ``sum_t lambda^2``, summed over shots, cropped)."""
         lib = _lib(self.prec)
         a = np.ascontiguousarray(np.asarray(adj)[..., 0].transpose(0, 2, 1).astype(self.real))
         g = np.zeros(((self.B,) if self.per_shot else ()) + self.shape, self.real)
         gw = np.zeros((self.B, 1, self.nt), self.real)
-        rc = lib.oracle_a2d_backward(*self._geo(), _ptr(a), _ptr(self.tape), _ptr(g), _ptr(gw))
+        i_s = np.zeros(self.shape, self.real) if illum else None
+        i_r = np.zeros(self.shape, self.real) if illum else None
+        rc = lib.oracle_a2d_backward(*self._geo(), _ptr(a), _ptr(self.tape), _ptr(g), _ptr(gw),
+                                     _ptr(i_s) if illum else None, _ptr(i_r) if illum else None)
         assert rc == 0
+        if illum:
+            return self.crop(g), gw[:, 0, :], self.crop(i_s), self.crop(i_r)
         return self.crop(g), gw[:, 0, :]
 
 
@@ -305,29 +337,39 @@ class Acoustic3D(_Acoustic):
         assert rc == 0
         return rec.transpose(0, 2, 1)[..., None]
 
-    def backward(self, adj):
+    def backward(self, adj, illum=False):
         lib = _lib(self.prec)
         a = np.ascontiguousarray(np.asarray(adj)[..., 0].transpose(0, 2, 1).astype(self.real))
         g = np.zeros(self.shape, self.real)
         gw = np.zeros((self.B, 1, self.nt), self.real)
-        rc = lib.oracle_a3d_backward(*self._geo(), _ptr(a), _ptr(self.tape), _ptr(g), _ptr(gw))
+        i_s = np.zeros(self.shape, self.real) if illum else None
+        i_r = np.zeros(self.shape, self.real) if illum else None
+        rc = lib.oracle_a3d_backward(*self._geo(), _ptr(a), _ptr(self.tape), _ptr(g), _ptr(gw),
+                                     _ptr(i_s) if illum else None, _ptr(i_r) if illum else None)
         assert rc == 0
+        if illum:
+            return self.crop(g), gw[:, 0, :], self.crop(i_s), self.crop(i_r)
         return self.crop(g), gw[:, 0, :]
 
 
-def acoustic_gradient(vp, wavelet, src, rec, obs, dh, dt, abcn, order=8, prec="f32", **kw):
+def acoustic_gradient(vp, wavelet, src, rec, obs, dh, dt, abcn, order=8, prec="f32", illum=False, **kw):
     """Record, loss ``0.5 ||pred - obs||^2``, model gradient (cropped, summed over
     shots for a shared model) and wavelet gradient (summed over shots for a
-    shared wavelet), like ``PropTorch(impl='c')`` + ``loss.backward()``."""
+    shared wavelet), like ``PropTorch(impl='c')`` + ``loss.backward()``.  With
+    ``illum``, two more results: the source and receiver illuminations, as
+    ``solver.compute_illumination = True`` gives them."""
     ndim = np.asarray(src).shape[-1]
     cls = Acoustic2D if ndim == 2 else Acoustic3D
     run = cls(vp, wavelet, src, rec, dh, dt, abcn, order, prec, **kw)
     pred = run.forward(keep_tape=True)
     res = pred - np.asarray(obs, run.real)
     loss = 0.5 * float(np.sum(res.astype(np.float64) ** 2))
-    g, gw = run.backward(res)
+    out = run.backward(res, illum=illum)
+    g, gw = out[0], out[1]
     if np.asarray(wavelet).ndim == 1:
         gw = gw.sum(0)
+    if illum:
+        return pred, loss, g, gw, out[2], out[3]
     return pred, loss, g, gw
 
 

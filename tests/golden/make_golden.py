@@ -10,14 +10,15 @@ which the reference's own tests hold to rel < 1e-5 of its CUDA core
 gradients, float32) are saved as small ``.npz`` files together with every input,
 so the parity tests never need the reference at run time.
 
-Usage (in a container that has the reference checked out)::
+Usage (with the reference's source tree checked out somewhere)::
 
-    TORCH_EXTENSIONS_DIR=/tmp/sweep_ref_build \
-    PYTHONPATH=/root/reference/src python tests/golden/make_golden.py
+    SWEEP_REFERENCE_SRC=<reference checkout>/src \
+    TORCH_EXTENSIONS_DIR=<scratch build dir> \
+    python tests/golden/make_golden.py [case ...]
 
-The reference's own build step (a one-time g++ build of its host core into
-``TORCH_EXTENSIONS_DIR``) runs on first use.  Nothing here is imported by the
-library or the tests.
+``SWEEP_REFERENCE_SRC`` is required.  The reference's own build step (a
+one-time g++ build of its host core into ``TORCH_EXTENSIONS_DIR``) runs on
+first use.  Nothing here is imported by the library or the tests.
 """
 from __future__ import annotations
 
@@ -28,7 +29,9 @@ from pathlib import Path
 import numpy as np
 import torch
 
-REF_SRC = os.environ.get("SWEEP_REFERENCE_SRC", "/root/reference/src")
+REF_SRC = os.environ.get("SWEEP_REFERENCE_SRC")
+if not REF_SRC:
+    sys.exit("make_golden.py: set SWEEP_REFERENCE_SRC to the reference's src directory")
 if REF_SRC not in sys.path:
     sys.path.insert(0, REF_SRC)
 
@@ -458,6 +461,158 @@ def acoustic3d_free_surface():
     )
 
 
+def _illum_model(shape):
+    """Ramp plus bump (the heterogeneous model of the reference's illumination
+    pins, test/test_illumination_pin.py:30-35)."""
+    idx = np.indices(shape).astype(np.float32)
+    bump = sum((i - n / 2) ** 2 / n for i, n in zip(idx, shape))
+    return (2500.0 + 4.0 * idx[0] + 60.0 * np.sin(bump)).astype(np.float32)
+
+
+def _illum_case(cls, shape, src, rec, nt, dt, dh, abcn):
+    """Gradient with solver.compute_illumination = True in boundary-saving and
+    full modes, plus the boundary-saving gradient with illumination off."""
+    vp_true = _illum_model(shape)
+    vp_init = (0.97 * vp_true).astype(np.float32)
+    w = _wavelet(nt, dt, 15.0, 0.05)
+    out = {}
+    obs = None
+    for tag, mem, illum in (("bs", BoundarySaving(), True), ("full", Full(), True),
+                            ("off", BoundarySaving(), False)):
+        solver = PropTorch(cls(spatial_order=8, device="cpu"), shape=shape, dh=dh, dt=dt, abcn=abcn,
+                           impl="c", device="cpu", memory=mem)
+        if obs is None:
+            obs = _forward(solver, w, src, rec, [vp_true])
+        solver.compute_illumination = illum
+        r = _run(solver, w, src, rec, [vp_init], obs, False)
+        out[f"pred_{tag}"] = r["pred"]
+        out[f"grad_vp_{tag}"] = r["grad0"]
+        if illum:
+            out[f"src_illum_{tag}"] = solver.source_illumination.detach().numpy().copy()
+            out[f"rec_illum_{tag}"] = solver.receiver_illumination.detach().numpy().copy()
+    return dict(vp_true=vp_true, vp_init=vp_init, wavelet=w, src=src, rec=rec, obs=obs, **out)
+
+
+def acoustic2d_illum():
+    """Source / receiver illumination (solver.compute_illumination = True) in
+    2-D: 2 shots on an 80 x 100 ramp-plus-bump model, boundary saving and full."""
+    nz, nx, nt, dt, dh, abcn = 80, 100, 260, 0.0012, 10.0, 8
+    src = np.array([[nx // 2, nz // 3], [20, 10]], np.int64)
+    rx = np.arange(4, nx - 4, 4, dtype=np.int64)
+    rec = np.broadcast_to(np.stack([rx, np.full(rx.size, 4)], -1), (2, rx.size, 2)).copy()
+    d = _illum_case(Acoustic, (nz, nx), src, rec, nt, dt, dh, abcn)
+    np.savez_compressed(OUT / "acoustic2d_illum.npz", nz=nz, nx=nx, nt=nt, dt=dt, dh=dh, abcn=abcn,
+                        order=8, **d)
+
+
+def acoustic3d_illum():
+    """Source / receiver illumination in 3-D: one shot on a 30 x 28 x 34
+    ramp-plus-bump model, boundary saving and full."""
+    nz, ny, nx, nt, dt, dh, abcn = 30, 28, 34, 160, 0.0012, 10.0, 8
+    src = np.array([[nx // 2, ny // 2, nz // 3]], np.int64)
+    rx = np.arange(4, nx - 4, 4, dtype=np.int64)
+    rec = np.stack([rx, np.full(rx.size, ny // 2), np.full(rx.size, 4)], -1)[None]
+    d = _illum_case(Acoustic3D, (nz, ny, nx), src, rec, nt, dt, dh, abcn)
+    np.savez_compressed(OUT / "acoustic3d_illum.npz", nz=nz, ny=ny, nx=nx, nt=nt, dt=dt, dh=dh,
+                        abcn=abcn, order=8, **d)
+
+
+def acoustic3d_clean():
+    """A 3-D grid whose clear box is wider than one 32 x 8 column block in x
+    and y (64 x 72 x 96, CPML 8): split into z chunks, the stencil kernels'
+    CTAs clear of the CPML shell take their clean path.  2 shots inside the
+    volume, 24 receivers spread through it; boundary saving."""
+    rng = np.random.default_rng(53)
+    nz, ny, nx, nt, dt, dh, abcn = 64, 72, 96, 220, 0.001, 10.0, 8
+    zz = (np.arange(nz)[:, None, None] + 3.0 * np.sin(np.arange(nx)[None, None, :] * 2 * np.pi / nx)
+          + 2.0 * np.cos(np.arange(ny)[None, :, None] * 2 * np.pi / ny))
+    vp_true = np.where(zz < nz / 2, 1800.0, 2600.0) + np.zeros((nz, ny, nx))
+    vp_true = np.where((zz > 0.7 * nz) & (np.arange(nx)[None, None, :] > nx / 3), 2300.0, vp_true)
+    vp_true = vp_true.astype(np.float32)
+    vp_init = np.full((nz, ny, nx), 2100.0, np.float32)
+    w = np.stack([_wavelet(nt, dt, 15.0, 0.06), _wavelet(nt, dt, 12.0, 0.07)]).astype(np.float32)
+    src = np.array([[48, 36, 20], [30, 44, 40]], np.int64)          # (x, y, z)
+    rec = np.zeros((2, 24, 3), np.int64)
+    for b in range(2):
+        rec[b, :, 0] = rng.integers(2, nx - 2, 24)
+        rec[b, :, 1] = rng.integers(2, ny - 2, 24)
+        rec[b, :, 2] = rng.integers(2, nz - 2, 24)
+    eq = Acoustic3D(spatial_order=8, device="cpu")
+    solver = PropTorch(eq, shape=(nz, ny, nx), dh=dh, dt=dt, abcn=abcn, impl="c", device="cpu",
+                       memory=BoundarySaving())
+    obs = _forward(solver, w, src, rec, [vp_true])
+    r = _run(solver, w, src, rec, [vp_init], obs, True)
+    np.savez_compressed(
+        OUT / "acoustic3d_clean.npz",
+        nz=nz, ny=ny, nx=nx, nt=nt, dt=dt, dh=dh, abcn=abcn, order=8,
+        vp_true=vp_true, vp_init=vp_init, wavelet=w, src=src, rec=rec,
+        obs=obs, pred=r["pred"], loss=r["loss"], grad_vp=r["grad0"], grad_wavelet=r["grad_wavelet"],
+    )
+
+
+def acoustic2d_many():
+    """20 shots of uneven geometry (per-shot wavelets, 5-30 receivers each
+    padded with off-grid coordinates, sources at several depths) on a
+    64 x 160 layered model: enough shots to fill 8- and 16-shot CTA groups."""
+    rng = np.random.default_rng(59)
+    nz, nx, nt, dt, dh, abcn = 64, 160, 300, 0.001, 10.0, 12
+    B = 20
+    vp_true = _layered(nz, nx, rng, 1500.0, 3200.0, 6)
+    vp_init = np.full((nz, nx), 1900.0, np.float32) + 20.0 * rng.standard_normal((nz, nx)).astype(np.float32)
+    w = np.stack([_wavelet(nt, dt, rng.uniform(10, 20), rng.uniform(0.05, 0.09)) for _ in range(B)])
+    w = w.astype(np.float32)
+    src = np.stack([rng.integers(2, nx - 2, B), rng.integers(1, nz // 3, B)], -1).astype(np.int64)
+    nrec = rng.integers(5, 31, B)
+    rec = np.full((B, int(nrec.max()), 2), -1000, np.int64)
+    for b, n in enumerate(nrec):
+        rec[b, :n, 0] = np.sort(rng.choice(np.arange(1, nx - 1), size=n, replace=False))
+        rec[b, :n, 1] = rng.integers(1, nz - 1, size=n)
+    eq = Acoustic(spatial_order=8, device="cpu")
+    solver = PropTorch(eq, shape=(nz, nx), dh=dh, dt=dt, abcn=abcn, impl="c", device="cpu",
+                       memory=BoundarySaving())
+    obs = _forward(solver, w, src, rec, [vp_true])
+    r = _run(solver, w, src, rec, [vp_init], obs, True)
+    np.savez_compressed(
+        OUT / "acoustic2d_many.npz",
+        nz=nz, nx=nx, nt=nt, dt=dt, dh=dh, abcn=abcn, order=8,
+        vp_true=vp_true, vp_init=vp_init, wavelet=w, src=src, rec=rec,
+        obs=obs, pred=r["pred"], loss=r["loss"], grad_vp=r["grad0"], grad_wavelet=r["grad_wavelet"],
+    )
+
+
+def elastic2d_interior():
+    """Isotropic elastic on a 120 x 170 model (CPML 10): the runtime grid has
+    32 x 32 tiles clear of the CPML band.  4 explosive shots, (vx, vz)
+    receivers; vp/vs/rho gradients, boundary saving."""
+    rng = np.random.default_rng(61)
+    nz, nx, nt, dt, dh, abcn = 120, 170, 320, 0.0005, 5.0, 10
+    vp_true = _layered(nz, nx, rng, 1800.0, 3200.0, 5)
+    vs_true = (vp_true / 1.73).astype(np.float32)
+    rho_true = (310.0 * vp_true ** 0.25).astype(np.float32)
+    vp_init = np.full((nz, nx), 2300.0, np.float32)
+    vs_init = (vp_init / 1.73).astype(np.float32)
+    rho_init = (310.0 * vp_init ** 0.25).astype(np.float32)
+    w = _wavelet(nt, dt, 25.0, 0.04)
+    src = np.array([[30, 40], [85, 60], [140, 30], [60, 90]], np.int64)
+    rec = np.zeros((4, 20, 2), np.int64)
+    for b in range(4):
+        rec[b, :, 0] = np.linspace(3, nx - 4, 20).astype(np.int64)
+        rec[b, :, 1] = 3 + 20 * b
+    eq = Elastic(spatial_order=8, device="cpu")
+    solver = PropTorch(eq, shape=(nz, nx), dh=dh, dt=dt, abcn=abcn, impl="c", device="cpu",
+                       memory=BoundarySaving())
+    obs = _forward(solver, w, src, rec, [vp_true, vs_true, rho_true])
+    r = _run(solver, w, src, rec, [vp_init, vs_init, rho_init], obs, False)
+    np.savez_compressed(
+        OUT / "elastic2d_interior.npz",
+        nz=nz, nx=nx, nt=nt, dt=dt, dh=dh, abcn=abcn, order=8,
+        vp_true=vp_true, vs_true=vs_true, rho_true=rho_true,
+        vp_init=vp_init, vs_init=vs_init, rho_init=rho_init,
+        wavelet=w, src=src, rec=rec, obs=obs, pred=r["pred"], loss=r["loss"],
+        grad_vp=r["grad0"], grad_vs=r["grad1"], grad_rho=r["grad2"],
+    )
+
+
 CASES = {
     "acoustic2d_c1": acoustic2d_c1,
     "acoustic2d_multi": acoustic2d_multi,
@@ -471,6 +626,11 @@ CASES = {
     "elastic2d": elastic2d,
     "elastic2d_storage": elastic2d_storage,
     "elastic2d_vsrc": elastic2d_vsrc,
+    "acoustic2d_illum": acoustic2d_illum,
+    "acoustic3d_illum": acoustic3d_illum,
+    "acoustic3d_clean": acoustic3d_clean,
+    "acoustic2d_many": acoustic2d_many,
+    "elastic2d_interior": elastic2d_interior,
 }
 
 if __name__ == "__main__":

@@ -148,3 +148,61 @@ def test_staggered_coefficients_match_compiled_constants():
     assert c == [Fraction(1225, 1024), Fraction(-245, 3072), Fraction(49, 5120), Fraction(-5, 7168)]
     assert O.staggered_coefficients(1) == [Fraction(1)]
     assert O.staggered_coefficients(2) == [Fraction(9, 8), Fraction(-1, 24)]
+
+
+@pytest.mark.parametrize("case", ["acoustic2d_illum", "acoustic3d_illum"])
+def test_illumination_oracle_matches_reference(case):
+    """Source and receiver illumination (sum_t u_tt^2, sum_t lambda^2 on the
+    physical box, summed over shots) of the reference's boundary-saving run
+    with solver.compute_illumination = True; its full-storage run agrees, and
+    turning illumination on left the reference's gradient bit-identical."""
+    d = np.load(GOLD / f"{case}.npz")
+    pred, loss, g, gw, i_s, i_r = O.acoustic_gradient(d["vp_init"], d["wavelet"], d["src"], d["rec"], d["obs"],
+                                                      *_args(d), illum=True)
+    assert rel(pred, d["pred_bs"]) < 2e-5
+    assert rel(g, d["grad_vp_bs"]) < 1e-5
+    assert rel(i_s, d["src_illum_bs"]) < 1e-5
+    assert rel(i_r, d["rec_illum_bs"]) < 1e-5
+    assert np.array_equal(d["grad_vp_bs"], d["grad_vp_off"])
+    assert rel(d["src_illum_full"], d["src_illum_bs"]) < 1e-4
+    assert rel(d["rec_illum_full"], d["rec_illum_bs"]) < 1e-4
+    # the same gradient with illumination off in the oracle
+    _, _, g_off, _ = O.acoustic_gradient(d["vp_init"], d["wavelet"], d["src"], d["rec"], d["obs"], *_args(d))
+    assert np.array_equal(g, g_off)
+
+
+def test_acoustic3d_clean_box_oracle_matches_reference():
+    """A 3-D grid whose clear box spans several 32 x 8 column blocks."""
+    d = np.load(GOLD / "acoustic3d_clean.npz")
+    pred, loss, g, gw = O.acoustic_gradient(d["vp_init"], d["wavelet"], d["src"], d["rec"], d["obs"], *_args(d))
+    assert rel(pred, d["pred"]) < 2e-5
+    assert rel(g, d["grad_vp"]) < 1e-5
+    # reference 3-D wavelet gradient: shot 0 only (see above)
+    assert rel(gw[0], d["grad_wavelet"][0]) < 1e-5
+
+
+def test_acoustic2d_many_shots_oracle_matches_reference():
+    d = np.load(GOLD / "acoustic2d_many.npz")
+    pred, loss, g, gw = O.acoustic_gradient(d["vp_init"], d["wavelet"], d["src"], d["rec"], d["obs"], *_args(d))
+    assert rel(pred, d["pred"]) < 2e-5
+    assert rel(g, d["grad_vp"]) < 1e-5
+    assert rel(gw, d["grad_wavelet"]) < 1e-5
+
+
+def test_elastic2d_interior_tiles_oracle_matches_reference():
+    d = np.load(GOLD / "elastic2d_interior.npz")
+    pred, loss, (gvp, gvs, grho) = O.elastic_gradient(
+        d["vp_init"], d["vs_init"], d["rho_init"], d["wavelet"], d["src"], d["rec"], d["obs"], *_el_args(d))
+    assert rel(pred, d["pred"]) < 2e-6
+    assert rel(gvp, d["grad_vp"]) < 1e-5
+    assert rel(gvs, d["grad_vs"]) < 1e-5
+    assert rel(grho, d["grad_rho"]) < 1e-5
+
+
+def test_library_tables_equal_the_oracle_restatement():
+    """The library derives its float32 tables in closed form; the oracle
+    restates the reference's own derivation.  They agree bit for bit."""
+    from sweep_b200.scalars import centred_tables
+    for M in range(1, 7):
+        lib, ora = centred_tables(M), O.fd_tables(M)
+        assert np.array_equal(lib[0], ora[0]) and np.array_equal(lib[1], ora[1]), M
