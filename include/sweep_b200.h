@@ -140,9 +140,12 @@ SWEEP_B200_API int sweep_b200_acoustic_backward(const sweep_acoustic_desc* d, in
  * than the array, or more than 65536 shot-tiles or 32768 sources / receivers,
  * is rejected with an error.  The first call on a device looks up the
  * array's address (cudaGetSymbolAddress) with that device current: make it
- * before any stream capture.  Every call shares the array: calls that overlap
- * on the GPU race; each call clears what must start at zero.  Calls no
- * cudaMalloc, cudaFree or other allocating routine. */
+ * before any stream capture.  The address is kept for the life of the
+ * process: cudaDeviceReset after the entry point has been used is not
+ * supported.  Every call shares the array: calls that overlap on the GPU
+ * race; calls of one process are serialised by one process-wide lock (on
+ * every device); each call clears what must start at zero.  Calls no cudaMalloc,
+ * cudaFree or other allocating routine on the device. */
 SWEEP_B200_API int sweep_b200_acoustic_forward_noalloc(const sweep_acoustic_desc* d, float* record,
                                                        void* stream, char* err, int32_t err_cap);
 
@@ -259,6 +262,19 @@ SWEEP_B200_API int sweep_b200_schedule_get(int32_t family, const void* desc, swe
 
 /* Forget every recorded schedule.  Host-side only. */
 SWEEP_B200_API int sweep_b200_schedule_clear(void);
+
+/* Runs the bounded-wait failure path on purpose.  No counterpart in the
+ * reference, whose kernels do not wait on barriers.  Every mbarrier wait of
+ * this library's step kernels gives up after a fixed budget (about 2 s of SM
+ * clock), raises the call's error word and returns, so that a tile load that
+ * never lands surfaces as an error return instead of a hung GPU.  This entry
+ * launches one CTA that waits, with `budget_cycles` (1 .. that budget), on an
+ * mbarrier nothing arrives at (no copy in flight), then reads its error word
+ * as the step loops do: it returns non-zero with a "did not complete in time"
+ * message.  With `arrive` non-zero the CTA arrives first and the call
+ * succeeds.  Allocates nothing; synchronises `stream`. */
+SWEEP_B200_API int sweep_b200_wait_selftest(int64_t budget_cycles, int32_t arrive, void* stream,
+                                            char* err, int32_t err_cap);
 
 /* ABI version (SWEEP_B200_ABI_VERSION) -- checked by the Python loader, like
  * the reference's sweep_core_abi_version() (reference loader.py:92-138). */

@@ -38,6 +38,7 @@ SYMBOLS = (
     "sweep_b200_schedule_set",
     "sweep_b200_schedule_get",
     "sweep_b200_schedule_clear",
+    "sweep_b200_wait_selftest",
 )
 
 MEM_BOUNDARY = 0
@@ -134,6 +135,7 @@ def load():
     lib.sweep_b200_schedule_set.argtypes = [c_i32, c_p, S, ctypes.c_char_p, c_i32]
     lib.sweep_b200_schedule_get.argtypes = [c_i32, c_p, S, ctypes.c_char_p, c_i32]
     lib.sweep_b200_schedule_clear.argtypes = []
+    lib.sweep_b200_wait_selftest.argtypes = [c_i64, c_i32, c_p, ctypes.c_char_p, c_i32]
     for s in SYMBOLS[1:]:
         getattr(lib, s).restype = ctypes.c_int
     _lib = lib

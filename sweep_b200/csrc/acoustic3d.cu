@@ -749,8 +749,10 @@ __global__ void __launch_bounds__(NTH, 4) a3_step(const __grid_constant__ A3Maps
                 A.l_next[i] = 2.0f * gun - lprevv + (Lx + Ly + Lz - Dgx - Dgy - Dgz);
             }
         }
-        // the last stage every thread has waited for (its slot is not one
-        // plane z reads: the ring holds NSA > 2M + 2 stages)
+        // the last stage every thread has waited for.  The ring holds exactly
+        // NSA = 2M + 2 stages: stage z + M + 2 is issued into the slot of
+        // z - M only after the barrier that ends plane z, so no thread still
+        // reads that slot when it is refilled
         int last = z + M;
         if (clean && z + 1 < ze) { await(z + M + 1); convert(z + M + 1); last = z + M + 1; }
         if (__syncthreads_or(bad)) { fail(z == zb && !clean ? q0 : last); return; }

@@ -12,8 +12,15 @@
 //     (cudaGetSymbolAddress, with that device current).  Make that first call
 //     before any stream capture;
 //   * every call on a device uses the same array: calls that overlap on the
-//     GPU (other streams, other host threads) race and corrupt each other; run
-//     them one after the other;
+//     GPU race and corrupt each other; run them one after the other.  Calls
+//     from this process are serialised by one process-wide lock held for the
+//     whole call (calls on different GPUs too, since they share the static
+//     host staging buffers), so the race concerns work that reaches the
+//     array some other way, e.g. another copy of this library loaded into
+//     the process;
+//   * the address looked up on a device's first call is kept for the life of
+//     the process: cudaDeviceReset on that device after the entry point has
+//     been used is not supported (the module may load at another address);
 //   * each call clears the fields that must start at zero, so a call never
 //     sees what the previous one left behind;
 //   * no cudaMalloc, cudaFree or any other allocating routine is called; host
@@ -32,6 +39,8 @@ constexpr int kMaxDevices = 64;
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
+// One process-wide lock over the static host staging buffers and the
+// per-device address table.
 std::mutex g_mutex;
 void* g_scratch_ptr[kMaxDevices] = {};
 
@@ -39,12 +48,18 @@ int32_t h_loc_src[2 * kMaxEvents], h_loc_rec[2 * kMaxEvents];
 int32_t h_off_src[kMaxKeys + 1], h_off_rec[kMaxKeys + 1], h_fill[kMaxKeys + 1], h_order[kMaxKeys + 1];
 int2 h_ev_src[kMaxEvents], h_ev_rec[kMaxEvents];
 
-// Device address of this device's scratch array, looked up once per device.
-void* scratch_of_current_device()
+int current_device()
 {
     int dev = -1;
     SWEEP_CUDA(cudaGetDevice(&dev));
     SWEEP_REQUIRE(dev >= 0 && dev < kMaxDevices, "device ordinal %d out of range", dev);
+    return dev;
+}
+
+// Device address of device `dev`'s scratch array (`dev` current), looked up
+// once per device; the caller holds g_mutex.
+void* scratch_of_device(int dev)
+{
     if (!g_scratch_ptr[dev]) {
         void* p = nullptr;
         SWEEP_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
@@ -76,7 +91,7 @@ extern "C" SWEEP_B200_API int sweep_b200_acoustic_forward_noalloc(const sweep_ac
                       "(got %lld, %lld, %lld)", kMaxKeys, kMaxEvents, (long long)nkey - 1,
                       (long long)nes, (long long)ner);
         std::lock_guard<std::mutex> lock(g_mutex);
-        void* ws = scratch_of_current_device();
+        void* ws = scratch_of_device(current_device());
         const a2d::HostStage stage{h_loc_src, h_loc_rec, h_off_src, h_off_rec, h_ev_src, h_ev_rec, h_fill, h_order};
         a2d::forward_with(d, SWEEP_MEM_BOUNDARY, 0, record, nullptr, ws, kNoAllocScratchBytes, static_cast<cudaStream_t>(stream),
                           &stage);

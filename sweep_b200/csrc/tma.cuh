@@ -96,18 +96,30 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
     return ok != 0;
 }
 
-// Wait for phase `parity` of `bar`; false (and *err = code) after kWaitCycles.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code)
+// Wait for phase `parity` of `bar`; false (and *err = code) after `budget`
+// SM clock cycles.
+__device__ __forceinline__ bool mbar_wait_for(uint64_t* bar, uint32_t parity, int* err, int code, long long budget)
 {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity)) {
-        if (clock64() - t0 > kWaitCycles) {
+        if (clock64() - t0 > budget) {
             atomicExch(err, code);
             return false;
         }
     }
     return true;
+}
+
+// The library's wait: gives up after kWaitCycles.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code)
+{
+    return mbar_wait_for(bar, parity, err, code, kWaitCycles);
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 // 3-D tiled load of the box at (x, y, z) of `map` into shared memory `dst`;

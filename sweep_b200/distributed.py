@@ -47,7 +47,10 @@ def sharded_gradient(compute: Callable[[slice], tuple], n_shots: int, group=None
     world = dist.get_world_size(group) if dist.is_initialized() else 1
     rank = dist.get_rank(group) if dist.is_initialized() else 0
     loss, grads = compute(shot_slice(n_shots, world, rank))
-    loss = torch.as_tensor(loss, dtype=torch.float64).reshape(1).clone()
     grads = [g.contiguous() for g in grads]
+    # the loss travels with the gradients (NCCL reduces device tensors only),
+    # whatever compute() returned it as: a Python float, a CPU or GPU tensor
+    dev = grads[0].device if grads else torch.device("cpu")
+    loss = torch.as_tensor(loss, dtype=torch.float64).to(dev).reshape(1).clone()
     all_reduce_([loss, *grads], group)
     return loss[0], grads
