@@ -1,22 +1,30 @@
-"""Benchmark of the FD hot path: one step = one full-waveform gradient
-(forward + adjoint) of a 32-shot 2-D acoustic survey (default), or with
-``--workload elastic2d`` of a 16-shot 2-D elastic survey (vp / vs / rho).
+"""Benchmark of the FD hot path: Gcell-updates/s of the forward + adjoint
+gradient, with every figure the measurement needs in one JSON line.
 
-Workload (synthetic, seeded): 256 x 768 grid (nz x nx), dh 12.5 m, dt 1 ms,
-nt 3000, order 8, CPML 40 cells; a 12-layer model with sinusoidally perturbed
-interfaces (1500 -> 4700 m/s, +-5% noise), Gaussian-smoothed (sigma 8 cells)
-start model; 32 shots at z = 2 with uneven x, each with its own line of
-200-384 receivers at z = 2 padded to 384 with off-grid coordinates; 8 Hz
-Ricker wavelet delayed 0.15 s.  Loss 0.5 ||pred - obs||^2 against data
-modelled once in the true model before timing.
+Default workload (``--workload acoustic3d``): the 3-D acoustic survey,
+256^3 (runtime grid 312^3), dh 10 m, dt 1 ms, nt 2000, order 8, CPML 24; an
+8-layer dipping model (1500-4000 m/s) with a +600 m/s Gaussian anomaly
+(seeded; its largest velocity 4247 m/s keeps the Courant number 0.425 below
+the 3-D limit 0.4529), Gaussian-smoothed start model; 16 shots on a 4 x 4
+surface grid, a 128 x 128 receiver array at 2-cell spacing, 10 Hz Ricker.
+The shots run in groups whose boundary-saving tape fits a 60 GB budget (3
+shots; a group that did not fit would checkpoint every 100 steps).
 
-Prints ONE JSON line.  ``value`` is Gcell-updates/s (runtime-grid cells x
-shots x nt per gradient, forward + adjoint) timed with CUDA events with every
-input resident in HBM; ``e2e`` is the same metric through the public API with
-the model, wavelet and observed data copied from pinned host memory and the
-gradient and loss copied back inside each timed step.  Multi-GPU: shots are
-independent (``--gpus N`` runs N ranks, each with the full 32-shot survey; weak
-scaling), with the per-step gradient all-reduced over NCCL as an FWI step does.
+One bench step is one FWI gradient step: each GPU computes the forward and
+adjoint of one shot group (the survey's shots taken in turn), then one NCCL
+all-reduce sums the loss and the gradient over the GPUs.  ``value`` counts
+runtime-grid cells x shots x nt of every GPU, timed with CUDA events with
+every input resident in HBM (max over ranks); ``e2e`` is the same through the
+public API with the model, wavelet and the group's observed data copied from
+pinned host memory and the gradient and loss read back inside each step.
+
+Other workloads: ``acoustic2d`` (the 32-shot 256 x 768 survey: one step is
+the 32-shot gradient), ``elastic2d`` (the 16-shot 400 x 1200 elastic
+survey), ``acoustic2d_c1`` (96 x 128, one shot) and ``fwi`` (learned vs
+plain FWI).
+
+``--gpus N`` without a launcher starts N ranks itself (torch.distributed.run
+on 127.0.0.1); under torchrun the ranks come from the environment.
 
 ``--impl reference`` times the CPU implementation of the same path (the
 float32 oracle restating the reference's impl='c', all host threads) on a
@@ -196,8 +204,7 @@ class AcousticWorkload:
     cpu_nt = 1000
     # ncu dram__bytes_read.sum + dram__bytes_write.sum of one rev_kernel launch of
     # this grid at 32 shots (241.9 + 69.3 MB; the capture's time axis is 20
-    # steps, which does not change a launch), per shot:
-    # profiles/acoustic2d_c2_launches.md
+    # steps, which does not change a launch), per shot
     traffic = {"bytes_per_shot": 311.2e6 / 32, "source": "ncu, one rev_kernel launch, 256x768 x 32 shots (nt 20)"}
 
     def config(self, args):
@@ -218,7 +225,7 @@ class AcousticWorkload:
                            abcn=ABCN, device=dev, memory=boundary_memory())
         return solver, [vp_true], [vp_init], w, src, rec
 
-    def launches(self):
+    def launches(self, group):
         # per gradient: the forward's prep_kernel and one fwd_kernel per step,
         # the backward's prep_kernel, one rev_kernel per step and finalize_kernel
         return 2 * self.nt + 3
@@ -279,7 +286,7 @@ class AcousticC1Workload:
                            dt=C1_DT, abcn=C1_ABCN, device=dev, memory=boundary_memory())
         return solver, [vp_true], [vp_init], w, src, rec
 
-    def launches(self):
+    def launches(self, group):
         # per gradient: the forward's prep_kernel and one fwd_kernel per step,
         # the backward's prep_kernel, one rev_kernel per step and finalize_kernel
         return 2 * self.nt + 3
@@ -320,7 +327,7 @@ class ElasticWorkload:
                            dt=E_DT, abcn=E_ABCN, device=dev)
         return solver, m_true, m_init, w, src, rec
 
-    def launches(self):
+    def launches(self, group):
         return 5 * self.nt + 2
 
     def cpu_run(self, nt_sample, shots=1):
@@ -333,12 +340,12 @@ class ElasticWorkload:
         return E_RT[0] * E_RT[1] * shots * nt_sample, time.perf_counter() - t0
 
 
-# 3-D workload (--workload acoustic3d): 256^3, dh 10 m, dt 1 ms, nt 2000,
-# order 8, CPML 24; 8-layer dipping model (1500-4000 m/s) with a +600 m/s
-# Gaussian anomaly; 16 shots on a 4 x 4 surface grid, a 128 x 128 receiver
-# array at 2-cell spacing, 10 Hz Ricker.  The 16 shots run as 4 calls of 4
-# shots: the boundary-saving tape of one call (4 shots x 2000 steps of
-# strips) is ~63 GB.
+# 3-D workload (--workload acoustic3d, the default): 256^3, dh 10 m, dt 1 ms,
+# nt 2000, order 8, CPML 24; 8-layer dipping model (1500-4000 m/s) with a
+# +600 m/s Gaussian anomaly; 16 shots on a 4 x 4 surface grid, a 128 x 128
+# receiver array at 2-cell spacing, 10 Hz Ricker.  Shots run in groups whose
+# boundary-saving tape fits the 60 GB budget: 3 shots (47 GB; 4 would be
+# 63 GB).
 A3_N, A3_NT, A3_DT, A3_DH, A3_ABCN = 256, 2000, 0.001, 10.0, 24
 A3_NSHOT, A3_BATCH, A3_F0, A3_DELAY = 16, 4, 10.0, 0.12
 # boundary storage budget of one call: a shot group whose boundary-saving tape
@@ -365,6 +372,9 @@ def acoustic3d_survey(seed=SEED):
     cz, cy, cx = rng.uniform(0.3 * n, 0.7 * n), rng.uniform(0.3 * n, 0.7 * n), rng.uniform(0.3 * n, 0.7 * n)
     vp += 600.0 * np.exp(-((z - cz) ** 2 + (y - cy) ** 2 + (x - cx) ** 2) / (2 * 30.0 ** 2))
     vp_true = vp.astype(np.float32)
+    courant = float(vp_true.max()) * A3_DT / A3_DH
+    if courant >= 0.4529:
+        raise ValueError(f"3-D survey: Courant number {courant:.3f} above the order-8 leapfrog limit 0.4529")
     vp_init = gaussian_filter(vp_true.astype(np.float64), 8.0).astype(np.float32)
     g = np.linspace(n / 8, n - n / 8, 4).astype(np.int64)
     src = np.array([[xs, ys, 2] for ys in g for xs in g], np.int64)
@@ -381,18 +391,20 @@ class Acoustic3DWorkload:
     nt, nshot, rt = A3_NT, A3_NSHOT, A3_RT
     bytes_fwd, bytes_rev = BYTES_FWD, BYTES_REV
     kernel = "sweep::a3d reverse step (a3_step + r3_recon + strip kernels)"
-    cpu_nt = 20
-    # ncu DRAM bytes of a3_step + r3_recon for one shot (881 + 873 MB,
-    # profiles/acoustic3d_c4_kernels.md), scaled by the shots of a reverse step:
-    # both kernels stream every shot's fields once, so traffic grows with shots
-    traffic = {"bytes_per_shot": 881e6 + 873e6,
+    cpu_nt = 16
+    # ncu DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of a3_step +
+    # r3_recon for one 256^3 shot (851 + 856 MB), scaled by the shots of a
+    # reverse step: both kernels stream every shot's fields once, so traffic
+    # grows with the shots
+    traffic = {"bytes_per_shot": 851e6 + 856e6,
                "source": "ncu, a3_step + r3_recon of one 256^3 shot, x shots per step"}
     batch = A3_BATCH
     budget_gb = A3_BUDGET_GB
 
     def config(self, args):
-        return {"workload": f"acoustic3d {A3_N}^3 (runtime {A3_RT[0]}^3), {A3_NSHOT} shots in calls of "
-                            f"{self.batch}, nt {self.nt}, order 8, CPML {A3_ABCN}, fwd+adj gradient, boundary saving",
+        return {"workload": f"acoustic3d {A3_N}^3 (runtime {A3_RT[0]}^3), {A3_NSHOT}-shot survey in calls of "
+                            f"{self.batch} shots, nt {self.nt}, order 8, CPML {A3_ABCN}, fwd+adj gradient, "
+                            f"boundary saving",
                 "grid": [A3_N] * 3, "runtime_grid": list(A3_RT), "shots_per_gpu": A3_NSHOT,
                 "shots_per_call": self.batch, "nt": self.nt, "dh": A3_DH, "dt": A3_DT, "abcn": A3_ABCN,
                 "order": ORDER, "receivers": 128 * 128, "seed": SEED,
@@ -403,7 +415,7 @@ class Acoustic3DWorkload:
                 "memory_rule": f"boundary saving when a call's tape fits {A3_BUDGET_GB:g} GB, else checkpoints "
                                f"every {A3_CKPT} steps; shots per call: the most whose boundary tape fits "
                                f"(at most {A3_BATCH}) unless --shots-per-call is given",
-                "parallelism": f"shots: {A3_NSHOT} per GPU x {args.gpus} GPU(s)"}
+                "courant_max": 4247.13 * A3_DT / A3_DH}
 
     def build(self, dev):
         from sweep_b200 import Acoustic3D, PropTorch
@@ -415,12 +427,12 @@ class Acoustic3DWorkload:
                                                  budget_gb=A3_BUDGET_GB, ckpt_chunks=A3_CKPT))
         return solver, m_true, m_init, w, src, rec
 
-    def launches(self):
-        # per call: forward 4 per step (stencil, strips, injection, gather) and
-        # reverse 7 (adjoint, cotangent injection, reconstruction, strip
-        # restore, strip un-injection, strip image, source re-injection); per
-        # pass prep3 and three pack_prof3, and finalize3
-        return -(-self.nshot // self.batch) * (11 * self.nt + 9)
+    def launches(self, group):
+        # per call (one shot group): forward 4 per step (stencil, strips,
+        # injection, gather) and reverse 7 (adjoint, cotangent injection,
+        # reconstruction, strip restore, strip un-injection, strip image, source
+        # re-injection); per pass prep3 and three pack_prof3, and finalize3
+        return 11 * self.nt + 9
 
     def cpu_run(self, nt_sample, shots=1):
         from oracle import oracle as O
@@ -474,10 +486,19 @@ def run_reference(args, wl):
 
 
 # ---------------------------------------------------------------------- GPU
+def step_shots(k, group, nshot, world, rank):
+    """Shots rank `rank` computes in step `k`: the step's window is the next
+    world x group shots of the survey (cyclically), split into contiguous
+    blocks by sweep_b200.distributed.shot_slice -- the same split
+    sharded_gradient makes, so each rank runs `group` shots of its own."""
+    from sweep_b200.distributed import shot_slice
+    window = [(k * world * group + i) % nshot for i in range(world * group)]
+    return window[shot_slice(len(window), world, rank)]
+
+
 def run_gpu(args, wl):
     import torch
     import torch.distributed as dist
-
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -487,7 +508,7 @@ def run_gpu(args, wl):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
 
-    from sweep_b200.distributed import all_reduce_
+    from sweep_b200.distributed import sharded_gradient
     solver, m_true, m_init, w, src, rec = wl.build(dev)
     solver.autotune = bool(args.autotune)
     src, rec = src[:wl.nshot], rec[:wl.nshot]
@@ -495,56 +516,58 @@ def run_gpu(args, wl):
         # shot groups: the most shots whose boundary-saving tape fits the budget
         per_shot = solver.tape_bytes(len(w), src[:1], rec[:1], [torch.tensor(m, device=dev) for m in m_init])
         wl.batch = max(1, min(wl.batch, wl.nshot, int(wl.budget_gb * 1e9 // per_shot)))
+    group = getattr(wl, "batch", wl.nshot)
     w_d = torch.tensor(w, device=dev)
-    bsz = getattr(wl, "batch", wl.nshot)
-    batches = [slice(b, min(b + bsz, wl.nshot)) for b in range(0, wl.nshot, bsz)]
     with torch.no_grad():
         mt = [torch.tensor(m, device=dev) for m in m_true]
-        # the first call of the shape tunes its schedule (untimed; --no-autotune skips it)
-        obs = torch.cat([solver(w_d, src[sl], rec[sl], models=mt) for sl in batches])
+        # observed data of every shot, modelled once in the true model; the
+        # first call of the shape tunes its schedule (untimed; --no-autotune skips it)
+        obs = torch.cat([solver(w_d, src[b:b + group], rec[b:b + group], models=mt)
+                         for b in range(0, wl.nshot, group)])
         del mt
     ms_d = [torch.tensor(m, device=dev) for m in m_init]
-    schedule = solver.launch_schedule(len(w), src[batches[0]], rec[batches[0]], ms_d)
+    schedule = solver.launch_schedule(len(w), src[:group], rec[:group], ms_d)
     torch.cuda.synchronize()
 
-    def step(ms_in, w_in, obs_in, ev=None):
-        # one gradient of the whole survey: the shot batches run one after the
-        # other and their gradients accumulate into the models' .grad
-        ms = [m.detach().requires_grad_(True) for m in ms_in]
-        loss = 0.0
-        for sl in batches:
+    def step(k, ms_in, w_in, obs_of, ev=None):
+        """One FWI gradient step: this rank's shot group (forward + adjoint),
+        then one SUM all-reduce of the loss and the model gradients over the
+        ranks (sharded_gradient).  obs_of(shots): their observed data."""
+        def compute(_):
+            sh = step_shots(k, group, wl.nshot, world, rank)
+            ms = [m.detach().requires_grad_(True) for m in ms_in]
             e = [torch.cuda.Event(enable_timing=True) for _ in range(3)] if ev is not None else None
             if e: e[0].record()
-            pred = solver(w_in, src[sl], rec[sl], models=ms)
-            lb = 0.5 * ((pred - obs_in[sl]) ** 2).sum()
+            pred = solver(w_in, src[sh], rec[sh], models=ms)
+            lb = 0.5 * ((pred - obs_of(sh)) ** 2).sum()
             if e: e[1].record()
             lb.backward()
             if e:
                 e[2].record()
                 ev.append(e)
-            loss = loss + lb.detach()
-        gs = [m.grad for m in ms]
-        if world > 1:
-            all_reduce_(gs)                  # shot-parallel FWI: one SUM per model gradient
-        return loss, gs
+            return lb.detach(), [m.grad for m in ms]
+        return sharded_gradient(compute, world * group)
 
     def barrier():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
 
-    for _ in range(args.warmup):
-        step(ms_d, w_d, obs)
+    def obs_dev(sh):
+        return obs[sh]
+
+    for k in range(args.warmup):
+        step(k, ms_d, w_d, obs_dev)
     barrier()
 
     # ---- device-resident timing
-    evs = [[] for _ in range(args.steps)]     # per step: (start, forward done, backward done) per batch
+    evs = [[] for _ in range(args.steps)]     # per step: (start, forward done, backward done)
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         barrier()
         t0.record()
         for k in range(args.steps):
-            step(ms_d, w_d, obs, evs[k])
+            step(args.warmup + k, ms_d, w_d, obs_dev, evs[k])
         t1.record()
         barrier()
     ms = t0.elapsed_time(t1) / args.steps
@@ -556,30 +579,45 @@ def run_gpu(args, wl):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t)
 
-    # ---- end-to-end through the public API with host buffers
+    # ---- end-to-end through the public API with host buffers: each step
+    # copies the models, the wavelet and its shots' observed data from pinned
+    # host memory and reads the gradients and the loss back
     ms_h = [torch.tensor(m).pin_memory() for m in m_init]
     w_h = torch.tensor(w).pin_memory()
     obs_h = obs.cpu().pin_memory()
     g_h = [torch.empty(m.shape, dtype=torch.float32).pin_memory() for m in m_init]
-    h2d = sum(m.numel() * 4 for m in ms_h) + w_h.numel() * 4 + obs_h.numel() * 4
-    d2h = sum(g.numel() * 4 for g in g_h) + 4
+    h2d = sum(m.numel() * 4 for m in ms_h) + w_h.numel() * 4 + obs_h[:group].numel() * 4
+    d2h = sum(g.numel() * 4 for g in g_h) + 8
 
-    def e2e_step():
-        loss, gs = step([m.to(dev, non_blocking=True) for m in ms_h], w_h.to(dev, non_blocking=True),
-                        obs_h.to(dev, non_blocking=True))
+    o_d = torch.empty((group,) + tuple(obs.shape[1:]), dtype=obs.dtype, device=dev)
+
+    def obs_host(sh):
+        # the shots' observed data from pinned host memory, one copy per run
+        # of consecutive shots
+        i = 0
+        while i < len(sh):
+            j = i + 1
+            while j < len(sh) and sh[j] == sh[j - 1] + 1:
+                j += 1
+            o_d[i:j].copy_(obs_h[sh[i]:sh[j - 1] + 1], non_blocking=True)
+            i = j
+        return o_d[:len(sh)]
+
+    def e2e_step(k):
+        loss, gs = step(k, [m.to(dev, non_blocking=True) for m in ms_h], w_h.to(dev, non_blocking=True), obs_host)
         for gh, g in zip(g_h, gs):
             gh.copy_(g, non_blocking=True)
         float(loss)
 
     e2e_ms = float("nan")
     if not args.no_e2e:
-        for _ in range(2):
-            e2e_step()
+        for k in range(2):
+            e2e_step(k)
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        for _ in range(args.steps):
-            e2e_step()
+        for k in range(args.steps):
+            e2e_step(k)
         e1.record()
         barrier()
         e2e_ms = e0.elapsed_time(e1) / args.steps
@@ -588,7 +626,8 @@ def run_gpu(args, wl):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t)
 
-    cells = int(np.prod(wl.rt)) * wl.nshot * wl.nt
+    per_launch_cells = int(np.prod(wl.rt)) * group
+    cells = per_launch_cells * wl.nt                  # per rank and step
     value = cells * world / (ms * 1e-3) / 1e9
     e2e_value = cells * world / (e2e_ms * 1e-3) / 1e9
     peaks = {}
@@ -596,7 +635,6 @@ def run_gpu(args, wl):
     if pk.exists():
         peaks = json.loads(pk.read_text())
     hbm = float(peaks.get("hbm_gbs", 6650.0))
-    per_launch_cells = int(np.prod(wl.rt)) * wl.nshot
     rev_launch_ms = rev_ms / wl.nt
     achieved = per_launch_cells * wl.bytes_rev / (rev_launch_ms * 1e-3) / 1e9
     line = {
@@ -604,24 +642,29 @@ def run_gpu(args, wl):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded layered model, see config)",
-        "config": dict(wl.config(args), schedule=schedule, memory=solver.last_memory,
+        "config": dict(wl.config(args), shots_per_step_per_gpu=group,
+                       step=f"one FWI gradient step: {group} shot(s) per GPU (forward + adjoint), the "
+                            f"survey's shots taken in turn, then one all-reduce of the gradient over the GPUs",
+                       parallelism=f"shots: {group} per GPU per step x {world} GPU(s), NCCL all-reduce "
+                                   f"of the gradient (weak scaling)",
+                       schedule=schedule, memory=solver.last_memory,
                        autotune=None if solver.tune_report is None else
                        {"seconds": solver.tune_report["seconds"], "nt": solver.tune_report["nt"],
-                        "trials_ms": {k: {str(v): 1e3 * t for v, t in r.items()}
-                                      for k, r in solver.tune_report["trials"].items()}}),
+                        "trials_ms": {kk: {str(v): 1e3 * t for v, t in r.items()}
+                                      for kk, r in solver.tune_report["trials"].items()}}),
         "forward_ms": fwd_ms, "backward_ms": rev_ms,
         "roofline": {"kernel": wl.kernel,
                      "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm,
-                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if pk.exists() else "fallback 6650",
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if pk.exists() else "fallback 6650",
                      "algorithmic_bytes_per_launch": per_launch_cells * wl.bytes_rev,
                      "launch_ms": rev_launch_ms,
                      "launch_ms_how": "CUDA events around the backward call on the launch stream / nt",
-                     "traffic": wl.traffic["bytes_per_shot"] * wl.nshot if wl.traffic else None,
+                     "traffic": wl.traffic["bytes_per_shot"] * group if wl.traffic else None,
                      "traffic_source": wl.traffic["source"] if wl.traffic else None},
         "forward_roofline": {"achieved": per_launch_cells * wl.bytes_fwd / (fwd_ms / wl.nt * 1e-3) / 1e9,
                              "unit": "GB/s", "bytes_per_cell_step": wl.bytes_fwd},
-        "gpu_launches": args.steps * wl.launches(),
+        "gpu_launches": args.steps * wl.launches(group),
         "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": "Gcell/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
@@ -692,6 +735,19 @@ def run_fwi(args):
     print(json.dumps(line))
 
 
+def relaunch(n):
+    """Start n ranks of this same command line under torch.distributed.run
+    (one process per GPU, rendezvous on 127.0.0.1) and exit with its status."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), str(Path(__file__).resolve()),
+           *sys.argv[1:]]
+    sys.exit(subprocess.call(cmd))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -709,9 +765,9 @@ def main():
                     help="skip the end-to-end leg (long workloads; the bench line then has no e2e value)")
     ap.add_argument("--pairs", type=int, default=2000, help="fwi workload: training pairs")
     ap.add_argument("--train-steps", type=int, default=20000, help="fwi workload: U-Net training steps")
-    ap.add_argument("--workload", default="acoustic2d", choices=sorted(WORKLOADS) + ["fwi"],
-                    help="acoustic2d: the 32-shot 256x768 survey (default); elastic2d: the 16-shot "
-                         "400x1200 elastic survey")
+    ap.add_argument("--workload", default="acoustic3d", choices=sorted(WORKLOADS) + ["fwi"],
+                    help="acoustic3d: the 16-shot 256^3 survey (default); acoustic2d: the 32-shot 256x768 "
+                         "survey; elastic2d: the 16-shot 400x1200 elastic survey")
     ap.add_argument("--graph-steps", type=int, default=None,
                     help="time steps per captured CUDA graph in the step loops (0: plain stream launches; "
                          "default: the library's built-in choice)")
@@ -723,6 +779,8 @@ def main():
     ap.add_argument("--shots", type=int, default=None,
                     help="fewer shots (profiling captures of a few GB only; the bench line is for the full survey)")
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        relaunch(args.gpus)
     STRIPS[:] = [args.storage, args.strip_dtype]
     if args.graph_steps is not None:
         os.environ["SWEEP_B200_GRAPH_STEPS"] = str(int(args.graph_steps))
