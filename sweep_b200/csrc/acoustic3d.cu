@@ -247,17 +247,18 @@ struct F3 {
 
 // Forward plane ring: stage q holds the wavefield plane u(q) with its x / y
 // halo, and the centre tiles of u_prev(q - M) and of the model for plane
-// q - M.  Computing plane z needs stages z - M .. z + M; with NS3 stages the
-// loads run NS3 - 2M - 1 = 3 planes ahead of the compute, TMA-issued by one
-// thread on one mbarrier per stage.
-constexpr int NS3 = 12;
-constexpr int NSC3 = NS3 - 2 * M;   // centre ring of the reverse kernels
+// q - M.  Each thread keeps the nine z-taps of its column in a register
+// queue: plane z reads its x / y taps from stage z and pushes the centre of
+// stage z + M into the queue, so stages z .. z + M must have landed; with NF3
+// stages the loads run NF3 - M - 1 planes ahead of the compute, TMA-issued by
+// one thread on one mbarrier per stage.
+constexpr int NF3 = 11;
 constexpr int CN3 = BXC * BYC;
 struct F3Smem {
-    float u[NS3][PN];
-    float up[NS3][CN3];
-    float cf[NS3][CN3];
-    uint64_t bar[NS3];
+    float u[NF3][PN];
+    float up[NF3][CN3];
+    float cf[NF3][CN3];
+    uint64_t bar[NF3];
 };
 
 struct F3Maps {
@@ -287,8 +288,8 @@ __global__ void __launch_bounds__(NTH, 4) f3_step(const __grid_constant__ F3Maps
     const long long bo = (long long)b * P.S;
     const long long colo = (long long)iy * P.P + ix;
     const int q0 = zb - M, q1 = ze + M;                // stages [q0, q1)
-    auto slot = [&](int q) { return (q - q0) % NS3; };
-    auto parity = [&](int q) { return (uint32_t)(((q - q0) / NS3) & 1); };
+    auto slot = [&](int q) { return (q - q0) % NF3; };
+    auto parity = [&](int q) { return (uint32_t)(((q - q0) / NF3) & 1); };
     auto issue = [&](int q) {
         const int sl = slot(q);
         const bool cen = q - M >= zb && q - M < ze;     // u_prev / model of plane q - M
@@ -300,13 +301,13 @@ __global__ void __launch_bounds__(NTH, 4) f3_step(const __grid_constant__ F3Maps
         }
     };
     if (tid == 0) {
-        for (int i = 0; i < NS3; ++i) tma::mbar_init(&sm.bar[i], 1);
+        for (int i = 0; i < NF3; ++i) tma::mbar_init(&sm.bar[i], 1);
         tma::fence_barrier_init();
     }
     __syncthreads();
     int next = q0;                                     // first stage not yet issued (thread 0)
     if (tid == 0)
-        for (; next < min(q1, q0 + NS3); ++next) issue(next);
+        for (; next < min(q1, q0 + NF3); ++next) issue(next);
     // a failed wait: drain (bounded) every stage still in flight, then exit
     auto fail = [&](int q) {
         if (tid == 0)
@@ -317,19 +318,23 @@ __global__ void __launch_bounds__(NTH, 4) f3_step(const __grid_constant__ F3Maps
     // block barrier a plane has (results are then invalid and the host
     // reports the error).  Leaving, thread 0 waits (bounded) for every stage
     // still in flight: from q0 at the first plane (no slot reused yet), else
-    // from z + M (every earlier stage was waited for at an earlier barrier).
+    // from z + M (every earlier stage was waited for at an earlier plane).
     bool bad = false;
     auto await = [&](int q) {
         if (!tma::mbar_wait(&sm.bar[slot(q)], parity(q), err, ERR_WAIT_F3)) bad = true;
     };
-    for (int q = q0; q < zb + M; ++q) await(q);
-    const int cidx = (ty + M) * PW + (tx + M);
+    const int cidx = (ty + M) * PW + (tx + M), cc = ty * BXC + tx;
+    // the z-queue: u of planes z - M .. z + M at this column (q[M] the centre)
+    float q[2 * M + 1];
+#pragma unroll
+    for (int k = 0; k < 2 * M; ++k) {
+        await(q0 + k);
+        q[k] = sm.u[slot(q0 + k)][cidx];
+    }
     for (int z = zb; z < ze; ++z) {
         await(z + M);
+        q[2 * M] = sm.u[slot(z + M)][cidx];
         if (col) {
-            float q[2 * M + 1];
-#pragma unroll
-            for (int k = 0; k <= 2 * M; ++k) q[k] = sm.u[slot(z - M + k)][cidx];
             const float* p = sm.u[slot(z)] + cidx;
             const float lx = lap_p(p, 1, P, P.dx);
             const float ly = lap_p(p, PW, P, P.dy);
@@ -383,12 +388,14 @@ __global__ void __launch_bounds__(NTH, 4) f3_step(const __grid_constant__ F3Maps
                     w += lz;
                 }
             }
-            const int cc = ty * BXC + tx;
             F.u_next[i] = 2.f * q[M] - sm.up[slot(z + M)][cc] + sm.cf[slot(z + M)][cc] * w;
         }
-        // every thread is done with stage z - M (and has waited for z + M)
+#pragma unroll
+        for (int k = 0; k < 2 * M; ++k) q[k] = q[k + 1];
+        // every thread is done with stage z and has waited for z + M
         if (__syncthreads_or(bad)) { fail(z == zb ? q0 : z + M); return; }
-        if (tid == 0 && next < q1) issue(next++);      // reuses the slot of stage z - M
+        if (tid == 0)
+            for (; next < q1 && next <= z + NF3; ++next) issue(next);     // slots of stages <= z are free
     }
 }
 
@@ -557,52 +564,55 @@ struct A3 {
 
 // The transposed CPML terms of one axis at linear offset i, stride st,
 // packed profiles pr = {a, b, db, da} at axis index c (reference
-// adjoint_split.cu:205-255).  cav / lav: (v*v)*dt^2 and lambda at the 2M+1
-// cells along the axis around i (from shared memory), gw = their product at i.
+// adjoint_split.cu:205-255).  g: gw = ((v*v)*dt^2) * lambda at the 2M+1
+// cells along the axis around i (g[M] at i, from shared memory or the
+// z-queue).
 __device__ __forceinline__ void adj_axis(const Params& P, const float4* __restrict__ pr,
-                                         const float (&cav)[2 * M + 1],
-                                         const float (&lav)[2 * M + 1], const float* __restrict__ psi,
-                                         const float* __restrict__ zeta, long long i, long long st, int c, float gw,
+                                         const float (&g)[2 * M + 1], const float* __restrict__ psi,
+                                         const float* __restrict__ zeta, long long i, long long st, int c,
                                          float h, float& L, float& Dg, float* pso, float* zto)
 {
+    const float gw = g[M];
     const float4 p0 = __ldg(pr + c);
     const float a_ = p0.x, b_ = p0.y, da = p0.w;
-    const float gt0 = b_ * zeta[i] + (1.0f + b_) * gw;
+    const float z0 = zeta[i];
+    const float gt0 = b_ * z0 + (1.0f + b_) * gw;
     const float l0 = (1.0f + b_) * gt0;
     float Lq = 0.0f, Dgg = 0.0f, Dq = 0.0f;
+    const float* zp = zeta + i;
+    const float* pp_ = psi + i;
 #pragma unroll
     for (int k = 1; k <= M; ++k) {
-        const long long np = i + k * st, nm = i - k * st;
         const float4 pp = __ldg(pr + c + k), pm = __ldg(pr + c - k);
         const float bp = pp.y, bm = pm.y;
-        const float tp = bp * zeta[np] + ((1.0f + bp) * cav[M + k]) * lav[M + k];
-        const float tm = bm * zeta[nm] + ((1.0f + bm) * cav[M - k]) * lav[M - k];
+        const float tp = bp * zp[k * st] + (1.0f + bp) * g[M + k];
+        const float tm = bm * zp[-k * st] + (1.0f + bm) * g[M - k];
         Lq += P.lc[k] * (tap((1.0f + bp) * tp, l0) + tap((1.0f + bm) * tm, l0));
-        Dgg += P.gc[k] * ((bp * psi[np] + pp.z * tp) - (bm * psi[nm] + pm.z * tm));
+        Dgg += P.gc[k] * ((bp * pp_[k * st] + pp.z * tp) - (bm * pp_[-k * st] + pm.z * tm));
         Dq += P.gc[k] * (pp.x * tp - pm.x * tm);
     }
     L = Lq * (1.0f / (h * h));
     Dg = Dgg * (1.0f / h);
     Dq = Dq * (1.0f / h);
-    pso[i] = (a_ * psi[i] + da * gt0) - Dq;
-    zto[i] = a_ * (zeta[i] + gw);
+    pso[i] = (a_ * pp_[0] + da * gt0) - Dq;
+    zto[i] = a_ * (z0 + gw);
 }
 
 // Adjoint plane ring: stage q holds lambda(q) and (v*v)*dt^2 of plane q with
-// their x / y halo; lambda(it+1) of plane q - M sits in a centre ring of
-// NSC3 stages.  A CTA whose columns and planes all lie in the clear box turns
-// the model plane into gw = ((v*v)*dt^2) * lambda in place once per stage;
-// the others form the tap products from the two planes.
-// The adjoint's ring is two stages shorter than the forward's (planes one
-// ahead instead of three), so that four CTAs fit an SM.
-constexpr int NSA = 2 * M + 2;
-constexpr int NSCA = NSA - 2 * M;
+// their x / y halo, and lambda(it+1) of plane q - M.  Each thread keeps
+// gw = ((v*v)*dt^2) * lambda of the nine z-taps of its column in a register
+// queue (plane z pushes the centre of stage z + M), and the CTA forms the gw
+// plane of the next plane's x / y taps once, in a double buffer, at the end
+// of each plane.  Stages z .. z + M must have landed at plane z; with NA3
+// stages the loads run NA3 - M - 1 planes ahead.
+constexpr int NA3 = 8;
 
 struct A3Smem {
-    float l[NSA][PN];
-    float c[NSA][PN];
-    float lp[NSCA][CN3];
-    uint64_t bar[NSA];
+    float l[NA3][PN];
+    float c[NA3][PN];
+    float lp[NA3][CN3];
+    float gw[2][PN];
+    uint64_t bar[NA3];
 };
 
 struct A3Maps {
@@ -630,133 +640,122 @@ __global__ void __launch_bounds__(NTH, 4) a3_step(const __grid_constant__ A3Maps
     const long long bo = (long long)b * P.S;
     const long long colo = (long long)iy * P.P + ix;
     const float invdx2 = 1.0f / (P.dx * P.dx), invdy2 = 1.0f / (P.dy * P.dy), invdz2 = 1.0f / (P.dz * P.dz);
-    // clean: every column of the CTA inside the x / y clear box, every plane inside the z one
-    const int cx0 = blockIdx.x * BXC, cy0 = blockIdx.y * BYC;
-    const bool clean = cx0 >= P.qx0 && cx0 + BXC <= P.qx1 && cy0 >= P.qy0 && cy0 + BYC <= P.qy1 &&
-                       zb >= P.qz0 && ze <= P.qz1;
+    const bool inx = ix < P.qx0 || ix >= P.qx1;
+    const bool iny = iy < P.qy0 || iy >= P.qy1;
     const int q0 = zb - M, q1 = ze + M;
-    auto slot = [&](int q) { return (q - q0) % NSA; };
-    auto cslot = [&](int z) { return (z - zb) % NSCA; };
-    auto parity = [&](int q) { return (uint32_t)(((q - q0) / NSA) & 1); };
+    auto slot = [&](int q) { return (q - q0) % NA3; };
+    auto parity = [&](int q) { return (uint32_t)(((q - q0) / NA3) & 1); };
     auto issue = [&](int q) {
         const int sl = slot(q), z = q - M;
         const bool cen = z >= zb && z < ze;
         tma::mbar_expect_tx(&sm.bar[sl], (uint32_t)(2 * PN + (cen ? CN3 : 0)) * 4u);
         tma::load_4d(sm.l[sl], &MP.lh[lnow], &sm.bar[sl], gx0, gy0, q, b);
         tma::load_3d(sm.c[sl], &MP.ch, &sm.bar[sl], gx0, gy0, q);
-        if (cen) tma::load_4d(sm.lp[cslot(z)], &MP.lc[lprev], &sm.bar[sl], gx0 + M, gy0 + M, z, b);
+        if (cen) tma::load_4d(sm.lp[sl], &MP.lc[lprev], &sm.bar[sl], gx0 + M, gy0 + M, z, b);
     };
     if (tid == 0) {
-        for (int i = 0; i < NSA; ++i) tma::mbar_init(&sm.bar[i], 1);
+        for (int i = 0; i < NA3; ++i) tma::mbar_init(&sm.bar[i], 1);
         tma::fence_barrier_init();
     }
     __syncthreads();
     int next = q0;
     if (tid == 0)
-        for (; next < min(q1, q0 + NSA); ++next) issue(next);
+        for (; next < min(q1, q0 + NA3); ++next) issue(next);
     auto fail = [&](int q) {
         if (tid == 0)
             for (int r = q; r < next; ++r) tma::mbar_wait(&sm.bar[slot(r)], parity(r), err, ERR_WAIT_F3);
     };
     // Each thread waits for the stages it reads itself; a failed wait is
-    // noted and the CTA leaves together at the next block barrier.  A clean
-    // CTA turns each stage's model plane into gw = ((v*v)*dt^2) * lambda, each
-    // thread its share: the first plane's stages before one barrier, then
-    // stage z + M + 1 at the end of plane z, before the barrier that ends the
-    // plane -- one barrier per plane in every CTA.
+    // noted and the CTA leaves together at the next block barrier, thread 0
+    // draining the loads in flight (from q0 before the first plane's barrier,
+    // else from z + M).
     bool bad = false;
     auto await = [&](int q) {
         if (!tma::mbar_wait(&sm.bar[slot(q)], parity(q), err, ERR_WAIT_F3)) bad = true;
     };
+    // the gw plane of plane q into gw buffer q & 1 (stage q has landed)
     auto convert = [&](int q) {
-        float* c = sm.c[slot(q)];
+        float* g = sm.gw[q & 1];
+        const float* c = sm.c[slot(q)];
         const float* l = sm.l[slot(q)];
-        for (int e = tid; e < PN; e += NTH) c[e] = c[e] * l[e];
+        for (int e = tid; e < PN; e += NTH) g[e] = c[e] * l[e];
     };
-    if (clean) {
-        for (int q = q0; q <= zb + M; ++q) { await(q); convert(q); }
-        if (__syncthreads_or(bad)) { fail(q0); return; }
-    } else {
-        for (int q = q0; q < zb + M; ++q) await(q);
-    }
     const int cidx = (ty + M) * PW + (tx + M), cc = ty * BXC + tx;
+    float qg[2 * M + 1];                                // gw of planes z - M .. z + M at this column
+#pragma unroll
+    for (int k = 0; k < 2 * M; ++k) {
+        await(q0 + k);
+        qg[k] = sm.c[slot(q0 + k)][cidx] * sm.l[slot(q0 + k)][cidx];
+    }
+    convert(zb);
+    if (__syncthreads_or(bad)) { fail(q0); return; }
+    // the stages before zb fed only the queue: their slots are free now, and
+    // refilling them brings stage zb + M (NA3 < 2M + 1 holds it back so far)
+    if (tid == 0)
+        for (; next < q1 && next < zb + NA3; ++next) issue(next);
     for (int z = zb; z < ze; ++z) {
-        if (!clean) await(z + M);
+        await(z + M);
+        qg[2 * M] = sm.c[slot(z + M)][cidx] * sm.l[slot(z + M)][cidx];
         if (col) {
-            const float* pl = sm.l[slot(z)] + cidx;
-            const float* pc = sm.c[slot(z)] + cidx;
-            // gw at offset o of plane slot s
-            auto gwat = [&](int s, int o) { return clean ? sm.c[s][cidx + o] : sm.c[s][cidx + o] * sm.l[s][cidx + o]; };
+            const float* g = sm.gw[z & 1] + cidx;
             const long long ic = z * P.SP + colo;
             const long long i = bo + ic;
-            const float gun = pl[0];
-            const float gw = clean ? pc[0] : pc[0] * gun;
-            const bool inx = ix < P.qx0 || ix >= P.qx1;
-            const bool iny = iy < P.qy0 || iy >= P.qy1;
+            const float gun = sm.l[slot(z)][cidx];
+            const float gw = qg[M];
             const bool inz = z < P.qz0 || z >= P.qz1;
-            const float lprevv = sm.lp[cslot(z)][cc];
-            const int sz = slot(z);
+            const float lprevv = sm.lp[slot(z + M)][cc];
             if (!inx && !iny && !inz) {
                 float lapx = 0.0f, lapy = 0.0f, lapz = 0.0f;
 #pragma unroll
                 for (int k = 1; k <= M; ++k) {
-                    lapx += P.lc[k] * (tap(gwat(sz, k), gw) + tap(gwat(sz, -k), gw));
-                    lapy += P.lc[k] * (tap(gwat(sz, k * PW), gw) + tap(gwat(sz, -k * PW), gw));
-                    lapz += P.lc[k] * (tap(gwat(slot(z + k), 0), gw) + tap(gwat(slot(z - k), 0), gw));
+                    lapx += P.lc[k] * (tap(g[k], gw) + tap(g[-k], gw));
+                    lapy += P.lc[k] * (tap(g[k * PW], gw) + tap(g[-k * PW], gw));
+                    lapz += P.lc[k] * (tap(qg[M + k], gw) + tap(qg[M - k], gw));
                 }
                 A.l_next[i] = 2.0f * gun - lprevv + lapx * invdx2 + lapy * invdy2 + lapz * invdz2;
             } else {
                 float Lx, Ly, Lz, Dgx = 0.f, Dgy = 0.f, Dgz = 0.f;
-                float cav[2 * M + 1], lav[2 * M + 1];
+                float ga[2 * M + 1];
                 if (inx) {
 #pragma unroll
-                    for (int k = -M; k <= M; ++k) { cav[M + k] = pc[k]; lav[M + k] = pl[k]; }
-                    adj_axis(P, P.px, cav, lav, A.px + bo, A.zx + bo, ic, 1, ix, gw, P.dx, Lx, Dgx, A.pxo + bo,
-                             A.zxo + bo);
+                    for (int k = -M; k <= M; ++k) ga[M + k] = g[k];
+                    adj_axis(P, P.px, ga, A.px + bo, A.zx + bo, ic, 1, ix, P.dx, Lx, Dgx, A.pxo + bo, A.zxo + bo);
                 } else {
                     Lx = 0.0f;
 #pragma unroll
-                    for (int k = 1; k <= M; ++k) Lx += P.lc[k] * (tap(gwat(sz, k), gw) + tap(gwat(sz, -k), gw));
+                    for (int k = 1; k <= M; ++k) Lx += P.lc[k] * (tap(g[k], gw) + tap(g[-k], gw));
                     Lx *= invdx2;
                 }
                 if (iny) {
 #pragma unroll
-                    for (int k = -M; k <= M; ++k) { cav[M + k] = pc[k * PW]; lav[M + k] = pl[k * PW]; }
-                    adj_axis(P, P.py, cav, lav, A.py + bo, A.zy + bo, ic, P.P, iy, gw, P.dy, Ly, Dgy, A.pyo + bo,
+                    for (int k = -M; k <= M; ++k) ga[M + k] = g[k * PW];
+                    adj_axis(P, P.py, ga, A.py + bo, A.zy + bo, ic, P.P, iy, P.dy, Ly, Dgy, A.pyo + bo,
                              A.zyo + bo);
                 } else {
                     Ly = 0.0f;
 #pragma unroll
-                    for (int k = 1; k <= M; ++k)
-                        Ly += P.lc[k] * (tap(gwat(sz, k * PW), gw) + tap(gwat(sz, -k * PW), gw));
+                    for (int k = 1; k <= M; ++k) Ly += P.lc[k] * (tap(g[k * PW], gw) + tap(g[-k * PW], gw));
                     Ly *= invdy2;
                 }
                 if (inz) {
-#pragma unroll
-                    for (int k = -M; k <= M; ++k) {
-                        cav[M + k] = sm.c[slot(z + k)][cidx];
-                        lav[M + k] = sm.l[slot(z + k)][cidx];
-                    }
-                    adj_axis(P, P.pz, cav, lav, A.pz + bo, A.zz + bo, ic, P.SP, z, gw, P.dz, Lz, Dgz, A.pzo + bo,
-                             A.zzo + bo);
+                    adj_axis(P, P.pz, qg, A.pz + bo, A.zz + bo, ic, P.SP, z, P.dz, Lz, Dgz, A.pzo + bo, A.zzo + bo);
                 } else {
                     Lz = 0.0f;
 #pragma unroll
-                    for (int k = 1; k <= M; ++k)
-                        Lz += P.lc[k] * (tap(gwat(slot(z + k), 0), gw) + tap(gwat(slot(z - k), 0), gw));
+                    for (int k = 1; k <= M; ++k) Lz += P.lc[k] * (tap(qg[M + k], gw) + tap(qg[M - k], gw));
                     Lz *= invdz2;
                 }
                 A.l_next[i] = 2.0f * gun - lprevv + (Lx + Ly + Lz - Dgx - Dgy - Dgz);
             }
         }
-        // the last stage every thread has waited for.  The ring holds exactly
-        // NSA = 2M + 2 stages: stage z + M + 2 is issued into the slot of
-        // z - M only after the barrier that ends plane z, so no thread still
-        // reads that slot when it is refilled
-        int last = z + M;
-        if (clean && z + 1 < ze) { await(z + M + 1); convert(z + M + 1); last = z + M + 1; }
-        if (__syncthreads_or(bad)) { fail(z == zb && !clean ? q0 : last); return; }
-        if (tid == 0 && next < q1) issue(next++);
+#pragma unroll
+        for (int k = 0; k < 2 * M; ++k) qg[k] = qg[k + 1];
+        // the next plane's gw (stage z + 1 has landed: z + 1 <= z + M); the
+        // buffer it overwrites was last read in plane z - 1
+        if (z + 1 < ze) convert(z + 1);
+        if (__syncthreads_or(bad)) { fail(z + M); return; }
+        if (tid == 0)
+            for (; next < q1 && next <= z + NA3; ++next) issue(next);    // slots of stages <= z are free
     }
 }
 
@@ -767,15 +766,19 @@ struct R3 {
     float *gacc, *gcomp, *is, *ir;                          // per-shot slots (B, S)
 };
 
-// Reconstruction plane ring: the halo planes of u(it) ring as in the
-// forward (NS3 stages); the per-plane centre tiles -- u(it+1), lambda(it),
-// the two model fields and the two Kahan slots -- sit in a ring of
-// NSC3 = NS3 - 2M stages, filled with the halo plane M planes ahead and
-// counted on its barrier.
+// Reconstruction plane ring: stage q holds the halo plane u(it)(q); the
+// per-plane centre tiles of plane q - M -- u(it+1), lambda(it), the two model
+// fields and the two Kahan slots -- sit in a ring of NRC3 stages indexed by
+// plane, filled with stage q and counted on its barrier.  Each thread keeps
+// the nine z-taps of its column in a register queue (plane z pushes the
+// centre of stage z + M), so stages z .. z + M must have landed at plane z:
+// the halo loads run NR3 - M - 1 planes ahead, the centre tiles NRC3 - 1.
+constexpr int NR3 = 9;
+constexpr int NRC3 = NR3 - M;
 struct R3Smem {
-    float u[NS3][PN];
-    float c[NSC3][6][CN3];
-    uint64_t bar[NS3];
+    float u[NR3][PN];
+    float c[NRC3][6][CN3];
+    uint64_t bar[NR3];
 };
 
 struct R3Maps {
@@ -805,9 +808,9 @@ __global__ void __launch_bounds__(NTH, 4) r3_recon(const __grid_constant__ R3Map
     const long long colo = (long long)iy * P.P + ix;
     const float dt2 = P.dt * P.dt;
     const int q0 = zb - M, q1 = ze + M;
-    auto slot = [&](int q) { return (q - q0) % NS3; };
-    auto cslot = [&](int z) { return (z - zb) % NSC3; };
-    auto parity = [&](int q) { return (uint32_t)(((q - q0) / NS3) & 1); };
+    auto slot = [&](int q) { return (q - q0) % NR3; };
+    auto cslot = [&](int z) { return (z - zb) % NRC3; };
+    auto parity = [&](int q) { return (uint32_t)(((q - q0) / NR3) & 1); };
     auto issue = [&](int q) {
         const int sl = slot(q), z = q - M;
         const bool cen = z >= zb && z < ze;
@@ -825,13 +828,16 @@ __global__ void __launch_bounds__(NTH, 4) r3_recon(const __grid_constant__ R3Map
         }
     };
     if (tid == 0) {
-        for (int i = 0; i < NS3; ++i) tma::mbar_init(&sm.bar[i], 1);
+        for (int i = 0; i < NR3; ++i) tma::mbar_init(&sm.bar[i], 1);
         tma::fence_barrier_init();
     }
     __syncthreads();
+    // The first issue fills the halo ring; a centre slot is refilled with a
+    // halo stage, so the halo stages issued up front are capped at M + NRC3
+    // (their centre tiles cover planes zb .. zb + NRC3 - 1).
     int next = q0;
     if (tid == 0)
-        for (; next < min(q1, q0 + NS3); ++next) issue(next);
+        for (; next < min(q1, q0 + M + NRC3); ++next) issue(next);
     auto fail = [&](int q) {
         if (tid == 0)
             for (int r = q; r < next; ++r) tma::mbar_wait(&sm.bar[slot(r)], parity(r), err, ERR_WAIT_F3);
@@ -841,14 +847,17 @@ __global__ void __launch_bounds__(NTH, 4) r3_recon(const __grid_constant__ R3Map
     auto await = [&](int q) {
         if (!tma::mbar_wait(&sm.bar[slot(q)], parity(q), err, ERR_WAIT_F3)) bad = true;
     };
-    for (int q = q0; q < zb + M; ++q) await(q);
     const int cidx = (ty + M) * PW + (tx + M), cc = ty * BXC + tx;
+    float q[2 * M + 1];
+#pragma unroll
+    for (int k = 0; k < 2 * M; ++k) {
+        await(q0 + k);
+        q[k] = sm.u[slot(q0 + k)][cidx];
+    }
     for (int z = zb; z < ze; ++z) {
         await(z + M);
+        q[2 * M] = sm.u[slot(z + M)][cidx];
         if (col) {
-            float q[2 * M + 1];
-#pragma unroll
-            for (int k = 0; k <= 2 * M; ++k) q[k] = sm.u[slot(z - M + k)][cidx];
             const float* p = sm.u[slot(z)] + cidx;
             const float w = (lap_p(p, 1, P, P.dx) + lap_p(p, PW, P, P.dy)) + lap_q(q, P, P.dz);
             const float(*c)[CN3] = sm.c[cslot(z)];
@@ -865,8 +874,13 @@ __global__ void __launch_bounds__(NTH, 4) r3_recon(const __grid_constant__ R3Map
             R.gacc[i] = t;
             if (R.is) { R.is[i] += utt * utt; R.ir[i] += lam * lam; }
         }
+#pragma unroll
+        for (int k = 0; k < 2 * M; ++k) q[k] = q[k + 1];
         if (__syncthreads_or(bad)) { fail(z == zb ? q0 : z + M); return; }
-        if (tid == 0 && next < q1) issue(next++);
+        // after plane z the halo slots of stages <= z and the centre slot of
+        // plane z are free: stage s refills centre slot s - M, so s <= z + NRC3
+        if (tid == 0)
+            for (; next < q1 && next <= min(z + NR3, z + M + NRC3); ++next) issue(next);
     }
 }
 
