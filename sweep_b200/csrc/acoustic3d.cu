@@ -59,6 +59,8 @@ struct Params {
     int zc, nzc;                               // z chunk length, chunks
     int graph_steps;                           // host only: time steps per captured CUDA graph
     float dt, dz, dy, dx;
+    float ih2z, ih2y, ih2x;                    // 1 / h^2 per axis
+    float ihz, ihy, ihx;                       // 1 / h per axis
     float lc[M + 1], gc[M + 1];
     int z0, z1, y0, y1, x0, x1;                // physical box
     int ex0, ex1, ey0, ey1, ez0, ez1;          // forward CPML branch: ix < ex0 || ix >= ex1 ...
@@ -77,45 +79,57 @@ struct Params {
 // ------------------------------------------------------------------ device
 __device__ __forceinline__ float tap(float uk, float u0) { return __fsub_rn(uk, u0); }
 
-// difference-form Laplacian at p along stride st (reference laplace.cuh:327-380)
-__device__ __forceinline__ float lap_p(const float* p, long long st, const Params& P, float h)
+// difference-form Laplacian at p along stride st (reference laplace.cuh:327-380),
+// scaled by ih2 = 1 / h^2
+__device__ __forceinline__ float lap_p(const float* p, long long st, const Params& P, float ih2)
 {
     const float u0 = p[0];
     float acc = P.lc[1] * (tap(p[-st], u0) + tap(p[st], u0));
     acc = acc + P.lc[2] * (tap(p[-2 * st], u0) + tap(p[2 * st], u0));
     acc = acc + P.lc[3] * (tap(p[-3 * st], u0) + tap(p[3 * st], u0));
     acc = acc + P.lc[4] * (tap(p[-4 * st], u0) + tap(p[4 * st], u0));
-    return acc / (h * h);
+    return acc * ih2;
 }
 
 // the same on a register queue q[0..8] (q[4] the centre)
-__device__ __forceinline__ float lap_q(const float* q, const Params& P, float h)
+__device__ __forceinline__ float lap_q(const float* q, const Params& P, float ih2)
 {
     const float u0 = q[M];
     float acc = P.lc[1] * (tap(q[M - 1], u0) + tap(q[M + 1], u0));
     acc = acc + P.lc[2] * (tap(q[M - 2], u0) + tap(q[M + 2], u0));
     acc = acc + P.lc[3] * (tap(q[M - 3], u0) + tap(q[M + 3], u0));
     acc = acc + P.lc[4] * (tap(q[M - 4], u0) + tap(q[M + 4], u0));
-    return acc / (h * h);
+    return acc * ih2;
 }
 
-// centred first derivative at p along stride st (reference gradient.cuh:49-88)
-__device__ __forceinline__ float grad_p(const float* p, long long st, const Params& P, float h)
+// centred first derivative at p along stride st (reference gradient.cuh:49-88),
+// scaled by ih = 1 / h
+__device__ __forceinline__ float grad_p(const float* p, long long st, const Params& P, float ih)
 {
     float acc = P.gc[1] * (p[st] - p[-st]);
     acc = acc + P.gc[2] * (p[2 * st] - p[-2 * st]);
     acc = acc + P.gc[3] * (p[3 * st] - p[-3 * st]);
     acc = acc + P.gc[4] * (p[4 * st] - p[-4 * st]);
-    return acc / h;
+    return acc * ih;
 }
 
-__device__ __forceinline__ float grad_q(const float* q, const Params& P, float h)
+// the same on a read-only global field (non-coherent cache path)
+__device__ __forceinline__ float grad_g(const float* __restrict__ p, long long st, const Params& P, float ih)
+{
+    float acc = P.gc[1] * (__ldg(p + st) - __ldg(p - st));
+    acc = acc + P.gc[2] * (__ldg(p + 2 * st) - __ldg(p - 2 * st));
+    acc = acc + P.gc[3] * (__ldg(p + 3 * st) - __ldg(p - 3 * st));
+    acc = acc + P.gc[4] * (__ldg(p + 4 * st) - __ldg(p - 4 * st));
+    return acc * ih;
+}
+
+__device__ __forceinline__ float grad_q(const float* q, const Params& P, float ih)
 {
     float acc = P.gc[1] * (q[M + 1] - q[M - 1]);
     acc = acc + P.gc[2] * (q[M + 2] - q[M - 2]);
     acc = acc + P.gc[3] * (q[M + 3] - q[M - 3]);
     acc = acc + P.gc[4] * (q[M + 4] - q[M - 4]);
-    return acc / h;
+    return acc * ih;
 }
 
 // strip cell s -> (iz, iy, ix): z faces (full x-y), y faces over the inner z
@@ -331,29 +345,32 @@ __global__ void __launch_bounds__(NTH, 4) f3_step(const __grid_constant__ F3Maps
         await(q0 + k);
         q[k] = sm.u[slot(q0 + k)][cidx];
     }
-    for (int z = zb; z < ze; ++z) {
-        await(z + M);
-        q[2 * M] = sm.u[slot(z + M)][cidx];
+    // rolling slots of stages z and z + M and the phase of z + M
+    int sz = M % NF3, sq = (2 * M) % NF3;
+    uint32_t ph = (uint32_t)(((2 * M) / NF3) & 1);
+    const bool inx = ix < P.ex0 || ix >= P.ex1;
+    const bool iny = iy < P.ey0 || iy >= P.ey1;
+    long long i = bo + (long long)zb * P.SP + colo;
+    for (int z = zb; z < ze; ++z, i += P.SP) {
+        if (!tma::mbar_wait(&sm.bar[sq], ph, err, ERR_WAIT_F3)) bad = true;
+        q[2 * M] = sm.u[sq][cidx];
         if (col) {
-            const float* p = sm.u[slot(z)] + cidx;
-            const float lx = lap_p(p, 1, P, P.dx);
-            const float ly = lap_p(p, PW, P, P.dy);
-            const float lz = lap_q(q, P, P.dz);
-            const bool inx = ix < P.ex0 || ix >= P.ex1;
-            const bool iny = iy < P.ey0 || iy >= P.ey1;
+            const float* p = sm.u[sz] + cidx;
+            const float lx = lap_p(p, 1, P, P.ih2x);
+            const float ly = lap_p(p, PW, P, P.ih2y);
+            const float lz = lap_q(q, P, P.ih2z);
             const bool inz = z < P.ez0 || z >= P.ez1;
-            const long long i = bo + z * P.SP + colo;
             float w;
             if (!inx && !iny && !inz) {
                 w = (lx + ly) + lz;
             } else {
                 w = 0.f;
                 if (inx) {
-                    const float du = grad_p(p, 1, P, P.dx);
-                    const float dps = grad_p(F.psx + i, 1, P, P.dx);
+                    const float du = grad_p(p, 1, P, P.ihx);
+                    const float dps = grad_g(F.psx + i, 1, P, P.ihx);
                     const float4 pr = __ldg(P.px + ix);
                     const float a = pr.x, bb = pr.y, db = pr.z, da = pr.w;
-                    const float ps = F.psx[i], zt = F.zx[i];
+                    const float ps = __ldg(F.psx + i), zt = F.zx[i];
                     const float tmp = (((1.f + bb) * lx + db * du) + a * dps) + da * ps;
                     w += (1.f + bb) * tmp + a * zt;
                     F.psxn[i] = bb * du + a * ps;
@@ -362,11 +379,11 @@ __global__ void __launch_bounds__(NTH, 4) f3_step(const __grid_constant__ F3Maps
                     w += lx;
                 }
                 if (iny) {
-                    const float du = grad_p(p, PW, P, P.dy);
-                    const float dps = grad_p(F.psy + i, P.P, P, P.dy);
+                    const float du = grad_p(p, PW, P, P.ihy);
+                    const float dps = grad_g(F.psy + i, P.P, P, P.ihy);
                     const float4 pr = __ldg(P.py + iy);
                     const float a = pr.x, bb = pr.y, db = pr.z, da = pr.w;
-                    const float ps = F.psy[i], zt = F.zy[i];
+                    const float ps = __ldg(F.psy + i), zt = F.zy[i];
                     const float tmp = (((1.f + bb) * ly + db * du) + a * dps) + da * ps;
                     w += (1.f + bb) * tmp + a * zt;
                     F.psyn[i] = bb * du + a * ps;
@@ -375,11 +392,11 @@ __global__ void __launch_bounds__(NTH, 4) f3_step(const __grid_constant__ F3Maps
                     w += ly;
                 }
                 if (inz) {
-                    const float du = grad_q(q, P, P.dz);
-                    const float dps = grad_p(F.psz + i, P.SP, P, P.dz);
+                    const float du = grad_q(q, P, P.ihz);
+                    const float dps = grad_g(F.psz + i, P.SP, P, P.ihz);
                     const float4 pr = __ldg(P.pz + z);
                     const float a = pr.x, bb = pr.y, db = pr.z, da = pr.w;
-                    const float ps = F.psz[i], zt = F.zz[i];
+                    const float ps = __ldg(F.psz + i), zt = F.zz[i];
                     const float tmp = (((1.f + bb) * lz + db * du) + a * dps) + da * ps;
                     w += (1.f + bb) * tmp + a * zt;
                     F.pszn[i] = bb * du + a * ps;
@@ -388,10 +405,12 @@ __global__ void __launch_bounds__(NTH, 4) f3_step(const __grid_constant__ F3Maps
                     w += lz;
                 }
             }
-            F.u_next[i] = 2.f * q[M] - sm.up[slot(z + M)][cc] + sm.cf[slot(z + M)][cc] * w;
+            F.u_next[i] = 2.f * q[M] - sm.up[sq][cc] + sm.cf[sq][cc] * w;
         }
 #pragma unroll
         for (int k = 0; k < 2 * M; ++k) q[k] = q[k + 1];
+        sz = sz + 1 == NF3 ? 0 : sz + 1;
+        if (++sq == NF3) { sq = 0; ph ^= 1u; }
         // every thread is done with stage z and has waited for z + M
         if (__syncthreads_or(bad)) { fail(z == zb ? q0 : z + M); return; }
         if (tid == 0)
@@ -570,31 +589,31 @@ struct A3 {
 __device__ __forceinline__ void adj_axis(const Params& P, const float4* __restrict__ pr,
                                          const float (&g)[2 * M + 1], const float* __restrict__ psi,
                                          const float* __restrict__ zeta, long long i, long long st, int c,
-                                         float h, float& L, float& Dg, float* pso, float* zto)
+                                         float ih2, float ih, float& L, float& Dg, float* pso, float* zto)
 {
     const float gw = g[M];
     const float4 p0 = __ldg(pr + c);
     const float a_ = p0.x, b_ = p0.y, da = p0.w;
-    const float z0 = zeta[i];
+    const float* zp = zeta + i;
+    const float* pp_ = psi + i;
+    const float z0 = __ldg(zp);
     const float gt0 = b_ * z0 + (1.0f + b_) * gw;
     const float l0 = (1.0f + b_) * gt0;
     float Lq = 0.0f, Dgg = 0.0f, Dq = 0.0f;
-    const float* zp = zeta + i;
-    const float* pp_ = psi + i;
 #pragma unroll
     for (int k = 1; k <= M; ++k) {
         const float4 pp = __ldg(pr + c + k), pm = __ldg(pr + c - k);
         const float bp = pp.y, bm = pm.y;
-        const float tp = bp * zp[k * st] + (1.0f + bp) * g[M + k];
-        const float tm = bm * zp[-k * st] + (1.0f + bm) * g[M - k];
+        const float tp = bp * __ldg(zp + k * st) + (1.0f + bp) * g[M + k];
+        const float tm = bm * __ldg(zp - k * st) + (1.0f + bm) * g[M - k];
         Lq += P.lc[k] * (tap((1.0f + bp) * tp, l0) + tap((1.0f + bm) * tm, l0));
-        Dgg += P.gc[k] * ((bp * pp_[k * st] + pp.z * tp) - (bm * pp_[-k * st] + pm.z * tm));
+        Dgg += P.gc[k] * ((bp * __ldg(pp_ + k * st) + pp.z * tp) - (bm * __ldg(pp_ - k * st) + pm.z * tm));
         Dq += P.gc[k] * (pp.x * tp - pm.x * tm);
     }
-    L = Lq * (1.0f / (h * h));
-    Dg = Dgg * (1.0f / h);
-    Dq = Dq * (1.0f / h);
-    pso[i] = (a_ * pp_[0] + da * gt0) - Dq;
+    L = Lq * ih2;
+    Dg = Dgg * ih;
+    Dq = Dq * ih;
+    pso[i] = (a_ * __ldg(pp_) + da * gt0) - Dq;
     zto[i] = a_ * (z0 + gw);
 }
 
@@ -639,7 +658,6 @@ __global__ void __launch_bounds__(NTH, 4) a3_step(const __grid_constant__ A3Maps
     const bool col = ix >= M && ix < P.nx - M && iy >= M && iy < P.ny - M;
     const long long bo = (long long)b * P.S;
     const long long colo = (long long)iy * P.P + ix;
-    const float invdx2 = 1.0f / (P.dx * P.dx), invdy2 = 1.0f / (P.dy * P.dy), invdz2 = 1.0f / (P.dz * P.dz);
     const bool inx = ix < P.qx0 || ix >= P.qx1;
     const bool iny = iy < P.qy0 || iy >= P.qy1;
     const int q0 = zb - M, q1 = ze + M;
@@ -693,17 +711,20 @@ __global__ void __launch_bounds__(NTH, 4) a3_step(const __grid_constant__ A3Maps
     // refilling them brings stage zb + M (NA3 < 2M + 1 holds it back so far)
     if (tid == 0)
         for (; next < q1 && next < zb + NA3; ++next) issue(next);
-    for (int z = zb; z < ze; ++z) {
-        await(z + M);
-        qg[2 * M] = sm.c[slot(z + M)][cidx] * sm.l[slot(z + M)][cidx];
+    // rolling slots of stages z and z + M and the phase of z + M
+    int sz = M % NA3, sq = (2 * M) % NA3;
+    uint32_t ph = (uint32_t)(((2 * M) / NA3) & 1);
+    long long ic = (long long)zb * P.SP + colo;
+    for (int z = zb; z < ze; ++z, ic += P.SP) {
+        if (!tma::mbar_wait(&sm.bar[sq], ph, err, ERR_WAIT_F3)) bad = true;
+        qg[2 * M] = sm.c[sq][cidx] * sm.l[sq][cidx];
         if (col) {
             const float* g = sm.gw[z & 1] + cidx;
-            const long long ic = z * P.SP + colo;
             const long long i = bo + ic;
-            const float gun = sm.l[slot(z)][cidx];
+            const float gun = sm.l[sz][cidx];
             const float gw = qg[M];
             const bool inz = z < P.qz0 || z >= P.qz1;
-            const float lprevv = sm.lp[slot(z + M)][cc];
+            const float lprevv = sm.lp[sq][cc];
             if (!inx && !iny && !inz) {
                 float lapx = 0.0f, lapy = 0.0f, lapz = 0.0f;
 #pragma unroll
@@ -712,47 +733,56 @@ __global__ void __launch_bounds__(NTH, 4) a3_step(const __grid_constant__ A3Maps
                     lapy += P.lc[k] * (tap(g[k * PW], gw) + tap(g[-k * PW], gw));
                     lapz += P.lc[k] * (tap(qg[M + k], gw) + tap(qg[M - k], gw));
                 }
-                A.l_next[i] = 2.0f * gun - lprevv + lapx * invdx2 + lapy * invdy2 + lapz * invdz2;
+                A.l_next[i] = 2.0f * gun - lprevv + lapx * P.ih2x + lapy * P.ih2y + lapz * P.ih2z;
             } else {
                 float Lx, Ly, Lz, Dgx = 0.f, Dgy = 0.f, Dgz = 0.f;
                 float ga[2 * M + 1];
                 if (inx) {
 #pragma unroll
                     for (int k = -M; k <= M; ++k) ga[M + k] = g[k];
-                    adj_axis(P, P.px, ga, A.px + bo, A.zx + bo, ic, 1, ix, P.dx, Lx, Dgx, A.pxo + bo, A.zxo + bo);
+                    adj_axis(P, P.px, ga, A.px + bo, A.zx + bo, ic, 1, ix, P.ih2x, P.ihx, Lx, Dgx, A.pxo + bo,
+                             A.zxo + bo);
                 } else {
                     Lx = 0.0f;
 #pragma unroll
                     for (int k = 1; k <= M; ++k) Lx += P.lc[k] * (tap(g[k], gw) + tap(g[-k], gw));
-                    Lx *= invdx2;
+                    Lx *= P.ih2x;
                 }
                 if (iny) {
 #pragma unroll
                     for (int k = -M; k <= M; ++k) ga[M + k] = g[k * PW];
-                    adj_axis(P, P.py, ga, A.py + bo, A.zy + bo, ic, P.P, iy, P.dy, Ly, Dgy, A.pyo + bo,
+                    adj_axis(P, P.py, ga, A.py + bo, A.zy + bo, ic, P.P, iy, P.ih2y, P.ihy, Ly, Dgy, A.pyo + bo,
                              A.zyo + bo);
                 } else {
                     Ly = 0.0f;
 #pragma unroll
                     for (int k = 1; k <= M; ++k) Ly += P.lc[k] * (tap(g[k * PW], gw) + tap(g[-k * PW], gw));
-                    Ly *= invdy2;
+                    Ly *= P.ih2y;
                 }
                 if (inz) {
-                    adj_axis(P, P.pz, qg, A.pz + bo, A.zz + bo, ic, P.SP, z, P.dz, Lz, Dgz, A.pzo + bo, A.zzo + bo);
+                    adj_axis(P, P.pz, qg, A.pz + bo, A.zz + bo, ic, P.SP, z, P.ih2z, P.ihz, Lz, Dgz, A.pzo + bo,
+                             A.zzo + bo);
                 } else {
                     Lz = 0.0f;
 #pragma unroll
                     for (int k = 1; k <= M; ++k) Lz += P.lc[k] * (tap(qg[M + k], gw) + tap(qg[M - k], gw));
-                    Lz *= invdz2;
+                    Lz *= P.ih2z;
                 }
                 A.l_next[i] = 2.0f * gun - lprevv + (Lx + Ly + Lz - Dgx - Dgy - Dgz);
             }
         }
 #pragma unroll
         for (int k = 0; k < 2 * M; ++k) qg[k] = qg[k + 1];
-        // the next plane's gw (stage z + 1 has landed: z + 1 <= z + M); the
-        // buffer it overwrites was last read in plane z - 1
-        if (z + 1 < ze) convert(z + 1);
+        sz = sz + 1 == NA3 ? 0 : sz + 1;
+        // the next plane's gw (stage z + 1, now in slot sz, has landed:
+        // z + 1 <= z + M); the buffer it overwrites was last read in plane z - 1
+        if (z + 1 < ze) {
+            float* gb = sm.gw[(z + 1) & 1];
+            const float* c = sm.c[sz];
+            const float* l = sm.l[sz];
+            for (int e = tid; e < PN; e += NTH) gb[e] = c[e] * l[e];
+        }
+        if (++sq == NA3) { sq = 0; ph ^= 1u; }
         if (__syncthreads_or(bad)) { fail(z + M); return; }
         if (tid == 0)
             for (; next < q1 && next <= z + NA3; ++next) issue(next);    // slots of stages <= z are free
@@ -854,14 +884,17 @@ __global__ void __launch_bounds__(NTH, 4) r3_recon(const __grid_constant__ R3Map
         await(q0 + k);
         q[k] = sm.u[slot(q0 + k)][cidx];
     }
-    for (int z = zb; z < ze; ++z) {
-        await(z + M);
-        q[2 * M] = sm.u[slot(z + M)][cidx];
+    // rolling slots: halo stages z and z + M, the phase of z + M, centre plane z
+    int sz = M % NR3, sq = (2 * M) % NR3, sc = 0;
+    uint32_t ph = (uint32_t)(((2 * M) / NR3) & 1);
+    long long i = bo + (long long)zb * P.SP + colo;
+    for (int z = zb; z < ze; ++z, i += P.SP) {
+        if (!tma::mbar_wait(&sm.bar[sq], ph, err, ERR_WAIT_F3)) bad = true;
+        q[2 * M] = sm.u[sq][cidx];
         if (col) {
-            const float* p = sm.u[slot(z)] + cidx;
-            const float w = (lap_p(p, 1, P, P.dx) + lap_p(p, PW, P, P.dy)) + lap_q(q, P, P.dz);
-            const float(*c)[CN3] = sm.c[cslot(z)];
-            const long long i = bo + z * P.SP + colo;
+            const float* p = sm.u[sz] + cidx;
+            const float w = (lap_p(p, 1, P, P.ih2x) + lap_p(p, PW, P, P.ih2y)) + lap_q(q, P, P.ih2z);
+            const float(*c)[CN3] = sm.c[sc];
             const float u0 = q[M], up = c[0][cc];
             const float un = 2.0f * u0 - up + c[2][cc] * w;
             R.r_next[i] = un;
@@ -876,6 +909,9 @@ __global__ void __launch_bounds__(NTH, 4) r3_recon(const __grid_constant__ R3Map
         }
 #pragma unroll
         for (int k = 0; k < 2 * M; ++k) q[k] = q[k + 1];
+        sz = sz + 1 == NR3 ? 0 : sz + 1;
+        sc = sc + 1 == NRC3 ? 0 : sc + 1;
+        if (++sq == NR3) { sq = 0; ph ^= 1u; }
         if (__syncthreads_or(bad)) { fail(z == zb ? q0 : z + M); return; }
         // after plane z the halo slots of stages <= z and the centre slot of
         // plane z are free: stage s refills centre slot s - M, so s <= z + NRC3
@@ -906,7 +942,7 @@ __global__ void pack_prof3(const float* __restrict__ a, const float* __restrict_
                            int n, float h, const Params P, float4* __restrict__ out)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const float da = (i >= M && i < n - M) ? grad_p(a + i, 1, P, h) : 0.f;
+        const float da = (i >= M && i < n - M) ? grad_p(a + i, 1, P, 1.0f / h) : 0.f;
         out[i] = make_float4(a[i], b[i], db[i], da);
     }
 }
@@ -969,6 +1005,8 @@ static Params make_params(const sweep_acoustic_desc* d)
     P.SP = (long long)d->ny * P.P;
     P.S = (long long)d->nz * P.SP;
     P.dt = d->dt; P.dz = d->dz; P.dy = d->dy; P.dx = d->dx;
+    P.ih2z = 1.0f / (d->dz * d->dz); P.ih2y = 1.0f / (d->dy * d->dy); P.ih2x = 1.0f / (d->dx * d->dx);
+    P.ihz = 1.0f / d->dz; P.ihy = 1.0f / d->dy; P.ihx = 1.0f / d->dx;
     for (int k = 0; k <= M; ++k) { P.lc[k] = d->lap[k]; P.gc[k] = d->grad[k]; }
     P.z0 = d->pad[0] + M; P.z1 = d->nz - d->pad[1] - M;
     P.y0 = d->pad[2] + M; P.y1 = d->ny - d->pad[3] - M;
