@@ -263,6 +263,54 @@ SWEEP_B200_API int sweep_b200_schedule_get(int32_t family, const void* desc, swe
 /* Forget every recorded schedule.  Host-side only. */
 SWEEP_B200_API int sweep_b200_schedule_clear(void);
 
+/* Stepped runners: a pass advanced segment by segment over the time axis
+ * (reference src/sweep/csrc/core/capi.h:236-243, sweep_forward_runner_* /
+ * sweep_backward_runner_*; eq_driver.cuh:199-453 and 715-925).  A runner is
+ * created over a problem and its caller-owned buffers -- descriptor (copied;
+ * the arrays it points at), record or gradients, tape, workspace (sized by the
+ * *_sizes query) -- which stay valid until destroy; nothing is allocated on
+ * the device.  Boundary saving only (every strip format, device or host
+ * tape), as the reference's runners.
+ *
+ * Forward runner: run(it_begin, it_end) advances steps [it_begin, it_end),
+ * segments in order from 0 to nt; the record holds every step run so far; the
+ * tape is complete once a segment ends at nt.  Backward runner (over that
+ * tape and the record cotangent): run(bw_it_begin, bw_it_end) reverses the
+ * steps [bw_it_end, bw_it_begin), segments in order from nt down to 0; the
+ * gradients (and illuminations) are overwritten after every segment with the
+ * contribution of every step reversed so far.  Segments compute what one call
+ * computes: the same kernels, in the same order, on the same state.
+ * step_phase must be 0: the reference's 1 / 2 split a step around a
+ * domain-decomposition halo exchange, which has no counterpart here.  A
+ * runner's calls run on its creation device. */
+SWEEP_B200_API int sweep_b200_acoustic_forward_runner_create(const sweep_acoustic_desc* d, int32_t mem_mode,
+                                                             float* record, void* tape, void* workspace,
+                                                             int64_t workspace_bytes, void** handle,
+                                                             char* err, int32_t err_cap);
+SWEEP_B200_API int sweep_b200_acoustic_backward_runner_create(const sweep_acoustic_desc* d, int32_t mem_mode,
+                                                              const float* adj, const void* tape,
+                                                              float* grad_vp, float* grad_wavelet,
+                                                              float* illum_src, float* illum_rec,
+                                                              void* workspace, int64_t workspace_bytes,
+                                                              void** handle, char* err, int32_t err_cap);
+SWEEP_B200_API int sweep_b200_elastic_forward_runner_create(const sweep_elastic_desc* d, int32_t mem_mode,
+                                                            float* record, void* tape, void* workspace,
+                                                            int64_t workspace_bytes, void** handle,
+                                                            char* err, int32_t err_cap);
+SWEEP_B200_API int sweep_b200_elastic_backward_runner_create(const sweep_elastic_desc* d, int32_t mem_mode,
+                                                             const float* adj, const void* tape,
+                                                             float* grad_vp, float* grad_vs, float* grad_rho,
+                                                             void* workspace, int64_t workspace_bytes,
+                                                             void** handle, char* err, int32_t err_cap);
+SWEEP_B200_API int sweep_b200_forward_runner_run(void* handle, int32_t it_begin, int32_t it_end,
+                                                 int32_t step_phase, void* stream, char* err, int32_t err_cap);
+SWEEP_B200_API int sweep_b200_backward_runner_run(void* handle, int32_t bw_it_begin, int32_t bw_it_end,
+                                                  int32_t step_phase, void* stream, char* err, int32_t err_cap);
+/* The device a runner was created on (-1 for a null handle). */
+SWEEP_B200_API int sweep_b200_runner_device_index(void* handle);
+/* Releases a runner of either kind (null: no-op). */
+SWEEP_B200_API void sweep_b200_runner_destroy(void* handle);
+
 /* Runs the bounded-wait failure path on purpose.  No counterpart in the
  * reference, whose kernels do not wait on barriers.  Every mbarrier wait of
  * this library's step kernels gives up after a fixed budget (about 2 s of SM

@@ -39,6 +39,14 @@ SYMBOLS = (
     "sweep_b200_schedule_get",
     "sweep_b200_schedule_clear",
     "sweep_b200_wait_selftest",
+    "sweep_b200_acoustic_forward_runner_create",
+    "sweep_b200_acoustic_backward_runner_create",
+    "sweep_b200_elastic_forward_runner_create",
+    "sweep_b200_elastic_backward_runner_create",
+    "sweep_b200_forward_runner_run",
+    "sweep_b200_backward_runner_run",
+    "sweep_b200_runner_device_index",
+    "sweep_b200_runner_destroy",
 )
 
 MEM_BOUNDARY = 0
@@ -136,8 +144,22 @@ def load():
     lib.sweep_b200_schedule_get.argtypes = [c_i32, c_p, S, ctypes.c_char_p, c_i32]
     lib.sweep_b200_schedule_clear.argtypes = []
     lib.sweep_b200_wait_selftest.argtypes = [c_i64, c_i32, c_p, ctypes.c_char_p, c_i32]
+    H = ctypes.POINTER(c_p)
+    lib.sweep_b200_acoustic_forward_runner_create.argtypes = [P, c_i32, c_p, c_p, c_p, c_i64, H, ctypes.c_char_p,
+                                                              c_i32]
+    lib.sweep_b200_acoustic_backward_runner_create.argtypes = [P, c_i32, c_p, c_p, c_p, c_p, c_p, c_p, c_p, c_i64, H,
+                                                               ctypes.c_char_p, c_i32]
+    lib.sweep_b200_elastic_forward_runner_create.argtypes = [E, c_i32, c_p, c_p, c_p, c_i64, H, ctypes.c_char_p,
+                                                             c_i32]
+    lib.sweep_b200_elastic_backward_runner_create.argtypes = [E, c_i32, c_p, c_p, c_p, c_p, c_p, c_p, c_i64, H,
+                                                              ctypes.c_char_p, c_i32]
+    lib.sweep_b200_forward_runner_run.argtypes = [c_p, c_i32, c_i32, c_i32, c_p, ctypes.c_char_p, c_i32]
+    lib.sweep_b200_backward_runner_run.argtypes = [c_p, c_i32, c_i32, c_i32, c_p, ctypes.c_char_p, c_i32]
+    lib.sweep_b200_runner_device_index.argtypes = [c_p]
+    lib.sweep_b200_runner_destroy.argtypes = [c_p]
     for s in SYMBOLS[1:]:
         getattr(lib, s).restype = ctypes.c_int
+    lib.sweep_b200_runner_destroy.restype = None
     _lib = lib
     return lib
 

@@ -1541,8 +1541,12 @@ static void copy_dd(float* dst, const float* src, long long n, cudaStream_t st)
 }
 
 void forward_with(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* record, void* tape, void* ws,
-                  int64_t ws_bytes, cudaStream_t st, const HostStage* stage)
+                  int64_t ws_bytes, cudaStream_t st, const HostStage* stage, StepState* seg, int seg0, int seg1)
 {
+    // a stepped run covers [seg0, seg1) of the time axis, continuing seg's state
+    const bool stepped = seg != nullptr;
+    const int a = stepped ? seg0 : 0, b = stepped ? seg1 : d->nt;
+    SWEEP_REQUIRE(!stepped || ckpt_every <= 0, "acoustic2d stepped forward: boundary saving only");
     SWEEP_REQUIRE(record != nullptr || d->nrec == 0, "acoustic2d forward: null record");
     SWEEP_REQUIRE(d->vp != nullptr, "acoustic2d forward: null vp");
     set_attrs();
@@ -1560,29 +1564,38 @@ void forward_with(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, fl
     }
     const Params& P = pl.P;
     const long long n = (long long)P.B * P.S;
-    for (auto* p : w.u) SWEEP_CUDA(cudaMemsetAsync(p, 0, n * 4, st));
-    for (auto* p : {w.psix, w.psiz, w.psixn, w.psizn, w.zetax, w.zetaz})
-        SWEEP_CUDA(cudaMemsetAsync(p, 0, n * 4, st));
-    if (d->nrec > 0)
-        SWEEP_CUDA(cudaMemsetAsync(record, 0, (size_t)d->B * d->nt * d->nrec * 4, st));
+    if (a == 0) {
+        for (auto* p : w.u) SWEEP_CUDA(cudaMemsetAsync(p, 0, n * 4, st));
+        for (auto* p : {w.psix, w.psiz, w.psixn, w.psizn, w.zetax, w.zetaz})
+            SWEEP_CUDA(cudaMemsetAsync(p, 0, n * 4, st));
+        if (d->nrec > 0)
+            SWEEP_CUDA(cudaMemsetAsync(record, 0, (size_t)d->B * d->nt * d->nrec * 4, st));
+    }
     const FwdMaps maps = fwd_maps(w, P);
     FwdState S;
     S.px = w.psix; S.pz = w.psiz; S.pxn = w.psixn; S.pzn = w.psizn;
+    if (stepped && a > 0) {
+        S.ip = seg->idx[0]; S.in = seg->idx[1]; S.ix = seg->idx[2];
+        S.px = static_cast<float*>(seg->ptr[0]); S.pz = static_cast<float*>(seg->ptr[1]);
+        S.pxn = static_cast<float*>(seg->ptr[2]); S.pzn = static_cast<float*>(seg->ptr[3]);
+    }
     // a caller-staged call (the allocation-free entry) issues plain launches:
     // instantiating a graph allocates
     const bool graphs = stage == nullptr;
     if (ckpt_every <= 0 && tape && pl.host_tape) {
         HostRing hr;
         hr.open(w.ring, tape, P.st.step, st);
-        forward_steps(pl, maps, w, record, S, 0, d->nt, [&](int it) { return hr.slot(it); }, st, &hr);
+        forward_steps(pl, maps, w, record, S, a, b, [&](int it) { return hr.slot(it); }, st, &hr);
         hr.close();
-        float* last = tape_last(tape, pl);
-        copy_any(last, w.u[S.ip], n * 4, st);
-        copy_any(last + n, w.u[S.in], n * 4, st);
+        if (b == d->nt) {
+            float* last = tape_last(tape, pl);
+            copy_any(last, w.u[S.ip], n * 4, st);
+            copy_any(last + n, w.u[S.in], n * 4, st);
+        }
     } else if (ckpt_every <= 0) {
-        forward_steps(pl, maps, w, record, S, 0, d->nt,
+        forward_steps(pl, maps, w, record, S, a, b,
                       [&](int it) { return tape ? tape_slot(tape, pl, it) : nullptr; }, st, nullptr, graphs);
-        if (tape) {
+        if (tape && b == d->nt) {
             float* last = tape_last(tape, pl);
             // (U[nt-1], U[nt]) per shot, pitched
             copy_dd(last, w.u[S.ip], n, st);
@@ -1604,6 +1617,10 @@ void forward_with(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, fl
                           st, nullptr, graphs);
         }
     }
+    if (stepped) {
+        seg->idx[0] = S.ip; seg->idx[1] = S.in; seg->idx[2] = S.ix;
+        seg->ptr[0] = S.px; seg->ptr[1] = S.pz; seg->ptr[2] = S.pxn; seg->ptr[3] = S.pzn;
+    }
     check_err(w.c, st, "forward");
 }
 
@@ -1618,7 +1635,17 @@ void forward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* 
     // replays from the initial state
     forward_with(d, mem_mode == SWEEP_MEM_RECURSIVE ? SWEEP_MEM_BOUNDARY : mem_mode,
                  mem_mode == SWEEP_MEM_CHECKPOINT ? ckpt_every : 0, record,
-                 mem_mode == SWEEP_MEM_RECURSIVE ? nullptr : tape, ws, ws_bytes, st, nullptr);
+                 mem_mode == SWEEP_MEM_RECURSIVE ? nullptr : tape, ws, ws_bytes, st, nullptr, nullptr, 0, 0);
+}
+
+void forward_segment(const sweep_acoustic_desc* d, int mem_mode, float* record, void* tape, void* ws,
+                     int64_t ws_bytes, cudaStream_t st, StepState& seg, int it0, int it1)
+{
+    int64_t need_ws, need_tape;
+    sizes(d, mem_mode, 0, &need_ws, &need_tape);
+    SWEEP_REQUIRE(ws != nullptr && ws_bytes >= need_ws, "acoustic2d forward runner: workspace too small (%lld < %lld)",
+                  (long long)ws_bytes, (long long)need_ws);
+    forward_with(d, mem_mode, 0, record, tape, ws, ws_bytes, st, nullptr, &seg, it0, it1);
 }
 
 // Recursive checkpointing (SWEEP_MEM_RECURSIVE; reference
@@ -1699,10 +1726,13 @@ static void backward_recursive(const Plan& pl, FwdWork& fw, RevWork& w, float* c
     process(0, P.nt, -1, count);
 }
 
-void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const float* adj, const void* tape,
-              float* grad_vp, float* grad_w, float* illum_s, float* illum_r,
-              void* ws, int64_t ws_bytes, cudaStream_t st)
+void backward_with(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const float* adj, const void* tape,
+                   float* grad_vp, float* grad_w, float* illum_s, float* illum_r,
+                   void* ws, int64_t ws_bytes, cudaStream_t st, StepState* seg, int bw0, int bw1)
 {
+    // a stepped run reverses [bw1, bw0) top down, continuing seg's state
+    const bool stepped = seg != nullptr;
+    const int top = stepped ? bw0 : d->nt, bottom = stepped ? bw1 : 0;
     int64_t need_ws, need_tape;
     sizes(d, mem_mode, ckpt_every, &need_ws, &need_tape);
     SWEEP_REQUIRE(ws != nullptr && ws_bytes >= need_ws, "acoustic2d backward: workspace too small");
@@ -1717,6 +1747,8 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     const bool illum = illum_s != nullptr;
     const bool ckpt = mem_mode == SWEEP_MEM_CHECKPOINT;
     const bool recursive = mem_mode == SWEEP_MEM_RECURSIVE;
+    SWEEP_REQUIRE(!stepped || (!ckpt && !recursive), "acoustic2d stepped backward: boundary saving only");
+    const bool first = top == d->nt;
     RevWork w;
     FwdWork fw{};
     float* chunk = nullptr;
@@ -1732,17 +1764,19 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     }
     const Params& P = pl.P;
     const long long n = (long long)P.B * P.S;
-    for (auto* p : w.l) SWEEP_CUDA(cudaMemsetAsync(p, 0, n * 4, st));
-    for (auto* p : w.aux) SWEEP_CUDA(cudaMemsetAsync(p, 0, n * 4, st));
-    SWEEP_CUDA(cudaMemsetAsync(w.r[2], 0, n * 4, st));
-    SWEEP_CUDA(cudaMemsetAsync(w.gacc, 0, (size_t)pl.nslot * P.S * 4, st));
-    SWEEP_CUDA(cudaMemsetAsync(w.gcomp, 0, (size_t)pl.nslot * P.S * 4, st));
-    if (illum) {
-        SWEEP_CUDA(cudaMemsetAsync(w.is, 0, (size_t)pl.nslot * P.S * 4, st));
-        SWEEP_CUDA(cudaMemsetAsync(w.ir, 0, (size_t)pl.nslot * P.S * 4, st));
+    if (first) {
+        for (auto* p : w.l) SWEEP_CUDA(cudaMemsetAsync(p, 0, n * 4, st));
+        for (auto* p : w.aux) SWEEP_CUDA(cudaMemsetAsync(p, 0, n * 4, st));
+        SWEEP_CUDA(cudaMemsetAsync(w.r[2], 0, n * 4, st));
+        SWEEP_CUDA(cudaMemsetAsync(w.gacc, 0, (size_t)pl.nslot * P.S * 4, st));
+        SWEEP_CUDA(cudaMemsetAsync(w.gcomp, 0, (size_t)pl.nslot * P.S * 4, st));
+        if (illum) {
+            SWEEP_CUDA(cudaMemsetAsync(w.is, 0, (size_t)pl.nslot * P.S * 4, st));
+            SWEEP_CUDA(cudaMemsetAsync(w.ir, 0, (size_t)pl.nslot * P.S * 4, st));
+        }
+        if (grad_w && d->nsrc > 0)
+            SWEEP_CUDA(cudaMemsetAsync(grad_w, 0, (size_t)d->B * d->nsrc * d->nt * 4, st));
     }
-    if (grad_w && d->nsrc > 0)
-        SWEEP_CUDA(cudaMemsetAsync(grad_w, 0, (size_t)d->B * d->nsrc * d->nt * 4, st));
     RevMaps maps;
     for (int i = 0; i < 3; ++i) {
         maps.lh[i] = field_map(w.l[i], P, P.B, true);
@@ -1758,13 +1792,19 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     R.illum_s = w.is; R.illum_r = w.ir;
     int lp = 0, ln = 1, lx = 2;
     int cur = 0;
-    // Reverse steps [it0, it1) top down; the reconstruction starts from
-    // r[0] = U[it1], r[1] = U[it1 - 1]; strips_of(it) holds the strips of U[it].
+    int rp = 0, rn = 1, rx = 2;
+    if (stepped && !first) {
+        lp = seg->idx[0]; ln = seg->idx[1]; lx = seg->idx[2]; cur = seg->idx[3];
+        rp = seg->idx[4]; rn = seg->idx[5]; rx = seg->idx[6];
+    }
+    // Reverse steps [it0, it1) top down; a fresh run starts the reconstruction
+    // from r[0] = U[it1], r[1] = U[it1 - 1], a continued one where the last
+    // stopped; strips_of(it) holds the strips of U[it].
     HostRing hr;
     const bool host = pl.host_tape && !ckpt && !recursive;
-    auto reverse = [&](int it0, int it1, auto strips_of) {
+    auto reverse = [&](int it0, int it1, auto strips_of, bool fresh) {
         StepGraphs gs(st, host ? 0 : pl.graph_steps);
-        int rp = 0, rn = 1, rx = 2;
+        if (fresh) { rp = 0; rn = 1; rx = 2; }
         for (int it = it1 - 1; it >= it0; --it) {
             const int do_recon = it > 0 ? 1 : 0;
             R.lprev = lp; R.lnow = ln; R.l_next = w.l[lx];
@@ -1778,7 +1818,7 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
             SWEEP_LAUNCH_CHECK();
             if (host && do_recon) {
                 hr.after_read(it - 1);
-                if (it - 1 - HostRing::R >= 0) hr.fetch(it - 1 - HostRing::R, true);
+                if (it - 1 - HostRing::R >= std::max(it0 - 1, 0)) hr.fetch(it - 1 - HostRing::R, true);
             }
             gs.step_done();
             int t = lp; lp = ln; ln = lx; lx = t;
@@ -1788,20 +1828,23 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
         gs.flush();
     };
     if (recursive) {
-        backward_recursive(pl, fw, w, chunk, snaps, ckpt_every, st, reverse);
+        auto rev = [&](int it0, int it1, auto strips_of) { reverse(it0, it1, strips_of, true); };
+        backward_recursive(pl, fw, w, chunk, snaps, ckpt_every, st, rev);
     } else if (!ckpt) {
-        const float* last = tape_last(const_cast<void*>(tape), pl);
-        // seed: prev = U[nt], now = U[nt-1]  (reference driver_traits.cuh:493-505; the
-        // rim outside the physical box is never read by the reconstruction)
-        copy_any(w.r[0], last + n, n * 4, st);
-        copy_any(w.r[1], last, n * 4, st);
+        if (first) {
+            const float* last = tape_last(const_cast<void*>(tape), pl);
+            // seed: prev = U[nt], now = U[nt-1]  (reference driver_traits.cuh:493-505; the
+            // rim outside the physical box is never read by the reconstruction)
+            copy_any(w.r[0], last + n, n * 4, st);
+            copy_any(w.r[1], last, n * 4, st);
+        }
         if (host) {
             hr.open(w.ring, const_cast<void*>(tape), P.st.step, st);
-            for (int t = d->nt - 2; t >= 0 && t > d->nt - 2 - HostRing::R; --t) hr.fetch(t, false);
-            reverse(0, d->nt, [&](int t) { return hr.slot(t); });
+            for (int t = top - 2; t >= std::max(bottom - 1, 0) && t > top - 2 - HostRing::R; --t) hr.fetch(t, false);
+            reverse(bottom, top, [&](int t) { return hr.slot(t); }, first);
             hr.close();
         } else {
-            reverse(0, d->nt, [&](int t) { return tape_slot(tape, pl, t); });
+            reverse(bottom, top, [&](int t) { return tape_slot(tape, pl, t); }, first);
         }
     } else {
         const int k = ckpt_every, C = nchunks(pl, k);
@@ -1830,14 +1873,33 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
                           [&](int it) { return chunk + (long long)(it - it0 + 1) * cs; }, st);
             copy_dd(w.r[0], fw.u[S.in], n, st);       // U[it1]
             copy_dd(w.r[1], fw.u[S.ip], n, st);       // U[it1 - 1]
-            reverse(it0, it1, [&](int t) { return chunk + (long long)(t - (it0 - 1)) * cs; });
+            reverse(it0, it1, [&](int t) { return chunk + (long long)(t - (it0 - 1)) * cs; }, true);
         }
+    }
+    if (stepped) {
+        const int keep[7] = {lp, ln, lx, cur, rp, rn, rx};
+        for (int k = 0; k < 7; ++k) seg->idx[k] = keep[k];
     }
     const int nout = P.per_shot ? d->B : 1;
     finalize_kernel<<<1184, 256, 0, st>>>(w.gacc, w.gcomp, w.is, w.ir, pl.nslot, nout, d->nz, d->nx, P.P,
                                           grad_vp, illum_s, illum_r);
     SWEEP_LAUNCH_CHECK();
     check_err(w.c, st, "backward");
+}
+
+void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const float* adj, const void* tape,
+              float* grad_vp, float* grad_w, float* illum_s, float* illum_r,
+              void* ws, int64_t ws_bytes, cudaStream_t st)
+{
+    backward_with(d, mem_mode, ckpt_every, adj, tape, grad_vp, grad_w, illum_s, illum_r, ws, ws_bytes, st, nullptr,
+                  0, 0);
+}
+
+void backward_segment(const sweep_acoustic_desc* d, int mem_mode, const float* adj, const void* tape,
+                      float* grad_vp, float* grad_w, float* illum_s, float* illum_r, void* ws, int64_t ws_bytes,
+                      cudaStream_t st, StepState& seg, int bw0, int bw1)
+{
+    backward_with(d, mem_mode, 0, adj, tape, grad_vp, grad_w, illum_s, illum_r, ws, ws_bytes, st, &seg, bw0, bw1);
 }
 
 }  // namespace a2d

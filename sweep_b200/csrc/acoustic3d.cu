@@ -1317,9 +1317,14 @@ static void state_fields(const FwdState& S, float* out[kStateFields])
     for (int a = 0; a < 3; ++a) { out[2 + a] = S.ps[a]; out[5 + a] = S.zeta(a); }
 }
 
-void forward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* record, void* tape,
-             void* ws, int64_t ws_bytes, cudaStream_t st)
+static void forward_with(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* record, void* tape,
+                         void* ws, int64_t ws_bytes, cudaStream_t st, StepState* seg, int seg0, int seg1)
 {
+    // a stepped run covers [seg0, seg1) of the time axis, continuing seg's state
+    const bool stepped = seg != nullptr;
+    const int a = stepped ? seg0 : 0, b = stepped ? seg1 : d->nt;
+    SWEEP_REQUIRE(!stepped || (mem_mode != SWEEP_MEM_CHECKPOINT && mem_mode != SWEEP_MEM_RECURSIVE),
+                  "acoustic3d stepped forward: boundary saving only");
     int64_t need_ws, need_tape;
     sizes(d, mem_mode, ckpt_every, &need_ws, &need_tape);
     SWEEP_REQUIRE(ws != nullptr && ws_bytes >= need_ws, "acoustic3d forward: workspace too small (%lld < %lld)",
@@ -1331,10 +1336,24 @@ void forward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* 
     Work w = carve(c, P, kFwdFields);
     prep_call(d, P, w, st);
     const long long n = (long long)P.B * P.S;
-    for (int i = 0; i < kFwdFields; ++i) SWEEP_CUDA(cudaMemsetAsync(w.f[i], 0, n * 4, st));
+    if (a == 0) {
+        for (int i = 0; i < kFwdFields; ++i) SWEEP_CUDA(cudaMemsetAsync(w.f[i], 0, n * 4, st));
+        if (d->nrec > 0) SWEEP_CUDA(cudaMemsetAsync(record, 0, (size_t)d->B * d->nt * d->nrec * 4, st));
+    }
     SWEEP_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
-    if (d->nrec > 0) SWEEP_CUDA(cudaMemsetAsync(record, 0, (size_t)d->B * d->nt * d->nrec * 4, st));
     FwdState S(w.f);
+    if (stepped && a > 0) {
+        S.ip = seg->idx[0]; S.in = seg->idx[1]; S.ix = seg->idx[2];
+        for (int k = 0; k < 3; ++k) {
+            S.ps[k] = static_cast<float*>(seg->ptr[k]);
+            S.psn[k] = static_cast<float*>(seg->ptr[3 + k]);
+        }
+    }
+    auto keep = [&] {
+        if (!stepped) return;
+        seg->idx[0] = S.ip; seg->idx[1] = S.in; seg->idx[2] = S.ix;
+        for (int k = 0; k < 3; ++k) { seg->ptr[k] = S.ps[k]; seg->ptr[3 + k] = S.psn[k]; }
+    };
     if (mem_mode == SWEEP_MEM_RECURSIVE) {
         // recursive checkpointing keeps nothing: the backward replays from the initial state
         forward_steps(d, P, S, record, 0, d->nt, [&](int) { return (void*)nullptr; }, w.err, w.scratch, st);
@@ -1344,21 +1363,25 @@ void forward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* 
     if (mem_mode != SWEEP_MEM_CHECKPOINT && tape && P.st.host) {
         HostRing hr;
         hr.open(w.ring, tape, P.st.step, st);
-        forward_steps(d, P, S, record, 0, d->nt, [&](int it) { return hr.slot(it); }, w.err, w.scratch, st, &hr);
+        forward_steps(d, P, S, record, a, b, [&](int it) { return hr.slot(it); }, w.err, w.scratch, st, &hr);
         hr.close();
-        float* last = tape_last(tape, P);
-        SWEEP_CUDA(cudaMemcpyAsync(last, S.f[S.ip], n * 4, cudaMemcpyDefault, st));       // U[nt-1]
-        SWEEP_CUDA(cudaMemcpyAsync(last + n, S.f[S.in], n * 4, cudaMemcpyDefault, st));   // U[nt]
+        if (b == d->nt) {
+            float* last = tape_last(tape, P);
+            SWEEP_CUDA(cudaMemcpyAsync(last, S.f[S.ip], n * 4, cudaMemcpyDefault, st));       // U[nt-1]
+            SWEEP_CUDA(cudaMemcpyAsync(last + n, S.f[S.in], n * 4, cudaMemcpyDefault, st));   // U[nt]
+        }
+        keep();
         check_err(w, st, "forward");
         return;
     } else if (mem_mode != SWEEP_MEM_CHECKPOINT) {
-        forward_steps(d, P, S, record, 0, d->nt, [&](int it) { return tape ? tape_slot(tape, P, it) : nullptr; },
+        forward_steps(d, P, S, record, a, b, [&](int it) { return tape ? tape_slot(tape, P, it) : nullptr; },
                       w.err, w.scratch, st);
-        if (tape) {
+        if (tape && b == d->nt) {
             float* last = tape_last(tape, P);
             copy_dd(last, S.f[S.ip], n, st);        // U[nt-1]
             copy_dd(last + n, S.f[S.in], n, st);    // U[nt]
         }
+        keep();
         check_err(w, st, "forward");
         return;
     }
@@ -1446,10 +1469,14 @@ static void backward_recursive(const sweep_acoustic_desc* d, const Params& P, Wo
     process(0, P.nt, -1, count);
 }
 
-void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const float* adj, const void* tape,
-              float* grad_vp, float* grad_w, float* illum_s, float* illum_r,
-              void* ws, int64_t ws_bytes, cudaStream_t st)
+static void backward_with(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const float* adj,
+                          const void* tape, float* grad_vp, float* grad_w, float* illum_s, float* illum_r,
+                          void* ws, int64_t ws_bytes, cudaStream_t st, StepState* seg, int bw0, int bw1)
 {
+    // a stepped run reverses [bw1, bw0) top down, continuing seg's state
+    const bool stepped = seg != nullptr;
+    const int top = stepped ? bw0 : d->nt, bottom = stepped ? bw1 : 0;
+    const bool first = top == d->nt;
     int64_t need_ws, need_tape;
     sizes(d, mem_mode, ckpt_every, &need_ws, &need_tape);
     SWEEP_REQUIRE(ws != nullptr && ws_bytes >= need_ws, "acoustic3d backward: workspace too small");
@@ -1458,6 +1485,7 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     SWEEP_REQUIRE((illum_s == nullptr) == (illum_r == nullptr), "acoustic3d backward: pass both illuminations or neither");
     const bool ckpt = mem_mode == SWEEP_MEM_CHECKPOINT;
     const bool recursive = mem_mode == SWEEP_MEM_RECURSIVE;
+    SWEEP_REQUIRE(!stepped || (!ckpt && !recursive), "acoustic3d stepped backward: boundary saving only");
     Params P = make_params(d);
     set_store(P, mem_mode);
     Carve c(ws);
@@ -1473,13 +1501,20 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     prep_call(d, P, w, st);
     const long long n = (long long)P.B * P.S;
     const bool illum = illum_s != nullptr;
-    for (int i = 0; i < kRevFields; ++i) SWEEP_CUDA(cudaMemsetAsync(w.f[i], 0, n * 4, st));
+    if (first) {
+        for (int i = 0; i < kRevFields; ++i) SWEEP_CUDA(cudaMemsetAsync(w.f[i], 0, n * 4, st));
+        if (grad_w && d->nsrc > 0) SWEEP_CUDA(cudaMemsetAsync(grad_w, 0, (size_t)d->B * d->nsrc * d->nt * 4, st));
+    }
     SWEEP_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
-    if (grad_w && d->nsrc > 0) SWEEP_CUDA(cudaMemsetAsync(grad_w, 0, (size_t)d->B * d->nsrc * d->nt * 4, st));
     const dim3 grid = stencil_grid(P), block(BXC, BYC);
     const unsigned gs = blocks_for((long long)P.B * P.nsrc, 128), gr = blocks_for((long long)P.B * P.nrec, 128);
     const unsigned gst = blocks_for((long long)P.B * P.nstrip, 256);
     int lp = 0, ln = 1, lx = 2, cur = 0;
+    int rp = 15, rn = 16, rx = 17;
+    if (stepped && !first) {
+        lp = seg->idx[0]; ln = seg->idx[1]; lx = seg->idx[2]; cur = seg->idx[3];
+        rp = seg->idx[4]; rn = seg->idx[5]; rx = seg->idx[6];
+    }
     float* gacc = w.f[18];
     float* gcomp = w.f[19];
     float* is = illum ? w.f[20] : nullptr;
@@ -1510,9 +1545,9 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
     // U[it1 - 1] (f[16]); strips_of(t) holds the strips of U[t].
     HostRing hr;
     const bool host = P.st.host && !ckpt && !recursive;
-    auto reverse = [&](int it0, int it1, auto strips_of) {
+    auto reverse = [&](int it0, int it1, auto strips_of, bool fresh) {
         StepGraphs sg(st, host ? 0 : P.graph_steps);
-        int rp = 15, rn = 16, rx = 17;
+        if (fresh) { rp = 15; rn = 16; rx = 17; }
         for (int it = it1 - 1; it >= it0; --it) {
             const cudaStream_t ls = sg.stream();
             float* a_in[6];
@@ -1536,7 +1571,7 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
                     strips3<<<gst, 256, 0, ls>>>(P, w.f[rx], strips_of(it - 1), nullptr, 1);
                     if (host) {
                         hr.after_read(it - 1);
-                        if (it - 1 - HostRing::R >= 0) hr.fetch(it - 1 - HostRing::R, true);
+                        if (it - 1 - HostRing::R >= std::max(it0 - 1, 0)) hr.fetch(it - 1 - HostRing::R, true);
                     }
                     if (d->nsrc > 0)
                         inject3<<<gs, 128, 0, ls>>>(P, w.f[rx], d->wavelet, d->src_loc, d->nsrc, it, 0, -1.f, 1);
@@ -1556,18 +1591,21 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
         sg.flush();
     };
     if (recursive) {
-        backward_recursive(d, P, w, chunk, snaps, ckpt_every, st, reverse);
+        auto rev = [&](int it0, int it1, auto strips_of) { reverse(it0, it1, strips_of, true); };
+        backward_recursive(d, P, w, chunk, snaps, ckpt_every, st, rev);
     } else if (!ckpt) {
-        const float* last = tape_last(const_cast<void*>(tape), P);
-        SWEEP_CUDA(cudaMemcpyAsync(w.f[15], last + n, n * 4, cudaMemcpyDefault, st));   // prev = U[nt]
-        SWEEP_CUDA(cudaMemcpyAsync(w.f[16], last, n * 4, cudaMemcpyDefault, st));       // now  = U[nt-1]
+        if (first) {
+            const float* last = tape_last(const_cast<void*>(tape), P);
+            SWEEP_CUDA(cudaMemcpyAsync(w.f[15], last + n, n * 4, cudaMemcpyDefault, st));   // prev = U[nt]
+            SWEEP_CUDA(cudaMemcpyAsync(w.f[16], last, n * 4, cudaMemcpyDefault, st));       // now  = U[nt-1]
+        }
         if (host && P.nstrip > 0) {
             hr.open(w.ring, const_cast<void*>(tape), P.st.step, st);
-            for (int t = d->nt - 2; t >= 0 && t > d->nt - 2 - HostRing::R; --t) hr.fetch(t, false);
-            reverse(0, d->nt, [&](int t) { return hr.slot(t); });
+            for (int t = top - 2; t >= std::max(bottom - 1, 0) && t > top - 2 - HostRing::R; --t) hr.fetch(t, false);
+            reverse(bottom, top, [&](int t) { return hr.slot(t); }, first);
             hr.close();
         } else {
-            reverse(0, d->nt, [&](int t) { return tape_slot(tape, P, t); });
+            reverse(bottom, top, [&](int t) { return tape_slot(tape, P, t); }, first);
         }
     } else {
         const int k = ckpt_every, C = nchunks(P, k);
@@ -1594,12 +1632,43 @@ void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const 
                           w.err, w.scratch, st);
             copy_dd(w.f[15], S.f[S.in], n, st);      // U[it1]
             copy_dd(w.f[16], S.f[S.ip], n, st);      // U[it1 - 1]
-            reverse(it0, it1, [&](int t) { return chunk + (long long)(t - (it0 - 1)) * cs; });
+            reverse(it0, it1, [&](int t) { return chunk + (long long)(t - (it0 - 1)) * cs; }, true);
         }
+    }
+    if (stepped) {
+        const int keep[7] = {lp, ln, lx, cur, rp, rn, rx};
+        for (int k = 0; k < 7; ++k) seg->idx[k] = keep[k];
     }
     finalize3<<<592, 256, 0, st>>>(gacc, gcomp, is, ir, P.B, (int)rows, d->nx, P.P, P.S, grad_vp, illum_s, illum_r);
     SWEEP_LAUNCH_CHECK();
     check_err(w, st, "backward");
+}
+
+void forward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, float* record, void* tape,
+             void* ws, int64_t ws_bytes, cudaStream_t st)
+{
+    forward_with(d, mem_mode, ckpt_every, record, tape, ws, ws_bytes, st, nullptr, 0, 0);
+}
+
+void backward(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, const float* adj, const void* tape,
+              float* grad_vp, float* grad_w, float* illum_s, float* illum_r,
+              void* ws, int64_t ws_bytes, cudaStream_t st)
+{
+    backward_with(d, mem_mode, ckpt_every, adj, tape, grad_vp, grad_w, illum_s, illum_r, ws, ws_bytes, st, nullptr,
+                  0, 0);
+}
+
+void forward_segment(const sweep_acoustic_desc* d, int mem_mode, float* record, void* tape, void* ws,
+                     int64_t ws_bytes, cudaStream_t st, StepState& seg, int it0, int it1)
+{
+    forward_with(d, mem_mode, 0, record, tape, ws, ws_bytes, st, &seg, it0, it1);
+}
+
+void backward_segment(const sweep_acoustic_desc* d, int mem_mode, const float* adj, const void* tape,
+                      float* grad_vp, float* grad_w, float* illum_s, float* illum_r, void* ws, int64_t ws_bytes,
+                      cudaStream_t st, StepState& seg, int bw0, int bw1)
+{
+    backward_with(d, mem_mode, 0, adj, tape, grad_vp, grad_w, illum_s, illum_r, ws, ws_bytes, st, &seg, bw0, bw1);
 }
 
 }  // namespace a3d

@@ -235,6 +235,19 @@ private:
     bool capturing_ = false;
 };
 
+// Between the segments of a stepped run (the sweep_b200_*_runner entries):
+// where the next segment starts and the rotating buffer state of the pass --
+// wavefield buffer indices, swapped CPML pointers -- which an equation saves
+// after a segment and restores before the next.  Segments run in order: a
+// forward [it_begin, it_end) starts where the last one ended, a backward
+// reverses [bw_end, bw_begin) starting where the last one stopped.
+struct StepState {
+    int next = 0;            // forward: next step; backward: the step above the next segment
+    bool begun = false;      // the first segment has run (fields set up)
+    int idx[8] = {};
+    void* ptr[8] = {};
+};
+
 // Source / receiver events grouped by (shot, tile): a CSR table so that the
 // CTA owning a tile finds its point sources and receivers without scanning the
 // whole list.  `cell` is the tile-local linear cell index, `id` the global

@@ -1618,10 +1618,16 @@ static void forward_steps(FwdArgs& A, int it0, int it1, StripsOf strips_of, floa
     gs.flush();
 }
 
-void forward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, float* record, void* tape,
-             void* ws, int64_t ws_bytes, cudaStream_t st)
+static void forward_with(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, float* record, void* tape,
+                         void* ws, int64_t ws_bytes, cudaStream_t st, StepState* seg, int seg0, int seg1)
 {
+    // a stepped run covers [seg0, seg1) of the time axis (the fields and CPML
+    // memories are updated in place: nothing rotates between segments)
+    const bool stepped = seg != nullptr;
+    const int a = stepped ? seg0 : 0;
     check_mode(mem_mode, ckpt_every);
+    SWEEP_REQUIRE(!stepped || (mem_mode != SWEEP_MEM_CHECKPOINT && mem_mode != SWEEP_MEM_RECURSIVE),
+                  "elastic2d stepped forward: boundary saving only");
     SWEEP_REQUIRE(record != nullptr || d->nrec == 0, "elastic2d forward: null record");
     Plan pl = make_plan(d);
     set_store(pl, mem_mode);
@@ -1630,9 +1636,12 @@ void forward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, float* r
     carve_fwd(c, pl, w);
     SWEEP_REQUIRE(ws != nullptr && c.off <= ws_bytes, "elastic2d forward: workspace too small (%lld < %lld bytes)",
                   (long long)ws_bytes, (long long)c.off);
-    SWEEP_CUDA(cudaMemsetAsync(w.zero0, 0, w.zero1 - w.zero0, st));
-    if (record && d->nrec)
-        SWEEP_CUDA(cudaMemsetAsync(record, 0, sizeof(float) * (size_t)d->B * d->nt * d->nrec * d->nrec_fields, st));
+    if (a == 0) {
+        SWEEP_CUDA(cudaMemsetAsync(w.zero0, 0, w.zero1 - w.zero0, st));
+        if (record && d->nrec)
+            SWEEP_CUDA(cudaMemsetAsync(record, 0, sizeof(float) * (size_t)d->B * d->nt * d->nrec * d->nrec_fields,
+                                       st));
+    }
     setup_common(d, pl, w.cm, st);
     FwdArgs A{};
     A.G = pl.G;
@@ -1646,12 +1655,13 @@ void forward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, float* r
     if (mem_mode != SWEEP_MEM_CHECKPOINT) {
         HostRing hr;
         const bool host = tape && pl.host_tape;
+        const int b = stepped ? seg1 : G.nt;
         if (host) hr.open(w.ring, tape, G.st.step, st);
-        forward_steps(A, 0, G.nt,
+        forward_steps(A, a, b,
                       [&](int it) { return !tape ? nullptr : host ? hr.slot(it) : tape_slot(tape, pl, it); },
                       w.scratch, st, pl.graph_steps, host ? &hr : nullptr);
         if (host) hr.close();
-        if (tape) {
+        if (tape && b == G.nt) {
             float* last = tape_last(tape, pl);
             for (int k = 0; k < 5; ++k)
                 SWEEP_CUDA(cudaMemcpyAsync(last + k * n, w.f[k], sizeof(float) * n, cudaMemcpyDefault, st));
@@ -1676,15 +1686,21 @@ void forward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, float* r
     check_err(w.cm, st, "forward");
 }
 
-void backward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, const float* adj, const void* tape,
-              float* grad_vp, float* grad_vs, float* grad_rho, void* ws, int64_t ws_bytes, cudaStream_t st)
+static void backward_with(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, const float* adj,
+                          const void* tape, float* grad_vp, float* grad_vs, float* grad_rho, void* ws,
+                          int64_t ws_bytes, cudaStream_t st, StepState* seg, int bw0, int bw1)
 {
+    // a stepped run reverses [bw1, bw0) top down, continuing seg's state
+    const bool stepped = seg != nullptr;
+    const int top = stepped ? bw0 : d->nt, bottom = stepped ? bw1 : 0;
+    const bool first = top == d->nt;
     check_mode(mem_mode, ckpt_every);
     SWEEP_REQUIRE(tape != nullptr, "elastic2d backward: null tape");
     SWEEP_REQUIRE(grad_vp && grad_vs && grad_rho, "elastic2d backward: null gradient output");
     SWEEP_REQUIRE(adj != nullptr || d->nrec == 0, "elastic2d backward: null adjoint source");
     const bool ckpt = mem_mode == SWEEP_MEM_CHECKPOINT;
     const bool recursive = mem_mode == SWEEP_MEM_RECURSIVE;
+    SWEEP_REQUIRE(!stepped || (!ckpt && !recursive), "elastic2d stepped backward: boundary saving only");
     Plan pl = make_plan(d);
     set_store(pl, mem_mode);
     Carve c(ws);
@@ -1697,7 +1713,7 @@ void backward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, const f
     } else carve_rev(c, pl, w);
     SWEEP_REQUIRE(ws != nullptr && c.off <= ws_bytes, "elastic2d backward: workspace too small (%lld < %lld bytes)",
                   (long long)ws_bytes, (long long)c.off);
-    SWEEP_CUDA(cudaMemsetAsync(w.zero0, 0, w.zero1 - w.zero0, st));
+    if (first) SWEEP_CUDA(cudaMemsetAsync(w.zero0, 0, w.zero1 - w.zero0, st));
     setup_common(d, pl, w.cm, st);
     const Geo& G = pl.G;
     const long long n = (long long)G.B * G.S;
@@ -1711,7 +1727,7 @@ void backward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, const f
     A.G_shots = pl.gshots;
     const dim3 block(TX, 8);
     const dim3 grid_s(G.ntx * G.ntz, pl.nslot), grid_b(G.ntx * G.ntz, G.B);
-    int cur = 0;
+    int cur = stepped && !first ? seg->idx[0] : 0;
     // Reverse steps it1 - 1 .. max(it0, 1) (the staggered reverse has no
     // it = 0 step) on the reconstruction state after step it1 - 1;
     // strips_of(t) holds the strips of the state after step t.
@@ -1733,7 +1749,7 @@ void backward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, const f
             rev_vadj<<<grid_b, block, SM_REV_VADJ, ls>>>(A);
             if (host) {
                 hr.after_read(it - 1);
-                if (it - 1 - HostRing::R >= 0) hr.fetch(it - 1 - HostRing::R, true);
+                if (it - 1 - HostRing::R >= std::max(it0 - 1, 0)) hr.fetch(it - 1 - HostRing::R, true);
             }
             SWEEP_LAUNCH_CHECK();
             gs.step_done();
@@ -1815,16 +1831,18 @@ void backward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, const f
         };
         process(0, G.nt, -1, count);
     } else if (!ckpt) {
-        const float* last = tape_last(const_cast<void*>(tape), pl);
-        for (int k = 0; k < 5; ++k)
-            SWEEP_CUDA(cudaMemcpyAsync(w.f[k], last + k * n, sizeof(float) * n, cudaMemcpyDefault, st));
+        if (first) {
+            const float* last = tape_last(const_cast<void*>(tape), pl);
+            for (int k = 0; k < 5; ++k)
+                SWEEP_CUDA(cudaMemcpyAsync(w.f[k], last + k * n, sizeof(float) * n, cudaMemcpyDefault, st));
+        }
         if (host) {
             hr.open(w.ring, const_cast<void*>(tape), G.st.step, st);
-            for (int t = G.nt - 2; t >= 0 && t > G.nt - 2 - HostRing::R; --t) hr.fetch(t, false);
-            reverse(0, G.nt, [&](int t) { return hr.slot(t); });
+            for (int t = top - 2; t >= std::max(bottom - 1, 0) && t > top - 2 - HostRing::R; --t) hr.fetch(t, false);
+            reverse(bottom, top, [&](int t) { return hr.slot(t); });
             hr.close();
         } else {
-            reverse(0, G.nt, [&](int t) { return tape_slot(tape, pl, t); });
+            reverse(bottom, top, [&](int t) { return tape_slot(tape, pl, t); });
         }
     } else {
         const int k = ckpt_every, C = nchunks(pl, k);
@@ -1857,12 +1875,38 @@ void backward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, const f
             reverse(it0, it1, [&](int t) { return (const float*)w.chunk + (long long)(t - (it0 - 1)) * cs; });
         }
     }
+    if (stepped) seg->idx[0] = cur;
     const int per_shot = G.ms != 0;
     finalize_kernel<<<592, 256, 0, st>>>(w.gvp, pl.nslot, per_shot, G, grad_vp);
     finalize_kernel<<<592, 256, 0, st>>>(w.gvs, pl.nslot, per_shot, G, grad_vs);
     finalize_kernel<<<592, 256, 0, st>>>(w.grho, pl.nslot, per_shot, G, grad_rho);
     SWEEP_LAUNCH_CHECK();
     check_err(w.cm, st, "backward");
+}
+
+void forward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, float* record, void* tape,
+             void* ws, int64_t ws_bytes, cudaStream_t st)
+{
+    forward_with(d, mem_mode, ckpt_every, record, tape, ws, ws_bytes, st, nullptr, 0, 0);
+}
+
+void backward(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, const float* adj, const void* tape,
+              float* grad_vp, float* grad_vs, float* grad_rho, void* ws, int64_t ws_bytes, cudaStream_t st)
+{
+    backward_with(d, mem_mode, ckpt_every, adj, tape, grad_vp, grad_vs, grad_rho, ws, ws_bytes, st, nullptr, 0, 0);
+}
+
+void forward_segment(const sweep_elastic_desc* d, int mem_mode, float* record, void* tape, void* ws,
+                     int64_t ws_bytes, cudaStream_t st, StepState& seg, int it0, int it1)
+{
+    forward_with(d, mem_mode, 0, record, tape, ws, ws_bytes, st, &seg, it0, it1);
+}
+
+void backward_segment(const sweep_elastic_desc* d, int mem_mode, const float* adj, const void* tape,
+                      float* grad_vp, float* grad_vs, float* grad_rho, void* ws, int64_t ws_bytes, cudaStream_t st,
+                      StepState& seg, int bw0, int bw1)
+{
+    backward_with(d, mem_mode, 0, adj, tape, grad_vp, grad_vs, grad_rho, ws, ws_bytes, st, &seg, bw0, bw1);
 }
 
 }  // namespace el2d

@@ -94,6 +94,6 @@ extern "C" SWEEP_B200_API int sweep_b200_acoustic_forward_noalloc(const sweep_ac
         void* ws = scratch_of_device(current_device());
         const a2d::HostStage stage{h_loc_src, h_loc_rec, h_off_src, h_off_rec, h_ev_src, h_ev_rec, h_fill, h_order};
         a2d::forward_with(d, SWEEP_MEM_BOUNDARY, 0, record, nullptr, ws, kNoAllocScratchBytes, static_cast<cudaStream_t>(stream),
-                          &stage);
+                          &stage, nullptr, 0, 0);
     });
 }

@@ -526,6 +526,22 @@ class PropTorch(torch.nn.Module):
 
     # ---------------------------------------------------------------- forward
     def forward(self, wavelet, sources, receivers, models=None, max_vel=4500.0, pml_freq=25.0):
+        geo, padded, wb, fields, mem_mode, ckpt_every, wavelet = self._prepare(
+            wavelet, sources, receivers, models, max_vel, pml_freq)
+        eq = self.equation
+        if isinstance(eq, (Acoustic, Acoustic3D)):
+            return _AcousticFn.apply(padded[0], wb, self, geo, mem_mode, ckpt_every)
+        if isinstance(eq, Elastic):
+            if wavelet.requires_grad and torch.is_grad_enabled():
+                raise NotImplementedError(
+                    "impl='c' Elastic does not return the wavelet gradient (its compiled backward "
+                    "returns the model gradients only). Detach the wavelet.")
+            return _ElasticFn.apply(*padded, wb, self, geo, fields, mem_mode, ckpt_every)
+        raise NotImplementedError(f"{type(eq).__name__} is not built")
+
+    def _prepare(self, wavelet, sources, receivers, models, max_vel, pml_freq):
+        """Checked inputs of a call: the geometry, the padded models, the
+        per-shot wavelet view, the elastic fields, and the memory mode."""
         eq = self.equation
         nd = eq.NDIM
         dev = self.device
@@ -565,14 +581,14 @@ class PropTorch(torch.nn.Module):
         if self.autotune or self.schedule is not None:
             self._apply_schedule(geo, padded, wb, fields, mem_mode, ckpt_every)
         mem_mode, ckpt_every = self._apply_budget(geo, padded, wb, fields, mem_mode, ckpt_every)
-        if isinstance(eq, (Acoustic, Acoustic3D)):
-            return _AcousticFn.apply(padded[0], wb, self, geo, mem_mode, ckpt_every)
-        if isinstance(eq, Elastic):
-            if len({m.dim() for m in models}) != 1:
-                raise ValueError("vp, vs and rho must all be shared (nz, nx) or all per shot (B, nz, nx)")
-            if wavelet.requires_grad and torch.is_grad_enabled():
-                raise NotImplementedError(
-                    "impl='c' Elastic does not return the wavelet gradient (its compiled backward "
-                    "returns the model gradients only). Detach the wavelet.")
-            return _ElasticFn.apply(*padded, wb, self, geo, fields, mem_mode, ckpt_every)
-        raise NotImplementedError(f"{type(eq).__name__} is not built")
+        if isinstance(eq, Elastic) and len({m.dim() for m in models}) != 1:
+            raise ValueError("vp, vs and rho must all be shared (nz, nx) or all per shot (B, nz, nx)")
+        return geo, padded, wb, fields, mem_mode, ckpt_every, wavelet
+
+    # ------------------------------------------------------- stepped runners
+    def forward_runner(self, wavelet, sources, receivers, models=None, max_vel=4500.0, pml_freq=25.0):
+        """A persistent forward over these inputs, advanced segment by segment
+        (reference ``sweep.backend.c.runners.ForwardRunner``): see
+        :class:`sweep_b200.runners.ForwardRunner`."""
+        from .runners import ForwardRunner
+        return ForwardRunner(self, wavelet, sources, receivers, models, max_vel, pml_freq)
