@@ -218,6 +218,12 @@ class AcousticWorkload:
                 "boundary_tape": f"{STRIPS[1]} strips in {STRIPS[0]} memory",
                 "parallelism": f"shots: {NSHOT} per GPU x {args.gpus} GPU(s)"}
 
+    dh, dt, abcn, ref_gpu_nt = DH, DT, ABCN, 3000
+
+    def survey_inputs(self):
+        vp_true, vp_init, w, src, rec = survey()
+        return [vp_true], [vp_init], w, src, rec
+
     def build(self, dev):
         from sweep_b200 import Acoustic, PropTorch
         vp_true, vp_init, w, src, rec = survey()
@@ -279,6 +285,12 @@ class AcousticC1Workload:
                 "boundary_tape": f"{STRIPS[1]} strips in {STRIPS[0]} memory",
                 "parallelism": f"replicas: 1 shot per GPU x {args.gpus} GPU(s)"}
 
+    dh, dt, abcn, ref_gpu_nt = C1_DH, C1_DT, C1_ABCN, C1_NT
+
+    def survey_inputs(self):
+        vp_true, vp_init, w, src, rec = c1_survey()
+        return [vp_true], [vp_init], w, src, rec
+
     def build(self, dev):
         from sweep_b200 import Acoustic, PropTorch
         vp_true, vp_init, w, src, rec = c1_survey()
@@ -319,6 +331,11 @@ class ElasticWorkload:
                 "physical_fraction": E_NZ * E_NX / (E_RT[0] * E_RT[1]),
                 "l2": "working set per step > L2 (inputs larger than L2; no flush)",
                 "parallelism": f"shots: {E_NSHOT} per GPU x {args.gpus} GPU(s)"}
+
+    dh, dt, abcn, ref_gpu_nt = E_DH, E_DT, E_ABCN, 1000
+
+    def survey_inputs(self):
+        return elastic_survey()
 
     def build(self, dev):
         from sweep_b200 import Elastic, PropTorch
@@ -417,6 +434,11 @@ class Acoustic3DWorkload:
                                f"(at most {A3_BATCH}) unless --shots-per-call is given",
                 "courant_max": 4247.13 * A3_DT / A3_DH}
 
+    dh, dt, abcn, ref_gpu_nt = A3_DH, A3_DT, A3_ABCN, 200
+
+    def survey_inputs(self):
+        return acoustic3d_survey()
+
     def build(self, dev):
         from sweep_b200 import Acoustic3D, PropTorch
         m_true, m_init, w, src, rec = acoustic3d_survey()
@@ -483,6 +505,61 @@ def run_reference(args, wl):
         "e2e": {"value": value, "unit": "Gcell/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
+
+
+# ------------------------------------------------- the reference's CUDA core
+REF_DIR = ROOT / "baseline" / "_ref"
+
+
+def reference_cuda(wl, group, nt_sample, dev, reps=2):
+    """The reference's own impl='c' CUDA core (installed under baseline/_ref
+    with its core built for this GPU) on the same workload: `group` shots of
+    the survey over the first `nt_sample` steps, forward + adjoint gradient
+    through its public PropTorch API, timed with CUDA events (best of `reps`
+    after one warm-up).  Runs after every timed region of this bench."""
+    import torch
+    core = list(REF_DIR.glob("sweep/lib/cu*/libsweep_core.so"))
+    if not core:
+        return {"unavailable": "the reference's CUDA core is not built under baseline/_ref"}
+    if str(REF_DIR) not in sys.path:
+        sys.path.insert(0, str(REF_DIR))
+    try:
+        from sweep.equations import Acoustic, Acoustic3D, Elastic
+        from sweep.propagator.options import BoundarySaving
+        from sweep.propagator.torch import PropTorch
+    except Exception as e:                       # noqa: BLE001
+        return {"unavailable": f"the reference does not import: {e}"}
+    m_true, m_init, w, src, rec = wl.survey_inputs()
+    eq = {"acoustic2d": Acoustic, "acoustic2d_c1": Acoustic, "elastic2d": Elastic,
+          "acoustic3d": Acoustic3D}[wl.name]
+    solver = PropTorch(eq(spatial_order=ORDER, device=dev), shape=tuple(m_true[0].shape), dh=wl.dh,
+                       dt=wl.dt, abcn=wl.abcn, impl="c", device=dev, memory=BoundarySaving())
+    wt = torch.tensor(w[:nt_sample], device=dev)
+    sh = list(range(min(group, len(src))))
+    with torch.no_grad():
+        obs = solver(wt, src[sh], rec[sh], models=[torch.tensor(m, device=dev) for m in m_true])
+    best = None
+    for r in range(reps + 1):
+        ms = [torch.tensor(m, device=dev, requires_grad=True) for m in m_init]
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        torch.cuda.synchronize()
+        e0.record()
+        pred = solver(wt, src[sh], rec[sh], models=ms)
+        loss = 0.5 * ((pred - obs) ** 2).sum()
+        e1.record()
+        loss.backward()
+        e2.record()
+        torch.cuda.synchronize()
+        t = (e0.elapsed_time(e2), e0.elapsed_time(e1), e1.elapsed_time(e2))
+        if r > 0 and (best is None or t[0] < best[0]):
+            best = t
+    cells = int(np.prod(wl.rt)) * len(sh) * nt_sample
+    return {"value": cells / (best[0] * 1e-3) / 1e9, "unit": "Gcell/s", "forward_ms": best[1],
+            "backward_ms": best[2], "sample": f"{len(sh)} shot(s), first {nt_sample} of {wl.nt} steps, "
+                                              "forward + adjoint gradient, boundary saving",
+            "how": "reference PropTorch(impl='c') on this GPU, CUDA events, best of "
+                   f"{reps} after a warm-up",
+            "core": str(core[0].relative_to(ROOT))}
 
 
 # ---------------------------------------------------------------------- GPU
@@ -677,6 +754,11 @@ def run_gpu(args, wl):
                                 "kind": "port",
                                 "sample": f"1 of {wl.nshot} shots, first {wl.cpu_nt} of {wl.nt} steps, "
                                           "fwd+adj gradient"}
+    if rank == 0 and not args.no_reference_gpu:
+        try:
+            line["reference_gpu"] = reference_cuda(wl, group, min(wl.nt, wl.ref_gpu_nt), dev)
+        except Exception as e:                   # noqa: BLE001
+            line["reference_gpu"] = {"unavailable": f"{type(e).__name__}: {e}"[:300]}
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
@@ -761,6 +843,8 @@ def main():
                     help="acoustic workloads: boundary tape in GPU memory or pinned host memory")
     ap.add_argument("--strip-dtype", default="fp32", choices=["fp32", "fp16", "bf16", "int8"],
                     help="acoustic workloads: boundary strip storage format (fp32 is exact)")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip the leg that times the reference's own CUDA core (baseline/_ref) on a sample")
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the end-to-end leg (long workloads; the bench line then has no e2e value)")
     ap.add_argument("--pairs", type=int, default=2000, help="fwi workload: training pairs")
