@@ -19,7 +19,7 @@
 // tcgen05.commit on a per-stage mbarrier releases each of the two shared-memory
 // stages, so the gather of one K tile overlaps the MMAs of the previous one.
 // The epilogue reads the accumulator with tcgen05.ld.  The weight gradient
-// (K = pixels) runs on mma.sync m16n8k16.
+// (K = pixels) runs on the same tensor-core path, transposed (wgrad_umma).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -30,16 +30,7 @@
 namespace sweep {
 namespace conv {
 
-constexpr int BM = 128, BN = 64, BK = 32, PADK = 8, NT = 256;
-
-__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2])
-{
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
-        "{%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, {%0, %1, %2, %3};"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
+constexpr int BM = 128, BN = 64, NT = 256;
 
 // ------------------------------------------------------------ tcgen05 path
 namespace umma {
@@ -229,108 +220,120 @@ __global__ void __launch_bounds__(NT) gather_gemm(const __nv_bfloat16* __restric
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(umma::TMEM_COLS));
 }
 
-// dw[co, k] += sum over this CTA's pixel range of dy[p, co] * X[p, k], where
-// X[p, k = t C + c] = x[p + off(t), c].  M = Co (64 per CTA), N = 9 C (64 per
-// CTA), K = pixels (split over blockIdx.z, partial sums added atomically).
-__global__ void __launch_bounds__(NT) weight_grad(const __nv_bfloat16* __restrict__ x,
-                                                  const __nv_bfloat16* __restrict__ dy, float* __restrict__ dw,
-                                                  int Nimg, int H, int W, int C, int Co, int pix_per_split)
+// Weight gradient on the 5th-generation tensor cores, transposed:
+//   dw[co, k] = sum_p X[p, k] dy[p, co],  X[p, k = t C + c] = x[p + off(t), c],
+// as D[k, co] = A[k, p] B[co, p] with M = 9 C (128 per CTA), N = Co (64 per
+// CTA) and K = pixels (64 per shared-memory stage; the pixel range split
+// over blockIdx.z, partial sums added atomically).  Both operands are
+// gathered K-major (pixels contiguous): a 16-byte load of x (8 channels of one
+// tap-shifted pixel) or of dy (8 output channels of one pixel) fills one
+// K column of 8 rows.  Same shared-memory layout, descriptors and MMA shape
+// (M 128, N 64, K 16) as gather_gemm; the epilogue reads the accumulator with
+// tcgen05.ld and adds it into dw.
+__global__ void __launch_bounds__(NT) wgrad_umma(const __nv_bfloat16* __restrict__ x,
+                                                 const __nv_bfloat16* __restrict__ dy, float* __restrict__ dw,
+                                                 int Nimg, int H, int W, int C, int Co, int pix_per_split, int* err)
 {
-    constexpr int WM = 64;
-    __shared__ __align__(16) __nv_bfloat16 As[WM][BK + PADK];   // [co][pixel]
-    __shared__ __align__(16) __nv_bfloat16 Bs[BN][BK + PADK];   // [k][pixel]
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;       // 8 warps: 2 (M) x 4 (N) of 32 x 16
-    const long long P = (long long)Nimg * H * W;
-    const int co0 = blockIdx.x * WM, kb0 = blockIdx.y * BN;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    umma::Smem& sm = *reinterpret_cast<umma::Smem*>(smem_raw);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const long long P = (long long)Nimg * H * W, HW = (long long)H * W;
     const int K = 9 * C;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
     const long long pbeg = (long long)blockIdx.z * pix_per_split;
     const long long pend = min(P, pbeg + pix_per_split);
-    float acc[2][2][4];
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 2; ++j)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
-    for (long long pp = pbeg; pp < pend; pp += BK) {
-        // A^T: dy[pp + r, co0 .. co0+63] -> As[co][r]; 32 pixels x 8 groups = 256 units
-        {
-            const int r = tid >> 3, gc = (tid & 7) * 8;
-            const long long p = pp + r;
-            const int co = co0 + gc;
-            __nv_bfloat16 v[8];
-            if (p < pend && co < Co) {
-                const uint4 u = *reinterpret_cast<const uint4*>(dy + p * Co + co);
-                memcpy(v, &u, 16);
-            } else {
-#pragma unroll
-                for (int e = 0; e < 8; ++e) v[e] = __float2bfloat16(0.f);
-            }
-#pragma unroll
-            for (int e = 0; e < 8; ++e) As[gc + e][r] = v[e];
-        }
-        // B^T: X[pp + r, kb0 .. kb0+63] -> Bs[k][r]
-        {
-            const int r = tid >> 3, gk = (tid & 7) * 8;
-            const long long p = pp + r;
-            const int k = kb0 + gk;
-            __nv_bfloat16 v[8];
-#pragma unroll
-            for (int e = 0; e < 8; ++e) v[e] = __float2bfloat16(0.f);
-            if (p < pend && k < K) {
-                const int t = k / C, c = k - t * C;
-                const int ddy = t / 3 - 1, ddx = t % 3 - 1;
-                const int img = (int)(p / ((long long)H * W));
-                const int rem = (int)(p - (long long)img * H * W);
-                const int h = rem / W + ddy, w = rem % W + ddx;
-                if (h >= 0 && h < H && w >= 0 && w < W) {
-                    const uint4 u = *reinterpret_cast<const uint4*>(x + (((long long)img * H + h) * W + w) * C + c);
-                    memcpy(v, &u, 16);
-                }
-            }
-#pragma unroll
-            for (int e = 0; e < 8; ++e) Bs[gk + e][r] = v[e];
-        }
-        __syncthreads();
-        const int g = lane >> 2, q = lane & 3;
-#pragma unroll
-        for (int kk = 0; kk < BK; kk += 16) {
-            uint32_t a[2][4], b[2][2];
-#pragma unroll
-            for (int i = 0; i < 2; ++i) {
-                const int r = wm + i * 16 + g;
-                a[i][0] = *reinterpret_cast<const uint32_t*>(&As[r][kk + 2 * q]);
-                a[i][1] = *reinterpret_cast<const uint32_t*>(&As[r + 8][kk + 2 * q]);
-                a[i][2] = *reinterpret_cast<const uint32_t*>(&As[r][kk + 2 * q + 8]);
-                a[i][3] = *reinterpret_cast<const uint32_t*>(&As[r + 8][kk + 2 * q + 8]);
-            }
-#pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                const int c = wn + j * 8 + g;
-                b[j][0] = *reinterpret_cast<const uint32_t*>(&Bs[c][kk + 2 * q]);
-                b[j][1] = *reinterpret_cast<const uint32_t*>(&Bs[c][kk + 2 * q + 8]);
-            }
-#pragma unroll
-            for (int i = 0; i < 2; ++i)
-#pragma unroll
-                for (int j = 0; j < 2; ++j) mma_bf16(acc[i][j], a[i], b[j]);
-        }
-        __syncthreads();
+    const int nk = (int)((pend - pbeg + umma::TK - 1) / umma::TK);
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tma::smem_u32(&sm.tmem)),
+                     "r"(umma::TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
-    const int g = lane >> 2, q = lane & 3;
+    if (tid == 0) {
+        tma::mbar_init(&sm.done[0], 1);
+        tma::mbar_init(&sm.done[1], 1);
+        tma::fence_barrier_init();
+    }
+    umma::fence_before();
+    __syncthreads();
+    umma::fence_after();
+    const uint32_t tmem = sm.tmem;
+    // this thread's pixel column of the stage: the same for every unit it gathers
+    const int pc = tid & (umma::TK - 1);
+    bool ok = true;
+    for (int kt = 0; kt < nk; ++kt) {
+        const int st = kt & 1;
+        if (kt >= 2) ok = ok && tma::mbar_wait(&sm.done[st], ((kt >> 1) - 1) & 1, err, umma::ERR_MMA_WAIT);
+        const long long p = pbeg + (long long)kt * umma::TK + pc;
+        const bool pin = p < pend;
+        const int img = pin ? (int)(p / HW) : 0;
+        const int rem = pin ? (int)(p - (long long)img * HW) : 0;
+        const int ph = rem / W, pw = rem - (rem / W) * W;
+        const uint32_t col = (uint32_t)(pc & 7) * 2;
+        // A: 16 row groups of 8 (k = m0 + 8 g .. + 7, one tap, 8 channels) x 64 pixels
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 2; ++j)
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int co = co0 + wm + i * 16 + g + 8 * h;
-                const int k = kb0 + wn + j * 8 + 2 * q;
-                if (co >= Co) continue;
-                if (k < K) atomicAdd(dw + (long long)co * K + k, acc[i][j][2 * h]);
-                if (k + 1 < K) atomicAdd(dw + (long long)co * K + k + 1, acc[i][j][2 * h + 1]);
+        for (int u = 0; u < 4; ++u) {
+            const int g = (tid >> 6) + 4 * u;             // 0..15
+            const int k = m0 + 8 * g;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (pin && k < K) {
+                const int t = k / C, c = k - t * C;
+                const int h = ph + (t / 3 - 1), w = pw + (t % 3 - 1);
+                if (h >= 0 && h < H && w >= 0 && w < W)
+                    v = *reinterpret_cast<const uint4*>(x + (((long long)img * H + h) * W + w) * C + c);
             }
+            const __nv_bfloat16* e = reinterpret_cast<const __nv_bfloat16*>(&v);
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+                *reinterpret_cast<__nv_bfloat16*>(sm.a[st] + umma::chunk_off(8 * g + r, pc >> 3) + col) = e[r];
+        }
+        // B: 8 row groups of 8 output channels x 64 pixels
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int g = (tid >> 6) + 4 * u;             // 0..7
+            const int co = n0 + 8 * g;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (pin && co < Co) v = *reinterpret_cast<const uint4*>(dy + p * Co + co);
+            const __nv_bfloat16* e = reinterpret_cast<const __nv_bfloat16*>(&v);
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+                *reinterpret_cast<__nv_bfloat16*>(sm.b[st] + umma::chunk_off(8 * g + r, pc >> 3) + col) = e[r];
+        }
+        umma::fence_async_smem();                        // generic writes -> tensor-core reads
+        __syncthreads();
+        if (tid == 0) {
+            umma::fence_after();
+            const uint32_t a0 = tma::smem_u32(sm.a[st]), b0 = tma::smem_u32(sm.b[st]);
+#pragma unroll
+            for (int kk = 0; kk < umma::TK / 16; ++kk)
+                umma::mma(tmem, umma::smem_desc(a0 + kk * 256), umma::smem_desc(b0 + kk * 256),
+                          (kt > 0 || kk > 0) ? 1u : 0u);
+            umma::commit(&sm.done[st]);
+        }
+    }
+    if (nk > 0) {
+        const int last = nk - 1;
+        ok = ok && tma::mbar_wait(&sm.done[last & 1], (last >> 1) & 1, err, umma::ERR_MMA_WAIT);
+    }
+    umma::fence_after();
+    const int q = warp & 3, half = warp >> 2;
+    const int k = m0 + 32 * q + lane;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        float v[8];
+        umma::ld8(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(32 * half + 8 * j), v);
+        umma::wait_ld();
+        const int co = n0 + 32 * half + 8 * j;
+        if (ok && nk > 0 && k < K) {
+#pragma unroll
+            for (int e = 0; e < 8; ++e)
+                if (co + e < Co) atomicAdd(dw + (long long)(co + e) * K + k, v[e]);
+        }
+    }
+    umma::fence_before();
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(umma::TMEM_COLS));
 }
 
 // Device error flag of the convolution kernels (one per process; zeroed
@@ -390,17 +393,25 @@ extern "C" int sweep_b200_conv3x3_wgrad(const void* x, const void* dy, float* dw
         SWEEP_REQUIRE(((uintptr_t)x & 15) == 0 && ((uintptr_t)dy & 15) == 0, "conv3x3 wgrad: operands must be 16-byte aligned");
         const long long P = (long long)n * h * w;
         const int K = 9 * c;
-        const unsigned gx = (unsigned)((co + 63) / 64), gy = (unsigned)((K + conv::BN - 1) / conv::BN);
-        // pixel splits: about four CTAs per SM in all, each split a multiple of 32 pixels
+        // tensor cores: M = 9 c (128 per CTA), N = co (64 per CTA), K = pixels
+        const unsigned gx = (unsigned)((K + conv::BM - 1) / conv::BM), gy = (unsigned)((co + conv::BN - 1) / conv::BN);
+        // pixel splits: about four CTAs per SM in all, each split a multiple of 64 pixels
         long long splits = std::max(1LL, (4LL * 148) / ((long long)gx * gy));
         long long per = (P + splits - 1) / splits;
-        per = (per + 31) / 32 * 32;
+        per = (per + 63) / 64 * 64;
         splits = (P + per - 1) / per;
         const dim3 grid(gx, gy, (unsigned)splits);
         cudaStream_t st = static_cast<cudaStream_t>(stream);
+        static bool attr = false;
+        if (!attr) {
+            SWEEP_CUDA(cudaFuncSetAttribute(conv::wgrad_umma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)sizeof(conv::umma::Smem)));
+            attr = true;
+        }
         SWEEP_CUDA(cudaMemsetAsync(dw, 0, sizeof(float) * (size_t)co * K, st));
-        conv::weight_grad<<<grid, conv::NT, 0, st>>>(static_cast<const __nv_bfloat16*>(x),
-                                                     static_cast<const __nv_bfloat16*>(dy), dw, n, h, w, c, co, (int)per);
+        conv::wgrad_umma<<<grid, conv::NT, sizeof(conv::umma::Smem), st>>>(
+            static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(dy), dw, n, h, w, c, co,
+            (int)per, conv::error_flag());
         SWEEP_LAUNCH_CHECK();
     });
 }
