@@ -266,7 +266,22 @@ struct F3 {
 // stage z + M into the queue, so stages z .. z + M must have landed; with NF3
 // stages the loads run NF3 - M - 1 planes ahead of the compute, TMA-issued by
 // one thread on one mbarrier per stage.
-constexpr int NF3 = 11;
+// Ring depths and CTAs per SM of the three stencil kernels: build-time knobs
+// (the shared-memory ring and the L1 share the same on-chip memory).
+#ifndef SWEEP_A3D_FWD_STAGES
+#define SWEEP_A3D_FWD_STAGES 11
+#endif
+#ifndef SWEEP_A3D_ADJ_STAGES
+#define SWEEP_A3D_ADJ_STAGES 8
+#endif
+#ifndef SWEEP_A3D_REC_STAGES
+#define SWEEP_A3D_REC_STAGES 9
+#endif
+#ifndef SWEEP_A3D_CTAS
+#define SWEEP_A3D_CTAS 4
+#endif
+constexpr int NF3 = SWEEP_A3D_FWD_STAGES;
+static_assert(NF3 >= 2 * M + 1, "the forward ring must hold the first plane's z-taps and one more stage");
 constexpr int CN3 = BXC * BYC;
 struct F3Smem {
     float u[NF3][PN];
@@ -287,7 +302,7 @@ enum { ERR_WAIT_F3 = 1 };
 // The CPML branch of an axis runs on its band plus one cell (reference
 // forward_split.cu:150-156) and uses the product-rule split
 // tmp = (((1 + b) Lap + db du) + a dpsi) + da psi (forward_split.cu:171-172).
-__global__ void __launch_bounds__(NTH, 4) f3_step(const __grid_constant__ F3Maps MP, const Params P, const F3 F,
+__global__ void __launch_bounds__(NTH, SWEEP_A3D_CTAS) f3_step(const __grid_constant__ F3Maps MP, const Params P, const F3 F,
                                                   const int uin, const int uprev, int* err)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -624,7 +639,8 @@ __device__ __forceinline__ void adj_axis(const Params& P, const float4* __restri
 // plane of the next plane's x / y taps once, in a double buffer, at the end
 // of each plane.  Stages z .. z + M must have landed at plane z; with NA3
 // stages the loads run NA3 - M - 1 planes ahead.
-constexpr int NA3 = 8;
+constexpr int NA3 = SWEEP_A3D_ADJ_STAGES;
+static_assert(NA3 >= 2 * M, "the adjoint ring must hold the 2M stages of the first plane's z-queue");
 
 struct A3Smem {
     float l[NA3][PN];
@@ -644,7 +660,7 @@ struct A3Maps {
 // pure interior  2 l - l_prev + Lap(gw) (difference form around gw);
 // shell          per axis outside the clear box the transposed CPML terms,
 //                inside it the bare Laplacian of gw.
-__global__ void __launch_bounds__(NTH, 4) a3_step(const __grid_constant__ A3Maps MP, const Params P, const A3 A,
+__global__ void __launch_bounds__(NTH, SWEEP_A3D_CTAS) a3_step(const __grid_constant__ A3Maps MP, const Params P, const A3 A,
                                                   const int lnow, const int lprev, int* err)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -803,7 +819,8 @@ struct R3 {
 // the nine z-taps of its column in a register queue (plane z pushes the
 // centre of stage z + M), so stages z .. z + M must have landed at plane z:
 // the halo loads run NR3 - M - 1 planes ahead, the centre tiles NRC3 - 1.
-constexpr int NR3 = 9;
+constexpr int NR3 = SWEEP_A3D_REC_STAGES;
+static_assert(NR3 >= 2 * M + 1, "the reconstruction ring must hold the first plane's z-taps and one more stage");
 constexpr int NRC3 = NR3 - M;
 struct R3Smem {
     float u[NR3][PN];
@@ -822,7 +839,7 @@ struct R3Maps {
 // u(it-1) = 2 u(it) - u(it+1) + vp^2 dt^2 Lap u(it) on the reconstruction box
 // (the physical box minus the restored strips) with the fused vp image
 // 2 dt^2 u_tt lambda(it) / vp (reference forward_split.cu:292-372).
-__global__ void __launch_bounds__(NTH, 4) r3_recon(const __grid_constant__ R3Maps MP, const Params P, const R3 R,
+__global__ void __launch_bounds__(NTH, SWEEP_A3D_CTAS) r3_recon(const __grid_constant__ R3Maps MP, const Params P, const R3 R,
                                                    const int rnow, const int rprev, const int lnow, int* err)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
