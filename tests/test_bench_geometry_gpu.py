@@ -77,12 +77,12 @@ def test_acoustic3d_clean_ctas_match_reference(z_chunks, clean_oracle):
     d = load("acoustic3d_clean")
     sched = None if z_chunks is None else {"z_chunks": z_chunks}
     s = _acoustic(d, schedule=sched)
+    pred, g, gw = _acoustic_grad(s, d)
     got = s.launch_schedule(d["wavelet"].shape[-1], d["src"], d["rec"], [torch.tensor(d["vp_init"], device=DEV)])
     if z_chunks is not None:
         assert got["z_chunks"] == z_chunks
     if z_chunks != 1:
         assert _clean_ctas(d, got["z_chunks"]) > 0          # the clean path runs
-    pred, g, gw = _acoustic_grad(s, d)
     p64, _, g64, gw64 = clean_oracle
     print(f"3-D clean, {got['z_chunks']} z chunks ({_clean_ctas(d, got['z_chunks'])} clean blocks per shot): "
           f"vs reference record {rel(pred, d['pred']):.2e} grad {rel(g, d['grad_vp']):.2e}; vs f64 oracle "
@@ -114,9 +114,9 @@ def many_oracle():
 def test_acoustic2d_shot_groups_match_reference(fwd, rev, many_oracle):
     d = load("acoustic2d_many")
     s = _acoustic(d, schedule={"shots_fwd": fwd, "shots_rev": rev})
+    pred, g, gw = _acoustic_grad(s, d)
     got = s.launch_schedule(d["wavelet"].shape[-1], d["src"], d["rec"], [torch.tensor(d["vp_init"], device=DEV)])
     assert (got["shots_fwd"], got["shots_rev"]) == (fwd, rev)
-    pred, g, gw = _acoustic_grad(s, d)
     p64, _, g64, gw64 = many_oracle
     print(f"2-D 20 shots, {fwd}/{rev} shots per CTA: vs reference record {rel(pred, d['pred']):.2e} "
           f"grad {rel(g, d['grad_vp']):.2e} wavelet {rel(gw, d['grad_wavelet']):.2e}; vs f64 oracle "
