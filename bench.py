@@ -410,10 +410,10 @@ class Acoustic3DWorkload:
     kernel = "sweep::a3d reverse step (a3_step + r3_recon + strip kernels)"
     cpu_nt = 16
     # ncu DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of a3_step +
-    # r3_recon for one 256^3 shot (851 + 856 MB), scaled by the shots of a
+    # r3_recon for one 256^3 shot (860 + 856 MB), scaled by the shots of a
     # reverse step: both kernels stream every shot's fields once, so traffic
     # grows with the shots
-    traffic = {"bytes_per_shot": 851e6 + 856e6,
+    traffic = {"bytes_per_shot": 860e6 + 856e6,
                "source": "ncu, a3_step + r3_recon of one 256^3 shot, x shots per step"}
     batch = A3_BATCH
     budget_gb = A3_BUDGET_GB

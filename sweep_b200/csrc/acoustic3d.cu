@@ -52,6 +52,8 @@ struct StripStore {
     int host;                        // the tape is pinned host memory (SWEEP_MEM_HOST_TAPE)
 };
 
+constexpr int kMaxXBlocks = 48;
+
 struct Params {
     int B, nz, ny, nx, nt, nsrc, nrec;
     int P;                                     // x pitch (floats)
@@ -74,6 +76,13 @@ struct Params {
     const float4 *pz, *py, *px;
     const float *cf, *ca, *vv;                 // model fields, pitched (one copy: shared model)
     StripStore st;
+    // x tiling of the forward (0) and adjoint (1) stencil grids: column block
+    // b starts at x = xo[k][b] (a multiple of 4, for the TMA row origin) and
+    // updates only the columns it owns, [xl[k][b], xh[k][b]); the blocks own
+    // [M, nx - M) exactly once, each lies wholly in the CPML x band or wholly
+    // clear of it, so no warp of a clear block takes the band path
+    int nbx[2];
+    short xo[2][kMaxXBlocks], xl[2][kMaxXBlocks], xh[2][kMaxXBlocks];
 };
 
 // ------------------------------------------------------------------ device
@@ -308,12 +317,13 @@ __global__ void __launch_bounds__(NTH, SWEEP_A3D_CTAS) f3_step(const __grid_cons
     extern __shared__ __align__(128) unsigned char smem_raw[];
     F3Smem& sm = *reinterpret_cast<F3Smem*>(smem_raw);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BXC + tx;
-    const int gx0 = blockIdx.x * BXC - M, gy0 = blockIdx.y * BYC - M;
-    const int ix = blockIdx.x * BXC + tx, iy = blockIdx.y * BYC + ty;
+    const int xb = P.xo[0][blockIdx.x];
+    const int gx0 = xb - M, gy0 = blockIdx.y * BYC - M;
+    const int ix = xb + tx, iy = blockIdx.y * BYC + ty;
     const int b = blockIdx.z / P.nzc, zci = blockIdx.z - b * P.nzc;
     const int zb = max(M, zci * P.zc), ze = min(P.nz - M, (zci + 1) * P.zc);
     if (zb >= ze) return;
-    const bool col = ix >= M && ix < P.nx - M && iy >= M && iy < P.ny - M;
+    const bool col = ix >= P.xl[0][blockIdx.x] && ix < P.xh[0][blockIdx.x] && iy >= M && iy < P.ny - M;
     const long long bo = (long long)b * P.S;
     const long long colo = (long long)iy * P.P + ix;
     const int q0 = zb - M, q1 = ze + M;                // stages [q0, q1)
@@ -666,12 +676,13 @@ __global__ void __launch_bounds__(NTH, SWEEP_A3D_CTAS) a3_step(const __grid_cons
     extern __shared__ __align__(128) unsigned char smem_raw[];
     A3Smem& sm = *reinterpret_cast<A3Smem*>(smem_raw);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BXC + tx;
-    const int gx0 = blockIdx.x * BXC - M, gy0 = blockIdx.y * BYC - M;
-    const int ix = blockIdx.x * BXC + tx, iy = blockIdx.y * BYC + ty;
+    const int xb = P.xo[1][blockIdx.x];
+    const int gx0 = xb - M, gy0 = blockIdx.y * BYC - M;
+    const int ix = xb + tx, iy = blockIdx.y * BYC + ty;
     const int b = blockIdx.z / P.nzc, zci = blockIdx.z - b * P.nzc;
     const int zb = max(M, zci * P.zc), ze = min(P.nz - M, (zci + 1) * P.zc);
     if (zb >= ze) return;
-    const bool col = ix >= M && ix < P.nx - M && iy >= M && iy < P.ny - M;
+    const bool col = ix >= P.xl[1][blockIdx.x] && ix < P.xh[1][blockIdx.x] && iy >= M && iy < P.ny - M;
     const long long bo = (long long)b * P.S;
     const long long colo = (long long)iy * P.P + ix;
     const bool inx = ix < P.qx0 || ix >= P.qx1;
@@ -1062,12 +1073,39 @@ static Params make_params(const sweep_acoustic_desc* d)
     P.graph_steps = resolve_graph_steps(sc.graph_steps);
     P.zc = (d->nz + nzc - 1) / nzc;
     P.nzc = (d->nz + P.zc - 1) / P.zc;
+    // x tiling: [M, nx - M) cut at the CPML x band edges (forward: the
+    // product-rule band ex; adjoint: the clear box q), each piece tiled by
+    // 32-column blocks from a 4-aligned origin
+    auto tile = [&](int k, int b0, int b1) {
+        const int lo = M, hi = d->nx - M;
+        b0 = std::min(std::max(b0, lo), hi);
+        b1 = std::min(std::max(b1, b0), hi);
+        const int cut[4] = {lo, b0, b1, hi};
+        int n = 0;
+        for (int sgm = 0; sgm < 3; ++sgm) {
+            const int a = cut[sgm], e = cut[sgm + 1];
+            for (int o = a / 4 * 4; o < e; o += BXC) {
+                SWEEP_REQUIRE(n < kMaxXBlocks, "acoustic3d: nx %d needs more than %d column blocks", d->nx,
+                              kMaxXBlocks);
+                P.xo[k][n] = (short)o;
+                P.xl[k][n] = (short)std::max(o, a);
+                P.xh[k][n] = (short)std::min(o + BXC, e);
+                ++n;
+            }
+        }
+        P.nbx[k] = n;
+    };
+    tile(0, P.ex0, P.ex1);
+    tile(1, P.qx0, P.qx1);
     return P;
 }
 
-static dim3 stencil_grid(const Params& P)
+// kind: 0 the forward step, 1 the adjoint step (their band-aligned x
+// tilings), 2 the reconstruction (plain 32-column blocks)
+static dim3 stencil_grid(const Params& P, int kind = 2)
 {
-    return dim3((P.nx + BXC - 1) / BXC, (P.ny + BYC - 1) / BYC, P.B * P.nzc);
+    const unsigned gx = kind < 2 ? (unsigned)P.nbx[kind] : (unsigned)((P.nx + BXC - 1) / BXC);
+    return dim3(gx, (P.ny + BYC - 1) / BYC, P.B * P.nzc);
 }
 
 struct Work {
@@ -1288,7 +1326,7 @@ static void forward_steps(const sweep_acoustic_desc* d, const Params& P, FwdStat
     const bool scaled = P.st.fmt == SF_F16 || P.st.fmt == SF_I8;
     int qper = 0;
     for (int f = 0; f < 6; ++f) qper += P.st.blocks[f];
-    const dim3 grid = stencil_grid(P), block(BXC, BYC);
+    const dim3 grid = stencil_grid(P, 0), block(BXC, BYC);
     const unsigned gs = blocks_for((long long)P.B * P.nsrc, 128), gr = blocks_for((long long)P.B * P.nrec, 128);
     const unsigned gst = blocks_for((long long)P.B * P.nstrip, 256);
     static bool attr = false;
@@ -1523,7 +1561,7 @@ static void backward_with(const sweep_acoustic_desc* d, int mem_mode, int ckpt_e
         if (grad_w && d->nsrc > 0) SWEEP_CUDA(cudaMemsetAsync(grad_w, 0, (size_t)d->B * d->nsrc * d->nt * 4, st));
     }
     SWEEP_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
-    const dim3 grid = stencil_grid(P), block(BXC, BYC);
+    const dim3 grid = stencil_grid(P), agrid = stencil_grid(P, 1), block(BXC, BYC);
     const unsigned gs = blocks_for((long long)P.B * P.nsrc, 128), gr = blocks_for((long long)P.B * P.nrec, 128);
     const unsigned gst = blocks_for((long long)P.B * P.nstrip, 256);
     int lp = 0, ln = 1, lx = 2, cur = 0;
@@ -1572,7 +1610,7 @@ static void backward_with(const sweep_acoustic_desc* d, int mem_mode, int ckpt_e
             for (int k = 0; k < 6; ++k) { a_in[k] = w.f[3 + 2 * k + cur]; a_out[k] = w.f[3 + 2 * k + 1 - cur]; }
             A3 A{w.f[ln], w.f[lp], w.f[lx], a_in[0], a_in[1], a_in[2], a_in[3], a_in[4], a_in[5],
                  a_out[0], a_out[1], a_out[2], a_out[3], a_out[4], a_out[5]};
-            a3_step<<<grid, block, sizeof(A3Smem), ls>>>(amaps, P, A, ln, lp, w.err);
+            a3_step<<<agrid, block, sizeof(A3Smem), ls>>>(amaps, P, A, ln, lp, w.err);
             SWEEP_LAUNCH_CHECK();
             if (d->nrec > 0)
                 inject3<<<gr, 128, 0, ls>>>(P, w.f[lx], adj, d->rec_loc, d->nrec, it, 1, 1.f, 0);
