@@ -53,6 +53,7 @@ struct StripStore {
 };
 
 constexpr int kMaxXBlocks = 48;
+constexpr int kMaxYBlocks = 160;
 
 struct Params {
     int B, nz, ny, nx, nt, nsrc, nrec;
@@ -83,6 +84,9 @@ struct Params {
     // clear of it, so no warp of a clear block takes the band path
     int nbx[2];
     short xo[2][kMaxXBlocks], xl[2][kMaxXBlocks], xh[2][kMaxXBlocks];
+    // the same along y with 8-row blocks (a row origin needs no alignment)
+    int nby[2];
+    short yo[2][kMaxYBlocks], yl[2][kMaxYBlocks], yh[2][kMaxYBlocks];
 };
 
 // ------------------------------------------------------------------ device
@@ -317,13 +321,14 @@ __global__ void __launch_bounds__(NTH, SWEEP_A3D_CTAS) f3_step(const __grid_cons
     extern __shared__ __align__(128) unsigned char smem_raw[];
     F3Smem& sm = *reinterpret_cast<F3Smem*>(smem_raw);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BXC + tx;
-    const int xb = P.xo[0][blockIdx.x];
-    const int gx0 = xb - M, gy0 = blockIdx.y * BYC - M;
-    const int ix = xb + tx, iy = blockIdx.y * BYC + ty;
+    const int xb = P.xo[0][blockIdx.x], yb = P.yo[0][blockIdx.y];
+    const int gx0 = xb - M, gy0 = yb - M;
+    const int ix = xb + tx, iy = yb + ty;
     const int b = blockIdx.z / P.nzc, zci = blockIdx.z - b * P.nzc;
     const int zb = max(M, zci * P.zc), ze = min(P.nz - M, (zci + 1) * P.zc);
     if (zb >= ze) return;
-    const bool col = ix >= P.xl[0][blockIdx.x] && ix < P.xh[0][blockIdx.x] && iy >= M && iy < P.ny - M;
+    const bool col = ix >= P.xl[0][blockIdx.x] && ix < P.xh[0][blockIdx.x] && iy >= P.yl[0][blockIdx.y] &&
+                     iy < P.yh[0][blockIdx.y];
     const long long bo = (long long)b * P.S;
     const long long colo = (long long)iy * P.P + ix;
     const int q0 = zb - M, q1 = ze + M;                // stages [q0, q1)
@@ -676,13 +681,14 @@ __global__ void __launch_bounds__(NTH, SWEEP_A3D_CTAS) a3_step(const __grid_cons
     extern __shared__ __align__(128) unsigned char smem_raw[];
     A3Smem& sm = *reinterpret_cast<A3Smem*>(smem_raw);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BXC + tx;
-    const int xb = P.xo[1][blockIdx.x];
-    const int gx0 = xb - M, gy0 = blockIdx.y * BYC - M;
-    const int ix = xb + tx, iy = blockIdx.y * BYC + ty;
+    const int xb = P.xo[1][blockIdx.x], yb = P.yo[1][blockIdx.y];
+    const int gx0 = xb - M, gy0 = yb - M;
+    const int ix = xb + tx, iy = yb + ty;
     const int b = blockIdx.z / P.nzc, zci = blockIdx.z - b * P.nzc;
     const int zb = max(M, zci * P.zc), ze = min(P.nz - M, (zci + 1) * P.zc);
     if (zb >= ze) return;
-    const bool col = ix >= P.xl[1][blockIdx.x] && ix < P.xh[1][blockIdx.x] && iy >= M && iy < P.ny - M;
+    const bool col = ix >= P.xl[1][blockIdx.x] && ix < P.xh[1][blockIdx.x] && iy >= P.yl[1][blockIdx.y] &&
+                     iy < P.yh[1][blockIdx.y];
     const long long bo = (long long)b * P.S;
     const long long colo = (long long)iy * P.P + ix;
     const bool inx = ix < P.qx0 || ix >= P.qx1;
@@ -1073,30 +1079,31 @@ static Params make_params(const sweep_acoustic_desc* d)
     P.graph_steps = resolve_graph_steps(sc.graph_steps);
     P.zc = (d->nz + nzc - 1) / nzc;
     P.nzc = (d->nz + P.zc - 1) / P.zc;
-    // x tiling: [M, nx - M) cut at the CPML x band edges (forward: the
-    // product-rule band ex; adjoint: the clear box q), each piece tiled by
-    // 32-column blocks from a 4-aligned origin
-    auto tile = [&](int k, int b0, int b1) {
-        const int lo = M, hi = d->nx - M;
+    // x / y tiling: [M, n - M) cut at the CPML band edges (forward: the
+    // product-rule band ex / ey; adjoint: the clear box q), each piece tiled
+    // by blocks of `w` from an origin rounded down to `align`
+    auto tile = [&](int n_axis, int b0, int b1, int w, int align, int cap, int& nb, short* o_, short* l_, short* h_) {
+        const int lo = M, hi = n_axis - M;
         b0 = std::min(std::max(b0, lo), hi);
         b1 = std::min(std::max(b1, b0), hi);
         const int cut[4] = {lo, b0, b1, hi};
         int n = 0;
         for (int sgm = 0; sgm < 3; ++sgm) {
             const int a = cut[sgm], e = cut[sgm + 1];
-            for (int o = a / 4 * 4; o < e; o += BXC) {
-                SWEEP_REQUIRE(n < kMaxXBlocks, "acoustic3d: nx %d needs more than %d column blocks", d->nx,
-                              kMaxXBlocks);
-                P.xo[k][n] = (short)o;
-                P.xl[k][n] = (short)std::max(o, a);
-                P.xh[k][n] = (short)std::min(o + BXC, e);
+            for (int o = a / align * align; o < e; o += w) {
+                SWEEP_REQUIRE(n < cap, "acoustic3d: an axis of %d cells needs more than %d blocks", n_axis, cap);
+                o_[n] = (short)o;
+                l_[n] = (short)std::max(o, a);
+                h_[n] = (short)std::min(o + w, e);
                 ++n;
             }
         }
-        P.nbx[k] = n;
+        nb = n;
     };
-    tile(0, P.ex0, P.ex1);
-    tile(1, P.qx0, P.qx1);
+    tile(d->nx, P.ex0, P.ex1, BXC, 4, kMaxXBlocks, P.nbx[0], P.xo[0], P.xl[0], P.xh[0]);
+    tile(d->nx, P.qx0, P.qx1, BXC, 4, kMaxXBlocks, P.nbx[1], P.xo[1], P.xl[1], P.xh[1]);
+    tile(d->ny, P.ey0, P.ey1, BYC, 1, kMaxYBlocks, P.nby[0], P.yo[0], P.yl[0], P.yh[0]);
+    tile(d->ny, P.qy0, P.qy1, BYC, 1, kMaxYBlocks, P.nby[1], P.yo[1], P.yl[1], P.yh[1]);
     return P;
 }
 
@@ -1104,8 +1111,8 @@ static Params make_params(const sweep_acoustic_desc* d)
 // tilings), 2 the reconstruction (plain 32-column blocks)
 static dim3 stencil_grid(const Params& P, int kind = 2)
 {
-    const unsigned gx = kind < 2 ? (unsigned)P.nbx[kind] : (unsigned)((P.nx + BXC - 1) / BXC);
-    return dim3(gx, (P.ny + BYC - 1) / BYC, P.B * P.nzc);
+    if (kind < 2) return dim3((unsigned)P.nbx[kind], (unsigned)P.nby[kind], P.B * P.nzc);
+    return dim3((P.nx + BXC - 1) / BXC, (P.ny + BYC - 1) / BYC, P.B * P.nzc);
 }
 
 struct Work {
