@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define SWEEP_B200_ABI_VERSION 3
+#define SWEEP_B200_ABI_VERSION 4
 
 #if defined(__GNUC__)
 #define SWEEP_B200_API __attribute__((visibility("default")))
@@ -245,6 +245,8 @@ typedef struct sweep_b200_schedule {
     int32_t graph_steps;  /* time steps per captured CUDA graph in the step loops
                            * (0: plain stream launches; < 0: built-in); host-tape
                            * loops always use plain launches */
+    int32_t tile_y;       /* 3-D acoustic: rows of the 32-column block a CTA of the
+                           * stencil kernels covers, 8 or 16 (0 = built-in 8) */
 } sweep_b200_schedule;
 
 #define SWEEP_FAMILY_ACOUSTIC 0   /* desc is a sweep_acoustic_desc (2-D or 3-D) */

@@ -17,7 +17,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIB_PATH = Path(os.environ.get("SWEEP_B200_LIB", HERE / "libsweep_b200.so"))
-ABI_VERSION = 3
+ABI_VERSION = 4
 ERR_CAP = 4096
 
 c_i32, c_i64, c_f32, c_p = ctypes.c_int32, ctypes.c_int64, ctypes.c_float, ctypes.c_void_p
@@ -96,7 +96,8 @@ class ElasticDesc(ctypes.Structure):
 
 class Schedule(ctypes.Structure):
     """Mirror of ``sweep_b200_schedule``."""
-    _fields_ = [("shots_fwd", c_i32), ("shots_rev", c_i32), ("z_chunks", c_i32), ("graph_steps", c_i32)]
+    _fields_ = [("shots_fwd", c_i32), ("shots_rev", c_i32), ("z_chunks", c_i32), ("graph_steps", c_i32),
+                ("tile_y", c_i32)]
 
 
 _lib = None

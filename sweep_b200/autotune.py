@@ -14,11 +14,14 @@ launch choices the core leaves open for one problem shape:
 * ``z_chunks`` -- z chunks each column block of the 3-D stencil kernels is cut
   into (the grid depth per shot, 3-D acoustic);
 * ``graph_steps`` -- time steps per captured CUDA graph in the step loops
-  (0: plain stream launches).
+  (0: plain stream launches);
+* ``tile_y`` -- 3-D acoustic: rows of the 32-column block each CTA of the
+  stencil kernels covers, 8 (256 threads, 4 CTAs per SM) or 16 (512 threads,
+  2 CTAs per SM, less halo per cell).
 
-The tile shapes are compile-time constants of the kernels (they fix the
-shared-memory staging and register blocking), and there is no temporal
-blocking to choose: every step is one pass over HBM.
+The 2-D and elastic tile shapes are compile-time constants of the kernels
+(they fix the shared-memory staging and register blocking), and there is no
+temporal blocking to choose: every step is one pass over HBM.
 
 :func:`tune` times the real forward and backward calls of one shape over a
 truncated time axis, one knob at a time from the built-in defaults
@@ -36,8 +39,8 @@ import torch
 
 from . import _lib
 
-FIELDS = ("shots_fwd", "shots_rev", "z_chunks", "graph_steps")
-BUILTIN = {"shots_fwd": 0, "shots_rev": 0, "z_chunks": 0, "graph_steps": -1}
+FIELDS = ("shots_fwd", "shots_rev", "z_chunks", "graph_steps", "tile_y")
+BUILTIN = {"shots_fwd": 0, "shots_rev": 0, "z_chunks": 0, "graph_steps": -1, "tile_y": 0}
 
 _tuned: dict = {}
 
@@ -99,6 +102,8 @@ def _candidates(desc, builtin: dict, mem_mode: int, nt_tune: int) -> list:
             knobs.append(("shots_fwd", sorted({g for g in (1, 2, 4, 8) if g <= B} | {builtin["shots_fwd"]}), True))
             knobs.append(("shots_rev", sorted({g for g in (2, 4, 8, 16) if g <= B} | {builtin["shots_rev"]}), False))
     else:
+        # the tile height first: the z-chunk count the core picks depends on it
+        knobs.append(("tile_y", [8, 16], False))
         z = builtin["z_chunks"]
         knobs.append(("z_chunks", sorted({max(1, z // 2), z, min(_zmax(desc), 2 * z)}), False))
     if not mem_mode & _lib.MEM_HOST_TAPE:
@@ -175,6 +180,11 @@ def tune(prop, geo, padded, wavelet, fields, mem_mode: int, ckpt_every: int,
     trials = {}
     try:
         for knob, values, forward_only in _candidates(desc, builtin, mem_mode, nt_tune):
+            if knob == "z_chunks":
+                # around the count the core picks for the tile height chosen so far
+                set_schedule(desc, current)
+                z = get_schedule(desc)["z_chunks"]
+                values = sorted({max(1, z // 2), z, min(_zmax(desc), 2 * z)})
             res = {}
             run = fwd if forward_only else fwd_bwd
             for v in values:

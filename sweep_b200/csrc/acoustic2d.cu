@@ -1464,6 +1464,7 @@ void schedule_of(const sweep_acoustic_desc* d, sweep_b200_schedule* out)
     out->shots_rev = pl.Gr;
     out->z_chunks = 0;
     out->graph_steps = pl.graph_steps;
+    out->tile_y = 0;
 }
 
 int64_t forward_only_bytes(const sweep_acoustic_desc* d)

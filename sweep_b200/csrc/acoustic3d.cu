@@ -29,10 +29,31 @@ namespace sweep {
 namespace a3d {
 
 constexpr int M = 4;
-constexpr int BXC = 32, BYC = 8;               // columns per CTA
-constexpr int PW = BXC + 2 * M, PH = BYC + 2 * M;
-constexpr int PN = PW * PH;                    // staged plane, floats
-constexpr int NTH = BXC * BYC;
+// Ring depths and CTAs per SM of the three stencil kernels: build-time knobs
+// (the shared-memory ring and the L1 share the same on-chip memory).
+#ifndef SWEEP_A3D_FWD_STAGES
+#define SWEEP_A3D_FWD_STAGES 11
+#endif
+#ifndef SWEEP_A3D_ADJ_STAGES
+#define SWEEP_A3D_ADJ_STAGES 8
+#endif
+#ifndef SWEEP_A3D_REC_STAGES
+#define SWEEP_A3D_REC_STAGES 9
+#endif
+#ifndef SWEEP_A3D_CTAS
+#define SWEEP_A3D_CTAS 4
+#endif
+constexpr int BXC = 32;                        // columns per CTA along x
+constexpr int PW = BXC + 2 * M;                // staged plane width, floats
+// A CTA covers BXC x BY columns; BY (8 or 16) is the schedule's tile height.
+template <int BY>
+struct TileY {
+    static constexpr int PH = BY + 2 * M;      // staged plane height
+    static constexpr int PN = PW * PH;         // staged plane, floats
+    static constexpr int NT = BXC * BY;        // threads per CTA
+    static constexpr int CN = BXC * BY;        // centre tile, floats
+    static constexpr int CTAS = SWEEP_A3D_CTAS * 8 / BY;   // CTAs per SM
+};
 
 // Boundary-strip storage of the boundary-saving tape.  fp32 and bf16 keep the
 // strip set (each cell once, strip_coord order); fp16 and int8 keep the
@@ -60,6 +81,7 @@ struct Params {
     int P;                                     // x pitch (floats)
     long long SP, S;                           // plane stride, shot stride
     int zc, nzc;                               // z chunk length, chunks
+    int rows;                                  // rows of a stencil CTA (tile height: 8 or 16)
     int graph_steps;                           // host only: time steps per captured CUDA graph
     float dt, dz, dy, dx;
     float ih2z, ih2y, ih2x;                    // 1 / h^2 per axis
@@ -234,36 +256,6 @@ __device__ __forceinline__ bool in_recon(const Params& P, int iz, int iy, int ix
     return iz >= P.qz0 && iz < P.qz1 && iy >= P.qy0 && iy < P.qy1 && ix >= P.qx0 && ix < P.qx1;
 }
 
-// Load plane iz of field f (one shot) with its x / y halo into registers
-// (staging for the plane that the next iteration will use).
-struct PlaneLoader {
-    static constexpr int PER = (PN + NTH - 1) / NTH;
-    float v[PER];
-    __device__ __forceinline__ void load(const float* __restrict__ f, const Params& P, int iz, int gy0, int gx0, int tid)
-    {
-#pragma unroll
-        for (int j = 0; j < PER; ++j) {
-            const int e = tid + j * NTH;
-            float x = 0.f;
-            if (e < PN) {
-                const int r = e / PW, c = e - r * PW;
-                const int gy = gy0 + r, gx = gx0 + c;
-                if (gy >= 0 && gy < P.ny && gx >= 0 && gx < P.nx)
-                    x = __ldg(f + iz * P.SP + (long long)gy * P.P + gx);
-            }
-            v[j] = x;
-        }
-    }
-    __device__ __forceinline__ void store(float* dst, int tid)
-    {
-#pragma unroll
-        for (int j = 0; j < PER; ++j) {
-            const int e = tid + j * NTH;
-            if (e < PN) dst[e] = v[j];
-        }
-    }
-};
-
 // ----------------------------------------------------------- forward step
 struct F3 {
     const float* u_now; const float* u_prev; float* u_next;
@@ -279,27 +271,13 @@ struct F3 {
 // stage z + M into the queue, so stages z .. z + M must have landed; with NF3
 // stages the loads run NF3 - M - 1 planes ahead of the compute, TMA-issued by
 // one thread on one mbarrier per stage.
-// Ring depths and CTAs per SM of the three stencil kernels: build-time knobs
-// (the shared-memory ring and the L1 share the same on-chip memory).
-#ifndef SWEEP_A3D_FWD_STAGES
-#define SWEEP_A3D_FWD_STAGES 11
-#endif
-#ifndef SWEEP_A3D_ADJ_STAGES
-#define SWEEP_A3D_ADJ_STAGES 8
-#endif
-#ifndef SWEEP_A3D_REC_STAGES
-#define SWEEP_A3D_REC_STAGES 9
-#endif
-#ifndef SWEEP_A3D_CTAS
-#define SWEEP_A3D_CTAS 4
-#endif
 constexpr int NF3 = SWEEP_A3D_FWD_STAGES;
 static_assert(NF3 >= 2 * M + 1, "the forward ring must hold the first plane's z-taps and one more stage");
-constexpr int CN3 = BXC * BYC;
+template <int BY>
 struct F3Smem {
-    float u[NF3][PN];
-    float up[NF3][CN3];
-    float cf[NF3][CN3];
+    float u[NF3][TileY<BY>::PN];
+    float up[NF3][TileY<BY>::CN];
+    float cf[NF3][TileY<BY>::CN];
     uint64_t bar[NF3];
 };
 
@@ -315,11 +293,13 @@ enum { ERR_WAIT_F3 = 1 };
 // The CPML branch of an axis runs on its band plus one cell (reference
 // forward_split.cu:150-156) and uses the product-rule split
 // tmp = (((1 + b) Lap + db du) + a dpsi) + da psi (forward_split.cu:171-172).
-__global__ void __launch_bounds__(NTH, SWEEP_A3D_CTAS) f3_step(const __grid_constant__ F3Maps MP, const Params P, const F3 F,
-                                                  const int uin, const int uprev, int* err)
+template <int BY>
+__global__ void __launch_bounds__(TileY<BY>::NT, TileY<BY>::CTAS)
+    f3_step(const __grid_constant__ F3Maps MP, const Params P, const F3 F, const int uin, const int uprev, int* err)
 {
+    constexpr int PN = TileY<BY>::PN, CN3 = TileY<BY>::CN;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    F3Smem& sm = *reinterpret_cast<F3Smem*>(smem_raw);
+    F3Smem<BY>& sm = *reinterpret_cast<F3Smem<BY>*>(smem_raw);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BXC + tx;
     const int xb = P.xo[0][blockIdx.x], yb = P.yo[0][blockIdx.y];
     const int gx0 = xb - M, gy0 = yb - M;
@@ -657,11 +637,12 @@ __device__ __forceinline__ void adj_axis(const Params& P, const float4* __restri
 constexpr int NA3 = SWEEP_A3D_ADJ_STAGES;
 static_assert(NA3 >= 2 * M, "the adjoint ring must hold the 2M stages of the first plane's z-queue");
 
+template <int BY>
 struct A3Smem {
-    float l[NA3][PN];
-    float c[NA3][PN];
-    float lp[NA3][CN3];
-    float gw[2][PN];
+    float l[NA3][TileY<BY>::PN];
+    float c[NA3][TileY<BY>::PN];
+    float lp[NA3][TileY<BY>::CN];
+    float gw[2][TileY<BY>::PN];
     uint64_t bar[NA3];
 };
 
@@ -675,11 +656,13 @@ struct A3Maps {
 // pure interior  2 l - l_prev + Lap(gw) (difference form around gw);
 // shell          per axis outside the clear box the transposed CPML terms,
 //                inside it the bare Laplacian of gw.
-__global__ void __launch_bounds__(NTH, SWEEP_A3D_CTAS) a3_step(const __grid_constant__ A3Maps MP, const Params P, const A3 A,
-                                                  const int lnow, const int lprev, int* err)
+template <int BY>
+__global__ void __launch_bounds__(TileY<BY>::NT, TileY<BY>::CTAS)
+    a3_step(const __grid_constant__ A3Maps MP, const Params P, const A3 A, const int lnow, const int lprev, int* err)
 {
+    constexpr int PN = TileY<BY>::PN, CN3 = TileY<BY>::CN, NTH = TileY<BY>::NT;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    A3Smem& sm = *reinterpret_cast<A3Smem*>(smem_raw);
+    A3Smem<BY>& sm = *reinterpret_cast<A3Smem<BY>*>(smem_raw);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BXC + tx;
     const int xb = P.xo[1][blockIdx.x], yb = P.yo[1][blockIdx.y];
     const int gx0 = xb - M, gy0 = yb - M;
@@ -839,9 +822,10 @@ struct R3 {
 constexpr int NR3 = SWEEP_A3D_REC_STAGES;
 static_assert(NR3 >= 2 * M + 1, "the reconstruction ring must hold the first plane's z-taps and one more stage");
 constexpr int NRC3 = NR3 - M;
+template <int BY>
 struct R3Smem {
-    float u[NR3][PN];
-    float c[NRC3][6][CN3];
+    float u[NR3][TileY<BY>::PN];
+    float c[NRC3][6][TileY<BY>::CN];
     uint64_t bar[NR3];
 };
 
@@ -856,14 +840,17 @@ struct R3Maps {
 // u(it-1) = 2 u(it) - u(it+1) + vp^2 dt^2 Lap u(it) on the reconstruction box
 // (the physical box minus the restored strips) with the fused vp image
 // 2 dt^2 u_tt lambda(it) / vp (reference forward_split.cu:292-372).
-__global__ void __launch_bounds__(NTH, SWEEP_A3D_CTAS) r3_recon(const __grid_constant__ R3Maps MP, const Params P, const R3 R,
-                                                   const int rnow, const int rprev, const int lnow, int* err)
+template <int BY>
+__global__ void __launch_bounds__(TileY<BY>::NT, TileY<BY>::CTAS)
+    r3_recon(const __grid_constant__ R3Maps MP, const Params P, const R3 R, const int rnow, const int rprev,
+             const int lnow, int* err)
 {
+    constexpr int PN = TileY<BY>::PN, CN3 = TileY<BY>::CN;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    R3Smem& sm = *reinterpret_cast<R3Smem*>(smem_raw);
+    R3Smem<BY>& sm = *reinterpret_cast<R3Smem<BY>*>(smem_raw);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BXC + tx;
-    const int gx0 = blockIdx.x * BXC - M, gy0 = blockIdx.y * BYC - M;
-    const int ix = blockIdx.x * BXC + tx, iy = blockIdx.y * BYC + ty;
+    const int gx0 = blockIdx.x * BXC - M, gy0 = blockIdx.y * BY - M;
+    const int ix = blockIdx.x * BXC + tx, iy = blockIdx.y * BY + ty;
     const int b = blockIdx.z / P.nzc, zci = blockIdx.z - b * P.nzc;
     const int zb = max(P.qz0, zci * P.zc), ze = min(P.qz1, (zci + 1) * P.zc);
     if (zb >= ze) return;
@@ -1072,8 +1059,9 @@ static Params make_params(const sweep_acoustic_desc* d)
     // across the SMs: measured on the 256^3 survey, 4-shot calls, 1 / 2 / 4
     // chunks per column took 96.7 / 86.7 / 83.2 ms for 16 steps), chunks of
     // at least 16 planes -- or the shape's recorded schedule value
-    const long long cols = (long long)((d->nx + BXC - 1) / BXC) * ((d->ny + BYC - 1) / BYC) * d->B;
     const sweep_b200_schedule sc = recorded_schedule(d);
+    P.rows = sc.tile_y == 16 ? 16 : 8;
+    const long long cols = (long long)((d->nx + BXC - 1) / BXC) * ((d->ny + P.rows - 1) / P.rows) * d->B;
     int nzc = sc.z_chunks >= 1 ? sc.z_chunks : (int)std::max(1LL, (8LL * 4 * 148 + cols - 1) / cols);
     nzc = std::max(1, std::min(nzc, d->nz / 16));
     P.graph_steps = resolve_graph_steps(sc.graph_steps);
@@ -1102,8 +1090,8 @@ static Params make_params(const sweep_acoustic_desc* d)
     };
     tile(d->nx, P.ex0, P.ex1, BXC, 4, kMaxXBlocks, P.nbx[0], P.xo[0], P.xl[0], P.xh[0]);
     tile(d->nx, P.qx0, P.qx1, BXC, 4, kMaxXBlocks, P.nbx[1], P.xo[1], P.xl[1], P.xh[1]);
-    tile(d->ny, P.ey0, P.ey1, BYC, 1, kMaxYBlocks, P.nby[0], P.yo[0], P.yl[0], P.yh[0]);
-    tile(d->ny, P.qy0, P.qy1, BYC, 1, kMaxYBlocks, P.nby[1], P.yo[1], P.yl[1], P.yh[1]);
+    tile(d->ny, P.ey0, P.ey1, P.rows, 1, kMaxYBlocks, P.nby[0], P.yo[0], P.yl[0], P.yh[0]);
+    tile(d->ny, P.qy0, P.qy1, P.rows, 1, kMaxYBlocks, P.nby[1], P.yo[1], P.yl[1], P.yh[1]);
     return P;
 }
 
@@ -1112,7 +1100,7 @@ static Params make_params(const sweep_acoustic_desc* d)
 static dim3 stencil_grid(const Params& P, int kind = 2)
 {
     if (kind < 2) return dim3((unsigned)P.nbx[kind], (unsigned)P.nby[kind], P.B * P.nzc);
-    return dim3((P.nx + BXC - 1) / BXC, (P.ny + BYC - 1) / BYC, P.B * P.nzc);
+    return dim3((P.nx + BXC - 1) / BXC, (P.ny + P.rows - 1) / P.rows, P.B * P.nzc);
 }
 
 struct Work {
@@ -1161,7 +1149,7 @@ static void check_err(const Work& w, cudaStream_t st, const char* what)
 // 4-D (x, y, z, shot) map of a wavefield buffer, or 3-D (x, y, z) of the model.
 static CUtensorMap plane_map(const float* base, const Params& P, int nb, bool halo)
 {
-    const uint32_t bx = halo ? PW : BXC, by = halo ? PH : BYC;
+    const uint32_t bx = halo ? PW : BXC, by = halo ? P.rows + 2 * M : P.rows;
     if (nb == 0) {
         const uint64_t dims[3] = {(uint64_t)P.nx, (uint64_t)P.ny, (uint64_t)P.nz};
         const uint64_t strides[2] = {(uint64_t)P.P, (uint64_t)P.SP};
@@ -1267,6 +1255,7 @@ void schedule_of(const sweep_acoustic_desc* d, sweep_b200_schedule* out)
     out->shots_rev = 0;
     out->z_chunks = P.nzc;
     out->graph_steps = P.graph_steps;
+    out->tile_y = P.rows;
 }
 
 void sizes(const sweep_acoustic_desc* d, int mem_mode, int ckpt_every, int64_t* ws, int64_t* tape)
@@ -1323,6 +1312,58 @@ struct FwdState {
     float* zeta(int a) const { return f[9 + a]; }
 };
 
+// The three stencil kernels at the plan's tile height, their shared memory
+// opted in once per instantiation.
+template <int BY>
+static void set_stencil_attrs()
+{
+    static bool done = false;
+    if (done) return;
+    SWEEP_CUDA(cudaFuncSetAttribute(f3_step<BY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(F3Smem<BY>)));
+    SWEEP_CUDA(cudaFuncSetAttribute(a3_step<BY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(A3Smem<BY>)));
+    SWEEP_CUDA(cudaFuncSetAttribute(r3_recon<BY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)sizeof(R3Smem<BY>)));
+    done = true;
+}
+
+static void launch_f3(const Params& P, const F3Maps& maps, const F3& F, int uin, int uprev, int* err, cudaStream_t st)
+{
+    const dim3 grid = stencil_grid(P, 0), block(BXC, P.rows);
+    if (P.rows == 16) {
+        set_stencil_attrs<16>();
+        f3_step<16><<<grid, block, sizeof(F3Smem<16>), st>>>(maps, P, F, uin, uprev, err);
+    } else {
+        set_stencil_attrs<8>();
+        f3_step<8><<<grid, block, sizeof(F3Smem<8>), st>>>(maps, P, F, uin, uprev, err);
+    }
+}
+
+static void launch_a3(const Params& P, const A3Maps& maps, const A3& A, int lnow, int lprev, int* err,
+                      cudaStream_t st)
+{
+    const dim3 grid = stencil_grid(P, 1), block(BXC, P.rows);
+    if (P.rows == 16) {
+        set_stencil_attrs<16>();
+        a3_step<16><<<grid, block, sizeof(A3Smem<16>), st>>>(maps, P, A, lnow, lprev, err);
+    } else {
+        set_stencil_attrs<8>();
+        a3_step<8><<<grid, block, sizeof(A3Smem<8>), st>>>(maps, P, A, lnow, lprev, err);
+    }
+}
+
+static void launch_r3(const Params& P, const R3Maps& maps, const R3& R, int rnow, int rprev, int lnow, int* err,
+                      cudaStream_t st)
+{
+    const dim3 grid = stencil_grid(P, 2), block(BXC, P.rows);
+    if (P.rows == 16) {
+        set_stencil_attrs<16>();
+        r3_recon<16><<<grid, block, sizeof(R3Smem<16>), st>>>(maps, P, R, rnow, rprev, lnow, err);
+    } else {
+        set_stencil_attrs<8>();
+        r3_recon<8><<<grid, block, sizeof(R3Smem<8>), st>>>(maps, P, R, rnow, rprev, lnow, err);
+    }
+}
+
 // Forward steps [it0, it1): stencil, strips of U[it] (strips_of(it), null:
 // none), source injection, receiver gather (record may be null).
 template <class StripsOf>
@@ -1333,14 +1374,8 @@ static void forward_steps(const sweep_acoustic_desc* d, const Params& P, FwdStat
     const bool scaled = P.st.fmt == SF_F16 || P.st.fmt == SF_I8;
     int qper = 0;
     for (int f = 0; f < 6; ++f) qper += P.st.blocks[f];
-    const dim3 grid = stencil_grid(P, 0), block(BXC, BYC);
     const unsigned gs = blocks_for((long long)P.B * P.nsrc, 128), gr = blocks_for((long long)P.B * P.nrec, 128);
     const unsigned gst = blocks_for((long long)P.B * P.nstrip, 256);
-    static bool attr = false;
-    if (!attr) {
-        SWEEP_CUDA(cudaFuncSetAttribute(f3_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(F3Smem)));
-        attr = true;
-    }
     F3Maps maps;
     for (int k = 0; k < 3; ++k) {
         maps.uh[k] = plane_map(S.f[k], P, P.B, true);
@@ -1352,7 +1387,7 @@ static void forward_steps(const sweep_acoustic_desc* d, const Params& P, FwdStat
         F3 F{S.f[S.in], S.f[S.ip], S.f[S.ix], S.ps[0], S.ps[1], S.ps[2], S.psn[0], S.psn[1], S.psn[2],
              S.zeta(0), S.zeta(1), S.zeta(2)};
         const cudaStream_t ls = sg.stream();
-        f3_step<<<grid, block, sizeof(F3Smem), ls>>>(maps, P, F, S.in, S.ip, err);
+        launch_f3(P, maps, F, S.in, S.ip, err, ls);
         SWEEP_LAUNCH_CHECK();
         void* slot = strips_of(it);
         if (slot && P.nstrip > 0) {
@@ -1568,7 +1603,6 @@ static void backward_with(const sweep_acoustic_desc* d, int mem_mode, int ckpt_e
         if (grad_w && d->nsrc > 0) SWEEP_CUDA(cudaMemsetAsync(grad_w, 0, (size_t)d->B * d->nsrc * d->nt * 4, st));
     }
     SWEEP_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
-    const dim3 grid = stencil_grid(P), agrid = stencil_grid(P, 1), block(BXC, BYC);
     const unsigned gs = blocks_for((long long)P.B * P.nsrc, 128), gr = blocks_for((long long)P.B * P.nrec, 128);
     const unsigned gst = blocks_for((long long)P.B * P.nstrip, 256);
     int lp = 0, ln = 1, lx = 2, cur = 0;
@@ -1581,12 +1615,6 @@ static void backward_with(const sweep_acoustic_desc* d, int mem_mode, int ckpt_e
     float* gcomp = w.f[19];
     float* is = illum ? w.f[20] : nullptr;
     float* ir = illum ? w.f[21] : nullptr;
-    static bool attr = false;
-    if (!attr) {
-        SWEEP_CUDA(cudaFuncSetAttribute(r3_recon, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(R3Smem)));
-        SWEEP_CUDA(cudaFuncSetAttribute(a3_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(A3Smem)));
-        attr = true;
-    }
     A3Maps amaps;
     for (int k = 0; k < 3; ++k) {
         amaps.lh[k] = plane_map(w.f[k], P, P.B, true);
@@ -1617,7 +1645,7 @@ static void backward_with(const sweep_acoustic_desc* d, int mem_mode, int ckpt_e
             for (int k = 0; k < 6; ++k) { a_in[k] = w.f[3 + 2 * k + cur]; a_out[k] = w.f[3 + 2 * k + 1 - cur]; }
             A3 A{w.f[ln], w.f[lp], w.f[lx], a_in[0], a_in[1], a_in[2], a_in[3], a_in[4], a_in[5],
                  a_out[0], a_out[1], a_out[2], a_out[3], a_out[4], a_out[5]};
-            a3_step<<<agrid, block, sizeof(A3Smem), ls>>>(amaps, P, A, ln, lp, w.err);
+            launch_a3(P, amaps, A, ln, lp, w.err, ls);
             SWEEP_LAUNCH_CHECK();
             if (d->nrec > 0)
                 inject3<<<gr, 128, 0, ls>>>(P, w.f[lx], adj, d->rec_loc, d->nrec, it, 1, 1.f, 0);
@@ -1627,7 +1655,7 @@ static void backward_with(const sweep_acoustic_desc* d, int mem_mode, int ckpt_e
                 gather3<<<gs, 128, 0, ls>>>(P, w.f[ln], grad_w, d->src_loc, d->nsrc, it, 0);
             if (it > 0) {
                 R3 R{w.f[rn], w.f[rp], w.f[rx], w.f[ln], gacc, gcomp, is, ir};
-                r3_recon<<<grid, block, sizeof(R3Smem), ls>>>(rmaps, P, R, rn - 15, rp - 15, ln, w.err);
+                launch_r3(P, rmaps, R, rn - 15, rp - 15, ln, w.err, ls);
                 if (P.nstrip > 0) {
                     if (host) hr.before_read(it - 1);
                     strips3<<<gst, 256, 0, ls>>>(P, w.f[rx], strips_of(it - 1), nullptr, 1);

@@ -1562,6 +1562,7 @@ void schedule_of(const sweep_elastic_desc* d, sweep_b200_schedule* out)
     out->shots_rev = pl.gshots;
     out->z_chunks = 0;
     out->graph_steps = pl.graph_steps;
+    out->tile_y = 0;
 }
 
 void sizes(const sweep_elastic_desc* d, int mem_mode, int ckpt_every, int64_t* ws, int64_t* tape)

@@ -82,6 +82,8 @@ static void check_schedule(const sweep_b200_schedule* s)
     SWEEP_REQUIRE(s->shots_rev >= 0 && s->shots_rev <= 16, "schedule: shots_rev must be 0..16 (got %d)", s->shots_rev);
     SWEEP_REQUIRE(s->z_chunks >= 0 && s->z_chunks <= 64, "schedule: z_chunks must be 0..64 (got %d)", s->z_chunks);
     SWEEP_REQUIRE(s->graph_steps <= 4096, "schedule: graph_steps must be <= 4096 (got %d)", s->graph_steps);
+    SWEEP_REQUIRE(s->tile_y == 0 || s->tile_y == 8 || s->tile_y == 16,
+                  "schedule: tile_y must be 0 (built-in), 8 or 16 (got %d)", s->tile_y);
 }
 
 extern "C" int sweep_b200_schedule_set(int32_t family, const void* desc, const sweep_b200_schedule* s,

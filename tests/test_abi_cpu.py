@@ -236,6 +236,11 @@ def test_schedule_table_is_host_only_and_keyed_by_shape():
             d3.pad[i] = 5
         autotune.set_schedule(d3, {"z_chunks": 2})
         assert autotune.get_schedule(d3)["z_chunks"] == 2
+        assert autotune.get_schedule(d3)["tile_y"] == 8       # the built-in tile height
+        autotune.set_schedule(d3, {"z_chunks": 2, "tile_y": 16})
+        assert autotune.get_schedule(d3)["tile_y"] == 16
+        with pytest.raises(RuntimeError, match="tile_y"):
+            autotune.set_schedule(d3, {"tile_y": 12})
         e = _lib.ElasticDesc()
         e.B, e.nz, e.nx, e.nt, e.M = 6, 80, 90, 10, 4
         for i in range(4):
@@ -292,6 +297,9 @@ def test_autotune_candidates_follow_the_shape():
     knobs3 = {k: v for k, v, _ in autotune._candidates(d3, dict(base, z_chunks=2), _lib.MEM_BOUNDARY, 16)}
     assert knobs3["z_chunks"] == [1, 2, 4] and autotune._zmax(d3) == 4
     assert knobs3["graph_steps"] == [0, 4]
+    assert knobs3["tile_y"] == [8, 16]
+    order = [k for k, _, _ in autotune._candidates(d3, dict(base, z_chunks=2), _lib.MEM_BOUNDARY, 16)]
+    assert order.index("tile_y") < order.index("z_chunks")
 
 
 def test_tape_budget_rule_is_host_side():

@@ -96,6 +96,25 @@ def test_acoustic3d_clean_ctas_match_reference(z_chunks, clean_oracle):
     assert rel(gw, gw64) < GRAD_TOL
 
 
+@pytest.mark.parametrize("z_chunks", [1, 3])
+def test_acoustic3d_tile_height_changes_nothing(z_chunks):
+    """16-row column blocks (512-thread CTAs) compute every cell with the same
+    taps in the same order as 8-row ones: records and gradients bit-identical,
+    and within the bars of the reference."""
+    d = load("acoustic3d_clean")
+    runs = {}
+    for ty in (8, 16):
+        s = _acoustic(d, schedule={"z_chunks": z_chunks, "tile_y": ty})
+        runs[ty] = _acoustic_grad(s, d)
+        got = s.launch_schedule(d["wavelet"].shape[-1], d["src"], d["rec"],
+                                [torch.tensor(d["vp_init"], device=DEV)])
+        assert got["tile_y"] == ty
+    for a, b in zip(runs[8], runs[16]):
+        assert np.array_equal(a, b)
+    assert rel(runs[16][0], d["pred"]) < REC_TOL
+    assert rel(runs[16][1], d["grad_vp"]) < GRAD_TOL
+
+
 def test_acoustic3d_z_chunking_changes_nothing_but_rounding():
     d = load("acoustic3d_clean")
     runs = [_acoustic_grad(_acoustic(d, schedule={"z_chunks": k}), d) for k in (1, 5)]
