@@ -98,6 +98,7 @@ struct Params {
     // centred derivative grad_p(a + i) on [M, n - M), 0 outside
     const float4 *pz, *py, *px;
     const float *cf, *ca, *vv;                 // model fields, pitched (one copy: shared model)
+    const int* soff;                           // strip cell -> its offset in a shot's field (strip_coord, tabled)
     StripStore st;
     // x tiling of the forward (0) and adjoint (1) stencil grids: column block
     // b starts at x = xo[k][b] (a multiple of 4, for the TMA row origin) and
@@ -480,9 +481,8 @@ __global__ void strips3(const Params P, float* __restrict__ u, void* slot, float
     const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (e >= (long long)P.B * P.nstrip) return;
     const int b = (int)(e / P.nstrip);
-    int iz, iy, ix;
-    strip_coord(P, e - (long long)b * P.nstrip, iz, iy, ix);
-    float* c = u + (long long)b * P.S + (long long)iz * P.SP + (long long)iy * P.P + ix;
+    const long long sidx = e - (long long)b * P.nstrip;
+    float* c = u + (long long)b * P.S + __ldg(P.soff + sidx);
     const StripStore& S = P.st;
     if (!restore) {
         if (S.fmt == SF_F32) static_cast<float*>(slot)[e] = *c;
@@ -492,7 +492,8 @@ __global__ void strips3(const Params P, float* __restrict__ u, void* slot, float
     }
     if (S.fmt == SF_F32) { *c = static_cast<const float*>(slot)[e]; return; }
     if (S.fmt == SF_BF16) { *c = __bfloat162float(static_cast<const __nv_bfloat16*>(slot)[e]); return; }
-    int f;
+    int iz, iy, ix, f;
+    strip_coord(P, sidx, iz, iy, ix);
     const long long i = face_index3(P, iz, iy, ix, f);
     const char* base = static_cast<const char*>(slot);
     const float scale = reinterpret_cast<const float*>(base + S.scl[f])[(long long)b * S.blocks[f] + i / kQB];
@@ -570,9 +571,7 @@ __global__ void strip_image3(const Params P, const Img I)
     const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (e >= (long long)P.B * P.nstrip) return;
     const int b = (int)(e / P.nstrip);
-    int iz, iy, ix;
-    strip_coord(P, e - (long long)b * P.nstrip, iz, iy, ix);
-    const long long c = (long long)iz * P.SP + (long long)iy * P.P + ix;
+    const long long c = __ldg(P.soff + (e - (long long)b * P.nstrip));
     const long long o = (long long)b * P.S + c;
     const float dt2 = P.dt * P.dt;
     const float utt = (I.r_next[o] - 2 * I.r_now[o] + I.r_prev[o]) / dt2;
@@ -956,6 +955,18 @@ __global__ void illum_tail3(const Params P, const float* __restrict__ lam, float
     }
 }
 
+// strip cell s -> offset of (iz, iy, ix) in a shot's pitched field, once per
+// call: the strip kernels of every step read it instead of decoding strip_coord
+__global__ void strip_table3(const Params P, int* __restrict__ soff)
+{
+    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < P.nstrip;
+         s += (long long)gridDim.x * blockDim.x) {
+        int iz, iy, ix;
+        strip_coord(P, s, iz, iy, ix);
+        soff[s] = (int)((long long)iz * P.SP + (long long)iy * P.P + ix);
+    }
+}
+
 // model fields, pitched: cf = ((v*v)*dt)*dt, ca = (v*v)*(dt*dt), vv = v
 // {a, b, d b, d a} per index of one axis (d a: grad_p of the a profile on
 // [M, n - M), as the stencil kernels computed it in place before).
@@ -1025,6 +1036,8 @@ static Params make_params(const sweep_acoustic_desc* d)
     P.P = (d->nx + 31) / 32 * 32;
     P.SP = (long long)d->ny * P.P;
     P.S = (long long)d->nz * P.SP;
+    SWEEP_REQUIRE(P.S < (1LL << 31), "acoustic3d: a shot's field of %lld cells exceeds the 2^31 offsets of the strip "
+                  "table", P.S);
     P.dt = d->dt; P.dz = d->dz; P.dy = d->dy; P.dx = d->dx;
     P.ih2z = 1.0f / (d->dz * d->dz); P.ih2y = 1.0f / (d->dy * d->dy); P.ih2x = 1.0f / (d->dx * d->dx);
     P.ihz = 1.0f / d->dz; P.ihy = 1.0f / d->dy; P.ihx = 1.0f / d->dx;
@@ -1110,6 +1123,7 @@ struct Work {
     float* scratch;                  // one step's fp32 strips ahead of their quantisation (scaled formats)
     char* ring;                      // host tape: HostRing::R device strip slots
     float4 *pz, *py, *px;            // packed CPML profiles per axis
+    int* soff;                       // strip cell offsets (strip_table3)
 };
 
 static Work carve(Carve& c, const Params& P, int nfields)
@@ -1119,6 +1133,7 @@ static Work carve(Carve& c, const Params& P, int nfields)
     w.pz = c.take<float4>(P.nz); w.py = c.take<float4>(P.ny); w.px = c.take<float4>(P.nx);
     for (int i = 0; i < nfields; ++i) w.f[i] = c.take<float>((long long)P.B * P.S);
     w.err = c.take<int>(1);
+    w.soff = c.take<int>(std::max(P.nstrip, 1LL));
     if (P.st.fmt == SF_F16 || P.st.fmt == SF_I8) w.scratch = c.take<float>((long long)P.B * P.nstrip);
     if (P.st.host) w.ring = c.take<char>((long long)HostRing::R * P.st.step);
     return w;
@@ -1136,6 +1151,11 @@ static void prep_call(const sweep_acoustic_desc* d, Params& P, const Work& w, cu
     pack_prof3<<<1, 256, 0, st>>>(d->ax, d->bx, d->dbx, d->nx, d->dx, P, w.px);
     SWEEP_LAUNCH_CHECK();
     P.pz = w.pz; P.py = w.py; P.px = w.px;
+    if (P.nstrip > 0) {
+        strip_table3<<<592, 256, 0, st>>>(P, w.soff);
+        SWEEP_LAUNCH_CHECK();
+    }
+    P.soff = w.soff;
 }
 
 static void check_err(const Work& w, cudaStream_t st, const char* what)
