@@ -18,7 +18,7 @@
  *   staggered D+/D-   src/sweep/csrc/cuda/operators/staggered.cuh:332-430
  *   Lame parameters   src/sweep/csrc/cuda/common/derived_models.cu:27-37
  *   velocity step     src/sweep/csrc/cuda/equations/elastic2d/kernels.cuh:48-138
- *   stress step       kernels.cuh:182-311 (no free surface)
+ *   stress step       kernels.cuh:182-311
  *   reverse (NOPML)   kernels.cuh:365-535
  *   stress adjoint    kernels.cuh:548-750 (prepare, fused vp/vs/rho imaging
  *                     601-663), 807-837 (apply)
@@ -37,6 +37,13 @@
  *                     222-318, 387-490, 659-826
  *   strip geometry    src/sweep/csrc/cuda/common/boundary/strip.cuh:46-123
  *                     (width M+1 at offset -M, physical box tangentially)
+ *   free top face     src/sweep/csrc/cuda/common/elastic_free_surface.cuh:
+ *                     200-465 (image values, order-2 band, reduced transpose
+ *                     and folds); elastic2d/kernels.cuh:216-234, 293-303
+ *                     (surface row in the CPML branch, Robertsson sxx
+ *                     correction, szz = 0), 592-700 (adjoint zeroing, surface
+ *                     imaging, transposed correction), 365-535 (reverse rows
+ *                     from M on a free face)
  */
 #include <stdlib.h>
 #include <string.h>
@@ -58,6 +65,7 @@ typedef struct {
     i64 ms;                     /* model stride between shots (0 = shared) */
     int nsrc; const int* src; const REAL* wavelet; int nsf; const int* sf;
     int nrec; const int* rec; int nrf; const int* rf;
+    int fs;                     /* bit 0: traction-free top face (pad[0] == 0) */
 } EL;
 
 /* D+ along stride s: sum_k c_k (u[i+k s] - u[i-(k-1) s]) * (1/h). */
@@ -77,6 +85,90 @@ static inline REAL dminus(const REAL* u, i64 i, i64 s, int M, const REAL* c, REA
 }
 
 static int in_grid(int ix, int iz, int nx, int nz) { return ix >= 0 && ix < nx && iz >= 0 && iz < nz; }
+
+/* ---- traction-free top face (image method) -------------------------------
+ * The surface is the first physical row, top = pad[0] + M = M (a free face
+ * has no PML pad); rows above it are air.  z-derivatives read an air row as
+ * the image of the row mirrored about the surface: about `top` for fields on
+ * integer rows (szz, vx), about top - 1/2 for fields half a cell below them
+ * (sxz, vz), negated for the odd fields.  The M rows from the surface down
+ * take a 2nd-order (unit-weight) difference instead of the full stencil. */
+static inline int fs_top_row(const EL* p) { return p->pad[0] + p->M; }
+
+static inline REAL fs_at(const EL* p, const REAL* u, int ix, int iz, int odd, int half)
+{
+    const int top = fs_top_row(p);
+    if (iz < top) {
+        const int m = half ? 2 * top - 1 - iz : 2 * top - iz;
+        const REAL v = u[(i64)m * p->nx + ix];
+        return odd ? -v : v;
+    }
+    return u[(i64)iz * p->nx + ix];
+}
+
+/* z-derivative at (ix, iz) on a free top face: fwd = 1 the D+ form (taps
+ * iz+k and iz-k+1), fwd = 0 the D- form (taps iz+k-1 and iz-k). */
+static REAL fs_dz(const EL* p, const REAL* u, int ix, int iz, int fwd, int odd, int half)
+{
+    const int top = fs_top_row(p), M = p->M;
+    if (iz - top >= 0 && iz - top < M) {
+        const REAL g = fwd ? fs_at(p, u, ix, iz + 1, odd, half) - fs_at(p, u, ix, iz, odd, half)
+                           : fs_at(p, u, ix, iz, odd, half) - fs_at(p, u, ix, iz - 1, odd, half);
+        return g / p->dz;
+    }
+    REAL g = R(0);
+    for (int k = 1; k <= M; ++k) {
+        const REAL up = fwd ? fs_at(p, u, ix, iz + k, odd, half) : fs_at(p, u, ix, iz + k - 1, odd, half);
+        const REAL um = fwd ? fs_at(p, u, ix, iz - k + 1, odd, half) : fs_at(p, u, ix, iz - k, odd, half);
+        g = g + p->c[k] * (up - um);
+    }
+    return g / p->dz;
+}
+
+static inline int fs_band(const EL* p, int j)
+{
+    const int top = fs_top_row(p);
+    return j >= top && j < top + p->M;
+}
+
+/* Transpose of fs_dz without the image (negated, in the sign convention of
+ * the plain adjoint stencils: D- for a D+ forward and vice versa) at input
+ * row m: each output row j contributes with the full weight if it lies below
+ * the order-2 band, with weight 1 if it lies in it; reads outside the grid
+ * are skipped. */
+static REAL fs_adj_plain(const EL* p, const REAL* q, int ix, int m, int fwd)
+{
+    const int M = p->M, nz = p->nz, nx = p->nx;
+    REAL acc = R(0);
+    for (int k = 1; k <= M; ++k) {
+        const int jp = fwd ? m + k - 1 : m + k;
+        const int jm = fwd ? m - k : m - k + 1;
+        if (jp >= 0 && jp < nz && !fs_band(p, jp)) acc = acc + p->c[k] * q[(i64)jp * nx + ix];
+        if (jm >= 0 && jm < nz && !fs_band(p, jm)) acc = acc - p->c[k] * q[(i64)jm * nx + ix];
+    }
+    if (fwd) {
+        if (fs_band(p, m)) acc = acc + q[(i64)m * nx + ix];
+        if (fs_band(p, m - 1)) acc = acc - q[(i64)(m - 1) * nx + ix];
+    } else {
+        if (fs_band(p, m + 1)) acc = acc + q[(i64)(m + 1) * nx + ix];
+        if (fs_band(p, m)) acc = acc - q[(i64)m * nx + ix];
+    }
+    return acc / p->dz;
+}
+
+/* Adjoint of fs_dz at row iz: zero on air rows (the forward overwrites them
+ * with images); else the plain transpose plus, where the row's mirror lies in
+ * the air, the transpose at that air row folded back with the field's
+ * parity. */
+static REAL fs_adj_dz(const EL* p, const REAL* q, int ix, int iz, int fwd, int odd, int half)
+{
+    const int top = fs_top_row(p);
+    if (iz < top) return R(0);
+    REAL g = fs_adj_plain(p, q, ix, iz, fwd);
+    const int miz = half ? 2 * top - 1 - iz : 2 * top - iz;
+    if (miz < top) g = g + (odd ? R(-1) : R(1)) * fs_adj_plain(p, q, ix, miz, fwd);
+    return g;
+}
 
 /* CPML test shared by the velocity step, the stress step (no free surface)
  * and both adjoint prepares: the PML pad plus the stencil halo, per face. */
@@ -110,9 +202,9 @@ static void velocity_step(const EL* p, int b, REAL** F)
         for (int ix = M; ix < nx - M; ++ix) {
             const i64 i = (i64)iz * nx + ix;
             REAL dsxx_dx = dplus(F[SXX], i, 1, M, p->c, ix_);
-            REAL dsxz_dz = dminus(F[SXZ], i, nx, M, p->c, iz_);
+            REAL dsxz_dz = p->fs ? fs_dz(p, F[SXZ], ix, iz, 0, 1, 1) : dminus(F[SXZ], i, nx, M, p->c, iz_);
             REAL dsxz_dx = dminus(F[SXZ], i, 1, M, p->c, ix_);
-            REAL dszz_dz = dplus(F[SZZ], i, nx, M, p->c, iz_);
+            REAL dszz_dz = p->fs ? fs_dz(p, F[SZZ], ix, iz, 1, 1, 0) : dplus(F[SZZ], i, nx, M, p->c, iz_);
             REAL inv_rho = R(1) / rho[i];
             if (in_pml(p, ix, iz)) {
                 REAL m;
@@ -136,11 +228,13 @@ static void stress_step(const EL* p, REAL** F, const REAL* lam_, const REAL* mu_
         for (int ix = M; ix < nx - M; ++ix) {
             const i64 i = (i64)iz * nx + ix;
             REAL dvx_dx = dminus(F[VX], i, 1, M, p->c, ix_);
-            REAL dvz_dz = dminus(F[VZ], i, nx, M, p->c, iz_);
-            REAL dvx_dz = dplus(F[VX], i, nx, M, p->c, iz_);
+            REAL dvz_dz = p->fs ? fs_dz(p, F[VZ], ix, iz, 0, 1, 1) : dminus(F[VZ], i, nx, M, p->c, iz_);
+            REAL dvx_dz = p->fs ? fs_dz(p, F[VX], ix, iz, 1, 0, 0) : dplus(F[VX], i, nx, M, p->c, iz_);
             REAL dvz_dx = dplus(F[VZ], i, 1, M, p->c, ix_);
             REAL lam = lam_[i], mu = mu_[i];
-            const int pml = in_pml(p, ix, iz);
+            /* a free surface row takes the CPML branch (kernels.cuh:216-234) */
+            const int surf = p->fs && iz == fs_top_row(p);
+            const int pml = in_pml(p, ix, iz) || surf;
             if (pml) {
                 REAL m;
                 m = p->az[iz] * F[M_VZZ][i] + p->bz[iz] * dvz_dz; F[M_VZZ][i] = m; dvz_dz = dvz_dz + m;
@@ -154,6 +248,10 @@ static void stress_step(const EL* p, REAL** F, const REAL* lam_, const REAL* mu_
                 m = p->axh[ix] * F[M_VZX][i] + p->bxh[ix] * dvz_dx; F[M_VZX][i] = m; dvz_dx = dvz_dx + m;
             }
             F[SXZ][i] = F[SXZ][i] + (p->dt * mu) * (dvx_dz + dvz_dx);
+            if (surf) {   /* Robertsson correction, then szz = 0 (kernels.cuh:293-303) */
+                F[SXX][i] = F[SXX][i] + (-p->dt) * lam * ((lam / (lam + R(2) * mu)) * dvx_dx + dvz_dz);
+                F[SZZ][i] = R(0);
+            }
         }
     }
 }
@@ -201,7 +299,7 @@ long long oracle_el2d_tape_len(int B, int nz, int nx, int nt, int M, const int* 
     EL p = {B, nz, nx, nt, M, {pad[0], pad[1], pad[2], pad[3]}, dt, dz, dx, coef,          \
             prof, prof + nz, prof + 2 * nz, prof + 3 * nz,                                 \
             prof + 4 * nz, prof + 4 * nz + nx, prof + 4 * nz + 2 * nx, prof + 4 * nz + 3 * nx, \
-            vp, vs, rho, m_stride, nsrc, src, wavelet, nsf, sfields, nrec, rec, nrf, rfields}
+            vp, vs, rho, m_stride, nsrc, src, wavelet, nsf, sfields, nrec, rec, nrf, rfields, fs}
 
 /* Forward (sg_driver.cuh:291-340): velocity step, stress step, source
  * injection per source field, band save of the 5 fields (tape non-NULL),
@@ -211,7 +309,7 @@ int oracle_el2d_forward(
     const REAL* coef, const REAL* prof,
     const REAL* vp, const REAL* vs, const REAL* rho, i64 m_stride,
     int nsrc, const int* src, const REAL* wavelet, int nsf, const int* sfields,
-    int nrec, const int* rec, int nrf, const int* rfields,
+    int nrec, const int* rec, int nrf, const int* rfields, int fs,
     REAL* record, REAL* tape)
 {
     SETUP_EL;
@@ -257,13 +355,14 @@ static void stress_reverse(const EL* p, REAL** F, const REAL* lam_, const REAL* 
 {
     const int nz = p->nz, nx = p->nx, M = p->M;
     const REAL ix_ = R(1) / p->dx, iz_ = R(1) / p->dz;
+    const int zlo = p->fs ? M : p->pad[0] + M + 1;   /* a free face narrows to the halo */
     #pragma omp parallel for schedule(static)
-    for (int iz = p->pad[0] + M + 1; iz < nz - (p->pad[1] + M + 1); ++iz) {
+    for (int iz = zlo; iz < nz - (p->pad[1] + M + 1); ++iz) {
         for (int ix = p->pad[2] + M + 1; ix < nx - (p->pad[3] + M + 1); ++ix) {
             const i64 i = (i64)iz * nx + ix;
             REAL dvx_dx = dminus(F[VX], i, 1, M, p->c, ix_);
-            REAL dvz_dz = dminus(F[VZ], i, nx, M, p->c, iz_);
-            REAL dvx_dz = dplus(F[VX], i, nx, M, p->c, iz_);
+            REAL dvz_dz = p->fs ? fs_dz(p, F[VZ], ix, iz, 0, 1, 1) : dminus(F[VZ], i, nx, M, p->c, iz_);
+            REAL dvx_dz = p->fs ? fs_dz(p, F[VX], ix, iz, 1, 0, 0) : dplus(F[VX], i, nx, M, p->c, iz_);
             REAL dvz_dx = dplus(F[VZ], i, 1, M, p->c, ix_);
             REAL lam = lam_[i], mu = mu_[i];
             F[SXX][i] = F[SXX][i] - p->dt * ((lam + R(2) * mu) * dvx_dx + lam * dvz_dz);
@@ -278,14 +377,15 @@ static void velocity_reverse(const EL* p, int b, REAL** F)
     const int nz = p->nz, nx = p->nx, M = p->M;
     const REAL* rho = p->rho + b * p->ms;
     const REAL ix_ = R(1) / p->dx, iz_ = R(1) / p->dz;
+    const int zlo = p->fs ? M : p->pad[0] + M + 1;
     #pragma omp parallel for schedule(static)
-    for (int iz = p->pad[0] + M + 1; iz < nz - (p->pad[1] + M + 1); ++iz) {
+    for (int iz = zlo; iz < nz - (p->pad[1] + M + 1); ++iz) {
         for (int ix = p->pad[2] + M + 1; ix < nx - (p->pad[3] + M + 1); ++ix) {
             const i64 i = (i64)iz * nx + ix;
             REAL dsxx_dx = dplus(F[SXX], i, 1, M, p->c, ix_);
-            REAL dsxz_dz = dminus(F[SXZ], i, nx, M, p->c, iz_);
+            REAL dsxz_dz = p->fs ? fs_dz(p, F[SXZ], ix, iz, 0, 1, 1) : dminus(F[SXZ], i, nx, M, p->c, iz_);
             REAL dsxz_dx = dminus(F[SXZ], i, 1, M, p->c, ix_);
-            REAL dszz_dz = dplus(F[SZZ], i, nx, M, p->c, iz_);
+            REAL dszz_dz = p->fs ? fs_dz(p, F[SZZ], ix, iz, 1, 1, 0) : dplus(F[SZZ], i, nx, M, p->c, iz_);
             REAL inv_rho = R(1) / rho[i];
             F[VX][i] = F[VX][i] - (p->dt * inv_rho) * (dsxx_dx + dsxz_dz);
             F[VZ][i] = F[VZ][i] - (p->dt * inv_rho) * (dsxz_dx + dszz_dz);
@@ -310,13 +410,25 @@ static void stress_adjoint_prepare(const EL* p, int b, REAL** A, REAL** Q, const
             const i64 i = (i64)iz * nx + ix;
             REAL lam = lam_[i], mu = mu_[i];
             REAL bsxx = A[SXX][i], bszz = A[SZZ][i], bsxz = A[SXZ][i];
+            const int surf = p->fs && iz == fs_top_row(p);
+            if (surf) { bszz = R(0); A[SZZ][i] = R(0); }
             if (gvp && ix >= x0 && ix < x1 && iz >= z0 && iz < z1) {
                 REAL fvx_x = dminus(Fw[VX], i, 1, M, p->c, ix_);
-                REAL fvz_z = dminus(Fw[VZ], i, nx, M, p->c, iz_);
-                REAL fvx_z = dplus(Fw[VX], i, nx, M, p->c, iz_);
+                REAL fvz_z = p->fs ? fs_dz(p, Fw[VZ], ix, iz, 0, 1, 1) : dminus(Fw[VZ], i, nx, M, p->c, iz_);
+                REAL fvx_z = p->fs ? fs_dz(p, Fw[VX], ix, iz, 1, 0, 0) : dplus(Fw[VX], i, nx, M, p->c, iz_);
                 REAL fvz_x = dplus(Fw[VZ], i, 1, M, p->c, ix_);
-                REAL gl = (bsxx + bszz) * (fvx_x + fvz_z);
-                REAL gm = R(2) * (bsxx * fvx_x + bszz * fvz_z);
+                REAL gl, gm;
+                if (surf) {
+                    /* d/d(lam, mu) of the surface row's sxx update,
+                     * dt C dvx_dx with C = 4 mu (lam + mu) / (lam + 2 mu) */
+                    const REAL vp2 = vp[i] * vp[i], vs2 = vs[i] * vs[i], vp4 = vp2 * vp2;
+                    const REAL a = bsxx * fvx_x;
+                    gl = a * R(4) * vs2 * vs2 / vp4;
+                    gm = a * R(4) * (vp4 - R(2) * vp2 * vs2 + R(2) * vs2 * vs2) / vp4;
+                } else {
+                    gl = (bsxx + bszz) * (fvx_x + fvz_z);
+                    gm = R(2) * (bsxx * fvx_x + bszz * fvz_z);
+                }
                 gm = gm + bsxz * (fvx_z + fvz_x);
                 gvp[i] = gvp[i] + ((R(-2) * rho[i]) * vp[i]) * gl * dt;
                 gvs[i] = gvs[i] + (-((((R(-4) * rho[i]) * vs[i]) * gl) + (((R(2) * rho[i]) * vs[i]) * gm))) * dt;
@@ -324,8 +436,15 @@ static void stress_adjoint_prepare(const EL* p, int b, REAL** A, REAL** Q, const
                 grho[i] = grho[i] - ((gl * ((vp[i] * vp[i]) - ((R(2) * vs[i]) * vs[i]))) * dt +
                                      (gm * (vs[i] * vs[i])) * dt);
             }
-            REAL bvx_x = dt * ((lam + R(2) * mu) * bsxx + lam * bszz);
-            REAL bvz_z = dt * ((lam + R(2) * mu) * bszz + lam * bsxx);
+            REAL bvx_x, bvz_z;
+            if (surf) {   /* transpose of the corrected surface update */
+                const REAL c_surf = R(4) * mu * (lam + mu) / (lam + R(2) * mu);
+                bvx_x = dt * c_surf * bsxx;
+                bvz_z = R(0);
+            } else {
+                bvx_x = dt * ((lam + R(2) * mu) * bsxx + lam * bszz);
+                bvz_z = dt * ((lam + R(2) * mu) * bszz + lam * bsxx);
+            }
             REAL bvx_z = (dt * mu) * bsxz;
             REAL bvz_x = (dt * mu) * bsxz;
             if (!in_pml(p, ix, iz)) {
@@ -357,9 +476,9 @@ static void stress_adjoint_apply(const EL* p, REAL** A, REAL** Q)
         for (int ix = M; ix < nx - M; ++ix) {
             const i64 i = (i64)iz * nx + ix;
             REAL dqxx_dx = dplus(Q[0], i, 1, M, p->c, ix_);
-            REAL dqxz_dz = dminus(Q[2], i, nx, M, p->c, iz_);
+            REAL dqxz_dz = p->fs ? fs_adj_dz(p, Q[2], ix, iz, 1, 0, 0) : dminus(Q[2], i, nx, M, p->c, iz_);
             REAL dqzx_dx = dminus(Q[3], i, 1, M, p->c, ix_);
-            REAL dqzz_dz = dplus(Q[1], i, nx, M, p->c, iz_);
+            REAL dqzz_dz = p->fs ? fs_adj_dz(p, Q[1], ix, iz, 0, 1, 1) : dplus(Q[1], i, nx, M, p->c, iz_);
             A[VX][i] = A[VX][i] + (dqxx_dx + dqxz_dz);
             A[VZ][i] = A[VZ][i] + (dqzx_dx + dqzz_dz);
         }
@@ -403,8 +522,8 @@ static void velocity_adjoint(const EL* p, int b, REAL** A, REAL** P)
         for (int ix = M; ix < nx - M; ++ix) {
             const i64 i = (i64)iz * nx + ix;
             REAL dpxx_dx = dminus(P[0], i, 1, M, p->c, ix_);
-            REAL dpzz_dz = dminus(P[1], i, nx, M, p->c, iz_);
-            REAL dpxz_dz = dplus(P[2], i, nx, M, p->c, iz_);
+            REAL dpzz_dz = p->fs ? fs_adj_dz(p, P[1], ix, iz, 1, 1, 0) : dminus(P[1], i, nx, M, p->c, iz_);
+            REAL dpxz_dz = p->fs ? fs_adj_dz(p, P[2], ix, iz, 0, 1, 1) : dplus(P[2], i, nx, M, p->c, iz_);
             REAL dpzx_dx = dplus(P[3], i, 1, M, p->c, ix_);
             A[SXX][i] = A[SXX][i] + dpxx_dx;
             A[SZZ][i] = A[SZZ][i] + dpzz_dz;
@@ -423,7 +542,7 @@ int oracle_el2d_backward(
     const REAL* coef, const REAL* prof,
     const REAL* vp, const REAL* vs, const REAL* rho, i64 m_stride,
     int nsrc, const int* src, const REAL* wavelet, int nsf, const int* sfields,
-    int nrec, const int* rec, int nrf, const int* rfields,
+    int nrec, const int* rec, int nrf, const int* rfields, int fs,
     const REAL* adj, const REAL* tape, REAL* grad_vp, REAL* grad_vs, REAL* grad_rho)
 {
     SETUP_EL;

@@ -96,7 +96,7 @@ def _lib(prec: str):
         lib.oracle_a3d_backward.restype = i
         lib.oracle_a3d_backward.argtypes = geo3 + [P, P, P, P, P, P]
         geo_el = [i, i, i, i, i, P, real, real, real, P, P, P, P, P, l,
-                  i, P, P, i, P, i, P, i, P]
+                  i, P, P, i, P, i, P, i, P, i]
         lib.oracle_el2d_tape_len.restype = l
         lib.oracle_el2d_tape_len.argtypes = [i, i, i, i, i, P]
         lib.oracle_el2d_forward.restype = i
@@ -387,11 +387,13 @@ class Elastic2D:
     """2-D isotropic elastic oracle run (``fd_oracle_el.c``): models
     ``vp, vs, rho`` of shape ``(nz, nx)`` or per shot ``(B, nz, nx)``; source
     fields default to the explosive ``(sxx, szz)``, receiver fields to
-    ``(vx, vz)`` (``src/sweep/equations/elastic.py:123-128``)."""
+    ``(vx, vz)`` (``src/sweep/equations/elastic.py:123-128``).
+    ``free_surface=True``: a traction-free top face with no PML pad
+    (reference ``PropTorch(free_surface=True)``)."""
 
     def __init__(self, vp, vs, rho, wavelet, src, rec, dh, dt, abcn, order=8, prec="f32",
                  source_fields=("sxx", "szz"), receiver_fields=("vx", "vz"),
-                 max_vel=4500.0, pml_freq=25.0):
+                 max_vel=4500.0, pml_freq=25.0, free_surface=False):
         self.prec = prec
         self.real = np.float32 if prec == "f32" else np.float64
         models = [np.asarray(m, np.float32) for m in (vp, vs, rho)]
@@ -400,9 +402,11 @@ class Elastic2D:
         w, s, r = _batch_io(wavelet, src, rec, 2)
         self.B, self.nt = w.shape[0], w.shape[-1]
         self.phys = models[0].shape[-2:]
-        self.pad = abcn
-        self.shape = tuple(n + 2 * abcn + 2 * M for n in self.phys)
-        padw = [(abcn + M, abcn + M)] * 2
+        self.fs = 1 if free_surface else 0
+        self.pads = [0 if free_surface else abcn, abcn, abcn, abcn]   # z_lo, z_hi, x_lo, x_hi
+        pz, px = self.pads[:2], self.pads[2:]
+        self.shape = (self.phys[0] + sum(pz) + 2 * M, self.phys[1] + sum(px) + 2 * M)
+        padw = [(pz[0] + M, pz[1] + M), (px[0] + M, px[1] + M)]
         lead = [(0, 0)] if self.per_shot else []
         self.models = [np.ascontiguousarray(np.pad(m, lead + padw, mode="edge").astype(self.real))
                        for m in models]
@@ -410,7 +414,7 @@ class Elastic2D:
         sp = dh if np.ndim(dh) else [dh] * 2
         self.spacing = [float(x) for x in sp]
         self.dt = float(dt)
-        prof = cpml_profiles_s([abcn] * 4, M, dt, self.spacing, self.shape, max_vel, pml_freq)
+        prof = cpml_profiles_s(self.pads, M, dt, self.spacing, self.shape, max_vel, pml_freq)
         (az, bz, azh, bzh), (ax, bx, axh, bxh) = prof
         self.prof = np.ascontiguousarray(
             np.concatenate([az, bz, azh, bzh, ax, bx, axh, bxh]).astype(self.real))
@@ -418,7 +422,7 @@ class Elastic2D:
         self.coef = np.array([0.0] + [float(x) for x in c], np.float64).astype(self.real)
         if self.real is np.float32:
             self.coef = np.array([0.0] + [np.float32(float(x)) for x in c], np.float32)
-        off = abcn + M
+        off = np.array([px[0] + M, pz[0] + M])          # (x, z)
         self.src = np.ascontiguousarray((s + off).astype(np.int32))
         self.rec = np.ascontiguousarray((r + off).astype(np.int32))
         self.wavelet = np.ascontiguousarray(w.astype(self.real))
@@ -428,16 +432,17 @@ class Elastic2D:
 
     def _geo(self):
         nz, nx = self.shape
-        self._pad = np.array([self.pad] * 4, np.int32)
+        self._pad = np.array(self.pads, np.int32)
         return [self.B, nz, nx, self.nt, self.M, _ptr(self._pad), self.dt, self.spacing[0],
                 self.spacing[1], _ptr(self.coef), _ptr(self.prof), _ptr(self.models[0]),
                 _ptr(self.models[1]), _ptr(self.models[2]), self.m_stride,
                 1, _ptr(self.src), _ptr(self.wavelet), len(self.sf), _ptr(self.sf),
-                self.nrec, _ptr(self.rec), len(self.rf), _ptr(self.rf)]
+                self.nrec, _ptr(self.rec), len(self.rf), _ptr(self.rf), self.fs]
 
     def crop(self, g):
-        M, a = self.M, self.pad
-        sl = tuple(slice(a + M, a + M + n) for n in self.phys)
+        M = self.M
+        lo = (self.pads[0], self.pads[2])
+        sl = tuple(slice(a + M, a + M + n) for a, n in zip(lo, self.phys))
         return g[(Ellipsis,) + sl]
 
     def forward(self, keep_tape=True):
@@ -447,7 +452,7 @@ class Elastic2D:
         rec = np.zeros((self.B, self.nt, self.nrec, len(self.rf)), self.real)
         self.tape = None
         if keep_tape:
-            pad = np.array([self.pad] * 4, np.int32)
+            pad = np.array(self.pads, np.int32)
             n = lib.oracle_el2d_tape_len(self.B, nz, nx, self.nt, self.M, _ptr(pad))
             self.tape = np.zeros(n, self.real)
         rc = lib.oracle_el2d_forward(*self._geo(), _ptr(rec),

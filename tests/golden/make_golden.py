@@ -613,6 +613,50 @@ def elastic2d_interior():
     )
 
 
+def elastic2d_free_surface():
+    """Isotropic elastic with a traction-free top face (reference
+    PropTorch(free_surface=True): no PML on top, the image method of
+    elastic_free_surface.cuh, the Robertsson sxx correction and szz = 0 on the
+    surface row).  2 explosive shots (one on the surface row, one 3 cells
+    below it); shot 0 records (vx, vz) on the surface row, shot 1 at depth
+    1 and 5; vp/vs/rho gradients, boundary saving and checkpoints."""
+    rng = np.random.default_rng(71)
+    nz, nx, nt, dt, dh, abcn = 40, 56, 300, 0.0005, 5.0, 10
+    vp_true = _layered(nz, nx, rng, 1800.0, 3200.0, 4)
+    vs_true = (vp_true / 1.73).astype(np.float32)
+    rho_true = (310.0 * vp_true ** 0.25).astype(np.float32)
+    vp_init = np.full((nz, nx), 2200.0, np.float32)
+    vs_init = (vp_init / 1.73).astype(np.float32)
+    rho_init = (310.0 * vp_init ** 0.25).astype(np.float32)
+    w = _wavelet(nt, dt, 25.0, 0.04)
+    src = np.array([[14, 0], [40, 3]], np.int64)
+    rec = np.zeros((2, 8, 2), np.int64)
+    for b in range(2):
+        rec[b, :, 0] = np.linspace(3, nx - 4, 8).astype(np.int64)
+    rec[0, :, 1] = 0
+    rec[1, :4, 1] = 1
+    rec[1, 4:, 1] = 5
+    res = {}
+    for mode, mem in (("bs", BoundarySaving()), ("ckpt", Ckpt(chunks=7))):
+        eq = Elastic(spatial_order=8, device="cpu")
+        solver = PropTorch(eq, shape=(nz, nx), dh=dh, dt=dt, abcn=abcn, impl="c",
+                           device="cpu", memory=mem, free_surface=True)
+        obs = _forward(solver, w, src, rec, [vp_true, vs_true, rho_true])
+        r = _run(solver, w, src, rec, [vp_init, vs_init, rho_init], obs, False)
+        res[mode] = (obs, r)
+    obs, r = res["bs"]
+    np.savez_compressed(
+        OUT / "elastic2d_free_surface.npz",
+        nz=nz, nx=nx, nt=nt, dt=dt, dh=dh, abcn=abcn, order=8,
+        vp_true=vp_true, vs_true=vs_true, rho_true=rho_true,
+        vp_init=vp_init, vs_init=vs_init, rho_init=rho_init,
+        wavelet=w, src=src, rec=rec, obs=obs, pred=r["pred"], loss=r["loss"],
+        grad_vp=r["grad0"], grad_vs=r["grad1"], grad_rho=r["grad2"],
+        grad_vp_ckpt=res["ckpt"][1]["grad0"], grad_vs_ckpt=res["ckpt"][1]["grad1"],
+        grad_rho_ckpt=res["ckpt"][1]["grad2"],
+    )
+
+
 CASES = {
     "acoustic2d_c1": acoustic2d_c1,
     "acoustic2d_multi": acoustic2d_multi,
@@ -631,6 +675,7 @@ CASES = {
     "acoustic3d_clean": acoustic3d_clean,
     "acoustic2d_many": acoustic2d_many,
     "elastic2d_interior": elastic2d_interior,
+    "elastic2d_free_surface": elastic2d_free_surface,
 }
 
 if __name__ == "__main__":

@@ -133,6 +133,34 @@ def test_elastic2d_velocity_sources_oracle_matches_reference(prec, tol):
     assert rel(grho, d["grad_rho"]) < 5 * tol
 
 
+@pytest.mark.parametrize("prec,tol", [("f32", 2e-6), ("f64", 5e-6)])
+def test_elastic2d_free_surface_oracle_matches_reference(prec, tol):
+    """Traction-free top face (image method, order-2 band, Robertsson sxx
+    correction, szz = 0 on the surface row): a shot on the surface row
+    recorded on it and a shot below it; records and vp / vs / rho gradients
+    of the reference's boundary-saving run.  Without the free surface the
+    records differ at order one, so the fixture pins the surface terms."""
+    d = np.load(GOLD / "elastic2d_free_surface.npz")
+    obs = O.elastic_forward(d["vp_true"], d["vs_true"], d["rho_true"], d["wavelet"], d["src"],
+                            d["rec"], *_el_args(d), prec=prec, free_surface=True)
+    assert obs.shape == d["obs"].shape
+    assert rel(obs, d["obs"]) < tol
+    plain = O.elastic_forward(d["vp_true"], d["vs_true"], d["rho_true"], d["wavelet"], d["src"],
+                              d["rec"], *_el_args(d), prec=prec)
+    assert rel(plain, d["obs"]) > 0.1
+    pred, loss, (gvp, gvs, grho) = O.elastic_gradient(
+        d["vp_init"], d["vs_init"], d["rho_init"], d["wavelet"], d["src"], d["rec"], d["obs"],
+        *_el_args(d), prec=prec, free_surface=True)
+    assert rel(pred, d["pred"]) < tol
+    assert abs(loss - float(d["loss"])) < 1e-5 * float(d["loss"])
+    assert rel(gvp, d["grad_vp"]) < 5 * tol
+    assert rel(gvs, d["grad_vs"]) < 5 * tol
+    assert rel(grho, d["grad_rho"]) < 5 * tol
+    # the reference's checkpointed run gives the boundary-saving gradient
+    for k in ("vp", "vs", "rho"):
+        assert rel(d[f"grad_{k}_ckpt"], d[f"grad_{k}"]) < 2e-6
+
+
 def test_elastic2d_reference_full_and_boundary_modes_agree():
     """The reference's full-storage gradient adds the it = 0 image the
     boundary-saving reverse skips; the two differ at the 1e-6 level."""
