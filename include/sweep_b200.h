@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define SWEEP_B200_ABI_VERSION 4
+#define SWEEP_B200_ABI_VERSION 5
 
 #if defined(__GNUC__)
 #define SWEEP_B200_API __attribute__((visibility("default")))
@@ -175,6 +175,12 @@ typedef struct sweep_elastic_desc {
     const int32_t* rec_loc;  /* (B, nrec, 2) */
     int32_t nrec_fields;     /* 1..5 */
     int32_t rec_fields[5];   /* wavefield indices recorded, in record order */
+    /* Traction-free faces z_lo, z_hi, x_lo, x_hi (reference PropTorch(
+     * free_surface=...) for Elastic: the image method of
+     * elastic_free_surface.cuh, the Robertsson sxx correction and szz = 0 on
+     * the surface row, elastic2d/kernels.cuh:293-303).  1 = free; a free face
+     * has pad 0.  The top face (z_lo) is built; the others must be 0. */
+    int32_t free_surface[4];
 } sweep_elastic_desc;
 
 /* Sizes of the elastic workspace and tape (as sweep_b200_acoustic_sizes). */

@@ -17,7 +17,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIB_PATH = Path(os.environ.get("SWEEP_B200_LIB", HERE / "libsweep_b200.so"))
-ABI_VERSION = 4
+ABI_VERSION = 5
 ERR_CAP = 4096
 
 c_i32, c_i64, c_f32, c_p = ctypes.c_int32, ctypes.c_int64, ctypes.c_float, ctypes.c_void_p
@@ -91,6 +91,7 @@ class ElasticDesc(ctypes.Structure):
         ("nsrc_fields", c_i32), ("src_fields", c_i32 * 5),
         ("nrec", c_i32), ("rec_loc", c_p),
         ("nrec_fields", c_i32), ("rec_fields", c_i32 * 5),
+        ("free_surface", c_i32 * 4),
     ]
 
 

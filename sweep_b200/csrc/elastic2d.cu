@@ -101,6 +101,7 @@ struct Geo {
     int gf;                         // shots per CTA of the forward kernels
     int* err;                       // bounded-wait failure flag (0 = none)
     StripStore st;
+    int fst;                        // traction-free top face: the surface is row z0 (no pad above)
 };
 
 enum { ERR_WAIT_FWD = 1, ERR_WAIT_REV = 2 };
@@ -253,6 +254,72 @@ __device__ __forceinline__ float dmz(const float* t, int c, float inv)
             C3 * (t[c + 2 * HX] - t[c - 3 * HX]) + C4 * (t[c + 3 * HX] - t[c - 4 * HX])) * inv;
 }
 
+// ------------------------------------------------- traction-free top face
+// Image method of the reference (common/elastic_free_surface.cuh:200-450,
+// elastic2d/kernels.cuh:216-234, 293-303, 592-700).  The surface is row z0,
+// the first physical row (a free face has no PML pad); the M rows above it
+// are air.  The M rows from the surface down take a unit-weight 2nd-order
+// z-difference instead of the full stencil.  Only the D- form on the surface
+// row reads the air: the row above it holds the image of the surface row,
+// negated, for both fields it is used on (sxz and vz sit half a cell below
+// the surface and are odd).  The surface row's sxx gets the Robertsson
+// correction and its szz is zeroed after the stress update.
+template <bool FS>
+__device__ __forceinline__ bool fs_band(const Geo& G, int iz)
+{
+    return FS && iz >= G.z0 && iz < G.z0 + M;
+}
+// D+ in z (szz, vx) on a free top face
+template <bool FS>
+__device__ __forceinline__ float dpz_fs(const Geo& G, const float* t, int c, int iz, float inv)
+{
+    return fs_band<FS>(G, iz) ? (t[c + HX] - t[c]) * inv : dpz(t, c, inv);
+}
+// D- in z (sxz, vz) on a free top face
+template <bool FS>
+__device__ __forceinline__ float dmz_fs(const Geo& G, const float* t, int c, int iz, float inv)
+{
+    if (!fs_band<FS>(G, iz)) return dmz(t, c, inv);
+    return (iz == G.z0 ? t[c] + t[c] : t[c] - t[c - HX]) * inv;
+}
+// Negated transposes of dpz_fs and dmz_fs at input row m (the plain ones are
+// dmz for a D+ forward and dpz for a D- forward): an output row in the band
+// contributes with weight 1, one below it with the full weight.  The image
+// read by the surface row adds -q[z0] to the D- transpose there.  Air rows
+// hold no adjoint (sources and receivers above a free surface are off the
+// grid), so nothing else folds back.  Rows from z0 + 2M down are plain.
+template <bool FS>
+__device__ __forceinline__ float adj_dpz_fs(const Geo& G, const float* q, int c, int m, float inv)
+{
+    if (!FS || m >= G.z0 + 2 * M) return dmz(q, c, inv);
+    const float w[M] = {C1, C2, C3, C4};
+    float acc = 0.f;
+#pragma unroll
+    for (int k = 1; k <= M; ++k) {
+        if (!fs_band<FS>(G, m + k - 1)) acc += w[k - 1] * q[c + (k - 1) * HX];
+        if (!fs_band<FS>(G, m - k)) acc -= w[k - 1] * q[c - k * HX];
+    }
+    if (fs_band<FS>(G, m)) acc += q[c];
+    if (fs_band<FS>(G, m - 1)) acc -= q[c - HX];
+    return acc * inv;
+}
+template <bool FS>
+__device__ __forceinline__ float adj_dmz_fs(const Geo& G, const float* q, int c, int m, float inv)
+{
+    if (!FS || m >= G.z0 + 2 * M) return dpz(q, c, inv);
+    const float w[M] = {C1, C2, C3, C4};
+    float acc = 0.f;
+#pragma unroll
+    for (int k = 1; k <= M; ++k) {
+        if (!fs_band<FS>(G, m + k)) acc += w[k - 1] * q[c + k * HX];
+        if (!fs_band<FS>(G, m - k + 1)) acc -= w[k - 1] * q[c - (k - 1) * HX];
+    }
+    if (fs_band<FS>(G, m + 1)) acc += q[c + HX];
+    if (fs_band<FS>(G, m)) acc -= q[c];
+    if (m == G.z0) acc -= q[c];
+    return acc * inv;
+}
+
 // Cooperative load of NF fields' tiles plus an M-cell halo (zero outside the
 // grid) into shared memory: every thread issues all its global loads before
 // its first shared store, so the loads of a CTA are in flight together.
@@ -328,10 +395,11 @@ struct MemPair {
     float a, b;
 };
 
-__device__ __forceinline__ MemPair load_mem_z(const Geo& G, const Slabs& m, int k0, int k1, int b, int iz, int ix)
+__device__ __forceinline__ MemPair load_mem_z(const Geo& G, const Slabs& m, int k0, int k1, int b, int iz, int ix,
+                                              bool surf = false)
 {
     MemPair p{-1, 0.f, 0.f};
-    if (iz >= G.nz || ix >= G.nx || !in_pml(G, ix, iz)) return p;
+    if (iz >= G.nz || ix >= G.nx || !(surf || in_pml(G, ix, iz))) return p;
     const int zs = zslab(G, iz);
     if (zs < 0) return p;
     p.at = ((long long)b * G.WZ + zs) * G.P + ix;
@@ -340,10 +408,11 @@ __device__ __forceinline__ MemPair load_mem_z(const Geo& G, const Slabs& m, int 
     return p;
 }
 
-__device__ __forceinline__ MemPair load_mem_x(const Geo& G, const Slabs& m, int k0, int k1, int b, int iz, int ix)
+__device__ __forceinline__ MemPair load_mem_x(const Geo& G, const Slabs& m, int k0, int k1, int b, int iz, int ix,
+                                              bool surf = false)
 {
     MemPair p{-1, 0.f, 0.f};
-    if (iz >= G.nz || ix >= G.nx || !in_pml(G, ix, iz)) return p;
+    if (iz >= G.nz || ix >= G.nx || !(surf || in_pml(G, ix, iz))) return p;
     const int xs = xslab(G, ix);
     if (xs < 0) return p;
     p.at = ((long long)b * G.nz + iz) * G.WX + xs;
@@ -402,6 +471,7 @@ __device__ __forceinline__ void drain(StageSmem<NH, NC>& sm, int g, int nloc, in
 }
 
 // Velocity step (reference kernels.cuh:48-138).
+template <bool FS>
 __global__ void __launch_bounds__(NTH, 4) fwd_vel(const __grid_constant__ FwdMaps MP, FwdArgs A)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -450,9 +520,9 @@ __global__ void __launch_bounds__(NTH, 4) fwd_vel(const __grid_constant__ FwdMap
             if (!in_core(G, ix, iz)) continue;
             const int c = (lz + M) * HX + lx + M;
             float dsxx_dx = dpx(tsxx, c, G.idx);
-            float dsxz_dz = dmz(tsxz, c, G.idz);
+            float dsxz_dz = dmz_fs<FS>(G, tsxz, c, iz, G.idz);
             float dsxz_dx = dmx(tsxz, c, G.idx);
-            float dszz_dz = dpz(tszz, c, G.idz);
+            float dszz_dz = dpz_fs<FS>(G, tszz, c, iz, G.idz);
             const long long i = (long long)iz * G.P + ix;
             if (ring && in_pml(G, ix, iz)) {
                 if (mz[r].at >= 0) {
@@ -484,10 +554,11 @@ __global__ void __launch_bounds__(NTH, 4) fwd_vel(const __grid_constant__ FwdMap
     }
 }
 
-// Stress step (reference kernels.cuh:182-311, no free surface), then the
+// Stress step (reference kernels.cuh:182-311, with the free top face), then the
 // step's point work for the cells this CTA owns: source injection into the
 // stress source fields, the 5-field strip save and the receiver gather
 // (reference sg_driver.cuh:300-340 order: inject, save, record).
+template <bool FS>
 __global__ void __launch_bounds__(NTH, 4) fwd_str(const __grid_constant__ FwdMaps MP, FwdArgs A)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -532,8 +603,11 @@ __global__ void __launch_bounds__(NTH, 4) fwd_str(const __grid_constant__ FwdMap
 #pragma unroll
             for (int r = 0; r < RPT; ++r) {
                 const int iz = tz0 + threadIdx.y + 8 * r;
-                mz[r] = load_mem_z(G, A.mem, ZM_VZZ, ZM_VXZ, b, iz, ix);
-                mx[r] = load_mem_x(G, A.mem, XM_VXX, XM_VZX, b, iz, ix);
+                // the free surface row takes the CPML branch at every column
+                // (reference kernels.cuh:216-234): the high side's half-cell
+                // profile is nonzero one cell inside the band there
+                mz[r] = load_mem_z(G, A.mem, ZM_VZZ, ZM_VXZ, b, iz, ix, FS && iz == G.z0);
+                mx[r] = load_mem_x(G, A.mem, XM_VXX, XM_VZX, b, iz, ix, FS && iz == G.z0);
             }
         }
         const int s0 = G.src.off[key], s1 = G.src.off[key + 1];
@@ -547,11 +621,11 @@ __global__ void __launch_bounds__(NTH, 4) fwd_str(const __grid_constant__ FwdMap
             float sxx = sm.c[s][0][cell], szz = sm.c[s][1][cell], sxz = sm.c[s][2][cell];
             if (in_core(G, ix, iz)) {
                 float dvx_dx = dmx(tvx, c, G.idx);
-                float dvz_dz = dmz(tvz, c, G.idz);
-                float dvx_dz = dpz(tvx, c, G.idz);
+                float dvz_dz = dmz_fs<FS>(G, tvz, c, iz, G.idz);
+                float dvx_dz = dpz_fs<FS>(G, tvx, c, iz, G.idz);
                 float dvz_dx = dpx(tvz, c, G.idx);
                 const float lam = lamr[r], mu = mur[r];
-                const bool pml = ring && in_pml(G, ix, iz);
+                const bool pml = ring && (in_pml(G, ix, iz) || (FS && iz == G.z0));
                 if (pml && mz[r].at >= 0) {
                     float m = G.az[iz] * mz[r].a + G.bz[iz] * dvz_dz;
                     A.mem.z[ZM_VZZ][mz[r].at] = m; dvz_dz += m;
@@ -571,6 +645,10 @@ __global__ void __launch_bounds__(NTH, 4) fwd_str(const __grid_constant__ FwdMap
                     A.mem.x[XM_VZX][mx[r].at] = m; dvz_dx += m;
                 }
                 sxz += G.dt * mu * (dvx_dz + dvz_dx);
+                if (FS && iz == G.z0) {   // surface row: Robertsson correction, then szz = 0
+                    sxx += -G.dt * lam * (lam / (lam + 2.f * mu) * dvx_dx + dvz_dz);
+                    szz = 0.f;
+                }
             }
             // point sources of this cell (usually none in the tile)
             for (int e = s0; e < s1; ++e) {
@@ -722,6 +800,7 @@ struct RevArgs {
 // fused vp / vs / rho imaging on the physical box (kernels.cuh:601-663) and
 // the receiver rho correction (common.cu:77-117).  The gradient contributions
 // of the CTA's shots are summed in registers and added to slot blockIdx.y.
+template <bool FS>
 __global__ void __launch_bounds__(NTH, 4) rev_str(RevArgs A)
 {
     extern __shared__ float sm[];
@@ -780,8 +859,8 @@ __global__ void __launch_bounds__(NTH, 4) rev_str(RevArgs A)
             }
             const int c = (lz + M) * HX + lx + M;
             const float dvx_dx = dmx(tvx, c, G.idx);
-            const float dvz_dz = dmz(tvz, c, G.idz);
-            const float dvx_dz = dpz(tvx, c, G.idz);
+            const float dvz_dz = dmz_fs<FS>(G, tvz, c, iz, G.idz);
+            const float dvx_dz = dpz_fs<FS>(G, tvx, c, iz, G.idz);
             const float dvz_dx = dpx(tvz, c, G.idx);
             if (in_recon(G, ix, iz)) {
                 float sxx = A.f[SXX][so + i], szz = A.f[SZZ][so + i], sxz = A.f[SXZ][so + i];
@@ -805,11 +884,23 @@ __global__ void __launch_bounds__(NTH, 4) rev_str(RevArgs A)
                 }
             }
             if (in_box(G, ix, iz)) {
-                const float bsxx = A.a[SXX][so + i], bszz = A.a[SZZ][so + i], bsxz = A.a[SXZ][so + i];
-                float gl = (bsxx + bszz) * (dvx_dx + dvz_dz);
-                float gm = 2.f * (bsxx * dvx_dx + bszz * dvz_dz);
-                gm += bsxz * (dvx_dz + dvz_dx);
+                const bool surf = FS && iz == G.z0;
+                const float bsxx = A.a[SXX][so + i], bsxz = A.a[SXZ][so + i];
+                const float bszz = surf ? 0.f : A.a[SZZ][so + i];   // zeroed on the surface row
                 const float rho = rho_[i], vp = vp_[i], vs = vs_[i];
+                float gl, gm;
+                if (surf) {
+                    // d / d(lam, mu) of the corrected surface update dt C dvx_dx,
+                    // C = 4 mu (lam + mu) / (lam + 2 mu) (kernels.cuh:633-646)
+                    const float vp2 = vp * vp, vs2 = vs * vs, vp4 = vp2 * vp2;
+                    const float a = bsxx * dvx_dx;
+                    gl = a * 4.f * vs2 * vs2 / vp4;
+                    gm = a * 4.f * (vp4 - 2.f * vp2 * vs2 + 2.f * vs2 * vs2) / vp4;
+                } else {
+                    gl = (bsxx + bszz) * (dvx_dx + dvz_dz);
+                    gm = 2.f * (bsxx * dvx_dx + bszz * dvz_dz);
+                }
+                gm += bsxz * (dvx_dz + dvz_dx);
                 gvp[r] += -2.f * rho * vp * gl * G.dt;
                 gvs[r] += -(-4.f * rho * vs * gl + 2.f * rho * vs * gm) * G.dt;
                 float gr = (A.a[VX][so + i] * (tvx[c] - A.cvx[so + i]) + A.a[VZ][so + i] * (tvz[c] - A.cvz[so + i])) / rho;
@@ -867,6 +958,7 @@ __device__ __forceinline__ bool owns(int lz, int lx)
 // qxz, qzx) of the stress-adjoint prepare (kernels.cuh:676-750) built in
 // shared memory for the tile and its halo.  The owner of a cell writes its new
 // adjoint CPML memories.
+template <bool FS>
 __global__ void __launch_bounds__(NTH, 4) rev_sadj(RevArgs A)
 {
     extern __shared__ float sm[];
@@ -908,8 +1000,15 @@ __global__ void __launch_bounds__(NTH, 4) rev_sadj(RevArgs A)
         const int lz = k / HX, lx = k - lz * HX;
         const int iz = tz0 - M + lz, ix = tx0 - M + lx;
         const float bsxx = rs[j][0], bszz = rs[j][1], bsxz = rs[j][2], lam = rs[j][3], mu = rs[j][4];
-        float q0 = G.dt * ((lam + 2.f * mu) * bsxx + lam * bszz);
-        float q1 = G.dt * ((lam + 2.f * mu) * bszz + lam * bsxx);
+        float q0, q1;
+        if (FS && iz == G.z0 && (unsigned)ix < (unsigned)G.nx) {
+            // surface row: szz zeroed, transpose of the corrected sxx update
+            q0 = G.dt * (4.f * mu * (lam + mu) / (lam + 2.f * mu)) * bsxx;
+            q1 = 0.f;
+        } else {
+            q0 = G.dt * ((lam + 2.f * mu) * bsxx + lam * bszz);
+            q1 = G.dt * ((lam + 2.f * mu) * bszz + lam * bsxx);
+        }
         float q2 = G.dt * mu * bsxz;
         float q3 = G.dt * mu * bsxz;
         if ((unsigned)iz < (unsigned)G.nz && (unsigned)ix < (unsigned)G.nx && in_pml(G, ix, iz)) {
@@ -946,8 +1045,8 @@ __global__ void __launch_bounds__(NTH, 4) rev_sadj(RevArgs A)
         if (!in_core(G, ix, iz)) continue;
         const int c = (lz + M) * HX + lx + M;
         const long long i = so + (long long)iz * G.P + ix;
-        A.a[VX][i] += dpx(tq[0], c, G.idx) + dmz(tq[2], c, G.idz);
-        A.a[VZ][i] += dmx(tq[3], c, G.idx) + dpz(tq[1], c, G.idz);
+        A.a[VX][i] += dpx(tq[0], c, G.idx) + adj_dpz_fs<FS>(G, tq[2], c, iz, G.idz);
+        A.a[VZ][i] += dmx(tq[3], c, G.idx) + adj_dmz_fs<FS>(G, tq[1], c, iz, G.idz);
     }
 }
 
@@ -956,6 +1055,7 @@ __global__ void __launch_bounds__(NTH, 4) rev_sadj(RevArgs A)
 // in shared memory, then the reverse velocity half of the forward
 // reconstruction: carrier capture of v(it) on the box, the NOPML velocity
 // step (kernels.cuh:365-401) and the velocity strip restore of step it - 1.
+template <bool FS>
 __global__ void __launch_bounds__(NTH, 4) rev_vadj(RevArgs A)
 {
     extern __shared__ float sm[];
@@ -1039,16 +1139,18 @@ __global__ void __launch_bounds__(NTH, 4) rev_vadj(RevArgs A)
         const int c = (lz + M) * HX + lx + M;
         const long long i = (long long)iz * G.P + ix;
         A.a[SXX][so + i] += dmx(tp[0], c, G.idx);
-        A.a[SZZ][so + i] += dmz(tp[1], c, G.idz);
-        A.a[SXZ][so + i] += dpz(tp[2], c, G.idz) + dpx(tp[3], c, G.idx);
+        // the surface row's adjoint szz was zeroed by this step's stress half
+        const float szz0 = FS && iz == G.z0 ? 0.f : A.a[SZZ][so + i];
+        A.a[SZZ][so + i] = szz0 + adj_dpz_fs<FS>(G, tp[1], c, iz, G.idz);
+        A.a[SXZ][so + i] += adj_dmz_fs<FS>(G, tp[2], c, iz, G.idz) + dpx(tp[3], c, G.idx);
         if (!in_box(G, ix, iz)) continue;
         const float vx = A.f[VX][so + i], vz = A.f[VZ][so + i];
         A.cvx[so + i] = vx;
         A.cvz[so + i] = vz;
         if (in_recon(G, ix, iz)) {
             const float k_ = bv_[i];
-            A.f[VX][so + i] = vx - k_ * (dpx(tsxx, c, G.idx) + dmz(tsxz, c, G.idz));
-            A.f[VZ][so + i] = vz - k_ * (dmx(tsxz, c, G.idx) + dpz(tszz, c, G.idz));
+            A.f[VX][so + i] = vx - k_ * (dpx(tsxx, c, G.idx) + dmz_fs<FS>(G, tsxz, c, iz, G.idz));
+            A.f[VZ][so + i] = vz - k_ * (dmx(tsxz, c, G.idx) + dpz_fs<FS>(G, tszz, c, iz, G.idz));
         }
     }
     // strips (box ring and the M cells outside it) of step it - 1
@@ -1187,10 +1289,18 @@ static Plan make_plan(const sweep_elastic_desc* d)
     SWEEP_REQUIRE(d->nrec_fields >= 1 && d->nrec_fields <= 5, "elastic2d: 1 to 5 receiver fields (got %d)", d->nrec_fields);
     for (int k = 0; k < d->nrec_fields; ++k)
         SWEEP_REQUIRE(d->rec_fields[k] >= 0 && d->rec_fields[k] <= SXZ, "elastic2d: bad receiver field %d", d->rec_fields[k]);
-    for (int f = 0; f < 4; ++f)
-        SWEEP_REQUIRE(d->pad[f] >= 1, "elastic2d: every face needs a PML pad >= 1 (face %d has %d)", f, d->pad[f]);
+    for (int f = 1; f < 4; ++f)
+        SWEEP_REQUIRE(!d->free_surface[f], "elastic2d: a traction-free face is built on the top face only (face %d)", f);
+    for (int f = 0; f < 4; ++f) {
+        if (f == 0 && d->free_surface[0])
+            SWEEP_REQUIRE(d->pad[0] == 0, "elastic2d: a free top face has no PML pad (got %d)", d->pad[0]);
+        else
+            SWEEP_REQUIRE(d->pad[f] >= 1, "elastic2d: every absorbing face needs a PML pad >= 1 (face %d has %d)", f,
+                          d->pad[f]);
+    }
     Plan pl{};
     Geo& G = pl.G;
+    G.fst = d->free_surface[0] ? 1 : 0;
     G.B = d->B; G.nz = d->nz; G.nx = d->nx; G.nt = d->nt;
     G.P = (d->nx + 31) / 32 * 32;
     G.S = (long long)d->nz * G.P;
@@ -1530,8 +1640,10 @@ static void set_attrs()
 {
     static bool done = false;
     if (done) return;
-    SWEEP_CUDA(cudaFuncSetAttribute(fwd_vel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_FWD_VEL));
-    SWEEP_CUDA(cudaFuncSetAttribute(fwd_str, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_FWD_STR));
+    SWEEP_CUDA(cudaFuncSetAttribute(fwd_vel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_FWD_VEL));
+    SWEEP_CUDA(cudaFuncSetAttribute(fwd_str<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_FWD_STR));
+    SWEEP_CUDA(cudaFuncSetAttribute(fwd_vel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_FWD_VEL));
+    SWEEP_CUDA(cudaFuncSetAttribute(fwd_str<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_FWD_STR));
     done = true;
 }
 constexpr size_t SM_REV_STR = 2 * HN * sizeof(float);
@@ -1607,9 +1719,11 @@ static void forward_steps(FwdArgs& A, int it0, int it1, StripsOf strips_of, floa
         void* slot = strips_of(it);
         A.strips = (slot && scaled) ? static_cast<void*>(scratch) : slot;
         const cudaStream_t ls = gs.stream();
-        fwd_vel<<<grid, block, SM_FWD_VEL, ls>>>(maps, A);
+        if (G.fst) fwd_vel<true><<<grid, block, SM_FWD_VEL, ls>>>(maps, A);
+        else fwd_vel<false><<<grid, block, SM_FWD_VEL, ls>>>(maps, A);
         if (slot && hr) hr->before_write(it);
-        fwd_str<<<grid, block, SM_FWD_STR, ls>>>(maps, A);
+        if (G.fst) fwd_str<true><<<grid, block, SM_FWD_STR, ls>>>(maps, A);
+        else fwd_str<false><<<grid, block, SM_FWD_STR, ls>>>(maps, A);
         if (G.nvf) vsrc_forward<<<G.B, 128, 0, ls>>>(G, A.f[VX], A.f[VZ], A.strips, A.record, it);
         if (slot && scaled) quantize_strips<<<qblocks, kQB, 0, ls>>>(G, scratch, slot);
         if (slot && hr) hr->after_write(it);
@@ -1745,9 +1859,15 @@ static void backward_with(const sweep_elastic_desc* d, int mem_mode, int ckpt_ev
             const cudaStream_t ls = gs.stream();
             if (G.nvf)
                 vsrc_reverse<<<G.B, 128, 0, ls>>>(G, A.a[VX], A.a[VZ], A.f[VX], A.f[VZ], A.grho, A.m.rho, A.G_shots, it);
-            rev_str<<<grid_s, block, SM_REV_STR, ls>>>(A);
-            rev_sadj<<<grid_b, block, SM_REV_SADJ, ls>>>(A);
-            rev_vadj<<<grid_b, block, SM_REV_VADJ, ls>>>(A);
+            if (G.fst) {
+                rev_str<true><<<grid_s, block, SM_REV_STR, ls>>>(A);
+                rev_sadj<true><<<grid_b, block, SM_REV_SADJ, ls>>>(A);
+                rev_vadj<true><<<grid_b, block, SM_REV_VADJ, ls>>>(A);
+            } else {
+                rev_str<false><<<grid_s, block, SM_REV_STR, ls>>>(A);
+                rev_sadj<false><<<grid_b, block, SM_REV_SADJ, ls>>>(A);
+                rev_vadj<false><<<grid_b, block, SM_REV_VADJ, ls>>>(A);
+            }
             if (host) {
                 hr.after_read(it - 1);
                 if (it - 1 - HostRing::R >= std::max(it0 - 1, 0)) hr.fetch(it - 1 - HostRing::R, true);

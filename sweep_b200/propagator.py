@@ -13,9 +13,10 @@ acoustic equations, the wavelet's) gradients through a
 Host-side conventions restated from the reference:
 * runtime grid = physical + ``abcn`` PML cells + ``M = so/2`` halo per face
   (``core/geometry.py:23-58``); coordinates shift by ``abcn + M``
-  (``_c.py:2196-2207``); ``free_surface=True`` (acoustic) drops the top
-  face's PML cells, so the surface row sits M cells from the grid's top and
-  the halo rows above it stay at zero pressure;
+  (``_c.py:2196-2207``); ``free_surface=True`` drops the top face's PML
+  cells, so the surface row sits M cells from the grid's top; acoustic keeps
+  the halo rows above it at zero pressure, elastic makes the face traction
+  free by the image method (``common/elastic_free_surface.cuh``);
 * models are replicate-padded to the runtime grid and the gradient cropped back
   (``utils/torch.py:8-41``); a shared model is used by every shot and its
   gradient summed over shots (``_c.py:2110-2155``);
@@ -130,6 +131,16 @@ class _Geometry:
         else:
             prof = cpml_profiles_r(pads, self.M, prop.dt, self.spacing, self.shape, max_vel, pml_freq)
         self.prof = [[torch.from_numpy(np.ascontiguousarray(a)).to(device) for a in p] for p in prof]
+        # Elastic with a free top face: the rows above the surface are air,
+        # which the image method overwrites, so a source or receiver there is
+        # off the grid (the reference would fold its adjoint back through the
+        # images of the air rows)
+        self.fs_top = isinstance(eq, Elastic) and bool(prop.fs_faces[0])
+        if self.fs_top:
+            src_rt, rec_rt = np.array(src_rt, np.int64), np.array(rec_rt, np.int64)
+            for loc in (src_rt, rec_rt):
+                air = loc[..., 1] < self.M
+                loc[air] = -(1 << 20)
         self.src = torch.from_numpy(np.ascontiguousarray(src_rt, dtype=np.int32)).to(device)
         self.rec = torch.from_numpy(np.ascontiguousarray(rec_rt, dtype=np.int32)).to(device)
         self.pads = list(prop.pads)          # per face in shape order: lo, hi per axis
@@ -204,6 +215,7 @@ class _Geometry:
         d.nrec_fields = len(rec_fields)
         for k, f in enumerate(rec_fields):
             d.rec_fields[k] = f
+        d.free_surface[0] = 1 if self.fs_top else 0
         return d
 
 
@@ -359,8 +371,9 @@ class PropTorch(torch.nn.Module):
         if self.abcn < 1:
             raise NotImplementedError("sweep_b200: the absorbing faces need a layer (abcn >= 1)")
         self.fs_faces = free_faces(free_surface, nd)
-        if any(self.fs_faces) and isinstance(equation, Elastic):
-            raise NotImplementedError("sweep_b200: an Elastic free surface (image method) is not built")
+        if any(self.fs_faces[1:]) and isinstance(equation, Elastic):
+            raise NotImplementedError("sweep_b200: an Elastic free surface is built on the top face only "
+                                      "(free_surface=True); the bottom / left / right image faces are not")
         if nd == 3 and any(self.fs_faces[1:]):
             raise NotImplementedError("per-face free surfaces are 2-D only (as in the reference); "
                                       "3-D takes free_surface=True (the top face)")

@@ -342,3 +342,31 @@ def test_recursive_sizes_every_equation():
         assert ws4.value > ws1.value > ws_bs.value
         with pytest.raises(RuntimeError, match="host tape"):
             _lib.call(name, d, _lib.MEM_RECURSIVE | _lib.MEM_HOST_TAPE, 2, ws1, tape)
+
+
+def test_elastic_free_surface_faces_checked():
+    """The elastic core takes a traction-free top face with no pad there and
+    refuses the other faces (host-side checks, no device work); the public
+    API refuses them before the core is reached."""
+    from sweep_b200 import Elastic, PropTorch, _lib
+    e = _lib.ElasticDesc()
+    e.B, e.nz, e.nx, e.nt, e.M = 2, 60, 80, 10, 4
+    e.pad[0], e.pad[1], e.pad[2], e.pad[3] = 0, 10, 10, 10
+    e.nsrc_fields, e.src_fields[0], e.nrec_fields = 1, 2, 1
+    ws, tape = _lib.c_i64(), _lib.c_i64()
+    with pytest.raises(RuntimeError, match="pad"):
+        _lib.call("sweep_b200_elastic_sizes", e, _lib.MEM_BOUNDARY, 0, ws, tape)
+    e.free_surface[0] = 1
+    _lib.call("sweep_b200_elastic_sizes", e, _lib.MEM_BOUNDARY, 0, ws, tape)
+    assert ws.value > 0 and tape.value > 0
+    e.pad[0] = 3
+    with pytest.raises(RuntimeError, match="free top face"):
+        _lib.call("sweep_b200_elastic_sizes", e, _lib.MEM_BOUNDARY, 0, ws, tape)
+    e.pad[0], e.free_surface[2] = 0, 1
+    with pytest.raises(RuntimeError, match="top face only"):
+        _lib.call("sweep_b200_elastic_sizes", e, _lib.MEM_BOUNDARY, 0, ws, tape)
+    eq = Elastic(spatial_order=8, device="cpu")
+    s = PropTorch(eq, shape=(30, 40), dh=5.0, dt=0.0005, abcn=8, device="cpu", free_surface=True)
+    assert s.pads == [0, 8, 8, 8] and s.runtime_shape == (30 + 8 + 8, 40 + 16 + 8)
+    with pytest.raises(NotImplementedError, match="top face only"):
+        PropTorch(eq, shape=(30, 40), dh=5.0, dt=0.0005, abcn=8, device="cpu", free_surface=["left"])
