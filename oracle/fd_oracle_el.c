@@ -65,7 +65,7 @@ typedef struct {
     i64 ms;                     /* model stride between shots (0 = shared) */
     int nsrc; const int* src; const REAL* wavelet; int nsf; const int* sf;
     int nrec; const int* rec; int nrf; const int* rf;
-    int fs;                     /* bit 0: traction-free top face (pad[0] == 0) */
+    int fs;                     /* bit f: traction-free face f (z_lo, z_hi, x_lo, x_hi; pad 0) */
 } EL;
 
 /* D+ along stride s: sum_k c_k (u[i+k s] - u[i-(k-1) s]) * (1/h). */
@@ -86,89 +86,159 @@ static inline REAL dminus(const REAL* u, i64 i, i64 s, int M, const REAL* c, REA
 
 static int in_grid(int ix, int iz, int nx, int nz) { return ix >= 0 && ix < nx && iz >= 0 && iz < nz; }
 
-/* ---- traction-free top face (image method) -------------------------------
- * The surface is the first physical row, top = pad[0] + M = M (a free face
- * has no PML pad); rows above it are air.  z-derivatives read an air row as
- * the image of the row mirrored about the surface: about `top` for fields on
- * integer rows (szz, vx), about top - 1/2 for fields half a cell below them
- * (sxz, vz), negated for the odd fields.  The M rows from the surface down
- * take a 2nd-order (unit-weight) difference instead of the full stencil. */
-static inline int fs_top_row(const EL* p) { return p->pad[0] + p->M; }
+/* ---- traction-free faces (image method) ---------------------------------
+ * Bit f of `fs` (0 z_lo, 1 z_hi, 2 x_lo, 3 x_hi) makes face f traction free;
+ * a free face has no PML pad.  Per axis (0 = z, 1 = x) the low surface is the
+ * first physical row / column and the high surface the last; the cells past
+ * them are air.  Derivatives along the axis read an air cell as the image of
+ * the cell mirrored about the surface -- about the surface node for fields
+ * on integer nodes, about the half cell next to it for fields half a cell
+ * along the axis ("half") -- negated for odd fields.  On the high side a
+ * half field's surface node is itself air.  The M cells from a surface
+ * inwards take a unit-weight 2nd-order difference instead of the full
+ * stencil.  (elastic_free_surface.cuh:200-465, 466-720.) */
+typedef struct { int lo_on, hi_on, lo, hi, n, M; i64 s; REAL h; } FSAX;
 
-static inline REAL fs_at(const EL* p, const REAL* u, int ix, int iz, int odd, int half)
+static FSAX fs_axis(const EL* p, int a)
 {
-    const int top = fs_top_row(p);
-    if (iz < top) {
-        const int m = half ? 2 * top - 1 - iz : 2 * top - iz;
-        const REAL v = u[(i64)m * p->nx + ix];
-        return odd ? -v : v;
+    FSAX x;
+    x.M = p->M;
+    if (a == 0) {
+        x.lo_on = p->fs & 1; x.hi_on = (p->fs >> 1) & 1;
+        x.lo = p->pad[0] + p->M; x.hi = p->nz - p->pad[1] - p->M - 1;
+        x.n = p->nz; x.s = p->nx; x.h = p->dz;
+    } else {
+        x.lo_on = (p->fs >> 2) & 1; x.hi_on = (p->fs >> 3) & 1;
+        x.lo = p->pad[2] + p->M; x.hi = p->nx - p->pad[3] - p->M - 1;
+        x.n = p->nx; x.s = 1; x.h = p->dx;
     }
-    return u[(i64)iz * p->nx + ix];
+    return x;
 }
 
-/* z-derivative at (ix, iz) on a free top face: fwd = 1 the D+ form (taps
- * iz+k and iz-k+1), fwd = 0 the D- form (taps iz+k-1 and iz-k). */
-static REAL fs_dz(const EL* p, const REAL* u, int ix, int iz, int fwd, int odd, int half)
+/* u at index j along the axis of the line through `base` (index 0) */
+static inline REAL fs_at(const FSAX* x, const REAL* u, i64 base, int j, int odd, int half)
 {
-    const int top = fs_top_row(p), M = p->M;
-    if (iz - top >= 0 && iz - top < M) {
-        const REAL g = fwd ? fs_at(p, u, ix, iz + 1, odd, half) - fs_at(p, u, ix, iz, odd, half)
-                           : fs_at(p, u, ix, iz, odd, half) - fs_at(p, u, ix, iz - 1, odd, half);
-        return g / p->dz;
+    int m;
+    if (x->lo_on && j < x->lo) m = half ? 2 * x->lo - 1 - j : 2 * x->lo - j;
+    else if (x->hi_on && j >= (half ? x->hi : x->hi + 1)) m = half ? 2 * x->hi - 1 - j : 2 * x->hi - j;
+    else return u[base + (i64)j * x->s];
+    const REAL v = u[base + (i64)m * x->s];
+    return odd ? -v : v;
+}
+
+static inline int fs_band(const FSAX* x, int j)
+{
+    return (x->lo_on && j >= x->lo && j < x->lo + x->M) || (x->hi_on && j > x->hi - x->M && j <= x->hi);
+}
+
+/* Derivative along axis a at (ix, iz): fwd = 1 the D+ form (taps j+k and
+ * j-k+1), fwd = 0 the D- form (taps j+k-1 and j-k); the plain stencil when
+ * neither face of the axis is free. */
+static REAL fs_d(const EL* p, const REAL* u, int a, int ix, int iz, int fwd, int odd, int half)
+{
+    const FSAX x = fs_axis(p, a);
+    const int M = p->M;
+    const i64 i = (i64)iz * p->nx + ix;
+    if (!x.lo_on && !x.hi_on)
+        return fwd ? dplus(u, i, x.s, M, p->c, R(1) / x.h) : dminus(u, i, x.s, M, p->c, R(1) / x.h);
+    const int j = a == 0 ? iz : ix;
+    const i64 base = i - (i64)j * x.s;
+    if (fs_band(&x, j)) {
+        const REAL g = fwd ? fs_at(&x, u, base, j + 1, odd, half) - fs_at(&x, u, base, j, odd, half)
+                           : fs_at(&x, u, base, j, odd, half) - fs_at(&x, u, base, j - 1, odd, half);
+        return g / x.h;
     }
     REAL g = R(0);
     for (int k = 1; k <= M; ++k) {
-        const REAL up = fwd ? fs_at(p, u, ix, iz + k, odd, half) : fs_at(p, u, ix, iz + k - 1, odd, half);
-        const REAL um = fwd ? fs_at(p, u, ix, iz - k + 1, odd, half) : fs_at(p, u, ix, iz - k, odd, half);
+        const REAL up = fwd ? fs_at(&x, u, base, j + k, odd, half) : fs_at(&x, u, base, j + k - 1, odd, half);
+        const REAL um = fwd ? fs_at(&x, u, base, j - k + 1, odd, half) : fs_at(&x, u, base, j - k, odd, half);
         g = g + p->c[k] * (up - um);
     }
-    return g / p->dz;
+    return g / x.h;
 }
 
-static inline int fs_band(const EL* p, int j)
-{
-    const int top = fs_top_row(p);
-    return j >= top && j < top + p->M;
-}
-
-/* Transpose of fs_dz without the image (negated, in the sign convention of
+/* Transpose of fs_d without the images (negated, in the sign convention of
  * the plain adjoint stencils: D- for a D+ forward and vice versa) at input
- * row m: each output row j contributes with the full weight if it lies below
- * the order-2 band, with weight 1 if it lies in it; reads outside the grid
- * are skipped. */
-static REAL fs_adj_plain(const EL* p, const REAL* q, int ix, int m, int fwd)
+ * index m: an output cell in a band contributes with weight 1, one outside
+ * with the full weight; reads outside the grid are skipped. */
+static REAL fs_adj_plain(const FSAX* x, const REAL* c, const REAL* q, i64 base, int m, int fwd)
 {
-    const int M = p->M, nz = p->nz, nx = p->nx;
     REAL acc = R(0);
-    for (int k = 1; k <= M; ++k) {
+    for (int k = 1; k <= x->M; ++k) {
         const int jp = fwd ? m + k - 1 : m + k;
         const int jm = fwd ? m - k : m - k + 1;
-        if (jp >= 0 && jp < nz && !fs_band(p, jp)) acc = acc + p->c[k] * q[(i64)jp * nx + ix];
-        if (jm >= 0 && jm < nz && !fs_band(p, jm)) acc = acc - p->c[k] * q[(i64)jm * nx + ix];
+        if (jp >= 0 && jp < x->n && !fs_band(x, jp)) acc = acc + c[k] * q[base + (i64)jp * x->s];
+        if (jm >= 0 && jm < x->n && !fs_band(x, jm)) acc = acc - c[k] * q[base + (i64)jm * x->s];
     }
     if (fwd) {
-        if (fs_band(p, m)) acc = acc + q[(i64)m * nx + ix];
-        if (fs_band(p, m - 1)) acc = acc - q[(i64)(m - 1) * nx + ix];
+        if (fs_band(x, m)) acc = acc + q[base + (i64)m * x->s];
+        if (fs_band(x, m - 1)) acc = acc - q[base + (i64)(m - 1) * x->s];
     } else {
-        if (fs_band(p, m + 1)) acc = acc + q[(i64)(m + 1) * nx + ix];
-        if (fs_band(p, m)) acc = acc - q[(i64)m * nx + ix];
+        if (fs_band(x, m + 1)) acc = acc + q[base + (i64)(m + 1) * x->s];
+        if (fs_band(x, m)) acc = acc - q[base + (i64)m * x->s];
     }
-    return acc / p->dz;
+    return acc / x->h;
 }
 
-/* Adjoint of fs_dz at row iz: zero on air rows (the forward overwrites them
- * with images); else the plain transpose plus, where the row's mirror lies in
- * the air, the transpose at that air row folded back with the field's
- * parity. */
-static REAL fs_adj_dz(const EL* p, const REAL* q, int ix, int iz, int fwd, int odd, int half)
+/* Adjoint of fs_d at (ix, iz): zero on air cells (the forward overwrites them
+ * with images); else the plain transpose plus, for each free face whose image
+ * of this cell lies in the air, the transpose at that air cell folded back
+ * with the field's parity. */
+static REAL fs_adj(const EL* p, const REAL* q, int a, int ix, int iz, int fwd, int odd, int half)
 {
-    const int top = fs_top_row(p);
-    if (iz < top) return R(0);
-    REAL g = fs_adj_plain(p, q, ix, iz, fwd);
-    const int miz = half ? 2 * top - 1 - iz : 2 * top - iz;
-    if (miz < top) g = g + (odd ? R(-1) : R(1)) * fs_adj_plain(p, q, ix, miz, fwd);
+    const FSAX x = fs_axis(p, a);
+    const int M = p->M;
+    const i64 i = (i64)iz * p->nx + ix;
+    if (!x.lo_on && !x.hi_on)
+        return fwd ? dminus(q, i, x.s, M, p->c, R(1) / x.h) : dplus(q, i, x.s, M, p->c, R(1) / x.h);
+    const int j = a == 0 ? iz : ix;
+    const i64 base = i - (i64)j * x.s;
+    if ((x.lo_on && j < x.lo) || (x.hi_on && j > x.hi)) return R(0);
+    const REAL parity = odd ? R(-1) : R(1);
+    REAL g = fs_adj_plain(&x, p->c, q, base, j, fwd);
+    if (x.lo_on) {
+        const int mj = half ? 2 * x.lo - 1 - j : 2 * x.lo - j;
+        if (mj < x.lo) g = g + parity * fs_adj_plain(&x, p->c, q, base, mj, fwd);
+    }
+    if (x.hi_on) {
+        const int mj = half ? 2 * x.hi - 1 - j : 2 * x.hi - j;
+        if (mj >= (half ? x.hi : x.hi + 1)) g = g + parity * fs_adj_plain(&x, p->c, q, base, mj, fwd);
+    }
     return g;
 }
+
+/* Surface rows / columns: the normal-stress conditions (z row: Robertsson
+ * sxx, szz = 0; x column: Robertsson szz, sxx = 0) and the shear zeroing of
+ * the high-side faces (kernels.cuh:293-303, elastic_free_surface.cuh:485-500). */
+static inline int fs_zrow(const EL* p, int iz)
+{
+    return ((p->fs & 1) && iz == p->pad[0] + p->M) || ((p->fs & 2) && iz == p->nz - p->pad[1] - p->M - 1);
+}
+static inline int fs_xcol(const EL* p, int ix)
+{
+    return ((p->fs & 4) && ix == p->pad[2] + p->M) || ((p->fs & 8) && ix == p->nx - p->pad[3] - p->M - 1);
+}
+static inline int fs_zero_shear(const EL* p, int ix, int iz)
+{
+    return ((p->fs & 2) && iz == p->nz - p->pad[1] - p->M - 1) || ((p->fs & 8) && ix == p->nx - p->pad[3] - p->M - 1);
+}
+
+/* The stress kernel's CPML test: a free surface row / column stays in the
+ * CPML branch (kernels.cuh:216-234). */
+static inline int in_pml_stress(const EL* p, int ix, int iz)
+{
+    const int M = p->M;
+    const int zlo = (p->fs & 1) ? p->pad[0] + M + 1 : p->pad[0] + M;
+    const int zhi = (p->fs & 2) ? p->nz - p->pad[1] - M - 1 : p->nz - p->pad[1] - M;
+    const int xlo = (p->fs & 4) ? p->pad[2] + M + 1 : p->pad[2] + M;
+    const int xhi = (p->fs & 8) ? p->nx - p->pad[3] - M - 1 : p->nx - p->pad[3] - M;
+    return ix < xlo || ix >= xhi || iz < zlo || iz >= zhi;
+}
+
+#define DZ(u, fwd, odd, half) fs_d(p, (u), 0, ix, iz, (fwd), (odd), (half))
+#define DX(u, fwd, odd, half) fs_d(p, (u), 1, ix, iz, (fwd), (odd), (half))
+#define AZ(q, fwd, odd, half) fs_adj(p, (q), 0, ix, iz, (fwd), (odd), (half))
+#define AX(q, fwd, odd, half) fs_adj(p, (q), 1, ix, iz, (fwd), (odd), (half))
 
 /* CPML test shared by the velocity step, the stress step (no free surface)
  * and both adjoint prepares: the PML pad plus the stencil halo, per face. */
@@ -196,15 +266,14 @@ static void velocity_step(const EL* p, int b, REAL** F)
 {
     const int nz = p->nz, nx = p->nx, M = p->M;
     const REAL* rho = p->rho + b * p->ms;
-    const REAL ix_ = R(1) / p->dx, iz_ = R(1) / p->dz;
     #pragma omp parallel for schedule(static)
     for (int iz = M; iz < nz - M; ++iz) {
         for (int ix = M; ix < nx - M; ++ix) {
             const i64 i = (i64)iz * nx + ix;
-            REAL dsxx_dx = dplus(F[SXX], i, 1, M, p->c, ix_);
-            REAL dsxz_dz = p->fs ? fs_dz(p, F[SXZ], ix, iz, 0, 1, 1) : dminus(F[SXZ], i, nx, M, p->c, iz_);
-            REAL dsxz_dx = dminus(F[SXZ], i, 1, M, p->c, ix_);
-            REAL dszz_dz = p->fs ? fs_dz(p, F[SZZ], ix, iz, 1, 1, 0) : dplus(F[SZZ], i, nx, M, p->c, iz_);
+            REAL dsxx_dx = DX(F[SXX], 1, 1, 0);
+            REAL dsxz_dz = DZ(F[SXZ], 0, 1, 1);
+            REAL dsxz_dx = DX(F[SXZ], 0, 1, 1);
+            REAL dszz_dz = DZ(F[SZZ], 1, 1, 0);
             REAL inv_rho = R(1) / rho[i];
             if (in_pml(p, ix, iz)) {
                 REAL m;
@@ -222,19 +291,16 @@ static void velocity_step(const EL* p, int b, REAL** F)
 static void stress_step(const EL* p, REAL** F, const REAL* lam_, const REAL* mu_)
 {
     const int nz = p->nz, nx = p->nx, M = p->M;
-    const REAL ix_ = R(1) / p->dx, iz_ = R(1) / p->dz;
     #pragma omp parallel for schedule(static)
     for (int iz = M; iz < nz - M; ++iz) {
         for (int ix = M; ix < nx - M; ++ix) {
             const i64 i = (i64)iz * nx + ix;
-            REAL dvx_dx = dminus(F[VX], i, 1, M, p->c, ix_);
-            REAL dvz_dz = p->fs ? fs_dz(p, F[VZ], ix, iz, 0, 1, 1) : dminus(F[VZ], i, nx, M, p->c, iz_);
-            REAL dvx_dz = p->fs ? fs_dz(p, F[VX], ix, iz, 1, 0, 0) : dplus(F[VX], i, nx, M, p->c, iz_);
-            REAL dvz_dx = dplus(F[VZ], i, 1, M, p->c, ix_);
+            REAL dvx_dx = DX(F[VX], 0, 1, 1);
+            REAL dvz_dz = DZ(F[VZ], 0, 1, 1);
+            REAL dvx_dz = DZ(F[VX], 1, 0, 0);
+            REAL dvz_dx = DX(F[VZ], 1, 0, 0);
             REAL lam = lam_[i], mu = mu_[i];
-            /* a free surface row takes the CPML branch (kernels.cuh:216-234) */
-            const int surf = p->fs && iz == fs_top_row(p);
-            const int pml = in_pml(p, ix, iz) || surf;
+            const int pml = in_pml_stress(p, ix, iz);
             if (pml) {
                 REAL m;
                 m = p->az[iz] * F[M_VZZ][i] + p->bz[iz] * dvz_dz; F[M_VZZ][i] = m; dvz_dz = dvz_dz + m;
@@ -248,10 +314,13 @@ static void stress_step(const EL* p, REAL** F, const REAL* lam_, const REAL* mu_
                 m = p->axh[ix] * F[M_VZX][i] + p->bxh[ix] * dvz_dx; F[M_VZX][i] = m; dvz_dx = dvz_dx + m;
             }
             F[SXZ][i] = F[SXZ][i] + (p->dt * mu) * (dvx_dz + dvz_dx);
-            if (surf) {   /* Robertsson correction, then szz = 0 (kernels.cuh:293-303) */
-                F[SXX][i] = F[SXX][i] + (-p->dt) * lam * ((lam / (lam + R(2) * mu)) * dvx_dx + dvz_dz);
-                F[SZZ][i] = R(0);
-            }
+            /* Robertsson corrections first, then the zeroing (kernels.cuh:293-303) */
+            const int zs = fs_zrow(p, iz), xs = fs_xcol(p, ix);
+            if (zs) F[SXX][i] = F[SXX][i] + (-p->dt) * lam * ((lam / (lam + R(2) * mu)) * dvx_dx + dvz_dz);
+            if (xs) F[SZZ][i] = F[SZZ][i] + (-p->dt) * lam * ((lam / (lam + R(2) * mu)) * dvz_dz + dvx_dx);
+            if (zs) F[SZZ][i] = R(0);
+            if (xs) F[SXX][i] = R(0);
+            if (fs_zero_shear(p, ix, iz)) F[SXZ][i] = R(0);
         }
     }
 }
@@ -350,20 +419,30 @@ int oracle_el2d_forward(
 }
 
 /* Reverse (NOPML) stress and velocity steps on the box minus one cell per
- * face (kernels.cuh:405-535, band pad + M + 1). */
+ * face (kernels.cuh:405-535, band pad + M + 1); a free face narrows to the
+ * halo M. */
+static void reverse_box(const EL* p, int lo[2], int hi[2])
+{
+    const int M = p->M;
+    lo[0] = (p->fs & 1) ? M : p->pad[0] + M + 1;
+    hi[0] = p->nz - ((p->fs & 2) ? M : p->pad[1] + M + 1);
+    lo[1] = (p->fs & 4) ? M : p->pad[2] + M + 1;
+    hi[1] = p->nx - ((p->fs & 8) ? M : p->pad[3] + M + 1);
+}
+
 static void stress_reverse(const EL* p, REAL** F, const REAL* lam_, const REAL* mu_)
 {
-    const int nz = p->nz, nx = p->nx, M = p->M;
-    const REAL ix_ = R(1) / p->dx, iz_ = R(1) / p->dz;
-    const int zlo = p->fs ? M : p->pad[0] + M + 1;   /* a free face narrows to the halo */
+    const int nx = p->nx;
+    int lo[2], hi[2];
+    reverse_box(p, lo, hi);
     #pragma omp parallel for schedule(static)
-    for (int iz = zlo; iz < nz - (p->pad[1] + M + 1); ++iz) {
-        for (int ix = p->pad[2] + M + 1; ix < nx - (p->pad[3] + M + 1); ++ix) {
+    for (int iz = lo[0]; iz < hi[0]; ++iz) {
+        for (int ix = lo[1]; ix < hi[1]; ++ix) {
             const i64 i = (i64)iz * nx + ix;
-            REAL dvx_dx = dminus(F[VX], i, 1, M, p->c, ix_);
-            REAL dvz_dz = p->fs ? fs_dz(p, F[VZ], ix, iz, 0, 1, 1) : dminus(F[VZ], i, nx, M, p->c, iz_);
-            REAL dvx_dz = p->fs ? fs_dz(p, F[VX], ix, iz, 1, 0, 0) : dplus(F[VX], i, nx, M, p->c, iz_);
-            REAL dvz_dx = dplus(F[VZ], i, 1, M, p->c, ix_);
+            REAL dvx_dx = DX(F[VX], 0, 1, 1);
+            REAL dvz_dz = DZ(F[VZ], 0, 1, 1);
+            REAL dvx_dz = DZ(F[VX], 1, 0, 0);
+            REAL dvz_dx = DX(F[VZ], 1, 0, 0);
             REAL lam = lam_[i], mu = mu_[i];
             F[SXX][i] = F[SXX][i] - p->dt * ((lam + R(2) * mu) * dvx_dx + lam * dvz_dz);
             F[SZZ][i] = F[SZZ][i] - p->dt * ((lam + R(2) * mu) * dvz_dz + lam * dvx_dx);
@@ -374,18 +453,18 @@ static void stress_reverse(const EL* p, REAL** F, const REAL* lam_, const REAL* 
 
 static void velocity_reverse(const EL* p, int b, REAL** F)
 {
-    const int nz = p->nz, nx = p->nx, M = p->M;
+    const int nx = p->nx;
     const REAL* rho = p->rho + b * p->ms;
-    const REAL ix_ = R(1) / p->dx, iz_ = R(1) / p->dz;
-    const int zlo = p->fs ? M : p->pad[0] + M + 1;
+    int lo[2], hi[2];
+    reverse_box(p, lo, hi);
     #pragma omp parallel for schedule(static)
-    for (int iz = zlo; iz < nz - (p->pad[1] + M + 1); ++iz) {
-        for (int ix = p->pad[2] + M + 1; ix < nx - (p->pad[3] + M + 1); ++ix) {
+    for (int iz = lo[0]; iz < hi[0]; ++iz) {
+        for (int ix = lo[1]; ix < hi[1]; ++ix) {
             const i64 i = (i64)iz * nx + ix;
-            REAL dsxx_dx = dplus(F[SXX], i, 1, M, p->c, ix_);
-            REAL dsxz_dz = p->fs ? fs_dz(p, F[SXZ], ix, iz, 0, 1, 1) : dminus(F[SXZ], i, nx, M, p->c, iz_);
-            REAL dsxz_dx = dminus(F[SXZ], i, 1, M, p->c, ix_);
-            REAL dszz_dz = p->fs ? fs_dz(p, F[SZZ], ix, iz, 1, 1, 0) : dplus(F[SZZ], i, nx, M, p->c, iz_);
+            REAL dsxx_dx = DX(F[SXX], 1, 1, 0);
+            REAL dsxz_dz = DZ(F[SXZ], 0, 1, 1);
+            REAL dsxz_dx = DX(F[SXZ], 0, 1, 1);
+            REAL dszz_dz = DZ(F[SZZ], 1, 1, 0);
             REAL inv_rho = R(1) / rho[i];
             F[VX][i] = F[VX][i] - (p->dt * inv_rho) * (dsxx_dx + dsxz_dz);
             F[VZ][i] = F[VZ][i] - (p->dt * inv_rho) * (dsxz_dx + dszz_dz);
@@ -403,26 +482,31 @@ static void stress_adjoint_prepare(const EL* p, int b, REAL** A, REAL** Q, const
     const int nz = p->nz, nx = p->nx, M = p->M;
     const int z0 = p->pad[0] + M, z1 = nz - p->pad[1] - M, x0 = p->pad[2] + M, x1 = nx - p->pad[3] - M;
     const REAL *vp = p->vp + b * p->ms, *vs = p->vs + b * p->ms, *rho = p->rho + b * p->ms;
-    const REAL ix_ = R(1) / p->dx, iz_ = R(1) / p->dz, dt = p->dt;
+    const REAL dt = p->dt;
     #pragma omp parallel for schedule(static)
     for (int iz = 0; iz < nz; ++iz) {
         for (int ix = 0; ix < nx; ++ix) {
             const i64 i = (i64)iz * nx + ix;
             REAL lam = lam_[i], mu = mu_[i];
             REAL bsxx = A[SXX][i], bszz = A[SZZ][i], bsxz = A[SXZ][i];
-            const int surf = p->fs && iz == fs_top_row(p);
-            if (surf) { bszz = R(0); A[SZZ][i] = R(0); }
+            const int zs = fs_zrow(p, iz), xs = fs_xcol(p, ix);
+            if (zs) { bszz = R(0); A[SZZ][i] = R(0); }
+            if (xs) { bsxx = R(0); A[SXX][i] = R(0); }
+            if (fs_zero_shear(p, ix, iz)) { bsxz = R(0); A[SXZ][i] = R(0); }
             if (gvp && ix >= x0 && ix < x1 && iz >= z0 && iz < z1) {
-                REAL fvx_x = dminus(Fw[VX], i, 1, M, p->c, ix_);
-                REAL fvz_z = p->fs ? fs_dz(p, Fw[VZ], ix, iz, 0, 1, 1) : dminus(Fw[VZ], i, nx, M, p->c, iz_);
-                REAL fvx_z = p->fs ? fs_dz(p, Fw[VX], ix, iz, 1, 0, 0) : dplus(Fw[VX], i, nx, M, p->c, iz_);
-                REAL fvz_x = dplus(Fw[VZ], i, 1, M, p->c, ix_);
+                REAL fvx_x = DX(Fw[VX], 0, 1, 1);
+                REAL fvz_z = DZ(Fw[VZ], 0, 1, 1);
+                REAL fvx_z = DZ(Fw[VX], 1, 0, 0);
+                REAL fvz_x = DX(Fw[VZ], 1, 0, 0);
                 REAL gl, gm;
-                if (surf) {
-                    /* d/d(lam, mu) of the surface row's sxx update,
-                     * dt C dvx_dx with C = 4 mu (lam + mu) / (lam + 2 mu) */
+                if (zs && xs) {
+                    gl = R(0); gm = R(0);     /* a corner: every stress zeroed */
+                } else if (zs || xs) {
+                    /* d/d(lam, mu) of the surface update of the tangential
+                     * normal stress, dt C d(tangential v) with
+                     * C = 4 mu (lam + mu) / (lam + 2 mu) (kernels.cuh:633-646) */
                     const REAL vp2 = vp[i] * vp[i], vs2 = vs[i] * vs[i], vp4 = vp2 * vp2;
-                    const REAL a = bsxx * fvx_x;
+                    const REAL a = zs ? bsxx * fvx_x : bszz * fvz_z;
                     gl = a * R(4) * vs2 * vs2 / vp4;
                     gm = a * R(4) * (vp4 - R(2) * vp2 * vs2 + R(2) * vs2 * vs2) / vp4;
                 } else {
@@ -437,10 +521,16 @@ static void stress_adjoint_prepare(const EL* p, int b, REAL** A, REAL** Q, const
                                      (gm * (vs[i] * vs[i])) * dt);
             }
             REAL bvx_x, bvz_z;
-            if (surf) {   /* transpose of the corrected surface update */
+            if (zs && xs) {
+                bvx_x = R(0); bvz_z = R(0);
+            } else if (zs) {   /* transposes of the corrected surface updates */
                 const REAL c_surf = R(4) * mu * (lam + mu) / (lam + R(2) * mu);
                 bvx_x = dt * c_surf * bsxx;
                 bvz_z = R(0);
+            } else if (xs) {
+                const REAL c_surf = R(4) * mu * (lam + mu) / (lam + R(2) * mu);
+                bvz_z = dt * c_surf * bszz;
+                bvx_x = R(0);
             } else {
                 bvx_x = dt * ((lam + R(2) * mu) * bsxx + lam * bszz);
                 bvz_z = dt * ((lam + R(2) * mu) * bszz + lam * bsxx);
@@ -470,15 +560,14 @@ static void stress_adjoint_prepare(const EL* p, int b, REAL** A, REAL** Q, const
 static void stress_adjoint_apply(const EL* p, REAL** A, REAL** Q)
 {
     const int nz = p->nz, nx = p->nx, M = p->M;
-    const REAL ix_ = R(1) / p->dx, iz_ = R(1) / p->dz;
     #pragma omp parallel for schedule(static)
     for (int iz = M; iz < nz - M; ++iz) {
         for (int ix = M; ix < nx - M; ++ix) {
             const i64 i = (i64)iz * nx + ix;
-            REAL dqxx_dx = dplus(Q[0], i, 1, M, p->c, ix_);
-            REAL dqxz_dz = p->fs ? fs_adj_dz(p, Q[2], ix, iz, 1, 0, 0) : dminus(Q[2], i, nx, M, p->c, iz_);
-            REAL dqzx_dx = dminus(Q[3], i, 1, M, p->c, ix_);
-            REAL dqzz_dz = p->fs ? fs_adj_dz(p, Q[1], ix, iz, 0, 1, 1) : dplus(Q[1], i, nx, M, p->c, iz_);
+            REAL dqxx_dx = AX(Q[0], 0, 1, 1);
+            REAL dqxz_dz = AZ(Q[2], 1, 0, 0);
+            REAL dqzx_dx = AX(Q[3], 1, 0, 0);
+            REAL dqzz_dz = AZ(Q[1], 0, 1, 1);
             A[VX][i] = A[VX][i] + (dqxx_dx + dqxz_dz);
             A[VZ][i] = A[VZ][i] + (dqzx_dx + dqzz_dz);
         }
@@ -491,7 +580,7 @@ static void velocity_adjoint(const EL* p, int b, REAL** A, REAL** P)
 {
     const int nz = p->nz, nx = p->nx, M = p->M;
     const REAL* rho = p->rho + b * p->ms;
-    const REAL ix_ = R(1) / p->dx, iz_ = R(1) / p->dz, dt = p->dt;
+    const REAL dt = p->dt;
     #pragma omp parallel for schedule(static)
     for (int iz = 0; iz < nz; ++iz) {
         for (int ix = 0; ix < nx; ++ix) {
@@ -521,10 +610,10 @@ static void velocity_adjoint(const EL* p, int b, REAL** A, REAL** P)
     for (int iz = M; iz < nz - M; ++iz) {
         for (int ix = M; ix < nx - M; ++ix) {
             const i64 i = (i64)iz * nx + ix;
-            REAL dpxx_dx = dminus(P[0], i, 1, M, p->c, ix_);
-            REAL dpzz_dz = p->fs ? fs_adj_dz(p, P[1], ix, iz, 1, 1, 0) : dminus(P[1], i, nx, M, p->c, iz_);
-            REAL dpxz_dz = p->fs ? fs_adj_dz(p, P[2], ix, iz, 0, 1, 1) : dplus(P[2], i, nx, M, p->c, iz_);
-            REAL dpzx_dx = dplus(P[3], i, 1, M, p->c, ix_);
+            REAL dpxx_dx = AX(P[0], 1, 1, 0);
+            REAL dpzz_dz = AZ(P[1], 1, 1, 0);
+            REAL dpxz_dz = AZ(P[2], 0, 1, 1);
+            REAL dpzx_dx = AX(P[3], 0, 1, 1);
             A[SXX][i] = A[SXX][i] + dpxx_dx;
             A[SZZ][i] = A[SZZ][i] + dpzz_dz;
             A[SXZ][i] = A[SXZ][i] + (dpxz_dz + dpzx_dx);

@@ -383,13 +383,29 @@ def acoustic_forward(vp, wavelet, src, rec, dh, dt, abcn, order=8, prec="f32", *
 ELASTIC_FIELDS = ("vx", "vz", "sxx", "szz", "sxz")
 
 
+def _el_faces(spec):
+    """Free faces (z_lo, z_hi, x_lo, x_hi) from the reference's spellings."""
+    names = ("top", "bottom", "left", "right")
+    if spec is None or isinstance(spec, (bool, np.bool_)):
+        return [bool(spec), False, False, False]
+    if isinstance(spec, str):
+        spec = [spec]
+    spec = list(spec)
+    if all(isinstance(v, str) for v in spec):
+        return [n in spec for n in names]
+    assert len(spec) == 4
+    return [bool(v) for v in spec]
+
+
 class Elastic2D:
     """2-D isotropic elastic oracle run (``fd_oracle_el.c``): models
     ``vp, vs, rho`` of shape ``(nz, nx)`` or per shot ``(B, nz, nx)``; source
     fields default to the explosive ``(sxx, szz)``, receiver fields to
     ``(vx, vz)`` (``src/sweep/equations/elastic.py:123-128``).
-    ``free_surface=True``: a traction-free top face with no PML pad
-    (reference ``PropTorch(free_surface=True)``)."""
+    ``free_surface``: traction-free faces with no PML pad, as the
+    reference's ``PropTorch(free_surface=...)`` spells them: ``True`` (the
+    top face), face names (``'top'``, ``'bottom'``, ``'left'``,
+    ``'right'``) or four bools (z_lo, z_hi, x_lo, x_hi)."""
 
     def __init__(self, vp, vs, rho, wavelet, src, rec, dh, dt, abcn, order=8, prec="f32",
                  source_fields=("sxx", "szz"), receiver_fields=("vx", "vz"),
@@ -402,8 +418,9 @@ class Elastic2D:
         w, s, r = _batch_io(wavelet, src, rec, 2)
         self.B, self.nt = w.shape[0], w.shape[-1]
         self.phys = models[0].shape[-2:]
-        self.fs = 1 if free_surface else 0
-        self.pads = [0 if free_surface else abcn, abcn, abcn, abcn]   # z_lo, z_hi, x_lo, x_hi
+        faces = _el_faces(free_surface)
+        self.fs = sum(1 << f for f in range(4) if faces[f])
+        self.pads = [0 if faces[f] else abcn for f in range(4)]   # z_lo, z_hi, x_lo, x_hi
         pz, px = self.pads[:2], self.pads[2:]
         self.shape = (self.phys[0] + sum(pz) + 2 * M, self.phys[1] + sum(px) + 2 * M)
         padw = [(pz[0] + M, pz[1] + M), (px[0] + M, px[1] + M)]

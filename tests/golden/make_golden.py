@@ -657,6 +657,46 @@ def elastic2d_free_surface():
     )
 
 
+def elastic2d_free_faces():
+    """Isotropic elastic with traction-free faces other than the top
+    (reference PropTorch(free_surface=[...]) per edge): ['bottom', 'right']
+    (the high-side images, zeroed shear on the surface row / column),
+    ['top', 'left'] and all four faces (corners where two surfaces meet).
+    One explosive shot near a corner, one in the middle; (vx, vz, sxx)
+    receivers on the surface rows and columns; vp/vs/rho gradients, boundary
+    saving."""
+    rng = np.random.default_rng(83)
+    nz, nx, nt, dt, dh, abcn = 36, 48, 260, 0.0005, 5.0, 8
+    vp_true = _layered(nz, nx, rng, 1800.0, 3000.0, 4)
+    vs_true = (vp_true / 1.73).astype(np.float32)
+    rho_true = (310.0 * vp_true ** 0.25).astype(np.float32)
+    vp_init = np.full((nz, nx), 2200.0, np.float32)
+    vs_init = (vp_init / 1.73).astype(np.float32)
+    rho_init = (310.0 * vp_init ** 0.25).astype(np.float32)
+    w = _wavelet(nt, dt, 25.0, 0.04)
+    src = np.array([[nx - 3, nz - 2], [20, 15]], np.int64)
+    rec = np.zeros((2, 12, 2), np.int64)
+    for b in range(2):
+        rec[b, :6, 0] = np.linspace(0, nx - 1, 6).astype(np.int64)
+        rec[b, :6, 1] = nz - 1 if b == 0 else 0
+        rec[b, 6:, 0] = nx - 1 if b == 0 else 0
+        rec[b, 6:, 1] = np.linspace(1, nz - 2, 6).astype(np.int64)
+    out = dict(nz=nz, nx=nx, nt=nt, dt=dt, dh=dh, abcn=abcn, order=8,
+               vp_true=vp_true, vs_true=vs_true, rho_true=rho_true,
+               vp_init=vp_init, vs_init=vs_init, rho_init=rho_init, wavelet=w, src=src, rec=rec)
+    for tag, faces in (("br", ["bottom", "right"]), ("tl", ["top", "left"]),
+                       ("all", ["top", "bottom", "left", "right"])):
+        eq = Elastic(spatial_order=8, device="cpu")
+        solver = PropTorch(eq, shape=(nz, nx), dh=dh, dt=dt, abcn=abcn, impl="c", device="cpu",
+                           memory=BoundarySaving(), free_surface=faces,
+                           receiver_type=["vx", "vz", "sxx"])
+        obs = _forward(solver, w, src, rec, [vp_true, vs_true, rho_true])
+        r = _run(solver, w, src, rec, [vp_init, vs_init, rho_init], obs, False)
+        out.update({f"obs_{tag}": obs, f"pred_{tag}": r["pred"], f"loss_{tag}": r["loss"],
+                    f"grad_vp_{tag}": r["grad0"], f"grad_vs_{tag}": r["grad1"], f"grad_rho_{tag}": r["grad2"]})
+    np.savez_compressed(OUT / "elastic2d_free_faces.npz", **out)
+
+
 CASES = {
     "acoustic2d_c1": acoustic2d_c1,
     "acoustic2d_multi": acoustic2d_multi,
@@ -676,6 +716,7 @@ CASES = {
     "acoustic2d_many": acoustic2d_many,
     "elastic2d_interior": elastic2d_interior,
     "elastic2d_free_surface": elastic2d_free_surface,
+    "elastic2d_free_faces": elastic2d_free_faces,
 }
 
 if __name__ == "__main__":

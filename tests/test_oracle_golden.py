@@ -161,6 +161,27 @@ def test_elastic2d_free_surface_oracle_matches_reference(prec, tol):
         assert rel(d[f"grad_{k}_ckpt"], d[f"grad_{k}"]) < 2e-6
 
 
+@pytest.mark.parametrize("tag,faces", [("br", ["bottom", "right"]), ("tl", ["top", "left"]),
+                                       ("all", ["top", "bottom", "left", "right"])])
+def test_elastic2d_free_faces_oracle_matches_reference(tag, faces):
+    """Traction-free faces per edge: the high-side images (a half field's
+    surface node is air; zeroed shear), the x-normal Robertsson correction of
+    szz, corners where two surfaces meet; (vx, vz, sxx) receivers on the
+    surface rows and columns."""
+    d = np.load(GOLD / "elastic2d_free_faces.npz")
+    kw = dict(free_surface=faces, receiver_fields=("vx", "vz", "sxx"))
+    obs = O.elastic_forward(d["vp_true"], d["vs_true"], d["rho_true"], d["wavelet"], d["src"],
+                            d["rec"], *_el_args(d), **kw)
+    assert rel(obs, d[f"obs_{tag}"]) < 2e-6
+    pred, loss, (gvp, gvs, grho) = O.elastic_gradient(
+        d["vp_init"], d["vs_init"], d["rho_init"], d["wavelet"], d["src"], d["rec"], d[f"obs_{tag}"],
+        *_el_args(d), **kw)
+    assert rel(pred, d[f"pred_{tag}"]) < 2e-6
+    assert rel(gvp, d[f"grad_vp_{tag}"]) < 1e-5
+    assert rel(gvs, d[f"grad_vs_{tag}"]) < 1e-5
+    assert rel(grho, d[f"grad_rho_{tag}"]) < 1e-5
+
+
 def test_elastic2d_reference_full_and_boundary_modes_agree():
     """The reference's full-storage gradient adds the it = 0 image the
     boundary-saving reverse skips; the two differ at the 1e-6 level."""
