@@ -178,8 +178,9 @@ typedef struct sweep_elastic_desc {
     /* Traction-free faces z_lo, z_hi, x_lo, x_hi (reference PropTorch(
      * free_surface=...) for Elastic: the image method of
      * elastic_free_surface.cuh, the Robertsson sxx correction and szz = 0 on
-     * the surface row, elastic2d/kernels.cuh:293-303).  1 = free; a free face
-     * has pad 0.  The top face (z_lo) is built; the others must be 0. */
+     * the surface row, elastic2d/kernels.cuh:293-303; the x <-> z swap on a
+     * free column, zeroed sxz on a high-side face).  1 = free; a free face
+     * has pad 0. */
     int32_t free_surface[4];
 } sweep_elastic_desc;
 

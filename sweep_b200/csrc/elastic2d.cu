@@ -101,7 +101,7 @@ struct Geo {
     int gf;                         // shots per CTA of the forward kernels
     int* err;                       // bounded-wait failure flag (0 = none)
     StripStore st;
-    int fst;                        // traction-free top face: the surface is row z0 (no pad above)
+    int fs;                         // bit f: traction-free face f (z_lo, z_hi, x_lo, x_hi), pad 0
 };
 
 enum { ERR_WAIT_FWD = 1, ERR_WAIT_REV = 2 };
@@ -254,70 +254,140 @@ __device__ __forceinline__ float dmz(const float* t, int c, float inv)
             C3 * (t[c + 2 * HX] - t[c - 3 * HX]) + C4 * (t[c + 3 * HX] - t[c - 4 * HX])) * inv;
 }
 
-// ------------------------------------------------- traction-free top face
-// Image method of the reference (common/elastic_free_surface.cuh:200-450,
-// elastic2d/kernels.cuh:216-234, 293-303, 592-700).  The surface is row z0,
-// the first physical row (a free face has no PML pad); the M rows above it
-// are air.  The M rows from the surface down take a unit-weight 2nd-order
-// z-difference instead of the full stencil.  Only the D- form on the surface
-// row reads the air: the row above it holds the image of the surface row,
-// negated, for both fields it is used on (sxz and vz sit half a cell below
-// the surface and are odd).  The surface row's sxx gets the Robertsson
-// correction and its szz is zeroed after the stress update.
-template <bool FS>
-__device__ __forceinline__ bool fs_band(const Geo& G, int iz)
+// ------------------------------------------------------ traction-free faces
+// Image method of the reference (common/elastic_free_surface.cuh:200-720,
+// elastic2d/kernels.cuh:216-303, 592-700).  Bit f of G.fs (z_lo, z_hi, x_lo,
+// x_hi) makes face f free; a free face has no PML pad, its surface is the
+// first / last physical row or column and the M halo cells past it are air.
+// Along an axis with a free face the M cells from the surface inwards take a
+// unit-weight 2nd-order difference, and a difference that reaches into the
+// air reads the image of the cell mirrored about the surface (about the node
+// for fields on integer nodes, about the half cell next to it for fields half
+// a cell along the axis; on the high side a half field's surface node is
+// itself air), negated for odd fields.  Below the band every stencil stays in
+// the medium: the D+ forms are only applied to integer fields and the D-
+// forms to half fields.  After the stress update a surface row's sxx (a
+// surface column's szz) takes the Robertsson correction, its szz (sxx) is
+// zeroed, and a high-side face zeroes sxz on its surface row / column.
+struct FsAx {
+    bool lo_on, hi_on;
+    int lo, hi;              // surface cells
+};
+__device__ __forceinline__ FsAx fs_zax(const Geo& G) { return {(G.fs & 1) != 0, (G.fs & 2) != 0, G.z0, G.z1 - 1}; }
+__device__ __forceinline__ FsAx fs_xax(const Geo& G) { return {(G.fs & 4) != 0, (G.fs & 8) != 0, G.x0, G.x1 - 1}; }
+
+__device__ __forceinline__ bool fs_band(const FsAx& a, int j)
 {
-    return FS && iz >= G.z0 && iz < G.z0 + M;
+    return (a.lo_on && j >= a.lo && j < a.lo + M) || (a.hi_on && j > a.hi - M && j <= a.hi);
 }
-// D+ in z (szz, vx) on a free top face
-template <bool FS>
-__device__ __forceinline__ float dpz_fs(const Geo& G, const float* t, int c, int iz, float inv)
+__device__ __forceinline__ bool fs_air(const FsAx& a, int j)
 {
-    return fs_band<FS>(G, iz) ? (t[c + HX] - t[c]) * inv : dpz(t, c, inv);
+    return (a.lo_on && j < a.lo) || (a.hi_on && j > a.hi);
 }
-// D- in z (sxz, vz) on a free top face
-template <bool FS>
-__device__ __forceinline__ float dmz_fs(const Geo& G, const float* t, int c, int iz, float inv)
+// a cell whose adjoint stencil reaches a band or an image
+__device__ __forceinline__ bool fs_near(const FsAx& a, int j)
 {
-    if (!fs_band<FS>(G, iz)) return dmz(t, c, inv);
-    return (iz == G.z0 ? t[c] + t[c] : t[c] - t[c - HX]) * inv;
+    return (a.lo_on && j < a.lo + 2 * M) || (a.hi_on && j > a.hi - 2 * M);
 }
-// Negated transposes of dpz_fs and dmz_fs at input row m (the plain ones are
-// dmz for a D+ forward and dpz for a D- forward): an output row in the band
-// contributes with weight 1, one below it with the full weight.  The image
-// read by the surface row adds -q[z0] to the D- transpose there.  Air rows
-// hold no adjoint (sources and receivers above a free surface are off the
-// grid), so nothing else folds back.  Rows from z0 + 2M down are plain.
-template <bool FS>
-__device__ __forceinline__ float adj_dpz_fs(const Geo& G, const float* q, int c, int m, float inv)
+__device__ __forceinline__ bool fs_zrow(const Geo& G, int iz)
 {
-    if (!FS || m >= G.z0 + 2 * M) return dmz(q, c, inv);
+    return ((G.fs & 1) && iz == G.z0) || ((G.fs & 2) && iz == G.z1 - 1);
+}
+__device__ __forceinline__ bool fs_xcol(const Geo& G, int ix)
+{
+    return ((G.fs & 4) && ix == G.x0) || ((G.fs & 8) && ix == G.x1 - 1);
+}
+__device__ __forceinline__ bool fs_zero_shear(const Geo& G, int ix, int iz)
+{
+    return ((G.fs & 2) && iz == G.z1 - 1) || ((G.fs & 8) && ix == G.x1 - 1);
+}
+// does the tile hold a surface row or column?
+__device__ __forceinline__ bool fs_tile(const Geo& G, int tz0, int tx0)
+{
+    auto in = [](int j, int t0, int w) { return j >= t0 && j < t0 + w; };
+    return ((G.fs & 1) && in(G.z0, tz0, TZ)) || ((G.fs & 2) && in(G.z1 - 1, tz0, TZ)) ||
+           ((G.fs & 4) && in(G.x0, tx0, TX)) || ((G.fs & 8) && in(G.x1 - 1, tx0, TX));
+}
+
+// Value at index j along the axis (stride S in the tile) of the line through
+// tile cell c, which sits at index j0, with the images of the free faces.
+template <int S>
+__device__ __forceinline__ float fs_val(const FsAx& a, const float* t, int c, int j0, int j, bool odd, bool half)
+{
+    int m;
+    if (a.lo_on && j < a.lo) m = half ? 2 * a.lo - 1 - j : 2 * a.lo - j;
+    else if (a.hi_on && j >= (half ? a.hi : a.hi + 1)) m = half ? 2 * a.hi - 1 - j : 2 * a.hi - j;
+    else return t[c + (j - j0) * S];
+    const float v = t[c + (m - j0) * S];
+    return odd ? -v : v;
+}
+
+template <int S, bool FWD>
+__device__ __forceinline__ float d_plain(const float* t, int c, float inv)
+{
+    if constexpr (S == 1) return FWD ? dpx(t, c, inv) : dmx(t, c, inv);
+    else return FWD ? dpz(t, c, inv) : dmz(t, c, inv);
+}
+
+// Forward derivative along an axis: D+ (FWD) or D-, at tile cell c, index j.
+template <bool FS, int S, bool FWD>
+__device__ __forceinline__ float d_fs(const FsAx& a, const float* t, int c, int j, bool odd, bool half, float inv)
+{
+    if (!FS || !fs_band(a, j)) return d_plain<S, FWD>(t, c, inv);
+    return (FWD ? fs_val<S>(a, t, c, j, j + 1, odd, half) - fs_val<S>(a, t, c, j, j, odd, half)
+                : fs_val<S>(a, t, c, j, j, odd, half) - fs_val<S>(a, t, c, j, j - 1, odd, half)) * inv;
+}
+
+// Transposed reduced stencil at index m, read from the tile line through
+// cell c (index j0): output cells in a band contribute with weight 1, the
+// others with the full weight; air cells hold no adjoint (sources and
+// receivers beyond a free surface are off the grid).  Every cell it reads
+// lies within M of j0; the range test only guards the tile.
+template <int S, bool FWD>
+__device__ __forceinline__ float adj_red(const FsAx& a, const float* q, int c, int j0, int m, int n)
+{
+    auto live = [&](int j) { return j >= 0 && j < n && !fs_band(a, j) && !fs_air(a, j) && j - j0 >= -M && j - j0 <= M; };
+    auto at = [&](int j) { return (j - j0 >= -M && j - j0 <= M) ? q[c + (j - j0) * S] : 0.f; };
     const float w[M] = {C1, C2, C3, C4};
     float acc = 0.f;
 #pragma unroll
     for (int k = 1; k <= M; ++k) {
-        if (!fs_band<FS>(G, m + k - 1)) acc += w[k - 1] * q[c + (k - 1) * HX];
-        if (!fs_band<FS>(G, m - k)) acc -= w[k - 1] * q[c - k * HX];
+        const int jp = FWD ? m + k - 1 : m + k;
+        const int jm = FWD ? m - k : m - k + 1;
+        if (live(jp)) acc += w[k - 1] * at(jp);
+        if (live(jm)) acc -= w[k - 1] * at(jm);
     }
-    if (fs_band<FS>(G, m)) acc += q[c];
-    if (fs_band<FS>(G, m - 1)) acc -= q[c - HX];
-    return acc * inv;
+    if (FWD) {
+        if (fs_band(a, m)) acc += at(m);
+        if (fs_band(a, m - 1)) acc -= at(m - 1);
+    } else {
+        if (fs_band(a, m + 1)) acc += at(m + 1);
+        if (fs_band(a, m)) acc -= at(m);
+    }
+    return acc;
 }
-template <bool FS>
-__device__ __forceinline__ float adj_dmz_fs(const Geo& G, const float* q, int c, int m, float inv)
+
+// Adjoint of d_fs (negated transpose; the plain one is D- for a D+ forward
+// and D+ for a D- forward): the reduced transpose plus, for each free face
+// whose image of this cell lies in the air, the transpose there folded back
+// with the field's parity.
+template <bool FS, int S, bool FWD>
+__device__ __forceinline__ float adj_fs(const FsAx& a, const float* q, int c, int j, int n, bool odd, bool half,
+                                        float inv)
 {
-    if (!FS || m >= G.z0 + 2 * M) return dpz(q, c, inv);
-    const float w[M] = {C1, C2, C3, C4};
-    float acc = 0.f;
-#pragma unroll
-    for (int k = 1; k <= M; ++k) {
-        if (!fs_band<FS>(G, m + k)) acc += w[k - 1] * q[c + k * HX];
-        if (!fs_band<FS>(G, m - k + 1)) acc -= w[k - 1] * q[c - (k - 1) * HX];
+    if (!FS || !fs_near(a, j)) return d_plain<S, !FWD>(q, c, inv);
+    if (fs_air(a, j)) return 0.f;
+    float g = adj_red<S, FWD>(a, q, c, j, j, n);
+    const float par = odd ? -1.f : 1.f;
+    if (a.lo_on) {
+        const int mj = half ? 2 * a.lo - 1 - j : 2 * a.lo - j;
+        if (mj < a.lo) g += par * adj_red<S, FWD>(a, q, c, j, mj, n);
     }
-    if (fs_band<FS>(G, m + 1)) acc += q[c + HX];
-    if (fs_band<FS>(G, m)) acc -= q[c];
-    if (m == G.z0) acc -= q[c];
-    return acc * inv;
+    if (a.hi_on) {
+        const int mj = half ? 2 * a.hi - 1 - j : 2 * a.hi - j;
+        if (mj >= (half ? a.hi : a.hi + 1)) g += par * adj_red<S, FWD>(a, q, c, j, mj, n);
+    }
+    return g * inv;
 }
 
 // Cooperative load of NF fields' tiles plus an M-cell halo (zero outside the
@@ -519,10 +589,11 @@ __global__ void __launch_bounds__(NTH, 4) fwd_vel(const __grid_constant__ FwdMap
             const int lz = threadIdx.y + 8 * r, iz = tz0 + lz;
             if (!in_core(G, ix, iz)) continue;
             const int c = (lz + M) * HX + lx + M;
-            float dsxx_dx = dpx(tsxx, c, G.idx);
-            float dsxz_dz = dmz_fs<FS>(G, tsxz, c, iz, G.idz);
-            float dsxz_dx = dmx(tsxz, c, G.idx);
-            float dszz_dz = dpz_fs<FS>(G, tszz, c, iz, G.idz);
+            const FsAx az = fs_zax(G), ax = fs_xax(G);
+            float dsxx_dx = d_fs<FS, 1, true>(ax, tsxx, c, ix, true, false, G.idx);
+            float dsxz_dz = d_fs<FS, HX, false>(az, tsxz, c, iz, true, true, G.idz);
+            float dsxz_dx = d_fs<FS, 1, false>(ax, tsxz, c, ix, true, true, G.idx);
+            float dszz_dz = d_fs<FS, HX, true>(az, tszz, c, iz, true, false, G.idz);
             const long long i = (long long)iz * G.P + ix;
             if (ring && in_pml(G, ix, iz)) {
                 if (mz[r].at >= 0) {
@@ -586,7 +657,7 @@ __global__ void __launch_bounds__(NTH, 4) fwd_str(const __grid_constant__ FwdMap
         mur[r] = in ? A.m.mu[i] : 0.f;
     }
     const int ntl = G.ntx * G.ntz;
-    const bool ring = tile_in_pml(G, tz0, tx0);
+    const bool ring = tile_in_pml(G, tz0, tx0) || (FS && fs_tile(G, tz0, tx0));
     const bool stile = A.strips != nullptr && tile_has_strips(G, tz0, tx0);
     for (int g = 0; g < nloc; ++g) {
         const int b = b0 + g, s = g & 1;
@@ -603,11 +674,12 @@ __global__ void __launch_bounds__(NTH, 4) fwd_str(const __grid_constant__ FwdMap
 #pragma unroll
             for (int r = 0; r < RPT; ++r) {
                 const int iz = tz0 + threadIdx.y + 8 * r;
-                // the free surface row takes the CPML branch at every column
-                // (reference kernels.cuh:216-234): the high side's half-cell
-                // profile is nonzero one cell inside the band there
-                mz[r] = load_mem_z(G, A.mem, ZM_VZZ, ZM_VXZ, b, iz, ix, FS && iz == G.z0);
-                mx[r] = load_mem_x(G, A.mem, XM_VXX, XM_VZX, b, iz, ix, FS && iz == G.z0);
+                // a free surface row / column takes the CPML branch at every
+                // cell (reference kernels.cuh:216-234): the high sides'
+                // half-cell profiles are nonzero one cell inside their band
+                const bool surf = FS && (fs_zrow(G, iz) || fs_xcol(G, ix));
+                mz[r] = load_mem_z(G, A.mem, ZM_VZZ, ZM_VXZ, b, iz, ix, surf);
+                mx[r] = load_mem_x(G, A.mem, XM_VXX, XM_VZX, b, iz, ix, surf);
             }
         }
         const int s0 = G.src.off[key], s1 = G.src.off[key + 1];
@@ -620,12 +692,14 @@ __global__ void __launch_bounds__(NTH, 4) fwd_str(const __grid_constant__ FwdMap
             const long long i = (long long)iz * G.P + ix;
             float sxx = sm.c[s][0][cell], szz = sm.c[s][1][cell], sxz = sm.c[s][2][cell];
             if (in_core(G, ix, iz)) {
-                float dvx_dx = dmx(tvx, c, G.idx);
-                float dvz_dz = dmz_fs<FS>(G, tvz, c, iz, G.idz);
-                float dvx_dz = dpz_fs<FS>(G, tvx, c, iz, G.idz);
-                float dvz_dx = dpx(tvz, c, G.idx);
+                const FsAx az = fs_zax(G), ax = fs_xax(G);
+                float dvx_dx = d_fs<FS, 1, false>(ax, tvx, c, ix, true, true, G.idx);
+                float dvz_dz = d_fs<FS, HX, false>(az, tvz, c, iz, true, true, G.idz);
+                float dvx_dz = d_fs<FS, HX, true>(az, tvx, c, iz, false, false, G.idz);
+                float dvz_dx = d_fs<FS, 1, true>(ax, tvz, c, ix, false, false, G.idx);
                 const float lam = lamr[r], mu = mur[r];
-                const bool pml = ring && (in_pml(G, ix, iz) || (FS && iz == G.z0));
+                const bool zs = FS && fs_zrow(G, iz), xs = FS && fs_xcol(G, ix);
+                const bool pml = ring && (in_pml(G, ix, iz) || zs || xs);
                 if (pml && mz[r].at >= 0) {
                     float m = G.az[iz] * mz[r].a + G.bz[iz] * dvz_dz;
                     A.mem.z[ZM_VZZ][mz[r].at] = m; dvz_dz += m;
@@ -645,9 +719,12 @@ __global__ void __launch_bounds__(NTH, 4) fwd_str(const __grid_constant__ FwdMap
                     A.mem.x[XM_VZX][mx[r].at] = m; dvz_dx += m;
                 }
                 sxz += G.dt * mu * (dvx_dz + dvz_dx);
-                if (FS && iz == G.z0) {   // surface row: Robertsson correction, then szz = 0
-                    sxx += -G.dt * lam * (lam / (lam + 2.f * mu) * dvx_dx + dvz_dz);
-                    szz = 0.f;
+                if (FS) {   // Robertsson corrections first, then the zeroing
+                    if (zs) sxx += -G.dt * lam * (lam / (lam + 2.f * mu) * dvx_dx + dvz_dz);
+                    if (xs) szz += -G.dt * lam * (lam / (lam + 2.f * mu) * dvz_dz + dvx_dx);
+                    if (zs) szz = 0.f;
+                    if (xs) sxx = 0.f;
+                    if (fs_zero_shear(G, ix, iz)) sxz = 0.f;
                 }
             }
             // point sources of this cell (usually none in the tile)
@@ -858,10 +935,11 @@ __global__ void __launch_bounds__(NTH, 4) rev_str(RevArgs A)
                 continue;
             }
             const int c = (lz + M) * HX + lx + M;
-            const float dvx_dx = dmx(tvx, c, G.idx);
-            const float dvz_dz = dmz_fs<FS>(G, tvz, c, iz, G.idz);
-            const float dvx_dz = dpz_fs<FS>(G, tvx, c, iz, G.idz);
-            const float dvz_dx = dpx(tvz, c, G.idx);
+            const FsAx az = fs_zax(G), ax = fs_xax(G);
+            const float dvx_dx = d_fs<FS, 1, false>(ax, tvx, c, ix, true, true, G.idx);
+            const float dvz_dz = d_fs<FS, HX, false>(az, tvz, c, iz, true, true, G.idz);
+            const float dvx_dz = d_fs<FS, HX, true>(az, tvx, c, iz, false, false, G.idz);
+            const float dvz_dx = d_fs<FS, 1, true>(ax, tvz, c, ix, false, false, G.idx);
             if (in_recon(G, ix, iz)) {
                 float sxx = A.f[SXX][so + i], szz = A.f[SZZ][so + i], sxz = A.f[SXZ][so + i];
                 const int cell = lz * TX + lx;
@@ -884,16 +962,21 @@ __global__ void __launch_bounds__(NTH, 4) rev_str(RevArgs A)
                 }
             }
             if (in_box(G, ix, iz)) {
-                const bool surf = FS && iz == G.z0;
-                const float bsxx = A.a[SXX][so + i], bsxz = A.a[SXZ][so + i];
-                const float bszz = surf ? 0.f : A.a[SZZ][so + i];   // zeroed on the surface row
+                // the stresses a surface zeroes carry no adjoint there
+                const bool zs = FS && fs_zrow(G, iz), xs = FS && fs_xcol(G, ix);
+                const float bsxx = xs ? 0.f : A.a[SXX][so + i];
+                const float bszz = zs ? 0.f : A.a[SZZ][so + i];
+                const float bsxz = FS && fs_zero_shear(G, ix, iz) ? 0.f : A.a[SXZ][so + i];
                 const float rho = rho_[i], vp = vp_[i], vs = vs_[i];
                 float gl, gm;
-                if (surf) {
-                    // d / d(lam, mu) of the corrected surface update dt C dvx_dx,
-                    // C = 4 mu (lam + mu) / (lam + 2 mu) (kernels.cuh:633-646)
+                if (zs && xs) {
+                    gl = gm = 0.f;           // a corner: every stress is zeroed
+                } else if (zs || xs) {
+                    // d / d(lam, mu) of the corrected surface update dt C d(v
+                    // along the surface), C = 4 mu (lam + mu) / (lam + 2 mu)
+                    // (kernels.cuh:633-646)
                     const float vp2 = vp * vp, vs2 = vs * vs, vp4 = vp2 * vp2;
-                    const float a = bsxx * dvx_dx;
+                    const float a = zs ? bsxx * dvx_dx : bszz * dvz_dz;
                     gl = a * 4.f * vs2 * vs2 / vp4;
                     gm = a * 4.f * (vp4 - 2.f * vp2 * vs2 + 2.f * vs2 * vs2) / vp4;
                 } else {
@@ -999,12 +1082,17 @@ __global__ void __launch_bounds__(NTH, 4) rev_sadj(RevArgs A)
         if (k >= HN) continue;
         const int lz = k / HX, lx = k - lz * HX;
         const int iz = tz0 - M + lz, ix = tx0 - M + lx;
-        const float bsxx = rs[j][0], bszz = rs[j][1], bsxz = rs[j][2], lam = rs[j][3], mu = rs[j][4];
+        const bool ing = (unsigned)iz < (unsigned)G.nz && (unsigned)ix < (unsigned)G.nx;
+        const bool zs = FS && ing && fs_zrow(G, iz), xs = FS && ing && fs_xcol(G, ix);
+        const float bsxx = xs ? 0.f : rs[j][0], bszz = zs ? 0.f : rs[j][1];
+        const float bsxz = FS && ing && fs_zero_shear(G, ix, iz) ? 0.f : rs[j][2];
+        const float lam = rs[j][3], mu = rs[j][4];
         float q0, q1;
-        if (FS && iz == G.z0 && (unsigned)ix < (unsigned)G.nx) {
-            // surface row: szz zeroed, transpose of the corrected sxx update
-            q0 = G.dt * (4.f * mu * (lam + mu) / (lam + 2.f * mu)) * bsxx;
-            q1 = 0.f;
+        if (zs || xs) {
+            // transposes of the corrected surface updates (a corner: none)
+            const float cs = zs && xs ? 0.f : G.dt * (4.f * mu * (lam + mu) / (lam + 2.f * mu));
+            q0 = zs ? cs * bsxx : 0.f;
+            q1 = xs ? cs * bszz : 0.f;
         } else {
             q0 = G.dt * ((lam + 2.f * mu) * bsxx + lam * bszz);
             q1 = G.dt * ((lam + 2.f * mu) * bszz + lam * bsxx);
@@ -1045,8 +1133,11 @@ __global__ void __launch_bounds__(NTH, 4) rev_sadj(RevArgs A)
         if (!in_core(G, ix, iz)) continue;
         const int c = (lz + M) * HX + lx + M;
         const long long i = so + (long long)iz * G.P + ix;
-        A.a[VX][i] += dpx(tq[0], c, G.idx) + adj_dpz_fs<FS>(G, tq[2], c, iz, G.idz);
-        A.a[VZ][i] += dmx(tq[3], c, G.idx) + adj_dmz_fs<FS>(G, tq[1], c, iz, G.idz);
+        const FsAx az = fs_zax(G), ax = fs_xax(G);
+        A.a[VX][i] += adj_fs<FS, 1, false>(ax, tq[0], c, ix, G.nx, true, true, G.idx) +
+                      adj_fs<FS, HX, true>(az, tq[2], c, iz, G.nz, false, false, G.idz);
+        A.a[VZ][i] += adj_fs<FS, 1, true>(ax, tq[3], c, ix, G.nx, false, false, G.idx) +
+                      adj_fs<FS, HX, false>(az, tq[1], c, iz, G.nz, true, true, G.idz);
     }
 }
 
@@ -1138,19 +1229,26 @@ __global__ void __launch_bounds__(NTH, 4) rev_vadj(RevArgs A)
         if (!in_core(G, ix, iz)) continue;
         const int c = (lz + M) * HX + lx + M;
         const long long i = (long long)iz * G.P + ix;
-        A.a[SXX][so + i] += dmx(tp[0], c, G.idx);
-        // the surface row's adjoint szz was zeroed by this step's stress half
-        const float szz0 = FS && iz == G.z0 ? 0.f : A.a[SZZ][so + i];
-        A.a[SZZ][so + i] = szz0 + adj_dpz_fs<FS>(G, tp[1], c, iz, G.idz);
-        A.a[SXZ][so + i] += adj_dmz_fs<FS>(G, tp[2], c, iz, G.idz) + dpx(tp[3], c, G.idx);
+        // the stresses a surface zeroes had their adjoint zeroed by this
+        // step's stress half
+        const FsAx az = fs_zax(G), ax = fs_xax(G);
+        const float sxx0 = FS && fs_xcol(G, ix) ? 0.f : A.a[SXX][so + i];
+        const float szz0 = FS && fs_zrow(G, iz) ? 0.f : A.a[SZZ][so + i];
+        const float sxz0 = FS && fs_zero_shear(G, ix, iz) ? 0.f : A.a[SXZ][so + i];
+        A.a[SXX][so + i] = sxx0 + adj_fs<FS, 1, true>(ax, tp[0], c, ix, G.nx, true, false, G.idx);
+        A.a[SZZ][so + i] = szz0 + adj_fs<FS, HX, true>(az, tp[1], c, iz, G.nz, true, false, G.idz);
+        A.a[SXZ][so + i] = sxz0 + (adj_fs<FS, HX, false>(az, tp[2], c, iz, G.nz, true, true, G.idz) +
+                                   adj_fs<FS, 1, false>(ax, tp[3], c, ix, G.nx, true, true, G.idx));
         if (!in_box(G, ix, iz)) continue;
         const float vx = A.f[VX][so + i], vz = A.f[VZ][so + i];
         A.cvx[so + i] = vx;
         A.cvz[so + i] = vz;
         if (in_recon(G, ix, iz)) {
             const float k_ = bv_[i];
-            A.f[VX][so + i] = vx - k_ * (dpx(tsxx, c, G.idx) + dmz_fs<FS>(G, tsxz, c, iz, G.idz));
-            A.f[VZ][so + i] = vz - k_ * (dmx(tsxz, c, G.idx) + dpz_fs<FS>(G, tszz, c, iz, G.idz));
+            A.f[VX][so + i] = vx - k_ * (d_fs<FS, 1, true>(ax, tsxx, c, ix, true, false, G.idx) +
+                                         d_fs<FS, HX, false>(az, tsxz, c, iz, true, true, G.idz));
+            A.f[VZ][so + i] = vz - k_ * (d_fs<FS, 1, false>(ax, tsxz, c, ix, true, true, G.idx) +
+                                         d_fs<FS, HX, true>(az, tszz, c, iz, true, false, G.idz));
         }
     }
     // strips (box ring and the M cells outside it) of step it - 1
@@ -1289,18 +1387,18 @@ static Plan make_plan(const sweep_elastic_desc* d)
     SWEEP_REQUIRE(d->nrec_fields >= 1 && d->nrec_fields <= 5, "elastic2d: 1 to 5 receiver fields (got %d)", d->nrec_fields);
     for (int k = 0; k < d->nrec_fields; ++k)
         SWEEP_REQUIRE(d->rec_fields[k] >= 0 && d->rec_fields[k] <= SXZ, "elastic2d: bad receiver field %d", d->rec_fields[k]);
-    for (int f = 1; f < 4; ++f)
-        SWEEP_REQUIRE(!d->free_surface[f], "elastic2d: a traction-free face is built on the top face only (face %d)", f);
     for (int f = 0; f < 4; ++f) {
-        if (f == 0 && d->free_surface[0])
-            SWEEP_REQUIRE(d->pad[0] == 0, "elastic2d: a free top face has no PML pad (got %d)", d->pad[0]);
+        if (d->free_surface[f])
+            SWEEP_REQUIRE(d->pad[f] == 0, "elastic2d: a free face has no PML pad (face %d has %d)", f, d->pad[f]);
         else
             SWEEP_REQUIRE(d->pad[f] >= 1, "elastic2d: every absorbing face needs a PML pad >= 1 (face %d has %d)", f,
                           d->pad[f]);
     }
     Plan pl{};
     Geo& G = pl.G;
-    G.fst = d->free_surface[0] ? 1 : 0;
+    G.fs = 0;
+    for (int f = 0; f < 4; ++f)
+        if (d->free_surface[f]) G.fs |= 1 << f;
     G.B = d->B; G.nz = d->nz; G.nx = d->nx; G.nt = d->nt;
     G.P = (d->nx + 31) / 32 * 32;
     G.S = (long long)d->nz * G.P;
@@ -1719,10 +1817,10 @@ static void forward_steps(FwdArgs& A, int it0, int it1, StripsOf strips_of, floa
         void* slot = strips_of(it);
         A.strips = (slot && scaled) ? static_cast<void*>(scratch) : slot;
         const cudaStream_t ls = gs.stream();
-        if (G.fst) fwd_vel<true><<<grid, block, SM_FWD_VEL, ls>>>(maps, A);
+        if (G.fs) fwd_vel<true><<<grid, block, SM_FWD_VEL, ls>>>(maps, A);
         else fwd_vel<false><<<grid, block, SM_FWD_VEL, ls>>>(maps, A);
         if (slot && hr) hr->before_write(it);
-        if (G.fst) fwd_str<true><<<grid, block, SM_FWD_STR, ls>>>(maps, A);
+        if (G.fs) fwd_str<true><<<grid, block, SM_FWD_STR, ls>>>(maps, A);
         else fwd_str<false><<<grid, block, SM_FWD_STR, ls>>>(maps, A);
         if (G.nvf) vsrc_forward<<<G.B, 128, 0, ls>>>(G, A.f[VX], A.f[VZ], A.strips, A.record, it);
         if (slot && scaled) quantize_strips<<<qblocks, kQB, 0, ls>>>(G, scratch, slot);
@@ -1859,7 +1957,7 @@ static void backward_with(const sweep_elastic_desc* d, int mem_mode, int ckpt_ev
             const cudaStream_t ls = gs.stream();
             if (G.nvf)
                 vsrc_reverse<<<G.B, 128, 0, ls>>>(G, A.a[VX], A.a[VZ], A.f[VX], A.f[VZ], A.grho, A.m.rho, A.G_shots, it);
-            if (G.fst) {
+            if (G.fs) {
                 rev_str<true><<<grid_s, block, SM_REV_STR, ls>>>(A);
                 rev_sadj<true><<<grid_b, block, SM_REV_SADJ, ls>>>(A);
                 rev_vadj<true><<<grid_b, block, SM_REV_VADJ, ls>>>(A);

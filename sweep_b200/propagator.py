@@ -131,15 +131,20 @@ class _Geometry:
         else:
             prof = cpml_profiles_r(pads, self.M, prop.dt, self.spacing, self.shape, max_vel, pml_freq)
         self.prof = [[torch.from_numpy(np.ascontiguousarray(a)).to(device) for a in p] for p in prof]
-        # Elastic with a free top face: the rows above the surface are air,
-        # which the image method overwrites, so a source or receiver there is
-        # off the grid (the reference would fold its adjoint back through the
-        # images of the air rows)
-        self.fs_top = isinstance(eq, Elastic) and bool(prop.fs_faces[0])
-        if self.fs_top:
+        # Elastic with free faces: the cells past a surface are air, which the
+        # image method overwrites, so a source or receiver there is off the
+        # grid (the reference would fold its adjoint back through the images)
+        self.fs_faces = tuple(prop.fs_faces) if isinstance(eq, Elastic) else (False,) * 4
+        if any(self.fs_faces):
             src_rt, rec_rt = np.array(src_rt, np.int64), np.array(rec_rt, np.int64)
+            nz, nx = self.shape
+            M = self.M
             for loc in (src_rt, rec_rt):
-                air = loc[..., 1] < self.M
+                x, z = loc[..., 0], loc[..., 1]
+                air = np.zeros(x.shape, bool)
+                for on, cut in zip(self.fs_faces, (z < M, z > nz - 1 - M, x < M, x > nx - 1 - M)):
+                    if on:
+                        air |= cut
                 loc[air] = -(1 << 20)
         self.src = torch.from_numpy(np.ascontiguousarray(src_rt, dtype=np.int32)).to(device)
         self.rec = torch.from_numpy(np.ascontiguousarray(rec_rt, dtype=np.int32)).to(device)
@@ -215,7 +220,8 @@ class _Geometry:
         d.nrec_fields = len(rec_fields)
         for k, f in enumerate(rec_fields):
             d.rec_fields[k] = f
-        d.free_surface[0] = 1 if self.fs_top else 0
+        for f in range(4):
+            d.free_surface[f] = 1 if self.fs_faces[f] else 0
         return d
 
 
@@ -371,9 +377,6 @@ class PropTorch(torch.nn.Module):
         if self.abcn < 1:
             raise NotImplementedError("sweep_b200: the absorbing faces need a layer (abcn >= 1)")
         self.fs_faces = free_faces(free_surface, nd)
-        if any(self.fs_faces[1:]) and isinstance(equation, Elastic):
-            raise NotImplementedError("sweep_b200: an Elastic free surface is built on the top face only "
-                                      "(free_surface=True); the bottom / left / right image faces are not")
         if nd == 3 and any(self.fs_faces[1:]):
             raise NotImplementedError("per-face free surfaces are 2-D only (as in the reference); "
                                       "3-D takes free_surface=True (the top face)")

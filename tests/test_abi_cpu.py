@@ -345,9 +345,9 @@ def test_recursive_sizes_every_equation():
 
 
 def test_elastic_free_surface_faces_checked():
-    """The elastic core takes a traction-free top face with no pad there and
-    refuses the other faces (host-side checks, no device work); the public
-    API refuses them before the core is reached."""
+    """The elastic core takes traction-free faces with no pad on them and an
+    absorbing pad on every other face (host-side checks, no device work);
+    the public API drops a free face's pad."""
     from sweep_b200 import Elastic, PropTorch, _lib
     e = _lib.ElasticDesc()
     e.B, e.nz, e.nx, e.nt, e.M = 2, 60, 80, 10, 4
@@ -360,13 +360,15 @@ def test_elastic_free_surface_faces_checked():
     _lib.call("sweep_b200_elastic_sizes", e, _lib.MEM_BOUNDARY, 0, ws, tape)
     assert ws.value > 0 and tape.value > 0
     e.pad[0] = 3
-    with pytest.raises(RuntimeError, match="free top face"):
+    with pytest.raises(RuntimeError, match="free face has no PML pad"):
         _lib.call("sweep_b200_elastic_sizes", e, _lib.MEM_BOUNDARY, 0, ws, tape)
-    e.pad[0], e.free_surface[2] = 0, 1
-    with pytest.raises(RuntimeError, match="top face only"):
+    e.pad[0], e.free_surface[3] = 0, 1
+    with pytest.raises(RuntimeError, match="free face has no PML pad"):
         _lib.call("sweep_b200_elastic_sizes", e, _lib.MEM_BOUNDARY, 0, ws, tape)
+    e.pad[3] = 0
+    _lib.call("sweep_b200_elastic_sizes", e, _lib.MEM_BOUNDARY, 0, ws, tape)
     eq = Elastic(spatial_order=8, device="cpu")
     s = PropTorch(eq, shape=(30, 40), dh=5.0, dt=0.0005, abcn=8, device="cpu", free_surface=True)
     assert s.pads == [0, 8, 8, 8] and s.runtime_shape == (30 + 8 + 8, 40 + 16 + 8)
-    with pytest.raises(NotImplementedError, match="top face only"):
-        PropTorch(eq, shape=(30, 40), dh=5.0, dt=0.0005, abcn=8, device="cpu", free_surface=["left"])
+    s = PropTorch(eq, shape=(30, 40), dh=5.0, dt=0.0005, abcn=8, device="cpu", free_surface=["left", "bottom"])
+    assert s.pads == [8, 0, 0, 8] and s.runtime_shape == (30 + 8 + 8, 40 + 8 + 8)

@@ -1,7 +1,8 @@
-"""Elastic traction-free top face on the GPU (reference PropTorch(Elastic,
-free_surface=True): the image method, the 2nd-order rows under the surface,
-the Robertsson sxx correction and szz = 0 on the surface row, and their exact
-transposes in the adjoint).
+"""Elastic traction-free faces on the GPU (reference PropTorch(Elastic,
+free_surface=...)): the image method, the 2nd-order cells next to a surface,
+the Robertsson corrections and the zeroed normal (and, on high-side faces,
+shear) stresses on the surface rows and columns, and their exact transposes
+in the adjoint.
 
 Bars: records within 1e-4 and vp / vs / rho gradients within 1e-3 relative L2
 of the reference's own run (golden fixture) and of the float32 CPU oracle."""
@@ -120,3 +121,65 @@ def test_velocity_sources_and_strip_formats():
     _, g16 = _grad_run(s16, c["w"], c["src"], c["rec"], [c["vp"], c["vs"], c["rho"]], c["obs"])
     for g, gb in zip(grads, g16):
         assert rel(gb, g) < 2e-2
+
+
+@pytest.mark.parametrize("tag,faces", [("br", ["bottom", "right"]), ("tl", ["top", "left"]),
+                                       ("all", ["top", "bottom", "left", "right"])])
+def test_free_faces_match_reference_golden(tag, faces):
+    """Traction-free faces per edge: high-side images with zeroed shear, the
+    x-normal correction of szz, corners; (vx, vz, sxx) receivers on the
+    surface rows and columns."""
+    from sweep_b200 import Elastic, PropTorch
+    d = load("elastic2d_free_faces")
+    s = PropTorch(Elastic(spatial_order=8, device=DEV), shape=tuple(d["vp_true"].shape), dh=float(d["dh"]),
+                  dt=float(d["dt"]), abcn=int(d["abcn"]), device=DEV, free_surface=faces,
+                  receiver_type=["vx", "vz", "sxx"])
+    with torch.no_grad():
+        obs = s(torch.tensor(d["wavelet"], device=DEV), d["src"], d["rec"],
+                models=[torch.tensor(d[k], device=DEV) for k in ("vp_true", "vs_true", "rho_true")])
+    assert rel(obs.cpu().numpy(), d[f"obs_{tag}"]) < REC_TOL
+    pred, (gvp, gvs, grho) = _grad_run(s, d["wavelet"], d["src"], d["rec"],
+                                       [d["vp_init"], d["vs_init"], d["rho_init"]], d[f"obs_{tag}"])
+    print(f"elastic free faces {faces} vs reference: record {rel(pred, d[f'pred_{tag}']):.2e} "
+          f"vp {rel(gvp, d[f'grad_vp_{tag}']):.2e} vs {rel(gvs, d[f'grad_vs_{tag}']):.2e} "
+          f"rho {rel(grho, d[f'grad_rho_{tag}']):.2e}")
+    assert rel(pred, d[f"pred_{tag}"]) < REC_TOL
+    assert rel(gvp, d[f"grad_vp_{tag}"]) < GRAD_TOL
+    assert rel(gvs, d[f"grad_vs_{tag}"]) < GRAD_TOL
+    assert rel(grho, d[f"grad_rho_{tag}"]) < GRAD_TOL
+
+
+@pytest.mark.parametrize("shape,faces,B", [((48, 48), ["bottom", "right"], 3),
+                                           ((70, 100), ["top", "bottom", "left", "right"], 4)])
+def test_free_faces_match_oracle(shape, faces, B):
+    """Surface rows and columns on tile edges (48 x 48 with CPML 12 puts the
+    bottom row and the right column on the last row / column of a tile),
+    several shots per CTA, (vx, vz, szz, sxz) receivers on the surfaces,
+    against the float32 oracle."""
+    from sweep_b200 import Elastic, PropTorch
+    nz, nx = shape
+    rng = np.random.default_rng(17)
+    vp = (2000.0 + 300.0 * rng.random(shape)).astype(np.float32)
+    vs = (vp / 1.8).astype(np.float32)
+    rho = (300.0 * vp ** 0.25).astype(np.float32)
+    nt, dt, dh, abcn = 420, 0.0005, 5.0, 12
+    t = np.arange(nt) * dt
+    a = (np.pi * 30 * (t - 0.035)) ** 2
+    w = ((1 - 2 * a) * np.exp(-a)).astype(np.float32)
+    src = np.stack([np.linspace(3, nx - 4, B), np.linspace(nz - 3, 2, B)], 1).astype(np.int64)
+    rec = np.zeros((B, 16, 2), np.int64)
+    rec[:, :8, 0] = np.linspace(0, nx - 1, 8).astype(np.int64)
+    rec[:, :8, 1] = nz - 1
+    rec[:, 8:, 0] = nx - 1
+    rec[:, 8:, 1] = np.linspace(0, nz - 1, 8).astype(np.int64)
+    fields = ["vx", "vz", "szz", "sxz"]
+    obs = (0.3 * rng.standard_normal((B, nt, 16, 4)) * 1e-9).astype(np.float32)
+    s = PropTorch(Elastic(spatial_order=8, device=DEV), shape=shape, dh=dh, dt=dt, abcn=abcn, device=DEV,
+                  free_surface=faces, receiver_type=fields)
+    pred, grads = _grad_run(s, w, src, rec, [vp, vs, rho], obs)
+    run = O.Elastic2D(vp, vs, rho, w, src, rec, dh, dt, abcn, receiver_fields=tuple(fields), free_surface=faces)
+    p_o = run.forward(keep_tape=True)
+    g_o = run.backward(p_o - obs)
+    assert rel(pred, p_o) < REC_TOL
+    for g, go in zip(grads, g_o):
+        assert rel(g, go) < GRAD_TOL
