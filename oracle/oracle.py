@@ -103,6 +103,14 @@ def _lib(prec: str):
         lib.oracle_el2d_forward.argtypes = geo_el + [P, P]
         lib.oracle_el2d_backward.restype = i
         lib.oracle_el2d_backward.argtypes = geo_el + [P, P, P, P, P]
+        geo_el3 = [i, i, i, i, i, i, P, real, real, real, real, P, P, P, P, P, l,
+                   i, P, P, i, P, i, P, i, P]
+        lib.oracle_el3d_tape_len.restype = l
+        lib.oracle_el3d_tape_len.argtypes = [i, i, i, i, i, i, P]
+        lib.oracle_el3d_forward.restype = i
+        lib.oracle_el3d_forward.argtypes = geo_el3 + [P, P]
+        lib.oracle_el3d_backward.restype = i
+        lib.oracle_el3d_backward.argtypes = geo_el3 + [P, P, P, P, P]
         _LIBS[prec] = _FlushToZero(lib)
     return _LIBS[prec]
 
@@ -503,3 +511,103 @@ def elastic_gradient(vp, vs, rho, wavelet, src, rec, obs, dh, dt, abcn, order=8,
 def elastic_forward(vp, vs, rho, wavelet, src, rec, dh, dt, abcn, order=8, prec="f32", **kw):
     return Elastic2D(vp, vs, rho, wavelet, src, rec, dh, dt, abcn, order, prec, **kw).forward(
         keep_tape=False)
+
+
+ELASTIC3D_FIELDS = ("vx", "vy", "vz", "sxx", "syy", "szz", "sxy", "sxz", "syz")
+
+
+class Elastic3D:
+    """3-D isotropic elastic oracle run (``fd_oracle_el3d.c``): models
+    ``vp, vs, rho`` of shape ``(nz, ny, nx)`` or per shot ``(B, nz, ny, nx)``;
+    coordinates ``(x, y, z)``; source fields default to the explosive
+    ``(sxx, syy, szz)``, receiver fields to ``(vx, vy, vz)``
+    (``src/sweep/equations/elastic3d.py:326-332``)."""
+
+    def __init__(self, vp, vs, rho, wavelet, src, rec, dh, dt, abcn, order=8, prec="f32",
+                 source_fields=("sxx", "syy", "szz"), receiver_fields=("vx", "vy", "vz"),
+                 max_vel=4500.0, pml_freq=25.0):
+        self.prec = prec
+        self.real = np.float32 if prec == "f32" else np.float64
+        models = [np.asarray(m, np.float32) for m in (vp, vs, rho)]
+        self.per_shot = models[0].ndim == 4
+        self.M = M = order // 2
+        w, s, r = _batch_io(wavelet, src, rec, 3)
+        self.B, self.nt = w.shape[0], w.shape[-1]
+        self.phys = models[0].shape[-3:]
+        self.pad = abcn
+        self.shape = tuple(n + 2 * abcn + 2 * M for n in self.phys)
+        padw = [(abcn + M, abcn + M)] * 3
+        lead = [(0, 0)] if self.per_shot else []
+        self.models = [np.ascontiguousarray(np.pad(m, lead + padw, mode="edge").astype(self.real))
+                       for m in models]
+        self.m_stride = int(np.prod(self.shape)) if self.per_shot else 0
+        sp = dh if np.ndim(dh) else [dh] * 3
+        self.spacing = [float(x) for x in sp]
+        self.dt = float(dt)
+        prof = cpml_profiles_s([abcn] * 6, M, dt, self.spacing, self.shape, max_vel, pml_freq)
+        self.prof = np.ascontiguousarray(np.concatenate([np.concatenate(p) for p in prof]).astype(self.real))
+        c = staggered_coefficients(M)
+        self.coef = np.array([0.0] + [float(x) for x in c], np.float64).astype(self.real)
+        if self.real is np.float32:
+            self.coef = np.array([0.0] + [np.float32(float(x)) for x in c], np.float32)
+        off = abcn + M
+        self.src = np.ascontiguousarray((s + off).astype(np.int32))
+        self.rec = np.ascontiguousarray((r + off).astype(np.int32))
+        self.wavelet = np.ascontiguousarray(w.astype(self.real))
+        self.nrec = self.rec.shape[1]
+        self.sf = np.array([ELASTIC3D_FIELDS.index(f) for f in source_fields], np.int32)
+        self.rf = np.array([ELASTIC3D_FIELDS.index(f) for f in receiver_fields], np.int32)
+
+    def _geo(self):
+        nz, ny, nx = self.shape
+        self._pad = np.array([self.pad] * 6, np.int32)
+        return [self.B, nz, ny, nx, self.nt, self.M, _ptr(self._pad), self.dt, self.spacing[0],
+                self.spacing[1], self.spacing[2], _ptr(self.coef), _ptr(self.prof), _ptr(self.models[0]),
+                _ptr(self.models[1]), _ptr(self.models[2]), self.m_stride,
+                1, _ptr(self.src), _ptr(self.wavelet), len(self.sf), _ptr(self.sf),
+                self.nrec, _ptr(self.rec), len(self.rf), _ptr(self.rf)]
+
+    def crop(self, g):
+        M, a = self.M, self.pad
+        sl = tuple(slice(a + M, a + M + n) for n in self.phys)
+        return g[(Ellipsis,) + sl]
+
+    def forward(self, keep_tape=True):
+        """Records ``(B, nt, nrec, nfield)``."""
+        lib = _lib(self.prec)
+        nz, ny, nx = self.shape
+        rec = np.zeros((self.B, self.nt, self.nrec, len(self.rf)), self.real)
+        self.tape = None
+        if keep_tape:
+            pad = np.array([self.pad] * 6, np.int32)
+            n = lib.oracle_el3d_tape_len(self.B, nz, ny, nx, self.nt, self.M, _ptr(pad))
+            self.tape = np.zeros(n, self.real)
+        rc = lib.oracle_el3d_forward(*self._geo(), _ptr(rec), _ptr(self.tape) if keep_tape else None)
+        assert rc == 0
+        return rec
+
+    def backward(self, adj):
+        """``adj``: record cotangent ``(B, nt, nrec, nfield)``; returns the
+        cropped ``(grad_vp, grad_vs, grad_rho)``."""
+        lib = _lib(self.prec)
+        a = np.ascontiguousarray(np.asarray(adj).astype(self.real))
+        shp = ((self.B,) if self.per_shot else ()) + self.shape
+        g = [np.zeros(shp, self.real) for _ in range(3)]
+        rc = lib.oracle_el3d_backward(*self._geo(), _ptr(a), _ptr(self.tape), _ptr(g[0]), _ptr(g[1]),
+                                      _ptr(g[2]))
+        assert rc == 0
+        return tuple(self.crop(x) for x in g)
+
+
+def elastic3d_gradient(vp, vs, rho, wavelet, src, rec, obs, dh, dt, abcn, order=8, prec="f32", **kw):
+    """Record, loss ``0.5 ||pred - obs||^2`` and cropped ``(vp, vs, rho)``
+    gradients of the 3-D elastic oracle (summed over shots for shared models)."""
+    run = Elastic3D(vp, vs, rho, wavelet, src, rec, dh, dt, abcn, order, prec, **kw)
+    pred = run.forward(keep_tape=True)
+    res = pred - np.asarray(obs, run.real)
+    loss = 0.5 * float(np.sum(res.astype(np.float64) ** 2))
+    return pred, loss, run.backward(res)
+
+
+def elastic3d_forward(vp, vs, rho, wavelet, src, rec, dh, dt, abcn, order=8, prec="f32", **kw):
+    return Elastic3D(vp, vs, rho, wavelet, src, rec, dh, dt, abcn, order, prec, **kw).forward(keep_tape=False)

@@ -697,6 +697,43 @@ def elastic2d_free_faces():
     np.savez_compressed(OUT / "elastic2d_free_faces.npz", **out)
 
 
+def elastic3d():
+    """3-D isotropic elastic (reference sweep.equations.Elastic3D, order 8):
+    2 explosive shots on a 20 x 22 x 24 layered model (CPML 6), (vx, vy, vz)
+    receivers, vp/vs/rho gradients, boundary saving; a third run with
+    body-force sources on (vx, vz) and (vx, vz, syy) receivers."""
+    from sweep.equations import Elastic3D
+    rng = np.random.default_rng(91)
+    nz, ny, nx, nt, dt, dh, abcn = 20, 22, 24, 160, 0.0005, 5.0, 6
+    base = _layered(nz, nx, rng, 1900.0, 3000.0, 3)
+    vp_true = np.ascontiguousarray(np.repeat(base[:, None, :], ny, axis=1)
+                                   * (1 + 0.02 * np.sin(np.arange(ny) / 3.0))[None, :, None]).astype(np.float32)
+    vs_true = (vp_true / 1.73).astype(np.float32)
+    rho_true = (310.0 * vp_true ** 0.25).astype(np.float32)
+    vp_init = np.full((nz, ny, nx), 2300.0, np.float32)
+    vs_init = (vp_init / 1.73).astype(np.float32)
+    rho_init = (310.0 * vp_init ** 0.25).astype(np.float32)
+    w = _wavelet(nt, dt, 30.0, 0.03)
+    src = np.array([[8, 10, 6], [16, 12, 13]], np.int64)            # (x, y, z)
+    rec = np.zeros((2, 10, 3), np.int64)
+    for b in range(2):
+        rec[b, :, 0] = np.linspace(1, nx - 2, 10).astype(np.int64)
+        rec[b, :, 1] = np.linspace(2, ny - 3, 10).astype(np.int64)
+        rec[b, :, 2] = 2 + 3 * b
+    out = dict(nz=nz, ny=ny, nx=nx, nt=nt, dt=dt, dh=dh, abcn=abcn, order=8,
+               vp_true=vp_true, vs_true=vs_true, rho_true=rho_true,
+               vp_init=vp_init, vs_init=vs_init, rho_init=rho_init, wavelet=w, src=src, rec=rec)
+    for tag, kw in (("", {}), ("_vsrc", dict(source_type=["vx", "vz"], receiver_type=["vx", "vz", "syy"]))):
+        eq = Elastic3D(spatial_order=8, device="cpu")
+        solver = PropTorch(eq, shape=(nz, ny, nx), dh=dh, dt=dt, abcn=abcn, impl="c", device="cpu",
+                           memory=BoundarySaving(), **kw)
+        obs = _forward(solver, w, src, rec, [vp_true, vs_true, rho_true])
+        r = _run(solver, w, src, rec, [vp_init, vs_init, rho_init], obs, False)
+        out.update({f"obs{tag}": obs, f"pred{tag}": r["pred"], f"loss{tag}": r["loss"],
+                    f"grad_vp{tag}": r["grad0"], f"grad_vs{tag}": r["grad1"], f"grad_rho{tag}": r["grad2"]})
+    np.savez_compressed(OUT / "elastic3d.npz", **out)
+
+
 CASES = {
     "acoustic2d_c1": acoustic2d_c1,
     "acoustic2d_multi": acoustic2d_multi,
@@ -717,6 +754,7 @@ CASES = {
     "elastic2d_interior": elastic2d_interior,
     "elastic2d_free_surface": elastic2d_free_surface,
     "elastic2d_free_faces": elastic2d_free_faces,
+    "elastic3d": elastic3d,
 }
 
 if __name__ == "__main__":

@@ -255,3 +255,27 @@ def test_library_tables_equal_the_oracle_restatement():
     for M in range(1, 7):
         lib, ora = centred_tables(M), O.fd_tables(M)
         assert np.array_equal(lib[0], ora[0]) and np.array_equal(lib[1], ora[1]), M
+
+
+@pytest.mark.parametrize("prec,tol", [("f32", 2e-6), ("f64", 5e-6)])
+@pytest.mark.parametrize("tag,kw", [("", {}),
+                                    ("_vsrc", dict(source_fields=("vx", "vz"), receiver_fields=("vx", "vz", "syy")))])
+def test_elastic3d_oracle_matches_reference(prec, tol, tag, kw):
+    """3-D isotropic elastic (reference Elastic3D, order 8, boundary saving):
+    explosive sources with (vx, vy, vz) receivers, and body-force sources on
+    (vx, vz) with (vx, vz, syy) receivers; records and vp / vs / rho
+    gradients."""
+    d = np.load(GOLD / "elastic3d.npz")
+    args = (float(d["dh"]), float(d["dt"]), int(d["abcn"]))
+    obs = O.elastic3d_forward(d["vp_true"], d["vs_true"], d["rho_true"], d["wavelet"], d["src"], d["rec"],
+                              *args, prec=prec, **kw)
+    assert obs.shape == d[f"obs{tag}"].shape
+    assert rel(obs, d[f"obs{tag}"]) < tol
+    pred, loss, (gvp, gvs, grho) = O.elastic3d_gradient(
+        d["vp_init"], d["vs_init"], d["rho_init"], d["wavelet"], d["src"], d["rec"], d[f"obs{tag}"],
+        *args, prec=prec, **kw)
+    assert rel(pred, d[f"pred{tag}"]) < tol
+    assert abs(loss - float(d[f"loss{tag}"])) < 1e-5 * float(d[f"loss{tag}"])
+    assert rel(gvp, d[f"grad_vp{tag}"]) < 5 * tol
+    assert rel(gvs, d[f"grad_vs{tag}"]) < 5 * tol
+    assert rel(grho, d[f"grad_rho{tag}"]) < 5 * tol
