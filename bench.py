@@ -466,8 +466,105 @@ class Acoustic3DWorkload:
         return A3_RT[0] ** 3 * shots * nt_sample, time.perf_counter() - t0
 
 
+# 3-D elastic workload (--workload elastic3d): 128^3, dh 10 m, dt 0.8 ms,
+# nt 600, order 8, CPML 16; 6-layer dipping model (1800-4200 m/s), vs =
+# vp / 1.73, rho = 310 vp^0.25; 4 explosive shots on a 2 x 2 surface grid, a
+# 64 x 64 three-component receiver array at 2-cell spacing, 15 Hz Ricker.
+E3_N, E3_NT, E3_DT, E3_DH, E3_ABCN = 128, 600, 0.0008, 10.0, 16
+E3_NSHOT, E3_F0, E3_DELAY = 4, 15.0, 0.08
+E3_RT = (E3_N + 2 * E3_ABCN + 2 * M,) * 3
+# algorithmic bytes per runtime cell-step: forward velocity 3 + 3 written, 6
+# stresses read; stress 6 read + 6 written, 3 velocities read (models and
+# CPML memories not counted); reverse: the two reconstructions (24), the
+# stress-adjoint prepare and apply (6 + 9 + 9 + 3 + 3 + 3 imaging reads and
+# 9 writes of q, 3 + 3 gradient slots read and written) and the
+# velocity-adjoint prepare and apply (3 + 9 + 9 + 6 + 6)
+E3_BYTES_FWD, E3_BYTES_REV = 4 * 21, 4 * 108
+
+
+def elastic3d_survey(seed=SEED):
+    from scipy.ndimage import gaussian_filter
+    from sweep_b200 import ricker
+    rng = np.random.default_rng(seed + 13)
+    n = E3_N
+    z, y, x = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    depth = np.sort(rng.uniform(0.1 * n, 0.9 * n, 5))
+    vel = np.linspace(1800.0, 4200.0, 6)
+    idx = np.zeros((n, n, n), np.int32)
+    for d0 in depth:
+        strike = rng.uniform(0, 2 * np.pi)
+        dip = np.deg2rad(rng.uniform(0, 12))
+        surf = d0 + np.tan(dip) * ((x - n / 2) * np.cos(strike) + (y - n / 2) * np.sin(strike))
+        idx += (z > surf).astype(np.int32)
+    vp_true = vel[idx].astype(np.float32)
+    courant = float(vp_true.max()) * E3_DT / E3_DH
+    if courant >= 0.4547:
+        raise ValueError(f"3-D elastic survey: Courant number {courant:.3f} above the staggered order-8 limit")
+    vp_init = gaussian_filter(vp_true.astype(np.float64), 6.0).astype(np.float32)
+    models = []
+    for vp in (vp_true, vp_init):
+        models.append([vp, (vp / 1.73).astype(np.float32), (310.0 * vp ** 0.25).astype(np.float32)])
+    g = np.linspace(n / 4, n - n / 4, 2).astype(np.int64)
+    src = np.array([[xs, ys, 3] for ys in g for xs in g], np.int64)
+    r = np.arange(0, 2 * 64, 2)
+    rx, ry = np.meshgrid(r, r, indexing="xy")
+    one = np.stack([rx.ravel(), ry.ravel(), np.full(rx.size, 3)], -1)
+    rec = np.broadcast_to(one, (E3_NSHOT,) + one.shape).copy()
+    w = ricker(np.arange(E3_NT) * E3_DT - E3_DELAY, E3_F0).astype(np.float32)
+    return models[0], models[1], w, src, rec
+
+
+class Elastic3DWorkload:
+    name = "elastic3d"
+    nt, nshot, rt = E3_NT, E3_NSHOT, E3_RT
+    bytes_fwd, bytes_rev = E3_BYTES_FWD, E3_BYTES_REV
+    kernel = ("sweep::el3d reverse step (srev3 + sprep3 + sapp3 + vprep3 + vapp3 + cap3 + vrev3 + strip "
+              "kernels)")
+    cpu_nt = 24
+    traffic = None
+
+    def config(self, args):
+        return {"workload": f"elastic3d {E3_N}^3 (runtime {E3_RT[0]}^3), {E3_NSHOT} shots, nt {E3_NT}, "
+                            f"order 8, CPML {E3_ABCN}, vp/vs/rho fwd+adj gradient, boundary saving",
+                "grid": [E3_N] * 3, "runtime_grid": list(E3_RT), "shots_per_gpu": E3_NSHOT, "nt": E3_NT,
+                "dh": E3_DH, "dt": E3_DT, "abcn": E3_ABCN, "order": ORDER, "receivers": 64 * 64,
+                "seed": SEED, "cells_counted": "runtime grid (physical + PML + halo) x shots x nt",
+                "physical_fraction": (E3_N / E3_RT[0]) ** 3,
+                "l2": "working set per step > L2 (inputs larger than L2; no flush)",
+                "parallelism": f"shots: {E3_NSHOT} per GPU x {args.gpus} GPU(s)"}
+
+    dh, dt, abcn, ref_gpu_nt = E3_DH, E3_DT, E3_ABCN, 200
+
+    def survey_inputs(self):
+        return elastic3d_survey()
+
+    def build(self, dev):
+        from sweep_b200 import Elastic3D, PropTorch
+        m_true, m_init, w, src, rec = elastic3d_survey()
+        solver = PropTorch(Elastic3D(spatial_order=ORDER, device=dev), shape=(E3_N,) * 3, dh=E3_DH,
+                           dt=E3_DT, abcn=E3_ABCN, device=dev)
+        return solver, m_true, m_init, w, src, rec
+
+    def launches(self, group):
+        # forward 5 per step (velocity, stress, source, strips, record);
+        # reverse 12 (body-force correction only with velocity sources: not
+        # here; residuals, source removal, two reconstructions, two restores,
+        # two prepares, two applies, carriers, receiver rho); prep3 and three
+        # finalize3 per pass
+        return 5 * self.nt + 12 * (self.nt - 1) + 4
+
+    def cpu_run(self, nt_sample, shots=1):
+        from oracle import oracle as O
+        m_true, m_init, w, src, rec = elastic3d_survey()
+        w, src, rec = w[:nt_sample], src[:shots], rec[:shots]
+        obs = O.elastic3d_forward(*m_true, w, src, rec, E3_DH, E3_DT, E3_ABCN)
+        t0 = time.perf_counter()
+        O.elastic3d_gradient(*m_init, w, src, rec, obs, E3_DH, E3_DT, E3_ABCN)
+        return E3_RT[0] ** 3 * shots * nt_sample, time.perf_counter() - t0
+
+
 WORKLOADS = {"acoustic2d": AcousticWorkload, "acoustic2d_c1": AcousticC1Workload, "elastic2d": ElasticWorkload,
-             "acoustic3d": Acoustic3DWorkload}
+             "acoustic3d": Acoustic3DWorkload, "elastic3d": Elastic3DWorkload}
 
 
 def cpu_threads():
@@ -524,14 +621,14 @@ def reference_cuda(wl, group, nt_sample, dev, reps=2):
     if str(REF_DIR) not in sys.path:
         sys.path.insert(0, str(REF_DIR))
     try:
-        from sweep.equations import Acoustic, Acoustic3D, Elastic
+        from sweep.equations import Acoustic, Acoustic3D, Elastic, Elastic3D
         from sweep.propagator.options import BoundarySaving
         from sweep.propagator.torch import PropTorch
     except Exception as e:                       # noqa: BLE001
         return {"unavailable": f"the reference does not import: {e}"}
     m_true, m_init, w, src, rec = wl.survey_inputs()
     eq = {"acoustic2d": Acoustic, "acoustic2d_c1": Acoustic, "elastic2d": Elastic,
-          "acoustic3d": Acoustic3D}[wl.name]
+          "acoustic3d": Acoustic3D, "elastic3d": Elastic3D}[wl.name]
     solver = PropTorch(eq(spatial_order=ORDER, device=dev), shape=tuple(m_true[0].shape), dh=wl.dh,
                        dt=wl.dt, abcn=wl.abcn, impl="c", device=dev, memory=BoundarySaving())
     wt = torch.tensor(w[:nt_sample], device=dev)

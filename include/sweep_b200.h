@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define SWEEP_B200_ABI_VERSION 5
+#define SWEEP_B200_ABI_VERSION 6
 
 #if defined(__GNUC__)
 #define SWEEP_B200_API __attribute__((visibility("default")))
@@ -207,6 +207,51 @@ SWEEP_B200_API int sweep_b200_elastic_backward(const sweep_elastic_desc* d, int3
                                                float* grad_vp, float* grad_vs, float* grad_rho,
                                                void* workspace, int64_t workspace_bytes,
                                                void* stream, char* err, int32_t err_cap);
+
+/* 3-D isotropic elastic problem (velocity-stress, staggered grid; reference
+ * sweep.equations.Elastic3D, entries 66-70: capi.h:105-110,
+ * elastic3d/driver_traits.cuh).  Wavefield indices: 0 vx, 1 vy, 2 vz, 3 sxx,
+ * 4 syy, 5 szz, 6 sxy, 7 sxz, 8 syz (reference common/elastic.h:736-749).
+ * Memory: boundary saving with fp32 strips in device memory (mem_mode
+ * SWEEP_MEM_BOUNDARY); the other modes are refused. */
+typedef struct sweep_elastic3d_desc {
+    int32_t B;               /* shots advanced together */
+    int32_t nz, ny, nx;      /* runtime grid */
+    int32_t nt;              /* time steps */
+    int32_t M;               /* stencil half-width (spatial order / 2); 4 */
+    int32_t pad[6];          /* PML pad per face: z_lo, z_hi, y_lo, y_hi, x_lo, x_hi */
+    float dt, dz, dy, dx;
+    const float *az, *bz, *azh, *bzh;   /* staggered CPML profiles per axis: */
+    const float *ay, *by, *ayh, *byh;   /* integer and half-cell positions */
+    const float *ax, *bx, *axh, *bxh;
+    const float *vp, *vs, *rho;  /* (B|1, nz, ny, nx) models on the runtime grid */
+    int64_t model_stride;    /* 0: models shared by every shot; else nz * ny * nx */
+    int32_t nsrc;            /* sources per shot */
+    const int32_t* src_loc;  /* (B, nsrc, 3) runtime (x, y, z) */
+    const float* wavelet;    /* (B, nsrc, nt) amplitude added to every source field */
+    int32_t nsrc_fields;     /* 1..9 */
+    int32_t src_fields[9];   /* wavefield indices the wavelet is added to */
+    int32_t nrec;            /* receivers per shot (padded to a rectangle) */
+    const int32_t* rec_loc;  /* (B, nrec, 3) */
+    int32_t nrec_fields;     /* 1..9 */
+    int32_t rec_fields[9];   /* wavefield indices recorded, in record order */
+} sweep_elastic3d_desc;
+
+/* Sizes, forward and backward of the 3-D elastic problem, as the 2-D
+ * elastic entries (record (B, nt, nrec, nrec_fields); gradients (B|1, nz, ny,
+ * nx), OVERWRITTEN, zero outside the physical box). */
+SWEEP_B200_API int sweep_b200_elastic3d_sizes(const sweep_elastic3d_desc* d, int32_t mem_mode, int32_t ckpt_every,
+                                              int64_t* workspace_bytes, int64_t* tape_bytes,
+                                              char* err, int32_t err_cap);
+SWEEP_B200_API int sweep_b200_elastic3d_forward(const sweep_elastic3d_desc* d, int32_t mem_mode, int32_t ckpt_every,
+                                                float* record, void* tape,
+                                                void* workspace, int64_t workspace_bytes,
+                                                void* stream, char* err, int32_t err_cap);
+SWEEP_B200_API int sweep_b200_elastic3d_backward(const sweep_elastic3d_desc* d, int32_t mem_mode, int32_t ckpt_every,
+                                                 const float* adj, const void* tape,
+                                                 float* grad_vp, float* grad_vs, float* grad_rho,
+                                                 void* workspace, int64_t workspace_bytes,
+                                                 void* stream, char* err, int32_t err_cap);
 
 /* BF16 3x3 convolution (stride 1, zero padding 1) as an implicit GEMM on the
  * tensor cores with FP32 accumulation, for the learned FWI preconditioner.

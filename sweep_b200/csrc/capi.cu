@@ -3,6 +3,7 @@
 // into (non-zero return, message) -- nothing is thrown across the boundary.
 #include "acoustic2d.cuh"
 #include "elastic2d.cuh"
+#include "elastic3d.cuh"
 
 namespace sweep {
 namespace a3d {
@@ -91,6 +92,38 @@ extern "C" int sweep_b200_elastic_backward(const sweep_elastic_desc* d, int32_t 
     return guarded(err, err_cap, [&] {
         SWEEP_REQUIRE(d != nullptr, "null descriptor");
         el2d::backward(d, mem_mode, ckpt_every, adj, tape, grad_vp, grad_vs, grad_rho, workspace,
+                       workspace_bytes, static_cast<cudaStream_t>(stream));
+    });
+}
+
+extern "C" int sweep_b200_elastic3d_sizes(const sweep_elastic3d_desc* d, int32_t mem_mode, int32_t ckpt_every,
+                                          int64_t* workspace_bytes, int64_t* tape_bytes, char* err, int32_t err_cap)
+{
+    return guarded(err, err_cap, [&] {
+        SWEEP_REQUIRE(d && workspace_bytes && tape_bytes, "null argument");
+        el3d::sizes(d, mem_mode, ckpt_every, workspace_bytes, tape_bytes);
+    });
+}
+
+extern "C" int sweep_b200_elastic3d_forward(const sweep_elastic3d_desc* d, int32_t mem_mode, int32_t ckpt_every,
+                                            float* record, void* tape, void* workspace, int64_t workspace_bytes,
+                                            void* stream, char* err, int32_t err_cap)
+{
+    return guarded(err, err_cap, [&] {
+        SWEEP_REQUIRE(d != nullptr, "null descriptor");
+        el3d::forward(d, mem_mode, ckpt_every, record, tape, workspace, workspace_bytes,
+                      static_cast<cudaStream_t>(stream));
+    });
+}
+
+extern "C" int sweep_b200_elastic3d_backward(const sweep_elastic3d_desc* d, int32_t mem_mode, int32_t ckpt_every,
+                                             const float* adj, const void* tape, float* grad_vp, float* grad_vs,
+                                             float* grad_rho, void* workspace, int64_t workspace_bytes,
+                                             void* stream, char* err, int32_t err_cap)
+{
+    return guarded(err, err_cap, [&] {
+        SWEEP_REQUIRE(d != nullptr, "null descriptor");
+        el3d::backward(d, mem_mode, ckpt_every, adj, tape, grad_vp, grad_vs, grad_rho, workspace,
                        workspace_bytes, static_cast<cudaStream_t>(stream));
     });
 }

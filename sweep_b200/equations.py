@@ -1,8 +1,9 @@
 """Equation descriptors of the hot path, mirroring the reference's
 ``src/sweep/equations/acoustic.py:48-133`` (``Acoustic``),
-``acoustic3d.py:50-185`` (``Acoustic3D``) and ``elastic.py:19-310``
-(``Elastic``): the constructor keywords, model names and default
-source / receiver fields the propagator reads."""
+``acoustic3d.py:50-185`` (``Acoustic3D``), ``elastic.py:19-310``
+(``Elastic``) and ``elastic3d.py:235-332`` (``Elastic3D``): the constructor
+keywords, model names and default source / receiver fields the propagator
+reads."""
 from __future__ import annotations
 
 
@@ -69,3 +70,15 @@ class Elastic(_Equation):
     RECEIVER_FIELDS = ("vx", "vz")
     FIELDS = ("vx", "vz", "sxx", "szz", "sxz")
     default_pml_type = "cpmls"
+
+
+class Elastic3D(Elastic):
+    """First-order 3-D isotropic elastic velocity-stress equation on a
+    staggered grid: fields vx, vy, vz, sxx, syy, szz, sxy, sxz, syz; models
+    vp, vs, rho; explosive source (sxx, syy, szz) and (vx, vy, vz) receivers
+    by default (reference ``equations/elastic3d.py:235-332``)."""
+    C_NAME = "elastic3d"
+    NDIM = 3
+    SOURCE_FIELDS = ("sxx", "syy", "szz")
+    RECEIVER_FIELDS = ("vx", "vy", "vz")
+    FIELDS = ("vx", "vy", "vz", "sxx", "syy", "szz", "sxy", "sxz", "syz")

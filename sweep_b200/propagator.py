@@ -33,7 +33,7 @@ import torch
 import torch.nn.functional as F
 
 from . import _lib
-from .equations import Acoustic, Acoustic3D, Elastic
+from .equations import Acoustic, Acoustic3D, Elastic, Elastic3D
 from .options import BoundarySaving, Ckpt, Full
 from .pml import cpml_profiles_r, cpml_profiles_s
 from .scalars import centred_tables, staggered_grid_coes
@@ -134,7 +134,7 @@ class _Geometry:
         # Elastic with free faces: the cells past a surface are air, which the
         # image method overwrites, so a source or receiver there is off the
         # grid (the reference would fold its adjoint back through the images)
-        self.fs_faces = tuple(prop.fs_faces) if isinstance(eq, Elastic) else (False,) * 4
+        self.fs_faces = tuple(prop.fs_faces) if isinstance(eq, Elastic) and self.ndim == 2 else (False,) * 4
         if any(self.fs_faces):
             src_rt, rec_rt = np.array(src_rt, np.int64), np.array(rec_rt, np.int64)
             nz, nx = self.shape
@@ -193,6 +193,8 @@ class _Geometry:
 
 
     def elastic_desc(self, models, wavelet, src_fields, rec_fields):
+        if self.ndim == 3:
+            return self.elastic3d_desc(models, wavelet, src_fields, rec_fields)
         vp, vs, rho = models
         d = _lib.ElasticDesc()
         d.B = self.B
@@ -222,6 +224,36 @@ class _Geometry:
             d.rec_fields[k] = f
         for f in range(4):
             d.free_surface[f] = 1 if self.fs_faces[f] else 0
+        return d
+
+
+    def elastic3d_desc(self, models, wavelet, src_fields, rec_fields):
+        vp, vs, rho = models
+        d = _lib.Elastic3DDesc()
+        d.B = self.B
+        d.nz, d.ny, d.nx = self.shape
+        d.nt = self.nt
+        d.M = self.M
+        for i in range(6):
+            d.pad[i] = self.pads[i]
+        d.dt = self.dt
+        d.dz, d.dy, d.dx = self.spacing
+        names = ("az", "bz", "azh", "bzh", "ay", "by", "ayh", "byh", "ax", "bx", "axh", "bxh")
+        for k, name in enumerate(names):
+            setattr(d, name, self.prof[k // 4][k % 4].data_ptr())
+        d.vp, d.vs, d.rho = vp.data_ptr(), vs.data_ptr(), rho.data_ptr()
+        d.model_stride = int(np.prod(self.shape)) if vp.dim() == 4 else 0
+        d.nsrc = self.nsrc
+        d.src_loc = self.src.data_ptr()
+        d.wavelet = wavelet.data_ptr()
+        d.nsrc_fields = len(src_fields)
+        for k, f in enumerate(src_fields):
+            d.src_fields[k] = f
+        d.nrec = self.nrec
+        d.rec_loc = self.rec.data_ptr()
+        d.nrec_fields = len(rec_fields)
+        for k, f in enumerate(rec_fields):
+            d.rec_fields[k] = f
         return d
 
 
@@ -297,8 +329,9 @@ class _ElasticFn(torch.autograd.Function):
         wavelet = wavelet.contiguous()
         sf, rf = fields
         desc = geo.elastic_desc(models, wavelet, sf, rf)
+        pre = "sweep_b200_elastic3d" if geo.ndim == 3 else "sweep_b200_elastic"
         ws_b, tape_b = _lib.c_i64(), _lib.c_i64()
-        _lib.call("sweep_b200_elastic_sizes", desc, mem_mode, ckpt_every, ws_b, tape_b)
+        _lib.call(pre + "_sizes", desc, mem_mode, ckpt_every, ws_b, tape_b)
         need_bwd = any(ctx.needs_input_grad[:3])
         dev = vp.device
         ws = prop._workspace(ws_b.value, dev)
@@ -309,7 +342,7 @@ class _ElasticFn(torch.autograd.Function):
         else:
             tape = torch.empty(tape_b.value, dtype=torch.uint8, device=dev)
         record = torch.empty((geo.B, geo.nt, geo.nrec, len(rf)), dtype=torch.float32, device=dev)
-        _lib.call("sweep_b200_elastic_forward", desc, mem_mode, ckpt_every, record.data_ptr(),
+        _lib.call(pre + "_forward", desc, mem_mode, ckpt_every, record.data_ptr(),
                   tape.data_ptr() if tape is not None else None, ws.data_ptr(), ws.numel(),
                   _stream_ptr(dev))
         ctx.save_for_backward(*models, wavelet)
@@ -327,11 +360,12 @@ class _ElasticFn(torch.autograd.Function):
         geo, prop = ctx.geo, ctx.prop
         adj = grad_record.to(torch.float32).contiguous()
         desc = geo.elastic_desc([vp, vs, rho], wavelet, *ctx.fields)
+        pre = "sweep_b200_elastic3d" if geo.ndim == 3 else "sweep_b200_elastic"
         ws_b, tape_b = _lib.c_i64(), _lib.c_i64()
-        _lib.call("sweep_b200_elastic_sizes", desc, ctx.mem_mode, ctx.ckpt_every, ws_b, tape_b)
+        _lib.call(pre + "_sizes", desc, ctx.mem_mode, ctx.ckpt_every, ws_b, tape_b)
         ws = prop._workspace(ws_b.value, vp.device)
         g = [torch.empty_like(vp) for _ in range(3)]
-        _lib.call("sweep_b200_elastic_backward", desc, ctx.mem_mode, ctx.ckpt_every, adj.data_ptr(),
+        _lib.call(pre + "_backward", desc, ctx.mem_mode, ctx.ckpt_every, adj.data_ptr(),
                   ctx.tape.data_ptr(), g[0].data_ptr(), g[1].data_ptr(), g[2].data_ptr(),
                   ws.data_ptr(), ws.numel(), _stream_ptr(vp.device))
         ctx.tape = None
@@ -377,6 +411,8 @@ class PropTorch(torch.nn.Module):
         if self.abcn < 1:
             raise NotImplementedError("sweep_b200: the absorbing faces need a layer (abcn >= 1)")
         self.fs_faces = free_faces(free_surface, nd)
+        if isinstance(equation, Elastic3D) and any(self.fs_faces):
+            raise NotImplementedError("sweep_b200: an Elastic3D free surface is not built")
         if nd == 3 and any(self.fs_faces[1:]):
             raise NotImplementedError("per-face free surfaces are 2-D only (as in the reference); "
                                       "3-D takes free_surface=True (the top face)")
@@ -455,7 +491,7 @@ class PropTorch(torch.nn.Module):
             if not kinds or missing:
                 raise ValueError(f"Invalid {role} entries {missing or kinds}; available wavefields are {names}")
         sf = [names.index(k) for k in self.source_type]
-        if len(set(sf)) != len(sf) or len(self.receiver_type) > 5:
+        if len(set(sf)) != len(sf) or len(self.receiver_type) > len(names):
             raise ValueError("source_type / receiver_type must not repeat a field")
         return sf, [names.index(k) for k in self.receiver_type]
 
@@ -479,7 +515,9 @@ class PropTorch(torch.nn.Module):
 
     def _tape_bytes(self, desc, fields, mem_mode, ckpt_every):
         ws_b, tape_b = _lib.c_i64(), _lib.c_i64()
-        name = "sweep_b200_elastic_sizes" if fields is not None else "sweep_b200_acoustic_sizes"
+        name = "sweep_b200_acoustic_sizes"
+        if fields is not None:
+            name = "sweep_b200_elastic3d_sizes" if isinstance(desc, _lib.Elastic3DDesc) else "sweep_b200_elastic_sizes"
         _lib.call(name, desc, mem_mode, ckpt_every, ws_b, tape_b)
         return int(tape_b.value)
 
@@ -517,7 +555,10 @@ class PropTorch(torch.nn.Module):
         """The schedule (resolved fields) a call with these inputs would run."""
         from . import autotune
         geo, padded, wb, fields = self._probe(wavelet_len, sources, receivers, models)
-        return autotune.get_schedule(self._desc(geo, padded, wb, fields))
+        desc = self._desc(geo, padded, wb, fields)
+        if isinstance(desc, _lib.Elastic3DDesc):
+            return {"fixed": "one thread per cell, 32 x 8 cell tiles per z plane and shot"}
+        return autotune.get_schedule(desc)
 
     def tape_bytes(self, wavelet_len, sources, receivers, models):
         """Bytes of the tape a gradient call with these inputs keeps between
@@ -594,11 +635,13 @@ class PropTorch(torch.nn.Module):
         mem_mode, ckpt_every = self._mem_mode()
         padded = [self._pad_model(m.to(dev)) for m in models]
         fields = self._elastic_fields() if isinstance(eq, Elastic) else None
+        if (self.autotune or self.schedule is not None) and isinstance(eq, Elastic3D):
+            raise NotImplementedError("sweep_b200: Elastic3D has one built-in launch schedule (no autotune)")
         if self.autotune or self.schedule is not None:
             self._apply_schedule(geo, padded, wb, fields, mem_mode, ckpt_every)
         mem_mode, ckpt_every = self._apply_budget(geo, padded, wb, fields, mem_mode, ckpt_every)
         if isinstance(eq, Elastic) and len({m.dim() for m in models}) != 1:
-            raise ValueError("vp, vs and rho must all be shared (nz, nx) or all per shot (B, nz, nx)")
+            raise ValueError("vp, vs and rho must all be shared or all per shot")
         return geo, padded, wb, fields, mem_mode, ckpt_every, wavelet
 
     # ------------------------------------------------------- stepped runners

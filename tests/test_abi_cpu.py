@@ -372,3 +372,29 @@ def test_elastic_free_surface_faces_checked():
     assert s.pads == [0, 8, 8, 8] and s.runtime_shape == (30 + 8 + 8, 40 + 16 + 8)
     s = PropTorch(eq, shape=(30, 40), dh=5.0, dt=0.0005, abcn=8, device="cpu", free_surface=["left", "bottom"])
     assert s.pads == [8, 0, 0, 8] and s.runtime_shape == (30 + 8 + 8, 40 + 8 + 8)
+
+
+def test_elastic3d_sizes_and_refusals():
+    """The 3-D elastic core sizes its workspace and tape on the host and
+    refuses what is not built (checkpoints, reduced strip formats, free
+    surfaces, launch schedules) before any device work."""
+    import numpy as np
+    import torch
+    from sweep_b200 import Ckpt, Elastic3D, PropTorch, _lib
+    eq = Elastic3D(spatial_order=8, device="cpu")
+    s = PropTorch(eq, shape=(20, 22, 24), dh=5.0, dt=0.0005, abcn=6, device="cpu")
+    assert s.runtime_shape == (40, 42, 44) and eq.default_source_fields == ["sxx", "syy", "szz"]
+    src, rec = np.array([[8, 10, 6]]), np.zeros((1, 4, 3), np.int64)
+    geo, padded, wb, fields = s._probe(50, src, rec, [torch.ones(20, 22, 24)] * 3)
+    d = s._desc(geo, padded, wb, fields)
+    ws, tape = _lib.c_i64(), _lib.c_i64()
+    _lib.call("sweep_b200_elastic3d_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
+    assert ws.value > 0 and tape.value > 50 * 9 * 4
+    for mode in (_lib.MEM_CHECKPOINT, _lib.MEM_BOUNDARY_FP16, _lib.MEM_BOUNDARY | _lib.MEM_HOST_TAPE):
+        with pytest.raises(RuntimeError, match="elastic3d"):
+            _lib.call("sweep_b200_elastic3d_sizes", d, mode, 10, ws, tape)
+    with pytest.raises(NotImplementedError, match="Elastic3D free surface"):
+        PropTorch(eq, shape=(20, 22, 24), dh=5.0, dt=0.0005, abcn=6, device="cpu", free_surface=True)
+    with pytest.raises(ValueError, match="source_type"):
+        PropTorch(eq, shape=(20, 22, 24), dh=5.0, dt=0.0005, abcn=6, device="cpu",
+                  source_type=["sxz", "pressure"])._elastic_fields()
