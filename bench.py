@@ -20,8 +20,8 @@ pinned host memory and the gradient and loss read back inside each step.
 
 Other workloads: ``acoustic2d`` (the 32-shot 256 x 768 survey: one step is
 the 32-shot gradient), ``elastic2d`` (the 16-shot 400 x 1200 elastic
-survey), ``acoustic2d_c1`` (96 x 128, one shot) and ``fwi`` (learned vs
-plain FWI).
+survey), ``elastic3d`` (the 4-shot 128^3 elastic survey), ``acoustic2d_c1``
+(96 x 128, one shot) and ``fwi`` (learned vs plain FWI).
 
 ``--gpus N`` without a launcher starts N ranks itself (torch.distributed.run
 on 127.0.0.1); under torchrun the ranks come from the environment.
@@ -473,13 +473,14 @@ class Acoustic3DWorkload:
 E3_N, E3_NT, E3_DT, E3_DH, E3_ABCN = 128, 600, 0.0008, 10.0, 16
 E3_NSHOT, E3_F0, E3_DELAY = 4, 15.0, 0.08
 E3_RT = (E3_N + 2 * E3_ABCN + 2 * M,) * 3
-# algorithmic bytes per runtime cell-step: forward velocity 3 + 3 written, 6
-# stresses read; stress 6 read + 6 written, 3 velocities read (models and
-# CPML memories not counted); reverse: the two reconstructions (24), the
-# stress-adjoint prepare and apply (6 + 9 + 9 + 3 + 3 + 3 imaging reads and
-# 9 writes of q, 3 + 3 gradient slots read and written) and the
-# velocity-adjoint prepare and apply (3 + 9 + 9 + 6 + 6)
-E3_BYTES_FWD, E3_BYTES_REV = 4 * 21, 4 * 108
+# algorithmic floats per runtime cell-step (one read and one write of every
+# field a kernel touches; models and CPML memories not counted): forward
+# velocity step 6 stresses read + 3 velocities read and written (12), stress
+# step 3 + 6 + 6 (15); reverse: stress reconstruction 15, stress-adjoint
+# prepare 6 + 3 + 3 + 3 read, 3 gradient slots read and written, 9 q written
+# (30), its apply 9 + 6 (15), velocity-adjoint prepare 3 + 9 (12), its apply
+# 9 + 12 (21), carriers 6, velocity reconstruction 12 (111)
+E3_BYTES_FWD, E3_BYTES_REV = 4 * 27, 4 * 111
 
 
 def elastic3d_survey(seed=SEED):
@@ -522,6 +523,7 @@ class Elastic3DWorkload:
               "kernels)")
     cpu_nt = 24
     traffic = None
+    tunable = False             # one built-in launch schedule
 
     def config(self, args):
         return {"workload": f"elastic3d {E3_N}^3 (runtime {E3_RT[0]}^3), {E3_NSHOT} shots, nt {E3_NT}, "
@@ -684,7 +686,7 @@ def run_gpu(args, wl):
 
     from sweep_b200.distributed import sharded_gradient
     solver, m_true, m_init, w, src, rec = wl.build(dev)
-    solver.autotune = bool(args.autotune)
+    solver.autotune = bool(args.autotune) and getattr(wl, "tunable", True)
     src, rec = src[:wl.nshot], rec[:wl.nshot]
     if getattr(wl, "budget_gb", None) and not args.shots_per_call:
         # shot groups: the most shots whose boundary-saving tape fits the budget
@@ -953,7 +955,8 @@ def main():
     ap.add_argument("--train-steps", type=int, default=20000, help="fwi workload: U-Net training steps")
     ap.add_argument("--workload", default="acoustic3d", choices=sorted(WORKLOADS) + ["fwi"],
                     help="acoustic3d: the 16-shot 256^3 survey (default); acoustic2d: the 32-shot 256x768 "
-                         "survey; elastic2d: the 16-shot 400x1200 elastic survey")
+                         "survey; elastic2d: the 16-shot 400x1200 elastic survey; elastic3d: the 4-shot "
+                         "128^3 elastic survey")
     ap.add_argument("--graph-steps", type=int, default=None,
                     help="time steps per captured CUDA graph in the step loops (0: plain stream launches; "
                          "default: the library's built-in choice)")
@@ -976,8 +979,8 @@ def main():
     wl = WORKLOADS[args.workload]()
     if args.nt:
         wl.nt = int(args.nt)
-        global NT, E_NT, A3_NT
-        NT, E_NT, A3_NT = wl.nt, wl.nt, wl.nt
+        global NT, E_NT, A3_NT, E3_NT
+        NT, E_NT, A3_NT, E3_NT = wl.nt, wl.nt, wl.nt, wl.nt
     if args.shots:
         wl.nshot = min(int(args.shots), wl.nshot)
     if args.shots_per_call and hasattr(wl, "batch"):

@@ -235,6 +235,10 @@ typedef struct sweep_elastic3d_desc {
     const int32_t* rec_loc;  /* (B, nrec, 3) */
     int32_t nrec_fields;     /* 1..9 */
     int32_t rec_fields[9];   /* wavefield indices recorded, in record order */
+    /* 1: traction-free top face (reference Elastic3D with free_surface=True:
+     * the full stencil over image values, Robertsson sxx / syy and szz = 0 on
+     * the surface row; common/elastic_free_surface.cuh:723-952); pad[0] = 0. */
+    int32_t free_surface;
 } sweep_elastic3d_desc;
 
 /* Sizes, forward and backward of the 3-D elastic problem, as the 2-D

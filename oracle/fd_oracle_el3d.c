@@ -27,6 +27,11 @@
  *   reverse order     equations/elastic3d/driver_traits.cuh:680-905,
  *                     524-640 (source and receiver rho corrections, signed
  *                     residuals: stress -1, velocity +1)
+ *   free top face     common/elastic_free_surface.cuh:723-952 (the full
+ *                     stencil over image values, its exact transpose), and
+ *                     elastic3d/kernels.cuh:360-372, 1421-1470, 1489-1499
+ *                     (Robertsson sxx / syy, szz = 0, their transposes and
+ *                     the surface row's image)
  */
 #include <stdlib.h>
 #include <string.h>
@@ -48,6 +53,7 @@ typedef struct {
     i64 ms;                     /* model stride between shots (0 = shared) */
     int nsrc; const int* src; const REAL* wavelet; int nsf; const int* sf;
     int nrec; const int* rec; int nrf; const int* rf;
+    int fs;                     /* 1: traction-free top face (pad[0] == 0) */
 } EL3;
 
 enum { VX, VY, VZ, SXX, SYY, SZZ, SXY, SXZ, SYZ,
@@ -68,6 +74,65 @@ static inline REAL dminus(const REAL* u, i64 i, i64 s, int M, const REAL* c, REA
     for (int k = 2; k <= M; ++k) g = g + c[k] * (u[i + (k - 1) * s] - u[i - k * s]);
     return g * inv;
 }
+
+/* ---- traction-free top face -----------------------------------------------
+ * The surface is the first physical row top = pad[0] + M; the rows above it
+ * are air, read by z-derivatives as the image of the row mirrored about the
+ * surface (about top for integer fields, top - 1/2 for fields half a cell
+ * below, negated for odd fields).  In 3-D the full stencil runs over those
+ * images (no reduced rows near the surface). */
+static inline REAL fs_at3(const EL3* p, const REAL* u, i64 base, i64 sz, int k, int odd, int half)
+{
+    const int top = p->pad[0] + p->M;
+    if (k < top) {
+        const int m = half ? 2 * top - 1 - k : 2 * top - k;
+        const REAL v = u[base + (i64)m * sz];
+        return odd ? -v : v;
+    }
+    return u[base + (i64)k * sz];
+}
+
+/* z-derivative at row iz of the column through `base` (row 0): fwd = 1 the
+ * D+ form, 0 the D- form; the plain stencil without a free surface. */
+static REAL dz3(const EL3* p, const REAL* u, i64 base, int iz, int fwd, int odd, int half)
+{
+    const i64 sz = (i64)p->nx * p->ny;
+    const i64 i = base + (i64)iz * sz;
+    if (!p->fs) return fwd ? dplus(u, i, sz, p->M, p->c, R(1) / p->dz) : dminus(u, i, sz, p->M, p->c, R(1) / p->dz);
+    REAL g = R(0);
+    for (int k = 1; k <= p->M; ++k) {
+        const REAL up = fwd ? fs_at3(p, u, base, sz, iz + k, odd, half) : fs_at3(p, u, base, sz, iz + k - 1, odd, half);
+        const REAL um = fwd ? fs_at3(p, u, base, sz, iz - k + 1, odd, half) : fs_at3(p, u, base, sz, iz - k, odd, half);
+        g = g + p->c[k] * (up - um);
+    }
+    return g / p->dz;
+}
+
+/* Exact transpose of dz3 (negated: the D- form for a D+ forward and vice
+ * versa): the direct taps from rows at or below the surface, and each air
+ * row's image folded back with the field's parity. */
+static REAL adz3(const EL3* p, const REAL* q, i64 base, int iz, int fwd, int odd, int half)
+{
+    const i64 sz = (i64)p->nx * p->ny;
+    const i64 i = base + (i64)iz * sz;
+    if (!p->fs) return fwd ? dminus(q, i, sz, p->M, p->c, R(1) / p->dz) : dplus(q, i, sz, p->M, p->c, R(1) / p->dz);
+    const int top = p->pad[0] + p->M, lo = half ? top - 1 : top;
+    const REAL parity = odd ? R(-1) : R(1);
+    REAL g = R(0);
+    for (int k = 1; k <= p->M; ++k) {
+        const int m = k - 1;
+        const int jp = fwd ? iz + m : iz + m + 1;
+        const int jm = fwd ? iz - m - 1 : iz - m;
+        const int jg = fwd ? (half ? 2 * top - 1 + m - iz : 2 * top + m - iz)
+                           : (half ? 2 * top + m - iz : 2 * top + m + 1 - iz);
+        if (jp >= top && jp < p->nz) g = g + p->c[k] * q[base + (i64)jp * sz];
+        if (jm >= top) g = g - p->c[k] * q[base + (i64)jm * sz];
+        if (iz > lo && jg >= top) g = g + p->c[k] * parity * q[base + (i64)jg * sz];
+    }
+    return g / p->dz;
+}
+
+static inline int surf_row(const EL3* p, int iz) { return p->fs && iz == p->pad[0] + p->M; }
 
 typedef struct { int z0, z1, y0, y1, x0, x1; } BOX;
 
@@ -109,19 +174,20 @@ static void velocity_step(const EL3* p, int b, REAL** F)
     const int nz = p->nz, ny = p->ny, nx = p->nx, M = p->M;
     const i64 sy = nx, sz = (i64)nx * ny;
     const REAL* rho = p->rho + b * p->ms;
-    const REAL ix_ = R(1) / p->dx, iy_ = R(1) / p->dy, iz_ = R(1) / p->dz;
+    const REAL ix_ = R(1) / p->dx, iy_ = R(1) / p->dy;
     const BOX bx_ = box_of(p);
     LOOP_CORE {
         const i64 i = iz * sz + iy * sy + ix;
+        const i64 col = i - iz * sz;
         REAL dsxx_dx = dplus(F[SXX], i, 1, M, p->c, ix_);
         REAL dsxy_dy = dminus(F[SXY], i, sy, M, p->c, iy_);
-        REAL dsxz_dz = dminus(F[SXZ], i, sz, M, p->c, iz_);
+        REAL dsxz_dz = dz3(p, F[SXZ], col, iz, 0, 1, 1);
         REAL dsxy_dx = dminus(F[SXY], i, 1, M, p->c, ix_);
         REAL dsyy_dy = dplus(F[SYY], i, sy, M, p->c, iy_);
-        REAL dsyz_dz = dminus(F[SYZ], i, sz, M, p->c, iz_);
+        REAL dsyz_dz = dz3(p, F[SYZ], col, iz, 0, 1, 1);
         REAL dsxz_dx = dminus(F[SXZ], i, 1, M, p->c, ix_);
         REAL dsyz_dy = dminus(F[SYZ], i, sy, M, p->c, iy_);
-        REAL dszz_dz = dplus(F[SZZ], i, sz, M, p->c, iz_);
+        REAL dszz_dz = dz3(p, F[SZZ], col, iz, 1, 1, 0);
         const REAL inv_rho = R(1) / rho[i];
         if (!interior(&bx_, ix, iy, iz)) {
             REAL m;
@@ -146,19 +212,19 @@ static void stress_step(const EL3* p, REAL** F, const REAL* lam_, const REAL* mu
 {
     const int nz = p->nz, ny = p->ny, nx = p->nx, M = p->M;
     const i64 sy = nx, sz = (i64)nx * ny;
-    const REAL ix_ = R(1) / p->dx, iy_ = R(1) / p->dy, iz_ = R(1) / p->dz;
+    const REAL ix_ = R(1) / p->dx, iy_ = R(1) / p->dy;
     const BOX bx_ = box_of(p);
     LOOP_CORE {
-        const i64 i = iz * sz + iy * sy + ix;
+        const i64 i = iz * sz + iy * sy + ix, col = i - iz * sz;
         REAL dvx_dx = dminus(F[VX], i, 1, M, p->c, ix_);
         REAL dvx_dy = dplus(F[VX], i, sy, M, p->c, iy_);
-        REAL dvx_dz = dplus(F[VX], i, sz, M, p->c, iz_);
+        REAL dvx_dz = dz3(p, F[VX], col, iz, 1, 0, 0);
         REAL dvy_dx = dplus(F[VY], i, 1, M, p->c, ix_);
         REAL dvy_dy = dminus(F[VY], i, sy, M, p->c, iy_);
-        REAL dvy_dz = dplus(F[VY], i, sz, M, p->c, iz_);
+        REAL dvy_dz = dz3(p, F[VY], col, iz, 1, 0, 0);
         REAL dvz_dx = dplus(F[VZ], i, 1, M, p->c, ix_);
         REAL dvz_dy = dplus(F[VZ], i, sy, M, p->c, iy_);
-        REAL dvz_dz = dminus(F[VZ], i, sz, M, p->c, iz_);
+        REAL dvz_dz = dz3(p, F[VZ], col, iz, 0, 1, 1);
         const REAL lam = lam_[i], mu = mu_[i];
         if (!interior(&bx_, ix, iy, iz)) {
             REAL m;
@@ -180,6 +246,12 @@ static void stress_step(const EL3* p, REAL** F, const REAL* lam_, const REAL* mu
         F[SXY][i] = F[SXY][i] + (p->dt * mu) * (dvx_dy + dvy_dx);
         F[SXZ][i] = F[SXZ][i] + (p->dt * mu) * (dvx_dz + dvz_dx);
         F[SYZ][i] = F[SYZ][i] + (p->dt * mu) * (dvy_dz + dvz_dy);
+        if (surf_row(p, iz)) {   /* Robertsson sxx / syy, then szz = 0 (kernels.cuh:360-372) */
+            const REAL rob = (-p->dt) * lam * ((lam / (lam + R(2) * mu)) * (dvx_dx + dvy_dy) + dvz_dz);
+            F[SXX][i] = F[SXX][i] + rob;
+            F[SYY][i] = F[SYY][i] + rob;
+            F[SZZ][i] = R(0);
+        }
     }
 }
 
@@ -234,7 +306,7 @@ long long oracle_el3d_tape_len(int B, int nz, int ny, int nx, int nt, int M, con
              prof + 4 * nz, prof + 4 * nz + ny, prof + 4 * nz + 2 * ny, prof + 4 * nz + 3 * ny,       \
              prof + 4 * nz + 4 * ny, prof + 4 * nz + 4 * ny + nx, prof + 4 * nz + 4 * ny + 2 * nx,    \
              prof + 4 * nz + 4 * ny + 3 * nx,                                                          \
-             vp, vs, rho, m_stride, nsrc, src, wavelet, nsf, sfields, nrec, rec, nrf, rfields}
+             vp, vs, rho, m_stride, nsrc, src, wavelet, nsf, sfields, nrec, rec, nrf, rfields, fs}
 
 /* Forward: velocity step, stress step, source injection per source field,
  * band save of the 9 fields (tape non-NULL), record per receiver field; the
@@ -244,7 +316,7 @@ int oracle_el3d_forward(
     const REAL* coef, const REAL* prof,
     const REAL* vp, const REAL* vs, const REAL* rho, i64 m_stride,
     int nsrc, const int* src, const REAL* wavelet, int nsf, const int* sfields,
-    int nrec, const int* rec, int nrf, const int* rfields,
+    int nrec, const int* rec, int nrf, const int* rfields, int fs,
     REAL* record, REAL* tape)
 {
     SETUP_EL3;
@@ -286,7 +358,7 @@ int oracle_el3d_forward(
 
 #define LOOP_REV                                                                \
     _Pragma("omp parallel for collapse(2) schedule(static)")                    \
-    for (int iz = bx_.z0 + 1; iz < bx_.z1 - 1; ++iz)                           \
+    for (int iz = p->fs ? p->M : bx_.z0 + 1; iz < bx_.z1 - 1; ++iz)             \
         for (int iy = bx_.y0 + 1; iy < bx_.y1 - 1; ++iy)                       \
             for (int ix = bx_.x0 + 1; ix < bx_.x1 - 1; ++ix)
 
@@ -294,19 +366,19 @@ static void stress_reverse(const EL3* p, REAL** F, const REAL* lam_, const REAL*
 {
     const int ny = p->ny, nx = p->nx, M = p->M;
     const i64 sy = nx, sz = (i64)nx * ny;
-    const REAL ix_ = R(1) / p->dx, iy_ = R(1) / p->dy, iz_ = R(1) / p->dz;
+    const REAL ix_ = R(1) / p->dx, iy_ = R(1) / p->dy;
     const BOX bx_ = box_of(p);
     LOOP_REV {
-        const i64 i = iz * sz + iy * sy + ix;
+        const i64 i = iz * sz + iy * sy + ix, col = i - iz * sz;
         const REAL dvx_dx = dminus(F[VX], i, 1, M, p->c, ix_);
         const REAL dvx_dy = dplus(F[VX], i, sy, M, p->c, iy_);
-        const REAL dvx_dz = dplus(F[VX], i, sz, M, p->c, iz_);
+        const REAL dvx_dz = dz3(p, F[VX], col, iz, 1, 0, 0);
         const REAL dvy_dx = dplus(F[VY], i, 1, M, p->c, ix_);
         const REAL dvy_dy = dminus(F[VY], i, sy, M, p->c, iy_);
-        const REAL dvy_dz = dplus(F[VY], i, sz, M, p->c, iz_);
+        const REAL dvy_dz = dz3(p, F[VY], col, iz, 1, 0, 0);
         const REAL dvz_dx = dplus(F[VZ], i, 1, M, p->c, ix_);
         const REAL dvz_dy = dplus(F[VZ], i, sy, M, p->c, iy_);
-        const REAL dvz_dz = dminus(F[VZ], i, sz, M, p->c, iz_);
+        const REAL dvz_dz = dz3(p, F[VZ], col, iz, 0, 1, 1);
         const REAL lam = lam_[i], mu = mu_[i];
         const REAL div = (dvx_dx + dvy_dy) + dvz_dz;
         F[SXX][i] = F[SXX][i] - p->dt * (lam * div + (R(2) * mu) * dvx_dx);
@@ -323,19 +395,19 @@ static void velocity_reverse(const EL3* p, int b, REAL** F)
     const int ny = p->ny, nx = p->nx, M = p->M;
     const i64 sy = nx, sz = (i64)nx * ny;
     const REAL* rho = p->rho + b * p->ms;
-    const REAL ix_ = R(1) / p->dx, iy_ = R(1) / p->dy, iz_ = R(1) / p->dz;
+    const REAL ix_ = R(1) / p->dx, iy_ = R(1) / p->dy;
     const BOX bx_ = box_of(p);
     LOOP_REV {
-        const i64 i = iz * sz + iy * sy + ix;
+        const i64 i = iz * sz + iy * sy + ix, col = i - iz * sz;
         const REAL dsxx_dx = dplus(F[SXX], i, 1, M, p->c, ix_);
         const REAL dsxy_dy = dminus(F[SXY], i, sy, M, p->c, iy_);
-        const REAL dsxz_dz = dminus(F[SXZ], i, sz, M, p->c, iz_);
+        const REAL dsxz_dz = dz3(p, F[SXZ], col, iz, 0, 1, 1);
         const REAL dsxy_dx = dminus(F[SXY], i, 1, M, p->c, ix_);
         const REAL dsyy_dy = dplus(F[SYY], i, sy, M, p->c, iy_);
-        const REAL dsyz_dz = dminus(F[SYZ], i, sz, M, p->c, iz_);
+        const REAL dsyz_dz = dz3(p, F[SYZ], col, iz, 0, 1, 1);
         const REAL dsxz_dx = dminus(F[SXZ], i, 1, M, p->c, ix_);
         const REAL dsyz_dy = dminus(F[SYZ], i, sy, M, p->c, iy_);
-        const REAL dszz_dz = dplus(F[SZZ], i, sz, M, p->c, iz_);
+        const REAL dszz_dz = dz3(p, F[SZZ], col, iz, 1, 1, 0);
         const REAL inv_rho = R(1) / rho[i];
         F[VX][i] = F[VX][i] - (p->dt * inv_rho) * ((dsxx_dx + dsxy_dy) + dsxz_dz);
         F[VY][i] = F[VY][i] - (p->dt * inv_rho) * ((dsxy_dx + dsyy_dy) + dsyz_dz);
@@ -353,29 +425,42 @@ static void stress_adjoint_prepare(const EL3* p, int b, REAL** A, REAL** Q, cons
     const i64 sy = nx, sz = (i64)nx * ny;
     const BOX bx_ = box_of(p);
     const REAL *vp = p->vp + b * p->ms, *vs = p->vs + b * p->ms, *rho = p->rho + b * p->ms;
-    const REAL ix_ = R(1) / p->dx, iy_ = R(1) / p->dy, iz_ = R(1) / p->dz, dt = p->dt;
+    const REAL ix_ = R(1) / p->dx, iy_ = R(1) / p->dy, dt = p->dt;
     _Pragma("omp parallel for collapse(2) schedule(static)")
     for (int iz = 0; iz < nz; ++iz)
         for (int iy = 0; iy < ny; ++iy)
             for (int ix = 0; ix < nx; ++ix) {
-                const i64 i = iz * sz + iy * sy + ix;
+                const i64 i = iz * sz + iy * sy + ix, col = i - iz * sz;
                 const REAL lam = lam_[i], mu = mu_[i], l2m = lam + R(2) * mu;
+                const int surf = surf_row(p, iz);
+                if (surf) A[SZZ][i] = R(0);
                 const REAL bsxx = A[SXX][i], bsyy = A[SYY][i], bszz = A[SZZ][i];
                 const REAL bsxy = A[SXY][i], bsxz = A[SXZ][i], bsyz = A[SYZ][i];
                 if (gvp && ix >= bx_.x0 && ix < bx_.x1 && iy >= bx_.y0 && iy < bx_.y1 && iz >= bx_.z0 &&
                     iz < bx_.z1) {
                     const REAL fvx_x = dminus(Fw[VX], i, 1, M, p->c, ix_);
                     const REAL fvx_y = dplus(Fw[VX], i, sy, M, p->c, iy_);
-                    const REAL fvx_z = dplus(Fw[VX], i, sz, M, p->c, iz_);
+                    const REAL fvx_z = dz3(p, Fw[VX], col, iz, 1, 0, 0);
                     const REAL fvy_x = dplus(Fw[VY], i, 1, M, p->c, ix_);
                     const REAL fvy_y = dminus(Fw[VY], i, sy, M, p->c, iy_);
-                    const REAL fvy_z = dplus(Fw[VY], i, sz, M, p->c, iz_);
+                    const REAL fvy_z = dz3(p, Fw[VY], col, iz, 1, 0, 0);
                     const REAL fvz_x = dplus(Fw[VZ], i, 1, M, p->c, ix_);
                     const REAL fvz_y = dplus(Fw[VZ], i, sy, M, p->c, iy_);
-                    const REAL fvz_z = dminus(Fw[VZ], i, sz, M, p->c, iz_);
-                    const REAL gl = ((bsxx + bsyy) + bszz) * ((fvx_x + fvy_y) + fvz_z);
-                    const REAL gm = R(2) * ((bsxx * fvx_x + bsyy * fvy_y) + bszz * fvz_z) + bsxz * (fvx_z + fvz_x) +
-                                    bsxy * (fvx_y + fvy_x) + bsyz * (fvy_z + fvz_y);
+                    const REAL fvz_z = dz3(p, Fw[VZ], col, iz, 0, 1, 1);
+                    REAL gl, gm;
+                    if (surf) {   /* the surface row's corrected sxx / syy updates (kernels.cuh:1440-1452) */
+                        const REAL vp2 = vp[i] * vp[i], vs2 = vs[i] * vs[i], vp4 = vp2 * vp2;
+                        const REAL dcl = R(4) * vs2 * vs2 / vp4;
+                        const REAL dcm = R(4) * (vp4 - R(2) * vp2 * vs2 + R(2) * vs2 * vs2) / vp4;
+                        const REAL dc2m = R(2) * (vp2 - R(2) * vs2) * (vp2 - R(2) * vs2) / vp4;
+                        gl = dcl * (bsxx + bsyy) * (fvx_x + fvy_y);
+                        gm = bsxx * (dcm * fvx_x + dc2m * fvy_y) + bsyy * (dc2m * fvx_x + dcm * fvy_y) +
+                             bsxz * (fvx_z + fvz_x) + bsxy * (fvx_y + fvy_x) + bsyz * (fvy_z + fvz_y);
+                    } else {
+                        gl = ((bsxx + bsyy) + bszz) * ((fvx_x + fvy_y) + fvz_z);
+                        gm = R(2) * ((bsxx * fvx_x + bsyy * fvy_y) + bszz * fvz_z) + bsxz * (fvx_z + fvz_x) +
+                             bsxy * (fvx_y + fvy_x) + bsyz * (fvy_z + fvz_y);
+                    }
                     gvp[i] = gvp[i] + ((R(-2) * rho[i]) * vp[i]) * gl * dt;
                     gvs[i] = gvs[i] + (-((((R(-4) * rho[i]) * vs[i]) * gl) + (((R(2) * rho[i]) * vs[i]) * gm))) * dt;
                     grho[i] = grho[i] + ((A[VX][i] * (Fw[VX][i] - vn[0][i]) + A[VY][i] * (Fw[VY][i] - vn[1][i])) +
@@ -383,9 +468,17 @@ static void stress_adjoint_prepare(const EL3* p, int b, REAL** A, REAL** Q, cons
                     grho[i] = grho[i] - ((gl * ((vp[i] * vp[i]) - ((R(2) * vs[i]) * vs[i]))) * dt +
                                          (gm * (vs[i] * vs[i])) * dt);
                 }
-                const REAL bvx_x = dt * ((l2m * bsxx + lam * bsyy) + lam * bszz);
-                const REAL bvy_y = dt * ((lam * bsxx + l2m * bsyy) + lam * bszz);
-                const REAL bvz_z = dt * ((lam * bsxx + lam * bsyy) + l2m * bszz);
+                REAL bvx_x, bvy_y, bvz_z;
+                if (surf) {   /* transposes of the corrected surface updates */
+                    const REAL coef = R(4) * mu * (lam + mu) / l2m, coef2 = R(2) * lam * mu / l2m;
+                    bvx_x = dt * (coef * bsxx + coef2 * bsyy);
+                    bvy_y = dt * (coef2 * bsxx + coef * bsyy);
+                    bvz_z = R(0);
+                } else {
+                    bvx_x = dt * ((l2m * bsxx + lam * bsyy) + lam * bszz);
+                    bvy_y = dt * ((lam * bsxx + l2m * bsyy) + lam * bszz);
+                    bvz_z = dt * ((lam * bsxx + lam * bsyy) + l2m * bszz);
+                }
                 const REAL bvx_y = (dt * mu) * bsxy, bvx_z = (dt * mu) * bsxz;
                 const REAL bvy_x = (dt * mu) * bsxy, bvy_z = (dt * mu) * bsyz;
                 const REAL bvz_x = (dt * mu) * bsxz, bvz_y = (dt * mu) * bsyz;
@@ -419,15 +512,15 @@ static void stress_adjoint_apply(const EL3* p, REAL** A, REAL** Q)
 {
     const int nz = p->nz, ny = p->ny, nx = p->nx, M = p->M;
     const i64 sy = nx, sz = (i64)nx * ny;
-    const REAL ix_ = R(1) / p->dx, iy_ = R(1) / p->dy, iz_ = R(1) / p->dz;
+    const REAL ix_ = R(1) / p->dx, iy_ = R(1) / p->dy;
     LOOP_CORE {
-        const i64 i = iz * sz + iy * sy + ix;
+        const i64 i = iz * sz + iy * sy + ix, col = i - iz * sz;
         const REAL qxx = dplus(Q[0], i, 1, M, p->c, ix_), qxy = dminus(Q[1], i, sy, M, p->c, iy_);
-        const REAL qxz = dminus(Q[2], i, sz, M, p->c, iz_);
+        const REAL qxz = adz3(p, Q[2], col, iz, 1, 0, 0);
         const REAL qyx = dminus(Q[3], i, 1, M, p->c, ix_), qyy = dplus(Q[4], i, sy, M, p->c, iy_);
-        const REAL qyz = dminus(Q[5], i, sz, M, p->c, iz_);
+        const REAL qyz = adz3(p, Q[5], col, iz, 1, 0, 0);
         const REAL qzx = dminus(Q[6], i, 1, M, p->c, ix_), qzy = dminus(Q[7], i, sy, M, p->c, iy_);
-        const REAL qzz = dplus(Q[8], i, sz, M, p->c, iz_);
+        const REAL qzz = adz3(p, Q[8], col, iz, 0, 1, 1);
         A[VX][i] = A[VX][i] + ((qxx + qxy) + qxz);
         A[VY][i] = A[VY][i] + ((qyx + qyy) + qyz);
         A[VZ][i] = A[VZ][i] + ((qzx + qzy) + qzz);
@@ -442,7 +535,7 @@ static void velocity_adjoint(const EL3* p, int b, REAL** A, REAL** P)
     const i64 sy = nx, sz = (i64)nx * ny;
     const BOX bx_ = box_of(p);
     const REAL* rho = p->rho + b * p->ms;
-    const REAL ix_ = R(1) / p->dx, iy_ = R(1) / p->dy, iz_ = R(1) / p->dz, dt = p->dt;
+    const REAL ix_ = R(1) / p->dx, iy_ = R(1) / p->dy, dt = p->dt;
     _Pragma("omp parallel for collapse(2) schedule(static)")
     for (int iz = 0; iz < nz; ++iz)
         for (int iy = 0; iy < ny; ++iy)
@@ -473,13 +566,13 @@ static void velocity_adjoint(const EL3* p, int b, REAL** A, REAL** P)
                 A[M_SXZZ][i] = p->az[iz] * t_sxzz; A[M_SYZZ][i] = p->az[iz] * t_syzz; A[M_SZZZ][i] = p->azh[iz] * t_szzz;
             }
     LOOP_CORE {
-        const i64 i = iz * sz + iy * sy + ix;
+        const i64 i = iz * sz + iy * sy + ix, col = i - iz * sz;
         const REAL pxx = dminus(P[0], i, 1, M, p->c, ix_), pxy = dplus(P[1], i, sy, M, p->c, iy_);
-        const REAL pxz = dplus(P[2], i, sz, M, p->c, iz_);
+        const REAL pxz = adz3(p, P[2], col, iz, 0, 1, 1);
         const REAL pyx = dplus(P[3], i, 1, M, p->c, ix_), pyy = dminus(P[4], i, sy, M, p->c, iy_);
-        const REAL pyz = dplus(P[5], i, sz, M, p->c, iz_);
+        const REAL pyz = adz3(p, P[5], col, iz, 0, 1, 1);
         const REAL pzx = dplus(P[6], i, 1, M, p->c, ix_), pzy = dplus(P[7], i, sy, M, p->c, iy_);
-        const REAL pzz = dminus(P[8], i, sz, M, p->c, iz_);
+        const REAL pzz = adz3(p, P[8], col, iz, 1, 1, 0);
         A[SXX][i] = A[SXX][i] + pxx;
         A[SXY][i] = A[SXY][i] + (pxy + pyx);
         A[SXZ][i] = A[SXZ][i] + (pxz + pzx);
@@ -497,7 +590,7 @@ int oracle_el3d_backward(
     const REAL* coef, const REAL* prof,
     const REAL* vp, const REAL* vs, const REAL* rho, i64 m_stride,
     int nsrc, const int* src, const REAL* wavelet, int nsf, const int* sfields,
-    int nrec, const int* rec, int nrf, const int* rfields,
+    int nrec, const int* rec, int nrf, const int* rfields, int fs,
     const REAL* adj, const REAL* tape, REAL* grad_vp, REAL* grad_vs, REAL* grad_rho)
 {
     SETUP_EL3;

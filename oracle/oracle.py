@@ -104,7 +104,7 @@ def _lib(prec: str):
         lib.oracle_el2d_backward.restype = i
         lib.oracle_el2d_backward.argtypes = geo_el + [P, P, P, P, P]
         geo_el3 = [i, i, i, i, i, i, P, real, real, real, real, P, P, P, P, P, l,
-                   i, P, P, i, P, i, P, i, P]
+                   i, P, P, i, P, i, P, i, P, i]
         lib.oracle_el3d_tape_len.restype = l
         lib.oracle_el3d_tape_len.argtypes = [i, i, i, i, i, i, P]
         lib.oracle_el3d_forward.restype = i
@@ -521,11 +521,12 @@ class Elastic3D:
     ``vp, vs, rho`` of shape ``(nz, ny, nx)`` or per shot ``(B, nz, ny, nx)``;
     coordinates ``(x, y, z)``; source fields default to the explosive
     ``(sxx, syy, szz)``, receiver fields to ``(vx, vy, vz)``
-    (``src/sweep/equations/elastic3d.py:326-332``)."""
+    (``src/sweep/equations/elastic3d.py:326-332``).  ``free_surface=True``:
+    a traction-free top face with no PML pad."""
 
     def __init__(self, vp, vs, rho, wavelet, src, rec, dh, dt, abcn, order=8, prec="f32",
                  source_fields=("sxx", "syy", "szz"), receiver_fields=("vx", "vy", "vz"),
-                 max_vel=4500.0, pml_freq=25.0):
+                 max_vel=4500.0, pml_freq=25.0, free_surface=False):
         self.prec = prec
         self.real = np.float32 if prec == "f32" else np.float64
         models = [np.asarray(m, np.float32) for m in (vp, vs, rho)]
@@ -534,9 +535,10 @@ class Elastic3D:
         w, s, r = _batch_io(wavelet, src, rec, 3)
         self.B, self.nt = w.shape[0], w.shape[-1]
         self.phys = models[0].shape[-3:]
-        self.pad = abcn
-        self.shape = tuple(n + 2 * abcn + 2 * M for n in self.phys)
-        padw = [(abcn + M, abcn + M)] * 3
+        self.fs = 1 if free_surface else 0
+        self.pads = [0 if free_surface else abcn] + [abcn] * 5   # z_lo, z_hi, y_lo, y_hi, x_lo, x_hi
+        self.shape = tuple(n + self.pads[2 * a] + self.pads[2 * a + 1] + 2 * M for a, n in enumerate(self.phys))
+        padw = [(self.pads[2 * a] + M, self.pads[2 * a + 1] + M) for a in range(3)]
         lead = [(0, 0)] if self.per_shot else []
         self.models = [np.ascontiguousarray(np.pad(m, lead + padw, mode="edge").astype(self.real))
                        for m in models]
@@ -544,13 +546,13 @@ class Elastic3D:
         sp = dh if np.ndim(dh) else [dh] * 3
         self.spacing = [float(x) for x in sp]
         self.dt = float(dt)
-        prof = cpml_profiles_s([abcn] * 6, M, dt, self.spacing, self.shape, max_vel, pml_freq)
+        prof = cpml_profiles_s(self.pads, M, dt, self.spacing, self.shape, max_vel, pml_freq)
         self.prof = np.ascontiguousarray(np.concatenate([np.concatenate(p) for p in prof]).astype(self.real))
         c = staggered_coefficients(M)
         self.coef = np.array([0.0] + [float(x) for x in c], np.float64).astype(self.real)
         if self.real is np.float32:
             self.coef = np.array([0.0] + [np.float32(float(x)) for x in c], np.float32)
-        off = abcn + M
+        off = np.array([self.pads[4] + M, self.pads[2] + M, self.pads[0] + M])   # (x, y, z)
         self.src = np.ascontiguousarray((s + off).astype(np.int32))
         self.rec = np.ascontiguousarray((r + off).astype(np.int32))
         self.wavelet = np.ascontiguousarray(w.astype(self.real))
@@ -560,16 +562,16 @@ class Elastic3D:
 
     def _geo(self):
         nz, ny, nx = self.shape
-        self._pad = np.array([self.pad] * 6, np.int32)
+        self._pad = np.array(self.pads, np.int32)
         return [self.B, nz, ny, nx, self.nt, self.M, _ptr(self._pad), self.dt, self.spacing[0],
                 self.spacing[1], self.spacing[2], _ptr(self.coef), _ptr(self.prof), _ptr(self.models[0]),
                 _ptr(self.models[1]), _ptr(self.models[2]), self.m_stride,
                 1, _ptr(self.src), _ptr(self.wavelet), len(self.sf), _ptr(self.sf),
-                self.nrec, _ptr(self.rec), len(self.rf), _ptr(self.rf)]
+                self.nrec, _ptr(self.rec), len(self.rf), _ptr(self.rf), self.fs]
 
     def crop(self, g):
-        M, a = self.M, self.pad
-        sl = tuple(slice(a + M, a + M + n) for n in self.phys)
+        M = self.M
+        sl = tuple(slice(self.pads[2 * a] + M, self.pads[2 * a] + M + n) for a, n in enumerate(self.phys))
         return g[(Ellipsis,) + sl]
 
     def forward(self, keep_tape=True):
@@ -579,7 +581,7 @@ class Elastic3D:
         rec = np.zeros((self.B, self.nt, self.nrec, len(self.rf)), self.real)
         self.tape = None
         if keep_tape:
-            pad = np.array([self.pad] * 6, np.int32)
+            pad = np.array(self.pads, np.int32)
             n = lib.oracle_el3d_tape_len(self.B, nz, ny, nx, self.nt, self.M, _ptr(pad))
             self.tape = np.zeros(n, self.real)
         rc = lib.oracle_el3d_forward(*self._geo(), _ptr(rec), _ptr(self.tape) if keep_tape else None)

@@ -112,6 +112,7 @@ class Elastic3DDesc(ctypes.Structure):
         ("nsrc_fields", c_i32), ("src_fields", c_i32 * 9),
         ("nrec", c_i32), ("rec_loc", c_p),
         ("nrec_fields", c_i32), ("rec_fields", c_i32 * 9),
+        ("free_surface", c_i32),
     ]
 
 

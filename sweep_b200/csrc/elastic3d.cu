@@ -9,25 +9,29 @@
 //               outside the physical box shrunk by one cell  kernels.cuh:104-248
 //     str3      stress update with the nine velocity-derivative memories
 //                                                             kernels.cuh:290-483
-//     src3 / save3 / rec3   source injection per source field, the nine
+//     src3 / strips3 / rec3   source injection per source field, the nine
 //               fields' boundary strips, the receiver gather  driver_traits.cuh:265-300
 //   reverse, per step (driver_traits.cuh:680-905):
 //     vsrc3     body-force rho correction (before the residuals)
 //     res3      signed residual injection (stress -1, velocity +1); src3 with
 //               -w takes the forward source back out
 //     srev3     stress reconstruction on the box minus one cell   kernels.cuh:653-768
-//     restore3  stress strips of step it - 1
+//     strips3   stress strips of step it - 1 restored
 //     sprep3    stress-adjoint prepare (q and the adjoint memories of the
 //               velocity derivatives) with the fused vp / vs / rho imaging
 //                                                             kernels.cuh:1367-1615
 //     rrho3     receiver rho correction                       common/common.cu:77-116
 //     sapp3     stress-adjoint apply (adjoint velocities)     kernels.cuh:1683-1780
 //     vprep3 / vapp3   velocity-adjoint prepare / apply       kernels.cuh:959-1236
-//     cap3, vrev3, restore3   v(it) carriers, velocity reconstruction,
+//     cap3, vrev3, strips3   v(it) carriers, velocity reconstruction,
 //               velocity strips of step it - 1                kernels.cuh:536-652
 //
 // One thread per cell on (32 x 8) tiles of x / y, one z plane and shot per
-// grid row; the stencils read global memory through the read-only path.
+// grid row; the stencils read global memory through the read-only path.  (A
+// z-marching variant with shared-memory planes and register z-queues, run at
+// two CTAs per SM without a load pipeline, measured 2.8x slower in the
+// forward; the kernels that beat this layout need the 3-D acoustic kernels'
+// TMA plane rings.)
 // Layout: fields (B, nz, ny, nx), x fastest; CPML memories in per-axis slabs
 // covering the cells outside the box shrunk by one cell along their axis
 // (x: (B, nz, ny, WX), y: (B, nz, WY, nx), z: (B, WZ, ny, nx)).  Cells in the
@@ -86,6 +90,7 @@ struct Geo {
     long long ms;                   // model stride between shots (0 or S)
     const int* cells;               // strip cell offsets in a shot grid
     int ns;                         // strip cells
+    int fst;                        // traction-free top face: the surface is row z0 (no pad above)
 };
 
 struct Models {
@@ -104,6 +109,60 @@ __device__ __forceinline__ float dm(const float* __restrict__ u, long long i, lo
     return (W1 * (__ldg(u + i) - __ldg(u + i - s)) + W2 * (__ldg(u + i + s) - __ldg(u + i - 2 * s)) +
             W3 * (__ldg(u + i + 2 * s) - __ldg(u + i - 3 * s)) + W4 * (__ldg(u + i + 3 * s) - __ldg(u + i - 4 * s))) *
            inv;
+}
+
+// ------------------------------------------------ traction-free top face
+// The reference's 3-D image method (common/elastic_free_surface.cuh:723-952,
+// elastic3d/kernels.cuh:360-372, 1421-1499): the rows above the surface row z0
+// are air, read by a z-derivative as the image of the row mirrored about the
+// surface (about z0 for integer fields, z0 - 1/2 for fields half a cell
+// below it, negated for odd fields); the full stencil runs over the images.
+// Only the M rows from the surface down reach the air; the adjoint is the
+// exact transpose, so it differs from the plain one on the M + 1 rows from
+// the surface down.  The surface row's sxx and syy take the Robertsson
+// correction and its szz is zeroed.
+template <bool FS, bool FWD>
+__device__ __forceinline__ float dz_fs(const Geo& G, const float* __restrict__ u, long long i, int iz, bool odd,
+                                       bool half)
+{
+    const long long sz = (long long)G.nx * G.ny;
+    if (!FS || iz >= G.z0 + M) return FWD ? dp(u, i, sz, G.idz) : dm(u, i, sz, G.idz);
+    auto at = [&](int k) {
+        if (k >= G.z0) return __ldg(u + i + (long long)(k - iz) * sz);
+        const int m = half ? 2 * G.z0 - 1 - k : 2 * G.z0 - k;
+        const float v = __ldg(u + i + (long long)(m - iz) * sz);
+        return odd ? -v : v;
+    };
+    const float w[M] = {W1, W2, W3, W4};
+    float g = 0.f;
+#pragma unroll
+    for (int m = 0; m < M; ++m)
+        g += w[m] * (FWD ? at(iz + m + 1) - at(iz - m) : at(iz + m) - at(iz - m - 1));
+    return g * G.idz;
+}
+// negated transpose of dz_fs (the plain one: D- for a D+ forward)
+template <bool FS, bool FWD>
+__device__ __forceinline__ float adz_fs(const Geo& G, const float* __restrict__ q, long long i, int iz, bool odd,
+                                        bool half)
+{
+    const long long sz = (long long)G.nx * G.ny;
+    if (!FS || iz > G.z0 + M) return FWD ? dm(q, i, sz, G.idz) : dp(q, i, sz, G.idz);
+    const int top = G.z0, lo = half ? top - 1 : top;
+    const float par = odd ? -1.f : 1.f;
+    auto at = [&](int k) { return __ldg(q + i + (long long)(k - iz) * sz); };
+    const float w[M] = {W1, W2, W3, W4};
+    float g = 0.f;
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        const int jp = FWD ? iz + m : iz + m + 1;
+        const int jm = FWD ? iz - m - 1 : iz - m;
+        const int jg = FWD ? (half ? 2 * top - 1 + m - iz : 2 * top + m - iz)
+                           : (half ? 2 * top + m - iz : 2 * top + m + 1 - iz);
+        if (jp >= top) g += w[m] * at(jp);
+        if (jm >= top) g -= w[m] * at(jm);
+        if (iz > lo && jg >= top) g += w[m] * par * at(jg);
+    }
+    return g * G.idz;
 }
 
 __device__ __forceinline__ bool interior(const Geo& G, int ix, int iy, int iz)
@@ -163,23 +222,24 @@ struct Fwd {
     Slabs mem;
 };
 
+template <bool FS>
 __global__ void __launch_bounds__(NTHX * NTHY) vel3(Fwd A)
 {
     const Geo& G = A.G;
     int b, iz, iy, ix;
     if (!cell_of(G, b, iz, iy, ix) || !in_core(G, ix, iy, iz)) return;
-    const long long sy = G.nx, sz = (long long)G.nx * G.ny;
+    const long long sy = G.nx;
     const long long c = (iz * (long long)G.ny + iy) * G.nx + ix, i = b * G.S + c;
     float* const* f = A.f;
     float dsxx_dx = dp(f[SXX], i, 1, G.idx);
     float dsxy_dy = dm(f[SXY], i, sy, G.idy);
-    float dsxz_dz = dm(f[SXZ], i, sz, G.idz);
+    float dsxz_dz = dz_fs<FS, false>(G, f[SXZ], i, iz, true, true);
     float dsxy_dx = dm(f[SXY], i, 1, G.idx);
     float dsyy_dy = dp(f[SYY], i, sy, G.idy);
-    float dsyz_dz = dm(f[SYZ], i, sz, G.idz);
+    float dsyz_dz = dz_fs<FS, false>(G, f[SYZ], i, iz, true, true);
     float dsxz_dx = dm(f[SXZ], i, 1, G.idx);
     float dsyz_dy = dm(f[SYZ], i, sy, G.idy);
-    float dszz_dz = dp(f[SZZ], i, sz, G.idz);
+    float dszz_dz = dz_fs<FS, true>(G, f[SZZ], i, iz, true, false);
     if (!interior(G, ix, iy, iz)) {
         const long long xo = xsl(G, b, iz, iy, ix), yo = ysl(G, b, iz, iy, ix), zo = zsl(G, b, iz, iy, ix);
         mem(A.mem.z[MZ_SZZ], zo, G.azh[iz], G.bzh[iz], dszz_dz);
@@ -198,23 +258,24 @@ __global__ void __launch_bounds__(NTHX * NTHY) vel3(Fwd A)
     f[VZ][i] += k * (dsxz_dx + dsyz_dy + dszz_dz);
 }
 
+template <bool FS>
 __global__ void __launch_bounds__(NTHX * NTHY) str3(Fwd A)
 {
     const Geo& G = A.G;
     int b, iz, iy, ix;
     if (!cell_of(G, b, iz, iy, ix) || !in_core(G, ix, iy, iz)) return;
-    const long long sy = G.nx, sz = (long long)G.nx * G.ny;
+    const long long sy = G.nx;
     const long long c = (iz * (long long)G.ny + iy) * G.nx + ix, i = b * G.S + c;
     float* const* f = A.f;
     float dvx_dx = dm(f[VX], i, 1, G.idx);
     float dvx_dy = dp(f[VX], i, sy, G.idy);
-    float dvx_dz = dp(f[VX], i, sz, G.idz);
+    float dvx_dz = dz_fs<FS, true>(G, f[VX], i, iz, false, false);
     float dvy_dx = dp(f[VY], i, 1, G.idx);
     float dvy_dy = dm(f[VY], i, sy, G.idy);
-    float dvy_dz = dp(f[VY], i, sz, G.idz);
+    float dvy_dz = dz_fs<FS, true>(G, f[VY], i, iz, false, false);
     float dvz_dx = dp(f[VZ], i, 1, G.idx);
     float dvz_dy = dp(f[VZ], i, sy, G.idy);
-    float dvz_dz = dm(f[VZ], i, sz, G.idz);
+    float dvz_dz = dz_fs<FS, false>(G, f[VZ], i, iz, true, true);
     if (!interior(G, ix, iy, iz)) {
         const long long xo = xsl(G, b, iz, iy, ix), yo = ysl(G, b, iz, iy, ix), zo = zsl(G, b, iz, iy, ix);
         mem(A.mem.z[MZ_VZ], zo, G.az[iz], G.bz[iz], dvz_dz);
@@ -236,6 +297,12 @@ __global__ void __launch_bounds__(NTHX * NTHY) str3(Fwd A)
     f[SXY][i] += G.dt * mu * (dvx_dy + dvy_dx);
     f[SXZ][i] += G.dt * mu * (dvx_dz + dvz_dx);
     f[SYZ][i] += G.dt * mu * (dvy_dz + dvz_dy);
+    if (FS && iz == G.z0) {   // surface row: Robertsson sxx / syy, then szz = 0
+        const float rob = -G.dt * lam * (lam / (lam + 2.f * mu) * (dvx_dx + dvy_dy) + dvz_dz);
+        f[SXX][i] += rob;
+        f[SYY][i] += rob;
+        f[SZZ][i] = 0.f;
+    }
 }
 
 // Source injection of step it with sign (+1 forward, -1 taking the forward
@@ -253,11 +320,12 @@ __global__ void src3(const Geo G, const Fields F, int it, float sign)
     }
 }
 
+// receivers: one thread per (shot, receiver), grid (receiver blocks, shots)
 __global__ void rec3(const Geo G, const Fields F, float* record, int it)
 {
     float* const* f = F.f;
-    const int b = blockIdx.x;
-    for (int r = threadIdx.x; r < G.nrec; r += blockDim.x) {
+    const int b = blockIdx.y;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < G.nrec; r += gridDim.x * blockDim.x) {
         const int* l = G.rec_loc + ((long long)b * G.nrec + r) * 3;
         if (l[0] < 0 || l[0] >= G.nx || l[1] < 0 || l[1] >= G.ny || l[2] < 0 || l[2] >= G.nz) continue;
         const long long i = b * G.S + ((long long)l[2] * G.ny + l[1]) * G.nx + l[0];
@@ -317,8 +385,8 @@ __global__ void vsrc3(Rev A)
 __global__ void res3(Rev A)
 {
     const Geo& G = A.G;
-    const int b = blockIdx.x;
-    for (int r = threadIdx.x; r < G.nrec; r += blockDim.x) {
+    const int b = blockIdx.y;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < G.nrec; r += gridDim.x * blockDim.x) {
         const int* l = G.rec_loc + ((long long)b * G.nrec + r) * 3;
         if (l[0] < 0 || l[0] >= G.nx || l[1] < 0 || l[1] >= G.ny || l[2] < 0 || l[2] >= G.nz) continue;
         const long long i = b * G.S + ((long long)l[2] * G.ny + l[1]) * G.nx + l[0];
@@ -334,8 +402,8 @@ __global__ void res3(Rev A)
 __global__ void rrho3(Rev A)
 {
     const Geo& G = A.G;
-    const int b = blockIdx.x;
-    for (int r = threadIdx.x; r < G.nrec; r += blockDim.x) {
+    const int b = blockIdx.y;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < G.nrec; r += gridDim.x * blockDim.x) {
         const int* l = G.rec_loc + ((long long)b * G.nrec + r) * 3;
         if (!in_core(G, l[0], l[1], l[2])) continue;
         const long long c = ((long long)l[2] * G.ny + l[1]) * G.nx + l[0];
@@ -349,17 +417,21 @@ __global__ void rrho3(Rev A)
     }
 }
 
+template <bool FS>
 __global__ void __launch_bounds__(NTHX * NTHY) srev3(Rev A)
 {
     const Geo& G = A.G;
     int b, iz, iy, ix;
     if (!cell_of(G, b, iz, iy, ix) || !interior(G, ix, iy, iz)) return;
-    const long long sy = G.nx, sz = (long long)G.nx * G.ny;
+    const long long sy = G.nx;
     const long long c = (iz * (long long)G.ny + iy) * G.nx + ix, i = b * G.S + c;
     float* const* f = A.f;
-    const float dvx_dx = dm(f[VX], i, 1, G.idx), dvx_dy = dp(f[VX], i, sy, G.idy), dvx_dz = dp(f[VX], i, sz, G.idz);
-    const float dvy_dx = dp(f[VY], i, 1, G.idx), dvy_dy = dm(f[VY], i, sy, G.idy), dvy_dz = dp(f[VY], i, sz, G.idz);
-    const float dvz_dx = dp(f[VZ], i, 1, G.idx), dvz_dy = dp(f[VZ], i, sy, G.idy), dvz_dz = dm(f[VZ], i, sz, G.idz);
+    const float dvx_dx = dm(f[VX], i, 1, G.idx), dvx_dy = dp(f[VX], i, sy, G.idy);
+    const float dvx_dz = dz_fs<FS, true>(G, f[VX], i, iz, false, false);
+    const float dvy_dx = dp(f[VY], i, 1, G.idx), dvy_dy = dm(f[VY], i, sy, G.idy);
+    const float dvy_dz = dz_fs<FS, true>(G, f[VY], i, iz, false, false);
+    const float dvz_dx = dp(f[VZ], i, 1, G.idx), dvz_dy = dp(f[VZ], i, sy, G.idy);
+    const float dvz_dz = dz_fs<FS, false>(G, f[VZ], i, iz, true, true);
     const long long mi = b * G.ms + c;
     const float lam = A.m.lam[mi], mu = A.m.mu[mi];
     const float div = dvx_dx + dvy_dy + dvz_dz;
@@ -371,19 +443,20 @@ __global__ void __launch_bounds__(NTHX * NTHY) srev3(Rev A)
     f[SYZ][i] -= G.dt * mu * (dvy_dz + dvz_dy);
 }
 
+template <bool FS>
 __global__ void __launch_bounds__(NTHX * NTHY) vrev3(Rev A)
 {
     const Geo& G = A.G;
     int b, iz, iy, ix;
     if (!cell_of(G, b, iz, iy, ix) || !interior(G, ix, iy, iz)) return;
-    const long long sy = G.nx, sz = (long long)G.nx * G.ny;
+    const long long sy = G.nx;
     const long long c = (iz * (long long)G.ny + iy) * G.nx + ix, i = b * G.S + c;
     float* const* f = A.f;
     const float dsxx_dx = dp(f[SXX], i, 1, G.idx), dsxy_dy = dm(f[SXY], i, sy, G.idy);
-    const float dsxz_dz = dm(f[SXZ], i, sz, G.idz), dsxy_dx = dm(f[SXY], i, 1, G.idx);
-    const float dsyy_dy = dp(f[SYY], i, sy, G.idy), dsyz_dz = dm(f[SYZ], i, sz, G.idz);
+    const float dsxz_dz = dz_fs<FS, false>(G, f[SXZ], i, iz, true, true), dsxy_dx = dm(f[SXY], i, 1, G.idx);
+    const float dsyy_dy = dp(f[SYY], i, sy, G.idy), dsyz_dz = dz_fs<FS, false>(G, f[SYZ], i, iz, true, true);
     const float dsxz_dx = dm(f[SXZ], i, 1, G.idx), dsyz_dy = dm(f[SYZ], i, sy, G.idy);
-    const float dszz_dz = dp(f[SZZ], i, sz, G.idz);
+    const float dszz_dz = dz_fs<FS, true>(G, f[SZZ], i, iz, true, false);
     const float k = A.m.kv[b * G.ms + c];
     f[VX][i] -= k * (dsxx_dx + dsxy_dy + dsxz_dz);
     f[VY][i] -= k * (dsxy_dx + dsyy_dy + dsyz_dz);
@@ -399,25 +472,43 @@ __device__ __forceinline__ float amem(float* __restrict__ m, long long at, float
     return bar + b * t;
 }
 
+template <bool FS>
 __global__ void __launch_bounds__(NTHX * NTHY) sprep3(Rev A)
 {
     const Geo& G = A.G;
     int b, iz, iy, ix;
     if (!cell_of(G, b, iz, iy, ix)) return;
-    const long long sy = G.nx, sz = (long long)G.nx * G.ny;
+    const long long sy = G.nx;
     const long long c = (iz * (long long)G.ny + iy) * G.nx + ix, i = b * G.S + c, mi = b * G.ms + c;
     const float lam = A.m.lam[mi], mu = A.m.mu[mi], l2m = lam + 2.f * mu;
-    const float bsxx = A.a[SXX][i], bsyy = A.a[SYY][i], bszz = A.a[SZZ][i];
+    const bool surf = FS && iz == G.z0;
+    if (surf) A.a[SZZ][i] = 0.f;   // the surface row's adjoint szz (its forward value is zeroed)
+    const float bsxx = A.a[SXX][i], bsyy = A.a[SYY][i], bszz = surf ? 0.f : A.a[SZZ][i];
     const float bsxy = A.a[SXY][i], bsxz = A.a[SXZ][i], bsyz = A.a[SYZ][i];
     if (in_box(G, ix, iy, iz)) {
         float* const* f = A.f;
-        const float fvx_x = dm(f[VX], i, 1, G.idx), fvx_y = dp(f[VX], i, sy, G.idy), fvx_z = dp(f[VX], i, sz, G.idz);
-        const float fvy_x = dp(f[VY], i, 1, G.idx), fvy_y = dm(f[VY], i, sy, G.idy), fvy_z = dp(f[VY], i, sz, G.idz);
-        const float fvz_x = dp(f[VZ], i, 1, G.idx), fvz_y = dp(f[VZ], i, sy, G.idy), fvz_z = dm(f[VZ], i, sz, G.idz);
-        const float gl = (bsxx + bsyy + bszz) * (fvx_x + fvy_y + fvz_z);
-        const float gm = 2.f * (bsxx * fvx_x + bsyy * fvy_y + bszz * fvz_z) + bsxz * (fvx_z + fvz_x) +
-                         bsxy * (fvx_y + fvy_x) + bsyz * (fvy_z + fvz_y);
+        const float fvx_x = dm(f[VX], i, 1, G.idx), fvx_y = dp(f[VX], i, sy, G.idy);
+        const float fvx_z = dz_fs<FS, true>(G, f[VX], i, iz, false, false);
+        const float fvy_x = dp(f[VY], i, 1, G.idx), fvy_y = dm(f[VY], i, sy, G.idy);
+        const float fvy_z = dz_fs<FS, true>(G, f[VY], i, iz, false, false);
+        const float fvz_x = dp(f[VZ], i, 1, G.idx), fvz_y = dp(f[VZ], i, sy, G.idy);
+        const float fvz_z = dz_fs<FS, false>(G, f[VZ], i, iz, true, true);
         const float rho = A.m.rho[mi], vp = A.m.vp[mi], vs = A.m.vs[mi];
+        float gl, gm;
+        if (surf) {
+            // the surface row's corrected sxx / syy updates (kernels.cuh:1440-1452)
+            const float vp2 = vp * vp, vs2 = vs * vs, vp4 = vp2 * vp2;
+            const float dcl = 4.f * vs2 * vs2 / vp4;
+            const float dcm = 4.f * (vp4 - 2.f * vp2 * vs2 + 2.f * vs2 * vs2) / vp4;
+            const float dc2m = 2.f * (vp2 - 2.f * vs2) * (vp2 - 2.f * vs2) / vp4;
+            gl = dcl * (bsxx + bsyy) * (fvx_x + fvy_y);
+            gm = bsxx * (dcm * fvx_x + dc2m * fvy_y) + bsyy * (dc2m * fvx_x + dcm * fvy_y) + bsxz * (fvx_z + fvz_x) +
+                 bsxy * (fvx_y + fvy_x) + bsyz * (fvy_z + fvz_y);
+        } else {
+            gl = (bsxx + bsyy + bszz) * (fvx_x + fvy_y + fvz_z);
+            gm = 2.f * (bsxx * fvx_x + bsyy * fvy_y + bszz * fvz_z) + bsxz * (fvx_z + fvz_x) +
+                 bsxy * (fvx_y + fvy_x) + bsyz * (fvy_z + fvz_y);
+        }
         A.gvp[i] += -2.f * rho * vp * gl * G.dt;
         A.gvs[i] += -(-4.f * rho * vs * gl + 2.f * rho * vs * gm) * G.dt;
         float gr = (A.a[VX][i] * (f[VX][i] - A.cv[0][i]) + A.a[VY][i] * (f[VY][i] - A.cv[1][i]) +
@@ -425,9 +516,17 @@ __global__ void __launch_bounds__(NTHX * NTHY) sprep3(Rev A)
         gr -= gl * (vp * vp - 2.f * vs * vs) * G.dt + gm * (vs * vs) * G.dt;
         A.grho[i] += gr;
     }
-    float qxx = G.dt * (l2m * bsxx + lam * bsyy + lam * bszz);
-    float qyy = G.dt * (lam * bsxx + l2m * bsyy + lam * bszz);
-    float qzz = G.dt * (lam * bsxx + lam * bsyy + l2m * bszz);
+    float qxx, qyy, qzz;
+    if (surf) {   // transposes of the corrected surface updates
+        const float coef = 4.f * mu * (lam + mu) / l2m, coef2 = 2.f * lam * mu / l2m;
+        qxx = G.dt * (coef * bsxx + coef2 * bsyy);
+        qyy = G.dt * (coef2 * bsxx + coef * bsyy);
+        qzz = 0.f;
+    } else {
+        qxx = G.dt * (l2m * bsxx + lam * bsyy + lam * bszz);
+        qyy = G.dt * (lam * bsxx + l2m * bsyy + lam * bszz);
+        qzz = G.dt * (lam * bsxx + lam * bsyy + l2m * bszz);
+    }
     float qxy = G.dt * mu * bsxy, qxz = G.dt * mu * bsxz;
     float qyx = G.dt * mu * bsxy, qyz = G.dt * mu * bsyz;
     float qzx = G.dt * mu * bsxz, qzy = G.dt * mu * bsyz;
@@ -448,17 +547,18 @@ __global__ void __launch_bounds__(NTHX * NTHY) sprep3(Rev A)
     A.q[6][i] = qzx; A.q[7][i] = qzy; A.q[8][i] = qzz;
 }
 
+template <bool FS>
 __global__ void __launch_bounds__(NTHX * NTHY) sapp3(Rev A)
 {
     const Geo& G = A.G;
     int b, iz, iy, ix;
     if (!cell_of(G, b, iz, iy, ix) || !in_core(G, ix, iy, iz)) return;
-    const long long sy = G.nx, sz = (long long)G.nx * G.ny;
+    const long long sy = G.nx;
     const long long i = b * G.S + (iz * (long long)G.ny + iy) * G.nx + ix;
     float* const* q = A.q;
-    A.a[VX][i] += dp(q[0], i, 1, G.idx) + dm(q[1], i, sy, G.idy) + dm(q[2], i, sz, G.idz);
-    A.a[VY][i] += dm(q[3], i, 1, G.idx) + dp(q[4], i, sy, G.idy) + dm(q[5], i, sz, G.idz);
-    A.a[VZ][i] += dm(q[6], i, 1, G.idx) + dm(q[7], i, sy, G.idy) + dp(q[8], i, sz, G.idz);
+    A.a[VX][i] += dp(q[0], i, 1, G.idx) + dm(q[1], i, sy, G.idy) + adz_fs<FS, true>(G, q[2], i, iz, false, false);
+    A.a[VY][i] += dm(q[3], i, 1, G.idx) + dp(q[4], i, sy, G.idy) + adz_fs<FS, true>(G, q[5], i, iz, false, false);
+    A.a[VZ][i] += dm(q[6], i, 1, G.idx) + dm(q[7], i, sy, G.idy) + adz_fs<FS, false>(G, q[8], i, iz, true, true);
 }
 
 __global__ void __launch_bounds__(NTHX * NTHY) vprep3(Rev A)
@@ -487,20 +587,21 @@ __global__ void __launch_bounds__(NTHX * NTHY) vprep3(Rev A)
     A.q[6][i] = pzx; A.q[7][i] = pzy; A.q[8][i] = pzz;
 }
 
+template <bool FS>
 __global__ void __launch_bounds__(NTHX * NTHY) vapp3(Rev A)
 {
     const Geo& G = A.G;
     int b, iz, iy, ix;
     if (!cell_of(G, b, iz, iy, ix) || !in_core(G, ix, iy, iz)) return;
-    const long long sy = G.nx, sz = (long long)G.nx * G.ny;
+    const long long sy = G.nx;
     const long long i = b * G.S + (iz * (long long)G.ny + iy) * G.nx + ix;
     float* const* p = A.q;
     A.a[SXX][i] += dm(p[0], i, 1, G.idx);
     A.a[SXY][i] += dp(p[1], i, sy, G.idy) + dp(p[3], i, 1, G.idx);
-    A.a[SXZ][i] += dp(p[2], i, sz, G.idz) + dp(p[6], i, 1, G.idx);
+    A.a[SXZ][i] += adz_fs<FS, false>(G, p[2], i, iz, true, true) + dp(p[6], i, 1, G.idx);
     A.a[SYY][i] += dm(p[4], i, sy, G.idy);
-    A.a[SYZ][i] += dp(p[5], i, sz, G.idz) + dp(p[7], i, sy, G.idy);
-    A.a[SZZ][i] += dm(p[8], i, sz, G.idz);
+    A.a[SYZ][i] += adz_fs<FS, false>(G, p[5], i, iz, true, true) + dp(p[7], i, sy, G.idy);
+    A.a[SZZ][i] += adz_fs<FS, true>(G, p[8], i, iz, true, false);
 }
 
 // v(it) carriers on the box (they hold v(it + 1) for the next reverse step)
@@ -573,10 +674,14 @@ static Plan make_plan(const sweep_elastic3d_desc* d, int mem_mode)
     for (int k = 0; k < d->nrec_fields; ++k)
         SWEEP_REQUIRE(d->rec_fields[k] >= 0 && d->rec_fields[k] < NFLD, "elastic3d: bad receiver field %d",
                       d->rec_fields[k]);
-    for (int f = 0; f < 6; ++f)
-        SWEEP_REQUIRE(d->pad[f] >= 1, "elastic3d: every face needs a PML pad >= 1 (face %d has %d)", f, d->pad[f]);
+    if (d->free_surface)
+        SWEEP_REQUIRE(d->pad[0] == 0, "elastic3d: a free top face has no PML pad (got %d)", d->pad[0]);
+    for (int f = d->free_surface ? 1 : 0; f < 6; ++f)
+        SWEEP_REQUIRE(d->pad[f] >= 1, "elastic3d: every absorbing face needs a PML pad >= 1 (face %d has %d)", f,
+                      d->pad[f]);
     Plan pl{};
     Geo& G = pl.G;
+    G.fst = d->free_surface ? 1 : 0;
     G.B = d->B; G.nz = d->nz; G.ny = d->ny; G.nx = d->nx; G.nt = d->nt;
     G.S = (long long)d->nz * d->ny * d->nx;
     SWEEP_REQUIRE(G.S < (1LL << 31), "elastic3d: one shot's grid must hold < 2^31 cells");
@@ -717,6 +822,11 @@ static Models models_of(const sweep_elastic3d_desc* d, const Common& w)
     return Models{w.lam, w.mu, w.kv, d->vp, d->vs, d->rho};
 }
 
+static dim3 rec_grid(const Geo& G)
+{
+    return dim3((unsigned)std::min((G.nrec + 127) / 128, 64), (unsigned)G.B);
+}
+
 static dim3 cell_grid(const Geo& G)
 {
     return dim3((G.nx + NTHX - 1) / NTHX, (G.ny + NTHY - 1) / NTHY, (unsigned)(G.nz * G.B));
@@ -748,12 +858,17 @@ void forward(const sweep_elastic3d_desc* d, int mem_mode, int, float* record, vo
     float* slots = static_cast<float*>(tape);
     const unsigned sblocks = (unsigned)std::min<long long>(((long long)G.B * G.ns + 255) / 256, 4096);
     for (int it = 0; it < G.nt; ++it) {
-        vel3<<<grid, block, 0, st>>>(A);
-        str3<<<grid, block, 0, st>>>(A);
+        if (G.fst) {
+            vel3<true><<<grid, block, 0, st>>>(A);
+            str3<true><<<grid, block, 0, st>>>(A);
+        } else {
+            vel3<false><<<grid, block, 0, st>>>(A);
+            str3<false><<<grid, block, 0, st>>>(A);
+        }
         if (G.nsrc > 0) src3<<<G.B, 128, 0, st>>>(G, F, it, 1.f);
         if (slots && G.ns > 0)
             strips3<<<sblocks, 256, 0, st>>>(G, F, slots + (long long)it * step_floats(pl), 0, NFLD, 0);
-        if (record && G.nrec > 0) rec3<<<G.B, 128, 0, st>>>(G, F, record, it);
+        if (record && G.nrec > 0) rec3<<<rec_grid(G), 128, 0, st>>>(G, F, record, it);
         SWEEP_LAUNCH_CHECK();
     }
     if (slots) {
@@ -802,17 +917,22 @@ void backward(const sweep_elastic3d_desc* d, int mem_mode, int, const float* adj
         A.it = it;
         float* prev = const_cast<float*>(slots) + (long long)(it - 1) * step_floats(pl);
         if (vsrc && G.nsrc > 0) vsrc3<<<G.B, 128, 0, st>>>(A);
-        if (G.nrec > 0) res3<<<G.B, 128, 0, st>>>(A);
+        if (G.nrec > 0) res3<<<rec_grid(G), 128, 0, st>>>(A);
         if (G.nsrc > 0) src3<<<G.B, 128, 0, st>>>(G, F, it, -1.f);
-        srev3<<<grid, block, 0, st>>>(A);
+        if (G.fst) srev3<true><<<grid, block, 0, st>>>(A);
+        else srev3<false><<<grid, block, 0, st>>>(A);
         if (G.ns > 0) strips3<<<sblocks, 256, 0, st>>>(G, F, prev, SXX, NFLD, 1);
-        sprep3<<<grid, block, 0, st>>>(A);
-        if (G.nrec > 0) rrho3<<<G.B, 128, 0, st>>>(A);
-        sapp3<<<grid, block, 0, st>>>(A);
+        if (G.fst) sprep3<true><<<grid, block, 0, st>>>(A);
+        else sprep3<false><<<grid, block, 0, st>>>(A);
+        if (G.nrec > 0) rrho3<<<rec_grid(G), 128, 0, st>>>(A);
+        if (G.fst) sapp3<true><<<grid, block, 0, st>>>(A);
+        else sapp3<false><<<grid, block, 0, st>>>(A);
         vprep3<<<grid, block, 0, st>>>(A);
-        vapp3<<<grid, block, 0, st>>>(A);
+        if (G.fst) vapp3<true><<<grid, block, 0, st>>>(A);
+        else vapp3<false><<<grid, block, 0, st>>>(A);
         cap3<<<grid, block, 0, st>>>(A);
-        vrev3<<<grid, block, 0, st>>>(A);
+        if (G.fst) vrev3<true><<<grid, block, 0, st>>>(A);
+        else vrev3<false><<<grid, block, 0, st>>>(A);
         if (G.ns > 0) strips3<<<sblocks, 256, 0, st>>>(G, F, prev, VX, SXX, 1);
         SWEEP_LAUNCH_CHECK();
     }

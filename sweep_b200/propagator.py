@@ -134,15 +134,16 @@ class _Geometry:
         # Elastic with free faces: the cells past a surface are air, which the
         # image method overwrites, so a source or receiver there is off the
         # grid (the reference would fold its adjoint back through the images)
-        self.fs_faces = tuple(prop.fs_faces) if isinstance(eq, Elastic) and self.ndim == 2 else (False,) * 4
+        self.fs_faces = tuple(prop.fs_faces) if isinstance(eq, Elastic) else (False,) * (2 * self.ndim)
         if any(self.fs_faces):
             src_rt, rec_rt = np.array(src_rt, np.int64), np.array(rec_rt, np.int64)
-            nz, nx = self.shape
+            nz, nx = self.shape[0], self.shape[-1]
             M = self.M
             for loc in (src_rt, rec_rt):
-                x, z = loc[..., 0], loc[..., 1]
+                x, z = loc[..., 0], loc[..., -1]
                 air = np.zeros(x.shape, bool)
-                for on, cut in zip(self.fs_faces, (z < M, z > nz - 1 - M, x < M, x > nx - 1 - M)):
+                faces = self.fs_faces if self.ndim == 2 else (self.fs_faces[0], False, False, False)
+                for on, cut in zip(faces, (z < M, z > nz - 1 - M, x < M, x > nx - 1 - M)):
                     if on:
                         air |= cut
                 loc[air] = -(1 << 20)
@@ -254,6 +255,7 @@ class _Geometry:
         d.nrec_fields = len(rec_fields)
         for k, f in enumerate(rec_fields):
             d.rec_fields[k] = f
+        d.free_surface = 1 if self.fs_faces[0] else 0
         return d
 
 
@@ -411,8 +413,6 @@ class PropTorch(torch.nn.Module):
         if self.abcn < 1:
             raise NotImplementedError("sweep_b200: the absorbing faces need a layer (abcn >= 1)")
         self.fs_faces = free_faces(free_surface, nd)
-        if isinstance(equation, Elastic3D) and any(self.fs_faces):
-            raise NotImplementedError("sweep_b200: an Elastic3D free surface is not built")
         if nd == 3 and any(self.fs_faces[1:]):
             raise NotImplementedError("per-face free surfaces are 2-D only (as in the reference); "
                                       "3-D takes free_surface=True (the top face)")

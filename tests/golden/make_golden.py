@@ -734,6 +734,44 @@ def elastic3d():
     np.savez_compressed(OUT / "elastic3d.npz", **out)
 
 
+def elastic3d_free_surface():
+    """3-D isotropic elastic with a traction-free top face (reference
+    Elastic3D, PropTorch(free_surface=True): no PML on top, the full stencil
+    over image values, Robertsson sxx / syy and szz = 0 on the surface row).
+    2 explosive shots, one on the surface row; (vx, vy, vz, sxx) receivers on
+    the surface row and two rows below; vp/vs/rho gradients."""
+    from sweep.equations import Elastic3D
+    rng = np.random.default_rng(97)
+    nz, ny, nx, nt, dt, dh, abcn = 18, 20, 22, 150, 0.0005, 5.0, 6
+    base = _layered(nz, nx, rng, 1900.0, 3000.0, 3)
+    vp_true = np.ascontiguousarray(np.repeat(base[:, None, :], ny, axis=1)
+                                   * (1 + 0.02 * np.cos(np.arange(ny) / 4.0))[None, :, None]).astype(np.float32)
+    vs_true = (vp_true / 1.73).astype(np.float32)
+    rho_true = (310.0 * vp_true ** 0.25).astype(np.float32)
+    vp_init = np.full((nz, ny, nx), 2300.0, np.float32)
+    vs_init = (vp_init / 1.73).astype(np.float32)
+    rho_init = (310.0 * vp_init ** 0.25).astype(np.float32)
+    w = _wavelet(nt, dt, 30.0, 0.03)
+    src = np.array([[8, 9, 0], [14, 11, 3]], np.int64)               # (x, y, z)
+    rec = np.zeros((2, 10, 3), np.int64)
+    for b in range(2):
+        rec[b, :, 0] = np.linspace(1, nx - 2, 10).astype(np.int64)
+        rec[b, :, 1] = np.linspace(2, ny - 3, 10).astype(np.int64)
+        rec[b, :, 2] = 2 * b
+    eq = Elastic3D(spatial_order=8, device="cpu")
+    solver = PropTorch(eq, shape=(nz, ny, nx), dh=dh, dt=dt, abcn=abcn, impl="c", device="cpu",
+                       memory=BoundarySaving(), free_surface=True, receiver_type=["vx", "vy", "vz", "sxx"])
+    obs = _forward(solver, w, src, rec, [vp_true, vs_true, rho_true])
+    r = _run(solver, w, src, rec, [vp_init, vs_init, rho_init], obs, False)
+    np.savez_compressed(
+        OUT / "elastic3d_free_surface.npz",
+        nz=nz, ny=ny, nx=nx, nt=nt, dt=dt, dh=dh, abcn=abcn, order=8,
+        vp_true=vp_true, vs_true=vs_true, rho_true=rho_true,
+        vp_init=vp_init, vs_init=vs_init, rho_init=rho_init, wavelet=w, src=src, rec=rec,
+        obs=obs, pred=r["pred"], loss=r["loss"], grad_vp=r["grad0"], grad_vs=r["grad1"], grad_rho=r["grad2"],
+    )
+
+
 CASES = {
     "acoustic2d_c1": acoustic2d_c1,
     "acoustic2d_multi": acoustic2d_multi,
@@ -755,6 +793,7 @@ CASES = {
     "elastic2d_free_surface": elastic2d_free_surface,
     "elastic2d_free_faces": elastic2d_free_faces,
     "elastic3d": elastic3d,
+    "elastic3d_free_surface": elastic3d_free_surface,
 }
 
 if __name__ == "__main__":

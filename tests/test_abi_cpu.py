@@ -376,8 +376,8 @@ def test_elastic_free_surface_faces_checked():
 
 def test_elastic3d_sizes_and_refusals():
     """The 3-D elastic core sizes its workspace and tape on the host and
-    refuses what is not built (checkpoints, reduced strip formats, free
-    surfaces, launch schedules) before any device work."""
+    refuses what is not built (checkpoints, reduced strip formats, faces
+    other than the top one as free surfaces) before any device work."""
     import numpy as np
     import torch
     from sweep_b200 import Ckpt, Elastic3D, PropTorch, _lib
@@ -393,8 +393,17 @@ def test_elastic3d_sizes_and_refusals():
     for mode in (_lib.MEM_CHECKPOINT, _lib.MEM_BOUNDARY_FP16, _lib.MEM_BOUNDARY | _lib.MEM_HOST_TAPE):
         with pytest.raises(RuntimeError, match="elastic3d"):
             _lib.call("sweep_b200_elastic3d_sizes", d, mode, 10, ws, tape)
-    with pytest.raises(NotImplementedError, match="Elastic3D free surface"):
-        PropTorch(eq, shape=(20, 22, 24), dh=5.0, dt=0.0005, abcn=6, device="cpu", free_surface=True)
+    fs = PropTorch(eq, shape=(20, 22, 24), dh=5.0, dt=0.0005, abcn=6, device="cpu", free_surface=True)
+    assert fs.pads == [0, 6, 6, 6, 6, 6]
+    geo, padded, wb, fields = fs._probe(50, src, rec, [torch.ones(20, 22, 24)] * 3)
+    d = fs._desc(geo, padded, wb, fields)
+    assert d.free_surface == 1 and d.pad[0] == 0
+    _lib.call("sweep_b200_elastic3d_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
+    d.pad[0] = 2
+    with pytest.raises(RuntimeError, match="free top face"):
+        _lib.call("sweep_b200_elastic3d_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
+    with pytest.raises(NotImplementedError, match="per-face"):
+        PropTorch(eq, shape=(20, 22, 24), dh=5.0, dt=0.0005, abcn=6, device="cpu", free_surface=["bottom"])
     with pytest.raises(ValueError, match="source_type"):
         PropTorch(eq, shape=(20, 22, 24), dh=5.0, dt=0.0005, abcn=6, device="cpu",
                   source_type=["sxz", "pressure"])._elastic_fields()

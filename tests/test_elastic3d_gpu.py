@@ -100,3 +100,52 @@ def test_matches_oracle(shape, B, per_shot):
             assert rel(pred, p_o) < REC_TOL
             for g, go in zip(grads, g_o):
                 assert rel(g, go) < GRAD_TOL
+
+
+def test_free_surface_matches_reference_golden():
+    """Traction-free top face: a shot on the surface row, (vx, vy, vz, sxx)
+    receivers on it and two rows below."""
+    d = load("elastic3d_free_surface")
+    s = _solver(tuple(d["vp_true"].shape), float(d["dh"]), float(d["dt"]), int(d["abcn"]), free_surface=True,
+                receiver_type=["vx", "vy", "vz", "sxx"])
+    with torch.no_grad():
+        obs = s(torch.tensor(d["wavelet"], device=DEV), d["src"], d["rec"],
+                models=[torch.tensor(d[k], device=DEV) for k in ("vp_true", "vs_true", "rho_true")])
+    assert rel(obs.cpu().numpy(), d["obs"]) < REC_TOL
+    pred, (gvp, gvs, grho) = _grad_run(s, d["wavelet"], d["src"], d["rec"],
+                                       [d["vp_init"], d["vs_init"], d["rho_init"]], d["obs"])
+    print(f"elastic3d free surface vs reference: record {rel(pred, d['pred']):.2e} "
+          f"vp {rel(gvp, d['grad_vp']):.2e} vs {rel(gvs, d['grad_vs']):.2e} rho {rel(grho, d['grad_rho']):.2e}")
+    assert rel(pred, d["pred"]) < REC_TOL
+    assert rel(gvp, d["grad_vp"]) < GRAD_TOL
+    assert rel(gvs, d["grad_vs"]) < GRAD_TOL
+    assert rel(grho, d["grad_rho"]) < GRAD_TOL
+
+
+def test_free_surface_matches_oracle():
+    """A larger box with the free top face, several shots near it, szz
+    receivers on the surface row (zero off the source cell), against the
+    float32 oracle."""
+    shape, B = (30, 36, 40), 3
+    c = _case(shape, B, 300)
+    c["src"][:, 2] = [0, 1, 3]
+    c["rec"][:, :, 2] = 0
+    c["rec"][-1, -1] = (shape[2] // 2, shape[1] // 2, -2)          # above the surface: off the grid
+    fields = ["vx", "vy", "vz", "szz"]
+    c["obs"] = np.concatenate([c["obs"], c["obs"][..., :1]], -1)
+    s = _solver(shape, c["dh"], c["dt"], c["abcn"], free_surface=True, receiver_type=fields)
+    pred, grads = _grad_run(s, c["w"], c["src"], c["rec"], [c["vp"], c["vs"], c["rho"]], c["obs"])
+    run = O.Elastic3D(c["vp"], c["vs"], c["rho"], c["w"], c["src"], c["rec"], c["dh"], c["dt"], c["abcn"],
+                      receiver_fields=tuple(fields), free_surface=True)
+    run.rec[-1, -1] = -(1 << 20)
+    p_o = run.forward(keep_tape=True)
+    g_o = run.backward(p_o - c["obs"])
+    assert np.all(pred[-1, :, -1] == 0)
+    for b in range(B):
+        off = [r for r in range(16) if tuple(c["rec"][b, r]) != tuple(c["src"][b])]
+        assert np.all(pred[b][:, off, 3] == 0)
+    print(f"elastic3d free surface vs f32 oracle: record {rel(pred, p_o):.2e} "
+          + " ".join(f"{n} {rel(g, go):.2e}" for n, g, go in zip(("vp", "vs", "rho"), grads, g_o)))
+    assert rel(pred, p_o) < REC_TOL
+    for g, go in zip(grads, g_o):
+        assert rel(g, go) < GRAD_TOL

@@ -279,3 +279,27 @@ def test_elastic3d_oracle_matches_reference(prec, tol, tag, kw):
     assert rel(gvp, d[f"grad_vp{tag}"]) < 5 * tol
     assert rel(gvs, d[f"grad_vs{tag}"]) < 5 * tol
     assert rel(grho, d[f"grad_rho{tag}"]) < 5 * tol
+
+
+@pytest.mark.parametrize("prec,tol", [("f32", 2e-6), ("f64", 5e-6)])
+def test_elastic3d_free_surface_oracle_matches_reference(prec, tol):
+    """3-D traction-free top face (the full stencil over image values, the
+    Robertsson sxx / syy correction, szz = 0 on the surface row): a shot on
+    the surface row, (vx, vy, vz, sxx) receivers on it and two rows below.
+    Without the surface terms the records differ at order one."""
+    d = np.load(GOLD / "elastic3d_free_surface.npz")
+    args = (float(d["dh"]), float(d["dt"]), int(d["abcn"]))
+    kw = dict(receiver_fields=("vx", "vy", "vz", "sxx"))
+    obs = O.elastic3d_forward(d["vp_true"], d["vs_true"], d["rho_true"], d["wavelet"], d["src"], d["rec"],
+                              *args, prec=prec, free_surface=True, **kw)
+    assert rel(obs, d["obs"]) < tol
+    plain = O.elastic3d_forward(d["vp_true"], d["vs_true"], d["rho_true"], d["wavelet"], d["src"], d["rec"],
+                                *args, prec=prec, **kw)
+    assert rel(plain, d["obs"]) > 0.1
+    pred, loss, (gvp, gvs, grho) = O.elastic3d_gradient(
+        d["vp_init"], d["vs_init"], d["rho_init"], d["wavelet"], d["src"], d["rec"], d["obs"],
+        *args, prec=prec, free_surface=True, **kw)
+    assert rel(pred, d["pred"]) < tol
+    assert rel(gvp, d["grad_vp"]) < 5 * tol
+    assert rel(gvs, d["grad_vs"]) < 5 * tol
+    assert rel(grho, d["grad_rho"]) < 5 * tol
