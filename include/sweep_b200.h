@@ -209,11 +209,13 @@ SWEEP_B200_API int sweep_b200_elastic_backward(const sweep_elastic_desc* d, int3
                                                void* stream, char* err, int32_t err_cap);
 
 /* 3-D isotropic elastic problem (velocity-stress, staggered grid; reference
- * sweep.equations.Elastic3D, entries 66-70: capi.h:105-110,
+ * sweep.equations.Elastic3D, entries 66-70: capi.h:105-109,
  * elastic3d/driver_traits.cuh).  Wavefield indices: 0 vx, 1 vy, 2 vz, 3 sxx,
  * 4 syy, 5 szz, 6 sxy, 7 sxz, 8 syz (reference common/elastic.h:736-749).
- * Memory: boundary saving with fp32 strips in device memory (mem_mode
- * SWEEP_MEM_BOUNDARY); the other modes are refused. */
+ * Memory: every SWEEP_MEM_* mode -- boundary saving with fp32 / fp16 / bf16 /
+ * int8 strips (entry 67; fp16 and int8 in the reference's per-face layout),
+ * the host tape, SWEEP_MEM_CHECKPOINT (entry 68, nine fields and 18 CPML
+ * memories per checkpoint) and SWEEP_MEM_RECURSIVE (entry 69). */
 typedef struct sweep_elastic3d_desc {
     int32_t B;               /* shots advanced together */
     int32_t nz, ny, nx;      /* runtime grid */

@@ -37,9 +37,12 @@
 // (x: (B, nz, ny, WX), y: (B, nz, WY, nx), z: (B, WZ, ny, nx)).  Cells in the
 // CPML branch because of another axis have zero coefficients on this one and
 // keep no memory (as the reference's stored() gating).
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 #include <vector>
 
 #include "common.cuh"
@@ -74,6 +77,25 @@ struct Fields {
     float* f[9];
 };
 
+// Boundary-strip storage of the boundary-saving tape.  fp32 and bf16 keep the
+// strip set (B, 9, ns), each cell once; fp16 and int8 keep the reference's six
+// faces per field -- bands M + 1 wide starting M cells outside the box (z faces
+// across the box, y and x faces over its z range, so edge cells sit in two or
+// three faces) -- each quantised per field and shot in blocks of kQB cells
+// against the block's max |value| (reference boundarysaver.cu:207-460 face
+// layout, boundary/strip.cuh:136-175 bands with offset -M and width M + 1,
+// boundary/runtime.cuh:313-330 and boundarysaver.cu:925-1095 quantisation).
+enum StripFmt { SF_F32 = 0, SF_F16 = 1, SF_BF16 = 2, SF_I8 = 3 };
+constexpr int kQB = 256;
+constexpr int BW = M + 1;           // face band width
+
+struct StripStore {
+    int fmt;                        // StripFmt
+    int cells[6], blocks[6];        // per field and shot, per face (top, bottom, front, back, left, right)
+    long long pay[6], scl[6];       // byte offsets of each face's codes (9, B, cells) and scales (9, B, blocks)
+    long long step;                 // bytes of one step slot
+};
+
 struct Geo {
     int B, nz, ny, nx, nt;
     long long S;                    // cells per shot
@@ -91,6 +113,7 @@ struct Geo {
     const int* cells;               // strip cell offsets in a shot grid
     int ns;                         // strip cells
     int fst;                        // traction-free top face: the surface is row z0 (no pad above)
+    StripStore st;
 };
 
 struct Models {
@@ -334,20 +357,131 @@ __global__ void rec3(const Geo G, const Fields F, float* record, int it)
     }
 }
 
+// Face f cell idx (of one field and shot) of the scaled formats -> grid cell:
+// z faces (band, box y, box x), y faces (box z, band, box x), x faces (box z,
+// box y, band).
+__device__ __forceinline__ void face_cell(const Geo& G, int f, int idx, int& iz, int& iy, int& ix)
+{
+    const int bx = G.x1 - G.x0, by = G.y1 - G.y0;
+    if (f < 2) {
+        ix = G.x0 + idx % bx; idx /= bx;
+        iy = G.y0 + idx % by;
+        iz = (f == 0 ? G.z0 - M : G.z1 - 1) + idx / by;
+    } else if (f < 4) {
+        ix = G.x0 + idx % bx; idx /= bx;
+        iy = (f == 2 ? G.y0 - M : G.y1 - 1) + idx % BW;
+        iz = G.z0 + idx / BW;
+    } else {
+        ix = (f == 4 ? G.x0 - M : G.x1 - 1) + idx % BW; idx /= BW;
+        iy = G.y0 + idx % by;
+        iz = G.z0 + idx / by;
+    }
+}
+
+// The face a scaled-format restore reads strip cell (iz, iy, ix) from: the
+// last of the faces holding it in the reference's write order (top, bottom,
+// front, back, left, right), and the cell's index in that face.
+__device__ __forceinline__ int face_index(const Geo& G, int iz, int iy, int ix, int& f)
+{
+    const int bx = G.x1 - G.x0, by = G.y1 - G.y0;
+    const bool zin = iz >= G.z0 && iz < G.z1, yin = iy >= G.y0 && iy < G.y1, xin = ix >= G.x0 && ix < G.x1;
+    if (zin && yin && ix >= G.x1 - 1 && ix < G.x1 - 1 + BW) { f = 5; return ((iz - G.z0) * by + iy - G.y0) * BW + ix - (G.x1 - 1); }
+    if (zin && yin && ix >= G.x0 - M && ix <= G.x0) { f = 4; return ((iz - G.z0) * by + iy - G.y0) * BW + ix - (G.x0 - M); }
+    if (zin && xin && iy >= G.y1 - 1 && iy < G.y1 - 1 + BW) { f = 3; return ((iz - G.z0) * BW + iy - (G.y1 - 1)) * bx + ix - G.x0; }
+    if (zin && xin && iy >= G.y0 - M && iy <= G.y0) { f = 2; return ((iz - G.z0) * BW + iy - (G.y0 - M)) * bx + ix - G.x0; }
+    if (iz >= G.z1 - 1) { f = 1; return ((iz - (G.z1 - 1)) * by + iy - G.y0) * bx + ix - G.x0; }
+    f = 0;
+    return ((iz - (G.z0 - M)) * by + iy - G.y0) * bx + ix - G.x0;
+}
+
+// Saved value of field fl at grid cell c of shot b in a scaled-format slot
+// (dequantised as the reference does: fp16 code x scale; int8
+// (code - 128) x scale / 127).
+__device__ __forceinline__ float face_val(const Geo& G, const void* slot, int fl, int b, int c)
+{
+    const int ix = c % G.nx, r = c / G.nx, iy = r % G.ny, iz = r / G.ny;
+    int f;
+    const int i = face_index(G, iz, iy, ix, f);
+    const StripStore& S = G.st;
+    const char* base = static_cast<const char*>(slot);
+    const long long row = (long long)fl * G.B + b;
+    const float scale = reinterpret_cast<const float*>(base + S.scl[f])[row * S.blocks[f] + i / kQB];
+    const long long q = row * S.cells[f] + i;
+    if (S.fmt == SF_F16) return __half2float(reinterpret_cast<const __half*>(base + S.pay[f])[q]) * scale;
+    return ((float)reinterpret_cast<const uint8_t*>(base + S.pay[f])[q] - 128.0f) * (scale * (1.0f / 127.0f));
+}
+
 // Strip save (restore = 0) of fields [f0, f1) into / restore out of one step
-// slot (B, 9, ns) of the tape.
-__global__ void strips3(const Geo G, const Fields F, float* slot, int f0, int f1, int restore)
+// slot in format fmt: fp32 / bf16 slots hold the strip set (B, 9, ns); a
+// scaled slot (written by quant3) is read from the field's faces.
+__global__ void strips3(const Geo G, const Fields F, void* slot, int fmt, int f0, int f1, int restore)
 {
     float* const* f = F.f;
     const long long n = (long long)G.B * G.ns;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
         const int b = (int)(e / G.ns), k = (int)(e - (long long)b * G.ns);
-        const long long i = b * G.S + G.cells[k];
+        const int c = G.cells[k];
+        const long long i = b * G.S + c;
         for (int fl = f0; fl < f1; ++fl) {
-            float* t = slot + ((long long)b * NFLD + fl) * G.ns + k;
-            if (restore) f[fl][i] = *t;
-            else *t = f[fl][i];
+            const long long t = ((long long)b * NFLD + fl) * G.ns + k;
+            if (fmt == SF_F32) {
+                float* p = static_cast<float*>(slot) + t;
+                if (restore) f[fl][i] = *p;
+                else *p = f[fl][i];
+            } else if (fmt == SF_BF16) {
+                __nv_bfloat16* p = static_cast<__nv_bfloat16*>(slot) + t;
+                if (restore) f[fl][i] = __bfloat162float(*p);
+                else *p = __float2bfloat16(f[fl][i]);
+            } else if (restore) {
+                f[fl][i] = face_val(G, slot, fl, b, c);
+            }
         }
+    }
+}
+
+// One step's nine fields into the scaled faces of a step slot: one CTA per
+// (field, shot, face, block of kQB cells) -- the block's max |value| (its
+// scale), then the codes (reference boundarysaver.cu:957-990, 1040-1075: int8
+// round(v 127 / max) + 128 clamped to [0, 255]; fp16 v (1 / max)).
+__global__ void __launch_bounds__(kQB) quant3(const Geo G, const Fields F, void* slot)
+{
+    const StripStore& S = G.st;
+    int per = 0;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) per += S.blocks[f];
+    const int row = blockIdx.x / per;                 // field * B + shot
+    const int fl = row / G.B, b = row - fl * G.B;
+    int j = blockIdx.x - row * per, f = 0;
+    while (f < 5 && j >= S.blocks[f]) { j -= S.blocks[f]; ++f; }
+    const int idx = j * kQB + threadIdx.x;
+    const bool in = idx < S.cells[f];
+    float v = 0.f;
+    if (in) {
+        int iz, iy, ix;
+        face_cell(G, f, idx, iz, iy, ix);
+        v = F.f[fl][b * G.S + ((long long)iz * G.ny + iy) * G.nx + ix];
+    }
+    float m = fabsf(v);
+#pragma unroll
+    for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __shared__ float wmax[kQB / 32];
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = m;
+    __syncthreads();
+    m = wmax[0];
+#pragma unroll
+    for (int i = 1; i < kQB / 32; ++i) m = fmaxf(m, wmax[i]);
+    char* base = static_cast<char*>(slot);
+    if (threadIdx.x == 0) reinterpret_cast<float*>(base + S.scl[f])[(long long)row * S.blocks[f] + j] = m;
+    if (!in) return;
+    const long long q = (long long)row * S.cells[f] + idx;
+    if (S.fmt == SF_F16) {
+        const float inv = m > 0.0f ? 1.0f / m : 0.0f;
+        reinterpret_cast<__half*>(base + S.pay[f])[q] = __float2half(v * inv);
+    } else {
+        const float qs = m > 0.0f ? 127.0f / m : 0.0f;
+        int c = __float2int_rn(v * qs) + 128;
+        c = c < 0 ? 0 : (c > 255 ? 255 : c);
+        reinterpret_cast<uint8_t*>(base + S.pay[f])[q] = (uint8_t)c;
     }
 }
 
@@ -649,15 +783,31 @@ __global__ void finalize3(const float* __restrict__ slots, int B, int per_shot, 
 struct Plan {
     Geo G;
     int nm;                      // model copies
+    bool host_tape;              // boundary-saving tape in pinned host memory (SWEEP_MEM_HOST_TAPE)
     std::vector<int> cells;      // strip cells
 };
 
-static Plan make_plan(const sweep_elastic3d_desc* d, int mem_mode)
+static void check_mode(int mem_mode, int ckpt_every)
+{
+    if (mem_mode & SWEEP_MEM_HOST_TAPE) {
+        mem_mode &= ~SWEEP_MEM_HOST_TAPE;
+        SWEEP_REQUIRE(mem_mode != SWEEP_MEM_CHECKPOINT && mem_mode != SWEEP_MEM_RECURSIVE,
+                      "elastic3d: a host tape goes with boundary saving only");
+    }
+    SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY || mem_mode == SWEEP_MEM_CHECKPOINT ||
+                      mem_mode == SWEEP_MEM_BOUNDARY_FP16 || mem_mode == SWEEP_MEM_BOUNDARY_BF16 ||
+                      mem_mode == SWEEP_MEM_BOUNDARY_INT8 || mem_mode == SWEEP_MEM_RECURSIVE,
+                  "elastic3d: unknown memory mode %d", mem_mode);
+    SWEEP_REQUIRE(mem_mode != SWEEP_MEM_CHECKPOINT || ckpt_every >= 1,
+                  "elastic3d: checkpoint interval must be >= 1 (got %d)", ckpt_every);
+    SWEEP_REQUIRE(mem_mode != SWEEP_MEM_RECURSIVE || ckpt_every >= 1,
+                  "elastic3d: the recursive checkpoint budget must be >= 1 (got %d)", ckpt_every);
+}
+
+static Plan make_plan(const sweep_elastic3d_desc* d)
 {
     SWEEP_REQUIRE(d != nullptr, "null descriptor");
     SWEEP_REQUIRE(d->M == M, "elastic3d: only spatial order 8 (M = 4) is built (got M = %d)", d->M);
-    SWEEP_REQUIRE(mem_mode == SWEEP_MEM_BOUNDARY,
-                  "elastic3d: boundary saving with fp32 strips in device memory is built (mem_mode %d)", mem_mode);
     SWEEP_REQUIRE(d->B >= 1 && d->nt >= 1, "elastic3d: B and nt must be >= 1");
     SWEEP_REQUIRE(d->nsrc >= 0 && d->nrec >= 0, "elastic3d: negative source/receiver count");
     SWEEP_REQUIRE(d->nsrc_fields >= 1 && d->nsrc_fields <= 9, "elastic3d: 1 to 9 source fields (got %d)",
@@ -725,6 +875,49 @@ static Plan make_plan(const sweep_elastic3d_desc* d, int mem_mode)
     return pl;
 }
 
+// Strip storage of a memory mode: the step-slot layout of the boundary-saving
+// tape (the checkpoint modes keep their chunk strips as fp32).
+static void set_store(Plan& pl, int mem_mode)
+{
+    pl.host_tape = (mem_mode & SWEEP_MEM_HOST_TAPE) != 0;
+    mem_mode &= ~SWEEP_MEM_HOST_TAPE;
+    Geo& G = pl.G;
+    StripStore& S = G.st;
+    S = StripStore{};
+    S.fmt = mem_mode == SWEEP_MEM_BOUNDARY_FP16 ? SF_F16
+          : mem_mode == SWEEP_MEM_BOUNDARY_BF16 ? SF_BF16
+          : mem_mode == SWEEP_MEM_BOUNDARY_INT8 ? SF_I8 : SF_F32;
+    auto up = [](long long v, long long a) { return (v + a - 1) / a * a; };
+    const long long per = (long long)G.B * NFLD * G.ns;
+    if (S.fmt == SF_F32 || S.fmt == SF_BF16) {
+        S.step = up(per * (S.fmt == SF_F32 ? 4 : 2), 256);
+        return;
+    }
+    const long long bx = G.x1 - G.x0, by = G.y1 - G.y0, bz = G.z1 - G.z0;
+    const long long cells[6] = {BW * by * bx, BW * by * bx, bz * BW * bx, bz * BW * bx, bz * by * BW, bz * by * BW};
+    const int esz = S.fmt == SF_F16 ? 2 : 1;
+    long long off = 0;
+    for (int f = 0; f < 6; ++f) {
+        SWEEP_REQUIRE(cells[f] * NFLD * G.B < (1LL << 31), "elastic3d: a strip face holds too many cells");
+        S.cells[f] = (int)cells[f];
+        S.blocks[f] = (int)((cells[f] + kQB - 1) / kQB);
+        S.pay[f] = off;
+        off = up(off + (long long)NFLD * G.B * cells[f] * esz, 16);
+    }
+    for (int f = 0; f < 6; ++f) {
+        S.scl[f] = off;
+        off = up(off + (long long)NFLD * G.B * S.blocks[f] * 4, 16);
+    }
+    S.step = up(off, 256);
+}
+
+static unsigned quant_blocks(const Geo& G)
+{
+    long long per = 0;
+    for (int f = 0; f < 6; ++f) per += G.st.blocks[f];
+    return (unsigned)(per * NFLD * G.B);
+}
+
 struct Common {
     float *lam, *mu, *kv;
     int* cells;
@@ -737,18 +930,27 @@ static void carve_common(Carve& c, const Plan& pl, Common& w)
     w.cells = c.take<int>(std::max(pl.G.ns, 1));
 }
 
+static long long slab_count(const Geo& G, int axis)
+{
+    return axis == 0 ? (long long)G.B * G.nz * G.ny * G.WX
+         : axis == 1 ? (long long)G.B * G.nz * G.WY * G.nx : (long long)G.B * G.WZ * G.ny * G.nx;
+}
+
 static void carve_slabs(Carve& c, const Geo& G, Slabs& s)
 {
-    for (int k = 0; k < 6; ++k) s.x[k] = c.take<float>((long long)G.B * G.nz * G.ny * G.WX);
-    for (int k = 0; k < 6; ++k) s.y[k] = c.take<float>((long long)G.B * G.nz * G.WY * G.nx);
-    for (int k = 0; k < 6; ++k) s.z[k] = c.take<float>((long long)G.B * G.WZ * G.ny * G.nx);
+    for (int k = 0; k < 6; ++k) s.x[k] = c.take<float>(slab_count(G, 0));
+    for (int k = 0; k < 6; ++k) s.y[k] = c.take<float>(slab_count(G, 1));
+    for (int k = 0; k < 6; ++k) s.z[k] = c.take<float>(slab_count(G, 2));
 }
+
+static float* slab_ptr(const Slabs& s, int k) { return k < 6 ? s.x[k] : k < 12 ? s.y[k - 6] : s.z[k - 12]; }
 
 struct FwdWs {
     Common cm;
     float* f[NFLD];
     Slabs mem;
     char *zero0, *zero1;
+    char* ring;                  // host tape: HostRing::R device strip slots
 };
 
 static void carve_fwd(Carve& c, const Plan& pl, FwdWs& w)
@@ -760,6 +962,7 @@ static void carve_fwd(Carve& c, const Plan& pl, FwdWs& w)
     carve_slabs(c, pl.G, w.mem);
     c.take<char>(0);
     w.zero1 = c.base ? c.base + c.off : nullptr;
+    if (pl.host_tape) w.ring = c.take<char>((long long)HostRing::R * pl.G.st.step);
 }
 
 struct RevWs {
@@ -771,6 +974,9 @@ struct RevWs {
     Slabs am;
     float *gvp, *gvs, *grho;
     char *zero0, *zero1;
+    char* ring;                  // host tape: HostRing::R device strip slots
+    Slabs fmem;                  // checkpoint modes: forward CPML memories of the replay
+    float* chunk;                // checkpoint modes: fp32 strips of one chunk, (k + 1, B, 9, ns)
 };
 
 static void carve_rev(Carve& c, const Plan& pl, RevWs& w)
@@ -788,24 +994,115 @@ static void carve_rev(Carve& c, const Plan& pl, RevWs& w)
     w.gvp = c.take<float>(n); w.gvs = c.take<float>(n); w.grho = c.take<float>(n);
     c.take<char>(0);
     w.zero1 = c.base ? c.base + c.off : nullptr;
+    if (pl.host_tape) w.ring = c.take<char>((long long)HostRing::R * G.st.step);
 }
 
-static long long step_floats(const Plan& pl) { return (long long)pl.G.B * NFLD * pl.G.ns; }
+static long long chunk_floats(const Plan& pl) { return (long long)pl.G.B * NFLD * pl.G.ns; }
+
+static void carve_rev_ckpt(Carve& c, const Plan& pl, int k, RevWs& w)
+{
+    carve_rev(c, pl, w);
+    carve_slabs(c, pl.G, w.fmem);
+    w.chunk = c.take<float>((long long)(k + 1) * chunk_floats(pl));
+}
+
+// Boundary-saving tape: one strip slot per step (G.st.step bytes), then the
+// final nine-field state (9, B, nz, ny, nx).
 static int64_t tape_bytes_of(const Plan& pl)
 {
-    return ((long long)pl.G.nt * step_floats(pl) + (long long)NFLD * pl.G.B * pl.G.S) * 4;
+    return (int64_t)pl.G.nt * pl.G.st.step + (int64_t)NFLD * pl.G.B * pl.G.S * 4;
 }
 
-void sizes(const sweep_elastic3d_desc* d, int mem_mode, int, int64_t* ws_bytes, int64_t* tape_bytes)
+static void* tape_slot(const void* tape, const Plan& pl, int it)
 {
-    const Plan pl = make_plan(d, mem_mode);
+    return const_cast<char*>(static_cast<const char*>(tape)) + (long long)it * pl.G.st.step;
+}
+
+static float* tape_last(const void* tape, const Plan& pl)
+{
+    return reinterpret_cast<float*>(static_cast<char*>(tape_slot(tape, pl, pl.G.nt)));
+}
+
+// Checkpointed boundary saving (SWEEP_MEM_CHECKPOINT, chunk length k): for
+// every chunk c >= 1 the tape holds the state after step c k - 1 -- the nine
+// fields and the 18 forward CPML memories -- and the fp32 strips of that step;
+// the backward replays each chunk from its checkpoint into the strips of that
+// chunk and runs the boundary-saving reverse steps over it (the reference's
+// staggered driver replays chunks as well, sg_driver.cuh:911-925).  The
+// recursive mode (SWEEP_MEM_RECURSIVE) keeps snapshots of the same layout.
+static long long slab_floats(const Geo& G) { return 6 * (slab_count(G, 0) + slab_count(G, 1) + slab_count(G, 2)); }
+
+static long long ckpt_stride(const Plan& pl)
+{
+    Carve c(nullptr);
+    c.take<float>((long long)NFLD * pl.G.B * pl.G.S);
+    c.take<float>(slab_floats(pl.G));
+    c.take<float>(chunk_floats(pl));
+    return (c.off + 255) & ~255LL;
+}
+
+static int nchunks(const Plan& pl, int k)
+{
+    SWEEP_REQUIRE(k >= 1, "elastic3d: checkpoint interval must be >= 1 (got %d)", k);
+    return (pl.G.nt + k - 1) / k;
+}
+
+struct Ckpt {
+    float* f[NFLD];
+    float* mem;           // the 18 slabs, x then y then z, in carve_slabs order
+    float* strips;
+};
+
+static Ckpt ckpt_at(void* tape, const Plan& pl, int ch)
+{
+    Carve c(static_cast<char*>(tape) + (long long)(ch - 1) * ckpt_stride(pl));
+    Ckpt k{};
+    for (int f = 0; f < NFLD; ++f) k.f[f] = c.take<float>((long long)pl.G.B * pl.G.S);
+    k.mem = c.take<float>(slab_floats(pl.G));
+    k.strips = c.take<float>(chunk_floats(pl));
+    return k;
+}
+
+// Copy the 18 slabs between a Slabs set and a packed checkpoint range.
+static void slabs_copy(const Slabs& s, float* packed, const Geo& G, bool to_packed, cudaStream_t st)
+{
+    long long o = 0;
+    for (int k = 0; k < 18; ++k) {
+        float* p = slab_ptr(s, k);
+        const long long cnt = slab_count(G, k / 6);
+        if (to_packed) SWEEP_CUDA(cudaMemcpyAsync(packed + o, p, cnt * 4, cudaMemcpyDeviceToDevice, st));
+        else SWEEP_CUDA(cudaMemcpyAsync(p, packed + o, cnt * 4, cudaMemcpyDeviceToDevice, st));
+        o += cnt;
+    }
+}
+
+static void slabs_zero(const Slabs& s, const Geo& G, cudaStream_t st)
+{
+    for (int k = 0; k < 18; ++k) SWEEP_CUDA(cudaMemsetAsync(slab_ptr(s, k), 0, slab_count(G, k / 6) * 4, st));
+}
+
+void sizes(const sweep_elastic3d_desc* d, int mem_mode, int ckpt_every, int64_t* ws_bytes, int64_t* tape_bytes)
+{
+    check_mode(mem_mode, ckpt_every);
+    Plan pl = make_plan(d);
+    set_store(pl, mem_mode);
+    const int mode = mem_mode & ~SWEEP_MEM_HOST_TAPE;
     Carve f(nullptr), r(nullptr);
     FwdWs fw{};
     RevWs rw{};
     carve_fwd(f, pl, fw);
-    carve_rev(r, pl, rw);
+    if (mode == SWEEP_MEM_CHECKPOINT) {
+        carve_rev_ckpt(r, pl, ckpt_every, rw);
+        *tape_bytes = (int64_t)std::max(nchunks(pl, ckpt_every) - 1, 1) * ckpt_stride(pl);
+    } else if (mode == SWEEP_MEM_RECURSIVE) {
+        carve_rev_ckpt(r, pl, SWEEP_RECURSIVE_LEAF, rw);
+        r.take<char>((long long)ckpt_every * ckpt_stride(pl));          // the snapshot slots
+        *tape_bytes = 256;                                               // nothing is kept
+    } else {
+        carve_rev(r, pl, rw);
+        *tape_bytes = tape_bytes_of(pl);
+    }
     *ws_bytes = std::max(f.off, r.off);
-    *tape_bytes = tape_bytes_of(pl);
 }
 
 static void setup_common(const sweep_elastic3d_desc* d, const Plan& pl, const Common& w, cudaStream_t st)
@@ -832,10 +1129,49 @@ static dim3 cell_grid(const Geo& G)
     return dim3((G.nx + NTHX - 1) / NTHX, (G.ny + NTHY - 1) / NTHY, (unsigned)(G.nz * G.B));
 }
 
-void forward(const sweep_elastic3d_desc* d, int mem_mode, int, float* record, void* tape, void* ws, int64_t ws_bytes,
-             cudaStream_t st)
+static unsigned strip_blocks(const Geo& G)
 {
-    Plan pl = make_plan(d, mem_mode);
+    return (unsigned)std::max<long long>(std::min<long long>(((long long)G.B * G.ns + 255) / 256, 4096), 1);
+}
+
+// Forward steps [it0, it1) on the fields / memories of A; strips_of(it) is
+// the slot (format fmt) that takes the strips of step it, or null.
+template <class StripsOf>
+static void forward_steps(const Fwd& A, int it0, int it1, StripsOf strips_of, int fmt, float* record, cudaStream_t st,
+                          HostRing* hr = nullptr)
+{
+    const Geo& G = A.G;
+    Fields F{};
+    for (int k = 0; k < NFLD; ++k) F.f[k] = A.f[k];
+    const dim3 grid = cell_grid(G), block(NTHX, NTHY);
+    const bool scaled = fmt == SF_F16 || fmt == SF_I8;
+    for (int it = it0; it < it1; ++it) {
+        if (G.fst) {
+            vel3<true><<<grid, block, 0, st>>>(A);
+            str3<true><<<grid, block, 0, st>>>(A);
+        } else {
+            vel3<false><<<grid, block, 0, st>>>(A);
+            str3<false><<<grid, block, 0, st>>>(A);
+        }
+        if (G.nsrc > 0) src3<<<G.B, 128, 0, st>>>(G, F, it, 1.f);
+        if (void* slot = strips_of(it)) {
+            if (hr) hr->before_write(it);
+            if (scaled) quant3<<<quant_blocks(G), kQB, 0, st>>>(G, F, slot);
+            else if (G.ns > 0) strips3<<<strip_blocks(G), 256, 0, st>>>(G, F, slot, fmt, 0, NFLD, 0);
+            if (hr) hr->after_write(it);
+        }
+        if (record && G.nrec > 0) rec3<<<rec_grid(G), 128, 0, st>>>(G, F, record, it);
+        SWEEP_LAUNCH_CHECK();
+    }
+}
+
+void forward(const sweep_elastic3d_desc* d, int mem_mode, int ckpt_every, float* record, void* tape, void* ws,
+             int64_t ws_bytes, cudaStream_t st)
+{
+    check_mode(mem_mode, ckpt_every);
+    Plan pl = make_plan(d);
+    set_store(pl, mem_mode);
+    const int mode = mem_mode & ~SWEEP_MEM_HOST_TAPE;
     Carve c(ws);
     FwdWs w{};
     carve_fwd(c, pl, w);
@@ -852,52 +1188,65 @@ void forward(const sweep_elastic3d_desc* d, int mem_mode, int, float* record, vo
     A.m = models_of(d, w.cm);
     for (int k = 0; k < NFLD; ++k) A.f[k] = w.f[k];
     A.mem = w.mem;
-    Fields F{};
-    for (int k = 0; k < NFLD; ++k) F.f[k] = w.f[k];
-    const dim3 grid = cell_grid(G), block(NTHX, NTHY);
-    float* slots = static_cast<float*>(tape);
-    const unsigned sblocks = (unsigned)std::min<long long>(((long long)G.B * G.ns + 255) / 256, 4096);
-    for (int it = 0; it < G.nt; ++it) {
-        if (G.fst) {
-            vel3<true><<<grid, block, 0, st>>>(A);
-            str3<true><<<grid, block, 0, st>>>(A);
-        } else {
-            vel3<false><<<grid, block, 0, st>>>(A);
-            str3<false><<<grid, block, 0, st>>>(A);
+    const long long n = (long long)G.B * G.S;
+    if (mode == SWEEP_MEM_RECURSIVE) tape = nullptr;     // the backward replays from the initial state
+    if (mode != SWEEP_MEM_CHECKPOINT) {
+        HostRing hr;
+        const bool host = tape && pl.host_tape;
+        if (host) hr.open(w.ring, tape, G.st.step, st);
+        forward_steps(A, 0, G.nt,
+                      [&](int it) -> void* { return !tape ? nullptr : host ? hr.slot(it) : tape_slot(tape, pl, it); },
+                      G.st.fmt, record, st, host ? &hr : nullptr);
+        if (host) hr.close();
+        if (tape) {
+            float* last = tape_last(tape, pl);
+            for (int k = 0; k < NFLD; ++k)
+                SWEEP_CUDA(cudaMemcpyAsync(last + k * n, w.f[k], sizeof(float) * n, cudaMemcpyDefault, st));
         }
-        if (G.nsrc > 0) src3<<<G.B, 128, 0, st>>>(G, F, it, 1.f);
-        if (slots && G.ns > 0)
-            strips3<<<sblocks, 256, 0, st>>>(G, F, slots + (long long)it * step_floats(pl), 0, NFLD, 0);
-        if (record && G.nrec > 0) rec3<<<rec_grid(G), 128, 0, st>>>(G, F, record, it);
-        SWEEP_LAUNCH_CHECK();
+        return;
     }
-    if (slots) {
-        float* fin = slots + (long long)G.nt * step_floats(pl);
-        for (int k = 0; k < NFLD; ++k)
-            SWEEP_CUDA(cudaMemcpyAsync(fin + (long long)k * G.B * G.S, w.f[k], sizeof(float) * G.B * G.S,
-                                       cudaMemcpyDeviceToDevice, st));
+    const int k = ckpt_every, C = nchunks(pl, k);
+    for (int ch = 0; ch < C; ++ch) {
+        const int it0 = ch * k, it1 = std::min(G.nt, it0 + k);
+        if (tape && ch >= 1) {
+            const Ckpt cp = ckpt_at(tape, pl, ch);
+            for (int f = 0; f < NFLD; ++f)
+                SWEEP_CUDA(cudaMemcpyAsync(cp.f[f], w.f[f], sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+            slabs_copy(w.mem, cp.mem, G, true, st);
+        }
+        // the last step of a chunk keeps its strips with the next checkpoint
+        forward_steps(A, it0, it1,
+                      [&](int it) -> void* {
+                          return (tape && it == it1 - 1 && ch + 1 < C) ? ckpt_at(tape, pl, ch + 1).strips : nullptr;
+                      },
+                      SF_F32, record, st);
     }
 }
 
-void backward(const sweep_elastic3d_desc* d, int mem_mode, int, const float* adj, const void* tape, float* grad_vp,
-              float* grad_vs, float* grad_rho, void* ws, int64_t ws_bytes, cudaStream_t st)
+void backward(const sweep_elastic3d_desc* d, int mem_mode, int ckpt_every, const float* adj, const void* tape,
+              float* grad_vp, float* grad_vs, float* grad_rho, void* ws, int64_t ws_bytes, cudaStream_t st)
 {
-    Plan pl = make_plan(d, mem_mode);
-    SWEEP_REQUIRE(tape != nullptr, "elastic3d backward: the forward's tape is required");
+    check_mode(mem_mode, ckpt_every);
+    Plan pl = make_plan(d);
+    set_store(pl, mem_mode);
+    const int mode = mem_mode & ~SWEEP_MEM_HOST_TAPE;
+    const bool ckpt = mode == SWEEP_MEM_CHECKPOINT, recursive = mode == SWEEP_MEM_RECURSIVE;
+    SWEEP_REQUIRE(recursive || tape != nullptr, "elastic3d backward: the forward's tape is required");
     Carve c(ws);
     RevWs w{};
-    carve_rev(c, pl, w);
+    char* snaps = nullptr;
+    if (ckpt) carve_rev_ckpt(c, pl, ckpt_every, w);
+    else if (recursive) {
+        carve_rev_ckpt(c, pl, SWEEP_RECURSIVE_LEAF, w);
+        snaps = c.take<char>((long long)ckpt_every * ckpt_stride(pl));
+    } else carve_rev(c, pl, w);
     SWEEP_REQUIRE(ws != nullptr && c.off <= ws_bytes, "elastic3d backward: workspace too small (%lld < %lld bytes)",
                   (long long)ws_bytes, (long long)c.off);
     Geo& G = pl.G;
     G.cells = w.cm.cells;
     setup_common(d, pl, w.cm, st);
     SWEEP_CUDA(cudaMemsetAsync(w.zero0, 0, w.zero1 - w.zero0, st));
-    const float* slots = static_cast<const float*>(tape);
-    const float* fin = slots + (long long)G.nt * step_floats(pl);
-    for (int k = 0; k < NFLD; ++k)
-        SWEEP_CUDA(cudaMemcpyAsync(w.f[k], fin + (long long)k * G.B * G.S, sizeof(float) * G.B * G.S,
-                                   cudaMemcpyDeviceToDevice, st));
+    const long long n = (long long)G.B * G.S;
     Rev A{};
     A.G = G;
     A.m = models_of(d, w.cm);
@@ -910,31 +1259,143 @@ void backward(const sweep_elastic3d_desc* d, int mem_mode, int, const float* adj
     Fields F{};
     for (int k = 0; k < NFLD; ++k) F.f[k] = w.f[k];
     const dim3 grid = cell_grid(G), block(NTHX, NTHY);
-    const unsigned sblocks = (unsigned)std::min<long long>(((long long)G.B * G.ns + 255) / 256, 4096);
     bool vsrc = false;
     for (int k = 0; k < G.nsf; ++k) vsrc |= G.sf[k] <= VZ;
-    for (int it = G.nt - 1; it >= 1; --it) {
-        A.it = it;
-        float* prev = const_cast<float*>(slots) + (long long)(it - 1) * step_floats(pl);
-        if (vsrc && G.nsrc > 0) vsrc3<<<G.B, 128, 0, st>>>(A);
-        if (G.nrec > 0) res3<<<rec_grid(G), 128, 0, st>>>(A);
-        if (G.nsrc > 0) src3<<<G.B, 128, 0, st>>>(G, F, it, -1.f);
-        if (G.fst) srev3<true><<<grid, block, 0, st>>>(A);
-        else srev3<false><<<grid, block, 0, st>>>(A);
-        if (G.ns > 0) strips3<<<sblocks, 256, 0, st>>>(G, F, prev, SXX, NFLD, 1);
-        if (G.fst) sprep3<true><<<grid, block, 0, st>>>(A);
-        else sprep3<false><<<grid, block, 0, st>>>(A);
-        if (G.nrec > 0) rrho3<<<rec_grid(G), 128, 0, st>>>(A);
-        if (G.fst) sapp3<true><<<grid, block, 0, st>>>(A);
-        else sapp3<false><<<grid, block, 0, st>>>(A);
-        vprep3<<<grid, block, 0, st>>>(A);
-        if (G.fst) vapp3<true><<<grid, block, 0, st>>>(A);
-        else vapp3<false><<<grid, block, 0, st>>>(A);
-        cap3<<<grid, block, 0, st>>>(A);
-        if (G.fst) vrev3<true><<<grid, block, 0, st>>>(A);
-        else vrev3<false><<<grid, block, 0, st>>>(A);
-        if (G.ns > 0) strips3<<<sblocks, 256, 0, st>>>(G, F, prev, VX, SXX, 1);
-        SWEEP_LAUNCH_CHECK();
+    HostRing hr;
+    const bool host = pl.host_tape && !ckpt && !recursive;
+    // Reverse steps it1 - 1 .. max(it0, 1) (the staggered reverse has no
+    // it = 0 step) on the reconstruction state after step it1 - 1;
+    // strips_of(t) holds the strips (format fmt) of the state after step t.
+    auto reverse = [&](int it0, int it1, auto strips_of, int fmt) {
+        for (int it = it1 - 1; it >= std::max(it0, 1); --it) {
+            A.it = it;
+            void* prev = strips_of(it - 1);
+            if (host) hr.before_read(it - 1);
+            if (vsrc && G.nsrc > 0) vsrc3<<<G.B, 128, 0, st>>>(A);
+            if (G.nrec > 0) res3<<<rec_grid(G), 128, 0, st>>>(A);
+            if (G.nsrc > 0) src3<<<G.B, 128, 0, st>>>(G, F, it, -1.f);
+            if (G.fst) srev3<true><<<grid, block, 0, st>>>(A);
+            else srev3<false><<<grid, block, 0, st>>>(A);
+            if (G.ns > 0) strips3<<<strip_blocks(G), 256, 0, st>>>(G, F, prev, fmt, SXX, NFLD, 1);
+            if (G.fst) sprep3<true><<<grid, block, 0, st>>>(A);
+            else sprep3<false><<<grid, block, 0, st>>>(A);
+            if (G.nrec > 0) rrho3<<<rec_grid(G), 128, 0, st>>>(A);
+            if (G.fst) sapp3<true><<<grid, block, 0, st>>>(A);
+            else sapp3<false><<<grid, block, 0, st>>>(A);
+            vprep3<<<grid, block, 0, st>>>(A);
+            if (G.fst) vapp3<true><<<grid, block, 0, st>>>(A);
+            else vapp3<false><<<grid, block, 0, st>>>(A);
+            cap3<<<grid, block, 0, st>>>(A);
+            if (G.fst) vrev3<true><<<grid, block, 0, st>>>(A);
+            else vrev3<false><<<grid, block, 0, st>>>(A);
+            if (G.ns > 0) strips3<<<strip_blocks(G), 256, 0, st>>>(G, F, prev, fmt, VX, SXX, 1);
+            if (host) {
+                hr.after_read(it - 1);
+                if (it - 1 - HostRing::R >= std::max(it0 - 1, 0)) hr.fetch(it - 1 - HostRing::R, true);
+            }
+            SWEEP_LAUNCH_CHECK();
+        }
+    };
+    // the replay of the checkpoint modes runs straight into the reconstruction
+    // fields, with its own forward CPML memories
+    Fwd R{};
+    R.G = G;
+    R.m = A.m;
+    for (int k = 0; k < NFLD; ++k) R.f[k] = w.f[k];
+    R.mem = w.fmem;
+    const long long cs = chunk_floats(pl);
+    auto chunk_slot = [&](int j) -> void* { return w.chunk + (long long)j * cs; };
+    if (recursive) {
+        // Recursive checkpointing: the bisection of the acoustic drivers; a
+        // snapshot slot has the checkpoint layout (nine fields, 18 CPML slabs,
+        // strips of the step before), leaves are SWEEP_RECURSIVE_LEAF steps.
+        const int L = SWEEP_RECURSIVE_LEAF, count = ckpt_every;
+        auto restore = [&](int k) {
+            if (k < 0) {
+                for (int f = 0; f < NFLD; ++f) SWEEP_CUDA(cudaMemsetAsync(w.f[f], 0, sizeof(float) * n, st));
+                slabs_zero(w.fmem, G, st);
+            } else {
+                const Ckpt cp = ckpt_at(snaps, pl, k + 1);
+                for (int f = 0; f < NFLD; ++f)
+                    SWEEP_CUDA(cudaMemcpyAsync(w.f[f], cp.f[f], sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+                slabs_copy(w.fmem, cp.mem, G, false, st);
+            }
+        };
+        auto save = [&](int k) {
+            const Ckpt cp = ckpt_at(snaps, pl, k + 1);
+            for (int f = 0; f < NFLD; ++f)
+                SWEEP_CUDA(cudaMemcpyAsync(cp.f[f], w.f[f], sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+            slabs_copy(w.fmem, cp.mem, G, true, st);
+        };
+        auto strips_from = [&](int k) {        // strips of the step before snapshot k into chunk slot 0
+            SWEEP_CUDA(cudaMemcpyAsync(w.chunk, ckpt_at(snaps, pl, k + 1).strips, sizeof(float) * cs,
+                                       cudaMemcpyDeviceToDevice, st));
+        };
+        auto leaf = [&](int a, int e) {
+            forward_steps(R, a, e, [&](int it) { return chunk_slot(it - a + 1); }, SF_F32, nullptr, st);
+            reverse(a, e, [&](int t) { return chunk_slot(t - (a - 1)); }, SF_F32);
+        };
+        std::function<void(int, int, int, int)> process = [&](int a, int b, int ka, int free) {
+            const int nleaf = (b - a + L - 1) / L;
+            if (nleaf <= 1) {
+                restore(ka);
+                if (a > 0) strips_from(ka);
+                leaf(a, b);
+                return;
+            }
+            if (free > 0) {
+                const int k = count - free, m = a + L * ((nleaf + 1) / 2);
+                restore(ka);
+                float* ks = ckpt_at(snaps, pl, k + 1).strips;
+                forward_steps(R, a, m, [&](int it) -> void* { return it == m - 1 ? ks : nullptr; }, SF_F32, nullptr,
+                              st);
+                save(k);
+                process(m, b, k, free - 1);
+                process(a, m, ka, free);
+                return;
+            }
+            for (int c0 = a + (nleaf - 1) * L; c0 >= a; c0 -= L) {
+                restore(ka);
+                if (c0 > a)
+                    forward_steps(R, a, c0, [&](int it) -> void* { return it == c0 - 1 ? w.chunk : nullptr; },
+                                  SF_F32, nullptr, st);
+                else if (a > 0)
+                    strips_from(ka);
+                leaf(c0, std::min(b, c0 + L));
+            }
+        };
+        process(0, G.nt, -1, count);
+    } else if (!ckpt) {
+        const float* last = tape_last(tape, pl);
+        for (int k = 0; k < NFLD; ++k)
+            SWEEP_CUDA(cudaMemcpyAsync(w.f[k], last + k * n, sizeof(float) * n, cudaMemcpyDefault, st));
+        if (host) {
+            hr.open(w.ring, const_cast<void*>(tape), G.st.step, st);
+            for (int t = G.nt - 2; t >= 0 && t > G.nt - 2 - HostRing::R; --t) hr.fetch(t, false);
+            reverse(0, G.nt, [&](int t) { return hr.slot(t); }, G.st.fmt);
+            hr.close();
+        } else {
+            reverse(0, G.nt, [&](int t) { return tape_slot(tape, pl, t); }, G.st.fmt);
+        }
+    } else {
+        const int k = ckpt_every, C = nchunks(pl, k);
+        void* tp = const_cast<void*>(tape);
+        for (int ch = C - 1; ch >= 0; --ch) {
+            const int it0 = ch * k, it1 = std::min(G.nt, it0 + k);
+            if (ch == 0) {
+                for (int f = 0; f < NFLD; ++f) SWEEP_CUDA(cudaMemsetAsync(w.f[f], 0, sizeof(float) * n, st));
+                slabs_zero(w.fmem, G, st);
+            } else {
+                const Ckpt cp = ckpt_at(tp, pl, ch);
+                for (int f = 0; f < NFLD; ++f)
+                    SWEEP_CUDA(cudaMemcpyAsync(w.f[f], cp.f[f], sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+                slabs_copy(w.fmem, cp.mem, G, false, st);
+                SWEEP_CUDA(cudaMemcpyAsync(w.chunk, cp.strips, sizeof(float) * cs, cudaMemcpyDeviceToDevice, st));
+            }
+            // replay: chunk slot j holds the strips after step it0 - 1 + j
+            forward_steps(R, it0, it1, [&](int it) { return chunk_slot(it - it0 + 1); }, SF_F32, nullptr, st);
+            reverse(it0, it1, [&](int t) { return chunk_slot(t - (it0 - 1)); }, SF_F32);
+        }
     }
     const int per_shot = d->model_stride != 0;
     finalize3<<<592, 256, 0, st>>>(w.gvp, G.B, per_shot, G, grad_vp);

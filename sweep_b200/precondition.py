@@ -146,21 +146,24 @@ def train(net, xs, ys, steps, batch=16, lr=1e-3, seed=0, log_every=0):
     return hist
 
 
-def _line_search(survey, vp, d, obs, f0, alpha0, shrink=4):
+def _line_search(survey, vp, d, obs, f0, alpha0, vmin, vmax, shrink=4):
     """3-point line search along d: misfit at 0, a and 2a; the parabola's
     minimiser (clipped to [0, 4a]) if it improves, else the best tried point.
-    Without a decrease the trial step shrinks 4-fold, ``shrink`` times at most."""
+    Without a decrease the trial step shrinks 4-fold, ``shrink`` times at most.
+    Every trial model is clamped to [vmin, vmax], so the misfit returned is
+    the one of the model a step would take."""
     a0 = alpha0
+    trial = lambda a: survey.misfit((vp + a * d).clamp(vmin, vmax), obs)  # noqa: E731
     for _ in range(shrink + 1):
-        f1 = survey.misfit(vp + a0 * d, obs)
-        f2 = survey.misfit(vp + 2 * a0 * d, obs)
+        f1 = trial(a0)
+        f2 = trial(2 * a0)
         den = f0 - 2 * f1 + f2
         best_a, best_f = (a0, f1) if f1 <= f2 else (2 * a0, f2)
         if den > 0:
             a = a0 * (3 * f0 - 4 * f1 + f2) / (2 * den)
             a = min(max(a, 0.0), 4 * a0)
             if a > 0:
-                fa = survey.misfit(vp + a * d, obs)
+                fa = trial(a)
                 if fa < best_f:
                     best_a, best_f = a, fa
         if best_f < f0:
@@ -176,7 +179,9 @@ def fwi(survey: Survey, v0, obs, iters, net=None, step_ms=20.0, vmin=1400.0, vma
     the plain direction, 4 ``step_ms`` the learned one, which predicts the
     whole remaining update).  With a network its direction is tried first and
     kept when it lowers the data misfit by at least the fraction ``accept``;
-    otherwise the plain illumination-preconditioned step is taken.  Returns (vp, misfit before
+    otherwise the plain illumination-preconditioned step is taken.  A step is
+    taken only when the misfit of the (clamped) model it leads to is below the
+    current one, so the misfit history decreases strictly.  Returns (vp, misfit before
     each iteration and after the last, wall-clock seconds after each
     iteration, number of learned steps taken)."""
     vp = v0.detach().clone()
@@ -188,21 +193,22 @@ def fwi(survey: Survey, v0, obs, iters, net=None, step_ms=20.0, vmin=1400.0, vma
         f0, g, il = survey.gradient(vp, obs)
         if not hist:
             hist.append(f0)
+        fcur = hist[-1]
         step = None
         if net is not None:
             with torch.no_grad():
                 dl = net(features(g, il, vp)[None])[0, 0].float()
             dl = dl / (dl.abs().max() + 1e-30)
-            al, fl = _line_search(survey, vp, dl, obs, f0, a_learned)
-            if fl < (1.0 - accept) * f0:
+            al, fl = _line_search(survey, vp, dl, obs, f0, a_learned, vmin, vmax)
+            if fl < (1.0 - accept) * fcur:
                 step = (fl, vp + al * dl)
                 a_learned = max(1.5 * al, step_ms)
                 learned += 1
         if step is None:
             dp = plain_direction(g, il)
             dp = dp / (dp.abs().max() + 1e-30)
-            ap, fp = _line_search(survey, vp, dp, obs, f0, a_plain)
-            if fp >= f0:
+            ap, fp = _line_search(survey, vp, dp, obs, f0, a_plain, vmin, vmax)
+            if fp >= fcur:
                 break
             step = (fp, vp + ap * dp)
             a_plain = max(1.5 * ap, 0.25 * step_ms)

@@ -772,6 +772,45 @@ def elastic3d_free_surface():
     )
 
 
+def elastic3d_storage():
+    """3-D elastic boundary saving with fp16 / bf16 / int8 strips (reference
+    Elastic3D, BoundarySaving(storage_dtype=...): each of the nine fields
+    quantised per face and shot on its own): 2 explosive shots on a
+    20 x 18 x 22 layered model (CPML 6), vp/vs/rho gradients per format."""
+    from sweep.equations import Elastic3D
+    rng = np.random.default_rng(103)
+    nz, ny, nx, nt, dt, dh, abcn = 20, 18, 22, 140, 0.0005, 5.0, 6
+    base = _layered(nz, nx, rng, 1900.0, 3000.0, 3)
+    vp_true = np.ascontiguousarray(np.repeat(base[:, None, :], ny, axis=1)
+                                   * (1 + 0.02 * np.sin(np.arange(ny) / 2.5))[None, :, None]).astype(np.float32)
+    vs_true = (vp_true / 1.73).astype(np.float32)
+    rho_true = (310.0 * vp_true ** 0.25).astype(np.float32)
+    vp_init = np.full((nz, ny, nx), 2300.0, np.float32)
+    vs_init = (vp_init / 1.73).astype(np.float32)
+    rho_init = (310.0 * vp_init ** 0.25).astype(np.float32)
+    w = _wavelet(nt, dt, 30.0, 0.03)
+    src = np.array([[7, 8, 5], [15, 10, 12]], np.int64)             # (x, y, z)
+    rec = np.zeros((2, 10, 3), np.int64)
+    for b in range(2):
+        rec[b, :, 0] = np.linspace(1, nx - 2, 10).astype(np.int64)
+        rec[b, :, 1] = np.linspace(2, ny - 3, 10).astype(np.int64)
+        rec[b, :, 2] = 2 + 2 * b
+    out = dict(nz=nz, ny=ny, nx=nx, nt=nt, dt=dt, dh=dh, abcn=abcn, order=8,
+               vp_true=vp_true, vs_true=vs_true, rho_true=rho_true,
+               vp_init=vp_init, vs_init=vs_init, rho_init=rho_init, wavelet=w, src=src, rec=rec)
+    for sd in ("fp32", "fp16", "bf16", "int8"):
+        eq = Elastic3D(spatial_order=8, device="cpu")
+        solver = PropTorch(eq, shape=(nz, ny, nx), dh=dh, dt=dt, abcn=abcn, impl="c", device="cpu",
+                           memory=BoundarySaving(storage_dtype=sd))
+        if sd == "fp32":
+            out["obs"] = _forward(solver, w, src, rec, [vp_true, vs_true, rho_true])
+        r = _run(solver, w, src, rec, [vp_init, vs_init, rho_init], out["obs"], False)
+        for i, name in enumerate(("vp", "vs", "rho")):
+            out[f"grad_{name}_{sd}"] = r[f"grad{i}"]
+        out[f"pred_{sd}"] = r["pred"]
+    np.savez_compressed(OUT / "elastic3d_storage.npz", **out)
+
+
 CASES = {
     "acoustic2d_c1": acoustic2d_c1,
     "acoustic2d_multi": acoustic2d_multi,
@@ -794,6 +833,7 @@ CASES = {
     "elastic2d_free_faces": elastic2d_free_faces,
     "elastic3d": elastic3d,
     "elastic3d_free_surface": elastic3d_free_surface,
+    "elastic3d_storage": elastic3d_storage,
 }
 
 if __name__ == "__main__":

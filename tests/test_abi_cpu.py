@@ -375,9 +375,10 @@ def test_elastic_free_surface_faces_checked():
 
 
 def test_elastic3d_sizes_and_refusals():
-    """The 3-D elastic core sizes its workspace and tape on the host and
-    refuses what is not built (checkpoints, reduced strip formats, faces
-    other than the top one as free surfaces) before any device work."""
+    """The 3-D elastic core sizes its workspace and tape on the host for every
+    memory mode and refuses bad ones (a host tape with checkpoints, unknown
+    modes, a zero interval, faces other than the top one as free surfaces)
+    before any device work."""
     import numpy as np
     import torch
     from sweep_b200 import Ckpt, Elastic3D, PropTorch, _lib
@@ -390,9 +391,21 @@ def test_elastic3d_sizes_and_refusals():
     ws, tape = _lib.c_i64(), _lib.c_i64()
     _lib.call("sweep_b200_elastic3d_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
     assert ws.value > 0 and tape.value > 50 * 9 * 4
-    for mode in (_lib.MEM_CHECKPOINT, _lib.MEM_BOUNDARY_FP16, _lib.MEM_BOUNDARY | _lib.MEM_HOST_TAPE):
-        with pytest.raises(RuntimeError, match="elastic3d"):
-            _lib.call("sweep_b200_elastic3d_sizes", d, mode, 10, ws, tape)
+    tapes = {}
+    for mode in (_lib.MEM_BOUNDARY, _lib.MEM_BOUNDARY_FP16, _lib.MEM_BOUNDARY_BF16, _lib.MEM_BOUNDARY_INT8,
+                 _lib.MEM_BOUNDARY | _lib.MEM_HOST_TAPE, _lib.MEM_CHECKPOINT, _lib.MEM_RECURSIVE):
+        _lib.call("sweep_b200_elastic3d_sizes", d, mode, 10, ws, tape)
+        tapes[mode] = tape.value
+    state = 9 * 40 * 42 * 44 * 4                     # the final nine-field state closes the tape
+    strips = tapes[_lib.MEM_BOUNDARY] - state
+    assert tapes[_lib.MEM_BOUNDARY | _lib.MEM_HOST_TAPE] == tapes[_lib.MEM_BOUNDARY]
+    assert abs((tapes[_lib.MEM_BOUNDARY_BF16] - state) / strips - 0.5) < 0.01
+    assert (tapes[_lib.MEM_BOUNDARY_INT8] - state) < (tapes[_lib.MEM_BOUNDARY_FP16] - state) < strips
+    assert tapes[_lib.MEM_CHECKPOINT] < tapes[_lib.MEM_BOUNDARY] and tapes[_lib.MEM_RECURSIVE] == 256
+    for mode, every, msg in ((_lib.MEM_CHECKPOINT | _lib.MEM_HOST_TAPE, 10, "host tape"), (77, 10, "unknown"),
+                             (_lib.MEM_CHECKPOINT, 0, "interval"), (_lib.MEM_RECURSIVE, 0, "budget")):
+        with pytest.raises(RuntimeError, match=msg):
+            _lib.call("sweep_b200_elastic3d_sizes", d, mode, every, ws, tape)
     fs = PropTorch(eq, shape=(20, 22, 24), dh=5.0, dt=0.0005, abcn=6, device="cpu", free_surface=True)
     assert fs.pads == [0, 6, 6, 6, 6, 6]
     geo, padded, wb, fields = fs._probe(50, src, rec, [torch.ones(20, 22, 24)] * 3)
@@ -404,6 +417,8 @@ def test_elastic3d_sizes_and_refusals():
         _lib.call("sweep_b200_elastic3d_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
     with pytest.raises(NotImplementedError, match="per-face"):
         PropTorch(eq, shape=(20, 22, 24), dh=5.0, dt=0.0005, abcn=6, device="cpu", free_surface=["bottom"])
+    with pytest.raises(NotImplementedError, match="Elastic3D runs whole passes"):
+        s.forward_runner(torch.zeros(50), src, rec, [torch.ones(20, 22, 24)] * 3)
     with pytest.raises(ValueError, match="source_type"):
         PropTorch(eq, shape=(20, 22, 24), dh=5.0, dt=0.0005, abcn=6, device="cpu",
                   source_type=["sxz", "pressure"])._elastic_fields()

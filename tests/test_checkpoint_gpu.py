@@ -138,3 +138,43 @@ def test_elastic_recursive_checkpointing(count):
     for a, b, ref in zip(g_rc, g_ck, ("grad_vp", "grad_vs", "grad_rho")):
         assert np.array_equal(a, b)
         assert rel(a, d[ref]) < GRAD_TOL
+
+
+def _elastic3d(d, memory):
+    from sweep_b200 import Elastic3D, PropTorch
+    s = PropTorch(Elastic3D(spatial_order=8, device=DEV), shape=tuple(d["vp_true"].shape), dh=float(d["dh"]),
+                  dt=float(d["dt"]), abcn=int(d["abcn"]), device=DEV, memory=memory)
+    ms = [torch.tensor(d[k], device=DEV, requires_grad=True) for k in ("vp_init", "vs_init", "rho_init")]
+    pred = s(torch.tensor(d["wavelet"], device=DEV), d["src"], d["rec"], models=ms)
+    (0.5 * ((pred - torch.tensor(d["obs"], device=DEV)) ** 2).sum()).backward()
+    torch.cuda.synchronize()
+    return pred.detach().cpu().numpy(), [m.grad.cpu().numpy() for m in ms]
+
+
+@pytest.mark.parametrize("chunks", [37, 1, 200])
+def test_elastic3d_checkpoint(chunks):
+    """Elastic3D with Ckpt(chunks=k): nine fields and 18 CPML memories per
+    checkpoint; records bit-identical to boundary saving, gradients within
+    1e-4 of it and within the bars of the reference (nt 160)."""
+    from sweep_b200 import BoundarySaving, Ckpt
+    d = load("elastic3d")
+    p_bs, g_bs = _elastic3d(d, BoundarySaving())
+    p_ck, g_ck = _elastic3d(d, Ckpt(chunks=chunks))
+    assert np.array_equal(p_ck, p_bs)
+    for name, a, b in zip(("vp", "vs", "rho"), g_ck, g_bs):
+        print(f"elastic3d chunks={chunks} {name}: ckpt vs boundary {rel(a, b):.2e}, "
+              f"vs reference {rel(a, d['grad_' + name]):.2e}")
+        assert rel(a, d["grad_" + name]) < GRAD_TOL
+        assert rel(a, b) < 1e-4
+
+
+@pytest.mark.parametrize("count", [1, 3])
+def test_elastic3d_recursive_checkpointing(count):
+    from sweep_b200 import Ckpt
+    d = load("elastic3d")
+    p_ck, g_ck = _elastic3d(d, Ckpt(chunks=64))
+    p_rc, g_rc = _elastic3d(d, Ckpt(mode="recursive", count=count))
+    assert np.array_equal(p_rc, p_ck)
+    for name, a, b in zip(("vp", "vs", "rho"), g_rc, g_ck):
+        assert np.array_equal(a, b)
+        assert rel(a, d["grad_" + name]) < GRAD_TOL
