@@ -30,8 +30,9 @@
 // grid row; the stencils read global memory through the read-only path.  (A
 // z-marching variant with shared-memory planes and register z-queues, run at
 // two CTAs per SM without a load pipeline, measured 2.8x slower in the
-// forward; the kernels that beat this layout need the 3-D acoustic kernels'
-// TMA plane rings.)
+// forward; four cells of a column per thread with the z taps in a register
+// window, at three CTAs per SM, 1.23x slower; the kernels that beat this
+// layout need the 3-D acoustic kernels' TMA plane rings.)
 // Layout: fields (B, nz, ny, nx), x fastest; CPML memories in per-axis slabs
 // covering the cells outside the box shrunk by one cell along their axis
 // (x: (B, nz, ny, WX), y: (B, nz, WY, nx), z: (B, WZ, ny, nx)).  Cells in the
@@ -394,6 +395,17 @@ __device__ __forceinline__ int face_index(const Geo& G, int iz, int iy, int ix, 
     return ((iz - (G.z0 - M)) * by + iy - G.y0) * bx + ix - G.x0;
 }
 
+// a[f] of a per-face parameter array without a local-memory copy of the array
+template <class T>
+__device__ __forceinline__ T pick6(const T (&a)[6], int f)
+{
+    T v = a[0];
+#pragma unroll
+    for (int k = 1; k < 6; ++k)
+        if (f == k) v = a[k];
+    return v;
+}
+
 // Saved value of field fl at grid cell c of shot b in a scaled-format slot
 // (dequantised as the reference does: fp16 code x scale; int8
 // (code - 128) x scale / 127).
@@ -405,10 +417,11 @@ __device__ __forceinline__ float face_val(const Geo& G, const void* slot, int fl
     const StripStore& S = G.st;
     const char* base = static_cast<const char*>(slot);
     const long long row = (long long)fl * G.B + b;
-    const float scale = reinterpret_cast<const float*>(base + S.scl[f])[row * S.blocks[f] + i / kQB];
-    const long long q = row * S.cells[f] + i;
-    if (S.fmt == SF_F16) return __half2float(reinterpret_cast<const __half*>(base + S.pay[f])[q]) * scale;
-    return ((float)reinterpret_cast<const uint8_t*>(base + S.pay[f])[q] - 128.0f) * (scale * (1.0f / 127.0f));
+    const float scale = reinterpret_cast<const float*>(base + pick6(S.scl, f))[row * pick6(S.blocks, f) + i / kQB];
+    const long long q = row * pick6(S.cells, f) + i;
+    const char* pay = base + pick6(S.pay, f);
+    if (S.fmt == SF_F16) return __half2float(reinterpret_cast<const __half*>(pay)[q]) * scale;
+    return ((float)reinterpret_cast<const uint8_t*>(pay)[q] - 128.0f) * (scale * (1.0f / 127.0f));
 }
 
 // Strip save (restore = 0) of fields [f0, f1) into / restore out of one step
@@ -452,9 +465,12 @@ __global__ void __launch_bounds__(kQB) quant3(const Geo G, const Fields F, void*
     const int row = blockIdx.x / per;                 // field * B + shot
     const int fl = row / G.B, b = row - fl * G.B;
     int j = blockIdx.x - row * per, f = 0;
-    while (f < 5 && j >= S.blocks[f]) { j -= S.blocks[f]; ++f; }
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+        if (f == k && j >= S.blocks[k]) { j -= S.blocks[k]; f = k + 1; }
     const int idx = j * kQB + threadIdx.x;
-    const bool in = idx < S.cells[f];
+    const int cells = pick6(S.cells, f), blocks = pick6(S.blocks, f);
+    const bool in = idx < cells;
     float v = 0.f;
     if (in) {
         int iz, iy, ix;
@@ -471,17 +487,18 @@ __global__ void __launch_bounds__(kQB) quant3(const Geo G, const Fields F, void*
 #pragma unroll
     for (int i = 1; i < kQB / 32; ++i) m = fmaxf(m, wmax[i]);
     char* base = static_cast<char*>(slot);
-    if (threadIdx.x == 0) reinterpret_cast<float*>(base + S.scl[f])[(long long)row * S.blocks[f] + j] = m;
+    if (threadIdx.x == 0) reinterpret_cast<float*>(base + pick6(S.scl, f))[(long long)row * blocks + j] = m;
     if (!in) return;
-    const long long q = (long long)row * S.cells[f] + idx;
+    const long long q = (long long)row * cells + idx;
+    char* pay = base + pick6(S.pay, f);
     if (S.fmt == SF_F16) {
         const float inv = m > 0.0f ? 1.0f / m : 0.0f;
-        reinterpret_cast<__half*>(base + S.pay[f])[q] = __float2half(v * inv);
+        reinterpret_cast<__half*>(pay)[q] = __float2half(v * inv);
     } else {
         const float qs = m > 0.0f ? 127.0f / m : 0.0f;
         int c = __float2int_rn(v * qs) + 128;
         c = c < 0 ? 0 : (c > 255 ? 255 : c);
-        reinterpret_cast<uint8_t*>(base + S.pay[f])[q] = (uint8_t)c;
+        reinterpret_cast<uint8_t*>(pay)[q] = (uint8_t)c;
     }
 }
 
