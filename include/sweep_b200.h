@@ -138,9 +138,11 @@ SWEEP_B200_API int sweep_b200_acoustic_backward(const sweep_acoustic_desc* d, in
  * GPU loading this library holds until exit.  The caller passes the inputs
  * (d) and the output (record, (B, nt, nrec)).  A problem needing more scratch
  * than the array, or more than 65536 shot-tiles or 32768 sources / receivers,
- * is rejected with an error.  The first call on a device looks up the
- * array's address (cudaGetSymbolAddress) with that device current: make it
- * before any stream capture.  The address is kept for the life of the
+ * is rejected with an error.  Every call synchronizes its stream (the
+ * source / receiver tables go through host memory and the error word is read
+ * back), so no call can run under stream capture.  The first call on a device
+ * looks up the array's address (cudaGetSymbolAddress) with that device
+ * current.  The address is kept for the life of the
  * process: cudaDeviceReset after the entry point has been used is not
  * supported.  Every call shares the array: calls that overlap on the GPU
  * race; calls of one process are serialised by one process-wide lock (on

@@ -8,9 +8,11 @@
 // Properties a caller must know:
 //   * the array (kNoAllocScratchBytes) exists on every GPU that loads this
 //     library, from load to process exit;
+//   * every call synchronizes its stream (the source / receiver tables are
+//     staged through host memory, the error word is read back), so no call
+//     can run under stream capture;
 //   * the first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress, with that device current).  Make that first call
-//     before any stream capture;
+//     (cudaGetSymbolAddress, with that device current);
 //   * every call on a device uses the same array: calls that overlap on the
 //     GPU race and corrupt each other; run them one after the other.  Calls
 //     from this process are serialised by one process-wide lock held for the
