@@ -115,11 +115,17 @@ static int strip_cells_2d(int nz, int nx, int M, const int* pad, int w, int* out
     return n;
 }
 
-/* 8th/any-order Laplacian along one axis in difference form (laplace.cuh:93,
- * 327-380): sum_k c_k ((u_-k - u0) + (u_+k - u0)) / h^2, minus tap first. */
+/* Laplacian along one axis as the forward and the reconstruction take it
+ * (laplace.cuh:68-100, 327-445): the difference form
+ * sum_k c_k ((u_-k - u0) + (u_+k - u0)) / h^2, minus tap first, at every order
+ * but 4; order 4 (M = 2) keeps the summed form
+ * (c1 (u_-1 + u_1) + c2 (u_-2 + u_2) - c0 u0) / h^2 with c0 = 5/2
+ * (laplace.cuh:145-200).  The adjoint takes the difference form everywhere. */
 static inline REAL lap_axis(const REAL* u, i64 i, i64 s, int M, const REAL* lc, REAL h)
 {
     REAL u0 = u[i];
+    if (M == 2)
+        return ((lc[1] * (u[i - s] + u[i + s]) + lc[2] * (u[i - 2 * s] + u[i + 2 * s])) - R(2.5) * u0) / (h * h);
     REAL acc = R(0);
     for (int k = 1; k <= M; ++k) {
         REAL t = lc[k] * ((u[i - k * s] - u0) + (u[i + k * s] - u0));

@@ -36,9 +36,13 @@ typedef struct {
     int nrec; const int* rec;
 } A3D;
 
+/* forward / reconstruction Laplacian along one axis: the difference form,
+ * order 4 in the summed form (laplace.cuh:68-100, 145-200; see fd_oracle.c) */
 static inline REAL lap1(const REAL* u, i64 i, i64 s, int M, const REAL* lc, REAL h)
 {
     REAL u0 = u[i], acc = R(0);
+    if (M == 2)
+        return ((lc[1] * (u[i - s] + u[i + s]) + lc[2] * (u[i - 2 * s] + u[i + 2 * s])) - R(2.5) * u0) / (h * h);
     for (int k = 1; k <= M; ++k) {
         REAL t = lc[k] * ((u[i - k * s] - u0) + (u[i + k * s] - u0));
         acc = (k == 1) ? t : acc + t;

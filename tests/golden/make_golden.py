@@ -772,6 +772,56 @@ def elastic3d_free_surface():
     )
 
 
+def acoustic_orders():
+    """Spatial orders other than 8 (the reference's Acoustic / Acoustic3D
+    default to order 4): 2-D at orders 2, 4, 6 and 12 (2 shots on a 40 x 60
+    layered model, CPML 10, a source inside the restore strip), 3-D at orders
+    4 and 6 (2 shots on a 16 x 18 x 20 model, CPML 6); records, vp and wavelet
+    gradients, boundary saving."""
+    rng = np.random.default_rng(211)
+    nz, nx, nt, dt, dh, abcn = 40, 60, 300, 0.001, 10.0, 10
+    vp_true = _layered(nz, nx, rng, 1500.0, 3000.0, 4)
+    vp_init = np.full((nz, nx), 1900.0, np.float32)
+    w = np.stack([_wavelet(nt, dt, 15.0, 0.06), _wavelet(nt, dt, 12.0, 0.07)]).astype(np.float32)
+    src = np.array([[12, 9], [40, 2]], np.int64)                 # (x, z); shot 1 in the restore strip
+    rec = np.zeros((2, 10, 2), np.int64)
+    for b in range(2):
+        rec[b, :, 0] = np.linspace(2, nx - 3, 10).astype(np.int64)
+        rec[b, :, 1] = 3 + 5 * b
+    out = dict(nz=nz, nx=nx, nt=nt, dt=dt, dh=dh, abcn=abcn, vp_true=vp_true, vp_init=vp_init,
+               wavelet=w, src=src, rec=rec)
+    for order in (2, 4, 6, 12):
+        solver = PropTorch(Acoustic(spatial_order=order, device="cpu"), shape=(nz, nx), dh=dh, dt=dt,
+                           abcn=abcn, impl="c", device="cpu", memory=BoundarySaving())
+        obs = _forward(solver, w, src, rec, [vp_true])
+        r = _run(solver, w, src, rec, [vp_init], obs, True)
+        out.update({f"obs_o{order}": obs, f"pred_o{order}": r["pred"], f"grad_vp_o{order}": r["grad0"],
+                    f"grad_wavelet_o{order}": r["grad_wavelet"]})
+    rng = np.random.default_rng(212)
+    nz3, ny3, nx3, nt3, dt3, abcn3 = 16, 18, 20, 150, 0.001, 6
+    vp3_true = np.full((nz3, ny3, nx3), 1800.0, np.float32)
+    vp3_true[nz3 // 2:] = 2500.0
+    vp3_true += (25.0 * rng.standard_normal((nz3, ny3, nx3))).astype(np.float32)
+    vp3_init = np.full((nz3, ny3, nx3), 2000.0, np.float32)
+    w3 = _wavelet(nt3, dt3, 15.0, 0.06)
+    src3 = np.array([[5, 6, 4], [14, 11, 1]], np.int64)          # (x, y, z)
+    rec3 = np.zeros((2, 6, 3), np.int64)
+    for b in range(2):
+        rec3[b, :, 0] = rng.integers(1, nx3 - 1, 6)
+        rec3[b, :, 1] = rng.integers(1, ny3 - 1, 6)
+        rec3[b, :, 2] = rng.integers(1, nz3 - 1, 6)
+    out.update(nz3=nz3, ny3=ny3, nx3=nx3, nt3=nt3, dt3=dt3, abcn3=abcn3, vp3_true=vp3_true, vp3_init=vp3_init,
+               wavelet3=w3, src3=src3, rec3=rec3)
+    for order in (4, 6):
+        solver = PropTorch(Acoustic3D(spatial_order=order, device="cpu"), shape=(nz3, ny3, nx3), dh=dh, dt=dt3,
+                           abcn=abcn3, impl="c", device="cpu", memory=BoundarySaving())
+        obs = _forward(solver, w3, src3, rec3, [vp3_true])
+        r = _run(solver, w3, src3, rec3, [vp3_init], obs, True)
+        out.update({f"obs3_o{order}": obs, f"pred3_o{order}": r["pred"], f"grad3_vp_o{order}": r["grad0"],
+                    f"grad3_wavelet_o{order}": r["grad_wavelet"]})
+    np.savez_compressed(OUT / "acoustic_orders.npz", **out)
+
+
 def elastic3d_storage():
     """3-D elastic boundary saving with fp16 / bf16 / int8 strips (reference
     Elastic3D, BoundarySaving(storage_dtype=...): each of the nine fields
@@ -834,6 +884,7 @@ CASES = {
     "elastic3d": elastic3d,
     "elastic3d_free_surface": elastic3d_free_surface,
     "elastic3d_storage": elastic3d_storage,
+    "acoustic_orders": acoustic_orders,
 }
 
 if __name__ == "__main__":

@@ -303,3 +303,31 @@ def test_elastic3d_free_surface_oracle_matches_reference(prec, tol):
     assert rel(gvp, d["grad_vp"]) < 5 * tol
     assert rel(gvs, d["grad_vs"]) < 5 * tol
     assert rel(grho, d["grad_rho"]) < 5 * tol
+
+
+@pytest.mark.parametrize("order", [2, 4, 6, 12])
+def test_acoustic2d_orders_oracle_matches_reference(order):
+    """Spatial orders other than 8: the oracle reproduces the reference's
+    records and gradients bit for bit in float32 (order 4 with the forward's
+    summed Laplacian)."""
+    d = np.load(GOLD / "acoustic_orders.npz")
+    a = (float(d["dh"]), float(d["dt"]), int(d["abcn"]))
+    obs = O.acoustic_forward(d["vp_true"], d["wavelet"], d["src"], d["rec"], *a, order=order)
+    assert np.array_equal(obs.astype(np.float32), d[f"obs_o{order}"])
+    pred, loss, g, gw = O.acoustic_gradient(d["vp_init"], d["wavelet"], d["src"], d["rec"], d[f"obs_o{order}"], *a,
+                                            order=order)
+    assert rel(pred, d[f"pred_o{order}"]) < 1e-6
+    assert rel(g, d[f"grad_vp_o{order}"]) < 1e-6
+    assert rel(gw, d[f"grad_wavelet_o{order}"]) < 1e-6
+
+
+@pytest.mark.parametrize("order", [4, 6])
+def test_acoustic3d_orders_oracle_matches_reference(order):
+    d = np.load(GOLD / "acoustic_orders.npz")
+    a = (float(d["dh"]), float(d["dt3"]), int(d["abcn3"]))
+    run = O.Acoustic3D(d["vp3_init"], d["wavelet3"], d["src3"], d["rec3"], *a, order=order)
+    pred = run.forward()
+    assert rel(pred, d[f"pred3_o{order}"]) < 1e-6
+    g, gw = run.backward(pred - d[f"obs3_o{order}"])
+    assert rel(g, d[f"grad3_vp_o{order}"]) < 1e-6
+    assert rel(gw[0], d[f"grad3_wavelet_o{order}"]) < 1e-6     # shot 0: the reference's 3-D defect
