@@ -209,7 +209,7 @@ class AcousticWorkload:
 
     def config(self, args):
         return {"workload": f"acoustic2d {NZ}x{NX} (runtime {RT[0]}x{RT[1]}), {NSHOT} shots, nt {NT}, "
-                            f"order 8, CPML {ABCN}, fwd+adj gradient, boundary saving",
+                            f"order {ORDER}, CPML {ABCN}, fwd+adj gradient, boundary saving",
                 "grid": [NZ, NX], "runtime_grid": list(RT), "shots_per_gpu": NSHOT, "nt": NT,
                 "dh": DH, "dt": DT, "abcn": ABCN, "order": ORDER, "seed": SEED,
                 "cells_counted": "runtime grid (physical + PML + halo) x shots x nt",
@@ -277,7 +277,7 @@ class AcousticC1Workload:
 
     def config(self, args):
         return {"workload": f"acoustic2d {C1_NZ}x{C1_NX} (runtime {C1_RT[0]}x{C1_RT[1]}), 1 shot, nt {C1_NT}, "
-                            f"order 8, CPML {C1_ABCN}, fwd+adj gradient, boundary saving",
+                            f"order {ORDER}, CPML {C1_ABCN}, fwd+adj gradient, boundary saving",
                 "grid": [C1_NZ, C1_NX], "runtime_grid": list(C1_RT), "shots_per_gpu": 1, "nt": C1_NT,
                 "dh": C1_DH, "dt": C1_DT, "abcn": C1_ABCN, "order": ORDER,
                 "cells_counted": "runtime grid (physical + PML + halo) x shots x nt",
@@ -420,7 +420,7 @@ class Acoustic3DWorkload:
 
     def config(self, args):
         return {"workload": f"acoustic3d {A3_N}^3 (runtime {A3_RT[0]}^3), {A3_NSHOT}-shot survey in calls of "
-                            f"{self.batch} shots, nt {self.nt}, order 8, CPML {A3_ABCN}, fwd+adj gradient, "
+                            f"{self.batch} shots, nt {self.nt}, order {ORDER}, CPML {A3_ABCN}, fwd+adj gradient, "
                             f"boundary saving",
                 "grid": [A3_N] * 3, "runtime_grid": list(A3_RT), "shots_per_gpu": A3_NSHOT,
                 "shots_per_call": self.batch, "nt": self.nt, "dh": A3_DH, "dt": A3_DT, "abcn": A3_ABCN,
@@ -686,7 +686,7 @@ def run_gpu(args, wl):
 
     from sweep_b200.distributed import sharded_gradient
     solver, m_true, m_init, w, src, rec = wl.build(dev)
-    solver.autotune = bool(args.autotune) and getattr(wl, "tunable", True)
+    solver.autotune = bool(args.autotune) and getattr(wl, "tunable", True) and ORDER == 8
     src, rec = src[:wl.nshot], rec[:wl.nshot]
     if getattr(wl, "budget_gb", None) and not args.shots_per_call:
         # shot groups: the most shots whose boundary-saving tape fits the budget
@@ -963,6 +963,9 @@ def main():
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="skip the launch-schedule autotuner (by default the first call of the workload's "
                          "shape tunes its schedule, before and outside the timed region)")
+    ap.add_argument("--order", type=int, default=8,
+                    help="spatial order of the acoustic workloads: 8 runs the tiled kernels, the other even "
+                         "orders 2-14 the any-order ones (the elastic workloads run order 8 only)")
     ap.add_argument("--nt", type=int, default=None,
                     help="shorter time axis (profiling captures only; the bench line is for the full nt)")
     ap.add_argument("--shots", type=int, default=None,
@@ -976,7 +979,14 @@ def main():
     if args.workload == "fwi":
         run_fwi(args)
         return
+    global ORDER
+    ORDER = int(args.order)
     wl = WORKLOADS[args.workload]()
+    if ORDER != 8:
+        # the any-order kernels: one reverse step is adj + recon + strip kernels
+        wl.kernel = (f"sweep::aord reverse step at order {ORDER} (adj{2 if wl.name != 'acoustic3d' else 3} + "
+                     "recon + strip kernels)")
+        wl.traffic = None
     if args.nt:
         wl.nt = int(args.nt)
         global NT, E_NT, A3_NT, E3_NT

@@ -4,6 +4,7 @@
 #include "acoustic2d.cuh"
 #include "elastic2d.cuh"
 #include "elastic3d.cuh"
+#include "acoustic_orders.cuh"
 
 namespace sweep {
 namespace a3d {
@@ -25,7 +26,8 @@ extern "C" int sweep_b200_acoustic_sizes(const sweep_acoustic_desc* d, int32_t m
     return guarded(err, err_cap, [&] {
         SWEEP_REQUIRE(d && workspace_bytes && tape_bytes, "null argument");
         SWEEP_REQUIRE(d->ndim == 2 || d->ndim == 3, "acoustic: ndim %d is not built", d->ndim);
-        if (d->ndim == 2) a2d::sizes(d, mem_mode, ckpt_every, workspace_bytes, tape_bytes);
+        if (d->M != 4) aord::sizes(d, mem_mode, ckpt_every, workspace_bytes, tape_bytes);
+        else if (d->ndim == 2) a2d::sizes(d, mem_mode, ckpt_every, workspace_bytes, tape_bytes);
         else a3d::sizes(d, mem_mode, ckpt_every, workspace_bytes, tape_bytes);
     });
 }
@@ -37,7 +39,10 @@ extern "C" int sweep_b200_acoustic_forward(const sweep_acoustic_desc* d, int32_t
     return guarded(err, err_cap, [&] {
         SWEEP_REQUIRE(d != nullptr, "null descriptor");
         SWEEP_REQUIRE(d->ndim == 2 || d->ndim == 3, "acoustic: ndim %d is not built", d->ndim);
-        if (d->ndim == 2)
+        if (d->M != 4)
+            aord::forward(d, mem_mode, ckpt_every, record, tape, workspace, workspace_bytes,
+                          static_cast<cudaStream_t>(stream));
+        else if (d->ndim == 2)
             a2d::forward(d, mem_mode, ckpt_every, record, tape, workspace, workspace_bytes,
                          static_cast<cudaStream_t>(stream));
         else
@@ -55,7 +60,10 @@ extern "C" int sweep_b200_acoustic_backward(const sweep_acoustic_desc* d, int32_
     return guarded(err, err_cap, [&] {
         SWEEP_REQUIRE(d != nullptr, "null descriptor");
         SWEEP_REQUIRE(d->ndim == 2 || d->ndim == 3, "acoustic: ndim %d is not built", d->ndim);
-        if (d->ndim == 2)
+        if (d->M != 4)
+            aord::backward(d, mem_mode, ckpt_every, adj, tape, grad_vp, grad_wavelet, illum_src, illum_rec,
+                           workspace, workspace_bytes, static_cast<cudaStream_t>(stream));
+        else if (d->ndim == 2)
             a2d::backward(d, mem_mode, ckpt_every, adj, tape, grad_vp, grad_wavelet, illum_src, illum_rec,
                           workspace, workspace_bytes, static_cast<cudaStream_t>(stream));
         else

@@ -404,6 +404,12 @@ class PropTorch(torch.nn.Module):
         self.equation = equation
         self.impl = "c"
         nd = equation.NDIM
+        if isinstance(equation, (Acoustic, Acoustic3D)) and equation.M > 7:
+            raise NotImplementedError(f"sweep_b200: acoustic spatial orders 2 to 14 are built "
+                                      f"(got {equation.spatial_order})")
+        if isinstance(equation, Elastic) and equation.M != 4:
+            raise NotImplementedError(f"sweep_b200: {type(equation).__name__} is built at spatial_order=8 only "
+                                      f"(got {equation.spatial_order}); pass spatial_order=8")
         if len(shape) != nd:
             raise ValueError(f"{type(equation).__name__} needs a {nd}-D shape, got {shape}")
         self.shape = tuple(int(s) for s in shape)

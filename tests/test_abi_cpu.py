@@ -56,10 +56,17 @@ def test_sizes_query_is_host_only():
 
 def test_errors_come_back_as_messages():
     from sweep_b200 import _lib
-    d = _desc(M=3)
+    d = _desc(M=8)
     ws, tape = _lib.c_i64(), _lib.c_i64()
-    with pytest.raises(RuntimeError, match="order 8"):
+    with pytest.raises(RuntimeError, match="orders 2 to 14"):
         _lib.call("sweep_b200_acoustic_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
+    d = _desc(M=3)                              # order 6: the any-order kernels, boundary saving only
+    _lib.call("sweep_b200_acoustic_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
+    px, pz = 60 - 2 * 8, 40 - 2 * 8
+    assert tape.value == (10 * 2 * (px * pz - (px - 8) * (pz - 8)) + 2 * 2 * 40 * 60) * 4
+    for mode in (_lib.MEM_CHECKPOINT, _lib.MEM_BOUNDARY_INT8, _lib.MEM_BOUNDARY | _lib.MEM_HOST_TAPE):
+        with pytest.raises(RuntimeError, match="boundary saving with fp32 strips"):
+            _lib.call("sweep_b200_acoustic_sizes", d, mode, 10, ws, tape)
     d = _desc()
     d.pad[0] = d.pad[5] = 0                    # free-surface faces (2-D: any)
     _lib.call("sweep_b200_acoustic_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
@@ -75,6 +82,21 @@ def test_errors_come_back_as_messages():
         _lib.call("sweep_b200_acoustic_sizes", d3, _lib.MEM_BOUNDARY, 0, ws, tape)
     with pytest.raises(RuntimeError, match="null"):
         _lib.call("sweep_b200_acoustic_sizes", None, _lib.MEM_BOUNDARY, 0, ws, tape)
+
+
+def test_spatial_orders_on_the_host():
+    """Acoustic orders 2 to 14 are accepted (order 8 on the tiled kernels, the
+    others on the any-order ones); higher acoustic orders and elastic orders
+    other than 8 are refused when the solver is built."""
+    from sweep_b200 import Acoustic, Acoustic3D, Elastic, Elastic3D, PropTorch
+    for order in (2, 4, 6, 8, 10, 14):
+        PropTorch(Acoustic(spatial_order=order), shape=(20, 20), abcn=5, device="cpu")
+        PropTorch(Acoustic3D(spatial_order=order), shape=(12, 12, 12), abcn=4, device="cpu")
+    with pytest.raises(NotImplementedError, match="orders 2 to 14"):
+        PropTorch(Acoustic(spatial_order=16), shape=(20, 20), abcn=5, device="cpu")
+    for eq in (Elastic, Elastic3D):
+        with pytest.raises(NotImplementedError, match="spatial_order=8"):
+            PropTorch(eq(), shape=(20, 20) if eq is Elastic else (12, 12, 12), abcn=5, device="cpu")
 
 
 def test_propagator_refuses_cpu_and_other_impls():
