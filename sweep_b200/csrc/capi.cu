@@ -5,6 +5,7 @@
 #include "elastic2d.cuh"
 #include "elastic3d.cuh"
 #include "acoustic_orders.cuh"
+#include "elastic_orders.cuh"
 
 namespace sweep {
 namespace a3d {
@@ -77,7 +78,8 @@ extern "C" int sweep_b200_elastic_sizes(const sweep_elastic_desc* d, int32_t mem
 {
     return guarded(err, err_cap, [&] {
         SWEEP_REQUIRE(d && workspace_bytes && tape_bytes, "null argument");
-        el2d::sizes(d, mem_mode, ckpt_every, workspace_bytes, tape_bytes);
+        if (d->M != 4) eord::sizes(d, mem_mode, ckpt_every, workspace_bytes, tape_bytes);
+        else el2d::sizes(d, mem_mode, ckpt_every, workspace_bytes, tape_bytes);
     });
 }
 
@@ -87,8 +89,12 @@ extern "C" int sweep_b200_elastic_forward(const sweep_elastic_desc* d, int32_t m
 {
     return guarded(err, err_cap, [&] {
         SWEEP_REQUIRE(d != nullptr, "null descriptor");
-        el2d::forward(d, mem_mode, ckpt_every, record, tape, workspace, workspace_bytes,
-                      static_cast<cudaStream_t>(stream));
+        if (d->M != 4)
+            eord::forward(d, mem_mode, ckpt_every, record, tape, workspace, workspace_bytes,
+                          static_cast<cudaStream_t>(stream));
+        else
+            el2d::forward(d, mem_mode, ckpt_every, record, tape, workspace, workspace_bytes,
+                          static_cast<cudaStream_t>(stream));
     });
 }
 
@@ -99,8 +105,12 @@ extern "C" int sweep_b200_elastic_backward(const sweep_elastic_desc* d, int32_t 
 {
     return guarded(err, err_cap, [&] {
         SWEEP_REQUIRE(d != nullptr, "null descriptor");
-        el2d::backward(d, mem_mode, ckpt_every, adj, tape, grad_vp, grad_vs, grad_rho, workspace,
-                       workspace_bytes, static_cast<cudaStream_t>(stream));
+        if (d->M != 4)
+            eord::backward(d, mem_mode, ckpt_every, adj, tape, grad_vp, grad_vs, grad_rho, workspace,
+                           workspace_bytes, static_cast<cudaStream_t>(stream));
+        else
+            el2d::backward(d, mem_mode, ckpt_every, adj, tape, grad_vp, grad_vs, grad_rho, workspace,
+                           workspace_bytes, static_cast<cudaStream_t>(stream));
     });
 }
 

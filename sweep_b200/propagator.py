@@ -404,12 +404,12 @@ class PropTorch(torch.nn.Module):
         self.equation = equation
         self.impl = "c"
         nd = equation.NDIM
-        if isinstance(equation, (Acoustic, Acoustic3D)) and equation.M > 7:
-            raise NotImplementedError(f"sweep_b200: acoustic spatial orders 2 to 14 are built "
-                                      f"(got {equation.spatial_order})")
-        if isinstance(equation, Elastic) and equation.M != 4:
-            raise NotImplementedError(f"sweep_b200: {type(equation).__name__} is built at spatial_order=8 only "
-                                      f"(got {equation.spatial_order}); pass spatial_order=8")
+        if isinstance(equation, Elastic3D):
+            if equation.M != 4:
+                raise NotImplementedError(f"sweep_b200: Elastic3D is built at spatial_order=8 only "
+                                          f"(got {equation.spatial_order}); pass spatial_order=8")
+        elif equation.M > 7:
+            raise NotImplementedError(f"sweep_b200: spatial orders 2 to 14 are built (got {equation.spatial_order})")
         if len(shape) != nd:
             raise ValueError(f"{type(equation).__name__} needs a {nd}-D shape, got {shape}")
         self.shape = tuple(int(s) for s in shape)
@@ -564,6 +564,8 @@ class PropTorch(torch.nn.Module):
         desc = self._desc(geo, padded, wb, fields)
         if isinstance(desc, _lib.Elastic3DDesc):
             return {"fixed": "one thread per cell, 32 x 8 cell tiles per z plane and shot"}
+        if desc.M != 4:
+            return {"fixed": f"order {2 * desc.M}: one thread per cell, 32 x 8 cell tiles per plane and shot"}
         return autotune.get_schedule(desc)
 
     def tape_bytes(self, wavelet_len, sources, receivers, models):
@@ -641,8 +643,9 @@ class PropTorch(torch.nn.Module):
         mem_mode, ckpt_every = self._mem_mode()
         padded = [self._pad_model(m.to(dev)) for m in models]
         fields = self._elastic_fields() if isinstance(eq, Elastic) else None
-        if (self.autotune or self.schedule is not None) and isinstance(eq, Elastic3D):
-            raise NotImplementedError("sweep_b200: Elastic3D has one built-in launch schedule (no autotune)")
+        if (self.autotune or self.schedule is not None) and (isinstance(eq, Elastic3D) or eq.M != 4):
+            raise NotImplementedError(f"sweep_b200: {type(eq).__name__} at spatial_order={eq.spatial_order} has one "
+                                      f"built-in launch schedule (no autotune)")
         if self.autotune or self.schedule is not None:
             self._apply_schedule(geo, padded, wb, fields, mem_mode, ckpt_every)
         mem_mode, ckpt_every = self._apply_budget(geo, padded, wb, fields, mem_mode, ckpt_every)

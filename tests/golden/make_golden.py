@@ -822,6 +822,40 @@ def acoustic_orders():
     np.savez_compressed(OUT / "acoustic_orders.npz", **out)
 
 
+def elastic_orders():
+    """2-D isotropic elastic at spatial orders 2, 4 and 6 (the reference's
+    Elastic defaults to order 4): 2 explosive shots on a 40 x 56 layered model
+    (CPML 10), (vx, vz) receivers, vp/vs/rho gradients; order 4 once more with
+    a traction-free top face, a shot on the surface row and (vx, vz, sxx)
+    receivers on it and below it."""
+    rng = np.random.default_rng(223)
+    nz, nx, nt, dt, dh, abcn = 40, 56, 300, 0.0005, 5.0, 10
+    vp_true = _layered(nz, nx, rng, 1800.0, 3200.0, 4)
+    vs_true = (vp_true / 1.73).astype(np.float32)
+    rho_true = (310.0 * vp_true ** 0.25).astype(np.float32)
+    vp_init = np.full((nz, nx), 2200.0, np.float32)
+    vs_init = (vp_init / 1.73).astype(np.float32)
+    rho_init = (310.0 * vp_init ** 0.25).astype(np.float32)
+    w = _wavelet(nt, dt, 25.0, 0.04)
+    src = np.array([[14, 6], [40, 0]], np.int64)                 # shot 1 on the surface row
+    rec = np.zeros((2, 8, 2), np.int64)
+    for b in range(2):
+        rec[b, :, 0] = np.linspace(3, nx - 4, 8).astype(np.int64)
+        rec[b, :, 1] = 2 * b
+    out = dict(nz=nz, nx=nx, nt=nt, dt=dt, dh=dh, abcn=abcn, vp_true=vp_true, vs_true=vs_true, rho_true=rho_true,
+               vp_init=vp_init, vs_init=vs_init, rho_init=rho_init, wavelet=w, src=src, rec=rec)
+    runs = [(f"o{o}", o, {}) for o in (2, 4, 6)]
+    runs.append(("o4_fs", 4, dict(free_surface=True, receiver_type=["vx", "vz", "sxx"])))
+    for tag, order, kw in runs:
+        solver = PropTorch(Elastic(spatial_order=order, device="cpu"), shape=(nz, nx), dh=dh, dt=dt, abcn=abcn,
+                           impl="c", device="cpu", memory=BoundarySaving(), **kw)
+        obs = _forward(solver, w, src, rec, [vp_true, vs_true, rho_true])
+        r = _run(solver, w, src, rec, [vp_init, vs_init, rho_init], obs, False)
+        out.update({f"obs_{tag}": obs, f"pred_{tag}": r["pred"], f"grad_vp_{tag}": r["grad0"],
+                    f"grad_vs_{tag}": r["grad1"], f"grad_rho_{tag}": r["grad2"]})
+    np.savez_compressed(OUT / "elastic_orders.npz", **out)
+
+
 def elastic3d_storage():
     """3-D elastic boundary saving with fp16 / bf16 / int8 strips (reference
     Elastic3D, BoundarySaving(storage_dtype=...): each of the nine fields
@@ -885,6 +919,7 @@ CASES = {
     "elastic3d_free_surface": elastic3d_free_surface,
     "elastic3d_storage": elastic3d_storage,
     "acoustic_orders": acoustic_orders,
+    "elastic_orders": elastic_orders,
 }
 
 if __name__ == "__main__":

@@ -85,18 +85,30 @@ def test_errors_come_back_as_messages():
 
 
 def test_spatial_orders_on_the_host():
-    """Acoustic orders 2 to 14 are accepted (order 8 on the tiled kernels, the
-    others on the any-order ones); higher acoustic orders and elastic orders
-    other than 8 are refused when the solver is built."""
-    from sweep_b200 import Acoustic, Acoustic3D, Elastic, Elastic3D, PropTorch
+    """Orders 2 to 14 are accepted for Acoustic, Acoustic3D and Elastic (order
+    8 on the tiled kernels, the others on the any-order ones); higher orders,
+    and Elastic3D at any order but 8, are refused when the solver is built;
+    the elastic core sizes an order-4 problem and refuses its checkpoints."""
+    import torch
+    from sweep_b200 import Acoustic, Acoustic3D, Elastic, Elastic3D, PropTorch, _lib
     for order in (2, 4, 6, 8, 10, 14):
         PropTorch(Acoustic(spatial_order=order), shape=(20, 20), abcn=5, device="cpu")
         PropTorch(Acoustic3D(spatial_order=order), shape=(12, 12, 12), abcn=4, device="cpu")
-    with pytest.raises(NotImplementedError, match="orders 2 to 14"):
-        PropTorch(Acoustic(spatial_order=16), shape=(20, 20), abcn=5, device="cpu")
-    for eq in (Elastic, Elastic3D):
-        with pytest.raises(NotImplementedError, match="spatial_order=8"):
-            PropTorch(eq(), shape=(20, 20) if eq is Elastic else (12, 12, 12), abcn=5, device="cpu")
+        PropTorch(Elastic(spatial_order=order), shape=(20, 20), abcn=5, device="cpu")
+    for eq in (Acoustic, Elastic):
+        with pytest.raises(NotImplementedError, match="orders 2 to 14"):
+            PropTorch(eq(spatial_order=16), shape=(20, 20), abcn=5, device="cpu")
+    with pytest.raises(NotImplementedError, match="spatial_order=8"):
+        PropTorch(Elastic3D(), shape=(12, 12, 12), abcn=5, device="cpu")
+    s = PropTorch(Elastic(), shape=(30, 40), dh=5.0, dt=5e-4, abcn=6, device="cpu")
+    geo, padded, wb, fields = s._probe(50, np.array([[8, 6]]), np.zeros((1, 4, 2), np.int64), [torch.ones(30, 40)] * 3)
+    d = s._desc(geo, padded, wb, fields)
+    assert d.M == 2
+    ws, tape = _lib.c_i64(), _lib.c_i64()
+    _lib.call("sweep_b200_elastic_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
+    assert tape.value > 50 * 5 * 4 and ws.value > 0
+    with pytest.raises(RuntimeError, match="boundary saving with fp32 strips"):
+        _lib.call("sweep_b200_elastic_sizes", d, _lib.MEM_CHECKPOINT, 10, ws, tape)
 
 
 def test_propagator_refuses_cpu_and_other_impls():
@@ -142,8 +154,13 @@ def test_elastic_sizes_and_errors():
     d.nsrc_fields, d.src_fields[0], d.src_fields[1] = 2, 3, 3
     with pytest.raises(RuntimeError, match="repeated"):
         _lib.call("sweep_b200_elastic_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
-    d = _edesc(M=2)
-    with pytest.raises(RuntimeError, match="order 8"):
+    d = _edesc(M=8)
+    with pytest.raises(RuntimeError, match="orders 2 to 14"):
+        _lib.call("sweep_b200_elastic_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
+    d = _edesc(M=2)                                   # order 4: the any-order kernels
+    _lib.call("sweep_b200_elastic_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
+    d.nsrc_fields, d.src_fields[0], d.src_fields[1] = 2, 3, 3
+    with pytest.raises(RuntimeError, match="repeated"):
         _lib.call("sweep_b200_elastic_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
 
 

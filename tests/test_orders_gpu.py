@@ -115,3 +115,76 @@ def test_other_memory_modes_are_refused_at_order_4():
         vp = torch.tensor(d["vp_init"], device=DEV, requires_grad=True)
         with pytest.raises(RuntimeError, match="boundary saving with fp32 strips"):
             s(torch.tensor(d["wavelet"], device=DEV), d["src"], d["rec"], models=[vp]).sum().backward()
+
+
+# ------------------------------------------------------------------ elastic
+@pytest.mark.parametrize("tag,order,kw", [("o2", 2, {}), ("o4", 4, {}), ("o6", 6, {}),
+                                          ("o4_fs", 4, dict(free_surface=True, receiver_type=["vx", "vz", "sxx"]))])
+def test_elastic_orders_match_reference(tag, order, kw):
+    """2-D elastic at orders 2, 4, 6 and at order 4 with a traction-free top
+    face (a shot and receivers on the surface row) against the reference."""
+    from sweep_b200 import Elastic, PropTorch
+    d = load("elastic_orders")
+    s = PropTorch(Elastic(spatial_order=order, device=DEV), shape=tuple(d["vp_true"].shape), dh=float(d["dh"]),
+                  dt=float(d["dt"]), abcn=int(d["abcn"]), device=DEV, **kw)
+    with torch.no_grad():
+        obs = s(torch.tensor(d["wavelet"], device=DEV), d["src"], d["rec"],
+                models=[torch.tensor(d[f"{n}_true"], device=DEV) for n in ("vp", "vs", "rho")]).cpu().numpy()
+    assert rel(obs, d[f"obs_{tag}"]) < REC_TOL
+    ms = [torch.tensor(d[f"{n}_init"], device=DEV, requires_grad=True) for n in ("vp", "vs", "rho")]
+    pred = s(torch.tensor(d["wavelet"], device=DEV), d["src"], d["rec"], models=ms)
+    (0.5 * ((pred - torch.tensor(d[f"obs_{tag}"], device=DEV)) ** 2).sum()).backward()
+    torch.cuda.synchronize()
+    pred = pred.detach().cpu().numpy()
+    errs = [rel(m.grad.cpu().numpy(), d[f"grad_{n}_{tag}"]) for m, n in zip(ms, ("vp", "vs", "rho"))]
+    print(f"elastic {tag}: record {rel(pred, d[f'pred_{tag}']):.2e}, vp / vs / rho "
+          + " / ".join(f"{e:.2e}" for e in errs))
+    assert rel(pred, d[f"pred_{tag}"]) < REC_TOL
+    assert max(errs) < GRAD_TOL
+
+
+def test_elastic_order4_per_shot_body_force_matches_oracle():
+    """Order 4, per-shot models, body-force sources on (vx, vz), (vx, vz,
+    szz) receivers, against the float32 oracle (float64 printed)."""
+    from sweep_b200 import Elastic, PropTorch
+    rng = np.random.default_rng(41)
+    nz, nx, nt, dt, dh, abcn, B = 34, 48, 220, 0.0005, 5.0, 8, 2
+    vp = np.stack([_layered(nz, nx, rng) + 600.0 for _ in range(B)]).astype(np.float32)
+    vs, rho = (vp / 1.8).astype(np.float32), (310.0 * vp ** 0.25).astype(np.float32)
+    v0 = np.full_like(vp, 2300.0)
+    v0s, r0 = (v0 / 1.8).astype(np.float32), (310.0 * v0 ** 0.25).astype(np.float32)
+    w = np.stack([np.sin(np.arange(nt) * dt * 2 * np.pi * f) * np.exp(-((np.arange(nt) * dt - 0.03) / 0.012) ** 2)
+                  for f in (20.0, 26.0)]).astype(np.float32)
+    src = np.array([[12, 8], [30, 14]], np.int64)
+    rec = np.zeros((B, 6, 2), np.int64)
+    for b in range(B):
+        rec[b, :, 0] = np.linspace(2, nx - 3, 6).astype(np.int64)
+        rec[b, :, 1] = 3 + 2 * b
+    kw = dict(source_fields=("vx", "vz"), receiver_fields=("vx", "vz", "szz"))
+    obs = O.elastic_forward(vp, vs, rho, w, src, rec, dh, dt, abcn, order=4, **kw)
+    s = PropTorch(Elastic(spatial_order=4, device=DEV), shape=(nz, nx), dh=dh, dt=dt, abcn=abcn, device=DEV,
+                  source_type=["vx", "vz"], receiver_type=["vx", "vz", "szz"])
+    ms = [torch.tensor(m, device=DEV, requires_grad=True) for m in (v0, v0s, r0)]
+    pred = s(torch.tensor(w, device=DEV), src, rec, models=ms)
+    (0.5 * ((pred - torch.tensor(obs, device=DEV)) ** 2).sum()).backward()
+    torch.cuda.synchronize()
+    pred = pred.detach().cpu().numpy()
+    for prec in ("f32", "f64"):
+        po, _, go = O.elastic_gradient(v0, v0s, r0, w, src, rec, obs, dh, dt, abcn, order=4, prec=prec, **kw)
+        errs = [rel(m.grad.cpu().numpy(), g) for m, g in zip(ms, go)]
+        print(f"elastic order 4 per-shot body force vs {prec} oracle: record {rel(pred, po):.2e}, vp / vs / rho "
+              + " / ".join(f"{e:.2e}" for e in errs))
+        if prec == "f32":
+            assert rel(pred, po) < REC_TOL
+            assert max(errs) < GRAD_TOL
+
+
+def test_elastic_other_memory_modes_are_refused_at_order_4():
+    from sweep_b200 import BoundarySaving, Ckpt, Elastic, PropTorch
+    d = load("elastic_orders")
+    for memory in (Ckpt(chunks=50), BoundarySaving(storage_dtype="int8")):
+        s = PropTorch(Elastic(spatial_order=4, device=DEV), shape=tuple(d["vp_true"].shape), dh=float(d["dh"]),
+                      dt=float(d["dt"]), abcn=int(d["abcn"]), device=DEV, memory=memory)
+        ms = [torch.tensor(d[f"{n}_init"], device=DEV, requires_grad=True) for n in ("vp", "vs", "rho")]
+        with pytest.raises(RuntimeError, match="boundary saving with fp32 strips"):
+            s(torch.tensor(d["wavelet"], device=DEV), d["src"], d["rec"], models=ms).sum().backward()
