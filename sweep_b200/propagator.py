@@ -405,9 +405,9 @@ class PropTorch(torch.nn.Module):
         self.impl = "c"
         nd = equation.NDIM
         if isinstance(equation, Elastic3D):
-            if equation.M != 4:
-                raise NotImplementedError(f"sweep_b200: Elastic3D is built at spatial_order=8 only "
-                                          f"(got {equation.spatial_order}); pass spatial_order=8")
+            if equation.M > 4:
+                raise NotImplementedError(f"sweep_b200: Elastic3D is built at spatial orders 2, 4, 6 and 8 "
+                                          f"(got {equation.spatial_order})")
         elif equation.M > 7:
             raise NotImplementedError(f"sweep_b200: spatial orders 2 to 14 are built (got {equation.spatial_order})")
         if len(shape) != nd:

@@ -856,6 +856,42 @@ def elastic_orders():
     np.savez_compressed(OUT / "elastic_orders.npz", **out)
 
 
+def elastic3d_orders():
+    """3-D isotropic elastic at spatial orders 2, 4 and 6 (the reference's
+    Elastic3D defaults to order 4): 2 explosive shots on an 18 x 20 x 22
+    layered model (CPML 6), (vx, vy, vz) receivers, vp/vs/rho gradients;
+    order 4 once more with a traction-free top face and a shot on it."""
+    from sweep.equations import Elastic3D
+    rng = np.random.default_rng(227)
+    nz, ny, nx, nt, dt, dh, abcn = 18, 20, 22, 140, 0.0005, 5.0, 6
+    base = _layered(nz, nx, rng, 1900.0, 3000.0, 3)
+    vp_true = np.ascontiguousarray(np.repeat(base[:, None, :], ny, axis=1)
+                                   * (1 + 0.02 * np.sin(np.arange(ny) / 3.0))[None, :, None]).astype(np.float32)
+    vs_true = (vp_true / 1.73).astype(np.float32)
+    rho_true = (310.0 * vp_true ** 0.25).astype(np.float32)
+    vp_init = np.full((nz, ny, nx), 2300.0, np.float32)
+    vs_init = (vp_init / 1.73).astype(np.float32)
+    rho_init = (310.0 * vp_init ** 0.25).astype(np.float32)
+    w = _wavelet(nt, dt, 30.0, 0.03)
+    src = np.array([[8, 9, 5], [14, 11, 0]], np.int64)              # (x, y, z); shot 1 on the top row
+    rec = np.zeros((2, 10, 3), np.int64)
+    for b in range(2):
+        rec[b, :, 0] = np.linspace(1, nx - 2, 10).astype(np.int64)
+        rec[b, :, 1] = np.linspace(2, ny - 3, 10).astype(np.int64)
+        rec[b, :, 2] = 2 * b
+    out = dict(nz=nz, ny=ny, nx=nx, nt=nt, dt=dt, dh=dh, abcn=abcn, vp_true=vp_true, vs_true=vs_true,
+               rho_true=rho_true, vp_init=vp_init, vs_init=vs_init, rho_init=rho_init, wavelet=w, src=src, rec=rec)
+    runs = [(f"o{o}", o, {}) for o in (2, 4, 6)] + [("o4_fs", 4, dict(free_surface=True))]
+    for tag, order, kw in runs:
+        solver = PropTorch(Elastic3D(spatial_order=order, device="cpu"), shape=(nz, ny, nx), dh=dh, dt=dt,
+                           abcn=abcn, impl="c", device="cpu", memory=BoundarySaving(), **kw)
+        obs = _forward(solver, w, src, rec, [vp_true, vs_true, rho_true])
+        r = _run(solver, w, src, rec, [vp_init, vs_init, rho_init], obs, False)
+        out.update({f"obs_{tag}": obs, f"pred_{tag}": r["pred"], f"grad_vp_{tag}": r["grad0"],
+                    f"grad_vs_{tag}": r["grad1"], f"grad_rho_{tag}": r["grad2"]})
+    np.savez_compressed(OUT / "elastic3d_orders.npz", **out)
+
+
 def elastic3d_storage():
     """3-D elastic boundary saving with fp16 / bf16 / int8 strips (reference
     Elastic3D, BoundarySaving(storage_dtype=...): each of the nine fields
@@ -920,6 +956,7 @@ CASES = {
     "elastic3d_storage": elastic3d_storage,
     "acoustic_orders": acoustic_orders,
     "elastic_orders": elastic_orders,
+    "elastic3d_orders": elastic3d_orders,
 }
 
 if __name__ == "__main__":

@@ -86,9 +86,9 @@ def test_errors_come_back_as_messages():
 
 def test_spatial_orders_on_the_host():
     """Orders 2 to 14 are accepted for Acoustic, Acoustic3D and Elastic (order
-    8 on the tiled kernels, the others on the any-order ones); higher orders,
-    and Elastic3D at any order but 8, are refused when the solver is built;
-    the elastic core sizes an order-4 problem and refuses its checkpoints."""
+    8 on the tiled kernels, the others on the any-order ones) and 2 to 8 for
+    Elastic3D; higher orders are refused when the solver is built; the
+    elastic core sizes an order-4 problem and refuses its checkpoints."""
     import torch
     from sweep_b200 import Acoustic, Acoustic3D, Elastic, Elastic3D, PropTorch, _lib
     for order in (2, 4, 6, 8, 10, 14):
@@ -98,8 +98,10 @@ def test_spatial_orders_on_the_host():
     for eq in (Acoustic, Elastic):
         with pytest.raises(NotImplementedError, match="orders 2 to 14"):
             PropTorch(eq(spatial_order=16), shape=(20, 20), abcn=5, device="cpu")
-    with pytest.raises(NotImplementedError, match="spatial_order=8"):
-        PropTorch(Elastic3D(), shape=(12, 12, 12), abcn=5, device="cpu")
+    for order in (2, 4, 6, 8):
+        PropTorch(Elastic3D(spatial_order=order), shape=(12, 12, 12), abcn=5, device="cpu")
+    with pytest.raises(NotImplementedError, match="orders 2, 4, 6 and 8"):
+        PropTorch(Elastic3D(spatial_order=10), shape=(12, 12, 12), abcn=5, device="cpu")
     s = PropTorch(Elastic(), shape=(30, 40), dh=5.0, dt=5e-4, abcn=6, device="cpu")
     geo, padded, wb, fields = s._probe(50, np.array([[8, 6]]), np.zeros((1, 4, 2), np.int64), [torch.ones(30, 40)] * 3)
     d = s._desc(geo, padded, wb, fields)
@@ -445,6 +447,11 @@ def test_elastic3d_sizes_and_refusals():
                              (_lib.MEM_CHECKPOINT, 0, "interval"), (_lib.MEM_RECURSIVE, 0, "budget")):
         with pytest.raises(RuntimeError, match=msg):
             _lib.call("sweep_b200_elastic3d_sizes", d, mode, every, ws, tape)
+    d.M = 2                                            # order 4: the same sizes rule, its own strips
+    _lib.call("sweep_b200_elastic3d_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
+    d.M = 5
+    with pytest.raises(RuntimeError, match="orders 2, 4, 6 and 8"):
+        _lib.call("sweep_b200_elastic3d_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
     fs = PropTorch(eq, shape=(20, 22, 24), dh=5.0, dt=0.0005, abcn=6, device="cpu", free_surface=True)
     assert fs.pads == [0, 6, 6, 6, 6, 6]
     geo, padded, wb, fields = fs._probe(50, src, rec, [torch.ones(20, 22, 24)] * 3)

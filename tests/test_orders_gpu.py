@@ -188,3 +188,24 @@ def test_elastic_other_memory_modes_are_refused_at_order_4():
         ms = [torch.tensor(d[f"{n}_init"], device=DEV, requires_grad=True) for n in ("vp", "vs", "rho")]
         with pytest.raises(RuntimeError, match="boundary saving with fp32 strips"):
             s(torch.tensor(d["wavelet"], device=DEV), d["src"], d["rec"], models=ms).sum().backward()
+
+
+@pytest.mark.parametrize("tag,order,kw", [("o2", 2, {}), ("o4", 4, {}), ("o6", 6, {}),
+                                          ("o4_fs", 4, dict(free_surface=True))])
+def test_elastic3d_orders_match_reference(tag, order, kw):
+    """3-D elastic at orders 2, 4, 6 and at order 4 with a traction-free top
+    face (a shot on the surface row) against the reference."""
+    from sweep_b200 import Elastic3D, PropTorch
+    d = load("elastic3d_orders")
+    s = PropTorch(Elastic3D(spatial_order=order, device=DEV), shape=tuple(d["vp_true"].shape), dh=float(d["dh"]),
+                  dt=float(d["dt"]), abcn=int(d["abcn"]), device=DEV, **kw)
+    ms = [torch.tensor(d[f"{n}_init"], device=DEV, requires_grad=True) for n in ("vp", "vs", "rho")]
+    pred = s(torch.tensor(d["wavelet"], device=DEV), d["src"], d["rec"], models=ms)
+    (0.5 * ((pred - torch.tensor(d[f"obs_{tag}"], device=DEV)) ** 2).sum()).backward()
+    torch.cuda.synchronize()
+    pred = pred.detach().cpu().numpy()
+    errs = [rel(m.grad.cpu().numpy(), d[f"grad_{n}_{tag}"]) for m, n in zip(ms, ("vp", "vs", "rho"))]
+    print(f"elastic3d {tag}: record {rel(pred, d[f'pred_{tag}']):.2e}, vp / vs / rho "
+          + " / ".join(f"{e:.2e}" for e in errs))
+    assert rel(pred, d[f"pred_{tag}"]) < REC_TOL
+    assert max(errs) < GRAD_TOL
