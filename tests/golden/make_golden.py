@@ -892,6 +892,45 @@ def elastic3d_orders():
     np.savez_compressed(OUT / "elastic3d_orders.npz", **out)
 
 
+def vti2d():
+    """First-order acoustic VTI (reference sweep.equations.AcousticVTI1st,
+    Duveneck et al. 2008; vx, vz, sH, sV on a staggered grid): 2 shots on a
+    40 x 56 layered model (CPML 10) with Thomsen epsilon / delta layers, the
+    default sources (sH, sV) and receivers (vz), vp / epsilon / delta / rho
+    gradients, boundary saving, at orders 8 and 4; at order 8 once more with
+    (vx, vz, sH) receivers and a second model set per shot."""
+    from sweep.equations.acoustic_vti_1st import AcousticVTI1st
+    rng = np.random.default_rng(229)
+    nz, nx, nt, dt, dh, abcn = 40, 56, 300, 0.0005, 5.0, 10
+    vp_true = _layered(nz, nx, rng, 1800.0, 3200.0, 4)
+    eps_true = (0.05 + 0.1 * (vp_true - 1800.0) / 1400.0).astype(np.float32)
+    dlt_true = (0.5 * eps_true).astype(np.float32)
+    rho_true = (310.0 * vp_true ** 0.25).astype(np.float32)
+    vp_init = np.full((nz, nx), 2300.0, np.float32)
+    eps_init = np.full((nz, nx), 0.1, np.float32)
+    dlt_init = np.full((nz, nx), 0.05, np.float32)
+    rho_init = (310.0 * vp_init ** 0.25).astype(np.float32)
+    w = _wavelet(nt, dt, 25.0, 0.04)
+    src = np.array([[14, 6], [40, 9]], np.int64)
+    rec = np.zeros((2, 8, 2), np.int64)
+    for b in range(2):
+        rec[b, :, 0] = np.linspace(3, nx - 4, 8).astype(np.int64)
+        rec[b, :, 1] = 3 + b
+    names = ("vp", "eps", "dlt", "rho")
+    true = [vp_true, eps_true, dlt_true, rho_true]
+    init = [vp_init, eps_init, dlt_init, rho_init]
+    out = dict(nz=nz, nx=nx, nt=nt, dt=dt, dh=dh, abcn=abcn, wavelet=w, src=src, rec=rec,
+               **{f"{n}_true": m for n, m in zip(names, true)}, **{f"{n}_init": m for n, m in zip(names, init)})
+    for tag, order, kw in (("o8", 8, {}), ("o4", 4, {}), ("o8_rec", 8, dict(receiver_type=["vx", "vz", "sH"]))):
+        solver = PropTorch(AcousticVTI1st(spatial_order=order, device="cpu"), shape=(nz, nx), dh=dh, dt=dt,
+                           abcn=abcn, impl="c", device="cpu", memory=BoundarySaving(), **kw)
+        obs = _forward(solver, w, src, rec, true)
+        r = _run(solver, w, src, rec, init, obs, False)
+        out.update({f"obs_{tag}": obs, f"pred_{tag}": r["pred"]})
+        out.update({f"grad_{n}_{tag}": r[f"grad{i}"] for i, n in enumerate(names)})
+    np.savez_compressed(OUT / "vti2d.npz", **out)
+
+
 def elastic3d_storage():
     """3-D elastic boundary saving with fp16 / bf16 / int8 strips (reference
     Elastic3D, BoundarySaving(storage_dtype=...): each of the nine fields
@@ -957,6 +996,7 @@ CASES = {
     "acoustic_orders": acoustic_orders,
     "elastic_orders": elastic_orders,
     "elastic3d_orders": elastic3d_orders,
+    "vti2d": vti2d,
 }
 
 if __name__ == "__main__":

@@ -365,3 +365,21 @@ def test_elastic3d_orders_oracle_matches_reference(tag, order, kw):
     assert rel(pred, d[f"pred_{tag}"]) < 1e-6
     for g, n in zip(grads, ("vp", "vs", "rho")):
         assert rel(g, d[f"grad_{n}_{tag}"]) < 1e-6
+
+
+@pytest.mark.parametrize("tag,order,kw", [("o8", 8, {}), ("o4", 4, {}),
+                                          ("o8_rec", 8, dict(receiver_fields=("vx", "vz", "sH")))])
+def test_vti2d_oracle_matches_reference(tag, order, kw):
+    """First-order acoustic VTI (AcousticVTI1st): records bit for bit in
+    float32, vp / epsilon / delta / rho gradients within 1e-6 of the
+    reference, at orders 8 and 4 and with stress receivers."""
+    d = np.load(GOLD / "vti2d.npz")
+    a = (float(d["dh"]), float(d["dt"]), int(d["abcn"]))
+    names = ("vp", "eps", "dlt", "rho")
+    obs = O.vti2d_forward(*[d[f"{n}_true"] for n in names], d["wavelet"], d["src"], d["rec"], *a, order=order, **kw)
+    assert np.array_equal(obs.astype(np.float32), d[f"obs_{tag}"])
+    pred, loss, grads = O.vti2d_gradient(*[d[f"{n}_init"] for n in names], d["wavelet"], d["src"], d["rec"],
+                                         d[f"obs_{tag}"], *a, order=order, **kw)
+    assert rel(pred, d[f"pred_{tag}"]) < 1e-6
+    for g, n in zip(grads, names):
+        assert rel(g, d[f"grad_{n}_{tag}"]) < 1e-6
