@@ -129,6 +129,26 @@ def elastic_survey(seed=SEED):
     return models[0], models[1], w, src, rec
 
 
+# Acoustic VTI workload (--workload vti2d): the elastic survey's grid, shots,
+# receivers and wavelet (400 x 1200, dh 5 m, dt 0.5 ms, nt 4000, CPML 40, 16
+# shots, vz receivers), vp the same layers, Thomsen epsilon 0.05-0.2 growing
+# with vp, delta = epsilon / 2, rho = 310 vp^0.25; sources on (sH, sV).
+# Algorithmic bytes per runtime cell-step (one read and one write of every
+# field a kernel touches; CPML memories and the models not counted): forward
+# velocity 6 floats + stress 6; reverse stress reconstruction 6, half-step A 4
+# + 6, gradient 8 + 8 slots, half-step B 4 + 6, velocity reconstruction 6.
+V_BYTES_FWD, V_BYTES_REV = 48, 192
+
+
+def vti_survey(seed=SEED):
+    (vp, _, rho), (vp0, _, rho0), w, src, rec = elastic_survey(seed)
+    out = []
+    for v, r in ((vp, rho), (vp0, rho0)):
+        eps = (0.05 + 0.15 * (v - 1800.0) / 2700.0).astype(np.float32)
+        out.append([v, eps, (0.5 * eps).astype(np.float32), r])
+    return out[0], out[1], w, src, rec
+
+
 # ------------------------------------------------------------------- clocks
 class ClockSampler:
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -357,6 +377,42 @@ class ElasticWorkload:
         return E_RT[0] * E_RT[1] * shots * nt_sample, time.perf_counter() - t0
 
 
+class VTIWorkload(ElasticWorkload):
+    name = "vti2d"
+    bytes_fwd, bytes_rev = V_BYTES_FWD, V_BYTES_REV
+    kernel = "sweep::vti reverse step (srev + premA + appA + grad + premB + appB + vrev + band restores)"
+    tunable = False
+
+    def config(self, args):
+        c = super().config(args)
+        c["workload"] = (f"vti2d (AcousticVTI1st) {E_NZ}x{E_NX} (runtime {E_RT[0]}x{E_RT[1]}), {E_NSHOT} shots, "
+                         f"nt {E_NT}, order {ORDER}, CPML {E_ABCN}, vp/epsilon/delta/rho fwd+adj gradient, "
+                         f"boundary saving")
+        return c
+
+    def survey_inputs(self):
+        return vti_survey()
+
+    def build(self, dev):
+        from sweep_b200 import AcousticVTI1st, PropTorch
+        m_true, m_init, w, src, rec = vti_survey()
+        solver = PropTorch(AcousticVTI1st(spatial_order=ORDER, device=dev), shape=(E_NZ, E_NX), dh=E_DH,
+                           dt=E_DT, abcn=E_ABCN, device=dev)
+        return solver, m_true, m_init, w, src, rec
+
+    def launches(self, group):
+        return 5 * self.nt + 11 * (self.nt - 1) + 6
+
+    def cpu_run(self, nt_sample, shots=1):
+        from oracle import oracle as O
+        m_true, m_init, w, src, rec = vti_survey()
+        w, src, rec = w[:nt_sample], src[:shots], rec[:shots]
+        obs = O.vti2d_forward(*m_true, w, src, rec, E_DH, E_DT, E_ABCN)
+        t0 = time.perf_counter()
+        O.vti2d_gradient(*m_init, w, src, rec, obs, E_DH, E_DT, E_ABCN)
+        return E_RT[0] * E_RT[1] * shots * nt_sample, time.perf_counter() - t0
+
+
 # 3-D workload (--workload acoustic3d, the default): 256^3, dh 10 m, dt 1 ms,
 # nt 2000, order 8, CPML 24; 8-layer dipping model (1500-4000 m/s) with a
 # +600 m/s Gaussian anomaly; 16 shots on a 4 x 4 surface grid, a 128 x 128
@@ -566,6 +622,7 @@ class Elastic3DWorkload:
 
 
 WORKLOADS = {"acoustic2d": AcousticWorkload, "acoustic2d_c1": AcousticC1Workload, "elastic2d": ElasticWorkload,
+             "vti2d": VTIWorkload,
              "acoustic3d": Acoustic3DWorkload, "elastic3d": Elastic3DWorkload}
 
 
@@ -624,12 +681,13 @@ def reference_cuda(wl, group, nt_sample, dev, reps=2):
         sys.path.insert(0, str(REF_DIR))
     try:
         from sweep.equations import Acoustic, Acoustic3D, Elastic, Elastic3D
+        from sweep.equations.acoustic_vti_1st import AcousticVTI1st
         from sweep.propagator.options import BoundarySaving
         from sweep.propagator.torch import PropTorch
     except Exception as e:                       # noqa: BLE001
         return {"unavailable": f"the reference does not import: {e}"}
     m_true, m_init, w, src, rec = wl.survey_inputs()
-    eq = {"acoustic2d": Acoustic, "acoustic2d_c1": Acoustic, "elastic2d": Elastic,
+    eq = {"acoustic2d": Acoustic, "acoustic2d_c1": Acoustic, "elastic2d": Elastic, "vti2d": AcousticVTI1st,
           "acoustic3d": Acoustic3D, "elastic3d": Elastic3D}[wl.name]
     solver = PropTorch(eq(spatial_order=ORDER, device=dev), shape=tuple(m_true[0].shape), dh=wl.dh,
                        dt=wl.dt, abcn=wl.abcn, impl="c", device=dev, memory=BoundarySaving())

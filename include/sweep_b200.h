@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define SWEEP_B200_ABI_VERSION 6
+#define SWEEP_B200_ABI_VERSION 7
 
 #if defined(__GNUC__)
 #define SWEEP_B200_API __attribute__((visibility("default")))
@@ -209,6 +209,54 @@ SWEEP_B200_API int sweep_b200_elastic_backward(const sweep_elastic_desc* d, int3
                                                float* grad_vp, float* grad_vs, float* grad_rho,
                                                void* workspace, int64_t workspace_bytes,
                                                void* stream, char* err, int32_t err_cap);
+
+/* 2-D first-order acoustic VTI problem (reference
+ * sweep.equations.AcousticVTI1st, Duveneck et al. 2008; equations/
+ * acoustic_vti_1st_2d/): velocities vx, vz and the horizontal / vertical
+ * stresses sH, sV on a staggered grid, stiffness c33 = rho vp^2,
+ * c11 = c33 (1 + 2 epsilon), c13 = c33 sqrt(1 + 2 delta).  Wavefield
+ * indices: 0 vx, 1 vz, 2 sH, 3 sV.  Every even spatial order 2..14; memory:
+ * boundary saving with fp32 strips in device memory (SWEEP_MEM_BOUNDARY). */
+typedef struct sweep_vti_desc {
+    int32_t B;               /* shots advanced together */
+    int32_t nz, nx;          /* runtime grid */
+    int32_t nt;              /* time steps */
+    int32_t M;               /* stencil half-width (spatial order / 2) */
+    int32_t pad[4];          /* PML pad per face: z_lo, z_hi, x_lo, x_hi (>= 1) */
+    float dt, dz, dx;
+    const float *az, *bz, *azh, *bzh;   /* staggered CPML profiles (length nz): */
+    const float *ax, *bx, *axh, *bxh;   /* integer and half-cell positions (nx) */
+    const float *vp, *epsilon, *delta, *rho;  /* (B|1, nz, nx) models on the runtime grid */
+    int64_t model_stride;    /* 0: models shared by every shot; else nz * nx */
+    int32_t nsrc;            /* sources per shot */
+    const int32_t* src_loc;  /* (B, nsrc, 2) runtime (x, z) */
+    const float* wavelet;    /* (B, nsrc, nt) amplitude added to every source field */
+    int32_t nsrc_fields;     /* 1..4 */
+    int32_t src_fields[4];   /* wavefield indices the wavelet is added to */
+    int32_t nrec;            /* receivers per shot (padded to a rectangle) */
+    const int32_t* rec_loc;  /* (B, nrec, 2) */
+    int32_t nrec_fields;     /* 1..4 */
+    int32_t rec_fields[4];   /* wavefield indices recorded, in record order */
+} sweep_vti_desc;
+
+/* Sizes of the VTI workspace and tape (as sweep_b200_acoustic_sizes). */
+SWEEP_B200_API int sweep_b200_vti_sizes(const sweep_vti_desc* d, int32_t mem_mode, int32_t ckpt_every,
+                                        int64_t* workspace_bytes, int64_t* tape_bytes, char* err, int32_t err_cap);
+
+/* VTI forward (reference acoustic_vti_1st_2d/forward.cu).  record:
+ * (B, nt, nrec, nrec_fields) out; tape: NULL or `tape_bytes` of device memory. */
+SWEEP_B200_API int sweep_b200_vti_forward(const sweep_vti_desc* d, int32_t mem_mode, int32_t ckpt_every,
+                                          float* record, void* tape, void* workspace, int64_t workspace_bytes,
+                                          void* stream, char* err, int32_t err_cap);
+
+/* VTI adjoint and vp / epsilon / delta / rho gradients (reference
+ * acoustic_vti_1st_2d/backward.cu:469-742, boundary saving).  adj:
+ * (B, nt, nrec, nrec_fields) record cotangent; the four gradients (B|1, nz, nx),
+ * same stride rule as the models, OVERWRITTEN (zero outside the physical box). */
+SWEEP_B200_API int sweep_b200_vti_backward(const sweep_vti_desc* d, int32_t mem_mode, int32_t ckpt_every,
+                                           const float* adj, const void* tape, float* grad_vp, float* grad_epsilon,
+                                           float* grad_delta, float* grad_rho, void* workspace,
+                                           int64_t workspace_bytes, void* stream, char* err, int32_t err_cap);
 
 /* 3-D isotropic elastic problem (velocity-stress, staggered grid; reference
  * sweep.equations.Elastic3D, entries 66-70: capi.h:105-109,

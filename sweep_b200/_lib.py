@@ -17,7 +17,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIB_PATH = Path(os.environ.get("SWEEP_B200_LIB", HERE / "libsweep_b200.so"))
-ABI_VERSION = 6
+ABI_VERSION = 7
 ERR_CAP = 4096
 
 c_i32, c_i64, c_f32, c_p = ctypes.c_int32, ctypes.c_int64, ctypes.c_float, ctypes.c_void_p
@@ -35,6 +35,9 @@ SYMBOLS = (
     "sweep_b200_elastic3d_sizes",
     "sweep_b200_elastic3d_forward",
     "sweep_b200_elastic3d_backward",
+    "sweep_b200_vti_sizes",
+    "sweep_b200_vti_forward",
+    "sweep_b200_vti_backward",
     "sweep_b200_conv3x3_gemm",
     "sweep_b200_conv3x3_wgrad",
     "sweep_b200_conv3x3_status",
@@ -116,6 +119,21 @@ class Elastic3DDesc(ctypes.Structure):
     ]
 
 
+class VTIDesc(ctypes.Structure):
+    """Mirror of ``sweep_vti_desc``."""
+    _fields_ = [
+        ("B", c_i32), ("nz", c_i32), ("nx", c_i32), ("nt", c_i32), ("M", c_i32), ("pad", c_i32 * 4),
+        ("dt", c_f32), ("dz", c_f32), ("dx", c_f32),
+        ("az", c_p), ("bz", c_p), ("azh", c_p), ("bzh", c_p),
+        ("ax", c_p), ("bx", c_p), ("axh", c_p), ("bxh", c_p),
+        ("vp", c_p), ("epsilon", c_p), ("delta", c_p), ("rho", c_p), ("model_stride", c_i64),
+        ("nsrc", c_i32), ("src_loc", c_p), ("wavelet", c_p),
+        ("nsrc_fields", c_i32), ("src_fields", c_i32 * 4),
+        ("nrec", c_i32), ("rec_loc", c_p),
+        ("nrec_fields", c_i32), ("rec_fields", c_i32 * 4),
+    ]
+
+
 class Schedule(ctypes.Structure):
     """Mirror of ``sweep_b200_schedule``."""
     _fields_ = [("shots_fwd", c_i32), ("shots_rev", c_i32), ("z_chunks", c_i32), ("graph_steps", c_i32),
@@ -164,6 +182,12 @@ def load():
                                                  ctypes.c_char_p, c_i32]
     lib.sweep_b200_elastic3d_backward.argtypes = [E3, c_i32, c_i32, c_p, c_p, c_p, c_p, c_p, c_p,
                                                   c_i64, c_p, ctypes.c_char_p, c_i32]
+    V = ctypes.POINTER(VTIDesc)
+    lib.sweep_b200_vti_sizes.argtypes = [V, c_i32, c_i32, ctypes.POINTER(c_i64), ctypes.POINTER(c_i64),
+                                         ctypes.c_char_p, c_i32]
+    lib.sweep_b200_vti_forward.argtypes = [V, c_i32, c_i32, c_p, c_p, c_p, c_i64, c_p, ctypes.c_char_p, c_i32]
+    lib.sweep_b200_vti_backward.argtypes = [V, c_i32, c_i32, c_p, c_p, c_p, c_p, c_p, c_p, c_p, c_i64, c_p,
+                                            ctypes.c_char_p, c_i32]
     lib.sweep_b200_conv3x3_gemm.argtypes = [c_p, c_p, c_p, c_p, c_i32, c_i32, c_i32, c_i32, c_i32, c_i32, c_p,
                                             ctypes.c_char_p, c_i32]
     lib.sweep_b200_conv3x3_wgrad.argtypes = [c_p, c_p, c_p, c_i32, c_i32, c_i32, c_i32, c_i32, c_p,

@@ -82,3 +82,18 @@ class Elastic3D(Elastic):
     SOURCE_FIELDS = ("sxx", "syy", "szz")
     RECEIVER_FIELDS = ("vx", "vy", "vz")
     FIELDS = ("vx", "vy", "vz", "sxx", "syy", "szz", "sxy", "sxz", "syz")
+
+
+class AcousticVTI1st(Elastic):
+    """First-order 2-D acoustic VTI velocity-stress equation (Duveneck et al.
+    2008) on a staggered grid: fields vx, vz, sH, sV; models vp (vertical),
+    Thomsen epsilon and delta, rho (c33 = rho vp^2, c11 = c33 (1 + 2 epsilon),
+    c13 = c33 sqrt(1 + 2 delta)); sources on (sH, sV) and vz receivers by
+    default (reference ``equations/acoustic_vti_1st.py:244-330``).  No free
+    surface, as in the reference."""
+    C_NAME = "vti2d"
+    MODEL_NAMES = ("vp", "epsilon", "delta", "rho")
+    NDIM = 2
+    SOURCE_FIELDS = ("sH", "sV")
+    RECEIVER_FIELDS = ("vz",)
+    FIELDS = ("vx", "vz", "sH", "sV")

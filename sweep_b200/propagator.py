@@ -33,7 +33,7 @@ import torch
 import torch.nn.functional as F
 
 from . import _lib
-from .equations import Acoustic, Acoustic3D, Elastic, Elastic3D
+from .equations import Acoustic, Acoustic3D, AcousticVTI1st, Elastic, Elastic3D
 from .options import BoundarySaving, Ckpt, Full
 from .pml import cpml_profiles_r, cpml_profiles_s
 from .scalars import centred_tables, staggered_grid_coes
@@ -196,6 +196,8 @@ class _Geometry:
     def elastic_desc(self, models, wavelet, src_fields, rec_fields):
         if self.ndim == 3:
             return self.elastic3d_desc(models, wavelet, src_fields, rec_fields)
+        if len(models) == 4:
+            return self.vti_desc(models, wavelet, src_fields, rec_fields)
         vp, vs, rho = models
         d = _lib.ElasticDesc()
         d.B = self.B
@@ -227,6 +229,36 @@ class _Geometry:
             d.free_surface[f] = 1 if self.fs_faces[f] else 0
         return d
 
+
+    def vti_desc(self, models, wavelet, src_fields, rec_fields):
+        vp, eps, dlt, rho = models
+        d = _lib.VTIDesc()
+        d.B = self.B
+        d.nz, d.nx = self.shape
+        d.nt = self.nt
+        d.M = self.M
+        for i in range(4):
+            d.pad[i] = self.pads[i]
+        d.dt = self.dt
+        d.dz, d.dx = self.spacing
+        (az, bz, azh, bzh), (ax, bx, axh, bxh) = self.prof
+        for name, t in (("az", az), ("bz", bz), ("azh", azh), ("bzh", bzh),
+                        ("ax", ax), ("bx", bx), ("axh", axh), ("bxh", bxh)):
+            setattr(d, name, t.data_ptr())
+        d.vp, d.epsilon, d.delta, d.rho = vp.data_ptr(), eps.data_ptr(), dlt.data_ptr(), rho.data_ptr()
+        d.model_stride = int(np.prod(self.shape)) if vp.dim() == 3 else 0
+        d.nsrc = self.nsrc
+        d.src_loc = self.src.data_ptr()
+        d.wavelet = wavelet.data_ptr()
+        d.nsrc_fields = len(src_fields)
+        for k, f in enumerate(src_fields):
+            d.src_fields[k] = f
+        d.nrec = self.nrec
+        d.rec_loc = self.rec.data_ptr()
+        d.nrec_fields = len(rec_fields)
+        for k, f in enumerate(rec_fields):
+            d.rec_fields[k] = f
+        return d
 
     def elastic3d_desc(self, models, wavelet, src_fields, rec_fields):
         vp, vs, rho = models
@@ -374,6 +406,52 @@ class _ElasticFn(torch.autograd.Function):
         return g[0], g[1], g[2], None, None, None, None, None, None
 
 
+class _VTIFn(torch.autograd.Function):
+    """vp, epsilon, delta, rho (runtime grid, shared or per shot, all alike)
+    and the wavelet ``(B, nsrc, nt)`` -> record ``(B, nt, nrec, nfield)``; the
+    backward returns the four model gradients (no wavelet gradient, as for
+    Elastic)."""
+
+    @staticmethod
+    def forward(ctx, vp, eps, dlt, rho, wavelet, prop, geo, fields, mem_mode, ckpt_every):
+        models = [m.contiguous() for m in (vp, eps, dlt, rho)]
+        wavelet = wavelet.contiguous()
+        sf, rf = fields
+        desc = geo.vti_desc(models, wavelet, sf, rf)
+        ws_b, tape_b = _lib.c_i64(), _lib.c_i64()
+        _lib.call("sweep_b200_vti_sizes", desc, mem_mode, ckpt_every, ws_b, tape_b)
+        dev = vp.device
+        ws = prop._workspace(ws_b.value, dev)
+        tape = torch.empty(tape_b.value, dtype=torch.uint8, device=dev) if any(ctx.needs_input_grad[:4]) else None
+        record = torch.empty((geo.B, geo.nt, geo.nrec, len(rf)), dtype=torch.float32, device=dev)
+        _lib.call("sweep_b200_vti_forward", desc, mem_mode, ckpt_every, record.data_ptr(),
+                  tape.data_ptr() if tape is not None else None, ws.data_ptr(), ws.numel(), _stream_ptr(dev))
+        ctx.save_for_backward(*models, wavelet)
+        ctx.tape = tape
+        ctx.geo, ctx.prop, ctx.fields = geo, prop, fields
+        ctx.mem_mode, ctx.ckpt_every = mem_mode, ckpt_every
+        return record
+
+    @staticmethod
+    def backward(ctx, grad_record):
+        if ctx.tape is None:
+            raise RuntimeError("sweep_b200: this forward has already been back-propagated (or ran "
+                               "without gradients); a second backward is refused")
+        vp, eps, dlt, rho, wavelet = ctx.saved_tensors
+        geo, prop = ctx.geo, ctx.prop
+        adj = grad_record.to(torch.float32).contiguous()
+        desc = geo.vti_desc([vp, eps, dlt, rho], wavelet, *ctx.fields)
+        ws_b, tape_b = _lib.c_i64(), _lib.c_i64()
+        _lib.call("sweep_b200_vti_sizes", desc, ctx.mem_mode, ctx.ckpt_every, ws_b, tape_b)
+        ws = prop._workspace(ws_b.value, vp.device)
+        g = [torch.empty_like(vp) for _ in range(4)]
+        _lib.call("sweep_b200_vti_backward", desc, ctx.mem_mode, ctx.ckpt_every, adj.data_ptr(),
+                  ctx.tape.data_ptr(), *[x.data_ptr() for x in g], ws.data_ptr(), ws.numel(),
+                  _stream_ptr(vp.device))
+        ctx.tape = None
+        return g[0], g[1], g[2], g[3], None, None, None, None, None, None
+
+
 class PropTorch(torch.nn.Module):
     """Propagator over the B200 core (``impl='c'``; the only implementation).
 
@@ -419,6 +497,9 @@ class PropTorch(torch.nn.Module):
         if self.abcn < 1:
             raise NotImplementedError("sweep_b200: the absorbing faces need a layer (abcn >= 1)")
         self.fs_faces = free_faces(free_surface, nd)
+        if isinstance(equation, AcousticVTI1st) and any(self.fs_faces):
+            raise NotImplementedError("AcousticVTI1st has no free surface (the reference refuses it too: the VTI "
+                                      "traction-free condition needs an anisotropic image method)")
         if nd == 3 and any(self.fs_faces[1:]):
             raise NotImplementedError("per-face free surfaces are 2-D only (as in the reference); "
                                       "3-D takes free_surface=True (the top face)")
@@ -523,7 +604,8 @@ class PropTorch(torch.nn.Module):
         ws_b, tape_b = _lib.c_i64(), _lib.c_i64()
         name = "sweep_b200_acoustic_sizes"
         if fields is not None:
-            name = "sweep_b200_elastic3d_sizes" if isinstance(desc, _lib.Elastic3DDesc) else "sweep_b200_elastic_sizes"
+            name = ("sweep_b200_elastic3d_sizes" if isinstance(desc, _lib.Elastic3DDesc) else
+                    "sweep_b200_vti_sizes" if isinstance(desc, _lib.VTIDesc) else "sweep_b200_elastic_sizes")
         _lib.call(name, desc, mem_mode, ckpt_every, ws_b, tape_b)
         return int(tape_b.value)
 
@@ -564,6 +646,8 @@ class PropTorch(torch.nn.Module):
         desc = self._desc(geo, padded, wb, fields)
         if isinstance(desc, _lib.Elastic3DDesc):
             return {"fixed": "one thread per cell, 32 x 8 cell tiles per z plane and shot"}
+        if isinstance(desc, _lib.VTIDesc):
+            return {"fixed": "one thread per cell, 32 x 8 cell tiles per shot"}
         if desc.M != 4:
             return {"fixed": f"order {2 * desc.M}: one thread per cell, 32 x 8 cell tiles per plane and shot"}
         return autotune.get_schedule(desc)
@@ -596,6 +680,12 @@ class PropTorch(torch.nn.Module):
         eq = self.equation
         if isinstance(eq, (Acoustic, Acoustic3D)):
             return _AcousticFn.apply(padded[0], wb, self, geo, mem_mode, ckpt_every)
+        if isinstance(eq, AcousticVTI1st):
+            if wavelet.requires_grad and torch.is_grad_enabled():
+                raise NotImplementedError(
+                    "impl='c' AcousticVTI1st does not return the wavelet gradient (its compiled backward "
+                    "returns the model gradients only). Detach the wavelet.")
+            return _VTIFn.apply(*padded, wb, self, geo, fields, mem_mode, ckpt_every)
         if isinstance(eq, Elastic):
             if wavelet.requires_grad and torch.is_grad_enabled():
                 raise NotImplementedError(
@@ -643,7 +733,7 @@ class PropTorch(torch.nn.Module):
         mem_mode, ckpt_every = self._mem_mode()
         padded = [self._pad_model(m.to(dev)) for m in models]
         fields = self._elastic_fields() if isinstance(eq, Elastic) else None
-        if (self.autotune or self.schedule is not None) and (isinstance(eq, Elastic3D) or eq.M != 4):
+        if (self.autotune or self.schedule is not None) and (isinstance(eq, (Elastic3D, AcousticVTI1st)) or eq.M != 4):
             raise NotImplementedError(f"sweep_b200: {type(eq).__name__} at spatial_order={eq.spatial_order} has one "
                                       f"built-in launch schedule (no autotune)")
         if self.autotune or self.schedule is not None:

@@ -23,7 +23,7 @@ import ctypes
 import torch
 
 from . import _lib
-from .equations import Elastic3D
+from .equations import AcousticVTI1st, Elastic3D
 
 
 def _check_memory(mem_mode):
@@ -67,9 +67,9 @@ class ForwardRunner:
     """A forward pass of ``prop`` over fixed inputs, run in segments."""
 
     def __init__(self, prop, wavelet, sources, receivers, models, max_vel=4500.0, pml_freq=25.0):
-        if isinstance(prop.equation, Elastic3D):
-            raise NotImplementedError("sweep_b200: stepped runners are built for Acoustic, Acoustic3D and "
-                                      "Elastic; Elastic3D runs whole passes only")
+        if isinstance(prop.equation, (Elastic3D, AcousticVTI1st)):
+            raise NotImplementedError(f"sweep_b200: stepped runners are built for Acoustic, Acoustic3D and "
+                                      f"Elastic; {type(prop.equation).__name__} runs whole passes only")
         models = [m.detach() for m in models]
         geo, padded, wb, fields, mem_mode, ckpt_every, _ = prop._prepare(
             wavelet.detach() if isinstance(wavelet, torch.Tensor) else wavelet, sources, receivers, models,

@@ -468,3 +468,36 @@ def test_elastic3d_sizes_and_refusals():
     with pytest.raises(ValueError, match="source_type"):
         PropTorch(eq, shape=(20, 22, 24), dh=5.0, dt=0.0005, abcn=6, device="cpu",
                   source_type=["sxz", "pressure"])._elastic_fields()
+
+
+def test_vti_sizes_and_refusals():
+    """The 2-D acoustic VTI core sizes its workspace and tape on the host,
+    takes every order 2 to 14, and refuses other memory modes, free surfaces,
+    stepped runners and tuning."""
+    import torch
+    from sweep_b200 import AcousticVTI1st, Ckpt, PropTorch, _lib
+    eq = AcousticVTI1st(spatial_order=8)
+    assert eq.default_source_fields == ["sH", "sV"] and eq.default_receiver_fields == ["vz"]
+    s = PropTorch(eq, shape=(30, 40), dh=5.0, dt=5e-4, abcn=6, device="cpu")
+    src, rec = np.array([[8, 6]]), np.zeros((1, 4, 2), np.int64)
+    models = [torch.full((30, 40), 2000.0), torch.full((30, 40), 0.1), torch.full((30, 40), 0.05),
+              torch.full((30, 40), 2000.0)]
+    geo, padded, wb, fields = s._probe(50, src, rec, models)
+    d = s._desc(geo, padded, wb, fields)
+    assert isinstance(d, _lib.VTIDesc) and d.M == 4 and list(d.pad) == [6, 6, 6, 6]
+    ws, tape = _lib.c_i64(), _lib.c_i64()
+    _lib.call("sweep_b200_vti_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
+    assert tape.value > 50 * 4 * 4 and ws.value > 0
+    assert s.launch_schedule(50, src, rec, models) == {"fixed": "one thread per cell, 32 x 8 cell tiles per shot"}
+    for mode in (_lib.MEM_CHECKPOINT, _lib.MEM_BOUNDARY_FP16, _lib.MEM_BOUNDARY | _lib.MEM_HOST_TAPE):
+        with pytest.raises(RuntimeError, match="boundary saving with fp32 strips"):
+            _lib.call("sweep_b200_vti_sizes", d, mode, 10, ws, tape)
+    d.M = 8
+    with pytest.raises(RuntimeError, match="orders 2 to 14"):
+        _lib.call("sweep_b200_vti_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
+    with pytest.raises(NotImplementedError, match="no free surface"):
+        PropTorch(eq, shape=(30, 40), abcn=6, device="cpu", free_surface=True)
+    with pytest.raises(NotImplementedError, match="whole passes"):
+        s.forward_runner(torch.zeros(50), src, rec, models)
+    with pytest.raises(ValueError, match="source_type"):
+        PropTorch(eq, shape=(30, 40), abcn=6, device="cpu", source_type=["sxx"])._elastic_fields()
