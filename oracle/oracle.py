@@ -119,6 +119,14 @@ def _lib(prec: str):
         lib.oracle_vti2d_forward.argtypes = geo_vti + [P, P]
         lib.oracle_vti2d_backward.restype = i
         lib.oracle_vti2d_backward.argtypes = geo_vti + [P, P, P, P, P, P]
+        geo_vti3 = [i, i, i, i, i, i, P, real, real, real, real, P, P, P, P, P, P, l,
+                    i, P, P, i, P, i, P, i, P]
+        lib.oracle_vti3d_tape_len.restype = l
+        lib.oracle_vti3d_tape_len.argtypes = [i, i, i, i, i, i, P]
+        lib.oracle_vti3d_forward.restype = i
+        lib.oracle_vti3d_forward.argtypes = geo_vti3 + [P, P]
+        lib.oracle_vti3d_backward.restype = i
+        lib.oracle_vti3d_backward.argtypes = geo_vti3 + [P, P, P, P, P, P]
         _LIBS[prec] = _FlushToZero(lib)
     return _LIBS[prec]
 
@@ -723,3 +731,102 @@ def vti2d_gradient(vp, eps, delta, rho, wavelet, src, rec, obs, dh, dt, abcn, or
 
 def vti2d_forward(vp, eps, delta, rho, wavelet, src, rec, dh, dt, abcn, order=8, prec="f32", **kw):
     return VTI2D(vp, eps, delta, rho, wavelet, src, rec, dh, dt, abcn, order, prec, **kw).forward(keep_tape=False)
+
+
+VTI3_FIELDS = ("vx", "vy", "vz", "sH", "sV")
+
+
+class VTI3D:
+    """One float32 / float64 run of the 3-D first-order acoustic VTI oracle
+    (``fd_oracle_vti3d.c``; reference ``sweep.equations.AcousticVTI1st3D``).
+
+    Models ``vp, epsilon, delta, rho`` of shape ``(nz, ny, nx)`` or per shot
+    ``(B, nz, ny, nx)``; coordinates ``(x, y, z)``; source fields default to
+    ``(sH, sV)``, receiver fields to ``(vz,)``
+    (``src/sweep/equations/acoustic_vti_1st.py:530-536``)."""
+
+    def __init__(self, vp, eps, delta, rho, wavelet, src, rec, dh, dt, abcn, order=4, prec="f32",
+                 source_fields=("sH", "sV"), receiver_fields=("vz",), max_vel=4500.0, pml_freq=25.0):
+        self.prec = prec
+        self.real = np.float32 if prec == "f32" else np.float64
+        models = [np.asarray(m, np.float32) for m in (vp, eps, delta, rho)]
+        self.per_shot = models[0].ndim == 4
+        self.M = M = order // 2
+        w, s, r = _batch_io(wavelet, src, rec, 3)
+        self.B, self.nt = w.shape[0], w.shape[-1]
+        self.phys = models[0].shape[-3:]
+        self.pads = [abcn] * 6                   # z_lo, z_hi, y_lo, y_hi, x_lo, x_hi
+        self.shape = tuple(n + 2 * abcn + 2 * M for n in self.phys)
+        padw = [(abcn + M, abcn + M)] * 3
+        lead = [(0, 0)] if self.per_shot else []
+        self.models = [np.ascontiguousarray(np.pad(m, lead + padw, mode="edge").astype(self.real))
+                       for m in models]
+        self.m_stride = int(np.prod(self.shape)) if self.per_shot else 0
+        sp = dh if np.ndim(dh) else [dh] * 3
+        self.spacing = [float(x) for x in sp]
+        self.dt = float(dt)
+        prof = cpml_profiles_s(self.pads, M, dt, self.spacing, self.shape, max_vel, pml_freq)
+        self.prof = np.ascontiguousarray(np.concatenate([np.concatenate(p) for p in prof]).astype(self.real))
+        c = staggered_coefficients(M)
+        if self.real is np.float32:
+            self.coef = np.array([0.0] + [np.float32(float(x)) for x in c], np.float32)
+        else:
+            self.coef = np.array([0.0] + [float(x) for x in c], np.float64)
+        off = np.full(3, abcn + M)
+        self.src = np.ascontiguousarray((s + off).astype(np.int32))
+        self.rec = np.ascontiguousarray((r + off).astype(np.int32))
+        self.wavelet = np.ascontiguousarray(w.astype(self.real))
+        self.nrec = self.rec.shape[1]
+        self.sf = np.array([VTI3_FIELDS.index(f) for f in source_fields], np.int32)
+        self.rf = np.array([VTI3_FIELDS.index(f) for f in receiver_fields], np.int32)
+        self._pad = np.array(self.pads, np.int32)
+
+    def _geo(self):
+        nz, ny, nx = self.shape
+        return [self.B, nz, ny, nx, self.nt, self.M, _ptr(self._pad), self.dt, *self.spacing,
+                _ptr(self.coef), _ptr(self.prof)] + [_ptr(m) for m in self.models] + [
+                self.m_stride, self.src.shape[1], _ptr(self.src), _ptr(self.wavelet), len(self.sf), _ptr(self.sf),
+                self.nrec, _ptr(self.rec), len(self.rf), _ptr(self.rf)]
+
+    def crop(self, g):
+        M, a = self.M, self.pads[0]
+        sl = tuple(slice(a + M, a + M + n) for n in self.phys)
+        return g[(Ellipsis,) + sl]
+
+    def forward(self, keep_tape=True):
+        """Records ``(B, nt, nrec, nfield)``."""
+        lib = _lib(self.prec)
+        nz, ny, nx = self.shape
+        rec = np.zeros((self.B, self.nt, self.nrec, len(self.rf)), self.real)
+        self.tape = None
+        if keep_tape:
+            self.tape = np.zeros(lib.oracle_vti3d_tape_len(self.B, nz, ny, nx, self.nt, self.M, _ptr(self._pad)),
+                                 self.real)
+        rc = lib.oracle_vti3d_forward(*self._geo(), _ptr(rec), _ptr(self.tape) if keep_tape else None)
+        assert rc == 0
+        return rec
+
+    def backward(self, adj):
+        """``adj``: record cotangent ``(B, nt, nrec, nfield)``; returns the
+        cropped ``(grad_vp, grad_epsilon, grad_delta, grad_rho)``."""
+        lib = _lib(self.prec)
+        a = np.ascontiguousarray(np.asarray(adj).astype(self.real))
+        shp = ((self.B,) if self.per_shot else ()) + self.shape
+        g = [np.zeros(shp, self.real) for _ in range(4)]
+        rc = lib.oracle_vti3d_backward(*self._geo(), _ptr(a), _ptr(self.tape), *[_ptr(x) for x in g])
+        assert rc == 0
+        return tuple(self.crop(x) for x in g)
+
+
+def vti3d_gradient(vp, eps, delta, rho, wavelet, src, rec, obs, dh, dt, abcn, order=4, prec="f32", **kw):
+    """Record, loss ``0.5 ||pred - obs||^2`` and cropped ``(vp, epsilon,
+    delta, rho)`` gradients (summed over shots for shared models)."""
+    run = VTI3D(vp, eps, delta, rho, wavelet, src, rec, dh, dt, abcn, order, prec, **kw)
+    pred = run.forward(keep_tape=True)
+    res = pred - np.asarray(obs, run.real)
+    loss = 0.5 * float(np.sum(res.astype(np.float64) ** 2))
+    return pred, loss, run.backward(res)
+
+
+def vti3d_forward(vp, eps, delta, rho, wavelet, src, rec, dh, dt, abcn, order=4, prec="f32", **kw):
+    return VTI3D(vp, eps, delta, rho, wavelet, src, rec, dh, dt, abcn, order, prec, **kw).forward(keep_tape=False)

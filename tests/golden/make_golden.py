@@ -931,6 +931,48 @@ def vti2d():
     np.savez_compressed(OUT / "vti2d.npz", **out)
 
 
+def vti3d():
+    """3-D first-order acoustic VTI (reference AcousticVTI1st3D; vx, vy, vz,
+    sH, sV): 2 shots on an 18 x 20 x 22 layered model (CPML 6) with Thomsen
+    epsilon / delta layers, the default sources (sH, sV) and receivers (vz),
+    vp / epsilon / delta / rho gradients, boundary saving, at orders 4 (the
+    reference's default) and 8; at order 4 once more with (vx, vy, sH)
+    receivers."""
+    from sweep.equations.acoustic_vti_1st import AcousticVTI1st3D
+    rng = np.random.default_rng(233)
+    nz, ny, nx, nt, dt, dh, abcn = 18, 20, 22, 140, 0.0005, 5.0, 6
+    base = _layered(nz, nx, rng, 1800.0, 3000.0, 3)
+    vp_true = np.ascontiguousarray(np.repeat(base[:, None, :], ny, axis=1)
+                                   * (1 + 0.02 * np.sin(np.arange(ny) / 3.0))[None, :, None]).astype(np.float32)
+    eps_true = (0.05 + 0.1 * (vp_true - 1800.0) / 1200.0).astype(np.float32)
+    dlt_true = (0.5 * eps_true).astype(np.float32)
+    rho_true = (310.0 * vp_true ** 0.25).astype(np.float32)
+    vp_init = np.full((nz, ny, nx), 2300.0, np.float32)
+    eps_init = np.full((nz, ny, nx), 0.1, np.float32)
+    dlt_init = np.full((nz, ny, nx), 0.05, np.float32)
+    rho_init = (310.0 * vp_init ** 0.25).astype(np.float32)
+    w = _wavelet(nt, dt, 30.0, 0.03)
+    src = np.array([[8, 9, 5], [14, 11, 7]], np.int64)              # (x, y, z)
+    rec = np.zeros((2, 10, 3), np.int64)
+    for b in range(2):
+        rec[b, :, 0] = np.linspace(1, nx - 2, 10).astype(np.int64)
+        rec[b, :, 1] = np.linspace(2, ny - 3, 10).astype(np.int64)
+        rec[b, :, 2] = 2 + b
+    names = ("vp", "eps", "dlt", "rho")
+    true = [vp_true, eps_true, dlt_true, rho_true]
+    init = [vp_init, eps_init, dlt_init, rho_init]
+    out = dict(nz=nz, ny=ny, nx=nx, nt=nt, dt=dt, dh=dh, abcn=abcn, wavelet=w, src=src, rec=rec,
+               **{f"{n}_true": m for n, m in zip(names, true)}, **{f"{n}_init": m for n, m in zip(names, init)})
+    for tag, order, kw in (("o4", 4, {}), ("o8", 8, {}), ("o4_rec", 4, dict(receiver_type=["vx", "vy", "sH"]))):
+        solver = PropTorch(AcousticVTI1st3D(spatial_order=order, device="cpu"), shape=(nz, ny, nx), dh=dh, dt=dt,
+                           abcn=abcn, impl="c", device="cpu", memory=BoundarySaving(), **kw)
+        obs = _forward(solver, w, src, rec, true)
+        r = _run(solver, w, src, rec, init, obs, False)
+        out.update({f"obs_{tag}": obs, f"pred_{tag}": r["pred"]})
+        out.update({f"grad_{n}_{tag}": r[f"grad{i}"] for i, n in enumerate(names)})
+    np.savez_compressed(OUT / "vti3d.npz", **out)
+
+
 def elastic3d_storage():
     """3-D elastic boundary saving with fp16 / bf16 / int8 strips (reference
     Elastic3D, BoundarySaving(storage_dtype=...): each of the nine fields
@@ -997,6 +1039,7 @@ CASES = {
     "elastic_orders": elastic_orders,
     "elastic3d_orders": elastic3d_orders,
     "vti2d": vti2d,
+    "vti3d": vti3d,
 }
 
 if __name__ == "__main__":
