@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define SWEEP_B200_ABI_VERSION 7
+#define SWEEP_B200_ABI_VERSION 8
 
 #if defined(__GNUC__)
 #define SWEEP_B200_API __attribute__((visibility("default")))
@@ -257,6 +257,50 @@ SWEEP_B200_API int sweep_b200_vti_backward(const sweep_vti_desc* d, int32_t mem_
                                            const float* adj, const void* tape, float* grad_vp, float* grad_epsilon,
                                            float* grad_delta, float* grad_rho, void* workspace,
                                            int64_t workspace_bytes, void* stream, char* err, int32_t err_cap);
+
+/* 3-D first-order acoustic VTI problem (reference
+ * sweep.equations.AcousticVTI1st3D, Duveneck et al. 2008; equations/
+ * acoustic_vti_1st_3d/): velocities vx, vy, vz and the horizontal / vertical
+ * stresses sH = s11 = s22, sV = s33 on a staggered grid, the 2-D problem's
+ * stiffness.  Wavefield indices: 0 vx, 1 vy, 2 vz, 3 sH, 4 sV.  Every even
+ * spatial order 2..14; memory: boundary saving with fp32 strips in device
+ * memory (SWEEP_MEM_BOUNDARY).  B * nz <= 65535. */
+typedef struct sweep_vti3d_desc {
+    int32_t B;               /* shots advanced together */
+    int32_t nz, ny, nx;      /* runtime grid */
+    int32_t nt;              /* time steps */
+    int32_t M;               /* stencil half-width (spatial order / 2) */
+    int32_t pad[6];          /* PML pad per face: z_lo, z_hi, y_lo, y_hi, x_lo, x_hi (>= 1) */
+    float dt, dz, dy, dx;
+    const float *az, *bz, *azh, *bzh;   /* staggered CPML profiles per axis: */
+    const float *ay, *by, *ayh, *byh;   /* integer and half-cell positions */
+    const float *ax, *bx, *axh, *bxh;
+    const float *vp, *epsilon, *delta, *rho;  /* (B|1, nz, ny, nx) models on the runtime grid */
+    int64_t model_stride;    /* 0: models shared by every shot; else nz * ny * nx */
+    int32_t nsrc;            /* sources per shot */
+    const int32_t* src_loc;  /* (B, nsrc, 3) runtime (x, y, z) */
+    const float* wavelet;    /* (B, nsrc, nt) amplitude added to every source field */
+    int32_t nsrc_fields;     /* 1..5 */
+    int32_t src_fields[5];   /* wavefield indices the wavelet is added to */
+    int32_t nrec;            /* receivers per shot (padded to a rectangle) */
+    const int32_t* rec_loc;  /* (B, nrec, 3) */
+    int32_t nrec_fields;     /* 1..5 */
+    int32_t rec_fields[5];   /* wavefield indices recorded, in record order */
+} sweep_vti3d_desc;
+
+/* Sizes, forward (reference acoustic_vti_1st_3d/forward.cu) and backward
+ * (acoustic_vti_1st_3d/backward.cu, boundary saving) of the 3-D VTI problem,
+ * as the 2-D VTI entries: record (B, nt, nrec, nrec_fields); the four
+ * gradients (B|1, nz, ny, nx), OVERWRITTEN, zero outside the physical box. */
+SWEEP_B200_API int sweep_b200_vti3d_sizes(const sweep_vti3d_desc* d, int32_t mem_mode, int32_t ckpt_every,
+                                          int64_t* workspace_bytes, int64_t* tape_bytes, char* err, int32_t err_cap);
+SWEEP_B200_API int sweep_b200_vti3d_forward(const sweep_vti3d_desc* d, int32_t mem_mode, int32_t ckpt_every,
+                                            float* record, void* tape, void* workspace, int64_t workspace_bytes,
+                                            void* stream, char* err, int32_t err_cap);
+SWEEP_B200_API int sweep_b200_vti3d_backward(const sweep_vti3d_desc* d, int32_t mem_mode, int32_t ckpt_every,
+                                             const float* adj, const void* tape, float* grad_vp, float* grad_epsilon,
+                                             float* grad_delta, float* grad_rho, void* workspace,
+                                             int64_t workspace_bytes, void* stream, char* err, int32_t err_cap);
 
 /* 3-D isotropic elastic problem (velocity-stress, staggered grid; reference
  * sweep.equations.Elastic3D, entries 66-70: capi.h:105-109,

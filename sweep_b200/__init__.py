@@ -3,9 +3,9 @@
 with adjoint gradients, on hand-written sm_100a CUDA kernels behind a C ABI
 (``include/sweep_b200.h``)."""
 from . import autotune
-from .equations import Acoustic, Acoustic3D, AcousticVTI1st, Elastic, Elastic3D
+from .equations import Acoustic, Acoustic3D, AcousticVTI1st, AcousticVTI1st3D, Elastic, Elastic3D
 from .options import BoundarySaving, Ckpt, Full
 from .propagator import PropTorch
 from .signal import ricker
 
-__all__ = ["autotune", "Acoustic", "Acoustic3D", "AcousticVTI1st", "Elastic", "Elastic3D", "BoundarySaving", "Ckpt", "Full", "PropTorch", "ricker"]
+__all__ = ["autotune", "Acoustic", "Acoustic3D", "AcousticVTI1st", "AcousticVTI1st3D", "Elastic", "Elastic3D", "BoundarySaving", "Ckpt", "Full", "PropTorch", "ricker"]

@@ -17,7 +17,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIB_PATH = Path(os.environ.get("SWEEP_B200_LIB", HERE / "libsweep_b200.so"))
-ABI_VERSION = 7
+ABI_VERSION = 8
 ERR_CAP = 4096
 
 c_i32, c_i64, c_f32, c_p = ctypes.c_int32, ctypes.c_int64, ctypes.c_float, ctypes.c_void_p
@@ -38,6 +38,9 @@ SYMBOLS = (
     "sweep_b200_vti_sizes",
     "sweep_b200_vti_forward",
     "sweep_b200_vti_backward",
+    "sweep_b200_vti3d_sizes",
+    "sweep_b200_vti3d_forward",
+    "sweep_b200_vti3d_backward",
     "sweep_b200_conv3x3_gemm",
     "sweep_b200_conv3x3_wgrad",
     "sweep_b200_conv3x3_status",
@@ -134,6 +137,22 @@ class VTIDesc(ctypes.Structure):
     ]
 
 
+class VTI3DDesc(ctypes.Structure):
+    """Mirror of ``sweep_vti3d_desc``."""
+    _fields_ = [
+        ("B", c_i32), ("nz", c_i32), ("ny", c_i32), ("nx", c_i32), ("nt", c_i32), ("M", c_i32),
+        ("pad", c_i32 * 6), ("dt", c_f32), ("dz", c_f32), ("dy", c_f32), ("dx", c_f32),
+        ("az", c_p), ("bz", c_p), ("azh", c_p), ("bzh", c_p),
+        ("ay", c_p), ("by", c_p), ("ayh", c_p), ("byh", c_p),
+        ("ax", c_p), ("bx", c_p), ("axh", c_p), ("bxh", c_p),
+        ("vp", c_p), ("epsilon", c_p), ("delta", c_p), ("rho", c_p), ("model_stride", c_i64),
+        ("nsrc", c_i32), ("src_loc", c_p), ("wavelet", c_p),
+        ("nsrc_fields", c_i32), ("src_fields", c_i32 * 5),
+        ("nrec", c_i32), ("rec_loc", c_p),
+        ("nrec_fields", c_i32), ("rec_fields", c_i32 * 5),
+    ]
+
+
 class Schedule(ctypes.Structure):
     """Mirror of ``sweep_b200_schedule``."""
     _fields_ = [("shots_fwd", c_i32), ("shots_rev", c_i32), ("z_chunks", c_i32), ("graph_steps", c_i32),
@@ -188,6 +207,12 @@ def load():
     lib.sweep_b200_vti_forward.argtypes = [V, c_i32, c_i32, c_p, c_p, c_p, c_i64, c_p, ctypes.c_char_p, c_i32]
     lib.sweep_b200_vti_backward.argtypes = [V, c_i32, c_i32, c_p, c_p, c_p, c_p, c_p, c_p, c_p, c_i64, c_p,
                                             ctypes.c_char_p, c_i32]
+    V3 = ctypes.POINTER(VTI3DDesc)
+    lib.sweep_b200_vti3d_sizes.argtypes = [V3, c_i32, c_i32, ctypes.POINTER(c_i64), ctypes.POINTER(c_i64),
+                                           ctypes.c_char_p, c_i32]
+    lib.sweep_b200_vti3d_forward.argtypes = [V3, c_i32, c_i32, c_p, c_p, c_p, c_i64, c_p, ctypes.c_char_p, c_i32]
+    lib.sweep_b200_vti3d_backward.argtypes = [V3, c_i32, c_i32, c_p, c_p, c_p, c_p, c_p, c_p, c_p, c_i64, c_p,
+                                              ctypes.c_char_p, c_i32]
     lib.sweep_b200_conv3x3_gemm.argtypes = [c_p, c_p, c_p, c_p, c_i32, c_i32, c_i32, c_i32, c_i32, c_i32, c_p,
                                             ctypes.c_char_p, c_i32]
     lib.sweep_b200_conv3x3_wgrad.argtypes = [c_p, c_p, c_p, c_i32, c_i32, c_i32, c_i32, c_i32, c_p,

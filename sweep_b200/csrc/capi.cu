@@ -7,6 +7,7 @@
 #include "acoustic_orders.cuh"
 #include "elastic_orders.cuh"
 #include "vti2d.cuh"
+#include "vti3d.cuh"
 
 namespace sweep {
 namespace a3d {
@@ -144,6 +145,38 @@ extern "C" int sweep_b200_vti_backward(const sweep_vti_desc* d, int32_t mem_mode
         SWEEP_REQUIRE(d != nullptr, "null descriptor");
         vti::backward(d, mem_mode, ckpt_every, adj, tape, grad_vp, grad_epsilon, grad_delta, grad_rho, workspace,
                       workspace_bytes, static_cast<cudaStream_t>(stream));
+    });
+}
+
+extern "C" int sweep_b200_vti3d_sizes(const sweep_vti3d_desc* d, int32_t mem_mode, int32_t ckpt_every,
+                                      int64_t* workspace_bytes, int64_t* tape_bytes, char* err, int32_t err_cap)
+{
+    return guarded(err, err_cap, [&] {
+        SWEEP_REQUIRE(d && workspace_bytes && tape_bytes, "null argument");
+        vti3::sizes(d, mem_mode, ckpt_every, workspace_bytes, tape_bytes);
+    });
+}
+
+extern "C" int sweep_b200_vti3d_forward(const sweep_vti3d_desc* d, int32_t mem_mode, int32_t ckpt_every,
+                                        float* record, void* tape, void* workspace, int64_t workspace_bytes,
+                                        void* stream, char* err, int32_t err_cap)
+{
+    return guarded(err, err_cap, [&] {
+        SWEEP_REQUIRE(d != nullptr, "null descriptor");
+        vti3::forward(d, mem_mode, ckpt_every, record, tape, workspace, workspace_bytes,
+                      static_cast<cudaStream_t>(stream));
+    });
+}
+
+extern "C" int sweep_b200_vti3d_backward(const sweep_vti3d_desc* d, int32_t mem_mode, int32_t ckpt_every,
+                                         const float* adj, const void* tape, float* grad_vp, float* grad_epsilon,
+                                         float* grad_delta, float* grad_rho, void* workspace,
+                                         int64_t workspace_bytes, void* stream, char* err, int32_t err_cap)
+{
+    return guarded(err, err_cap, [&] {
+        SWEEP_REQUIRE(d != nullptr, "null descriptor");
+        vti3::backward(d, mem_mode, ckpt_every, adj, tape, grad_vp, grad_epsilon, grad_delta, grad_rho, workspace,
+                       workspace_bytes, static_cast<cudaStream_t>(stream));
     });
 }
 

@@ -97,3 +97,14 @@ class AcousticVTI1st(Elastic):
     SOURCE_FIELDS = ("sH", "sV")
     RECEIVER_FIELDS = ("vz",)
     FIELDS = ("vx", "vz", "sH", "sV")
+
+
+class AcousticVTI1st3D(AcousticVTI1st):
+    """First-order 3-D acoustic VTI velocity-stress equation (Duveneck et al.
+    2008) on a staggered grid: fields vx, vy, vz, sH (= s11 = s22) and sV
+    (= s33); the 2-D equation's models and stiffness; sources on (sH, sV) and
+    vz receivers by default (reference ``equations/acoustic_vti_1st.py:
+    445-600``).  No free surface, as in the reference."""
+    C_NAME = "vti3d"
+    NDIM = 3
+    FIELDS = ("vx", "vy", "vz", "sH", "sV")

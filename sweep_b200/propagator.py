@@ -194,6 +194,8 @@ class _Geometry:
 
 
     def elastic_desc(self, models, wavelet, src_fields, rec_fields):
+        if self.ndim == 3 and len(models) == 4:
+            return self.vti3d_desc(models, wavelet, src_fields, rec_fields)
         if self.ndim == 3:
             return self.elastic3d_desc(models, wavelet, src_fields, rec_fields)
         if len(models) == 4:
@@ -247,6 +249,35 @@ class _Geometry:
             setattr(d, name, t.data_ptr())
         d.vp, d.epsilon, d.delta, d.rho = vp.data_ptr(), eps.data_ptr(), dlt.data_ptr(), rho.data_ptr()
         d.model_stride = int(np.prod(self.shape)) if vp.dim() == 3 else 0
+        d.nsrc = self.nsrc
+        d.src_loc = self.src.data_ptr()
+        d.wavelet = wavelet.data_ptr()
+        d.nsrc_fields = len(src_fields)
+        for k, f in enumerate(src_fields):
+            d.src_fields[k] = f
+        d.nrec = self.nrec
+        d.rec_loc = self.rec.data_ptr()
+        d.nrec_fields = len(rec_fields)
+        for k, f in enumerate(rec_fields):
+            d.rec_fields[k] = f
+        return d
+
+    def vti3d_desc(self, models, wavelet, src_fields, rec_fields):
+        vp, eps, dlt, rho = models
+        d = _lib.VTI3DDesc()
+        d.B = self.B
+        d.nz, d.ny, d.nx = self.shape
+        d.nt = self.nt
+        d.M = self.M
+        for i in range(6):
+            d.pad[i] = self.pads[i]
+        d.dt = self.dt
+        d.dz, d.dy, d.dx = self.spacing
+        names = ("az", "bz", "azh", "bzh", "ay", "by", "ayh", "byh", "ax", "bx", "axh", "bxh")
+        for k, name in enumerate(names):
+            setattr(d, name, self.prof[k // 4][k % 4].data_ptr())
+        d.vp, d.epsilon, d.delta, d.rho = vp.data_ptr(), eps.data_ptr(), dlt.data_ptr(), rho.data_ptr()
+        d.model_stride = int(np.prod(self.shape)) if vp.dim() == 4 else 0
         d.nsrc = self.nsrc
         d.src_loc = self.src.data_ptr()
         d.wavelet = wavelet.data_ptr()
@@ -417,14 +448,15 @@ class _VTIFn(torch.autograd.Function):
         models = [m.contiguous() for m in (vp, eps, dlt, rho)]
         wavelet = wavelet.contiguous()
         sf, rf = fields
-        desc = geo.vti_desc(models, wavelet, sf, rf)
+        desc = geo.elastic_desc(models, wavelet, sf, rf)
+        pre = "sweep_b200_vti3d" if geo.ndim == 3 else "sweep_b200_vti"
         ws_b, tape_b = _lib.c_i64(), _lib.c_i64()
-        _lib.call("sweep_b200_vti_sizes", desc, mem_mode, ckpt_every, ws_b, tape_b)
+        _lib.call(pre + "_sizes", desc, mem_mode, ckpt_every, ws_b, tape_b)
         dev = vp.device
         ws = prop._workspace(ws_b.value, dev)
         tape = torch.empty(tape_b.value, dtype=torch.uint8, device=dev) if any(ctx.needs_input_grad[:4]) else None
         record = torch.empty((geo.B, geo.nt, geo.nrec, len(rf)), dtype=torch.float32, device=dev)
-        _lib.call("sweep_b200_vti_forward", desc, mem_mode, ckpt_every, record.data_ptr(),
+        _lib.call(pre + "_forward", desc, mem_mode, ckpt_every, record.data_ptr(),
                   tape.data_ptr() if tape is not None else None, ws.data_ptr(), ws.numel(), _stream_ptr(dev))
         ctx.save_for_backward(*models, wavelet)
         ctx.tape = tape
@@ -440,12 +472,13 @@ class _VTIFn(torch.autograd.Function):
         vp, eps, dlt, rho, wavelet = ctx.saved_tensors
         geo, prop = ctx.geo, ctx.prop
         adj = grad_record.to(torch.float32).contiguous()
-        desc = geo.vti_desc([vp, eps, dlt, rho], wavelet, *ctx.fields)
+        desc = geo.elastic_desc([vp, eps, dlt, rho], wavelet, *ctx.fields)
+        pre = "sweep_b200_vti3d" if geo.ndim == 3 else "sweep_b200_vti"
         ws_b, tape_b = _lib.c_i64(), _lib.c_i64()
-        _lib.call("sweep_b200_vti_sizes", desc, ctx.mem_mode, ctx.ckpt_every, ws_b, tape_b)
+        _lib.call(pre + "_sizes", desc, ctx.mem_mode, ctx.ckpt_every, ws_b, tape_b)
         ws = prop._workspace(ws_b.value, vp.device)
         g = [torch.empty_like(vp) for _ in range(4)]
-        _lib.call("sweep_b200_vti_backward", desc, ctx.mem_mode, ctx.ckpt_every, adj.data_ptr(),
+        _lib.call(pre + "_backward", desc, ctx.mem_mode, ctx.ckpt_every, adj.data_ptr(),
                   ctx.tape.data_ptr(), *[x.data_ptr() for x in g], ws.data_ptr(), ws.numel(),
                   _stream_ptr(vp.device))
         ctx.tape = None
@@ -498,7 +531,7 @@ class PropTorch(torch.nn.Module):
             raise NotImplementedError("sweep_b200: the absorbing faces need a layer (abcn >= 1)")
         self.fs_faces = free_faces(free_surface, nd)
         if isinstance(equation, AcousticVTI1st) and any(self.fs_faces):
-            raise NotImplementedError("AcousticVTI1st has no free surface (the reference refuses it too: the VTI "
+            raise NotImplementedError(f"{type(equation).__name__} has no free surface (the reference refuses it too: the VTI "
                                       "traction-free condition needs an anisotropic image method)")
         if nd == 3 and any(self.fs_faces[1:]):
             raise NotImplementedError("per-face free surfaces are 2-D only (as in the reference); "
@@ -605,7 +638,8 @@ class PropTorch(torch.nn.Module):
         name = "sweep_b200_acoustic_sizes"
         if fields is not None:
             name = ("sweep_b200_elastic3d_sizes" if isinstance(desc, _lib.Elastic3DDesc) else
-                    "sweep_b200_vti_sizes" if isinstance(desc, _lib.VTIDesc) else "sweep_b200_elastic_sizes")
+                    "sweep_b200_vti_sizes" if isinstance(desc, _lib.VTIDesc) else
+                    "sweep_b200_vti3d_sizes" if isinstance(desc, _lib.VTI3DDesc) else "sweep_b200_elastic_sizes")
         _lib.call(name, desc, mem_mode, ckpt_every, ws_b, tape_b)
         return int(tape_b.value)
 
@@ -648,6 +682,8 @@ class PropTorch(torch.nn.Module):
             return {"fixed": "one thread per cell, 32 x 8 cell tiles per z plane and shot"}
         if isinstance(desc, _lib.VTIDesc):
             return {"fixed": "one thread per cell, 32 x 8 cell tiles per shot"}
+        if isinstance(desc, _lib.VTI3DDesc):
+            return {"fixed": "one thread per cell, 32 x 8 cell tiles per z plane and shot"}
         if desc.M != 4:
             return {"fixed": f"order {2 * desc.M}: one thread per cell, 32 x 8 cell tiles per plane and shot"}
         return autotune.get_schedule(desc)
@@ -683,7 +719,7 @@ class PropTorch(torch.nn.Module):
         if isinstance(eq, AcousticVTI1st):
             if wavelet.requires_grad and torch.is_grad_enabled():
                 raise NotImplementedError(
-                    "impl='c' AcousticVTI1st does not return the wavelet gradient (its compiled backward "
+                    f"impl='c' {type(eq).__name__} does not return the wavelet gradient (its compiled backward "
                     "returns the model gradients only). Detach the wavelet.")
             return _VTIFn.apply(*padded, wb, self, geo, fields, mem_mode, ckpt_every)
         if isinstance(eq, Elastic):

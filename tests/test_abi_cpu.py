@@ -501,3 +501,52 @@ def test_vti_sizes_and_refusals():
         s.forward_runner(torch.zeros(50), src, rec, models)
     with pytest.raises(ValueError, match="source_type"):
         PropTorch(eq, shape=(30, 40), abcn=6, device="cpu", source_type=["sxx"])._elastic_fields()
+
+
+def test_vti3d_sizes_and_refusals():
+    """The 3-D acoustic VTI core sizes its workspace and tape on the host (the
+    tape: nt steps of five fields' band cells plus the five final fields),
+    takes every order 2 to 14, and refuses other memory modes, B * nz above
+    the grid limit, free surfaces and stepped runners."""
+    import torch
+    from sweep_b200 import AcousticVTI1st3D, PropTorch, _lib
+    eq = AcousticVTI1st3D()
+    assert eq.spatial_order == 4 and eq.FIELDS == ("vx", "vy", "vz", "sH", "sV")
+    assert eq.default_source_fields == ["sH", "sV"] and eq.default_receiver_fields == ["vz"]
+    shape = (10, 12, 14)
+    s = PropTorch(eq, shape=shape, dh=5.0, dt=5e-4, abcn=3, device="cpu", receiver_type=["vx", "vy", "sV"])
+    src, rec = np.array([[4, 5, 3]]), np.zeros((1, 4, 3), np.int64)
+    models = [torch.full(shape, 2000.0), torch.full(shape, 0.1), torch.full(shape, 0.05), torch.full(shape, 2000.0)]
+    geo, padded, wb, fields = s._probe(50, src, rec, models)
+    d = s._desc(geo, padded, wb, fields)
+    assert isinstance(d, _lib.VTI3DDesc) and d.M == 2 and list(d.pad) == [3] * 6
+    assert (d.nz, d.ny, d.nx) == (20, 22, 24) and list(d.rec_fields)[:3] == [0, 1, 4]
+    ws, tape = _lib.c_i64(), _lib.c_i64()
+    _lib.call("sweep_b200_vti3d_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
+    # band cells: the three face pairs (M + 1 = 3 deep) over the 10 x 12 x 14 box, each cell once
+    box = np.zeros((20, 22, 24), bool)
+    z0, y0, x0 = 5, 5, 5
+    for lo, hi in ((z0 - 2, z0 + 1), (z0 + 9, z0 + 12)):
+        box[lo:hi, y0:y0 + 12, x0:x0 + 14] = True
+    for lo, hi in ((y0 - 2, y0 + 1), (y0 + 11, y0 + 14)):
+        box[z0:z0 + 10, lo:hi, x0:x0 + 14] = True
+    for lo, hi in ((x0 - 2, x0 + 1), (x0 + 13, x0 + 16)):
+        box[z0:z0 + 10, y0:y0 + 12, lo:hi] = True
+    assert tape.value == 4 * (50 * 5 * int(box.sum()) + 5 * 20 * 22 * 24)
+    assert s.launch_schedule(50, src, rec, models) == {
+        "fixed": "one thread per cell, 32 x 8 cell tiles per z plane and shot"}
+    for mode in (_lib.MEM_CHECKPOINT, _lib.MEM_BOUNDARY_FP16):
+        with pytest.raises(RuntimeError, match="boundary saving with fp32 strips"):
+            _lib.call("sweep_b200_vti3d_sizes", d, mode, 10, ws, tape)
+    d.B = 4000
+    with pytest.raises(RuntimeError, match="65535"):
+        _lib.call("sweep_b200_vti3d_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
+    d.B, d.M = 1, 8
+    with pytest.raises(RuntimeError, match="orders 2 to 14"):
+        _lib.call("sweep_b200_vti3d_sizes", d, _lib.MEM_BOUNDARY, 0, ws, tape)
+    with pytest.raises(NotImplementedError, match="no free surface"):
+        PropTorch(eq, shape=shape, abcn=3, device="cpu", free_surface=True)
+    with pytest.raises(NotImplementedError, match="whole passes"):
+        s.forward_runner(torch.zeros(50), src, rec, models)
+    with pytest.raises(NotImplementedError, match="orders 2 to 14"):
+        PropTorch(AcousticVTI1st3D(spatial_order=16), shape=shape, abcn=3, device="cpu")
