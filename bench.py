@@ -621,8 +621,70 @@ class Elastic3DWorkload:
         return E3_RT[0] ** 3 * shots * nt_sample, time.perf_counter() - t0
 
 
+# 3-D acoustic VTI workload (--workload vti3d): the 3-D elastic survey's grid,
+# shots, receivers and wavelet (128^3, dh 10 m, dt 0.8 ms, nt 600, CPML 16,
+# 4 shots, vz receivers), vp the same dipping layers, Thomsen epsilon
+# 0.05-0.2 growing with vp, delta = epsilon / 2, rho = 310 vp^0.25; sources
+# on (sH, sV).  Algorithmic floats per runtime cell-step (one read and one
+# write of every field a kernel touches; CPML memories and the models not
+# counted): forward velocity step 2 stresses read + 3 velocities read and
+# written (8), stress step 3 + 4 (7); reverse: stress reconstruction 7,
+# half-step A pre-multiply 2 + 3 and apply 3 + 6, gradient 10 + 8 slots,
+# half-step B 3 + 3 and 3 + 4, velocity reconstruction 8 (60).
+V3_BYTES_FWD, V3_BYTES_REV = 4 * 15, 4 * 60
+
+
+def vti3d_survey(seed=SEED):
+    (vp, _, rho), (vp0, _, rho0), w, src, rec = elastic3d_survey(seed)
+    out = []
+    for v, r in ((vp, rho), (vp0, rho0)):
+        eps = (0.05 + 0.15 * (v - 1800.0) / 2400.0).astype(np.float32)
+        out.append([v, eps, (0.5 * eps).astype(np.float32), r])
+    return out[0], out[1], w, src, rec
+
+
+class VTI3DWorkload(Elastic3DWorkload):
+    name = "vti3d"
+    bytes_fwd, bytes_rev = V3_BYTES_FWD, V3_BYTES_REV
+    kernel = "sweep::vti3 reverse step (srev + premA + appA + grad + premB + appB + vrev + band restores)"
+    cpu_nt = 24
+
+    def config(self, args):
+        c = super().config(args)
+        c["workload"] = (f"vti3d (AcousticVTI1st3D) {E3_N}^3 (runtime {E3_RT[0]}^3), {E3_NSHOT} shots, "
+                         f"nt {E3_NT}, order {ORDER}, CPML {E3_ABCN}, vp/epsilon/delta/rho fwd+adj gradient, "
+                         f"boundary saving")
+        return c
+
+    def survey_inputs(self):
+        return vti3d_survey()
+
+    def build(self, dev):
+        from sweep_b200 import AcousticVTI1st3D, PropTorch
+        m_true, m_init, w, src, rec = vti3d_survey()
+        solver = PropTorch(AcousticVTI1st3D(spatial_order=ORDER, device=dev), shape=(E3_N,) * 3, dh=E3_DH,
+                           dt=E3_DT, abcn=E3_ABCN, device=dev, receiver_type=["vz"])
+        return solver, m_true, m_init, w, src, rec
+
+    def launches(self, group):
+        # forward 5 per step (velocity, stress, source, bands, record); reverse
+        # 11 (residuals, source removal, two reconstructions, two band
+        # restores, two pre-multiplies, two applies, gradient); prep per pass
+        # and four finalize
+        return 5 * self.nt + 11 * (self.nt - 1) + 6
+
+    def cpu_run(self, nt_sample, shots=1):
+        from oracle import oracle as O
+        m_true, m_init, w, src, rec = vti3d_survey()
+        w, src, rec = w[:nt_sample], src[:shots], rec[:shots]
+        obs = O.vti3d_forward(*m_true, w, src, rec, E3_DH, E3_DT, E3_ABCN, order=ORDER)
+        t0 = time.perf_counter()
+        O.vti3d_gradient(*m_init, w, src, rec, obs, E3_DH, E3_DT, E3_ABCN, order=ORDER)
+        return E3_RT[0] ** 3 * shots * nt_sample, time.perf_counter() - t0
+
+
 WORKLOADS = {"acoustic2d": AcousticWorkload, "acoustic2d_c1": AcousticC1Workload, "elastic2d": ElasticWorkload,
-             "vti2d": VTIWorkload,
+             "vti2d": VTIWorkload, "vti3d": VTI3DWorkload,
              "acoustic3d": Acoustic3DWorkload, "elastic3d": Elastic3DWorkload}
 
 
@@ -681,14 +743,14 @@ def reference_cuda(wl, group, nt_sample, dev, reps=2):
         sys.path.insert(0, str(REF_DIR))
     try:
         from sweep.equations import Acoustic, Acoustic3D, Elastic, Elastic3D
-        from sweep.equations.acoustic_vti_1st import AcousticVTI1st
+        from sweep.equations.acoustic_vti_1st import AcousticVTI1st, AcousticVTI1st3D
         from sweep.propagator.options import BoundarySaving
         from sweep.propagator.torch import PropTorch
     except Exception as e:                       # noqa: BLE001
         return {"unavailable": f"the reference does not import: {e}"}
     m_true, m_init, w, src, rec = wl.survey_inputs()
     eq = {"acoustic2d": Acoustic, "acoustic2d_c1": Acoustic, "elastic2d": Elastic, "vti2d": AcousticVTI1st,
-          "acoustic3d": Acoustic3D, "elastic3d": Elastic3D}[wl.name]
+          "acoustic3d": Acoustic3D, "elastic3d": Elastic3D, "vti3d": AcousticVTI1st3D}[wl.name]
     solver = PropTorch(eq(spatial_order=ORDER, device=dev), shape=tuple(m_true[0].shape), dh=wl.dh,
                        dt=wl.dt, abcn=wl.abcn, impl="c", device=dev, memory=BoundarySaving())
     wt = torch.tensor(w[:nt_sample], device=dev)
