@@ -21,8 +21,8 @@
 //     through the velocity step's transposed CPML; lambda_sH += -dt (D-x qx +
 //     D-y qy), lambda_sV += -dt D-z qz), velocity reconstruction, velocity
 //     bands.
-// One thread per cell on 32 x 8 (x, y) tiles, one z plane and shot per grid
-// row; stencils through the read-only path.
+// One thread per cell on 32 x 4 x 2 (x, y, z) blocks, two z planes of a shot
+// per grid row; stencils through the read-only path.
 // Layout: every field and memory (B, nz, ny, nx), x fastest; models and the
 // derived stiffness (B|1, nz, ny, nx).  Boundary bands: per face a band M + 1
 // wide from M cells outside the box, spanning the box along the other two
@@ -86,16 +86,18 @@ __device__ __forceinline__ float dminus(const float* __restrict__ u, long long i
     return g * inv;
 }
 
-// the thread's cell; o = the shot's offset, i = the cell within the shot
+// the thread's cell (32 x 4 x 2 blocks: two z planes of a shot per grid row);
+// o = the shot's offset, i = the cell within the shot
 __device__ __forceinline__ bool cell3(const Geo& G, int& b, int& iz, int& iy, int& ix, long long& o, long long& i)
 {
+    const int zb = (G.nz + 1) >> 1;
     ix = blockIdx.x * 32 + threadIdx.x;
-    iy = blockIdx.y * 8 + threadIdx.y;
-    b = blockIdx.z / G.nz;
-    iz = blockIdx.z - b * G.nz;
+    iy = blockIdx.y * 4 + threadIdx.y;
+    b = blockIdx.z / zb;
+    iz = (blockIdx.z - b * zb) * 2 + threadIdx.z;
     o = b * G.S;
     i = ((long long)iz * G.ny + iy) * G.nx + ix;
-    return ix < G.nx && iy < G.ny;
+    return ix < G.nx && iy < G.ny && iz < G.nz;
 }
 __device__ __forceinline__ bool core(const Geo& G, int ix, int iy, int iz)
 {
@@ -569,7 +571,7 @@ static void setup(const sweep_vti3d_desc* d, Plan& pl, const Ws& w, cudaStream_t
     SWEEP_CUDA(cudaMemsetAsync(w.zero0, 0, w.zero1 - w.zero0, st));
 }
 
-static dim3 grid_of(const Geo& G) { return dim3((G.nx + 31) / 32, (G.ny + 7) / 8, (unsigned)(G.B * G.nz)); }
+static dim3 grid_of(const Geo& G) { return dim3((G.nx + 31) / 32, (G.ny + 3) / 4, (unsigned)(G.B * ((G.nz + 1) / 2))); }
 static unsigned blocks(long long n) { return (unsigned)std::max<long long>(std::min<long long>((n + 255) / 256, 8192), 1); }
 
 template <int M>
@@ -589,7 +591,7 @@ static void forward_m(const sweep_vti3d_desc* d, Plan& pl, float* record, void* 
     for (int k = 0; k < NF; ++k) F.f[k] = w.f[k];
     for (int k = 0; k < NMEM; ++k) W.f[k] = w.m[k];
     float* tp = static_cast<float*>(tape);
-    const dim3 grid = grid_of(G), block(32, 8);
+    const dim3 grid = grid_of(G), block(32, 4, 2);
     for (int it = 0; it < G.nt; ++it) {
         vel<M><<<grid, block, 0, st>>>(G, F, W);
         str<M><<<grid, block, 0, st>>>(G, F, W);
@@ -630,7 +632,7 @@ static void backward_m(const sweep_vti3d_desc* d, Plan& pl, const float* adj, co
     for (int k = 0; k < NMEM; ++k) W.f[k] = w.m[k];
     const Scratch S{{w.s[0], w.s[1], w.s[2]}};
     const Grads g{w.gvp, w.geps, w.gdlt, w.grho};
-    const dim3 grid = grid_of(G), block(32, 8);
+    const dim3 grid = grid_of(G), block(32, 4, 2);
     const unsigned srcb = (unsigned)(G.B * G.nsrc + 127) / 128, recb = (unsigned)(G.B * G.nrec + 127) / 128;
     const unsigned bb = blocks((long long)G.B * G.ns);
     for (int it = G.nt - 1; it >= 1; --it) {

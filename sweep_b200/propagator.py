@@ -683,7 +683,7 @@ class PropTorch(torch.nn.Module):
         if isinstance(desc, _lib.VTIDesc):
             return {"fixed": "one thread per cell, 32 x 8 cell tiles per shot"}
         if isinstance(desc, _lib.VTI3DDesc):
-            return {"fixed": "one thread per cell, 32 x 8 cell tiles per z plane and shot"}
+            return {"fixed": "one thread per cell, 32 x 4 x 2 cell blocks, two z planes of a shot per grid row"}
         if desc.M != 4:
             return {"fixed": f"order {2 * desc.M}: one thread per cell, 32 x 8 cell tiles per plane and shot"}
         return autotune.get_schedule(desc)

@@ -534,7 +534,7 @@ def test_vti3d_sizes_and_refusals():
         box[z0:z0 + 10, y0:y0 + 12, lo:hi] = True
     assert tape.value == 4 * (50 * 5 * int(box.sum()) + 5 * 20 * 22 * 24)
     assert s.launch_schedule(50, src, rec, models) == {
-        "fixed": "one thread per cell, 32 x 8 cell tiles per z plane and shot"}
+        "fixed": "one thread per cell, 32 x 4 x 2 cell blocks, two z planes of a shot per grid row"}
     for mode in (_lib.MEM_CHECKPOINT, _lib.MEM_BOUNDARY_FP16):
         with pytest.raises(RuntimeError, match="boundary saving with fp32 strips"):
             _lib.call("sweep_b200_vti3d_sizes", d, mode, 10, ws, tape)
