@@ -28,13 +28,14 @@
 //     cap3, vrev3, strips3   v(it) carriers, velocity reconstruction,
 //               velocity strips of step it - 1                kernels.cuh:536-652
 //
-// One thread per cell on (32 x 8) tiles of x / y, one z plane and shot per
-// grid row; the stencils read global memory through the read-only path.  (A
-// z-marching variant with shared-memory planes and register z-queues, run at
-// two CTAs per SM without a load pipeline, measured 2.8x slower in the
-// forward; four cells of a column per thread with the z taps in a register
-// window, at three CTAs per SM, 1.23x slower; the kernels that beat this
-// layout need the 3-D acoustic kernels' TMA plane rings.)
+// One thread per cell on 32 x 4 x 2 (x, y, z) blocks, two z planes of a shot
+// per grid row (against 32 x 8 tiles of one plane: 4.47 against 4.2 Gcell/s);
+// the stencils read global memory through the read-only path.  (A z-marching
+// variant with shared-memory planes and register z-queues, run at two CTAs
+// per SM without a load pipeline, measured 2.8x slower in the forward; four
+// cells of a column per thread with the z taps in a register window, at
+// three CTAs per SM, 1.23x slower; the kernels that beat this layout need the
+// 3-D acoustic kernels' TMA plane rings.)
 // Layout: fields (B, nz, ny, nx), x fastest; CPML memories in per-axis slabs
 // covering the cells outside the box shrunk by one cell along their axis
 // (x: (B, nz, ny, WX), y: (B, nz, WY, nx), z: (B, WZ, ny, nx)).  Cells in the

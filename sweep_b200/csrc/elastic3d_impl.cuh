@@ -14,7 +14,7 @@ namespace sweep {
 namespace EL3D_NS {
 
 constexpr int M = EL3D_M;
-constexpr int NTHX = 32, NTHY = 8;
+constexpr int NTHX = 32, NTHY = 4, NTHZ = 2;
 
 // Staggered first-derivative weight k of order 2M (reference
 // operators/staggered.cuh:146-147 order 4, 248-250 order 6, 351-354 order 8;
@@ -209,14 +209,16 @@ __device__ __forceinline__ long long zsl(const Geo& G, int b, int iz, int iy, in
     return s < 0 ? -1 : (((long long)b * G.WZ + s) * G.ny + iy) * G.nx + ix;
 }
 
-// thread -> (b, iz, iy, ix); false past the grid
+// thread -> (b, iz, iy, ix) on NTHX x NTHY x NTHZ blocks (NTHZ z planes of a
+// shot per grid row); false past the grid
 __device__ __forceinline__ bool cell_of(const Geo& G, int& b, int& iz, int& iy, int& ix)
 {
+    const int zb = (G.nz + NTHZ - 1) / NTHZ;
     ix = blockIdx.x * NTHX + threadIdx.x;
     iy = blockIdx.y * NTHY + threadIdx.y;
-    b = blockIdx.z / G.nz;
-    iz = blockIdx.z - b * G.nz;
-    return ix < G.nx && iy < G.ny;
+    b = blockIdx.z / zb;
+    iz = (blockIdx.z - b * zb) * NTHZ + threadIdx.z;
+    return ix < G.nx && iy < G.ny && iz < G.nz;
 }
 
 // forward CPML memory update of derivative d along an axis: m = a m + b d,
@@ -238,7 +240,7 @@ struct Fwd {
 };
 
 template <bool FS>
-__global__ void __launch_bounds__(NTHX * NTHY) vel3(Fwd A)
+__global__ void __launch_bounds__(NTHX * NTHY * NTHZ) vel3(Fwd A)
 {
     const Geo& G = A.G;
     int b, iz, iy, ix;
@@ -274,7 +276,7 @@ __global__ void __launch_bounds__(NTHX * NTHY) vel3(Fwd A)
 }
 
 template <bool FS>
-__global__ void __launch_bounds__(NTHX * NTHY) str3(Fwd A)
+__global__ void __launch_bounds__(NTHX * NTHY * NTHZ) str3(Fwd A)
 {
     const Geo& G = A.G;
     int b, iz, iy, ix;
@@ -560,7 +562,7 @@ __global__ void rrho3(Rev A)
 }
 
 template <bool FS>
-__global__ void __launch_bounds__(NTHX * NTHY) srev3(Rev A)
+__global__ void __launch_bounds__(NTHX * NTHY * NTHZ) srev3(Rev A)
 {
     const Geo& G = A.G;
     int b, iz, iy, ix;
@@ -586,7 +588,7 @@ __global__ void __launch_bounds__(NTHX * NTHY) srev3(Rev A)
 }
 
 template <bool FS>
-__global__ void __launch_bounds__(NTHX * NTHY) vrev3(Rev A)
+__global__ void __launch_bounds__(NTHX * NTHY * NTHZ) vrev3(Rev A)
 {
     const Geo& G = A.G;
     int b, iz, iy, ix;
@@ -615,7 +617,7 @@ __device__ __forceinline__ float amem(float* __restrict__ m, long long at, float
 }
 
 template <bool FS>
-__global__ void __launch_bounds__(NTHX * NTHY) sprep3(Rev A)
+__global__ void __launch_bounds__(NTHX * NTHY * NTHZ) sprep3(Rev A)
 {
     const Geo& G = A.G;
     int b, iz, iy, ix;
@@ -690,7 +692,7 @@ __global__ void __launch_bounds__(NTHX * NTHY) sprep3(Rev A)
 }
 
 template <bool FS>
-__global__ void __launch_bounds__(NTHX * NTHY) sapp3(Rev A)
+__global__ void __launch_bounds__(NTHX * NTHY * NTHZ) sapp3(Rev A)
 {
     const Geo& G = A.G;
     int b, iz, iy, ix;
@@ -703,7 +705,7 @@ __global__ void __launch_bounds__(NTHX * NTHY) sapp3(Rev A)
     A.a[VZ][i] += dm(q[6], i, 1, G.idx) + dm(q[7], i, sy, G.idy) + adz_fs<FS, false>(G, q[8], i, iz, true, true);
 }
 
-__global__ void __launch_bounds__(NTHX * NTHY) vprep3(Rev A)
+__global__ void __launch_bounds__(NTHX * NTHY * NTHZ) vprep3(Rev A)
 {
     const Geo& G = A.G;
     int b, iz, iy, ix;
@@ -730,7 +732,7 @@ __global__ void __launch_bounds__(NTHX * NTHY) vprep3(Rev A)
 }
 
 template <bool FS>
-__global__ void __launch_bounds__(NTHX * NTHY) vapp3(Rev A)
+__global__ void __launch_bounds__(NTHX * NTHY * NTHZ) vapp3(Rev A)
 {
     const Geo& G = A.G;
     int b, iz, iy, ix;
@@ -747,7 +749,7 @@ __global__ void __launch_bounds__(NTHX * NTHY) vapp3(Rev A)
 }
 
 // v(it) carriers on the box (they hold v(it + 1) for the next reverse step)
-__global__ void __launch_bounds__(NTHX * NTHY) cap3(Rev A)
+__global__ void __launch_bounds__(NTHX * NTHY * NTHZ) cap3(Rev A)
 {
     const Geo& G = A.G;
     int b, iz, iy, ix;
@@ -1134,7 +1136,7 @@ static dim3 rec_grid(const Geo& G)
 
 static dim3 cell_grid(const Geo& G)
 {
-    return dim3((G.nx + NTHX - 1) / NTHX, (G.ny + NTHY - 1) / NTHY, (unsigned)(G.nz * G.B));
+    return dim3((G.nx + NTHX - 1) / NTHX, (G.ny + NTHY - 1) / NTHY, (unsigned)((G.nz + NTHZ - 1) / NTHZ * G.B));
 }
 
 static unsigned strip_blocks(const Geo& G)
@@ -1151,7 +1153,7 @@ static void forward_steps(const Fwd& A, int it0, int it1, StripsOf strips_of, in
     const Geo& G = A.G;
     Fields F{};
     for (int k = 0; k < NFLD; ++k) F.f[k] = A.f[k];
-    const dim3 grid = cell_grid(G), block(NTHX, NTHY);
+    const dim3 grid = cell_grid(G), block(NTHX, NTHY, NTHZ);
     const bool scaled = fmt == SF_F16 || fmt == SF_I8;
     for (int it = it0; it < it1; ++it) {
         if (G.fst) {
@@ -1266,7 +1268,7 @@ void backward(const sweep_elastic3d_desc* d, int mem_mode, int ckpt_every, const
     A.adj = adj;
     Fields F{};
     for (int k = 0; k < NFLD; ++k) F.f[k] = w.f[k];
-    const dim3 grid = cell_grid(G), block(NTHX, NTHY);
+    const dim3 grid = cell_grid(G), block(NTHX, NTHY, NTHZ);
     bool vsrc = false;
     for (int k = 0; k < G.nsf; ++k) vsrc |= G.sf[k] <= VZ;
     HostRing hr;

@@ -679,7 +679,7 @@ class PropTorch(torch.nn.Module):
         geo, padded, wb, fields = self._probe(wavelet_len, sources, receivers, models)
         desc = self._desc(geo, padded, wb, fields)
         if isinstance(desc, _lib.Elastic3DDesc):
-            return {"fixed": "one thread per cell, 32 x 8 cell tiles per z plane and shot"}
+            return {"fixed": "one thread per cell, 32 x 4 x 2 cell blocks, two z planes of a shot per grid row"}
         if isinstance(desc, _lib.VTIDesc):
             return {"fixed": "one thread per cell, 32 x 8 cell tiles per shot"}
         if isinstance(desc, _lib.VTI3DDesc):
